@@ -1,0 +1,424 @@
+"""Benchmark of the P-frame inter-analysis stage at 1080p (1920x1080, QP 27, 1 reference, 8 slice bands).
+
+One step = one P picture through the stage: the half-sample planes of its reference (K1) and the
+analysis of all 8160 macroblocks (P_Skip vector + SAD, best_inter with its motion searches; K2), in
+replay mode: each macroblock is analysed against its neighbours' final decisions (made beforehand by
+the stage's own auto mode, outside the timed region), so all macroblocks are independent.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+- ``value``: macroblocks per second over all ranks, inputs resident in device memory (device-pointer
+  entry points), K steps timed with CUDA events between a barrier + synchronize on both sides, the max
+  over ranks;
+- ``e2e``: the same through the host-buffer C ABI calls (ironav_set_source, ironav_push_reference,
+  ironav_analyse_picture_replay) from pinned host memory, copies included;
+- ``roofline``: the analysis kernel against the measured 32-bit integer issue rate; ``roofline_planes``:
+  the plane kernel against the measured HBM bandwidth;
+- ``cpu_baseline``: the C restatement of the reference's stage (oracle/) over all host cores on a
+  bounded sample of the same workload, rank 0 only.
+- ``--impl reference``: the reference's algorithm on the host cores (the oracle port: the Rust
+  reference cannot be built here), same workload and metric.
+
+Multi-GPU: the stage does not shard within a stream (each picture depends on the previous one and all
+slice bands read the whole reference), so N GPUs run N independent replicas (weak scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "1080p inter-analysis MB/s: plain bit-exact vs learned at ≤1% bitrate delta"
+WIDTH, HEIGHT, QP, NSLICES = 1920, 1080, 27, 8
+RING = 40  # frames in the ring: luma + decisions + results of the ring exceed the 126 MB L2
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--cpu-seconds", type=float, default=12.0, help="bound on the CPU baseline sample")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def dist_setup(args):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        from datetime import timedelta
+
+        backend = "nccl" if (args.impl == "ours" and torch.cuda.is_available()) else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=timedelta(seconds=120))
+    elif torch.cuda.is_available() and args.impl == "ours":
+        torch.cuda.set_device(0)
+    return rank, world, local
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = os.path.join("/tmp", f"ironav_clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            self.out = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.out, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.out.close()
+        sm, smax, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = max(smax, float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_frames(rank: int, n: int):
+    from ironav_b200.synth import CONFIGS, Sequence
+
+    w, h, seed, pan_q, nobj, vmax, sigma = CONFIGS["1080p"]
+    seq = Sequence(w, h, n, seed + 0x1000 * rank, pan_q, nobj, vmax, sigma)
+    return np.stack([seq.frame(t) for t in range(n)])
+
+
+def cpu_baseline(frames, states, seconds: float):
+    """The oracle (C restatement of the reference's stage) in replay mode over all host cores, on as
+    many of the ring's pictures as fit in `seconds`."""
+    from tests.oracle_lib import oracle_library
+    from ironav_b200.inter import InterStage
+
+    lib = oracle_library()
+    cores = os.cpu_count() or 1
+    st = InterStage(WIDTH, HEIGHT, nslices=NSLICES, lib=lib)
+    lib.oracle_set_threads(st.ctx, cores)
+    done_mb, elapsed, pics = 0, 0.0, 0
+    t = 1
+    while elapsed < seconds and t < len(frames):
+        st.clear_references()
+        st.push_reference(frames[t - 1], col=states[t - 1] if t >= 2 else None)
+        st.set_source(frames[t])
+        st.begin_p_picture(QP)
+        t0 = time.perf_counter()
+        st.analyse_replay(states[t])
+        elapsed += time.perf_counter() - t0
+        done_mb += st.nmb
+        pics += 1
+        t += 1
+    st.close()
+    return {"value": done_mb / elapsed, "unit": "MB/s", "cores": cores, "kind": "port",
+            "sample": f"{pics} pictures of the 1080p ring ({done_mb} macroblocks), replay mode, "
+                      f"{cores} threads, {elapsed:.2f} s; half-sample planes built outside the timing"}
+
+
+def run_reference(args, rank, world):
+    """The reference's algorithm on the host cores (the C port: the Rust reference cannot be built here)."""
+    if rank != 0:
+        return
+    from tests.oracle_lib import oracle_library
+    from ironav_b200.inter import InterStage
+
+    lib = oracle_library()
+    cores = os.cpu_count() or 1
+    nfr = args.steps + args.warmup + 2
+    frames = make_frames(0, min(nfr, RING))
+    # decisions of every picture by the oracle's own auto mode (the reference's slice loop)
+    st = InterStage(WIDTH, HEIGHT, nslices=NSLICES, lib=lib)
+    lib.oracle_set_threads(st.ctx, cores)
+    states = [None]
+    for t in range(1, len(frames)):
+        st.clear_references()
+        st.push_reference(frames[t - 1], col=states[t - 1])
+        st.set_source(frames[t])
+        st.begin_p_picture(QP)
+        s, _ = st.analyse_auto()
+        states.append(s)
+    times = []
+    for i in range(args.warmup + args.steps):
+        t = 1 + i % (len(frames) - 1)
+        st.clear_references()
+        t0 = time.perf_counter()
+        st.push_reference(frames[t - 1], col=states[t - 1])
+        st.set_source(frames[t])
+        st.begin_p_picture(QP)
+        st.analyse_replay(states[t])
+        dt = time.perf_counter() - t0
+        if i >= args.warmup:
+            times.append(dt)
+    total = sum(times)
+    value = st.nmb * len(times) / total
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "MB/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+        "data": "synthetic: seeded 4-octave value noise panned per frame + 8 moving rectangles, sigma 3",
+        "config": config_dict(),
+        "cpu_baseline": {"value": value, "unit": "MB/s", "cores": cores, "kind": "port",
+                         "sample": f"each step one 1080p picture (8160 macroblocks): planes + replay analysis, "
+                                   f"{cores} threads"},
+        "e2e": {"value": value, "unit": "MB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def config_dict():
+    return {"workload": "1080p P-picture inter analysis, replay mode: half-sample planes (K1) + all 8160 "
+                        "macroblocks' P_Skip test and best_inter (K2) per step",
+            "width": WIDTH, "height": HEIGHT, "qp": QP, "refs": 1, "slices": NSLICES, "mode": "replay",
+            "l2": f"inputs larger than L2: ring of {RING} pictures (luma, decisions, results ~140 MB)",
+            "parallelism": "replicas"}
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_setup(args)
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return finish(world)
+
+    import torch
+    import torch.distributed as dist
+    from ironav_b200.inter import MBRESULT_DTYPE, MBSTATE_DTYPE, InterStage, cuda_library
+
+    lib = cuda_library()
+    dev = torch.device("cuda", torch.cuda.current_device())
+    frames = make_frames(rank, RING)
+    stream = torch.cuda.Stream()
+    st = InterStage(WIDTH, HEIGHT, nslices=NSLICES, lib=lib)
+    st.set_stream(stream.cuda_stream)
+    nmb = st.nmb
+    d_frames = torch.from_numpy(frames).to(dev)
+    d_states = torch.zeros((RING, nmb * 72), dtype=torch.uint8, device=dev)
+    d_res = torch.zeros((RING, nmb * 104), dtype=torch.uint8, device=dev)
+    fp = lambda t: d_frames[t].data_ptr()
+    # decisions of every picture of the ring by the stage's auto mode (untimed set-up)
+    with torch.cuda.stream(stream):
+        for t in range(1, RING):
+            st.clear_references()
+            st.push_reference_device(fp(t - 1), WIDTH, WIDTH, HEIGHT, d_states[t - 1].data_ptr() if t >= 2 else None)
+            st.set_source_device(fp(t), WIDTH)
+            st.begin_p_picture(QP)
+            st.analyse_auto_device(d_states[t].data_ptr(), d_res[t].data_ptr())
+        st.sync()
+
+    def step(i, ev=None):
+        t = 1 + i % (RING - 1)
+        st.clear_references()
+        st.push_reference_device(fp(t - 1), WIDTH, WIDTH, HEIGHT, d_states[t - 1].data_ptr() if t >= 2 else None)
+        st.set_source_device(fp(t), WIDTH)
+        st.begin_p_picture(QP)
+        if ev is not None:
+            ev[0].record(stream)
+        st.analyse_replay_device(d_states[t].data_ptr(), d_res[t].data_ptr())
+        if ev is not None:
+            ev[1].record(stream)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    with torch.cuda.stream(stream):
+        for i in range(args.warmup):
+            step(i)
+        barrier()
+        clocks = Clocks(local)
+        clocks.start()
+        k2_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for i in range(args.steps):
+            step(args.warmup + i, k2_ev[i])
+        e1.record(stream)
+        barrier()
+        clk = clocks.stop()
+    st.sync()
+    ms = e0.elapsed_time(e1)
+    k2_ms = [a.elapsed_time(b) for a, b in k2_ev]
+    t_max = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
+    ms_max = float(t_max.item())
+    value = world * nmb * args.steps / (ms_max * 1e-3)
+
+    # algorithmic work of the timed launches (from the kernel's own per-macroblock counts)
+    ops = []
+    for i in range(args.steps):
+        t = 1 + (args.warmup + i) % (RING - 1)
+        r = d_res[t].cpu().numpy().view(MBRESULT_DTYPE)
+        ops.append(3.0 * r["sad_px"].astype(np.float64).sum() + 9.0 * r["satd_px"].astype(np.float64).sum())
+    k2_mean = float(np.mean(k2_ms))
+    achieved = float(np.mean(ops)) / (k2_mean * 1e-3) / 1e12
+    peak = ctypes_peak(lib)
+
+    # the plane kernel alone, for its HBM roofline (one launch per picture, timed in isolation)
+    planes_ms = time_planes(st, fp, stream, torch)
+    planes_bytes = WIDTH * HEIGHT + 4 * st.sw * st.sh  # luma read once + 4 planes written
+    hbm = measured_hbm()
+
+    # end to end through the host-buffer C ABI, pinned host memory
+    e2e = run_e2e(args, st, frames, d_states, nmb, world, torch, dist, dev, stream)
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "MB/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u8",
+        "data": "synthetic: seeded 4-octave value noise panned per frame + 8 moving rectangles, sigma 3",
+        "config": config_dict(),
+        "e2e": e2e,
+        "gpu_launches": 4 * args.steps,
+        "roofline": {"bound": "int32", "kernel": "analyse_kernel<false>", "achieved": achieved, "peak": peak,
+                     "unit": "Tops/s", "frac": achieved / peak if peak else None, "traffic": None,
+                     "ms_per_launch": k2_mean,
+                     "note": "achieved = algorithmic ops (3 per SAD sample, 9 per SATD sample, counted by the "
+                             "kernel in the reference's evaluation order) / event time; peak = measured 32-bit "
+                             "integer issue rate (add+xor chains on every SM)"},
+        "roofline_planes": {"bound": "hbm", "kernel": "halfpel_planes_kernel",
+                            "achieved": planes_bytes / (planes_ms * 1e-3) / 1e9, "peak": hbm[0], "unit": "GB/s",
+                            "frac": planes_bytes / (planes_ms * 1e-3) / 1e9 / hbm[0], "peak_source": hbm[1],
+                            "ms_per_launch": planes_ms, "traffic": None},
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        host_states = [None] + [d_states[t].cpu().numpy().view(MBSTATE_DTYPE) for t in range(1, RING)]
+        line["cpu_baseline"] = cpu_baseline(frames, host_states, args.cpu_seconds)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    st.close()
+    return finish(world)
+
+
+def ctypes_peak(lib):
+    import ctypes
+
+    v = ctypes.c_double()
+    f = lib.ironav_measure_int32_peak
+    f.argtypes = [ctypes.POINTER(ctypes.c_double)]
+    return v.value if f(ctypes.byref(v)) == 0 else None
+
+
+def measured_hbm():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs (measured)"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback 6.65 TB/s"
+
+
+def time_planes(st, fp, stream, torch, n=20):
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(n)]
+    with torch.cuda.stream(stream):
+        for i in range(n):
+            st.clear_references()
+            evs[i][0].record(stream)
+            st.push_reference_device(fp(i % RING), WIDTH, WIDTH, HEIGHT, None)
+            evs[i][1].record(stream)
+        st.sync()
+    return float(np.mean([a.elapsed_time(b) for a, b in evs[3:]]))
+
+
+def run_e2e(args, st, frames, d_states, nmb, world, torch, dist, dev, stream):
+    """The same steps through the host-buffer ABI: source, reference and decisions copied in from pinned
+    memory, results copied out, every step."""
+    from ironav_b200.inter import MBRESULT_DTYPE, MBSTATE_DTYPE
+
+    n = min(RING, 12)
+    pin_frames = torch.from_numpy(frames[:n]).pin_memory()
+    pin_states = d_states[:n].cpu().pin_memory()
+    pin_out = torch.zeros((nmb * 104,), dtype=torch.uint8).pin_memory()
+    fr = pin_frames.numpy()
+    stv = pin_states.numpy()
+    out = pin_out.numpy().view(MBRESULT_DTYPE)
+    lib = st.lib
+    import ctypes
+
+    def step(i):
+        t = 1 + i % (n - 1)
+        lib.ironav_clear_references(st.ctx)
+        col = stv[t - 1].ctypes.data if t >= 2 else None
+        s = lib.ironav_push_reference(st.ctx, fr[t - 1].ctypes.data, WIDTH, WIDTH, HEIGHT, col)
+        s |= lib.ironav_set_source(st.ctx, fr[t].ctypes.data, WIDTH)
+        s |= lib.ironav_begin_p_picture(st.ctx, QP, lib.ironav_lambda(QP), lib.ironav_skip_threshold(QP), 1, 0, 0)
+        s |= lib.ironav_analyse_picture_replay(st.ctx, stv[t].ctypes.data, out.ctypes.data)
+        if s:
+            raise RuntimeError(f"e2e step failed: {s}")
+
+    for i in range(args.warmup):
+        step(i)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        step(args.warmup + i)
+    torch.cuda.synchronize()
+    el = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(el, op=dist.ReduceOp.MAX)
+    el = float(el.item())
+    return {"value": world * nmb * args.steps / el, "unit": "MB/s",
+            "h2d_bytes_per_step": 2 * WIDTH * HEIGHT + 2 * nmb * 72, "d2h_bytes_per_step": nmb * 104,
+            "ms_per_step": 1e3 * el / args.steps,
+            "note": "host-buffer C ABI calls (each returns when its work is done), pinned host memory; "
+                    "wall clock around K steps, max over ranks"}
+
+
+def finish(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,164 @@
+/*
+ * ironav_inter.h — C ABI of the P-picture inter-analysis stage of IronAV's software H.264 encoder
+ * (crate ironav-codec, module h264::enc), re-implemented for NVIDIA B200 (sm_100a).
+ *
+ * The stage covers:
+ *   - the half-sample planes of each reference picture      (HalfPel::new, enc/subpel.rs:42-115)
+ *   - the P_Skip vector and its SAD                          (code_mb, enc/frame.rs:722-729; skip_mv 597-603)
+ *   - the inter partition decision with motion search       (best_inter, enc/frame.rs:839-938;
+ *                                                             motion_search 949-1019)
+ * and nothing after it: the rate-distortion choice against intra, residual coding and entropy
+ * coding stay with the caller (code_mb, enc/frame.rs:752-790; decide_rd 1462-1513).
+ *
+ * Two libraries implement this header:
+ *   libironav_inter_cuda.so  the product: CUDA kernels for sm_100a (ironav_b200/).
+ *   libironav_inter_cpu.so   the CPU restatement used as the parity checker (oracle/).
+ * A caller switches between them by linking the other library; every entry point, argument and
+ * status code means the same in both.
+ *
+ * Conventions
+ *   - Plain C types, caller-owned host buffers unless a name ends in _device (device pointers,
+ *     work queued on the context's stream, no host synchronisation).
+ *   - Vectors are in quarter luma samples, (x, y), int16, exactly as the encoder keeps them.
+ *   - Macroblocks are numbered in raster order, mb_w * mb_h of them, mb_w = ceil(width / 16).
+ *   - Every entry point returns an ironav_status; none throws, none aborts.
+ *   - A context is not thread-safe; many contexts may live in one process.
+ */
+#ifndef IRONAV_INTER_H
+#define IRONAV_INTER_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes: 1 + the index of ironav_core::ErrorCode (crates/ironav-core/src/error.rs:9-27), so a
+ * Rust binding maps them back with ErrorCode::ALL[status - 1]. IRONAV_TIMEOUT has no counterpart
+ * there (the reference never waits on another device); a binding maps it to ErrorCode::Internal. */
+typedef enum ironav_status {
+    IRONAV_OK = 0,
+    IRONAV_INVALID_INPUT = 2,         /* ErrorCode::InvalidInput: a frame or state that does not fit the context */
+    IRONAV_INVALID_ARGUMENT = 3,      /* ErrorCode::InvalidArgument: bad sizes, null pointers, out-of-range params */
+    IRONAV_HARDWARE_UNAVAILABLE = 8,  /* ErrorCode::HardwareUnavailable: no CUDA device / kernels not loadable */
+    IRONAV_INTERNAL = 13,             /* ErrorCode::Internal: a CUDA call failed */
+    IRONAV_TIMEOUT = 100              /* a bounded device-side wait gave up (wavefront dependency never published) */
+} ironav_status;
+
+/* What later macroblocks need to know about a decided one: the list-0 subset of MbState
+ * (enc/frame.rs:246-272) that the vector predictors read (nb_motion, enc/frame.rs:522-538), and, for
+ * the newest reference picture, what col_mv (enc/frame.rs:944-947) reads of MbInfo (h264/mb.rs:34-64). */
+typedef struct ironav_mbstate {
+    uint8_t inter;        /* Kind::Inter (P_L0_*, P_8x8 and P_Skip); 0 for intra or not coded */
+    int8_t refs[4];       /* refs[0]: ref_idx_l0 per 8x8 block, -1 for none */
+    uint8_t pad[3];
+    int16_t mvs[16][2];   /* list-0 vector per 4x4 block, raster order */
+} ironav_mbstate;         /* 72 bytes */
+
+/* The stage's answer for one macroblock. */
+typedef struct ironav_mbresult {
+    int16_t skip_mv[2];   /* P_Skip vector (8.4.1.1), skip_mv enc/frame.rs:597-603 */
+    int32_t skip_sad;     /* SAD of the 16x16 P_Skip prediction against the source, enc/frame.rs:725-729 */
+    uint8_t part;         /* best_inter: 0 16x16, 1 16x8, 2 8x16, 3 8x8 (PARTS, enc/frame.rs:182) */
+    uint8_t refs[4];      /* best_inter: reference index of each partition / 8x8 block */
+    uint8_t sub[4];       /* best_inter: sub_mb_type of each 8x8 block of P_8x8 (SUB, enc/frame.rs:204) */
+    uint8_t flags;        /* IRONAV_RESULT_* below */
+    uint8_t pad[2];
+    int32_t cost;         /* best_inter: SATD + lambda * (mv, mb_type, ref bits) of the winner */
+    int16_t mvs[16][2];   /* best_inter: vector of each partition in coding order (rects, enc/frame.rs:208-213) */
+    int32_t cost16;       /* the 16x16 candidate's cost for the winning reference */
+    uint32_t sad_px;      /* samples compared by integer SAD evaluations in the reference's order (work count) */
+    uint32_t satd_px;     /* samples compared by sub-sample SATD evaluations (work count) */
+    uint32_t pad2;
+} ironav_mbresult;        /* 112 bytes */
+
+#define IRONAV_RESULT_INTER 1u   /* best_inter was evaluated (fields part..cost16 are valid) */
+#define IRONAV_RESULT_SKIP  2u   /* auto policy only: the macroblock was decided as P_Skip */
+
+/* ---- host helpers (f64 arithmetic that the reference does on the host) -------------------------- */
+
+/* lambda(qp') = max(1, round(2^((qp' - 12) / 6))), enc/frame.rs:164-166. */
+int ironav_lambda(int qp_prime);
+/* Smallest integer T with (sad < T) <=> (sad as f64 < 256 * 0.625 * 2^(qp'/6)), the P_Skip test of
+ * enc/frame.rs:730,742 rewritten on integers. */
+int ironav_skip_threshold(int qp_prime);
+/* Bits of se(v) / ue(v) Exp-Golomb codes, enc/bitw.rs:81-89. */
+int ironav_se_bits(int v);
+int ironav_ue_bits(unsigned v);
+/* Version string of the implementation ("cuda-sm_100a ..." or "cpu-oracle ..."). */
+const char* ironav_version(void);
+
+/* ---- context -------------------------------------------------------------------------------------- */
+
+typedef struct ironav_ctx ironav_ctx;
+
+/* One stream: width x height 8-bit luma (even, mb_w and mb_h <= 1024 like H264Encoder::new,
+ * enc/mod.rs:143-152), up to max_refs reference pictures (1..16, with_refs enc/mod.rs:265-268), and
+ * nslices slice bands. band_rows holds nslices + 1 macroblock-row boundaries, or is NULL for the
+ * encoder's own split, band i = [i*mb_h/n, (i+1)*mb_h/n) (enc/mod.rs:603). Neighbours in an earlier
+ * band are unavailable to the vector predictors (nb_state, enc/frame.rs:509-515). */
+int ironav_ctx_create(ironav_ctx** out, int width, int height, int bd, int max_refs, int nslices,
+                      const int* band_rows);
+int ironav_ctx_destroy(ironav_ctx* ctx);
+/* Geometry: mb_w, mb_h, and the padded plane size sw x sh of each half-sample plane
+ * (sw = 16*mb_w + 96, sh = 16*mb_h + 96, PAD = 48 on each side, enc/subpel.rs:7). */
+int ironav_ctx_dims(const ironav_ctx* ctx, int* mb_w, int* mb_h, int* sw, int* sh);
+/* Makes the context queue its device work on this cudaStream_t (NULL: the legacy default stream). */
+int ironav_ctx_set_stream(ironav_ctx* ctx, void* cuda_stream);
+
+/* The picture to analyse: width x height luma rows `stride` bytes apart, padded to whole macroblocks by
+ * repeating its right and bottom edges (H264Encoder::source, enc/mod.rs:481-529). */
+int ironav_set_source(ironav_ctx* ctx, const uint8_t* y, int stride);
+
+/* Adds the newest reference picture (a decoded/reconstructed luma plane) and builds its half-sample
+ * planes (HalfPel::new, enc/subpel.rs:42-115; the reference list, enc/mod.rs:551-559,660-666). w x h is
+ * either the picture size (edges repeated to whole macroblocks) or the macroblock-aligned size
+ * 16*mb_w x 16*mb_h (a reconstruction, used as is). col holds the picture's own macroblock decisions
+ * (mb_w*mb_h), read for the co-located candidate (col_mv, enc/frame.rs:944-947), or NULL when the
+ * picture was intra coded. The oldest reference is dropped once max_refs are held. */
+int ironav_push_reference(ironav_ctx* ctx, const uint8_t* y, int stride, int w, int h,
+                          const ironav_mbstate* col);
+/* Forgets every reference (an IDR picture, enc/mod.rs:541-545). */
+int ironav_clear_references(ironav_ctx* ctx);
+/* Copies reference `idx` (0 = newest) planes G, b, h, j to out (4 * sw * sh bytes), for checks. */
+int ironav_get_planes(ironav_ctx* ctx, int idx, uint8_t* out);
+
+/* Parameters of the P picture to analyse (FrameCoder::new / with_sub8x8 / with_fast,
+ * enc/frame.rs:381-440): qp_prime = QP'Y; lambda and skip_thresh from the helpers above (the host
+ * works them out in f64 like the reference); nrefs_active = list-0 length (enc/mod.rs:559);
+ * fast = H264Encoder::realtime's shorter search; sub8 = sub-partitions of P_8x8 searched. */
+int ironav_begin_p_picture(ironav_ctx* ctx, int qp_prime, int lambda, int skip_thresh, int nrefs_active,
+                           int fast, int sub8);
+
+/* Replay mode: final_states holds every macroblock's final decision (mb_w*mb_h), as the caller's
+ * mode decision made it; each macroblock is analysed against its neighbours' final states, so all
+ * macroblocks are independent. out receives mb_w*mb_h results, with P_Skip and best_inter for every
+ * macroblock. */
+int ironav_analyse_picture_replay(ironav_ctx* ctx, const ironav_mbstate* final_states,
+                                  ironav_mbresult* out);
+
+/* Auto mode: the stage decides every macroblock itself with the analysis policy (P_Skip when
+ * skip_sad < skip_thresh, else the best_inter result) and the macroblocks follow their left, top and
+ * top-right neighbours' decisions in a wavefront within each slice band. out_states receives the
+ * decisions (usable as the next picture's col and as replay input). */
+int ironav_analyse_picture_auto(ironav_ctx* ctx, ironav_mbstate* out_states, ironav_mbresult* out);
+
+/* ---- device-resident forms (pointers in device memory; asynchronous on the context's stream) ------ */
+
+int ironav_set_source_device(ironav_ctx* ctx, const uint8_t* d_y, int stride);
+int ironav_push_reference_device(ironav_ctx* ctx, const uint8_t* d_y, int stride, int w, int h,
+                                 const ironav_mbstate* d_col);
+int ironav_analyse_picture_replay_device(ironav_ctx* ctx, const ironav_mbstate* d_final_states,
+                                         ironav_mbresult* d_out);
+int ironav_analyse_picture_auto_device(ironav_ctx* ctx, ironav_mbstate* d_out_states,
+                                       ironav_mbresult* d_out);
+/* Waits for the context's queued work; returns a pending device error (IRONAV_TIMEOUT for a wavefront
+ * wait that gave up). */
+int ironav_ctx_sync(ironav_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* IRONAV_INTER_H */

@@ -1,0 +1,44 @@
+// common.cuh — shared definitions of the sm_100a inter-analysis kernels.
+#pragma once
+#include <cstdint>
+
+#include "../../include/ironav_inter.h"
+
+namespace ironav {
+
+constexpr int PAD = 48;        // border kept around each half-sample plane (enc/subpel.rs:7)
+constexpr int MAX_REFS = 16;   // list-0 length limit (with_refs, enc/mod.rs:265-268)
+
+// The co-located candidate of one macroblock of the newest reference picture (col_mv,
+// enc/frame.rs:944-947): mvs[5] of an inter macroblock.
+struct ColMv {
+    int16_t mv[2];
+    int32_t valid;
+};
+
+// Everything one analysis launch reads and writes. Passed by value (kernel parameter space).
+struct AnalyseParams {
+    const uint8_t* src;               // padded source luma, pw x ph, rows ls bytes apart
+    int ls;
+    const uint8_t* planes[MAX_REFS];  // reference r (0 = newest): G, b, h, j planes, plane k at k * psize
+    long long psize;
+    int sw;                           // plane stride (pw + 2 * PAD)
+    const ColMv* col;                 // newest reference's co-located vectors (mb_w * mb_h)
+    int mb_w, mb_h, pw, ph;
+    int nact, lambda, skip_thresh, fast, sub8;
+    const int* band_start;            // per macroblock row: first row of its slice band
+    const ironav_mbstate* states_in;  // replay mode: final decisions of every macroblock
+    ironav_mbstate* states_out;       // auto mode: decisions written here
+    ironav_mbresult* results;
+    // work distribution and the wavefront's progress flags (auto mode)
+    const int* order;                 // ticket -> macroblock index
+    unsigned* ticket;                 // next ticket
+    unsigned* flags;                  // per macroblock: epoch when its decision is published
+    unsigned epoch;
+    unsigned* err;                    // nonzero: a wait gave up (1) or an index left its plane (2)
+    int nmb;
+    int withhold;                     // test hook: this macroblock's flag is never published (-1: none)
+    unsigned wait_limit;              // polls before a wavefront wait gives up
+};
+
+}  // namespace ironav

@@ -1,0 +1,416 @@
+// ironav_inter.cu — the C ABI of include/ironav_inter.h on B200 (sm_100a).
+//
+// A context owns, in device memory: the padded source luma, one slot per reference picture (its
+// four half-sample planes and co-located vectors), the analysis results and decisions, and the
+// wavefront's progress flags. Host-buffer entry points copy in, run the kernels and copy out on the
+// context's stream and return when done; *_device entry points only queue work.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "analyse.cuh"
+#include "planes.cuh"
+#include "peaks.cuh"
+
+using namespace ironav;
+
+static_assert(sizeof(ironav_mbstate) == 72, "ironav_mbstate layout");
+static_assert(sizeof(ironav_mbresult) == 104, "ironav_mbresult layout");
+
+struct ironav_ctx {
+    int width = 0, height = 0, bd = 8, mb_w = 0, mb_h = 0, pw = 0, ph = 0, sw = 0, sh = 0;
+    int max_refs = 0, nslices = 0, nmb = 0;
+    int device = 0, nsm = 0, k2_blocks = 0;
+    cudaStream_t stream = nullptr;
+    long long psize = 0;
+    uint8_t* d_src = nullptr;
+    uint8_t* d_stage = nullptr;  // reference luma as given, rows pw apart
+    uint8_t* d_planes[MAX_REFS] = {};
+    ColMv* d_col[MAX_REFS] = {};
+    int slot_of[MAX_REFS] = {};  // reference index (0 = newest) -> slot
+    int nrefs = 0;
+    int* d_band_start = nullptr;
+    int* d_order = nullptr;
+    unsigned* d_flags = nullptr;
+    unsigned* d_counters = nullptr;  // [0] ticket, [1] error
+    unsigned epoch = 0;
+    ironav_mbstate* d_states = nullptr;
+    ironav_mbstate* d_col_stage = nullptr;
+    ironav_mbresult* d_results = nullptr;
+    // picture parameters
+    int qpp = 0, lambda = 0, skip_thresh = 0, nact = 0, fast = 0, sub8 = 0;
+    bool have_params = false;
+    int withhold = -1;
+    unsigned wait_limit = 1u << 22;
+};
+
+namespace {
+
+int cuda_status(cudaError_t e) {
+    if (e == cudaSuccess) return IRONAV_OK;
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver || e == cudaErrorNoKernelImageForDevice)
+        return IRONAV_HARDWARE_UNAVAILABLE;
+    return IRONAV_INTERNAL;
+}
+
+#define CK(x)                                  \
+    do {                                       \
+        cudaError_t e_ = (x);                  \
+        if (e_ != cudaSuccess) return cuda_status(e_); \
+    } while (0)
+
+void free_ctx(ironav_ctx* c) {
+    cudaFree(c->d_src);
+    cudaFree(c->d_stage);
+    for (int i = 0; i < MAX_REFS; i++) {
+        cudaFree(c->d_planes[i]);
+        cudaFree(c->d_col[i]);
+    }
+    cudaFree(c->d_band_start);
+    cudaFree(c->d_order);
+    cudaFree(c->d_flags);
+    cudaFree(c->d_counters);
+    cudaFree(c->d_states);
+    cudaFree(c->d_col_stage);
+    cudaFree(c->d_results);
+    delete c;
+}
+
+int launch_planes(ironav_ctx* c, const uint8_t* d_luma, int stride, int w, int h, const ironav_mbstate* d_col) {
+    // the new picture takes the slot of the oldest (dropped) one, or a free one
+    int slot;
+    if (c->nrefs == c->max_refs) {
+        slot = c->slot_of[c->max_refs - 1];
+        c->nrefs--;
+    } else {
+        bool used[MAX_REFS] = {};
+        for (int i = 0; i < c->nrefs; i++) used[c->slot_of[i]] = true;
+        slot = 0;
+        while (used[slot]) slot++;
+    }
+    for (int i = c->nrefs; i > 0; i--) c->slot_of[i] = c->slot_of[i - 1];
+    c->slot_of[0] = slot;
+    c->nrefs++;
+    dim3 grid((c->sw + K1_TW - 1) / K1_TW, (c->sh + K1_TH - 1) / K1_TH);
+    halfpel_planes_kernel<<<grid, K1_THREADS, 0, c->stream>>>(d_luma, stride, w, h, c->d_planes[slot], c->psize, c->sw, c->sh);
+    col_extract_kernel<<<(c->nmb + 255) / 256, 256, 0, c->stream>>>(d_col, c->d_col[slot], c->nmb);
+    return cuda_status(cudaGetLastError());
+}
+
+int launch_analyse(ironav_ctx* c, bool auto_mode, const ironav_mbstate* d_in, ironav_mbstate* d_out, ironav_mbresult* d_res) {
+    AnalyseParams p;
+    memset(&p, 0, sizeof(p));
+    p.src = c->d_src;
+    p.ls = c->pw;
+    for (int i = 0; i < c->nact; i++) p.planes[i] = c->d_planes[c->slot_of[i]];
+    p.psize = c->psize;
+    p.sw = c->sw;
+    p.col = c->d_col[c->slot_of[0]];
+    p.mb_w = c->mb_w;
+    p.mb_h = c->mb_h;
+    p.pw = c->pw;
+    p.ph = c->ph;
+    p.nact = c->nact;
+    p.lambda = c->lambda;
+    p.skip_thresh = c->skip_thresh;
+    p.fast = c->fast;
+    p.sub8 = c->sub8;
+    p.band_start = c->d_band_start;
+    p.states_in = d_in;
+    p.states_out = d_out;
+    p.results = d_res;
+    p.order = auto_mode ? c->d_order : nullptr;
+    p.ticket = c->d_counters;
+    p.flags = c->d_flags;
+    p.err = c->d_counters + 1;
+    p.nmb = c->nmb;
+    p.withhold = c->withhold;
+    p.wait_limit = c->wait_limit;
+    if (auto_mode) p.epoch = ++c->epoch;
+    CK(cudaMemsetAsync(c->d_counters, 0, 2 * sizeof(unsigned), c->stream));
+    if (auto_mode)
+        analyse_kernel<true><<<c->k2_blocks, K2_WARPS * 32, 0, c->stream>>>(p);
+    else
+        analyse_kernel<false><<<c->k2_blocks, K2_WARPS * 32, 0, c->stream>>>(p);
+    return cuda_status(cudaGetLastError());
+}
+
+int check_device_error(ironav_ctx* c) {
+    unsigned err = 0;
+    CK(cudaMemcpyAsync(&err, c->d_counters + 1, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (err & 1u) return IRONAV_TIMEOUT;
+    if (err) return IRONAV_INTERNAL;
+    return IRONAV_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ironav_lambda(int qp) {  // enc/frame.rs:164-166
+    int l = (int)std::lround(std::pow(2.0, ((double)qp - 12.0) / 6.0));
+    return l < 1 ? 1 : l;
+}
+
+int ironav_skip_threshold(int qpp) {  // enc/frame.rs:730,742
+    return (int)std::ceil(256.0 * 0.625 * std::pow(2.0, (double)qpp / 6.0));
+}
+
+int ironav_ue_bits(unsigned v) { return 2 * (32 - __builtin_clz(v + 1)) - 1; }  // enc/bitw.rs:81-83
+
+int ironav_se_bits(int v) {  // enc/bitw.rs:86-89
+    return ironav_ue_bits(v > 0 ? 2u * (unsigned)v - 1u : (unsigned)(-2 * (long long)v));
+}
+
+const char* ironav_version(void) { return "cuda-sm_100a ironav-inter-b200 0.1 (K1 halfpel_planes, K2 analyse)"; }
+
+int ironav_ctx_create(ironav_ctx** out, int width, int height, int bd, int max_refs, int nslices, const int* band_rows) {
+    if (!out) return IRONAV_INVALID_ARGUMENT;
+    *out = nullptr;
+    if (width <= 0 || height <= 0 || (width & 1) || (height & 1) || bd != 8) return IRONAV_INVALID_ARGUMENT;
+    const int mb_w = (width + 15) / 16, mb_h = (height + 15) / 16;
+    if (mb_w > 1024 || mb_h > 1024 || max_refs < 1 || max_refs > MAX_REFS || nslices < 1 || nslices > mb_h)
+        return IRONAV_INVALID_ARGUMENT;
+    std::vector<int> bands(nslices + 1);
+    for (int i = 0; i <= nslices; i++) bands[i] = band_rows ? band_rows[i] : i * mb_h / nslices;
+    if (bands[0] != 0 || bands[nslices] != mb_h) return IRONAV_INVALID_ARGUMENT;
+    for (int i = 0; i < nslices; i++)
+        if (bands[i + 1] <= bands[i]) return IRONAV_INVALID_ARGUMENT;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return IRONAV_HARDWARE_UNAVAILABLE;
+    }
+    ironav_ctx* c = new ironav_ctx();
+    c->width = width;
+    c->height = height;
+    c->mb_w = mb_w;
+    c->mb_h = mb_h;
+    c->pw = mb_w * 16;
+    c->ph = mb_h * 16;
+    c->sw = c->pw + 2 * PAD;
+    c->sh = c->ph + 2 * PAD;
+    c->max_refs = max_refs;
+    c->nslices = nslices;
+    c->nmb = mb_w * mb_h;
+    c->psize = (long long)c->sw * c->sh;
+    auto fail = [&](cudaError_t e) {
+        int s = cuda_status(e);
+        free_ctx(c);
+        return s;
+    };
+    cudaError_t e = cudaGetDevice(&c->device);
+    if (e != cudaSuccess) return fail(e);
+    cudaDeviceProp prop;
+    if ((e = cudaGetDeviceProperties(&prop, c->device)) != cudaSuccess) return fail(e);
+    c->nsm = prop.multiProcessorCount;
+    int per_sm = 0;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, analyse_kernel<true>, K2_WARPS * 32, 0)) != cudaSuccess) return fail(e);
+    c->k2_blocks = std::max(1, per_sm) * c->nsm;
+    const size_t slack = 256;  // word-granular reads may touch a few bytes past a plane's last sample
+    if ((e = cudaMalloc(&c->d_src, (size_t)c->pw * c->ph + slack)) != cudaSuccess) return fail(e);
+    if ((e = cudaMalloc(&c->d_stage, (size_t)c->pw * c->ph + slack)) != cudaSuccess) return fail(e);
+    for (int i = 0; i < max_refs; i++) {
+        if ((e = cudaMalloc(&c->d_planes[i], 4 * (size_t)c->psize + slack)) != cudaSuccess) return fail(e);
+        if ((e = cudaMalloc(&c->d_col[i], sizeof(ColMv) * c->nmb)) != cudaSuccess) return fail(e);
+    }
+    if ((e = cudaMalloc(&c->d_band_start, sizeof(int) * mb_h)) != cudaSuccess) return fail(e);
+    if ((e = cudaMalloc(&c->d_order, sizeof(int) * c->nmb)) != cudaSuccess) return fail(e);
+    if ((e = cudaMalloc(&c->d_flags, sizeof(unsigned) * c->nmb)) != cudaSuccess) return fail(e);
+    if ((e = cudaMalloc(&c->d_counters, sizeof(unsigned) * 2)) != cudaSuccess) return fail(e);
+    if ((e = cudaMalloc(&c->d_states, sizeof(ironav_mbstate) * c->nmb)) != cudaSuccess) return fail(e);
+    if ((e = cudaMalloc(&c->d_col_stage, sizeof(ironav_mbstate) * c->nmb)) != cudaSuccess) return fail(e);
+    if ((e = cudaMalloc(&c->d_results, sizeof(ironav_mbresult) * c->nmb)) != cudaSuccess) return fail(e);
+    if ((e = cudaMemset(c->d_flags, 0, sizeof(unsigned) * c->nmb)) != cudaSuccess) return fail(e);
+    // per row: its band's first row; tickets in wavefront order: t = x + 2 * (y - band start), then band
+    std::vector<int> start(mb_h);
+    for (int i = 0; i < nslices; i++)
+        for (int r = bands[i]; r < bands[i + 1]; r++) start[r] = bands[i];
+    std::vector<int> order(c->nmb);
+    for (int i = 0; i < c->nmb; i++) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        int ax = a % mb_w, ay = a / mb_w, bx = b % mb_w, by = b / mb_w;
+        return ax + 2 * (ay - start[ay]) < bx + 2 * (by - start[by]);
+    });
+    if ((e = cudaMemcpy(c->d_band_start, start.data(), sizeof(int) * mb_h, cudaMemcpyHostToDevice)) != cudaSuccess) return fail(e);
+    if ((e = cudaMemcpy(c->d_order, order.data(), sizeof(int) * c->nmb, cudaMemcpyHostToDevice)) != cudaSuccess) return fail(e);
+    *out = c;
+    return IRONAV_OK;
+}
+
+int ironav_ctx_destroy(ironav_ctx* c) {
+    if (!c) return IRONAV_INVALID_ARGUMENT;
+    cudaStreamSynchronize(c->stream);
+    free_ctx(c);
+    return IRONAV_OK;
+}
+
+int ironav_ctx_dims(const ironav_ctx* c, int* mb_w, int* mb_h, int* sw, int* sh) {
+    if (!c) return IRONAV_INVALID_ARGUMENT;
+    if (mb_w) *mb_w = c->mb_w;
+    if (mb_h) *mb_h = c->mb_h;
+    if (sw) *sw = c->sw;
+    if (sh) *sh = c->sh;
+    return IRONAV_OK;
+}
+
+int ironav_ctx_set_stream(ironav_ctx* c, void* s) {
+    if (!c) return IRONAV_INVALID_ARGUMENT;
+    c->stream = static_cast<cudaStream_t>(s);
+    return IRONAV_OK;
+}
+
+int ironav_set_source_device(ironav_ctx* c, const uint8_t* d_y, int stride) {
+    if (!c || !d_y || stride < c->width) return IRONAV_INVALID_ARGUMENT;
+    CK(cudaMemcpy2DAsync(c->d_src, c->pw, d_y, stride, c->width, c->height, cudaMemcpyDeviceToDevice, c->stream));
+    if (c->width != c->pw || c->height != c->ph) {
+        dim3 grid((c->pw + 255) / 256, c->ph);
+        pad_edges_kernel<<<grid, 256, 0, c->stream>>>(c->d_src, c->width, c->height, c->pw, c->ph);
+    }
+    return cuda_status(cudaGetLastError());
+}
+
+int ironav_set_source(ironav_ctx* c, const uint8_t* y, int stride) {
+    if (!c || !y || stride < c->width) return IRONAV_INVALID_ARGUMENT;
+    CK(cudaMemcpy2DAsync(c->d_src, c->pw, y, stride, c->width, c->height, cudaMemcpyHostToDevice, c->stream));
+    if (c->width != c->pw || c->height != c->ph) {
+        dim3 grid((c->pw + 255) / 256, c->ph);
+        pad_edges_kernel<<<grid, 256, 0, c->stream>>>(c->d_src, c->width, c->height, c->pw, c->ph);
+        CK(cudaGetLastError());
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    return IRONAV_OK;
+}
+
+static bool ref_size_ok(const ironav_ctx* c, int stride, int w, int h) {
+    return ((w == c->width && h == c->height) || (w == c->pw && h == c->ph)) && stride >= w;
+}
+
+int ironav_push_reference_device(ironav_ctx* c, const uint8_t* d_y, int stride, int w, int h, const ironav_mbstate* d_col) {
+    if (!c || !d_y || !ref_size_ok(c, stride, w, h)) return IRONAV_INVALID_ARGUMENT;
+    return launch_planes(c, d_y, stride, w, h, d_col);
+}
+
+int ironav_push_reference(ironav_ctx* c, const uint8_t* y, int stride, int w, int h, const ironav_mbstate* col) {
+    if (!c || !y || !ref_size_ok(c, stride, w, h)) return IRONAV_INVALID_ARGUMENT;
+    CK(cudaMemcpy2DAsync(c->d_stage, w, y, stride, w, h, cudaMemcpyHostToDevice, c->stream));
+    if (col) CK(cudaMemcpyAsync(c->d_col_stage, col, sizeof(ironav_mbstate) * c->nmb, cudaMemcpyHostToDevice, c->stream));
+    int s = launch_planes(c, c->d_stage, w, w, h, col ? c->d_col_stage : nullptr);
+    if (s != IRONAV_OK) return s;
+    CK(cudaStreamSynchronize(c->stream));
+    return IRONAV_OK;
+}
+
+int ironav_clear_references(ironav_ctx* c) {
+    if (!c) return IRONAV_INVALID_ARGUMENT;
+    c->nrefs = 0;
+    c->have_params = false;
+    return IRONAV_OK;
+}
+
+int ironav_get_planes(ironav_ctx* c, int idx, uint8_t* out) {
+    if (!c || !out || idx < 0 || idx >= c->nrefs) return IRONAV_INVALID_ARGUMENT;
+    CK(cudaMemcpyAsync(out, c->d_planes[c->slot_of[idx]], 4 * (size_t)c->psize, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return IRONAV_OK;
+}
+
+int ironav_begin_p_picture(ironav_ctx* c, int qpp, int lambda, int skip_thresh, int nact, int fast, int sub8) {
+    if (!c || lambda < 1 || nact < 1 || nact > c->nrefs || qpp < 0 || qpp > 63) return IRONAV_INVALID_ARGUMENT;
+    c->qpp = qpp;
+    c->lambda = lambda;
+    c->skip_thresh = skip_thresh;
+    c->nact = nact;
+    c->fast = fast ? 1 : 0;
+    c->sub8 = sub8 ? 1 : 0;
+    c->have_params = true;
+    return IRONAV_OK;
+}
+
+int ironav_analyse_picture_replay_device(ironav_ctx* c, const ironav_mbstate* d_states, ironav_mbresult* d_out) {
+    if (!c || !d_states || !d_out || !c->have_params || c->nact > c->nrefs) return IRONAV_INVALID_ARGUMENT;
+    return launch_analyse(c, false, d_states, nullptr, d_out);
+}
+
+int ironav_analyse_picture_auto_device(ironav_ctx* c, ironav_mbstate* d_states, ironav_mbresult* d_out) {
+    if (!c || !d_states || !d_out || !c->have_params || c->nact > c->nrefs) return IRONAV_INVALID_ARGUMENT;
+    return launch_analyse(c, true, nullptr, d_states, d_out);
+}
+
+int ironav_analyse_picture_replay(ironav_ctx* c, const ironav_mbstate* states, ironav_mbresult* out) {
+    if (!c || !states || !out || !c->have_params || c->nact > c->nrefs) return IRONAV_INVALID_ARGUMENT;
+    CK(cudaMemcpyAsync(c->d_states, states, sizeof(ironav_mbstate) * c->nmb, cudaMemcpyHostToDevice, c->stream));
+    int s = launch_analyse(c, false, c->d_states, nullptr, c->d_results);
+    if (s != IRONAV_OK) return s;
+    CK(cudaMemcpyAsync(out, c->d_results, sizeof(ironav_mbresult) * c->nmb, cudaMemcpyDeviceToHost, c->stream));
+    return check_device_error(c);
+}
+
+int ironav_analyse_picture_auto(ironav_ctx* c, ironav_mbstate* states, ironav_mbresult* out) {
+    if (!c || !states || !out || !c->have_params || c->nact > c->nrefs) return IRONAV_INVALID_ARGUMENT;
+    int s = launch_analyse(c, true, nullptr, c->d_states, c->d_results);
+    if (s != IRONAV_OK) return s;
+    CK(cudaMemcpyAsync(out, c->d_results, sizeof(ironav_mbresult) * c->nmb, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(states, c->d_states, sizeof(ironav_mbstate) * c->nmb, cudaMemcpyDeviceToHost, c->stream));
+    return check_device_error(c);
+}
+
+int ironav_ctx_sync(ironav_ctx* c) {
+    if (!c) return IRONAV_INVALID_ARGUMENT;
+    CK(cudaStreamSynchronize(c->stream));
+    return check_device_error(c);
+}
+
+// Measures the 32-bit integer issue rate of the current device (operations per second, 1e12 units in
+// *tops): the roofline denominator for the analysis kernel (not in the public header).
+int ironav_measure_int32_peak(double* tops) {
+    if (!tops) return IRONAV_INVALID_ARGUMENT;
+    int dev = 0, nsm = 0, per_sm = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, int32_peak_kernel, 256, 0));
+    unsigned* d = nullptr;
+    CK(cudaMalloc(&d, sizeof(unsigned) * nsm * per_sm));
+    const int blocks = nsm * per_sm, iters = 4096;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    double best = 0.0;
+    for (int rep = 0; rep < 4; rep++) {
+        cudaEventRecord(e0);
+        int32_peak_kernel<<<blocks, 256>>>(d, iters, 12345u + rep);
+        cudaEventRecord(e1);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        double ops = 2.0 * 16.0 * 8.0 * iters * 256.0 * blocks;
+        if (rep > 0) best = std::max(best, ops / (ms * 1e-3) / 1e12);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(d);
+    CK(cudaGetLastError());
+    *tops = best;
+    return IRONAV_OK;
+}
+
+// Test hooks (not in the public header): a macroblock whose decision is never published, so the
+// wavefront waits behind it run out, and the number of polls a wait makes before it gives up.
+int ironav_debug_withhold(ironav_ctx* c, int mb) {
+    if (!c || mb < -1 || mb >= c->nmb) return IRONAV_INVALID_ARGUMENT;
+    c->withhold = mb;
+    return IRONAV_OK;
+}
+
+int ironav_debug_wait_limit(ironav_ctx* c, unsigned polls) {
+    if (!c || polls == 0) return IRONAV_INVALID_ARGUMENT;
+    c->wait_limit = polls;
+    return IRONAV_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,270 @@
+"""Python binding of the inter-analysis C ABI (include/ironav_inter.h).
+
+`InterStage` mirrors the calls the reference encoder makes into this stage for one stream
+(crates/ironav-codec/src/h264/enc/):
+
+- ``push_reference``   -> ``HalfPel::new`` of a new reference picture (mod.rs:660) and the
+  reference list update (mod.rs:663-666);
+- ``begin_p_picture``  -> ``FrameCoder::new`` / ``with_refs`` / ``with_fast`` / ``with_sub8x8``
+  (frame.rs:381-440) for a P picture;
+- ``analyse_replay``   -> for every macroblock, the P_Skip vector and SAD of ``code_mb``
+  (frame.rs:722-729) and ``best_inter`` (frame.rs:839-849), given the final decisions of the
+  neighbours;
+- ``analyse_auto``     -> the same, with the stage deciding each macroblock itself (P_Skip below the
+  threshold, else the best inter partitioning) in wavefront order.
+
+The library is ``ironav_b200/lib/libironav_inter_cuda.so``; loading fails loudly when it is missing
+or no CUDA device is present. Another library implementing the same header may be passed as ``lib``.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import build as _build
+
+MBSTATE_DTYPE = np.dtype(
+    [("inter", "u1"), ("refs", "i1", (4,)), ("pad", "u1", (3,)), ("mvs", "<i2", (16, 2))]
+)
+MBRESULT_DTYPE = np.dtype(
+    [
+        ("skip_mv", "<i2", (2,)),
+        ("skip_sad", "<i4"),
+        ("part", "u1"),
+        ("refs", "u1", (4,)),
+        ("sub", "u1", (4,)),
+        ("flags", "u1"),
+        ("pad", "u1", (2,)),
+        ("cost", "<i4"),
+        ("mvs", "<i2", (16, 2)),
+        ("cost16", "<i4"),
+        ("sad_px", "<u4"),
+        ("satd_px", "<u4"),
+        ("pad2", "<u4"),
+    ]
+)
+assert MBSTATE_DTYPE.itemsize == 72 and MBRESULT_DTYPE.itemsize == 104
+
+RESULT_INTER = 1
+RESULT_SKIP = 2
+
+# ironav_status: 1 + the index of ironav_core::ErrorCode (crates/ironav-core/src/error.rs:9-27)
+STATUS_NAMES = {
+    0: "Ok",
+    2: "InvalidInput",
+    3: "InvalidArgument",
+    8: "HardwareUnavailable",
+    13: "Internal",
+    100: "Timeout",
+}
+
+# Every entry point include/ironav_inter.h declares.
+EXPORTS = (
+    "ironav_lambda", "ironav_skip_threshold", "ironav_se_bits", "ironav_ue_bits", "ironav_version",
+    "ironav_ctx_create", "ironav_ctx_destroy", "ironav_ctx_dims", "ironav_ctx_set_stream",
+    "ironav_set_source", "ironav_push_reference", "ironav_clear_references", "ironav_get_planes",
+    "ironav_begin_p_picture", "ironav_analyse_picture_replay", "ironav_analyse_picture_auto",
+    "ironav_set_source_device", "ironav_push_reference_device",
+    "ironav_analyse_picture_replay_device", "ironav_analyse_picture_auto_device", "ironav_ctx_sync",
+)
+
+
+class IronavError(RuntimeError):
+    """A non-zero ironav_status; `.status` holds the code and `.name` the ErrorCode it maps to."""
+
+    def __init__(self, status: int, what: str):
+        self.status = status
+        self.name = STATUS_NAMES.get(status, f"status {status}")
+        super().__init__(f"{what}: {self.name} ({status})")
+
+
+_VP = ctypes.c_void_p
+_I = ctypes.c_int
+
+
+def _declare(lib: ctypes.CDLL) -> ctypes.CDLL:
+    lib.ironav_lambda.argtypes = [_I]
+    lib.ironav_skip_threshold.argtypes = [_I]
+    lib.ironav_se_bits.argtypes = [_I]
+    lib.ironav_ue_bits.argtypes = [ctypes.c_uint]
+    lib.ironav_version.restype = ctypes.c_char_p
+    lib.ironav_ctx_create.argtypes = [ctypes.POINTER(_VP), _I, _I, _I, _I, _I, _VP]
+    lib.ironav_ctx_destroy.argtypes = [_VP]
+    lib.ironav_ctx_dims.argtypes = [_VP] + [ctypes.POINTER(_I)] * 4
+    lib.ironav_ctx_set_stream.argtypes = [_VP, _VP]
+    lib.ironav_set_source.argtypes = [_VP, _VP, _I]
+    lib.ironav_push_reference.argtypes = [_VP, _VP, _I, _I, _I, _VP]
+    lib.ironav_clear_references.argtypes = [_VP]
+    lib.ironav_get_planes.argtypes = [_VP, _I, _VP]
+    lib.ironav_begin_p_picture.argtypes = [_VP, _I, _I, _I, _I, _I, _I]
+    lib.ironav_analyse_picture_replay.argtypes = [_VP, _VP, _VP]
+    lib.ironav_analyse_picture_auto.argtypes = [_VP, _VP, _VP]
+    lib.ironav_set_source_device.argtypes = [_VP, _VP, _I]
+    lib.ironav_push_reference_device.argtypes = [_VP, _VP, _I, _I, _I, _VP]
+    lib.ironav_analyse_picture_replay_device.argtypes = [_VP, _VP, _VP]
+    lib.ironav_analyse_picture_auto_device.argtypes = [_VP, _VP, _VP]
+    lib.ironav_ctx_sync.argtypes = [_VP]
+    for name in ("ironav_debug_withhold", "ironav_debug_wait_limit"):
+        if hasattr(lib, name):
+            getattr(lib, name).argtypes = [_VP, ctypes.c_int if name.endswith("withhold") else ctypes.c_uint]
+    return lib
+
+
+_CUDA = None
+
+
+def cuda_library() -> ctypes.CDLL:
+    """The sm_100a library, built in-tree. Raises when it is absent: there is no CPU fallback."""
+    global _CUDA
+    if _CUDA is None:
+        path = _build.CUDA_LIB
+        if not os.path.exists(path):
+            raise RuntimeError(f"{path} is missing: build it with `python -m ironav_b200.build`")
+        _CUDA = _declare(ctypes.CDLL(path))
+    return _CUDA
+
+
+def load_library(path: str) -> ctypes.CDLL:
+    """Another implementation of include/ironav_inter.h (same entry points, same meaning)."""
+    return _declare(ctypes.CDLL(path))
+
+
+def _ptr(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+def lambda_of(qp_prime: int, lib: ctypes.CDLL | None = None) -> int:
+    return (lib or cuda_library()).ironav_lambda(qp_prime)
+
+
+@dataclass
+class PictureParams:
+    qp_prime: int
+    nrefs_active: int = 1
+    fast: bool = False
+    sub8: bool = False
+
+
+class InterStage:
+    """One stream's inter-analysis context (ironav_ctx)."""
+
+    def __init__(self, width: int, height: int, max_refs: int = 1, nslices: int = 1,
+                 band_rows: list[int] | None = None, lib: ctypes.CDLL | None = None):
+        self.lib = lib if lib is not None else cuda_library()
+        self.width, self.height = width, height
+        h = _VP()
+        bands = None
+        if band_rows is not None:
+            self._bands = np.asarray(band_rows, dtype=np.int32)
+            bands = _ptr(self._bands)
+        self._check(self.lib.ironav_ctx_create(ctypes.byref(h), width, height, 8, max_refs, nslices, bands),
+                    "ironav_ctx_create")
+        self.ctx = h
+        mw, mh, sw, sh = _I(), _I(), _I(), _I()
+        self.lib.ironav_ctx_dims(self.ctx, ctypes.byref(mw), ctypes.byref(mh), ctypes.byref(sw), ctypes.byref(sh))
+        self.mb_w, self.mb_h, self.sw, self.sh = mw.value, mh.value, sw.value, sh.value
+        self.nmb = self.mb_w * self.mb_h
+
+    @staticmethod
+    def _check(status: int, what: str) -> None:
+        if status != 0:
+            raise IronavError(status, what)
+
+    def close(self) -> None:
+        if getattr(self, "ctx", None):
+            self.lib.ironav_ctx_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- pictures ------------------------------------------------------------------------------------
+
+    def set_source(self, luma: np.ndarray) -> None:
+        luma = np.ascontiguousarray(luma, dtype=np.uint8)
+        assert luma.shape == (self.height, self.width)
+        self._check(self.lib.ironav_set_source(self.ctx, _ptr(luma), self.width), "ironav_set_source")
+
+    def push_reference(self, luma: np.ndarray, col: np.ndarray | None = None) -> None:
+        luma = np.ascontiguousarray(luma, dtype=np.uint8)
+        h, w = luma.shape
+        colp = None
+        if col is not None:
+            col = np.ascontiguousarray(col, dtype=MBSTATE_DTYPE)
+            assert col.shape == (self.nmb,)
+            colp = _ptr(col)
+        self._check(self.lib.ironav_push_reference(self.ctx, _ptr(luma), w, w, h, colp), "ironav_push_reference")
+
+    def clear_references(self) -> None:
+        self._check(self.lib.ironav_clear_references(self.ctx), "ironav_clear_references")
+
+    def planes(self, idx: int = 0) -> np.ndarray:
+        out = np.empty((4, self.sh, self.sw), dtype=np.uint8)
+        self._check(self.lib.ironav_get_planes(self.ctx, idx, _ptr(out)), "ironav_get_planes")
+        return out
+
+    def begin_p_picture(self, qp_prime: int, nrefs_active: int = 1, fast: bool = False, sub8: bool = False) -> None:
+        lam = self.lib.ironav_lambda(qp_prime)
+        thr = self.lib.ironav_skip_threshold(qp_prime)
+        self._check(self.lib.ironav_begin_p_picture(self.ctx, qp_prime, lam, thr, nrefs_active, int(fast), int(sub8)),
+                    "ironav_begin_p_picture")
+
+    def analyse_replay(self, states: np.ndarray) -> np.ndarray:
+        states = np.ascontiguousarray(states, dtype=MBSTATE_DTYPE)
+        assert states.shape == (self.nmb,)
+        out = np.zeros(self.nmb, dtype=MBRESULT_DTYPE)
+        self._check(self.lib.ironav_analyse_picture_replay(self.ctx, _ptr(states), _ptr(out)),
+                    "ironav_analyse_picture_replay")
+        return out
+
+    def analyse_auto(self) -> tuple[np.ndarray, np.ndarray]:
+        states = np.zeros(self.nmb, dtype=MBSTATE_DTYPE)
+        out = np.zeros(self.nmb, dtype=MBRESULT_DTYPE)
+        self._check(self.lib.ironav_analyse_picture_auto(self.ctx, _ptr(states), _ptr(out)),
+                    "ironav_analyse_picture_auto")
+        return states, out
+
+    # -- device-resident forms (integer device pointers, e.g. torch tensor.data_ptr()) ---------------
+
+    def set_stream(self, stream_handle: int) -> None:
+        self._check(self.lib.ironav_ctx_set_stream(self.ctx, stream_handle), "ironav_ctx_set_stream")
+
+    def set_source_device(self, d_luma: int, stride: int) -> None:
+        self._check(self.lib.ironav_set_source_device(self.ctx, d_luma, stride), "ironav_set_source_device")
+
+    def push_reference_device(self, d_luma: int, stride: int, w: int, h: int, d_col: int | None) -> None:
+        self._check(self.lib.ironav_push_reference_device(self.ctx, d_luma, stride, w, h, d_col),
+                    "ironav_push_reference_device")
+
+    def analyse_replay_device(self, d_states: int, d_out: int) -> None:
+        self._check(self.lib.ironav_analyse_picture_replay_device(self.ctx, d_states, d_out),
+                    "ironav_analyse_picture_replay_device")
+
+    def analyse_auto_device(self, d_states: int, d_out: int) -> None:
+        self._check(self.lib.ironav_analyse_picture_auto_device(self.ctx, d_states, d_out),
+                    "ironav_analyse_picture_auto_device")
+
+    def sync(self) -> None:
+        self._check(self.lib.ironav_ctx_sync(self.ctx), "ironav_ctx_sync")
+
+
+def default_bands(mb_h: int, nslices: int) -> list[int]:
+    """Slice bands as the encoder cuts them: band i = [i*mb_h/n, (i+1)*mb_h/n) (enc/mod.rs:603)."""
+    return [i * mb_h // nslices for i in range(nslices + 1)]
+
+
+def reference_slices(mb_h: int, cores: int) -> int:
+    """The encoder's slice count, min(cores, max(mb_h/8, 1)) (enc/mod.rs:192)."""
+    return min(cores, max(mb_h // 8, 1))

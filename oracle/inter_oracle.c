@@ -1,0 +1,1001 @@
+/*
+ * inter_oracle.c — CPU restatement of IronAV's H.264 P-picture inter-analysis stage.
+ *
+ * TEST INFRASTRUCTURE ONLY. This file is the parity checker and the timed CPU baseline. It is never
+ * part of the product path: only the tests, the smoke check and the benchmark's CPU-baseline leg load
+ * the library built from it (liboracle: oracle/_build/libironav_inter_cpu.so).
+ *
+ * The reference is Rust (nervosys/IronAV 0.1.10, crate ironav-codec) and no Rust toolchain exists
+ * here, so this is a line-by-line restatement in C of the functions listed below, each citing the file
+ * and lines it follows (paths relative to crates/ironav-codec/src/h264/):
+ *   HalfPel::build / predict / rows ........ enc/subpel.rs:21-151
+ *   luma_mc_ref (decoder's per-sample form)  inter.rs:466-546   (only to pin predict, as enc/subpel.rs:160-194 does)
+ *   satd4, lambda, mvd_bits, median ........ enc/frame.rs:144-175
+ *   se_bits / ue_bits ...................... enc/bitw.rs:81-89
+ *   PARTS, SUB, rects, spread, paint ....... enc/frame.rs:182-236
+ *   nb_state, nb_motion, pred_mv, mv_pred,
+ *   part_mvps, skip_mv ..................... enc/frame.rs:509-603
+ *   satd, sad_int, luma_pred, ref_bits ..... enc/frame.rs:641-711
+ *   P_Skip SAD ............................. enc/frame.rs:722-729
+ *   best_inter, best_inter_ref, sub_search,
+ *   col_mv, motion_search .................. enc/frame.rs:839-1019
+ *   slice bands ............................ enc/mod.rs:192,603
+ *   source padding ......................... enc/mod.rs:481-529
+ *
+ * Pinning. The interpolation (planes + predict) is pinned by the reference's own known-answer test,
+ * predict == the decoder's interpolation over the same grid of blocks and vectors (enc/subpel.rs:160-194,
+ * restated in tests/test_oracle.py against luma_mc_ref below), and the Exp-Golomb bit counts by the
+ * code lengths of enc/bitw.rs:110-135. The motion search and partition decision have no golden
+ * vectors in the reference (no test pins MVs, costs or partitions): for them parity is UNPINNED beyond
+ * this restatement, which follows the Rust statement by statement (strict '<' with first-wins order,
+ * the same clamps, the same early breaks).
+ *
+ * Samples are kept as uint16 like the reference, so the 10-bit planes of the known-answer test run
+ * through the same code.
+ */
+#include "../include/ironav_inter.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define PAD 48 /* enc/subpel.rs:7 */
+
+/* ---------------------------------------------------------------------------------------------------
+ * HalfPel (enc/subpel.rs)
+ * ------------------------------------------------------------------------------------------------- */
+
+typedef struct halfpel {
+    int stride, pw, ph, sh;
+    uint16_t* planes[4]; /* G, b, h, j */
+} halfpel;
+
+static int tap6(int a, int b, int c, int d, int e, int f) { return a - 5 * b + 20 * c + 20 * d - 5 * e + f; } /* subpel.rs:21-23 */
+
+static int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+static int mini(int a, int b) { return a < b ? a : b; }
+static int maxi(int a, int b) { return a > b ? a : b; }
+
+/* HalfPel::build, enc/subpel.rs:57-115 (single-threaded; the threaded form gives the same planes). */
+static void halfpel_build(halfpel* hp, const uint16_t* luma, int pw, int ph, int bd) {
+    int maxv = (1 << bd) - 1;
+    int sw = pw + 2 * PAD, sh = ph + 2 * PAD;
+    size_t n = (size_t)sw * sh;
+    hp->stride = sw;
+    hp->pw = pw;
+    hp->ph = ph;
+    hp->sh = sh;
+    for (int k = 0; k < 4; k++) hp->planes[k] = (uint16_t*)calloc(n, sizeof(uint16_t));
+    int32_t* b1 = (int32_t*)calloc(n, sizeof(int32_t));
+    uint16_t *g = hp->planes[0], *b = hp->planes[1], *h = hp->planes[2], *j = hp->planes[3];
+    /* round1: integer samples with the edges repeated, and the horizontal half samples (subpel.rs:71-85) */
+    for (int y = 0; y < sh; y++) {
+        int sy = mini(y >= PAD ? y - PAD : 0, ph - 1);
+        uint16_t* gr = g + (size_t)y * sw;
+        for (int x = 0; x < sw; x++) gr[x] = luma[(size_t)sy * pw + mini(x >= PAD ? x - PAD : 0, pw - 1)];
+        for (int x = 2; x < sw - 3; x++) {
+            int v = tap6(gr[x - 2], gr[x - 1], gr[x], gr[x + 1], gr[x + 2], gr[x + 3]);
+            b1[(size_t)y * sw + x] = v;
+            b[(size_t)y * sw + x] = (uint16_t)clampi((v + 16) >> 5, 0, maxv);
+        }
+    }
+    /* round2: vertical half samples from G and diagonal ones from the unrounded sums (subpel.rs:93-108) */
+    for (int y = 2; y < sh - 3; y++) {
+        for (int x = 0; x < sw; x++) {
+#define G_(yy) ((int)g[(size_t)(yy) * sw + x])
+#define B1_(yy) (b1[(size_t)(yy) * sw + x])
+            int v = tap6(G_(y - 2), G_(y - 1), G_(y), G_(y + 1), G_(y + 2), G_(y + 3));
+            h[(size_t)y * sw + x] = (uint16_t)clampi((v + 16) >> 5, 0, maxv);
+            v = tap6(B1_(y - 2), B1_(y - 1), B1_(y), B1_(y + 1), B1_(y + 2), B1_(y + 3));
+            j[(size_t)y * sw + x] = (uint16_t)clampi((v + 512) >> 10, 0, maxv);
+#undef G_
+#undef B1_
+        }
+    }
+    free(b1);
+}
+
+static void halfpel_free(halfpel* hp) {
+    for (int k = 0; k < 4; k++) {
+        free(hp->planes[k]);
+        hp->planes[k] = NULL;
+    }
+}
+
+/* MIX, enc/subpel.rs:26-38: [fy][fx] -> (plane a, dx, dy, plane b, dx, dy) with G=0, B=1, H=2, J=3. */
+static const unsigned char MIX[4][4][6] = {
+    {{0, 0, 0, 0, 0, 0}, {0, 0, 0, 1, 0, 0}, {1, 0, 0, 1, 0, 0}, {0, 1, 0, 1, 0, 0}},
+    {{0, 0, 0, 2, 0, 0}, {1, 0, 0, 2, 0, 0}, {1, 0, 0, 3, 0, 0}, {1, 0, 0, 2, 1, 0}},
+    {{2, 0, 0, 2, 0, 0}, {2, 0, 0, 3, 0, 0}, {3, 0, 0, 3, 0, 0}, {3, 0, 0, 2, 1, 0}},
+    {{0, 0, 1, 2, 0, 0}, {2, 0, 0, 1, 0, 1}, {3, 0, 0, 1, 0, 1}, {2, 1, 0, 1, 0, 1}},
+};
+
+static size_t hp_offset(const halfpel* hp, int x, int y) { return (size_t)(y + PAD) * hp->stride + (size_t)(x + PAD); } /* subpel.rs:117-119 */
+
+/* HalfPel::predict, enc/subpel.rs:122-145. */
+static void halfpel_predict(const halfpel* hp, int x, int y, int mvx, int mvy, int w, int h, uint16_t* out) {
+    int fx = mvx & 3, fy = mvy & 3;
+    int ix = clampi(x + (mvx >> 2), -w - 3, hp->pw + 1);
+    int iy = clampi(y + (mvy >> 2), -h - 3, hp->ph + 1);
+    const unsigned char* m = MIX[fy][fx];
+    int s = hp->stride;
+    const uint16_t* a = hp->planes[m[0]] + hp_offset(hp, ix + m[1], iy + m[2]);
+    if (m[0] == m[3] && m[1] == m[4] && m[2] == m[5]) {
+        for (int r = 0; r < h; r++)
+            for (int c = 0; c < w; c++) out[r * w + c] = a[r * s + c];
+    } else {
+        const uint16_t* b = hp->planes[m[3]] + hp_offset(hp, ix + m[4], iy + m[5]);
+        for (int r = 0; r < h; r++)
+            for (int c = 0; c < w; c++) out[r * w + c] = (uint16_t)(((unsigned)a[r * s + c] + b[r * s + c] + 1) >> 1);
+    }
+}
+
+/* ---------------------------------------------------------------------------------------------------
+ * luma_mc_ref, h264/inter.rs:466-546: the decoder's per-sample interpolation (8.4.2.2.1), restated to
+ * pin HalfPel::predict as the reference's test enc/subpel.rs:160-194 does.
+ * ------------------------------------------------------------------------------------------------- */
+
+static int clip1(int v, int maxv) { return clampi(v, 0, maxv); } /* inter.rs:3-5 */
+
+void oracle_luma_mc_ref(const uint16_t* refp, int stride, int pw, int ph, int x, int y, int mx, int my, int w, int h,
+                        uint16_t* out, int maxv) {
+    int fx = mx & 3, fy = my & 3;
+    int x0 = x + (mx >> 2), y0 = y + (my >> 2);
+    if (fx == 0 && fy == 0) {
+        for (int r = 0; r < h; r++) {
+            int yy = clampi(y0 + r, 0, ph - 1);
+            for (int c = 0; c < w; c++) out[r * w + c] = refp[(size_t)yy * stride + clampi(x0 + c, 0, pw - 1)];
+        }
+        return; /* the in-picture fast path of inter.rs:470-475 reads the same samples */
+    }
+    /* window of (w+5) x (h+5) samples from 2 left of and 2 above the block, edges repeated (inter.rs:489-506) */
+    int ww = w + 5, wh = h + 5;
+    int win[21 * 21];
+    for (int r = 0; r < wh; r++) {
+        int yy = clampi(y0 - 2 + r, 0, ph - 1);
+        for (int c = 0; c < ww; c++) win[r * ww + c] = refp[(size_t)yy * stride + clampi(x0 - 2 + c, 0, pw - 1)];
+    }
+#define GW(c, r) (win[((r) + 2) * ww + (c) + 2])
+    /* unrounded horizontal sums at (window column c, window row rr) (inter.rs:509-520) */
+    int b1[21 * 21];
+    memset(b1, 0, sizeof(b1));
+    for (int rr = 0; rr < wh; rr++)
+        for (int c = 0; c < w; c++) {
+            const int* t = &win[rr * ww + c];
+            b1[rr * ww + c] = tap6(t[0], t[1], t[2], t[3], t[4], t[5]);
+        }
+#define BH(c, r) (clip1((b1[((r) + 2) * ww + (c)] + 16) >> 5, maxv))
+#define HV(c, r) (clip1((tap6(win[(r)*ww + (c) + 2], win[((r) + 1) * ww + (c) + 2], win[((r) + 2) * ww + (c) + 2],       \
+                              win[((r) + 3) * ww + (c) + 2], win[((r) + 4) * ww + (c) + 2], win[((r) + 5) * ww + (c) + 2]) + \
+                         16) >> 5,                                                                                        \
+                        maxv))
+#define JJ(c, r) (clip1((tap6(b1[(r)*ww + (c)], b1[((r) + 1) * ww + (c)], b1[((r) + 2) * ww + (c)],                       \
+                              b1[((r) + 3) * ww + (c)], b1[((r) + 4) * ww + (c)], b1[((r) + 5) * ww + (c)]) + 512) >> 10, \
+                        maxv))
+    for (int r = 0; r < h; r++) {
+        for (int c = 0; c < w; c++) {
+            int v;
+            switch (fy * 4 + fx) { /* (fx, fy) cases of inter.rs:529-545 */
+            case 0 * 4 + 1: v = (GW(c, r) + BH(c, r) + 1) >> 1; break;
+            case 0 * 4 + 2: v = BH(c, r); break;
+            case 0 * 4 + 3: v = (GW(c + 1, r) + BH(c, r) + 1) >> 1; break;
+            case 1 * 4 + 0: v = (GW(c, r) + HV(c, r) + 1) >> 1; break;
+            case 2 * 4 + 0: v = HV(c, r); break;
+            case 3 * 4 + 0: v = (GW(c, r + 1) + HV(c, r) + 1) >> 1; break;
+            case 1 * 4 + 1: v = (BH(c, r) + HV(c, r) + 1) >> 1; break;
+            case 1 * 4 + 3: v = (BH(c, r) + HV(c + 1, r) + 1) >> 1; break;
+            case 3 * 4 + 1: v = (HV(c, r) + BH(c, r + 1) + 1) >> 1; break;
+            case 3 * 4 + 3: v = (HV(c + 1, r) + BH(c, r + 1) + 1) >> 1; break;
+            case 1 * 4 + 2: v = (BH(c, r) + JJ(c, r) + 1) >> 1; break;
+            case 3 * 4 + 2: v = (JJ(c, r) + BH(c, r + 1) + 1) >> 1; break;
+            case 2 * 4 + 1: v = (HV(c, r) + JJ(c, r) + 1) >> 1; break;
+            case 2 * 4 + 3: v = (JJ(c, r) + HV(c + 1, r) + 1) >> 1; break;
+            default: v = JJ(c, r); break;
+            }
+            out[r * w + c] = (uint16_t)v;
+        }
+    }
+#undef GW
+#undef BH
+#undef HV
+#undef JJ
+}
+
+/* ---------------------------------------------------------------------------------------------------
+ * Costs and bit counts
+ * ------------------------------------------------------------------------------------------------- */
+
+/* satd4, enc/frame.rs:144-161 */
+static int satd4(const int d[16]) {
+    int t[16];
+    for (int r = 0; r < 4; r++) {
+        int a = d[r * 4], b = d[r * 4 + 1], c = d[r * 4 + 2], e = d[r * 4 + 3];
+        int s0 = a + b, s1 = c + e, d0 = a - b, d1 = c - e;
+        t[r * 4] = s0 + s1;
+        t[r * 4 + 1] = s0 - s1;
+        t[r * 4 + 2] = d0 - d1;
+        t[r * 4 + 3] = d0 + d1;
+    }
+    int sum = 0;
+    for (int c = 0; c < 4; c++) {
+        int a = t[c], b = t[4 + c], cc = t[8 + c], e = t[12 + c];
+        int s0 = a + b, s1 = cc + e, d0 = a - b, d1 = cc - e;
+        sum += abs(s0 + s1) + abs(s0 - s1) + abs(d0 - d1) + abs(d0 + d1);
+    }
+    return sum >> 1;
+}
+
+/* ue_bits / se_bits, enc/bitw.rs:81-89 */
+int ironav_ue_bits(unsigned v) {
+    unsigned x = v + 1;
+    int len = 32 - __builtin_clz(x);
+    return 2 * len - 1;
+}
+int ironav_se_bits(int v) {
+    unsigned u = v > 0 ? 2u * (unsigned)v - 1u : (unsigned)(-2 * (long long)v);
+    return ironav_ue_bits(u);
+}
+
+/* lambda, enc/frame.rs:164-166 */
+int ironav_lambda(int qp) {
+    int l = (int)round(pow(2.0, ((double)qp - 12.0) / 6.0));
+    return l < 1 ? 1 : l;
+}
+
+/* The P_Skip test `(sad as f64) < 256.0 * 0.625 * step` with step = 2^(qp'/6), enc/frame.rs:730,742,
+ * as an integer bound: sad < ceil(x) for every integer sad. */
+int ironav_skip_threshold(int qpp) {
+    double x = 256.0 * 0.625 * pow(2.0, (double)qpp / 6.0);
+    return (int)ceil(x);
+}
+
+/* mvd_bits, enc/frame.rs:169-171 */
+static int mvd_bits(int mx, int my, int px, int py) { return ironav_se_bits(mx - px) + ironav_se_bits(my - py); }
+
+/* median, enc/frame.rs:173-175 */
+static int median3(int a, int b, int c) { return mini(maxi(a, b), maxi(mini(a, b), c)); }
+
+const char* ironav_version(void) { return "cpu-oracle (C restatement of ironav-codec 0.1.10 h264::enc inter analysis)"; }
+
+/* ---------------------------------------------------------------------------------------------------
+ * Partition geometry, enc/frame.rs:182-236
+ * ------------------------------------------------------------------------------------------------- */
+
+typedef struct { int x, y, w, h; } rect4;
+
+static const rect4 PARTS_[4][4] = {
+    {{0, 0, 4, 4}}, {{0, 0, 4, 2}, {0, 2, 4, 2}}, {{0, 0, 2, 4}, {2, 0, 2, 4}}, {{0, 0, 2, 2}, {2, 0, 2, 2}, {0, 2, 2, 2}, {2, 2, 2, 2}}};
+static const int NPARTS[4] = {1, 2, 2, 4};
+static const rect4 SUB_[4][4] = {
+    {{0, 0, 2, 2}}, {{0, 0, 2, 1}, {0, 1, 2, 1}}, {{0, 0, 1, 2}, {1, 0, 1, 2}}, {{0, 0, 1, 1}, {1, 0, 1, 1}, {0, 1, 1, 1}, {1, 1, 1, 1}}};
+static const int NSUB[4] = {1, 2, 2, 4};
+
+/* rects, enc/frame.rs:208-213: returns the count */
+static int rects(int part, const uint8_t sub[4], rect4 out[16]) {
+    if (part != 3) {
+        for (int k = 0; k < NPARTS[part]; k++) out[k] = PARTS_[part][k];
+        return NPARTS[part];
+    }
+    int n = 0;
+    for (int k = 0; k < 4; k++)
+        for (int s = 0; s < NSUB[sub[k]]; s++) {
+            rect4 r = SUB_[sub[k]][s];
+            r.x += (k & 1) * 2;
+            r.y += (k >> 1) * 2;
+            out[n++] = r;
+        }
+    return n;
+}
+
+/* ref_of (enc/frame.rs:217-223) is not needed: a P macroblock's partitions all use the reference
+ * best_inter_ref searches (refs = [r; 4], enc/frame.rs:854). */
+
+/* ---------------------------------------------------------------------------------------------------
+ * One picture's analysis (FrameCoder, enc/frame.rs:337-1019, the parts the stage covers)
+ * ------------------------------------------------------------------------------------------------- */
+
+typedef struct colmv { int16_t mv[2]; uint8_t valid; } colmv;
+
+typedef struct refpic {
+    halfpel hp;
+    colmv* col; /* per macroblock: mvs[5] when the macroblock was inter (col_mv, enc/frame.rs:944-947) */
+} refpic;
+
+struct ironav_ctx {
+    int width, height, bd, mb_w, mb_h, pw, ph, max_refs, nslices;
+    int* band_start; /* per macroblock row: first row of its slice band */
+    uint16_t* src;   /* padded source, pw x ph */
+    refpic* refs;    /* newest first */
+    int nrefs;
+    /* picture parameters */
+    int qpp, lambda, skip_thresh, nact, fast, sub8;
+    int threads;
+};
+
+typedef struct fc {
+    const struct ironav_ctx* c;
+    const ironav_mbstate* states; /* final states of the whole picture */
+} fc;
+
+/* nb_state, enc/frame.rs:509-515 */
+static const ironav_mbstate* nb_state(const fc* f, int mbx, int mby, int cur_mby) {
+    const struct ironav_ctx* c = f->c;
+    int start = c->band_start[cur_mby];
+    if (mbx < 0 || mby < start || mbx >= c->mb_w || mby >= c->mb_h) return NULL;
+    return &f->states[(size_t)mby * c->mb_w + mbx];
+}
+
+typedef struct nbm { int avail, ref, mv[2]; } nbm;
+
+/* nb_motion, enc/frame.rs:522-538 (list 0; P slices never set the high `done` bits) */
+static nbm nb_motion(const fc* f, int mbx, int mby, const int16_t cur[16][2], const int8_t cref[16], uint32_t done, int x, int y) {
+    nbm r = {0, -1, {0, 0}};
+    int dx, dy, bx, by;
+    if (x < 0 && y < 0) { dx = -1; dy = -1; bx = 3; by = 3; }
+    else if (x < 0) { dx = -1; dy = 0; bx = 3; by = y; }
+    else if (x >= 4 && y < 0) { dx = 1; dy = -1; bx = 0; by = 3; }
+    else if (x >= 4) return r;
+    else if (y < 0) { dx = 0; dy = -1; bx = x; by = 3; }
+    else {
+        int b = y * 4 + x;
+        if ((done >> b) & 1) {
+            r.avail = 1;
+            if ((done >> (16 + b)) & 1) return r; /* (-1, [0, 0]) */
+            r.ref = cref[b];
+            r.mv[0] = cur[b][0];
+            r.mv[1] = cur[b][1];
+        }
+        return r;
+    }
+    const ironav_mbstate* s = nb_state(f, mbx + dx, mby + dy, mby);
+    if (!s) return r;
+    r.avail = 1;
+    int rf = s->refs[(by / 2) * 2 + bx / 2];
+    if (s->inter && rf >= 0) {
+        r.ref = rf;
+        r.mv[0] = s->mvs[by * 4 + bx][0];
+        r.mv[1] = s->mvs[by * 4 + bx][1];
+    }
+    return r;
+}
+
+/* pred_mv, enc/frame.rs:543-570 */
+static void pred_mv(const fc* f, int mbx, int mby, const int16_t cur[16][2], const int8_t cref[16], uint32_t done, int bx, int by,
+                    int w, int dir, int rf, int out[2]) {
+    nbm a = nb_motion(f, mbx, mby, cur, cref, done, bx - 1, by);
+    nbm b = nb_motion(f, mbx, mby, cur, cref, done, bx, by - 1);
+    nbm c = nb_motion(f, mbx, mby, cur, cref, done, bx + w, by - 1);
+    if (!c.avail) c = nb_motion(f, mbx, mby, cur, cref, done, bx - 1, by - 1);
+    /* r(n) = n.map_or(-1, ref) — an unavailable neighbour has ref -1 and vector 0 */
+    const nbm* pick = NULL;
+    if (dir == 1 && by == 0 && b.ref == rf) pick = &b;
+    else if (dir == 1 && by != 0 && a.ref == rf) pick = &a;
+    else if (dir == 2 && bx == 0 && a.ref == rf) pick = &a;
+    else if (dir == 2 && bx != 0 && c.ref == rf) pick = &c;
+    if (pick) { out[0] = pick->mv[0]; out[1] = pick->mv[1]; return; }
+    if (!b.avail && !c.avail && a.avail) { out[0] = a.mv[0]; out[1] = a.mv[1]; return; }
+    int ra = a.ref == rf, rb = b.ref == rf, rc = c.ref == rf;
+    if (ra + rb + rc == 1) {
+        const nbm* p = ra ? &a : (rb ? &b : &c);
+        out[0] = p->mv[0];
+        out[1] = p->mv[1];
+        return;
+    }
+    out[0] = median3(a.mv[0], b.mv[0], c.mv[0]);
+    out[1] = median3(a.mv[1], b.mv[1], c.mv[1]);
+}
+
+static const int16_t ZERO_MVS[16][2];
+static const int8_t NO_REF[16];
+
+/* mv_pred, enc/frame.rs:573-575 */
+static void mv_pred(const fc* f, int mbx, int mby, int rf, int out[2]) { pred_mv(f, mbx, mby, ZERO_MVS, NO_REF, 0, 0, 0, 4, 0, rf, out); }
+
+/* part_mvps, enc/frame.rs:579-594: the predictor of partition k of `part` given mvs of those before */
+static void part_mvp(const fc* f, int mbx, int mby, int part, const int16_t mvs[16][2], int rf, int want, int out[2]) {
+    int16_t cur[16][2];
+    int8_t cref[16];
+    uint32_t done = 0;
+    memset(cur, 0, sizeof(cur));
+    memset(cref, 0, sizeof(cref));
+    static const uint8_t nosub[4] = {0, 0, 0, 0};
+    rect4 rs[16];
+    int n = rects(part, nosub, rs);
+    int dir = part == 1 ? 1 : (part == 2 ? 2 : 0);
+    for (int k = 0; k < n; k++) {
+        rect4 r = rs[k];
+        if (k == want) {
+            pred_mv(f, mbx, mby, cur, cref, done, r.x, r.y, r.w, dir, rf, out);
+            return;
+        }
+        for (int by = r.y; by < r.y + r.h; by++)
+            for (int bx = r.x; bx < r.x + r.w; bx++) {
+                cur[by * 4 + bx][0] = mvs[k][0];
+                cur[by * 4 + bx][1] = mvs[k][1];
+                cref[by * 4 + bx] = (int8_t)rf;
+                done |= 1u << (by * 4 + bx);
+            }
+    }
+}
+
+/* skip_mv, enc/frame.rs:597-603 */
+static void skip_mv(const fc* f, int mbx, int mby, int out[2]) {
+    nbm a = nb_motion(f, mbx, mby, ZERO_MVS, NO_REF, 0, -1, 0);
+    nbm b = nb_motion(f, mbx, mby, ZERO_MVS, NO_REF, 0, 0, -1);
+    if (!a.avail || !b.avail || (a.ref == 0 && a.mv[0] == 0 && a.mv[1] == 0) || (b.ref == 0 && b.mv[0] == 0 && b.mv[1] == 0)) {
+        out[0] = out[1] = 0;
+        return;
+    }
+    mv_pred(f, mbx, mby, 0, out);
+}
+
+/* satd, enc/frame.rs:641-659 (luma) */
+static int satd_blk(const fc* f, int x, int y, int w, int h, const uint16_t* pred) {
+    int s = f->c->pw;
+    const uint16_t* src = f->c->src;
+    int total = 0;
+    for (int by = 0; by < h; by += 4)
+        for (int bx = 0; bx < w; bx += 4) {
+            int d[16];
+            for (int r = 0; r < 4; r++)
+                for (int c = 0; c < 4; c++) d[r * 4 + c] = (int)src[(size_t)(y + by + r) * s + x + bx + c] - (int)pred[(by + r) * w + bx + c];
+            total += satd4(d);
+        }
+    return total;
+}
+
+/* sad_int, enc/frame.rs:662-671 with HalfPel::rows, enc/subpel.rs:148-151 */
+static int sad_int(const fc* f, int r, int x, int y, int w, int h, int mvx, int mvy) {
+    const halfpel* hp = &f->c->refs[r].hp;
+    const uint16_t* g = hp->planes[0] + hp_offset(hp, x + (mvx >> 2), y + (mvy >> 2));
+    const uint16_t* src = f->c->src + (size_t)y * f->c->pw + x;
+    int sad = 0;
+    for (int rr = 0; rr < h; rr++)
+        for (int c = 0; c < w; c++) sad += abs((int)src[(size_t)rr * f->c->pw + c] - (int)g[(size_t)rr * hp->stride + c]);
+    return sad;
+}
+
+/* ref_bits, enc/frame.rs:705-711 */
+static int ref_bits(const fc* f, int r) {
+    int n = f->c->nact;
+    if (n <= 1) return 0;
+    if (n == 2) return 1;
+    unsigned v = (unsigned)r + 1;
+    return 2 * (31 - __builtin_clz(v)) + 1;
+}
+
+typedef struct counters { uint32_t sad_px, satd_px; } counters;
+
+/* motion_search, enc/frame.rs:949-1019 (list 0). Returns the cost without the vector's bits. */
+static int motion_search(const fc* f, counters* cnt, int r, int mbx, int mby, rect4 pr, const int mvp[2], const int (*extra)[2],
+                         int nextra, int out[2]) {
+    const struct ironav_ctx* c = f->c;
+    int lam = c->lambda;
+    int x0 = mbx * 16 + pr.x * 4, y0 = mby * 16 + pr.y * 4, w = pr.w * 4, h = pr.h * 4;
+    int lo_x = -(x0 + 24) * 4, hi_x = (c->mb_w * 16 - x0 + 8) * 4;
+    int lo_y = -(y0 + 24) * 4, hi_y = (c->mb_h * 16 - y0 + 8) * 4;
+    int cxlo = maxi(lo_x, -2048), cxhi = mini(hi_x, 2047), cylo = maxi(lo_y, -512), cyhi = mini(hi_y, 511);
+#define CLX(v) clampi((v), cxlo, cxhi)
+#define CLY(v) clampi((v), cylo, cyhi)
+#define INTR(v) (((v) + 2) & ~3)
+#define COST_INT(mx, my) (cnt->sad_px += (uint32_t)(w * h), sad_int(f, r, x0, y0, w, h, (mx), (my)) + lam * mvd_bits((mx), (my), mvp[0], mvp[1]))
+    int cands[8][2];
+    int nc = 0;
+    cands[nc][0] = INTR(CLX(mvp[0]));
+    cands[nc][1] = INTR(CLY(mvp[1]));
+    nc++;
+    cands[nc][0] = 0;
+    cands[nc][1] = 0;
+    nc++;
+    static const int NB[3][2] = {{-1, 0}, {0, -1}, {4, -1}};
+    for (int k = 0; k < 3; k++) {
+        nbm n = nb_motion(f, mbx, mby, ZERO_MVS, NO_REF, 0, NB[k][0], NB[k][1]);
+        if (n.avail && n.ref == r) {
+            cands[nc][0] = INTR(CLX(n.mv[0]));
+            cands[nc][1] = INTR(CLY(n.mv[1]));
+            nc++;
+        }
+    }
+    for (int k = 0; k < nextra; k++) {
+        cands[nc][0] = INTR(CLX(extra[k][0]));
+        cands[nc][1] = INTR(CLY(extra[k][1]));
+        nc++;
+    }
+    int bx = 0, by = 0, bc = 0x7fffffff;
+    for (int k = 0; k < nc; k++) {
+        int cost = COST_INT(cands[k][0], cands[k][1]);
+        if (cost < bc) {
+            bx = cands[k][0];
+            by = cands[k][1];
+            bc = cost;
+        }
+    }
+    /* large diamond steps, then the small diamond (enc/frame.rs:973-988) */
+    static const int STEPS[3] = {16, 8, 4}, STEPS_FAST[2] = {8, 4};
+    const int* steps = c->fast ? STEPS_FAST : STEPS;
+    int nsteps = c->fast ? 2 : 3;
+    for (int si = 0; si < nsteps; si++) {
+        int step = steps[si];
+        int iters = step == 4 ? 32 : 4;
+        for (int it = 0; it < iters; it++) {
+            int moved = 0;
+            const int D[4][2] = {{-step, 0}, {step, 0}, {0, -step}, {0, step}};
+            for (int d = 0; d < 4; d++) {
+                int cx = CLX(bx + D[d][0]), cy = CLY(by + D[d][1]);
+                int cost = COST_INT(cx, cy);
+                if (cost < bc) {
+                    bx = cx;
+                    by = cy;
+                    bc = cost;
+                    moved = 1;
+                }
+            }
+            if (!moved) break;
+        }
+    }
+    /* live coding stops at the integer vector when it is already as good as the reference gets (990-992) */
+    if (c->fast && bc < (w * h) / 8 + lam) {
+        out[0] = bx;
+        out[1] = by;
+        return bc - lam * mvd_bits(bx, by, mvp[0], mvp[1]);
+    }
+    /* sub-sample refinement by SATD (994-1017) */
+    uint16_t pred[256];
+    const halfpel* hp = &c->refs[r].hp;
+#define COST_SUB(mx, my)                                                                                   \
+    (cnt->satd_px += (uint32_t)(w * h), halfpel_predict(hp, x0, y0, (mx), (my), w, h, pred),              \
+     satd_blk(f, x0, y0, w, h, pred) + lam * mvd_bits((mx), (my), mvp[0], mvp[1]))
+    bc = COST_SUB(bx, by);
+    static const int SQUARE[8][2] = {{-1, -1}, {0, -1}, {1, -1}, {-1, 0}, {1, 0}, {-1, 1}, {0, 1}, {1, 1}};
+    static const int DIAMOND[4][2] = {{0, -1}, {-1, 0}, {1, 0}, {0, 1}};
+    for (int stage = 0; stage < 2; stage++) {
+        if (c->fast && stage == 1) break;
+        int step = stage == 0 ? 2 : 1;
+        const int(*pts)[2] = stage == 0 ? SQUARE : DIAMOND;
+        int npts = stage == 0 ? 8 : 4;
+        int ccx = bx, ccy = by;
+        for (int k = 0; k < npts; k++) {
+            int cx = CLX(ccx + pts[k][0] * step), cy = CLY(ccy + pts[k][1] * step);
+            int cost = COST_SUB(cx, cy);
+            if (cost < bc) {
+                bx = cx;
+                by = cy;
+                bc = cost;
+            }
+        }
+    }
+    out[0] = bx;
+    out[1] = by;
+    return bc - lam * mvd_bits(bx, by, mvp[0], mvp[1]);
+#undef CLX
+#undef CLY
+#undef INTR
+#undef COST_INT
+#undef COST_SUB
+}
+
+typedef struct sub_st { int16_t mv[16][2]; int8_t ref[16]; uint32_t done; } sub_st;
+
+/* sub_search, enc/frame.rs:911-938 */
+static int sub_search(const fc* f, counters* cnt, int mbx, int mby, int r, int k, const int extra[2], sub_st* st, int* cost_out) {
+    int lam = f->c->lambda;
+    int ox = (k & 1) * 2, oy = (k >> 1) * 2;
+    int have = 0, best_s = 0, best_cost = 0;
+    sub_st best_t;
+    int ns = f->c->sub8 ? 4 : 1;
+    for (int s = 0; s < ns; s++) {
+        sub_st t = *st;
+        int cost = lam * (s == 0 ? 0 : 2);
+        for (int q = 0; q < NSUB[s]; q++) {
+            rect4 rr = SUB_[s][q];
+            rr.x += ox;
+            rr.y += oy;
+            int mvp[2], m[2];
+            pred_mv(f, mbx, mby, (const int16_t(*)[2])t.mv, t.ref, t.done, rr.x, rr.y, rr.w, 0, r, mvp);
+            int ex[1][2] = {{extra[0], extra[1]}};
+            int cst = motion_search(f, cnt, r, mbx, mby, rr, mvp, (const int(*)[2])ex, 1, m);
+            cost += cst + lam * mvd_bits(m[0], m[1], mvp[0], mvp[1]);
+            for (int by = rr.y; by < rr.y + rr.h; by++)
+                for (int bx = rr.x; bx < rr.x + rr.w; bx++) {
+                    t.mv[by * 4 + bx][0] = (int16_t)m[0];
+                    t.mv[by * 4 + bx][1] = (int16_t)m[1];
+                    t.ref[by * 4 + bx] = (int8_t)r;
+                    t.done |= 1u << (by * 4 + bx);
+                }
+        }
+        if (!have || cost < best_cost) {
+            have = 1;
+            best_s = s;
+            best_cost = cost;
+            best_t = t;
+        }
+    }
+    *st = best_t;
+    *cost_out = best_cost;
+    return best_s;
+}
+
+typedef struct inter_res { int part; int16_t mvs[16][2]; uint8_t sub[4]; int cost; int cost16; } inter_res;
+
+/* best_inter_ref, enc/frame.rs:852-905 */
+static void best_inter_ref(const fc* f, counters* cnt, int mbx, int mby, int r, inter_res* best) {
+    const struct ironav_ctx* c = f->c;
+    int lam = c->lambda;
+    int rb = lam * ref_bits(f, r);
+    int mvp[2];
+    mv_pred(f, mbx, mby, r, mvp);
+    /* col_mv of the newest reference (self.refp), enc/frame.rs:857,944-947 */
+    const colmv* col = &c->refs[0].col[(size_t)mby * c->mb_w + mbx];
+    int colv[1][2] = {{col->mv[0], col->mv[1]}};
+    int mv[2];
+    int cost = motion_search(f, cnt, r, mbx, mby, PARTS_[0][0], mvp, (const int(*)[2])colv, col->valid ? 1 : 0, mv);
+    memset(best, 0, sizeof(*best));
+    best->part = 0;
+    for (int i = 0; i < 16; i++) {
+        best->mvs[i][0] = (int16_t)mv[0];
+        best->mvs[i][1] = (int16_t)mv[1];
+    }
+    best->cost = cost + lam * (mvd_bits(mv[0], mv[1], mvp[0], mvp[1]) + 1) + rb;
+    best->cost16 = best->cost;
+    if (c->fast) return;
+    /* P_8x8 (868-876) */
+    sub_st st;
+    memset(&st, 0, sizeof(st));
+    uint8_t sub[4] = {0, 0, 0, 0};
+    int cost8 = lam * 9;
+    for (int k = 0; k < 4; k++) {
+        int ck;
+        sub[k] = (uint8_t)sub_search(f, cnt, mbx, mby, r, k, mv, &st, &ck);
+        cost8 += ck + rb;
+        if (cost8 >= best->cost) break;
+    }
+#define AT8(b) (st.mv[((b) / 2) * 8 + ((b) % 2) * 2])
+    if (cost8 < best->cost) {
+        rect4 rs[16];
+        int n = rects(3, sub, rs);
+        int16_t v8[16][2];
+        memset(v8, 0, sizeof(v8));
+        for (int q = 0; q < n; q++) {
+            v8[q][0] = st.mv[rs[q].y * 4 + rs[q].x][0];
+            v8[q][1] = st.mv[rs[q].y * 4 + rs[q].x][1];
+        }
+        best->part = 3;
+        memcpy(best->mvs, v8, sizeof(v8));
+        memcpy(best->sub, sub, 4);
+        best->cost = cost8;
+        for (int part = 1; part < 3; part++) {
+            int16_t mvs[16][2];
+            memset(mvs, 0, sizeof(mvs));
+            int pc = lam * 3;
+            for (int k = 0; k < 2; k++) {
+                int p[2];
+                part_mvp(f, mbx, mby, part, (const int16_t(*)[2])mvs, r, k, p);
+                int cands[2][2];
+                int i0 = part == 1 ? 2 * k : k, i1 = part == 1 ? 2 * k + 1 : k + 2;
+                cands[0][0] = AT8(i0)[0];
+                cands[0][1] = AT8(i0)[1];
+                cands[1][0] = AT8(i1)[0];
+                cands[1][1] = AT8(i1)[1];
+                int m[2];
+                int cc = motion_search(f, cnt, r, mbx, mby, PARTS_[part][k], p, (const int(*)[2])cands, 2, m);
+                mvs[k][0] = (int16_t)m[0];
+                mvs[k][1] = (int16_t)m[1];
+                pc += cc + lam * mvd_bits(m[0], m[1], p[0], p[1]) + rb;
+                if (pc >= best->cost) break;
+            }
+            if (pc < best->cost) {
+                best->part = part;
+                memcpy(best->mvs, mvs, sizeof(mvs));
+                memset(best->sub, 0, 4);
+                best->cost = pc;
+            }
+        }
+    }
+#undef AT8
+}
+
+/* best_inter, enc/frame.rs:839-849 */
+static void best_inter(const fc* f, counters* cnt, int mbx, int mby, ironav_mbresult* out) {
+    inter_res best, cur;
+    int have = 0, bestr = 0;
+    for (int r = 0; r < f->c->nact; r++) {
+        best_inter_ref(f, cnt, mbx, mby, r, &cur);
+        if (!have || cur.cost < best.cost) {
+            best = cur;
+            bestr = r;
+            have = 1;
+        }
+    }
+    out->part = (uint8_t)best.part;
+    for (int k = 0; k < 4; k++) {
+        out->refs[k] = (uint8_t)bestr;
+        out->sub[k] = best.sub[k];
+    }
+    memcpy(out->mvs, best.mvs, sizeof(best.mvs));
+    out->cost = best.cost;
+    out->cost16 = best.cost16;
+    out->flags |= IRONAV_RESULT_INTER;
+}
+
+/* The P_Skip vector and SAD of code_mb, enc/frame.rs:722-729 */
+static void skip_test(const fc* f, counters* cnt, int mbx, int mby, ironav_mbresult* out) {
+    int sv[2];
+    skip_mv(f, mbx, mby, sv);
+    uint16_t pred[256];
+    halfpel_predict(&f->c->refs[0].hp, mbx * 16, mby * 16, sv[0], sv[1], 16, 16, pred);
+    const uint16_t* src = f->c->src + (size_t)mby * 16 * f->c->pw + mbx * 16;
+    int sad = 0;
+    for (int i = 0; i < 256; i++) sad += abs((int)src[(size_t)(i / 16) * f->c->pw + i % 16] - (int)pred[i]);
+    cnt->sad_px += 256;
+    out->skip_mv[0] = (int16_t)sv[0];
+    out->skip_mv[1] = (int16_t)sv[1];
+    out->skip_sad = sad;
+}
+
+/* The MbState a decided macroblock leaves (finish_mb, enc/frame.rs:2281-2321): a P macroblock's
+ * vectors painted over its partitions and the reference index of each 8x8 block. */
+static void state_from_result(const ironav_mbresult* r, int skip, ironav_mbstate* s) {
+    memset(s, 0, sizeof(*s));
+    s->inter = 1;
+    if (skip) {
+        for (int i = 0; i < 16; i++) {
+            s->mvs[i][0] = r->skip_mv[0];
+            s->mvs[i][1] = r->skip_mv[1];
+        }
+        for (int k = 0; k < 4; k++) s->refs[k] = 0;
+        return;
+    }
+    rect4 rs[16];
+    int n = rects(r->part, r->sub, rs);
+    for (int q = 0; q < n; q++)
+        for (int by = rs[q].y; by < rs[q].y + rs[q].h; by++)
+            for (int bx = rs[q].x; bx < rs[q].x + rs[q].w; bx++) {
+                s->mvs[by * 4 + bx][0] = r->mvs[q][0];
+                s->mvs[by * 4 + bx][1] = r->mvs[q][1];
+            }
+    /* spread(part, refs) then the 8x8 block's first 4x4 block (2298-2300) */
+    for (int b8 = 0; b8 < 4; b8++) {
+        int blk = (b8 / 2) * 8 + (b8 % 2) * 2, bx = blk % 4, by = blk / 4, k = 0;
+        if (r->part == 1) k = by >= 2;
+        else if (r->part == 2) k = bx >= 2;
+        else if (r->part == 3) k = (by / 2) * 2 + bx / 2;
+        s->refs[b8] = (int8_t)r->refs[k];
+    }
+}
+
+static void analyse_mb(const fc* f, int mbx, int mby, int auto_policy, ironav_mbresult* out, ironav_mbstate* state_out) {
+    counters cnt = {0, 0};
+    memset(out, 0, sizeof(*out));
+    skip_test(f, &cnt, mbx, mby, out);
+    int skip = auto_policy && out->skip_sad < f->c->skip_thresh;
+    if (skip) out->flags |= IRONAV_RESULT_SKIP;
+    else best_inter(f, &cnt, mbx, mby, out);
+    out->sad_px = cnt.sad_px;
+    out->satd_px = cnt.satd_px;
+    if (state_out) state_from_result(out, skip, state_out);
+}
+
+/* ---------------------------------------------------------------------------------------------------
+ * The C ABI on the CPU
+ * ------------------------------------------------------------------------------------------------- */
+
+static void refpic_free(refpic* r) {
+    halfpel_free(&r->hp);
+    free(r->col);
+    r->col = NULL;
+}
+
+int ironav_ctx_create(ironav_ctx** out, int width, int height, int bd, int max_refs, int nslices, const int* band_rows) {
+    if (!out) return IRONAV_INVALID_ARGUMENT;
+    *out = NULL;
+    if (width <= 0 || height <= 0 || (width & 1) || (height & 1) || bd != 8) return IRONAV_INVALID_ARGUMENT;
+    int mb_w = (width + 15) / 16, mb_h = (height + 15) / 16;
+    if (mb_w > 1024 || mb_h > 1024 || max_refs < 1 || max_refs > 16 || nslices < 1 || nslices > mb_h) return IRONAV_INVALID_ARGUMENT;
+    if (band_rows) {
+        if (band_rows[0] != 0 || band_rows[nslices] != mb_h) return IRONAV_INVALID_ARGUMENT;
+        for (int i = 0; i < nslices; i++)
+            if (band_rows[i + 1] <= band_rows[i]) return IRONAV_INVALID_ARGUMENT;
+    }
+    struct ironav_ctx* c = (struct ironav_ctx*)calloc(1, sizeof(*c));
+    c->width = width;
+    c->height = height;
+    c->bd = bd;
+    c->mb_w = mb_w;
+    c->mb_h = mb_h;
+    c->pw = mb_w * 16;
+    c->ph = mb_h * 16;
+    c->max_refs = max_refs;
+    c->nslices = nslices;
+    c->band_start = (int*)calloc((size_t)mb_h, sizeof(int));
+    for (int i = 0; i < nslices; i++) {
+        int a = band_rows ? band_rows[i] : i * mb_h / nslices, b = band_rows ? band_rows[i + 1] : (i + 1) * mb_h / nslices;
+        for (int r = a; r < b; r++) c->band_start[r] = a;
+    }
+    c->src = (uint16_t*)calloc((size_t)c->pw * c->ph, sizeof(uint16_t));
+    c->refs = (refpic*)calloc((size_t)max_refs, sizeof(refpic));
+    c->threads = 1;
+    *out = c;
+    return IRONAV_OK;
+}
+
+int ironav_ctx_destroy(ironav_ctx* c) {
+    if (!c) return IRONAV_INVALID_ARGUMENT;
+    for (int i = 0; i < c->nrefs; i++) refpic_free(&c->refs[i]);
+    free(c->refs);
+    free(c->src);
+    free(c->band_start);
+    free(c);
+    return IRONAV_OK;
+}
+
+int ironav_ctx_dims(const ironav_ctx* c, int* mb_w, int* mb_h, int* sw, int* sh) {
+    if (!c) return IRONAV_INVALID_ARGUMENT;
+    if (mb_w) *mb_w = c->mb_w;
+    if (mb_h) *mb_h = c->mb_h;
+    if (sw) *sw = c->pw + 2 * PAD;
+    if (sh) *sh = c->ph + 2 * PAD;
+    return IRONAV_OK;
+}
+
+int ironav_ctx_set_stream(ironav_ctx* c, void* s) {
+    (void)s;
+    return c ? IRONAV_OK : IRONAV_INVALID_ARGUMENT;
+}
+
+/* Edge-repeated padding to whole macroblocks, H264Encoder::source, enc/mod.rs:502-519 */
+static void pad_plane(const uint8_t* y, int stride, int w, int h, int pw, int ph, uint16_t* out) {
+    for (int r = 0; r < ph; r++) {
+        const uint8_t* row = y + (size_t)mini(r, h - 1) * stride;
+        uint16_t* o = out + (size_t)r * pw;
+        for (int x = 0; x < w; x++) o[x] = row[x];
+        for (int x = w; x < pw; x++) o[x] = row[w - 1];
+    }
+}
+
+int ironav_set_source(ironav_ctx* c, const uint8_t* y, int stride) {
+    if (!c || !y || stride < c->width) return IRONAV_INVALID_ARGUMENT;
+    pad_plane(y, stride, c->width, c->height, c->pw, c->ph, c->src);
+    return IRONAV_OK;
+}
+
+int ironav_push_reference(ironav_ctx* c, const uint8_t* y, int stride, int w, int h, const ironav_mbstate* col) {
+    if (!c || !y) return IRONAV_INVALID_ARGUMENT;
+    if (!((w == c->width && h == c->height) || (w == c->pw && h == c->ph)) || stride < w) return IRONAV_INVALID_ARGUMENT;
+    if (c->nrefs == c->max_refs) {
+        refpic_free(&c->refs[c->max_refs - 1]);
+        c->nrefs--;
+    }
+    memmove(&c->refs[1], &c->refs[0], sizeof(refpic) * (size_t)c->nrefs);
+    refpic* r = &c->refs[0];
+    memset(r, 0, sizeof(*r));
+    uint16_t* luma = (uint16_t*)malloc(sizeof(uint16_t) * (size_t)c->pw * c->ph);
+    pad_plane(y, stride, w, h, c->pw, c->ph, luma);
+    halfpel_build(&r->hp, luma, c->pw, c->ph, c->bd);
+    free(luma);
+    size_t nmb = (size_t)c->mb_w * c->mb_h;
+    r->col = (colmv*)calloc(nmb, sizeof(colmv));
+    if (col)
+        for (size_t i = 0; i < nmb; i++)
+            if (col[i].inter) {
+                r->col[i].valid = 1;
+                r->col[i].mv[0] = col[i].mvs[5][0];
+                r->col[i].mv[1] = col[i].mvs[5][1];
+            }
+    c->nrefs++;
+    return IRONAV_OK;
+}
+
+int ironav_clear_references(ironav_ctx* c) {
+    if (!c) return IRONAV_INVALID_ARGUMENT;
+    for (int i = 0; i < c->nrefs; i++) refpic_free(&c->refs[i]);
+    c->nrefs = 0;
+    return IRONAV_OK;
+}
+
+int ironav_get_planes(ironav_ctx* c, int idx, uint8_t* out) {
+    if (!c || !out || idx < 0 || idx >= c->nrefs) return IRONAV_INVALID_ARGUMENT;
+    size_t n = (size_t)c->refs[idx].hp.stride * c->refs[idx].hp.sh;
+    for (int k = 0; k < 4; k++)
+        for (size_t i = 0; i < n; i++) out[k * n + i] = (uint8_t)c->refs[idx].hp.planes[k][i];
+    return IRONAV_OK;
+}
+
+int ironav_begin_p_picture(ironav_ctx* c, int qpp, int lambda, int skip_thresh, int nact, int fast, int sub8) {
+    if (!c || lambda < 1 || nact < 1 || nact > c->nrefs || qpp < 0 || qpp > 63) return IRONAV_INVALID_ARGUMENT;
+    c->qpp = qpp;
+    c->lambda = lambda;
+    c->skip_thresh = skip_thresh;
+    c->nact = nact;
+    c->fast = fast ? 1 : 0;
+    c->sub8 = sub8 ? 1 : 0;
+    return IRONAV_OK;
+}
+
+/* Threads for the replay mode's all-core run (oracle only; not part of the header). */
+int oracle_set_threads(ironav_ctx* c, int n) {
+    if (!c || n < 1) return IRONAV_INVALID_ARGUMENT;
+    c->threads = n;
+    return IRONAV_OK;
+}
+
+int ironav_analyse_picture_replay(ironav_ctx* c, const ironav_mbstate* states, ironav_mbresult* out) {
+    if (!c || !states || !out || c->nact < 1) return IRONAV_INVALID_ARGUMENT;
+    fc f = {c, states};
+    long n = (long)c->mb_w * c->mb_h;
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 16) num_threads(c->threads)
+#endif
+    for (long i = 0; i < n; i++) analyse_mb(&f, (int)(i % c->mb_w), (int)(i / c->mb_w), 0, &out[i], NULL);
+    return IRONAV_OK;
+}
+
+/* Replay over a subset of macroblocks (indices), for bounded CPU-baseline samples. */
+int oracle_analyse_replay_subset(ironav_ctx* c, const ironav_mbstate* states, const int* idx, int count, ironav_mbresult* out) {
+    if (!c || !states || !out || !idx || c->nact < 1) return IRONAV_INVALID_ARGUMENT;
+    fc f = {c, states};
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 16) num_threads(c->threads)
+#endif
+    for (int i = 0; i < count; i++) analyse_mb(&f, idx[i] % c->mb_w, idx[i] / c->mb_w, 0, &out[i], NULL);
+    return IRONAV_OK;
+}
+
+/* Auto mode: each slice band in raster order (FrameCoder::encode, enc/frame.rs:467-478), bands in
+ * parallel when threads > 1 (enc/mod.rs:620-628); the decision is the analysis policy. */
+int ironav_analyse_picture_auto(ironav_ctx* c, ironav_mbstate* states, ironav_mbresult* out) {
+    if (!c || !states || !out || c->nact < 1) return IRONAV_INVALID_ARGUMENT;
+    memset(states, 0, sizeof(ironav_mbstate) * (size_t)c->mb_w * c->mb_h);
+    fc f = {c, states};
+    int nb = 0;
+    int starts[1025];
+    for (int r = 0; r < c->mb_h; r++)
+        if (c->band_start[r] == r) starts[nb++] = r;
+    starts[nb] = c->mb_h;
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 1) num_threads(c->threads)
+#endif
+    for (int b = 0; b < nb; b++)
+        for (int mby = starts[b]; mby < starts[b + 1]; mby++)
+            for (int mbx = 0; mbx < c->mb_w; mbx++) {
+                size_t i = (size_t)mby * c->mb_w + mbx;
+                analyse_mb(&f, mbx, mby, 1, &out[i], &states[i]);
+            }
+    return IRONAV_OK;
+}
+
+int ironav_set_source_device(ironav_ctx* c, const uint8_t* d, int s) { (void)c; (void)d; (void)s; return IRONAV_HARDWARE_UNAVAILABLE; }
+int ironav_push_reference_device(ironav_ctx* c, const uint8_t* d, int s, int w, int h, const ironav_mbstate* col) {
+    (void)c; (void)d; (void)s; (void)w; (void)h; (void)col;
+    return IRONAV_HARDWARE_UNAVAILABLE;
+}
+int ironav_analyse_picture_replay_device(ironav_ctx* c, const ironav_mbstate* s, ironav_mbresult* o) { (void)c; (void)s; (void)o; return IRONAV_HARDWARE_UNAVAILABLE; }
+int ironav_analyse_picture_auto_device(ironav_ctx* c, ironav_mbstate* s, ironav_mbresult* o) { (void)c; (void)s; (void)o; return IRONAV_HARDWARE_UNAVAILABLE; }
+int ironav_ctx_sync(ironav_ctx* c) { return c ? IRONAV_OK : IRONAV_INVALID_ARGUMENT; }
+
+/* ---------------------------------------------------------------------------------------------------
+ * 16-bit entry points for the interpolation known-answer test (8- and 10-bit)
+ * ------------------------------------------------------------------------------------------------- */
+
+typedef struct oracle_halfpel { halfpel hp; } oracle_halfpel;
+
+oracle_halfpel* oracle_halfpel_new(const uint16_t* luma, int pw, int ph, int bd) {
+    oracle_halfpel* o = (oracle_halfpel*)calloc(1, sizeof(*o));
+    halfpel_build(&o->hp, luma, pw, ph, bd);
+    return o;
+}
+void oracle_halfpel_free(oracle_halfpel* o) {
+    if (!o) return;
+    halfpel_free(&o->hp);
+    free(o);
+}
+void oracle_halfpel_predict(const oracle_halfpel* o, int x, int y, int mvx, int mvy, int w, int h, uint16_t* out) {
+    halfpel_predict(&o->hp, x, y, mvx, mvy, w, h, out);
+}
+/* Copies plane k (sw x sh samples). */
+void oracle_halfpel_plane(const oracle_halfpel* o, int k, uint16_t* out) {
+    memcpy(out, o->hp.planes[k], sizeof(uint16_t) * (size_t)o->hp.stride * o->hp.sh);
+}
+int oracle_satd4(const int* d) { return satd4(d); }

@@ -1,0 +1,229 @@
+"""GPU parity: the sm_100a library (libironav_inter_cuda.so) against the oracle, through the C ABI.
+
+Everything here is integer work, so the bar is bit-exactness: planes byte for byte, and every field
+of every macroblock's result (vectors, costs, partitions, sub-partitions, references, P_Skip vector
+and SAD, evaluation counts) and decision.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from ironav_b200.inter import MBRESULT_DTYPE, MBSTATE_DTYPE, InterStage, IronavError
+from ironav_b200.synth import Sequence
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def assert_same(a, b, what):
+    if np.array_equal(a, b):
+        return
+    bad = np.nonzero(a != b)[0]
+    i = int(bad[0])
+    fields = [f for f in a.dtype.names if not np.array_equal(a[i][f], b[i][f])]
+    raise AssertionError(f"{what}: {len(bad)} macroblocks differ; first {i}, fields {fields}: "
+                         f"got {a[i][fields[0]]} want {b[i][fields[0]]}")
+
+
+def stage_pair(oracle_lib, cuda_lib, w, h, **kw):
+    return InterStage(w, h, lib=oracle_lib, **kw), InterStage(w, h, lib=cuda_lib, **kw)
+
+
+def run_both(pair, fn):
+    return fn(pair[0]), fn(pair[1])
+
+
+@pytest.mark.parametrize("size", [(352, 288), (34, 18), (64, 48), (1920, 1080)])
+def test_planes_byte_exact(oracle_lib, cuda_lib, size):
+    w, h = size
+    rng = np.random.default_rng(w * 7 + h)
+    luma = rng.integers(0, 256, size=(h, w), dtype=np.uint8)
+    o, c = stage_pair(oracle_lib, cuda_lib, w, h)
+    o.push_reference(luma)
+    c.push_reference(luma)
+    po, pc = o.planes(0), c.planes(0)
+    for k, name in enumerate("Gbhj"):
+        assert np.array_equal(po[k], pc[k]), f"plane {name} of {w}x{h} differs at {np.argwhere(po[k] != pc[k])[:3]}"
+
+
+def test_planes_of_a_macroblock_aligned_reconstruction(oracle_lib, cuda_lib):
+    """A reconstruction is 16*mb_w x 16*mb_h and is used as is (no edge repetition inside it)."""
+    w, h = 40, 20  # mb 3 x 2
+    rng = np.random.default_rng(5)
+    recon = rng.integers(0, 256, size=(32, 48), dtype=np.uint8)
+    o, c = stage_pair(oracle_lib, cuda_lib, w, h)
+    o.push_reference(recon)
+    c.push_reference(recon)
+    assert np.array_equal(o.planes(0), c.planes(0))
+
+
+def test_golden_cases(cuda_lib):
+    """The CUDA library reproduces the committed oracle fixtures (tests/golden/oracle_cif.npz)."""
+    from tests.golden.make_golden import CASES, run_case
+
+    data = np.load(os.path.join(GOLDEN, "oracle_cif.npz"))
+    for name, case in CASES.items():
+        luma_hash, states, res, rstates, rres = run_case(cuda_lib, **case)
+        assert luma_hash == str(data[f"{name}_hash"]), f"{name}: synthetic input changed"
+        assert_same(states, data[f"{name}_states"].view(MBSTATE_DTYPE), f"{name} decisions")
+        assert_same(res, data[f"{name}_results"].view(MBRESULT_DTYPE), f"{name} auto results")
+        assert_same(rres, data[f"{name}_replay"].view(MBRESULT_DTYPE), f"{name} replay results")
+
+
+def _sequence_case(oracle_lib, cuda_lib, cfg, qp, nslices, src=2, size=None, **pic):
+    seq = Sequence.config(cfg, src + 1, size=size)
+    f = [seq.frame(t) for t in range(src + 1)]
+    o, c = stage_pair(oracle_lib, cuda_lib, seq.width, seq.height, nslices=nslices)
+    oracle_lib.oracle_set_threads(o.ctx, os.cpu_count() or 1)
+    # the reference picture's own decisions give the co-located candidates
+    for st in (o, c):
+        st.push_reference(f[src - 2])
+        st.set_source(f[src - 1])
+        st.begin_p_picture(qp)
+    col_o, _ = o.analyse_auto()
+    col_c, _ = c.analyse_auto()
+    assert_same(col_c, col_o, "decisions of the reference picture")
+    for st in (o, c):
+        st.clear_references()
+        st.push_reference(f[src - 1], col=col_o)
+        st.set_source(f[src])
+        st.begin_p_picture(qp, **pic)
+    return o, c
+
+
+@pytest.mark.parametrize("qp", [22, 27, 32])
+def test_1080p_auto_and_replay(oracle_lib, cuda_lib, qp):
+    o, c = _sequence_case(oracle_lib, cuda_lib, "1080p", qp, nslices=8)
+    so, ro = o.analyse_auto()
+    sc, rc = c.analyse_auto()
+    assert_same(sc, so, f"1080p qp{qp} auto decisions")
+    assert_same(rc, ro, f"1080p qp{qp} auto results")
+    assert_same(c.analyse_replay(so), o.analyse_replay(so), f"1080p qp{qp} replay")
+
+
+def test_4k_replay(oracle_lib, cuda_lib):
+    o, c = _sequence_case(oracle_lib, cuda_lib, "4k", 27, nslices=16)
+    so, ro = o.analyse_auto()
+    sc, rc = c.analyse_auto()
+    assert_same(sc, so, "4k auto decisions")
+    assert_same(c.analyse_replay(so), o.analyse_replay(so), "4k replay")
+
+
+@pytest.mark.parametrize("mode", [dict(fast=True), dict(sub8=True), dict(fast=False)])
+def test_modes_720p(oracle_lib, cuda_lib, mode):
+    o, c = _sequence_case(oracle_lib, cuda_lib, "1080p", 20 if mode.get("sub8") else 27, nslices=5, size=(1280, 720),
+                          **mode)
+    so, ro = o.analyse_auto()
+    sc, rc = c.analyse_auto()
+    assert_same(sc, so, f"{mode} decisions")
+    assert_same(rc, ro, f"{mode} results")
+
+
+def test_random_decisions_exercise_the_clamps(oracle_lib, cuda_lib):
+    """Replay against arbitrary neighbour vectors, up to the level limits (+-2048 x +-512 quarter samples):
+    the predictors and candidates land on the search bounds, where clamped diamond moves are scored on
+    demand."""
+    seq = Sequence.config("cif", 3)
+    o, c = stage_pair(oracle_lib, cuda_lib, 352, 288, nslices=2)
+    rng = np.random.default_rng(11)
+    nmb = o.nmb
+    col = np.zeros(nmb, dtype=MBSTATE_DTYPE)
+    col["inter"] = rng.integers(0, 2, nmb)
+    col["mvs"] = rng.integers(-600, 600, size=(nmb, 16, 2))
+    for st in (o, c):
+        st.push_reference(seq.frame(0), col=col)
+        st.set_source(seq.frame(1))
+        st.begin_p_picture(26)
+    states = np.zeros(nmb, dtype=MBSTATE_DTYPE)
+    states["inter"] = rng.integers(0, 4, nmb) > 0
+    states["refs"] = np.where(states["inter"][:, None] == 1, 0, -1)
+    mv = np.stack([rng.integers(-2048, 2048, size=(nmb, 16)), rng.integers(-512, 512, size=(nmb, 16))], axis=-1)
+    small = rng.integers(0, 2, size=(nmb, 1, 1)) == 1
+    states["mvs"] = np.where(small, mv // 64, mv)
+    assert_same(c.analyse_replay(states), o.analyse_replay(states), "replay on random decisions")
+
+
+@pytest.mark.parametrize("size", [(16, 16), (32, 16), (48, 32), (80, 64)])
+def test_small_pictures(oracle_lib, cuda_lib, size):
+    w, h = size
+    rng = np.random.default_rng(w + 100 * h)
+    base = rng.integers(0, 256, size=(h + 40, w + 40), dtype=np.uint8)
+    ref, src = base[:h, :w].copy(), base[3:h + 3, 5:w + 5].copy()
+    o, c = stage_pair(oracle_lib, cuda_lib, w, h, max_refs=2, nslices=min(2, (h + 15) // 16))
+    for st in (o, c):
+        st.push_reference(base[7:h + 7, 2:w + 2].copy())
+        st.push_reference(ref)
+        st.set_source(src)
+        st.begin_p_picture(24, nrefs_active=2)
+    so, ro = o.analyse_auto()
+    sc, rc = c.analyse_auto()
+    assert_same(sc, so, f"{size} decisions")
+    assert_same(rc, ro, f"{size} results")
+    assert_same(c.analyse_replay(so), o.analyse_replay(so), f"{size} replay")
+
+
+def test_device_forms_match_host_forms(cuda_lib):
+    import torch
+
+    seq = Sequence.config("cif", 2)
+    f0, f1 = seq.frame(0), seq.frame(1)
+    st = InterStage(352, 288, nslices=2, lib=cuda_lib)
+    st.push_reference(f0)
+    st.set_source(f1)
+    st.begin_p_picture(26)
+    states, res = st.analyse_auto()
+    rep = st.analyse_replay(states)
+
+    d = InterStage(352, 288, nslices=2, lib=cuda_lib)
+    stream = torch.cuda.current_stream()
+    d.set_stream(stream.cuda_stream)
+    t0 = torch.from_numpy(f0).cuda()
+    t1 = torch.from_numpy(f1).cuda()
+    d.push_reference_device(t0.data_ptr(), 352, 352, 288, None)
+    d.set_source_device(t1.data_ptr(), 352)
+    d.begin_p_picture(26)
+    ds = torch.zeros(d.nmb * 72, dtype=torch.uint8, device="cuda")
+    dr = torch.zeros(d.nmb * 104, dtype=torch.uint8, device="cuda")
+    d.analyse_auto_device(ds.data_ptr(), dr.data_ptr())
+    d.sync()
+    assert_same(ds.cpu().numpy().view(MBSTATE_DTYPE), states, "device auto decisions")
+    assert_same(dr.cpu().numpy().view(MBRESULT_DTYPE), res, "device auto results")
+    d.analyse_replay_device(ds.data_ptr(), dr.data_ptr())
+    d.sync()
+    assert_same(dr.cpu().numpy().view(MBRESULT_DTYPE), rep, "device replay results")
+
+
+def test_wavefront_wait_times_out_and_the_context_recovers(oracle_lib, cuda_lib):
+    """A macroblock whose decision is never published (the test withholds it) makes the waits behind it
+    give up after a bounded number of polls; the call reports a timeout and the next call works."""
+    seq = Sequence.config("cif", 2)
+    c = InterStage(352, 288, nslices=2, lib=cuda_lib)
+    o = InterStage(352, 288, nslices=2, lib=oracle_lib)
+    for st in (o, c):
+        st.push_reference(seq.frame(0))
+        st.set_source(seq.frame(1))
+        st.begin_p_picture(26)
+    assert cuda_lib.ironav_debug_wait_limit(c.ctx, 20000) == 0
+    assert cuda_lib.ironav_debug_withhold(c.ctx, 5) == 0
+    with pytest.raises(IronavError) as e:
+        c.analyse_auto()
+    assert e.value.status == 100
+    assert cuda_lib.ironav_debug_withhold(c.ctx, -1) == 0
+    sc, rc = c.analyse_auto()
+    so, ro = o.analyse_auto()
+    assert_same(sc, so, "decisions after a timeout")
+    assert_same(rc, ro, "results after a timeout")
+
+
+def test_bad_arguments_are_rejected(cuda_lib):
+    with pytest.raises(IronavError) as e:
+        InterStage(351, 288, lib=cuda_lib)
+    assert e.value.status == 3
+    st = InterStage(64, 48, lib=cuda_lib)
+    with pytest.raises(IronavError) as e:
+        st.begin_p_picture(26)  # no reference yet
+    assert e.value.status == 3
+    with pytest.raises(IronavError):
+        st.analyse_replay(np.zeros(st.nmb, dtype=MBSTATE_DTYPE))
