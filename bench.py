@@ -49,6 +49,9 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="bound on the CPU baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--ring", type=int, default=RING,
+                   help="pictures in the ring (fewer than 36 fits in L2: for profiling runs only)")
+    p.add_argument("--no-e2e", action="store_true", help="skip the host-buffer pass (profiling runs)")
     return p.parse_args()
 
 
@@ -136,12 +139,12 @@ def cpu_baseline(frames, states, seconds: float):
     from ironav_b200.inter import InterStage
 
     lib = oracle_library()
-    cores = os.cpu_count() or 1
+    cores = host_cores()
     st = InterStage(WIDTH, HEIGHT, nslices=NSLICES, lib=lib)
     lib.oracle_set_threads(st.ctx, cores)
     done_mb, elapsed, pics = 0, 0.0, 0
-    t = 1
-    while elapsed < seconds and t < len(frames):
+    while elapsed < seconds:
+        t = 1 + pics % (len(frames) - 1)
         st.clear_references()
         st.push_reference(frames[t - 1], col=states[t - 1] if t >= 2 else None)
         st.set_source(frames[t])
@@ -151,11 +154,17 @@ def cpu_baseline(frames, states, seconds: float):
         elapsed += time.perf_counter() - t0
         done_mb += st.nmb
         pics += 1
-        t += 1
     st.close()
     return {"value": done_mb / elapsed, "unit": "MB/s", "cores": cores, "kind": "port",
             "sample": f"{pics} pictures of the 1080p ring ({done_mb} macroblocks), replay mode, "
                       f"{cores} threads, {elapsed:.2f} s; half-sample planes built outside the timing"}
+
+
+def host_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
 
 
 def run_reference(args, rank, world):
@@ -166,7 +175,7 @@ def run_reference(args, rank, world):
     from ironav_b200.inter import InterStage
 
     lib = oracle_library()
-    cores = os.cpu_count() or 1
+    cores = host_cores()
     nfr = args.steps + args.warmup + 2
     frames = make_frames(0, min(nfr, RING))
     # decisions of every picture by the oracle's own auto mode (the reference's slice loop)
@@ -217,7 +226,9 @@ def config_dict():
 
 
 def main():
+    global RING
     args = parse()
+    RING = max(3, args.ring)
     rank, world, local = dist_setup(args)
     if args.impl == "reference":
         run_reference(args, rank, world)
@@ -305,7 +316,7 @@ def main():
     hbm = measured_hbm()
 
     # end to end through the host-buffer C ABI, pinned host memory
-    e2e = run_e2e(args, st, frames, d_states, nmb, world, torch, dist, dev, stream)
+    e2e = None if args.no_e2e else run_e2e(args, st, frames, d_states, nmb, world, torch, dist, dev, stream)
 
     line = {
         "metric": METRIC, "value": value, "unit": "MB/s", "n_gpus": world, "steps": args.steps,

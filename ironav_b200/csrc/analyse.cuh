@@ -170,7 +170,7 @@ class MbWarp {
     }
 
     // pred_mv, enc/frame.rs:543-570
-    __device__ void pred_mv(const BlkState* cur, int bx, int by, int w, int dir, int rf, int& ox, int& oy) const {
+    __device__ __noinline__ void pred_mv(const BlkState* cur, int bx, int by, int w, int dir, int rf, int& ox, int& oy) const {
         Nb a = nb_motion(cur, bx - 1, by);
         Nb b = nb_motion(cur, bx, by - 1);
         Nb c = nb_motion(cur, bx + w, by - 1);
@@ -204,7 +204,7 @@ class MbWarp {
     // ---- scoring -------------------------------------------------------------------------------------
 
     // Integer SAD (sad_int, enc/frame.rs:662-671) + lambda * mvd_bits of S.cand[0..n) -> S.cost.
-    __device__ void sad_batch(int r, int bx, int by, int w, int h, int n, int mvpx, int mvpy) {
+    __device__ __noinline__ void sad_batch(int r, int bx, int by, int w, int h, int n, int mvpx, int mvpy) {
         const int cb = n <= 1 ? 0 : (n <= 2 ? 1 : (n <= 4 ? 2 : 3));
         const int c = lane & ((1 << cb) - 1), rg = lane >> cb, nrg = 32 >> cb;
         const int cpr = w >= 16 ? 2 : 1;           // 8-sample chunks per row (4-sample rows when w == 4)
@@ -240,7 +240,7 @@ class MbWarp {
     // Quarter-sample prediction (HalfPel::predict, enc/subpel.rs:122-145) scored by SATD (satd,
     // enc/frame.rs:641-659) + lambda * mvd_bits, or by SAD when `sad` (the P_Skip test), for
     // S.cand[0..n) -> S.cost.
-    __device__ void pred_batch(int r, int bx, int by, int w, int h, int n, int mvpx, int mvpy, bool sad) {
+    __device__ __noinline__ void pred_batch(int r, int bx, int by, int w, int h, int n, int mvpx, int mvpy, bool sad) {
         const int nbw = w >> 2, nblk = nbw * (h >> 2), total = n * nblk;
         if (lane < n) S.cost[lane] = 0;
         __syncwarp();
@@ -288,7 +288,7 @@ class MbWarp {
 
     // ---- motion_search, enc/frame.rs:949-1019 --------------------------------------------------------
 
-    __device__ int motion_search(int r, Rect4 pr, int mvpx, int mvpy, const int2* extra, int nextra, int& ox, int& oy) {
+    __device__ __noinline__ int motion_search(int r, Rect4 pr, int mvpx, int mvpy, const int2* extra, int nextra, int& ox, int& oy) {
         const int lam = P.lambda;
         const int x0 = mbx * 16 + pr.x * 4, y0 = mby * 16 + pr.y * 4, w = pr.w * 4, h = pr.h * 4;
         const int cxlo = max(-(x0 + 24) * 4, -2048), cxhi = min((P.mb_w * 16 - x0 + 8) * 4, 2047);
@@ -521,7 +521,7 @@ class MbWarp {
     }
 
     // sub_search, enc/frame.rs:911-938: returns sub_mb_type, cost in `cost`; leaves the block in S.st.
-    __device__ int sub_search(int r, int k, int ex, int ey, int& cost_out) {
+    __device__ __noinline__ int sub_search(int r, int k, int ex, int ey, int& cost_out) {
         const int lam = P.lambda;
         const int ox = (k & 1) * 2, oy = (k >> 1) * 2;
         const int ns = P.sub8 ? 4 : 1;
