@@ -157,6 +157,35 @@ int ironav_analyse_picture_auto_device(ironav_ctx* ctx, ironav_mbstate* d_out_st
  * wait that gave up). */
 int ironav_ctx_sync(ironav_ctx* ctx);
 
+/* ---- analysis without allocation ------------------------------------------------------------------ */
+
+/* No counterpart in the reference: an entry point for callers that cannot allocate device memory (a
+ * host callback or real-time thread with a fixed memory budget, a custom allocator that owns all device
+ * memory, a plugin host that only hands out its own buffers), which therefore cannot create an
+ * ironav_ctx. It runs the auto-mode analysis of one P picture against one reference picture, with every
+ * input and output in the caller's device memory, and allocates nothing (no cudaMalloc, no library
+ * allocation): its scratch (progress flags, counters, slice bands, co-located vectors) is one fixed
+ * array of about 444 KB in the library's device memory, which every GPU that loads the library keeps
+ * until the process exits.
+ *   d_src      the source, padded to whole macroblocks (16*mb_w x 16*mb_h, edges repeated as
+ *              ironav_set_source does), 16-byte aligned, rows src_stride bytes apart (a multiple of 16)
+ *   d_ref      the reference luma, ref_w x ref_h = width x height or 16*mb_w x 16*mb_h, rows ref_stride apart
+ *   d_col      the reference picture's own decisions (mb_w*mb_h) or NULL when it was intra coded
+ *   d_planes   out: its half-sample planes G, b, h, j (4 * sw * sh bytes, 4-byte aligned)
+ *   d_states   out: the decisions (mb_w*mb_h); d_results: out, the results (mb_w*mb_h)
+ *   stream     cudaStream_t for the work (NULL: the legacy default stream)
+ * At most IRONAV_NOALLOC_MAX_MBS macroblocks (larger pictures: IRONAV_INVALID_ARGUMENT). The call
+ * returns when the work is done (IRONAV_TIMEOUT if a wavefront wait gave up). Every call uses the same
+ * scratch array and clears what must start at zero; calls that overlap on the GPU (other streams or
+ * host threads) race on it, so make them one after another. The first call on a device looks up the
+ * array's address with that device current: make it before any stream capture. */
+#define IRONAV_NOALLOC_MAX_MBS 36864
+int ironav_analyse_auto_noalloc(const uint8_t* d_src, int src_stride, const uint8_t* d_ref, int ref_stride,
+                                int ref_w, int ref_h, const ironav_mbstate* d_col, int width, int height,
+                                int nslices, int qp_prime, int lambda, int skip_thresh, int fast, int sub8,
+                                uint8_t* d_planes, ironav_mbstate* d_states, ironav_mbresult* d_results,
+                                void* stream);
+
 #ifdef __cplusplus
 }
 #endif

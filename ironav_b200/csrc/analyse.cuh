@@ -29,7 +29,7 @@ constexpr int K2_WARPS = 4;  // warps per CTA; each warp works alone
 constexpr unsigned FULL = 0xffffffffu;
 
 // MIX, enc/subpel.rs:26-38, packed per [fy][fx]: pa | ax<<2 | ay<<3 | pb<<4 | bx<<6 | by<<7
-__constant__ uint8_t c_mix[16] = {
+static __constant__ uint8_t c_mix[16] = {
     0x00, 0x10, 0x11, 0x14,
     0x20, 0x21, 0x31, 0x61,
     0x22, 0x32, 0x33, 0x63,
@@ -40,11 +40,11 @@ struct Rect4 {
     int x, y, w, h;
 };
 
-__device__ __constant__ int8_t c_parts[4][4][4] = {
+static __device__ __constant__ int8_t c_parts[4][4][4] = {
     {{0, 0, 4, 4}}, {{0, 0, 4, 2}, {0, 2, 4, 2}}, {{0, 0, 2, 4}, {2, 0, 2, 4}}, {{0, 0, 2, 2}, {2, 0, 2, 2}, {0, 2, 2, 2}, {2, 2, 2, 2}}};
-__device__ __constant__ int8_t c_sub[4][4][4] = {
+static __device__ __constant__ int8_t c_sub[4][4][4] = {
     {{0, 0, 2, 2}}, {{0, 0, 2, 1}, {0, 1, 2, 1}}, {{0, 0, 1, 2}, {1, 0, 1, 2}}, {{0, 0, 1, 1}, {1, 0, 1, 1}, {0, 1, 1, 1}, {1, 1, 1, 1}}};
-__device__ __constant__ int8_t c_nsub[4] = {1, 2, 2, 4};
+static __device__ __constant__ int8_t c_nsub[4] = {1, 2, 2, 4};
 
 // Vector state of the 4x4 blocks of the macroblock being analysed (nb_motion's cur/cref/done).
 struct BlkState {
@@ -760,7 +760,7 @@ __device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
 
 // Waits until macroblock `m`'s decision is published, at most P.wait_limit polls. Returns false when
 // it gave up or another warp already did (the launch is then abandoned and the host reports a timeout).
-__device__ bool wait_published(const AnalyseParams& P, int m) {
+static __device__ bool wait_published(const AnalyseParams& P, int m) {
     for (unsigned i = 0;; i++) {
         if (ld_acquire(&P.flags[m]) == P.epoch) return true;
         if (ld_acquire(P.err) != 0) return false;

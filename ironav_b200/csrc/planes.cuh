@@ -26,7 +26,7 @@ __device__ __forceinline__ uint32_t k1_clip8(int v) { return (uint32_t)min(max(v
 // luma: w x h samples, rows `stride` apart. Samples outside it repeat its edges, which is both the
 // macroblock padding of H264Encoder::source (enc/mod.rs:502-519) when w x h is the picture size and
 // the plane border of round1 (enc/subpel.rs:72-76).
-__global__ void __launch_bounds__(K1_THREADS) halfpel_planes_kernel(const uint8_t* __restrict__ luma, int stride, int w, int h,
+static __global__ void __launch_bounds__(K1_THREADS) halfpel_planes_kernel(const uint8_t* __restrict__ luma, int stride, int w, int h,
                                                                       uint8_t* __restrict__ out, long long psize, int sw, int sh) {
     __shared__ int g[K1_TH + 5][K1_TW + 8];       // integer samples, column c <-> x0 - 2 + c
     __shared__ int b1[K1_TH + 5][K1_TW];          // unrounded horizontal sums at x0 + c
@@ -74,7 +74,7 @@ __global__ void __launch_bounds__(K1_THREADS) halfpel_planes_kernel(const uint8_
 
 // The co-located vector of each macroblock (col_mv, enc/frame.rs:944-947) from the reference
 // picture's own decisions; none when the picture was intra coded (states == nullptr).
-__global__ void col_extract_kernel(const ironav_mbstate* __restrict__ states, ColMv* __restrict__ col, int nmb) {
+static __global__ void col_extract_kernel(const ironav_mbstate* __restrict__ states, ColMv* __restrict__ col, int nmb) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nmb) return;
     ColMv c;
@@ -91,7 +91,7 @@ __global__ void col_extract_kernel(const ironav_mbstate* __restrict__ states, Co
 
 // Repeats the right and bottom edges of a w x h picture stored in a pw x ph buffer (rows pw apart)
 // to whole macroblocks (H264Encoder::source, enc/mod.rs:502-519). Reads only the w x h part.
-__global__ void pad_edges_kernel(uint8_t* __restrict__ p, int w, int h, int pw, int ph) {
+static __global__ void pad_edges_kernel(uint8_t* __restrict__ p, int w, int h, int pw, int ph) {
     int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
     if (x >= pw || y >= ph || (x < w && y < h)) return;
     p[(size_t)y * pw + x] = p[(size_t)min(y, h - 1) * pw + min(x, w - 1)];

@@ -69,6 +69,7 @@ EXPORTS = (
     "ironav_begin_p_picture", "ironav_analyse_picture_replay", "ironav_analyse_picture_auto",
     "ironav_set_source_device", "ironav_push_reference_device",
     "ironav_analyse_picture_replay_device", "ironav_analyse_picture_auto_device", "ironav_ctx_sync",
+    "ironav_analyse_auto_noalloc",
 )
 
 
@@ -107,6 +108,11 @@ def _declare(lib: ctypes.CDLL) -> ctypes.CDLL:
     lib.ironav_analyse_picture_replay_device.argtypes = [_VP, _VP, _VP]
     lib.ironav_analyse_picture_auto_device.argtypes = [_VP, _VP, _VP]
     lib.ironav_ctx_sync.argtypes = [_VP]
+    if hasattr(lib, "ironav_analyse_auto_noalloc"):
+        # (d_src, src_stride, d_ref, ref_stride, ref_w, ref_h, d_col, width, height, nslices, qp_prime, lambda,
+        #  skip_thresh, fast, sub8, d_planes, d_states, d_results, stream)
+        lib.ironav_analyse_auto_noalloc.argtypes = [_VP, _I, _VP, _I, _I, _I, _VP, _I, _I, _I, _I, _I, _I, _I, _I,
+                                                    _VP, _VP, _VP, _VP]
     for name in ("ironav_debug_withhold", "ironav_debug_wait_limit"):
         if hasattr(lib, name):
             getattr(lib, name).argtypes = [_VP, ctypes.c_int if name.endswith("withhold") else ctypes.c_uint]

@@ -999,3 +999,11 @@ void oracle_halfpel_plane(const oracle_halfpel* o, int k, uint16_t* out) {
     memcpy(out, o->hp.planes[k], sizeof(uint16_t) * (size_t)o->hp.stride * o->hp.sh);
 }
 int oracle_satd4(const int* d) { return satd4(d); }
+
+/* Device-memory entry point of the CUDA library; the CPU library has no device memory. */
+int ironav_analyse_auto_noalloc(const uint8_t* d_src, int src_stride, const uint8_t* d_ref, int ref_stride, int ref_w, int ref_h,
+                                const ironav_mbstate* d_col, int width, int height, int nslices, int qp_prime, int lambda,
+                                int skip_thresh, int fast, int sub8, uint8_t* d_planes, ironav_mbstate* d_states,
+                                ironav_mbresult* d_results, void* stream) {
+    return IRONAV_HARDWARE_UNAVAILABLE;
+}
