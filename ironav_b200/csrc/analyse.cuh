@@ -34,13 +34,13 @@ constexpr int K2_WARPS = 4;  // warps per CTA; each warp works alone
 constexpr unsigned FULL = 0xffffffffu;
 constexpr int BIG = 0x7fffffff;
 
-// MIX, enc/subpel.rs:26-38, packed per [fy][fx]: pa | ax<<2 | ay<<3 | pb<<4 | bx<<6 | by<<7
-static __constant__ uint8_t c_mix[16] = {
-    0x00, 0x10, 0x11, 0x14,
-    0x20, 0x21, 0x31, 0x61,
-    0x22, 0x32, 0x33, 0x63,
-    0x28, 0x92, 0x93, 0x96,
-};
+// MIX, enc/subpel.rs:26-38: per [fy][fx] the byte pa | ax<<2 | ay<<3 | pb<<4 | bx<<6 | by<<7 (planes G=0,
+// b=1, h=2, j=3), four entries per 32-bit word so a lane picks its entry from registers (no constant-memory
+// reads that would serialise when the lanes' vectors differ).
+__device__ __forceinline__ unsigned mix_entry(int fx, int fy) {
+    const unsigned w = fy == 0 ? 0x14111000u : (fy == 1 ? 0x61312120u : (fy == 2 ? 0x63333222u : 0x96939228u));
+    return (w >> (8 * fx)) & 0xffu;
+}
 
 // PARTS and SUB, enc/frame.rs:182,204: (x, y, w, h) in 4x4 blocks
 static __device__ __constant__ int8_t c_parts[4][4][4] = {
@@ -59,7 +59,8 @@ struct WarpSmem {
     Blk st[16];               // P_8x8: blocks decided so far (sub_search's `st`)
     Blk t[16];                // trial blocks (sub_search's `t`, part_mvps's `cur`)
     Blk bt[16];               // best trial
-    int cost[16];             // sub-sample batch sums
+    int2 cand[16];            // the sub-sample batch's vectors
+    int cost[16];             // sub-sample batch sums (and a clamped round's square)
     int16_t best_mvs[16][2];  // best_inter_ref's running best, in coding order
     int16_t win_mvs[16][2];   // best over the references
     ironav_mbresult res;
@@ -184,10 +185,12 @@ class MbWarp {
         int sad = 0;
         if (valid) {
             const int x0 = mbx * 16 + bx * 4, y0 = mby * 16 + by * 4;
-            const uint8_t* G = P.planes[r] + (long long)(y0 + (py >> 2) + PAD) * P.sw + (x0 + (px >> 2) + PAD);
+            const int row0 = lane >> 3;
+            const uint8_t* G = P.planes[r] + (unsigned)((y0 + (py >> 2) + PAD + row0) * P.sw + (x0 + (px >> 2) + PAD));
             const uint32_t* s = &S.src[by * 16 + bx];
-            for (int row = lane >> 3; row < h; row += 4) {
-                const uintptr_t a = reinterpret_cast<uintptr_t>(G + (long long)row * P.sw);
+            const int step4 = 4 * P.sw;
+            for (int row = row0; row < h; row += 4, G += step4) {
+                const uintptr_t a = reinterpret_cast<uintptr_t>(G);
                 const uint32_t* q = reinterpret_cast<const uint32_t*>(a & ~uintptr_t(3));
                 const unsigned sh = (unsigned)(a & 3) * 8u;
                 const uint32_t* sr = s + row * 4;
@@ -208,43 +211,42 @@ class MbWarp {
         return sad;
     }
 
-    // Quarter-sample prediction (HalfPel::predict, enc/subpel.rs:122-145) of the w x h partition at 4x4
-    // block (bx, by) scored by SATD (satd, enc/frame.rs:641-659), or by SAD when `sad` (the P_Skip test),
-    // for the n vectors cand(c); the sums land in S.cost[0..n).
-    template <typename CandFn>
-    __device__ __forceinline__ void pred_batch(int r, int bx, int by, int w, int h, int n, bool sad, CandFn cand) {
-        const int nbw = w >> 2, nblk = nbw * (h >> 2), total = n * nblk;
+    // Quarter-sample prediction (HalfPel::predict, enc/subpel.rs:122-145) of the partition at 4x4 block
+    // (bx, by), (4 << lgw) x (4 << lgh) samples, scored by SATD (satd, enc/frame.rs:641-659), or by SAD
+    // when `sad` (the P_Skip test), for the n vectors S.cand[0..n); the sums land in S.cost[0..n).
+    __device__ __noinline__ void pred_batch(int r, int bx, int by, int lgw, int lgh, int n, bool sad) {
+        const int lg = lgw + lgh, total = n << lg, w = 4 << lgw, h = 4 << lgh;
         if (lane < n) S.cost[lane] = 0;
         __syncwarp();
         const int x0 = mbx * 16 + bx * 4, y0 = mby * 16 + by * 4;
         const uint8_t* base = P.planes[r];
+        const int sw = P.sw, psize = (int)P.psize;
         for (int t = lane; t < total; t += 32) {
-            const int c = t / nblk, b = t - c * nblk, bxx = b % nbw, byy = b / nbw;
-            const int2 mv = cand(c);
-            const int ix = min(max(x0 + (mv.x >> 2), -w - 3), P.pw + 1);
-            const int iy = min(max(y0 + (mv.y >> 2), -h - 3), P.ph + 1);
-            const unsigned m = c_mix[(mv.y & 3) * 4 + (mv.x & 3)];
+            const int c = t >> lg, b = t & ((1 << lg) - 1), bxx = b & ((1 << lgw) - 1), byy = b >> lgw;
+            const int2 mv = S.cand[c];
+            const int ix = min(max(x0 + (mv.x >> 2), -w - 3), P.pw + 1) + PAD + bxx * 4;
+            const int iy = min(max(y0 + (mv.y >> 2), -h - 3), P.ph + 1) + PAD + byy * 4;
+            const unsigned m = mix_entry(mv.x & 3, mv.y & 3);
             const int pa = m & 3, ax = (m >> 2) & 1, ay = (m >> 3) & 1, pb = (m >> 4) & 3, bbx = (m >> 6) & 1, bby = (m >> 7) & 1;
             const bool same = (m & 0xf) == (m >> 4);
-            const long long ox = ix + PAD + bxx * 4, oy = iy + PAD + byy * 4;
-            const uint8_t* A = base + pa * P.psize + (oy + ay) * P.sw + ox + ax;
-            const uint8_t* B = base + pb * P.psize + (oy + bby) * P.sw + ox + bbx;
+            const uint8_t* A = base + (unsigned)(pa * psize + (iy + ay) * sw + ix + ax);
+            const uint8_t* B = base + (unsigned)(pb * psize + (iy + bby) * sw + ix + bbx);
             const uint32_t* s = &S.src[(by + byy) * 16 + bx + bxx];
             int v;
             if (sad) {
                 v = 0;
 #pragma unroll
                 for (int row = 0; row < 4; row++) {
-                    const uint32_t wa = ldu32(A + row * P.sw);
-                    const uint32_t wp = same ? wa : __vavgu4(wa, ldu32(B + row * P.sw));
+                    const uint32_t wa = ldu32(A + row * sw);
+                    const uint32_t wp = same ? wa : __vavgu4(wa, ldu32(B + row * sw));
                     v += __vsadu4(s[row * 4], wp);
                 }
             } else {
                 int d[16];
 #pragma unroll
                 for (int row = 0; row < 4; row++) {
-                    const uint32_t wa = ldu32(A + row * P.sw);
-                    const uint32_t wp = same ? wa : __vavgu4(wa, ldu32(B + row * P.sw));
+                    const uint32_t wa = ldu32(A + row * sw);
+                    const uint32_t wp = same ? wa : __vavgu4(wa, ldu32(B + row * sw));
                     const uint32_t ws = s[row * 4];
 #pragma unroll
                     for (int k = 0; k < 4; k++) d[row * 4 + k] = (int)((ws >> (8 * k)) & 255u) - (int)((wp >> (8 * k)) & 255u);
@@ -257,6 +259,40 @@ class MbWarp {
     }
 
     // ---- motion_search, enc/frame.rs:949-1019 --------------------------------------------------------
+
+    // One diamond round whose moves were bent by the search clamps: the reference's four moves replayed
+    // against the scored 3x3 square (S.cost[0..9), centre at 4), scoring on demand the points it lacks.
+    // Returns whether the best moved.
+    __device__ __noinline__ bool round_clamped(int r, int bx, int by, int w, int h, int mvpx, int mvpy, int step, int cxlo,
+                                               int cxhi, int cylo, int cyhi, int& bxv, int& byv, int& bc) {
+        const int cx = bxv, cy = byv;
+        const int X0 = min(max(cx - step, cxlo), cxhi), X2 = min(max(cx + step, cxlo), cxhi);
+        const int Y0 = min(max(cy - step, cylo), cyhi), Y2 = min(max(cy + step, cylo), cyhi);
+        bool moved = false;
+        for (int d = 0; d < 4; d++) {
+            int nx = bxv, ny = byv;
+            if (d == 0) nx = min(max(bxv - step, cxlo), cxhi);
+            else if (d == 1) nx = min(max(bxv + step, cxlo), cxhi);
+            else if (d == 2) ny = min(max(byv - step, cylo), cyhi);
+            else ny = min(max(byv + step, cylo), cyhi);
+            const int ix = nx == X0 ? 0 : (nx == cx ? 1 : (nx == X2 ? 2 : -1));
+            const int iy = ny == Y0 ? 0 : (ny == cy ? 1 : (ny == Y2 ? 2 : -1));
+            int v;
+            if (ix >= 0 && iy >= 0) {
+                v = S.cost[iy * 3 + ix];
+            } else {
+                const int s1 = sad_lane(r, bx, by, w, h, nx, ny, (lane & 7) == 0);
+                v = __shfl_sync(FULL, s1, 0) + P.lambda * mvd_bits_d(nx, ny, mvpx, mvpy);
+            }
+            if (v < bc) {
+                bxv = nx;
+                byv = ny;
+                bc = v;
+                moved = true;
+            }
+        }
+        return moved;
+    }
 
     // Returns the best vector in (ox, oy) and its cost without the vector's bits. (e0x, e0y) and
     // (e1x, e1y) are the extra candidates (nextra of them).
@@ -310,51 +346,48 @@ class MbWarp {
         // the diamond (973-988): each round scores the 3x3 square of its step around the centre in one
         // batch (group g -> square position k = g < 4 ? g : g + 1), then replays the four moves in order
         const int nsteps = P.fast ? 2 : 3;
+        const int k = g < 4 ? g : g + 1, kx = k % 3, ky = k / 3;
         for (int si = 0; si < nsteps; si++) {
             const int step = P.fast ? (si == 0 ? 8 : 4) : (16 >> si);
             const int iters = step == 4 ? 32 : 4;
             for (int it = 0; it < iters; it++) {
                 const int cx = bxv, cy = byv, c0 = bc;
                 const int X0 = clx(cx - step), X2 = clx(cx + step), Y0 = cly(cy - step), Y2 = cly(cy + step);
-                const int k = g < 4 ? g : g + 1, kx = k % 3, ky = k / 3;
                 const int qx = kx == 0 ? X0 : (kx == 1 ? cx : X2), qy = ky == 0 ? Y0 : (ky == 1 ? cy : Y2);
                 const int sc = sad_lane(r, bx, by, w, h, qx, qy, true) + lam * mvd_bits_d(qx, qy, mvpx, mvpy);
-                int sq[9];
-#pragma unroll
-                for (int j = 0; j < 8; j++) sq[j < 4 ? j : j + 1] = __shfl_sync(FULL, sc, j);
-                sq[4] = c0;
-                // the cost of point (x, y): from the square, or scored now (a clamp bent the move)
-                auto score = [&](int x, int y) {
-                    const int ix = x == X0 ? 0 : (x == cx ? 1 : (x == X2 ? 2 : -1));
-                    const int iy = y == Y0 ? 0 : (y == cy ? 1 : (y == Y2 ? 2 : -1));
-                    if (ix >= 0 && iy >= 0) {
-                        const int j = iy * 3 + ix;
-                        int v = sq[0];
-#pragma unroll
-                        for (int i = 1; i < 9; i++)
-                            if (j == i) v = sq[i];
-                        return v;
-                    }
-                    const int s1 = sad_lane(r, bx, by, w, h, x, y, g == 0);
-                    return __shfl_sync(FULL, s1, 0) + lam * mvd_bits_d(x, y, mvpx, mvpy);
-                };
-                bool moved = false;
-                int nx = clx(bxv - step), ny = byv;
-                int v = score(nx, ny);
-                if (v < bc) { bxv = nx; byv = ny; bc = v; moved = true; }
-                nx = clx(bxv + step);
-                ny = byv;
-                v = score(nx, ny);
-                if (v < bc) { bxv = nx; byv = ny; bc = v; moved = true; }
-                nx = bxv;
-                ny = cly(byv - step);
-                v = score(nx, ny);
-                if (v < bc) { bxv = nx; byv = ny; bc = v; moved = true; }
-                nx = bxv;
-                ny = cly(byv + step);
-                v = score(nx, ny);
-                if (v < bc) { bxv = nx; byv = ny; bc = v; moved = true; }
                 sad_px += (uint32_t)(4 * w * h);
+                bool moved;
+                if (X0 == cx - step && X2 == cx + step && Y0 == cy - step && Y2 == cy + step) {
+                    // no clamp: left, else right; then up from that column, else down
+                    const int sL = __shfl_sync(FULL, sc, 3), sR = __shfl_sync(FULL, sc, 4);
+                    int col = 1, b1 = c0;
+                    if (sL < c0) {
+                        col = 0;
+                        b1 = sL;
+                    } else if (sR < c0) {
+                        col = 2;
+                        b1 = sR;
+                    }
+                    const int sU = __shfl_sync(FULL, sc, col), sD = __shfl_sync(FULL, sc, 5 + col);
+                    int row = 1, b2 = b1;
+                    if (sU < b1) {
+                        row = 0;
+                        b2 = sU;
+                    } else if (sD < b1) {
+                        row = 2;
+                        b2 = sD;
+                    }
+                    bxv = col == 0 ? X0 : (col == 1 ? cx : X2);
+                    byv = row == 0 ? Y0 : (row == 1 ? cy : Y2);
+                    bc = b2;
+                    moved = col != 1 || row != 1;
+                } else {
+                    if (lane < 8) S.cost[k] = sc;
+                    if (lane == 0) S.cost[4] = c0;
+                    __syncwarp();
+                    moved = round_clamped(r, bx, by, w, h, mvpx, mvpy, step, cxlo, cxhi, cylo, cyhi, bxv, byv, bc);
+                    __syncwarp();
+                }
                 if (!moved) break;
             }
         }
@@ -364,56 +397,54 @@ class MbWarp {
             oy = byv;
             return bc - lam * mvd_bits_d(bxv, byv, mvpx, mvpy);
         }
+        const int lgw = w4 == 4 ? 2 : (w4 == 2 ? 1 : 0), lgh = h4 == 4 ? 2 : (h4 == 2 ? 1 : 0);
         // sub-sample refinement (994-1017): the centre and the 8 half samples around it in one batch,
-        // then the 4 quarter samples around the new centre
-        {
-            const int cx = bxv, cy = byv;
-            auto sqc = [&](int c) {
-                if (c == 0) return make_int2(cx, cy);
-                const int k = c <= 4 ? c - 1 : c;  // square (-1,-1) (0,-1) (1,-1) (-1,0) (1,0) (-1,1) (0,1) (1,1)
-                return make_int2(clx(cx + (k % 3 - 1) * 2), cly(cy + (k / 3 - 1) * 2));
-            };
-            pred_batch(r, bx, by, w, h, 9, false, sqc);
-            if (lane < 9) {
-                const int2 q = sqc(lane);
-                S.cost[lane] += lam * mvd_bits_d(q.x, q.y, mvpx, mvpy);
+        // square (-1,-1) (0,-1) (1,-1) (-1,0) (1,0) (-1,1) (0,1) (1,1) in order
+        if (lane < 9) {
+            int2 q = make_int2(bxv, byv);
+            if (lane > 0) {
+                const int kk = lane <= 4 ? lane - 1 : lane;
+                q = make_int2(clx(bxv + (kk % 3 - 1) * 2), cly(byv + (kk / 3 - 1) * 2));
             }
-            __syncwarp();
-            satd_px += (uint32_t)(9 * w * h);
-            bc = S.cost[0];
-            for (int c = 1; c < 9; c++) {
-                const int v = S.cost[c];
-                if (v < bc) {
-                    const int2 q = sqc(c);
-                    bxv = q.x;
-                    byv = q.y;
-                    bc = v;
-                }
-            }
-            __syncwarp();
+            S.cand[lane] = q;
         }
-        if (!P.fast) {
-            const int cx = bxv, cy = byv;
-            auto dmc = [&](int c) {  // (0,-1) (-1,0) (1,0) (0,1)
-                const int dx = c == 1 ? -1 : (c == 2 ? 1 : 0), dy = c == 0 ? -1 : (c == 3 ? 1 : 0);
-                return make_int2(clx(cx + dx), cly(cy + dy));
-            };
-            pred_batch(r, bx, by, w, h, 4, false, dmc);
-            if (lane < 4) {
-                const int2 q = dmc(lane);
-                S.cost[lane] += lam * mvd_bits_d(q.x, q.y, mvpx, mvpy);
+        __syncwarp();
+        pred_batch(r, bx, by, lgw, lgh, 9, false);
+        if (lane < 9) S.cost[lane] += lam * mvd_bits_d(S.cand[lane].x, S.cand[lane].y, mvpx, mvpy);
+        __syncwarp();
+        satd_px += (uint32_t)(9 * w * h);
+        bc = S.cost[0];
+        for (int c = 1; c < 9; c++) {
+            const int v = S.cost[c];
+            if (v < bc) {
+                bxv = S.cand[c].x;
+                byv = S.cand[c].y;
+                bc = v;
             }
+        }
+        __syncwarp();
+        if (!P.fast) {
+            // the 4 quarter samples around the new centre: (0,-1) (-1,0) (1,0) (0,1)
+            if (lane < 4) {
+                const int dx = lane == 1 ? -1 : (lane == 2 ? 1 : 0), dy = lane == 0 ? -1 : (lane == 3 ? 1 : 0);
+                S.cand[lane] = make_int2(clx(bxv + dx), cly(byv + dy));
+            }
+            __syncwarp();
+            pred_batch(r, bx, by, lgw, lgh, 4, false);
+            if (lane < 4) S.cost[lane] += lam * mvd_bits_d(S.cand[lane].x, S.cand[lane].y, mvpx, mvpy);
             __syncwarp();
             satd_px += (uint32_t)(4 * w * h);
+            int nbx = bxv, nby = byv;
             for (int c = 0; c < 4; c++) {
                 const int v = S.cost[c];
                 if (v < bc) {
-                    const int2 q = dmc(c);
-                    bxv = q.x;
-                    byv = q.y;
+                    nbx = S.cand[c].x;
+                    nby = S.cand[c].y;
                     bc = v;
                 }
             }
+            bxv = nbx;
+            byv = nby;
             __syncwarp();
         }
         ox = bxv;
@@ -577,7 +608,9 @@ class MbWarp {
         sad_px = satd_px = 0;
         // P_Skip (enc/frame.rs:722-729)
         const int2 sv = skip_mv();
-        pred_batch(0, 0, 0, 16, 16, 1, true, [&](int) { return sv; });
+        if (lane == 0) S.cand[0] = sv;
+        __syncwarp();
+        pred_batch(0, 0, 0, 2, 2, 1, true);
         const int skip_sad = S.cost[0];
         __syncwarp();
         sad_px += 256;
