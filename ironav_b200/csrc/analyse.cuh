@@ -30,7 +30,8 @@
 
 namespace ironav {
 
-constexpr int K2_WARPS = 4;  // warps per CTA; each warp works alone
+constexpr int K2_WARPS = 4;       // warps per CTA; each warp works alone
+constexpr int K2_MIN_BLOCKS = 4;  // CTAs per SM the register budget must allow (128 registers a thread)
 constexpr unsigned FULL = 0xffffffffu;
 constexpr int BIG = 0x7fffffff;
 
@@ -65,6 +66,8 @@ struct WarpSmem {
     int16_t win_mvs[16][2];   // best over the references
     ironav_mbresult res;
     ironav_mbstate out;
+    int mb, mbx, mby;         // the macroblock being analysed
+    uint32_t sad_px, satd_px; // its work counts
 };
 
 __device__ __forceinline__ int ue_bits_d(unsigned v) { return 2 * (32 - __clz(v + 1)) - 1; }  // enc/bitw.rs:81-83
@@ -74,629 +77,623 @@ __device__ __forceinline__ int se_bits_d(int v) {                               
 __device__ __forceinline__ int mvd_bits_d(int mx, int my, int px, int py) { return se_bits_d(mx - px) + se_bits_d(my - py); }
 __device__ __forceinline__ int median3_d(int a, int b, int c) { return min(max(a, b), max(min(a, b), c)); }
 
-// 4 bytes at any address, as aligned 32-bit loads and a funnel shift.
-__device__ __forceinline__ uint32_t ldu32(const uint8_t* p) {
-    uintptr_t a = reinterpret_cast<uintptr_t>(p);
-    const uint32_t* q = reinterpret_cast<const uint32_t*>(a & ~uintptr_t(3));
-    return __funnelshift_r(__ldg(q), __ldg(q + 1), (unsigned)(a & 3) * 8u);
+// dp4a with unsigned bytes in a and signed bytes in b: c + sum of a_k * b_k.
+__device__ __forceinline__ int dp4a_us(uint32_t a, uint32_t b, int c) {
+    int d;
+    asm("dp4a.u32.s32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c));
+    return d;
 }
 
-// satd4, enc/frame.rs:144-161, with its last butterfly stage folded: |a+b| + |a-b| = 2 max(|a|, |b|), so
-// (sum of the 16 magnitudes) >> 1 is the sum over the 8 last-stage pairs of max(|a|, |b|).
-__device__ __forceinline__ int satd4_d(const int d[16]) {
-    int t[16];
+// satd4, enc/frame.rs:144-161, of the 4x4 block with source rows s[r] and prediction rows p[r] (4 packed
+// bytes each). The row transform is the 4-point Hadamard of each row's differences, H(s - p) = Hs - Hp,
+// taken straight from the packed bytes with dp4a (rows (1,1,1,1), (1,1,-1,-1), (1,-1,-1,1), (1,-1,1,-1):
+// the reference's outputs in its order); the column transform's last stage is folded, |a+b| + |a-b| =
+// 2 max(|a|, |b|), so (sum of the 16 magnitudes) >> 1 is the sum over the 8 last-stage pairs of max(|a|, |b|).
+__device__ __forceinline__ int satd4_packed(const uint32_t s[4], const uint32_t p[4]) {
+    const uint32_t H[4] = {0x01010101u, 0xFFFF0101u, 0x01FFFF01u, 0xFF01FF01u};
+    const uint32_t NH[4] = {0xFFFFFFFFu, 0x0101FFFFu, 0xFF0101FFu, 0x01FF01FFu};
+    int t[4][4];
 #pragma unroll
-    for (int r = 0; r < 4; r++) {
-        int a = d[r * 4], b = d[r * 4 + 1], c = d[r * 4 + 2], e = d[r * 4 + 3];
-        int s0 = a + b, s1 = c + e, d0 = a - b, d1 = c - e;
-        t[r * 4] = s0 + s1;
-        t[r * 4 + 1] = s0 - s1;
-        t[r * 4 + 2] = d0 - d1;
-        t[r * 4 + 3] = d0 + d1;
-    }
+    for (int r = 0; r < 4; r++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) t[r][j] = dp4a_us(p[r], NH[j], dp4a_us(s[r], H[j], 0));
     int sum = 0;
 #pragma unroll
     for (int c = 0; c < 4; c++) {
-        int a = t[c], b = t[4 + c], cc = t[8 + c], e = t[12 + c];
-        int s0 = a + b, s1 = cc + e, d0 = a - b, d1 = cc - e;
+        const int a = t[0][c], b = t[1][c], cc = t[2][c], e = t[3][c];
+        const int s0 = a + b, s1 = cc + e, d0 = a - b, d1 = cc - e;
         sum += max(abs(s0), abs(s1)) + max(abs(d0), abs(d1));
     }
     return sum;
 }
 
-class MbWarp {
-  public:
-    const AnalyseParams& P;
-    WarpSmem& S;
-    const int lane;
-    int mbx, mby, mb;
-    uint32_t sad_px, satd_px;
+// ---- neighbours (nb_state / nb_motion, enc/frame.rs:509-538) ----------------------------------
 
-    __device__ MbWarp(const AnalyseParams& p, WarpSmem& s, int l) : P(p), S(s), lane(l) {}
-
-    // ---- neighbours (nb_state / nb_motion, enc/frame.rs:509-538) ----------------------------------
-
-    // Fills the table of blocks around the macroblock: left column (x = -1), top row (y = -1), top-right
-    // (4, -1), top-left (-1, -1); (4, y >= 0) is never available; inside slots are unused.
-    __device__ void load_neighbours(const ironav_mbstate* states) {
-        if (lane < 30) {
-            const int ex = lane % 6 - 1, ey = lane / 6 - 1;
-            Blk e = make_int4(0, 0, -1, 0);
-            if (ey < 0 || ex < 0) {
-                const int nx = mbx + (ex < 0 ? -1 : (ex >= 4 ? 1 : 0)), ny = mby + (ey < 0 ? -1 : 0);
-                const int bx = ex < 0 ? 3 : (ex >= 4 ? 0 : ex), by = ey < 0 ? 3 : ey;
-                // macroblocks of earlier slices are not available (enc/frame.rs:509-515)
-                if (nx >= 0 && nx < P.mb_w && ny >= P.band_start[mby] && ny < P.mb_h) {
-                    const ironav_mbstate* s = &states[(size_t)ny * P.mb_w + nx];
-                    e.w = 1;
-                    const int rf = s->refs[(by >> 1) * 2 + (bx >> 1)];
-                    if (s->inter && rf >= 0) {
-                        const uint32_t mv = *reinterpret_cast<const uint32_t*>(&s->mvs[by * 4 + bx][0]);
-                        e.x = (int)(int16_t)(mv & 0xffffu);
-                        e.y = (int)(int16_t)(mv >> 16);
-                        e.z = rf;
-                    }
-                }
-            }
-            S.ext[lane] = e;
-        }
-        __syncwarp();
-    }
-
-    // nb_motion for the block at (x, y) relative to the macroblock; inside it, `cur` holds the decided
-    // blocks (nullptr: none decided).
-    __device__ __forceinline__ Blk nb(const Blk* cur, int x, int y) const {
-        if (x >= 0 && x < 4 && y >= 0) return cur ? cur[y * 4 + x] : make_int4(0, 0, -1, 0);
-        return S.ext[(y + 1) * 6 + (x + 1)];
-    }
-
-    // pred_mv, enc/frame.rs:543-570
-    __device__ __noinline__ int2 pred_mv(const Blk* cur, int bx, int by, int w, int dir, int rf) const {
-        const Blk a = nb(cur, bx - 1, by), b = nb(cur, bx, by - 1);
-        Blk c = nb(cur, bx + w, by - 1);
-        if (!c.w) c = nb(cur, bx - 1, by - 1);
-        if (dir == 1 && by == 0 && b.z == rf) return make_int2(b.x, b.y);
-        if (dir == 1 && by != 0 && a.z == rf) return make_int2(a.x, a.y);
-        if (dir == 2 && bx == 0 && a.z == rf) return make_int2(a.x, a.y);
-        if (dir == 2 && bx != 0 && c.z == rf) return make_int2(c.x, c.y);
-        if (!b.w && !c.w && a.w) return make_int2(a.x, a.y);
-        const int ra = a.z == rf, rb = b.z == rf, rc = c.z == rf;
-        if (ra + rb + rc == 1) {
-            if (ra) return make_int2(a.x, a.y);
-            if (rb) return make_int2(b.x, b.y);
-            return make_int2(c.x, c.y);
-        }
-        return make_int2(median3_d(a.x, b.x, c.x), median3_d(a.y, b.y, c.y));
-    }
-
-    // skip_mv, enc/frame.rs:597-603
-    __device__ int2 skip_mv() const {
-        const Blk a = nb(nullptr, -1, 0), b = nb(nullptr, 0, -1);
-        if (!a.w || !b.w || (a.z == 0 && a.x == 0 && a.y == 0) || (b.z == 0 && b.x == 0 && b.y == 0)) return make_int2(0, 0);
-        return pred_mv(nullptr, 0, 0, 4, 0, 0);
-    }
-
-    // ---- scoring -------------------------------------------------------------------------------------
-
-    // Integer SAD (sad_int, enc/frame.rs:662-671) of the w x h partition at 4x4 block (bx, by) at this
-    // lane's candidate (px, py) of reference r; the lanes of a group (same lane & 7) share a candidate and
-    // split its rows. Returns the group's sum in every lane of the group.
-    __device__ __forceinline__ int sad_lane(int r, int bx, int by, int w, int h, int px, int py, bool valid) const {
-        int sad = 0;
-        if (valid) {
-            const int x0 = mbx * 16 + bx * 4, y0 = mby * 16 + by * 4;
-            const int row0 = lane >> 3;
-            const uint8_t* G = P.planes[r] + (unsigned)((y0 + (py >> 2) + PAD + row0) * P.sw + (x0 + (px >> 2) + PAD));
-            const uint32_t* s = &S.src[by * 16 + bx];
-            const int step4 = 4 * P.sw;
-            for (int row = row0; row < h; row += 4, G += step4) {
-                const uintptr_t a = reinterpret_cast<uintptr_t>(G);
-                const uint32_t* q = reinterpret_cast<const uint32_t*>(a & ~uintptr_t(3));
-                const unsigned sh = (unsigned)(a & 3) * 8u;
-                const uint32_t* sr = s + row * 4;
-                const uint32_t w0 = __ldg(q), w1 = __ldg(q + 1);
-                sad += __vsadu4(sr[0], __funnelshift_r(w0, w1, sh));
-                if (w >= 8) {
-                    const uint32_t w2 = __ldg(q + 2);
-                    sad += __vsadu4(sr[1], __funnelshift_r(w1, w2, sh));
-                    if (w == 16) {
-                        const uint32_t w3 = __ldg(q + 3), w4 = __ldg(q + 4);
-                        sad += __vsadu4(sr[2], __funnelshift_r(w2, w3, sh)) + __vsadu4(sr[3], __funnelshift_r(w3, w4, sh));
-                    }
+// Fills the table of blocks around the macroblock: left column (x = -1), top row (y = -1), top-right
+// (4, -1), top-left (-1, -1); (4, y >= 0) is never available; inside slots are unused.
+static __device__ void load_neighbours(const AnalyseParams& P, WarpSmem& S, const ironav_mbstate* states) {
+    const int lane = threadIdx.x & 31;
+    if (lane < 30) {
+        const int ex = lane % 6 - 1, ey = lane / 6 - 1;
+        Blk e = make_int4(0, 0, -1, 0);
+        if (ey < 0 || ex < 0) {
+            const int nx = S.mbx + (ex < 0 ? -1 : (ex >= 4 ? 1 : 0)), ny = S.mby + (ey < 0 ? -1 : 0);
+            const int bx = ex < 0 ? 3 : (ex >= 4 ? 0 : ex), by = ey < 0 ? 3 : ey;
+            // macroblocks of earlier slices are not available (enc/frame.rs:509-515)
+            if (nx >= 0 && nx < P.mb_w && ny >= P.band_start[S.mby] && ny < P.mb_h) {
+                const ironav_mbstate* s = &states[(size_t)ny * P.mb_w + nx];
+                e.w = 1;
+                const int rf = s->refs[(by >> 1) * 2 + (bx >> 1)];
+                if (s->inter && rf >= 0) {
+                    const uint32_t mv = *reinterpret_cast<const uint32_t*>(&s->mvs[by * 4 + bx][0]);
+                    e.x = (int)(int16_t)(mv & 0xffffu);
+                    e.y = (int)(int16_t)(mv >> 16);
+                    e.z = rf;
                 }
             }
         }
-        sad += __shfl_xor_sync(FULL, sad, 8);
-        sad += __shfl_xor_sync(FULL, sad, 16);
-        return sad;
+        S.ext[lane] = e;
     }
+    __syncwarp();
+}
 
-    // Quarter-sample prediction (HalfPel::predict, enc/subpel.rs:122-145) of the partition at 4x4 block
-    // (bx, by), (4 << lgw) x (4 << lgh) samples, scored by SATD (satd, enc/frame.rs:641-659), or by SAD
-    // when `sad` (the P_Skip test), for the n vectors S.cand[0..n); the sums land in S.cost[0..n).
-    __device__ __noinline__ void pred_batch(int r, int bx, int by, int lgw, int lgh, int n, bool sad) {
-        const int lg = lgw + lgh, total = n << lg, w = 4 << lgw, h = 4 << lgh;
-        if (lane < n) S.cost[lane] = 0;
-        __syncwarp();
-        const int x0 = mbx * 16 + bx * 4, y0 = mby * 16 + by * 4;
-        const uint8_t* base = P.planes[r];
-        const int sw = P.sw, psize = (int)P.psize;
-        for (int t = lane; t < total; t += 32) {
-            const int c = t >> lg, b = t & ((1 << lg) - 1), bxx = b & ((1 << lgw) - 1), byy = b >> lgw;
-            const int2 mv = S.cand[c];
-            const int ix = min(max(x0 + (mv.x >> 2), -w - 3), P.pw + 1) + PAD + bxx * 4;
-            const int iy = min(max(y0 + (mv.y >> 2), -h - 3), P.ph + 1) + PAD + byy * 4;
-            const unsigned m = mix_entry(mv.x & 3, mv.y & 3);
-            const int pa = m & 3, ax = (m >> 2) & 1, ay = (m >> 3) & 1, pb = (m >> 4) & 3, bbx = (m >> 6) & 1, bby = (m >> 7) & 1;
-            const bool same = (m & 0xf) == (m >> 4);
-            const uint8_t* A = base + (unsigned)(pa * psize + (iy + ay) * sw + ix + ax);
-            const uint8_t* B = base + (unsigned)(pb * psize + (iy + bby) * sw + ix + bbx);
-            const uint32_t* s = &S.src[(by + byy) * 16 + bx + bxx];
-            int v;
-            if (sad) {
-                v = 0;
+// nb_motion for the block at (x, y) relative to the macroblock; inside it, `cur` holds the decided
+// blocks (nullptr: none decided).
+static __device__ __forceinline__ Blk nb(const AnalyseParams& P, WarpSmem& S, const Blk* cur, int x, int y) {
+    if (x >= 0 && x < 4 && y >= 0) return cur ? cur[y * 4 + x] : make_int4(0, 0, -1, 0);
+    return S.ext[(y + 1) * 6 + (x + 1)];
+}
+
+// pred_mv, enc/frame.rs:543-570
+static __device__ __noinline__ int2 pred_mv(const AnalyseParams& P, WarpSmem& S, const Blk* cur, int bx, int by, int w, int dir, int rf) {
+    const Blk a = nb(P, S, cur, bx - 1, by), b = nb(P, S, cur, bx, by - 1);
+    Blk c = nb(P, S, cur, bx + w, by - 1);
+    if (!c.w) c = nb(P, S, cur, bx - 1, by - 1);
+    if (dir == 1 && by == 0 && b.z == rf) return make_int2(b.x, b.y);
+    if (dir == 1 && by != 0 && a.z == rf) return make_int2(a.x, a.y);
+    if (dir == 2 && bx == 0 && a.z == rf) return make_int2(a.x, a.y);
+    if (dir == 2 && bx != 0 && c.z == rf) return make_int2(c.x, c.y);
+    if (!b.w && !c.w && a.w) return make_int2(a.x, a.y);
+    const int ra = a.z == rf, rb = b.z == rf, rc = c.z == rf;
+    if (ra + rb + rc == 1) {
+        if (ra) return make_int2(a.x, a.y);
+        if (rb) return make_int2(b.x, b.y);
+        return make_int2(c.x, c.y);
+    }
+    return make_int2(median3_d(a.x, b.x, c.x), median3_d(a.y, b.y, c.y));
+}
+
+// skip_mv, enc/frame.rs:597-603
+static __device__ int2 skip_mv(const AnalyseParams& P, WarpSmem& S) {
+    const Blk a = nb(P, S, nullptr, -1, 0), b = nb(P, S, nullptr, 0, -1);
+    if (!a.w || !b.w || (a.z == 0 && a.x == 0 && a.y == 0) || (b.z == 0 && b.x == 0 && b.y == 0)) return make_int2(0, 0);
+    return pred_mv(P, S, nullptr, 0, 0, 4, 0, 0);
+}
+
+// ---- scoring -------------------------------------------------------------------------------------
+
+// Integer SAD (sad_int, enc/frame.rs:662-671) of the w x h partition at 4x4 block (bx, by) at this
+// lane's candidate (px, py) of reference r; the lanes of a group (same lane & 7) share a candidate and
+// split its rows. Returns the group's sum in every lane of the group.
+static __device__ __forceinline__ int sad_lane(const AnalyseParams& P, WarpSmem& S, int r, int bx, int by, int w, int h, int px, int py, bool valid) {
+    const int lane = threadIdx.x & 31;
+    int sad = 0;
+    if (valid) {
+        const int x0 = S.mbx * 16 + bx * 4, y0 = S.mby * 16 + by * 4;
+        const int row0 = lane >> 3;
+        const uint8_t* G = P.planes[r] + (unsigned)((y0 + (py >> 2) + PAD + row0) * P.sw + (x0 + (px >> 2) + PAD));
+        const uint32_t* s = &S.src[by * 16 + bx];
+        const int step4 = 4 * P.sw;
+        for (int row = row0; row < h; row += 4, G += step4) {
+            const uintptr_t a = reinterpret_cast<uintptr_t>(G);
+            const uint32_t* q = reinterpret_cast<const uint32_t*>(a & ~uintptr_t(3));
+            const unsigned sh = (unsigned)(a & 3) * 8u;
+            const uint32_t* sr = s + row * 4;
+            const uint32_t w0 = __ldg(q), w1 = __ldg(q + 1);
+            sad += __vsadu4(sr[0], __funnelshift_r(w0, w1, sh));
+            if (w >= 8) {
+                const uint32_t w2 = __ldg(q + 2);
+                sad += __vsadu4(sr[1], __funnelshift_r(w1, w2, sh));
+                if (w == 16) {
+                    const uint32_t w3 = __ldg(q + 3), w4 = __ldg(q + 4);
+                    sad += __vsadu4(sr[2], __funnelshift_r(w2, w3, sh)) + __vsadu4(sr[3], __funnelshift_r(w3, w4, sh));
+                }
+            }
+        }
+    }
+    sad += __shfl_xor_sync(FULL, sad, 8);
+    sad += __shfl_xor_sync(FULL, sad, 16);
+    return sad;
+}
+
+// Quarter-sample prediction (HalfPel::predict, enc/subpel.rs:122-145) of the partition at 4x4 block
+// (bx, by), (4 << lgw) x (4 << lgh) samples, scored by SATD (satd, enc/frame.rs:641-659), or by SAD
+// when `sad` (the P_Skip test), for the n vectors S.cand[0..n); the sums land in S.cost[0..n).
+static __device__ __noinline__ void pred_batch(const AnalyseParams& P, WarpSmem& S, int r, int bx, int by, int lgw, int lgh, int n, bool sad) {
+    const int lane = threadIdx.x & 31;
+    const int lg = lgw + lgh, total = n << lg, w = 4 << lgw, h = 4 << lgh;
+    if (lane < n) S.cost[lane] = 0;
+    __syncwarp();
+    const int x0 = S.mbx * 16 + bx * 4, y0 = S.mby * 16 + by * 4;
+    const uint8_t* base = P.planes[r];
+    const int sw = P.sw, psize = (int)P.psize;
+    for (int t = lane; t < total; t += 32) {
+        const int c = t >> lg, b = t & ((1 << lg) - 1), bxx = b & ((1 << lgw) - 1), byy = b >> lgw;
+        const int2 mv = S.cand[c];
+        const int ix = min(max(x0 + (mv.x >> 2), -w - 3), P.pw + 1) + PAD + bxx * 4;
+        const int iy = min(max(y0 + (mv.y >> 2), -h - 3), P.ph + 1) + PAD + byy * 4;
+        const unsigned m = mix_entry(mv.x & 3, mv.y & 3);
+        const int pa = m & 3, ax = (m >> 2) & 1, ay = (m >> 3) & 1, pb = (m >> 4) & 3, bbx = (m >> 6) & 1, bby = (m >> 7) & 1;
+        const bool same = (m & 0xf) == (m >> 4);
+        // every row of a plane block has the same alignment (sw is a multiple of 16)
+        const uintptr_t ua = reinterpret_cast<uintptr_t>(base + (unsigned)(pa * psize + (iy + ay) * sw + ix + ax));
+        const uint32_t* qa = reinterpret_cast<const uint32_t*>(ua & ~uintptr_t(3));
+        const unsigned sha = (unsigned)(ua & 3) * 8u;
+        const int swq = sw >> 2;
+        uint32_t pr[4], sr[4];
 #pragma unroll
-                for (int row = 0; row < 4; row++) {
-                    const uint32_t wa = ldu32(A + row * sw);
-                    const uint32_t wp = same ? wa : __vavgu4(wa, ldu32(B + row * sw));
-                    v += __vsadu4(s[row * 4], wp);
+        for (int row = 0; row < 4; row++) pr[row] = __funnelshift_r(__ldg(qa + row * swq), __ldg(qa + row * swq + 1), sha);
+        if (!same) {
+            const uintptr_t ub = reinterpret_cast<uintptr_t>(base + (unsigned)(pb * psize + (iy + bby) * sw + ix + bbx));
+            const uint32_t* qb = reinterpret_cast<const uint32_t*>(ub & ~uintptr_t(3));
+            const unsigned shb = (unsigned)(ub & 3) * 8u;
+#pragma unroll
+            for (int row = 0; row < 4; row++)
+                pr[row] = __vavgu4(pr[row], __funnelshift_r(__ldg(qb + row * swq), __ldg(qb + row * swq + 1), shb));
+        }
+        const uint32_t* s = &S.src[(by + byy) * 16 + bx + bxx];
+#pragma unroll
+        for (int row = 0; row < 4; row++) sr[row] = s[row * 4];
+        int v;
+        if (sad) {
+            v = __vsadu4(sr[0], pr[0]) + __vsadu4(sr[1], pr[1]) + __vsadu4(sr[2], pr[2]) + __vsadu4(sr[3], pr[3]);
+        } else {
+            v = satd4_packed(sr, pr);
+        }
+        atomicAdd(&S.cost[c], v);
+    }
+    __syncwarp();
+}
+
+// ---- motion_search, enc/frame.rs:949-1019 --------------------------------------------------------
+
+// One diamond round whose moves were bent by the search clamps: the reference's four moves replayed
+// against the scored 3x3 square (S.cost[0..9), centre at 4), scoring on demand the points it lacks.
+// Returns whether the best moved.
+static __device__ __noinline__ int4 round_clamped(const AnalyseParams& P, WarpSmem& S, int r, int bx, int by, int w, int h, int mvpx, int mvpy, int step, int cxlo,
+                                           int cxhi, int cylo, int cyhi, int bxv, int byv, int bc) {
+    const int lane = threadIdx.x & 31;
+    const int cx = bxv, cy = byv;
+    const int X0 = min(max(cx - step, cxlo), cxhi), X2 = min(max(cx + step, cxlo), cxhi);
+    const int Y0 = min(max(cy - step, cylo), cyhi), Y2 = min(max(cy + step, cylo), cyhi);
+    bool moved = false;
+    for (int d = 0; d < 4; d++) {
+        int nx = bxv, ny = byv;
+        if (d == 0) nx = min(max(bxv - step, cxlo), cxhi);
+        else if (d == 1) nx = min(max(bxv + step, cxlo), cxhi);
+        else if (d == 2) ny = min(max(byv - step, cylo), cyhi);
+        else ny = min(max(byv + step, cylo), cyhi);
+        const int ix = nx == X0 ? 0 : (nx == cx ? 1 : (nx == X2 ? 2 : -1));
+        const int iy = ny == Y0 ? 0 : (ny == cy ? 1 : (ny == Y2 ? 2 : -1));
+        int v;
+        if (ix >= 0 && iy >= 0) {
+            v = S.cost[iy * 3 + ix];
+        } else {
+            const int s1 = sad_lane(P, S, r, bx, by, w, h, nx, ny, (lane & 7) == 0);
+            v = __shfl_sync(FULL, s1, 0) + P.lambda * mvd_bits_d(nx, ny, mvpx, mvpy);
+        }
+        if (v < bc) {
+            bxv = nx;
+            byv = ny;
+            bc = v;
+            moved = true;
+        }
+    }
+    return make_int4(moved, bxv, byv, bc);
+}
+
+// Returns the best vector in (ox, oy) and its cost without the vector's bits. (e0x, e0y) and
+// (e1x, e1y) are the extra candidates (nextra of them).
+static __device__ __noinline__ int4 motion_search(const AnalyseParams& P, WarpSmem& S, int r, int bx, int by, int w4, int h4, int mvpx, int mvpy, int e0x, int e0y,
+                                          int e1x, int e1y, int nextra) {
+    const int lane = threadIdx.x & 31;
+    const int lam = P.lambda;
+    const int x0 = S.mbx * 16 + bx * 4, y0 = S.mby * 16 + by * 4, w = w4 * 4, h = h4 * 4;
+    const int cxlo = max(-(x0 + 24) * 4, -2048), cxhi = min((P.mb_w * 16 - x0 + 8) * 4, 2047);
+    const int cylo = max(-(y0 + 24) * 4, -512), cyhi = min((P.mb_h * 16 - y0 + 8) * 4, 511);
+    auto clx = [&](int v) { return min(max(v, cxlo), cxhi); };
+    auto cly = [&](int v) { return min(max(v, cylo), cyhi); };
+    auto intr = [](int v) { return (v + 2) & ~3; };
+    const int g = lane & 7;
+    // candidates (958-964): lane group g scores candidate g; absent ones are skipped in order
+    int px = 0, py = 0;
+    bool valid = true;
+    if (g == 0) {
+        px = intr(clx(mvpx));
+        py = intr(cly(mvpy));
+    } else if (g >= 2 && g <= 4) {
+        const Blk n = g == 2 ? nb(P, S, nullptr, -1, 0) : (g == 3 ? nb(P, S, nullptr, 0, -1) : nb(P, S, nullptr, 4, -1));
+        valid = n.w && n.z == r;
+        px = intr(clx(n.x));
+        py = intr(cly(n.y));
+    } else if (g == 5) {
+        valid = nextra > 0;
+        px = intr(clx(e0x));
+        py = intr(cly(e0y));
+    } else if (g == 6) {
+        valid = nextra > 1;
+        px = intr(clx(e1x));
+        py = intr(cly(e1y));
+    } else if (g == 7) {
+        valid = false;
+    }
+    int cost = sad_lane(P, S, r, bx, by, w, h, px, py, valid);
+    cost = valid ? cost + lam * mvd_bits_d(px, py, mvpx, mvpy) : BIG;
+    const unsigned vmask = __ballot_sync(FULL, valid) & 0xffu;
+    if (lane == 0) S.sad_px += (uint32_t)(__popc(vmask) * w * h);
+    int bxv = 0, byv = 0, bc = BIG;
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        const int ck = __shfl_sync(FULL, cost, k);
+        const int xk = __shfl_sync(FULL, px, k), yk = __shfl_sync(FULL, py, k);
+        if (ck < bc) {
+            bc = ck;
+            bxv = xk;
+            byv = yk;
+        }
+    }
+    // the diamond (973-988): each round scores the 3x3 square of its step around the centre in one
+    // batch (group g -> square position k = g < 4 ? g : g + 1), then replays the four moves in order
+    const int nsteps = P.fast ? 2 : 3;
+    const int k = g < 4 ? g : g + 1, kx = k % 3, ky = k / 3;
+    for (int si = 0; si < nsteps; si++) {
+        const int step = P.fast ? (si == 0 ? 8 : 4) : (16 >> si);
+        const int iters = step == 4 ? 32 : 4;
+        for (int it = 0; it < iters; it++) {
+            const int cx = bxv, cy = byv, c0 = bc;
+            const int X0 = clx(cx - step), X2 = clx(cx + step), Y0 = cly(cy - step), Y2 = cly(cy + step);
+            const int qx = kx == 0 ? X0 : (kx == 1 ? cx : X2), qy = ky == 0 ? Y0 : (ky == 1 ? cy : Y2);
+            const int sc = sad_lane(P, S, r, bx, by, w, h, qx, qy, true) + lam * mvd_bits_d(qx, qy, mvpx, mvpy);
+            if (lane == 0) S.sad_px += (uint32_t)(4 * w * h);
+            bool moved;
+            if (X0 == cx - step && X2 == cx + step && Y0 == cy - step && Y2 == cy + step) {
+                // no clamp: left, else right; then up from that column, else down
+                const int sL = __shfl_sync(FULL, sc, 3), sR = __shfl_sync(FULL, sc, 4);
+                int col = 1, b1 = c0;
+                if (sL < c0) {
+                    col = 0;
+                    b1 = sL;
+                } else if (sR < c0) {
+                    col = 2;
+                    b1 = sR;
                 }
+                const int sU = __shfl_sync(FULL, sc, col), sD = __shfl_sync(FULL, sc, 5 + col);
+                int row = 1, b2 = b1;
+                if (sU < b1) {
+                    row = 0;
+                    b2 = sU;
+                } else if (sD < b1) {
+                    row = 2;
+                    b2 = sD;
+                }
+                bxv = col == 0 ? X0 : (col == 1 ? cx : X2);
+                byv = row == 0 ? Y0 : (row == 1 ? cy : Y2);
+                bc = b2;
+                moved = col != 1 || row != 1;
             } else {
-                int d[16];
-#pragma unroll
-                for (int row = 0; row < 4; row++) {
-                    const uint32_t wa = ldu32(A + row * sw);
-                    const uint32_t wp = same ? wa : __vavgu4(wa, ldu32(B + row * sw));
-                    const uint32_t ws = s[row * 4];
-#pragma unroll
-                    for (int k = 0; k < 4; k++) d[row * 4 + k] = (int)((ws >> (8 * k)) & 255u) - (int)((wp >> (8 * k)) & 255u);
-                }
-                v = satd4_d(d);
+                if (lane < 8) S.cost[k] = sc;
+                if (lane == 0) S.cost[4] = c0;
+                __syncwarp();
+                const int4 rc = round_clamped(P, S, r, bx, by, w, h, mvpx, mvpy, step, cxlo, cxhi, cylo, cyhi, bxv, byv, bc);
+                moved = rc.x != 0;
+                bxv = rc.y;
+                byv = rc.z;
+                bc = rc.w;
+                __syncwarp();
             }
-            atomicAdd(&S.cost[c], v);
+            if (!moved) break;
         }
-        __syncwarp();
     }
-
-    // ---- motion_search, enc/frame.rs:949-1019 --------------------------------------------------------
-
-    // One diamond round whose moves were bent by the search clamps: the reference's four moves replayed
-    // against the scored 3x3 square (S.cost[0..9), centre at 4), scoring on demand the points it lacks.
-    // Returns whether the best moved.
-    __device__ __noinline__ bool round_clamped(int r, int bx, int by, int w, int h, int mvpx, int mvpy, int step, int cxlo,
-                                               int cxhi, int cylo, int cyhi, int& bxv, int& byv, int& bc) {
-        const int cx = bxv, cy = byv;
-        const int X0 = min(max(cx - step, cxlo), cxhi), X2 = min(max(cx + step, cxlo), cxhi);
-        const int Y0 = min(max(cy - step, cylo), cyhi), Y2 = min(max(cy + step, cylo), cyhi);
-        bool moved = false;
-        for (int d = 0; d < 4; d++) {
-            int nx = bxv, ny = byv;
-            if (d == 0) nx = min(max(bxv - step, cxlo), cxhi);
-            else if (d == 1) nx = min(max(bxv + step, cxlo), cxhi);
-            else if (d == 2) ny = min(max(byv - step, cylo), cyhi);
-            else ny = min(max(byv + step, cylo), cyhi);
-            const int ix = nx == X0 ? 0 : (nx == cx ? 1 : (nx == X2 ? 2 : -1));
-            const int iy = ny == Y0 ? 0 : (ny == cy ? 1 : (ny == Y2 ? 2 : -1));
-            int v;
-            if (ix >= 0 && iy >= 0) {
-                v = S.cost[iy * 3 + ix];
-            } else {
-                const int s1 = sad_lane(r, bx, by, w, h, nx, ny, (lane & 7) == 0);
-                v = __shfl_sync(FULL, s1, 0) + P.lambda * mvd_bits_d(nx, ny, mvpx, mvpy);
-            }
-            if (v < bc) {
-                bxv = nx;
-                byv = ny;
-                bc = v;
-                moved = true;
-            }
+    // live coding's early exit (990-992)
+    if (P.fast && bc < (w * h) / 8 + lam) return make_int4(bc - lam * mvd_bits_d(bxv, byv, mvpx, mvpy), bxv, byv, 0);
+    const int lgw = w4 == 4 ? 2 : (w4 == 2 ? 1 : 0), lgh = h4 == 4 ? 2 : (h4 == 2 ? 1 : 0);
+    // sub-sample refinement (994-1017): the centre and the 8 half samples around it in one batch,
+    // square (-1,-1) (0,-1) (1,-1) (-1,0) (1,0) (-1,1) (0,1) (1,1) in order
+    if (lane < 9) {
+        int2 q = make_int2(bxv, byv);
+        if (lane > 0) {
+            const int kk = lane <= 4 ? lane - 1 : lane;
+            q = make_int2(clx(bxv + (kk % 3 - 1) * 2), cly(byv + (kk / 3 - 1) * 2));
         }
-        return moved;
+        S.cand[lane] = q;
     }
-
-    // Returns the best vector in (ox, oy) and its cost without the vector's bits. (e0x, e0y) and
-    // (e1x, e1y) are the extra candidates (nextra of them).
-    __device__ __noinline__ int motion_search(int r, int bx, int by, int w4, int h4, int mvpx, int mvpy, int e0x, int e0y,
-                                              int e1x, int e1y, int nextra, int& ox, int& oy) {
-        const int lam = P.lambda;
-        const int x0 = mbx * 16 + bx * 4, y0 = mby * 16 + by * 4, w = w4 * 4, h = h4 * 4;
-        const int cxlo = max(-(x0 + 24) * 4, -2048), cxhi = min((P.mb_w * 16 - x0 + 8) * 4, 2047);
-        const int cylo = max(-(y0 + 24) * 4, -512), cyhi = min((P.mb_h * 16 - y0 + 8) * 4, 511);
-        auto clx = [&](int v) { return min(max(v, cxlo), cxhi); };
-        auto cly = [&](int v) { return min(max(v, cylo), cyhi); };
-        auto intr = [](int v) { return (v + 2) & ~3; };
-        const int g = lane & 7;
-        // candidates (958-964): lane group g scores candidate g; absent ones are skipped in order
-        int px = 0, py = 0;
-        bool valid = true;
-        if (g == 0) {
-            px = intr(clx(mvpx));
-            py = intr(cly(mvpy));
-        } else if (g >= 2 && g <= 4) {
-            const Blk n = g == 2 ? nb(nullptr, -1, 0) : (g == 3 ? nb(nullptr, 0, -1) : nb(nullptr, 4, -1));
-            valid = n.w && n.z == r;
-            px = intr(clx(n.x));
-            py = intr(cly(n.y));
-        } else if (g == 5) {
-            valid = nextra > 0;
-            px = intr(clx(e0x));
-            py = intr(cly(e0y));
-        } else if (g == 6) {
-            valid = nextra > 1;
-            px = intr(clx(e1x));
-            py = intr(cly(e1y));
-        } else if (g == 7) {
-            valid = false;
+    __syncwarp();
+    pred_batch(P, S, r, bx, by, lgw, lgh, 9, false);
+    if (lane < 9) S.cost[lane] += lam * mvd_bits_d(S.cand[lane].x, S.cand[lane].y, mvpx, mvpy);
+    __syncwarp();
+    if (lane == 0) S.satd_px += (uint32_t)(9 * w * h);
+    bc = S.cost[0];
+    for (int c = 1; c < 9; c++) {
+        const int v = S.cost[c];
+        if (v < bc) {
+            bxv = S.cand[c].x;
+            byv = S.cand[c].y;
+            bc = v;
         }
-        int cost = sad_lane(r, bx, by, w, h, px, py, valid);
-        cost = valid ? cost + lam * mvd_bits_d(px, py, mvpx, mvpy) : BIG;
-        const unsigned vmask = __ballot_sync(FULL, valid) & 0xffu;
-        sad_px += (uint32_t)(__popc(vmask) * w * h);
-        int bxv = 0, byv = 0, bc = BIG;
-#pragma unroll
-        for (int k = 0; k < 8; k++) {
-            const int ck = __shfl_sync(FULL, cost, k);
-            const int xk = __shfl_sync(FULL, px, k), yk = __shfl_sync(FULL, py, k);
-            if (ck < bc) {
-                bc = ck;
-                bxv = xk;
-                byv = yk;
-            }
-        }
-        // the diamond (973-988): each round scores the 3x3 square of its step around the centre in one
-        // batch (group g -> square position k = g < 4 ? g : g + 1), then replays the four moves in order
-        const int nsteps = P.fast ? 2 : 3;
-        const int k = g < 4 ? g : g + 1, kx = k % 3, ky = k / 3;
-        for (int si = 0; si < nsteps; si++) {
-            const int step = P.fast ? (si == 0 ? 8 : 4) : (16 >> si);
-            const int iters = step == 4 ? 32 : 4;
-            for (int it = 0; it < iters; it++) {
-                const int cx = bxv, cy = byv, c0 = bc;
-                const int X0 = clx(cx - step), X2 = clx(cx + step), Y0 = cly(cy - step), Y2 = cly(cy + step);
-                const int qx = kx == 0 ? X0 : (kx == 1 ? cx : X2), qy = ky == 0 ? Y0 : (ky == 1 ? cy : Y2);
-                const int sc = sad_lane(r, bx, by, w, h, qx, qy, true) + lam * mvd_bits_d(qx, qy, mvpx, mvpy);
-                sad_px += (uint32_t)(4 * w * h);
-                bool moved;
-                if (X0 == cx - step && X2 == cx + step && Y0 == cy - step && Y2 == cy + step) {
-                    // no clamp: left, else right; then up from that column, else down
-                    const int sL = __shfl_sync(FULL, sc, 3), sR = __shfl_sync(FULL, sc, 4);
-                    int col = 1, b1 = c0;
-                    if (sL < c0) {
-                        col = 0;
-                        b1 = sL;
-                    } else if (sR < c0) {
-                        col = 2;
-                        b1 = sR;
-                    }
-                    const int sU = __shfl_sync(FULL, sc, col), sD = __shfl_sync(FULL, sc, 5 + col);
-                    int row = 1, b2 = b1;
-                    if (sU < b1) {
-                        row = 0;
-                        b2 = sU;
-                    } else if (sD < b1) {
-                        row = 2;
-                        b2 = sD;
-                    }
-                    bxv = col == 0 ? X0 : (col == 1 ? cx : X2);
-                    byv = row == 0 ? Y0 : (row == 1 ? cy : Y2);
-                    bc = b2;
-                    moved = col != 1 || row != 1;
-                } else {
-                    if (lane < 8) S.cost[k] = sc;
-                    if (lane == 0) S.cost[4] = c0;
-                    __syncwarp();
-                    moved = round_clamped(r, bx, by, w, h, mvpx, mvpy, step, cxlo, cxhi, cylo, cyhi, bxv, byv, bc);
-                    __syncwarp();
-                }
-                if (!moved) break;
-            }
-        }
-        // live coding's early exit (990-992)
-        if (P.fast && bc < (w * h) / 8 + lam) {
-            ox = bxv;
-            oy = byv;
-            return bc - lam * mvd_bits_d(bxv, byv, mvpx, mvpy);
-        }
-        const int lgw = w4 == 4 ? 2 : (w4 == 2 ? 1 : 0), lgh = h4 == 4 ? 2 : (h4 == 2 ? 1 : 0);
-        // sub-sample refinement (994-1017): the centre and the 8 half samples around it in one batch,
-        // square (-1,-1) (0,-1) (1,-1) (-1,0) (1,0) (-1,1) (0,1) (1,1) in order
-        if (lane < 9) {
-            int2 q = make_int2(bxv, byv);
-            if (lane > 0) {
-                const int kk = lane <= 4 ? lane - 1 : lane;
-                q = make_int2(clx(bxv + (kk % 3 - 1) * 2), cly(byv + (kk / 3 - 1) * 2));
-            }
-            S.cand[lane] = q;
+    }
+    __syncwarp();
+    if (!P.fast) {
+        // the 4 quarter samples around the new centre: (0,-1) (-1,0) (1,0) (0,1)
+        if (lane < 4) {
+            const int dx = lane == 1 ? -1 : (lane == 2 ? 1 : 0), dy = lane == 0 ? -1 : (lane == 3 ? 1 : 0);
+            S.cand[lane] = make_int2(clx(bxv + dx), cly(byv + dy));
         }
         __syncwarp();
-        pred_batch(r, bx, by, lgw, lgh, 9, false);
-        if (lane < 9) S.cost[lane] += lam * mvd_bits_d(S.cand[lane].x, S.cand[lane].y, mvpx, mvpy);
+        pred_batch(P, S, r, bx, by, lgw, lgh, 4, false);
+        if (lane < 4) S.cost[lane] += lam * mvd_bits_d(S.cand[lane].x, S.cand[lane].y, mvpx, mvpy);
         __syncwarp();
-        satd_px += (uint32_t)(9 * w * h);
-        bc = S.cost[0];
-        for (int c = 1; c < 9; c++) {
+        if (lane == 0) S.satd_px += (uint32_t)(4 * w * h);
+        int nbx = bxv, nby = byv;
+        for (int c = 0; c < 4; c++) {
             const int v = S.cost[c];
             if (v < bc) {
-                bxv = S.cand[c].x;
-                byv = S.cand[c].y;
+                nbx = S.cand[c].x;
+                nby = S.cand[c].y;
                 bc = v;
             }
         }
+        bxv = nbx;
+        byv = nby;
         __syncwarp();
-        if (!P.fast) {
-            // the 4 quarter samples around the new centre: (0,-1) (-1,0) (1,0) (0,1)
-            if (lane < 4) {
-                const int dx = lane == 1 ? -1 : (lane == 2 ? 1 : 0), dy = lane == 0 ? -1 : (lane == 3 ? 1 : 0);
-                S.cand[lane] = make_int2(clx(bxv + dx), cly(byv + dy));
-            }
-            __syncwarp();
-            pred_batch(r, bx, by, lgw, lgh, 4, false);
-            if (lane < 4) S.cost[lane] += lam * mvd_bits_d(S.cand[lane].x, S.cand[lane].y, mvpx, mvpy);
-            __syncwarp();
-            satd_px += (uint32_t)(4 * w * h);
-            int nbx = bxv, nby = byv;
-            for (int c = 0; c < 4; c++) {
-                const int v = S.cost[c];
-                if (v < bc) {
-                    nbx = S.cand[c].x;
-                    nby = S.cand[c].y;
-                    bc = v;
+    }
+    return make_int4(bc - lam * mvd_bits_d(bxv, byv, mvpx, mvpy), bxv, byv, 0);
+}
+
+// ---- partition decision ----------------------------------------------------------------------------
+
+static __device__ __forceinline__ void blk_clear(const AnalyseParams& P, WarpSmem& S, Blk* b) {
+    const int lane = threadIdx.x & 31;
+    if (lane < 16) b[lane] = make_int4(0, 0, -1, 0);
+    __syncwarp();
+}
+static __device__ __forceinline__ void blk_copy(const AnalyseParams& P, WarpSmem& S, Blk* d, const Blk* s) {
+    const int lane = threadIdx.x & 31;
+    if (lane < 16) d[lane] = s[lane];
+    __syncwarp();
+}
+// Marks rectangle (x, y, w, h) of `b` as decided with vector (mx, my) and reference rf.
+static __device__ __forceinline__ void blk_paint(const AnalyseParams& P, WarpSmem& S, Blk* b, int x, int y, int w, int h, int mx, int my, int rf) {
+    const int lane = threadIdx.x & 31;
+    if (lane < 16) {
+        const int bx = lane & 3, by = lane >> 2;
+        if (bx >= x && bx < x + w && by >= y && by < y + h) b[lane] = make_int4(mx, my, rf, 1);
+    }
+    __syncwarp();
+}
+
+// sub_search, enc/frame.rs:911-938: returns sub_mb_type, its cost in cost_out; leaves the 8x8
+// block's vectors in S.st.
+static __device__ __noinline__ int2 sub_search(const AnalyseParams& P, WarpSmem& S, int r, int k, int ex, int ey) {
+    const int lam = P.lambda;
+    const int ox = (k & 1) * 2, oy = (k >> 1) * 2;
+    const int ns = P.sub8 ? 4 : 1;
+    int best_s = 0, best_cost = 0;
+    for (int s = 0; s < ns; s++) {
+        blk_copy(P, S, S.t, S.st);
+        int cost = lam * (s == 0 ? 0 : 2);
+        for (int q = 0; q < c_nsub[s]; q++) {
+            const int x = ox + c_sub[s][q][0], y = oy + c_sub[s][q][1], w = c_sub[s][q][2], h = c_sub[s][q][3];
+            const int2 p = pred_mv(P, S, S.t, x, y, w, 0, r);
+            const int4 ms = motion_search(P, S, r, x, y, w, h, p.x, p.y, ex, ey, 0, 0, 1);
+            const int c = ms.x, mx = ms.y, my = ms.z;
+            cost += c + lam * mvd_bits_d(mx, my, p.x, p.y);
+            blk_paint(P, S, S.t, x, y, w, h, mx, my, r);
+        }
+        if (s == 0 || cost < best_cost) {
+            best_s = s;
+            best_cost = cost;
+            if (ns > 1) blk_copy(P, S, S.bt, S.t);
+        }
+    }
+    blk_copy(P, S, S.st, ns > 1 ? S.bt : S.t);
+    return make_int2(best_s, best_cost);
+}
+
+// best_inter_ref, enc/frame.rs:852-905. Leaves the winner's vectors in S.best_mvs.
+static __device__ __noinline__ int4 best_inter_ref(const AnalyseParams& P, WarpSmem& S, int r) {
+    const int lane = threadIdx.x & 31;
+    const int lam = P.lambda;
+    int rb = 0;
+    if (P.nact == 2) rb = lam;  // ref_bits, enc/frame.rs:705-711
+    else if (P.nact > 2) rb = lam * (2 * (31 - __clz(r + 1)) + 1);
+    const int2 mvp = pred_mv(P, S, nullptr, 0, 0, 4, 0, r);
+    const ColMv col = P.col[S.mb];
+    const int4 ms = motion_search(P, S, r, 0, 0, 4, 4, mvp.x, mvp.y, col.mv[0], col.mv[1], 0, 0, col.valid ? 1 : 0);
+    const int c = ms.x, mx = ms.y, my = ms.z;
+    int best_part = 0, best_cost = c + lam * (mvd_bits_d(mx, my, mvp.x, mvp.y) + 1) + rb;
+    const int cost16 = best_cost;
+    uint32_t sub_out = 0;
+    if (lane < 16) {
+        S.best_mvs[lane][0] = (int16_t)mx;
+        S.best_mvs[lane][1] = (int16_t)my;
+    }
+    __syncwarp();
+    if (P.fast) return make_int4(best_cost, 0, 0, cost16);
+    // P_8x8 (868-876)
+    blk_clear(P, S, S.st);
+    uint32_t sub = 0;
+    int cost8 = lam * 9;
+    for (int k = 0; k < 4; k++) {
+        const int2 ss = sub_search(P, S, r, k, mx, my);
+        const int ck = ss.y;
+        sub |= (uint32_t)ss.x << (8 * k);
+        cost8 += ck + rb;
+        if (cost8 >= best_cost) break;
+    }
+    if (cost8 < best_cost) {
+        // v8: the vectors of rects(3, sub) in coding order (882-885)
+        if (lane == 0) {
+            int n = 0;
+            for (int k = 0; k < 4; k++) {
+                const int s = (sub >> (8 * k)) & 0xff;
+                for (int q = 0; q < c_nsub[s]; q++) {
+                    const int x = (k & 1) * 2 + c_sub[s][q][0], y = (k >> 1) * 2 + c_sub[s][q][1];
+                    S.best_mvs[n][0] = (int16_t)S.st[y * 4 + x].x;
+                    S.best_mvs[n][1] = (int16_t)S.st[y * 4 + x].y;
+                    n++;
                 }
             }
-            bxv = nbx;
-            byv = nby;
-            __syncwarp();
+            for (; n < 16; n++) S.best_mvs[n][0] = S.best_mvs[n][1] = 0;
         }
-        ox = bxv;
-        oy = byv;
-        return bc - lam * mvd_bits_d(bxv, byv, mvpx, mvpy);
-    }
-
-    // ---- partition decision ----------------------------------------------------------------------------
-
-    __device__ __forceinline__ void blk_clear(Blk* b) {
-        if (lane < 16) b[lane] = make_int4(0, 0, -1, 0);
         __syncwarp();
+        best_part = 3;
+        best_cost = cost8;
+        sub_out = sub;
+        // 16x8 and 8x16 halves searched from the 8x8 vectors they cover (886-902)
+        for (int part = 1; part < 3; part++) {
+            int pc = lam * 3;
+            int h0x = 0, h0y = 0, h1x = 0, h1y = 0;
+            for (int k = 0; k < 2; k++) {
+                // part_mvps(...)[k]: the halves before k are decided
+                blk_clear(P, S, S.t);
+                if (k == 1)
+                    blk_paint(P, S, S.t, c_parts[part][0][0], c_parts[part][0][1], c_parts[part][0][2], c_parts[part][0][3], h0x, h0y, r);
+                const int x = c_parts[part][k][0], y = c_parts[part][k][1], w = c_parts[part][k][2], h = c_parts[part][k][3];
+                const int2 p = pred_mv(P, S, S.t, x, y, w, part, r);
+                const int i0 = part == 1 ? 2 * k : k, i1 = part == 1 ? 2 * k + 1 : k + 2;
+                const Blk a0 = S.st[(i0 / 2) * 8 + (i0 % 2) * 2], a1 = S.st[(i1 / 2) * 8 + (i1 % 2) * 2];
+                const int4 ms = motion_search(P, S, r, x, y, w, h, p.x, p.y, a0.x, a0.y, a1.x, a1.y, 2);
+                const int cc = ms.x, m0 = ms.y, m1 = ms.z;
+                if (k == 0) {
+                    h0x = m0;
+                    h0y = m1;
+                } else {
+                    h1x = m0;
+                    h1y = m1;
+                }
+                pc += cc + lam * mvd_bits_d(m0, m1, p.x, p.y) + rb;
+                if (pc >= best_cost) break;
+            }
+            if (pc < best_cost) {
+                best_part = part;
+                best_cost = pc;
+                sub_out = 0;
+                if (lane < 16) {
+                    S.best_mvs[lane][0] = (int16_t)(lane == 0 ? h0x : (lane == 1 ? h1x : 0));
+                    S.best_mvs[lane][1] = (int16_t)(lane == 0 ? h0y : (lane == 1 ? h1y : 0));
+                }
+                __syncwarp();
+            }
+        }
     }
-    __device__ __forceinline__ void blk_copy(Blk* d, const Blk* s) {
-        if (lane < 16) d[lane] = s[lane];
-        __syncwarp();
+    return make_int4(best_cost, best_part, (int)sub_out, cost16);
+}
+
+// ---- one macroblock --------------------------------------------------------------------------------
+
+static __device__ void analyse(const AnalyseParams& P, WarpSmem& S, bool auto_policy) {
+    const int lane = threadIdx.x & 31;
+    // the current macroblock: 16 rows of 16 bytes, as 128-bit loads
+    if (lane < 16) {
+        const uint4 v = *reinterpret_cast<const uint4*>(P.src + (size_t)(S.mby * 16 + lane) * P.ls + S.mbx * 16);
+        S.src[lane * 4 + 0] = v.x;
+        S.src[lane * 4 + 1] = v.y;
+        S.src[lane * 4 + 2] = v.z;
+        S.src[lane * 4 + 3] = v.w;
     }
-    // Marks rectangle (x, y, w, h) of `b` as decided with vector (mx, my) and reference rf.
-    __device__ __forceinline__ void blk_paint(Blk* b, int x, int y, int w, int h, int mx, int my, int rf) {
+    if (lane < 26) reinterpret_cast<uint32_t*>(&S.res)[lane] = 0;
+    __syncwarp();
+    if (lane == 0) S.sad_px = S.satd_px = 0;
+    // P_Skip (enc/frame.rs:722-729)
+    const int2 sv = skip_mv(P, S);
+    if (lane == 0) S.cand[0] = sv;
+    __syncwarp();
+    pred_batch(P, S, 0, 0, 0, 2, 2, 1, true);
+    const int skip_sad = S.cost[0];
+    __syncwarp();
+    if (lane == 0) S.sad_px += 256;
+    const bool skip = auto_policy && skip_sad < P.skip_thresh;
+    int part = 0, cost = 0, cost16 = 0, bestr = 0;
+    uint32_t sub = 0;
+    if (!skip) {
+        // best_inter, enc/frame.rs:839-849: every reference, the cheapest (first on ties) wins
+        for (int r = 0; r < P.nact; r++) {
+            const int4 bi = best_inter_ref(P, S, r);
+            const int c = bi.x, p = bi.y, c16 = bi.w;
+            const uint32_t sb = (uint32_t)bi.z;
+            if (r == 0 || c < cost) {
+                part = p;
+                cost = c;
+                cost16 = c16;
+                bestr = r;
+                sub = sb;
+                if (lane < 16) {
+                    S.win_mvs[lane][0] = S.best_mvs[lane][0];
+                    S.win_mvs[lane][1] = S.best_mvs[lane][1];
+                }
+                __syncwarp();
+            }
+        }
+    }
+    // the result
+    if (lane == 0) {
+        ironav_mbresult& R = S.res;
+        R.skip_mv[0] = (int16_t)sv.x;
+        R.skip_mv[1] = (int16_t)sv.y;
+        R.skip_sad = skip_sad;
+        R.flags = skip ? IRONAV_RESULT_SKIP : IRONAV_RESULT_INTER;
+        if (!skip) {
+            R.part = (uint8_t)part;
+            for (int i = 0; i < 4; i++) {
+                R.refs[i] = (uint8_t)bestr;
+                R.sub[i] = (uint8_t)((sub >> (8 * i)) & 0xff);
+            }
+            R.cost = cost;
+            R.cost16 = cost16;
+        }
+        R.sad_px = S.sad_px;
+        R.satd_px = S.satd_px;
+    }
+    __syncwarp();
+    if (lane < 16 && !skip) {
+        S.res.mvs[lane][0] = S.win_mvs[lane][0];
+        S.res.mvs[lane][1] = S.win_mvs[lane][1];
+    }
+    __syncwarp();
+    if (lane < 26) reinterpret_cast<uint32_t*>(&P.results[S.mb])[lane] = reinterpret_cast<const uint32_t*>(&S.res)[lane];
+    if (auto_policy) {
+        // the decision's MbState (finish_mb, enc/frame.rs:2281-2321)
         if (lane < 16) {
             const int bx = lane & 3, by = lane >> 2;
-            if (bx >= x && bx < x + w && by >= y && by < y + h) b[lane] = make_int4(mx, my, rf, 1);
-        }
-        __syncwarp();
-    }
-
-    // sub_search, enc/frame.rs:911-938: returns sub_mb_type, its cost in cost_out; leaves the 8x8
-    // block's vectors in S.st.
-    __device__ __noinline__ int sub_search(int r, int k, int ex, int ey, int& cost_out) {
-        const int lam = P.lambda;
-        const int ox = (k & 1) * 2, oy = (k >> 1) * 2;
-        const int ns = P.sub8 ? 4 : 1;
-        int best_s = 0, best_cost = 0;
-        for (int s = 0; s < ns; s++) {
-            blk_copy(S.t, S.st);
-            int cost = lam * (s == 0 ? 0 : 2);
-            for (int q = 0; q < c_nsub[s]; q++) {
-                const int x = ox + c_sub[s][q][0], y = oy + c_sub[s][q][1], w = c_sub[s][q][2], h = c_sub[s][q][3];
-                const int2 p = pred_mv(S.t, x, y, w, 0, r);
-                int mx, my;
-                const int c = motion_search(r, x, y, w, h, p.x, p.y, ex, ey, 0, 0, 1, mx, my);
-                cost += c + lam * mvd_bits_d(mx, my, p.x, p.y);
-                blk_paint(S.t, x, y, w, h, mx, my, r);
-            }
-            if (s == 0 || cost < best_cost) {
-                best_s = s;
-                best_cost = cost;
-                if (ns > 1) blk_copy(S.bt, S.t);
-            }
-        }
-        blk_copy(S.st, ns > 1 ? S.bt : S.t);
-        cost_out = best_cost;
-        return best_s;
-    }
-
-    // best_inter_ref, enc/frame.rs:852-905. Leaves the winner's vectors in S.best_mvs.
-    __device__ __noinline__ int best_inter_ref(int r, int& part_out, uint32_t& sub_out, int& cost16) {
-        const int lam = P.lambda;
-        int rb = 0;
-        if (P.nact == 2) rb = lam;  // ref_bits, enc/frame.rs:705-711
-        else if (P.nact > 2) rb = lam * (2 * (31 - __clz(r + 1)) + 1);
-        const int2 mvp = pred_mv(nullptr, 0, 0, 4, 0, r);
-        const ColMv col = P.col[mb];
-        int mx, my;
-        const int c = motion_search(r, 0, 0, 4, 4, mvp.x, mvp.y, col.mv[0], col.mv[1], 0, 0, col.valid ? 1 : 0, mx, my);
-        int best_part = 0, best_cost = c + lam * (mvd_bits_d(mx, my, mvp.x, mvp.y) + 1) + rb;
-        cost16 = best_cost;
-        if (lane < 16) {
-            S.best_mvs[lane][0] = (int16_t)mx;
-            S.best_mvs[lane][1] = (int16_t)my;
-        }
-        __syncwarp();
-        sub_out = 0;
-        if (P.fast) {
-            part_out = 0;
-            return best_cost;
-        }
-        // P_8x8 (868-876)
-        blk_clear(S.st);
-        uint32_t sub = 0;
-        int cost8 = lam * 9;
-        for (int k = 0; k < 4; k++) {
-            int ck;
-            sub |= (uint32_t)sub_search(r, k, mx, my, ck) << (8 * k);
-            cost8 += ck + rb;
-            if (cost8 >= best_cost) break;
-        }
-        if (cost8 < best_cost) {
-            // v8: the vectors of rects(3, sub) in coding order (882-885)
-            if (lane == 0) {
-                int n = 0;
-                for (int k = 0; k < 4; k++) {
-                    const int s = (sub >> (8 * k)) & 0xff;
-                    for (int q = 0; q < c_nsub[s]; q++) {
-                        const int x = (k & 1) * 2 + c_sub[s][q][0], y = (k >> 1) * 2 + c_sub[s][q][1];
-                        S.best_mvs[n][0] = (int16_t)S.st[y * 4 + x].x;
-                        S.best_mvs[n][1] = (int16_t)S.st[y * 4 + x].y;
-                        n++;
-                    }
-                }
-                for (; n < 16; n++) S.best_mvs[n][0] = S.best_mvs[n][1] = 0;
-            }
-            __syncwarp();
-            best_part = 3;
-            best_cost = cost8;
-            sub_out = sub;
-            // 16x8 and 8x16 halves searched from the 8x8 vectors they cover (886-902)
-            for (int part = 1; part < 3; part++) {
-                int pc = lam * 3;
-                int h0x = 0, h0y = 0, h1x = 0, h1y = 0;
-                for (int k = 0; k < 2; k++) {
-                    // part_mvps(...)[k]: the halves before k are decided
-                    blk_clear(S.t);
-                    if (k == 1)
-                        blk_paint(S.t, c_parts[part][0][0], c_parts[part][0][1], c_parts[part][0][2], c_parts[part][0][3], h0x, h0y, r);
-                    const int x = c_parts[part][k][0], y = c_parts[part][k][1], w = c_parts[part][k][2], h = c_parts[part][k][3];
-                    const int2 p = pred_mv(S.t, x, y, w, part, r);
-                    const int i0 = part == 1 ? 2 * k : k, i1 = part == 1 ? 2 * k + 1 : k + 2;
-                    const Blk a0 = S.st[(i0 / 2) * 8 + (i0 % 2) * 2], a1 = S.st[(i1 / 2) * 8 + (i1 % 2) * 2];
-                    int m0, m1;
-                    const int cc = motion_search(r, x, y, w, h, p.x, p.y, a0.x, a0.y, a1.x, a1.y, 2, m0, m1);
-                    if (k == 0) {
-                        h0x = m0;
-                        h0y = m1;
-                    } else {
-                        h1x = m0;
-                        h1y = m1;
-                    }
-                    pc += cc + lam * mvd_bits_d(m0, m1, p.x, p.y) + rb;
-                    if (pc >= best_cost) break;
-                }
-                if (pc < best_cost) {
-                    best_part = part;
-                    best_cost = pc;
-                    sub_out = 0;
-                    if (lane < 16) {
-                        S.best_mvs[lane][0] = (int16_t)(lane == 0 ? h0x : (lane == 1 ? h1x : 0));
-                        S.best_mvs[lane][1] = (int16_t)(lane == 0 ? h0y : (lane == 1 ? h1y : 0));
-                    }
-                    __syncwarp();
-                }
-            }
-        }
-        part_out = best_part;
-        return best_cost;
-    }
-
-    // ---- one macroblock --------------------------------------------------------------------------------
-
-    __device__ void analyse(bool auto_policy) {
-        // the current macroblock: 16 rows of 16 bytes, as 128-bit loads
-        if (lane < 16) {
-            const uint4 v = *reinterpret_cast<const uint4*>(P.src + (size_t)(mby * 16 + lane) * P.ls + mbx * 16);
-            S.src[lane * 4 + 0] = v.x;
-            S.src[lane * 4 + 1] = v.y;
-            S.src[lane * 4 + 2] = v.z;
-            S.src[lane * 4 + 3] = v.w;
-        }
-        if (lane < 26) reinterpret_cast<uint32_t*>(&S.res)[lane] = 0;
-        __syncwarp();
-        sad_px = satd_px = 0;
-        // P_Skip (enc/frame.rs:722-729)
-        const int2 sv = skip_mv();
-        if (lane == 0) S.cand[0] = sv;
-        __syncwarp();
-        pred_batch(0, 0, 0, 2, 2, 1, true);
-        const int skip_sad = S.cost[0];
-        __syncwarp();
-        sad_px += 256;
-        const bool skip = auto_policy && skip_sad < P.skip_thresh;
-        int part = 0, cost = 0, cost16 = 0, bestr = 0;
-        uint32_t sub = 0;
-        if (!skip) {
-            // best_inter, enc/frame.rs:839-849: every reference, the cheapest (first on ties) wins
-            for (int r = 0; r < P.nact; r++) {
-                int p, c16;
-                uint32_t sb;
-                const int c = best_inter_ref(r, p, sb, c16);
-                if (r == 0 || c < cost) {
-                    part = p;
-                    cost = c;
-                    cost16 = c16;
-                    bestr = r;
-                    sub = sb;
-                    if (lane < 16) {
-                        S.win_mvs[lane][0] = S.best_mvs[lane][0];
-                        S.win_mvs[lane][1] = S.best_mvs[lane][1];
-                    }
-                    __syncwarp();
-                }
-            }
-        }
-        // the result
-        if (lane == 0) {
-            ironav_mbresult& R = S.res;
-            R.skip_mv[0] = (int16_t)sv.x;
-            R.skip_mv[1] = (int16_t)sv.y;
-            R.skip_sad = skip_sad;
-            R.flags = skip ? IRONAV_RESULT_SKIP : IRONAV_RESULT_INTER;
+            int mx = sv.x, my = sv.y;
             if (!skip) {
-                R.part = (uint8_t)part;
-                for (int i = 0; i < 4; i++) {
-                    R.refs[i] = (uint8_t)bestr;
-                    R.sub[i] = (uint8_t)((sub >> (8 * i)) & 0xff);
+                // the rectangle of rects(part, sub) holding this block, in coding order
+                int idx = 0;
+                if (part == 1) idx = by >> 1;
+                else if (part == 2) idx = bx >> 1;
+                else if (part == 3) {
+                    const int k = (by >> 1) * 2 + (bx >> 1);
+                    int n = 0;
+                    for (int q = 0; q < k; q++) n += c_nsub[(sub >> (8 * q)) & 0xff];
+                    const int s = (sub >> (8 * k)) & 0xff, lx = bx & 1, ly = by & 1;
+                    idx = n + (s == 0 ? 0 : (s == 1 ? ly : (s == 2 ? lx : ly * 2 + lx)));
                 }
-                R.cost = cost;
-                R.cost16 = cost16;
+                mx = S.win_mvs[idx][0];
+                my = S.win_mvs[idx][1];
             }
-            R.sad_px = sad_px;
-            R.satd_px = satd_px;
+            S.out.mvs[lane][0] = (int16_t)mx;
+            S.out.mvs[lane][1] = (int16_t)my;
+        }
+        if (lane == 0) {
+            S.out.inter = 1;
+            for (int i = 0; i < 4; i++) S.out.refs[i] = (int8_t)(skip ? 0 : bestr);
+            S.out.pad[0] = S.out.pad[1] = S.out.pad[2] = 0;
         }
         __syncwarp();
-        if (lane < 16 && !skip) {
-            S.res.mvs[lane][0] = S.win_mvs[lane][0];
-            S.res.mvs[lane][1] = S.win_mvs[lane][1];
-        }
-        __syncwarp();
-        if (lane < 26) reinterpret_cast<uint32_t*>(&P.results[mb])[lane] = reinterpret_cast<const uint32_t*>(&S.res)[lane];
-        if (auto_policy) {
-            // the decision's MbState (finish_mb, enc/frame.rs:2281-2321)
-            if (lane < 16) {
-                const int bx = lane & 3, by = lane >> 2;
-                int mx = sv.x, my = sv.y;
-                if (!skip) {
-                    // the rectangle of rects(part, sub) holding this block, in coding order
-                    int idx = 0;
-                    if (part == 1) idx = by >> 1;
-                    else if (part == 2) idx = bx >> 1;
-                    else if (part == 3) {
-                        const int k = (by >> 1) * 2 + (bx >> 1);
-                        int n = 0;
-                        for (int q = 0; q < k; q++) n += c_nsub[(sub >> (8 * q)) & 0xff];
-                        const int s = (sub >> (8 * k)) & 0xff, lx = bx & 1, ly = by & 1;
-                        idx = n + (s == 0 ? 0 : (s == 1 ? ly : (s == 2 ? lx : ly * 2 + lx)));
-                    }
-                    mx = S.win_mvs[idx][0];
-                    my = S.win_mvs[idx][1];
-                }
-                S.out.mvs[lane][0] = (int16_t)mx;
-                S.out.mvs[lane][1] = (int16_t)my;
-            }
-            if (lane == 0) {
-                S.out.inter = 1;
-                for (int i = 0; i < 4; i++) S.out.refs[i] = (int8_t)(skip ? 0 : bestr);
-                S.out.pad[0] = S.out.pad[1] = S.out.pad[2] = 0;
-            }
-            __syncwarp();
-            if (lane < 18) reinterpret_cast<uint32_t*>(&P.states_out[mb])[lane] = reinterpret_cast<const uint32_t*>(&S.out)[lane];
-        }
-        __syncwarp();
+        if (lane < 18) reinterpret_cast<uint32_t*>(&P.states_out[S.mb])[lane] = reinterpret_cast<const uint32_t*>(&S.out)[lane];
     }
-};
+    __syncwarp();
+}
 
 __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
     unsigned v;
@@ -722,32 +719,36 @@ static __device__ bool wait_published(const AnalyseParams& P, int m) {
 }
 
 template <bool AUTO>
-__global__ void __launch_bounds__(K2_WARPS * 32) analyse_kernel(const AnalyseParams P) {
+__global__ void __launch_bounds__(K2_WARPS * 32, K2_MIN_BLOCKS) analyse_kernel(const __grid_constant__ AnalyseParams P) {
     __shared__ WarpSmem smem[K2_WARPS];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    MbWarp W(P, smem[wid], lane);
+    WarpSmem& S = smem[wid];
     for (;;) {
         unsigned t = 0;
         if (lane == 0) t = atomicAdd(P.ticket, 1u);
         t = __shfl_sync(FULL, t, 0);
         if (t >= (unsigned)P.nmb) break;
         const int mb = P.order ? P.order[t] : (int)t;
-        W.mb = mb;
-        W.mbx = mb % P.mb_w;
-        W.mby = mb / P.mb_w;
+        const int mbx = mb % P.mb_w, mby = mb / P.mb_w;
+        if (lane == 0) {
+            S.mb = mb;
+            S.mbx = mbx;
+            S.mby = mby;
+        }
+        __syncwarp();
         if (AUTO) {
             // the left and top-right (top at the right edge) neighbours; their own waits cover the rest
-            const int start = P.band_start[W.mby];
+            const int start = P.band_start[mby];
             bool ok = true;
-            if (W.mbx > 0) ok = wait_published(P, mb - 1);
-            if (ok && W.mby > start) ok = wait_published(P, (W.mbx + 1 < P.mb_w) ? mb - P.mb_w + 1 : mb - P.mb_w);
+            if (mbx > 0) ok = wait_published(P, mb - 1);
+            if (ok && mby > start) ok = wait_published(P, (mbx + 1 < P.mb_w) ? mb - P.mb_w + 1 : mb - P.mb_w);
             ok = __all_sync(FULL, ok);
             if (!ok) break;
-            W.load_neighbours(P.states_out);
+            load_neighbours(P, S, P.states_out);
         } else {
-            W.load_neighbours(P.states_in);
+            load_neighbours(P, S, P.states_in);
         }
-        W.analyse(AUTO);
+        analyse(P, S, AUTO);
         if (AUTO) {
             __threadfence();
             __syncwarp();

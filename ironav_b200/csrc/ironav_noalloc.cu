@@ -82,10 +82,11 @@ __global__ void noalloc_init_kernel(uint32_t* scr, const ironav_mbstate* col, in
 // The wavefront analysis with tickets in row-interleaved order: ticket T covers row slot R = T / mb_w
 // (the R / nslices-th row of band R % nslices) and column T % mb_w. A macroblock's left and top-right
 // neighbours always hold smaller tickets, so a waiting warp only waits on running warps.
-__global__ void __launch_bounds__(K2_WARPS * 32) analyse_noalloc_kernel(const AnalyseParams P, int nslices, int max_rows) {
+__global__ void __launch_bounds__(K2_WARPS * 32, K2_MIN_BLOCKS) analyse_noalloc_kernel(const __grid_constant__ AnalyseParams P, int nslices,
+                                                                       int max_rows) {
     __shared__ WarpSmem smem[K2_WARPS];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    MbWarp W(P, smem[wid], lane);
+    WarpSmem& S = smem[wid];
     const unsigned total = (unsigned)nslices * (unsigned)max_rows * (unsigned)P.mb_w;
     for (;;) {
         unsigned t = 0;
@@ -97,16 +98,19 @@ __global__ void __launch_bounds__(K2_WARPS * 32) analyse_noalloc_kernel(const An
         const int y0 = b * P.mb_h / nslices, y1 = (b + 1) * P.mb_h / nslices;
         if (y0 + r >= y1) continue;  // this band has fewer rows
         const int mby = y0 + r, mb = mby * P.mb_w + x;
-        W.mb = mb;
-        W.mbx = x;
-        W.mby = mby;
+        if (lane == 0) {
+            S.mb = mb;
+            S.mbx = x;
+            S.mby = mby;
+        }
+        __syncwarp();
         bool ok = true;
         if (x > 0) ok = wait_published(P, mb - 1);
         if (ok && mby > y0) ok = wait_published(P, (x + 1 < P.mb_w) ? mb - P.mb_w + 1 : mb - P.mb_w);
         ok = __all_sync(FULL, ok);
         if (!ok) break;
-        W.load_neighbours(P.states_out);
-        W.analyse(true);
+        load_neighbours(P, S, P.states_out);
+        analyse(P, S, true);
         __threadfence();
         __syncwarp();
         if (lane == 0) st_release(&P.flags[mb], P.epoch);
