@@ -331,17 +331,13 @@ static __device__ __noinline__ int4 motion_search(const AnalyseParams& P, WarpSm
     cost = valid ? cost + lam * mvd_bits_d(px, py, mvpx, mvpy) : BIG;
     const unsigned vmask = __ballot_sync(FULL, valid) & 0xffu;
     if (lane == 0) S.sad_px += (uint32_t)(__popc(vmask) * w * h);
-    int bxv = 0, byv = 0, bc = BIG;
+    // the first candidate of least cost: min over (cost, position in the list)
+    unsigned long long key = ((unsigned long long)(unsigned)cost << 3) | (unsigned)g;
 #pragma unroll
-    for (int k = 0; k < 8; k++) {
-        const int ck = __shfl_sync(FULL, cost, k);
-        const int xk = __shfl_sync(FULL, px, k), yk = __shfl_sync(FULL, py, k);
-        if (ck < bc) {
-            bc = ck;
-            bxv = xk;
-            byv = yk;
-        }
-    }
+    for (int off = 1; off < 8; off <<= 1) key = min(key, __shfl_xor_sync(FULL, key, off));
+    const int win = (int)(key & 7u);
+    int bc = (int)(key >> 3);
+    int bxv = __shfl_sync(FULL, px, win), byv = __shfl_sync(FULL, py, win);
     // the diamond (973-988): each round scores the 3x3 square of its step around the centre in one
     // batch (group g -> square position k = g < 4 ? g : g + 1), then replays the four moves in order
     const int nsteps = P.fast ? 2 : 3;
