@@ -121,7 +121,8 @@ class Clocks:
         os.unlink(self.path)
         if not sm:
             return None
-        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm),
+                "window": "0.6 s of untimed steps, then the timed steps"}
 
 
 def make_frames(rank: int, n: int):
@@ -280,9 +281,18 @@ def main():
     with torch.cuda.stream(stream):
         for i in range(args.warmup):
             step(i)
-        barrier()
+        # nvidia-smi samples every 100 ms, longer than a few timed steps: keep the GPU busy with untimed
+        # steps for half a second before the timed ones so the samples cover the load around them
         clocks = Clocks(local)
         clocks.start()
+        t_load = time.perf_counter()
+        i = 0
+        while time.perf_counter() - t_load < 0.6:
+            for _ in range(8):
+                step(args.warmup + i)
+                i += 1
+            torch.cuda.synchronize()
+        barrier()
         k2_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)

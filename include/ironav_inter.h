@@ -157,6 +157,32 @@ int ironav_analyse_picture_auto_device(ironav_ctx* ctx, ironav_mbstate* d_out_st
  * wait that gave up). */
 int ironav_ctx_sync(ironav_ctx* ctx);
 
+/* ---- in-loop mode ---------------------------------------------------------------------------------- */
+
+/* The encoder's own loop (FrameCoder::encode, enc/frame.rs:467-478): the caller makes each macroblock's
+ * final decision itself (code_mb's rate-distortion choice, enc/frame.rs:752-790) and commits it
+ * (finish_mb, enc/frame.rs:2281-2339); the device analyses every macroblock as soon as the decisions of
+ * its left and top-right neighbours are committed, and publishes its result. Results and decisions
+ * travel through host memory mapped into the device.
+ *
+ * The caller must read results and commit decisions in the order it names here, which is also the
+ * order the device takes macroblocks in, so that no macroblock it waits for sits behind one that waits
+ * for it:
+ *   IRONAV_INLOOP_RASTER  one caller thread, picture raster order (slice band after slice band);
+ *   IRONAV_INLOOP_BANDS   one caller thread per slice band, raster order within the band.
+ * Every device wait is bounded in time (ironav_inloop_set_wait, 10 s by default); a wait that runs out
+ * ends the picture with IRONAV_TIMEOUT from ironav_inloop_end. */
+#define IRONAV_INLOOP_RASTER 0
+#define IRONAV_INLOOP_BANDS 1
+int ironav_inloop_begin(ironav_ctx* ctx, int order);
+/* Waits (at most timeout_ms) for macroblock mb's result and copies it to out. */
+int ironav_inloop_result(ironav_ctx* ctx, int mb, ironav_mbresult* out, int timeout_ms);
+/* Commits macroblock mb's final decision. */
+int ironav_inloop_commit(ironav_ctx* ctx, int mb, const ironav_mbstate* final_state);
+/* Ends the picture: waits for the device, reports IRONAV_TIMEOUT if any wait gave up. */
+int ironav_inloop_end(ironav_ctx* ctx);
+int ironav_inloop_set_wait(ironav_ctx* ctx, int wait_ms);
+
 /* ---- analysis without allocation ------------------------------------------------------------------ */
 
 /* No counterpart in the reference: an entry point for callers that cannot allocate device memory (a

@@ -714,7 +714,69 @@ static __device__ bool wait_published(const AnalyseParams& P, int m) {
     }
 }
 
-template <bool AUTO>
+enum : int { MODE_REPLAY = 0, MODE_AUTO = 1, MODE_INLOOP = 2 };
+
+__device__ __forceinline__ unsigned ld_acquire_sys(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.sys.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_sys(unsigned* p, unsigned v) {
+    asm volatile("st.release.sys.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long globaltimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// In-loop mode: waits until the caller has committed macroblock m's final decision, for at most
+// P.wait_ns of wall time (the caller's own mode decision sits between two macroblocks). Backs off to
+// microsecond sleeps: the flag lives in host memory, so every poll crosses the bus.
+static __device__ bool wait_committed(const AnalyseParams& P, int m) {
+    const unsigned long long t0 = globaltimer();
+    for (unsigned i = 0;; i++) {
+        if (ld_acquire_sys(&P.commit_flags[m]) == P.epoch) return true;
+        if (ld_acquire(P.err) != 0) return false;
+        if ((i & 15) == 15 && globaltimer() - t0 > P.wait_ns) {
+            atomicOr(P.err, 1u);
+            return false;
+        }
+        __nanosleep(i < 32 ? 256 : 4000);
+    }
+}
+
+// The neighbours of an in-loop macroblock from the caller's committed decisions (host memory: read
+// around the caches, after the acquire of their flags).
+static __device__ void load_committed(const AnalyseParams& P, WarpSmem& S) {
+    const int lane = threadIdx.x & 31;
+    if (lane < 30) {
+        const int ex = lane % 6 - 1, ey = lane / 6 - 1;
+        Blk e = make_int4(0, 0, -1, 0);
+        if (ey < 0 || ex < 0) {
+            const int nx = S.mbx + (ex < 0 ? -1 : (ex >= 4 ? 1 : 0)), ny = S.mby + (ey < 0 ? -1 : 0);
+            const int bx = ex < 0 ? 3 : (ex >= 4 ? 0 : ex), by = ey < 0 ? 3 : ey;
+            if (nx >= 0 && nx < P.mb_w && ny >= P.band_start[S.mby] && ny < P.mb_h) {
+                const uint32_t* w = reinterpret_cast<const uint32_t*>(&P.committed[(size_t)ny * P.mb_w + nx]);
+                const uint32_t w0 = __ldcv(w), w1 = __ldcv(w + 1);  // inter, refs[0..2] | refs[3], pad
+                const uint32_t mv = __ldcv(w + 2 + by * 4 + bx);
+                const int inter = w0 & 0xff;
+                const int rsel = (by >> 1) * 2 + (bx >> 1);
+                const int rf = (int)(int8_t)(rsel < 3 ? (w0 >> (8 * (rsel + 1))) & 0xff : w1 & 0xff);
+                e.w = 1;
+                if (inter && rf >= 0) {
+                    e.x = (int)(int16_t)(mv & 0xffffu);
+                    e.y = (int)(int16_t)(mv >> 16);
+                    e.z = rf;
+                }
+            }
+        }
+        S.ext[lane] = e;
+    }
+    __syncwarp();
+}
+
+template <int MODE>
 __global__ void __launch_bounds__(K2_WARPS * 32, K2_MIN_BLOCKS) analyse_kernel(const __grid_constant__ AnalyseParams P) {
     __shared__ WarpSmem smem[K2_WARPS];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -732,23 +794,35 @@ __global__ void __launch_bounds__(K2_WARPS * 32, K2_MIN_BLOCKS) analyse_kernel(c
             S.mby = mby;
         }
         __syncwarp();
-        if (AUTO) {
+        if (MODE == MODE_REPLAY) {
+            load_neighbours(P, S, P.states_in);
+        } else {
             // the left and top-right (top at the right edge) neighbours; their own waits cover the rest
             const int start = P.band_start[mby];
+            const int m1 = mb - 1, m2 = (mbx + 1 < P.mb_w) ? mb - P.mb_w + 1 : mb - P.mb_w;
             bool ok = true;
-            if (mbx > 0) ok = wait_published(P, mb - 1);
-            if (ok && mby > start) ok = wait_published(P, (mbx + 1 < P.mb_w) ? mb - P.mb_w + 1 : mb - P.mb_w);
+            if (MODE == MODE_AUTO) {
+                if (mbx > 0) ok = wait_published(P, m1);
+                if (ok && mby > start) ok = wait_published(P, m2);
+            } else {
+                if (mbx > 0) ok = wait_committed(P, m1);
+                if (ok && mby > start) ok = wait_committed(P, m2);
+            }
             ok = __all_sync(FULL, ok);
             if (!ok) break;
-            load_neighbours(P, S, P.states_out);
-        } else {
-            load_neighbours(P, S, P.states_in);
+            if (MODE == MODE_AUTO) load_neighbours(P, S, P.states_out);
+            else load_committed(P, S);
         }
-        analyse(P, S, AUTO);
-        if (AUTO) {
+        analyse(P, S, MODE == MODE_AUTO);
+        if (MODE == MODE_AUTO) {
             __threadfence();
             __syncwarp();
             if (lane == 0 && mb != P.withhold) st_release(&P.flags[mb], P.epoch);
+        } else if (MODE == MODE_INLOOP) {
+            // the result is in host memory: make it visible there before its flag
+            __threadfence_system();
+            __syncwarp();
+            if (lane == 0) st_release_sys(&P.done_flags[mb], P.epoch);
         }
     }
 }

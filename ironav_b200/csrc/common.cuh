@@ -39,6 +39,12 @@ struct AnalyseParams {
     int nmb;
     int withhold;                     // test hook: this macroblock's flag is never published (-1: none)
     unsigned wait_limit;              // polls before a wavefront wait gives up
+    // in-loop mode: the caller's final decisions and their flags, and the per-macroblock done flags, all in
+    // host memory mapped into the device's address space; results go to host memory too (`results`)
+    const ironav_mbstate* committed;
+    const unsigned* commit_flags;
+    unsigned* done_flags;
+    unsigned long long wait_ns;       // how long an in-loop wait for the caller may take
 };
 
 }  // namespace ironav

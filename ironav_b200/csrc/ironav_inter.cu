@@ -10,6 +10,8 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <atomic>
+#include <chrono>
 #include <vector>
 
 #include "analyse.cuh"
@@ -46,6 +48,15 @@ struct ironav_ctx {
     bool have_params = false;
     int withhold = -1;
     unsigned wait_limit = 1u << 22;
+    // in-loop mode: host memory mapped into the device (allocated on first use)
+    int* d_order_bands = nullptr;         // tickets: rows interleaved across bands, raster within each
+    ironav_mbresult* h_results = nullptr;
+    unsigned* h_done = nullptr;
+    ironav_mbstate* h_committed = nullptr;
+    unsigned* h_commit = nullptr;
+    unsigned inloop_epoch = 0;
+    bool inloop_active = false;
+    unsigned long long inloop_wait_ns = 10ull * 1000 * 1000 * 1000;
 };
 
 namespace {
@@ -77,6 +88,11 @@ void free_ctx(ironav_ctx* c) {
     cudaFree(c->d_states);
     cudaFree(c->d_col_stage);
     cudaFree(c->d_results);
+    cudaFree(c->d_order_bands);
+    cudaFreeHost(c->h_results);
+    cudaFreeHost(c->h_done);
+    cudaFreeHost(c->h_committed);
+    cudaFreeHost(c->h_commit);
     delete c;
 }
 
@@ -133,9 +149,9 @@ int launch_analyse(ironav_ctx* c, bool auto_mode, const ironav_mbstate* d_in, ir
     if (auto_mode) p.epoch = ++c->epoch;
     CK(cudaMemsetAsync(c->d_counters, 0, 2 * sizeof(unsigned), c->stream));
     if (auto_mode)
-        analyse_kernel<true><<<c->k2_blocks, K2_WARPS * 32, 0, c->stream>>>(p);
+        analyse_kernel<MODE_AUTO><<<c->k2_blocks, K2_WARPS * 32, 0, c->stream>>>(p);
     else
-        analyse_kernel<false><<<c->k2_blocks, K2_WARPS * 32, 0, c->stream>>>(p);
+        analyse_kernel<MODE_REPLAY><<<c->k2_blocks, K2_WARPS * 32, 0, c->stream>>>(p);
     return cuda_status(cudaGetLastError());
 }
 
@@ -210,7 +226,7 @@ int ironav_ctx_create(ironav_ctx** out, int width, int height, int bd, int max_r
     if ((e = cudaGetDeviceProperties(&prop, c->device)) != cudaSuccess) return fail(e);
     c->nsm = prop.multiProcessorCount;
     int per_sm = 0;
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, analyse_kernel<true>, K2_WARPS * 32, 0)) != cudaSuccess) return fail(e);
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, analyse_kernel<MODE_AUTO>, K2_WARPS * 32, 0)) != cudaSuccess) return fail(e);
     c->k2_blocks = std::max(1, per_sm) * c->nsm;
     const size_t slack = 256;  // word-granular reads may touch a few bytes past a plane's last sample
     if ((e = cudaMalloc(&c->d_src, (size_t)c->pw * c->ph + slack)) != cudaSuccess) return fail(e);
@@ -239,6 +255,15 @@ int ironav_ctx_create(ironav_ctx** out, int width, int height, int bd, int max_r
     });
     if ((e = cudaMemcpy(c->d_band_start, start.data(), sizeof(int) * mb_h, cudaMemcpyHostToDevice)) != cudaSuccess) return fail(e);
     if ((e = cudaMemcpy(c->d_order, order.data(), sizeof(int) * c->nmb, cudaMemcpyHostToDevice)) != cudaSuccess) return fail(e);
+    // in-loop tickets for one caller thread per band: row r of every band, band after band, then row r + 1
+    std::vector<int> rows_order;
+    rows_order.reserve(c->nmb);
+    for (int r = 0; r < mb_h; r++)
+        for (int i = 0; i < nslices; i++)
+            if (bands[i] + r < bands[i + 1])
+                for (int x = 0; x < mb_w; x++) rows_order.push_back((bands[i] + r) * mb_w + x);
+    if ((e = cudaMalloc(&c->d_order_bands, sizeof(int) * c->nmb)) != cudaSuccess) return fail(e);
+    if ((e = cudaMemcpy(c->d_order_bands, rows_order.data(), sizeof(int) * c->nmb, cudaMemcpyHostToDevice)) != cudaSuccess) return fail(e);
     *out = c;
     return IRONAV_OK;
 }
@@ -396,6 +421,91 @@ int ironav_measure_int32_peak(double* tops) {
     cudaFree(d);
     CK(cudaGetLastError());
     *tops = best;
+    return IRONAV_OK;
+}
+
+// ---- in-loop mode ----------------------------------------------------------------------------------
+
+int ironav_inloop_begin(ironav_ctx* c, int order) {
+    if (!c || !c->have_params || c->nact > c->nrefs || (order != IRONAV_INLOOP_RASTER && order != IRONAV_INLOOP_BANDS))
+        return IRONAV_INVALID_ARGUMENT;
+    if (c->inloop_active) return IRONAV_INVALID_INPUT;
+    if (!c->h_results) {
+        CK(cudaHostAlloc(&c->h_results, sizeof(ironav_mbresult) * c->nmb, cudaHostAllocMapped));
+        CK(cudaHostAlloc(&c->h_done, sizeof(unsigned) * c->nmb, cudaHostAllocMapped));
+        CK(cudaHostAlloc(&c->h_committed, sizeof(ironav_mbstate) * c->nmb, cudaHostAllocMapped));
+        CK(cudaHostAlloc(&c->h_commit, sizeof(unsigned) * c->nmb, cudaHostAllocMapped));
+        memset(c->h_done, 0, sizeof(unsigned) * c->nmb);
+        memset(c->h_commit, 0, sizeof(unsigned) * c->nmb);
+    }
+    AnalyseParams p;
+    memset(&p, 0, sizeof(p));
+    p.src = c->d_src;
+    p.ls = c->pw;
+    for (int i = 0; i < c->nact; i++) p.planes[i] = c->d_planes[c->slot_of[i]];
+    p.psize = c->psize;
+    p.sw = c->sw;
+    p.col = c->d_col[c->slot_of[0]];
+    p.mb_w = c->mb_w;
+    p.mb_h = c->mb_h;
+    p.pw = c->pw;
+    p.ph = c->ph;
+    p.nact = c->nact;
+    p.lambda = c->lambda;
+    p.skip_thresh = c->skip_thresh;
+    p.fast = c->fast;
+    p.sub8 = c->sub8;
+    p.band_start = c->d_band_start;
+    p.order = order == IRONAV_INLOOP_BANDS ? c->d_order_bands : nullptr;
+    p.ticket = c->d_counters;
+    p.err = c->d_counters + 1;
+    p.nmb = c->nmb;
+    p.withhold = -1;
+    p.epoch = ++c->inloop_epoch;
+    p.wait_ns = c->inloop_wait_ns;
+    CK(cudaHostGetDevicePointer((void**)&p.results, c->h_results, 0));
+    CK(cudaHostGetDevicePointer((void**)&p.done_flags, c->h_done, 0));
+    CK(cudaHostGetDevicePointer((void**)&p.committed, c->h_committed, 0));
+    CK(cudaHostGetDevicePointer((void**)&p.commit_flags, c->h_commit, 0));
+    CK(cudaMemsetAsync(c->d_counters, 0, 2 * sizeof(unsigned), c->stream));
+    // few warps: the caller's pace bounds this mode, and every waiting warp polls host memory
+    const int blocks = std::min(c->k2_blocks, 64);
+    analyse_kernel<MODE_INLOOP><<<blocks, K2_WARPS * 32, 0, c->stream>>>(p);
+    CK(cudaGetLastError());
+    c->inloop_active = true;
+    return IRONAV_OK;
+}
+
+int ironav_inloop_result(ironav_ctx* c, int mb, ironav_mbresult* out, int timeout_ms) {
+    if (!c || !out || mb < 0 || mb >= c->nmb || !c->inloop_active) return IRONAV_INVALID_ARGUMENT;
+    const volatile unsigned* flag = c->h_done + mb;
+    const auto t0 = std::chrono::steady_clock::now();
+    for (unsigned i = 0; *flag != c->inloop_epoch; i++) {
+        if ((i & 255) == 255 && std::chrono::steady_clock::now() - t0 > std::chrono::milliseconds(timeout_ms)) return IRONAV_TIMEOUT;
+    }
+    std::atomic_thread_fence(std::memory_order_acquire);
+    memcpy(out, (const void*)(c->h_results + mb), sizeof(ironav_mbresult));
+    return IRONAV_OK;
+}
+
+int ironav_inloop_commit(ironav_ctx* c, int mb, const ironav_mbstate* s) {
+    if (!c || !s || mb < 0 || mb >= c->nmb || !c->inloop_active) return IRONAV_INVALID_ARGUMENT;
+    memcpy((void*)(c->h_committed + mb), s, sizeof(ironav_mbstate));
+    std::atomic_thread_fence(std::memory_order_release);
+    *(volatile unsigned*)(c->h_commit + mb) = c->inloop_epoch;
+    return IRONAV_OK;
+}
+
+int ironav_inloop_end(ironav_ctx* c) {
+    if (!c || !c->inloop_active) return IRONAV_INVALID_ARGUMENT;
+    c->inloop_active = false;
+    return check_device_error(c);
+}
+
+// How long an in-loop wait for the caller's commit may take on the device (milliseconds).
+int ironav_inloop_set_wait(ironav_ctx* c, int ms) {
+    if (!c || ms <= 0) return IRONAV_INVALID_ARGUMENT;
+    c->inloop_wait_ns = (unsigned long long)ms * 1000000ull;
     return IRONAV_OK;
 }
 

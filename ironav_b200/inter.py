@@ -69,7 +69,8 @@ EXPORTS = (
     "ironav_begin_p_picture", "ironav_analyse_picture_replay", "ironav_analyse_picture_auto",
     "ironav_set_source_device", "ironav_push_reference_device",
     "ironav_analyse_picture_replay_device", "ironav_analyse_picture_auto_device", "ironav_ctx_sync",
-    "ironav_analyse_auto_noalloc",
+    "ironav_inloop_begin", "ironav_inloop_result", "ironav_inloop_commit", "ironav_inloop_end",
+    "ironav_inloop_set_wait", "ironav_analyse_auto_noalloc",
 )
 
 
@@ -108,6 +109,11 @@ def _declare(lib: ctypes.CDLL) -> ctypes.CDLL:
     lib.ironav_analyse_picture_replay_device.argtypes = [_VP, _VP, _VP]
     lib.ironav_analyse_picture_auto_device.argtypes = [_VP, _VP, _VP]
     lib.ironav_ctx_sync.argtypes = [_VP]
+    lib.ironav_inloop_begin.argtypes = [_VP, _I]
+    lib.ironav_inloop_result.argtypes = [_VP, _I, _VP, _I]
+    lib.ironav_inloop_commit.argtypes = [_VP, _I, _VP]
+    lib.ironav_inloop_end.argtypes = [_VP]
+    lib.ironav_inloop_set_wait.argtypes = [_VP, _I]
     if hasattr(lib, "ironav_analyse_auto_noalloc"):
         # (d_src, src_stride, d_ref, ref_stride, ref_w, ref_h, d_col, width, height, nslices, qp_prime, lambda,
         #  skip_thresh, fast, sub8, d_planes, d_states, d_results, stream)
@@ -242,6 +248,29 @@ class InterStage:
                     "ironav_analyse_picture_auto")
         return states, out
 
+    # -- in-loop mode: the caller decides each macroblock (the encoder's own loop) ---------------------
+
+    INLOOP_RASTER = 0
+    INLOOP_BANDS = 1
+
+    def inloop_begin(self, order: int = 0) -> None:
+        self._check(self.lib.ironav_inloop_begin(self.ctx, order), "ironav_inloop_begin")
+
+    def inloop_result(self, mb: int, timeout_ms: int = 10000) -> np.ndarray:
+        out = np.zeros(1, dtype=MBRESULT_DTYPE)
+        self._check(self.lib.ironav_inloop_result(self.ctx, mb, _ptr(out), timeout_ms), "ironav_inloop_result")
+        return out[0]
+
+    def inloop_commit(self, mb: int, state: np.ndarray) -> None:
+        st = np.ascontiguousarray(np.asarray(state, dtype=MBSTATE_DTYPE).reshape(1))
+        self._check(self.lib.ironav_inloop_commit(self.ctx, mb, _ptr(st)), "ironav_inloop_commit")
+
+    def inloop_end(self) -> None:
+        self._check(self.lib.ironav_inloop_end(self.ctx), "ironav_inloop_end")
+
+    def inloop_set_wait(self, ms: int) -> None:
+        self._check(self.lib.ironav_inloop_set_wait(self.ctx, ms), "ironav_inloop_set_wait")
+
     # -- device-resident forms (integer device pointers, e.g. torch tensor.data_ptr()) ---------------
 
     def set_stream(self, stream_handle: int) -> None:
@@ -264,6 +293,35 @@ class InterStage:
 
     def sync(self) -> None:
         self._check(self.lib.ironav_ctx_sync(self.ctx), "ironav_ctx_sync")
+
+
+# Sub-partitions of P_8x8 (SUB, enc/frame.rs:204): (x, y, w, h) in 4x4 blocks.
+_SUB = [[(0, 0, 2, 2)], [(0, 0, 2, 1), (0, 1, 2, 1)], [(0, 0, 1, 2), (1, 0, 1, 2)],
+        [(0, 0, 1, 1), (1, 0, 1, 1), (0, 1, 1, 1), (1, 1, 1, 1)]]
+_PARTS = [[(0, 0, 4, 4)], [(0, 0, 4, 2), (0, 2, 4, 2)], [(0, 0, 2, 4), (2, 0, 2, 4)],
+          [(0, 0, 2, 2), (2, 0, 2, 2), (0, 2, 2, 2), (2, 2, 2, 2)]]
+
+
+def decision_state(res, skip: bool) -> np.ndarray:
+    """The MbState a P macroblock leaves once decided (finish_mb, enc/frame.rs:2281-2321): P_Skip with
+    the skip vector, or the best_inter partitioning's vectors painted over its 4x4 blocks."""
+    st = np.zeros(1, dtype=MBSTATE_DTYPE)[0]
+    st["inter"] = 1
+    if skip:
+        st["mvs"][:] = res["skip_mv"]
+        st["refs"][:] = 0
+        return st
+    part = int(res["part"])
+    if part == 3:
+        rects = [((k & 1) * 2 + x, (k >> 1) * 2 + y, w, h) for k in range(4) for (x, y, w, h) in _SUB[int(res["sub"][k])]]
+    else:
+        rects = _PARTS[part]
+    for n, (x, y, w, h) in enumerate(rects):
+        for by in range(y, y + h):
+            for bx in range(x, x + w):
+                st["mvs"][by * 4 + bx] = res["mvs"][n]
+    st["refs"][:] = res["refs"]
+    return st
 
 
 def default_bands(mb_h: int, nslices: int) -> list[int]:

@@ -313,6 +313,7 @@ struct ironav_ctx {
     /* picture parameters */
     int qpp, lambda, skip_thresh, nact, fast, sub8;
     int threads;
+    void* inloop; /* in-loop mode state */
 };
 
 typedef struct fc {
@@ -827,6 +828,8 @@ int ironav_ctx_destroy(ironav_ctx* c) {
     free(c->refs);
     free(c->src);
     free(c->band_start);
+    if (c->inloop) free(((ironav_mbstate**)c->inloop)[0]);
+    free(c->inloop);
     free(c);
     return IRONAV_OK;
 }
@@ -1007,3 +1010,41 @@ int ironav_analyse_auto_noalloc(const uint8_t* d_src, int src_stride, const uint
                                 ironav_mbresult* d_results, void* stream) {
     return IRONAV_HARDWARE_UNAVAILABLE;
 }
+
+/* In-loop mode on the CPU: a macroblock is analysed when its result is asked for, against the decisions
+ * committed so far (the caller's order guarantees its neighbours are among them). */
+typedef struct inloop_state { ironav_mbstate* committed; int active; } inloop_state;
+static inloop_state* inloop_of(ironav_ctx* c) { return (inloop_state*)c->inloop; }
+
+int ironav_inloop_begin(ironav_ctx* c, int order) {
+    if (!c || c->nact < 1 || (order != IRONAV_INLOOP_RASTER && order != IRONAV_INLOOP_BANDS)) return IRONAV_INVALID_ARGUMENT;
+    if (!c->inloop) c->inloop = calloc(1, sizeof(inloop_state));
+    inloop_state* s = inloop_of(c);
+    if (s->active) return IRONAV_INVALID_INPUT;
+    free(s->committed);
+    s->committed = (ironav_mbstate*)calloc((size_t)c->mb_w * c->mb_h, sizeof(ironav_mbstate));
+    s->active = 1;
+    return IRONAV_OK;
+}
+
+int ironav_inloop_result(ironav_ctx* c, int mb, ironav_mbresult* out, int timeout_ms) {
+    (void)timeout_ms;
+    if (!c || !out || !c->inloop || !inloop_of(c)->active || mb < 0 || mb >= c->mb_w * c->mb_h) return IRONAV_INVALID_ARGUMENT;
+    fc f = {c, inloop_of(c)->committed};
+    analyse_mb(&f, mb % c->mb_w, mb / c->mb_w, 0, out, NULL);
+    return IRONAV_OK;
+}
+
+int ironav_inloop_commit(ironav_ctx* c, int mb, const ironav_mbstate* st) {
+    if (!c || !st || !c->inloop || !inloop_of(c)->active || mb < 0 || mb >= c->mb_w * c->mb_h) return IRONAV_INVALID_ARGUMENT;
+    inloop_of(c)->committed[mb] = *st;
+    return IRONAV_OK;
+}
+
+int ironav_inloop_end(ironav_ctx* c) {
+    if (!c || !c->inloop || !inloop_of(c)->active) return IRONAV_INVALID_ARGUMENT;
+    inloop_of(c)->active = 0;
+    return IRONAV_OK;
+}
+
+int ironav_inloop_set_wait(ironav_ctx* c, int ms) { return (c && ms > 0) ? IRONAV_OK : IRONAV_INVALID_ARGUMENT; }
