@@ -111,7 +111,7 @@ __device__ __forceinline__ int satd4_packed(const uint32_t s[4], const uint32_t 
 
 // Fills the table of blocks around the macroblock: left column (x = -1), top row (y = -1), top-right
 // (4, -1), top-left (-1, -1); (4, y >= 0) is never available; inside slots are unused.
-static __device__ void load_neighbours(const AnalyseParams& P, WarpSmem& S, const ironav_mbstate* states) {
+static __device__ void load_neighbours(const AnalyseParams& __restrict__ P, WarpSmem& __restrict__ S, const ironav_mbstate* states) {
     const int lane = threadIdx.x & 31;
     if (lane < 30) {
         const int ex = lane % 6 - 1, ey = lane / 6 - 1;
@@ -139,13 +139,13 @@ static __device__ void load_neighbours(const AnalyseParams& P, WarpSmem& S, cons
 
 // nb_motion for the block at (x, y) relative to the macroblock; inside it, `cur` holds the decided
 // blocks (nullptr: none decided).
-static __device__ __forceinline__ Blk nb(const AnalyseParams& P, WarpSmem& S, const Blk* cur, int x, int y) {
+static __device__ __forceinline__ Blk nb(const AnalyseParams& __restrict__ P, WarpSmem& __restrict__ S, const Blk* cur, int x, int y) {
     if (x >= 0 && x < 4 && y >= 0) return cur ? cur[y * 4 + x] : make_int4(0, 0, -1, 0);
     return S.ext[(y + 1) * 6 + (x + 1)];
 }
 
 // pred_mv, enc/frame.rs:543-570
-static __device__ __noinline__ int2 pred_mv(const AnalyseParams& P, WarpSmem& S, const Blk* cur, int bx, int by, int w, int dir, int rf) {
+static __device__ __noinline__ int2 pred_mv(const AnalyseParams& __restrict__ P, WarpSmem& __restrict__ S, const Blk* cur, int bx, int by, int w, int dir, int rf) {
     const Blk a = nb(P, S, cur, bx - 1, by), b = nb(P, S, cur, bx, by - 1);
     Blk c = nb(P, S, cur, bx + w, by - 1);
     if (!c.w) c = nb(P, S, cur, bx - 1, by - 1);
@@ -164,7 +164,7 @@ static __device__ __noinline__ int2 pred_mv(const AnalyseParams& P, WarpSmem& S,
 }
 
 // skip_mv, enc/frame.rs:597-603
-static __device__ int2 skip_mv(const AnalyseParams& P, WarpSmem& S) {
+static __device__ int2 skip_mv(const AnalyseParams& __restrict__ P, WarpSmem& __restrict__ S) {
     const Blk a = nb(P, S, nullptr, -1, 0), b = nb(P, S, nullptr, 0, -1);
     if (!a.w || !b.w || (a.z == 0 && a.x == 0 && a.y == 0) || (b.z == 0 && b.x == 0 && b.y == 0)) return make_int2(0, 0);
     return pred_mv(P, S, nullptr, 0, 0, 4, 0, 0);
@@ -172,23 +172,23 @@ static __device__ int2 skip_mv(const AnalyseParams& P, WarpSmem& S) {
 
 // ---- scoring -------------------------------------------------------------------------------------
 
-// Integer SAD (sad_int, enc/frame.rs:662-671) of the w x h partition at 4x4 block (bx, by) at this
-// lane's candidate (px, py) of reference r; the lanes of a group (same lane & 7) share a candidate and
-// split its rows. Returns the group's sum in every lane of the group.
-static __device__ __forceinline__ int sad_lane(const AnalyseParams& P, WarpSmem& S, int r, int bx, int by, int w, int h, int px, int py, bool valid) {
+// Integer SAD (sad_int, enc/frame.rs:662-671) of the partition at this lane's candidate (px, py): g0 is the
+// reference plane G at the partition's origin, src the partition's first source word, w x h its size.
+// The lanes of a group (same lane & 7) share a candidate and split its rows; every lane of the group gets
+// the sum.
+static __device__ __forceinline__ int sad_lane(const uint8_t* __restrict__ g0, const uint32_t* __restrict__ src, int sw, int w,
+                                               int h, int px, int py, bool valid) {
     const int lane = threadIdx.x & 31;
     int sad = 0;
     if (valid) {
-        const int x0 = S.mbx * 16 + bx * 4, y0 = S.mby * 16 + by * 4;
         const int row0 = lane >> 3;
-        const uint8_t* G = P.planes[r] + (unsigned)((y0 + (py >> 2) + PAD + row0) * P.sw + (x0 + (px >> 2) + PAD));
-        const uint32_t* s = &S.src[by * 16 + bx];
-        const int step4 = 4 * P.sw;
+        const uint8_t* G = g0 + ((py >> 2) + row0) * sw + (px >> 2);
+        const int step4 = 4 * sw;
         for (int row = row0; row < h; row += 4, G += step4) {
             const uintptr_t a = reinterpret_cast<uintptr_t>(G);
             const uint32_t* q = reinterpret_cast<const uint32_t*>(a & ~uintptr_t(3));
             const unsigned sh = (unsigned)(a & 3) * 8u;
-            const uint32_t* sr = s + row * 4;
+            const uint32_t* sr = src + row * 4;
             const uint32_t w0 = __ldg(q), w1 = __ldg(q + 1);
             sad += __vsadu4(sr[0], __funnelshift_r(w0, w1, sh));
             if (w >= 8) {
@@ -209,7 +209,7 @@ static __device__ __forceinline__ int sad_lane(const AnalyseParams& P, WarpSmem&
 // Quarter-sample prediction (HalfPel::predict, enc/subpel.rs:122-145) of the partition at 4x4 block
 // (bx, by), (4 << lgw) x (4 << lgh) samples, scored by SATD (satd, enc/frame.rs:641-659), or by SAD
 // when `sad` (the P_Skip test), for the n vectors S.cand[0..n); the sums land in S.cost[0..n).
-static __device__ __noinline__ void pred_batch(const AnalyseParams& P, WarpSmem& S, int r, int bx, int by, int lgw, int lgh, int n, bool sad) {
+static __device__ __noinline__ void pred_batch(const AnalyseParams& __restrict__ P, WarpSmem& __restrict__ S, int r, int bx, int by, int lgw, int lgh, int n, bool sad) {
     const int lane = threadIdx.x & 31;
     const int lg = lgw + lgh, total = n << lg, w = 4 << lgw, h = 4 << lgh;
     if (lane < n) S.cost[lane] = 0;
@@ -260,7 +260,7 @@ static __device__ __noinline__ void pred_batch(const AnalyseParams& P, WarpSmem&
 // One diamond round whose moves were bent by the search clamps: the reference's four moves replayed
 // against the scored 3x3 square (S.cost[0..9), centre at 4), scoring on demand the points it lacks.
 // Returns whether the best moved.
-static __device__ __noinline__ int4 round_clamped(const AnalyseParams& P, WarpSmem& S, int r, int bx, int by, int w, int h, int mvpx, int mvpy, int step, int cxlo,
+static __device__ __noinline__ int4 round_clamped(const AnalyseParams& __restrict__ P, WarpSmem& __restrict__ S, int r, int bx, int by, int w, int h, int mvpx, int mvpy, int step, int cxlo,
                                            int cxhi, int cylo, int cyhi, int bxv, int byv, int bc) {
     const int lane = threadIdx.x & 31;
     const int cx = bxv, cy = byv;
@@ -279,7 +279,8 @@ static __device__ __noinline__ int4 round_clamped(const AnalyseParams& P, WarpSm
         if (ix >= 0 && iy >= 0) {
             v = S.cost[iy * 3 + ix];
         } else {
-            const int s1 = sad_lane(P, S, r, bx, by, w, h, nx, ny, (lane & 7) == 0);
+            const uint8_t* g0 = P.planes[r] + (S.mby * 16 + by * 4 + PAD) * P.sw + S.mbx * 16 + bx * 4 + PAD;
+            const int s1 = sad_lane(g0, &S.src[by * 16 + bx], P.sw, w, h, nx, ny, (lane & 7) == 0);
             v = __shfl_sync(FULL, s1, 0) + P.lambda * mvd_bits_d(nx, ny, mvpx, mvpy);
         }
         if (v < bc) {
@@ -294,7 +295,7 @@ static __device__ __noinline__ int4 round_clamped(const AnalyseParams& P, WarpSm
 
 // Returns the best vector in (ox, oy) and its cost without the vector's bits. (e0x, e0y) and
 // (e1x, e1y) are the extra candidates (nextra of them).
-static __device__ __noinline__ int4 motion_search(const AnalyseParams& P, WarpSmem& S, int r, int bx, int by, int w4, int h4, int mvpx, int mvpy, int e0x, int e0y,
+static __device__ __noinline__ int4 motion_search(const AnalyseParams& __restrict__ P, WarpSmem& __restrict__ S, int r, int bx, int by, int w4, int h4, int mvpx, int mvpy, int e0x, int e0y,
                                           int e1x, int e1y, int nextra) {
     const int lane = threadIdx.x & 31;
     const int lam = P.lambda;
@@ -327,7 +328,10 @@ static __device__ __noinline__ int4 motion_search(const AnalyseParams& P, WarpSm
     } else if (g == 7) {
         valid = false;
     }
-    int cost = sad_lane(P, S, r, bx, by, w, h, px, py, valid);
+    const int sw = P.sw;
+    const uint8_t* const g0 = P.planes[r] + (y0 + PAD) * sw + x0 + PAD;
+    const uint32_t* const src0 = &S.src[by * 16 + bx];
+    int cost = sad_lane(g0, src0, sw, w, h, px, py, valid);
     cost = valid ? cost + lam * mvd_bits_d(px, py, mvpx, mvpy) : BIG;
     const unsigned vmask = __ballot_sync(FULL, valid) & 0xffu;
     if (lane == 0) S.sad_px += (uint32_t)(__popc(vmask) * w * h);
@@ -340,16 +344,17 @@ static __device__ __noinline__ int4 motion_search(const AnalyseParams& P, WarpSm
     int bxv = __shfl_sync(FULL, px, win), byv = __shfl_sync(FULL, py, win);
     // the diamond (973-988): each round scores the 3x3 square of its step around the centre in one
     // batch (group g -> square position k = g < 4 ? g : g + 1), then replays the four moves in order
-    const int nsteps = P.fast ? 2 : 3;
+    const bool fast = P.fast != 0;
+    const int nsteps = fast ? 2 : 3;
     const int k = g < 4 ? g : g + 1, kx = k % 3, ky = k / 3;
     for (int si = 0; si < nsteps; si++) {
-        const int step = P.fast ? (si == 0 ? 8 : 4) : (16 >> si);
+        const int step = fast ? (si == 0 ? 8 : 4) : (16 >> si);
         const int iters = step == 4 ? 32 : 4;
         for (int it = 0; it < iters; it++) {
             const int cx = bxv, cy = byv, c0 = bc;
             const int X0 = clx(cx - step), X2 = clx(cx + step), Y0 = cly(cy - step), Y2 = cly(cy + step);
             const int qx = kx == 0 ? X0 : (kx == 1 ? cx : X2), qy = ky == 0 ? Y0 : (ky == 1 ? cy : Y2);
-            const int sc = sad_lane(P, S, r, bx, by, w, h, qx, qy, true) + lam * mvd_bits_d(qx, qy, mvpx, mvpy);
+            const int sc = sad_lane(g0, src0, sw, w, h, qx, qy, true) + lam * mvd_bits_d(qx, qy, mvpx, mvpy);
             if (lane == 0) S.sad_px += (uint32_t)(4 * w * h);
             bool moved;
             if (X0 == cx - step && X2 == cx + step && Y0 == cy - step && Y2 == cy + step) {
@@ -447,18 +452,18 @@ static __device__ __noinline__ int4 motion_search(const AnalyseParams& P, WarpSm
 
 // ---- partition decision ----------------------------------------------------------------------------
 
-static __device__ __forceinline__ void blk_clear(const AnalyseParams& P, WarpSmem& S, Blk* b) {
+static __device__ __forceinline__ void blk_clear(const AnalyseParams& __restrict__ P, WarpSmem& __restrict__ S, Blk* b) {
     const int lane = threadIdx.x & 31;
     if (lane < 16) b[lane] = make_int4(0, 0, -1, 0);
     __syncwarp();
 }
-static __device__ __forceinline__ void blk_copy(const AnalyseParams& P, WarpSmem& S, Blk* d, const Blk* s) {
+static __device__ __forceinline__ void blk_copy(const AnalyseParams& __restrict__ P, WarpSmem& __restrict__ S, Blk* d, const Blk* s) {
     const int lane = threadIdx.x & 31;
     if (lane < 16) d[lane] = s[lane];
     __syncwarp();
 }
 // Marks rectangle (x, y, w, h) of `b` as decided with vector (mx, my) and reference rf.
-static __device__ __forceinline__ void blk_paint(const AnalyseParams& P, WarpSmem& S, Blk* b, int x, int y, int w, int h, int mx, int my, int rf) {
+static __device__ __forceinline__ void blk_paint(const AnalyseParams& __restrict__ P, WarpSmem& __restrict__ S, Blk* b, int x, int y, int w, int h, int mx, int my, int rf) {
     const int lane = threadIdx.x & 31;
     if (lane < 16) {
         const int bx = lane & 3, by = lane >> 2;
@@ -469,7 +474,7 @@ static __device__ __forceinline__ void blk_paint(const AnalyseParams& P, WarpSme
 
 // sub_search, enc/frame.rs:911-938: returns sub_mb_type, its cost in cost_out; leaves the 8x8
 // block's vectors in S.st.
-static __device__ __noinline__ int2 sub_search(const AnalyseParams& P, WarpSmem& S, int r, int k, int ex, int ey) {
+static __device__ __noinline__ int2 sub_search(const AnalyseParams& __restrict__ P, WarpSmem& __restrict__ S, int r, int k, int ex, int ey) {
     const int lam = P.lambda;
     const int ox = (k & 1) * 2, oy = (k >> 1) * 2;
     const int ns = P.sub8 ? 4 : 1;
@@ -496,7 +501,7 @@ static __device__ __noinline__ int2 sub_search(const AnalyseParams& P, WarpSmem&
 }
 
 // best_inter_ref, enc/frame.rs:852-905. Leaves the winner's vectors in S.best_mvs.
-static __device__ __noinline__ int4 best_inter_ref(const AnalyseParams& P, WarpSmem& S, int r) {
+static __device__ __noinline__ int4 best_inter_ref(const AnalyseParams& __restrict__ P, WarpSmem& __restrict__ S, int r) {
     const int lane = threadIdx.x & 31;
     const int lam = P.lambda;
     int rb = 0;
@@ -587,7 +592,7 @@ static __device__ __noinline__ int4 best_inter_ref(const AnalyseParams& P, WarpS
 
 // ---- one macroblock --------------------------------------------------------------------------------
 
-static __device__ void analyse(const AnalyseParams& P, WarpSmem& S, bool auto_policy) {
+static __device__ void analyse(const AnalyseParams& __restrict__ P, WarpSmem& __restrict__ S, bool auto_policy) {
     const int lane = threadIdx.x & 31;
     // the current macroblock: 16 rows of 16 bytes, as 128-bit loads
     if (lane < 16) {
@@ -748,7 +753,7 @@ static __device__ bool wait_committed(const AnalyseParams& P, int m) {
 
 // The neighbours of an in-loop macroblock from the caller's committed decisions (host memory: read
 // around the caches, after the acquire of their flags).
-static __device__ void load_committed(const AnalyseParams& P, WarpSmem& S) {
+static __device__ void load_committed(const AnalyseParams& __restrict__ P, WarpSmem& __restrict__ S) {
     const int lane = threadIdx.x & 31;
     if (lane < 30) {
         const int ex = lane % 6 - 1, ey = lane / 6 - 1;

@@ -109,11 +109,12 @@ def _declare(lib: ctypes.CDLL) -> ctypes.CDLL:
     lib.ironav_analyse_picture_replay_device.argtypes = [_VP, _VP, _VP]
     lib.ironav_analyse_picture_auto_device.argtypes = [_VP, _VP, _VP]
     lib.ironav_ctx_sync.argtypes = [_VP]
-    lib.ironav_inloop_begin.argtypes = [_VP, _I]
-    lib.ironav_inloop_result.argtypes = [_VP, _I, _VP, _I]
-    lib.ironav_inloop_commit.argtypes = [_VP, _I, _VP]
-    lib.ironav_inloop_end.argtypes = [_VP]
-    lib.ironav_inloop_set_wait.argtypes = [_VP, _I]
+    if hasattr(lib, "ironav_inloop_begin"):
+        lib.ironav_inloop_begin.argtypes = [_VP, _I]
+        lib.ironav_inloop_result.argtypes = [_VP, _I, _VP, _I]
+        lib.ironav_inloop_commit.argtypes = [_VP, _I, _VP]
+        lib.ironav_inloop_end.argtypes = [_VP]
+        lib.ironav_inloop_set_wait.argtypes = [_VP, _I]
     if hasattr(lib, "ironav_analyse_auto_noalloc"):
         # (d_src, src_stride, d_ref, ref_stride, ref_w, ref_h, d_col, width, height, nslices, qp_prime, lambda,
         #  skip_thresh, fast, sub8, d_planes, d_states, d_results, stream)
