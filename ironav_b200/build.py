@@ -60,8 +60,8 @@ def build_cuda(force: bool = False, verbose: bool = False) -> str:
     deps = _sources((".cu", ".cuh"))
     if force or _stale(CUDA_LIB, deps):
         os.makedirs(LIB, exist_ok=True)
-        cmd = [_nvcc(), *NVCC_FLAGS, os.path.join(CSRC, "ironav_inter.cu"), os.path.join(CSRC, "ironav_noalloc.cu"),
-               "-o", CUDA_LIB]
+        units = ["ironav_inter.cu", "ironav_batch.cu", "ironav_noalloc.cu"]
+        cmd = [_nvcc(), *NVCC_FLAGS, *[os.path.join(CSRC, u) for u in units], "-o", CUDA_LIB]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
         subprocess.run(cmd, check=True)

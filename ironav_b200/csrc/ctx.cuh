@@ -1,0 +1,50 @@
+// ctx.cuh — the state of one stream's context (ironav_ctx), shared by the translation units of the library.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+using ironav::ColMv;
+using ironav::MAX_REFS;
+
+// One stream: device buffers, the reference ring, picture parameters and the wavefront scratch.
+struct ironav_ctx {
+    int width = 0, height = 0, bd = 8, mb_w = 0, mb_h = 0, pw = 0, ph = 0, sw = 0, sh = 0;
+    int max_refs = 0, nslices = 0, nmb = 0;
+    int device = 0, nsm = 0, k2_blocks = 0;
+    cudaStream_t stream = nullptr;
+    long long psize = 0;
+    uint8_t* d_src = nullptr;
+    uint8_t* d_stage = nullptr;  // reference luma as given, rows pw apart
+    uint8_t* d_planes[MAX_REFS] = {};
+    ColMv* d_col[MAX_REFS] = {};
+    int slot_of[MAX_REFS] = {};  // reference index (0 = newest) -> slot
+    int nrefs = 0;
+    int* d_band_start = nullptr;
+    int* d_order = nullptr;
+    unsigned* d_flags = nullptr;
+    unsigned* d_counters = nullptr;  // [0] ticket, [1] error
+    unsigned epoch = 0;
+    ironav_mbstate* d_states = nullptr;
+    ironav_mbstate* d_col_stage = nullptr;
+    ironav_mbresult* d_results = nullptr;
+    // picture parameters
+    int qpp = 0, lambda = 0, skip_thresh = 0, nact = 0, fast = 0, sub8 = 0;
+    bool have_params = false;
+    int withhold = -1;
+    unsigned wait_limit = 1u << 22;
+    // in-loop mode: host memory mapped into the device (allocated on first use)
+    int* d_order_bands = nullptr;         // tickets: rows interleaved across bands, raster within each
+    ironav_mbresult* h_results = nullptr;
+    unsigned* h_done = nullptr;
+    ironav_mbstate* h_committed = nullptr;
+    unsigned* h_commit = nullptr;
+    unsigned inloop_epoch = 0;
+    bool inloop_active = false;
+    unsigned long long inloop_wait_ns = 10ull * 1000 * 1000 * 1000;
+};
+
+
+// Helpers the translation units share (ironav_inter.cu).
+int take_ref_slot(ironav_ctx* c);
+void fill_params(const ironav_ctx* c, ironav::AnalyseParams& p);

@@ -1,0 +1,304 @@
+// ironav_batch.cu — the batched form: many streams (contexts) analysed with one launch per stage and
+// frame step. The sources of every stream are copied and padded by one kernel, the new references'
+// half-sample planes and co-located vectors are built by one kernel each, and one persistent launch runs
+// every stream's macroblock wavefronts (auto mode) together: tickets follow the streams' merged
+// wavefront order, so a waiting warp only waits on warps holding smaller tickets of its own stream.
+// With many streams in flight the wavefronts fill the GPU, which one stream's wavefront cannot.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <tuple>
+#include <vector>
+
+#include "analyse.cuh"
+#include "ctx.cuh"
+#include "planes.cuh"
+
+using namespace ironav;
+
+namespace {
+
+// One stream's new reference picture: its luma, its planes' slot and its co-located vectors.
+struct PlaneJob {
+    const uint8_t* luma;
+    int stride, w, h;
+    uint8_t* out;
+    long long psize;
+    int sw, sh, tiles_x, tile0;  // tile0: the job's first tile in the launch
+    const ironav_mbstate* col_states;
+    ColMv* col;
+    int nmb, mb0;  // mb0: the job's first macroblock in the launch
+};
+
+// One stream's new source picture, copied into its context and padded to whole macroblocks.
+struct SrcJob {
+    const uint8_t* src;
+    int stride, w, h;
+    uint8_t* dst;
+    int pw, ph, row0;  // row0: the job's first row in the launch
+};
+
+template <typename Job, typename Key>
+__device__ __forceinline__ int find_job(const Job* jobs, int n, int idx, Key key) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (key(jobs[mid]) <= idx) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(K1_THREADS) planes_batch_kernel(const PlaneJob* __restrict__ jobs, int njobs) {
+    const int j = find_job(jobs, njobs, (int)blockIdx.x, [](const PlaneJob& p) { return p.tile0; });
+    const PlaneJob& J = jobs[j];
+    const int t = (int)blockIdx.x - J.tile0;
+    planes_tile(J.luma, J.stride, J.w, J.h, J.out, J.psize, J.sw, J.sh, (t % J.tiles_x) * K1_TW, (t / J.tiles_x) * K1_TH);
+}
+
+// col_mv, enc/frame.rs:944-947, for every stream's new reference
+__global__ void col_batch_kernel(const PlaneJob* __restrict__ jobs, int njobs, int total) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    const int j = find_job(jobs, njobs, i, [](const PlaneJob& p) { return p.mb0; });
+    const PlaneJob& J = jobs[j];
+    const int m = i - J.mb0;
+    ColMv c;
+    c.mv[0] = c.mv[1] = 0;
+    c.valid = 0;
+    if (J.col_states && J.col_states[m].inter) {
+        c.mv[0] = J.col_states[m].mvs[5][0];
+        c.mv[1] = J.col_states[m].mvs[5][1];
+        c.valid = 1;
+    }
+    J.col[m] = c;
+}
+
+// H264Encoder::source (enc/mod.rs:502-519) for every stream: one block per padded row.
+__global__ void source_batch_kernel(const SrcJob* __restrict__ jobs, int njobs) {
+    const int j = find_job(jobs, njobs, (int)blockIdx.x, [](const SrcJob& p) { return p.row0; });
+    const SrcJob& J = jobs[j];
+    const int y = (int)blockIdx.x - J.row0;
+    const uint8_t* row = J.src + (size_t)min(y, J.h - 1) * J.stride;
+    uint8_t* out = J.dst + (size_t)y * J.pw;
+    for (int x = threadIdx.x; x < J.pw; x += blockDim.x) out[x] = row[min(x, J.w - 1)];
+}
+
+// Every stream's auto-mode analysis in one launch (each stream's parameters in the table).
+__global__ void __launch_bounds__(K2_WARPS * 32, K2_MIN_BLOCKS) analyse_batch_kernel(const AnalyseParams* __restrict__ table,
+                                                                                     const uint32_t* __restrict__ order,
+                                                                                     unsigned ntickets, unsigned* ticket,
+                                                                                     const unsigned* err) {
+    __shared__ WarpSmem smem[K2_WARPS];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    WarpSmem& S = smem[wid];
+    for (;;) {
+        unsigned t = 0;
+        if (lane == 0) t = atomicAdd(ticket, 1u);
+        t = __shfl_sync(FULL, t, 0);
+        if (t >= ntickets || ld_acquire(err) != 0) break;
+        const uint32_t e = order[t];
+        const AnalyseParams& P = table[e >> 20];
+        const int mb = (int)(e & 0xFFFFFu), mbx = mb % P.mb_w, mby = mb / P.mb_w;
+        if (lane == 0) {
+            S.mb = mb;
+            S.mbx = mbx;
+            S.mby = mby;
+        }
+        __syncwarp();
+        const int start = P.band_start[mby];
+        bool ok = true;
+        if (mbx > 0) ok = wait_published(P, mb - 1);
+        if (ok && mby > start) ok = wait_published(P, (mbx + 1 < P.mb_w) ? mb - P.mb_w + 1 : mb - P.mb_w);
+        ok = __all_sync(FULL, ok);
+        if (!ok) break;
+        load_neighbours(P, S, P.states_out);
+        analyse(P, S, true);
+        __threadfence();
+        __syncwarp();
+        if (lane == 0) st_release(&P.flags[mb], P.epoch);
+    }
+}
+
+int cuda_status(cudaError_t e) {
+    if (e == cudaSuccess) return IRONAV_OK;
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver || e == cudaErrorNoKernelImageForDevice)
+        return IRONAV_HARDWARE_UNAVAILABLE;
+    return IRONAV_INTERNAL;
+}
+
+#define CK(x)                                           \
+    do {                                                \
+        cudaError_t e_ = (x);                           \
+        if (e_ != cudaSuccess) return cuda_status(e_); \
+    } while (0)
+
+}  // namespace
+
+struct ironav_batch {
+    std::vector<ironav_ctx*> ctx;
+    cudaStream_t stream = nullptr;
+    int n = 0, total_mbs = 0, total_tiles = 0, total_rows = 0, k2_blocks = 0;
+    std::vector<int> mb0;  // each stream's first flag
+    uint32_t* d_order = nullptr;
+    unsigned* d_flags = nullptr;
+    unsigned* d_counters = nullptr;  // [0] ticket, [1] error
+    PlaneJob* d_pjobs = nullptr;
+    SrcJob* d_sjobs = nullptr;
+    AnalyseParams* d_table = nullptr;
+    // pinned staging of the per-step tables, reused once the previous step's copies are done
+    PlaneJob* h_pjobs = nullptr;
+    SrcJob* h_sjobs = nullptr;
+    AnalyseParams* h_table = nullptr;
+    cudaEvent_t copied = nullptr;
+    bool pending = false;
+};
+
+static void free_batch(ironav_batch* b) {
+    cudaFree(b->d_order);
+    cudaFree(b->d_flags);
+    cudaFree(b->d_counters);
+    cudaFree(b->d_pjobs);
+    cudaFree(b->d_sjobs);
+    cudaFree(b->d_table);
+    cudaFreeHost(b->h_pjobs);
+    cudaFreeHost(b->h_sjobs);
+    cudaFreeHost(b->h_table);
+    if (b->copied) cudaEventDestroy(b->copied);
+    delete b;
+}
+
+extern "C" int ironav_batch_create(ironav_batch** out, ironav_ctx* const* ctxs, int n) {
+    if (!out || !ctxs || n < 1 || n > 4096) return IRONAV_INVALID_ARGUMENT;
+    *out = nullptr;
+    for (int i = 0; i < n; i++)
+        if (!ctxs[i] || ctxs[i]->stream != ctxs[0]->stream || ctxs[i]->nmb > (1 << 20)) return IRONAV_INVALID_ARGUMENT;
+    ironav_batch* b = new ironav_batch();
+    b->ctx.assign(ctxs, ctxs + n);
+    b->n = n;
+    b->stream = ctxs[0]->stream;
+    // the streams' wavefronts merged: key x + 2 * (y - band start), then stream, then raster
+    std::vector<std::tuple<int, int, int>> keys;
+    for (int i = 0; i < n; i++) {
+        const ironav_ctx* c = ctxs[i];
+        std::vector<int> start(c->mb_h);
+        cudaMemcpy(start.data(), c->d_band_start, sizeof(int) * c->mb_h, cudaMemcpyDeviceToHost);
+        b->mb0.push_back(b->total_mbs);
+        for (int m = 0; m < c->nmb; m++) {
+            const int x = m % c->mb_w, y = m / c->mb_w;
+            keys.emplace_back(x + 2 * (y - start[y]), i, m);
+        }
+        b->total_mbs += c->nmb;
+        b->total_tiles += ((c->sw + K1_TW - 1) / K1_TW) * ((c->sh + K1_TH - 1) / K1_TH);
+        b->total_rows += c->ph;
+    }
+    std::sort(keys.begin(), keys.end());
+    std::vector<uint32_t> order(keys.size());
+    for (size_t k = 0; k < keys.size(); k++) order[k] = ((uint32_t)std::get<1>(keys[k]) << 20) | (uint32_t)std::get<2>(keys[k]);
+    auto fail = [&](cudaError_t e) {
+        const int s = cuda_status(e);
+        free_batch(b);
+        return s;
+    };
+    cudaError_t e;
+    if ((e = cudaMalloc(&b->d_order, sizeof(uint32_t) * order.size())) != cudaSuccess) return fail(e);
+    if ((e = cudaMemcpy(b->d_order, order.data(), sizeof(uint32_t) * order.size(), cudaMemcpyHostToDevice)) != cudaSuccess) return fail(e);
+    if ((e = cudaMalloc(&b->d_flags, sizeof(unsigned) * b->total_mbs)) != cudaSuccess) return fail(e);
+    if ((e = cudaMalloc(&b->d_counters, sizeof(unsigned) * 2)) != cudaSuccess) return fail(e);
+    if ((e = cudaMalloc(&b->d_pjobs, sizeof(PlaneJob) * n)) != cudaSuccess) return fail(e);
+    if ((e = cudaMalloc(&b->d_sjobs, sizeof(SrcJob) * n)) != cudaSuccess) return fail(e);
+    if ((e = cudaMalloc(&b->d_table, sizeof(AnalyseParams) * n)) != cudaSuccess) return fail(e);
+    if ((e = cudaHostAlloc(&b->h_pjobs, sizeof(PlaneJob) * n, cudaHostAllocDefault)) != cudaSuccess) return fail(e);
+    if ((e = cudaHostAlloc(&b->h_sjobs, sizeof(SrcJob) * n, cudaHostAllocDefault)) != cudaSuccess) return fail(e);
+    if ((e = cudaHostAlloc(&b->h_table, sizeof(AnalyseParams) * n, cudaHostAllocDefault)) != cudaSuccess) return fail(e);
+    if ((e = cudaEventCreateWithFlags(&b->copied, cudaEventDisableTiming)) != cudaSuccess) return fail(e);
+    int per_sm = 0;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, analyse_batch_kernel, K2_WARPS * 32, 0)) != cudaSuccess) return fail(e);
+    b->k2_blocks = std::max(1, per_sm) * ctxs[0]->nsm;
+    *out = b;
+    return IRONAV_OK;
+}
+
+extern "C" int ironav_batch_destroy(ironav_batch* b) {
+    if (!b) return IRONAV_INVALID_ARGUMENT;
+    cudaStreamSynchronize(b->stream);
+    free_batch(b);
+    return IRONAV_OK;
+}
+
+extern "C" int ironav_batch_step(ironav_batch* b, const uint8_t* const* d_src, const uint8_t* const* d_ref,
+                                 const ironav_mbstate* const* d_col, ironav_mbstate* const* d_states,
+                                 ironav_mbresult* const* d_results) {
+    if (!b || !d_src || !d_ref || !d_states || !d_results) return IRONAV_INVALID_ARGUMENT;
+    for (int i = 0; i < b->n; i++) {
+        const ironav_ctx* c = b->ctx[i];
+        // the step pushes one reference: afterwards min(nrefs + 1, max_refs) are held
+        if (!d_src[i] || !d_ref[i] || !d_states[i] || !d_results[i] || !c->have_params || c->nact > std::min(c->nrefs + 1, c->max_refs))
+            return IRONAV_INVALID_ARGUMENT;
+    }
+    // the staging tables are reused: the previous step's copies must have left them
+    if (b->pending) CK(cudaEventSynchronize(b->copied));
+    int tile = 0, row = 0;
+    for (int i = 0; i < b->n; i++) {
+        ironav_ctx* c = b->ctx[i];
+        const int slot = take_ref_slot(c);
+        PlaneJob& pj = b->h_pjobs[i];
+        pj.luma = d_ref[i];
+        pj.stride = c->width;
+        pj.w = c->width;
+        pj.h = c->height;
+        pj.out = c->d_planes[slot];
+        pj.psize = c->psize;
+        pj.sw = c->sw;
+        pj.sh = c->sh;
+        pj.tiles_x = (c->sw + K1_TW - 1) / K1_TW;
+        pj.tile0 = tile;
+        pj.col_states = d_col ? d_col[i] : nullptr;
+        pj.col = c->d_col[slot];
+        pj.nmb = c->nmb;
+        pj.mb0 = b->mb0[i];
+        tile += pj.tiles_x * ((c->sh + K1_TH - 1) / K1_TH);
+        SrcJob& sj = b->h_sjobs[i];
+        sj.src = d_src[i];
+        sj.stride = c->width;
+        sj.w = c->width;
+        sj.h = c->height;
+        sj.dst = c->d_src;
+        sj.pw = c->pw;
+        sj.ph = c->ph;
+        sj.row0 = row;
+        row += c->ph;
+        AnalyseParams& p = b->h_table[i];
+        fill_params(c, p);
+        p.states_out = d_states[i];
+        p.results = d_results[i];
+        p.flags = b->d_flags + b->mb0[i];
+        p.epoch = 1;  // the flags are cleared every step
+        p.err = b->d_counters + 1;
+        p.nmb = c->nmb;
+    }
+    CK(cudaMemcpyAsync(b->d_pjobs, b->h_pjobs, sizeof(PlaneJob) * b->n, cudaMemcpyHostToDevice, b->stream));
+    CK(cudaMemcpyAsync(b->d_sjobs, b->h_sjobs, sizeof(SrcJob) * b->n, cudaMemcpyHostToDevice, b->stream));
+    CK(cudaMemcpyAsync(b->d_table, b->h_table, sizeof(AnalyseParams) * b->n, cudaMemcpyHostToDevice, b->stream));
+    CK(cudaEventRecord(b->copied, b->stream));
+    b->pending = true;
+    source_batch_kernel<<<b->total_rows, 128, 0, b->stream>>>(b->d_sjobs, b->n);
+    planes_batch_kernel<<<b->total_tiles, K1_THREADS, 0, b->stream>>>(b->d_pjobs, b->n);
+    col_batch_kernel<<<(b->total_mbs + 255) / 256, 256, 0, b->stream>>>(b->d_pjobs, b->n, b->total_mbs);
+    CK(cudaMemsetAsync(b->d_flags, 0, sizeof(unsigned) * b->total_mbs, b->stream));
+    CK(cudaMemsetAsync(b->d_counters, 0, sizeof(unsigned) * 2, b->stream));
+    analyse_batch_kernel<<<b->k2_blocks, K2_WARPS * 32, 0, b->stream>>>(b->d_table, b->d_order, (unsigned)b->total_mbs,
+                                                                        b->d_counters, b->d_counters + 1);
+    return cuda_status(cudaGetLastError());
+}
+
+extern "C" int ironav_batch_sync(ironav_batch* b) {
+    if (!b) return IRONAV_INVALID_ARGUMENT;
+    unsigned err = 0;
+    CK(cudaMemcpyAsync(&err, b->d_counters + 1, sizeof(unsigned), cudaMemcpyDeviceToHost, b->stream));
+    CK(cudaStreamSynchronize(b->stream));
+    b->pending = false;  // the staging tables are free again
+    if (err & 1u) return IRONAV_TIMEOUT;
+    return err ? IRONAV_INTERNAL : IRONAV_OK;
+}

@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "analyse.cuh"
+#include "ctx.cuh"
 #include "planes.cuh"
 #include "peaks.cuh"
 
@@ -23,41 +24,47 @@ using namespace ironav;
 static_assert(sizeof(ironav_mbstate) == 72, "ironav_mbstate layout");
 static_assert(sizeof(ironav_mbresult) == 104, "ironav_mbresult layout");
 
-struct ironav_ctx {
-    int width = 0, height = 0, bd = 8, mb_w = 0, mb_h = 0, pw = 0, ph = 0, sw = 0, sh = 0;
-    int max_refs = 0, nslices = 0, nmb = 0;
-    int device = 0, nsm = 0, k2_blocks = 0;
-    cudaStream_t stream = nullptr;
-    long long psize = 0;
-    uint8_t* d_src = nullptr;
-    uint8_t* d_stage = nullptr;  // reference luma as given, rows pw apart
-    uint8_t* d_planes[MAX_REFS] = {};
-    ColMv* d_col[MAX_REFS] = {};
-    int slot_of[MAX_REFS] = {};  // reference index (0 = newest) -> slot
-    int nrefs = 0;
-    int* d_band_start = nullptr;
-    int* d_order = nullptr;
-    unsigned* d_flags = nullptr;
-    unsigned* d_counters = nullptr;  // [0] ticket, [1] error
-    unsigned epoch = 0;
-    ironav_mbstate* d_states = nullptr;
-    ironav_mbstate* d_col_stage = nullptr;
-    ironav_mbresult* d_results = nullptr;
-    // picture parameters
-    int qpp = 0, lambda = 0, skip_thresh = 0, nact = 0, fast = 0, sub8 = 0;
-    bool have_params = false;
-    int withhold = -1;
-    unsigned wait_limit = 1u << 22;
-    // in-loop mode: host memory mapped into the device (allocated on first use)
-    int* d_order_bands = nullptr;         // tickets: rows interleaved across bands, raster within each
-    ironav_mbresult* h_results = nullptr;
-    unsigned* h_done = nullptr;
-    ironav_mbstate* h_committed = nullptr;
-    unsigned* h_commit = nullptr;
-    unsigned inloop_epoch = 0;
-    bool inloop_active = false;
-    unsigned long long inloop_wait_ns = 10ull * 1000 * 1000 * 1000;
-};
+// The reference slot for a new picture: the oldest one's once max_refs are held, else a free one; the
+// new picture becomes reference 0 (enc/mod.rs:663-666).
+int take_ref_slot(ironav_ctx* c) {
+    int slot;
+    if (c->nrefs == c->max_refs) {
+        slot = c->slot_of[c->max_refs - 1];
+        c->nrefs--;
+    } else {
+        bool used[MAX_REFS] = {};
+        for (int i = 0; i < c->nrefs; i++) used[c->slot_of[i]] = true;
+        slot = 0;
+        while (used[slot]) slot++;
+    }
+    for (int i = c->nrefs; i > 0; i--) c->slot_of[i] = c->slot_of[i - 1];
+    c->slot_of[0] = slot;
+    c->nrefs++;
+    return slot;
+}
+
+// The analysis parameters of the context's current picture (everything but the mode's own fields).
+void fill_params(const ironav_ctx* c, AnalyseParams& p) {
+    memset(&p, 0, sizeof(p));
+    p.src = c->d_src;
+    p.ls = c->pw;
+    for (int i = 0; i < c->nact; i++) p.planes[i] = c->d_planes[c->slot_of[i]];
+    p.psize = c->psize;
+    p.sw = c->sw;
+    p.col = c->d_col[c->slot_of[0]];
+    p.mb_w = c->mb_w;
+    p.mb_h = c->mb_h;
+    p.pw = c->pw;
+    p.ph = c->ph;
+    p.nact = c->nact;
+    p.lambda = c->lambda;
+    p.skip_thresh = c->skip_thresh;
+    p.fast = c->fast;
+    p.sub8 = c->sub8;
+    p.band_start = c->d_band_start;
+    p.withhold = -1;
+    p.wait_limit = c->wait_limit;
+}
 
 namespace {
 
@@ -97,20 +104,7 @@ void free_ctx(ironav_ctx* c) {
 }
 
 int launch_planes(ironav_ctx* c, const uint8_t* d_luma, int stride, int w, int h, const ironav_mbstate* d_col) {
-    // the new picture takes the slot of the oldest (dropped) one, or a free one
-    int slot;
-    if (c->nrefs == c->max_refs) {
-        slot = c->slot_of[c->max_refs - 1];
-        c->nrefs--;
-    } else {
-        bool used[MAX_REFS] = {};
-        for (int i = 0; i < c->nrefs; i++) used[c->slot_of[i]] = true;
-        slot = 0;
-        while (used[slot]) slot++;
-    }
-    for (int i = c->nrefs; i > 0; i--) c->slot_of[i] = c->slot_of[i - 1];
-    c->slot_of[0] = slot;
-    c->nrefs++;
+    const int slot = take_ref_slot(c);
     dim3 grid((c->sw + K1_TW - 1) / K1_TW, (c->sh + K1_TH - 1) / K1_TH);
     halfpel_planes_kernel<<<grid, K1_THREADS, 0, c->stream>>>(d_luma, stride, w, h, c->d_planes[slot], c->psize, c->sw, c->sh);
     col_extract_kernel<<<(c->nmb + 255) / 256, 256, 0, c->stream>>>(d_col, c->d_col[slot], c->nmb);
@@ -119,23 +113,7 @@ int launch_planes(ironav_ctx* c, const uint8_t* d_luma, int stride, int w, int h
 
 int launch_analyse(ironav_ctx* c, bool auto_mode, const ironav_mbstate* d_in, ironav_mbstate* d_out, ironav_mbresult* d_res) {
     AnalyseParams p;
-    memset(&p, 0, sizeof(p));
-    p.src = c->d_src;
-    p.ls = c->pw;
-    for (int i = 0; i < c->nact; i++) p.planes[i] = c->d_planes[c->slot_of[i]];
-    p.psize = c->psize;
-    p.sw = c->sw;
-    p.col = c->d_col[c->slot_of[0]];
-    p.mb_w = c->mb_w;
-    p.mb_h = c->mb_h;
-    p.pw = c->pw;
-    p.ph = c->ph;
-    p.nact = c->nact;
-    p.lambda = c->lambda;
-    p.skip_thresh = c->skip_thresh;
-    p.fast = c->fast;
-    p.sub8 = c->sub8;
-    p.band_start = c->d_band_start;
+    fill_params(c, p);
     p.states_in = d_in;
     p.states_out = d_out;
     p.results = d_res;
@@ -439,23 +417,7 @@ int ironav_inloop_begin(ironav_ctx* c, int order) {
         memset(c->h_commit, 0, sizeof(unsigned) * c->nmb);
     }
     AnalyseParams p;
-    memset(&p, 0, sizeof(p));
-    p.src = c->d_src;
-    p.ls = c->pw;
-    for (int i = 0; i < c->nact; i++) p.planes[i] = c->d_planes[c->slot_of[i]];
-    p.psize = c->psize;
-    p.sw = c->sw;
-    p.col = c->d_col[c->slot_of[0]];
-    p.mb_w = c->mb_w;
-    p.mb_h = c->mb_h;
-    p.pw = c->pw;
-    p.ph = c->ph;
-    p.nact = c->nact;
-    p.lambda = c->lambda;
-    p.skip_thresh = c->skip_thresh;
-    p.fast = c->fast;
-    p.sub8 = c->sub8;
-    p.band_start = c->d_band_start;
+    fill_params(c, p);
     p.order = order == IRONAV_INLOOP_BANDS ? c->d_order_bands : nullptr;
     p.ticket = c->d_counters;
     p.err = c->d_counters + 1;

@@ -23,14 +23,14 @@ __device__ __forceinline__ int k1_tap6(int a, int b, int c, int d, int e, int f)
 
 __device__ __forceinline__ uint32_t k1_clip8(int v) { return (uint32_t)min(max(v, 0), 255); }
 
-// luma: w x h samples, rows `stride` apart. Samples outside it repeat its edges, which is both the
-// macroblock padding of H264Encoder::source (enc/mod.rs:502-519) when w x h is the picture size and
-// the plane border of round1 (enc/subpel.rs:72-76).
-static __global__ void __launch_bounds__(K1_THREADS) halfpel_planes_kernel(const uint8_t* __restrict__ luma, int stride, int w, int h,
-                                                                      uint8_t* __restrict__ out, long long psize, int sw, int sh) {
+// One TW x TH tile of the four planes, whose top-left sample is (x0, y0). luma: w x h samples, rows
+// `stride` apart. Samples outside it repeat its edges, which is both the macroblock padding of
+// H264Encoder::source (enc/mod.rs:502-519) when w x h is the picture size and the plane border of round1
+// (enc/subpel.rs:72-76). All K1_THREADS threads of the block take part.
+__device__ __forceinline__ void planes_tile(const uint8_t* __restrict__ luma, int stride, int w, int h, uint8_t* __restrict__ out,
+                                            long long psize, int sw, int sh, int x0, int y0) {
     __shared__ int g[K1_TH + 5][K1_TW + 8];       // integer samples, column c <-> x0 - 2 + c
     __shared__ int b1[K1_TH + 5][K1_TW];          // unrounded horizontal sums at x0 + c
-    const int x0 = blockIdx.x * K1_TW, y0 = blockIdx.y * K1_TH;
     const int tid = threadIdx.x;
     // stage rows y0-2 .. y0+TH+2 and columns x0-2 .. x0+TW+5 of G (clamped to the plane; values
     // outside it are never used by an output that is not forced to zero)
@@ -70,6 +70,11 @@ static __global__ void __launch_bounds__(K1_THREADS) halfpel_planes_kernel(const
     *reinterpret_cast<uint32_t*>(out + psize + o) = pb;
     *reinterpret_cast<uint32_t*>(out + 2 * psize + o) = ph;
     *reinterpret_cast<uint32_t*>(out + 3 * psize + o) = pj;
+}
+
+static __global__ void __launch_bounds__(K1_THREADS) halfpel_planes_kernel(const uint8_t* __restrict__ luma, int stride, int w, int h,
+                                                                             uint8_t* __restrict__ out, long long psize, int sw, int sh) {
+    planes_tile(luma, stride, w, h, out, psize, sw, sh, blockIdx.x * K1_TW, blockIdx.y * K1_TH);
 }
 
 // The co-located vector of each macroblock (col_mv, enc/frame.rs:944-947) from the reference

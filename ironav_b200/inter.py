@@ -70,7 +70,8 @@ EXPORTS = (
     "ironav_set_source_device", "ironav_push_reference_device",
     "ironav_analyse_picture_replay_device", "ironav_analyse_picture_auto_device", "ironav_ctx_sync",
     "ironav_inloop_begin", "ironav_inloop_result", "ironav_inloop_commit", "ironav_inloop_end",
-    "ironav_inloop_set_wait", "ironav_analyse_auto_noalloc",
+    "ironav_inloop_set_wait", "ironav_batch_create", "ironav_batch_destroy", "ironav_batch_step",
+    "ironav_batch_sync", "ironav_analyse_auto_noalloc",
 )
 
 
@@ -115,6 +116,11 @@ def _declare(lib: ctypes.CDLL) -> ctypes.CDLL:
         lib.ironav_inloop_commit.argtypes = [_VP, _I, _VP]
         lib.ironav_inloop_end.argtypes = [_VP]
         lib.ironav_inloop_set_wait.argtypes = [_VP, _I]
+    if hasattr(lib, "ironav_batch_create"):
+        lib.ironav_batch_create.argtypes = [ctypes.POINTER(_VP), ctypes.POINTER(_VP), _I]
+        lib.ironav_batch_destroy.argtypes = [_VP]
+        lib.ironav_batch_step.argtypes = [_VP] + [ctypes.POINTER(_VP)] * 5
+        lib.ironav_batch_sync.argtypes = [_VP]
     if hasattr(lib, "ironav_analyse_auto_noalloc"):
         # (d_src, src_stride, d_ref, ref_stride, ref_w, ref_h, d_col, width, height, nslices, qp_prime, lambda,
         #  skip_thresh, fast, sub8, d_planes, d_states, d_results, stream)
@@ -323,6 +329,39 @@ def decision_state(res, skip: bool) -> np.ndarray:
                 st["mvs"][by * 4 + bx] = res["mvs"][n]
     st["refs"][:] = res["refs"]
     return st
+
+
+class InterBatch:
+    """The batched form: several InterStage streams stepped together, one launch per stage (ironav_batch)."""
+
+    def __init__(self, stages: list[InterStage]):
+        self.stages = stages
+        self.lib = stages[0].lib
+        arr = (_VP * len(stages))(*[s.ctx.value for s in stages])
+        h = _VP()
+        InterStage._check(self.lib.ironav_batch_create(ctypes.byref(h), arr, len(stages)), "ironav_batch_create")
+        self.h = h
+
+    def step(self, d_src, d_ref, d_col, d_states, d_results) -> None:
+        """Lists of device pointers (ints; None in d_col for a reference without decisions)."""
+        n = len(self.stages)
+        mk = lambda xs: (_VP * n)(*[x if x is not None else None for x in xs])
+        InterStage._check(self.lib.ironav_batch_step(self.h, mk(d_src), mk(d_ref), mk(d_col), mk(d_states), mk(d_results)),
+                          "ironav_batch_step")
+
+    def sync(self) -> None:
+        InterStage._check(self.lib.ironav_batch_sync(self.h), "ironav_batch_sync")
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.ironav_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def default_bands(mb_h: int, nslices: int) -> list[int]:

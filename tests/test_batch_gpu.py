@@ -1,0 +1,80 @@
+"""The batched form (ironav_batch_*): several streams of different sizes stepped together, one launch
+per stage, must give every stream exactly the results of its own single-stream auto mode."""
+import numpy as np
+import pytest
+
+from ironav_b200.inter import MBRESULT_DTYPE, MBSTATE_DTYPE, InterBatch, InterStage
+from ironav_b200.synth import Sequence
+
+pytestmark = pytest.mark.gpu
+
+# (width, height, slice bands): the batched configuration's resolutions and their pinned band counts
+STREAMS = [(640, 360, 2), (854, 480, 3), (352, 288, 2), (1280, 720, 5), (1920, 1080, 8), (176, 144, 1)]
+
+
+def _frames(i, w, h, n=3):
+    seq = Sequence.config("1080p", n, seed=0x1A2B0300 + i, size=(w, h))
+    return [seq.frame(t) for t in range(n)]
+
+
+def test_batch_equals_single_stream_auto_mode(cuda_lib):
+    import torch
+
+    stream = torch.cuda.Stream()
+    frames = [_frames(i, w, h) for i, (w, h, _) in enumerate(STREAMS)]
+    # each stream alone (host-buffer calls)
+    want = []
+    for (w, h, ns), f in zip(STREAMS, frames):
+        st = InterStage(w, h, nslices=ns, lib=cuda_lib)
+        per = []
+        col = None
+        for t in (1, 2):
+            st.clear_references()
+            st.push_reference(f[t - 1], col=col)
+            st.set_source(f[t])
+            st.begin_p_picture(27)
+            states, res = st.analyse_auto()
+            per.append((states, res))
+            col = states
+        st.close()
+        want.append(per)
+    # all streams together: each context primed with a reference so its picture parameters are valid
+    stages = []
+    dev = [[torch.from_numpy(x).cuda() for x in f] for f in frames]
+    for (w, h, ns), f in zip(STREAMS, dev):
+        st = InterStage(w, h, nslices=ns, lib=cuda_lib)
+        st.set_stream(stream.cuda_stream)
+        st.push_reference_device(f[0].data_ptr(), w, w, h, None)
+        st.begin_p_picture(27)
+        stages.append(st)
+    n = len(stages)
+    d_states = [[torch.zeros(s.nmb * 72, dtype=torch.uint8, device="cuda") for _ in range(2)] for s in stages]
+    d_res = [[torch.zeros(s.nmb * 104, dtype=torch.uint8, device="cuda") for _ in range(2)] for s in stages]
+    torch.cuda.synchronize()
+    batch = InterBatch(stages)
+    for k, t in enumerate((1, 2)):
+        col = [None] * n if k == 0 else [d_states[i][0].data_ptr() for i in range(n)]
+        batch.step([f[t].data_ptr() for f in dev], [f[t - 1].data_ptr() for f in dev], col,
+                   [d_states[i][k].data_ptr() for i in range(n)], [d_res[i][k].data_ptr() for i in range(n)])
+        batch.sync()
+        for i in range(n):
+            got_s = d_states[i][k].cpu().numpy().view(MBSTATE_DTYPE)
+            got_r = d_res[i][k].cpu().numpy().view(MBRESULT_DTYPE)
+            assert np.array_equal(got_s, want[i][k][0]), f"stream {i} step {k}: decisions"
+            assert np.array_equal(got_r, want[i][k][1]), f"stream {i} step {k}: results"
+
+    # a frame step captured in a CUDA graph replays to the same results
+    for i in range(n):
+        d_res[i][1].zero_()
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=stream):
+        batch.step([f[2].data_ptr() for f in dev], [f[1].data_ptr() for f in dev], [d_states[i][0].data_ptr() for i in range(n)],
+                   [d_states[i][1].data_ptr() for i in range(n)], [d_res[i][1].data_ptr() for i in range(n)])
+    g.replay()
+    torch.cuda.synchronize()
+    batch.sync()
+    for i in range(n):
+        assert np.array_equal(d_res[i][1].cpu().numpy().view(MBRESULT_DTYPE), want[i][1][1]), f"stream {i}: graph replay"
+    del g
+    batch.close()
