@@ -155,6 +155,14 @@ int ironav_synth_frame(void* h, int t, uint8_t* out, int stride) {
     return 0;
 }
 
+// n draws of std::mt19937_64(seed) reduced modulo m (the batched configuration's resolution choices).
+int ironav_synth_draws(uint64_t seed, int n, int m, int* out) {
+    if (n < 0 || m <= 0 || !out) return 3;
+    std::mt19937_64 g(seed);
+    for (int i = 0; i < n; i++) out[i] = int(g() % uint64_t(m));
+    return 0;
+}
+
 // The cumulative pan of frame t in quarter samples (for tests that check recovered motion).
 int ironav_synth_pan(void* h, int t, int* qx, int* qy) {
     Synth* s = static_cast<Synth*>(h);

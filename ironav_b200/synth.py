@@ -38,10 +38,24 @@ def _lib() -> ctypes.CDLL:
                                             ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double]
         lib.ironav_synth_destroy.argtypes = [ctypes.c_void_p]
         lib.ironav_synth_frame.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int]
+        lib.ironav_synth_draws.argtypes = [ctypes.c_uint64, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
         lib.ironav_synth_pan.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                          ctypes.POINTER(ctypes.c_int)]
         _LIB = lib
     return _LIB
+
+
+# The batched configuration: 64 streams, resolutions drawn from these by std::mt19937_64(0x1A2B03FF),
+# stream s seeded 0x1A2B0300 + s, each with the encoder's slice count on a >= 8-core host.
+BATCH_SIZES = [(640, 360, 2), (854, 480, 3), (1280, 720, 5), (1920, 1080, 8)]
+BATCH_SEED = 0x1A2B03FF
+
+
+def batch_streams(n: int = 64) -> list[tuple[int, int, int, int]]:
+    """(width, height, slice bands, seed) of the batched configuration's streams."""
+    idx = np.zeros(n, dtype=np.int32)
+    _lib().ironav_synth_draws(BATCH_SEED, n, len(BATCH_SIZES), idx.ctypes.data)
+    return [BATCH_SIZES[int(k)] + (0x1A2B0300 + s,) for s, k in enumerate(idx)]
 
 
 class Sequence:
