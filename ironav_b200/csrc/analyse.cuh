@@ -145,7 +145,7 @@ static __device__ __forceinline__ Blk nb(const AnalyseParams& __restrict__ P, Wa
 }
 
 // pred_mv, enc/frame.rs:543-570
-static __device__ __noinline__ int2 pred_mv(const AnalyseParams& __restrict__ P, WarpSmem& __restrict__ S, const Blk* cur, int bx, int by, int w, int dir, int rf) {
+static __device__ __forceinline__ int2 pred_mv(const AnalyseParams& __restrict__ P, WarpSmem& __restrict__ S, const Blk* cur, int bx, int by, int w, int dir, int rf) {
     const Blk a = nb(P, S, cur, bx - 1, by), b = nb(P, S, cur, bx, by - 1);
     Blk c = nb(P, S, cur, bx + w, by - 1);
     if (!c.w) c = nb(P, S, cur, bx - 1, by - 1);
@@ -180,7 +180,8 @@ static __device__ __forceinline__ int sad_lane(const uint8_t* __restrict__ g0, c
                                                int h, int px, int py, bool valid) {
     const int lane = threadIdx.x & 31;
     int sad = 0;
-    if (valid) {
+    if (!valid) px = py = 0;  // scored at a position always inside the planes, and discarded: no divergent branch
+    {
         const int row0 = lane >> 3;
         const uint8_t* G = g0 + ((py >> 2) + row0) * sw + (px >> 2);
         const int step4 = 4 * sw;
@@ -209,7 +210,7 @@ static __device__ __forceinline__ int sad_lane(const uint8_t* __restrict__ g0, c
 // Quarter-sample prediction (HalfPel::predict, enc/subpel.rs:122-145) of the partition at 4x4 block
 // (bx, by), (4 << lgw) x (4 << lgh) samples, scored by SATD (satd, enc/frame.rs:641-659), or by SAD
 // when `sad` (the P_Skip test), for the n vectors S.cand[0..n); the sums land in S.cost[0..n).
-static __device__ __noinline__ void pred_batch(const AnalyseParams& __restrict__ P, WarpSmem& __restrict__ S, int r, int bx, int by, int lgw, int lgh, int n, bool sad) {
+static __device__ __forceinline__ void pred_batch(const AnalyseParams& __restrict__ P, WarpSmem& __restrict__ S, int r, int bx, int by, int lgw, int lgh, int n, bool sad) {
     const int lane = threadIdx.x & 31;
     const int lg = lgw + lgh, total = n << lg, w = 4 << lgw, h = 4 << lgh;
     if (lane < n) S.cost[lane] = 0;
