@@ -52,7 +52,7 @@ def parse():
     p.add_argument("--ring", type=int, default=RING,
                    help="pictures in the ring (fewer than 36 fits in L2: for profiling runs only)")
     p.add_argument("--no-e2e", action="store_true", help="skip the host-buffer pass (profiling runs)")
-    p.add_argument("--workload", default="1080p", choices=["1080p", "batched"],
+    p.add_argument("--workload", default="1080p", choices=["1080p", "batched", "scenecut"],
                    help="1080p: one stream, replay mode (the headline); batched: 64 mixed-resolution streams in auto "
                         "mode, one launch per stage and frame step, against the per-stream launch loop")
     p.add_argument("--streams", type=int, default=64, help="streams of the batched workload")
@@ -240,6 +240,9 @@ def main():
         return finish(world)
     if args.workload == "batched":
         run_batched(args, rank, world)
+        return finish(world)
+    if args.workload == "scenecut":
+        run_scenecut(args, rank, world)
         return finish(world)
 
     import torch
@@ -480,6 +483,45 @@ def run_batched(args, rank, world):
     batch.close()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def run_scenecut(args, rank, world):
+    """The scene-cut measure at 1080p (change_threads, codec/change.rs:56-90): low-resolution luma of two
+    pictures and the +-4 search of every 8x8 low-resolution block, device-resident, against the oracle on
+    the host. One step = one picture pair."""
+    import torch
+    from ironav_b200.inter import InterStage, cuda_library
+    from tests.oracle_lib import oracle_library
+
+    dev = torch.device("cuda", torch.cuda.current_device())
+    frames = make_frames(rank, 8)
+    d = torch.from_numpy(frames).to(dev)
+    st = InterStage(WIDTH, HEIGHT, lib=cuda_library())
+    out = np.zeros(2, dtype=np.int64)
+    lib = st.lib
+    for i in range(args.warmup):
+        lib.ironav_scene_change_device(st.ctx, d[i % 7].data_ptr(), d[i % 7 + 1].data_ptr(), WIDTH, out.ctypes.data)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        lib.ironav_scene_change_device(st.ctx, d[i % 7].data_ptr(), d[i % 7 + 1].data_ptr(), WIDTH, out.ctypes.data)
+    el = time.perf_counter() - t0
+    o = InterStage(WIDTH, HEIGHT, lib=oracle_library())
+    t0 = time.perf_counter()
+    n_cpu = 0
+    while time.perf_counter() - t0 < 3.0:
+        o.scene_change(frames[n_cpu % 7], frames[n_cpu % 7 + 1])
+        n_cpu += 1
+    el_cpu = time.perf_counter() - t0
+    if rank == 0:
+        print(json.dumps({
+            "metric": "1080p scene-cut measure, picture pairs per second", "value": args.steps / el, "unit": "pairs/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+            "higher_is_better": True, "scaling": "replicas", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+            "config": {"workload": "low-resolution luma of both pictures + +-4 search of 2040 8x8 blocks, one call per pair "
+                                   "(synchronous: returns the totals)"},
+            "cpu_baseline": {"value": n_cpu / el_cpu, "unit": "pairs/s", "cores": 1, "kind": "port",
+                             "sample": f"{n_cpu} pairs, one thread (the reference's non-live setting)"}}), flush=True)
 
 
 def ctypes_peak(lib):

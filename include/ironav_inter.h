@@ -157,6 +157,17 @@ int ironav_analyse_picture_auto_device(ironav_ctx* ctx, ironav_mbstate* d_out_st
  * wait that gave up). */
 int ironav_ctx_sync(ironav_ctx* ctx);
 
+/* ---- scene-cut measure ------------------------------------------------------------------------------ */
+
+/* How well cur_y is predicted from prev_y against from itself (change_threads, codec/change.rs:56-90), on
+ * the low-resolution luma the encoder takes of its padded source (H264Encoder::low_res, enc/mod.rs:689-693;
+ * LowRes::new, codec/change.rs:16-24): out[0] = inter, out[1] = intra totals. The encoder starts an IDR
+ * picture when (double)inter > 0.8 * (double)intra (SCENE_CUT, enc/mod.rs:707-711); the comparison stays
+ * with the caller, in f64 like the reference. Both pictures are width x height, rows `stride` apart. */
+int ironav_scene_change(ironav_ctx* ctx, const uint8_t* prev_y, const uint8_t* cur_y, int stride, int64_t* out);
+/* The same on device pointers (returns when the totals are in out, a host array). */
+int ironav_scene_change_device(ironav_ctx* ctx, const uint8_t* d_prev, const uint8_t* d_cur, int stride, int64_t* out);
+
 /* ---- in-loop mode ---------------------------------------------------------------------------------- */
 
 /* The encoder's own loop (FrameCoder::encode, enc/frame.rs:467-478): the caller makes each macroblock's

@@ -42,6 +42,10 @@ struct ironav_ctx {
     unsigned inloop_epoch = 0;
     bool inloop_active = false;
     unsigned long long inloop_wait_ns = 10ull * 1000 * 1000 * 1000;
+    // scene-cut measure (allocated on first use): two pictures' luma, their low-resolution luma, totals
+    uint8_t* d_scene_luma = nullptr;
+    uint8_t* d_lowres = nullptr;
+    unsigned long long* d_scene_sums = nullptr;
 };
 
 

@@ -18,6 +18,7 @@
 #include "ctx.cuh"
 #include "planes.cuh"
 #include "peaks.cuh"
+#include "scene.cuh"
 
 using namespace ironav;
 
@@ -96,6 +97,9 @@ void free_ctx(ironav_ctx* c) {
     cudaFree(c->d_col_stage);
     cudaFree(c->d_results);
     cudaFree(c->d_order_bands);
+    cudaFree(c->d_scene_luma);
+    cudaFree(c->d_lowres);
+    cudaFree(c->d_scene_sums);
     cudaFreeHost(c->h_results);
     cudaFreeHost(c->h_done);
     cudaFreeHost(c->h_committed);
@@ -367,6 +371,55 @@ int ironav_ctx_sync(ironav_ctx* c) {
     if (!c) return IRONAV_INVALID_ARGUMENT;
     CK(cudaStreamSynchronize(c->stream));
     return check_device_error(c);
+}
+
+// ---- scene-cut measure ---------------------------------------------------------------------------
+
+static int scene_alloc(ironav_ctx* c) {
+    if (c->d_lowres) return IRONAV_OK;
+    const size_t lsz = (size_t)(c->mb_w * 4) * (c->mb_h * 4) + 64;  // slack: rows are read as whole words
+    CK(cudaMalloc(&c->d_scene_luma, 2 * (size_t)c->width * c->height));
+    CK(cudaMalloc(&c->d_lowres, 2 * lsz));
+    CK(cudaMalloc(&c->d_scene_sums, 2 * sizeof(unsigned long long)));
+    CK(cudaMemset(c->d_lowres, 0, 2 * lsz));
+    return IRONAV_OK;
+}
+
+static int scene_run(ironav_ctx* c, const uint8_t* d_prev, int sp, const uint8_t* d_cur, int sc, int64_t* out) {
+    const int lw = c->mb_w * 4, lh = c->mb_h * 4;
+    const size_t lsz = (size_t)lw * lh + 64;
+    uint8_t* lp = c->d_lowres;
+    uint8_t* lc = c->d_lowres + lsz;
+    lowres_kernel<<<(lw * lh + 255) / 256, 256, 0, c->stream>>>(d_prev, sp, c->width, c->height, lw, lh, lp);
+    lowres_kernel<<<(lw * lh + 255) / 256, 256, 0, c->stream>>>(d_cur, sc, c->width, c->height, lw, lh, lc);
+    CK(cudaMemsetAsync(c->d_scene_sums, 0, 2 * sizeof(unsigned long long), c->stream));
+    const int nb = (lw >= 8 && lh >= 8) ? ((lw - 8) / 8 + 1) * ((lh - 8) / 8 + 1) : 0;
+    if (nb > 0) change_kernel<<<(nb + 3) / 4, 128, 0, c->stream>>>(lp, lc, lw, lh, c->d_scene_sums);
+    CK(cudaGetLastError());
+    unsigned long long h[2];
+    CK(cudaMemcpyAsync(h, c->d_scene_sums, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    out[0] = (int64_t)h[0];
+    out[1] = (int64_t)h[1];
+    return IRONAV_OK;
+}
+
+int ironav_scene_change(ironav_ctx* c, const uint8_t* prev_y, const uint8_t* cur_y, int stride, int64_t* out) {
+    if (!c || !prev_y || !cur_y || !out || stride < c->width) return IRONAV_INVALID_ARGUMENT;
+    int s = scene_alloc(c);
+    if (s != IRONAV_OK) return s;
+    uint8_t* a = c->d_scene_luma;
+    uint8_t* b = c->d_scene_luma + (size_t)c->width * c->height;
+    CK(cudaMemcpy2DAsync(a, c->width, prev_y, stride, c->width, c->height, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpy2DAsync(b, c->width, cur_y, stride, c->width, c->height, cudaMemcpyHostToDevice, c->stream));
+    return scene_run(c, a, c->width, b, c->width, out);
+}
+
+int ironav_scene_change_device(ironav_ctx* c, const uint8_t* d_prev, const uint8_t* d_cur, int stride, int64_t* out) {
+    if (!c || !d_prev || !d_cur || !out || stride < c->width) return IRONAV_INVALID_ARGUMENT;
+    int s = scene_alloc(c);
+    if (s != IRONAV_OK) return s;
+    return scene_run(c, d_prev, stride, d_cur, stride, out);
 }
 
 // Measures the 32-bit integer issue rate of the current device (operations per second, 1e12 units in

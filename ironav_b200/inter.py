@@ -71,8 +71,10 @@ EXPORTS = (
     "ironav_analyse_picture_replay_device", "ironav_analyse_picture_auto_device", "ironav_ctx_sync",
     "ironav_inloop_begin", "ironav_inloop_result", "ironav_inloop_commit", "ironav_inloop_end",
     "ironav_inloop_set_wait", "ironav_batch_create", "ironav_batch_destroy", "ironav_batch_step",
-    "ironav_batch_sync", "ironav_analyse_auto_noalloc",
+    "ironav_batch_sync", "ironav_scene_change", "ironav_scene_change_device", "ironav_analyse_auto_noalloc",
 )
+
+SCENE_CUT = 0.8  # codec/change.rs:6
 
 
 class IronavError(RuntimeError):
@@ -116,6 +118,9 @@ def _declare(lib: ctypes.CDLL) -> ctypes.CDLL:
         lib.ironav_inloop_commit.argtypes = [_VP, _I, _VP]
         lib.ironav_inloop_end.argtypes = [_VP]
         lib.ironav_inloop_set_wait.argtypes = [_VP, _I]
+    if hasattr(lib, "ironav_scene_change"):
+        lib.ironav_scene_change.argtypes = [_VP, _VP, _VP, _I, _VP]
+        lib.ironav_scene_change_device.argtypes = [_VP, _VP, _VP, _I, _VP]
     if hasattr(lib, "ironav_batch_create"):
         lib.ironav_batch_create.argtypes = [ctypes.POINTER(_VP), ctypes.POINTER(_VP), _I]
         lib.ironav_batch_destroy.argtypes = [_VP]
@@ -254,6 +259,22 @@ class InterStage:
         self._check(self.lib.ironav_analyse_picture_auto(self.ctx, _ptr(states), _ptr(out)),
                     "ironav_analyse_picture_auto")
         return states, out
+
+    # -- scene-cut measure (change_threads, codec/change.rs:56-90) -----------------------------------------
+
+    def scene_change(self, prev: np.ndarray, cur: np.ndarray) -> tuple[int, int]:
+        """(inter, intra) totals of cur against prev on the low-resolution luma."""
+        prev = np.ascontiguousarray(prev, dtype=np.uint8)
+        cur = np.ascontiguousarray(cur, dtype=np.uint8)
+        out = np.zeros(2, dtype=np.int64)
+        self._check(self.lib.ironav_scene_change(self.ctx, _ptr(prev), _ptr(cur), self.width, _ptr(out)),
+                    "ironav_scene_change")
+        return int(out[0]), int(out[1])
+
+    def scene_cut(self, prev: np.ndarray, cur: np.ndarray) -> bool:
+        """Whether cur starts a new scene: inter > SCENE_CUT * intra, in f64 (enc/mod.rs:707-711)."""
+        inter, intra = self.scene_change(prev, cur)
+        return float(inter) > SCENE_CUT * float(intra)
 
     # -- in-loop mode: the caller decides each macroblock (the encoder's own loop) ---------------------
 

@@ -36,6 +36,7 @@
 #include "../include/ironav_inter.h"
 
 #include <math.h>
+#include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
 #ifdef _OPENMP
@@ -1058,3 +1059,66 @@ int ironav_batch_step(ironav_batch* b, const uint8_t* const* s, const uint8_t* c
     return IRONAV_HARDWARE_UNAVAILABLE;
 }
 int ironav_batch_sync(ironav_batch* b) { (void)b; return IRONAV_INVALID_ARGUMENT; }
+
+/* ---------------------------------------------------------------------------------------------------
+ * Scene-cut measure: LowRes::new (codec/change.rs:16-24) on the padded source as H264Encoder::low_res
+ * takes it (enc/mod.rs:689-693), and change_threads (codec/change.rs:56-90; single-threaded: the
+ * threaded form gives the same totals).
+ * ------------------------------------------------------------------------------------------------- */
+
+static void lowres_of(const uint16_t* src, int pw, int lw, int lh, int32_t* out) {
+    for (int i = 0; i < lw * lh; i++) {
+        int x0 = i % lw * 4, y0 = i / lw * 4, sum = 0;
+        for (int k = 0; k < 16; k++) sum += src[(size_t)(y0 + k / 4) * pw + x0 + k % 4];
+        out[i] = sum >> 4;
+    }
+}
+
+static void change_of(const int32_t* prev, const int32_t* cur, int lw, int lh, int64_t* inter_out, int64_t* intra_out) {
+    int64_t inter = 0, intra = 0;
+    for (int by = 0; by + 7 < lh; by += 8)
+        for (int bx = 0; bx + 7 < lw; bx += 8) {
+#define AT(x, y) cur[(size_t)(by + (y)) * lw + bx + (x)]
+            int sum = 0;
+            for (int k = 0; k < 64; k++) sum += AT(k % 8, k / 8);
+            int mean = sum / 64;
+            for (int k = 0; k < 64; k++) intra += abs(AT(k % 8, k / 8) - mean);
+            int64_t best = INT64_MAX;
+            for (int dy = -4; dy <= 4; dy++)
+                for (int dx = -4; dx <= 4; dx++) {
+                    int ox = bx + dx, oy = by + dy;
+                    if (ox < 0 || oy < 0 || ox + 8 > lw || oy + 8 > lh) continue;
+                    int64_t sad = 0;
+                    for (int k = 0; k < 64; k++) sad += abs(AT(k % 8, k / 8) - prev[(size_t)(oy + k / 8) * lw + ox + k % 8]);
+                    if (sad < best) best = sad;
+                }
+            inter += best;
+#undef AT
+        }
+    *inter_out = inter;
+    *intra_out = intra;
+}
+
+int ironav_scene_change(ironav_ctx* c, const uint8_t* prev_y, const uint8_t* cur_y, int stride, int64_t* out) {
+    if (!c || !prev_y || !cur_y || !out || stride < c->width) return IRONAV_INVALID_ARGUMENT;
+    int lw = c->mb_w * 4, lh = c->mb_h * 4;
+    uint16_t* a = (uint16_t*)malloc(sizeof(uint16_t) * (size_t)c->pw * c->ph);
+    uint16_t* b = (uint16_t*)malloc(sizeof(uint16_t) * (size_t)c->pw * c->ph);
+    int32_t* la = (int32_t*)malloc(sizeof(int32_t) * (size_t)lw * lh);
+    int32_t* lb = (int32_t*)malloc(sizeof(int32_t) * (size_t)lw * lh);
+    pad_plane(prev_y, stride, c->width, c->height, c->pw, c->ph, a);
+    pad_plane(cur_y, stride, c->width, c->height, c->pw, c->ph, b);
+    lowres_of(a, c->pw, lw, lh, la);
+    lowres_of(b, c->pw, lw, lh, lb);
+    change_of(la, lb, lw, lh, &out[0], &out[1]);
+    free(a);
+    free(b);
+    free(la);
+    free(lb);
+    return IRONAV_OK;
+}
+
+int ironav_scene_change_device(ironav_ctx* c, const uint8_t* d_prev, const uint8_t* d_cur, int stride, int64_t* out) {
+    (void)c; (void)d_prev; (void)d_cur; (void)stride; (void)out;
+    return IRONAV_HARDWARE_UNAVAILABLE;
+}
