@@ -93,8 +93,8 @@ const char* ironav_version(void);
 
 typedef struct ironav_ctx ironav_ctx;
 
-/* One stream: width x height 8-bit luma (even, mb_w and mb_h <= 1024 like H264Encoder::new,
- * enc/mod.rs:143-152), up to max_refs reference pictures (1..16, with_refs enc/mod.rs:265-268), and
+/* One stream: width x height luma of bd = 8 or 10 bits (the encoder's Yuv420p and Yuv420p10 formats,
+ * enc/mod.rs:140-143; even sizes, mb_w and mb_h <= 1024 like H264Encoder::new, enc/mod.rs:143-152), up to max_refs reference pictures (1..16, with_refs enc/mod.rs:265-268), and
  * nslices slice bands. band_rows holds nslices + 1 macroblock-row boundaries, or is NULL for the
  * encoder's own split, band i = [i*mb_h/n, (i+1)*mb_h/n) (enc/mod.rs:603). Neighbours in an earlier
  * band are unavailable to the vector predictors (nb_state, enc/frame.rs:509-515). */
@@ -107,9 +107,13 @@ int ironav_ctx_dims(const ironav_ctx* ctx, int* mb_w, int* mb_h, int* sw, int* s
 /* Makes the context queue its device work on this cudaStream_t (NULL: the legacy default stream). */
 int ironav_ctx_set_stream(ironav_ctx* ctx, void* cuda_stream);
 
-/* The picture to analyse: width x height luma rows `stride` bytes apart, padded to whole macroblocks by
- * repeating its right and bottom edges (H264Encoder::source, enc/mod.rs:481-529). */
-int ironav_set_source(ironav_ctx* ctx, const uint8_t* y, int stride);
+/* Sample buffers. Every luma buffer the entry points below take or fill holds samples of the context's
+ * depth: uint8_t when bd = 8, uint16_t (host byte order, values below 2^bd) when bd = 10, as the
+ * reference's Source keeps them (enc/mod.rs:486-526). Strides count samples, not bytes. */
+
+/* The picture to analyse: width x height luma, rows `stride` samples apart, padded to whole macroblocks
+ * by repeating its right and bottom edges (H264Encoder::source, enc/mod.rs:481-529). */
+int ironav_set_source(ironav_ctx* ctx, const void* y, int stride);
 
 /* Adds the newest reference picture (a decoded/reconstructed luma plane) and builds its half-sample
  * planes (HalfPel::new, enc/subpel.rs:42-115; the reference list, enc/mod.rs:551-559,660-666). w x h is
@@ -117,12 +121,12 @@ int ironav_set_source(ironav_ctx* ctx, const uint8_t* y, int stride);
  * 16*mb_w x 16*mb_h (a reconstruction, used as is). col holds the picture's own macroblock decisions
  * (mb_w*mb_h), read for the co-located candidate (col_mv, enc/frame.rs:944-947), or NULL when the
  * picture was intra coded. The oldest reference is dropped once max_refs are held. */
-int ironav_push_reference(ironav_ctx* ctx, const uint8_t* y, int stride, int w, int h,
+int ironav_push_reference(ironav_ctx* ctx, const void* y, int stride, int w, int h,
                           const ironav_mbstate* col);
 /* Forgets every reference (an IDR picture, enc/mod.rs:541-545). */
 int ironav_clear_references(ironav_ctx* ctx);
-/* Copies reference `idx` (0 = newest) planes G, b, h, j to out (4 * sw * sh bytes), for checks. */
-int ironav_get_planes(ironav_ctx* ctx, int idx, uint8_t* out);
+/* Copies reference `idx` (0 = newest) planes G, b, h, j to out (4 * sw * sh samples), for checks. */
+int ironav_get_planes(ironav_ctx* ctx, int idx, void* out);
 
 /* Parameters of the P picture to analyse (FrameCoder::new / with_sub8x8 / with_fast,
  * enc/frame.rs:381-440): qp_prime = QP'Y; lambda and skip_thresh from the helpers above (the host
@@ -146,8 +150,8 @@ int ironav_analyse_picture_auto(ironav_ctx* ctx, ironav_mbstate* out_states, iro
 
 /* ---- device-resident forms (pointers in device memory; asynchronous on the context's stream) ------ */
 
-int ironav_set_source_device(ironav_ctx* ctx, const uint8_t* d_y, int stride);
-int ironav_push_reference_device(ironav_ctx* ctx, const uint8_t* d_y, int stride, int w, int h,
+int ironav_set_source_device(ironav_ctx* ctx, const void* d_y, int stride);
+int ironav_push_reference_device(ironav_ctx* ctx, const void* d_y, int stride, int w, int h,
                                  const ironav_mbstate* d_col);
 int ironav_analyse_picture_replay_device(ironav_ctx* ctx, const ironav_mbstate* d_final_states,
                                          ironav_mbresult* d_out);
@@ -164,9 +168,9 @@ int ironav_ctx_sync(ironav_ctx* ctx);
  * LowRes::new, codec/change.rs:16-24): out[0] = inter, out[1] = intra totals. The encoder starts an IDR
  * picture when (double)inter > 0.8 * (double)intra (SCENE_CUT, enc/mod.rs:707-711); the comparison stays
  * with the caller, in f64 like the reference. Both pictures are width x height, rows `stride` apart. */
-int ironav_scene_change(ironav_ctx* ctx, const uint8_t* prev_y, const uint8_t* cur_y, int stride, int64_t* out);
+int ironav_scene_change(ironav_ctx* ctx, const void* prev_y, const void* cur_y, int stride, int64_t* out);
 /* The same on device pointers (returns when the totals are in out, a host array). */
-int ironav_scene_change_device(ironav_ctx* ctx, const uint8_t* d_prev, const uint8_t* d_cur, int stride, int64_t* out);
+int ironav_scene_change_device(ironav_ctx* ctx, const void* d_prev, const void* d_cur, int stride, int64_t* out);
 
 /* ---- in-loop mode ---------------------------------------------------------------------------------- */
 
@@ -199,7 +203,8 @@ int ironav_inloop_set_wait(ironav_ctx* ctx, int wait_ms);
 /* Many streams analysed together: each stream is a context (its own size, slice bands, references and
  * picture parameters); a frame step copies every stream's new picture, builds every stream's new
  * reference planes and then analyses every stream's macroblock wavefronts in auto mode in one
- * persistent launch. All contexts of a batch must use the same CUDA stream (ironav_ctx_set_stream); the
+ * persistent launch. All contexts of a batch must be 8-bit (bd = 8) and use the same CUDA stream
+ * (ironav_ctx_set_stream); the
  * work is queued there, so a frame step can be captured in a CUDA graph. */
 typedef struct ironav_batch ironav_batch;
 int ironav_batch_create(ironav_batch** out, ironav_ctx* const* ctxs, int n);

@@ -53,9 +53,10 @@ static __device__ __constant__ int8_t c_nsub[4] = {1, 2, 2, 4};
 // A 4x4 block's list-0 motion as the predictors see it: (mx, my, ref (-1 none), available).
 using Blk = int4;
 
-// Per-warp shared memory.
+// Per-warp shared memory; T is the sample type (uint8_t for 8-bit pictures, uint16_t for 10-bit).
+template <class T>
 struct WarpSmem {
-    uint32_t src[64];         // current macroblock, 16 rows x 4 words
+    uint32_t src[64 * sizeof(T)];  // current macroblock, 16 rows of 16 samples (4 * sizeof(T) words each)
     Blk ext[30];              // blocks around the macroblock: index (y + 1) * 6 + (x + 1), x in -1..4, y in -1..3
     Blk st[16];               // P_8x8: blocks decided so far (sub_search's `st`)
     Blk t[16];                // trial blocks (sub_search's `t`, part_mvps's `cur`)
@@ -107,11 +108,45 @@ __device__ __forceinline__ int satd4_packed(const uint32_t s[4], const uint32_t 
     return sum;
 }
 
+// Two-way dot products of the unsigned 16-bit halves of a with the signed bytes 0-1 (lo) or 2-3 (hi) of b.
+__device__ __forceinline__ int dp2a_lo_us(uint32_t a, uint32_t b, int c) {
+    int d;
+    asm("dp2a.lo.u32.s32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c));
+    return d;
+}
+__device__ __forceinline__ int dp2a_hi_us(uint32_t a, uint32_t b, int c) {
+    int d;
+    asm("dp2a.hi.u32.s32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c));
+    return d;
+}
+
+// satd4 of a 4x4 block of 16-bit samples: rows s[r][0..1] and p[r][0..1] hold 2 samples per word. The same
+// transform as satd4_packed, the row Hadamard taken with dp2a over the two words of each row.
+__device__ __forceinline__ int satd4_packed16(const uint32_t s[4][2], const uint32_t p[4][2]) {
+    const uint32_t H[4] = {0x01010101u, 0xFFFF0101u, 0x01FFFF01u, 0xFF01FF01u};
+    const uint32_t NH[4] = {0xFFFFFFFFu, 0x0101FFFFu, 0xFF0101FFu, 0x01FF01FFu};
+    int t[4][4];
+#pragma unroll
+    for (int r = 0; r < 4; r++)
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+            t[r][j] = dp2a_hi_us(p[r][1], NH[j], dp2a_lo_us(p[r][0], NH[j], dp2a_hi_us(s[r][1], H[j], dp2a_lo_us(s[r][0], H[j], 0))));
+    int sum = 0;
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+        const int a = t[0][c], b = t[1][c], cc = t[2][c], e = t[3][c];
+        const int s0 = a + b, s1 = cc + e, d0 = a - b, d1 = cc - e;
+        sum += max(abs(s0), abs(s1)) + max(abs(d0), abs(d1));
+    }
+    return sum;
+}
+
 // ---- neighbours (nb_state / nb_motion, enc/frame.rs:509-538) ----------------------------------
 
 // Fills the table of blocks around the macroblock: left column (x = -1), top row (y = -1), top-right
 // (4, -1), top-left (-1, -1); (4, y >= 0) is never available; inside slots are unused.
-static __device__ void load_neighbours(const AnalyseParams& __restrict__ P, WarpSmem& __restrict__ S, const ironav_mbstate* states) {
+template <class T>
+static __device__ void load_neighbours(const AnalyseParams& __restrict__ P, WarpSmem<T>& __restrict__ S, const ironav_mbstate* states) {
     const int lane = threadIdx.x & 31;
     if (lane < 30) {
         const int ex = lane % 6 - 1, ey = lane / 6 - 1;
@@ -139,13 +174,15 @@ static __device__ void load_neighbours(const AnalyseParams& __restrict__ P, Warp
 
 // nb_motion for the block at (x, y) relative to the macroblock; inside it, `cur` holds the decided
 // blocks (nullptr: none decided).
-static __device__ __forceinline__ Blk nb(const AnalyseParams& __restrict__ P, WarpSmem& __restrict__ S, const Blk* cur, int x, int y) {
+template <class T>
+static __device__ __forceinline__ Blk nb(const AnalyseParams& __restrict__ P, WarpSmem<T>& __restrict__ S, const Blk* cur, int x, int y) {
     if (x >= 0 && x < 4 && y >= 0) return cur ? cur[y * 4 + x] : make_int4(0, 0, -1, 0);
     return S.ext[(y + 1) * 6 + (x + 1)];
 }
 
 // pred_mv, enc/frame.rs:543-570
-static __device__ __forceinline__ int2 pred_mv(const AnalyseParams& __restrict__ P, WarpSmem& __restrict__ S, const Blk* cur, int bx, int by, int w, int dir, int rf) {
+template <class T>
+static __device__ __forceinline__ int2 pred_mv(const AnalyseParams& __restrict__ P, WarpSmem<T>& __restrict__ S, const Blk* cur, int bx, int by, int w, int dir, int rf) {
     const Blk a = nb(P, S, cur, bx - 1, by), b = nb(P, S, cur, bx, by - 1);
     Blk c = nb(P, S, cur, bx + w, by - 1);
     if (!c.w) c = nb(P, S, cur, bx - 1, by - 1);
@@ -164,7 +201,8 @@ static __device__ __forceinline__ int2 pred_mv(const AnalyseParams& __restrict__
 }
 
 // skip_mv, enc/frame.rs:597-603
-static __device__ int2 skip_mv(const AnalyseParams& __restrict__ P, WarpSmem& __restrict__ S) {
+template <class T>
+static __device__ int2 skip_mv(const AnalyseParams& __restrict__ P, WarpSmem<T>& __restrict__ S) {
     const Blk a = nb(P, S, nullptr, -1, 0), b = nb(P, S, nullptr, 0, -1);
     if (!a.w || !b.w || (a.z == 0 && a.x == 0 && a.y == 0) || (b.z == 0 && b.x == 0 && b.y == 0)) return make_int2(0, 0);
     return pred_mv(P, S, nullptr, 0, 0, 4, 0, 0);
@@ -173,31 +211,52 @@ static __device__ int2 skip_mv(const AnalyseParams& __restrict__ P, WarpSmem& __
 // ---- scoring -------------------------------------------------------------------------------------
 
 // Integer SAD (sad_int, enc/frame.rs:662-671) of the partition at this lane's candidate (px, py): g0 is the
-// reference plane G at the partition's origin, src the partition's first source word, w x h its size.
-// The lanes of a group (same lane & 7) share a candidate and split its rows; every lane of the group gets
-// the sum.
+// reference plane G at the partition's origin (a byte address), src the partition's first source word, w x h
+// its size, sw the plane stride in samples. The lanes of a group (same lane & 7) share a candidate and split
+// its rows; every lane of the group gets the sum. Rows are read as aligned 32-bit words realigned with funnel
+// shifts: 4 samples a word compared with __vsadu4 (8-bit), 2 with __vsadu2 (16-bit).
+template <class T>
 static __device__ __forceinline__ int sad_lane(const uint8_t* __restrict__ g0, const uint32_t* __restrict__ src, int sw, int w,
                                                int h, int px, int py, bool valid) {
+    constexpr int B = sizeof(T);
     const int lane = threadIdx.x & 31;
     int sad = 0;
     if (!valid) px = py = 0;  // scored at a position always inside the planes, and discarded: no divergent branch
     {
         const int row0 = lane >> 3;
-        const uint8_t* G = g0 + ((py >> 2) + row0) * sw + (px >> 2);
-        const int step4 = 4 * sw;
+        const uint8_t* G = g0 + (((py >> 2) + row0) * sw + (px >> 2)) * B;
+        const int step4 = 4 * sw * B;
         for (int row = row0; row < h; row += 4, G += step4) {
             const uintptr_t a = reinterpret_cast<uintptr_t>(G);
             const uint32_t* q = reinterpret_cast<const uint32_t*>(a & ~uintptr_t(3));
             const unsigned sh = (unsigned)(a & 3) * 8u;
-            const uint32_t* sr = src + row * 4;
-            const uint32_t w0 = __ldg(q), w1 = __ldg(q + 1);
-            sad += __vsadu4(sr[0], __funnelshift_r(w0, w1, sh));
-            if (w >= 8) {
-                const uint32_t w2 = __ldg(q + 2);
-                sad += __vsadu4(sr[1], __funnelshift_r(w1, w2, sh));
-                if (w == 16) {
+            const uint32_t* sr = src + row * 4 * B;
+            if constexpr (B == 1) {
+                const uint32_t w0 = __ldg(q), w1 = __ldg(q + 1);
+                sad += __vsadu4(sr[0], __funnelshift_r(w0, w1, sh));
+                if (w >= 8) {
+                    const uint32_t w2 = __ldg(q + 2);
+                    sad += __vsadu4(sr[1], __funnelshift_r(w1, w2, sh));
+                    if (w == 16) {
+                        const uint32_t w3 = __ldg(q + 3), w4 = __ldg(q + 4);
+                        sad += __vsadu4(sr[2], __funnelshift_r(w2, w3, sh)) + __vsadu4(sr[3], __funnelshift_r(w3, w4, sh));
+                    }
+                }
+            } else {
+                const uint32_t w0 = __ldg(q), w1 = __ldg(q + 1), w2 = __ldg(q + 2);
+                sad += __vsadu2(sr[0], __funnelshift_r(w0, w1, sh)) + __vsadu2(sr[1], __funnelshift_r(w1, w2, sh));
+                if (w >= 8) {
                     const uint32_t w3 = __ldg(q + 3), w4 = __ldg(q + 4);
-                    sad += __vsadu4(sr[2], __funnelshift_r(w2, w3, sh)) + __vsadu4(sr[3], __funnelshift_r(w3, w4, sh));
+                    sad += __vsadu2(sr[2], __funnelshift_r(w2, w3, sh)) + __vsadu2(sr[3], __funnelshift_r(w3, w4, sh));
+                    if (w == 16) {
+                        uint32_t pv = w4;
+#pragma unroll
+                        for (int k = 4; k < 8; k++) {
+                            const uint32_t nx = __ldg(q + k + 1);
+                            sad += __vsadu2(sr[k], __funnelshift_r(pv, nx, sh));
+                            pv = nx;
+                        }
+                    }
                 }
             }
         }
@@ -210,12 +269,14 @@ static __device__ __forceinline__ int sad_lane(const uint8_t* __restrict__ g0, c
 // Quarter-sample prediction (HalfPel::predict, enc/subpel.rs:122-145) of the partition at 4x4 block
 // (bx, by), (4 << lgw) x (4 << lgh) samples, scored by SATD (satd, enc/frame.rs:641-659), or by SAD
 // when `sad` (the P_Skip test), for the n vectors S.cand[0..n); the sums land in S.cost[0..n).
-static __device__ __forceinline__ void pred_batch(const AnalyseParams& __restrict__ P, WarpSmem& __restrict__ S, int r, int bx, int by, int lgw, int lgh, int n, bool sad) {
+template <class T>
+static __device__ __forceinline__ void pred_batch(const AnalyseParams& __restrict__ P, WarpSmem<T>& __restrict__ S, int r, int bx, int by, int lgw, int lgh, int n, bool sad) {
     const int lane = threadIdx.x & 31;
     const int lg = lgw + lgh, total = n << lg, w = 4 << lgw, h = 4 << lgh;
     if (lane < n) S.cost[lane] = 0;
     __syncwarp();
     const int x0 = S.mbx * 16 + bx * 4, y0 = S.mby * 16 + by * 4;
+    constexpr int B = sizeof(T);
     const uint8_t* base = P.planes[r];
     const int sw = P.sw, psize = (int)P.psize;
     for (int t = lane; t < total; t += 32) {
@@ -226,30 +287,57 @@ static __device__ __forceinline__ void pred_batch(const AnalyseParams& __restric
         const unsigned m = mix_entry(mv.x & 3, mv.y & 3);
         const int pa = m & 3, ax = (m >> 2) & 1, ay = (m >> 3) & 1, pb = (m >> 4) & 3, bbx = (m >> 6) & 1, bby = (m >> 7) & 1;
         const bool same = (m & 0xf) == (m >> 4);
-        // every row of a plane block has the same alignment (sw is a multiple of 16)
-        const uintptr_t ua = reinterpret_cast<uintptr_t>(base + (unsigned)(pa * psize + (iy + ay) * sw + ix + ax));
+        // every row of a plane block has the same alignment (sw is a multiple of 16); a row of 4 samples is
+        // B words (B = sizeof(T)), read as B + 1 aligned words
+        const uintptr_t ua = reinterpret_cast<uintptr_t>(base + (unsigned)(pa * psize + (iy + ay) * sw + ix + ax) * B);
         const uint32_t* qa = reinterpret_cast<const uint32_t*>(ua & ~uintptr_t(3));
         const unsigned sha = (unsigned)(ua & 3) * 8u;
-        const int swq = sw >> 2;
-        uint32_t pr[4], sr[4];
+        const int swq = (sw * B) >> 2;
+        uint32_t pr[4][B], sr[4][B];
 #pragma unroll
-        for (int row = 0; row < 4; row++) pr[row] = __funnelshift_r(__ldg(qa + row * swq), __ldg(qa + row * swq + 1), sha);
+        for (int row = 0; row < 4; row++) {
+            uint32_t pv = __ldg(qa + row * swq);
+#pragma unroll
+            for (int k = 0; k < B; k++) {
+                const uint32_t nx = __ldg(qa + row * swq + k + 1);
+                pr[row][k] = __funnelshift_r(pv, nx, sha);
+                pv = nx;
+            }
+        }
         if (!same) {
-            const uintptr_t ub = reinterpret_cast<uintptr_t>(base + (unsigned)(pb * psize + (iy + bby) * sw + ix + bbx));
+            const uintptr_t ub = reinterpret_cast<uintptr_t>(base + (unsigned)(pb * psize + (iy + bby) * sw + ix + bbx) * B);
             const uint32_t* qb = reinterpret_cast<const uint32_t*>(ub & ~uintptr_t(3));
             const unsigned shb = (unsigned)(ub & 3) * 8u;
 #pragma unroll
-            for (int row = 0; row < 4; row++)
-                pr[row] = __vavgu4(pr[row], __funnelshift_r(__ldg(qb + row * swq), __ldg(qb + row * swq + 1), shb));
-        }
-        const uint32_t* s = &S.src[(by + byy) * 16 + bx + bxx];
+            for (int row = 0; row < 4; row++) {
+                uint32_t pv = __ldg(qb + row * swq);
 #pragma unroll
-        for (int row = 0; row < 4; row++) sr[row] = s[row * 4];
-        int v;
+                for (int k = 0; k < B; k++) {
+                    const uint32_t nx = __ldg(qb + row * swq + k + 1);
+                    const uint32_t o = __funnelshift_r(pv, nx, shb);
+                    pr[row][k] = B == 1 ? __vavgu4(pr[row][k], o) : __vavgu2(pr[row][k], o);
+                    pv = nx;
+                }
+            }
+        }
+        const uint32_t* sp = &S.src[((by + byy) * 16 + bx + bxx) * B];
+#pragma unroll
+        for (int row = 0; row < 4; row++)
+#pragma unroll
+            for (int k = 0; k < B; k++) sr[row][k] = sp[row * 4 * B + k];
+        int v = 0;
         if (sad) {
-            v = __vsadu4(sr[0], pr[0]) + __vsadu4(sr[1], pr[1]) + __vsadu4(sr[2], pr[2]) + __vsadu4(sr[3], pr[3]);
+#pragma unroll
+            for (int row = 0; row < 4; row++)
+#pragma unroll
+                for (int k = 0; k < B; k++) v += B == 1 ? __vsadu4(sr[row][k], pr[row][k]) : __vsadu2(sr[row][k], pr[row][k]);
         } else {
-            v = satd4_packed(sr, pr);
+            if constexpr (B == 1) {
+                const uint32_t s1[4] = {sr[0][0], sr[1][0], sr[2][0], sr[3][0]}, p1[4] = {pr[0][0], pr[1][0], pr[2][0], pr[3][0]};
+                v = satd4_packed(s1, p1);
+            } else {
+                v = satd4_packed16(sr, pr);
+            }
         }
         atomicAdd(&S.cost[c], v);
     }
@@ -261,7 +349,8 @@ static __device__ __forceinline__ void pred_batch(const AnalyseParams& __restric
 // One diamond round whose moves were bent by the search clamps: the reference's four moves replayed
 // against the scored 3x3 square (S.cost[0..9), centre at 4), scoring on demand the points it lacks.
 // Returns whether the best moved.
-static __device__ __noinline__ int4 round_clamped(const AnalyseParams& __restrict__ P, WarpSmem& __restrict__ S, int r, int bx, int by, int w, int h, int mvpx, int mvpy, int step, int cxlo,
+template <class T>
+static __device__ __noinline__ int4 round_clamped(const AnalyseParams& __restrict__ P, WarpSmem<T>& __restrict__ S, int r, int bx, int by, int w, int h, int mvpx, int mvpy, int step, int cxlo,
                                            int cxhi, int cylo, int cyhi, int bxv, int byv, int bc) {
     const int lane = threadIdx.x & 31;
     const int cx = bxv, cy = byv;
@@ -280,8 +369,8 @@ static __device__ __noinline__ int4 round_clamped(const AnalyseParams& __restric
         if (ix >= 0 && iy >= 0) {
             v = S.cost[iy * 3 + ix];
         } else {
-            const uint8_t* g0 = P.planes[r] + (S.mby * 16 + by * 4 + PAD) * P.sw + S.mbx * 16 + bx * 4 + PAD;
-            const int s1 = sad_lane(g0, &S.src[by * 16 + bx], P.sw, w, h, nx, ny, (lane & 7) == 0);
+            const uint8_t* g0 = P.planes[r] + ((S.mby * 16 + by * 4 + PAD) * P.sw + S.mbx * 16 + bx * 4 + PAD) * (int)sizeof(T);
+            const int s1 = sad_lane<T>(g0, &S.src[(by * 16 + bx) * (int)sizeof(T)], P.sw, w, h, nx, ny, (lane & 7) == 0);
             v = __shfl_sync(FULL, s1, 0) + P.lambda * mvd_bits_d(nx, ny, mvpx, mvpy);
         }
         if (v < bc) {
@@ -296,7 +385,8 @@ static __device__ __noinline__ int4 round_clamped(const AnalyseParams& __restric
 
 // Returns the best vector in (ox, oy) and its cost without the vector's bits. (e0x, e0y) and
 // (e1x, e1y) are the extra candidates (nextra of them).
-static __device__ __noinline__ int4 motion_search(const AnalyseParams& __restrict__ P, WarpSmem& __restrict__ S, int r, int bx, int by, int w4, int h4, int mvpx, int mvpy, int e0x, int e0y,
+template <class T>
+static __device__ __noinline__ int4 motion_search(const AnalyseParams& __restrict__ P, WarpSmem<T>& __restrict__ S, int r, int bx, int by, int w4, int h4, int mvpx, int mvpy, int e0x, int e0y,
                                           int e1x, int e1y, int nextra) {
     const int lane = threadIdx.x & 31;
     const int lam = P.lambda;
@@ -330,9 +420,9 @@ static __device__ __noinline__ int4 motion_search(const AnalyseParams& __restric
         valid = false;
     }
     const int sw = P.sw;
-    const uint8_t* const g0 = P.planes[r] + (y0 + PAD) * sw + x0 + PAD;
-    const uint32_t* const src0 = &S.src[by * 16 + bx];
-    int cost = sad_lane(g0, src0, sw, w, h, px, py, valid);
+    const uint8_t* const g0 = P.planes[r] + ((y0 + PAD) * sw + x0 + PAD) * (int)sizeof(T);
+    const uint32_t* const src0 = &S.src[(by * 16 + bx) * (int)sizeof(T)];
+    int cost = sad_lane<T>(g0, src0, sw, w, h, px, py, valid);
     cost = valid ? cost + lam * mvd_bits_d(px, py, mvpx, mvpy) : BIG;
     const unsigned vmask = __ballot_sync(FULL, valid) & 0xffu;
     if (lane == 0) S.sad_px += (uint32_t)(__popc(vmask) * w * h);
@@ -355,7 +445,7 @@ static __device__ __noinline__ int4 motion_search(const AnalyseParams& __restric
             const int cx = bxv, cy = byv, c0 = bc;
             const int X0 = clx(cx - step), X2 = clx(cx + step), Y0 = cly(cy - step), Y2 = cly(cy + step);
             const int qx = kx == 0 ? X0 : (kx == 1 ? cx : X2), qy = ky == 0 ? Y0 : (ky == 1 ? cy : Y2);
-            const int sc = sad_lane(g0, src0, sw, w, h, qx, qy, true) + lam * mvd_bits_d(qx, qy, mvpx, mvpy);
+            const int sc = sad_lane<T>(g0, src0, sw, w, h, qx, qy, true) + lam * mvd_bits_d(qx, qy, mvpx, mvpy);
             if (lane == 0) S.sad_px += (uint32_t)(4 * w * h);
             bool moved;
             if (X0 == cx - step && X2 == cx + step && Y0 == cy - step && Y2 == cy + step) {
@@ -453,18 +543,21 @@ static __device__ __noinline__ int4 motion_search(const AnalyseParams& __restric
 
 // ---- partition decision ----------------------------------------------------------------------------
 
-static __device__ __forceinline__ void blk_clear(const AnalyseParams& __restrict__ P, WarpSmem& __restrict__ S, Blk* b) {
+template <class T>
+static __device__ __forceinline__ void blk_clear(const AnalyseParams& __restrict__ P, WarpSmem<T>& __restrict__ S, Blk* b) {
     const int lane = threadIdx.x & 31;
     if (lane < 16) b[lane] = make_int4(0, 0, -1, 0);
     __syncwarp();
 }
-static __device__ __forceinline__ void blk_copy(const AnalyseParams& __restrict__ P, WarpSmem& __restrict__ S, Blk* d, const Blk* s) {
+template <class T>
+static __device__ __forceinline__ void blk_copy(const AnalyseParams& __restrict__ P, WarpSmem<T>& __restrict__ S, Blk* d, const Blk* s) {
     const int lane = threadIdx.x & 31;
     if (lane < 16) d[lane] = s[lane];
     __syncwarp();
 }
 // Marks rectangle (x, y, w, h) of `b` as decided with vector (mx, my) and reference rf.
-static __device__ __forceinline__ void blk_paint(const AnalyseParams& __restrict__ P, WarpSmem& __restrict__ S, Blk* b, int x, int y, int w, int h, int mx, int my, int rf) {
+template <class T>
+static __device__ __forceinline__ void blk_paint(const AnalyseParams& __restrict__ P, WarpSmem<T>& __restrict__ S, Blk* b, int x, int y, int w, int h, int mx, int my, int rf) {
     const int lane = threadIdx.x & 31;
     if (lane < 16) {
         const int bx = lane & 3, by = lane >> 2;
@@ -475,7 +568,8 @@ static __device__ __forceinline__ void blk_paint(const AnalyseParams& __restrict
 
 // sub_search, enc/frame.rs:911-938: returns sub_mb_type, its cost in cost_out; leaves the 8x8
 // block's vectors in S.st.
-static __device__ __noinline__ int2 sub_search(const AnalyseParams& __restrict__ P, WarpSmem& __restrict__ S, int r, int k, int ex, int ey) {
+template <class T>
+static __device__ __noinline__ int2 sub_search(const AnalyseParams& __restrict__ P, WarpSmem<T>& __restrict__ S, int r, int k, int ex, int ey) {
     const int lam = P.lambda;
     const int ox = (k & 1) * 2, oy = (k >> 1) * 2;
     const int ns = P.sub8 ? 4 : 1;
@@ -502,7 +596,8 @@ static __device__ __noinline__ int2 sub_search(const AnalyseParams& __restrict__
 }
 
 // best_inter_ref, enc/frame.rs:852-905. Leaves the winner's vectors in S.best_mvs.
-static __device__ __noinline__ int4 best_inter_ref(const AnalyseParams& __restrict__ P, WarpSmem& __restrict__ S, int r) {
+template <class T>
+static __device__ __noinline__ int4 best_inter_ref(const AnalyseParams& __restrict__ P, WarpSmem<T>& __restrict__ S, int r) {
     const int lane = threadIdx.x & 31;
     const int lam = P.lambda;
     int rb = 0;
@@ -593,11 +688,14 @@ static __device__ __noinline__ int4 best_inter_ref(const AnalyseParams& __restri
 
 // ---- one macroblock --------------------------------------------------------------------------------
 
-static __device__ void analyse(const AnalyseParams& __restrict__ P, WarpSmem& __restrict__ S, bool auto_policy) {
+template <class T>
+static __device__ void analyse(const AnalyseParams& __restrict__ P, WarpSmem<T>& __restrict__ S, bool auto_policy) {
     const int lane = threadIdx.x & 31;
-    // the current macroblock: 16 rows of 16 bytes, as 128-bit loads
-    if (lane < 16) {
-        const uint4 v = *reinterpret_cast<const uint4*>(P.src + (size_t)(S.mby * 16 + lane) * P.ls + S.mbx * 16);
+    // the current macroblock: 16 rows of 16 samples, as 128-bit loads (sizeof(T) per row)
+    constexpr int B = sizeof(T);
+    if (lane < 16 * B) {
+        const int row = lane / B, part = lane % B;
+        const uint4 v = *reinterpret_cast<const uint4*>(P.src + ((size_t)(S.mby * 16 + row) * P.ls + S.mbx * 16) * B + part * 16);
         S.src[lane * 4 + 0] = v.x;
         S.src[lane * 4 + 1] = v.y;
         S.src[lane * 4 + 2] = v.z;
@@ -754,7 +852,8 @@ static __device__ bool wait_committed(const AnalyseParams& P, int m) {
 
 // The neighbours of an in-loop macroblock from the caller's committed decisions (host memory: read
 // around the caches, after the acquire of their flags).
-static __device__ void load_committed(const AnalyseParams& __restrict__ P, WarpSmem& __restrict__ S) {
+template <class T>
+static __device__ void load_committed(const AnalyseParams& __restrict__ P, WarpSmem<T>& __restrict__ S) {
     const int lane = threadIdx.x & 31;
     if (lane < 30) {
         const int ex = lane % 6 - 1, ey = lane / 6 - 1;
@@ -782,11 +881,11 @@ static __device__ void load_committed(const AnalyseParams& __restrict__ P, WarpS
     __syncwarp();
 }
 
-template <int MODE>
+template <int MODE, class T>
 __global__ void __launch_bounds__(K2_WARPS * 32, K2_MIN_BLOCKS) analyse_kernel(const __grid_constant__ AnalyseParams P) {
-    __shared__ WarpSmem smem[K2_WARPS];
+    __shared__ WarpSmem<T> smem[K2_WARPS];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    WarpSmem& S = smem[wid];
+    WarpSmem<T>& S = smem[wid];
     for (;;) {
         unsigned t = 0;
         if (lane == 0) t = atomicAdd(P.ticket, 1u);

@@ -54,7 +54,7 @@ __global__ void __launch_bounds__(K1_THREADS) planes_batch_kernel(const PlaneJob
     const int j = find_job(jobs, njobs, (int)blockIdx.x, [](const PlaneJob& p) { return p.tile0; });
     const PlaneJob& J = jobs[j];
     const int t = (int)blockIdx.x - J.tile0;
-    planes_tile(J.luma, J.stride, J.w, J.h, J.out, J.psize, J.sw, J.sh, (t % J.tiles_x) * K1_TW, (t / J.tiles_x) * K1_TH);
+    planes_tile(J.luma, J.stride, J.w, J.h, J.out, J.psize, J.sw, J.sh, (t % J.tiles_x) * K1_TW, (t / J.tiles_x) * K1_TH, 255);
 }
 
 // col_mv, enc/frame.rs:944-947, for every stream's new reference
@@ -90,9 +90,9 @@ __global__ void __launch_bounds__(K2_WARPS * 32, K2_MIN_BLOCKS) analyse_batch_ke
                                                                                      const uint32_t* __restrict__ order,
                                                                                      unsigned ntickets, unsigned* ticket,
                                                                                      const unsigned* err) {
-    __shared__ WarpSmem smem[K2_WARPS];
+    __shared__ WarpSmem<uint8_t> smem[K2_WARPS];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    WarpSmem& S = smem[wid];
+    WarpSmem<uint8_t>& S = smem[wid];
     for (;;) {
         unsigned t = 0;
         if (lane == 0) t = atomicAdd(ticket, 1u);
@@ -173,7 +173,7 @@ extern "C" int ironav_batch_create(ironav_batch** out, ironav_ctx* const* ctxs, 
     if (!out || !ctxs || n < 1 || n > 4096) return IRONAV_INVALID_ARGUMENT;
     *out = nullptr;
     for (int i = 0; i < n; i++)
-        if (!ctxs[i] || ctxs[i]->stream != ctxs[0]->stream || ctxs[i]->nmb > (1 << 20)) return IRONAV_INVALID_ARGUMENT;
+        if (!ctxs[i] || ctxs[i]->bd != 8 || ctxs[i]->stream != ctxs[0]->stream || ctxs[i]->nmb > (1 << 20)) return IRONAV_INVALID_ARGUMENT;
     ironav_batch* b = new ironav_batch();
     b->ctx.assign(ctxs, ctxs + n);
     b->n = n;

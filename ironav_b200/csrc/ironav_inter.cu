@@ -107,10 +107,19 @@ void free_ctx(ironav_ctx* c) {
     delete c;
 }
 
-int launch_planes(ironav_ctx* c, const uint8_t* d_luma, int stride, int w, int h, const ironav_mbstate* d_col) {
+// Bytes per sample: 1 for 8-bit pictures, 2 (uint16_t) above.
+inline int sample_bytes(const ironav_ctx* c) { return c->bd > 8 ? 2 : 1; }
+
+int launch_planes(ironav_ctx* c, const void* d_luma, int stride, int w, int h, const ironav_mbstate* d_col) {
     const int slot = take_ref_slot(c);
     dim3 grid((c->sw + K1_TW - 1) / K1_TW, (c->sh + K1_TH - 1) / K1_TH);
-    halfpel_planes_kernel<<<grid, K1_THREADS, 0, c->stream>>>(d_luma, stride, w, h, c->d_planes[slot], c->psize, c->sw, c->sh);
+    const int maxv = (1 << c->bd) - 1;
+    if (c->bd > 8)
+        halfpel_planes_kernel<uint16_t><<<grid, K1_THREADS, 0, c->stream>>>(static_cast<const uint16_t*>(d_luma), stride, w, h,
+                                                                           reinterpret_cast<uint16_t*>(c->d_planes[slot]), c->psize, c->sw, c->sh, maxv);
+    else
+        halfpel_planes_kernel<uint8_t><<<grid, K1_THREADS, 0, c->stream>>>(static_cast<const uint8_t*>(d_luma), stride, w, h, c->d_planes[slot],
+                                                                          c->psize, c->sw, c->sh, maxv);
     col_extract_kernel<<<(c->nmb + 255) / 256, 256, 0, c->stream>>>(d_col, c->d_col[slot], c->nmb);
     return cuda_status(cudaGetLastError());
 }
@@ -130,10 +139,13 @@ int launch_analyse(ironav_ctx* c, bool auto_mode, const ironav_mbstate* d_in, ir
     p.wait_limit = c->wait_limit;
     if (auto_mode) p.epoch = ++c->epoch;
     CK(cudaMemsetAsync(c->d_counters, 0, 2 * sizeof(unsigned), c->stream));
-    if (auto_mode)
-        analyse_kernel<MODE_AUTO><<<c->k2_blocks, K2_WARPS * 32, 0, c->stream>>>(p);
-    else
-        analyse_kernel<MODE_REPLAY><<<c->k2_blocks, K2_WARPS * 32, 0, c->stream>>>(p);
+    if (c->bd > 8) {
+        if (auto_mode) analyse_kernel<MODE_AUTO, uint16_t><<<c->k2_blocks, K2_WARPS * 32, 0, c->stream>>>(p);
+        else analyse_kernel<MODE_REPLAY, uint16_t><<<c->k2_blocks, K2_WARPS * 32, 0, c->stream>>>(p);
+    } else {
+        if (auto_mode) analyse_kernel<MODE_AUTO, uint8_t><<<c->k2_blocks, K2_WARPS * 32, 0, c->stream>>>(p);
+        else analyse_kernel<MODE_REPLAY, uint8_t><<<c->k2_blocks, K2_WARPS * 32, 0, c->stream>>>(p);
+    }
     return cuda_status(cudaGetLastError());
 }
 
@@ -143,6 +155,44 @@ int check_device_error(ironav_ctx* c) {
     CK(cudaStreamSynchronize(c->stream));
     if (err & 1u) return IRONAV_TIMEOUT;
     if (err) return IRONAV_INTERNAL;
+    return IRONAV_OK;
+}
+
+// ---- scene-cut measure ----------------------------------------------------------------------------
+
+int scene_alloc(ironav_ctx* c) {
+    if (c->d_lowres) return IRONAV_OK;
+    const size_t B = (size_t)sample_bytes(c);
+    const size_t lsz = (size_t)(c->mb_w * 4) * (c->mb_h * 4) * B + 64;  // slack: rows are read as whole words
+    CK(cudaMalloc(&c->d_scene_luma, 2 * (size_t)c->width * c->height * B));
+    CK(cudaMalloc(&c->d_lowres, 2 * lsz));
+    CK(cudaMalloc(&c->d_scene_sums, 2 * sizeof(unsigned long long)));
+    CK(cudaMemset(c->d_lowres, 0, 2 * lsz));
+    return IRONAV_OK;
+}
+
+template <class T>
+void scene_kernels(ironav_ctx* c, const void* d_prev, int sp, const void* d_cur, int sc) {
+    const int lw = c->mb_w * 4, lh = c->mb_h * 4;
+    const size_t lsz = (size_t)lw * lh * sizeof(T) + 64;
+    T* lp = reinterpret_cast<T*>(c->d_lowres);
+    T* lc = reinterpret_cast<T*>(c->d_lowres + lsz);
+    lowres_kernel<T><<<(lw * lh + 255) / 256, 256, 0, c->stream>>>(static_cast<const T*>(d_prev), sp, c->width, c->height, lw, lh, lp);
+    lowres_kernel<T><<<(lw * lh + 255) / 256, 256, 0, c->stream>>>(static_cast<const T*>(d_cur), sc, c->width, c->height, lw, lh, lc);
+    cudaMemsetAsync(c->d_scene_sums, 0, 2 * sizeof(unsigned long long), c->stream);
+    const int nb = (lw >= 8 && lh >= 8) ? ((lw - 8) / 8 + 1) * ((lh - 8) / 8 + 1) : 0;
+    if (nb > 0) change_kernel<T><<<(nb + 3) / 4, 128, 0, c->stream>>>(lp, lc, lw, lh, c->d_scene_sums);
+}
+
+int scene_run(ironav_ctx* c, const void* d_prev, int sp, const void* d_cur, int sc, int64_t* out) {
+    if (c->bd > 8) scene_kernels<uint16_t>(c, d_prev, sp, d_cur, sc);
+    else scene_kernels<uint8_t>(c, d_prev, sp, d_cur, sc);
+    CK(cudaGetLastError());
+    unsigned long long h[2];
+    CK(cudaMemcpyAsync(h, c->d_scene_sums, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    out[0] = (int64_t)h[0];
+    out[1] = (int64_t)h[1];
     return IRONAV_OK;
 }
 
@@ -170,7 +220,8 @@ const char* ironav_version(void) { return "cuda-sm_100a ironav-inter-b200 0.1 (K
 int ironav_ctx_create(ironav_ctx** out, int width, int height, int bd, int max_refs, int nslices, const int* band_rows) {
     if (!out) return IRONAV_INVALID_ARGUMENT;
     *out = nullptr;
-    if (width <= 0 || height <= 0 || (width & 1) || (height & 1) || bd != 8) return IRONAV_INVALID_ARGUMENT;
+    // 8-bit (Yuv420p) or 10-bit (Yuv420p10) pictures, the encoder's two formats (enc/mod.rs:140-143)
+    if (width <= 0 || height <= 0 || (width & 1) || (height & 1) || (bd != 8 && bd != 10)) return IRONAV_INVALID_ARGUMENT;
     const int mb_w = (width + 15) / 16, mb_h = (height + 15) / 16;
     if (mb_w > 1024 || mb_h > 1024 || max_refs < 1 || max_refs > MAX_REFS || nslices < 1 || nslices > mb_h)
         return IRONAV_INVALID_ARGUMENT;
@@ -187,6 +238,7 @@ int ironav_ctx_create(ironav_ctx** out, int width, int height, int bd, int max_r
     ironav_ctx* c = new ironav_ctx();
     c->width = width;
     c->height = height;
+    c->bd = bd;
     c->mb_w = mb_w;
     c->mb_h = mb_h;
     c->pw = mb_w * 16;
@@ -208,13 +260,16 @@ int ironav_ctx_create(ironav_ctx** out, int width, int height, int bd, int max_r
     if ((e = cudaGetDeviceProperties(&prop, c->device)) != cudaSuccess) return fail(e);
     c->nsm = prop.multiProcessorCount;
     int per_sm = 0;
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, analyse_kernel<MODE_AUTO>, K2_WARPS * 32, 0)) != cudaSuccess) return fail(e);
+    e = bd > 8 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, analyse_kernel<MODE_AUTO, uint16_t>, K2_WARPS * 32, 0)
+               : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, analyse_kernel<MODE_AUTO, uint8_t>, K2_WARPS * 32, 0);
+    if (e != cudaSuccess) return fail(e);
     c->k2_blocks = std::max(1, per_sm) * c->nsm;
     const size_t slack = 256;  // word-granular reads may touch a few bytes past a plane's last sample
-    if ((e = cudaMalloc(&c->d_src, (size_t)c->pw * c->ph + slack)) != cudaSuccess) return fail(e);
-    if ((e = cudaMalloc(&c->d_stage, (size_t)c->pw * c->ph + slack)) != cudaSuccess) return fail(e);
+    const size_t bytes = (size_t)sample_bytes(c);
+    if ((e = cudaMalloc(&c->d_src, (size_t)c->pw * c->ph * bytes + slack)) != cudaSuccess) return fail(e);
+    if ((e = cudaMalloc(&c->d_stage, (size_t)c->pw * c->ph * bytes + slack)) != cudaSuccess) return fail(e);
     for (int i = 0; i < max_refs; i++) {
-        if ((e = cudaMalloc(&c->d_planes[i], 4 * (size_t)c->psize + slack)) != cudaSuccess) return fail(e);
+        if ((e = cudaMalloc(&c->d_planes[i], 4 * (size_t)c->psize * bytes + slack)) != cudaSuccess) return fail(e);
         if ((e = cudaMalloc(&c->d_col[i], sizeof(ColMv) * c->nmb)) != cudaSuccess) return fail(e);
     }
     if ((e = cudaMalloc(&c->d_band_start, sizeof(int) * mb_h)) != cudaSuccess) return fail(e);
@@ -272,24 +327,27 @@ int ironav_ctx_set_stream(ironav_ctx* c, void* s) {
     return IRONAV_OK;
 }
 
-int ironav_set_source_device(ironav_ctx* c, const uint8_t* d_y, int stride) {
-    if (!c || !d_y || stride < c->width) return IRONAV_INVALID_ARGUMENT;
-    CK(cudaMemcpy2DAsync(c->d_src, c->pw, d_y, stride, c->width, c->height, cudaMemcpyDeviceToDevice, c->stream));
+// The padded source from a picture whose rows are `stride` samples apart (kind: the copy's direction).
+static int load_source(ironav_ctx* c, const void* y, int stride, cudaMemcpyKind kind) {
+    const int B = sample_bytes(c);
+    CK(cudaMemcpy2DAsync(c->d_src, (size_t)c->pw * B, y, (size_t)stride * B, (size_t)c->width * B, c->height, kind, c->stream));
     if (c->width != c->pw || c->height != c->ph) {
         dim3 grid((c->pw + 255) / 256, c->ph);
-        pad_edges_kernel<<<grid, 256, 0, c->stream>>>(c->d_src, c->width, c->height, c->pw, c->ph);
+        if (B == 2) pad_edges_kernel<uint16_t><<<grid, 256, 0, c->stream>>>(reinterpret_cast<uint16_t*>(c->d_src), c->width, c->height, c->pw, c->ph);
+        else pad_edges_kernel<uint8_t><<<grid, 256, 0, c->stream>>>(c->d_src, c->width, c->height, c->pw, c->ph);
     }
     return cuda_status(cudaGetLastError());
 }
 
-int ironav_set_source(ironav_ctx* c, const uint8_t* y, int stride) {
+int ironav_set_source_device(ironav_ctx* c, const void* d_y, int stride) {
+    if (!c || !d_y || stride < c->width) return IRONAV_INVALID_ARGUMENT;
+    return load_source(c, d_y, stride, cudaMemcpyDeviceToDevice);
+}
+
+int ironav_set_source(ironav_ctx* c, const void* y, int stride) {
     if (!c || !y || stride < c->width) return IRONAV_INVALID_ARGUMENT;
-    CK(cudaMemcpy2DAsync(c->d_src, c->pw, y, stride, c->width, c->height, cudaMemcpyHostToDevice, c->stream));
-    if (c->width != c->pw || c->height != c->ph) {
-        dim3 grid((c->pw + 255) / 256, c->ph);
-        pad_edges_kernel<<<grid, 256, 0, c->stream>>>(c->d_src, c->width, c->height, c->pw, c->ph);
-        CK(cudaGetLastError());
-    }
+    const int s = load_source(c, y, stride, cudaMemcpyHostToDevice);
+    if (s != IRONAV_OK) return s;
     CK(cudaStreamSynchronize(c->stream));
     return IRONAV_OK;
 }
@@ -298,14 +356,15 @@ static bool ref_size_ok(const ironav_ctx* c, int stride, int w, int h) {
     return ((w == c->width && h == c->height) || (w == c->pw && h == c->ph)) && stride >= w;
 }
 
-int ironav_push_reference_device(ironav_ctx* c, const uint8_t* d_y, int stride, int w, int h, const ironav_mbstate* d_col) {
+int ironav_push_reference_device(ironav_ctx* c, const void* d_y, int stride, int w, int h, const ironav_mbstate* d_col) {
     if (!c || !d_y || !ref_size_ok(c, stride, w, h)) return IRONAV_INVALID_ARGUMENT;
     return launch_planes(c, d_y, stride, w, h, d_col);
 }
 
-int ironav_push_reference(ironav_ctx* c, const uint8_t* y, int stride, int w, int h, const ironav_mbstate* col) {
+int ironav_push_reference(ironav_ctx* c, const void* y, int stride, int w, int h, const ironav_mbstate* col) {
     if (!c || !y || !ref_size_ok(c, stride, w, h)) return IRONAV_INVALID_ARGUMENT;
-    CK(cudaMemcpy2DAsync(c->d_stage, w, y, stride, w, h, cudaMemcpyHostToDevice, c->stream));
+    const size_t B = (size_t)sample_bytes(c);
+    CK(cudaMemcpy2DAsync(c->d_stage, w * B, y, stride * B, w * B, h, cudaMemcpyHostToDevice, c->stream));
     if (col) CK(cudaMemcpyAsync(c->d_col_stage, col, sizeof(ironav_mbstate) * c->nmb, cudaMemcpyHostToDevice, c->stream));
     int s = launch_planes(c, c->d_stage, w, w, h, col ? c->d_col_stage : nullptr);
     if (s != IRONAV_OK) return s;
@@ -320,9 +379,9 @@ int ironav_clear_references(ironav_ctx* c) {
     return IRONAV_OK;
 }
 
-int ironav_get_planes(ironav_ctx* c, int idx, uint8_t* out) {
+int ironav_get_planes(ironav_ctx* c, int idx, void* out) {
     if (!c || !out || idx < 0 || idx >= c->nrefs) return IRONAV_INVALID_ARGUMENT;
-    CK(cudaMemcpyAsync(out, c->d_planes[c->slot_of[idx]], 4 * (size_t)c->psize, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(out, c->d_planes[c->slot_of[idx]], 4 * (size_t)c->psize * sample_bytes(c), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     return IRONAV_OK;
 }
@@ -375,47 +434,19 @@ int ironav_ctx_sync(ironav_ctx* c) {
 
 // ---- scene-cut measure ---------------------------------------------------------------------------
 
-static int scene_alloc(ironav_ctx* c) {
-    if (c->d_lowres) return IRONAV_OK;
-    const size_t lsz = (size_t)(c->mb_w * 4) * (c->mb_h * 4) + 64;  // slack: rows are read as whole words
-    CK(cudaMalloc(&c->d_scene_luma, 2 * (size_t)c->width * c->height));
-    CK(cudaMalloc(&c->d_lowres, 2 * lsz));
-    CK(cudaMalloc(&c->d_scene_sums, 2 * sizeof(unsigned long long)));
-    CK(cudaMemset(c->d_lowres, 0, 2 * lsz));
-    return IRONAV_OK;
-}
-
-static int scene_run(ironav_ctx* c, const uint8_t* d_prev, int sp, const uint8_t* d_cur, int sc, int64_t* out) {
-    const int lw = c->mb_w * 4, lh = c->mb_h * 4;
-    const size_t lsz = (size_t)lw * lh + 64;
-    uint8_t* lp = c->d_lowres;
-    uint8_t* lc = c->d_lowres + lsz;
-    lowres_kernel<<<(lw * lh + 255) / 256, 256, 0, c->stream>>>(d_prev, sp, c->width, c->height, lw, lh, lp);
-    lowres_kernel<<<(lw * lh + 255) / 256, 256, 0, c->stream>>>(d_cur, sc, c->width, c->height, lw, lh, lc);
-    CK(cudaMemsetAsync(c->d_scene_sums, 0, 2 * sizeof(unsigned long long), c->stream));
-    const int nb = (lw >= 8 && lh >= 8) ? ((lw - 8) / 8 + 1) * ((lh - 8) / 8 + 1) : 0;
-    if (nb > 0) change_kernel<<<(nb + 3) / 4, 128, 0, c->stream>>>(lp, lc, lw, lh, c->d_scene_sums);
-    CK(cudaGetLastError());
-    unsigned long long h[2];
-    CK(cudaMemcpyAsync(h, c->d_scene_sums, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
-    out[0] = (int64_t)h[0];
-    out[1] = (int64_t)h[1];
-    return IRONAV_OK;
-}
-
-int ironav_scene_change(ironav_ctx* c, const uint8_t* prev_y, const uint8_t* cur_y, int stride, int64_t* out) {
+int ironav_scene_change(ironav_ctx* c, const void* prev_y, const void* cur_y, int stride, int64_t* out) {
     if (!c || !prev_y || !cur_y || !out || stride < c->width) return IRONAV_INVALID_ARGUMENT;
     int s = scene_alloc(c);
     if (s != IRONAV_OK) return s;
+    const size_t B = (size_t)sample_bytes(c);
     uint8_t* a = c->d_scene_luma;
-    uint8_t* b = c->d_scene_luma + (size_t)c->width * c->height;
-    CK(cudaMemcpy2DAsync(a, c->width, prev_y, stride, c->width, c->height, cudaMemcpyHostToDevice, c->stream));
-    CK(cudaMemcpy2DAsync(b, c->width, cur_y, stride, c->width, c->height, cudaMemcpyHostToDevice, c->stream));
+    uint8_t* b = c->d_scene_luma + (size_t)c->width * c->height * B;
+    CK(cudaMemcpy2DAsync(a, c->width * B, prev_y, stride * B, c->width * B, c->height, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpy2DAsync(b, c->width * B, cur_y, stride * B, c->width * B, c->height, cudaMemcpyHostToDevice, c->stream));
     return scene_run(c, a, c->width, b, c->width, out);
 }
 
-int ironav_scene_change_device(ironav_ctx* c, const uint8_t* d_prev, const uint8_t* d_cur, int stride, int64_t* out) {
+int ironav_scene_change_device(ironav_ctx* c, const void* d_prev, const void* d_cur, int stride, int64_t* out) {
     if (!c || !d_prev || !d_cur || !out || stride < c->width) return IRONAV_INVALID_ARGUMENT;
     int s = scene_alloc(c);
     if (s != IRONAV_OK) return s;
@@ -485,7 +516,8 @@ int ironav_inloop_begin(ironav_ctx* c, int order) {
     CK(cudaMemsetAsync(c->d_counters, 0, 2 * sizeof(unsigned), c->stream));
     // few warps: the caller's pace bounds this mode, and every waiting warp polls host memory
     const int blocks = std::min(c->k2_blocks, 64);
-    analyse_kernel<MODE_INLOOP><<<blocks, K2_WARPS * 32, 0, c->stream>>>(p);
+    if (c->bd > 8) analyse_kernel<MODE_INLOOP, uint16_t><<<blocks, K2_WARPS * 32, 0, c->stream>>>(p);
+    else analyse_kernel<MODE_INLOOP, uint8_t><<<blocks, K2_WARPS * 32, 0, c->stream>>>(p);
     CK(cudaGetLastError());
     c->inloop_active = true;
     return IRONAV_OK;

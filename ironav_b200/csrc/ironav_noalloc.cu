@@ -84,9 +84,9 @@ __global__ void noalloc_init_kernel(uint32_t* scr, const ironav_mbstate* col, in
 // neighbours always hold smaller tickets, so a waiting warp only waits on running warps.
 __global__ void __launch_bounds__(K2_WARPS * 32, K2_MIN_BLOCKS) analyse_noalloc_kernel(const __grid_constant__ AnalyseParams P, int nslices,
                                                                        int max_rows) {
-    __shared__ WarpSmem smem[K2_WARPS];
+    __shared__ WarpSmem<uint8_t> smem[K2_WARPS];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    WarpSmem& S = smem[wid];
+    WarpSmem<uint8_t>& S = smem[wid];
     const unsigned total = (unsigned)nslices * (unsigned)max_rows * (unsigned)P.mb_w;
     for (;;) {
         unsigned t = 0;
@@ -167,7 +167,7 @@ extern "C" int ironav_analyse_auto_noalloc(const uint8_t* d_src, int src_stride,
     const int init_n = nmb > mb_h ? nmb : mb_h;
     noalloc_init_kernel<<<(init_n + 255) / 256, 256, 0, s>>>(scr, d_col, nmb, mb_h, nslices);
     dim3 grid((sw + K1_TW - 1) / K1_TW, (sh + K1_TH - 1) / K1_TH);
-    halfpel_planes_kernel<<<grid, K1_THREADS, 0, s>>>(d_ref, ref_stride, ref_w, ref_h, d_planes, (long long)sw * sh, sw, sh);
+    halfpel_planes_kernel<uint8_t><<<grid, K1_THREADS, 0, s>>>(d_ref, ref_stride, ref_w, ref_h, d_planes, (long long)sw * sh, sw, sh, 255);
 
     AnalyseParams p;
     memset(&p, 0, sizeof(p));

@@ -173,18 +173,20 @@ class PictureParams:
 
 
 class InterStage:
-    """One stream's inter-analysis context (ironav_ctx)."""
+    """One stream's inter-analysis context (ironav_ctx). ``bd`` is the sample depth, 8 or 10 (the
+    encoder's Yuv420p / Yuv420p10, enc/mod.rs:140-143): luma arrays are uint8 at 8 bits and uint16 at 10."""
 
     def __init__(self, width: int, height: int, max_refs: int = 1, nslices: int = 1,
-                 band_rows: list[int] | None = None, lib: ctypes.CDLL | None = None):
+                 band_rows: list[int] | None = None, lib: ctypes.CDLL | None = None, bd: int = 8):
         self.lib = lib if lib is not None else cuda_library()
-        self.width, self.height = width, height
+        self.width, self.height, self.bd = width, height, bd
+        self.dtype = np.uint8 if bd == 8 else np.uint16
         h = _VP()
         bands = None
         if band_rows is not None:
             self._bands = np.asarray(band_rows, dtype=np.int32)
             bands = _ptr(self._bands)
-        self._check(self.lib.ironav_ctx_create(ctypes.byref(h), width, height, 8, max_refs, nslices, bands),
+        self._check(self.lib.ironav_ctx_create(ctypes.byref(h), width, height, bd, max_refs, nslices, bands),
                     "ironav_ctx_create")
         self.ctx = h
         mw, mh, sw, sh = _I(), _I(), _I(), _I()
@@ -216,13 +218,18 @@ class InterStage:
 
     # -- pictures ------------------------------------------------------------------------------------
 
+    def _luma(self, luma: np.ndarray) -> np.ndarray:
+        if luma.dtype != self.dtype:
+            raise TypeError(f"{self.bd}-bit context takes {np.dtype(self.dtype).name} luma, got {luma.dtype}")
+        return np.ascontiguousarray(luma)
+
     def set_source(self, luma: np.ndarray) -> None:
-        luma = np.ascontiguousarray(luma, dtype=np.uint8)
+        luma = self._luma(luma)
         assert luma.shape == (self.height, self.width)
         self._check(self.lib.ironav_set_source(self.ctx, _ptr(luma), self.width), "ironav_set_source")
 
     def push_reference(self, luma: np.ndarray, col: np.ndarray | None = None) -> None:
-        luma = np.ascontiguousarray(luma, dtype=np.uint8)
+        luma = self._luma(luma)
         h, w = luma.shape
         colp = None
         if col is not None:
@@ -235,7 +242,7 @@ class InterStage:
         self._check(self.lib.ironav_clear_references(self.ctx), "ironav_clear_references")
 
     def planes(self, idx: int = 0) -> np.ndarray:
-        out = np.empty((4, self.sh, self.sw), dtype=np.uint8)
+        out = np.empty((4, self.sh, self.sw), dtype=self.dtype)
         self._check(self.lib.ironav_get_planes(self.ctx, idx, _ptr(out)), "ironav_get_planes")
         return out
 
@@ -264,8 +271,8 @@ class InterStage:
 
     def scene_change(self, prev: np.ndarray, cur: np.ndarray) -> tuple[int, int]:
         """(inter, intra) totals of cur against prev on the low-resolution luma."""
-        prev = np.ascontiguousarray(prev, dtype=np.uint8)
-        cur = np.ascontiguousarray(cur, dtype=np.uint8)
+        prev = self._luma(prev)
+        cur = self._luma(cur)
         out = np.zeros(2, dtype=np.int64)
         self._check(self.lib.ironav_scene_change(self.ctx, _ptr(prev), _ptr(cur), self.width, _ptr(out)),
                     "ironav_scene_change")

@@ -63,7 +63,7 @@ class Sequence:
 
     def __init__(self, width: int, height: int, frames: int, seed: int, pan_q: int, nobj: int, vmax: float,
                  sigma: float):
-        self.width, self.height, self.frames = width, height, frames
+        self.width, self.height, self.frames, self.seed = width, height, frames, seed
         self._h = _lib().ironav_synth_create(width, height, frames, seed, pan_q, nobj, vmax, sigma)
         if not self._h:
             raise ValueError("bad synthetic sequence parameters")
@@ -81,6 +81,13 @@ class Sequence:
         if st != 0:
             raise IndexError(t)
         return out
+
+    def frame10(self, t: int) -> np.ndarray:
+        """Frame t as 10-bit luma (the encoder's Yuv420p10 input): the 8-bit frame times 4 plus two seeded
+        low bits per sample, so the low bits carry detail the 8-bit frame does not have."""
+        rng = np.random.default_rng([self.seed, t, 10])
+        low = rng.integers(0, 4, size=(self.height, self.width), dtype=np.uint16)
+        return (self.frame(t).astype(np.uint16) << 2) | low
 
     def pan(self, t: int) -> tuple[int, int]:
         qx, qy = ctypes.c_int(), ctypes.c_int()

@@ -793,7 +793,8 @@ static void refpic_free(refpic* r) {
 int ironav_ctx_create(ironav_ctx** out, int width, int height, int bd, int max_refs, int nslices, const int* band_rows) {
     if (!out) return IRONAV_INVALID_ARGUMENT;
     *out = NULL;
-    if (width <= 0 || height <= 0 || (width & 1) || (height & 1) || bd != 8) return IRONAV_INVALID_ARGUMENT;
+    /* 8-bit (Yuv420p) or 10-bit (Yuv420p10) pictures, enc/mod.rs:140-143 */
+    if (width <= 0 || height <= 0 || (width & 1) || (height & 1) || (bd != 8 && bd != 10)) return IRONAV_INVALID_ARGUMENT;
     int mb_w = (width + 15) / 16, mb_h = (height + 15) / 16;
     if (mb_w > 1024 || mb_h > 1024 || max_refs < 1 || max_refs > 16 || nslices < 1 || nslices > mb_h) return IRONAV_INVALID_ARGUMENT;
     if (band_rows) {
@@ -849,23 +850,29 @@ int ironav_ctx_set_stream(ironav_ctx* c, void* s) {
     return c ? IRONAV_OK : IRONAV_INVALID_ARGUMENT;
 }
 
-/* Edge-repeated padding to whole macroblocks, H264Encoder::source, enc/mod.rs:502-519 */
-static void pad_plane(const uint8_t* y, int stride, int w, int h, int pw, int ph, uint16_t* out) {
+/* Edge-repeated padding to whole macroblocks, H264Encoder::source, enc/mod.rs:502-519. y holds uint8_t
+ * samples (8-bit contexts) or uint16_t samples (bd > 8), rows `stride` samples apart. */
+static int sample_bytes(const struct ironav_ctx* c) { return c->bd > 8 ? 2 : 1; }
+
+static void pad_plane(const void* y, int bytes, int stride, int w, int h, int pw, int ph, uint16_t* out) {
     for (int r = 0; r < ph; r++) {
-        const uint8_t* row = y + (size_t)mini(r, h - 1) * stride;
+        size_t row = (size_t)mini(r, h - 1) * stride;
         uint16_t* o = out + (size_t)r * pw;
-        for (int x = 0; x < w; x++) o[x] = row[x];
-        for (int x = w; x < pw; x++) o[x] = row[w - 1];
+        if (bytes == 2)
+            for (int x = 0; x < w; x++) o[x] = ((const uint16_t*)y)[row + x];
+        else
+            for (int x = 0; x < w; x++) o[x] = ((const uint8_t*)y)[row + x];
+        for (int x = w; x < pw; x++) o[x] = o[w - 1];
     }
 }
 
-int ironav_set_source(ironav_ctx* c, const uint8_t* y, int stride) {
+int ironav_set_source(ironav_ctx* c, const void* y, int stride) {
     if (!c || !y || stride < c->width) return IRONAV_INVALID_ARGUMENT;
-    pad_plane(y, stride, c->width, c->height, c->pw, c->ph, c->src);
+    pad_plane(y, sample_bytes(c), stride, c->width, c->height, c->pw, c->ph, c->src);
     return IRONAV_OK;
 }
 
-int ironav_push_reference(ironav_ctx* c, const uint8_t* y, int stride, int w, int h, const ironav_mbstate* col) {
+int ironav_push_reference(ironav_ctx* c, const void* y, int stride, int w, int h, const ironav_mbstate* col) {
     if (!c || !y) return IRONAV_INVALID_ARGUMENT;
     if (!((w == c->width && h == c->height) || (w == c->pw && h == c->ph)) || stride < w) return IRONAV_INVALID_ARGUMENT;
     if (c->nrefs == c->max_refs) {
@@ -876,7 +883,7 @@ int ironav_push_reference(ironav_ctx* c, const uint8_t* y, int stride, int w, in
     refpic* r = &c->refs[0];
     memset(r, 0, sizeof(*r));
     uint16_t* luma = (uint16_t*)malloc(sizeof(uint16_t) * (size_t)c->pw * c->ph);
-    pad_plane(y, stride, w, h, c->pw, c->ph, luma);
+    pad_plane(y, sample_bytes(c), stride, w, h, c->pw, c->ph, luma);
     halfpel_build(&r->hp, luma, c->pw, c->ph, c->bd);
     free(luma);
     size_t nmb = (size_t)c->mb_w * c->mb_h;
@@ -899,11 +906,14 @@ int ironav_clear_references(ironav_ctx* c) {
     return IRONAV_OK;
 }
 
-int ironav_get_planes(ironav_ctx* c, int idx, uint8_t* out) {
+int ironav_get_planes(ironav_ctx* c, int idx, void* out) {
     if (!c || !out || idx < 0 || idx >= c->nrefs) return IRONAV_INVALID_ARGUMENT;
     size_t n = (size_t)c->refs[idx].hp.stride * c->refs[idx].hp.sh;
     for (int k = 0; k < 4; k++)
-        for (size_t i = 0; i < n; i++) out[k * n + i] = (uint8_t)c->refs[idx].hp.planes[k][i];
+        for (size_t i = 0; i < n; i++) {
+            if (c->bd > 8) ((uint16_t*)out)[k * n + i] = c->refs[idx].hp.planes[k][i];
+            else ((uint8_t*)out)[k * n + i] = (uint8_t)c->refs[idx].hp.planes[k][i];
+        }
     return IRONAV_OK;
 }
 
@@ -970,8 +980,8 @@ int ironav_analyse_picture_auto(ironav_ctx* c, ironav_mbstate* states, ironav_mb
     return IRONAV_OK;
 }
 
-int ironav_set_source_device(ironav_ctx* c, const uint8_t* d, int s) { (void)c; (void)d; (void)s; return IRONAV_HARDWARE_UNAVAILABLE; }
-int ironav_push_reference_device(ironav_ctx* c, const uint8_t* d, int s, int w, int h, const ironav_mbstate* col) {
+int ironav_set_source_device(ironav_ctx* c, const void* d, int s) { (void)c; (void)d; (void)s; return IRONAV_HARDWARE_UNAVAILABLE; }
+int ironav_push_reference_device(ironav_ctx* c, const void* d, int s, int w, int h, const ironav_mbstate* col) {
     (void)c; (void)d; (void)s; (void)w; (void)h; (void)col;
     return IRONAV_HARDWARE_UNAVAILABLE;
 }
@@ -1099,15 +1109,15 @@ static void change_of(const int32_t* prev, const int32_t* cur, int lw, int lh, i
     *intra_out = intra;
 }
 
-int ironav_scene_change(ironav_ctx* c, const uint8_t* prev_y, const uint8_t* cur_y, int stride, int64_t* out) {
+int ironav_scene_change(ironav_ctx* c, const void* prev_y, const void* cur_y, int stride, int64_t* out) {
     if (!c || !prev_y || !cur_y || !out || stride < c->width) return IRONAV_INVALID_ARGUMENT;
     int lw = c->mb_w * 4, lh = c->mb_h * 4;
     uint16_t* a = (uint16_t*)malloc(sizeof(uint16_t) * (size_t)c->pw * c->ph);
     uint16_t* b = (uint16_t*)malloc(sizeof(uint16_t) * (size_t)c->pw * c->ph);
     int32_t* la = (int32_t*)malloc(sizeof(int32_t) * (size_t)lw * lh);
     int32_t* lb = (int32_t*)malloc(sizeof(int32_t) * (size_t)lw * lh);
-    pad_plane(prev_y, stride, c->width, c->height, c->pw, c->ph, a);
-    pad_plane(cur_y, stride, c->width, c->height, c->pw, c->ph, b);
+    pad_plane(prev_y, sample_bytes(c), stride, c->width, c->height, c->pw, c->ph, a);
+    pad_plane(cur_y, sample_bytes(c), stride, c->width, c->height, c->pw, c->ph, b);
     lowres_of(a, c->pw, lw, lh, la);
     lowres_of(b, c->pw, lw, lh, lb);
     change_of(la, lb, lw, lh, &out[0], &out[1]);
@@ -1118,7 +1128,7 @@ int ironav_scene_change(ironav_ctx* c, const uint8_t* prev_y, const uint8_t* cur
     return IRONAV_OK;
 }
 
-int ironav_scene_change_device(ironav_ctx* c, const uint8_t* d_prev, const uint8_t* d_cur, int stride, int64_t* out) {
+int ironav_scene_change_device(ironav_ctx* c, const void* d_prev, const void* d_cur, int stride, int64_t* out) {
     (void)c; (void)d_prev; (void)d_cur; (void)stride; (void)out;
     return IRONAV_HARDWARE_UNAVAILABLE;
 }
