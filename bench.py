@@ -57,6 +57,8 @@ def parse():
                         "mode, one launch per stage and frame step, against the per-stream launch loop")
     p.add_argument("--streams", type=int, default=64, help="streams of the batched workload")
     p.add_argument("--e2e-threads", type=int, default=4, help="host threads (each with a context) of the e2e pass")
+    p.add_argument("--bd", type=int, default=8, choices=[8, 10],
+                   help="sample depth of the 1080p workload: 8 (Yuv420p) or 10 (Yuv420p10, QP' = QP + 12)")
     return p.parse_args()
 
 
@@ -130,15 +132,20 @@ class Clocks:
                 "window": "0.6 s of untimed steps, then the timed steps"}
 
 
-def make_frames(rank: int, n: int):
+def make_frames(rank: int, n: int, bd: int = 8):
     from ironav_b200.synth import CONFIGS, Sequence
 
     w, h, seed, pan_q, nobj, vmax, sigma = CONFIGS["1080p"]
     seq = Sequence(w, h, n, seed + 0x1000 * rank, pan_q, nobj, vmax, sigma)
-    return np.stack([seq.frame(t) for t in range(n)])
+    return np.stack([seq.frame10(t) if bd > 8 else seq.frame(t) for t in range(n)])
 
 
-def cpu_baseline(frames, states, seconds: float):
+def qp_prime(bd: int) -> int:
+    """QP'Y of the workload's P pictures: QP + 6 * (bd - 8) (FrameCoder::new, enc/frame.rs:381-412)."""
+    return QP + 6 * (bd - 8)
+
+
+def cpu_baseline(frames, states, seconds: float, bd: int = 8):
     """The oracle (C restatement of the reference's stage) in replay mode over all host cores, on as
     many of the ring's pictures as fit in `seconds`."""
     from tests.oracle_lib import oracle_library
@@ -146,7 +153,7 @@ def cpu_baseline(frames, states, seconds: float):
 
     lib = oracle_library()
     cores = host_cores()
-    st = InterStage(WIDTH, HEIGHT, nslices=NSLICES, lib=lib)
+    st = InterStage(WIDTH, HEIGHT, nslices=NSLICES, lib=lib, bd=bd)
     lib.oracle_set_threads(st.ctx, cores)
     done_mb, elapsed, pics = 0, 0.0, 0
     while elapsed < seconds:
@@ -154,7 +161,7 @@ def cpu_baseline(frames, states, seconds: float):
         st.clear_references()
         st.push_reference(frames[t - 1], col=states[t - 1] if t >= 2 else None)
         st.set_source(frames[t])
-        st.begin_p_picture(QP)
+        st.begin_p_picture(qp_prime(bd))
         t0 = time.perf_counter()
         st.analyse_replay(states[t])
         elapsed += time.perf_counter() - t0
@@ -162,7 +169,7 @@ def cpu_baseline(frames, states, seconds: float):
         pics += 1
     st.close()
     return {"value": done_mb / elapsed, "unit": "MB/s", "cores": cores, "kind": "port",
-            "sample": f"{pics} pictures of the 1080p ring ({done_mb} macroblocks), replay mode, "
+            "sample": f"{pics} pictures of the 1080p {bd}-bit ring ({done_mb} macroblocks), replay mode, "
                       f"{cores} threads, {elapsed:.2f} s; half-sample planes built outside the timing"}
 
 
@@ -183,16 +190,17 @@ def run_reference(args, rank, world):
     lib = oracle_library()
     cores = host_cores()
     nfr = args.steps + args.warmup + 2
-    frames = make_frames(0, min(nfr, RING))
+    frames = make_frames(0, min(nfr, RING), args.bd)
+    qpp = qp_prime(args.bd)
     # decisions of every picture by the oracle's own auto mode (the reference's slice loop)
-    st = InterStage(WIDTH, HEIGHT, nslices=NSLICES, lib=lib)
+    st = InterStage(WIDTH, HEIGHT, nslices=NSLICES, lib=lib, bd=args.bd)
     lib.oracle_set_threads(st.ctx, cores)
     states = [None]
     for t in range(1, len(frames)):
         st.clear_references()
         st.push_reference(frames[t - 1], col=states[t - 1])
         st.set_source(frames[t])
-        st.begin_p_picture(QP)
+        st.begin_p_picture(qpp)
         s, _ = st.analyse_auto()
         states.append(s)
     times = []
@@ -202,7 +210,7 @@ def run_reference(args, rank, world):
         t0 = time.perf_counter()
         st.push_reference(frames[t - 1], col=states[t - 1])
         st.set_source(frames[t])
-        st.begin_p_picture(QP)
+        st.begin_p_picture(qpp)
         st.analyse_replay(states[t])
         dt = time.perf_counter() - t0
         if i >= args.warmup:
@@ -212,9 +220,9 @@ def run_reference(args, rank, world):
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "MB/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / len(times),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
-        "data": "synthetic: seeded 4-octave value noise panned per frame + 8 moving rectangles, sigma 3",
-        "config": config_dict(),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8" if args.bd == 8 else "u16",
+        "data": data_desc(args.bd),
+        "config": config_dict(args.bd),
         "cpu_baseline": {"value": value, "unit": "MB/s", "cores": cores, "kind": "port",
                          "sample": f"each step one 1080p picture (8160 macroblocks): planes + replay analysis, "
                                    f"{cores} threads"},
@@ -223,10 +231,16 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-def config_dict():
-    return {"workload": "1080p P-picture inter analysis, replay mode: half-sample planes (K1) + all 8160 "
+def data_desc(bd: int = 8) -> str:
+    d = "synthetic: seeded 4-octave value noise panned per frame + 8 moving rectangles, sigma 3"
+    return d if bd == 8 else d + "; 10-bit: the 8-bit frame x 4 + 2 seeded low bits per sample"
+
+
+def config_dict(bd: int = 8):
+    return {"workload": f"1080p {bd}-bit P-picture inter analysis, replay mode: half-sample planes (K1) + all 8160 "
                         "macroblocks' P_Skip test and best_inter (K2) per step",
-            "width": WIDTH, "height": HEIGHT, "qp": QP, "refs": 1, "slices": NSLICES, "mode": "replay",
+            "width": WIDTH, "height": HEIGHT, "bit_depth": bd, "qp": QP, "qp_prime": qp_prime(bd), "refs": 1,
+            "slices": NSLICES, "mode": "replay",
             "l2": f"inputs larger than L2: ring of {RING} pictures (luma, decisions, results ~140 MB)",
             "parallelism": "replicas"}
 
@@ -252,12 +266,13 @@ def main():
 
     lib = cuda_library()
     dev = torch.device("cuda", torch.cuda.current_device())
-    frames = make_frames(rank, RING)
+    bd, qpp = args.bd, qp_prime(args.bd)
+    frames = make_frames(rank, RING, bd)
     stream = torch.cuda.Stream()
-    st = InterStage(WIDTH, HEIGHT, nslices=NSLICES, lib=lib)
+    st = InterStage(WIDTH, HEIGHT, nslices=NSLICES, lib=lib, bd=bd)
     st.set_stream(stream.cuda_stream)
     nmb = st.nmb
-    d_frames = torch.from_numpy(frames).to(dev)
+    d_frames = torch.from_numpy(frames.view(np.int16) if bd > 8 else frames).to(dev)
     d_states = torch.zeros((RING, nmb * 72), dtype=torch.uint8, device=dev)
     d_res = torch.zeros((RING, nmb * 104), dtype=torch.uint8, device=dev)
     fp = lambda t: d_frames[t].data_ptr()
@@ -267,7 +282,7 @@ def main():
             st.clear_references()
             st.push_reference_device(fp(t - 1), WIDTH, WIDTH, HEIGHT, d_states[t - 1].data_ptr() if t >= 2 else None)
             st.set_source_device(fp(t), WIDTH)
-            st.begin_p_picture(QP)
+            st.begin_p_picture(qpp)
             st.analyse_auto_device(d_states[t].data_ptr(), d_res[t].data_ptr())
         st.sync()
 
@@ -276,7 +291,7 @@ def main():
         st.clear_references()
         st.push_reference_device(fp(t - 1), WIDTH, WIDTH, HEIGHT, d_states[t - 1].data_ptr() if t >= 2 else None)
         st.set_source_device(fp(t), WIDTH)
-        st.begin_p_picture(QP)
+        st.begin_p_picture(qpp)
         if ev is not None:
             ev[0].record(stream)
         st.analyse_replay_device(d_states[t].data_ptr(), d_res[t].data_ptr())
@@ -333,7 +348,7 @@ def main():
 
     # the plane kernel alone, for its HBM roofline (one launch per picture, timed in isolation)
     planes_ms = time_planes(st, fp, stream, torch)
-    planes_bytes = WIDTH * HEIGHT + 4 * st.sw * st.sh  # luma read once + 4 planes written
+    planes_bytes = (WIDTH * HEIGHT + 4 * st.sw * st.sh) * (2 if bd > 8 else 1)  # luma read once + 4 planes written
     hbm = measured_hbm()
 
     # end to end through the host-buffer C ABI, pinned host memory
@@ -342,18 +357,18 @@ def main():
     line = {
         "metric": METRIC, "value": value, "unit": "MB/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "u8",
-        "data": "synthetic: seeded 4-octave value noise panned per frame + 8 moving rectangles, sigma 3",
-        "config": config_dict(),
+        "vs_baseline": None, "dtype": "u8" if bd == 8 else "u16",
+        "data": data_desc(bd),
+        "config": config_dict(bd),
         "e2e": e2e,
-        "gpu_launches": 4 * args.steps,
-        "roofline": {"bound": "int32", "kernel": "analyse_kernel<false>", "achieved": achieved, "peak": peak,
+        "gpu_launches": 3 * args.steps,  # per step: half-sample planes (+ co-located vectors), edge padding, analysis
+        "roofline": {"bound": "int32", "kernel": f"analyse_kernel<MODE_REPLAY, {'uint8_t' if bd == 8 else 'uint16_t'}>", "achieved": achieved, "peak": peak,
                      "unit": "Tops/s", "frac": achieved / peak if peak else None, "traffic": None,
                      "ms_per_launch": k2_mean,
                      "note": "achieved = algorithmic ops (3 per SAD sample, 9 per SATD sample, counted by the "
                              "kernel in the reference's evaluation order) / event time; peak = measured 32-bit "
                              "integer issue rate (add+xor chains on every SM)"},
-        "roofline_planes": {"bound": "hbm", "kernel": "halfpel_planes_kernel",
+        "roofline_planes": {"bound": "hbm", "kernel": f"halfpel_planes_kernel<{'uint8_t' if bd == 8 else 'uint16_t'}>",
                             "achieved": planes_bytes / (planes_ms * 1e-3) / 1e9, "peak": hbm[0], "unit": "GB/s",
                             "frac": planes_bytes / (planes_ms * 1e-3) / 1e9 / hbm[0], "peak_source": hbm[1],
                             "ms_per_launch": planes_ms, "traffic": None},
@@ -361,7 +376,7 @@ def main():
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         host_states = [None] + [d_states[t].cpu().numpy().view(MBSTATE_DTYPE) for t in range(1, RING)]
-        line["cpu_baseline"] = cpu_baseline(frames, host_states, args.cpu_seconds)
+        line["cpu_baseline"] = cpu_baseline(frames, host_states, args.cpu_seconds, bd)
     if rank == 0:
         print(json.dumps(line), flush=True)
     st.close()
@@ -566,19 +581,20 @@ def run_e2e(args, st, frames, d_states, nmb, world, torch, dist, dev, stream):
 
     n = min(RING, 12)
     nthreads = max(1, args.e2e_threads)
-    pin_frames = torch.from_numpy(frames[:n]).pin_memory()
+    pin_frames = torch.from_numpy(frames[:n].view(np.int16) if frames.dtype == np.uint16 else frames[:n]).pin_memory()
     pin_states = d_states[:n].cpu().pin_memory()
     fr = pin_frames.numpy()
     stv = pin_states.numpy()
     lib = st.lib
     workers = []
     for k in range(nthreads):
-        ws = InterStage(WIDTH, HEIGHT, nslices=NSLICES, lib=lib)
+        ws = InterStage(WIDTH, HEIGHT, nslices=NSLICES, lib=lib, bd=args.bd)
         wstream = torch.cuda.Stream()
         ws.set_stream(wstream.cuda_stream)
         out = torch.zeros((nmb * 104,), dtype=torch.uint8).pin_memory()
         workers.append((ws, wstream, out, out.numpy().view(MBRESULT_DTYPE)))
-    lam, thr = lib.ironav_lambda(QP), lib.ironav_skip_threshold(QP)
+    qpp = qp_prime(args.bd)
+    lam, thr = lib.ironav_lambda(qpp), lib.ironav_skip_threshold(qpp)
 
     def step(w, i):
         ws, _, _, out = workers[w]
@@ -587,7 +603,7 @@ def run_e2e(args, st, frames, d_states, nmb, world, torch, dist, dev, stream):
         s = lib.ironav_clear_references(ws.ctx)
         s |= lib.ironav_push_reference(ws.ctx, fr[t - 1].ctypes.data, WIDTH, WIDTH, HEIGHT, col)
         s |= lib.ironav_set_source(ws.ctx, fr[t].ctypes.data, WIDTH)
-        s |= lib.ironav_begin_p_picture(ws.ctx, QP, lam, thr, 1, 0, 0)
+        s |= lib.ironav_begin_p_picture(ws.ctx, qpp, lam, thr, 1, 0, 0)
         s |= lib.ironav_analyse_picture_replay(ws.ctx, stv[t].ctypes.data, out.ctypes.data)
         if s:
             raise RuntimeError(f"e2e step failed: {s}")
@@ -624,7 +640,7 @@ def run_e2e(args, st, frames, d_states, nmb, world, torch, dist, dev, stream):
     for ws, *_ in workers:
         ws.close()
     return {"value": world * nmb * args.steps / el, "unit": "MB/s",
-            "h2d_bytes_per_step": 2 * WIDTH * HEIGHT + 2 * nmb * 72, "d2h_bytes_per_step": nmb * 104,
+            "h2d_bytes_per_step": 2 * WIDTH * HEIGHT * fr.itemsize + 2 * nmb * 72, "d2h_bytes_per_step": nmb * 104,
             "ms_per_step": 1e3 * el / args.steps, "host_threads": nthreads,
             "note": "host-buffer C ABI calls (each returns when its work is done) from pinned host memory, "
                     f"K steps spread over {nthreads} host threads with a context and CUDA stream each; wall clock "

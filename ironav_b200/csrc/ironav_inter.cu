@@ -116,11 +116,11 @@ int launch_planes(ironav_ctx* c, const void* d_luma, int stride, int w, int h, c
     const int maxv = (1 << c->bd) - 1;
     if (c->bd > 8)
         halfpel_planes_kernel<uint16_t><<<grid, K1_THREADS, 0, c->stream>>>(static_cast<const uint16_t*>(d_luma), stride, w, h,
-                                                                           reinterpret_cast<uint16_t*>(c->d_planes[slot]), c->psize, c->sw, c->sh, maxv);
+                                                                           reinterpret_cast<uint16_t*>(c->d_planes[slot]), c->psize, c->sw, c->sh, maxv,
+                                                                           d_col, c->d_col[slot], c->nmb);
     else
         halfpel_planes_kernel<uint8_t><<<grid, K1_THREADS, 0, c->stream>>>(static_cast<const uint8_t*>(d_luma), stride, w, h, c->d_planes[slot],
-                                                                          c->psize, c->sw, c->sh, maxv);
-    col_extract_kernel<<<(c->nmb + 255) / 256, 256, 0, c->stream>>>(d_col, c->d_col[slot], c->nmb);
+                                                                          c->psize, c->sw, c->sh, maxv, d_col, c->d_col[slot], c->nmb);
     return cuda_status(cudaGetLastError());
 }
 

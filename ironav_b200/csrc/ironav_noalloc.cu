@@ -167,7 +167,8 @@ extern "C" int ironav_analyse_auto_noalloc(const uint8_t* d_src, int src_stride,
     const int init_n = nmb > mb_h ? nmb : mb_h;
     noalloc_init_kernel<<<(init_n + 255) / 256, 256, 0, s>>>(scr, d_col, nmb, mb_h, nslices);
     dim3 grid((sw + K1_TW - 1) / K1_TW, (sh + K1_TH - 1) / K1_TH);
-    halfpel_planes_kernel<uint8_t><<<grid, K1_THREADS, 0, s>>>(d_ref, ref_stride, ref_w, ref_h, d_planes, (long long)sw * sh, sw, sh, 255);
+    halfpel_planes_kernel<uint8_t><<<grid, K1_THREADS, 0, s>>>(d_ref, ref_stride, ref_w, ref_h, d_planes, (long long)sw * sh, sw, sh, 255,
+                                                                nullptr, nullptr, 0);
 
     AnalyseParams p;
     memset(&p, 0, sizeof(p));
