@@ -172,6 +172,46 @@ int ironav_scene_change(ironav_ctx* ctx, const void* prev_y, const void* cur_y, 
 /* The same on device pointers (returns when the totals are in out, a host array). */
 int ironav_scene_change_device(ironav_ctx* ctx, const void* d_prev, const void* d_cur, int stride, int64_t* out);
 
+/* ---- deblocking of the reconstruction ------------------------------------------------------------ */
+
+/* The in-loop deblocking filter (h264/deblock.rs:410-720, ITU-T H.264 8.7) of a reconstructed picture,
+ * frame coded (not MBAFF) and 4:2:0 as the encoder codes it (enc/mod.rs:633,650-655), before the
+ * picture becomes a reference (ironav_push_reference). The result is the reference's deblock_picture
+ * (raster order), which deblock_picture_par reproduces with a macroblock-row wavefront; so does this.
+ *
+ * One macroblock as the filter sees it: the MbInfo fields deblock.rs reads (h264/mb.rs:34-68). */
+typedef struct ironav_dbk_mb {
+    uint16_t slice;         /* 1-based slice id (an index into the slice table + 1); 0: not coded, left alone */
+    uint8_t inter;          /* 1: Kind::Inter (P or B, skipped or not); 0: an intra kind */
+    int8_t qp;              /* QP_Y */
+    uint8_t t8x8;           /* 8x8 transform: only the even luma edges are filtered */
+    uint8_t keep;           /* I_PCM or lossless: its samples are put back after each filtered line */
+    uint8_t pad[2];
+    uint8_t nnz[16];        /* non-zero coefficient counts of the 16 luma 4x4 blocks, raster order */
+    int8_t ref_idx[2][4];   /* per list and 8x8 block; -1 when the list is not used */
+    int32_t ref_id[2][4];   /* identity of the picture behind ref_idx; -1 when not used */
+    int16_t mv[2][16][2];   /* per list and 4x4 block, quarter samples */
+} ironav_dbk_mb;            /* 192 bytes */
+
+/* A slice's filter parameters (SliceParams, h264/mb.rs:115-120). */
+typedef struct ironav_dbk_slice {
+    int32_t disable_deblocking;   /* 0: filter; 1: leave the slice alone; 2: not across its edges */
+    int32_t alpha_offset;         /* FilterOffsetA */
+    int32_t beta_offset;          /* FilterOffsetB */
+    int32_t chroma_qp_offset[2];  /* Cb, Cr */
+} ironav_dbk_slice;
+
+/* Filters a picture of the context's size and sample depth in place: luma 16*mb_w x 16*mb_h samples,
+ * rows y_stride samples apart; Cb and Cr 8*mb_w x 8*mb_h, rows c_stride apart (the layout of
+ * Picture::planes). mbs: mb_w*mb_h records; slices: nslices entries, the slice ids of mbs index them.
+ * A slice id above nslices gives IRONAV_INVALID_INPUT (the picture is then left partly filtered). */
+int ironav_deblock_picture(ironav_ctx* ctx, void* y, int y_stride, void* cb, void* cr, int c_stride,
+                           const ironav_dbk_mb* mbs, const ironav_dbk_slice* slices, int nslices);
+/* The same on device pointers (planes and mbs), queued on the context's stream; slices is a host array,
+ * copied before the call returns. ironav_ctx_sync reports a slice id out of range. */
+int ironav_deblock_picture_device(ironav_ctx* ctx, void* d_y, int y_stride, void* d_cb, void* d_cr, int c_stride,
+                                  const ironav_dbk_mb* d_mbs, const ironav_dbk_slice* slices, int nslices);
+
 /* ---- in-loop mode ---------------------------------------------------------------------------------- */
 
 /* The encoder's own loop (FrameCoder::encode, enc/frame.rs:467-478): the caller makes each macroblock's

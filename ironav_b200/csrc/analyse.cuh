@@ -795,14 +795,6 @@ static __device__ void analyse(const AnalyseParams& __restrict__ P, WarpSmem<T>&
     __syncwarp();
 }
 
-__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
-    unsigned v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-__device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
-    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
 
 // Waits until macroblock `m`'s decision is published, at most P.wait_limit polls. Returns false when
 // it gave up or another warp already did (the launch is then abandoned and the host reports a timeout).

@@ -47,4 +47,14 @@ struct AnalyseParams {
     unsigned long long wait_ns;       // how long an in-loop wait for the caller may take
 };
 
+// Device-scope acquire load and release store of a progress word shared by warps of different CTAs.
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
 }  // namespace ironav

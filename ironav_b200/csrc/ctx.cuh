@@ -46,6 +46,13 @@ struct ironav_ctx {
     uint8_t* d_scene_luma = nullptr;
     uint8_t* d_lowres = nullptr;
     unsigned long long* d_scene_sums = nullptr;
+    // deblocking (allocated on first use): per-row progress, the slice table, and for the host-buffer form
+    // the macroblock records and the three planes
+    unsigned* d_dbk_progress = nullptr;
+    ironav_dbk_slice* d_dbk_slices = nullptr;
+    int dbk_slice_cap = 0;
+    ironav_dbk_mb* d_dbk_mbs = nullptr;
+    uint8_t* d_dbk_planes = nullptr;
 };
 
 

@@ -19,11 +19,14 @@
 #include "planes.cuh"
 #include "peaks.cuh"
 #include "scene.cuh"
+#include "deblock.cuh"
 
 using namespace ironav;
 
 static_assert(sizeof(ironav_mbstate) == 72, "ironav_mbstate layout");
 static_assert(sizeof(ironav_mbresult) == 104, "ironav_mbresult layout");
+static_assert(sizeof(ironav_dbk_mb) == 192, "ironav_dbk_mb layout");
+static_assert(sizeof(ironav_dbk_slice) == 20, "ironav_dbk_slice layout");
 
 // The reference slot for a new picture: the oldest one's once max_refs are held, else a free one; the
 // new picture becomes reference 0 (enc/mod.rs:663-666).
@@ -100,6 +103,10 @@ void free_ctx(ironav_ctx* c) {
     cudaFree(c->d_scene_luma);
     cudaFree(c->d_lowres);
     cudaFree(c->d_scene_sums);
+    cudaFree(c->d_dbk_progress);
+    cudaFree(c->d_dbk_slices);
+    cudaFree(c->d_dbk_mbs);
+    cudaFree(c->d_dbk_planes);
     cudaFreeHost(c->h_results);
     cudaFreeHost(c->h_done);
     cudaFreeHost(c->h_committed);
@@ -154,6 +161,7 @@ int check_device_error(ironav_ctx* c) {
     CK(cudaMemcpyAsync(&err, c->d_counters + 1, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     if (err & 1u) return IRONAV_TIMEOUT;
+    if (err & 4u) return IRONAV_INVALID_INPUT;
     if (err) return IRONAV_INTERNAL;
     return IRONAV_OK;
 }
@@ -194,6 +202,52 @@ int scene_run(ironav_ctx* c, const void* d_prev, int sp, const void* d_cur, int 
     out[0] = (int64_t)h[0];
     out[1] = (int64_t)h[1];
     return IRONAV_OK;
+}
+
+// ---- deblocking ------------------------------------------------------------------------------------
+
+// Queues the filter of the picture whose planes are at d_y / d_cb / d_cr (strides in samples), with the
+// macroblock records at d_mbs and the slice table from the host.
+int deblock_launch(ironav_ctx* c, void* d_y, int ys, void* d_cb, void* d_cr, int cs, const ironav_dbk_mb* d_mbs,
+                   const ironav_dbk_slice* slices, int nslices) {
+    if (!c->d_dbk_progress) CK(cudaMalloc(&c->d_dbk_progress, sizeof(unsigned) * c->mb_h));
+    if (nslices > c->dbk_slice_cap) {
+        CK(cudaStreamSynchronize(c->stream));  // the old table may still be read by queued work
+        cudaFree(c->d_dbk_slices);
+        c->d_dbk_slices = nullptr;
+        c->dbk_slice_cap = 0;
+        const int cap = std::max(nslices, 64);
+        CK(cudaMalloc(&c->d_dbk_slices, sizeof(ironav_dbk_slice) * cap));
+        c->dbk_slice_cap = cap;
+    }
+    CK(cudaMemcpyAsync(c->d_dbk_slices, slices, sizeof(ironav_dbk_slice) * nslices, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemsetAsync(c->d_dbk_progress, 0, sizeof(unsigned) * c->mb_h, c->stream));
+    CK(cudaMemsetAsync(c->d_counters, 0, 2 * sizeof(unsigned), c->stream));
+    DbkParams p;
+    p.planes[0] = static_cast<uint8_t*>(d_y);
+    p.planes[1] = static_cast<uint8_t*>(d_cb);
+    p.planes[2] = static_cast<uint8_t*>(d_cr);
+    p.ys = ys;
+    p.cs = cs;
+    p.mbs = d_mbs;
+    p.slices = c->d_dbk_slices;
+    p.nslices = nslices;
+    p.mb_w = c->mb_w;
+    p.mb_h = c->mb_h;
+    p.bd = c->bd;
+    p.progress = c->d_dbk_progress;
+    p.ticket = c->d_counters;
+    p.err = c->d_counters + 1;
+    p.wait_limit = c->wait_limit;
+    const int blocks = (c->mb_h + DBK_WARPS - 1) / DBK_WARPS;
+    if (c->bd > 8) deblock_kernel<uint16_t><<<blocks, DBK_WARPS * 32, 0, c->stream>>>(p);
+    else deblock_kernel<uint8_t><<<blocks, DBK_WARPS * 32, 0, c->stream>>>(p);
+    return cuda_status(cudaGetLastError());
+}
+
+bool deblock_args_ok(const ironav_ctx* c, const void* y, int ys, const void* cb, const void* cr, int cs, const void* mbs,
+                     const ironav_dbk_slice* slices, int nslices) {
+    return c && y && cb && cr && mbs && slices && nslices >= 1 && nslices <= 65535 && ys >= c->pw && cs >= c->pw / 2;
 }
 
 }  // namespace
@@ -451,6 +505,33 @@ int ironav_scene_change_device(ironav_ctx* c, const void* d_prev, const void* d_
     int s = scene_alloc(c);
     if (s != IRONAV_OK) return s;
     return scene_run(c, d_prev, stride, d_cur, stride, out);
+}
+
+int ironav_deblock_picture_device(ironav_ctx* c, void* d_y, int ys, void* d_cb, void* d_cr, int cs, const ironav_dbk_mb* d_mbs,
+                                  const ironav_dbk_slice* slices, int nslices) {
+    if (!deblock_args_ok(c, d_y, ys, d_cb, d_cr, cs, d_mbs, slices, nslices)) return IRONAV_INVALID_ARGUMENT;
+    return deblock_launch(c, d_y, ys, d_cb, d_cr, cs, d_mbs, slices, nslices);
+}
+
+int ironav_deblock_picture(ironav_ctx* c, void* y, int ys, void* cb, void* cr, int cs, const ironav_dbk_mb* mbs,
+                           const ironav_dbk_slice* slices, int nslices) {
+    if (!deblock_args_ok(c, y, ys, cb, cr, cs, mbs, slices, nslices)) return IRONAV_INVALID_ARGUMENT;
+    const size_t B = (size_t)sample_bytes(c), pw = (size_t)c->pw, ph = (size_t)c->ph;
+    if (!c->d_dbk_planes) CK(cudaMalloc(&c->d_dbk_planes, (pw * ph + 2 * (pw / 2) * (ph / 2)) * B));
+    if (!c->d_dbk_mbs) CK(cudaMalloc(&c->d_dbk_mbs, sizeof(ironav_dbk_mb) * c->nmb));
+    uint8_t* dy = c->d_dbk_planes;
+    uint8_t* dcb = dy + pw * ph * B;
+    uint8_t* dcr = dcb + (pw / 2) * (ph / 2) * B;
+    CK(cudaMemcpy2DAsync(dy, pw * B, y, (size_t)ys * B, pw * B, ph, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpy2DAsync(dcb, pw / 2 * B, cb, (size_t)cs * B, pw / 2 * B, ph / 2, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpy2DAsync(dcr, pw / 2 * B, cr, (size_t)cs * B, pw / 2 * B, ph / 2, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->d_dbk_mbs, mbs, sizeof(ironav_dbk_mb) * c->nmb, cudaMemcpyHostToDevice, c->stream));
+    int s = deblock_launch(c, dy, (int)pw, dcb, dcr, (int)(pw / 2), c->d_dbk_mbs, slices, nslices);
+    if (s != IRONAV_OK) return s;
+    CK(cudaMemcpy2DAsync(y, (size_t)ys * B, dy, pw * B, pw * B, ph, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpy2DAsync(cb, (size_t)cs * B, dcb, pw / 2 * B, pw / 2 * B, ph / 2, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpy2DAsync(cr, (size_t)cs * B, dcr, pw / 2 * B, pw / 2 * B, ph / 2, cudaMemcpyDeviceToHost, c->stream));
+    return check_device_error(c);
 }
 
 // Measures the 32-bit integer issue rate of the current device (operations per second, 1e12 units in

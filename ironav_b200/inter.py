@@ -46,7 +46,27 @@ MBRESULT_DTYPE = np.dtype(
         ("pad2", "<u4"),
     ]
 )
+# One macroblock as the deblocking filter sees it (ironav_dbk_mb: the MbInfo fields of h264/mb.rs:34-68 that
+# h264/deblock.rs reads) and a slice's filter parameters (ironav_dbk_slice, SliceParams, h264/mb.rs:115-120).
+DBK_MB_DTYPE = np.dtype(
+    [
+        ("slice", "<u2"),
+        ("inter", "u1"),
+        ("qp", "i1"),
+        ("t8x8", "u1"),
+        ("keep", "u1"),
+        ("pad", "u1", (2,)),
+        ("nnz", "u1", (16,)),
+        ("ref_idx", "i1", (2, 4)),
+        ("ref_id", "<i4", (2, 4)),
+        ("mv", "<i2", (2, 16, 2)),
+    ]
+)
+DBK_SLICE_DTYPE = np.dtype(
+    [("disable_deblocking", "<i4"), ("alpha_offset", "<i4"), ("beta_offset", "<i4"), ("chroma_qp_offset", "<i4", (2,))]
+)
 assert MBSTATE_DTYPE.itemsize == 72 and MBRESULT_DTYPE.itemsize == 104
+assert DBK_MB_DTYPE.itemsize == 192 and DBK_SLICE_DTYPE.itemsize == 20
 
 RESULT_INTER = 1
 RESULT_SKIP = 2
@@ -72,6 +92,7 @@ EXPORTS = (
     "ironav_inloop_begin", "ironav_inloop_result", "ironav_inloop_commit", "ironav_inloop_end",
     "ironav_inloop_set_wait", "ironav_batch_create", "ironav_batch_destroy", "ironav_batch_step",
     "ironav_batch_sync", "ironav_scene_change", "ironav_scene_change_device", "ironav_analyse_auto_noalloc",
+    "ironav_deblock_picture", "ironav_deblock_picture_device",
 )
 
 SCENE_CUT = 0.8  # codec/change.rs:6
@@ -121,6 +142,9 @@ def _declare(lib: ctypes.CDLL) -> ctypes.CDLL:
     if hasattr(lib, "ironav_scene_change"):
         lib.ironav_scene_change.argtypes = [_VP, _VP, _VP, _I, _VP]
         lib.ironav_scene_change_device.argtypes = [_VP, _VP, _VP, _I, _VP]
+    if hasattr(lib, "ironav_deblock_picture"):
+        lib.ironav_deblock_picture.argtypes = [_VP, _VP, _I, _VP, _VP, _I, _VP, _VP, _I]
+        lib.ironav_deblock_picture_device.argtypes = [_VP, _VP, _I, _VP, _VP, _I, _VP, _VP, _I]
     if hasattr(lib, "ironav_batch_create"):
         lib.ironav_batch_create.argtypes = [ctypes.POINTER(_VP), ctypes.POINTER(_VP), _I]
         lib.ironav_batch_destroy.argtypes = [_VP]
@@ -282,6 +306,26 @@ class InterStage:
         """Whether cur starts a new scene: inter > SCENE_CUT * intra, in f64 (enc/mod.rs:707-711)."""
         inter, intra = self.scene_change(prev, cur)
         return float(inter) > SCENE_CUT * float(intra)
+
+    # -- deblocking of the reconstruction (h264/deblock.rs) ------------------------------------------------
+
+    def deblock(self, y: np.ndarray, cb: np.ndarray, cr: np.ndarray, mbs: np.ndarray,
+                slices: np.ndarray) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+        """The filtered copies of a reconstructed 4:2:0 picture (luma 16*mb_w x 16*mb_h, chroma half that)
+        given its macroblock records (DBK_MB_DTYPE, mb_w*mb_h) and slice table (DBK_SLICE_DTYPE)."""
+        y, cb, cr = (self._luma(a).copy() for a in (y, cb, cr))
+        assert y.shape == (self.mb_h * 16, self.mb_w * 16) and cb.shape == cr.shape == (self.mb_h * 8, self.mb_w * 8)
+        mbs = np.ascontiguousarray(mbs, dtype=DBK_MB_DTYPE)
+        slices = np.ascontiguousarray(slices, dtype=DBK_SLICE_DTYPE)
+        assert mbs.shape == (self.nmb,)
+        self._check(self.lib.ironav_deblock_picture(self.ctx, _ptr(y), y.shape[1], _ptr(cb), _ptr(cr), cb.shape[1],
+                                                    _ptr(mbs), _ptr(slices), len(slices)), "ironav_deblock_picture")
+        return y, cb, cr
+
+    def deblock_device(self, d_y: int, ys: int, d_cb: int, d_cr: int, cs: int, d_mbs: int, slices: np.ndarray) -> None:
+        slices = np.ascontiguousarray(slices, dtype=DBK_SLICE_DTYPE)
+        self._check(self.lib.ironav_deblock_picture_device(self.ctx, d_y, ys, d_cb, d_cr, cs, d_mbs, _ptr(slices),
+                                                           len(slices)), "ironav_deblock_picture_device")
 
     # -- in-loop mode: the caller decides each macroblock (the encoder's own loop) ---------------------
 

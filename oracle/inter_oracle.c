@@ -1132,3 +1132,282 @@ int ironav_scene_change_device(ironav_ctx* c, const void* d_prev, const void* d_
     (void)c; (void)d_prev; (void)d_cur; (void)stride; (void)out;
     return IRONAV_HARDWARE_UNAVAILABLE;
 }
+
+/* ---------------------------------------------------------------------------------------------------
+ * Deblocking of the reconstruction (h264/deblock.rs): frame pictures, 4:2:0, macroblocks in raster
+ * order (deblock_picture / deblock_rows, deblock.rs:410-429), on 16-bit planes of 16*mb_w x 16*mb_h
+ * luma and 8*mb_w x 8*mb_h chroma (rows 16*mb_w and 8*mb_w apart, as Picture::planes).
+ * ------------------------------------------------------------------------------------------------- */
+
+/* alpha', beta' (indexA / indexB) and tC0 (indexA, bS 1..3) of the standard's Tables 8-16 and 8-17, as
+ * h264/tables.rs holds them (ALPHA, BETA, TC0), and the chroma QP mapping for qPi >= 30 (mb.rs:211). */
+static const uint8_t DBK_ALPHA[52] = {0,  0,  0,  0,  0,  0,  0,  0,  0,  0,  0,  0,  0,   0,   0,   0,   4,   4,
+                                      5,  6,  7,  8,  9,  10, 12, 13, 15, 17, 20, 22, 25,  28,  32,  36,  40,  45,
+                                      50, 56, 63, 71, 80, 90, 101, 113, 127, 144, 162, 182, 203, 226, 255, 255};
+static const uint8_t DBK_BETA[52] = {0, 0, 0, 0, 0, 0, 0, 0, 0,  0,  0,  0,  0,  0,  0,  0,  2,  2,  2,  3,  3,  3,  3,  4,  4,  4,
+                                     6, 6, 7, 7, 8, 8, 9, 9, 10, 10, 11, 11, 12, 12, 13, 13, 14, 14, 15, 15, 16, 16, 17, 17, 18, 18};
+static const uint8_t DBK_TC0[52][3] = {
+    {0, 0, 0},  {0, 0, 0},   {0, 0, 0},   {0, 0, 0},   {0, 0, 0},   {0, 0, 0},    {0, 0, 0},    {0, 0, 0},    {0, 0, 0},
+    {0, 0, 0},  {0, 0, 0},   {0, 0, 0},   {0, 0, 0},   {0, 0, 0},   {0, 0, 0},    {0, 0, 0},    {0, 0, 0},    {0, 0, 1},
+    {0, 0, 1},  {0, 0, 1},   {0, 0, 1},   {0, 1, 1},   {0, 1, 1},   {1, 1, 1},    {1, 1, 1},    {1, 1, 1},    {1, 1, 1},
+    {1, 1, 2},  {1, 1, 2},   {1, 1, 2},   {1, 1, 2},   {1, 2, 3},   {1, 2, 3},    {2, 2, 3},    {2, 2, 4},    {2, 3, 4},
+    {2, 3, 4},  {3, 3, 5},   {3, 4, 6},   {3, 4, 6},   {4, 5, 7},   {4, 5, 8},    {4, 6, 9},    {5, 7, 10},   {6, 8, 11},
+    {6, 8, 13}, {7, 10, 14}, {8, 11, 16}, {9, 12, 18}, {10, 13, 20}, {11, 15, 23}, {13, 17, 25}};
+static const uint8_t DBK_CHROMA_QP[22] = {29, 30, 31, 32, 32, 33, 34, 34, 35, 35, 36, 36, 37, 37, 37, 38, 38, 38, 39, 39, 39, 39};
+
+/* chroma_qp, mb.rs:214-221 */
+static int dbk_chroma_qp(int qp, int off, int bd) {
+    int qpi = clampi(qp + off, -6 * (bd - 8), 51);
+    return qpi < 30 ? qpi : DBK_CHROMA_QP[qpi - 30];
+}
+
+static uint16_t dbk_clip1(int v, int bd) { return (uint16_t)clampi(v, 0, (1 << bd) - 1); } /* deblock.rs:13-15 */
+
+/* filter_line, deblock.rs:279-333: the line through q (first sample past the edge), step xs across it */
+static void dbk_filter_line(uint16_t* pl, long q, long xs, int b, int tc0, int alpha, int beta, int chroma, int bd) {
+    int p0 = pl[q - xs], q0 = pl[q], p1 = pl[q - 2 * xs], q1 = pl[q + xs];
+    if (abs(p0 - q0) >= alpha || abs(p1 - p0) >= beta || abs(q1 - q0) >= beta) return;
+    if (chroma) {
+        if (b < 4) {
+            int tc = tc0 + 1;
+            int delta = clampi((((q0 - p0) << 2) + (p1 - q1) + 4) >> 3, -tc, tc);
+            pl[q - xs] = dbk_clip1(p0 + delta, bd);
+            pl[q] = dbk_clip1(q0 - delta, bd);
+        } else {
+            pl[q - xs] = (uint16_t)((2 * p1 + p0 + q1 + 2) >> 2);
+            pl[q] = (uint16_t)((2 * q1 + q0 + p1 + 2) >> 2);
+        }
+        return;
+    }
+    int p2 = pl[q - 3 * xs], q2 = pl[q + 2 * xs];
+    int ap = abs(p2 - p0), aq = abs(q2 - q0);
+    if (b < 4) {
+        int tc = tc0 + (ap < beta) + (aq < beta);
+        int delta = clampi((((q0 - p0) << 2) + (p1 - q1) + 4) >> 3, -tc, tc);
+        pl[q - xs] = dbk_clip1(p0 + delta, bd);
+        pl[q] = dbk_clip1(q0 - delta, bd);
+        if (ap < beta) pl[q - 2 * xs] = (uint16_t)(p1 + clampi((p2 + ((p0 + q0 + 1) >> 1) - (p1 << 1)) >> 1, -tc0, tc0));
+        if (aq < beta) pl[q + xs] = (uint16_t)(q1 + clampi((q2 + ((p0 + q0 + 1) >> 1) - (q1 << 1)) >> 1, -tc0, tc0));
+    } else {
+        int small = abs(p0 - q0) < (alpha >> 2) + 2;
+        if (ap < beta && small) {
+            int p3 = pl[q - 4 * xs];
+            pl[q - xs] = (uint16_t)((p2 + 2 * p1 + 2 * p0 + 2 * q0 + q1 + 4) >> 3);
+            pl[q - 2 * xs] = (uint16_t)((p2 + p1 + p0 + q0 + 2) >> 2);
+            pl[q - 3 * xs] = (uint16_t)((2 * p3 + 3 * p2 + p1 + p0 + q0 + 4) >> 3);
+        } else {
+            pl[q - xs] = (uint16_t)((2 * p1 + p0 + q1 + 2) >> 2);
+        }
+        if (aq < beta && small) {
+            int q3 = pl[q + 3 * xs];
+            pl[q] = (uint16_t)((p1 + 2 * p0 + 2 * q0 + 2 * q1 + q2 + 4) >> 3);
+            pl[q + xs] = (uint16_t)((p0 + q0 + q1 + q2 + 2) >> 2);
+            pl[q + 2 * xs] = (uint16_t)((2 * q3 + 3 * q2 + q1 + q0 + p0 + 4) >> 3);
+        } else {
+            pl[q] = (uint16_t)((2 * q1 + q0 + p1 + 2) >> 2);
+        }
+    }
+}
+
+/* filter_edge, deblock.rs:232-276: four segments of per_bs lines, one strength each; the samples of a
+ * keep (I_PCM / lossless) side are put back after each line */
+static void dbk_filter_edge(uint16_t* pl, long pos, long xs, long ys, int per_bs, const uint8_t bs[4], int alpha, int beta, int ia,
+                            int chroma, int bd, int keep_p, int keep_q) {
+    if (alpha == 0 || beta == 0) return;
+    int n = chroma ? 1 : 3;
+    for (int s = 0; s < 4; s++) {
+        int b = bs[s];
+        if (b == 0) continue;
+        int tc0 = b < 4 ? DBK_TC0[ia][b - 1] << (bd - 8) : 0;
+        for (int k = s * per_bs; k < (s + 1) * per_bs; k++) {
+            long q = pos + k * ys;
+            uint16_t sp[3], sq[3];
+            for (int i = 0; i < n; i++) {
+                sp[i] = pl[q - (i + 1) * xs];
+                sq[i] = pl[q + i * xs];
+            }
+            dbk_filter_line(pl, q, xs, b, tc0, alpha, beta, chroma, bd);
+            for (int i = 0; i < n; i++) {
+                if (keep_p) pl[q - (i + 1) * xs] = sp[i];
+                if (keep_q) pl[q + i * xs] = sq[i];
+            }
+        }
+    }
+}
+
+/* coded, deblock.rs:336-345 */
+static int dbk_coded(const ironav_dbk_mb* m, int bx, int by) {
+    if (m->t8x8) {
+        int x0 = bx & 2, y0 = by & 2;
+        return m->nnz[y0 * 4 + x0] || m->nnz[y0 * 4 + x0 + 1] || m->nnz[(y0 + 1) * 4 + x0] || m->nnz[(y0 + 1) * 4 + x0 + 1];
+    }
+    return m->nnz[by * 4 + bx] > 0;
+}
+
+/* far, deblock.rs:347-350 */
+static int dbk_far(const int16_t* a, const int16_t* b, int mvy) { return abs(a[0] - b[0]) >= 4 || abs(a[1] - b[1]) >= mvy; }
+
+/* motion_differs, deblock.rs:352-383 */
+static int dbk_motion_differs(const ironav_dbk_mb* p, int pbx, int pby, const ironav_dbk_mb* q, int qbx, int qby, int mvy) {
+    int pi = pby * 4 + pbx, qi = qby * 4 + qbx;
+    int p8 = (pby >> 1) * 2 + (pbx >> 1), q8 = (qby >> 1) * 2 + (qbx >> 1);
+    int32_t pr[2] = {p->ref_id[0][p8], p->ref_id[1][p8]}, qr[2] = {q->ref_id[0][q8], q->ref_id[1][q8]};
+    const int16_t *pm[2] = {p->mv[0][pi], p->mv[1][pi]}, *qm[2] = {q->mv[0][qi], q->mv[1][qi]};
+    int np = (pr[0] >= 0) + (pr[1] >= 0), nq = (qr[0] >= 0) + (qr[1] >= 0);
+    if (np != nq) return 1;
+    if (np == 1) {
+        int lp = pr[0] >= 0 ? 0 : 1, lq = qr[0] >= 0 ? 0 : 1;
+        return pr[lp] != qr[lq] || dbk_far(pm[lp], qm[lq], mvy);
+    }
+    if (!((pr[0] == qr[0] && pr[1] == qr[1]) || (pr[0] == qr[1] && pr[1] == qr[0]))) return 1;
+    if (pr[0] != pr[1]) {
+        if (pr[0] == qr[0]) return dbk_far(pm[0], qm[0], mvy) || dbk_far(pm[1], qm[1], mvy);
+        return dbk_far(pm[0], qm[1], mvy) || dbk_far(pm[1], qm[0], mvy);
+    }
+    return (dbk_far(pm[0], qm[0], mvy) || dbk_far(pm[1], qm[1], mvy)) && (dbk_far(pm[0], qm[1], mvy) || dbk_far(pm[1], qm[0], mvy));
+}
+
+/* uniform_motion, deblock.rs:385-389 */
+static int dbk_uniform(const ironav_dbk_mb* m) {
+    for (int l = 0; l < 2; l++) {
+        for (int k = 0; k < 4; k++)
+            if (m->ref_idx[l][k] != m->ref_idx[l][0] || m->ref_id[l][k] != m->ref_id[l][0]) return 0;
+        for (int k = 0; k < 16; k++)
+            if (m->mv[l][k][0] != m->mv[l][0][0] || m->mv[l][k][1] != m->mv[l][0][1]) return 0;
+    }
+    return 1;
+}
+
+/* strength, deblock.rs:391-408 */
+static void dbk_strength(const ironav_dbk_mb* m, const ironav_dbk_mb* other, int dir, int e, int mvy, uint8_t out[4]) {
+    int mb_edge = e == 0;
+    if (!m->inter || !other->inter) {
+        for (int i = 0; i < 4; i++) out[i] = mb_edge ? 4 : 3;
+        return;
+    }
+    for (int i = 0; i < 4; i++) {
+        int qx, qy, px, py;
+        if (dir == 0) {
+            qx = e; qy = i; px = mb_edge ? 3 : e - 1; py = i;
+        } else {
+            qx = i; qy = e; px = i; py = mb_edge ? 3 : e - 1;
+        }
+        if (dbk_coded(m, qx, qy) || dbk_coded(other, px, py)) out[i] = 2;
+        else out[i] = dbk_motion_differs(other, px, py, m, qx, qy, mvy) ? 1 : 0;
+    }
+}
+
+/* deblock_mb, deblock.rs:608-695, for 4:2:0 (chroma 8 rows a macroblock). Returns nonzero for a slice id
+ * beyond the table. */
+static int dbk_mb(uint16_t* planes[3], const ironav_dbk_mb* mbs, const ironav_dbk_slice* slices, int nslices, int mb_w, int bd,
+                  int mbx, int mby) {
+    int w = mb_w, ls = w * 16, cs = w * 8, idx = mby * w + mbx;
+    const ironav_dbk_mb* m = &mbs[idx];
+    if (m->slice == 0) return 0;
+    if (m->slice > nslices) return 1;
+    const ironav_dbk_slice* sp = &slices[m->slice - 1];
+    if (sp->disable_deblocking == 1) return 0;
+#define USABLE(o) ((o)->slice != 0 && (sp->disable_deblocking == 0 || (o)->slice == m->slice))
+    int left_ok = mbx > 0 && USABLE(&mbs[idx - 1]);
+    int top_ok = mby > 0 && USABLE(&mbs[idx - w]);
+#undef USABLE
+    const ironav_dbk_mb* edge_mb[2] = {mbx > 0 ? &mbs[idx - 1] : m, mby > 0 ? &mbs[idx - w] : m};
+    uint8_t bs[2][4][4];
+    memset(bs, 0, sizeof(bs));
+    int still = m->inter && dbk_uniform(m);
+    for (int k = 0; k < 16 && still; k++)
+        if (m->nnz[k]) still = 0;
+    for (int dir = 0; dir < 2; dir++)
+        for (int e = 0; e < 4; e++) {
+            if (e > 0 && still) continue;
+            dbk_strength(m, e == 0 ? edge_mb[dir] : m, dir, e, 4, bs[dir][e]);
+        }
+#define ALL0(v) ((v)[0] == 0 && (v)[1] == 0 && (v)[2] == 0 && (v)[3] == 0)
+    /* luma */
+    for (int dir = 0; dir < 2; dir++)
+        for (int e = 0; e < 4; e++) {
+            if (e == 0 && !(dir == 0 ? left_ok : top_ok)) continue;
+            if ((m->t8x8 && (e & 1)) || ALL0(bs[dir][e])) continue;
+            const ironav_dbk_mb* other = e == 0 ? edge_mb[dir] : m;
+            int qpav = (other->qp + m->qp + 1) >> 1;
+            int ia = clampi(qpav + sp->alpha_offset, 0, 51), ib = clampi(qpav + sp->beta_offset, 0, 51);
+            int alpha = DBK_ALPHA[ia] << (bd - 8), beta = DBK_BETA[ib] << (bd - 8);
+            long x0 = mbx * 16, y0 = mby * 16;
+            if (dir == 0)
+                dbk_filter_edge(planes[0], y0 * ls + x0 + e * 4, 1, ls, 4, bs[dir][e], alpha, beta, ia, 0, bd, other->keep, m->keep);
+            else
+                dbk_filter_edge(planes[0], (y0 + e * 4) * ls + x0, ls, 1, 4, bs[dir][e], alpha, beta, ia, 0, bd, other->keep, m->keep);
+        }
+    /* chroma: vertical edges at 0 and 4, horizontal edges at rows 0 and 4, each with the strength of the
+     * luma edge it lines up with */
+    for (int comp = 0; comp < 2; comp++) {
+        int off = sp->chroma_qp_offset[comp];
+        for (int dir = 0; dir < 2; dir++)
+            for (int e = 0; e < 4; e += 2) {
+                if ((e == 0 && !(dir == 0 ? left_ok : top_ok)) || ALL0(bs[dir][e])) continue;
+                const ironav_dbk_mb* other = e == 0 ? edge_mb[dir] : m;
+                int qpav = (dbk_chroma_qp(other->qp, off, bd) + dbk_chroma_qp(m->qp, off, bd) + 1) >> 1;
+                int ia = clampi(qpav + sp->alpha_offset, 0, 51), ib = clampi(qpav + sp->beta_offset, 0, 51);
+                int alpha = DBK_ALPHA[ia] << (bd - 8), beta = DBK_BETA[ib] << (bd - 8);
+                long x0 = mbx * 8, y0 = mby * 8;
+                if (dir == 0)
+                    dbk_filter_edge(planes[1 + comp], y0 * cs + x0 + e * 2, 1, cs, 2, bs[dir][e], alpha, beta, ia, 1, bd, other->keep, m->keep);
+                else
+                    dbk_filter_edge(planes[1 + comp], (y0 + e * 2) * cs + x0, cs, 1, 2, bs[dir][e], alpha, beta, ia, 1, bd, other->keep, m->keep);
+            }
+    }
+#undef ALL0
+    return 0;
+}
+
+static void dbk_copy_in(uint16_t* dst, const void* src, int bytes, int stride, int w, int h) {
+    for (int r = 0; r < h; r++)
+        for (int x = 0; x < w; x++)
+            dst[(size_t)r * w + x] = bytes == 2 ? ((const uint16_t*)src)[(size_t)r * stride + x] : ((const uint8_t*)src)[(size_t)r * stride + x];
+}
+
+static void dbk_copy_out(void* dst, const uint16_t* src, int bytes, int stride, int w, int h) {
+    for (int r = 0; r < h; r++)
+        for (int x = 0; x < w; x++) {
+            if (bytes == 2) ((uint16_t*)dst)[(size_t)r * stride + x] = src[(size_t)r * w + x];
+            else ((uint8_t*)dst)[(size_t)r * stride + x] = (uint8_t)src[(size_t)r * w + x];
+        }
+}
+
+int ironav_deblock_picture(ironav_ctx* c, void* y, int y_stride, void* cb, void* cr, int c_stride, const ironav_dbk_mb* mbs,
+                           const ironav_dbk_slice* slices, int nslices) {
+    if (!c || !y || !cb || !cr || !mbs || !slices || nslices < 1 || nslices > 65535 || y_stride < c->pw || c_stride < c->pw / 2)
+        return IRONAV_INVALID_ARGUMENT;
+    int pw = c->pw, ph = c->ph, B = sample_bytes(c);
+    uint16_t* planes[3];
+    planes[0] = (uint16_t*)malloc(sizeof(uint16_t) * (size_t)pw * ph);
+    planes[1] = (uint16_t*)malloc(sizeof(uint16_t) * (size_t)pw * ph / 4);
+    planes[2] = (uint16_t*)malloc(sizeof(uint16_t) * (size_t)pw * ph / 4);
+    dbk_copy_in(planes[0], y, B, y_stride, pw, ph);
+    dbk_copy_in(planes[1], cb, B, c_stride, pw / 2, ph / 2);
+    dbk_copy_in(planes[2], cr, B, c_stride, pw / 2, ph / 2);
+    int bad = 0;
+    for (int mby = 0; mby < c->mb_h; mby++)
+        for (int mbx = 0; mbx < c->mb_w; mbx++) bad |= dbk_mb(planes, mbs, slices, nslices, c->mb_w, c->bd, mbx, mby);
+    dbk_copy_out(y, planes[0], B, y_stride, pw, ph);
+    dbk_copy_out(cb, planes[1], B, c_stride, pw / 2, ph / 2);
+    dbk_copy_out(cr, planes[2], B, c_stride, pw / 2, ph / 2);
+    for (int k = 0; k < 3; k++) free(planes[k]);
+    return bad ? IRONAV_INVALID_INPUT : IRONAV_OK;
+}
+
+int ironav_deblock_picture_device(ironav_ctx* c, void* d_y, int y_stride, void* d_cb, void* d_cr, int c_stride, const ironav_dbk_mb* d_mbs,
+                                  const ironav_dbk_slice* slices, int nslices) {
+    (void)c; (void)d_y; (void)y_stride; (void)d_cb; (void)d_cr; (void)c_stride; (void)d_mbs; (void)slices; (void)nslices;
+    return IRONAV_HARDWARE_UNAVAILABLE;
+}
+
+/* The deblocking tables as the oracle holds them (tests only): alpha[52], beta[52], tc0[52][3] (bS 1..3),
+ * chroma_qp[22]. */
+int oracle_dbk_tables(uint8_t* alpha, uint8_t* beta, uint8_t* tc0, uint8_t* cqp) {
+    memcpy(alpha, DBK_ALPHA, 52);
+    memcpy(beta, DBK_BETA, 52);
+    memcpy(tc0, DBK_TC0, 52 * 3);
+    memcpy(cqp, DBK_CHROMA_QP, 22);
+    return 0;
+}
