@@ -52,7 +52,7 @@ def parse():
     p.add_argument("--ring", type=int, default=RING,
                    help="pictures in the ring (fewer than 36 fits in L2: for profiling runs only)")
     p.add_argument("--no-e2e", action="store_true", help="skip the host-buffer pass (profiling runs)")
-    p.add_argument("--workload", default="1080p", choices=["1080p", "batched", "scenecut"],
+    p.add_argument("--workload", default="1080p", choices=["1080p", "batched", "scenecut", "deblock"],
                    help="1080p: one stream, replay mode (the headline); batched: 64 mixed-resolution streams in auto "
                         "mode, one launch per stage and frame step, against the per-stream launch loop")
     p.add_argument("--streams", type=int, default=64, help="streams of the batched workload")
@@ -258,6 +258,9 @@ def main():
         return finish(world)
     if args.workload == "scenecut":
         run_scenecut(args, rank, world)
+        return finish(world)
+    if args.workload == "deblock":
+        run_deblock(args, rank, world)
         return finish(world)
 
     import torch
@@ -538,6 +541,138 @@ def run_scenecut(args, rank, world):
                                    "(synchronous: returns the totals)"},
             "cpu_baseline": {"value": n_cpu / el_cpu, "unit": "pairs/s", "cores": 1, "kind": "port",
                              "sample": f"{n_cpu} pairs, one thread (the reference's non-live setting)"}}), flush=True)
+
+
+def run_deblock(args, rank, world):
+    """The deblocking filter of 1080p reconstructions (h264/deblock.rs, 4:2:0, frame pictures; the encoder's
+    slice table: 8 row bands, filtered across their edges), device-resident: one step = restore a pristine
+    picture into the working buffers (device copy) + filter it in place. A ring of pictures and records
+    larger than L2. The oracle (the reference's raster-order deblock_picture restated, one thread) is timed
+    on the host over a bounded sample."""
+    import torch
+    from ironav_b200.inter import InterStage, cuda_library
+    from ironav_b200.synth import dbk_encoder_slices, dbk_planes, dbk_records
+
+    bd = args.bd
+    dev = torch.device("cuda", torch.cuda.current_device())
+    lib = cuda_library()
+    st = InterStage(WIDTH, HEIGHT, lib=lib, bd=bd)
+    stream = torch.cuda.Stream()
+    st.set_stream(stream.cuda_stream)
+    mb_w, mb_h, nmb = st.mb_w, st.mb_h, st.nmb
+    ring = max(3, min(args.ring, 40))
+    rng = np.random.default_rng(0xDB0C + rank)
+    pics, recs = [], []
+    for _ in range(ring):
+        pics.append(dbk_planes(rng, mb_w, mb_h, bd))
+        recs.append(dbk_records(rng, mb_w, mb_h, NSLICES, bd, slice_rows=True)[0])
+    slices = dbk_encoder_slices(NSLICES)
+    itemsize = pics[0][0].dtype.itemsize
+    tv = (lambda a: torch.from_numpy(a.view(np.int16) if itemsize == 2 else a))
+    d_y = torch.stack([tv(p[0]) for p in pics]).to(dev)
+    d_cb = torch.stack([tv(p[1]) for p in pics]).to(dev)
+    d_cr = torch.stack([tv(p[2]) for p in pics]).to(dev)
+    d_m = torch.stack([torch.from_numpy(r.view(np.uint8)) for r in recs]).to(dev)
+    w_y, w_cb, w_cr = torch.empty_like(d_y[0]), torch.empty_like(d_cb[0]), torch.empty_like(d_cr[0])
+    ys, cs = mb_w * 16, mb_w * 8
+
+    def step(i, ev=None):
+        t = i % ring
+        w_y.copy_(d_y[t])
+        w_cb.copy_(d_cb[t])
+        w_cr.copy_(d_cr[t])
+        if ev is not None:
+            ev[0].record(stream)
+        st.deblock_device(w_y.data_ptr(), ys, w_cb.data_ptr(), w_cr.data_ptr(), cs, d_m[t].data_ptr(), slices)
+        if ev is not None:
+            ev[1].record(stream)
+
+    with torch.cuda.stream(stream):
+        for i in range(args.warmup):
+            step(i)
+        clocks = Clocks(int(os.environ.get("LOCAL_RANK", 0)))
+        clocks.start()
+        t_load = time.perf_counter()
+        i = 0
+        while time.perf_counter() - t_load < 0.6:
+            step(args.warmup + i)
+            i += 1
+            if i % 8 == 0:
+                torch.cuda.synchronize()
+        torch.cuda.synchronize()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for i in range(args.steps):
+            step(args.warmup + i, evs[i])
+        e1.record(stream)
+        torch.cuda.synchronize()
+        clk = clocks.stop()
+    st.sync()
+    ms = e0.elapsed_time(e1)
+    k_ms = float(np.mean([a.elapsed_time(b) for a, b in evs]))
+    value = world * nmb * args.steps / (ms * 1e-3)
+    bytes_per = 2 * (mb_w * 16 * mb_h * 16 * 3 // 2) * itemsize + nmb * 192  # planes read + written, records read
+    hbm = measured_hbm()
+
+    # end to end through the host-buffer call, pinned host memory
+    pin = [[torch.from_numpy(a.view(np.int16) if itemsize == 2 else a).pin_memory().numpy() for a in p] for p in pics[:8]]
+    pin_m = [torch.from_numpy(r.view(np.uint8)).pin_memory().numpy() for r in recs[:8]]
+    ho = InterStage(WIDTH, HEIGHT, lib=lib, bd=bd)
+    for i in range(args.warmup):
+        lib.ironav_deblock_picture(ho.ctx, pin[i % 8][0].ctypes.data, ys, pin[i % 8][1].ctypes.data, pin[i % 8][2].ctypes.data,
+                                   cs, pin_m[i % 8].ctypes.data, slices.ctypes.data, NSLICES)
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        k = i % 8
+        s_ = lib.ironav_deblock_picture(ho.ctx, pin[k][0].ctypes.data, ys, pin[k][1].ctypes.data, pin[k][2].ctypes.data,
+                                        cs, pin_m[k].ctypes.data, slices.ctypes.data, NSLICES)
+        if s_:
+            raise RuntimeError(f"ironav_deblock_picture: {s_}")
+    el = time.perf_counter() - t0
+
+    line = {
+        "metric": f"1080p deblocking MB/s ({bd}-bit, 4:2:0)", "value": value, "unit": "MB/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u8" if bd == 8 else "u16",
+        "data": "synthetic: ramp + per-4x4-block steps + noise; seeded macroblock records (intra/inter, coded blocks, "
+                "one/two lists, 8x8 transform, keep macroblocks)",
+        "config": {"workload": f"deblock one 1920x1088 {bd}-bit 4:2:0 picture per step (restored from a ring of {ring} "
+                               "by a device copy, then filtered in place)", "slices": NSLICES, "mode": "device pointers",
+                   "l2": f"ring of {ring} pictures and records (> L2)"},
+        "gpu_launches": args.steps,
+        "e2e": {"value": world * nmb * args.steps / el, "unit": "MB/s",
+                "h2d_bytes_per_step": (mb_w * 16 * mb_h * 16 * 3 // 2) * itemsize + nmb * 192 + NSLICES * 20,
+                "d2h_bytes_per_step": (mb_w * 16 * mb_h * 16 * 3 // 2) * itemsize,
+                "ms_per_step": 1e3 * el / args.steps, "note": "ironav_deblock_picture on pinned host buffers, one thread"},
+        "roofline": {"bound": "hbm", "kernel": f"deblock_kernel<{'uint8_t' if bd == 8 else 'uint16_t'}>",
+                     "achieved": bytes_per / (k_ms * 1e-3) / 1e9, "peak": hbm[0], "unit": "GB/s",
+                     "frac": bytes_per / (k_ms * 1e-3) / 1e9 / hbm[0], "peak_source": hbm[1], "ms_per_launch": k_ms,
+                     "traffic": None,
+                     "note": f"latency bound: the macroblock-row wavefront's critical path is mb_w + 2 (mb_h - 1) = "
+                             f"{mb_w + 2 * (mb_h - 1)} macroblock steps"},
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from tests.oracle_lib import oracle_library
+
+        o = InterStage(WIDTH, HEIGHT, lib=oracle_library(), bd=bd)
+        n_cpu, t_cpu = 0, 0.0
+        while t_cpu < min(args.cpu_seconds, 10.0):
+            k = n_cpu % ring
+            y, cb, cr = (a.copy() for a in pics[k])
+            t0 = time.perf_counter()
+            o.lib.ironav_deblock_picture(o.ctx, y.ctypes.data, ys, cb.ctypes.data, cr.ctypes.data, cs, recs[k].ctypes.data,
+                                         slices.ctypes.data, NSLICES)
+            t_cpu += time.perf_counter() - t0
+            n_cpu += 1
+        line["cpu_baseline"] = {"value": n_cpu * nmb / t_cpu, "unit": "MB/s", "cores": 1, "kind": "port",
+                                "sample": f"{n_cpu} pictures, the oracle's raster-order filter on one thread "
+                                          f"(deblock_picture), {t_cpu:.1f} s"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    st.close()
+    ho.close()
 
 
 def ctypes_peak(lib):

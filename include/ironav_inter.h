@@ -208,7 +208,9 @@ typedef struct ironav_dbk_slice {
 int ironav_deblock_picture(ironav_ctx* ctx, void* y, int y_stride, void* cb, void* cr, int c_stride,
                            const ironav_dbk_mb* mbs, const ironav_dbk_slice* slices, int nslices);
 /* The same on device pointers (planes and mbs), queued on the context's stream; slices is a host array,
- * copied before the call returns. ironav_ctx_sync reports a slice id out of range. */
+ * copied before the call returns. ironav_ctx_sync reports a slice id out of range. The planes must start
+ * on 16-byte boundaries, luma rows a multiple of 16 bytes apart and chroma rows a multiple of 8 samples
+ * apart (IRONAV_INVALID_ARGUMENT otherwise; the host form has no such rule). */
 int ironav_deblock_picture_device(ironav_ctx* ctx, void* d_y, int y_stride, void* d_cb, void* d_cr, int c_stride,
                                   const ironav_dbk_mb* d_mbs, const ironav_dbk_slice* slices, int nslices);
 

@@ -53,6 +53,7 @@ struct ironav_ctx {
     int dbk_slice_cap = 0;
     ironav_dbk_mb* d_dbk_mbs = nullptr;
     uint8_t* d_dbk_planes = nullptr;
+    void* d_dbk_edges = nullptr;  // per macroblock: strengths and edge thresholds (pass 1 -> pass 2)
 };
 
 

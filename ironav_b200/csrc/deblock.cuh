@@ -44,19 +44,12 @@ struct DbkParams {
     const ironav_dbk_mb* mbs;
     const ironav_dbk_slice* slices;
     int nslices, mb_w, mb_h, bd;
-    unsigned* progress;               // per macroblock row: macroblocks filtered (zeroed before the launch)
+    unsigned* progress;               // per macroblock row, luma then chroma: macroblocks done (zeroed before the launch)
     unsigned* ticket;                 // next row
     unsigned* err;                    // 1: a wait gave up; 4: a slice id beyond the table
     unsigned wait_limit;              // polls before a wait gives up
 };
 
-// Per-warp shared memory.
-struct DbkWarp {
-    int L[20][21];                    // luma rows y0-4..y0+15 (index +4), columns x0-4..x0+15 (index +4); odd stride
-    int C[2][10][11];                 // Cb, Cr rows yc-2..yc+7, columns xc-2..xc+7
-    ironav_dbk_mb mb[3];              // the macroblock, its left and its top neighbour
-    uint8_t bs[2][4][4];              // boundary strengths [dir][edge][segment]
-};
 
 // chroma_qp, h264/mb.rs:214-221
 __device__ __forceinline__ int dbk_chroma_qp(int qp, int off, int bd) {
@@ -159,165 +152,325 @@ __device__ __forceinline__ void dbk_line(int* q, int xs, int b, int tc0, int alp
     }
 }
 
-// The thresholds of one edge (deblock.rs:647-651, 680-683): alpha, beta, and indexA in .z; alpha == 0
-// or beta == 0 means the edge is left alone (filter_edge, deblock.rs:233-235).
-__device__ __forceinline__ int3 dbk_thresholds(int qpav, const ironav_dbk_slice& sp, int bd) {
+// The thresholds of one edge (deblock.rs:647-651, 680-683), packed alpha' | beta' << 8 | tC0(bS 1, 2, 3)
+// << 13, 18, 23 (all before the bit-depth shift; beta' <= 18 and tC0 <= 25 fit 5 bits); 0 when alpha' or
+// beta' is 0 (filter_edge leaves the edge alone, deblock.rs:233-235).
+__device__ __forceinline__ uint32_t dbk_thresholds(int qpav, const ironav_dbk_slice& sp) {
     const int ia = min(max(qpav + sp.alpha_offset, 0), 51), ib = min(max(qpav + sp.beta_offset, 0), 51);
-    return make_int3((int)c_dbk_alpha[ia] << (bd - 8), (int)c_dbk_beta[ib] << (bd - 8), ia);
+    const uint32_t a = c_dbk_alpha[ia], b = c_dbk_beta[ib];
+    if (a == 0 || b == 0) return 0u;
+    return a | b << 8 | (uint32_t)c_dbk_tc0[ia][0] << 13 | (uint32_t)c_dbk_tc0[ia][1] << 18 | (uint32_t)c_dbk_tc0[ia][2] << 23;
 }
 
-// deblock_mb, deblock.rs:608-695, for macroblock (x, y) of a 4:2:0 frame picture, by one warp.
-template <class T>
-__device__ void dbk_mb(const DbkParams& __restrict__ P, DbkWarp& __restrict__ W, int x, int y) {
-    const int lane = threadIdx.x & 31;
-    const int idx = y * P.mb_w + x;
-    // the three macroblock records (48 words each)
-    for (int k = lane; k < 3 * 48; k += 32) {
-        const int which = k / 48, wd = k % 48;
-        const int src = which == 0 ? idx : (which == 1 ? (x > 0 ? idx - 1 : idx) : (y > 0 ? idx - P.mb_w : idx));
-        reinterpret_cast<uint32_t*>(&W.mb[which])[wd] = __ldg(reinterpret_cast<const uint32_t*>(&P.mbs[src]) + wd);
-    }
-    __syncwarp();
-    const ironav_dbk_mb& m = W.mb[0];
-    if (m.slice == 0) return;
-    if (m.slice > P.nslices) {
-        if (lane == 0) atomicOr(P.err, 4u);
-        return;
-    }
-    const ironav_dbk_slice sp = P.slices[m.slice - 1];
-    if (sp.disable_deblocking == 1) return;
-    // the neighbours across the left and top edges; at the picture's edges the macroblock itself, whose
-    // outer edges are then not filtered (deblock.rs:618-621)
-    const ironav_dbk_mb& lm = W.mb[1];
-    const ironav_dbk_mb& tm = W.mb[2];
-    const bool left_ok = x > 0 && lm.slice != 0 && (sp.disable_deblocking == 0 || lm.slice == m.slice);
-    const bool top_ok = y > 0 && tm.slice != 0 && (sp.disable_deblocking == 0 || tm.slice == m.slice);
-    // inner edges of an inter macroblock moving as a whole with no coefficients are not filtered
-    // (uniform_motion, deblock.rs:385-389, and deblock.rs:625)
-    bool same = true;
-    if (lane < 16) {
-        same = m.nnz[lane] == 0 && m.mv[0][lane][0] == m.mv[0][0][0] && m.mv[0][lane][1] == m.mv[0][0][1] &&
-               m.mv[1][lane][0] == m.mv[1][0][0] && m.mv[1][lane][1] == m.mv[1][0][1];
-        if (lane < 4)
-            same = same && m.ref_idx[0][lane] == m.ref_idx[0][0] && m.ref_idx[1][lane] == m.ref_idx[1][0] &&
-                   m.ref_id[0][lane] == m.ref_id[0][0] && m.ref_id[1][lane] == m.ref_id[1][0];
-    }
-    const bool still = m.inter && __all_sync(DBK_ALL, same);
-    // boundary strengths (strength, deblock.rs:391-408): lane = dir * 16 + edge * 4 + segment
-    {
-        const int dir = lane >> 4, e = (lane >> 2) & 3, i = lane & 3;
-        const ironav_dbk_mb& o = e == 0 ? (dir == 0 ? lm : tm) : m;
-        int b = 0;
-        if (!(e > 0 && still)) {
-            if (!m.inter || !o.inter) {
-                b = e == 0 ? 4 : 3;
-            } else {
-                const int qx = dir == 0 ? e : i, qy = dir == 0 ? i : e;
-                const int px = dir == 0 ? (e == 0 ? 3 : e - 1) : i, py = dir == 0 ? i : (e == 0 ? 3 : e - 1);
-                b = (dbk_coded(m, qx, qy) || dbk_coded(o, px, py)) ? 2 : (dbk_motion_differs(o, px, py, m, qx, qy) ? 1 : 0);
-            }
+// What the filter of one macroblock needs besides its samples, worked out before the wavefront (it depends
+// on the macroblock records only). An edge word is its thresholds (dbk_thresholds) | keep << 28 (bit 0:
+// the p side is a keep macroblock, bit 1: the q side); 0 means the edge is not filtered at all.
+struct DbkEdges {
+    uint8_t bs[2][4][4];        // [dir][edge][segment]
+    uint32_t luma[2][4];        // [dir][edge]
+    uint32_t chroma[2][2][2];   // [comp][dir][edge / 2]
+};
+static_assert(sizeof(DbkEdges) == 96, "DbkEdges layout");
+
+// Pass 1: the boundary strengths (strength, deblock.rs:391-408) and edge words of every macroblock
+// (deblock_mb's decisions, deblock.rs:608-695), one warp per macroblock, all macroblocks independent.
+__global__ void __launch_bounds__(DBK_WARPS * 32) deblock_edges_kernel(const __grid_constant__ DbkParams P, DbkEdges* __restrict__ out) {
+    __shared__ ironav_dbk_mb rec[DBK_WARPS][3];
+    __shared__ uint8_t bsm[DBK_WARPS][2][4][4];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int nmb = P.mb_w * P.mb_h;
+    for (int idx = blockIdx.x * DBK_WARPS + wid; idx < nmb; idx += gridDim.x * DBK_WARPS) {
+        const int x = idx % P.mb_w, y = idx / P.mb_w;
+        for (int k = lane; k < 3 * 48; k += 32) {
+            const int which = k / 48, wd = k % 48;
+            const int src = which == 0 ? idx : (which == 1 ? (x > 0 ? idx - 1 : idx) : (y > 0 ? idx - P.mb_w : idx));
+            reinterpret_cast<uint32_t*>(&rec[wid][which])[wd] = __ldg(reinterpret_cast<const uint32_t*>(&P.mbs[src]) + wd);
         }
-        W.bs[dir][e][i] = (uint8_t)b;
-    }
-    // stage the macroblock's samples with 4 (luma) / 2 (chroma) samples to the left and above
-    const T* Y = reinterpret_cast<const T*>(P.planes[0]);
-    const int x0 = x * 16, y0 = y * 16, xc = x * 8, yc = y * 8;
-    for (int t = lane; t < 400; t += 32) {
-        const int rr = t / 20, cc = t % 20;
-        if ((rr < 4 && (y == 0 || cc < 4)) || (cc < 4 && x == 0)) continue;
-        W.L[rr][cc] = __ldcg(Y + (size_t)(y0 - 4 + rr) * P.ys + (x0 - 4 + cc));
-    }
-    for (int t = lane; t < 200; t += 32) {
-        const int comp = t / 100, rr = (t % 100) / 10, cc = t % 10;
-        if ((rr < 2 && (y == 0 || cc < 2)) || (cc < 2 && x == 0)) continue;
-        const T* Cp = reinterpret_cast<const T*>(P.planes[1 + comp]);
-        W.C[comp][rr][cc] = __ldcg(Cp + (size_t)(yc - 2 + rr) * P.cs + (xc - 2 + cc));
-    }
-    __syncwarp();
-    const int maxv = (1 << P.bd) - 1;
-    // dir 0: vertical edges, a lane per row; dir 1: horizontal edges, a lane per column
-    for (int dir = 0; dir < 2; dir++) {
-        const bool outer_ok = dir == 0 ? left_ok : top_ok;
-        const ironav_dbk_mb& o0 = dir == 0 ? lm : tm;
+        __syncwarp();
+        const ironav_dbk_mb& m = rec[wid][0];
+        // the neighbours across the left and top edges; at the picture's edges the macroblock itself, whose
+        // outer edges are then not filtered (deblock.rs:618-621)
+        const ironav_dbk_mb& lm = rec[wid][1];
+        const ironav_dbk_mb& tm = rec[wid][2];
+        bool live = m.slice != 0;
+        if (live && m.slice > P.nslices) {
+            if (lane == 0) atomicOr(P.err, 4u);
+            live = false;
+        }
+        ironav_dbk_slice sp = {};
+        if (live) sp = P.slices[m.slice - 1];
+        live = live && sp.disable_deblocking != 1;
+        const bool left_ok = x > 0 && lm.slice != 0 && (sp.disable_deblocking == 0 || lm.slice == m.slice);
+        const bool top_ok = y > 0 && tm.slice != 0 && (sp.disable_deblocking == 0 || tm.slice == m.slice);
+        // inner edges of an inter macroblock moving as a whole with no coefficients are not filtered
+        // (uniform_motion, deblock.rs:385-389, and deblock.rs:625)
+        bool same = true;
         if (lane < 16) {
-            const int line = lane;
-            for (int e = 0; e < 4; e++) {
-                if (e == 0 && !outer_ok) continue;
-                if (m.t8x8 && (e & 1)) continue;
-                const int b = W.bs[dir][e][line >> 2];
-                if (b == 0) continue;
-                const ironav_dbk_mb& o = e == 0 ? o0 : m;
-                const int3 th = dbk_thresholds((o.qp + m.qp + 1) >> 1, sp, P.bd);
-                if (th.x == 0 || th.y == 0) continue;
-                const int tc0 = b < 4 ? (int)c_dbk_tc0[th.z][b - 1] << (P.bd - 8) : 0;
-                int* q = dir == 0 ? &W.L[line + 4][4 * e + 4] : &W.L[4 * e + 4][line + 4];
-                dbk_line(q, dir == 0 ? 1 : 21, b, tc0, th.x, th.y, false, maxv, o.keep, m.keep);
+            same = m.nnz[lane] == 0 && m.mv[0][lane][0] == m.mv[0][0][0] && m.mv[0][lane][1] == m.mv[0][0][1] &&
+                   m.mv[1][lane][0] == m.mv[1][0][0] && m.mv[1][lane][1] == m.mv[1][0][1];
+            if (lane < 4)
+                same = same && m.ref_idx[0][lane] == m.ref_idx[0][0] && m.ref_idx[1][lane] == m.ref_idx[1][0] &&
+                       m.ref_id[0][lane] == m.ref_id[0][0] && m.ref_id[1][lane] == m.ref_id[1][0];
+        }
+        const bool still = m.inter && __all_sync(DBK_ALL, same);
+        // boundary strengths: lane = dir * 16 + edge * 4 + segment
+        {
+            const int dir = lane >> 4, e = (lane >> 2) & 3, i = lane & 3;
+            const ironav_dbk_mb& o = e == 0 ? (dir == 0 ? lm : tm) : m;
+            int b = 0;
+            if (!(e > 0 && still)) {
+                if (!m.inter || !o.inter) {
+                    b = e == 0 ? 4 : 3;
+                } else {
+                    const int qx = dir == 0 ? e : i, qy = dir == 0 ? i : e;
+                    const int px = dir == 0 ? (e == 0 ? 3 : e - 1) : i, py = dir == 0 ? i : (e == 0 ? 3 : e - 1);
+                    b = (dbk_coded(m, qx, qy) || dbk_coded(o, px, py)) ? 2 : (dbk_motion_differs(o, px, py, m, qx, qy) ? 1 : 0);
+                }
             }
-        } else {
-            const int comp = (lane - 16) >> 3, line = lane & 7;
-            for (int e = 0; e < 4; e += 2) {
-                if (e == 0 && !outer_ok) continue;
-                const int b = W.bs[dir][e][line >> 1];
-                if (b == 0) continue;
-                const ironav_dbk_mb& o = e == 0 ? o0 : m;
-                const int off = sp.chroma_qp_offset[comp];
-                const int3 th = dbk_thresholds((dbk_chroma_qp(o.qp, off, P.bd) + dbk_chroma_qp(m.qp, off, P.bd) + 1) >> 1, sp, P.bd);
-                if (th.x == 0 || th.y == 0) continue;
-                const int tc0 = b < 4 ? (int)c_dbk_tc0[th.z][b - 1] << (P.bd - 8) : 0;
-                int* q = dir == 0 ? &W.C[comp][line + 2][2 * e + 2] : &W.C[comp][2 * e + 2][line + 2];
-                dbk_line(q, dir == 0 ? 1 : 11, b, tc0, th.x, th.y, true, maxv, o.keep, m.keep);
+            bsm[wid][dir][e][i] = (uint8_t)b;
+        }
+        __syncwarp();
+        DbkEdges& E = out[idx];
+        if (lane < 8) reinterpret_cast<uint32_t*>(E.bs)[lane] = reinterpret_cast<const uint32_t*>(bsm[wid])[lane];
+        // edge words: lanes 0-7 luma (dir, edge), lanes 8-15 chroma (comp, dir, edge / 2)
+        if (lane < 16) {
+            const bool chroma = lane >= 8;
+            const int dir = chroma ? ((lane - 8) >> 1) & 1 : lane >> 2;
+            const int e = chroma ? ((lane - 8) & 1) * 2 : lane & 3;
+            const int comp = (lane - 8) >> 2;
+            const ironav_dbk_mb& o = e == 0 ? (dir == 0 ? lm : tm) : m;
+            const bool any = *reinterpret_cast<const uint32_t*>(bsm[wid][dir][e]) != 0;
+            uint32_t wv = 0;
+            if (live && any && !(e == 0 && !(dir == 0 ? left_ok : top_ok)) && !(!chroma && m.t8x8 && (e & 1))) {
+                if (chroma) {
+                    const int off = sp.chroma_qp_offset[comp];
+                    wv = dbk_thresholds((dbk_chroma_qp(o.qp, off, P.bd) + dbk_chroma_qp(m.qp, off, P.bd) + 1) >> 1, sp);
+                } else {
+                    wv = dbk_thresholds((o.qp + m.qp + 1) >> 1, sp);
+                }
+                if (wv) wv |= (uint32_t)((o.keep ? 1 : 0) | (m.keep ? 2 : 0)) << 28;
             }
+            if (chroma) E.chroma[comp][dir][e >> 1] = wv;
+            else E.luma[dir][e] = wv;
         }
         __syncwarp();
     }
-    // write back what the filter may have changed: the macroblock, 3 luma / 1 chroma samples to its left
-    // and above
-    T* Yw = reinterpret_cast<T*>(P.planes[0]);
-    for (int t = lane; t < 400; t += 32) {
-        const int rr = t / 20, cc = t % 20;
-        if (rr == 0 || cc == 0 || (rr < 4 && (y == 0 || cc < 4)) || (cc < 4 && x == 0)) continue;
-        __stcg(Yw + (size_t)(y0 - 4 + rr) * P.ys + (x0 - 4 + cc), (T)W.L[rr][cc]);
+}
+
+// ---- pass 2: the samples, in the row wavefront ---------------------------------------------------------
+
+// N samples of type T at p (aligned to their size, at most 16 bytes) into ints, through L2; and back.
+template <class T, int N>
+__device__ __forceinline__ void dbk_load(const T* p, int* v) {
+    constexpr int NB = N * (int)sizeof(T);
+    uint32_t w[NB >= 4 ? NB / 4 : 1];
+    if constexpr (NB == 16) {
+        const uint4 q = __ldcg(reinterpret_cast<const uint4*>(p));
+        w[0] = q.x, w[1] = q.y, w[2] = q.z, w[3] = q.w;
+    } else if constexpr (NB == 8) {
+        const uint2 q = __ldcg(reinterpret_cast<const uint2*>(p));
+        w[0] = q.x, w[1] = q.y;
+    } else if constexpr (NB == 4) {
+        w[0] = __ldcg(reinterpret_cast<const unsigned*>(p));
+    } else {
+        w[0] = __ldcg(reinterpret_cast<const unsigned short*>(p));
     }
-    for (int t = lane; t < 200; t += 32) {
-        const int comp = t / 100, rr = (t % 100) / 10, cc = t % 10;
-        if (rr == 0 || cc == 0 || (rr < 2 && (y == 0 || cc < 2)) || (cc < 2 && x == 0)) continue;
-        T* Cp = reinterpret_cast<T*>(P.planes[1 + comp]);
-        __stcg(Cp + (size_t)(yc - 2 + rr) * P.cs + (xc - 2 + cc), (T)W.C[comp][rr][cc]);
+#pragma unroll
+    for (int k = 0; k < N; k++) v[k] = (int)((w[(k * (int)sizeof(T)) >> 2] >> ((k * 8 * (int)sizeof(T)) & 31)) & ((1u << (8 * sizeof(T))) - 1));
+}
+template <class T, int N>
+__device__ __forceinline__ void dbk_store(T* p, const int* v) {
+    constexpr int NB = N * (int)sizeof(T);
+    uint32_t w[NB >= 4 ? NB / 4 : 1] = {};
+#pragma unroll
+    for (int k = 0; k < N; k++) w[(k * (int)sizeof(T)) >> 2] |= (uint32_t)v[k] << ((k * 8 * (int)sizeof(T)) & 31);
+    if constexpr (NB == 16) __stcg(reinterpret_cast<uint4*>(p), make_uint4(w[0], w[1], w[2], w[3]));
+    else if constexpr (NB == 8) __stcg(reinterpret_cast<uint2*>(p), make_uint2(w[0], w[1]));
+    else if constexpr (NB == 4) __stcg(reinterpret_cast<unsigned*>(p), w[0]);
+    else __stcg(reinterpret_cast<unsigned short*>(p), (unsigned short)w[0]);
+}
+// Up to 16 samples (two 16-byte pieces for 16 samples of 16 bits).
+template <class T, int N>
+__device__ __forceinline__ void dbk_load_row(const T* p, int* v) {
+    if constexpr (N * sizeof(T) > 16) {
+        dbk_load<T, N / 2>(p, v);
+        dbk_load<T, N / 2>(p + N / 2, v + N / 2);
+    } else {
+        dbk_load<T, N>(p, v);
+    }
+}
+template <class T, int N>
+__device__ __forceinline__ void dbk_store_row(T* p, const int* v) {
+    if constexpr (N * sizeof(T) > 16) {
+        dbk_store<T, N / 2>(p, v);
+        dbk_store<T, N / 2>(p + N / 2, v + N / 2);
+    } else {
+        dbk_store<T, N>(p, v);
     }
 }
 
-// Waits until row `row` has filtered `need` macroblocks, at most P.wait_limit polls; false when it gave up
-// or another warp already did.
-__device__ __forceinline__ bool dbk_wait(const DbkParams& P, int row, unsigned need) {
+// Filters the edges across one line of NS samples (luma: 20 = 4 before the macroblock + 16; chroma: 10 =
+// 2 + 8) in registers: luma edges at 4, 8, 12, 16; chroma edges at 2 and 6.
+template <bool CHROMA, int NS>
+__device__ __forceinline__ void dbk_filter_lines(int (&v)[NS], const uint32_t* words, const uint8_t (*bs)[4], int seg, int bd, int maxv) {
+#pragma unroll
+    for (int k = 0; k < (CHROMA ? 2 : 4); k++) {
+        const uint32_t wv = words[k];
+        const int e = CHROMA ? 2 * k : k;
+        const int b = bs[e][seg];
+        if (wv == 0 || b == 0) continue;
+        const int alpha = (int)(wv & 0xff) << (bd - 8), beta = (int)((wv >> 8) & 0x1f) << (bd - 8);
+        const int tc0 = b < 4 ? (int)((wv >> (8 + 5 * b)) & 0x1f) << (bd - 8) : 0;
+        dbk_line(&v[CHROMA ? 2 + 4 * k : 4 + 4 * k], 1, b, tc0, alpha, beta, CHROMA, maxv, (wv >> 28) & 1, (wv >> 29) & 1);
+    }
+}
+
+__device__ __forceinline__ unsigned ld_relaxed(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Waits until progress word `w` reaches `need`, at most P.wait_limit polls; false when it gave up or
+// another warp already did (the error word is looked at every 64 polls). Relaxed polls, then one acquire
+// fence: with the writer's release store they order the writer's samples before this warp's loads.
+__device__ __forceinline__ bool dbk_wait(const DbkParams& P, const unsigned* w, unsigned need) {
     for (unsigned i = 0;; i++) {
-        if (ld_acquire(&P.progress[row]) >= need) return true;
-        if (ld_acquire(P.err) & 1u) return false;
-        if (i >= P.wait_limit) {
-            atomicOr(P.err, 1u);
-            return false;
+        if (ld_relaxed(w) >= need) {
+            asm volatile("fence.acq_rel.gpu;" ::: "memory");
+            return true;
         }
-        __nanosleep(i < 64 ? 32 : 256);
+        if ((i & 63) == 63) {
+            if (ld_acquire(P.err) & 1u) return false;
+            if (i >= P.wait_limit) {
+                atomicOr(P.err, 1u);
+                return false;
+            }
+        }
+        if (i >= 16) __nanosleep(64);
     }
 }
 
-template <class T>
-__global__ void __launch_bounds__(DBK_WARPS * 32) deblock_kernel(const __grid_constant__ DbkParams P) {
-    __shared__ DbkWarp smem[DBK_WARPS];
-    DbkWarp& W = smem[threadIdx.x >> 5];
+// Pass 2 for one macroblock row of one plane kind, left to right, by one warp. Luma: lanes 0-15 hold the
+// macroblock's 16 rows (each with the 4 samples to its left); chroma: lanes 0-7 the Cb rows, 8-15 the Cr
+// rows (each with 2 to the left); lanes 16-31 idle. The vertical edges are filtered in those registers,
+// the horizontal ones on columns read back from a shared-memory tile that also holds the rows above (4
+// luma / 2 chroma). The next macroblock's own samples and edge words are loaded while the current one
+// waits and filters. The vertical edges come first and need nothing from the row above; they make the
+// previous macroblock final (its last columns are the left edge's p side), so the warp stores those columns
+// and publishes progress x + 1 (macroblocks 0..x-1 final) before it waits for the row above, loads the rows
+// above and filters the horizontal edges.
+template <class T, bool CHROMA>
+__device__ __forceinline__ void dbk_row(const DbkParams& P, const DbkEdges* __restrict__ edges, int y, int (*L)[17],
+                                        DbkEdges& E) {
+    constexpr int W = CHROMA ? 8 : 16;   // samples of a macroblock row
+    constexpr int LEFT = CHROMA ? 2 : 4; // samples kept to its left
+    constexpr int H = CHROMA ? 2 : 4;    // rows above
     const int lane = threadIdx.x & 31;
+    const bool active = lane < 16;
+    const int comp = CHROMA ? lane >> 3 : 0, line = CHROMA ? lane & 7 : lane;
+    T* const Pl = reinterpret_cast<T*>(P.planes[CHROMA ? 1 + comp : 0]);
+    const int stride = CHROMA ? P.cs : P.ys;
+    // the tile: luma rows y0-4..y0+15 in L[0..19]; chroma comp c rows yc-2..yc+7 in L[10c .. 10c+9]
+    int (*Tl)[17] = CHROMA ? L + 10 * comp : L;
+    const size_t lrow = (size_t)(y * (CHROMA ? 8 : 16) + line) * stride;
+    const unsigned* above = P.progress + (CHROMA ? P.mb_h : 0) + (y - 1);
+    unsigned* mine = P.progress + (CHROMA ? P.mb_h : 0) + y;
+    const int maxv = (1 << P.bd) - 1;
+    int lv[LEFT + W];
+    int own[W];
+    uint32_t ew = 0;
+    auto prefetch = [&](int x) {
+        if (active) dbk_load_row<T, W>(Pl + lrow + x * W, own);
+        if (lane < 24) ew = __ldg(reinterpret_cast<const uint32_t*>(&edges[(size_t)y * P.mb_w + x]) + lane);
+    };
+    prefetch(0);
+    for (int x = 0; x < P.mb_w; x++) {
+        if (active) {
+#pragma unroll
+            for (int k = 0; k < W; k++) lv[LEFT + k] = own[k];
+        }
+        if (lane < 24) reinterpret_cast<uint32_t*>(&E)[lane] = ew;
+        __syncwarp();
+        // vertical edges, in registers: they touch this row of macroblocks only, so they need nothing
+        // from the row above
+        if (active) {
+            const uint32_t* words = CHROMA ? E.chroma[comp][0] : E.luma[0];
+            dbk_filter_lines<CHROMA, LEFT + W>(lv, words, E.bs[0], CHROMA ? line >> 1 : line >> 2, P.bd, maxv);
+            // the previous macroblock's last columns are final now: store them and publish it
+            if (x > 0) dbk_store<T, LEFT>(Pl + lrow + x * W - LEFT, lv);
+        }
+        __syncwarp();
+        if (lane == 0) st_release(mine, (unsigned)(x + 1));  // the warp's stores, ordered by the barrier above
+        // the next macroblock's samples and edge words (after the fence, which would wait for them)
+        if (x + 1 < P.mb_w) prefetch(x + 1);
+        // macroblocks 0..x+1 of the row above final (its last two macroblocks: the whole row, whose final
+        // publish is mb_w + 1)
+        const unsigned need = x + 2 < P.mb_w ? (unsigned)(x + 2) : (unsigned)P.mb_w + 1;
+        if (y > 0 && !__all_sync(DBK_ALL, dbk_wait(P, above, need))) return;
+        // the rows above, one lane each
+        if (y > 0 && lane < 4) {
+            const int cc = CHROMA ? lane >> 1 : 0, rr = CHROMA ? lane & 1 : lane;
+            const T* src = reinterpret_cast<const T*>(P.planes[CHROMA ? 1 + cc : 0]) + (size_t)(y * (CHROMA ? 8 : 16) - H + rr) * stride + x * W;
+            int r[W];
+            dbk_load_row<T, W>(src, r);
+            int (*dst)[17] = CHROMA ? L + 10 * cc : L;
+#pragma unroll
+            for (int k = 0; k < W; k++) dst[rr][k] = r[k];
+        }
+        if (active) {
+#pragma unroll
+            for (int k = 0; k < W; k++) Tl[H + line][k] = lv[LEFT + k];
+        }
+        __syncwarp();
+        if (active) {
+            // horizontal edges, a lane per column of the tile
+            int cv[H + W];
+#pragma unroll
+            for (int k = 0; k < H + W; k++) cv[k] = Tl[k][line];
+            const uint32_t* words = CHROMA ? E.chroma[comp][1] : E.luma[1];
+            dbk_filter_lines<CHROMA, H + W>(cv, words, E.bs[1], CHROMA ? line >> 1 : line >> 2, P.bd, maxv);
+#pragma unroll
+            for (int k = 1; k < H + W; k++) Tl[k][line] = cv[k];
+        }
+        __syncwarp();
+        if (active) {
+#pragma unroll
+            for (int k = 0; k < W; k++) lv[LEFT + k] = Tl[H + line][k];
+            dbk_store_row<T, W>(Pl + lrow + x * W, &lv[LEFT]);
+            if (y > 0 && line >= 1 && line < H) {
+                int r[W];
+#pragma unroll
+                for (int k = 0; k < W; k++) r[k] = Tl[line][k];
+                dbk_store_row<T, W>(Pl + (size_t)(y * (CHROMA ? 8 : 16) - H + line) * stride + x * W, r);
+            }
+            // this macroblock's last columns are the next one's left samples
+#pragma unroll
+            for (int k = 0; k < LEFT; k++) lv[k] = lv[W + k];
+        }
+        __syncwarp();
+    }
+    // the last macroblock's own rows were stored after the last publish: publish them too
+    __syncwarp();
+    if (lane == 0) st_release(mine, (unsigned)P.mb_w + 1);
+}
+
+// Pass 2: macroblock rows of the two plane kinds handed out by ticket (2y: luma row y, 2y + 1: chroma row y);
+// a row waits only on the row above of its own kind, which holds a smaller ticket.
+template <class T>
+__global__ void __launch_bounds__(DBK_WARPS * 32) deblock_rows_kernel(const __grid_constant__ DbkParams P,
+                                                                      const DbkEdges* __restrict__ edges) {
+    __shared__ int Ls[DBK_WARPS][20][17];
+    __shared__ DbkEdges Es[DBK_WARPS];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     for (;;) {
         unsigned t = 0;
         if (lane == 0) t = atomicAdd(P.ticket, 1u);
         t = __shfl_sync(DBK_ALL, t, 0);
-        if (t >= (unsigned)P.mb_h) return;
-        const int y = (int)t;
-        for (int x = 0; x < P.mb_w; x++) {
-            if (y > 0 && !__all_sync(DBK_ALL, dbk_wait(P, y - 1, (unsigned)min(x + 2, P.mb_w)))) return;
-            dbk_mb<T>(P, W, x, y);
-            __threadfence();
-            __syncwarp();
-            if (lane == 0) st_release(&P.progress[y], (unsigned)(x + 1));
-        }
+        if (t >= 2u * (unsigned)P.mb_h) return;
+        if (t & 1u) dbk_row<T, true>(P, edges, (int)(t >> 1), Ls[wid], Es[wid]);
+        else dbk_row<T, false>(P, edges, (int)(t >> 1), Ls[wid], Es[wid]);
+        if (ld_acquire(P.err) & 1u) return;
     }
 }
 

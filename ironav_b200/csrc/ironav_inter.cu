@@ -107,6 +107,7 @@ void free_ctx(ironav_ctx* c) {
     cudaFree(c->d_dbk_slices);
     cudaFree(c->d_dbk_mbs);
     cudaFree(c->d_dbk_planes);
+    cudaFree(c->d_dbk_edges);
     cudaFreeHost(c->h_results);
     cudaFreeHost(c->h_done);
     cudaFreeHost(c->h_committed);
@@ -210,7 +211,8 @@ int scene_run(ironav_ctx* c, const void* d_prev, int sp, const void* d_cur, int 
 // macroblock records at d_mbs and the slice table from the host.
 int deblock_launch(ironav_ctx* c, void* d_y, int ys, void* d_cb, void* d_cr, int cs, const ironav_dbk_mb* d_mbs,
                    const ironav_dbk_slice* slices, int nslices) {
-    if (!c->d_dbk_progress) CK(cudaMalloc(&c->d_dbk_progress, sizeof(unsigned) * c->mb_h));
+    if (!c->d_dbk_progress) CK(cudaMalloc(&c->d_dbk_progress, sizeof(unsigned) * 2 * c->mb_h));
+    if (!c->d_dbk_edges) CK(cudaMalloc(&c->d_dbk_edges, sizeof(DbkEdges) * c->nmb));
     if (nslices > c->dbk_slice_cap) {
         CK(cudaStreamSynchronize(c->stream));  // the old table may still be read by queued work
         cudaFree(c->d_dbk_slices);
@@ -221,7 +223,7 @@ int deblock_launch(ironav_ctx* c, void* d_y, int ys, void* d_cb, void* d_cr, int
         c->dbk_slice_cap = cap;
     }
     CK(cudaMemcpyAsync(c->d_dbk_slices, slices, sizeof(ironav_dbk_slice) * nslices, cudaMemcpyHostToDevice, c->stream));
-    CK(cudaMemsetAsync(c->d_dbk_progress, 0, sizeof(unsigned) * c->mb_h, c->stream));
+    CK(cudaMemsetAsync(c->d_dbk_progress, 0, sizeof(unsigned) * 2 * c->mb_h, c->stream));
     CK(cudaMemsetAsync(c->d_counters, 0, 2 * sizeof(unsigned), c->stream));
     DbkParams p;
     p.planes[0] = static_cast<uint8_t*>(d_y);
@@ -239,15 +241,22 @@ int deblock_launch(ironav_ctx* c, void* d_y, int ys, void* d_cb, void* d_cr, int
     p.ticket = c->d_counters;
     p.err = c->d_counters + 1;
     p.wait_limit = c->wait_limit;
-    const int blocks = (c->mb_h + DBK_WARPS - 1) / DBK_WARPS;
-    if (c->bd > 8) deblock_kernel<uint16_t><<<blocks, DBK_WARPS * 32, 0, c->stream>>>(p);
-    else deblock_kernel<uint8_t><<<blocks, DBK_WARPS * 32, 0, c->stream>>>(p);
+    DbkEdges* edges = static_cast<DbkEdges*>(c->d_dbk_edges);
+    const int eblocks = std::min((c->nmb + DBK_WARPS - 1) / DBK_WARPS, c->nsm * 16);
+    deblock_edges_kernel<<<eblocks, DBK_WARPS * 32, 0, c->stream>>>(p, edges);
+    const int blocks = (2 * c->mb_h + DBK_WARPS - 1) / DBK_WARPS;
+    if (c->bd > 8) deblock_rows_kernel<uint16_t><<<blocks, DBK_WARPS * 32, 0, c->stream>>>(p, edges);
+    else deblock_rows_kernel<uint8_t><<<blocks, DBK_WARPS * 32, 0, c->stream>>>(p, edges);
     return cuda_status(cudaGetLastError());
 }
 
+// The kernel moves whole rows of a macroblock with 16-byte (luma) and 8 / 16-byte (chroma) accesses: plane
+// bases 16-byte aligned, luma rows a multiple of 16 bytes apart, chroma rows a multiple of 8 samples apart.
 bool deblock_args_ok(const ironav_ctx* c, const void* y, int ys, const void* cb, const void* cr, int cs, const void* mbs,
                      const ironav_dbk_slice* slices, int nslices) {
-    return c && y && cb && cr && mbs && slices && nslices >= 1 && nslices <= 65535 && ys >= c->pw && cs >= c->pw / 2;
+    if (!(c && y && cb && cr && mbs && slices && nslices >= 1 && nslices <= 65535 && ys >= c->pw && cs >= c->pw / 2)) return false;
+    const uintptr_t align = reinterpret_cast<uintptr_t>(y) | reinterpret_cast<uintptr_t>(cb) | reinterpret_cast<uintptr_t>(cr);
+    return (align & 15) == 0 && ((size_t)ys * sample_bytes(c)) % 16 == 0 && cs % 8 == 0;
 }
 
 }  // namespace

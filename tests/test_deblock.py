@@ -13,7 +13,7 @@ import numpy as np
 import pytest
 
 from ironav_b200.inter import InterStage, IronavError
-from tests.deblock_cases import encoder_slices, planes, records
+from ironav_b200.synth import dbk_encoder_slices as encoder_slices, dbk_planes as planes, dbk_records as records
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 TABLES = json.load(open(os.path.join(GOLDEN, "deblock_tables.json")))
@@ -298,3 +298,25 @@ def test_gpu_deblock_rejects_a_slice_id_beyond_the_table(cuda_lib):
     assert e.value.status == 2
     mbs["slice"][5] = 1
     c.deblock(y, cb, cr, mbs, slices)  # the context is usable after the error
+
+
+@pytest.mark.gpu
+def test_gpu_deblock_device_form_checks_alignment(cuda_lib):
+    import torch
+
+    c = InterStage(64, 48, lib=cuda_lib)
+    y = torch.zeros((48, 80), dtype=torch.uint8, device="cuda")
+    ch = torch.zeros((2, 24, 40), dtype=torch.uint8, device="cuda")
+    m = torch.zeros(c.nmb * 192, dtype=torch.uint8, device="cuda")
+    from ironav_b200.synth import dbk_encoder_slices
+
+    s = dbk_encoder_slices(1)
+    c.deblock_device(y.data_ptr(), 80, ch[0].data_ptr(), ch[1].data_ptr(), 40, m.data_ptr(), s)  # aligned: accepted
+    c.sync()
+    for args in [(y.data_ptr(), 72, ch[0].data_ptr(), ch[1].data_ptr(), 40),      # luma rows 72 bytes apart
+                 (y.data_ptr() + 4, 80, ch[0].data_ptr(), ch[1].data_ptr(), 40),  # luma base off a 16-byte boundary
+                 (y.data_ptr(), 80, ch[0].data_ptr(), ch[1].data_ptr(), 36)]:     # chroma rows 36 samples apart
+        with pytest.raises(IronavError) as e:
+            c.deblock_device(*args, m.data_ptr(), s)
+        assert e.value.status == 3
+
