@@ -172,6 +172,54 @@ int ironav_scene_change(ironav_ctx* ctx, const void* prev_y, const void* cur_y, 
 /* The same on device pointers (returns when the totals are in out, a host array). */
 int ironav_scene_change_device(ironav_ctx* ctx, const void* d_prev, const void* d_cur, int stride, int64_t* out);
 
+/* ---- B pictures ------------------------------------------------------------------------------------- */
+
+/* The searches of a B macroblock (decide_b, enc/frame.rs:1518-1572; best_b_parts 1626-1687; spatial direct
+ * direct_mvs 1715-1747), in replay mode: every macroblock against its neighbours' final decisions. The
+ * rate-distortion choice among B_Skip / B_Direct_16x16, the 16x16 and smaller partitionings and intra
+ * stays with the caller, which codes the residuals (decide_b's rd_cost).
+ *
+ * A B macroblock's final decision as its neighbours' predictors see it (MbState with both lists,
+ * enc/frame.rs:246-272): per list the reference index of each 8x8 block (-1: the list is not used there)
+ * and the vector of each 4x4 block. */
+typedef struct ironav_mbstate_b {
+    uint8_t inter;
+    int8_t refs[2][4];
+    uint8_t pad[3];
+    int16_t mvs[2][16][2];
+} ironav_mbstate_b;                /* 140 bytes */
+
+typedef struct ironav_bresult {
+    int16_t direct_mv[2][16][2];   /* spatial direct vectors per list and 4x4 block */
+    uint8_t direct_use[2];         /* the lists the direct prediction uses */
+    uint8_t dir16;                 /* the best 16x16: 1 list 0, 2 list 1, 3 both averaged */
+    uint8_t has_parts;             /* best_b_parts found a partitioning cheaper than the best 16x16 */
+    uint8_t part;                  /* its partitioning: 1 16x8, 2 8x16, 3 8x8 */
+    uint8_t bdir[4];               /* per partition: 0 direct (8x8 only), bit 0 list 0, bit 1 list 1 */
+    uint8_t pad[3];
+    int16_t mv16[2][2];            /* the 16x16 vector of each list */
+    int32_t cost16[2];             /* per list: SATD + lambda (the vector's bits + 3) */
+    int32_t cost_bi;               /* both lists averaged: SATD + lambda (both vectors' bits + 5) */
+    int16_t pmv[2][4][2];          /* per list and partition, the partitioning's vectors */
+    uint32_t sad_px, satd_px;      /* samples compared by SAD and by SATD, in the reference's order */
+} ironav_bresult;                  /* 200 bytes */
+
+/* Parameters of the B picture to analyse (FrameCoder for a B picture, enc/frame.rs:381-440): qp_prime and
+ * lambda as for P pictures (the B picture's own QP'); ref_l0 / ref_l1: which held references (0 = newest)
+ * are list 0 and list 1 (the encoder's refp and refp1, one picture each); col: the list-1 picture's own
+ * decisions (mb_w*mb_h; its list-0 motion feeds spatial direct and the co-located candidate), or NULL
+ * when it was intra coded; tb, td: the picture's distance from the list-0 picture and the distance between
+ * the two (FrameCoder::dist), both nonzero; fast: H264Encoder::realtime's shorter search. col is copied
+ * before the call returns; the _device form keeps the device pointer d_col, which must stay valid until
+ * the pictures analysed with these parameters are done. */
+int ironav_begin_b_picture(ironav_ctx* ctx, int qp_prime, int lambda, int ref_l0, int ref_l1, const ironav_mbstate* col,
+                           int tb, int td, int fast);
+int ironav_begin_b_picture_device(ironav_ctx* ctx, int qp_prime, int lambda, int ref_l0, int ref_l1,
+                                  const ironav_mbstate* d_col, int tb, int td, int fast);
+/* final_states: every macroblock's final decision (mb_w*mb_h); out: mb_w*mb_h results. */
+int ironav_analyse_b_replay(ironav_ctx* ctx, const ironav_mbstate_b* final_states, ironav_bresult* out);
+int ironav_analyse_b_replay_device(ironav_ctx* ctx, const ironav_mbstate_b* d_final_states, ironav_bresult* d_out);
+
 /* ---- deblocking of the reconstruction ------------------------------------------------------------ */
 
 /* The in-loop deblocking filter (h264/deblock.rs:410-720, ITU-T H.264 8.7) of a reconstructed picture,
@@ -228,7 +276,12 @@ int ironav_deblock_picture_device(ironav_ctx* ctx, void* d_y, int y_stride, void
  *   IRONAV_INLOOP_RASTER  one caller thread, picture raster order (slice band after slice band);
  *   IRONAV_INLOOP_BANDS   one caller thread per slice band, raster order within the band.
  * Every device wait is bounded in time (ironav_inloop_set_wait, 10 s by default); a wait that runs out
- * ends the picture with IRONAV_TIMEOUT from ironav_inloop_end. */
+ * ends the picture with IRONAV_TIMEOUT from ironav_inloop_end.
+ *
+ * While a picture is open its kernel stays resident waiting for the caller's commits, so a CUDA call that
+ * synchronises the whole device — cudaFree, cudaDeviceSynchronize, destroying any context
+ * (ironav_ctx_destroy frees device memory) — waits for the picture to end. Make no such call from a thread
+ * whose commits the picture still needs (it would stall until the wait bound) before ironav_inloop_end. */
 #define IRONAV_INLOOP_RASTER 0
 #define IRONAV_INLOOP_BANDS 1
 int ironav_inloop_begin(ironav_ctx* ctx, int order);

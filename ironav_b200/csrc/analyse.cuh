@@ -172,20 +172,21 @@ static __device__ void load_neighbours(const AnalyseParams& __restrict__ P, Warp
     __syncwarp();
 }
 
-// nb_motion for the block at (x, y) relative to the macroblock; inside it, `cur` holds the decided
-// blocks (nullptr: none decided).
+// nb_motion for the block at (x, y) relative to the macroblock, from the neighbour table `ext` of one list;
+// inside the macroblock, `cur` holds the decided blocks (nullptr: none decided).
 template <class T>
-static __device__ __forceinline__ Blk nb(const AnalyseParams& __restrict__ P, WarpSmem<T>& __restrict__ S, const Blk* cur, int x, int y) {
+static __device__ __forceinline__ Blk nb(const AnalyseParams& __restrict__ P, WarpSmem<T>& __restrict__ S, const Blk* ext, const Blk* cur, int x, int y) {
     if (x >= 0 && x < 4 && y >= 0) return cur ? cur[y * 4 + x] : make_int4(0, 0, -1, 0);
-    return S.ext[(y + 1) * 6 + (x + 1)];
+    return ext[(y + 1) * 6 + (x + 1)];
 }
 
 // pred_mv, enc/frame.rs:543-570
 template <class T>
-static __device__ __forceinline__ int2 pred_mv(const AnalyseParams& __restrict__ P, WarpSmem<T>& __restrict__ S, const Blk* cur, int bx, int by, int w, int dir, int rf) {
-    const Blk a = nb(P, S, cur, bx - 1, by), b = nb(P, S, cur, bx, by - 1);
-    Blk c = nb(P, S, cur, bx + w, by - 1);
-    if (!c.w) c = nb(P, S, cur, bx - 1, by - 1);
+static __device__ __forceinline__ int2 pred_mv(const AnalyseParams& __restrict__ P, WarpSmem<T>& __restrict__ S, const Blk* ext, const Blk* cur, int bx, int by, int w,
+                                               int dir, int rf) {
+    const Blk a = nb(P, S, ext, cur, bx - 1, by), b = nb(P, S, ext, cur, bx, by - 1);
+    Blk c = nb(P, S, ext, cur, bx + w, by - 1);
+    if (!c.w) c = nb(P, S, ext, cur, bx - 1, by - 1);
     if (dir == 1 && by == 0 && b.z == rf) return make_int2(b.x, b.y);
     if (dir == 1 && by != 0 && a.z == rf) return make_int2(a.x, a.y);
     if (dir == 2 && bx == 0 && a.z == rf) return make_int2(a.x, a.y);
@@ -203,9 +204,9 @@ static __device__ __forceinline__ int2 pred_mv(const AnalyseParams& __restrict__
 // skip_mv, enc/frame.rs:597-603
 template <class T>
 static __device__ int2 skip_mv(const AnalyseParams& __restrict__ P, WarpSmem<T>& __restrict__ S) {
-    const Blk a = nb(P, S, nullptr, -1, 0), b = nb(P, S, nullptr, 0, -1);
+    const Blk a = nb(P, S, S.ext, nullptr, -1, 0), b = nb(P, S, S.ext, nullptr, 0, -1);
     if (!a.w || !b.w || (a.z == 0 && a.x == 0 && a.y == 0) || (b.z == 0 && b.x == 0 && b.y == 0)) return make_int2(0, 0);
-    return pred_mv(P, S, nullptr, 0, 0, 4, 0, 0);
+    return pred_mv(P, S, S.ext, nullptr, 0, 0, 4, 0, 0);
 }
 
 // ---- scoring -------------------------------------------------------------------------------------
@@ -266,9 +267,82 @@ static __device__ __forceinline__ int sad_lane(const uint8_t* __restrict__ g0, c
     return sad;
 }
 
-// Quarter-sample prediction (HalfPel::predict, enc/subpel.rs:122-145) of the partition at 4x4 block
-// (bx, by), (4 << lgw) x (4 << lgh) samples, scored by SATD (satd, enc/frame.rs:641-659), or by SAD
-// when `sad` (the P_Skip test), for the n vectors S.cand[0..n); the sums land in S.cost[0..n).
+// The quarter-sample prediction (HalfPel::predict, enc/subpel.rs:122-145) of the 4x4 block (bxx, byy), in
+// 4x4 blocks, of the w x h partition at picture sample (x0, y0), from the half-sample planes at `base`:
+// 4 rows of sizeof(T) words (4 samples a row).
+template <class T>
+__device__ __forceinline__ void pred4(const AnalyseParams& __restrict__ P, const uint8_t* base, int x0, int y0, int w, int h, int bxx, int byy, int2 mv,
+                                      uint32_t (&pr)[4][sizeof(T)]) {
+    constexpr int B = sizeof(T);
+    const int sw = P.sw, psize = (int)P.psize;
+    const int ix = min(max(x0 + (mv.x >> 2), -w - 3), P.pw + 1) + PAD + bxx * 4;
+    const int iy = min(max(y0 + (mv.y >> 2), -h - 3), P.ph + 1) + PAD + byy * 4;
+    const unsigned m = mix_entry(mv.x & 3, mv.y & 3);
+    const int pa = m & 3, ax = (m >> 2) & 1, ay = (m >> 3) & 1, pb = (m >> 4) & 3, bbx = (m >> 6) & 1, bby = (m >> 7) & 1;
+    const bool same = (m & 0xf) == (m >> 4);
+    // every row of a plane block has the same alignment (sw is a multiple of 16); a row of 4 samples is
+    // B words, read as B + 1 aligned words
+    const uintptr_t ua = reinterpret_cast<uintptr_t>(base + (unsigned)(pa * psize + (iy + ay) * sw + ix + ax) * B);
+    const uint32_t* qa = reinterpret_cast<const uint32_t*>(ua & ~uintptr_t(3));
+    const unsigned sha = (unsigned)(ua & 3) * 8u;
+    const int swq = (sw * B) >> 2;
+#pragma unroll
+    for (int row = 0; row < 4; row++) {
+        uint32_t pv = __ldg(qa + row * swq);
+#pragma unroll
+        for (int k = 0; k < B; k++) {
+            const uint32_t nx = __ldg(qa + row * swq + k + 1);
+            pr[row][k] = __funnelshift_r(pv, nx, sha);
+            pv = nx;
+        }
+    }
+    if (!same) {
+        const uintptr_t ub = reinterpret_cast<uintptr_t>(base + (unsigned)(pb * psize + (iy + bby) * sw + ix + bbx) * B);
+        const uint32_t* qb = reinterpret_cast<const uint32_t*>(ub & ~uintptr_t(3));
+        const unsigned shb = (unsigned)(ub & 3) * 8u;
+#pragma unroll
+        for (int row = 0; row < 4; row++) {
+            uint32_t pv = __ldg(qb + row * swq);
+#pragma unroll
+            for (int k = 0; k < B; k++) {
+                const uint32_t nx = __ldg(qb + row * swq + k + 1);
+                const uint32_t o = __funnelshift_r(pv, nx, shb);
+                pr[row][k] = B == 1 ? __vavgu4(pr[row][k], o) : __vavgu2(pr[row][k], o);
+                pv = nx;
+            }
+        }
+    }
+}
+
+// The score of prediction rows pr against the source's 4x4 block (sbx, sby) of the macroblock: SATD
+// (satd, enc/frame.rs:641-659), or SAD when `sad`.
+template <class T>
+__device__ __forceinline__ int score4(const WarpSmem<T>& __restrict__ S, int sbx, int sby, const uint32_t (&pr)[4][sizeof(T)], bool sad) {
+    constexpr int B = sizeof(T);
+    uint32_t sr[4][B];
+    const uint32_t* sp = &S.src[(sby * 16 + sbx) * B];
+#pragma unroll
+    for (int row = 0; row < 4; row++)
+#pragma unroll
+        for (int k = 0; k < B; k++) sr[row][k] = sp[row * 4 * B + k];
+    int v = 0;
+    if (sad) {
+#pragma unroll
+        for (int row = 0; row < 4; row++)
+#pragma unroll
+            for (int k = 0; k < B; k++) v += B == 1 ? __vsadu4(sr[row][k], pr[row][k]) : __vsadu2(sr[row][k], pr[row][k]);
+    } else if constexpr (B == 1) {
+        const uint32_t s1[4] = {sr[0][0], sr[1][0], sr[2][0], sr[3][0]}, p1[4] = {pr[0][0], pr[1][0], pr[2][0], pr[3][0]};
+        v = satd4_packed(s1, p1);
+    } else {
+        v = satd4_packed16(sr, pr);
+    }
+    return v;
+}
+
+// Quarter-sample prediction of the partition at 4x4 block (bx, by), (4 << lgw) x (4 << lgh) samples, scored
+// by SATD, or by SAD when `sad` (the P_Skip test), for the n vectors S.cand[0..n) on the planes of
+// reference r; the sums land in S.cost[0..n). Lanes over (vector, 4x4 block).
 template <class T>
 static __device__ __forceinline__ void pred_batch(const AnalyseParams& __restrict__ P, WarpSmem<T>& __restrict__ S, int r, int bx, int by, int lgw, int lgh, int n, bool sad) {
     const int lane = threadIdx.x & 31;
@@ -276,70 +350,12 @@ static __device__ __forceinline__ void pred_batch(const AnalyseParams& __restric
     if (lane < n) S.cost[lane] = 0;
     __syncwarp();
     const int x0 = S.mbx * 16 + bx * 4, y0 = S.mby * 16 + by * 4;
-    constexpr int B = sizeof(T);
     const uint8_t* base = P.planes[r];
-    const int sw = P.sw, psize = (int)P.psize;
     for (int t = lane; t < total; t += 32) {
         const int c = t >> lg, b = t & ((1 << lg) - 1), bxx = b & ((1 << lgw) - 1), byy = b >> lgw;
-        const int2 mv = S.cand[c];
-        const int ix = min(max(x0 + (mv.x >> 2), -w - 3), P.pw + 1) + PAD + bxx * 4;
-        const int iy = min(max(y0 + (mv.y >> 2), -h - 3), P.ph + 1) + PAD + byy * 4;
-        const unsigned m = mix_entry(mv.x & 3, mv.y & 3);
-        const int pa = m & 3, ax = (m >> 2) & 1, ay = (m >> 3) & 1, pb = (m >> 4) & 3, bbx = (m >> 6) & 1, bby = (m >> 7) & 1;
-        const bool same = (m & 0xf) == (m >> 4);
-        // every row of a plane block has the same alignment (sw is a multiple of 16); a row of 4 samples is
-        // B words (B = sizeof(T)), read as B + 1 aligned words
-        const uintptr_t ua = reinterpret_cast<uintptr_t>(base + (unsigned)(pa * psize + (iy + ay) * sw + ix + ax) * B);
-        const uint32_t* qa = reinterpret_cast<const uint32_t*>(ua & ~uintptr_t(3));
-        const unsigned sha = (unsigned)(ua & 3) * 8u;
-        const int swq = (sw * B) >> 2;
-        uint32_t pr[4][B], sr[4][B];
-#pragma unroll
-        for (int row = 0; row < 4; row++) {
-            uint32_t pv = __ldg(qa + row * swq);
-#pragma unroll
-            for (int k = 0; k < B; k++) {
-                const uint32_t nx = __ldg(qa + row * swq + k + 1);
-                pr[row][k] = __funnelshift_r(pv, nx, sha);
-                pv = nx;
-            }
-        }
-        if (!same) {
-            const uintptr_t ub = reinterpret_cast<uintptr_t>(base + (unsigned)(pb * psize + (iy + bby) * sw + ix + bbx) * B);
-            const uint32_t* qb = reinterpret_cast<const uint32_t*>(ub & ~uintptr_t(3));
-            const unsigned shb = (unsigned)(ub & 3) * 8u;
-#pragma unroll
-            for (int row = 0; row < 4; row++) {
-                uint32_t pv = __ldg(qb + row * swq);
-#pragma unroll
-                for (int k = 0; k < B; k++) {
-                    const uint32_t nx = __ldg(qb + row * swq + k + 1);
-                    const uint32_t o = __funnelshift_r(pv, nx, shb);
-                    pr[row][k] = B == 1 ? __vavgu4(pr[row][k], o) : __vavgu2(pr[row][k], o);
-                    pv = nx;
-                }
-            }
-        }
-        const uint32_t* sp = &S.src[((by + byy) * 16 + bx + bxx) * B];
-#pragma unroll
-        for (int row = 0; row < 4; row++)
-#pragma unroll
-            for (int k = 0; k < B; k++) sr[row][k] = sp[row * 4 * B + k];
-        int v = 0;
-        if (sad) {
-#pragma unroll
-            for (int row = 0; row < 4; row++)
-#pragma unroll
-                for (int k = 0; k < B; k++) v += B == 1 ? __vsadu4(sr[row][k], pr[row][k]) : __vsadu2(sr[row][k], pr[row][k]);
-        } else {
-            if constexpr (B == 1) {
-                const uint32_t s1[4] = {sr[0][0], sr[1][0], sr[2][0], sr[3][0]}, p1[4] = {pr[0][0], pr[1][0], pr[2][0], pr[3][0]};
-                v = satd4_packed(s1, p1);
-            } else {
-                v = satd4_packed16(sr, pr);
-            }
-        }
-        atomicAdd(&S.cost[c], v);
+        uint32_t pr[4][sizeof(T)];
+        pred4<T>(P, base, x0, y0, w, h, bxx, byy, S.cand[c], pr);
+        atomicAdd(&S.cost[c], score4<T>(S, bx + bxx, by + byy, pr, sad));
     }
     __syncwarp();
 }
@@ -383,11 +399,14 @@ static __device__ __noinline__ int4 round_clamped(const AnalyseParams& __restric
     return make_int4(moved, bxv, byv, bc);
 }
 
-// Returns the best vector in (ox, oy) and its cost without the vector's bits. (e0x, e0y) and
-// (e1x, e1y) are the extra candidates (nextra of them).
+// Returns the best vector in (ox, oy) and its cost without the vector's bits. The search runs on the
+// half-sample planes P.planes[r]; the neighbour candidates come from the table `ext` of the list searched
+// and count when their reference index is rsel. (e0x, e0y) and (e1x, e1y) are the first extra candidates
+// (nextra of them), more[0..nmore) the ones after them (B-picture partitions; at most 9).
 template <class T>
-static __device__ __noinline__ int4 motion_search(const AnalyseParams& __restrict__ P, WarpSmem<T>& __restrict__ S, int r, int bx, int by, int w4, int h4, int mvpx, int mvpy, int e0x, int e0y,
-                                          int e1x, int e1y, int nextra) {
+static __device__ __noinline__ int4 motion_search(const AnalyseParams& __restrict__ P, WarpSmem<T>& __restrict__ S, const Blk* ext, int rsel, int r, int bx, int by,
+                                                  int w4, int h4, int mvpx, int mvpy, int e0x, int e0y, int e1x, int e1y, int nextra,
+                                                  const int2* more, int nmore) {
     const int lane = threadIdx.x & 31;
     const int lam = P.lambda;
     const int x0 = S.mbx * 16 + bx * 4, y0 = S.mby * 16 + by * 4, w = w4 * 4, h = h4 * 4;
@@ -404,8 +423,8 @@ static __device__ __noinline__ int4 motion_search(const AnalyseParams& __restric
         px = intr(clx(mvpx));
         py = intr(cly(mvpy));
     } else if (g >= 2 && g <= 4) {
-        const Blk n = g == 2 ? nb(P, S, nullptr, -1, 0) : (g == 3 ? nb(P, S, nullptr, 0, -1) : nb(P, S, nullptr, 4, -1));
-        valid = n.w && n.z == r;
+        const Blk n = g == 2 ? nb(P, S, ext, nullptr, -1, 0) : (g == 3 ? nb(P, S, ext, nullptr, 0, -1) : nb(P, S, ext, nullptr, 4, -1));
+        valid = n.w && n.z == rsel;
         px = intr(clx(n.x));
         py = intr(cly(n.y));
     } else if (g == 5) {
@@ -417,7 +436,11 @@ static __device__ __noinline__ int4 motion_search(const AnalyseParams& __restric
         px = intr(clx(e1x));
         py = intr(cly(e1y));
     } else if (g == 7) {
-        valid = false;
+        valid = nmore > 0;
+        if (valid) {
+            px = intr(clx(more[0].x));
+            py = intr(cly(more[0].y));
+        }
     }
     const int sw = P.sw;
     const uint8_t* const g0 = P.planes[r] + ((y0 + PAD) * sw + x0 + PAD) * (int)sizeof(T);
@@ -427,11 +450,28 @@ static __device__ __noinline__ int4 motion_search(const AnalyseParams& __restric
     const unsigned vmask = __ballot_sync(FULL, valid) & 0xffu;
     if (lane == 0) S.sad_px += (uint32_t)(__popc(vmask) * w * h);
     // the first candidate of least cost: min over (cost, position in the list)
-    unsigned long long key = ((unsigned long long)(unsigned)cost << 3) | (unsigned)g;
+    unsigned long long key = ((unsigned long long)(unsigned)cost << 4) | (unsigned)g;
+    if (nmore > 1) {
+        // the candidates after the eighth (list positions 8..15): a second batch
+        const bool v2 = g + 1 < nmore;
+        int qx = 0, qy = 0;
+        if (v2) {
+            qx = intr(clx(more[g + 1].x));
+            qy = intr(cly(more[g + 1].y));
+        }
+        int c2 = sad_lane<T>(g0, src0, sw, w, h, qx, qy, v2);
+        c2 = v2 ? c2 + lam * mvd_bits_d(qx, qy, mvpx, mvpy) : BIG;
+        const unsigned vm2 = __ballot_sync(FULL, v2) & 0xffu;
+        if (lane == 0) S.sad_px += (uint32_t)(__popc(vm2) * w * h);
+        key = min(key, ((unsigned long long)(unsigned)c2 << 4) | (unsigned)(8 + g));
+        // the lane keeps the vector of whichever of its two candidates its key now names
+        px = (key & 15u) >= 8 ? qx : px;
+        py = (key & 15u) >= 8 ? qy : py;
+    }
 #pragma unroll
     for (int off = 1; off < 8; off <<= 1) key = min(key, __shfl_xor_sync(FULL, key, off));
-    const int win = (int)(key & 7u);
-    int bc = (int)(key >> 3);
+    const int win = (int)(key & 7u);  // the lane group holding the winning candidate
+    int bc = (int)(key >> 4);
     int bxv = __shfl_sync(FULL, px, win), byv = __shfl_sync(FULL, py, win);
     // the diamond (973-988): each round scores the 3x3 square of its step around the centre in one
     // batch (group g -> square position k = g < 4 ? g : g + 1), then replays the four moves in order
@@ -579,8 +619,8 @@ static __device__ __noinline__ int2 sub_search(const AnalyseParams& __restrict__
         int cost = lam * (s == 0 ? 0 : 2);
         for (int q = 0; q < c_nsub[s]; q++) {
             const int x = ox + c_sub[s][q][0], y = oy + c_sub[s][q][1], w = c_sub[s][q][2], h = c_sub[s][q][3];
-            const int2 p = pred_mv(P, S, S.t, x, y, w, 0, r);
-            const int4 ms = motion_search(P, S, r, x, y, w, h, p.x, p.y, ex, ey, 0, 0, 1);
+            const int2 p = pred_mv(P, S, S.ext, S.t, x, y, w, 0, r);
+            const int4 ms = motion_search(P, S, S.ext, r, r, x, y, w, h, p.x, p.y, ex, ey, 0, 0, 1, nullptr, 0);
             const int c = ms.x, mx = ms.y, my = ms.z;
             cost += c + lam * mvd_bits_d(mx, my, p.x, p.y);
             blk_paint(P, S, S.t, x, y, w, h, mx, my, r);
@@ -603,9 +643,9 @@ static __device__ __noinline__ int4 best_inter_ref(const AnalyseParams& __restri
     int rb = 0;
     if (P.nact == 2) rb = lam;  // ref_bits, enc/frame.rs:705-711
     else if (P.nact > 2) rb = lam * (2 * (31 - __clz(r + 1)) + 1);
-    const int2 mvp = pred_mv(P, S, nullptr, 0, 0, 4, 0, r);
+    const int2 mvp = pred_mv(P, S, S.ext, nullptr, 0, 0, 4, 0, r);
     const ColMv col = P.col[S.mb];
-    const int4 ms = motion_search(P, S, r, 0, 0, 4, 4, mvp.x, mvp.y, col.mv[0], col.mv[1], 0, 0, col.valid ? 1 : 0);
+    const int4 ms = motion_search(P, S, S.ext, r, r, 0, 0, 4, 4, mvp.x, mvp.y, col.mv[0], col.mv[1], 0, 0, col.valid ? 1 : 0, nullptr, 0);
     const int c = ms.x, mx = ms.y, my = ms.z;
     int best_part = 0, best_cost = c + lam * (mvd_bits_d(mx, my, mvp.x, mvp.y) + 1) + rb;
     const int cost16 = best_cost;
@@ -656,10 +696,10 @@ static __device__ __noinline__ int4 best_inter_ref(const AnalyseParams& __restri
                 if (k == 1)
                     blk_paint(P, S, S.t, c_parts[part][0][0], c_parts[part][0][1], c_parts[part][0][2], c_parts[part][0][3], h0x, h0y, r);
                 const int x = c_parts[part][k][0], y = c_parts[part][k][1], w = c_parts[part][k][2], h = c_parts[part][k][3];
-                const int2 p = pred_mv(P, S, S.t, x, y, w, part, r);
+                const int2 p = pred_mv(P, S, S.ext, S.t, x, y, w, part, r);
                 const int i0 = part == 1 ? 2 * k : k, i1 = part == 1 ? 2 * k + 1 : k + 2;
                 const Blk a0 = S.st[(i0 / 2) * 8 + (i0 % 2) * 2], a1 = S.st[(i1 / 2) * 8 + (i1 % 2) * 2];
-                const int4 ms = motion_search(P, S, r, x, y, w, h, p.x, p.y, a0.x, a0.y, a1.x, a1.y, 2);
+                const int4 ms = motion_search(P, S, S.ext, r, r, x, y, w, h, p.x, p.y, a0.x, a0.y, a1.x, a1.y, 2, nullptr, 0);
                 const int cc = ms.x, m0 = ms.y, m1 = ms.z;
                 if (k == 0) {
                     h0x = m0;
@@ -688,10 +728,10 @@ static __device__ __noinline__ int4 best_inter_ref(const AnalyseParams& __restri
 
 // ---- one macroblock --------------------------------------------------------------------------------
 
+// The current macroblock into shared memory: 16 rows of 16 samples, as 128-bit loads (sizeof(T) per row).
 template <class T>
-static __device__ void analyse(const AnalyseParams& __restrict__ P, WarpSmem<T>& __restrict__ S, bool auto_policy) {
+static __device__ __forceinline__ void stage_source(const AnalyseParams& __restrict__ P, WarpSmem<T>& __restrict__ S) {
     const int lane = threadIdx.x & 31;
-    // the current macroblock: 16 rows of 16 samples, as 128-bit loads (sizeof(T) per row)
     constexpr int B = sizeof(T);
     if (lane < 16 * B) {
         const int row = lane / B, part = lane % B;
@@ -701,6 +741,12 @@ static __device__ void analyse(const AnalyseParams& __restrict__ P, WarpSmem<T>&
         S.src[lane * 4 + 2] = v.z;
         S.src[lane * 4 + 3] = v.w;
     }
+}
+
+template <class T>
+static __device__ void analyse(const AnalyseParams& __restrict__ P, WarpSmem<T>& __restrict__ S, bool auto_policy) {
+    const int lane = threadIdx.x & 31;
+    stage_source(P, S);
     if (lane < 26) reinterpret_cast<uint32_t*>(&S.res)[lane] = 0;
     __syncwarp();
     if (lane == 0) S.sad_px = S.satd_px = 0;

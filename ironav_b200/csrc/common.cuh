@@ -45,6 +45,11 @@ struct AnalyseParams {
     const unsigned* commit_flags;
     unsigned* done_flags;
     unsigned long long wait_ns;       // how long an in-loop wait for the caller may take
+    // B pictures (planes[0]: list 0's reference, planes[1]: list 1's)
+    const ironav_mbstate_b* bstates_in;  // final decisions of every macroblock (both lists)
+    ironav_bresult* bresults;
+    const ironav_mbstate* bcol;       // the list-1 picture's decisions, or nullptr (intra)
+    int tb, td;                       // picture distances (FrameCoder::dist)
 };
 
 // Device-scope acquire load and release store of a progress word shared by warps of different CTAs.

@@ -54,6 +54,15 @@ struct ironav_ctx {
     ironav_dbk_mb* d_dbk_mbs = nullptr;
     uint8_t* d_dbk_planes = nullptr;
     void* d_dbk_edges = nullptr;  // per macroblock: strengths and edge thresholds (pass 1 -> pass 2)
+    // B pictures: the references used as list 0 and list 1, the list-1 picture's decisions (a copy, or the
+    // caller's device pointer), picture distances; host-form buffers allocated on first use
+    int b_ref[2] = {0, 0};
+    int b_tb = 0, b_td = 0;
+    bool b_set = false;
+    ironav_mbstate* d_bcol_copy = nullptr;
+    const ironav_mbstate* b_col = nullptr;
+    ironav_mbstate_b* d_bstates = nullptr;
+    ironav_bresult* d_bresults = nullptr;
 };
 
 

@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "analyse.cuh"
+#include "bpicture.cuh"
 #include "ctx.cuh"
 #include "planes.cuh"
 #include "peaks.cuh"
@@ -26,6 +27,8 @@ using namespace ironav;
 static_assert(sizeof(ironav_mbstate) == 72, "ironav_mbstate layout");
 static_assert(sizeof(ironav_mbresult) == 104, "ironav_mbresult layout");
 static_assert(sizeof(ironav_dbk_mb) == 192, "ironav_dbk_mb layout");
+static_assert(sizeof(ironav_mbstate_b) == 140, "ironav_mbstate_b layout");
+static_assert(sizeof(ironav_bresult) == 200, "ironav_bresult layout");
 static_assert(sizeof(ironav_dbk_slice) == 20, "ironav_dbk_slice layout");
 
 // The reference slot for a new picture: the oldest one's once max_refs are held, else a free one; the
@@ -108,6 +111,9 @@ void free_ctx(ironav_ctx* c) {
     cudaFree(c->d_dbk_mbs);
     cudaFree(c->d_dbk_planes);
     cudaFree(c->d_dbk_edges);
+    cudaFree(c->d_bcol_copy);
+    cudaFree(c->d_bstates);
+    cudaFree(c->d_bresults);
     cudaFreeHost(c->h_results);
     cudaFreeHost(c->h_done);
     cudaFreeHost(c->h_committed);
@@ -540,6 +546,81 @@ int ironav_deblock_picture(ironav_ctx* c, void* y, int ys, void* cb, void* cr, i
     CK(cudaMemcpy2DAsync(y, (size_t)ys * B, dy, pw * B, pw * B, ph, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaMemcpy2DAsync(cb, (size_t)cs * B, dcb, pw / 2 * B, pw / 2 * B, ph / 2, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaMemcpy2DAsync(cr, (size_t)cs * B, dcr, pw / 2 * B, pw / 2 * B, ph / 2, cudaMemcpyDeviceToHost, c->stream));
+    return check_device_error(c);
+}
+
+// ---- B pictures -------------------------------------------------------------------------------------
+
+static int b_params(ironav_ctx* c, int qpp, int lambda, int l0, int l1, int tb, int td, int fast) {
+    if (!c || lambda < 1 || qpp < 0 || qpp > 63 || l0 < 0 || l0 >= c->nrefs || l1 < 0 || l1 >= c->nrefs || tb == 0 || td == 0)
+        return IRONAV_INVALID_ARGUMENT;
+    c->qpp = qpp;
+    c->lambda = lambda;
+    c->fast = fast ? 1 : 0;
+    c->b_ref[0] = l0;
+    c->b_ref[1] = l1;
+    c->b_tb = tb;
+    c->b_td = td;
+    return IRONAV_OK;
+}
+
+int ironav_begin_b_picture(ironav_ctx* c, int qpp, int lambda, int ref_l0, int ref_l1, const ironav_mbstate* col, int tb, int td, int fast) {
+    int s = b_params(c, qpp, lambda, ref_l0, ref_l1, tb, td, fast);
+    if (s != IRONAV_OK) return s;
+    c->b_col = nullptr;
+    if (col) {
+        if (!c->d_bcol_copy) CK(cudaMalloc(&c->d_bcol_copy, sizeof(ironav_mbstate) * c->nmb));
+        CK(cudaMemcpyAsync(c->d_bcol_copy, col, sizeof(ironav_mbstate) * c->nmb, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        c->b_col = c->d_bcol_copy;
+    }
+    c->b_set = true;
+    return IRONAV_OK;
+}
+
+int ironav_begin_b_picture_device(ironav_ctx* c, int qpp, int lambda, int ref_l0, int ref_l1, const ironav_mbstate* d_col, int tb, int td,
+                                  int fast) {
+    int s = b_params(c, qpp, lambda, ref_l0, ref_l1, tb, td, fast);
+    if (s != IRONAV_OK) return s;
+    c->b_col = d_col;
+    c->b_set = true;
+    return IRONAV_OK;
+}
+
+static int launch_b(ironav_ctx* c, const ironav_mbstate_b* d_states, ironav_bresult* d_out) {
+    if (!c->b_set || c->b_ref[0] >= c->nrefs || c->b_ref[1] >= c->nrefs) return IRONAV_INVALID_ARGUMENT;
+    AnalyseParams p;
+    fill_params(c, p);
+    p.planes[0] = c->d_planes[c->slot_of[c->b_ref[0]]];
+    p.planes[1] = c->d_planes[c->slot_of[c->b_ref[1]]];
+    p.nact = 2;
+    p.bstates_in = d_states;
+    p.bresults = d_out;
+    p.bcol = c->b_col;
+    p.tb = c->b_tb;
+    p.td = c->b_td;
+    p.ticket = c->d_counters;
+    p.err = c->d_counters + 1;
+    p.nmb = c->nmb;
+    CK(cudaMemsetAsync(c->d_counters, 0, 2 * sizeof(unsigned), c->stream));
+    if (c->bd > 8) analyse_b_kernel<uint16_t><<<c->k2_blocks, K2_WARPS * 32, 0, c->stream>>>(p);
+    else analyse_b_kernel<uint8_t><<<c->k2_blocks, K2_WARPS * 32, 0, c->stream>>>(p);
+    return cuda_status(cudaGetLastError());
+}
+
+int ironav_analyse_b_replay_device(ironav_ctx* c, const ironav_mbstate_b* d_states, ironav_bresult* d_out) {
+    if (!c || !d_states || !d_out) return IRONAV_INVALID_ARGUMENT;
+    return launch_b(c, d_states, d_out);
+}
+
+int ironav_analyse_b_replay(ironav_ctx* c, const ironav_mbstate_b* states, ironav_bresult* out) {
+    if (!c || !states || !out) return IRONAV_INVALID_ARGUMENT;
+    if (!c->d_bstates) CK(cudaMalloc(&c->d_bstates, sizeof(ironav_mbstate_b) * c->nmb));
+    if (!c->d_bresults) CK(cudaMalloc(&c->d_bresults, sizeof(ironav_bresult) * c->nmb));
+    CK(cudaMemcpyAsync(c->d_bstates, states, sizeof(ironav_mbstate_b) * c->nmb, cudaMemcpyHostToDevice, c->stream));
+    int s = launch_b(c, c->d_bstates, c->d_bresults);
+    if (s != IRONAV_OK) return s;
+    CK(cudaMemcpyAsync(out, c->d_bresults, sizeof(ironav_bresult) * c->nmb, cudaMemcpyDeviceToHost, c->stream));
     return check_device_error(c);
 }
 

@@ -65,7 +65,28 @@ DBK_MB_DTYPE = np.dtype(
 DBK_SLICE_DTYPE = np.dtype(
     [("disable_deblocking", "<i4"), ("alpha_offset", "<i4"), ("beta_offset", "<i4"), ("chroma_qp_offset", "<i4", (2,))]
 )
+# B pictures: a macroblock's final decision with both lists (ironav_mbstate_b) and the B searches' results
+# (ironav_bresult).
+MBSTATE_B_DTYPE = np.dtype([("inter", "u1"), ("refs", "i1", (2, 4)), ("pad", "u1", (3,)), ("mvs", "<i2", (2, 16, 2))])
+BRESULT_DTYPE = np.dtype(
+    [
+        ("direct_mv", "<i2", (2, 16, 2)),
+        ("direct_use", "u1", (2,)),
+        ("dir16", "u1"),
+        ("has_parts", "u1"),
+        ("part", "u1"),
+        ("bdir", "u1", (4,)),
+        ("pad", "u1", (3,)),
+        ("mv16", "<i2", (2, 2)),
+        ("cost16", "<i4", (2,)),
+        ("cost_bi", "<i4"),
+        ("pmv", "<i2", (2, 4, 2)),
+        ("sad_px", "<u4"),
+        ("satd_px", "<u4"),
+    ]
+)
 assert MBSTATE_DTYPE.itemsize == 72 and MBRESULT_DTYPE.itemsize == 104
+assert MBSTATE_B_DTYPE.itemsize == 140 and BRESULT_DTYPE.itemsize == 200
 assert DBK_MB_DTYPE.itemsize == 192 and DBK_SLICE_DTYPE.itemsize == 20
 
 RESULT_INTER = 1
@@ -93,6 +114,7 @@ EXPORTS = (
     "ironav_inloop_set_wait", "ironav_batch_create", "ironav_batch_destroy", "ironav_batch_step",
     "ironav_batch_sync", "ironav_scene_change", "ironav_scene_change_device", "ironav_analyse_auto_noalloc",
     "ironav_deblock_picture", "ironav_deblock_picture_device",
+    "ironav_begin_b_picture", "ironav_begin_b_picture_device", "ironav_analyse_b_replay", "ironav_analyse_b_replay_device",
 )
 
 SCENE_CUT = 0.8  # codec/change.rs:6
@@ -142,6 +164,11 @@ def _declare(lib: ctypes.CDLL) -> ctypes.CDLL:
     if hasattr(lib, "ironav_scene_change"):
         lib.ironav_scene_change.argtypes = [_VP, _VP, _VP, _I, _VP]
         lib.ironav_scene_change_device.argtypes = [_VP, _VP, _VP, _I, _VP]
+    if hasattr(lib, "ironav_begin_b_picture"):
+        lib.ironav_begin_b_picture.argtypes = [_VP, _I, _I, _I, _I, _VP, _I, _I, _I]
+        lib.ironav_begin_b_picture_device.argtypes = [_VP, _I, _I, _I, _I, _VP, _I, _I, _I]
+        lib.ironav_analyse_b_replay.argtypes = [_VP, _VP, _VP]
+        lib.ironav_analyse_b_replay_device.argtypes = [_VP, _VP, _VP]
     if hasattr(lib, "ironav_deblock_picture"):
         lib.ironav_deblock_picture.argtypes = [_VP, _VP, _I, _VP, _VP, _I, _VP, _VP, _I]
         lib.ironav_deblock_picture_device.argtypes = [_VP, _VP, _I, _VP, _VP, _I, _VP, _VP, _I]
@@ -162,6 +189,42 @@ def _declare(lib: ctypes.CDLL) -> ctypes.CDLL:
 
 
 _CUDA = None
+
+# An open in-loop picture is a kernel that stays resident until the caller has committed every decision.
+# A call that synchronises the whole device (cudaFree when a context is destroyed, among others) waits for
+# it, so a context destroyed from a thread the picture needs — Python's garbage collector may run in any
+# thread — would stall the picture until its wait bound. While in-loop pictures are open, contexts that go
+# out of use are therefore destroyed only when the last of those pictures ends.
+import threading as _threading
+
+_INLOOP_LOCK = _threading.Lock()
+_INLOOP_OPEN = 0
+_DEFERRED: list = []
+
+
+def _destroy_later_or_now(lib, ctx) -> None:
+    with _INLOOP_LOCK:
+        if _INLOOP_OPEN > 0:
+            _DEFERRED.append((lib, ctx))
+            return
+    lib.ironav_ctx_destroy(ctx)
+
+
+def _inloop_opened() -> None:
+    global _INLOOP_OPEN
+    with _INLOOP_LOCK:
+        _INLOOP_OPEN += 1
+
+
+def _inloop_closed() -> None:
+    global _INLOOP_OPEN
+    with _INLOOP_LOCK:
+        _INLOOP_OPEN -= 1
+        todo = []
+        if _INLOOP_OPEN == 0:
+            todo, _DEFERRED[:] = list(_DEFERRED), []
+    for lib, ctx in todo:
+        lib.ironav_ctx_destroy(ctx)
 
 
 def cuda_library() -> ctypes.CDLL:
@@ -225,7 +288,9 @@ class InterStage:
 
     def close(self) -> None:
         if getattr(self, "ctx", None):
-            self.lib.ironav_ctx_destroy(self.ctx)
+            if getattr(self, "_inloop_open", False):
+                self.inloop_end_quietly()
+            _destroy_later_or_now(self.lib, self.ctx)
             self.ctx = None
 
     def __del__(self):
@@ -307,6 +372,26 @@ class InterStage:
         inter, intra = self.scene_change(prev, cur)
         return float(inter) > SCENE_CUT * float(intra)
 
+    # -- B pictures (decide_b's searches, enc/frame.rs:1518-1572, 1626-1747) ------------------------------
+
+    def begin_b_picture(self, qp_prime: int, ref_l0: int, ref_l1: int, col: np.ndarray | None, tb: int, td: int,
+                        fast: bool = False) -> None:
+        lam = self.lib.ironav_lambda(qp_prime)
+        colp = None
+        if col is not None:
+            self._bcol = np.ascontiguousarray(col, dtype=MBSTATE_DTYPE)
+            assert self._bcol.shape == (self.nmb,)
+            colp = _ptr(self._bcol)
+        self._check(self.lib.ironav_begin_b_picture(self.ctx, qp_prime, lam, ref_l0, ref_l1, colp, tb, td, int(fast)),
+                    "ironav_begin_b_picture")
+
+    def analyse_b_replay(self, states: np.ndarray) -> np.ndarray:
+        states = np.ascontiguousarray(states, dtype=MBSTATE_B_DTYPE)
+        assert states.shape == (self.nmb,)
+        out = np.zeros(self.nmb, dtype=BRESULT_DTYPE)
+        self._check(self.lib.ironav_analyse_b_replay(self.ctx, _ptr(states), _ptr(out)), "ironav_analyse_b_replay")
+        return out
+
     # -- deblocking of the reconstruction (h264/deblock.rs) ------------------------------------------------
 
     def deblock(self, y: np.ndarray, cb: np.ndarray, cr: np.ndarray, mbs: np.ndarray,
@@ -334,6 +419,8 @@ class InterStage:
 
     def inloop_begin(self, order: int = 0) -> None:
         self._check(self.lib.ironav_inloop_begin(self.ctx, order), "ironav_inloop_begin")
+        self._inloop_open = True
+        _inloop_opened()
 
     def inloop_result(self, mb: int, timeout_ms: int = 10000) -> np.ndarray:
         out = np.zeros(1, dtype=MBRESULT_DTYPE)
@@ -345,7 +432,17 @@ class InterStage:
         self._check(self.lib.ironav_inloop_commit(self.ctx, mb, _ptr(st)), "ironav_inloop_commit")
 
     def inloop_end(self) -> None:
-        self._check(self.lib.ironav_inloop_end(self.ctx), "ironav_inloop_end")
+        status = self.lib.ironav_inloop_end(self.ctx)
+        if getattr(self, "_inloop_open", False):
+            self._inloop_open = False
+            _inloop_closed()
+        self._check(status, "ironav_inloop_end")
+
+    def inloop_end_quietly(self) -> None:
+        try:
+            self.inloop_end()
+        except IronavError:
+            pass
 
     def inloop_set_wait(self, ms: int) -> None:
         self._check(self.lib.ironav_inloop_set_wait(self.ctx, ms), "ironav_inloop_set_wait")
@@ -379,6 +476,18 @@ _SUB = [[(0, 0, 2, 2)], [(0, 0, 2, 1), (0, 1, 2, 1)], [(0, 0, 1, 2), (1, 0, 1, 2
         [(0, 0, 1, 1), (1, 0, 1, 1), (0, 1, 1, 1), (1, 1, 1, 1)]]
 _PARTS = [[(0, 0, 4, 4)], [(0, 0, 4, 2), (0, 2, 4, 2)], [(0, 0, 2, 4), (2, 0, 2, 4)],
           [(0, 0, 2, 2), (2, 0, 2, 2), (0, 2, 2, 2), (2, 2, 2, 2)]]
+
+
+def b_decision_states(res: np.ndarray) -> np.ndarray:
+    """A plausible final decision per B macroblock from its search results (the 16x16 of the best
+    direction), for replaying a picture against decisions the stage itself would favour."""
+    st = np.zeros(len(res), dtype=MBSTATE_B_DTYPE)
+    st["inter"] = 1
+    for l in (0, 1):
+        used = (res["dir16"] >> l) & 1
+        st["refs"][:, l] = np.where(used[:, None] == 1, 0, -1)
+        st["mvs"][:, l] = np.where(used[:, None, None] == 1, res["mv16"][:, l][:, None, :], 0)
+    return st
 
 
 def decision_state(res, skip: bool) -> np.ndarray:

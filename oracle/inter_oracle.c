@@ -315,19 +315,26 @@ struct ironav_ctx {
     int qpp, lambda, skip_thresh, nact, fast, sub8;
     int threads;
     void* inloop; /* in-loop mode state */
+    /* B picture parameters */
+    int b_ref[2];           /* held references used as list 0 and list 1 */
+    ironav_mbstate* b_col;  /* the list-1 picture's decisions, or NULL */
+    int b_tb, b_td, b_set;
 };
 
 typedef struct fc {
     const struct ironav_ctx* c;
-    const ironav_mbstate* states; /* final states of the whole picture */
+    const ironav_mbstate* states;    /* final states of the whole picture (P pictures) */
+    const ironav_mbstate_b* bstates; /* B pictures: final states with both lists (NULL for P pictures) */
+    int list;                        /* B pictures: the list the neighbour lookups and searches use */
+    const halfpel* bhp;              /* B pictures: that list's reference picture */
 } fc;
 
-/* nb_state, enc/frame.rs:509-515 */
-static const ironav_mbstate* nb_state(const fc* f, int mbx, int mby, int cur_mby) {
+/* nb_state, enc/frame.rs:509-515: the index of the neighbour's state, or -1 when it is not available */
+static long nb_index(const fc* f, int mbx, int mby, int cur_mby) {
     const struct ironav_ctx* c = f->c;
     int start = c->band_start[cur_mby];
-    if (mbx < 0 || mby < start || mbx >= c->mb_w || mby >= c->mb_h) return NULL;
-    return &f->states[(size_t)mby * c->mb_w + mbx];
+    if (mbx < 0 || mby < start || mbx >= c->mb_w || mby >= c->mb_h) return -1;
+    return (long)mby * c->mb_w + mbx;
 }
 
 typedef struct nbm { int avail, ref, mv[2]; } nbm;
@@ -352,9 +359,21 @@ static nbm nb_motion(const fc* f, int mbx, int mby, const int16_t cur[16][2], co
         }
         return r;
     }
-    const ironav_mbstate* s = nb_state(f, mbx + dx, mby + dy, mby);
-    if (!s) return r;
+    long i = nb_index(f, mbx + dx, mby + dy, mby);
+    if (i < 0) return r;
     r.avail = 1;
+    if (f->bstates) {
+        /* a B picture's neighbour, in list f->list (MbState.refs[l], mvs / mvs1) */
+        const ironav_mbstate_b* sb = &f->bstates[i];
+        int rf = sb->refs[f->list][(by / 2) * 2 + bx / 2];
+        if (sb->inter && rf >= 0) {
+            r.ref = rf;
+            r.mv[0] = sb->mvs[f->list][by * 4 + bx][0];
+            r.mv[1] = sb->mvs[f->list][by * 4 + bx][1];
+        }
+        return r;
+    }
+    const ironav_mbstate* s = &f->states[i];
     int rf = s->refs[(by / 2) * 2 + bx / 2];
     if (s->inter && rf >= 0) {
         r.ref = rf;
@@ -451,7 +470,7 @@ static int satd_blk(const fc* f, int x, int y, int w, int h, const uint16_t* pre
 
 /* sad_int, enc/frame.rs:662-671 with HalfPel::rows, enc/subpel.rs:148-151 */
 static int sad_int(const fc* f, int r, int x, int y, int w, int h, int mvx, int mvy) {
-    const halfpel* hp = &f->c->refs[r].hp;
+    const halfpel* hp = f->bhp ? f->bhp : &f->c->refs[r].hp;
     const uint16_t* g = hp->planes[0] + hp_offset(hp, x + (mvx >> 2), y + (mvy >> 2));
     const uint16_t* src = f->c->src + (size_t)y * f->c->pw + x;
     int sad = 0;
@@ -484,7 +503,7 @@ static int motion_search(const fc* f, counters* cnt, int r, int mbx, int mby, re
 #define CLY(v) clampi((v), cylo, cyhi)
 #define INTR(v) (((v) + 2) & ~3)
 #define COST_INT(mx, my) (cnt->sad_px += (uint32_t)(w * h), sad_int(f, r, x0, y0, w, h, (mx), (my)) + lam * mvd_bits((mx), (my), mvp[0], mvp[1]))
-    int cands[8][2];
+    int cands[16][2];
     int nc = 0;
     cands[nc][0] = INTR(CLX(mvp[0]));
     cands[nc][1] = INTR(CLY(mvp[1]));
@@ -546,7 +565,7 @@ static int motion_search(const fc* f, counters* cnt, int r, int mbx, int mby, re
     }
     /* sub-sample refinement by SATD (994-1017) */
     uint16_t pred[256];
-    const halfpel* hp = &c->refs[r].hp;
+    const halfpel* hp = f->bhp ? f->bhp : &c->refs[r].hp;
 #define COST_SUB(mx, my)                                                                                   \
     (cnt->satd_px += (uint32_t)(w * h), halfpel_predict(hp, x0, y0, (mx), (my), w, h, pred),              \
      satd_blk(f, x0, y0, w, h, pred) + lam * mvd_bits((mx), (my), mvp[0], mvp[1]))
@@ -830,6 +849,7 @@ int ironav_ctx_destroy(ironav_ctx* c) {
     free(c->refs);
     free(c->src);
     free(c->band_start);
+    free(c->b_col);
     if (c->inloop) free(((ironav_mbstate**)c->inloop)[0]);
     free(c->inloop);
     free(c);
@@ -937,7 +957,7 @@ int oracle_set_threads(ironav_ctx* c, int n) {
 
 int ironav_analyse_picture_replay(ironav_ctx* c, const ironav_mbstate* states, ironav_mbresult* out) {
     if (!c || !states || !out || c->nact < 1) return IRONAV_INVALID_ARGUMENT;
-    fc f = {c, states};
+    fc f = {c, states, NULL, 0, NULL};
     long n = (long)c->mb_w * c->mb_h;
 #ifdef _OPENMP
 #pragma omp parallel for schedule(dynamic, 16) num_threads(c->threads)
@@ -949,7 +969,7 @@ int ironav_analyse_picture_replay(ironav_ctx* c, const ironav_mbstate* states, i
 /* Replay over a subset of macroblocks (indices), for bounded CPU-baseline samples. */
 int oracle_analyse_replay_subset(ironav_ctx* c, const ironav_mbstate* states, const int* idx, int count, ironav_mbresult* out) {
     if (!c || !states || !out || !idx || c->nact < 1) return IRONAV_INVALID_ARGUMENT;
-    fc f = {c, states};
+    fc f = {c, states, NULL, 0, NULL};
 #ifdef _OPENMP
 #pragma omp parallel for schedule(dynamic, 16) num_threads(c->threads)
 #endif
@@ -962,7 +982,7 @@ int oracle_analyse_replay_subset(ironav_ctx* c, const ironav_mbstate* states, co
 int ironav_analyse_picture_auto(ironav_ctx* c, ironav_mbstate* states, ironav_mbresult* out) {
     if (!c || !states || !out || c->nact < 1) return IRONAV_INVALID_ARGUMENT;
     memset(states, 0, sizeof(ironav_mbstate) * (size_t)c->mb_w * c->mb_h);
-    fc f = {c, states};
+    fc f = {c, states, NULL, 0, NULL};
     int nb = 0;
     int starts[1025];
     for (int r = 0; r < c->mb_h; r++)
@@ -1041,7 +1061,7 @@ int ironav_inloop_begin(ironav_ctx* c, int order) {
 int ironav_inloop_result(ironav_ctx* c, int mb, ironav_mbresult* out, int timeout_ms) {
     (void)timeout_ms;
     if (!c || !out || !c->inloop || !inloop_of(c)->active || mb < 0 || mb >= c->mb_w * c->mb_h) return IRONAV_INVALID_ARGUMENT;
-    fc f = {c, inloop_of(c)->committed};
+    fc f = {c, inloop_of(c)->committed, NULL, 0, NULL};
     analyse_mb(&f, mb % c->mb_w, mb / c->mb_w, 0, out, NULL);
     return IRONAV_OK;
 }
@@ -1411,3 +1431,274 @@ int oracle_dbk_tables(uint8_t* alpha, uint8_t* beta, uint8_t* tc0, uint8_t* cqp)
     memcpy(cqp, DBK_CHROMA_QP, 22);
     return 0;
 }
+
+/* ---------------------------------------------------------------------------------------------------
+ * B pictures: the searches of decide_b (enc/frame.rs:1518-1572), best_b_parts (1626-1687) and spatial
+ * direct (direct_mvs, 1715-1747), for replay mode. One reference picture per list, reference index 0.
+ * ------------------------------------------------------------------------------------------------- */
+
+/* the co-located vector scaled by picture distances, enc/frame.rs:1553-1554 (i32 division, toward zero) */
+static int bscale(int v, int num, int den) { return (int16_t)(v * num / den); }
+
+/* minpos of direct_mvs: the smaller of two reference indices that are both present, else the present one */
+static int minpos(int x, int y) { return (x >= 0 && y >= 0) ? mini(x, y) : maxi(x, y); }
+
+/* direct_mvs, enc/frame.rs:1715-1747 */
+static void b_direct(const fc fl[2], int mbx, int mby, const ironav_mbstate* col, int16_t d[2][16][2], uint8_t use[2]) {
+    int refs[2];
+    for (int l = 0; l < 2; l++) {
+        nbm a = nb_motion(&fl[l], mbx, mby, ZERO_MVS, NO_REF, 0, -1, 0);
+        nbm b = nb_motion(&fl[l], mbx, mby, ZERO_MVS, NO_REF, 0, 0, -1);
+        nbm c = nb_motion(&fl[l], mbx, mby, ZERO_MVS, NO_REF, 0, 4, -1);
+        if (!c.avail) c = nb_motion(&fl[l], mbx, mby, ZERO_MVS, NO_REF, 0, -1, -1);
+        refs[l] = minpos(a.ref, minpos(b.ref, c.ref)); /* an unavailable neighbour has ref -1 */
+    }
+    memset(d, 0, sizeof(int16_t) * 2 * 16 * 2);
+    if (refs[0] < 0 && refs[1] < 0) {
+        use[0] = use[1] = 1;
+        return;
+    }
+    for (int l = 0; l < 2; l++) {
+        if (refs[l] < 0) continue;
+        int mv[2];
+        mv_pred(&fl[l], mbx, mby, 0, mv);
+        for (int b = 0; b < 16; b++) {
+            d[l][b][0] = (int16_t)mv[0];
+            d[l][b][1] = (int16_t)mv[1];
+        }
+    }
+    if (col && col->inter) {
+        for (int b = 0; b < 16; b++) {
+            /* the corner 4x4 block of each 8x8 block stands for it (direct_8x8_inference_flag) */
+            int cx = ((b % 4) >> 1) * 3, cy = ((b / 4) >> 1) * 3;
+            const int16_t* m = col->mvs[cy * 4 + cx];
+            if (col->refs[(cy >> 1) * 2 + (cx >> 1)] == 0 && abs(m[0]) <= 1 && abs(m[1]) <= 1)
+                for (int l = 0; l < 2; l++)
+                    if (refs[l] == 0) d[l][b][0] = d[l][b][1] = 0;
+        }
+    }
+    use[0] = refs[0] >= 0;
+    use[1] = refs[1] >= 0;
+}
+
+/* the search of one partition of best_b_parts (its `search` closure, enc/frame.rs:1631-1657): each list,
+ * both averaged, and (8x8 blocks) direct prediction; returns the direction, its cost, and the vectors */
+static int b_part_search(const fc fl[2], counters* cnt, int mbx, int mby, rect4 pr, const int mvps[2][2], const int (*extra[2])[2],
+                         const int nextra[2], int direct, const uint16_t dpred[256], int mv[2][2], int* dir_out) {
+    int lam = fl[0].c->lambda;
+    int x0 = mbx * 16 + pr.x * 4, y0 = mby * 16 + pr.y * 4, pw = pr.w * 4, ph = pr.h * 4;
+    int cost[2];
+    uint16_t preds[2][128];
+    for (int l = 0; l < 2; l++) {
+        cost[l] = motion_search(&fl[l], cnt, 0, mbx, mby, pr, mvps[l], extra[l], nextra[l], mv[l]);
+        halfpel_predict(fl[l].bhp, x0, y0, mv[l][0], mv[l][1], pw, ph, preds[l]);
+    }
+    uint16_t avg[128];
+    for (int i = 0; i < pw * ph; i++) avg[i] = (uint16_t)((preds[0][i] + preds[1][i] + 1) >> 1);
+    cnt->satd_px += (uint32_t)(pw * ph);
+    int bi = satd_blk(&fl[0], x0, y0, pw, ph, avg) + lam * (mvd_bits(mv[0][0], mv[0][1], mvps[0][0], mvps[0][1]) +
+                                                           mvd_bits(mv[1][0], mv[1][1], mvps[1][0], mvps[1][1]) + 2);
+    int bd, bc;
+    if (bi < mini(cost[0], cost[1])) { bd = 3; bc = bi; }
+    else if (cost[0] <= cost[1]) { bd = 1; bc = cost[0]; }
+    else { bd = 2; bc = cost[1]; }
+    if (direct) {
+        /* sub_mb_type takes about one bin for direct and three for the others */
+        bc += lam * 3;
+        uint16_t sub[128];
+        for (int i = 0; i < pw * ph; i++) sub[i] = dpred[(pr.y * 4 + i / pw) * 16 + pr.x * 4 + i % pw];
+        cnt->satd_px += (uint32_t)(pw * ph);
+        int dc = satd_blk(&fl[0], x0, y0, pw, ph, sub) + lam;
+        if (dc < bc) { bd = 0; bc = dc; }
+    }
+    *dir_out = bd;
+    return bc;
+}
+
+/* best_b_parts, enc/frame.rs:1626-1687: returns 0 when no partitioning costs less than cost16 */
+static int b_parts(const fc fl[2], counters* cnt, int mbx, int mby, const int mvs16[2][2], const int mvps[2][2], int cost16,
+                   const uint16_t dpred[256], ironav_bresult* out) {
+    int lam = fl[0].c->lambda;
+    int dirs[4] = {0, 0, 0, 0}, pmv[2][4][2];
+    memset(pmv, 0, sizeof(pmv));
+    int total = lam * 6;
+    for (int k = 0; k < 4; k++) {
+        int ex[2][1][2] = {{{mvs16[0][0], mvs16[0][1]}}, {{mvs16[1][0], mvs16[1][1]}}};
+        const int (*extra[2])[2] = {ex[0], ex[1]};
+        const int nex[2] = {1, 1};
+        int mv[2][2], d;
+        total += b_part_search(fl, cnt, mbx, mby, PARTS_[3][k], mvps, extra, nex, 1, dpred, mv, &d);
+        dirs[k] = d;
+        for (int l = 0; l < 2; l++) {
+            pmv[l][k][0] = mv[l][0];
+            pmv[l][k][1] = mv[l][1];
+        }
+        if (total >= cost16) return 0;
+    }
+    int best_part = 3, best_dirs[4], best_mv[2][4][2], best_total = total;
+    memcpy(best_dirs, dirs, sizeof(dirs));
+    memcpy(best_mv, pmv, sizeof(pmv));
+    for (int part = 1; part < 3; part++) {
+        int pd[4] = {0, 0, 0, 0}, pm[2][4][2], pt = lam * 7;
+        memset(pm, 0, sizeof(pm));
+        int ex[2][5][2];
+        for (int l = 0; l < 2; l++) {
+            for (int k = 0; k < 4; k++) {
+                ex[l][k][0] = pmv[l][k][0];
+                ex[l][k][1] = pmv[l][k][1];
+            }
+            ex[l][4][0] = mvs16[l][0];
+            ex[l][4][1] = mvs16[l][1];
+        }
+        const int (*extra[2])[2] = {ex[0], ex[1]};
+        const int nex[2] = {5, 5};
+        for (int k = 0; k < NPARTS[part]; k++) {
+            int mv[2][2], d;
+            pt += b_part_search(fl, cnt, mbx, mby, PARTS_[part][k], mvps, extra, nex, 0, dpred, mv, &d);
+            pd[k] = d;
+            for (int l = 0; l < 2; l++) {
+                pm[l][k][0] = mv[l][0];
+                pm[l][k][1] = mv[l][1];
+            }
+            if (pt >= best_total) break;
+        }
+        if (pt < best_total) {
+            best_part = part;
+            memcpy(best_dirs, pd, sizeof(pd));
+            memcpy(best_mv, pm, sizeof(pm));
+            best_total = pt;
+        }
+    }
+    out->part = (uint8_t)best_part;
+    for (int k = 0; k < 4; k++) {
+        out->bdir[k] = (uint8_t)best_dirs[k];
+        for (int l = 0; l < 2; l++) {
+            out->pmv[l][k][0] = (int16_t)best_mv[l][k][0];
+            out->pmv[l][k][1] = (int16_t)best_mv[l][k][1];
+        }
+    }
+    return 1;
+}
+
+/* The searches of decide_b for macroblock (mbx, mby), enc/frame.rs:1518-1572. */
+static void analyse_b_mb(const struct ironav_ctx* c, const ironav_mbstate_b* states, int mbx, int mby, ironav_bresult* out) {
+    fc fl[2];
+    for (int l = 0; l < 2; l++) {
+        fl[l].c = c;
+        fl[l].states = NULL;
+        fl[l].bstates = states;
+        fl[l].list = l;
+        fl[l].bhp = &c->refs[c->b_ref[l]].hp;
+    }
+    counters cnt = {0, 0};
+    memset(out, 0, sizeof(*out));
+    int lam = c->lambda;
+    size_t idx = (size_t)mby * c->mb_w + mbx;
+    const ironav_mbstate* col = c->b_col ? &c->b_col[idx] : NULL;
+    /* spatial direct and its luma prediction (b_pred with the direct vectors, 1749-1781) */
+    int16_t direct[2][16][2];
+    uint8_t duse[2];
+    b_direct(fl, mbx, mby, col, direct, duse);
+    memcpy(out->direct_mv, direct, sizeof(direct));
+    out->direct_use[0] = duse[0];
+    out->direct_use[1] = duse[1];
+    int x0 = mbx * 16, y0 = mby * 16;
+    uint16_t dpred[256];
+    for (int i8 = 0; i8 < 4; i8++) {
+        int bx = (i8 & 1) * 8, by = (i8 >> 1) * 8;
+        uint16_t lp[2][64];
+        memset(lp, 0, sizeof(lp));
+        for (int l = 0; l < 2; l++)
+            if (duse[l]) {
+                const int16_t* v = direct[l][(by / 4) * 4 + bx / 4];
+                halfpel_predict(fl[l].bhp, x0 + bx, y0 + by, v[0], v[1], 8, 8, lp[l]);
+            }
+        for (int k = 0; k < 64; k++) {
+            int a = lp[0][k], b = lp[1][k];
+            dpred[(by + k / 8) * 16 + bx + k % 8] = (uint16_t)(duse[0] && duse[1] ? (a + b + 1) >> 1 : (duse[0] ? a : b));
+        }
+    }
+    /* 16x16 from either list or both */
+    int mvps[2][2], mvs[2][2], costs[2];
+    for (int l = 0; l < 2; l++) mv_pred(&fl[l], mbx, mby, 0, mvps[l]);
+    int tb = c->b_tb, td = c->b_td;
+    uint16_t preds[2][256];
+    for (int l = 0; l < 2; l++) {
+        int extra[2][2], n = 0;
+        if (col && col->inter) {
+            extra[n][0] = l == 0 ? bscale(col->mvs[5][0], tb, td) : bscale(col->mvs[5][0], tb - td, td);
+            extra[n][1] = l == 0 ? bscale(col->mvs[5][1], tb, td) : bscale(col->mvs[5][1], tb - td, td);
+            n++;
+        }
+        if (l == 1) {
+            extra[n][0] = bscale(mvs[0][0], tb - td, tb);
+            extra[n][1] = bscale(mvs[0][1], tb - td, tb);
+            n++;
+        }
+        int cst = motion_search(&fl[l], &cnt, 0, mbx, mby, PARTS_[0][0], mvps[l], (const int(*)[2])extra, n, mvs[l]);
+        costs[l] = cst + lam * (mvd_bits(mvs[l][0], mvs[l][1], mvps[l][0], mvps[l][1]) + 3);
+        halfpel_predict(fl[l].bhp, x0, y0, mvs[l][0], mvs[l][1], 16, 16, preds[l]);
+    }
+    uint16_t avg[256];
+    for (int i = 0; i < 256; i++) avg[i] = (uint16_t)((preds[0][i] + preds[1][i] + 1) >> 1);
+    cnt.satd_px += 256;
+    int bi = satd_blk(&fl[0], x0, y0, 16, 16, avg) +
+             lam * (mvd_bits(mvs[0][0], mvs[0][1], mvps[0][0], mvps[0][1]) + mvd_bits(mvs[1][0], mvs[1][1], mvps[1][0], mvps[1][1]) + 5);
+    out->dir16 = (uint8_t)(bi < mini(costs[0], costs[1]) ? 3 : (costs[0] <= costs[1] ? 1 : 2));
+    for (int l = 0; l < 2; l++) {
+        out->mv16[l][0] = (int16_t)mvs[l][0];
+        out->mv16[l][1] = (int16_t)mvs[l][1];
+        out->cost16[l] = costs[l];
+    }
+    out->cost_bi = bi;
+    out->has_parts = (uint8_t)b_parts(fl, &cnt, mbx, mby, (const int(*)[2])mvs, (const int(*)[2])mvps, mini(bi, mini(costs[0], costs[1])),
+                                      dpred, out);
+    out->sad_px = cnt.sad_px;
+    out->satd_px = cnt.satd_px;
+}
+
+static int b_params_ok(struct ironav_ctx* c, int qpp, int lambda, int l0, int l1, int tb, int td) {
+    return c && lambda >= 1 && qpp >= 0 && qpp <= 63 && l0 >= 0 && l0 < c->nrefs && l1 >= 0 && l1 < c->nrefs && tb != 0 && td != 0;
+}
+
+int ironav_begin_b_picture(ironav_ctx* c, int qpp, int lambda, int ref_l0, int ref_l1, const ironav_mbstate* col, int tb, int td, int fast) {
+    if (!b_params_ok(c, qpp, lambda, ref_l0, ref_l1, tb, td)) return IRONAV_INVALID_ARGUMENT;
+    c->qpp = qpp;
+    c->lambda = lambda;
+    c->fast = fast ? 1 : 0;
+    c->b_ref[0] = ref_l0;
+    c->b_ref[1] = ref_l1;
+    c->b_tb = tb;
+    c->b_td = td;
+    free(c->b_col);
+    c->b_col = NULL;
+    if (col) {
+        size_t n = (size_t)c->mb_w * c->mb_h;
+        c->b_col = (ironav_mbstate*)malloc(sizeof(ironav_mbstate) * n);
+        memcpy(c->b_col, col, sizeof(ironav_mbstate) * n);
+    }
+    c->b_set = 1;
+    return IRONAV_OK;
+}
+
+int ironav_begin_b_picture_device(ironav_ctx* c, int qpp, int lambda, int ref_l0, int ref_l1, const ironav_mbstate* d_col, int tb, int td,
+                                  int fast) {
+    (void)c; (void)qpp; (void)lambda; (void)ref_l0; (void)ref_l1; (void)d_col; (void)tb; (void)td; (void)fast;
+    return IRONAV_HARDWARE_UNAVAILABLE;
+}
+
+int ironav_analyse_b_replay(ironav_ctx* c, const ironav_mbstate_b* states, ironav_bresult* out) {
+    if (!c || !states || !out || !c->b_set || c->b_ref[0] >= c->nrefs || c->b_ref[1] >= c->nrefs) return IRONAV_INVALID_ARGUMENT;
+    long n = (long)c->mb_w * c->mb_h;
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 16) num_threads(c->threads)
+#endif
+    for (long i = 0; i < n; i++) analyse_b_mb(c, states, (int)(i % c->mb_w), (int)(i / c->mb_w), &out[i]);
+    return IRONAV_OK;
+}
+
+int ironav_analyse_b_replay_device(ironav_ctx* c, const ironav_mbstate_b* s, ironav_bresult* o) {
+    (void)c; (void)s; (void)o;
+    return IRONAV_HARDWARE_UNAVAILABLE;
+}
+
