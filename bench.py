@@ -52,7 +52,7 @@ def parse():
     p.add_argument("--ring", type=int, default=RING,
                    help="pictures in the ring (fewer than 36 fits in L2: for profiling runs only)")
     p.add_argument("--no-e2e", action="store_true", help="skip the host-buffer pass (profiling runs)")
-    p.add_argument("--workload", default="1080p", choices=["1080p", "batched", "scenecut", "deblock"],
+    p.add_argument("--workload", default="1080p", choices=["1080p", "batched", "scenecut", "deblock", "bpicture"],
                    help="1080p: one stream, replay mode (the headline); batched: 64 mixed-resolution streams in auto "
                         "mode, one launch per stage and frame step, against the per-stream launch loop")
     p.add_argument("--streams", type=int, default=64, help="streams of the batched workload")
@@ -261,6 +261,9 @@ def main():
         return finish(world)
     if args.workload == "deblock":
         run_deblock(args, rank, world)
+        return finish(world)
+    if args.workload == "bpicture":
+        run_bpicture(args, rank, world)
         return finish(world)
 
     import torch
@@ -541,6 +544,137 @@ def run_scenecut(args, rank, world):
                                    "(synchronous: returns the totals)"},
             "cpu_baseline": {"value": n_cpu / el_cpu, "unit": "pairs/s", "cores": 1, "kind": "port",
                              "sample": f"{n_cpu} pairs, one thread (the reference's non-live setting)"}}), flush=True)
+
+
+def run_bpicture(args, rank, world):
+    """The B-picture searches at 1080p (decide_b's 16x16 list 0 / list 1 / bi, best_b_parts, spatial direct;
+    enc/frame.rs:1518-1747), replay mode, device-resident: one step = all 8160 macroblocks of one B picture
+    (frames t, t+1, t+2 of a synthetic sequence: list 0, the B picture, list 1). A ring of contexts (each
+    with its two reference pictures) larger than L2; the decisions replayed are those the B results favour,
+    made before the timed region. The oracle runs the same pictures on all host cores."""
+    import torch
+    from ironav_b200.inter import BRESULT_DTYPE, MBSTATE_B_DTYPE, InterStage, b_decision_states, cuda_library
+    from ironav_b200.synth import CONFIGS, Sequence
+
+    lib = cuda_library()
+    ring = max(2, min(args.ring, 6))
+    w, h, seed, pan_q, nobj, vmax, sigma = CONFIGS["1080p"]
+    seq = Sequence(w, h, 2 * ring + 1, seed + 0x1000 * rank, pan_q, nobj, vmax, sigma)
+    qpp = QP + 2  # the encoder's B pictures: QP + 2
+    stream = torch.cuda.Stream()
+    stages, d_states, d_res, frames, states_h = [], [], [], [], []
+    for k in range(ring):
+        f = [seq.frame(2 * k + t) for t in range(3)]
+        st = InterStage(w, h, max_refs=2, nslices=NSLICES, lib=lib)
+        st.push_reference(f[0])
+        st.set_source(f[2])
+        st.begin_p_picture(QP)
+        col, _ = st.analyse_auto()
+        st.push_reference(f[2], col=col)
+        st.set_source(f[1])
+        st.begin_b_picture(qpp, ref_l0=1, ref_l1=0, col=col, tb=1, td=2)
+        states = b_decision_states(st.analyse_b_replay(np.zeros(st.nmb, dtype=MBSTATE_B_DTYPE)))
+        st.set_stream(stream.cuda_stream)
+        stages.append(st)
+        frames.append((f, col))
+        states_h.append(states)
+        d_states.append(torch.from_numpy(states.view(np.uint8)).cuda())
+        d_res.append(torch.zeros(st.nmb * 200, dtype=torch.uint8, device="cuda"))
+    nmb = stages[0].nmb
+
+    def step(i, ev=None):
+        k = i % ring
+        if ev is not None:
+            ev[0].record(stream)
+        lib.ironav_analyse_b_replay_device(stages[k].ctx, d_states[k].data_ptr(), d_res[k].data_ptr())
+        if ev is not None:
+            ev[1].record(stream)
+
+    with torch.cuda.stream(stream):
+        for i in range(args.warmup):
+            step(i)
+        clocks = Clocks(int(os.environ.get("LOCAL_RANK", 0)))
+        clocks.start()
+        t_load = time.perf_counter()
+        i = 0
+        while time.perf_counter() - t_load < 0.6:
+            step(args.warmup + i)
+            i += 1
+            if i % 8 == 0:
+                torch.cuda.synchronize()
+        torch.cuda.synchronize()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for i in range(args.steps):
+            step(args.warmup + i, evs[i])
+        e1.record(stream)
+        torch.cuda.synchronize()
+        clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    k_ms = float(np.mean([a.elapsed_time(b) for a, b in evs]))
+    value = world * nmb * args.steps / (ms * 1e-3)
+    ops = []
+    for i in range(args.steps):
+        r = d_res[(args.warmup + i) % ring].cpu().numpy().view(BRESULT_DTYPE)
+        ops.append(3.0 * r["sad_px"].astype(np.float64).sum() + 9.0 * r["satd_px"].astype(np.float64).sum())
+    achieved = float(np.mean(ops)) / (k_ms * 1e-3) / 1e12
+    peak = ctypes_peak(lib)
+    # end to end: decisions in and results out through the host-buffer call, pinned memory
+    pin_s = [torch.from_numpy(s_.view(np.uint8)).pin_memory() for s_ in states_h]
+    pin_r = [torch.zeros(nmb * 200, dtype=torch.uint8).pin_memory() for _ in range(ring)]
+    for st in stages:
+        st.set_stream(None)
+    for i in range(args.warmup):
+        lib.ironav_analyse_b_replay(stages[i % ring].ctx, pin_s[i % ring].data_ptr(), pin_r[i % ring].data_ptr())
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        k = i % ring
+        s_ = lib.ironav_analyse_b_replay(stages[k].ctx, pin_s[k].data_ptr(), pin_r[k].data_ptr())
+        if s_:
+            raise RuntimeError(f"ironav_analyse_b_replay: {s_}")
+    el = time.perf_counter() - t0
+    line = {
+        "metric": "1080p B-picture inter-analysis MB/s", "value": value, "unit": "MB/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+        "data": "synthetic: seeded 4-octave value noise panned per frame + 8 moving rectangles, sigma 3",
+        "config": {"workload": f"1080p B picture (list 0 = frame t, list 1 = frame t+2, QP' {qpp}, tb 1, td 2), replay mode: "
+                               "spatial direct, 16x16 list 0 / list 1 / bi, best_b_parts for all 8160 macroblocks per step",
+                   "slices": NSLICES, "mode": "replay", "l2": f"ring of {ring} contexts (two reference pictures each, > L2)"},
+        "gpu_launches": args.steps,
+        "e2e": {"value": world * nmb * args.steps / el, "unit": "MB/s", "h2d_bytes_per_step": nmb * 140,
+                "d2h_bytes_per_step": nmb * 200, "ms_per_step": 1e3 * el / args.steps,
+                "note": "ironav_analyse_b_replay on pinned host buffers, one thread"},
+        "roofline": {"bound": "int32", "kernel": "analyse_b_kernel<uint8_t>", "achieved": achieved, "peak": peak,
+                     "unit": "Tops/s", "frac": achieved / peak if peak else None, "traffic": None, "ms_per_launch": k_ms,
+                     "note": "algorithmic ops: 3 per SAD sample, 9 per SATD sample (searches, bi and direct SATDs)"},
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from tests.oracle_lib import oracle_library
+
+        olib = oracle_library()
+        cores = host_cores()
+        f, col = frames[0]
+        o = InterStage(w, h, max_refs=2, nslices=NSLICES, lib=olib)
+        olib.oracle_set_threads(o.ctx, cores)
+        o.push_reference(f[0])
+        o.push_reference(f[2], col=col)
+        o.set_source(f[1])
+        o.begin_b_picture(qpp, ref_l0=1, ref_l1=0, col=col, tb=1, td=2)
+        n_cpu, t_cpu = 0, 0.0
+        while t_cpu < min(args.cpu_seconds, 10.0):
+            t0 = time.perf_counter()
+            o.analyse_b_replay(states_h[0])
+            t_cpu += time.perf_counter() - t0
+            n_cpu += 1
+        line["cpu_baseline"] = {"value": n_cpu * nmb / t_cpu, "unit": "MB/s", "cores": cores, "kind": "port",
+                                "sample": f"{n_cpu} B pictures (the ring's first), replay mode, {cores} threads, {t_cpu:.1f} s"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    for st in stages:
+        st.close()
 
 
 def run_deblock(args, rank, world):

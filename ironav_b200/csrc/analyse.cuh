@@ -402,8 +402,9 @@ static __device__ __noinline__ int4 round_clamped(const AnalyseParams& __restric
 // Returns the best vector in (ox, oy) and its cost without the vector's bits. The search runs on the
 // half-sample planes P.planes[r]; the neighbour candidates come from the table `ext` of the list searched
 // and count when their reference index is rsel. (e0x, e0y) and (e1x, e1y) are the first extra candidates
-// (nextra of them), more[0..nmore) the ones after them (B-picture partitions; at most 9).
-template <class T>
+// (nextra of them), more[0..nmore) the ones after them (B-picture partitions; at most 9; compiled in only
+// when MORE).
+template <class T, bool MORE>
 static __device__ __noinline__ int4 motion_search(const AnalyseParams& __restrict__ P, WarpSmem<T>& __restrict__ S, const Blk* ext, int rsel, int r, int bx, int by,
                                                   int w4, int h4, int mvpx, int mvpy, int e0x, int e0y, int e1x, int e1y, int nextra,
                                                   const int2* more, int nmore) {
@@ -423,8 +424,11 @@ static __device__ __noinline__ int4 motion_search(const AnalyseParams& __restric
         px = intr(clx(mvpx));
         py = intr(cly(mvpy));
     } else if (g >= 2 && g <= 4) {
-        const Blk n = g == 2 ? nb(P, S, ext, nullptr, -1, 0) : (g == 3 ? nb(P, S, ext, nullptr, 0, -1) : nb(P, S, ext, nullptr, 4, -1));
-        valid = n.w && n.z == rsel;
+        // P pictures: the list-0 table and the searched reference (the arguments are those)
+        const Blk* E = MORE ? ext : S.ext;
+        const int rs = MORE ? rsel : r;
+        const Blk n = g == 2 ? nb(P, S, E, nullptr, -1, 0) : (g == 3 ? nb(P, S, E, nullptr, 0, -1) : nb(P, S, E, nullptr, 4, -1));
+        valid = n.w && n.z == rs;
         px = intr(clx(n.x));
         py = intr(cly(n.y));
     } else if (g == 5) {
@@ -436,8 +440,8 @@ static __device__ __noinline__ int4 motion_search(const AnalyseParams& __restric
         px = intr(clx(e1x));
         py = intr(cly(e1y));
     } else if (g == 7) {
-        valid = nmore > 0;
-        if (valid) {
+        valid = MORE && nmore > 0;
+        if (MORE && valid) {
             px = intr(clx(more[0].x));
             py = intr(cly(more[0].y));
         }
@@ -451,7 +455,7 @@ static __device__ __noinline__ int4 motion_search(const AnalyseParams& __restric
     if (lane == 0) S.sad_px += (uint32_t)(__popc(vmask) * w * h);
     // the first candidate of least cost: min over (cost, position in the list)
     unsigned long long key = ((unsigned long long)(unsigned)cost << 4) | (unsigned)g;
-    if (nmore > 1) {
+    if (MORE && nmore > 1) {
         // the candidates after the eighth (list positions 8..15): a second batch
         const bool v2 = g + 1 < nmore;
         int qx = 0, qy = 0;
@@ -620,7 +624,7 @@ static __device__ __noinline__ int2 sub_search(const AnalyseParams& __restrict__
         for (int q = 0; q < c_nsub[s]; q++) {
             const int x = ox + c_sub[s][q][0], y = oy + c_sub[s][q][1], w = c_sub[s][q][2], h = c_sub[s][q][3];
             const int2 p = pred_mv(P, S, S.ext, S.t, x, y, w, 0, r);
-            const int4 ms = motion_search(P, S, S.ext, r, r, x, y, w, h, p.x, p.y, ex, ey, 0, 0, 1, nullptr, 0);
+            const int4 ms = motion_search<T, false>(P, S, S.ext, r, r, x, y, w, h, p.x, p.y, ex, ey, 0, 0, 1, nullptr, 0);
             const int c = ms.x, mx = ms.y, my = ms.z;
             cost += c + lam * mvd_bits_d(mx, my, p.x, p.y);
             blk_paint(P, S, S.t, x, y, w, h, mx, my, r);
@@ -645,7 +649,7 @@ static __device__ __noinline__ int4 best_inter_ref(const AnalyseParams& __restri
     else if (P.nact > 2) rb = lam * (2 * (31 - __clz(r + 1)) + 1);
     const int2 mvp = pred_mv(P, S, S.ext, nullptr, 0, 0, 4, 0, r);
     const ColMv col = P.col[S.mb];
-    const int4 ms = motion_search(P, S, S.ext, r, r, 0, 0, 4, 4, mvp.x, mvp.y, col.mv[0], col.mv[1], 0, 0, col.valid ? 1 : 0, nullptr, 0);
+    const int4 ms = motion_search<T, false>(P, S, S.ext, r, r, 0, 0, 4, 4, mvp.x, mvp.y, col.mv[0], col.mv[1], 0, 0, col.valid ? 1 : 0, nullptr, 0);
     const int c = ms.x, mx = ms.y, my = ms.z;
     int best_part = 0, best_cost = c + lam * (mvd_bits_d(mx, my, mvp.x, mvp.y) + 1) + rb;
     const int cost16 = best_cost;
@@ -699,7 +703,7 @@ static __device__ __noinline__ int4 best_inter_ref(const AnalyseParams& __restri
                 const int2 p = pred_mv(P, S, S.ext, S.t, x, y, w, part, r);
                 const int i0 = part == 1 ? 2 * k : k, i1 = part == 1 ? 2 * k + 1 : k + 2;
                 const Blk a0 = S.st[(i0 / 2) * 8 + (i0 % 2) * 2], a1 = S.st[(i1 / 2) * 8 + (i1 % 2) * 2];
-                const int4 ms = motion_search(P, S, S.ext, r, r, x, y, w, h, p.x, p.y, a0.x, a0.y, a1.x, a1.y, 2, nullptr, 0);
+                const int4 ms = motion_search<T, false>(P, S, S.ext, r, r, x, y, w, h, p.x, p.y, a0.x, a0.y, a1.x, a1.y, 2, nullptr, 0);
                 const int cc = ms.x, m0 = ms.y, m1 = ms.z;
                 if (k == 0) {
                     h0x = m0;

@@ -89,9 +89,9 @@ static __device__ int4 b_part_search(const AnalyseParams& __restrict__ P, WarpSm
                                      const int2* ex0, const int2* ex1, int nex, bool direct, int2 dv0, int2 dv1, int duse) {
     const int lam = P.lambda;
     // the extra candidates of each list: the first two as registers, the rest (the halves' 3) by pointer
-    const int4 m0 = motion_search(P, S, S.ext, 0, 0, bx, by, w4, h4, mvp0.x, mvp0.y, ex0[0].x, ex0[0].y, nex > 1 ? ex0[1].x : 0,
+    const int4 m0 = motion_search<T, true>(P, S, S.ext, 0, 0, bx, by, w4, h4, mvp0.x, mvp0.y, ex0[0].x, ex0[0].y, nex > 1 ? ex0[1].x : 0,
                                   nex > 1 ? ex0[1].y : 0, min(nex, 2), nex > 2 ? ex0 + 2 : nullptr, max(nex - 2, 0));
-    const int4 m1 = motion_search(P, S, S.ext1, 0, 1, bx, by, w4, h4, mvp1.x, mvp1.y, ex1[0].x, ex1[0].y, nex > 1 ? ex1[1].x : 0,
+    const int4 m1 = motion_search<T, true>(P, S, S.ext1, 0, 1, bx, by, w4, h4, mvp1.x, mvp1.y, ex1[0].x, ex1[0].y, nex > 1 ? ex1[1].x : 0,
                                   nex > 1 ? ex1[1].y : 0, min(nex, 2), nex > 2 ? ex1 + 2 : nullptr, max(nex - 2, 0));
     const int2 v0 = make_int2(m0.y, m0.z), v1 = make_int2(m1.y, m1.z);
     const int lgw = w4 == 4 ? 2 : (w4 == 2 ? 1 : 0), lgh = h4 == 4 ? 2 : (h4 == 2 ? 1 : 0);
@@ -254,14 +254,14 @@ static __device__ void analyse_b(const AnalyseParams& __restrict__ P, WarpSmemB<
         cy = col->mvs[5][1];
     }
     const int tb = P.tb, td = P.td;
-    const int4 s0 = motion_search(P, S, S.ext, 0, 0, 0, 0, 4, 4, mvp0.x, mvp0.y, bscale_d(cx, tb, td), bscale_d(cy, tb, td), 0, 0, ce,
+    const int4 s0 = motion_search<T, true>(P, S, S.ext, 0, 0, 0, 0, 4, 4, mvp0.x, mvp0.y, bscale_d(cx, tb, td), bscale_d(cy, tb, td), 0, 0, ce,
                                   (const int2*)nullptr, 0);
     const int2 v0 = make_int2(s0.y, s0.z);
     // list 1: the co-located vector (if any), then list 0's vector scaled
     const int e1x = bscale_d(v0.x, tb - td, tb), e1y = bscale_d(v0.y, tb - td, tb);
-    const int4 s1 = col_inter ? motion_search(P, S, S.ext1, 0, 1, 0, 0, 4, 4, mvp1.x, mvp1.y, bscale_d(cx, tb - td, td),
+    const int4 s1 = col_inter ? motion_search<T, true>(P, S, S.ext1, 0, 1, 0, 0, 4, 4, mvp1.x, mvp1.y, bscale_d(cx, tb - td, td),
                                               bscale_d(cy, tb - td, td), e1x, e1y, 2, (const int2*)nullptr, 0)
-                              : motion_search(P, S, S.ext1, 0, 1, 0, 0, 4, 4, mvp1.x, mvp1.y, e1x, e1y, 0, 0, 1,
+                              : motion_search<T, true>(P, S, S.ext1, 0, 1, 0, 0, 4, 4, mvp1.x, mvp1.y, e1x, e1y, 0, 0, 1,
                                               (const int2*)nullptr, 0);
     const int2 v1 = make_int2(s1.y, s1.z);
     const int c0 = s0.x + lam * (mvd_bits_d(v0.x, v0.y, mvp0.x, mvp0.y) + 3);
