@@ -220,6 +220,58 @@ int ironav_begin_b_picture_device(ironav_ctx* ctx, int qp_prime, int lambda, int
 int ironav_analyse_b_replay(ironav_ctx* ctx, const ironav_mbstate_b* final_states, ironav_bresult* out);
 int ironav_analyse_b_replay_device(ironav_ctx* ctx, const ironav_mbstate_b* d_final_states, ironav_bresult* d_out);
 
+/* ---- inter residual coding and reconstruction --------------------------------------------------------- */
+
+/* The coding of inter macroblocks once their decisions are made (code_inter / code_inter_residual /
+ * code_luma8 / code_chroma, enc/frame.rs:1202-1305, 1856-1915): the luma and chroma prediction, the
+ * transform, quantisation and decimation of the residual, and the reconstruction. Every inter macroblock
+ * is independent of its neighbours here, so a whole picture is coded at once; intra macroblocks (coded in
+ * order against their neighbours' reconstruction) and the entropy coding stay with the caller.
+ *
+ * Chroma is 4:2:0. The source's chroma (width/2 x height/2, padded to 8*mb_w x 8*mb_h by repeating its
+ * edges like the luma) and each reference picture's chroma (its reconstruction, 8*mb_w x 8*mb_h, or the
+ * picture size to be padded) come in through: */
+int ironav_set_source_chroma(ironav_ctx* ctx, const void* cb, const void* cr, int stride);
+/* attaches chroma to reference 0 (the newest, as pushed with ironav_push_reference) */
+int ironav_push_reference_chroma(ironav_ctx* ctx, const void* cb, const void* cr, int stride, int w, int h);
+
+/* One macroblock's inter coding decision (code_inter's arguments). */
+typedef struct ironav_interdec {
+    uint8_t mode;          /* 0: not an inter macroblock (left alone); 1: P_Skip (the prediction is the
+                              reconstruction, no residual); 2: coded with its residual */
+    uint8_t part;          /* 0 16x16, 1 16x8, 2 8x16, 3 8x8 */
+    uint8_t sub[4];        /* sub_mb_type per 8x8 block (part 3) */
+    uint8_t refs[4];       /* reference index per partition (per 8x8 block for part 3) */
+    uint8_t t8;            /* the 8x8 transform is tried (kept only when some luma is coded) */
+    uint8_t pad[3];
+    int16_t mvs[16][2];    /* one vector per partition, in coding order (rects(part, sub)) */
+} ironav_interdec;         /* 78 bytes */
+
+/* The coded residual of an inter macroblock (MbCode's levels; enc/frame.rs:1217-1305, 1856-1915). */
+typedef struct ironav_intercode {
+    int16_t luma[16][16];  /* 4x4 transform: the levels of each 4x4 block (raster order), zigzag order */
+    int16_t luma8[4][64];  /* 8x8 transform (t8x8): the levels of each 8x8 block, 8x8 zigzag order */
+    int16_t cdc[2][4];     /* chroma DC levels of Cb and Cr */
+    int16_t cac[2][4][16]; /* chroma AC levels per 4x4 block, zigzag order (position 0 unused) */
+    uint8_t nnz[16];       /* non-zero levels per 4x4 luma block (for the 8x8 transform: its 8x8 block's) */
+    uint8_t cnnz[2][4];    /* non-zero AC levels per chroma 4x4 block */
+    uint8_t cbp;           /* coded_block_pattern: luma in bits 0-3, chroma (0, 1 DC, 2 AC) in bits 4-5 */
+    uint8_t t8x8;          /* the 8x8 transform is used */
+    uint8_t pad[2];
+} ironav_intercode;        /* 1324 bytes */
+
+/* Codes the inter macroblocks of the current picture (the source set with ironav_set_source and
+ * ironav_set_source_chroma) at QP_Y qp: decs and codes hold mb_w*mb_h entries; the reconstruction
+ * planes (luma 16*mb_w x 16*mb_h, rows y_stride samples apart; chroma 8*mb_w x 8*mb_h, rows c_stride
+ * apart) receive the inter macroblocks and keep every other macroblock as they were. References are
+ * those held (0 = newest), each with its chroma. */
+int ironav_code_inter_picture(ironav_ctx* ctx, int qp, const ironav_interdec* decs, ironav_intercode* codes, void* rec_y,
+                              int y_stride, void* rec_cb, void* rec_cr, int c_stride);
+/* The same on device pointers, queued on the context's stream; the reconstruction planes as for
+ * ironav_deblock_picture_device (16-byte aligned, aligned row strides). */
+int ironav_code_inter_picture_device(ironav_ctx* ctx, int qp, const ironav_interdec* d_decs, ironav_intercode* d_codes,
+                                     void* d_rec_y, int y_stride, void* d_rec_cb, void* d_rec_cr, int c_stride);
+
 /* ---- deblocking of the reconstruction ------------------------------------------------------------ */
 
 /* The in-loop deblocking filter (h264/deblock.rs:410-720, ITU-T H.264 8.7) of a reconstructed picture,

@@ -63,6 +63,14 @@ struct ironav_ctx {
     const ironav_mbstate* b_col = nullptr;
     ironav_mbstate_b* d_bstates = nullptr;
     ironav_bresult* d_bresults = nullptr;
+    // inter residual coding: the source's chroma, each reference slot's chroma (Cb then Cr, 8*mb_w x
+    // 8*mb_h each; c_ok: attached since the slot took its picture), host-form staging
+    uint8_t* d_src_c = nullptr;
+    uint8_t* d_ref_c[MAX_REFS] = {};
+    bool ref_c_ok[MAX_REFS] = {};
+    ironav_interdec* d_decs = nullptr;
+    ironav_intercode* d_codes = nullptr;
+    uint8_t* d_rec = nullptr;
 };
 
 

@@ -21,6 +21,7 @@
 #include "peaks.cuh"
 #include "scene.cuh"
 #include "deblock.cuh"
+#include "residual.cuh"
 
 using namespace ironav;
 
@@ -29,6 +30,8 @@ static_assert(sizeof(ironav_mbresult) == 104, "ironav_mbresult layout");
 static_assert(sizeof(ironav_dbk_mb) == 192, "ironav_dbk_mb layout");
 static_assert(sizeof(ironav_mbstate_b) == 140, "ironav_mbstate_b layout");
 static_assert(sizeof(ironav_bresult) == 200, "ironav_bresult layout");
+static_assert(sizeof(ironav_interdec) == 78, "ironav_interdec layout");
+static_assert(sizeof(ironav_intercode) == 1324, "ironav_intercode layout");
 static_assert(sizeof(ironav_dbk_slice) == 20, "ironav_dbk_slice layout");
 
 // The reference slot for a new picture: the oldest one's once max_refs are held, else a free one; the
@@ -114,6 +117,11 @@ void free_ctx(ironav_ctx* c) {
     cudaFree(c->d_bcol_copy);
     cudaFree(c->d_bstates);
     cudaFree(c->d_bresults);
+    cudaFree(c->d_src_c);
+    for (int i = 0; i < MAX_REFS; i++) cudaFree(c->d_ref_c[i]);
+    cudaFree(c->d_decs);
+    cudaFree(c->d_codes);
+    cudaFree(c->d_rec);
     cudaFreeHost(c->h_results);
     cudaFreeHost(c->h_done);
     cudaFreeHost(c->h_committed);
@@ -126,6 +134,7 @@ inline int sample_bytes(const ironav_ctx* c) { return c->bd > 8 ? 2 : 1; }
 
 int launch_planes(ironav_ctx* c, const void* d_luma, int stride, int w, int h, const ironav_mbstate* d_col) {
     const int slot = take_ref_slot(c);
+    c->ref_c_ok[slot] = false;  // its chroma, if any, was the previous picture's
     dim3 grid((c->sw + K1_TW - 1) / K1_TW, (c->sh + K1_TH - 1) / K1_TH);
     const int maxv = (1 << c->bd) - 1;
     if (c->bd > 8)
@@ -621,6 +630,112 @@ int ironav_analyse_b_replay(ironav_ctx* c, const ironav_mbstate_b* states, irona
     int s = launch_b(c, c->d_bstates, c->d_bresults);
     if (s != IRONAV_OK) return s;
     CK(cudaMemcpyAsync(out, c->d_bresults, sizeof(ironav_bresult) * c->nmb, cudaMemcpyDeviceToHost, c->stream));
+    return check_device_error(c);
+}
+
+// ---- inter residual coding ----------------------------------------------------------------------------
+
+// Copies a w x h chroma plane (rows `stride` samples apart) into dst (cw x ch, rows cw apart), padded by
+// repeating its right and bottom edges.
+static int load_chroma(ironav_ctx* c, uint8_t* dst, const void* src, int stride, int w, int h, cudaMemcpyKind kind) {
+    const int B = sample_bytes(c), cw = c->mb_w * 8, ch = c->mb_h * 8;
+    CK(cudaMemcpy2DAsync(dst, (size_t)cw * B, src, (size_t)stride * B, (size_t)w * B, h, kind, c->stream));
+    if (w != cw || h != ch) {
+        dim3 grid((cw + 255) / 256, ch);
+        if (B == 2) pad_edges_kernel<uint16_t><<<grid, 256, 0, c->stream>>>(reinterpret_cast<uint16_t*>(dst), w, h, cw, ch);
+        else pad_edges_kernel<uint8_t><<<grid, 256, 0, c->stream>>>(dst, w, h, cw, ch);
+    }
+    return cuda_status(cudaGetLastError());
+}
+
+int ironav_set_source_chroma(ironav_ctx* c, const void* cb, const void* cr, int stride) {
+    if (!c || !cb || !cr || stride < c->width / 2) return IRONAV_INVALID_ARGUMENT;
+    const size_t plane = (size_t)c->mb_w * 8 * c->mb_h * 8 * sample_bytes(c);
+    if (!c->d_src_c) CK(cudaMalloc(&c->d_src_c, 2 * plane + 256));
+    int s = load_chroma(c, c->d_src_c, cb, stride, c->width / 2, c->height / 2, cudaMemcpyHostToDevice);
+    if (s == IRONAV_OK) s = load_chroma(c, c->d_src_c + plane, cr, stride, c->width / 2, c->height / 2, cudaMemcpyHostToDevice);
+    if (s != IRONAV_OK) return s;
+    CK(cudaStreamSynchronize(c->stream));
+    return IRONAV_OK;
+}
+
+int ironav_push_reference_chroma(ironav_ctx* c, const void* cb, const void* cr, int stride, int w, int h) {
+    if (!c || !cb || !cr || c->nrefs < 1) return IRONAV_INVALID_ARGUMENT;
+    const int cw = c->mb_w * 8, ch = c->mb_h * 8;
+    if (!((w == c->width / 2 && h == c->height / 2) || (w == cw && h == ch)) || stride < w) return IRONAV_INVALID_ARGUMENT;
+    const int slot = c->slot_of[0];
+    const size_t plane = (size_t)cw * ch * sample_bytes(c);
+    if (!c->d_ref_c[slot]) CK(cudaMalloc(&c->d_ref_c[slot], 2 * plane + 256));
+    int s = load_chroma(c, c->d_ref_c[slot], cb, stride, w, h, cudaMemcpyHostToDevice);
+    if (s == IRONAV_OK) s = load_chroma(c, c->d_ref_c[slot] + plane, cr, stride, w, h, cudaMemcpyHostToDevice);
+    if (s != IRONAV_OK) return s;
+    CK(cudaStreamSynchronize(c->stream));
+    c->ref_c_ok[slot] = true;
+    return IRONAV_OK;
+}
+
+static int launch_code_inter(ironav_ctx* c, int qp, const ironav_interdec* d_decs, ironav_intercode* d_codes, void* y, int ys, void* cb,
+                             void* cr, int cs) {
+    if (qp < -6 * (c->bd - 8) || qp > 51 || !c->d_src_c || c->nrefs < 1) return IRONAV_INVALID_ARGUMENT;
+    for (int i = 0; i < c->nrefs; i++)
+        if (!c->ref_c_ok[c->slot_of[i]]) return IRONAV_INVALID_ARGUMENT;  // a reference without chroma
+    CodeParams p;
+    memset(&p, 0, sizeof(p));
+    fill_params(c, p.A);
+    for (int i = 0; i < c->nrefs; i++) {
+        p.A.planes[i] = c->d_planes[c->slot_of[i]];
+        p.ref_c[i] = c->d_ref_c[c->slot_of[i]];
+    }
+    p.src_c = c->d_src_c;
+    p.cw = c->mb_w * 8;
+    p.ch = c->mb_h * 8;
+    p.decs = d_decs;
+    p.codes = d_codes;
+    p.rec[0] = static_cast<uint8_t*>(y);
+    p.rec[1] = static_cast<uint8_t*>(cb);
+    p.rec[2] = static_cast<uint8_t*>(cr);
+    p.ys = ys;
+    p.cs = cs;
+    p.qp = qp;
+    p.bd = c->bd;
+    p.nrefs = c->nrefs;
+    p.err = c->d_counters + 1;
+    CK(cudaMemsetAsync(c->d_counters, 0, 2 * sizeof(unsigned), c->stream));
+    const int blocks = std::min((c->nmb + 3) / 4, c->nsm * 8);
+    if (c->bd > 8) code_inter_kernel<uint16_t><<<blocks, 128, 0, c->stream>>>(p);
+    else code_inter_kernel<uint8_t><<<blocks, 128, 0, c->stream>>>(p);
+    return cuda_status(cudaGetLastError());
+}
+
+int ironav_code_inter_picture_device(ironav_ctx* c, int qp, const ironav_interdec* d_decs, ironav_intercode* d_codes, void* y, int ys, void* cb,
+                                     void* cr, int cs) {
+    if (!c || !d_decs || !d_codes || !y || !cb || !cr || ys < c->pw || cs < c->pw / 2) return IRONAV_INVALID_ARGUMENT;
+    // the same alignment as the deblocking filter's device form
+    const uintptr_t a = reinterpret_cast<uintptr_t>(y) | reinterpret_cast<uintptr_t>(cb) | reinterpret_cast<uintptr_t>(cr);
+    if ((a & 15) || ((size_t)ys * sample_bytes(c)) % 16 || cs % 8) return IRONAV_INVALID_ARGUMENT;
+    return launch_code_inter(c, qp, d_decs, d_codes, y, ys, cb, cr, cs);
+}
+
+int ironav_code_inter_picture(ironav_ctx* c, int qp, const ironav_interdec* decs, ironav_intercode* codes, void* y, int ys, void* cb, void* cr,
+                              int cs) {
+    if (!c || !decs || !codes || !y || !cb || !cr || ys < c->pw || cs < c->pw / 2) return IRONAV_INVALID_ARGUMENT;
+    const size_t B = (size_t)sample_bytes(c), pw = (size_t)c->pw, ph = (size_t)c->ph;
+    if (!c->d_decs) CK(cudaMalloc(&c->d_decs, sizeof(ironav_interdec) * c->nmb));
+    if (!c->d_codes) CK(cudaMalloc(&c->d_codes, sizeof(ironav_intercode) * c->nmb));
+    if (!c->d_rec) CK(cudaMalloc(&c->d_rec, (pw * ph + 2 * (pw / 2) * (ph / 2)) * B));
+    uint8_t* dy = c->d_rec;
+    uint8_t* dcb = dy + pw * ph * B;
+    uint8_t* dcr = dcb + (pw / 2) * (ph / 2) * B;
+    CK(cudaMemcpyAsync(c->d_decs, decs, sizeof(ironav_interdec) * c->nmb, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpy2DAsync(dy, pw * B, y, (size_t)ys * B, pw * B, ph, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpy2DAsync(dcb, pw / 2 * B, cb, (size_t)cs * B, pw / 2 * B, ph / 2, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpy2DAsync(dcr, pw / 2 * B, cr, (size_t)cs * B, pw / 2 * B, ph / 2, cudaMemcpyHostToDevice, c->stream));
+    int s = launch_code_inter(c, qp, c->d_decs, c->d_codes, dy, (int)pw, dcb, dcr, (int)(pw / 2));
+    if (s != IRONAV_OK) return s;
+    CK(cudaMemcpyAsync(codes, c->d_codes, sizeof(ironav_intercode) * c->nmb, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpy2DAsync(y, (size_t)ys * B, dy, pw * B, pw * B, ph, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpy2DAsync(cb, (size_t)cs * B, dcb, pw / 2 * B, pw / 2 * B, ph / 2, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpy2DAsync(cr, (size_t)cs * B, dcr, pw / 2 * B, pw / 2 * B, ph / 2, cudaMemcpyDeviceToHost, c->stream));
     return check_device_error(c);
 }
 

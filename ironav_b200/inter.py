@@ -87,6 +87,13 @@ BRESULT_DTYPE = np.dtype(
 )
 assert MBSTATE_DTYPE.itemsize == 72 and MBRESULT_DTYPE.itemsize == 104
 assert MBSTATE_B_DTYPE.itemsize == 140 and BRESULT_DTYPE.itemsize == 200
+# Inter residual coding: a macroblock's decision (ironav_interdec) and its coded residual (ironav_intercode).
+INTERDEC_DTYPE = np.dtype([("mode", "u1"), ("part", "u1"), ("sub", "u1", (4,)), ("refs", "u1", (4,)), ("t8", "u1"),
+                           ("pad", "u1", (3,)), ("mvs", "<i2", (16, 2))])
+INTERCODE_DTYPE = np.dtype([("luma", "<i2", (16, 16)), ("luma8", "<i2", (4, 64)), ("cdc", "<i2", (2, 4)),
+                            ("cac", "<i2", (2, 4, 16)), ("nnz", "u1", (16,)), ("cnnz", "u1", (2, 4)), ("cbp", "u1"),
+                            ("t8x8", "u1"), ("pad", "u1", (2,))])
+assert INTERDEC_DTYPE.itemsize == 78 and INTERCODE_DTYPE.itemsize == 1324
 assert DBK_MB_DTYPE.itemsize == 192 and DBK_SLICE_DTYPE.itemsize == 20
 
 RESULT_INTER = 1
@@ -115,6 +122,7 @@ EXPORTS = (
     "ironav_batch_sync", "ironav_scene_change", "ironav_scene_change_device", "ironav_analyse_auto_noalloc",
     "ironav_deblock_picture", "ironav_deblock_picture_device",
     "ironav_begin_b_picture", "ironav_begin_b_picture_device", "ironav_analyse_b_replay", "ironav_analyse_b_replay_device",
+    "ironav_set_source_chroma", "ironav_push_reference_chroma", "ironav_code_inter_picture", "ironav_code_inter_picture_device",
 )
 
 SCENE_CUT = 0.8  # codec/change.rs:6
@@ -169,6 +177,11 @@ def _declare(lib: ctypes.CDLL) -> ctypes.CDLL:
         lib.ironav_begin_b_picture_device.argtypes = [_VP, _I, _I, _I, _I, _VP, _I, _I, _I]
         lib.ironav_analyse_b_replay.argtypes = [_VP, _VP, _VP]
         lib.ironav_analyse_b_replay_device.argtypes = [_VP, _VP, _VP]
+    if hasattr(lib, "ironav_code_inter_picture"):
+        lib.ironav_set_source_chroma.argtypes = [_VP, _VP, _VP, _I]
+        lib.ironav_push_reference_chroma.argtypes = [_VP, _VP, _VP, _I, _I, _I]
+        lib.ironav_code_inter_picture.argtypes = [_VP, _I, _VP, _VP, _VP, _I, _VP, _VP, _I]
+        lib.ironav_code_inter_picture_device.argtypes = [_VP, _I, _VP, _VP, _VP, _I, _VP, _VP, _I]
     if hasattr(lib, "ironav_deblock_picture"):
         lib.ironav_deblock_picture.argtypes = [_VP, _VP, _I, _VP, _VP, _I, _VP, _VP, _I]
         lib.ironav_deblock_picture_device.argtypes = [_VP, _VP, _I, _VP, _VP, _I, _VP, _VP, _I]
@@ -392,6 +405,28 @@ class InterStage:
         self._check(self.lib.ironav_analyse_b_replay(self.ctx, _ptr(states), _ptr(out)), "ironav_analyse_b_replay")
         return out
 
+    # -- inter residual coding and reconstruction (enc/frame.rs:1202-1305, 1856-1915) -------------------------
+
+    def set_source_chroma(self, cb: np.ndarray, cr: np.ndarray) -> None:
+        cb, cr = self._luma(cb), self._luma(cr)
+        self._check(self.lib.ironav_set_source_chroma(self.ctx, _ptr(cb), _ptr(cr), cb.shape[1]), "ironav_set_source_chroma")
+
+    def push_reference_chroma(self, cb: np.ndarray, cr: np.ndarray) -> None:
+        cb, cr = self._luma(cb), self._luma(cr)
+        h, w = cb.shape
+        self._check(self.lib.ironav_push_reference_chroma(self.ctx, _ptr(cb), _ptr(cr), w, w, h), "ironav_push_reference_chroma")
+
+    def code_inter(self, qp: int, decs: np.ndarray, rec: tuple[np.ndarray, np.ndarray, np.ndarray]):
+        """Codes the inter macroblocks of decs (INTERDEC_DTYPE) into copies of the reconstruction planes rec
+        (luma 16*mb_w x 16*mb_h, chroma 8*mb_w x 8*mb_h); returns (codes, (y, cb, cr))."""
+        decs = np.ascontiguousarray(decs, dtype=INTERDEC_DTYPE)
+        assert decs.shape == (self.nmb,)
+        y, cb, cr = (self._luma(a).copy() for a in rec)
+        codes = np.zeros(self.nmb, dtype=INTERCODE_DTYPE)
+        self._check(self.lib.ironav_code_inter_picture(self.ctx, qp, _ptr(decs), _ptr(codes), _ptr(y), y.shape[1], _ptr(cb),
+                                                       _ptr(cr), cb.shape[1]), "ironav_code_inter_picture")
+        return codes, (y, cb, cr)
+
     # -- deblocking of the reconstruction (h264/deblock.rs) ------------------------------------------------
 
     def deblock(self, y: np.ndarray, cb: np.ndarray, cr: np.ndarray, mbs: np.ndarray,
@@ -476,6 +511,22 @@ _SUB = [[(0, 0, 2, 2)], [(0, 0, 2, 1), (0, 1, 2, 1)], [(0, 0, 1, 2), (1, 0, 1, 2
         [(0, 0, 1, 1), (1, 0, 1, 1), (0, 1, 1, 1), (1, 1, 1, 1)]]
 _PARTS = [[(0, 0, 4, 4)], [(0, 0, 4, 2), (0, 2, 4, 2)], [(0, 0, 2, 4), (2, 0, 2, 4)],
           [(0, 0, 2, 2), (2, 0, 2, 2), (0, 2, 2, 2), (2, 2, 2, 2)]]
+
+
+def inter_decisions(res: np.ndarray, t8: bool = False) -> np.ndarray:
+    """The inter coding decision of each macroblock from P analysis results (auto mode): P_Skip where the
+    policy skipped (its vector), else the best_inter partitioning with its vectors and reference."""
+    d = np.zeros(len(res), dtype=INTERDEC_DTYPE)
+    skip = (res["flags"] & RESULT_SKIP) != 0
+    inter = (res["flags"] & RESULT_INTER) != 0
+    d["mode"] = np.where(skip, 1, np.where(inter, 2, 0))
+    d["part"] = np.where(skip, 0, res["part"])
+    d["sub"] = np.where(skip[:, None], 0, res["sub"])
+    d["refs"] = np.where(skip[:, None], 0, res["refs"])
+    d["t8"] = 1 if t8 else 0
+    d["mvs"] = res["mvs"]
+    d["mvs"][skip, 0] = res["skip_mv"][skip]
+    return d
 
 
 def b_decision_states(res: np.ndarray) -> np.ndarray:

@@ -90,6 +90,19 @@ class Sequence:
         low = rng.integers(0, 4, size=(self.height, self.width), dtype=np.uint16)
         return (self.frame(t).astype(np.uint16) << 2) | low
 
+    def chroma(self, t: int, bd: int = 8) -> tuple[np.ndarray, np.ndarray]:
+        """4:2:0 chroma for frame t (the sequences are generated as luma; chroma is derived from it so that it
+        moves with the picture): Cb from the 2x2 luma means compressed around 128, Cr inverted; 10-bit
+        from the 10-bit frame."""
+        y = (self.frame10(t) if bd > 8 else self.frame(t)).astype(np.int32)
+        h2, w2 = self.height // 2, self.width // 2
+        m = (y[0:2 * h2:2, 0:2 * w2:2] + y[1:2 * h2:2, 0:2 * w2:2] + y[0:2 * h2:2, 1:2 * w2:2] + y[1:2 * h2:2, 1:2 * w2:2] + 2) >> 2
+        half = 1 << (bd - 1)
+        cb = half + ((m - half) * 3 >> 2)
+        cr = half - ((m - half) >> 1)
+        dt = np.uint8 if bd == 8 else np.uint16
+        return cb.astype(dt), cr.astype(dt)
+
     def pan(self, t: int) -> tuple[int, int]:
         qx, qy = ctypes.c_int(), ctypes.c_int()
         _lib().ironav_synth_pan(self._h, t, ctypes.byref(qx), ctypes.byref(qy))

@@ -302,7 +302,8 @@ typedef struct colmv { int16_t mv[2]; uint8_t valid; } colmv;
 
 typedef struct refpic {
     halfpel hp;
-    colmv* col; /* per macroblock: mvs[5] when the macroblock was inter (col_mv, enc/frame.rs:944-947) */
+    colmv* col;         /* per macroblock: mvs[5] when the macroblock was inter (col_mv, enc/frame.rs:944-947) */
+    uint16_t* chroma[2]; /* Cb, Cr of the reconstruction (8*mb_w x 8*mb_h), when attached */
 } refpic;
 
 struct ironav_ctx {
@@ -319,6 +320,7 @@ struct ironav_ctx {
     int b_ref[2];           /* held references used as list 0 and list 1 */
     ironav_mbstate* b_col;  /* the list-1 picture's decisions, or NULL */
     int b_tb, b_td, b_set;
+    uint16_t* src_c[2]; /* the source's chroma, padded to 8*mb_w x 8*mb_h */
 };
 
 typedef struct fc {
@@ -807,6 +809,9 @@ static void refpic_free(refpic* r) {
     halfpel_free(&r->hp);
     free(r->col);
     r->col = NULL;
+    free(r->chroma[0]);
+    free(r->chroma[1]);
+    r->chroma[0] = r->chroma[1] = NULL;
 }
 
 int ironav_ctx_create(ironav_ctx** out, int width, int height, int bd, int max_refs, int nslices, const int* band_rows) {
@@ -850,6 +855,8 @@ int ironav_ctx_destroy(ironav_ctx* c) {
     free(c->src);
     free(c->band_start);
     free(c->b_col);
+    free(c->src_c[0]);
+    free(c->src_c[1]);
     if (c->inloop) free(((ironav_mbstate**)c->inloop)[0]);
     free(c->inloop);
     free(c);
@@ -1699,6 +1706,452 @@ int ironav_analyse_b_replay(ironav_ctx* c, const ironav_mbstate_b* states, irona
 
 int ironav_analyse_b_replay_device(ironav_ctx* c, const ironav_mbstate_b* s, ironav_bresult* o) {
     (void)c; (void)s; (void)o;
+    return IRONAV_HARDWARE_UNAVAILABLE;
+}
+
+/* ---------------------------------------------------------------------------------------------------
+ * Inter residual coding and reconstruction: code_inter, code_inter_residual, code_luma8, code_chroma
+ * (enc/frame.rs:1202-1305, 1856-1915) with quant_block (1025-1046), quant8 (56-72), fdct4 / fdct8
+ * (46-54, 79-98), decimate_score(8) (2369-2440), chroma_mc (h264/inter.rs:549-568) and idct4_add /
+ * idct8_add (h264/idct.rs:8-76).
+ * ------------------------------------------------------------------------------------------------- */
+
+/* quantisation multipliers / dequantisation scales by QP % 6 and class (enc/frame.rs:20-21), the 8x8
+ * transform's (MF8 enc/frame.rs:33-40; DEQUANT8_COEFF_INIT h264/tables.rs:4278), the scans (ZIGZAG4
+ * h264/ps.rs:12, ZIGZAG_DIRECT h264/tables.rs:4291) */
+static const int Q_MF[6][3] = {{13107, 5243, 8066}, {11916, 4660, 7490}, {10082, 4194, 6554},
+                               {9362, 3647, 5825},  {8192, 3355, 5243}, {7282, 2893, 4559}};
+static const int Q_V[6][3] = {{10, 16, 13}, {11, 18, 14}, {13, 20, 16}, {14, 23, 18}, {16, 25, 20}, {18, 29, 23}};
+static const int Q_MF8[6][6] = {{13107, 11428, 20972, 12222, 16777, 15481}, {11916, 10826, 19174, 11058, 14980, 14290},
+                                {10082, 8943, 15978, 9675, 12710, 11985},   {9362, 8228, 14913, 8931, 11984, 11259},
+                                {8192, 7346, 13159, 7740, 10486, 9777},     {7282, 6428, 11570, 6830, 9118, 8640}};
+static const int Q_DQ8[6][6] = {{20, 18, 32, 19, 25, 24}, {22, 19, 35, 21, 28, 26}, {26, 23, 42, 24, 33, 31},
+                                {28, 25, 45, 26, 35, 33}, {32, 28, 51, 30, 40, 38}, {36, 32, 58, 34, 46, 43}};
+static const int ZZ4[16] = {0, 1, 4, 8, 5, 2, 3, 6, 9, 12, 13, 10, 7, 11, 14, 15};
+static const int ZZ8[64] = {0,  1,  8,  16, 9,  2,  3,  10, 17, 24, 32, 25, 18, 11, 4,  5,  12, 19, 26, 33, 40, 48,
+                            41, 34, 27, 20, 13, 6,  7,  14, 21, 28, 35, 42, 49, 56, 57, 50, 43, 36, 29, 22, 15, 23,
+                            30, 37, 44, 51, 58, 59, 52, 45, 38, 31, 39, 46, 53, 60, 61, 54, 47, 55, 62, 63};
+
+static int q_class(int i) { return ((i & 1) == 0 && ((i >> 2) & 1) == 0) ? 0 : (((i & 1) == 1 && ((i >> 2) & 1) == 1) ? 1 : 2); }
+static int q_class8(int p) {
+    int i = p / 8, j = p % 8;
+    if (i % 4 == 0 && j % 4 == 0) return 0;
+    if (i % 2 == 1 && j % 2 == 1) return 1;
+    if (i % 4 == 2 && j % 4 == 2) return 2;
+    if ((i % 4 == 0 && j % 2 == 1) || (i % 2 == 1 && j % 4 == 0)) return 3;
+    if ((i % 4 == 0 && j % 4 == 2) || (i % 4 == 2 && j % 4 == 0)) return 4;
+    return 5;
+}
+
+static void q_fdct4(const int d[16], int o[16]) {
+    int t[16];
+    for (int r = 0; r < 4; r++) {
+        const int* a = d + r * 4;
+        int s03 = a[0] + a[3], d03 = a[0] - a[3], s12 = a[1] + a[2], d12 = a[1] - a[2];
+        t[r * 4] = s03 + s12;
+        t[r * 4 + 1] = 2 * d03 + d12;
+        t[r * 4 + 2] = s03 - s12;
+        t[r * 4 + 3] = d03 - 2 * d12;
+    }
+    for (int c = 0; c < 4; c++) {
+        int s03 = t[c] + t[12 + c], d03 = t[c] - t[12 + c], s12 = t[4 + c] + t[8 + c], d12 = t[4 + c] - t[8 + c];
+        o[c] = s03 + s12;
+        o[4 + c] = 2 * d03 + d12;
+        o[8 + c] = s03 - s12;
+        o[12 + c] = d03 - 2 * d12;
+    }
+}
+
+static void q_fdct8_1d(const int d[8], int o[8]) {
+    int s07 = d[0] + d[7], s16 = d[1] + d[6], s25 = d[2] + d[5], s34 = d[3] + d[4];
+    int a0 = s07 + s34, a1 = s16 + s25, a2 = s07 - s34, a3 = s16 - s25;
+    int d07 = d[0] - d[7], d16 = d[1] - d[6], d25 = d[2] - d[5], d34 = d[3] - d[4];
+    int a4 = d16 + d25 + (d07 + (d07 >> 1));
+    int a5 = d07 - d34 - (d25 + (d25 >> 1));
+    int a6 = d07 + d34 - (d16 + (d16 >> 1));
+    int a7 = d16 - d25 + (d34 + (d34 >> 1));
+    o[0] = a0 + a1;
+    o[1] = a4 + (a7 >> 2);
+    o[2] = a2 + (a3 >> 1);
+    o[3] = a5 + (a6 >> 2);
+    o[4] = a0 - a1;
+    o[5] = a6 - (a5 >> 2);
+    o[6] = (a2 >> 1) - a3;
+    o[7] = (a4 >> 2) - a7;
+}
+
+static void q_fdct8(const int d[64], int o[64]) {
+    int t[64], v[8], w[8];
+    for (int r = 0; r < 8; r++) q_fdct8_1d(d + r * 8, t + r * 8);
+    for (int c = 0; c < 8; c++) {
+        for (int r = 0; r < 8; r++) v[r] = t[r * 8 + c];
+        q_fdct8_1d(v, w);
+        for (int r = 0; r < 8; r++) o[r * 8 + c] = w[r];
+    }
+}
+
+/* quant, enc/frame.rs:134-141 */
+static int q_quant(int c, int mf, int f, int qbits) {
+    int a = (int)(((int64_t)(c < 0 ? -(int64_t)c : c) * mf + f) >> qbits);
+    return c < 0 ? -a : a;
+}
+
+/* quant_block, enc/frame.rs:1025-1046 */
+static void q_block(const int src[16], const int pred[16], int qp, int intra, int skip_dc, int lv[16], int co[16], int* dc) {
+    int d[16], c[16];
+    for (int k = 0; k < 16; k++) d[k] = src[k] - pred[k];
+    q_fdct4(d, c);
+    int qbits = 15 + qp / 6, f = (1 << qbits) / (intra ? 3 : 6), m = qp % 6;
+    memset(lv, 0, sizeof(int) * 16);
+    memset(co, 0, sizeof(int) * 16);
+    for (int k = 0; k < 16; k++) {
+        int p = ZZ4[k];
+        if (skip_dc && p == 0) continue;
+        int l = q_quant(c[p], Q_MF[m][q_class(p)], f, qbits);
+        lv[k] = l;
+        co[p] = (l * Q_V[m][q_class(p)]) << (qp / 6);
+    }
+    *dc = c[0];
+}
+
+/* quant8, enc/frame.rs:56-72 */
+static void q_block8(const int src[64], const int pred[64], int qp, int intra, int lv[64], int co[64]) {
+    int d[64], c[64];
+    for (int k = 0; k < 64; k++) d[k] = src[k] - pred[k];
+    q_fdct8(d, c);
+    int m = qp % 6, qbits = 16 + qp / 6, f = (1 << qbits) / (intra ? 3 : 6);
+    memset(lv, 0, sizeof(int) * 64);
+    memset(co, 0, sizeof(int) * 64);
+    for (int k = 0; k < 64; k++) {
+        int p = ZZ8[k];
+        int l = q_quant(c[p], Q_MF8[m][q_class8(p)], f, qbits);
+        lv[k] = l;
+        if (l != 0) {
+            int v = l * 16 * Q_DQ8[m][q_class8(p)];
+            co[p] = qp >= 36 ? v << (qp / 6 - 6) : (v + (1 << (5 - qp / 6))) >> (6 - qp / 6);
+        }
+    }
+}
+
+/* idct4_add / idct8_add, h264/idct.rs:8-76 (wrapping 32-bit arithmetic) */
+static void q_idct4_add(const int c[16], uint16_t* dst, int stride, int maxv) {
+    int32_t t[16];
+    for (int i = 0; i < 4; i++) {
+        const int* d = c + i * 4;
+        int32_t e0 = (int32_t)((uint32_t)d[0] + (uint32_t)d[2]), e1 = (int32_t)((uint32_t)d[0] - (uint32_t)d[2]);
+        int32_t e2 = (int32_t)((uint32_t)(d[1] >> 1) - (uint32_t)d[3]), e3 = (int32_t)((uint32_t)d[1] + (uint32_t)(d[3] >> 1));
+        t[i * 4] = (int32_t)((uint32_t)e0 + (uint32_t)e3);
+        t[i * 4 + 1] = (int32_t)((uint32_t)e1 + (uint32_t)e2);
+        t[i * 4 + 2] = (int32_t)((uint32_t)e1 - (uint32_t)e2);
+        t[i * 4 + 3] = (int32_t)((uint32_t)e0 - (uint32_t)e3);
+    }
+    for (int j = 0; j < 4; j++) {
+        int32_t g0 = (int32_t)((uint32_t)t[j] + (uint32_t)t[8 + j]), g1 = (int32_t)((uint32_t)t[j] - (uint32_t)t[8 + j]);
+        int32_t g2 = (int32_t)((uint32_t)(t[4 + j] >> 1) - (uint32_t)t[12 + j]), g3 = (int32_t)((uint32_t)t[4 + j] + (uint32_t)(t[12 + j] >> 1));
+        int32_t h[4] = {(int32_t)((uint32_t)g0 + (uint32_t)g3), (int32_t)((uint32_t)g1 + (uint32_t)g2), (int32_t)((uint32_t)g1 - (uint32_t)g2),
+                        (int32_t)((uint32_t)g0 - (uint32_t)g3)};
+        for (int i = 0; i < 4; i++) {
+            uint16_t* p = dst + (size_t)i * stride + j;
+            *p = (uint16_t)clampi(*p + ((int32_t)((uint32_t)h[i] + 32u) >> 6), 0, maxv);
+        }
+    }
+}
+
+static void q_row8(const int32_t d[8], int32_t o[8]) {
+#define W(x) ((uint32_t)(x))
+    int32_t a0 = (int32_t)(W(d[0]) + W(d[4])), a4 = (int32_t)(W(d[0]) - W(d[4]));
+    int32_t a2 = (int32_t)(W(d[2] >> 1) - W(d[6])), a6 = (int32_t)(W(d[2]) + W(d[6] >> 1));
+    int32_t b0 = (int32_t)(W(a0) + W(a6)), b2 = (int32_t)(W(a4) + W(a2)), b4 = (int32_t)(W(a4) - W(a2)), b6 = (int32_t)(W(a0) - W(a6));
+    int32_t a1 = (int32_t)(W(d[5]) - W(d[3]) - W(d[7]) - W(d[7] >> 1));
+    int32_t a3 = (int32_t)(W(d[1]) + W(d[7]) - W(d[3]) - W(d[3] >> 1));
+    int32_t a5 = (int32_t)(W(d[7]) - W(d[1]) + W(d[5]) + W(d[5] >> 1));
+    int32_t a7 = (int32_t)(W(d[3]) + W(d[5]) + W(d[1]) + W(d[1] >> 1));
+    int32_t b1 = (int32_t)(W(a1) + W(a7 >> 2)), b7 = (int32_t)(W(a7) - W(a1 >> 2));
+    int32_t b3 = (int32_t)(W(a3) + W(a5 >> 2)), b5 = (int32_t)(W(a3 >> 2) - W(a5));
+    o[0] = (int32_t)(W(b0) + W(b7));
+    o[1] = (int32_t)(W(b2) + W(b5));
+    o[2] = (int32_t)(W(b4) + W(b3));
+    o[3] = (int32_t)(W(b6) + W(b1));
+    o[4] = (int32_t)(W(b6) - W(b1));
+    o[5] = (int32_t)(W(b4) - W(b3));
+    o[6] = (int32_t)(W(b2) - W(b5));
+    o[7] = (int32_t)(W(b0) - W(b7));
+#undef W
+}
+
+static void q_idct8_add(const int c[64], uint16_t* dst, int stride, int maxv) {
+    int32_t t[64], d[8], h[8];
+    for (int i = 0; i < 8; i++) q_row8(c + i * 8, t + i * 8);
+    for (int j = 0; j < 8; j++) {
+        for (int i = 0; i < 8; i++) d[i] = t[i * 8 + j];
+        q_row8(d, h);
+        for (int i = 0; i < 8; i++) {
+            uint16_t* p = dst + (size_t)i * stride + j;
+            *p = (uint16_t)clampi(*p + ((int32_t)((uint32_t)h[i] + 32u) >> 6), 0, maxv);
+        }
+    }
+}
+
+/* decimate_score / decimate_score8, enc/frame.rs:2369-2440 */
+static int q_decimate(const int* lv, int n) {
+    static const int RUN4[16] = {3, 2, 2, 1, 1, 1, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    static const int RUN8[25] = {3, 3, 3, 3, 2, 2, 2, 2, 2, 2, 2, 2, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 0};
+    int score = 0, i = n - 1;
+    while (i >= 0 && lv[i] == 0) i--;
+    while (i >= 0) {
+        if (abs(lv[i]) > 1) return 9;
+        i--;
+        int run = 0;
+        while (i >= 0 && lv[i] == 0) {
+            i--;
+            run++;
+        }
+        score += n == 16 ? RUN4[mini(run, 15)] : RUN8[mini(run, 24)];
+    }
+    return score;
+}
+
+/* chroma_mc, h264/inter.rs:549-568: eighth-sample bilinear, coordinates clamped to the plane */
+static void q_chroma_mc(const uint16_t* refp, int pw, int ph, int x, int y, int mx, int my, int w, int h, uint16_t* out) {
+    int fx = mx & 7, fy = my & 7, x0 = x + (mx >> 3), y0 = y + (my >> 3);
+    int wa = (8 - fx) * (8 - fy), wb = fx * (8 - fy), wc = (8 - fx) * fy, wd = fx * fy;
+#define AT(c, r) ((int)refp[(size_t)clampi(y0 + (r), 0, ph - 1) * pw + clampi(x0 + (c), 0, pw - 1)])
+    for (int r = 0; r < h; r++)
+        for (int c = 0; c < w; c++) out[r * w + c] = (uint16_t)((wa * AT(c, r) + wb * AT(c + 1, r) + wc * AT(c, r + 1) + wd * AT(c + 1, r + 1) + 32) >> 6);
+#undef AT
+}
+
+/* inter_pred, enc/frame.rs:1783-1804 */
+static void q_inter_pred(const struct ironav_ctx* c, int mbx, int mby, const ironav_interdec* d, uint16_t pred[256], uint16_t cpred[2][64]) {
+    rect4 rs[16];
+    int n = rects(d->part, d->sub, rs);
+    int cw = c->mb_w * 8, ch = c->mb_h * 8;
+    uint16_t tmp[256];
+    for (int k = 0; k < n; k++) {
+        rect4 r = rs[k];
+        int ri = d->part == 3 ? (r.y / 2) * 2 + r.x / 2 : k;
+        const refpic* rp = &c->refs[d->refs[ri]];
+        int mx = d->mvs[k][0], my = d->mvs[k][1];
+        halfpel_predict(&rp->hp, mbx * 16 + r.x * 4, mby * 16 + r.y * 4, mx, my, r.w * 4, r.h * 4, tmp);
+        for (int row = 0; row < r.h * 4; row++)
+            for (int col = 0; col < r.w * 4; col++) pred[(r.y * 4 + row) * 16 + r.x * 4 + col] = tmp[row * r.w * 4 + col];
+        for (int cc = 0; cc < 2; cc++) {
+            q_chroma_mc(rp->chroma[cc], cw, ch, mbx * 8 + r.x * 2, mby * 8 + r.y * 2, mx, my, r.w * 2, r.h * 2, tmp);
+            for (int row = 0; row < r.h * 2; row++)
+                for (int col = 0; col < r.w * 2; col++) cpred[cc][(r.y * 2 + row) * 8 + r.x * 2 + col] = tmp[row * r.w * 2 + col];
+        }
+    }
+}
+
+/* code_chroma (inter), enc/frame.rs:1856-1915 */
+static void q_code_chroma(const struct ironav_ctx* c, int mbx, int mby, int qp_y, const uint16_t cpred[2][64], ironav_intercode* out,
+                          uint16_t* rec_c[2], int cs) {
+    int x0 = mbx * 8, y0 = mby * 8, scs = c->mb_w * 8;
+    int qoff = 6 * (c->bd - 8), maxv = (1 << c->bd) - 1;
+    int qp = dbk_chroma_qp(qp_y, 0, c->bd) + qoff, m = qp % 6;
+    int lv[2][4][16], cos[2][4][16], cdc[2][4];
+    int any_dc = 0, any_ac = 0;
+    for (int cc = 0; cc < 2; cc++) {
+        int dcs[4];
+        for (int blk = 0; blk < 4; blk++) {
+            int bx = blk & 1, by = blk >> 1, s[16], pr[16];
+            for (int r = 0; r < 4; r++)
+                for (int k = 0; k < 4; k++) {
+                    s[r * 4 + k] = c->src_c[cc][(size_t)(y0 + by * 4 + r) * scs + x0 + bx * 4 + k];
+                    pr[r * 4 + k] = cpred[cc][(by * 4 + r) * 8 + bx * 4 + k];
+                }
+            q_block(s, pr, qp, 0, 1, lv[cc][blk], cos[cc][blk], &dcs[blk]);
+            for (int k = 0; k < 16; k++)
+                if (lv[cc][blk][k]) any_ac = 1;
+        }
+        int f[4] = {dcs[0] + dcs[1] + dcs[2] + dcs[3], dcs[0] - dcs[1] + dcs[2] - dcs[3], dcs[0] + dcs[1] - dcs[2] - dcs[3],
+                    dcs[0] - dcs[1] - dcs[2] + dcs[3]};
+        int qbits = 16 + qp / 6, fr = (1 << qbits) / 6;
+        for (int k = 0; k < 4; k++) {
+            cdc[cc][k] = q_quant(f[k], Q_MF[m][0], fr, qbits);
+            if (cdc[cc][k]) any_dc = 1;
+        }
+    }
+    /* a lone small AC level is not worth signalling chroma AC for */
+    int ac_score = 0;
+    for (int cc = 0; cc < 2; cc++)
+        for (int blk = 0; blk < 4; blk++) ac_score += q_decimate(lv[cc][blk], 16);
+    if (ac_score < 7) any_ac = 0;
+    if (!any_ac) {
+        memset(lv, 0, sizeof(lv));
+        memset(cos, 0, sizeof(cos));
+    }
+    int cbpc = any_ac ? 2 : (any_dc ? 1 : 0);
+    out->cbp |= (uint8_t)(cbpc << 4);
+    int lsd = 16 * Q_V[m][0];
+    for (int cc = 0; cc < 2; cc++) {
+        const int* l = cdc[cc];
+        int f[4] = {l[0] + l[1] + l[2] + l[3], l[0] - l[1] + l[2] - l[3], l[0] + l[1] - l[2] - l[3], l[0] - l[1] - l[2] + l[3]};
+        for (int y = 0; y < 8; y++)
+            for (int x = 0; x < 8; x++) rec_c[cc][(size_t)(y0 + y) * cs + x0 + x] = cpred[cc][y * 8 + x];
+        for (int blk = 0; blk < 4; blk++) {
+            int co[16];
+            memcpy(co, cos[cc][blk], sizeof(co));
+            co[0] = cbpc > 0 ? ((f[blk] * lsd) << (qp / 6)) >> 5 : 0;
+            int nz = 0, any = 0;
+            for (int k = 0; k < 16; k++) {
+                out->cac[cc][blk][k] = (int16_t)lv[cc][blk][k];
+                if (lv[cc][blk][k]) nz++;
+                if (co[k]) any = 1;
+            }
+            out->cnnz[cc][blk] = (uint8_t)nz;
+            if (any) q_idct4_add(co, rec_c[cc] + (size_t)(y0 + (blk >> 1) * 4) * cs + x0 + (blk & 1) * 4, cs, maxv);
+        }
+        for (int k = 0; k < 4; k++) out->cdc[cc][k] = (int16_t)cdc[cc][k];
+    }
+}
+
+/* code_inter_residual / code_luma8, enc/frame.rs:1217-1305, of one macroblock into the reconstruction */
+static void q_code_inter(const struct ironav_ctx* c, int mbx, int mby, int qp_y, const ironav_interdec* d, ironav_intercode* out,
+                         uint16_t* rec[3], int ys, int cs) {
+    memset(out, 0, sizeof(*out));
+    uint16_t pred[256], cpred[2][64];
+    q_inter_pred(c, mbx, mby, d, pred, cpred);
+    int x0 = mbx * 16, y0 = mby * 16, sls = c->pw, maxv = (1 << c->bd) - 1;
+    int qp = qp_y + 6 * (c->bd - 8);
+    if (d->mode == 1) {
+        /* P_Skip: the prediction is the reconstruction */
+        for (int y = 0; y < 16; y++)
+            for (int x = 0; x < 16; x++) rec[0][(size_t)(y0 + y) * ys + x0 + x] = pred[y * 16 + x];
+        for (int cc = 0; cc < 2; cc++)
+            for (int y = 0; y < 8; y++)
+                for (int x = 0; x < 8; x++) rec[1 + cc][(size_t)(mby * 8 + y) * cs + mbx * 8 + x] = cpred[cc][y * 8 + x];
+        return;
+    }
+    for (int y = 0; y < 16; y++)
+        for (int x = 0; x < 16; x++) rec[0][(size_t)(y0 + y) * ys + x0 + x] = pred[y * 16 + x];
+    if (d->t8) {
+        int lv[4][64], cos[4][64], score[4];
+        for (int i8 = 0; i8 < 4; i8++) {
+            int bx = (i8 & 1) * 8, by = (i8 >> 1) * 8, s[64], pr[64];
+            for (int k = 0; k < 64; k++) {
+                s[k] = c->src[(size_t)(y0 + by + k / 8) * sls + x0 + bx + k % 8];
+                pr[k] = pred[(by + k / 8) * 16 + bx + k % 8];
+            }
+            q_block8(s, pr, qp, 0, lv[i8], cos[i8]);
+            score[i8] = q_decimate(lv[i8], 64);
+        }
+        int total = score[0] + score[1] + score[2] + score[3];
+        for (int i8 = 0; i8 < 4; i8++) {
+            if (score[i8] < 4 || total < 6) continue; /* levels dropped (out stays zero) */
+            int n = 0;
+            for (int k = 0; k < 64; k++) {
+                out->luma8[i8][k] = (int16_t)lv[i8][k];
+                if (lv[i8][k]) n++;
+            }
+            if (n > 0) {
+                q_idct8_add(cos[i8], rec[0] + (size_t)(y0 + (i8 >> 1) * 8) * ys + x0 + (i8 & 1) * 8, ys, maxv);
+                out->cbp |= (uint8_t)(1 << i8);
+            }
+            for (int j = 0; j < 4; j++) out->nnz[((i8 >> 1) * 2 + (j >> 1)) * 4 + (i8 & 1) * 2 + (j & 1)] = (uint8_t)n;
+        }
+        out->t8x8 = (out->cbp & 15) != 0;
+    } else {
+        int lv[16][16], cos[16][16], score[4] = {0, 0, 0, 0};
+        for (int b = 0; b < 16; b++) {
+            int bx = b % 4, by = b / 4, s[16], pr[16], dc;
+            for (int r = 0; r < 4; r++)
+                for (int k = 0; k < 4; k++) {
+                    s[r * 4 + k] = c->src[(size_t)(y0 + by * 4 + r) * sls + x0 + bx * 4 + k];
+                    pr[r * 4 + k] = pred[(by * 4 + r) * 16 + bx * 4 + k];
+                }
+            q_block(s, pr, qp, 0, 0, lv[b], cos[b], &dc);
+            score[(by / 2) * 2 + bx / 2] += q_decimate(lv[b], 16);
+        }
+        /* drop 8x8 blocks (and whole macroblocks) whose few small levels cost more than they give */
+        int total = score[0] + score[1] + score[2] + score[3];
+        for (int i8 = 0; i8 < 4; i8++)
+            if (score[i8] < 4 || total < 6)
+                for (int dy = 0; dy < 2; dy++)
+                    for (int dx = 0; dx < 2; dx++) {
+                        int b = ((i8 >> 1) * 2 + dy) * 4 + (i8 & 1) * 2 + dx;
+                        memset(lv[b], 0, sizeof(lv[b]));
+                        memset(cos[b], 0, sizeof(cos[b]));
+                    }
+        for (int b = 0; b < 16; b++) {
+            int n = 0;
+            for (int k = 0; k < 16; k++) {
+                out->luma[b][k] = (int16_t)lv[b][k];
+                if (lv[b][k]) n++;
+            }
+            out->nnz[b] = (uint8_t)n;
+            if (n > 0) {
+                int bx = b % 4, by = b / 4;
+                q_idct4_add(cos[b], rec[0] + (size_t)(y0 + by * 4) * ys + x0 + bx * 4, ys, maxv);
+                out->cbp |= (uint8_t)(1 << ((by / 2) * 2 + bx / 2));
+            }
+        }
+    }
+    q_code_chroma(c, mbx, mby, qp_y, cpred, out, rec + 1, cs);
+}
+
+int ironav_set_source_chroma(ironav_ctx* c, const void* cb, const void* cr, int stride) {
+    if (!c || !cb || !cr || stride < c->width / 2) return IRONAV_INVALID_ARGUMENT;
+    int cw = c->mb_w * 8, ch = c->mb_h * 8;
+    for (int k = 0; k < 2; k++) {
+        if (!c->src_c[k]) c->src_c[k] = (uint16_t*)malloc(sizeof(uint16_t) * (size_t)cw * ch);
+        pad_plane(k ? cr : cb, sample_bytes(c), stride, c->width / 2, c->height / 2, cw, ch, c->src_c[k]);
+    }
+    return IRONAV_OK;
+}
+
+int ironav_push_reference_chroma(ironav_ctx* c, const void* cb, const void* cr, int stride, int w, int h) {
+    if (!c || !cb || !cr || c->nrefs < 1) return IRONAV_INVALID_ARGUMENT;
+    int cw = c->mb_w * 8, ch = c->mb_h * 8;
+    if (!((w == c->width / 2 && h == c->height / 2) || (w == cw && h == ch)) || stride < w) return IRONAV_INVALID_ARGUMENT;
+    refpic* r = &c->refs[0];
+    for (int k = 0; k < 2; k++) {
+        if (!r->chroma[k]) r->chroma[k] = (uint16_t*)malloc(sizeof(uint16_t) * (size_t)cw * ch);
+        pad_plane(k ? cr : cb, sample_bytes(c), stride, w, h, cw, ch, r->chroma[k]);
+    }
+    return IRONAV_OK;
+}
+
+int ironav_code_inter_picture(ironav_ctx* c, int qp, const ironav_interdec* decs, ironav_intercode* codes, void* rec_y, int ys, void* rec_cb,
+                              void* rec_cr, int cs) {
+    if (!c || !decs || !codes || !rec_y || !rec_cb || !rec_cr || ys < c->pw || cs < c->pw / 2 || qp < -6 * (c->bd - 8) || qp > 51 || !c->src_c[0])
+        return IRONAV_INVALID_ARGUMENT;
+    long n = (long)c->mb_w * c->mb_h;
+    for (long i = 0; i < n; i++) {
+        const ironav_interdec* d = &decs[i];
+        if (d->mode == 0) continue;
+        if (d->mode > 2 || d->part > 3) return IRONAV_INVALID_INPUT;
+        for (int k = 0; k < 4; k++)
+            if (d->refs[k] >= c->nrefs || !c->refs[d->refs[k]].chroma[0] || d->sub[k] > 3) return IRONAV_INVALID_INPUT;
+    }
+    int B = sample_bytes(c), cw = c->mb_w * 8, ch = c->mb_h * 8;
+    uint16_t* rec[3];
+    rec[0] = (uint16_t*)malloc(sizeof(uint16_t) * (size_t)c->pw * c->ph);
+    rec[1] = (uint16_t*)malloc(sizeof(uint16_t) * (size_t)cw * ch);
+    rec[2] = (uint16_t*)malloc(sizeof(uint16_t) * (size_t)cw * ch);
+    dbk_copy_in(rec[0], rec_y, B, ys, c->pw, c->ph);
+    dbk_copy_in(rec[1], rec_cb, B, cs, cw, ch);
+    dbk_copy_in(rec[2], rec_cr, B, cs, cw, ch);
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 16) num_threads(c->threads)
+#endif
+    for (long i = 0; i < n; i++) {
+        if (decs[i].mode == 0) {
+            memset(&codes[i], 0, sizeof(codes[i]));
+            continue;
+        }
+        q_code_inter(c, (int)(i % c->mb_w), (int)(i / c->mb_w), qp, &decs[i], &codes[i], rec, c->pw, cw);
+    }
+    dbk_copy_out(rec_y, rec[0], B, ys, c->pw, c->ph);
+    dbk_copy_out(rec_cb, rec[1], B, cs, cw, ch);
+    dbk_copy_out(rec_cr, rec[2], B, cs, cw, ch);
+    for (int k = 0; k < 3; k++) free(rec[k]);
+    return IRONAV_OK;
+}
+
+int ironav_code_inter_picture_device(ironav_ctx* c, int qp, const ironav_interdec* d, ironav_intercode* o, void* y, int ys, void* cb, void* cr,
+                                     int cs) {
+    (void)c; (void)qp; (void)d; (void)o; (void)y; (void)ys; (void)cb; (void)cr; (void)cs;
     return IRONAV_HARDWARE_UNAVAILABLE;
 }
 
