@@ -52,7 +52,7 @@ def parse():
     p.add_argument("--ring", type=int, default=RING,
                    help="pictures in the ring (fewer than 36 fits in L2: for profiling runs only)")
     p.add_argument("--no-e2e", action="store_true", help="skip the host-buffer pass (profiling runs)")
-    p.add_argument("--workload", default="1080p", choices=["1080p", "batched", "scenecut", "deblock", "bpicture"],
+    p.add_argument("--workload", default="1080p", choices=["1080p", "batched", "scenecut", "deblock", "bpicture", "residual"],
                    help="1080p: one stream, replay mode (the headline); batched: 64 mixed-resolution streams in auto "
                         "mode, one launch per stage and frame step, against the per-stream launch loop")
     p.add_argument("--streams", type=int, default=64, help="streams of the batched workload")
@@ -264,6 +264,9 @@ def main():
         return finish(world)
     if args.workload == "bpicture":
         run_bpicture(args, rank, world)
+        return finish(world)
+    if args.workload == "residual":
+        run_residual(args, rank, world)
         return finish(world)
 
     import torch
@@ -674,6 +677,205 @@ def run_bpicture(args, rank, world):
     if rank == 0:
         print(json.dumps(line), flush=True)
     for st in stages:
+        st.close()
+
+
+def run_residual(args, rank, world):
+    """Inter residual coding and reconstruction at 1080p (code_inter / code_inter_residual / code_luma8 /
+    code_chroma, enc/frame.rs:1202-1305, 1856-1915), device-resident: one step = every macroblock of one P
+    picture coded from its decision (P_Skip prediction, or luma and chroma motion compensation, 4x4 or 8x8
+    transform, quantisation, decimation, chroma DC/AC, dequantisation, inverse transform into the
+    reconstruction). The decisions are those of the stage's own auto-mode analysis (8x8 transform allowed),
+    made before the timed region. A ring of contexts (reference planes, chroma, codes, reconstructions) larger
+    than L2. The oracle codes the same picture on all host cores."""
+    import torch
+    from ironav_b200.inter import INTERCODE_DTYPE, InterStage, cuda_library, inter_decisions
+    from ironav_b200.synth import CONFIGS, Sequence
+
+    bd = args.bd
+    lib = cuda_library()
+    ring = max(2, min(args.ring, 6))
+    w, h, seed, pan_q, nobj, vmax, sigma = CONFIGS["1080p"]
+    seq = Sequence(w, h, ring + 1, seed + 0x2000 * rank, pan_q, nobj, vmax, sigma)
+    qp = QP
+    frame = (lambda t: seq.frame10(t)) if bd == 10 else seq.frame
+    stream = torch.cuda.Stream()
+    dev = torch.device("cuda", torch.cuda.current_device())
+    stages, d_decs, d_codes, d_rec, decs_h, srcs = [], [], [], [], [], []
+    for k in range(ring):
+        st = InterStage(w, h, max_refs=1, nslices=NSLICES, lib=lib, bd=bd)
+        st.push_reference(frame(k))
+        st.push_reference_chroma(*seq.chroma(k, bd))
+        st.set_source(frame(k + 1))
+        st.set_source_chroma(*seq.chroma(k + 1, bd))
+        st.begin_p_picture(qp + 6 * (bd - 8))
+        _, res = st.analyse_auto()
+        decs = inter_decisions(res, t8=True)
+        st.set_stream(stream.cuda_stream)
+        stages.append(st)
+        decs_h.append(decs)
+        srcs.append((frame(k), seq.chroma(k, bd), frame(k + 1), seq.chroma(k + 1, bd)))
+        d_decs.append(torch.from_numpy(decs.view(np.uint8)).to(dev))
+        d_codes.append(torch.zeros(st.nmb * INTERCODE_DTYPE.itemsize, dtype=torch.uint8, device=dev))
+        dt = torch.uint8 if bd == 8 else torch.int16
+        d_rec.append((torch.zeros((st.mb_h * 16, st.mb_w * 16), dtype=dt, device=dev),
+                      torch.zeros((2, st.mb_h * 8, st.mb_w * 8), dtype=dt, device=dev)))
+    nmb, mb_w, mb_h = stages[0].nmb, stages[0].mb_w, stages[0].mb_h
+    modes = np.bincount(decs_h[0]["mode"], minlength=3)
+
+    def step(i, ev=None):
+        k = i % ring
+        y, c = d_rec[k]
+        if ev is not None:
+            ev[0].record(stream)
+        s_ = lib.ironav_code_inter_picture_device(stages[k].ctx, qp + 6 * (bd - 8), d_decs[k].data_ptr(), d_codes[k].data_ptr(),
+                                                  y.data_ptr(), y.shape[1], c[0].data_ptr(), c[1].data_ptr(), c.shape[2])
+        if s_:
+            raise RuntimeError(f"ironav_code_inter_picture_device: {s_}")
+        if ev is not None:
+            ev[1].record(stream)
+
+    with torch.cuda.stream(stream):
+        for i in range(args.warmup):
+            step(i)
+        clocks = Clocks(int(os.environ.get("LOCAL_RANK", 0)))
+        clocks.start()
+        t_load = time.perf_counter()
+        i = 0
+        while time.perf_counter() - t_load < 0.6:
+            step(args.warmup + i)
+            i += 1
+            if i % 8 == 0:
+                torch.cuda.synchronize()
+        torch.cuda.synchronize()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for i in range(args.steps):
+            step(args.warmup + i, evs[i])
+        e1.record(stream)
+        torch.cuda.synchronize()
+        clk = clocks.stop()
+    for st in stages:
+        st.sync()
+    ms = e0.elapsed_time(e1)
+    k_ms = float(np.mean([a.elapsed_time(b) for a, b in evs]))
+    value = world * nmb * args.steps / (ms * 1e-3)
+    B = 1 if bd == 8 else 2
+    # algorithmic bytes of one picture: every decision read and code record written; per P_Skip or inter
+    # macroblock its reference samples read once (luma 16x16, chroma 2 x 8x8) and its reconstruction written;
+    # per inter macroblock its source luma and chroma read
+    def algo_bytes(m):
+        return nmb * (78 + 1324) + int(m[1] + m[2]) * 2 * 384 * B + int(m[2]) * 384 * B
+    bytes_per = algo_bytes(modes)
+    hbm = measured_hbm()
+
+    # the residual path everywhere: the same vectors, every macroblock coded with its residual (no P_Skip)
+    coded = []
+    for k in range(ring):
+        d = decs_h[k].copy()
+        d["mode"] = 2
+        coded.append(torch.from_numpy(d.view(np.uint8)).to(dev))
+    ev_c = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with torch.cuda.stream(stream):
+        for i in range(args.warmup + args.steps):
+            k = i % ring
+            y, c = d_rec[k]
+            if i >= args.warmup:
+                ev_c[i - args.warmup][0].record(stream)
+            s_ = lib.ironav_code_inter_picture_device(stages[k].ctx, qp + 6 * (bd - 8), coded[k].data_ptr(), d_codes[k].data_ptr(),
+                                                      y.data_ptr(), y.shape[1], c[0].data_ptr(), c[1].data_ptr(), c.shape[2])
+            if s_:
+                raise RuntimeError(f"ironav_code_inter_picture_device: {s_}")
+            if i >= args.warmup:
+                ev_c[i - args.warmup][1].record(stream)
+        torch.cuda.synchronize()
+    kc_ms = float(np.mean([a.elapsed_time(b) for a, b in ev_c]))
+    bytes_c = algo_bytes([0, 0, nmb])
+
+    # end to end through the host-buffer call: decisions and the reconstruction planes in, codes and planes out
+    ho = [InterStage(w, h, max_refs=1, nslices=NSLICES, lib=lib, bd=bd) for _ in range(2)]
+    for k, o_ in enumerate(ho):
+        f0, c0, f1, c1 = srcs[k]
+        o_.push_reference(f0)
+        o_.push_reference_chroma(*c0)
+        o_.set_source(f1)
+        o_.set_source_chroma(*c1)
+        o_.begin_p_picture(qp + 6 * (bd - 8))
+    tnp = (lambda a: torch.from_numpy(a).pin_memory())
+    pin_d = [tnp(decs_h[k].view(np.uint8)) for k in range(2)]
+    pin_c = [torch.zeros(nmb * INTERCODE_DTYPE.itemsize, dtype=torch.uint8).pin_memory() for _ in range(2)]
+    dt_np = np.uint8 if bd == 8 else np.int16
+    pin_y = [tnp(np.zeros((mb_h * 16, mb_w * 16), dt_np)) for _ in range(2)]
+    pin_ch = [tnp(np.zeros((2, mb_h * 8, mb_w * 8), dt_np)) for _ in range(2)]
+
+    def host_call(k):
+        return lib.ironav_code_inter_picture(ho[k].ctx, qp + 6 * (bd - 8), pin_d[k].data_ptr(), pin_c[k].data_ptr(),
+                                             pin_y[k].data_ptr(), mb_w * 16, pin_ch[k][0].data_ptr(), pin_ch[k][1].data_ptr(),
+                                             mb_w * 8)
+    for i in range(args.warmup):
+        host_call(i % 2)
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        s_ = host_call(i % 2)
+        if s_:
+            raise RuntimeError(f"ironav_code_inter_picture: {s_}")
+    el = time.perf_counter() - t0
+    plane_bytes = nmb * 384 * B
+    line = {
+        "metric": f"1080p P-picture inter residual coding + reconstruction MB/s ({bd}-bit)", "value": value, "unit": "MB/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic: seeded 4-octave value noise panned per frame + 8 moving rectangles, sigma 3; chroma "
+                "from the 2x2 luma means",
+        "config": {"workload": f"code every macroblock of one 1920x1088 {bd}-bit P picture per step (QP {qp}, 8x8 "
+                               f"transform allowed) from the stage's own decisions: {int(modes[1])} P_Skip, "
+                               f"{int(modes[2])} inter, {int(modes[0])} left to intra",
+                   "slices": NSLICES, "mode": "device pointers",
+                   "l2": f"ring of {ring} contexts (reference planes, chroma, codes, reconstructions > L2)"},
+        "gpu_launches": args.steps,
+        "e2e": {"value": world * nmb * args.steps / el, "unit": "MB/s",
+                "h2d_bytes_per_step": nmb * 78 + plane_bytes, "d2h_bytes_per_step": nmb * 1324 + plane_bytes,
+                "ms_per_step": 1e3 * el / args.steps,
+                "note": "ironav_code_inter_picture on pinned host buffers, one thread"},
+        "roofline": {"bound": "hbm", "kernel": f"code_inter_kernel<{'uint8_t' if bd == 8 else 'uint16_t'}>",
+                     "achieved": bytes_per / (k_ms * 1e-3) / 1e9, "peak": hbm[0], "unit": "GB/s",
+                     "frac": bytes_per / (k_ms * 1e-3) / 1e9 / hbm[0], "peak_source": hbm[1], "ms_per_launch": k_ms,
+                     "traffic": None,
+                     "note": "algorithmic bytes: decisions, source, reference samples once, codes and reconstruction"},
+        "all_coded": {"ms_per_launch": kc_ms, "MB/s": nmb / (kc_ms * 1e-3), "achieved_gbs": bytes_c / (kc_ms * 1e-3) / 1e9,
+                      "frac": bytes_c / (kc_ms * 1e-3) / 1e9 / hbm[0],
+                      "note": "the same vectors with every macroblock coded with its residual (mode 2), timed after the "
+                              "timed region with the same events and ring"},
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from tests.oracle_lib import oracle_library
+
+        olib = oracle_library()
+        cores = host_cores()
+        o = InterStage(w, h, max_refs=1, nslices=NSLICES, lib=olib, bd=bd)
+        olib.oracle_set_threads(o.ctx, cores)
+        f0, c0, f1, c1 = srcs[0]
+        o.push_reference(f0)
+        o.push_reference_chroma(*c0)
+        o.set_source(f1)
+        o.set_source_chroma(*c1)
+        o.begin_p_picture(qp + 6 * (bd - 8))
+        dt_np = np.uint8 if bd == 8 else np.uint16
+        rec = (np.zeros((mb_h * 16, mb_w * 16), dt_np), np.zeros((mb_h * 8, mb_w * 8), dt_np), np.zeros((mb_h * 8, mb_w * 8), dt_np))
+        n_cpu, t_cpu = 0, 0.0
+        while t_cpu < min(args.cpu_seconds, 10.0):
+            t0 = time.perf_counter()
+            o.code_inter(qp + 6 * (bd - 8), decs_h[0], rec)
+            t_cpu += time.perf_counter() - t0
+            n_cpu += 1
+        line["cpu_baseline"] = {"value": n_cpu * nmb / t_cpu, "unit": "MB/s", "cores": cores, "kind": "port",
+                                "sample": f"{n_cpu} P pictures (the ring's first), {cores} threads, {t_cpu:.1f} s"}
+        o.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    for st in stages + ho:
         st.close()
 
 

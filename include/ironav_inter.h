@@ -263,12 +263,13 @@ typedef struct ironav_intercode {
 /* Codes the inter macroblocks of the current picture (the source set with ironav_set_source and
  * ironav_set_source_chroma) at QP_Y qp: decs and codes hold mb_w*mb_h entries; the reconstruction
  * planes (luma 16*mb_w x 16*mb_h, rows y_stride samples apart; chroma 8*mb_w x 8*mb_h, rows c_stride
- * apart) receive the inter macroblocks and keep every other macroblock as they were. References are
- * those held (0 = newest), each with its chroma. */
+ * apart) receive the inter macroblocks and keep every other macroblock as they were; the codes of a
+ * macroblock that is not inter are zero. References are those held (0 = newest), each with its chroma. */
 int ironav_code_inter_picture(ironav_ctx* ctx, int qp, const ironav_interdec* decs, ironav_intercode* codes, void* rec_y,
                               int y_stride, void* rec_cb, void* rec_cr, int c_stride);
 /* The same on device pointers, queued on the context's stream; the reconstruction planes as for
- * ironav_deblock_picture_device (16-byte aligned, aligned row strides). */
+ * ironav_deblock_picture_device (16-byte aligned, aligned row strides), d_decs 2-byte and d_codes 4-byte
+ * aligned. */
 int ironav_code_inter_picture_device(ironav_ctx* ctx, int qp, const ironav_interdec* d_decs, ironav_intercode* d_codes,
                                      void* d_rec_y, int y_stride, void* d_rec_cb, void* d_rec_cr, int c_stride);
 

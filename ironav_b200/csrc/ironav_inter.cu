@@ -710,9 +710,11 @@ static int launch_code_inter(ironav_ctx* c, int qp, const ironav_interdec* d_dec
 int ironav_code_inter_picture_device(ironav_ctx* c, int qp, const ironav_interdec* d_decs, ironav_intercode* d_codes, void* y, int ys, void* cb,
                                      void* cr, int cs) {
     if (!c || !d_decs || !d_codes || !y || !cb || !cr || ys < c->pw || cs < c->pw / 2) return IRONAV_INVALID_ARGUMENT;
-    // the same alignment as the deblocking filter's device form
+    // the planes: the same alignment as the deblocking filter's device form; the records: the kernel reads a
+    // decision as 16-bit words and writes a code record as 32-bit words
     const uintptr_t a = reinterpret_cast<uintptr_t>(y) | reinterpret_cast<uintptr_t>(cb) | reinterpret_cast<uintptr_t>(cr);
     if ((a & 15) || ((size_t)ys * sample_bytes(c)) % 16 || cs % 8) return IRONAV_INVALID_ARGUMENT;
+    if ((reinterpret_cast<uintptr_t>(d_decs) & 1) || (reinterpret_cast<uintptr_t>(d_codes) & 3)) return IRONAV_INVALID_ARGUMENT;
     return launch_code_inter(c, qp, d_decs, d_codes, y, ys, cb, cr, cs);
 }
 

@@ -7,7 +7,9 @@
 // h264/inter.rs:549-568). The 4x4 transform path takes a lane per 4x4 block (fdct4, quantisation, the
 // decimation score, the 8x8 sums by shuffles, inverse transform and the reconstruction's 4x4); the 8x8 path
 // takes 8 lanes per 8x8 block, a row then a column each, transposed through shared memory; chroma takes a
-// lane per 4x4 block of Cb and Cr, the 2x2 DC transform by shuffles among a component's 4 lanes.
+// lane per 4x4 block of Cb and Cr, the 2x2 DC transform by shuffles among a component's 4 lanes. Levels
+// pass through shared memory across the shuffles (no 16-entry array live there), which holds the kernel
+// to 128 registers: 4 blocks (16 warps) an SM.
 #pragma once
 #include "analyse.cuh"
 #include "deblock.cuh"
@@ -39,7 +41,9 @@ static __device__ __constant__ int c_q_mf8[6][6] = {{13107, 11428, 20972, 12222,
                                                     {8192, 7346, 13159, 7740, 10486, 9777},     {7282, 6428, 11570, 6830, 9118, 8640}};
 static __device__ __constant__ int c_q_dq8[6][6] = {{20, 18, 32, 19, 25, 24}, {22, 19, 35, 21, 28, 26}, {26, 23, 42, 24, 33, 31},
                                                     {28, 25, 45, 26, 35, 33}, {32, 28, 51, 30, 40, 38}, {36, 32, 58, 34, 46, 43}};
-static __device__ __constant__ uint8_t c_zz4[16] = {0, 1, 4, 8, 5, 2, 3, 6, 9, 12, 13, 10, 7, 11, 14, 15};
+// ZIGZAG4 as nibbles (entry k in bits 4k..4k+3): folds to a constant in an unrolled loop, so the
+// coefficient arrays it indexes stay in registers
+__device__ __forceinline__ constexpr int zz4_at(int k) { return (int)((0xFEB7ADC963258410ull >> (4 * k)) & 15); }
 static __device__ __constant__ uint8_t c_zz8[64] = {0,  1,  8,  16, 9,  2,  3,  10, 17, 24, 32, 25, 18, 11, 4,  5,
                                                     12, 19, 26, 33, 40, 48, 41, 34, 27, 20, 13, 6,  7,  14, 21, 28,
                                                     35, 42, 49, 56, 57, 50, 43, 36, 29, 22, 15, 23, 30, 37, 44, 51,
@@ -206,7 +210,7 @@ __device__ __forceinline__ int4 rect_of(int part, const uint8_t* sub, int bx, in
 }
 
 template <class T>
-__global__ void __launch_bounds__(128) code_inter_kernel(const __grid_constant__ CodeParams P) {
+__global__ void __launch_bounds__(128, 4) code_inter_kernel(const __grid_constant__ CodeParams P) {
     __shared__ CodeSmem smem[4];
     CodeSmem& S = smem[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
@@ -220,6 +224,9 @@ __global__ void __launch_bounds__(128) code_inter_kernel(const __grid_constant__
         __syncwarp();
         const ironav_interdec& D = *reinterpret_cast<const ironav_interdec*>(S.dec);
         const int mode = D.mode;
+        // the output record starts from zero (and stays so for a macroblock that is not inter)
+        uint32_t* outw = reinterpret_cast<uint32_t*>(&P.codes[mb]);
+        for (int k = lane; k < (int)(sizeof(ironav_intercode) / 4); k += 32) outw[k] = 0;
         if (mode == 0) continue;
         // a decision that would read outside the tables: the macroblock is left alone, the call reports it
         bool bad = mode > 2 || D.part > 3;
@@ -229,9 +236,6 @@ __global__ void __launch_bounds__(128) code_inter_kernel(const __grid_constant__
             continue;
         }
         const int mbx = mb % P.A.mb_w, mby = mb / P.A.mb_w, x0 = mbx * 16, y0 = mby * 16;
-        // the output record starts from zero
-        uint32_t* outw = reinterpret_cast<uint32_t*>(&P.codes[mb]);
-        for (int k = lane; k < (int)(sizeof(ironav_intercode) / 4); k += 32) outw[k] = 0;
         // luma prediction, a lane per 4x4 block
         if (lane < 16) {
             const int bx = lane & 3, by = lane >> 2;
@@ -271,30 +275,23 @@ __global__ void __launch_bounds__(128) code_inter_kernel(const __grid_constant__
             // P_Skip: the prediction is the reconstruction
             for (int i = lane; i < 256; i += 32) RY[(size_t)(y0 + (i >> 4)) * P.ys + x0 + (i & 15)] = (T)S.pred[i];
         } else if (!D.t8) {
-            // 4x4 transform: a lane per block
-            int lv[16], co[16], p[16];
+            // 4x4 transform: a lane per block; the levels go to shared memory and come back after the
+            // decimation sums, so that no 16-entry array stays live across the shuffles
             int score = 0;
+            const int bx = lane & 3, by = lane >> 2;
             if (lane < 16) {
-                const int bx = lane & 3, by = lane >> 2;
                 int d[16], c[16];
 #pragma unroll
                 for (int r = 0; r < 4; r++)
 #pragma unroll
-                    for (int k = 0; k < 4; k++) {
-                        p[r * 4 + k] = S.pred[(by * 4 + r) * 16 + bx * 4 + k];
-                        d[r * 4 + k] = (int)SY[(size_t)(y0 + by * 4 + r) * P.A.ls + x0 + bx * 4 + k] - p[r * 4 + k];
-                    }
+                    for (int k = 0; k < 4; k++)
+                        d[r * 4 + k] = (int)SY[(size_t)(y0 + by * 4 + r) * P.A.ls + x0 + bx * 4 + k] - S.pred[(by * 4 + r) * 16 + bx * 4 + k];
                 q_fdct4_d(d, c);
                 const int qbits = 15 + qp / 6, f = (1 << qbits) / 6, m = qp % 6;
 #pragma unroll
-                for (int k = 0; k < 16; k++) co[k] = 0;
-#pragma unroll
                 for (int k = 0; k < 16; k++) {
-                    const int pz = c_zz4[k];
-                    const int l = q_quant_d(c[pz], c_q_mf[m][q_class_d(pz)], f, qbits);
-                    lv[k] = l;
-                    S.lv4[lane][k] = (int16_t)l;
-                    co[pz] = (l * c_q_v[m][q_class_d(pz)]) << (qp / 6);
+                    const int pz = zz4_at(k);
+                    S.lv4[lane][k] = (int16_t)q_quant_d(c[pz], c_q_mf[m][q_class_d(pz)], f, qbits);
                 }
                 score = q_decimate_d(S.lv4[lane], 16);
             }
@@ -314,15 +311,24 @@ __global__ void __launch_bounds__(128) code_inter_kernel(const __grid_constant__
             }
             if (lane < 16) {
                 const bool drop = s8 < 4 || tot < 6;
-                const int bx = lane & 3, by = lane >> 2;
-                int nz = 0;
+                const int m = qp % 6, sh = qp / 6;
+                int co[16], p[16], nz = 0;
+                uint32_t packed[8];
 #pragma unroll
                 for (int k = 0; k < 16; k++) {
-                    if (drop) lv[k] = 0;
-                    nz += lv[k] != 0;
+                    const int pz = zz4_at(k);
+                    const int l = drop ? 0 : S.lv4[lane][k];
+                    nz += l != 0;
+                    co[pz] = (l * c_q_v[m][q_class_d(pz)]) << sh;
+                    if (k & 1) packed[k >> 1] |= (uint32_t)(l & 0xffff) << 16;
+                    else packed[k >> 1] = (uint32_t)(l & 0xffff);
                 }
+#pragma unroll
+                for (int r = 0; r < 4; r++)
+#pragma unroll
+                    for (int k = 0; k < 4; k++) p[r * 4 + k] = S.pred[(by * 4 + r) * 16 + bx * 4 + k];
                 int out[16];
-                if (!drop && nz > 0) {
+                if (nz > 0) {
                     q_idct4_d(co, p, maxv, out);
                 } else {
 #pragma unroll
@@ -333,8 +339,9 @@ __global__ void __launch_bounds__(128) code_inter_kernel(const __grid_constant__
 #pragma unroll
                     for (int k = 0; k < 4; k++) RY[(size_t)(y0 + by * 4 + r) * P.ys + x0 + bx * 4 + k] = (T)out[r * 4 + k];
                 ironav_intercode& O = P.codes[mb];
+                uint32_t* lw = reinterpret_cast<uint32_t*>(O.luma[lane]);
 #pragma unroll
-                for (int k = 0; k < 16; k++) O.luma[lane][k] = (int16_t)lv[k];
+                for (int k = 0; k < 8; k++) lw[k] = packed[k];
                 O.nnz[lane] = (uint8_t)nz;
                 if (nz > 0) cbp |= 1u << ((by >> 1) * 2 + (bx >> 1));
             }
@@ -429,8 +436,8 @@ __global__ void __launch_bounds__(128) code_inter_kernel(const __grid_constant__
         // the luma part of the coded block pattern, from every lane
 #pragma unroll
         for (int off = 16; off >= 1; off >>= 1) cbp |= __shfl_xor_sync(FULL, cbp, off);
-        // chroma (code_chroma, inter), a lane per 4x4 block of Cb (lanes 0-3) and Cr (4-7)
-        int clv[16], cco[16], cp[16];
+        // chroma (code_chroma, inter), a lane per 4x4 block of Cb (lanes 0-3) and Cr (4-7); the AC levels
+        // go to shared memory and come back after the DC transform's shuffles
         int dc = 0, cscore = 0, anyac = 0;
         const int qpc = dbk_chroma_qp(P.qp, 0, P.bd) + 6 * (P.bd - 8), mc = qpc % 6;
         const int cc = (lane >> 2) & 1, blk = lane & 3, cbx = blk & 1, cby = blk >> 1;
@@ -440,23 +447,14 @@ __global__ void __launch_bounds__(128) code_inter_kernel(const __grid_constant__
 #pragma unroll
             for (int r = 0; r < 4; r++)
 #pragma unroll
-                for (int k = 0; k < 4; k++) {
-                    cp[r * 4 + k] = S.cpred[cc][(cby * 4 + r) * 8 + cbx * 4 + k];
-                    d[r * 4 + k] = (int)SC[(size_t)(mby * 8 + cby * 4 + r) * P.cw + mbx * 8 + cbx * 4 + k] - cp[r * 4 + k];
-                }
+                for (int k = 0; k < 4; k++)
+                    d[r * 4 + k] = (int)SC[(size_t)(mby * 8 + cby * 4 + r) * P.cw + mbx * 8 + cbx * 4 + k] - S.cpred[cc][(cby * 4 + r) * 8 + cbx * 4 + k];
             q_fdct4_d(d, c);
             const int qbits = 15 + qpc / 6, f = (1 << qbits) / 6;
 #pragma unroll
-            for (int k = 0; k < 16; k++) cco[k] = 0;
-#pragma unroll
             for (int k = 0; k < 16; k++) {
-                const int pz = c_zz4[k];
-                int l = 0;
-                if (pz != 0) {
-                    l = q_quant_d(c[pz], c_q_mf[mc][q_class_d(pz)], f, qbits);
-                    cco[pz] = (l * c_q_v[mc][q_class_d(pz)]) << (qpc / 6);
-                }
-                clv[k] = l;
+                const int pz = zz4_at(k);
+                const int l = pz != 0 ? q_quant_d(c[pz], c_q_mf[mc][q_class_d(pz)], f, qbits) : 0;
                 S.cl[cc][blk][k] = (int16_t)l;
                 anyac |= l != 0;
             }
@@ -484,23 +482,30 @@ __global__ void __launch_bounds__(128) code_inter_kernel(const __grid_constant__
             const int fl = blk == 0 ? l0 + l1 + l2 + l3 : (blk == 1 ? l0 - l1 + l2 - l3 : (blk == 2 ? l0 + l1 - l2 - l3 : l0 - l1 - l2 + l3));
             if (lane < 8) {
                 ironav_intercode& O = P.codes[mb];
-                if (!any_ac) {
-#pragma unroll
-                    for (int k = 0; k < 16; k++) {
-                        clv[k] = 0;
-                        cco[k] = 0;
-                    }
-                }
-                cco[0] = cbpc > 0 ? ((fl * (16 * c_q_v[mc][0])) << (qpc / 6)) >> 5 : 0;
-                int nz = 0, any = 0;
+                const int sh = qpc / 6;
+                int cco[16], cp[16], nz = 0, any = 0;
+                uint32_t packed[8];
 #pragma unroll
                 for (int k = 0; k < 16; k++) {
-                    O.cac[cc][blk][k] = (int16_t)clv[k];
-                    nz += clv[k] != 0;
-                    any |= cco[k] != 0;
+                    const int pz = zz4_at(k);
+                    const int l = any_ac ? S.cl[cc][blk][k] : 0;
+                    nz += l != 0;
+                    cco[pz] = (l * c_q_v[mc][q_class_d(pz)]) << sh;
+                    if (k & 1) packed[k >> 1] |= (uint32_t)(l & 0xffff) << 16;
+                    else packed[k >> 1] = (uint32_t)(l & 0xffff);
                 }
+                cco[0] = cbpc > 0 ? ((fl * (16 * c_q_v[mc][0])) << sh) >> 5 : 0;
+#pragma unroll
+                for (int k = 0; k < 16; k++) any |= cco[k];
+                uint32_t* aw = reinterpret_cast<uint32_t*>(O.cac[cc][blk]);
+#pragma unroll
+                for (int k = 0; k < 8; k++) aw[k] = packed[k];
                 O.cnnz[cc][blk] = (uint8_t)nz;
                 O.cdc[cc][blk] = (int16_t)cdc;
+#pragma unroll
+                for (int r = 0; r < 4; r++)
+#pragma unroll
+                    for (int k = 0; k < 4; k++) cp[r * 4 + k] = S.cpred[cc][(cby * 4 + r) * 8 + cbx * 4 + k];
                 int out[16];
                 if (any) {
                     q_idct4_d(cco, cp, maxv, out);

@@ -172,14 +172,19 @@ def test_gpu_code_inter_rejects_bad_decisions_and_device_form(oracle_lib, cuda_l
     with pytest.raises(IronavError) as e:
         c.code_inter(22, bad, blank_rec(c))
     assert e.value.status == 2
+    decs["mode"][::7] = 0  # left alone: their codes come back zero whatever the buffer held
     want = o.code_inter(22, decs, blank_rec(o))
     c.set_stream(torch.cuda.current_stream().cuda_stream)
     y = torch.zeros((c.mb_h * 16, c.mb_w * 16), dtype=torch.uint8, device="cuda")
     cc = torch.zeros((2, c.mb_h * 8, c.mb_w * 8), dtype=torch.uint8, device="cuda")
     td = torch.from_numpy(decs.view(np.uint8)).cuda()
-    tc = torch.zeros(c.nmb * 1324, dtype=torch.uint8, device="cuda")
+    tc = torch.full((c.nmb * 1324,), 0x5A, dtype=torch.uint8, device="cuda")
     assert c.lib.ironav_code_inter_picture_device(c.ctx, 22, td.data_ptr(), tc.data_ptr(), y.data_ptr(), y.shape[1], cc[0].data_ptr(),
                                                   cc[1].data_ptr(), cc.shape[2]) == 0
     c.sync()
     got = (tc.cpu().numpy().view(INTERCODE_DTYPE), (y.cpu().numpy(), cc[0].cpu().numpy(), cc[1].cpu().numpy()))
+    # records the kernel cannot address word-wise are refused before any launch
+    for dd, cd in ((td.data_ptr() + 1, tc.data_ptr()), (td.data_ptr(), tc.data_ptr() + 2)):
+        assert c.lib.ironav_code_inter_picture_device(c.ctx, 22, dd, cd, y.data_ptr(), y.shape[1], cc[0].data_ptr(),
+                                                      cc[1].data_ptr(), cc.shape[2]) == 3
     _check_same(got, want, "device form")
