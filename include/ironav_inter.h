@@ -273,6 +273,49 @@ int ironav_code_inter_picture(ironav_ctx* ctx, int qp, const ironav_interdec* de
 int ironav_code_inter_picture_device(ironav_ctx* ctx, int qp, const ironav_interdec* d_decs, ironav_intercode* d_codes,
                                      void* d_rec_y, int y_stride, void* d_rec_cb, void* d_rec_cr, int c_stride);
 
+/* ---- the P macroblock decision (decide mode) -------------------------------------------------------- */
+
+/* The whole of code_mb for a P picture coded with CAVLC (enc/frame.rs:715-790): P_Skip when the skip
+ * vector leaves nothing to code (the fast test on luma and chroma SADs, then code_inter's cbp == 0), else
+ * the best Intra16x16 mode (best_i16, 812-835), the best inter partitioning (best_inter), Intra4x4 coded
+ * block by block when intra is competitive (code_i4, 1050-1138), and the cheapest of them coded: inter
+ * (code_inter), Intra4x4 or Intra16x16 (code_i16, 1140-1200) with intra chroma (code_intra_chroma,
+ * 1807-1854). Macroblocks are decided in each slice band's raster order on the device (a wavefront: a
+ * macroblock waits for its left and top-right neighbours), each against the final decisions and the
+ * unfiltered reconstruction of those before it, as FrameCoder::encode does (452-487); the host is left
+ * the entropy coding. The picture parameters are those of ironav_begin_p_picture (QP', lambda, the P_Skip
+ * threshold, active references, fast, sub8x8); the source and every active reference need their chroma.
+ * The code of one macroblock (MbCode, 275-300): */
+typedef struct ironav_mbcode {
+    ironav_intercode res;  /* levels: luma (4x4 blocks; Intra16x16: AC, scan position 0 unused), cdc, cac,
+                              nnz, cnnz, cbp (luma bits 0-3, chroma 4-5); luma8 and t8x8 are zero (the
+                              CAVLC encoder codes no 8x8 transform) */
+    int16_t dc[16];        /* Intra16x16 luma DC levels, zigzag order */
+    int16_t mvs[16][2];    /* inter: a vector per partition in coding order (rects(part, sub)); P_Skip and
+                              16x16: the vector in all 16 */
+    int16_t mvds[16][2];   /* inter, not skipped: each vector less its predictor (part_mvps) */
+    uint8_t modes[16];     /* Intra4x4 prediction modes, raster 4x4 order (2 elsewhere) */
+    uint8_t kind;          /* the reference's Kind: 1 Intra4x4, 3 Intra16x16, 5 inter */
+    uint8_t skip;          /* P_Skip */
+    uint8_t i16_mode;      /* Intra16x16 prediction mode */
+    uint8_t chroma_mode;   /* intra chroma prediction mode */
+    uint8_t part;          /* inter partitioning */
+    uint8_t sub[4];        /* sub_mb_type per 8x8 block (part 3) */
+    uint8_t refs[4];       /* reference index per 8x8 block (per partition for 16x8 / 8x16) */
+    uint8_t pad[3];
+} ironav_mbcode;           /* 1516 bytes */
+
+/* Decides and codes every macroblock of the current P picture: states receives each macroblock's
+ * MbState (the ironav_mbstate a later picture reads as co-located; intra: inter 0, refs -1), codes the
+ * codes, and the reconstruction planes (luma 16*mb_w x 16*mb_h, rows y_stride samples apart; chroma
+ * 8*mb_w x 8*mb_h, rows c_stride apart) every macroblock's reconstruction before deblocking. */
+int ironav_decide_p_picture(ironav_ctx* ctx, ironav_mbstate* states, ironav_mbcode* codes, void* rec_y, int y_stride, void* rec_cb,
+                            void* rec_cr, int c_stride);
+/* The same on device pointers, queued on the context's stream (planes as for
+ * ironav_deblock_picture_device; states and codes 4-byte aligned). */
+int ironav_decide_p_picture_device(ironav_ctx* ctx, ironav_mbstate* d_states, ironav_mbcode* d_codes, void* d_rec_y, int y_stride,
+                                   void* d_rec_cb, void* d_rec_cr, int c_stride);
+
 /* ---- deblocking of the reconstruction ------------------------------------------------------------ */
 
 /* The in-loop deblocking filter (h264/deblock.rs:410-720, ITU-T H.264 8.7) of a reconstructed picture,

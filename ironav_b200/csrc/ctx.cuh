@@ -71,6 +71,9 @@ struct ironav_ctx {
     ironav_interdec* d_decs = nullptr;
     ironav_intercode* d_codes = nullptr;
     uint8_t* d_rec = nullptr;
+    // decide mode: its persistent grid (from the kernel's occupancy, on first use) and host-form codes
+    int k7_blocks = 0;
+    ironav_mbcode* d_mbcodes = nullptr;
 };
 
 

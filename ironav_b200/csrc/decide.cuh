@@ -1,0 +1,793 @@
+// decide.cuh — K7: the P macroblock decision of the CAVLC encoder (code_mb, enc/frame.rs:715-790) on the
+// device, one warp per macroblock in the auto mode's wavefront: P_Skip tests (the fast luma and chroma SADs,
+// then code_inter's cbp == 0), best_i16, best_inter (K2's searches), code_i4 when intra is competitive, and
+// the coding of the cheapest (code_inter, code_i16 or the Intra4x4 trial, code_intra_chroma) into the
+// unfiltered reconstruction that later macroblocks' intra prediction reads.
+//
+// A macroblock's intra prediction reads the reconstruction of its left, top, top-left and top-right
+// neighbours; the wavefront's waits (left and top-right, K2's auto mode) cover all four, and a macroblock
+// publishes its flag after its reconstruction, code and state are written (fence, then release store).
+//
+// Lanes: best_i16 takes a 4x4 block and two modes a lane; the Intra4x4 trial goes block by block in
+// decoding order (each block predicts from the ones before), its nine modes on lanes 0-8 and the chosen
+// block's transform on the winning lane; code_i16 takes a lane per 4x4 block with the DC transform on lane
+// 0; intra chroma takes a lane per (mode, component, 4x4 block) for the search and then code_chroma_mb.
+#pragma once
+#include "residual.cuh"
+
+namespace ironav {
+
+struct DecideParams {
+    CodeParams C;          // C.A: the analysis' parameters and the wavefront's (order, ticket, flags, epoch, err)
+    ironav_mbcode* codes;  // every macroblock's code (neighbours' Intra4x4 modes are read back from here)
+    int fast_t, fast_tc;   // the fast mode's P_Skip bounds on the luma and chroma SADs
+};
+
+constexpr int K7_WARPS = 4;
+constexpr int K7_MIN_BLOCKS = 4;
+constexpr int KIND_I4 = 1, KIND_I16 = 3, KIND_INTER = 5;  // Kind, h264/mb.rs:21-30
+
+template <class T>
+struct DecideSmem {
+    WarpSmem<T> a;         // the analysis' working set (source, neighbour table, searches)
+    CodeSmem c;            // the coder's
+    int top[21];           // luma row above the macroblock: x = -1 (top-left) .. 19 (the top-right macroblock's first 4)
+    int left[16];          // luma column to its left
+    int ctop[2][9];        // chroma rows above: x = -1 .. 7
+    int cleft[2][8];       // chroma columns to the left
+    int i4rec[256];        // the Intra4x4 trial's reconstruction
+    int16_t i4lv[16][16];  // its levels: raster 4x4 blocks, scan order
+    int edge[13];          // the current 4x4 block's edges: top-left, 8 above, 4 to the left
+    int dcs[16];           // Intra16x16: each block's DC coefficient, then its dequantised DC
+    int nbm[8];            // pred_i4_mode: the left macroblock's modes down its right column, then the top's along its
+                           // bottom row (2 for a macroblock that is not Intra4x4, -1 unavailable)
+    uint8_t i4modes[16];
+    uint8_t i4nnz[16];
+};
+
+// A source sample of the staged macroblock (WarpSmem::src: 16 rows of 16 samples, packed).
+template <class T>
+__device__ __forceinline__ int src_at(const WarpSmem<T>& S, int x, int y) {
+    if (sizeof(T) == 1) return (int)((S.src[y * 4 + (x >> 2)] >> (8 * (x & 3))) & 0xffu);
+    return (int)((S.src[y * 8 + (x >> 1)] >> (16 * (x & 1))) & 0xffffu);
+}
+
+// satd4, enc/frame.rs:144-161, of 16 differences (raster)
+__device__ __forceinline__ int satd4_d(const int (&d)[16]) {
+    int t[16];
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+        const int a = d[r * 4], b = d[r * 4 + 1], c = d[r * 4 + 2], e = d[r * 4 + 3];
+        const int s0 = a + b, s1 = c + e, d0 = a - b, d1 = c - e;
+        t[r * 4] = s0 + s1;
+        t[r * 4 + 1] = s0 - s1;
+        t[r * 4 + 2] = d0 - d1;
+        t[r * 4 + 3] = d0 + d1;
+    }
+    int sum = 0;
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+        const int a = t[c], b = t[4 + c], cc = t[8 + c], e = t[12 + c];
+        const int s0 = a + b, s1 = cc + e, d0 = a - b, d1 = cc - e;
+        sum += abs(s0 + s1) + abs(s0 - s1) + abs(d0 - d1) + abs(d0 + d1);
+    }
+    return sum >> 1;
+}
+
+// predict_nxn for a 4x4 block, h264/intra.rs:30-128 (ITU-T H.264 8.3.1.2), from the edge array E (E[0] the
+// top-left sample, E[1 + i] the 8 above, E[9 + j] the 4 to the left).
+__device__ __forceinline__ void i_pred4_d(int mode, const int* E, bool ht, bool hl, int bd, int (&out)[16]) {
+#define T_(i) E[1 + (i)]
+#define L_(j) ((j) < 0 ? E[0] : E[9 + (j)])
+#pragma unroll
+    for (int y = 0; y < 4; y++)
+#pragma unroll
+        for (int x = 0; x < 4; x++) {
+            int v;
+            switch (mode) {
+            case 0: v = T_(x); break;
+            case 1: v = L_(y); break;
+            case 2: {
+                const int st = T_(0) + T_(1) + T_(2) + T_(3), sl = L_(0) + L_(1) + L_(2) + L_(3);
+                v = (ht && hl) ? (st + sl + 4) >> 3 : (hl ? (sl + 2) >> 2 : (ht ? (st + 2) >> 2 : 1 << (bd - 1)));
+                break;
+            }
+            case 3: v = (x == 3 && y == 3) ? (T_(6) + 3 * T_(7) + 2) >> 2 : (T_(x + y) + 2 * T_(x + y + 1) + T_(x + y + 2) + 2) >> 2; break;
+            case 4:
+                if (x > y) v = (T_(x - y - 2) + 2 * T_(x - y - 1) + T_(x - y) + 2) >> 2;
+                else if (x < y) v = (L_(y - x - 2) + 2 * L_(y - x - 1) + L_(y - x) + 2) >> 2;
+                else v = (T_(0) + 2 * E[0] + L_(0) + 2) >> 2;
+                break;
+            case 5: {
+                const int z = 2 * x - y, i = x - (y >> 1);
+                if (z >= 0 && (z & 1) == 0) v = (T_(i - 1) + T_(i) + 1) >> 1;
+                else if (z >= 0) v = (T_(i - 2) + 2 * T_(i - 1) + T_(i) + 2) >> 2;
+                else if (z == -1) v = (L_(0) + 2 * E[0] + T_(0) + 2) >> 2;
+                else v = (L_(y - 2 * x - 1) + 2 * L_(y - 2 * x - 2) + L_(y - 2 * x - 3) + 2) >> 2;
+                break;
+            }
+            case 6: {
+                const int z = 2 * y - x, j = y - (x >> 1);
+                if (z >= 0 && (z & 1) == 0) v = (L_(j - 1) + L_(j) + 1) >> 1;
+                else if (z >= 0) v = (L_(j - 2) + 2 * L_(j - 1) + L_(j) + 2) >> 2;
+                else if (z == -1) v = (L_(0) + 2 * E[0] + T_(0) + 2) >> 2;
+                else v = (T_(x - 2 * y - 1) + 2 * T_(x - 2 * y - 2) + T_(x - 2 * y - 3) + 2) >> 2;
+                break;
+            }
+            case 7: {
+                const int i = x + (y >> 1);
+                v = (y & 1) == 0 ? (T_(i) + T_(i + 1) + 1) >> 1 : (T_(i) + 2 * T_(i + 1) + T_(i + 2) + 2) >> 2;
+                break;
+            }
+            default: {
+                const int z = x + 2 * y, j = y + (x >> 1);
+                if (z > 5) v = L_(3);
+                else if (z == 5) v = (L_(2) + 3 * L_(3) + 2) >> 2;
+                else if ((z & 1) == 0) v = (L_(j) + L_(j + 1) + 1) >> 1;
+                else v = (L_(j) + 2 * L_(j + 1) + L_(j + 2) + 2) >> 2;
+                break;
+            }
+            }
+            out[y * 4 + x] = v;
+        }
+#undef T_
+#undef L_
+}
+
+// The Intra16x16 prediction of sample (x, y) (predict_16x16, h264/intra.rs:161-209): dcv the DC value, (pa,
+// pb, pc) the plane parameters.
+template <class T>
+__device__ __forceinline__ int i16_sample(const DecideSmem<T>& S, int mode, int x, int y, int dcv, int pa, int pb, int pc, int maxv) {
+    if (mode == 0) return S.top[1 + x];
+    if (mode == 1) return S.left[y];
+    if (mode == 2) return dcv;
+    return min(max((pa + pb * (x - 7) + pc * (y - 7) + 16) >> 5, 0), maxv);
+}
+
+// The DC value and plane parameters of the Intra16x16 prediction from the neighbours in S.
+template <class T>
+__device__ __forceinline__ void i16_params(const DecideSmem<T>& S, bool ta, bool la, int bd, int* dcv, int* pa, int* pb, int* pc) {
+    int st = 0, sl = 0, h = 0, v = 0;
+#pragma unroll
+    for (int i = 0; i < 16; i++) {
+        st += S.top[1 + i];
+        sl += S.left[i];
+    }
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        h += (k + 1) * (S.top[1 + 8 + k] - S.top[1 + 6 - k]);  // top[-1] is the top-left sample (S.top[0])
+        v += (k + 1) * (S.left[8 + k] - (6 - k < 0 ? S.top[0] : S.left[6 - k]));
+    }
+    *dcv = (ta && la) ? (st + sl + 16) >> 5 : (la ? (sl + 8) >> 4 : (ta ? (st + 8) >> 4 : 1 << (bd - 1)));
+    *pa = 16 * (S.left[15] + S.top[16]);
+    *pb = (5 * h + 32) >> 6;
+    *pc = (5 * v + 32) >> 6;
+}
+
+// The chroma prediction of sample (x, y) of component cc (predict_chroma, h264/intra.rs:212-287, 8x8).
+template <class T>
+__device__ __forceinline__ int chroma_sample(const DecideSmem<T>& S, int mode, int cc, int x, int y, bool ta, bool la, int bd) {
+    if (mode == 1) return S.cleft[cc][y];
+    if (mode == 2) return S.ctop[cc][1 + x];
+    if (mode == 3) {
+        int hh = 0, vv = 0;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            hh += (k + 1) * (S.ctop[cc][1 + 4 + k] - S.ctop[cc][1 + 2 - k]);
+            vv += (k + 1) * (S.cleft[cc][4 + k] - (2 - k < 0 ? S.ctop[cc][0] : S.cleft[cc][2 - k]));
+        }
+        const int a = 16 * (S.cleft[cc][7] + S.ctop[cc][8]), b = (34 * hh + 32) >> 6, c = (34 * vv + 32) >> 6;
+        return min(max((a + b * (x - 3) + c * (y - 3) + 16) >> 5, 0), (1 << bd) - 1);
+    }
+    const int bx = x >> 2, by = y >> 2, mid = 1 << (bd - 1);
+    const int st = S.ctop[cc][1 + bx * 4] + S.ctop[cc][2 + bx * 4] + S.ctop[cc][3 + bx * 4] + S.ctop[cc][4 + bx * 4];
+    const int sl = S.cleft[cc][by * 4] + S.cleft[cc][by * 4 + 1] + S.cleft[cc][by * 4 + 2] + S.cleft[cc][by * 4 + 3];
+    if (bx == by) return (ta && la) ? (st + sl + 4) >> 3 : (la ? (sl + 2) >> 2 : (ta ? (st + 2) >> 2 : mid));
+    if (bx > 0) return ta ? (st + 2) >> 2 : (la ? (sl + 2) >> 2 : mid);
+    return la ? (sl + 2) >> 2 : (ta ? (st + 2) >> 2 : mid);
+}
+
+// Loads the reconstructed samples around the macroblock (luma row above with the top-left and top-right
+// samples, luma column to the left, the same for both chroma components) and the neighbours' Intra4x4 modes.
+template <class T>
+__device__ void load_intra_neighbours(const DecideParams& P, DecideSmem<T>& S, int mb, int mbx, int mby, bool ta, bool la, bool tra) {
+    const int lane = threadIdx.x & 31;
+    const CodeParams& C = P.C;
+    const T* Y = reinterpret_cast<const T*>(C.rec[0]);
+    const int x0 = mbx * 16, y0 = mby * 16;
+    if (lane < 21) {
+        const int x = lane - 1;
+        const bool ok = x < 0 ? (ta && la) : (x < 16 ? ta : tra);
+        S.top[lane] = ok ? (int)Y[(size_t)(y0 - 1) * C.ys + x0 + x] : 0;
+    }
+    if (lane < 16) S.left[lane] = la ? (int)Y[(size_t)(y0 + lane) * C.ys + x0 - 1] : 0;
+    const int cx0 = mbx * 8, cy0 = mby * 8;
+    if (lane < 18) {
+        const int cc = lane / 9, x = lane % 9 - 1;
+        const T* Cp = reinterpret_cast<const T*>(C.rec[1 + cc]);
+        const bool ok = x < 0 ? (ta && la) : ta;
+        S.ctop[cc][x + 1] = ok ? (int)Cp[(size_t)(cy0 - 1) * C.cs + cx0 + x] : 0;
+    }
+    if (lane >= 16) {
+        const int cc = (lane - 16) >> 3, y = lane & 7;
+        const T* Cp = reinterpret_cast<const T*>(C.rec[1 + cc]);
+        S.cleft[cc][y] = la ? (int)Cp[(size_t)(cy0 + y) * C.cs + cx0 - 1] : 0;
+    }
+    if (lane < 8) {
+        // pred_i4_mode's neighbours (enc/frame.rs:619-629): not Intra4x4 counts as DC
+        const bool left = lane < 4;
+        const bool ok = left ? la : ta;
+        int m = -1;
+        if (ok) {
+            const ironav_mbcode* n = &P.codes[left ? mb - 1 : mb - C.A.mb_w];
+            m = n->kind == KIND_I4 ? (int)n->modes[left ? lane * 4 + 3 : 12 + (lane - 4)] : 2;
+        }
+        S.nbm[lane] = m;
+    }
+    __syncwarp();
+}
+
+// best_i16, enc/frame.rs:812-835: the cheapest Intra16x16 mode by SATD + lambda (modes other than DC);
+// returns (mode, cost) on every lane.
+template <class T>
+__device__ int2 best_i16_d(const DecideParams& P, DecideSmem<T>& S, bool ta, bool la) {
+    const int lane = threadIdx.x & 31;
+    const int bd = P.C.bd, maxv = (1 << bd) - 1;
+    int dcv, pa, pb, pc;
+    i16_params(S, ta, la, bd, &dcv, &pa, &pb, &pc);
+    const int b = lane & 15, bx = b & 3, by = b >> 2, half = lane >> 4;
+    int sums[2];
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+        const int mode = half + 2 * q;  // lanes 0-15: modes 0 and 2; lanes 16-31: modes 1 and 3
+        int d[16];
+#pragma unroll
+        for (int r = 0; r < 4; r++)
+#pragma unroll
+            for (int k = 0; k < 4; k++)
+                d[r * 4 + k] = src_at(S.a, bx * 4 + k, by * 4 + r) - i16_sample(S, mode, bx * 4 + k, by * 4 + r, dcv, pa, pb, pc, maxv);
+        int s = satd4_d(d);
+#pragma unroll
+        for (int off = 8; off >= 1; off >>= 1) s += __shfl_xor_sync(FULL, s, off);
+        sums[q] = s;
+    }
+    const int c0 = __shfl_sync(FULL, sums[0], 0), c2 = __shfl_sync(FULL, sums[1], 0);
+    const int c1 = __shfl_sync(FULL, sums[0], 16), c3 = __shfl_sync(FULL, sums[1], 16);
+    const int lam = P.C.A.lambda;
+    int bm = 2, bc = BIG;
+    if (ta && c0 + lam < bc) bm = 0, bc = c0 + lam;
+    if (la && c1 + lam < bc) bm = 1, bc = c1 + lam;
+    if (c2 < bc) bm = 2, bc = c2;
+    if (ta && la && c3 + lam < bc) bm = 3, bc = c3 + lam;
+    return make_int2(bm, bc);
+}
+
+__device__ __forceinline__ int zorder_d(int bx, int by) { return ((by >> 1) << 3) | ((bx >> 1) << 2) | ((by & 1) << 1) | (bx & 1); }
+
+// code_i4, enc/frame.rs:1050-1138, as a trial: block by block in decoding order, each predicted from the
+// reconstruction so far (S.i4rec inside the macroblock, the neighbours' around it), its mode the cheapest
+// by SATD + lambda * (1 for the predicted mode, 4 otherwise), coded with the intra rounding and
+// reconstructed into S.i4rec. Returns the summed cost (every lane).
+template <class T>
+__device__ int code_i4_trial(const DecideParams& P, DecideSmem<T>& S, bool ta, bool la, bool tra) {
+    const int lane = threadIdx.x & 31;
+    const int bd = P.C.bd, maxv = (1 << bd) - 1, lam = P.C.A.lambda;
+    const int qp = P.C.qp + 6 * (bd - 8), m6 = qp % 6, qbits = 15 + qp / 6, f = (1 << qbits) / 3;
+    const bool tla = ta && la;
+    if (lane < 16) S.i4modes[lane] = 2;
+    __syncwarp();
+    int total = 0;
+    for (int n = 0; n < 16; n++) {
+        const int bx = ((n >> 2) & 1) * 2 + (n & 1), by = ((n >> 3) & 1) * 2 + ((n >> 1) & 1);  // block_pos, 108-110
+        const bool hl = bx > 0 || la, ht = by > 0 || ta;
+        const bool htl = bx > 0 ? (by > 0 ? true : ta) : (by > 0 ? la : tla);
+        // above-right: the macroblocks above for the top row, else a block decoded earlier (zorder, 2363-2365)
+        const bool htr = by == 0 ? (bx < 3 ? ta : tra) : (bx == 3 ? false : zorder_d(bx + 1, by - 1) < zorder_d(bx, by));
+        if (lane < 13) {
+            int v = 0;
+            if (lane == 0) {
+                if (htl) v = by == 0 ? S.top[bx * 4] : (bx == 0 ? S.left[by * 4 - 1] : S.i4rec[(by * 4 - 1) * 16 + bx * 4 - 1]);
+            } else if (lane < 9) {
+                const int i = lane - 1;
+                const bool avail = ht && (i < 4 || htr);
+                const int xi = avail ? i : 3;  // above-right not available: the last sample above repeated
+                if (ht) v = by == 0 ? S.top[1 + bx * 4 + xi] : S.i4rec[(by * 4 - 1) * 16 + bx * 4 + xi];
+            } else {
+                const int j = lane - 9;
+                if (hl) v = bx == 0 ? S.left[by * 4 + j] : S.i4rec[(by * 4 + j) * 16 + bx * 4 - 1];
+            }
+            S.edge[lane] = v;
+        }
+        __syncwarp();
+        // pred_i4_mode, enc/frame.rs:619-629
+        const int a = bx > 0 ? S.i4modes[by * 4 + bx - 1] : S.nbm[by];
+        const int b = by > 0 ? S.i4modes[(by - 1) * 4 + bx] : S.nbm[4 + bx];
+        const int predicted = (a >= 0 && b >= 0) ? min(a, b) : 2;
+        int pr[16];
+        unsigned key = 0xffffffffu;
+        if (lane < 9) {
+            const int mode = lane;
+            const bool ok = (mode == 0 || mode == 3 || mode == 7) ? ht : ((mode == 1 || mode == 8) ? hl : (mode == 2 ? true : (ht && hl && htl)));
+            if (ok) {
+                i_pred4_d(mode, S.edge, ht, hl, bd, pr);
+                int d[16];
+#pragma unroll
+                for (int r = 0; r < 4; r++)
+#pragma unroll
+                    for (int k = 0; k < 4; k++) d[r * 4 + k] = src_at(S.a, bx * 4 + k, by * 4 + r) - pr[r * 4 + k];
+                const int cost = satd4_d(d) + lam * (mode == predicted ? 1 : 4);
+                key = ((unsigned)cost << 4) | (unsigned)mode;  // the cheapest, the lowest mode on ties
+            }
+        }
+#pragma unroll
+        for (int off = 16; off >= 1; off >>= 1) key = min(key, __shfl_xor_sync(FULL, key, off));
+        const int bm = (int)(key & 15u);
+        total += (int)(key >> 4);
+        if (lane == bm) {
+            // quant_block (intra), enc/frame.rs:1025-1046, then the reconstruction
+            int d[16], c[16], co[16];
+#pragma unroll
+            for (int r = 0; r < 4; r++)
+#pragma unroll
+                for (int k = 0; k < 4; k++) d[r * 4 + k] = src_at(S.a, bx * 4 + k, by * 4 + r) - pr[r * 4 + k];
+            q_fdct4_d(d, c);
+            int nz = 0;
+#pragma unroll
+            for (int k = 0; k < 16; k++) {
+                const int pz = zz4_at(k);
+                const int l = q_quant_d(c[pz], c_q_mf[m6][q_class_d(pz)], f, qbits);
+                S.i4lv[by * 4 + bx][k] = (int16_t)l;
+                co[pz] = (l * c_q_v[m6][q_class_d(pz)]) << (qp / 6);
+                nz += l != 0;
+            }
+            int rb[16];
+            if (nz > 0) {
+                q_idct4_d(co, pr, maxv, rb);
+            } else {
+#pragma unroll
+                for (int k = 0; k < 16; k++) rb[k] = pr[k];
+            }
+#pragma unroll
+            for (int r = 0; r < 4; r++)
+#pragma unroll
+                for (int k = 0; k < 4; k++) S.i4rec[(by * 4 + r) * 16 + bx * 4 + k] = rb[r * 4 + k];
+            S.i4nnz[by * 4 + bx] = (uint8_t)nz;
+            S.i4modes[by * 4 + bx] = (uint8_t)bm;
+        }
+        __syncwarp();
+    }
+    return total;
+}
+
+// code_i16, enc/frame.rs:1140-1200: the AC of each 4x4 block (a lane per block), the DC through the
+// Hadamard transform halved and quantised with doubled precision (lane 0), reconstructed as a decoder does.
+// Returns the luma coded block pattern (every lane).
+template <class T>
+__device__ uint32_t code_i16_d(const DecideParams& P, DecideSmem<T>& S, int mbx, int mby, int mode, bool ta, bool la, ironav_mbcode* out) {
+    const int lane = threadIdx.x & 31;
+    const int bd = P.C.bd, maxv = (1 << bd) - 1;
+    const int qp = P.C.qp + 6 * (bd - 8), m6 = qp % 6, sh = qp / 6;
+    int dcv, pa, pb, pc;
+    i16_params(S, ta, la, bd, &dcv, &pa, &pb, &pc);
+    const int bx = lane & 3, by = (lane >> 2) & 3;
+    bool any_ac = false;
+    if (lane < 16) {
+        int d[16], c[16];
+#pragma unroll
+        for (int r = 0; r < 4; r++)
+#pragma unroll
+            for (int k = 0; k < 4; k++)
+                d[r * 4 + k] = src_at(S.a, bx * 4 + k, by * 4 + r) - i16_sample(S, mode, bx * 4 + k, by * 4 + r, dcv, pa, pb, pc, maxv);
+        q_fdct4_d(d, c);
+        const int qbits = 15 + qp / 6, f = (1 << qbits) / 3;
+#pragma unroll
+        for (int k = 0; k < 16; k++) {
+            const int pz = zz4_at(k);
+            const int l = pz != 0 ? q_quant_d(c[pz], c_q_mf[m6][q_class_d(pz)], f, qbits) : 0;
+            S.c.lv4[lane][k] = (int16_t)l;
+            any_ac |= l != 0;
+        }
+        S.dcs[lane] = c[0];
+    }
+    const bool ac = __ballot_sync(FULL, any_ac) != 0;
+    __syncwarp();
+    if (lane == 0) {
+        // hadamard4 (h264/idct.rs:76-95) of the DC coefficients, quantised; then the decoder's inverse
+        int h[16], t[16];
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const int s0 = S.dcs[i * 4] + S.dcs[i * 4 + 1], s1 = S.dcs[i * 4] - S.dcs[i * 4 + 1];
+            const int s2 = S.dcs[i * 4 + 2] + S.dcs[i * 4 + 3], s3 = S.dcs[i * 4 + 2] - S.dcs[i * 4 + 3];
+            t[i * 4] = s0 + s2;
+            t[i * 4 + 1] = s0 - s2;
+            t[i * 4 + 2] = s1 - s3;
+            t[i * 4 + 3] = s1 + s3;
+        }
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const int s0 = t[j] + t[4 + j], s1 = t[j] - t[4 + j], s2 = t[8 + j] + t[12 + j], s3 = t[8 + j] - t[12 + j];
+            h[j] = s0 + s2;
+            h[4 + j] = s0 - s2;
+            h[8 + j] = s1 - s3;
+            h[12 + j] = s1 + s3;
+        }
+        const int qbits = 16 + qp / 6, f = (1 << qbits) / 3;
+        int dl[16];
+#pragma unroll
+        for (int k = 0; k < 16; k++) {
+            const int pz = zz4_at(k);
+            const int l = q_quant_d(h[pz] >> 1, c_q_mf[m6][0], f, qbits);
+            out->dc[k] = (int16_t)l;
+            dl[pz] = l;
+        }
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const int s0 = dl[i * 4] + dl[i * 4 + 1], s1 = dl[i * 4] - dl[i * 4 + 1], s2 = dl[i * 4 + 2] + dl[i * 4 + 3], s3 = dl[i * 4 + 2] - dl[i * 4 + 3];
+            t[i * 4] = s0 + s2;
+            t[i * 4 + 1] = s0 - s2;
+            t[i * 4 + 2] = s1 - s3;
+            t[i * 4 + 3] = s1 + s3;
+        }
+        const int lsd = 16 * c_q_v[m6][0];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const int s0 = t[j] + t[4 + j], s1 = t[j] - t[4 + j], s2 = t[8 + j] + t[12 + j], s3 = t[8 + j] - t[12 + j];
+            const int fv[4] = {s0 + s2, s0 - s2, s1 - s3, s1 + s3};
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+                S.dcs[i * 4 + j] = qp >= 36 ? (fv[i] * lsd) << (qp / 6 - 6) : (fv[i] * lsd + (1 << (5 - qp / 6))) >> (6 - qp / 6);
+        }
+    }
+    __syncwarp();
+    if (lane < 16) {
+        int co[16], p[16], nz = 0, any = 0;
+        uint32_t packed[8];
+#pragma unroll
+        for (int k = 0; k < 16; k++) {
+            const int pz = zz4_at(k);
+            const int l = ac ? S.c.lv4[lane][k] : 0;
+            nz += l != 0;
+            co[pz] = (l * c_q_v[m6][q_class_d(pz)]) << sh;
+            if (k & 1) packed[k >> 1] |= (uint32_t)(l & 0xffff) << 16;
+            else packed[k >> 1] = (uint32_t)(l & 0xffff);
+        }
+        co[0] = S.dcs[lane];
+#pragma unroll
+        for (int k = 0; k < 16; k++) any |= co[k];
+#pragma unroll
+        for (int r = 0; r < 4; r++)
+#pragma unroll
+            for (int k = 0; k < 4; k++) p[r * 4 + k] = i16_sample(S, mode, bx * 4 + k, by * 4 + r, dcv, pa, pb, pc, maxv);
+        int rb[16];
+        if (any) {
+            q_idct4_d(co, p, maxv, rb);
+        } else {
+#pragma unroll
+            for (int k = 0; k < 16; k++) rb[k] = p[k];
+        }
+        T* RY = reinterpret_cast<T*>(P.C.rec[0]);
+#pragma unroll
+        for (int r = 0; r < 4; r++)
+#pragma unroll
+            for (int k = 0; k < 4; k++) RY[(size_t)(mby * 16 + by * 4 + r) * P.C.ys + mbx * 16 + bx * 4 + k] = (T)rb[r * 4 + k];
+        uint32_t* lw = reinterpret_cast<uint32_t*>(out->res.luma[lane]);
+#pragma unroll
+        for (int k = 0; k < 8; k++) lw[k] = packed[k];
+        out->res.nnz[lane] = (uint8_t)nz;
+    }
+    __syncwarp();
+    return ac ? 15u : 0u;
+}
+
+// code_intra_chroma, enc/frame.rs:1807-1854: the chroma mode of least lambda * (1 DC, 3 otherwise) + SATD
+// of both components (a lane per mode, component and 4x4 block), then code_chroma with the intra rounding.
+// Returns the chroma part of the coded block pattern (every lane).
+template <class T>
+__device__ uint32_t code_intra_chroma_d(const DecideParams& P, DecideSmem<T>& S, int mbx, int mby, bool ta, bool la, ironav_mbcode* out) {
+    const int lane = threadIdx.x & 31;
+    const CodeParams& C = P.C;
+    const int mode = lane >> 3, cc = (lane >> 2) & 1, blk = lane & 3, bx = blk & 1, by = blk >> 1;
+    const T* SC = reinterpret_cast<const T*>(C.src_c) + (size_t)cc * C.cw * C.ch;
+    int pr[16], d[16];
+#pragma unroll
+    for (int r = 0; r < 4; r++)
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            pr[r * 4 + k] = chroma_sample(S, mode, cc, bx * 4 + k, by * 4 + r, ta, la, C.bd);
+            d[r * 4 + k] = (int)SC[(size_t)(mby * 8 + by * 4 + r) * C.cw + mbx * 8 + bx * 4 + k] - pr[r * 4 + k];
+        }
+    int s = satd4_d(d);
+#pragma unroll
+    for (int off = 4; off >= 1; off >>= 1) s += __shfl_xor_sync(FULL, s, off);
+    const int lam = C.A.lambda;
+    int bm = 0, bc = BIG;
+#pragma unroll
+    for (int m = 0; m < 4; m++) {
+        const int cm = __shfl_sync(FULL, s, m * 8) + lam * (m == 0 ? 1 : 3);
+        const bool ok = m == 0 || (m == 1 && la) || (m == 2 && ta) || (m == 3 && la && ta);
+        if (ok && cm < bc) bm = m, bc = cm;
+    }
+    if (mode == bm) {
+#pragma unroll
+        for (int r = 0; r < 4; r++)
+#pragma unroll
+            for (int k = 0; k < 4; k++) S.c.cpred[cc][(by * 4 + r) * 8 + bx * 4 + k] = pr[r * 4 + k];
+    }
+    if (lane == 0) out->chroma_mode = (uint8_t)bm;
+    __syncwarp();
+    return code_chroma_mb<T>(C, S.c, mbx, mby, &out->res, true);
+}
+
+// The rectangle (x, y, w, h in 4x4 blocks) of partition n of rects(part, sub) in coding order
+// (enc/frame.rs:208-223), and its reference index slot (ref_of).
+__device__ __forceinline__ int4 rect_n(int part, const uint8_t* sub, int n, int* rslot) {
+    if (part < 3) {
+        *rslot = part == 0 ? 0 : n;
+        return make_int4(c_parts[part][n][0], c_parts[part][n][1], c_parts[part][n][2], c_parts[part][n][3]);
+    }
+    int k = 0;
+    while (n >= c_nsub[sub[k]]) n -= c_nsub[sub[k++]];
+    *rslot = k;
+    const int s = sub[k];
+    return make_int4((k & 1) * 2 + c_sub[s][n][0], (k >> 1) * 2 + c_sub[s][n][1], c_sub[s][n][2], c_sub[s][n][3]);
+}
+
+// part_mvps, enc/frame.rs:579-594: each partition's predictor with the partitions before it in place; writes
+// the differences (every vector less its predictor; beyond the partitions, the vector itself) and the
+// macroblock's state.
+template <class T>
+__device__ void inter_tail(const DecideParams& P, DecideSmem<T>& S, const ironav_interdec& D, ironav_mbcode* out) {
+    const int lane = threadIdx.x & 31;
+    const AnalyseParams& A = P.C.A;
+    const int part = D.part;
+    const int count = part == 0 ? 1 : (part < 3 ? 2 : c_nsub[D.sub[0]] + c_nsub[D.sub[1]] + c_nsub[D.sub[2]] + c_nsub[D.sub[3]]);
+    const int dir = part == 1 ? 1 : (part == 2 ? 2 : 0);
+    if (lane < 16) S.a.t[lane] = make_int4(0, 0, -1, 0);
+    if (lane >= count && lane < 16) {
+        out->mvds[lane][0] = D.mvs[lane][0];
+        out->mvds[lane][1] = D.mvs[lane][1];
+    }
+    __syncwarp();
+    for (int n = 0; n < count; n++) {
+        int rs;
+        const int4 r = rect_n(part, D.sub, n, &rs);
+        const int rf = D.refs[rs];
+        const int2 p = pred_mv(A, S.a, S.a.ext, S.a.t, r.x, r.y, r.z, dir, rf);
+        if (lane == 0) {
+            out->mvds[n][0] = (int16_t)(D.mvs[n][0] - p.x);
+            out->mvds[n][1] = (int16_t)(D.mvs[n][1] - p.y);
+        }
+        blk_paint(A, S.a, S.a.t, r.x, r.y, r.z, r.w, D.mvs[n][0], D.mvs[n][1], rf);
+    }
+    // the state (finish_mb, enc/frame.rs:2281-2321): the vectors painted over the partitions, the reference
+    // of each 8x8 block
+    if (lane < 16) {
+        const int bx = lane & 3, by = lane >> 2;
+        int n, rs;
+        rect_of(part, D.sub, bx, by, &n, &rs);
+        S.a.out.mvs[lane][0] = D.mvs[n][0];
+        S.a.out.mvs[lane][1] = D.mvs[n][1];
+        if ((bx & 1) == 0 && (by & 1) == 0) S.a.out.refs[(by >> 1) * 2 + (bx >> 1)] = (int8_t)D.refs[rs];
+    }
+    if (lane == 0) {
+        S.a.out.inter = 1;
+        S.a.out.pad[0] = S.a.out.pad[1] = S.a.out.pad[2] = 0;
+        out->kind = KIND_INTER;
+        out->part = D.part;
+        for (int k = 0; k < 4; k++) {
+            out->sub[k] = D.sub[k];
+            out->refs[k] = D.refs[k];
+        }
+    }
+    if (lane < 16) {
+        out->mvs[lane][0] = D.mvs[lane][0];
+        out->mvs[lane][1] = D.mvs[lane][1];
+    }
+    __syncwarp();
+}
+
+// code_mb for one P macroblock without CABAC, enc/frame.rs:715-790.
+template <class T>
+__device__ void decide_mb(const DecideParams& P, DecideSmem<T>& S, int mb, int mbx, int mby) {
+    const int lane = threadIdx.x & 31;
+    const AnalyseParams& A = P.C.A;
+    const CodeParams& C = P.C;
+    const int lam = A.lambda, x0 = mbx * 16, y0 = mby * 16;
+    const bool ta = mby > A.band_start[mby], la = mbx > 0, tra = ta && mbx + 1 < A.mb_w;
+    ironav_mbcode* out = &P.codes[mb];
+    // the code starts as MbCode::new: zero, Intra4x4 modes 2
+    {
+        uint32_t* w = reinterpret_cast<uint32_t*>(out);
+        for (int k = lane; k < (int)(sizeof(ironav_mbcode) / 4); k += 32) w[k] = (k >= 371 && k < 375) ? 0x02020202u : 0u;
+    }
+    stage_source(A, S.a);
+    __syncwarp();
+    // P_Skip first (722-751)
+    const int2 sv = skip_mv(A, S.a);
+    if (lane == 0) S.a.cand[0] = sv;
+    __syncwarp();
+    pred_batch(A, S.a, 0, 0, 0, 2, 2, 1, true);
+    const int sad = S.a.cost[0];
+    __syncwarp();
+    ironav_interdec& D = *reinterpret_cast<ironav_interdec*>(S.c.dec);
+    // the skip vector's decision: 16x16 from reference 0
+    if (lane == 0) {
+        D.mode = 2;
+        D.part = 0;
+        D.t8 = 0;
+        for (int k = 0; k < 4; k++) D.sub[k] = D.refs[k] = 0;
+        D.pad[0] = D.pad[1] = D.pad[2] = 0;
+    }
+    if (lane < 16) {
+        D.mvs[lane][0] = (int16_t)sv.x;
+        D.mvs[lane][1] = (int16_t)sv.y;
+    }
+    __syncwarp();
+    if (A.fast && sad < P.fast_t) {
+        // close to the reference: P_Skip when the chroma is too, nothing transformed
+        if (lane == 0) D.mode = 1;
+        __syncwarp();
+        for (int i = lane; i < 128; i += 32) {
+            const int cc = i >> 6, cy = (i >> 3) & 7, cx = i & 7;
+            const T* rc = reinterpret_cast<const T*>(C.ref_c[0]) + (size_t)cc * C.cw * C.ch;
+            const int fx = sv.x & 7, fy = sv.y & 7;
+            const int xs = mbx * 8 + cx + (sv.x >> 3), ysm = mby * 8 + cy + (sv.y >> 3);
+            const int xa = min(max(xs, 0), C.cw - 1), xb = min(max(xs + 1, 0), C.cw - 1);
+            const int ya = min(max(ysm, 0), C.ch - 1), yb = min(max(ysm + 1, 0), C.ch - 1);
+            const int v = ((8 - fx) * (8 - fy) * rc[(size_t)ya * C.cw + xa] + fx * (8 - fy) * rc[(size_t)ya * C.cw + xb] +
+                           (8 - fx) * fy * rc[(size_t)yb * C.cw + xa] + fx * fy * rc[(size_t)yb * C.cw + xb] + 32) >> 6;
+            const T* SC = reinterpret_cast<const T*>(C.src_c) + (size_t)cc * C.cw * C.ch;
+            S.c.cpred[cc][cy * 8 + cx] = abs((int)SC[(size_t)(mby * 8 + cy) * C.cw + mbx * 8 + cx] - v);
+        }
+        __syncwarp();
+        int csad = 0;
+        for (int i = lane; i < 128; i += 32) csad += S.c.cpred[i >> 6][i & 63];
+#pragma unroll
+        for (int off = 16; off >= 1; off >>= 1) csad += __shfl_xor_sync(FULL, csad, off);
+        __syncwarp();
+        if (csad < P.fast_tc) {
+            // put_pred (1397-1403): code_inter_mb with a P_Skip decision writes exactly the prediction
+            code_inter_mb<T>(C, S.c, mb, &out->res);
+            if (lane == 0) out->skip = 1;
+            D.mode = 2;
+            inter_tail(P, S, D, out);
+            if (lane < 16) out->mvds[lane][0] = out->mvds[lane][1] = 0;  // a P_Skip code carries no differences
+            return;
+        }
+        if (lane == 0) D.mode = 2;
+        __syncwarp();
+    }
+    if (sad < A.skip_thresh) {
+        const uint32_t cbp = code_inter_mb<T>(C, S.c, mb, &out->res);
+        if (cbp == 0) {
+            inter_tail(P, S, D, out);
+            if (lane == 0) out->skip = 1;
+            return;
+        }
+    }
+    load_intra_neighbours(P, S, mb, mbx, mby, ta, la, tra);
+    const int2 i16 = best_i16_d(P, S, ta, la);
+    int best_intra = i16.y + lam * 4;
+    // best_inter, enc/frame.rs:839-849
+    int part = 0, cost = 0, bestr = 0;
+    uint32_t sub = 0;
+    for (int r = 0; r < A.nact; r++) {
+        const int4 bi = best_inter_ref(A, S.a, r);
+        if (r == 0 || bi.x < cost) {
+            part = bi.y;
+            cost = bi.x;
+            bestr = r;
+            sub = (uint32_t)bi.z;
+            if (lane < 16) {
+                S.a.win_mvs[lane][0] = S.a.best_mvs[lane][0];
+                S.a.win_mvs[lane][1] = S.a.best_mvs[lane][1];
+            }
+            __syncwarp();
+        }
+    }
+    // Intra4x4 is tried by coding it when intra is competitive (766-779)
+    bool i4 = false;
+    if (best_intra < cost) {
+        const int c4 = code_i4_trial(P, S, ta, la, tra) + lam * 6;
+        if (c4 < best_intra) {
+            best_intra = c4;
+            i4 = true;
+        }
+    }
+    if (cost <= best_intra) {
+        if (lane == 0) {
+            D.mode = 2;
+            D.part = (uint8_t)part;
+            for (int k = 0; k < 4; k++) {
+                D.sub[k] = (uint8_t)((sub >> (8 * k)) & 0xff);
+                D.refs[k] = (uint8_t)bestr;
+            }
+        }
+        if (lane < 16) {
+            D.mvs[lane][0] = S.a.win_mvs[lane][0];
+            D.mvs[lane][1] = S.a.win_mvs[lane][1];
+        }
+        __syncwarp();
+        const uint32_t cbp = code_inter_mb<T>(C, S.c, mb, &out->res);
+        inter_tail(P, S, D, out);
+        if (lane == 0 && cbp == 0 && part == 0 && D.mvs[0][0] == sv.x && D.mvs[0][1] == sv.y && bestr == 0) out->skip = 1;
+        return;
+    }
+    uint32_t cbp;
+    if (i4) {
+        T* RY = reinterpret_cast<T*>(C.rec[0]);
+        for (int i = lane; i < 256; i += 32) RY[(size_t)(y0 + (i >> 4)) * C.ys + x0 + (i & 15)] = (T)S.i4rec[i];
+        if (lane < 16) {
+            uint32_t* lw = reinterpret_cast<uint32_t*>(out->res.luma[lane]);
+            const uint32_t* src = reinterpret_cast<const uint32_t*>(S.i4lv[lane]);
+#pragma unroll
+            for (int k = 0; k < 8; k++) lw[k] = src[k];
+            out->res.nnz[lane] = S.i4nnz[lane];
+            out->modes[lane] = S.i4modes[lane];
+        }
+        const bool coded = lane < 16 && S.i4nnz[lane] > 0;
+        const unsigned bal = __ballot_sync(FULL, coded);
+        cbp = 0;
+#pragma unroll
+        for (int i8 = 0; i8 < 4; i8++) {
+            const unsigned mask = 0x33u << ((i8 >> 1) * 8 + (i8 & 1) * 2);
+            if (bal & mask) cbp |= 1u << i8;
+        }
+        if (lane == 0) out->kind = KIND_I4;
+    } else {
+        cbp = code_i16_d(P, S, mbx, mby, i16.x, ta, la, out);
+        if (lane == 0) {
+            out->kind = KIND_I16;
+            out->i16_mode = (uint8_t)i16.x;
+        }
+    }
+    cbp |= code_intra_chroma_d(P, S, mbx, mby, ta, la, out);
+    if (lane == 0) out->res.cbp = (uint8_t)cbp;
+    // the state of an intra macroblock: no motion
+    if (lane < 16) S.a.out.mvs[lane][0] = S.a.out.mvs[lane][1] = 0;
+    if (lane == 0) {
+        S.a.out.inter = 0;
+        for (int k = 0; k < 4; k++) S.a.out.refs[k] = -1;
+        S.a.out.pad[0] = S.a.out.pad[1] = S.a.out.pad[2] = 0;
+    }
+    __syncwarp();
+}
+
+template <class T>
+__global__ void __launch_bounds__(K7_WARPS * 32, K7_MIN_BLOCKS) decide_kernel(const __grid_constant__ DecideParams P) {
+    __shared__ DecideSmem<T> smem[K7_WARPS];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    DecideSmem<T>& S = smem[wid];
+    const AnalyseParams& A = P.C.A;
+    for (;;) {
+        unsigned t = 0;
+        if (lane == 0) t = atomicAdd(A.ticket, 1u);
+        t = __shfl_sync(FULL, t, 0);
+        if (t >= (unsigned)A.nmb) break;
+        const int mb = A.order[t];
+        const int mbx = mb % A.mb_w, mby = mb / A.mb_w;
+        if (lane == 0) {
+            S.a.mb = mb;
+            S.a.mbx = mbx;
+            S.a.mby = mby;
+        }
+        __syncwarp();
+        // the left and top-right (top at the right edge) neighbours; their own waits cover the rest
+        const int start = A.band_start[mby];
+        const int m1 = mb - 1, m2 = (mbx + 1 < A.mb_w) ? mb - A.mb_w + 1 : mb - A.mb_w;
+        bool ok = true;
+        if (mbx > 0) ok = wait_published(A, m1);
+        if (ok && mby > start) ok = wait_published(A, m2);
+        ok = __all_sync(FULL, ok);
+        if (!ok) break;
+        load_neighbours(A, S.a, A.states_out);
+        decide_mb<T>(P, S, mb, mbx, mby);
+        if (lane < 18) reinterpret_cast<uint32_t*>(&A.states_out[mb])[lane] = reinterpret_cast<const uint32_t*>(&S.a.out)[lane];
+        // the reconstruction, code and state before the flag
+        __threadfence();
+        __syncwarp();
+        if (lane == 0 && mb != A.withhold) st_release(&A.flags[mb], A.epoch);
+    }
+}
+
+}  // namespace ironav

@@ -22,6 +22,7 @@
 #include "scene.cuh"
 #include "deblock.cuh"
 #include "residual.cuh"
+#include "decide.cuh"
 
 using namespace ironav;
 
@@ -32,6 +33,7 @@ static_assert(sizeof(ironav_mbstate_b) == 140, "ironav_mbstate_b layout");
 static_assert(sizeof(ironav_bresult) == 200, "ironav_bresult layout");
 static_assert(sizeof(ironav_interdec) == 78, "ironav_interdec layout");
 static_assert(sizeof(ironav_intercode) == 1324, "ironav_intercode layout");
+static_assert(sizeof(ironav_mbcode) == 1516 && offsetof(ironav_mbcode, kind) == 1500 && offsetof(ironav_mbcode, modes) == 1484, "ironav_mbcode layout");
 static_assert(sizeof(ironav_dbk_slice) == 20, "ironav_dbk_slice layout");
 
 // The reference slot for a new picture: the oldest one's once max_refs are held, else a free one; the
@@ -122,6 +124,7 @@ void free_ctx(ironav_ctx* c) {
     cudaFree(c->d_decs);
     cudaFree(c->d_codes);
     cudaFree(c->d_rec);
+    cudaFree(c->d_mbcodes);
     cudaFreeHost(c->h_results);
     cudaFreeHost(c->h_done);
     cudaFreeHost(c->h_committed);
@@ -735,6 +738,87 @@ int ironav_code_inter_picture(ironav_ctx* c, int qp, const ironav_interdec* decs
     int s = launch_code_inter(c, qp, c->d_decs, c->d_codes, dy, (int)pw, dcb, dcr, (int)(pw / 2));
     if (s != IRONAV_OK) return s;
     CK(cudaMemcpyAsync(codes, c->d_codes, sizeof(ironav_intercode) * c->nmb, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpy2DAsync(y, (size_t)ys * B, dy, pw * B, pw * B, ph, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpy2DAsync(cb, (size_t)cs * B, dcb, pw / 2 * B, pw / 2 * B, ph / 2, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpy2DAsync(cr, (size_t)cs * B, dcr, pw / 2 * B, pw / 2 * B, ph / 2, cudaMemcpyDeviceToHost, c->stream));
+    return check_device_error(c);
+}
+
+// ---- decide mode ------------------------------------------------------------------------------------
+
+// The fast mode's P_Skip tests `sad < 256 * 0.05 * step` and `csad < 128 * 0.05 * step` with step =
+// 2^(QP'/6) (enc/frame.rs:735,740), as integer bounds like ironav_skip_threshold.
+static void fast_thresholds(int qpp, int* luma, int* chroma) {
+    const double step = std::pow(2.0, (double)qpp / 6.0);
+    *luma = (int)std::ceil(256.0 * 0.05 * step);
+    *chroma = (int)std::ceil(128.0 * 0.05 * step);
+}
+
+static int launch_decide(ironav_ctx* c, ironav_mbstate* d_states, ironav_mbcode* d_codes, void* y, int ys, void* cb, void* cr, int cs) {
+    if (!c->have_params || c->nact < 1 || c->nact > c->nrefs || !c->d_src_c) return IRONAV_INVALID_ARGUMENT;
+    for (int i = 0; i < c->nact; i++)
+        if (!c->ref_c_ok[c->slot_of[i]]) return IRONAV_INVALID_ARGUMENT;  // an active reference without chroma
+    if (!c->k7_blocks) {
+        int per_sm = 0;
+        const cudaError_t e = c->bd > 8 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, decide_kernel<uint16_t>, K7_WARPS * 32, 0)
+                                        : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, decide_kernel<uint8_t>, K7_WARPS * 32, 0);
+        if (e != cudaSuccess) return cuda_status(e);
+        c->k7_blocks = std::max(1, per_sm) * c->nsm;
+    }
+    DecideParams p;
+    memset(&p, 0, sizeof(p));
+    fill_params(c, p.C.A);
+    AnalyseParams& A = p.C.A;
+    A.states_out = d_states;
+    A.order = c->d_order;
+    A.ticket = c->d_counters;
+    A.flags = c->d_flags;
+    A.err = c->d_counters + 1;
+    A.nmb = c->nmb;
+    A.withhold = c->withhold;
+    A.epoch = ++c->epoch;
+    for (int i = 0; i < c->nact; i++) p.C.ref_c[i] = c->d_ref_c[c->slot_of[i]];
+    p.C.src_c = c->d_src_c;
+    p.C.cw = c->mb_w * 8;
+    p.C.ch = c->mb_h * 8;
+    p.C.rec[0] = static_cast<uint8_t*>(y);
+    p.C.rec[1] = static_cast<uint8_t*>(cb);
+    p.C.rec[2] = static_cast<uint8_t*>(cr);
+    p.C.ys = ys;
+    p.C.cs = cs;
+    p.C.qp = c->qpp - 6 * (c->bd - 8);
+    p.C.bd = c->bd;
+    p.C.nrefs = c->nact;
+    p.C.err = c->d_counters + 1;
+    p.codes = d_codes;
+    fast_thresholds(c->qpp, &p.fast_t, &p.fast_tc);
+    CK(cudaMemsetAsync(c->d_counters, 0, 2 * sizeof(unsigned), c->stream));
+    if (c->bd > 8) decide_kernel<uint16_t><<<c->k7_blocks, K7_WARPS * 32, 0, c->stream>>>(p);
+    else decide_kernel<uint8_t><<<c->k7_blocks, K7_WARPS * 32, 0, c->stream>>>(p);
+    return cuda_status(cudaGetLastError());
+}
+
+int ironav_decide_p_picture_device(ironav_ctx* c, ironav_mbstate* d_states, ironav_mbcode* d_codes, void* y, int ys, void* cb, void* cr, int cs) {
+    if (!c || !d_states || !d_codes || !y || !cb || !cr || ys < c->pw || cs < c->pw / 2) return IRONAV_INVALID_ARGUMENT;
+    // the planes as the deblocking filter's device form; states and codes are written as 32-bit words
+    const uintptr_t a = reinterpret_cast<uintptr_t>(y) | reinterpret_cast<uintptr_t>(cb) | reinterpret_cast<uintptr_t>(cr);
+    if ((a & 15) || ((size_t)ys * sample_bytes(c)) % 16 || cs % 8) return IRONAV_INVALID_ARGUMENT;
+    if ((reinterpret_cast<uintptr_t>(d_states) | reinterpret_cast<uintptr_t>(d_codes)) & 3) return IRONAV_INVALID_ARGUMENT;
+    return launch_decide(c, d_states, d_codes, y, ys, cb, cr, cs);
+}
+
+int ironav_decide_p_picture(ironav_ctx* c, ironav_mbstate* states, ironav_mbcode* codes, void* y, int ys, void* cb, void* cr, int cs) {
+    if (!c || !states || !codes || !y || !cb || !cr || ys < c->pw || cs < c->pw / 2) return IRONAV_INVALID_ARGUMENT;
+    const size_t B = (size_t)sample_bytes(c), pw = (size_t)c->pw, ph = (size_t)c->ph;
+    if (!c->d_mbcodes) CK(cudaMalloc(&c->d_mbcodes, sizeof(ironav_mbcode) * c->nmb));
+    if (!c->d_rec) CK(cudaMalloc(&c->d_rec, (pw * ph + 2 * (pw / 2) * (ph / 2)) * B));
+    uint8_t* dy = c->d_rec;
+    uint8_t* dcb = dy + pw * ph * B;
+    uint8_t* dcr = dcb + (pw / 2) * (ph / 2) * B;
+    int s = launch_decide(c, c->d_states, c->d_mbcodes, dy, (int)pw, dcb, dcr, (int)(pw / 2));
+    if (s != IRONAV_OK) return s;
+    CK(cudaMemcpyAsync(states, c->d_states, sizeof(ironav_mbstate) * c->nmb, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(codes, c->d_mbcodes, sizeof(ironav_mbcode) * c->nmb, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaMemcpy2DAsync(y, (size_t)ys * B, dy, pw * B, pw * B, ph, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaMemcpy2DAsync(cb, (size_t)cs * B, dcb, pw / 2 * B, pw / 2 * B, ph / 2, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaMemcpy2DAsync(cr, (size_t)cs * B, dcr, pw / 2 * B, pw / 2 * B, ph / 2, cudaMemcpyDeviceToHost, c->stream));

@@ -209,14 +209,334 @@ __device__ __forceinline__ int4 rect_of(int part, const uint8_t* sub, int bx, in
     return make_int4(ox + lx, oy + ly, 1, 1);
 }
 
+// code_chroma, enc/frame.rs:1856-1915: both chroma components of the macroblock at (mbx, mby) against the
+// prediction in S.cpred, into `out` and the reconstruction, a lane per 4x4 block of Cb (lanes 0-3) and Cr
+// (4-7); the AC levels go to shared memory and come back after the DC transform's shuffles. intra: the
+// intra rounding (f = 1/3) and no AC decimation. Returns the chroma part of the coded block pattern
+// (bits 4-5), on every lane.
+template <class T>
+__device__ __forceinline__ uint32_t code_chroma_mb(const CodeParams& P, CodeSmem& S, int mbx, int mby, ironav_intercode* out, bool intra) {
+    const int lane = threadIdx.x & 31;
+    const int maxv = (1 << P.bd) - 1;
+    int dc = 0, cscore = 0, anyac = 0;
+    const int qpc = dbk_chroma_qp(P.qp, 0, P.bd) + 6 * (P.bd - 8), mc = qpc % 6;
+    const int cc = (lane >> 2) & 1, blk = lane & 3, cbx = blk & 1, cby = blk >> 1;
+    const T* SC = reinterpret_cast<const T*>(P.src_c) + (size_t)cc * P.cw * P.ch;
+    if (lane < 8) {
+        int d[16], c[16];
+#pragma unroll
+        for (int r = 0; r < 4; r++)
+#pragma unroll
+            for (int k = 0; k < 4; k++)
+                d[r * 4 + k] = (int)SC[(size_t)(mby * 8 + cby * 4 + r) * P.cw + mbx * 8 + cbx * 4 + k] - S.cpred[cc][(cby * 4 + r) * 8 + cbx * 4 + k];
+        q_fdct4_d(d, c);
+        const int qbits = 15 + qpc / 6, f = (1 << qbits) / (intra ? 3 : 6);
+#pragma unroll
+        for (int k = 0; k < 16; k++) {
+            const int pz = zz4_at(k);
+            const int l = pz != 0 ? q_quant_d(c[pz], c_q_mf[mc][q_class_d(pz)], f, qbits) : 0;
+            S.cl[cc][blk][k] = (int16_t)l;
+            anyac |= l != 0;
+        }
+        dc = c[0];
+        cscore = q_decimate_d(S.cl[cc][blk], 16);
+    }
+    // the DC transform over a component's 4 blocks (lanes 4cc..4cc+3)
+    const int base = (lane & 4);
+    const int d0 = __shfl_sync(FULL, dc, base), d1 = __shfl_sync(FULL, dc, base + 1), d2 = __shfl_sync(FULL, dc, base + 2),
+              d3 = __shfl_sync(FULL, dc, base + 3);
+    const int fdc = blk == 0 ? d0 + d1 + d2 + d3 : (blk == 1 ? d0 - d1 + d2 - d3 : (blk == 2 ? d0 + d1 - d2 - d3 : d0 - d1 - d2 + d3));
+    const int qbits = 16 + qpc / 6, fr = (1 << qbits) / (intra ? 3 : 6);
+    const int cdc = lane < 8 ? q_quant_d(fdc, c_q_mf[mc][0], fr, qbits) : 0;
+    int acs = lane < 8 ? cscore : 0;
+#pragma unroll
+    for (int off = 16; off >= 1; off >>= 1) acs += __shfl_xor_sync(FULL, acs, off);
+    const bool any_ac = (__ballot_sync(FULL, lane < 8 && anyac) != 0) && (intra || acs >= 7);
+    const bool any_dc = __ballot_sync(FULL, lane < 8 && cdc != 0) != 0;
+    const int cbpc = any_ac ? 2 : (any_dc ? 1 : 0);
+    // the reconstruction: the DC levels' inverse 2x2 transform scaled, the AC as coded
+    const int l0 = __shfl_sync(FULL, cdc, base), l1 = __shfl_sync(FULL, cdc, base + 1), l2 = __shfl_sync(FULL, cdc, base + 2),
+              l3 = __shfl_sync(FULL, cdc, base + 3);
+    const int fl = blk == 0 ? l0 + l1 + l2 + l3 : (blk == 1 ? l0 - l1 + l2 - l3 : (blk == 2 ? l0 + l1 - l2 - l3 : l0 - l1 - l2 + l3));
+    if (lane < 8) {
+        ironav_intercode& O = *out;
+        const int sh = qpc / 6;
+        int cco[16], cp[16], nz = 0, any = 0;
+        uint32_t packed[8];
+#pragma unroll
+        for (int k = 0; k < 16; k++) {
+            const int pz = zz4_at(k);
+            const int l = any_ac ? S.cl[cc][blk][k] : 0;
+            nz += l != 0;
+            cco[pz] = (l * c_q_v[mc][q_class_d(pz)]) << sh;
+            if (k & 1) packed[k >> 1] |= (uint32_t)(l & 0xffff) << 16;
+            else packed[k >> 1] = (uint32_t)(l & 0xffff);
+        }
+        cco[0] = cbpc > 0 ? ((fl * (16 * c_q_v[mc][0])) << sh) >> 5 : 0;
+#pragma unroll
+        for (int k = 0; k < 16; k++) any |= cco[k];
+        uint32_t* aw = reinterpret_cast<uint32_t*>(O.cac[cc][blk]);
+#pragma unroll
+        for (int k = 0; k < 8; k++) aw[k] = packed[k];
+        O.cnnz[cc][blk] = (uint8_t)nz;
+        O.cdc[cc][blk] = (int16_t)cdc;
+#pragma unroll
+        for (int r = 0; r < 4; r++)
+#pragma unroll
+            for (int k = 0; k < 4; k++) cp[r * 4 + k] = S.cpred[cc][(cby * 4 + r) * 8 + cbx * 4 + k];
+        int recb[16];
+        if (any) {
+            q_idct4_d(cco, cp, maxv, recb);
+        } else {
+#pragma unroll
+            for (int k = 0; k < 16; k++) recb[k] = cp[k];
+        }
+        T* RC = reinterpret_cast<T*>(P.rec[1 + cc]);
+#pragma unroll
+        for (int r = 0; r < 4; r++)
+#pragma unroll
+            for (int k = 0; k < 4; k++) RC[(size_t)(mby * 8 + cby * 4 + r) * P.cs + mbx * 8 + cbx * 4 + k] = (T)recb[r * 4 + k];
+    }
+    return (uint32_t)cbpc << 4;
+}
+
+// code_inter / code_inter_residual / code_luma8, enc/frame.rs:1202-1305: the macroblock whose decision
+// (mode 1 P_Skip or 2 coded, validated) is in S.dec, into `out` (zeroed by the caller) and the
+// reconstruction. Returns the coded block pattern, on every lane.
+template <class T>
+__device__ __forceinline__ uint32_t code_inter_mb(const CodeParams& P, CodeSmem& S, int mb, ironav_intercode* out) {
+    const int lane = threadIdx.x & 31;
+    const int maxv = (1 << P.bd) - 1;
+    const int qp = P.qp + 6 * (P.bd - 8);
+    const int mbx = mb % P.A.mb_w, mby = mb / P.A.mb_w, x0 = mbx * 16, y0 = mby * 16;
+    const ironav_interdec& D = *reinterpret_cast<const ironav_interdec*>(S.dec);
+    const int mode = D.mode;
+    // luma prediction, a lane per 4x4 block
+    if (lane < 16) {
+        const int bx = lane & 3, by = lane >> 2;
+        int n, rs;
+        const int4 r = rect_of(D.part, D.sub, bx, by, &n, &rs);
+        const int2 mv = make_int2(D.mvs[n][0], D.mvs[n][1]);
+        uint32_t pr[4][sizeof(T)];
+        pred4<T>(P.A, P.A.planes[D.refs[rs]], x0 + r.x * 4, y0 + r.y * 4, r.z * 4, r.w * 4, bx - r.x, by - r.y, mv, pr);
+#pragma unroll
+        for (int row = 0; row < 4; row++)
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const uint32_t wv = pr[row][(k * (int)sizeof(T)) >> 2];
+                S.pred[(by * 4 + row) * 16 + bx * 4 + k] = (int)((wv >> ((k * 8 * (int)sizeof(T)) & 31)) & (uint32_t)maxv);
+            }
+    }
+    // chroma prediction (chroma_mc from each partition's vector, in eighth samples), 4 samples a lane
+    for (int i = lane; i < 128; i += 32) {
+        const int cc = i >> 6, cy = (i >> 3) & 7, cx = i & 7;
+        int n, rs;
+        const int4 r = rect_of(D.part, D.sub, cx >> 1, cy >> 1, &n, &rs);
+        (void)r;
+        const int mx = D.mvs[n][0], my = D.mvs[n][1];
+        const T* rc = reinterpret_cast<const T*>(P.ref_c[D.refs[rs]]) + (size_t)cc * P.cw * P.ch;
+        const int fx = mx & 7, fy = my & 7;
+        const int xs = mbx * 8 + cx + (mx >> 3), ysm = mby * 8 + cy + (my >> 3);
+        const int xa = min(max(xs, 0), P.cw - 1), xb = min(max(xs + 1, 0), P.cw - 1);
+        const int ya = min(max(ysm, 0), P.ch - 1), yb = min(max(ysm + 1, 0), P.ch - 1);
+        const int A_ = rc[(size_t)ya * P.cw + xa], B_ = rc[(size_t)ya * P.cw + xb], C_ = rc[(size_t)yb * P.cw + xa], D_ = rc[(size_t)yb * P.cw + xb];
+        S.cpred[cc][cy * 8 + cx] = ((8 - fx) * (8 - fy) * A_ + fx * (8 - fy) * B_ + (8 - fx) * fy * C_ + fx * fy * D_ + 32) >> 6;
+    }
+    __syncwarp();
+    T* const RY = reinterpret_cast<T*>(P.rec[0]);
+    const T* const SY = reinterpret_cast<const T*>(P.A.src);
+    uint32_t cbp = 0;
+    if (mode == 1) {
+        // P_Skip: the prediction is the reconstruction
+        for (int i = lane; i < 256; i += 32) RY[(size_t)(y0 + (i >> 4)) * P.ys + x0 + (i & 15)] = (T)S.pred[i];
+    } else if (!D.t8) {
+        // 4x4 transform: a lane per block; the levels go to shared memory and come back after the
+        // decimation sums, so that no 16-entry array stays live across the shuffles
+        int score = 0;
+        const int bx = lane & 3, by = lane >> 2;
+        if (lane < 16) {
+            int d[16], c[16];
+#pragma unroll
+            for (int r = 0; r < 4; r++)
+#pragma unroll
+                for (int k = 0; k < 4; k++)
+                    d[r * 4 + k] = (int)SY[(size_t)(y0 + by * 4 + r) * P.A.ls + x0 + bx * 4 + k] - S.pred[(by * 4 + r) * 16 + bx * 4 + k];
+            q_fdct4_d(d, c);
+            const int qbits = 15 + qp / 6, f = (1 << qbits) / 6, m = qp % 6;
+#pragma unroll
+            for (int k = 0; k < 16; k++) {
+                const int pz = zz4_at(k);
+                S.lv4[lane][k] = (int16_t)q_quant_d(c[pz], c_q_mf[m][q_class_d(pz)], f, qbits);
+            }
+            score = q_decimate_d(S.lv4[lane], 16);
+        }
+        // per 8x8 block: lanes (2i8x, 2i8y) quad sums; blocks b = by*4+bx, 8x8 index (by/2)*2 + bx/2
+        const int i8 = ((lane >> 3) & 1) * 2 + ((lane & 3) >> 1);
+        int s8 = 0, tot = 0;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            int sq = 0;
+#pragma unroll
+            for (int b = 0; b < 16; b++) {
+                const int v = __shfl_sync(FULL, score, b);
+                if (((b >> 3) & 1) * 2 + ((b & 3) >> 1) == q) sq += v;
+            }
+            if (q == i8) s8 = sq;
+            tot += sq;
+        }
+        if (lane < 16) {
+            const bool drop = s8 < 4 || tot < 6;
+            const int m = qp % 6, sh = qp / 6;
+            int co[16], p[16], nz = 0;
+            uint32_t packed[8];
+#pragma unroll
+            for (int k = 0; k < 16; k++) {
+                const int pz = zz4_at(k);
+                const int l = drop ? 0 : S.lv4[lane][k];
+                nz += l != 0;
+                co[pz] = (l * c_q_v[m][q_class_d(pz)]) << sh;
+                if (k & 1) packed[k >> 1] |= (uint32_t)(l & 0xffff) << 16;
+                else packed[k >> 1] = (uint32_t)(l & 0xffff);
+            }
+#pragma unroll
+            for (int r = 0; r < 4; r++)
+#pragma unroll
+                for (int k = 0; k < 4; k++) p[r * 4 + k] = S.pred[(by * 4 + r) * 16 + bx * 4 + k];
+            int recb[16];
+            if (nz > 0) {
+                q_idct4_d(co, p, maxv, recb);
+            } else {
+#pragma unroll
+                for (int k = 0; k < 16; k++) recb[k] = p[k];
+            }
+#pragma unroll
+            for (int r = 0; r < 4; r++)
+#pragma unroll
+                for (int k = 0; k < 4; k++) RY[(size_t)(y0 + by * 4 + r) * P.ys + x0 + bx * 4 + k] = (T)recb[r * 4 + k];
+            ironav_intercode& O = *out;
+            uint32_t* lw = reinterpret_cast<uint32_t*>(O.luma[lane]);
+#pragma unroll
+            for (int k = 0; k < 8; k++) lw[k] = packed[k];
+            O.nnz[lane] = (uint8_t)nz;
+            if (nz > 0) cbp |= 1u << ((by >> 1) * 2 + (bx >> 1));
+        }
+    } else {
+        // 8x8 transform: 8 lanes per 8x8 block, a row then a column each
+        const int b8 = lane >> 3, j = lane & 7, bx8 = (b8 & 1) * 8, by8 = (b8 >> 1) * 8;
+        {
+            int d[8], o[8];
+#pragma unroll
+            for (int k = 0; k < 8; k++)
+                d[k] = (int)SY[(size_t)(y0 + by8 + j) * P.A.ls + x0 + bx8 + k] - S.pred[(by8 + j) * 16 + bx8 + k];
+            q_fdct8_1d_d(d, o);
+#pragma unroll
+            for (int k = 0; k < 8; k++) S.t8[b8][j][k] = o[k];
+        }
+        __syncwarp();
+        {
+            int d[8], o[8];
+#pragma unroll
+            for (int k = 0; k < 8; k++) d[k] = S.t8[b8][k][j];
+            q_fdct8_1d_d(d, o);
+            __syncwarp();
+#pragma unroll
+            for (int k = 0; k < 8; k++) S.co8[b8][k * 8 + j] = o[k];  // raster (row k, column j)
+        }
+        __syncwarp();
+        // quantise 8 scan positions a lane (quant8, enc/frame.rs:56-72)
+        {
+            const int m = qp % 6, qbits = 16 + qp / 6, f = (1 << qbits) / 6;
+            int dq[8];
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                const int sk = j * 8 + k, pz = c_zz8[sk];
+                const int l = q_quant_d(S.co8[b8][pz], c_q_mf8[m][q_class8_d(pz)], f, qbits);
+                S.lv8[b8][sk] = (int16_t)l;
+                int v = 0;
+                if (l != 0) {
+                    const int vv = l * 16 * c_q_dq8[m][q_class8_d(pz)];
+                    v = qp >= 36 ? vv << (qp / 6 - 6) : (vv + (1 << (5 - qp / 6))) >> (6 - qp / 6);
+                }
+                dq[k] = v;
+            }
+            __syncwarp();
+#pragma unroll
+            for (int k = 0; k < 8; k++) S.co8[b8][c_zz8[j * 8 + k]] = dq[k];
+        }
+        __syncwarp();
+        int score = 0;
+        if (j == 0) score = q_decimate_d(S.lv8[b8], 64);
+        score = __shfl_sync(FULL, score, b8 * 8);
+        const int tot = __shfl_sync(FULL, score, 0) + __shfl_sync(FULL, score, 8) + __shfl_sync(FULL, score, 16) + __shfl_sync(FULL, score, 24);
+        const bool drop = score < 4 || tot < 6;
+        int nz = 0;
+#pragma unroll
+        for (int k = 0; k < 8; k++) nz += S.lv8[b8][j * 8 + k] != 0;
+#pragma unroll
+        for (int off = 1; off < 8; off <<= 1) nz += __shfl_xor_sync(FULL, nz, off);
+        if (drop) nz = 0;
+        // the reconstruction: rows of the inverse transform, then its columns onto the prediction
+        const bool idct = !drop && nz > 0;
+        if (idct) {
+            int d[8], o[8];
+#pragma unroll
+            for (int k = 0; k < 8; k++) d[k] = S.co8[b8][j * 8 + k];
+            q_row8_d(d, o);
+#pragma unroll
+            for (int k = 0; k < 8; k++) S.t8[b8][j][k] = o[k];
+        }
+        __syncwarp();
+        {
+            int o[8];
+            if (idct) {
+                int d[8];
+#pragma unroll
+                for (int k = 0; k < 8; k++) d[k] = S.t8[b8][k][j];
+                q_row8_d(d, o);
+            }
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+                const int pv = S.pred[(by8 + i) * 16 + bx8 + j];
+                RY[(size_t)(y0 + by8 + i) * P.ys + x0 + bx8 + j] = (T)(idct ? min(max(pv + ((o[i] + 32) >> 6), 0), maxv) : pv);
+            }
+        }
+        ironav_intercode& O = *out;
+        if (!drop) {
+#pragma unroll
+            for (int k = 0; k < 8; k++) O.luma8[b8][j * 8 + k] = S.lv8[b8][j * 8 + k];
+        }
+        if (j < 4 && !drop) O.nnz[((b8 >> 1) * 2 + (j >> 1)) * 4 + (b8 & 1) * 2 + (j & 1)] = (uint8_t)nz;
+        if (j == 0 && nz > 0) cbp |= 1u << b8;
+    }
+    // the luma part of the coded block pattern, from every lane
+#pragma unroll
+    for (int off = 16; off >= 1; off >>= 1) cbp |= __shfl_xor_sync(FULL, cbp, off);
+    // the luma part of the coded block pattern, from every lane
+#pragma unroll
+    for (int off = 16; off >= 1; off >>= 1) cbp |= __shfl_xor_sync(FULL, cbp, off);
+    if (mode == 2) {
+        cbp |= code_chroma_mb<T>(P, S, mbx, mby, out, false);
+    } else {
+        // P_Skip: the chroma prediction is the reconstruction
+        for (int i = lane; i < 128; i += 32) {
+            T* RC = reinterpret_cast<T*>(P.rec[1 + (i >> 6)]);
+            RC[(size_t)(mby * 8 + ((i >> 3) & 7)) * P.cs + mbx * 8 + (i & 7)] = (T)S.cpred[i >> 6][i & 63];
+        }
+    }
+    if (lane == 0 && mode == 2) {
+        out->cbp = (uint8_t)cbp;
+        out->t8x8 = (uint8_t)(D.t8 && (cbp & 15) != 0);
+    }
+    __syncwarp();
+    return cbp;
+}
+
 template <class T>
 __global__ void __launch_bounds__(128, 4) code_inter_kernel(const __grid_constant__ CodeParams P) {
     __shared__ CodeSmem smem[4];
     CodeSmem& S = smem[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
     const int nmb = P.A.mb_w * P.A.mb_h;
-    const int maxv = (1 << P.bd) - 1;
-    const int qp = P.qp + 6 * (P.bd - 8);
     for (int mb = blockIdx.x * 4 + (threadIdx.x >> 5); mb < nmb; mb += gridDim.x * 4) {
         // the decision (78 bytes: 2-byte aligned)
         const uint16_t* dp = reinterpret_cast<const uint16_t*>(reinterpret_cast<const uint8_t*>(P.decs) + (size_t)mb * sizeof(ironav_interdec));
@@ -235,302 +555,7 @@ __global__ void __launch_bounds__(128, 4) code_inter_kernel(const __grid_constan
             if (lane == 0) atomicOr(P.err, 4u);
             continue;
         }
-        const int mbx = mb % P.A.mb_w, mby = mb / P.A.mb_w, x0 = mbx * 16, y0 = mby * 16;
-        // luma prediction, a lane per 4x4 block
-        if (lane < 16) {
-            const int bx = lane & 3, by = lane >> 2;
-            int n, rs;
-            const int4 r = rect_of(D.part, D.sub, bx, by, &n, &rs);
-            const int2 mv = make_int2(D.mvs[n][0], D.mvs[n][1]);
-            uint32_t pr[4][sizeof(T)];
-            pred4<T>(P.A, P.A.planes[D.refs[rs]], x0 + r.x * 4, y0 + r.y * 4, r.z * 4, r.w * 4, bx - r.x, by - r.y, mv, pr);
-#pragma unroll
-            for (int row = 0; row < 4; row++)
-#pragma unroll
-                for (int k = 0; k < 4; k++) {
-                    const uint32_t wv = pr[row][(k * (int)sizeof(T)) >> 2];
-                    S.pred[(by * 4 + row) * 16 + bx * 4 + k] = (int)((wv >> ((k * 8 * (int)sizeof(T)) & 31)) & (uint32_t)maxv);
-                }
-        }
-        // chroma prediction (chroma_mc from each partition's vector, in eighth samples), 4 samples a lane
-        for (int i = lane; i < 128; i += 32) {
-            const int cc = i >> 6, cy = (i >> 3) & 7, cx = i & 7;
-            int n, rs;
-            const int4 r = rect_of(D.part, D.sub, cx >> 1, cy >> 1, &n, &rs);
-            (void)r;
-            const int mx = D.mvs[n][0], my = D.mvs[n][1];
-            const T* rc = reinterpret_cast<const T*>(P.ref_c[D.refs[rs]]) + (size_t)cc * P.cw * P.ch;
-            const int fx = mx & 7, fy = my & 7;
-            const int xs = mbx * 8 + cx + (mx >> 3), ysm = mby * 8 + cy + (my >> 3);
-            const int xa = min(max(xs, 0), P.cw - 1), xb = min(max(xs + 1, 0), P.cw - 1);
-            const int ya = min(max(ysm, 0), P.ch - 1), yb = min(max(ysm + 1, 0), P.ch - 1);
-            const int A_ = rc[(size_t)ya * P.cw + xa], B_ = rc[(size_t)ya * P.cw + xb], C_ = rc[(size_t)yb * P.cw + xa], D_ = rc[(size_t)yb * P.cw + xb];
-            S.cpred[cc][cy * 8 + cx] = ((8 - fx) * (8 - fy) * A_ + fx * (8 - fy) * B_ + (8 - fx) * fy * C_ + fx * fy * D_ + 32) >> 6;
-        }
-        __syncwarp();
-        T* const RY = reinterpret_cast<T*>(P.rec[0]);
-        const T* const SY = reinterpret_cast<const T*>(P.A.src);
-        uint32_t cbp = 0;
-        if (mode == 1) {
-            // P_Skip: the prediction is the reconstruction
-            for (int i = lane; i < 256; i += 32) RY[(size_t)(y0 + (i >> 4)) * P.ys + x0 + (i & 15)] = (T)S.pred[i];
-        } else if (!D.t8) {
-            // 4x4 transform: a lane per block; the levels go to shared memory and come back after the
-            // decimation sums, so that no 16-entry array stays live across the shuffles
-            int score = 0;
-            const int bx = lane & 3, by = lane >> 2;
-            if (lane < 16) {
-                int d[16], c[16];
-#pragma unroll
-                for (int r = 0; r < 4; r++)
-#pragma unroll
-                    for (int k = 0; k < 4; k++)
-                        d[r * 4 + k] = (int)SY[(size_t)(y0 + by * 4 + r) * P.A.ls + x0 + bx * 4 + k] - S.pred[(by * 4 + r) * 16 + bx * 4 + k];
-                q_fdct4_d(d, c);
-                const int qbits = 15 + qp / 6, f = (1 << qbits) / 6, m = qp % 6;
-#pragma unroll
-                for (int k = 0; k < 16; k++) {
-                    const int pz = zz4_at(k);
-                    S.lv4[lane][k] = (int16_t)q_quant_d(c[pz], c_q_mf[m][q_class_d(pz)], f, qbits);
-                }
-                score = q_decimate_d(S.lv4[lane], 16);
-            }
-            // per 8x8 block: lanes (2i8x, 2i8y) quad sums; blocks b = by*4+bx, 8x8 index (by/2)*2 + bx/2
-            const int i8 = ((lane >> 3) & 1) * 2 + ((lane & 3) >> 1);
-            int s8 = 0, tot = 0;
-#pragma unroll
-            for (int q = 0; q < 4; q++) {
-                int sq = 0;
-#pragma unroll
-                for (int b = 0; b < 16; b++) {
-                    const int v = __shfl_sync(FULL, score, b);
-                    if (((b >> 3) & 1) * 2 + ((b & 3) >> 1) == q) sq += v;
-                }
-                if (q == i8) s8 = sq;
-                tot += sq;
-            }
-            if (lane < 16) {
-                const bool drop = s8 < 4 || tot < 6;
-                const int m = qp % 6, sh = qp / 6;
-                int co[16], p[16], nz = 0;
-                uint32_t packed[8];
-#pragma unroll
-                for (int k = 0; k < 16; k++) {
-                    const int pz = zz4_at(k);
-                    const int l = drop ? 0 : S.lv4[lane][k];
-                    nz += l != 0;
-                    co[pz] = (l * c_q_v[m][q_class_d(pz)]) << sh;
-                    if (k & 1) packed[k >> 1] |= (uint32_t)(l & 0xffff) << 16;
-                    else packed[k >> 1] = (uint32_t)(l & 0xffff);
-                }
-#pragma unroll
-                for (int r = 0; r < 4; r++)
-#pragma unroll
-                    for (int k = 0; k < 4; k++) p[r * 4 + k] = S.pred[(by * 4 + r) * 16 + bx * 4 + k];
-                int out[16];
-                if (nz > 0) {
-                    q_idct4_d(co, p, maxv, out);
-                } else {
-#pragma unroll
-                    for (int k = 0; k < 16; k++) out[k] = p[k];
-                }
-#pragma unroll
-                for (int r = 0; r < 4; r++)
-#pragma unroll
-                    for (int k = 0; k < 4; k++) RY[(size_t)(y0 + by * 4 + r) * P.ys + x0 + bx * 4 + k] = (T)out[r * 4 + k];
-                ironav_intercode& O = P.codes[mb];
-                uint32_t* lw = reinterpret_cast<uint32_t*>(O.luma[lane]);
-#pragma unroll
-                for (int k = 0; k < 8; k++) lw[k] = packed[k];
-                O.nnz[lane] = (uint8_t)nz;
-                if (nz > 0) cbp |= 1u << ((by >> 1) * 2 + (bx >> 1));
-            }
-        } else {
-            // 8x8 transform: 8 lanes per 8x8 block, a row then a column each
-            const int b8 = lane >> 3, j = lane & 7, bx8 = (b8 & 1) * 8, by8 = (b8 >> 1) * 8;
-            {
-                int d[8], o[8];
-#pragma unroll
-                for (int k = 0; k < 8; k++)
-                    d[k] = (int)SY[(size_t)(y0 + by8 + j) * P.A.ls + x0 + bx8 + k] - S.pred[(by8 + j) * 16 + bx8 + k];
-                q_fdct8_1d_d(d, o);
-#pragma unroll
-                for (int k = 0; k < 8; k++) S.t8[b8][j][k] = o[k];
-            }
-            __syncwarp();
-            {
-                int d[8], o[8];
-#pragma unroll
-                for (int k = 0; k < 8; k++) d[k] = S.t8[b8][k][j];
-                q_fdct8_1d_d(d, o);
-                __syncwarp();
-#pragma unroll
-                for (int k = 0; k < 8; k++) S.co8[b8][k * 8 + j] = o[k];  // raster (row k, column j)
-            }
-            __syncwarp();
-            // quantise 8 scan positions a lane (quant8, enc/frame.rs:56-72)
-            {
-                const int m = qp % 6, qbits = 16 + qp / 6, f = (1 << qbits) / 6;
-                int dq[8];
-#pragma unroll
-                for (int k = 0; k < 8; k++) {
-                    const int sk = j * 8 + k, pz = c_zz8[sk];
-                    const int l = q_quant_d(S.co8[b8][pz], c_q_mf8[m][q_class8_d(pz)], f, qbits);
-                    S.lv8[b8][sk] = (int16_t)l;
-                    int v = 0;
-                    if (l != 0) {
-                        const int vv = l * 16 * c_q_dq8[m][q_class8_d(pz)];
-                        v = qp >= 36 ? vv << (qp / 6 - 6) : (vv + (1 << (5 - qp / 6))) >> (6 - qp / 6);
-                    }
-                    dq[k] = v;
-                }
-                __syncwarp();
-#pragma unroll
-                for (int k = 0; k < 8; k++) S.co8[b8][c_zz8[j * 8 + k]] = dq[k];
-            }
-            __syncwarp();
-            int score = 0;
-            if (j == 0) score = q_decimate_d(S.lv8[b8], 64);
-            score = __shfl_sync(FULL, score, b8 * 8);
-            const int tot = __shfl_sync(FULL, score, 0) + __shfl_sync(FULL, score, 8) + __shfl_sync(FULL, score, 16) + __shfl_sync(FULL, score, 24);
-            const bool drop = score < 4 || tot < 6;
-            int nz = 0;
-#pragma unroll
-            for (int k = 0; k < 8; k++) nz += S.lv8[b8][j * 8 + k] != 0;
-#pragma unroll
-            for (int off = 1; off < 8; off <<= 1) nz += __shfl_xor_sync(FULL, nz, off);
-            if (drop) nz = 0;
-            // the reconstruction: rows of the inverse transform, then its columns onto the prediction
-            const bool idct = !drop && nz > 0;
-            if (idct) {
-                int d[8], o[8];
-#pragma unroll
-                for (int k = 0; k < 8; k++) d[k] = S.co8[b8][j * 8 + k];
-                q_row8_d(d, o);
-#pragma unroll
-                for (int k = 0; k < 8; k++) S.t8[b8][j][k] = o[k];
-            }
-            __syncwarp();
-            {
-                int o[8];
-                if (idct) {
-                    int d[8];
-#pragma unroll
-                    for (int k = 0; k < 8; k++) d[k] = S.t8[b8][k][j];
-                    q_row8_d(d, o);
-                }
-#pragma unroll
-                for (int i = 0; i < 8; i++) {
-                    const int pv = S.pred[(by8 + i) * 16 + bx8 + j];
-                    RY[(size_t)(y0 + by8 + i) * P.ys + x0 + bx8 + j] = (T)(idct ? min(max(pv + ((o[i] + 32) >> 6), 0), maxv) : pv);
-                }
-            }
-            ironav_intercode& O = P.codes[mb];
-            if (!drop) {
-#pragma unroll
-                for (int k = 0; k < 8; k++) O.luma8[b8][j * 8 + k] = S.lv8[b8][j * 8 + k];
-            }
-            if (j < 4 && !drop) O.nnz[((b8 >> 1) * 2 + (j >> 1)) * 4 + (b8 & 1) * 2 + (j & 1)] = (uint8_t)nz;
-            if (j == 0 && nz > 0) cbp |= 1u << b8;
-        }
-        // the luma part of the coded block pattern, from every lane
-#pragma unroll
-        for (int off = 16; off >= 1; off >>= 1) cbp |= __shfl_xor_sync(FULL, cbp, off);
-        // chroma (code_chroma, inter), a lane per 4x4 block of Cb (lanes 0-3) and Cr (4-7); the AC levels
-        // go to shared memory and come back after the DC transform's shuffles
-        int dc = 0, cscore = 0, anyac = 0;
-        const int qpc = dbk_chroma_qp(P.qp, 0, P.bd) + 6 * (P.bd - 8), mc = qpc % 6;
-        const int cc = (lane >> 2) & 1, blk = lane & 3, cbx = blk & 1, cby = blk >> 1;
-        const T* SC = reinterpret_cast<const T*>(P.src_c) + (size_t)cc * P.cw * P.ch;
-        if (mode == 2 && lane < 8) {
-            int d[16], c[16];
-#pragma unroll
-            for (int r = 0; r < 4; r++)
-#pragma unroll
-                for (int k = 0; k < 4; k++)
-                    d[r * 4 + k] = (int)SC[(size_t)(mby * 8 + cby * 4 + r) * P.cw + mbx * 8 + cbx * 4 + k] - S.cpred[cc][(cby * 4 + r) * 8 + cbx * 4 + k];
-            q_fdct4_d(d, c);
-            const int qbits = 15 + qpc / 6, f = (1 << qbits) / 6;
-#pragma unroll
-            for (int k = 0; k < 16; k++) {
-                const int pz = zz4_at(k);
-                const int l = pz != 0 ? q_quant_d(c[pz], c_q_mf[mc][q_class_d(pz)], f, qbits) : 0;
-                S.cl[cc][blk][k] = (int16_t)l;
-                anyac |= l != 0;
-            }
-            dc = c[0];
-            cscore = q_decimate_d(S.cl[cc][blk], 16);
-        }
-        if (mode == 2) {
-            // the DC transform over a component's 4 blocks (lanes 4cc..4cc+3)
-            const int base = (lane & 4);
-            const int d0 = __shfl_sync(FULL, dc, base), d1 = __shfl_sync(FULL, dc, base + 1), d2 = __shfl_sync(FULL, dc, base + 2),
-                      d3 = __shfl_sync(FULL, dc, base + 3);
-            const int fdc = blk == 0 ? d0 + d1 + d2 + d3 : (blk == 1 ? d0 - d1 + d2 - d3 : (blk == 2 ? d0 + d1 - d2 - d3 : d0 - d1 - d2 + d3));
-            const int qbits = 16 + qpc / 6, fr = (1 << qbits) / 6;
-            const int cdc = lane < 8 ? q_quant_d(fdc, c_q_mf[mc][0], fr, qbits) : 0;
-            int acs = lane < 8 ? cscore : 0;
-#pragma unroll
-            for (int off = 16; off >= 1; off >>= 1) acs += __shfl_xor_sync(FULL, acs, off);
-            const bool any_ac = (__ballot_sync(FULL, lane < 8 && anyac) != 0) && acs >= 7;
-            const bool any_dc = __ballot_sync(FULL, lane < 8 && cdc != 0) != 0;
-            const int cbpc = any_ac ? 2 : (any_dc ? 1 : 0);
-            cbp |= (uint32_t)cbpc << 4;
-            // the reconstruction: the DC levels' inverse 2x2 transform scaled, the AC as coded
-            const int l0 = __shfl_sync(FULL, cdc, base), l1 = __shfl_sync(FULL, cdc, base + 1), l2 = __shfl_sync(FULL, cdc, base + 2),
-                      l3 = __shfl_sync(FULL, cdc, base + 3);
-            const int fl = blk == 0 ? l0 + l1 + l2 + l3 : (blk == 1 ? l0 - l1 + l2 - l3 : (blk == 2 ? l0 + l1 - l2 - l3 : l0 - l1 - l2 + l3));
-            if (lane < 8) {
-                ironav_intercode& O = P.codes[mb];
-                const int sh = qpc / 6;
-                int cco[16], cp[16], nz = 0, any = 0;
-                uint32_t packed[8];
-#pragma unroll
-                for (int k = 0; k < 16; k++) {
-                    const int pz = zz4_at(k);
-                    const int l = any_ac ? S.cl[cc][blk][k] : 0;
-                    nz += l != 0;
-                    cco[pz] = (l * c_q_v[mc][q_class_d(pz)]) << sh;
-                    if (k & 1) packed[k >> 1] |= (uint32_t)(l & 0xffff) << 16;
-                    else packed[k >> 1] = (uint32_t)(l & 0xffff);
-                }
-                cco[0] = cbpc > 0 ? ((fl * (16 * c_q_v[mc][0])) << sh) >> 5 : 0;
-#pragma unroll
-                for (int k = 0; k < 16; k++) any |= cco[k];
-                uint32_t* aw = reinterpret_cast<uint32_t*>(O.cac[cc][blk]);
-#pragma unroll
-                for (int k = 0; k < 8; k++) aw[k] = packed[k];
-                O.cnnz[cc][blk] = (uint8_t)nz;
-                O.cdc[cc][blk] = (int16_t)cdc;
-#pragma unroll
-                for (int r = 0; r < 4; r++)
-#pragma unroll
-                    for (int k = 0; k < 4; k++) cp[r * 4 + k] = S.cpred[cc][(cby * 4 + r) * 8 + cbx * 4 + k];
-                int out[16];
-                if (any) {
-                    q_idct4_d(cco, cp, maxv, out);
-                } else {
-#pragma unroll
-                    for (int k = 0; k < 16; k++) out[k] = cp[k];
-                }
-                T* RC = reinterpret_cast<T*>(P.rec[1 + cc]);
-#pragma unroll
-                for (int r = 0; r < 4; r++)
-#pragma unroll
-                    for (int k = 0; k < 4; k++) RC[(size_t)(mby * 8 + cby * 4 + r) * P.cs + mbx * 8 + cbx * 4 + k] = (T)out[r * 4 + k];
-            }
-        } else {
-            // P_Skip: the chroma prediction is the reconstruction
-            for (int i = lane; i < 128; i += 32) {
-                T* RC = reinterpret_cast<T*>(P.rec[1 + (i >> 6)]);
-                RC[(size_t)(mby * 8 + ((i >> 3) & 7)) * P.cs + mbx * 8 + (i & 7)] = (T)S.cpred[i >> 6][i & 63];
-            }
-        }
-        if (lane == 0 && mode == 2) {
-            P.codes[mb].cbp = (uint8_t)cbp;
-            P.codes[mb].t8x8 = (uint8_t)(D.t8 && (cbp & 15) != 0);
-        }
-        __syncwarp();
+        code_inter_mb<T>(P, S, mb, &P.codes[mb]);
     }
 }
 

@@ -94,6 +94,12 @@ INTERCODE_DTYPE = np.dtype([("luma", "<i2", (16, 16)), ("luma8", "<i2", (4, 64))
                             ("cac", "<i2", (2, 4, 16)), ("nnz", "u1", (16,)), ("cnnz", "u1", (2, 4)), ("cbp", "u1"),
                             ("t8x8", "u1"), ("pad", "u1", (2,))])
 assert INTERDEC_DTYPE.itemsize == 78 and INTERCODE_DTYPE.itemsize == 1324
+# Decide mode: a macroblock's code (ironav_mbcode, MbCode) and the reference's Kind values it carries.
+MBCODE_DTYPE = np.dtype([("res", INTERCODE_DTYPE), ("dc", "<i2", (16,)), ("mvs", "<i2", (16, 2)), ("mvds", "<i2", (16, 2)),
+                         ("modes", "u1", (16,)), ("kind", "u1"), ("skip", "u1"), ("i16_mode", "u1"), ("chroma_mode", "u1"),
+                         ("part", "u1"), ("sub", "u1", (4,)), ("refs", "u1", (4,)), ("pad", "u1", (3,))])
+assert MBCODE_DTYPE.itemsize == 1516
+KIND_I4X4, KIND_I16X16, KIND_INTER = 1, 3, 5
 assert DBK_MB_DTYPE.itemsize == 192 and DBK_SLICE_DTYPE.itemsize == 20
 
 RESULT_INTER = 1
@@ -123,6 +129,7 @@ EXPORTS = (
     "ironav_deblock_picture", "ironav_deblock_picture_device",
     "ironav_begin_b_picture", "ironav_begin_b_picture_device", "ironav_analyse_b_replay", "ironav_analyse_b_replay_device",
     "ironav_set_source_chroma", "ironav_push_reference_chroma", "ironav_code_inter_picture", "ironav_code_inter_picture_device",
+    "ironav_decide_p_picture", "ironav_decide_p_picture_device",
 )
 
 SCENE_CUT = 0.8  # codec/change.rs:6
@@ -182,6 +189,9 @@ def _declare(lib: ctypes.CDLL) -> ctypes.CDLL:
         lib.ironav_push_reference_chroma.argtypes = [_VP, _VP, _VP, _I, _I, _I]
         lib.ironav_code_inter_picture.argtypes = [_VP, _I, _VP, _VP, _VP, _I, _VP, _VP, _I]
         lib.ironav_code_inter_picture_device.argtypes = [_VP, _I, _VP, _VP, _VP, _I, _VP, _VP, _I]
+    if hasattr(lib, "ironav_decide_p_picture"):
+        lib.ironav_decide_p_picture.argtypes = [_VP, _VP, _VP, _VP, _I, _VP, _VP, _I]
+        lib.ironav_decide_p_picture_device.argtypes = [_VP, _VP, _VP, _VP, _I, _VP, _VP, _I]
     if hasattr(lib, "ironav_deblock_picture"):
         lib.ironav_deblock_picture.argtypes = [_VP, _VP, _I, _VP, _VP, _I, _VP, _VP, _I]
         lib.ironav_deblock_picture_device.argtypes = [_VP, _VP, _I, _VP, _VP, _I, _VP, _VP, _I]
@@ -426,6 +436,19 @@ class InterStage:
         self._check(self.lib.ironav_code_inter_picture(self.ctx, qp, _ptr(decs), _ptr(codes), _ptr(y), y.shape[1], _ptr(cb),
                                                        _ptr(cr), cb.shape[1]), "ironav_code_inter_picture")
         return codes, (y, cb, cr)
+
+    def decide_p_picture(self):
+        """Decides and codes every macroblock of the current P picture (code_mb, CAVLC): returns (states,
+        codes, (y, cb, cr)) with the unfiltered reconstruction."""
+        dt = np.uint8 if self.bd == 8 else np.uint16
+        y = np.zeros((self.mb_h * 16, self.mb_w * 16), dt)
+        cb = np.zeros((self.mb_h * 8, self.mb_w * 8), dt)
+        cr = np.zeros_like(cb)
+        states = np.zeros(self.nmb, dtype=MBSTATE_DTYPE)
+        codes = np.zeros(self.nmb, dtype=MBCODE_DTYPE)
+        self._check(self.lib.ironav_decide_p_picture(self.ctx, _ptr(states), _ptr(codes), _ptr(y), y.shape[1], _ptr(cb), _ptr(cr),
+                                                     cb.shape[1]), "ironav_decide_p_picture")
+        return states, codes, (y, cb, cr)
 
     # -- deblocking of the reconstruction (h264/deblock.rs) ------------------------------------------------
 

@@ -1943,9 +1943,9 @@ static void q_inter_pred(const struct ironav_ctx* c, int mbx, int mby, const iro
     }
 }
 
-/* code_chroma (inter), enc/frame.rs:1856-1915 */
+/* code_chroma, enc/frame.rs:1856-1915 (intra: the intra rounding and no AC decimation) */
 static void q_code_chroma(const struct ironav_ctx* c, int mbx, int mby, int qp_y, const uint16_t cpred[2][64], ironav_intercode* out,
-                          uint16_t* rec_c[2], int cs) {
+                          uint16_t* const rec_c[2], int cs, int intra) {
     int x0 = mbx * 8, y0 = mby * 8, scs = c->mb_w * 8;
     int qoff = 6 * (c->bd - 8), maxv = (1 << c->bd) - 1;
     int qp = dbk_chroma_qp(qp_y, 0, c->bd) + qoff, m = qp % 6;
@@ -1960,13 +1960,13 @@ static void q_code_chroma(const struct ironav_ctx* c, int mbx, int mby, int qp_y
                     s[r * 4 + k] = c->src_c[cc][(size_t)(y0 + by * 4 + r) * scs + x0 + bx * 4 + k];
                     pr[r * 4 + k] = cpred[cc][(by * 4 + r) * 8 + bx * 4 + k];
                 }
-            q_block(s, pr, qp, 0, 1, lv[cc][blk], cos[cc][blk], &dcs[blk]);
+            q_block(s, pr, qp, intra, 1, lv[cc][blk], cos[cc][blk], &dcs[blk]);
             for (int k = 0; k < 16; k++)
                 if (lv[cc][blk][k]) any_ac = 1;
         }
         int f[4] = {dcs[0] + dcs[1] + dcs[2] + dcs[3], dcs[0] - dcs[1] + dcs[2] - dcs[3], dcs[0] + dcs[1] - dcs[2] - dcs[3],
                     dcs[0] - dcs[1] - dcs[2] + dcs[3]};
-        int qbits = 16 + qp / 6, fr = (1 << qbits) / 6;
+        int qbits = 16 + qp / 6, fr = (1 << qbits) / (intra ? 3 : 6);
         for (int k = 0; k < 4; k++) {
             cdc[cc][k] = q_quant(f[k], Q_MF[m][0], fr, qbits);
             if (cdc[cc][k]) any_dc = 1;
@@ -1976,7 +1976,7 @@ static void q_code_chroma(const struct ironav_ctx* c, int mbx, int mby, int qp_y
     int ac_score = 0;
     for (int cc = 0; cc < 2; cc++)
         for (int blk = 0; blk < 4; blk++) ac_score += q_decimate(lv[cc][blk], 16);
-    if (ac_score < 7) any_ac = 0;
+    if (!intra && ac_score < 7) any_ac = 0;
     if (!any_ac) {
         memset(lv, 0, sizeof(lv));
         memset(cos, 0, sizeof(cos));
@@ -2008,7 +2008,7 @@ static void q_code_chroma(const struct ironav_ctx* c, int mbx, int mby, int qp_y
 
 /* code_inter_residual / code_luma8, enc/frame.rs:1217-1305, of one macroblock into the reconstruction */
 static void q_code_inter(const struct ironav_ctx* c, int mbx, int mby, int qp_y, const ironav_interdec* d, ironav_intercode* out,
-                         uint16_t* rec[3], int ys, int cs) {
+                         uint16_t* const rec[3], int ys, int cs) {
     memset(out, 0, sizeof(*out));
     uint16_t pred[256], cpred[2][64];
     q_inter_pred(c, mbx, mby, d, pred, cpred);
@@ -2087,7 +2087,7 @@ static void q_code_inter(const struct ironav_ctx* c, int mbx, int mby, int qp_y,
             }
         }
     }
-    q_code_chroma(c, mbx, mby, qp_y, cpred, out, rec + 1, cs);
+    q_code_chroma(c, mbx, mby, qp_y, cpred, out, rec + 1, cs, 0);
 }
 
 int ironav_set_source_chroma(ironav_ctx* c, const void* cb, const void* cr, int stride) {
@@ -2155,3 +2155,576 @@ int ironav_code_inter_picture_device(ironav_ctx* c, int qp, const ironav_interde
     return IRONAV_HARDWARE_UNAVAILABLE;
 }
 
+
+/* ---------------------------------------------------------------------------------------------------
+ * The P macroblock decision (decide mode): code_mb without CABAC, enc/frame.rs:715-790
+ * ------------------------------------------------------------------------------------------------- */
+
+enum { KIND_I4 = 1, KIND_I16 = 3, KIND_INTER = 5 }; /* Kind, h264/mb.rs:21-30 */
+
+/* Edges, h264/intra.rs:17-26 (a 4x4 block: 8 samples above, 4 to the left) */
+typedef struct i_edges { int top[8], left[4], topleft, have_top, have_left, have_topleft; } i_edges;
+
+/* predict_nxn for n = 4, h264/intra.rs:30-128 (ITU-T H.264 8.3.1.2) */
+static void i_pred4(int mode, const i_edges* e, int bd, int out[16]) {
+#define T(i) ((i) < 0 ? e->topleft : e->top[(i)])
+#define L(j) ((j) < 0 ? e->topleft : e->left[(j)])
+    for (int y = 0; y < 4; y++)
+        for (int x = 0; x < 4; x++) {
+            int v;
+            switch (mode) {
+            case 0: v = T(x); break;
+            case 1: v = L(y); break;
+            case 2: {
+                int st = T(0) + T(1) + T(2) + T(3), sl = L(0) + L(1) + L(2) + L(3);
+                if (e->have_top && e->have_left) v = (st + sl + 4) >> 3;
+                else if (e->have_left) v = (sl + 2) >> 2;
+                else if (e->have_top) v = (st + 2) >> 2;
+                else v = 1 << (bd - 1);
+                break;
+            }
+            case 3: v = (x == 3 && y == 3) ? (T(6) + 3 * T(7) + 2) >> 2 : (T(x + y) + 2 * T(x + y + 1) + T(x + y + 2) + 2) >> 2; break;
+            case 4:
+                if (x > y) v = (T(x - y - 2) + 2 * T(x - y - 1) + T(x - y) + 2) >> 2;
+                else if (x < y) v = (L(y - x - 2) + 2 * L(y - x - 1) + L(y - x) + 2) >> 2;
+                else v = (T(0) + 2 * e->topleft + L(0) + 2) >> 2;
+                break;
+            case 5: {
+                int z = 2 * x - y, i = x - (y >> 1);
+                if (z >= 0 && (z & 1) == 0) v = (T(i - 1) + T(i) + 1) >> 1;
+                else if (z >= 0) v = (T(i - 2) + 2 * T(i - 1) + T(i) + 2) >> 2;
+                else if (z == -1) v = (L(0) + 2 * e->topleft + T(0) + 2) >> 2;
+                else v = (L(y - 2 * x - 1) + 2 * L(y - 2 * x - 2) + L(y - 2 * x - 3) + 2) >> 2;
+                break;
+            }
+            case 6: {
+                int z = 2 * y - x, j = y - (x >> 1);
+                if (z >= 0 && (z & 1) == 0) v = (L(j - 1) + L(j) + 1) >> 1;
+                else if (z >= 0) v = (L(j - 2) + 2 * L(j - 1) + L(j) + 2) >> 2;
+                else if (z == -1) v = (L(0) + 2 * e->topleft + T(0) + 2) >> 2;
+                else v = (T(x - 2 * y - 1) + 2 * T(x - 2 * y - 2) + T(x - 2 * y - 3) + 2) >> 2;
+                break;
+            }
+            case 7: {
+                int i = x + (y >> 1);
+                v = (y & 1) == 0 ? (T(i) + T(i + 1) + 1) >> 1 : (T(i) + 2 * T(i + 1) + T(i + 2) + 2) >> 2;
+                break;
+            }
+            default: {
+                int z = x + 2 * y, j = y + (x >> 1);
+                if (z > 5) v = L(3);
+                else if (z == 5) v = (L(2) + 3 * L(3) + 2) >> 2;
+                else if ((z & 1) == 0) v = (L(j) + L(j + 1) + 1) >> 1;
+                else v = (L(j) + 2 * L(j + 1) + L(j + 2) + 2) >> 2;
+                break;
+            }
+            }
+            out[y * 4 + x] = v;
+        }
+#undef T
+#undef L
+}
+
+/* predict_16x16, h264/intra.rs:161-209 (8.3.3) */
+static void i_pred16(int mode, const int top[16], const int left[16], int tl, int ht, int hl, int bd, int out[256]) {
+    if (mode == 0 || mode == 1) {
+        for (int i = 0; i < 256; i++) out[i] = mode == 0 ? top[i % 16] : left[i / 16];
+    } else if (mode == 2) {
+        int st = 0, sl = 0, v;
+        for (int i = 0; i < 16; i++) st += top[i], sl += left[i];
+        if (ht && hl) v = (st + sl + 16) >> 5;
+        else if (hl) v = (sl + 8) >> 4;
+        else if (ht) v = (st + 8) >> 4;
+        else v = 1 << (bd - 1);
+        for (int i = 0; i < 256; i++) out[i] = v;
+    } else {
+        int h = 0, v = 0;
+        for (int k = 0; k < 8; k++) {
+            h += (k + 1) * (top[8 + k] - (6 - k < 0 ? tl : top[6 - k]));
+            v += (k + 1) * (left[8 + k] - (6 - k < 0 ? tl : left[6 - k]));
+        }
+        int a = 16 * (left[15] + top[15]), b = (5 * h + 32) >> 6, c = (5 * v + 32) >> 6, maxv = (1 << bd) - 1;
+        for (int y = 0; y < 16; y++)
+            for (int x = 0; x < 16; x++) out[y * 16 + x] = clampi((a + b * (x - 7) + c * (y - 7) + 16) >> 5, 0, maxv);
+    }
+}
+
+/* predict_chroma for an 8x8 component, h264/intra.rs:212-287 (8.3.4); mode 0 DC, 1 horizontal, 2 vertical, 3 plane */
+static void i_pred_chroma(int mode, const int top[8], const int left[8], int tl, int ht, int hl, int bd, int out[64]) {
+    if (mode == 0) {
+        for (int by = 0; by < 2; by++)
+            for (int bx = 0; bx < 2; bx++) {
+                int st = top[bx * 4] + top[bx * 4 + 1] + top[bx * 4 + 2] + top[bx * 4 + 3];
+                int sl = left[by * 4] + left[by * 4 + 1] + left[by * 4 + 2] + left[by * 4 + 3];
+                int v, mid = 1 << (bd - 1);
+                if (bx == by) v = (ht && hl) ? (st + sl + 4) >> 3 : (hl ? (sl + 2) >> 2 : (ht ? (st + 2) >> 2 : mid));
+                else if (bx > 0) v = ht ? (st + 2) >> 2 : (hl ? (sl + 2) >> 2 : mid); /* top row, right: the row above first */
+                else v = hl ? (sl + 2) >> 2 : (ht ? (st + 2) >> 2 : mid);             /* left column, below: the column first */
+                for (int y = 0; y < 4; y++)
+                    for (int x = 0; x < 4; x++) out[(by * 4 + y) * 8 + bx * 4 + x] = v;
+            }
+    } else if (mode == 1 || mode == 2) {
+        for (int i = 0; i < 64; i++) out[i] = mode == 1 ? left[i / 8] : top[i % 8];
+    } else {
+        int hh = 0, vv = 0;
+        for (int k = 0; k < 4; k++) {
+            hh += (k + 1) * (top[4 + k] - (2 - k < 0 ? tl : top[2 - k]));
+            vv += (k + 1) * (left[4 + k] - (2 - k < 0 ? tl : left[2 - k]));
+        }
+        int a = 16 * (left[7] + top[7]), b = (34 * hh + 32) >> 6, c = (34 * vv + 32) >> 6, maxv = (1 << bd) - 1;
+        for (int y = 0; y < 8; y++)
+            for (int x = 0; x < 8; x++) out[y * 8 + x] = clampi((a + b * (x - 3) + c * (y - 3) + 16) >> 5, 0, maxv);
+    }
+}
+
+/* hadamard4, h264/idct.rs:76-95 */
+static void i_hadamard4(const int c[16], int o[16]) {
+    int t[16];
+    for (int i = 0; i < 4; i++) {
+        const int* d = c + i * 4;
+        int s0 = d[0] + d[1], s1 = d[0] - d[1], s2 = d[2] + d[3], s3 = d[2] - d[3];
+        t[i * 4] = s0 + s2;
+        t[i * 4 + 1] = s0 - s2;
+        t[i * 4 + 2] = s1 - s3;
+        t[i * 4 + 3] = s1 + s3;
+    }
+    for (int j = 0; j < 4; j++) {
+        int s0 = t[j] + t[4 + j], s1 = t[j] - t[4 + j], s2 = t[8 + j] + t[12 + j], s3 = t[8 + j] - t[12 + j];
+        o[j] = s0 + s2;
+        o[4 + j] = s0 - s2;
+        o[8 + j] = s1 - s3;
+        o[12 + j] = s1 + s3;
+    }
+}
+
+/* The decision's working set: the picture being reconstructed (unfiltered), the codes so far, QP. */
+typedef struct dctx {
+    const fc* f;
+    uint16_t* rec[3]; /* luma pw x ph, chroma cw x ch */
+    ironav_mbcode* codes;
+    int qp_y, qp;     /* QP_Y and QP'Y */
+    int fast_t, fast_tc;
+} dctx;
+
+static void code_new(ironav_mbcode* code, int kind) { /* MbCode::new, enc/frame.rs:302-306 */
+    memset(code, 0, sizeof(*code));
+    memset(code->modes, 2, sizeof(code->modes));
+    code->kind = (uint8_t)kind;
+}
+
+static int d_up(const struct ironav_ctx* c, int mby) { return mby > c->band_start[mby]; } /* up, enc/frame.rs:495-497 */
+
+/* SATD of the 4x4 source block at (x, y) of plane 0 (luma) or 1/2 (chroma) against pred (4x4) */
+static int d_satd4(const dctx* D, int plane, int x, int y, const int pred[16]) {
+    const struct ironav_ctx* c = D->f->c;
+    const uint16_t* s = plane == 0 ? c->src : c->src_c[plane - 1];
+    int st = plane == 0 ? c->pw : c->mb_w * 8, d[16];
+    for (int r = 0; r < 4; r++)
+        for (int k = 0; k < 4; k++) d[r * 4 + k] = (int)s[(size_t)(y + r) * st + x + k] - pred[r * 4 + k];
+    return satd4(d);
+}
+
+/* i16_neighbours + best_i16, enc/frame.rs:792-835 */
+static void i16_nb(const dctx* D, int mbx, int mby, int top[16], int left[16], int* tl) {
+    const struct ironav_ctx* c = D->f->c;
+    const uint16_t* p = D->rec[0];
+    int ls = c->pw, x0 = mbx * 16, y0 = mby * 16, ta = d_up(c, mby);
+    for (int i = 0; i < 16; i++) {
+        top[i] = ta ? p[(size_t)(y0 - 1) * ls + x0 + i] : 0;
+        left[i] = mbx > 0 ? p[(size_t)(y0 + i) * ls + x0 - 1] : 0;
+    }
+    *tl = (mbx > 0 && ta) ? p[(size_t)(y0 - 1) * ls + x0 - 1] : 0;
+}
+
+static void best_i16(const dctx* D, int mbx, int mby, int* mode_out, int* cost_out) {
+    const struct ironav_ctx* c = D->f->c;
+    int ta = d_up(c, mby), la = mbx > 0, top[16], left[16], tl, pred[256];
+    i16_nb(D, mbx, mby, top, left, &tl);
+    int bm = 2, bc = INT32_MAX;
+    for (int mode = 0; mode < 4; mode++) {
+        if ((mode == 0 && !ta) || (mode == 1 && !la) || (mode == 3 && !(ta && la))) continue;
+        i_pred16(mode, top, left, tl, ta, la, c->bd, pred);
+        int cost = c->lambda * (mode == 2 ? 0 : 1);
+        for (int b = 0; b < 16; b++) {
+            int pb[16];
+            for (int r = 0; r < 4; r++)
+                for (int k = 0; k < 4; k++) pb[r * 4 + k] = pred[((b / 4) * 4 + r) * 16 + (b % 4) * 4 + k];
+            cost += d_satd4(D, 0, mbx * 16 + (b % 4) * 4, mby * 16 + (b / 4) * 4, pb);
+        }
+        if (cost < bc) {
+            bm = mode;
+            bc = cost;
+        }
+    }
+    *mode_out = bm;
+    *cost_out = bc;
+}
+
+/* pred_i4_mode, enc/frame.rs:619-629 (a neighbour that is not Intra4x4 counts as DC) */
+static int pred_i4_mode(const dctx* D, const uint8_t cur[16], int mbx, int mby, int bx, int by) {
+    int a = -1, b = -1;
+    if (bx > 0) a = cur[by * 4 + bx - 1];
+    else {
+        long i = nb_index(D->f, mbx - 1, mby, mby);
+        if (i >= 0) a = D->codes[i].kind == KIND_I4 ? D->codes[i].modes[by * 4 + 3] : 2;
+    }
+    if (by > 0) b = cur[(by - 1) * 4 + bx];
+    else {
+        long i = nb_index(D->f, mbx, mby - 1, mby);
+        if (i >= 0) b = D->codes[i].kind == KIND_I4 ? D->codes[i].modes[12 + bx] : 2;
+    }
+    return (a >= 0 && b >= 0) ? mini(a, b) : 2;
+}
+
+static int zorder4(int bx, int by) { return ((by >> 1) << 3) | ((bx >> 1) << 2) | ((by & 1) << 1) | (bx & 1); } /* enc/frame.rs:2363-2365 */
+
+/* code_i4, enc/frame.rs:1050-1138: block by block in decoding order, each predicted from the
+ * reconstruction so far, its mode the cheapest by SATD + lambda * (1 predicted, 4 otherwise), coded and
+ * reconstructed in place. Returns the summed cost. */
+static int code_i4(const dctx* D, int mbx, int mby, ironav_mbcode* code) {
+    const struct ironav_ctx* c = D->f->c;
+    code_new(code, KIND_I4);
+    int ta = d_up(c, mby), la = mbx > 0, tla = la && ta, tra = ta && mbx + 1 < c->mb_w;
+    uint16_t* p = D->rec[0];
+    int ls = c->pw, maxv = (1 << c->bd) - 1, cost = 0;
+    for (int n = 0; n < 16; n++) {
+        int bx = ((n >> 2) & 1) * 2 + (n & 1), by = ((n >> 3) & 1) * 2 + ((n >> 1) & 1); /* block_pos, 108-110 */
+        int x = mbx * 16 + bx * 4, y = mby * 16 + by * 4;
+        i_edges e;
+        memset(&e, 0, sizeof(e));
+        e.have_left = bx > 0 || la;
+        e.have_top = by > 0 || ta;
+        e.have_topleft = bx > 0 ? (by > 0 ? 1 : ta) : (by > 0 ? la : tla);
+        int have_tr = by == 0 ? (bx < 3 ? ta : tra) : (bx == 3 ? 0 : zorder4(bx + 1, by - 1) < zorder4(bx, by));
+        if (e.have_top) {
+            for (int i = 0; i < 4; i++) e.top[i] = p[(size_t)(y - 1) * ls + x + i];
+            for (int i = 4; i < 8; i++) e.top[i] = have_tr ? p[(size_t)(y - 1) * ls + x + i] : e.top[3];
+        }
+        if (e.have_left)
+            for (int j = 0; j < 4; j++) e.left[j] = p[(size_t)(y + j) * ls + x - 1];
+        if (e.have_topleft) e.topleft = p[(size_t)(y - 1) * ls + x - 1];
+        int predicted = pred_i4_mode(D, code->modes, mbx, mby, bx, by);
+        int bm = 2, bc = INT32_MAX, bp[16];
+        for (int mode = 0; mode < 9; mode++) {
+            int ok = (mode == 0 || mode == 3 || mode == 7) ? e.have_top
+                   : (mode == 1 || mode == 8) ? e.have_left
+                   : mode == 2 ? 1 : (e.have_top && e.have_left && e.have_topleft);
+            if (!ok) continue;
+            int pr[16];
+            i_pred4(mode, &e, c->bd, pr);
+            int cc = d_satd4(D, 0, x, y, pr) + c->lambda * (mode == predicted ? 1 : 4);
+            if (cc < bc) {
+                bm = mode;
+                bc = cc;
+                memcpy(bp, pr, sizeof(bp));
+            }
+        }
+        cost += bc;
+        code->modes[by * 4 + bx] = (uint8_t)bm;
+        int s[16], lv[16], co[16], dc;
+        for (int r = 0; r < 4; r++)
+            for (int k = 0; k < 4; k++) s[r * 4 + k] = c->src[(size_t)(y + r) * c->pw + x + k];
+        q_block(s, bp, D->qp, 1, 0, lv, co, &dc);
+        for (int r = 0; r < 4; r++)
+            for (int k = 0; k < 4; k++) p[(size_t)(y + r) * ls + x + k] = (uint16_t)bp[r * 4 + k];
+        int nz = 0;
+        for (int k = 0; k < 16; k++) {
+            code->res.luma[by * 4 + bx][k] = (int16_t)lv[k];
+            nz += lv[k] != 0;
+        }
+        if (nz) q_idct4_add(co, p + (size_t)y * ls + x, ls, maxv);
+        code->res.nnz[by * 4 + bx] = (uint8_t)nz;
+    }
+    for (int i8 = 0; i8 < 4; i8++) {
+        int bx = (i8 & 1) * 2, by = (i8 >> 1) * 2;
+        if (code->res.nnz[by * 4 + bx] || code->res.nnz[by * 4 + bx + 1] || code->res.nnz[(by + 1) * 4 + bx] || code->res.nnz[(by + 1) * 4 + bx + 1])
+            code->res.cbp |= (uint8_t)(1 << i8);
+    }
+    return cost;
+}
+
+/* code_i16, enc/frame.rs:1140-1200: the AC of every 4x4 block, the DC through the Hadamard transform
+ * (halved, quantised with doubled precision), reconstructed as a decoder does */
+static void code_i16(const dctx* D, int mbx, int mby, int mode, ironav_mbcode* code) {
+    const struct ironav_ctx* c = D->f->c;
+    code_new(code, KIND_I16);
+    code->i16_mode = (uint8_t)mode;
+    int top[16], left[16], tl, pred[256];
+    i16_nb(D, mbx, mby, top, left, &tl);
+    i_pred16(mode, top, left, tl, d_up(c, mby), mbx > 0, c->bd, pred);
+    int x0 = mbx * 16, y0 = mby * 16, ls = c->pw, qp = D->qp, maxv = (1 << c->bd) - 1;
+    int dcs[16], cos[16][16], lvs[16][16], ac = 0;
+    for (int b = 0; b < 16; b++) {
+        int bx = b % 4, by = b / 4, s[16], pr[16];
+        for (int r = 0; r < 4; r++)
+            for (int k = 0; k < 4; k++) {
+                s[r * 4 + k] = c->src[(size_t)(y0 + by * 4 + r) * c->pw + x0 + bx * 4 + k];
+                pr[r * 4 + k] = pred[(by * 4 + r) * 16 + bx * 4 + k];
+            }
+        q_block(s, pr, qp, 1, 1, lvs[b], cos[b], &dcs[b]);
+        for (int k = 0; k < 16; k++) ac |= lvs[b][k] != 0;
+    }
+    int h[16], dl[16];
+    i_hadamard4(dcs, h);
+    int qbits = 16 + qp / 6, f = (1 << qbits) / 3, m = qp % 6;
+    for (int k = 0; k < 16; k++) {
+        int l = q_quant(h[ZZ4[k]] >> 1, Q_MF[m][0], f, qbits);
+        code->dc[k] = (int16_t)l;
+        dl[ZZ4[k]] = l;
+    }
+    if (!ac) {
+        memset(lvs, 0, sizeof(lvs));
+        memset(cos, 0, sizeof(cos));
+    }
+    code->res.cbp = ac ? 15 : 0;
+    int fdc[16], lsd = 16 * Q_V[m][0];
+    i_hadamard4(dl, fdc);
+    uint16_t* p = D->rec[0];
+    for (int y = 0; y < 16; y++)
+        for (int x = 0; x < 16; x++) p[(size_t)(y0 + y) * ls + x0 + x] = (uint16_t)pred[y * 16 + x];
+    for (int b = 0; b < 16; b++) {
+        int co[16], any = 0, nz = 0;
+        memcpy(co, cos[b], sizeof(co));
+        co[0] = qp >= 36 ? (fdc[b] * lsd) << (qp / 6 - 6) : (fdc[b] * lsd + (1 << (5 - qp / 6))) >> (6 - qp / 6);
+        for (int k = 0; k < 16; k++) {
+            any |= co[k] != 0;
+            code->res.luma[b][k] = (int16_t)lvs[b][k];
+            nz += lvs[b][k] != 0;
+        }
+        if (any) q_idct4_add(co, p + (size_t)(y0 + (b / 4) * 4) * ls + x0 + (b % 4) * 4, ls, maxv);
+        code->res.nnz[b] = (uint8_t)nz;
+    }
+}
+
+/* code_intra_chroma, enc/frame.rs:1807-1854: the cheapest mode by lambda * (1 DC, 3 otherwise) + both
+ * components' SATD, then code_chroma with the intra rounding */
+static void code_intra_chroma(const dctx* D, int mbx, int mby, ironav_mbcode* code) {
+    const struct ironav_ctx* c = D->f->c;
+    int la = mbx > 0, ta = d_up(c, mby), x0 = mbx * 8, y0 = mby * 8, cs = c->mb_w * 8;
+    int top[2][8], left[2][8], tl[2];
+    for (int cc = 0; cc < 2; cc++) {
+        const uint16_t* p = D->rec[1 + cc];
+        for (int i = 0; i < 8; i++) {
+            top[cc][i] = ta ? p[(size_t)(y0 - 1) * cs + x0 + i] : 0;
+            left[cc][i] = la ? p[(size_t)(y0 + i) * cs + x0 - 1] : 0;
+        }
+        tl[cc] = (la && ta) ? p[(size_t)(y0 - 1) * cs + x0 - 1] : 0;
+    }
+    int bm = 0, bc = INT32_MAX, bp[2][64];
+    for (int mode = 0; mode < 4; mode++) {
+        if ((mode == 1 && !la) || (mode == 2 && !ta) || (mode == 3 && !(la && ta))) continue;
+        int pr[2][64], cost = c->lambda * (mode == 0 ? 1 : 3);
+        for (int cc = 0; cc < 2; cc++) {
+            i_pred_chroma(mode, top[cc], left[cc], tl[cc], ta, la, c->bd, pr[cc]);
+            for (int b = 0; b < 4; b++) {
+                int pb[16];
+                for (int r = 0; r < 4; r++)
+                    for (int k = 0; k < 4; k++) pb[r * 4 + k] = pr[cc][((b / 2) * 4 + r) * 8 + (b % 2) * 4 + k];
+                cost += d_satd4(D, 1 + cc, x0 + (b % 2) * 4, y0 + (b / 2) * 4, pb);
+            }
+        }
+        if (cost < bc) {
+            bm = mode;
+            bc = cost;
+            memcpy(bp, pr, sizeof(bp));
+        }
+    }
+    code->chroma_mode = (uint8_t)bm;
+    uint16_t cpred[2][64];
+    for (int cc = 0; cc < 2; cc++)
+        for (int i = 0; i < 64; i++) cpred[cc][i] = (uint16_t)bp[cc][i];
+    q_code_chroma(c, mbx, mby, D->qp_y, cpred, &code->res, D->rec + 1, cs, 1);
+}
+
+/* part_mvps, enc/frame.rs:579-594, with sub-partitions */
+static void part_mvps(const fc* f, int mbx, int mby, int part, const uint8_t sub[4], const int16_t mvs[16][2], const uint8_t refs[4],
+                      int16_t out[16][2]) {
+    int16_t cur[16][2];
+    int8_t cref[16];
+    uint32_t done = 0;
+    memset(cur, 0, sizeof(cur));
+    memset(cref, 0, sizeof(cref));
+    memset(out, 0, sizeof(int16_t) * 32);
+    rect4 rs[16];
+    int n = rects(part, sub, rs), dir = part == 1 ? 1 : (part == 2 ? 2 : 0);
+    for (int k = 0; k < n; k++) {
+        rect4 r = rs[k];
+        int rf = refs[part == 3 ? (r.y / 2) * 2 + r.x / 2 : (part == 0 ? 0 : k)], p[2];
+        pred_mv(f, mbx, mby, cur, cref, done, r.x, r.y, r.w, dir, rf, p);
+        out[k][0] = (int16_t)p[0];
+        out[k][1] = (int16_t)p[1];
+        for (int by = r.y; by < r.y + r.h; by++)
+            for (int bx = r.x; bx < r.x + r.w; bx++) {
+                cur[by * 4 + bx][0] = mvs[k][0];
+                cur[by * 4 + bx][1] = mvs[k][1];
+                cref[by * 4 + bx] = (int8_t)rf;
+                done |= 1u << (by * 4 + bx);
+            }
+    }
+}
+
+/* code_inter, enc/frame.rs:1202-1215, with the 4x4 transform */
+static void d_code_inter(const dctx* D, int mbx, int mby, int part, const uint8_t sub[4], const uint8_t refs[4], const int16_t mvs[16][2],
+                         ironav_mbcode* code) {
+    const struct ironav_ctx* c = D->f->c;
+    code_new(code, KIND_INTER);
+    code->part = (uint8_t)part;
+    memcpy(code->sub, sub, 4);
+    memcpy(code->refs, refs, 4);
+    memcpy(code->mvs, mvs, sizeof(code->mvs));
+    int16_t mvp[16][2];
+    part_mvps(D->f, mbx, mby, part, sub, mvs, refs, mvp);
+    for (int n = 0; n < 16; n++)
+        for (int k = 0; k < 2; k++) code->mvds[n][k] = (int16_t)(mvs[n][k] - mvp[n][k]);
+    ironav_interdec d;
+    memset(&d, 0, sizeof(d));
+    d.mode = 2;
+    d.part = (uint8_t)part;
+    memcpy(d.sub, sub, 4);
+    memcpy(d.refs, refs, 4);
+    memcpy(d.mvs, mvs, sizeof(d.mvs));
+    q_code_inter(c, mbx, mby, D->qp_y, &d, &code->res, D->rec, c->pw, c->mb_w * 8);
+}
+
+/* The MbState of a decided macroblock (finish_mb, enc/frame.rs:2281-2321) */
+static void d_state(const ironav_mbcode* code, ironav_mbstate* s) {
+    memset(s, 0, sizeof(*s));
+    if (code->kind != KIND_INTER) {
+        for (int k = 0; k < 4; k++) s->refs[k] = -1;
+        return;
+    }
+    ironav_mbresult r;
+    memset(&r, 0, sizeof(r));
+    r.part = code->part;
+    memcpy(r.sub, code->sub, 4);
+    memcpy(r.refs, code->refs, 4);
+    memcpy(r.mvs, code->mvs, sizeof(r.mvs));
+    state_from_result(&r, 0, s);
+}
+
+/* code_mb for a P macroblock without CABAC, enc/frame.rs:715-790 */
+static void decide_mb(const dctx* D, int mbx, int mby, ironav_mbcode* code, ironav_mbstate* st) {
+    const fc* f = D->f;
+    const struct ironav_ctx* c = f->c;
+    int x0 = mbx * 16, y0 = mby * 16, lam = c->lambda, cw = c->mb_w * 8;
+    static const uint8_t zero4[4] = {0, 0, 0, 0};
+    /* P_Skip first (722-751) */
+    int sv[2];
+    skip_mv(f, mbx, mby, sv);
+    uint16_t pred[256];
+    halfpel_predict(&c->refs[0].hp, x0, y0, sv[0], sv[1], 16, 16, pred);
+    int sad = 0;
+    for (int i = 0; i < 256; i++) sad += abs((int)c->src[(size_t)(y0 + i / 16) * c->pw + x0 + i % 16] - (int)pred[i]);
+    int16_t smv[16][2];
+    for (int i = 0; i < 16; i++) smv[i][0] = (int16_t)sv[0], smv[i][1] = (int16_t)sv[1];
+    if (c->fast && sad < D->fast_t) {
+        ironav_interdec d;
+        memset(&d, 0, sizeof(d));
+        memcpy(d.mvs, smv, sizeof(d.mvs));
+        uint16_t lp[256], cp[2][64];
+        q_inter_pred(c, mbx, mby, &d, lp, cp);
+        int csad = 0;
+        for (int cc = 0; cc < 2; cc++)
+            for (int i = 0; i < 64; i++) csad += abs((int)c->src_c[cc][(size_t)(mby * 8 + i / 8) * cw + mbx * 8 + i % 8] - (int)cp[cc][i]);
+        if (csad < D->fast_tc) {
+            code_new(code, KIND_INTER);
+            code->skip = 1;
+            memcpy(code->mvs, smv, sizeof(code->mvs));
+            for (int i = 0; i < 256; i++) D->rec[0][(size_t)(y0 + i / 16) * c->pw + x0 + i % 16] = pred[i]; /* put_pred, 1397-1403 */
+            for (int cc = 0; cc < 2; cc++)
+                for (int i = 0; i < 64; i++) D->rec[1 + cc][(size_t)(mby * 8 + i / 8) * cw + mbx * 8 + i % 8] = cp[cc][i];
+            d_state(code, st);
+            return;
+        }
+    }
+    if (sad < c->skip_thresh) {
+        d_code_inter(D, mbx, mby, 0, zero4, zero4, smv, code);
+        if (code->res.cbp == 0) {
+            code->skip = 1;
+            d_state(code, st);
+            return;
+        }
+    }
+    int i16m, i16c;
+    best_i16(D, mbx, mby, &i16m, &i16c);
+    int best_intra = i16c + lam * 4;
+    counters cnt = {0, 0};
+    ironav_mbresult r;
+    memset(&r, 0, sizeof(r));
+    best_inter(f, &cnt, mbx, mby, &r);
+    /* Intra4x4 is tried by coding it when intra is competitive (766-779) */
+    ironav_mbcode* i4 = NULL;
+    ironav_mbcode i4code;
+    if (best_intra < r.cost) {
+        int cost = code_i4(D, mbx, mby, &i4code) + lam * 6;
+        if (cost < best_intra) {
+            best_intra = cost;
+            i4 = &i4code;
+        }
+    }
+    if (r.cost <= best_intra) {
+        d_code_inter(D, mbx, mby, r.part, r.sub, r.refs, (const int16_t(*)[2])r.mvs, code);
+        if (code->res.cbp == 0 && r.part == 0 && r.mvs[0][0] == sv[0] && r.mvs[0][1] == sv[1] && r.refs[0] == 0) code->skip = 1;
+        d_state(code, st);
+        return;
+    }
+    if (i4) *code = *i4;
+    else code_i16(D, mbx, mby, i16m, code);
+    code_intra_chroma(D, mbx, mby, code);
+    d_state(code, st);
+}
+
+/* The fast mode's P_Skip tests `sad < 256 * 0.05 * step` and `csad < 128 * 0.05 * step` (enc/frame.rs:735,
+ * 740) as integer bounds, like ironav_skip_threshold */
+static void fast_thresholds(int qpp, int* luma, int* chroma) {
+    double step = pow(2.0, (double)qpp / 6.0);
+    *luma = (int)ceil(256.0 * 0.05 * step);
+    *chroma = (int)ceil(128.0 * 0.05 * step);
+}
+
+int ironav_decide_p_picture(ironav_ctx* c, ironav_mbstate* states, ironav_mbcode* codes, void* rec_y, int ys, void* rec_cb, void* rec_cr,
+                            int cs) {
+    if (!c || !states || !codes || !rec_y || !rec_cb || !rec_cr || ys < c->pw || cs < c->pw / 2 || c->nact < 1 || !c->src_c[0])
+        return IRONAV_INVALID_ARGUMENT;
+    for (int r = 0; r < c->nact; r++)
+        if (!c->refs[r].chroma[0]) return IRONAV_INVALID_ARGUMENT;
+    long n = (long)c->mb_w * c->mb_h;
+    int B = sample_bytes(c), cw = c->mb_w * 8, ch = c->mb_h * 8;
+    dctx D;
+    memset(&D, 0, sizeof(D));
+    fc f = {c, states, NULL, 0, NULL};
+    D.f = &f;
+    D.rec[0] = (uint16_t*)calloc((size_t)c->pw * c->ph, sizeof(uint16_t));
+    D.rec[1] = (uint16_t*)calloc((size_t)cw * ch, sizeof(uint16_t));
+    D.rec[2] = (uint16_t*)calloc((size_t)cw * ch, sizeof(uint16_t));
+    D.codes = codes;
+    D.qp = c->qpp;
+    D.qp_y = c->qpp - 6 * (c->bd - 8);
+    fast_thresholds(c->qpp, &D.fast_t, &D.fast_tc);
+    memset(states, 0, sizeof(ironav_mbstate) * (size_t)n);
+    memset(codes, 0, sizeof(ironav_mbcode) * (size_t)n);
+    int nb = 0;
+    int starts[1025];
+    for (int r = 0; r < c->mb_h; r++)
+        if (c->band_start[r] == r) starts[nb++] = r;
+    starts[nb] = c->mb_h;
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 1) num_threads(c->threads)
+#endif
+    for (int b = 0; b < nb; b++)
+        for (int mby = starts[b]; mby < starts[b + 1]; mby++)
+            for (int mbx = 0; mbx < c->mb_w; mbx++) {
+                size_t i = (size_t)mby * c->mb_w + mbx;
+                decide_mb(&D, mbx, mby, &codes[i], &states[i]);
+            }
+    dbk_copy_out(rec_y, D.rec[0], B, ys, c->pw, c->ph);
+    dbk_copy_out(rec_cb, D.rec[1], B, cs, cw, ch);
+    dbk_copy_out(rec_cr, D.rec[2], B, cs, cw, ch);
+    for (int k = 0; k < 3; k++) free(D.rec[k]);
+    return IRONAV_OK;
+}
+
+int ironav_decide_p_picture_device(ironav_ctx* c, ironav_mbstate* s, ironav_mbcode* o, void* y, int ys, void* cb, void* cr, int cs) {
+    (void)c; (void)s; (void)o; (void)y; (void)ys; (void)cb; (void)cr; (void)cs;
+    return IRONAV_HARDWARE_UNAVAILABLE;
+}
