@@ -52,7 +52,7 @@ def parse():
     p.add_argument("--ring", type=int, default=RING,
                    help="pictures in the ring (fewer than 36 fits in L2: for profiling runs only)")
     p.add_argument("--no-e2e", action="store_true", help="skip the host-buffer pass (profiling runs)")
-    p.add_argument("--workload", default="1080p", choices=["1080p", "batched", "scenecut", "deblock", "bpicture", "residual"],
+    p.add_argument("--workload", default="1080p", choices=["1080p", "batched", "scenecut", "deblock", "bpicture", "residual", "decide"],
                    help="1080p: one stream, replay mode (the headline); batched: 64 mixed-resolution streams in auto "
                         "mode, one launch per stage and frame step, against the per-stream launch loop")
     p.add_argument("--streams", type=int, default=64, help="streams of the batched workload")
@@ -267,6 +267,9 @@ def main():
         return finish(world)
     if args.workload == "residual":
         run_residual(args, rank, world)
+        return finish(world)
+    if args.workload == "decide":
+        run_decide(args, rank, world)
         return finish(world)
 
     import torch
@@ -674,6 +677,141 @@ def run_bpicture(args, rank, world):
             n_cpu += 1
         line["cpu_baseline"] = {"value": n_cpu * nmb / t_cpu, "unit": "MB/s", "cores": cores, "kind": "port",
                                 "sample": f"{n_cpu} B pictures (the ring's first), replay mode, {cores} threads, {t_cpu:.1f} s"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    for st in stages:
+        st.close()
+
+
+def run_decide(args, rank, world):
+    """The whole P macroblock decision of the CAVLC encoder at 1080p (code_mb, enc/frame.rs:715-790: P_Skip
+    tests, best_i16, best_inter, the Intra4x4 trial, the coding of the chosen macroblock into the unfiltered
+    reconstruction) in the device wavefront, device-resident: one step = every macroblock of one P picture.
+    A ring of contexts (reference planes and chroma, states, codes, reconstructions) larger than L2. The
+    oracle decides the same picture on all host cores (slice bands in parallel, as the reference's slice
+    threads)."""
+    import torch
+    from ironav_b200.inter import MBCODE_DTYPE, InterStage, cuda_library
+    from ironav_b200.synth import CONFIGS, Sequence
+
+    bd = args.bd
+    lib = cuda_library()
+    ring = max(2, min(args.ring, 6))
+    w, h, seed, pan_q, nobj, vmax, sigma = CONFIGS["1080p"]
+    seq = Sequence(w, h, ring + 1, seed + 0x3000 * rank, pan_q, nobj, vmax, sigma)
+    frame = (lambda t: seq.frame10(t)) if bd == 10 else seq.frame
+    qpp = QP + 6 * (bd - 8)
+    stream = torch.cuda.Stream()
+    dev = torch.device("cuda", torch.cuda.current_device())
+    stages, bufs, srcs = [], [], []
+    dt = torch.uint8 if bd == 8 else torch.int16
+    for k in range(ring):
+        st = InterStage(w, h, max_refs=1, nslices=NSLICES, lib=lib, bd=bd)
+        st.push_reference(frame(k))
+        st.push_reference_chroma(*seq.chroma(k, bd))
+        st.set_source(frame(k + 1))
+        st.set_source_chroma(*seq.chroma(k + 1, bd))
+        st.begin_p_picture(qpp)
+        st.set_stream(stream.cuda_stream)
+        stages.append(st)
+        srcs.append((frame(k), seq.chroma(k, bd), frame(k + 1), seq.chroma(k + 1, bd)))
+        bufs.append((torch.zeros(st.nmb * 72, dtype=torch.uint8, device=dev), torch.zeros(st.nmb * MBCODE_DTYPE.itemsize, dtype=torch.uint8, device=dev),
+                     torch.zeros((st.mb_h * 16, st.mb_w * 16), dtype=dt, device=dev), torch.zeros((2, st.mb_h * 8, st.mb_w * 8), dtype=dt, device=dev)))
+    nmb, mb_w, mb_h = stages[0].nmb, stages[0].mb_w, stages[0].mb_h
+
+    def step(i, ev=None):
+        k = i % ring
+        s_, c_, y, c = bufs[k]
+        if ev is not None:
+            ev[0].record(stream)
+        r = lib.ironav_decide_p_picture_device(stages[k].ctx, s_.data_ptr(), c_.data_ptr(), y.data_ptr(), y.shape[1], c[0].data_ptr(),
+                                               c[1].data_ptr(), c.shape[2])
+        if r:
+            raise RuntimeError(f"ironav_decide_p_picture_device: {r}")
+        if ev is not None:
+            ev[1].record(stream)
+
+    with torch.cuda.stream(stream):
+        for i in range(args.warmup):
+            step(i)
+        clocks = Clocks(int(os.environ.get("LOCAL_RANK", 0)))
+        clocks.start()
+        t_load = time.perf_counter()
+        i = 0
+        while time.perf_counter() - t_load < 0.6:
+            step(args.warmup + i)
+            i += 1
+            if i % 8 == 0:
+                torch.cuda.synchronize()
+        torch.cuda.synchronize()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for i in range(args.steps):
+            step(args.warmup + i, evs[i])
+        e1.record(stream)
+        torch.cuda.synchronize()
+        clk = clocks.stop()
+    for st in stages:
+        st.sync()
+    ms = e0.elapsed_time(e1)
+    k_ms = float(np.mean([a.elapsed_time(b) for a, b in evs]))
+    value = world * nmb * args.steps / (ms * 1e-3)
+    codes = bufs[0][1].cpu().numpy().view(MBCODE_DTYPE)
+    kinds = {"skip": int(codes["skip"].sum()), "inter": int(((codes["kind"] == 5) & (codes["skip"] == 0)).sum()),
+             "i16": int((codes["kind"] == 3).sum()), "i4": int((codes["kind"] == 1).sum())}
+    # end to end through the host-buffer call (states, codes and the reconstruction back every step)
+    for st in stages:
+        st.set_stream(None)
+    for i in range(args.warmup):
+        stages[i % ring].decide_p_picture()
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        stages[i % ring].decide_p_picture()
+    el = time.perf_counter() - t0
+    B = 1 if bd == 8 else 2
+    line = {
+        "metric": f"1080p P-picture macroblock decision + coding MB/s ({bd}-bit, CAVLC code_mb)", "value": value, "unit": "MB/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic: seeded 4-octave value noise panned per frame + 8 moving rectangles, sigma 3; chroma from the 2x2 "
+                "luma means",
+        "config": {"workload": f"decide and code every macroblock of one 1920x1088 {bd}-bit P picture per step (QP {QP}, one "
+                               f"reference, 8 slice bands, wavefront); decisions: {kinds}",
+                   "slices": NSLICES, "mode": "decide (device pointers)",
+                   "l2": f"ring of {ring} contexts (reference planes, chroma, states, codes, reconstructions > L2)"},
+        "gpu_launches": args.steps,
+        "e2e": {"value": world * nmb * args.steps / el, "unit": "MB/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": nmb * (72 + MBCODE_DTYPE.itemsize + 384 * B), "ms_per_step": 1e3 * el / args.steps,
+                "note": "ironav_decide_p_picture with host buffers (sources and references already held by the contexts)"},
+        "roofline": {"bound": "latency", "kernel": f"decide_kernel<{'uint8_t' if bd == 8 else 'uint16_t'}>", "achieved": None,
+                     "peak": None, "unit": None, "frac": None, "traffic": None, "ms_per_launch": k_ms,
+                     "note": f"one stream's wavefront: a critical path of mb_w + 2 (band rows - 1) = {mb_w + 2 * (-(-mb_h // NSLICES) - 1)} "
+                             "dependent macroblocks; see the per-macroblock latency in the profile"},
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from tests.oracle_lib import oracle_library
+
+        olib = oracle_library()
+        cores = host_cores()
+        o = InterStage(w, h, max_refs=1, nslices=NSLICES, lib=olib, bd=bd)
+        olib.oracle_set_threads(o.ctx, cores)
+        f0, c0, f1, c1 = srcs[0]
+        o.push_reference(f0)
+        o.push_reference_chroma(*c0)
+        o.set_source(f1)
+        o.set_source_chroma(*c1)
+        o.begin_p_picture(qpp)
+        n_cpu, t_cpu = 0, 0.0
+        while t_cpu < min(args.cpu_seconds, 10.0):
+            t0 = time.perf_counter()
+            o.decide_p_picture()
+            t_cpu += time.perf_counter() - t0
+            n_cpu += 1
+        line["cpu_baseline"] = {"value": n_cpu * nmb / t_cpu, "unit": "MB/s", "cores": min(cores, NSLICES), "kind": "port",
+                                "sample": f"{n_cpu} P pictures (the ring's first), slice bands on {min(cores, NSLICES)} threads, {t_cpu:.1f} s"}
+        o.close()
     if rank == 0:
         print(json.dumps(line), flush=True)
     for st in stages:

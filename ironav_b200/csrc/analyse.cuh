@@ -848,10 +848,18 @@ static __device__ void analyse(const AnalyseParams& __restrict__ P, WarpSmem<T>&
 
 // Waits until macroblock `m`'s decision is published, at most P.wait_limit polls. Returns false when
 // it gave up or another warp already did (the launch is then abandoned and the host reports a timeout).
+// Polls are relaxed loads and one fence.acq_rel follows the flag (the acquire pattern of the PTX memory
+// model): an acquire load per poll would order, and cost, every poll of every waiting warp.
 static __device__ bool wait_published(const AnalyseParams& P, int m) {
     for (unsigned i = 0;; i++) {
-        if (ld_acquire(&P.flags[m]) == P.epoch) return true;
-        if (ld_acquire(P.err) != 0) return false;
+        unsigned f, e;
+        asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(f) : "l"(&P.flags[m]) : "memory");
+        if (f == P.epoch) {
+            asm volatile("fence.acq_rel.gpu;" ::: "memory");
+            return true;
+        }
+        asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(e) : "l"(P.err) : "memory");
+        if (e != 0) return false;
         if (i >= P.wait_limit) {
             atomicOr(P.err, 1u);
             return false;

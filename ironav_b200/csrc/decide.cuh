@@ -74,65 +74,77 @@ __device__ __forceinline__ int satd4_d(const int (&d)[16]) {
     return sum >> 1;
 }
 
-// predict_nxn for a 4x4 block, h264/intra.rs:30-128 (ITU-T H.264 8.3.1.2), from the edge array E (E[0] the
-// top-left sample, E[1 + i] the 8 above, E[9 + j] the 4 to the left).
-__device__ __forceinline__ void i_pred4_d(int mode, const int* E, bool ht, bool hl, int bd, int (&out)[16]) {
-#define T_(i) E[1 + (i)]
-#define L_(j) ((j) < 0 ? E[0] : E[9 + (j)])
-#pragma unroll
-    for (int y = 0; y < 4; y++)
-#pragma unroll
-        for (int x = 0; x < 4; x++) {
-            int v;
-            switch (mode) {
-            case 0: v = T_(x); break;
-            case 1: v = L_(y); break;
-            case 2: {
-                const int st = T_(0) + T_(1) + T_(2) + T_(3), sl = L_(0) + L_(1) + L_(2) + L_(3);
-                v = (ht && hl) ? (st + sl + 4) >> 3 : (hl ? (sl + 2) >> 2 : (ht ? (st + 2) >> 2 : 1 << (bd - 1)));
-                break;
-            }
-            case 3: v = (x == 3 && y == 3) ? (T_(6) + 3 * T_(7) + 2) >> 2 : (T_(x + y) + 2 * T_(x + y + 1) + T_(x + y + 2) + 2) >> 2; break;
-            case 4:
-                if (x > y) v = (T_(x - y - 2) + 2 * T_(x - y - 1) + T_(x - y) + 2) >> 2;
-                else if (x < y) v = (L_(y - x - 2) + 2 * L_(y - x - 1) + L_(y - x) + 2) >> 2;
-                else v = (T_(0) + 2 * E[0] + L_(0) + 2) >> 2;
-                break;
-            case 5: {
-                const int z = 2 * x - y, i = x - (y >> 1);
-                if (z >= 0 && (z & 1) == 0) v = (T_(i - 1) + T_(i) + 1) >> 1;
-                else if (z >= 0) v = (T_(i - 2) + 2 * T_(i - 1) + T_(i) + 2) >> 2;
-                else if (z == -1) v = (L_(0) + 2 * E[0] + T_(0) + 2) >> 2;
-                else v = (L_(y - 2 * x - 1) + 2 * L_(y - 2 * x - 2) + L_(y - 2 * x - 3) + 2) >> 2;
-                break;
-            }
-            case 6: {
-                const int z = 2 * y - x, j = y - (x >> 1);
-                if (z >= 0 && (z & 1) == 0) v = (L_(j - 1) + L_(j) + 1) >> 1;
-                else if (z >= 0) v = (L_(j - 2) + 2 * L_(j - 1) + L_(j) + 2) >> 2;
-                else if (z == -1) v = (L_(0) + 2 * E[0] + T_(0) + 2) >> 2;
-                else v = (T_(x - 2 * y - 1) + 2 * T_(x - 2 * y - 2) + T_(x - 2 * y - 3) + 2) >> 2;
-                break;
-            }
-            case 7: {
-                const int i = x + (y >> 1);
-                v = (y & 1) == 0 ? (T_(i) + T_(i + 1) + 1) >> 1 : (T_(i) + 2 * T_(i + 1) + T_(i + 2) + 2) >> 2;
-                break;
-            }
-            default: {
-                const int z = x + 2 * y, j = y + (x >> 1);
-                if (z > 5) v = L_(3);
-                else if (z == 5) v = (L_(2) + 3 * L_(3) + 2) >> 2;
-                else if ((z & 1) == 0) v = (L_(j) + L_(j + 1) + 1) >> 1;
-                else v = (L_(j) + 2 * L_(j + 1) + L_(j + 2) + 2) >> 2;
-                break;
-            }
-            }
-            out[y * 4 + x] = v;
-        }
-#undef T_
-#undef L_
+// The 4x4 intra predictors (predict_nxn, h264/intra.rs:30-128; ITU-T H.264 8.3.1.2) as a table: every sample
+// of every mode other than DC is (E[a] + 2 E[b] + E[c] + 2) >> 2 over the block's edge array E (E[0] the
+// top-left sample, E[1 + i] the 8 above, E[9 + j] the 4 to the left): a copy has a = b = c, a two-sample
+// average (x + y + 1) >> 1 has a = c = x, b = y, and (x + 3y + 2) >> 2 has b = c = y. Entry: a | b << 4 | c << 8.
+__device__ __forceinline__ unsigned i4_entry(int mode, int x, int y) {
+    auto T = [](int i) { return 1 + i; };                 // i >= -1: i = -1 is the top-left sample
+    auto L = [](int j) { return j < 0 ? 0 : 9 + j; };
+    auto e3 = [](int a, int b, int c) { return (unsigned)(a | b << 4 | c << 8); };
+    switch (mode) {
+    case 0: return e3(T(x), T(x), T(x));
+    case 1: return e3(L(y), L(y), L(y));
+    case 3: return (x == 3 && y == 3) ? e3(T(6), T(7), T(7)) : e3(T(x + y), T(x + y + 1), T(x + y + 2));
+    case 4:
+        if (x > y) return e3(T(x - y - 2), T(x - y - 1), T(x - y));
+        if (x < y) return e3(L(y - x - 2), L(y - x - 1), L(y - x));
+        return e3(T(0), 0, L(0));
+    case 5: {
+        const int z = 2 * x - y, i = x - (y >> 1);
+        if (z >= 0 && (z & 1) == 0) return e3(T(i - 1), T(i), T(i - 1));
+        if (z >= 0) return e3(T(i - 2), T(i - 1), T(i));
+        if (z == -1) return e3(L(0), 0, T(0));
+        return e3(L(y - 2 * x - 1), L(y - 2 * x - 2), L(y - 2 * x - 3));
+    }
+    case 6: {
+        const int z = 2 * y - x, j = y - (x >> 1);
+        if (z >= 0 && (z & 1) == 0) return e3(L(j - 1), L(j), L(j - 1));
+        if (z >= 0) return e3(L(j - 2), L(j - 1), L(j));
+        if (z == -1) return e3(L(0), 0, T(0));
+        return e3(T(x - 2 * y - 1), T(x - 2 * y - 2), T(x - 2 * y - 3));
+    }
+    case 7: {
+        const int i = x + (y >> 1);
+        return (y & 1) == 0 ? e3(T(i), T(i + 1), T(i)) : e3(T(i), T(i + 1), T(i + 2));
+    }
+    case 8: {
+        const int z = x + 2 * y, j = y + (x >> 1);
+        if (z > 5) return e3(L(3), L(3), L(3));
+        if (z == 5) return e3(L(2), L(3), L(3));
+        if ((z & 1) == 0) return e3(L(j), L(j + 1), L(j));
+        return e3(L(j), L(j + 1), L(j + 2));
+    }
+    default: return 0;  // DC: not a table entry
+    }
 }
+
+// fdct4 (enc/frame.rs:113-132) of a 4x4 block held one value a lane (lane 4r + c, lanes 0-15): the lane's
+// coefficient at raster position (r, c). Every lane takes part in the shuffles.
+__device__ __forceinline__ int fdct4_lanes(int v) {
+    const int lane = threadIdx.x & 31, r = (lane >> 2) & 3, c = lane & 3, base = lane & ~3;
+    const int a0 = __shfl_sync(FULL, v, base), a1 = __shfl_sync(FULL, v, base + 1), a2 = __shfl_sync(FULL, v, base + 2), a3 = __shfl_sync(FULL, v, base + 3);
+    int s03 = a0 + a3, d03 = a0 - a3, s12 = a1 + a2, d12 = a1 - a2;
+    const int t = c == 0 ? s03 + s12 : (c == 1 ? 2 * d03 + d12 : (c == 2 ? s03 - s12 : d03 - 2 * d12));
+    const int b0 = __shfl_sync(FULL, t, c), b1 = __shfl_sync(FULL, t, 4 + c), b2 = __shfl_sync(FULL, t, 8 + c), b3 = __shfl_sync(FULL, t, 12 + c);
+    s03 = b0 + b3, d03 = b0 - b3, s12 = b1 + b2, d12 = b1 - b2;
+    return r == 0 ? s03 + s12 : (r == 1 ? 2 * d03 + d12 : (r == 2 ? s03 - s12 : d03 - 2 * d12));
+}
+
+// idct4_add (h264/idct.rs:8-31) of raster coefficients held one a lane onto the lane's prediction sample.
+__device__ __forceinline__ int idct4_lanes(int co, int pred, int maxv) {
+    const int lane = threadIdx.x & 31, r = (lane >> 2) & 3, c = lane & 3, base = lane & ~3;
+    const int c0 = __shfl_sync(FULL, co, base), c1 = __shfl_sync(FULL, co, base + 1), c2 = __shfl_sync(FULL, co, base + 2), c3 = __shfl_sync(FULL, co, base + 3);
+    const int e0 = c0 + c2, e1 = c0 - c2, e2 = (c1 >> 1) - c3, e3 = c1 + (c3 >> 1);
+    const int t = c == 0 ? e0 + e3 : (c == 1 ? e1 + e2 : (c == 2 ? e1 - e2 : e0 - e3));
+    const int t0 = __shfl_sync(FULL, t, c), t1 = __shfl_sync(FULL, t, 4 + c), t2 = __shfl_sync(FULL, t, 8 + c), t3 = __shfl_sync(FULL, t, 12 + c);
+    const int g0 = t0 + t2, g1 = t0 - t2, g2 = (t1 >> 1) - t3, g3 = t1 + (t3 >> 1);
+    const int h = r == 0 ? g0 + g3 : (r == 1 ? g1 + g2 : (r == 2 ? g1 - g2 : g0 - g3));
+    return min(max(pred + ((h + 32) >> 6), 0), maxv);
+}
+
+// The scan position of raster coefficient p (the inverse of ZIGZAG4), as nibbles.
+__device__ __forceinline__ int invzz4_at(int p) { return (int)((0xFEA9DB83C7426510ull >> (4 * p)) & 15); }
 
 // The Intra16x16 prediction of sample (x, y) (predict_16x16, h264/intra.rs:161-209): dcv the DC value, (pa,
 // pb, pc) the plane parameters.
@@ -266,10 +278,11 @@ __device__ __forceinline__ int zorder_d(int bx, int by) { return ((by >> 1) << 3
 
 // code_i4, enc/frame.rs:1050-1138, as a trial: block by block in decoding order, each predicted from the
 // reconstruction so far (S.i4rec inside the macroblock, the neighbours' around it), its mode the cheapest
-// by SATD + lambda * (1 for the predicted mode, 4 otherwise), coded with the intra rounding and
-// reconstructed into S.i4rec. Returns the summed cost (every lane).
+// by SATD + lambda * (1 for the predicted mode, 4 otherwise; lanes 0-8, a mode each, from the table tab),
+// coded with the intra rounding and reconstructed into S.i4rec (lanes 0-15, a coefficient each). Returns
+// the summed cost (every lane).
 template <class T>
-__device__ int code_i4_trial(const DecideParams& P, DecideSmem<T>& S, bool ta, bool la, bool tra) {
+__device__ int code_i4_trial(const DecideParams& P, DecideSmem<T>& S, const unsigned* tab, bool ta, bool la, bool tra) {
     const int lane = threadIdx.x & 31;
     const int bd = P.C.bd, maxv = (1 << bd) - 1, lam = P.C.A.lambda;
     const int qp = P.C.qp + 6 * (bd - 8), m6 = qp % 6, qbits = 15 + qp / 6, f = (1 << qbits) / 3;
@@ -289,8 +302,7 @@ __device__ int code_i4_trial(const DecideParams& P, DecideSmem<T>& S, bool ta, b
                 if (htl) v = by == 0 ? S.top[bx * 4] : (bx == 0 ? S.left[by * 4 - 1] : S.i4rec[(by * 4 - 1) * 16 + bx * 4 - 1]);
             } else if (lane < 9) {
                 const int i = lane - 1;
-                const bool avail = ht && (i < 4 || htr);
-                const int xi = avail ? i : 3;  // above-right not available: the last sample above repeated
+                const int xi = (i < 4 || htr) ? i : 3;  // above-right not available: the last sample above repeated
                 if (ht) v = by == 0 ? S.top[1 + bx * 4 + xi] : S.i4rec[(by * 4 - 1) * 16 + bx * 4 + xi];
             } else {
                 const int j = lane - 9;
@@ -303,54 +315,42 @@ __device__ int code_i4_trial(const DecideParams& P, DecideSmem<T>& S, bool ta, b
         const int a = bx > 0 ? S.i4modes[by * 4 + bx - 1] : S.nbm[by];
         const int b = by > 0 ? S.i4modes[(by - 1) * 4 + bx] : S.nbm[4 + bx];
         const int predicted = (a >= 0 && b >= 0) ? min(a, b) : 2;
-        int pr[16];
+        // the DC value (8.3.1.2.3)
+        const int st = S.edge[1] + S.edge[2] + S.edge[3] + S.edge[4], sl = S.edge[9] + S.edge[10] + S.edge[11] + S.edge[12];
+        const int dcv = (ht && hl) ? (st + sl + 4) >> 3 : (hl ? (sl + 2) >> 2 : (ht ? (st + 2) >> 2 : 1 << (bd - 1)));
         unsigned key = 0xffffffffu;
-        if (lane < 9) {
-            const int mode = lane;
-            const bool ok = (mode == 0 || mode == 3 || mode == 7) ? ht : ((mode == 1 || mode == 8) ? hl : (mode == 2 ? true : (ht && hl && htl)));
-            if (ok) {
-                i_pred4_d(mode, S.edge, ht, hl, bd, pr);
-                int d[16];
+        {
+            const int mode = lane < 9 ? lane : 2;
+            const bool ok = lane < 9 &&
+                            ((mode == 0 || mode == 3 || mode == 7) ? ht : ((mode == 1 || mode == 8) ? hl : (mode == 2 ? true : (ht && hl && htl))));
+            int d[16];
 #pragma unroll
-                for (int r = 0; r < 4; r++)
-#pragma unroll
-                    for (int k = 0; k < 4; k++) d[r * 4 + k] = src_at(S.a, bx * 4 + k, by * 4 + r) - pr[r * 4 + k];
-                const int cost = satd4_d(d) + lam * (mode == predicted ? 1 : 4);
-                key = ((unsigned)cost << 4) | (unsigned)mode;  // the cheapest, the lowest mode on ties
+            for (int k = 0; k < 16; k++) {
+                const unsigned e = tab[mode * 17 + k];
+                const int pv = mode == 2 ? dcv : (S.edge[e & 15] + 2 * S.edge[(e >> 4) & 15] + S.edge[(e >> 8) & 15] + 2) >> 2;
+                d[k] = src_at(S.a, bx * 4 + (k & 3), by * 4 + (k >> 2)) - pv;
             }
+            const int cost = satd4_d(d) + lam * (mode == predicted ? 1 : 4);
+            if (ok) key = ((unsigned)cost << 4) | (unsigned)mode;  // the cheapest, the lowest mode on ties
         }
 #pragma unroll
         for (int off = 16; off >= 1; off >>= 1) key = min(key, __shfl_xor_sync(FULL, key, off));
         const int bm = (int)(key & 15u);
         total += (int)(key >> 4);
-        if (lane == bm) {
-            // quant_block (intra), enc/frame.rs:1025-1046, then the reconstruction
-            int d[16], c[16], co[16];
-#pragma unroll
-            for (int r = 0; r < 4; r++)
-#pragma unroll
-                for (int k = 0; k < 4; k++) d[r * 4 + k] = src_at(S.a, bx * 4 + k, by * 4 + r) - pr[r * 4 + k];
-            q_fdct4_d(d, c);
-            int nz = 0;
-#pragma unroll
-            for (int k = 0; k < 16; k++) {
-                const int pz = zz4_at(k);
-                const int l = q_quant_d(c[pz], c_q_mf[m6][q_class_d(pz)], f, qbits);
-                S.i4lv[by * 4 + bx][k] = (int16_t)l;
-                co[pz] = (l * c_q_v[m6][q_class_d(pz)]) << (qp / 6);
-                nz += l != 0;
-            }
-            int rb[16];
-            if (nz > 0) {
-                q_idct4_d(co, pr, maxv, rb);
-            } else {
-#pragma unroll
-                for (int k = 0; k < 16; k++) rb[k] = pr[k];
-            }
-#pragma unroll
-            for (int r = 0; r < 4; r++)
-#pragma unroll
-                for (int k = 0; k < 4; k++) S.i4rec[(by * 4 + r) * 16 + bx * 4 + k] = rb[r * 4 + k];
+        // quant_block (intra), enc/frame.rs:1025-1046, and the reconstruction: a coefficient a lane
+        const int p = lane & 15, r = p >> 2, c = p & 3;
+        const unsigned e = tab[bm * 17 + p];
+        const int pv = bm == 2 ? dcv : (S.edge[e & 15] + 2 * S.edge[(e >> 4) & 15] + S.edge[(e >> 8) & 15] + 2) >> 2;
+        const int coef = fdct4_lanes(src_at(S.a, bx * 4 + c, by * 4 + r) - pv);
+        const int cls = q_class_d(p);
+        const int l = q_quant_d(coef, c_q_mf[m6][cls], f, qbits);
+        const int nz = __popc(__ballot_sync(FULL, lane < 16 && l != 0));
+        const int rec = idct4_lanes((l * c_q_v[m6][cls]) << (qp / 6), pv, maxv);
+        if (lane < 16) {
+            S.i4lv[by * 4 + bx][invzz4_at(p)] = (int16_t)l;
+            S.i4rec[(by * 4 + r) * 16 + bx * 4 + c] = nz > 0 ? rec : pv;
+        }
+        if (lane == 0) {
             S.i4nnz[by * 4 + bx] = (uint8_t)nz;
             S.i4modes[by * 4 + bx] = (uint8_t)bm;
         }
@@ -588,7 +588,7 @@ __device__ void inter_tail(const DecideParams& P, DecideSmem<T>& S, const ironav
 
 // code_mb for one P macroblock without CABAC, enc/frame.rs:715-790.
 template <class T>
-__device__ void decide_mb(const DecideParams& P, DecideSmem<T>& S, int mb, int mbx, int mby) {
+__device__ void decide_mb(const DecideParams& P, DecideSmem<T>& S, const unsigned* i4tab, int mb, int mbx, int mby) {
     const int lane = threadIdx.x & 31;
     const AnalyseParams& A = P.C.A;
     const CodeParams& C = P.C;
@@ -688,7 +688,7 @@ __device__ void decide_mb(const DecideParams& P, DecideSmem<T>& S, int mb, int m
     // Intra4x4 is tried by coding it when intra is competitive (766-779)
     bool i4 = false;
     if (best_intra < cost) {
-        const int c4 = code_i4_trial(P, S, ta, la, tra) + lam * 6;
+        const int c4 = code_i4_trial(P, S, i4tab, ta, la, tra) + lam * 6;
         if (c4 < best_intra) {
             best_intra = c4;
             i4 = true;
@@ -756,6 +756,9 @@ __device__ void decide_mb(const DecideParams& P, DecideSmem<T>& S, int mb, int m
 template <class T>
 __global__ void __launch_bounds__(K7_WARPS * 32, K7_MIN_BLOCKS) decide_kernel(const __grid_constant__ DecideParams P) {
     __shared__ DecideSmem<T> smem[K7_WARPS];
+    __shared__ unsigned i4tab[9 * 17];  // i4_entry per mode and sample, rows padded against bank conflicts
+    for (int t = threadIdx.x; t < 9 * 16; t += blockDim.x) i4tab[(t >> 4) * 17 + (t & 15)] = i4_entry(t >> 4, t & 3, (t >> 2) & 3);
+    __syncthreads();
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     DecideSmem<T>& S = smem[wid];
     const AnalyseParams& A = P.C.A;
@@ -781,7 +784,7 @@ __global__ void __launch_bounds__(K7_WARPS * 32, K7_MIN_BLOCKS) decide_kernel(co
         ok = __all_sync(FULL, ok);
         if (!ok) break;
         load_neighbours(A, S.a, A.states_out);
-        decide_mb<T>(P, S, mb, mbx, mby);
+        decide_mb<T>(P, S, i4tab, mb, mbx, mby);
         if (lane < 18) reinterpret_cast<uint32_t*>(&A.states_out[mb])[lane] = reinterpret_cast<const uint32_t*>(&S.a.out)[lane];
         // the reconstruction, code and state before the flag
         __threadfence();
