@@ -24,7 +24,7 @@ struct DecideParams {
 };
 
 constexpr int K7_WARPS = 4;
-constexpr int K7_MIN_BLOCKS = 4;
+constexpr int K7_MIN_BLOCKS = 2;  // the wavefront keeps few macroblocks in flight: registers (255, no spills) over occupancy
 constexpr int KIND_I4 = 1, KIND_I16 = 3, KIND_INTER = 5;  // Kind, h264/mb.rs:21-30
 
 template <class T>

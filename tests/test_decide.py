@@ -426,3 +426,14 @@ def test_gpu_decide_device_form_and_refusals(oracle_lib, cuda_lib):
     c.begin_p_picture(22)
     with pytest.raises(Exception):
         c.decide_p_picture()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("size,nslices", [((16, 16), 1), ((32, 16), 1), ((48, 48), 3), ((176, 144), 9), ((200, 120), 2)])
+def test_gpu_decide_small_and_ragged_pictures(oracle_lib, cuda_lib, size, nslices):
+    """One macroblock, one row, a slice per macroblock row, and sizes that are not whole macroblocks
+    (the source and references padded by repeating their edges)."""
+    for new_content in (False, True):
+        o, _, _ = decide_case(oracle_lib, size=size, nslices=nslices, new_content=new_content, qp=24)
+        c, _, _ = decide_case(cuda_lib, size=size, nslices=nslices, new_content=new_content, qp=24, threads=False)
+        _same_decisions(c.decide_p_picture(), o.decide_p_picture(), f"{size} {nslices} {new_content}")
