@@ -52,7 +52,7 @@ def parse():
     p.add_argument("--ring", type=int, default=RING,
                    help="pictures in the ring (fewer than 36 fits in L2: for profiling runs only)")
     p.add_argument("--no-e2e", action="store_true", help="skip the host-buffer pass (profiling runs)")
-    p.add_argument("--workload", default="1080p", choices=["1080p", "batched", "scenecut", "deblock", "bpicture", "residual", "decide"],
+    p.add_argument("--workload", default="1080p", choices=["1080p", "batched", "scenecut", "deblock", "bpicture", "residual", "decide", "decide_batched"],
                    help="1080p: one stream, replay mode (the headline); batched: 64 mixed-resolution streams in auto "
                         "mode, one launch per stage and frame step, against the per-stream launch loop")
     p.add_argument("--streams", type=int, default=64, help="streams of the batched workload")
@@ -270,6 +270,9 @@ def main():
         return finish(world)
     if args.workload == "decide":
         run_decide(args, rank, world)
+        return finish(world)
+    if args.workload == "decide_batched":
+        run_decide_batched(args, rank, world)
         return finish(world)
 
     import torch
@@ -679,6 +682,156 @@ def run_bpicture(args, rank, world):
                                 "sample": f"{n_cpu} B pictures (the ring's first), replay mode, {cores} threads, {t_cpu:.1f} s"}
     if rank == 0:
         print(json.dumps(line), flush=True)
+    for st in stages:
+        st.close()
+
+
+def run_decide_batched(args, rank, world):
+    """Decide mode for many streams in one launch (ironav_batch_decide): streams with resolutions drawn
+    from {640x360, 854x480, 1280x720, 1920x1080} (the batched configuration's), QP 27, one reference each;
+    one step = every stream's P picture decided and coded. Compared with the per-stream loop (each
+    stream's own decide launch, one after another). Streams are split across ranks."""
+    import torch
+    from ironav_b200.inter import MBCODE_DTYPE, InterBatch, InterStage, cuda_library
+    from ironav_b200.synth import Sequence, batch_streams
+
+    lib = cuda_library()
+    dev = torch.device("cuda", torch.cuda.current_device())
+    mine = batch_streams(args.streams)[rank::world]
+    stream = torch.cuda.Stream()
+    stages, bufs, pin_src, d_src, seqs = [], [], [], [], []
+    for (w, h, ns, seed) in mine:
+        seq = Sequence.config("1080p", 2, seed=seed, size=(w, h))
+        st = InterStage(w, h, nslices=ns, lib=lib)
+        st.push_reference(seq.frame(0))
+        st.push_reference_chroma(*seq.chroma(0))
+        st.set_source(seq.frame(1))
+        st.set_source_chroma(*seq.chroma(1))
+        st.begin_p_picture(QP)
+        st.set_stream(stream.cuda_stream)
+        stages.append(st)
+        seqs.append((seq.frame(0), seq.chroma(0), seq.frame(1), seq.chroma(1)))
+        pin_src.append(torch.from_numpy(seq.frame(1)).pin_memory())
+        d_src.append(torch.empty((h, w), dtype=torch.uint8, device=dev))
+        bufs.append((torch.zeros(st.nmb * 72, dtype=torch.uint8, device=dev), torch.zeros(st.nmb * MBCODE_DTYPE.itemsize, dtype=torch.uint8, device=dev),
+                     torch.zeros((st.mb_h * 16, st.mb_w * 16), dtype=torch.uint8, device=dev),
+                     torch.zeros((2, st.mb_h * 8, st.mb_w * 8), dtype=torch.uint8, device=dev)))
+    n = len(stages)
+    nmb = sum(st.nmb for st in stages)
+    torch.cuda.synchronize()
+    batch = InterBatch(stages)
+    dargs = ([b[0].data_ptr() for b in bufs], [b[1].data_ptr() for b in bufs], [b[2].data_ptr() for b in bufs],
+             [b[2].shape[1] for b in bufs], [b[3][0].data_ptr() for b in bufs], [b[3][1].data_ptr() for b in bufs],
+             [b[3].shape[2] for b in bufs])
+
+    def batched():
+        batch.decide(*dargs)
+
+    def plain():
+        for k, st in enumerate(stages):
+            s_, c_, y, c = bufs[k]
+            r = lib.ironav_decide_p_picture_device(st.ctx, s_.data_ptr(), c_.data_ptr(), y.data_ptr(), y.shape[1], c[0].data_ptr(),
+                                                   c[1].data_ptr(), c.shape[2])
+            if r:
+                raise RuntimeError(f"ironav_decide_p_picture_device: {r}")
+
+    def timed(fn, k):
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(k)]
+        for i in range(k):
+            evs[i][0].record(stream)
+            fn()
+            evs[i][1].record(stream)
+        torch.cuda.synchronize()
+        return [a.elapsed_time(b) for a, b in evs]
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            batched()
+        batch.sync()
+        clocks = Clocks(int(os.environ.get("LOCAL_RANK", 0)))
+        clocks.start()
+        t_load = time.perf_counter()
+        while time.perf_counter() - t_load < 0.6:
+            batched()
+            batch.sync()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        per = timed(batched, args.steps)
+        e1.record(stream)
+        batch.sync()
+        clk = clocks.stop()
+        ms = e0.elapsed_time(e1)
+        plain_ms = float(np.median(timed(plain, max(2, min(args.steps, 5)))))
+        # end to end: every stream's source luma from pinned host memory, the launch, and the states, codes
+        # and reconstructions back to pinned host memory, each step
+        host = [(torch.empty(b[0].shape, dtype=torch.uint8).pin_memory(), torch.empty(b[1].shape, dtype=torch.uint8).pin_memory(),
+                 torch.empty(b[2].shape, dtype=torch.uint8).pin_memory(), torch.empty(b[3].shape, dtype=torch.uint8).pin_memory())
+                for b in bufs]
+
+        def e2e_step():
+            for k, st in enumerate(stages):
+                d_src[k].copy_(pin_src[k], non_blocking=True)
+                st.set_source_device(d_src[k].data_ptr(), d_src[k].shape[1])
+            batched()
+            for k in range(n):
+                for a, b in zip(host[k], bufs[k]):
+                    a.copy_(b, non_blocking=True)
+        for _ in range(2):
+            e2e_step()
+        batch.sync()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            e2e_step()
+        batch.sync()
+        el = time.perf_counter() - t0
+    value = world * nmb * args.steps / (ms * 1e-3)
+    line = {
+        "metric": "P-picture macroblock decision + coding MB/s, many streams in one launch (CAVLC code_mb)", "value": value,
+        "unit": "MB/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+        "data": "synthetic: per-stream seeded value noise, pan, 8 moving rectangles, sigma 3; chroma from the 2x2 luma means",
+        "config": {"workload": f"{args.streams} streams ({n} on rank 0) of 640x360..1920x1080, {nmb} macroblocks per step on rank 0, QP "
+                               f"{QP}, one reference each, decide mode, ironav_batch_decide",
+                   "per_stream_loop_ms": plain_ms, "batched_ms": float(np.median(per)),
+                   "l2": "inputs of all streams (planes, chroma, codes, reconstructions) exceed L2"},
+        "gpu_launches": args.steps,
+        "e2e": {"value": world * nmb * args.steps / el, "unit": "MB/s",
+                "h2d_bytes_per_step": sum(int(p.numel()) for p in pin_src),
+                "d2h_bytes_per_step": sum(sum(int(t.numel()) for t in b) for b in bufs), "ms_per_step": 1e3 * el / args.steps,
+                "note": "each stream's source luma from pinned host memory (its chroma stays resident) + the launch + states, "
+                        "codes and reconstructions back to pinned host memory"},
+        "roofline": {"bound": "latency", "kernel": "decide_batch_kernel", "achieved": None, "peak": None, "unit": None, "frac": None,
+                     "traffic": None, "ms_per_launch": float(np.median(per)),
+                     "note": "many wavefronts interleaved; the per-stream loop above is the same work one stream at a time"},
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from tests.oracle_lib import oracle_library
+
+        olib = oracle_library()
+        cores = host_cores()
+        (w, h, ns, seed) = mine[0]
+        o = InterStage(w, h, nslices=ns, lib=olib)
+        olib.oracle_set_threads(o.ctx, cores)
+        f0, c0, f1, c1 = seqs[0]
+        o.push_reference(f0)
+        o.push_reference_chroma(*c0)
+        o.set_source(f1)
+        o.set_source_chroma(*c1)
+        o.begin_p_picture(QP)
+        n_cpu, t_cpu = 0, 0.0
+        while t_cpu < min(args.cpu_seconds, 10.0):
+            t0 = time.perf_counter()
+            o.decide_p_picture()
+            t_cpu += time.perf_counter() - t0
+            n_cpu += 1
+        line["cpu_baseline"] = {"value": n_cpu * o.nmb / t_cpu, "unit": "MB/s", "cores": min(cores, ns), "kind": "port",
+                                "sample": f"{n_cpu} pictures of the first stream ({w}x{h}, {ns} slice bands on {min(cores, ns)} threads), {t_cpu:.1f} s"}
+        o.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    batch.close()
     for st in stages:
         st.close()
 

@@ -7,8 +7,11 @@
  *   - the P_Skip vector and its SAD                          (code_mb, enc/frame.rs:722-729; skip_mv 597-603)
  *   - the inter partition decision with motion search       (best_inter, enc/frame.rs:839-938;
  *                                                             motion_search 949-1019)
- * and nothing after it: the rate-distortion choice against intra, residual coding and entropy
- * coding stay with the caller (code_mb, enc/frame.rs:752-790; decide_rd 1462-1513).
+ * and, around it, the steps either side that keep a P picture on the device: the coding of inter
+ * macroblocks once decided (code_inter, enc/frame.rs:1202-1305), the whole CAVLC macroblock decision
+ * with intra prediction (decide mode: code_mb, enc/frame.rs:715-790), B-picture searches, the deblocking
+ * filter and the scene-cut measure. Entropy coding and the CABAC rate-distortion decision (decide_rd,
+ * enc/frame.rs:1462-1513) stay with the caller.
  *
  * Two libraries implement this header:
  *   libironav_inter_cuda.so  the product: CUDA kernels for sm_100a (ironav_b200/).
@@ -410,6 +413,12 @@ int ironav_batch_step(ironav_batch* batch, const uint8_t* const* d_src, const ui
                       ironav_mbresult* const* d_results);
 /* Waits for the batch's queued work; IRONAV_TIMEOUT if a wavefront wait gave up. */
 int ironav_batch_sync(ironav_batch* batch);
+/* Decide mode for the current P picture of every stream in one persistent launch (the streams' wavefronts
+ * merged as in ironav_batch_step): each context prepared as for ironav_decide_p_picture_device (source,
+ * chroma, references with chroma, picture parameters); arrays of n device pointers and strides, stream
+ * i's outputs as that call's. Asynchronous; ironav_batch_sync waits. */
+int ironav_batch_decide(ironav_batch* batch, ironav_mbstate* const* d_states, ironav_mbcode* const* d_codes, void* const* d_rec_y,
+                        const int* y_strides, void* const* d_rec_cb, void* const* d_rec_cr, const int* c_strides);
 
 /* ---- analysis without allocation ------------------------------------------------------------------ */
 

@@ -70,7 +70,7 @@ __device__ __forceinline__ bool dbk_coded(const ironav_dbk_mb& m, int bx, int by
 __device__ __forceinline__ bool dbk_far(const int16_t* a, const int16_t* b) { return abs(a[0] - b[0]) >= 4 || abs(a[1] - b[1]) >= 4; }
 
 // motion_differs, deblock.rs:352-383 (frame macroblocks: the vertical limit is 4 quarter samples)
-__device__ bool dbk_motion_differs(const ironav_dbk_mb& p, int pbx, int pby, const ironav_dbk_mb& q, int qbx, int qby) {
+static __device__ bool dbk_motion_differs(const ironav_dbk_mb& p, int pbx, int pby, const ironav_dbk_mb& q, int qbx, int qby) {
     const int pi = pby * 4 + pbx, qi = qby * 4 + qbx;
     const int p8 = (pby >> 1) * 2 + (pbx >> 1), q8 = (qby >> 1) * 2 + (qbx >> 1);
     const int pr0 = p.ref_id[0][p8], pr1 = p.ref_id[1][p8], qr0 = q.ref_id[0][q8], qr1 = q.ref_id[1][q8];
@@ -174,7 +174,7 @@ static_assert(sizeof(DbkEdges) == 96, "DbkEdges layout");
 
 // Pass 1: the boundary strengths (strength, deblock.rs:391-408) and edge words of every macroblock
 // (deblock_mb's decisions, deblock.rs:608-695), one warp per macroblock, all macroblocks independent.
-__global__ void __launch_bounds__(DBK_WARPS * 32) deblock_edges_kernel(const __grid_constant__ DbkParams P, DbkEdges* __restrict__ out) {
+static __global__ void __launch_bounds__(DBK_WARPS * 32) deblock_edges_kernel(const __grid_constant__ DbkParams P, DbkEdges* __restrict__ out) {
     __shared__ ironav_dbk_mb rec[DBK_WARPS][3];
     __shared__ uint8_t bsm[DBK_WARPS][2][4][4];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;

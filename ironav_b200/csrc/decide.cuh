@@ -753,44 +753,93 @@ __device__ void decide_mb(const DecideParams& P, DecideSmem<T>& S, const unsigne
     __syncwarp();
 }
 
+// One macroblock of decide mode: waits for its left and top-right (top at the right edge) neighbours,
+// decides and codes it, and publishes it. Returns false when a wait gave up (the launch is abandoned).
+template <class T>
+__device__ bool decide_one(const DecideParams& P, DecideSmem<T>& S, const unsigned* i4tab, int mb) {
+    const int lane = threadIdx.x & 31;
+    const AnalyseParams& A = P.C.A;
+    const int mbx = mb % A.mb_w, mby = mb / A.mb_w;
+    if (lane == 0) {
+        S.a.mb = mb;
+        S.a.mbx = mbx;
+        S.a.mby = mby;
+    }
+    __syncwarp();
+    // their own waits cover the other neighbours
+    const int start = A.band_start[mby];
+    bool ok = true;
+    if (mbx > 0) ok = wait_published(A, mb - 1);
+    if (ok && mby > start) ok = wait_published(A, (mbx + 1 < A.mb_w) ? mb - A.mb_w + 1 : mb - A.mb_w);
+    if (!__all_sync(FULL, ok)) return false;
+    load_neighbours(A, S.a, A.states_out);
+    decide_mb<T>(P, S, i4tab, mb, mbx, mby);
+    if (lane < 18) reinterpret_cast<uint32_t*>(&A.states_out[mb])[lane] = reinterpret_cast<const uint32_t*>(&S.a.out)[lane];
+    // the reconstruction, code and state before the flag
+    __threadfence();
+    __syncwarp();
+    if (lane == 0 && mb != A.withhold) st_release(&A.flags[mb], A.epoch);
+    return true;
+}
+
+// The Intra4x4 predictor table of a CTA (i4_entry per mode and sample; rows padded against bank conflicts).
+__device__ __forceinline__ void fill_i4tab(unsigned* tab) {
+    for (int t = threadIdx.x; t < 9 * 16; t += blockDim.x) tab[(t >> 4) * 17 + (t & 15)] = i4_entry(t >> 4, t & 3, (t >> 2) & 3);
+    __syncthreads();
+}
+
 template <class T>
 __global__ void __launch_bounds__(K7_WARPS * 32, K7_MIN_BLOCKS) decide_kernel(const __grid_constant__ DecideParams P) {
     __shared__ DecideSmem<T> smem[K7_WARPS];
-    __shared__ unsigned i4tab[9 * 17];  // i4_entry per mode and sample, rows padded against bank conflicts
-    for (int t = threadIdx.x; t < 9 * 16; t += blockDim.x) i4tab[(t >> 4) * 17 + (t & 15)] = i4_entry(t >> 4, t & 3, (t >> 2) & 3);
-    __syncthreads();
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    DecideSmem<T>& S = smem[wid];
+    __shared__ unsigned i4tab[9 * 17];
+    fill_i4tab(i4tab);
+    const int lane = threadIdx.x & 31;
+    DecideSmem<T>& S = smem[threadIdx.x >> 5];
     const AnalyseParams& A = P.C.A;
     for (;;) {
         unsigned t = 0;
         if (lane == 0) t = atomicAdd(A.ticket, 1u);
         t = __shfl_sync(FULL, t, 0);
         if (t >= (unsigned)A.nmb) break;
-        const int mb = A.order[t];
-        const int mbx = mb % A.mb_w, mby = mb / A.mb_w;
-        if (lane == 0) {
-            S.a.mb = mb;
-            S.a.mbx = mbx;
-            S.a.mby = mby;
-        }
-        __syncwarp();
-        // the left and top-right (top at the right edge) neighbours; their own waits cover the rest
-        const int start = A.band_start[mby];
-        const int m1 = mb - 1, m2 = (mbx + 1 < A.mb_w) ? mb - A.mb_w + 1 : mb - A.mb_w;
-        bool ok = true;
-        if (mbx > 0) ok = wait_published(A, m1);
-        if (ok && mby > start) ok = wait_published(A, m2);
-        ok = __all_sync(FULL, ok);
-        if (!ok) break;
-        load_neighbours(A, S.a, A.states_out);
-        decide_mb<T>(P, S, i4tab, mb, mbx, mby);
-        if (lane < 18) reinterpret_cast<uint32_t*>(&A.states_out[mb])[lane] = reinterpret_cast<const uint32_t*>(&S.a.out)[lane];
-        // the reconstruction, code and state before the flag
-        __threadfence();
-        __syncwarp();
-        if (lane == 0 && mb != A.withhold) st_release(&A.flags[mb], A.epoch);
+        if (!decide_one<T>(P, S, i4tab, A.order[t])) break;
     }
 }
+
+// Decide mode for many streams in one launch: ticket t is order[t] = stream << 20 | macroblock, in the
+// streams' merged wavefront order (the batched form's); each stream's parameters in table[stream], copied
+// into the warp's shared memory when the warp moves to another stream.
+static __global__ void __launch_bounds__(K7_WARPS * 32, K7_MIN_BLOCKS) decide_batch_kernel(const DecideParams* __restrict__ table,
+                                                                                  const uint32_t* __restrict__ order, unsigned ntickets,
+                                                                                  unsigned* ticket, const unsigned* err) {
+    __shared__ DecideSmem<uint8_t> smem[K7_WARPS];
+    __shared__ DecideParams prm[K7_WARPS];
+    __shared__ unsigned i4tab[9 * 17];
+    fill_i4tab(i4tab);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    DecideSmem<uint8_t>& S = smem[wid];
+    int cur = -1;
+    for (;;) {
+        unsigned t = 0;
+        if (lane == 0) t = atomicAdd(ticket, 1u);
+        t = __shfl_sync(FULL, t, 0);
+        if (t >= ntickets || ld_acquire(err) != 0) break;
+        const uint32_t e = order[t];
+        const int stream = (int)(e >> 20);
+        if (stream != cur) {
+            const uint32_t* src = reinterpret_cast<const uint32_t*>(&table[stream]);
+            uint32_t* dst = reinterpret_cast<uint32_t*>(&prm[wid]);
+            for (int k = lane; k < (int)(sizeof(DecideParams) / 4); k += 32) dst[k] = src[k];
+            __syncwarp();
+            cur = stream;
+        }
+        if (!decide_one<uint8_t>(prm[wid], S, i4tab, (int)(e & 0xFFFFFu))) break;
+    }
+}
+
+// Fills decide mode's parameters for the context's current picture (host side, ironav_inter.cu): the
+// coding and the analysis parameters, the outputs; the caller sets the wavefront's fields (order, ticket,
+// flags, epoch, err). Returns IRONAV_INVALID_ARGUMENT when the picture is not ready for decide mode.
+int fill_decide_params(ironav_ctx* c, DecideParams& p, ironav_mbstate* d_states, ironav_mbcode* d_codes, void* y, int ys, void* cb, void* cr,
+                       int cs);
 
 }  // namespace ironav

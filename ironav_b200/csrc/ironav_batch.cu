@@ -13,6 +13,7 @@
 
 #include "analyse.cuh"
 #include "ctx.cuh"
+#include "decide.cuh"
 #include "planes.cuh"
 
 using namespace ironav;
@@ -153,6 +154,10 @@ struct ironav_batch {
     AnalyseParams* h_table = nullptr;
     cudaEvent_t copied = nullptr;
     bool pending = false;
+    // decide mode (allocated on first use): the streams' parameters and the launch's grid
+    DecideParams* d_dtable = nullptr;
+    DecideParams* h_dtable = nullptr;
+    int k7_blocks = 0;
 };
 
 static void free_batch(ironav_batch* b) {
@@ -165,6 +170,8 @@ static void free_batch(ironav_batch* b) {
     cudaFreeHost(b->h_pjobs);
     cudaFreeHost(b->h_sjobs);
     cudaFreeHost(b->h_table);
+    cudaFree(b->d_dtable);
+    cudaFreeHost(b->h_dtable);
     if (b->copied) cudaEventDestroy(b->copied);
     delete b;
 }
@@ -301,4 +308,42 @@ extern "C" int ironav_batch_sync(ironav_batch* b) {
     b->pending = false;  // the staging tables are free again
     if (err & 1u) return IRONAV_TIMEOUT;
     return err ? IRONAV_INTERNAL : IRONAV_OK;
+}
+
+extern "C" int ironav_batch_decide(ironav_batch* b, ironav_mbstate* const* d_states, ironav_mbcode* const* d_codes, void* const* d_y,
+                                   const int* y_strides, void* const* d_cb, void* const* d_cr, const int* c_strides) {
+    if (!b || !d_states || !d_codes || !d_y || !y_strides || !d_cb || !d_cr || !c_strides) return IRONAV_INVALID_ARGUMENT;
+    if (!b->d_dtable) {
+        CK(cudaMalloc(&b->d_dtable, sizeof(DecideParams) * b->n));
+        CK(cudaHostAlloc(&b->h_dtable, sizeof(DecideParams) * b->n, cudaHostAllocDefault));
+        int per_sm = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, decide_batch_kernel, K7_WARPS * 32, 0));
+        b->k7_blocks = std::max(1, per_sm) * b->ctx[0]->nsm;
+    }
+    // the staging table is reused: the previous step's copies must have left it
+    if (b->pending) CK(cudaEventSynchronize(b->copied));
+    for (int i = 0; i < b->n; i++) {
+        ironav_ctx* c = b->ctx[i];
+        if (!d_states[i] || !d_codes[i] || !d_y[i] || !d_cb[i] || !d_cr[i] || y_strides[i] < c->pw || c_strides[i] < c->pw / 2)
+            return IRONAV_INVALID_ARGUMENT;
+        // the planes as the single-stream device form; states and codes are written as 32-bit words
+        const uintptr_t a = reinterpret_cast<uintptr_t>(d_y[i]) | reinterpret_cast<uintptr_t>(d_cb[i]) | reinterpret_cast<uintptr_t>(d_cr[i]);
+        if ((a & 15) || y_strides[i] % 16 || c_strides[i] % 8) return IRONAV_INVALID_ARGUMENT;
+        if ((reinterpret_cast<uintptr_t>(d_states[i]) | reinterpret_cast<uintptr_t>(d_codes[i])) & 3) return IRONAV_INVALID_ARGUMENT;
+        DecideParams& p = b->h_dtable[i];
+        const int s = fill_decide_params(c, p, d_states[i], d_codes[i], d_y[i], y_strides[i], d_cb[i], d_cr[i], c_strides[i]);
+        if (s != IRONAV_OK) return s;
+        p.C.A.flags = b->d_flags + b->mb0[i];
+        p.C.A.epoch = 1;  // the flags are cleared every step
+        p.C.A.err = b->d_counters + 1;
+        p.C.err = b->d_counters + 1;
+    }
+    CK(cudaMemcpyAsync(b->d_dtable, b->h_dtable, sizeof(DecideParams) * b->n, cudaMemcpyHostToDevice, b->stream));
+    CK(cudaEventRecord(b->copied, b->stream));
+    b->pending = true;
+    CK(cudaMemsetAsync(b->d_flags, 0, sizeof(unsigned) * b->total_mbs, b->stream));
+    CK(cudaMemsetAsync(b->d_counters, 0, sizeof(unsigned) * 2, b->stream));
+    decide_batch_kernel<<<b->k7_blocks, K7_WARPS * 32, 0, b->stream>>>(b->d_dtable, b->d_order, (unsigned)b->total_mbs, b->d_counters,
+                                                                       b->d_counters + 1);
+    return cuda_status(cudaGetLastError());
 }

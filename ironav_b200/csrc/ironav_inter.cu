@@ -754,29 +754,19 @@ static void fast_thresholds(int qpp, int* luma, int* chroma) {
     *chroma = (int)std::ceil(128.0 * 0.05 * step);
 }
 
-static int launch_decide(ironav_ctx* c, ironav_mbstate* d_states, ironav_mbcode* d_codes, void* y, int ys, void* cb, void* cr, int cs) {
+}  // extern "C"
+
+// shared with the batched form (ironav_batch.cu)
+int ironav::fill_decide_params(ironav_ctx* c, DecideParams& p, ironav_mbstate* d_states, ironav_mbcode* d_codes, void* y, int ys, void* cb, void* cr,
+                               int cs) {
     if (!c->have_params || c->nact < 1 || c->nact > c->nrefs || !c->d_src_c) return IRONAV_INVALID_ARGUMENT;
     for (int i = 0; i < c->nact; i++)
         if (!c->ref_c_ok[c->slot_of[i]]) return IRONAV_INVALID_ARGUMENT;  // an active reference without chroma
-    if (!c->k7_blocks) {
-        int per_sm = 0;
-        const cudaError_t e = c->bd > 8 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, decide_kernel<uint16_t>, K7_WARPS * 32, 0)
-                                        : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, decide_kernel<uint8_t>, K7_WARPS * 32, 0);
-        if (e != cudaSuccess) return cuda_status(e);
-        c->k7_blocks = std::max(1, per_sm) * c->nsm;
-    }
-    DecideParams p;
     memset(&p, 0, sizeof(p));
     fill_params(c, p.C.A);
-    AnalyseParams& A = p.C.A;
-    A.states_out = d_states;
-    A.order = c->d_order;
-    A.ticket = c->d_counters;
-    A.flags = c->d_flags;
-    A.err = c->d_counters + 1;
-    A.nmb = c->nmb;
-    A.withhold = c->withhold;
-    A.epoch = ++c->epoch;
+    p.C.A.states_out = d_states;
+    p.C.A.nmb = c->nmb;
+    p.C.A.withhold = c->withhold;
     for (int i = 0; i < c->nact; i++) p.C.ref_c[i] = c->d_ref_c[c->slot_of[i]];
     p.C.src_c = c->d_src_c;
     p.C.cw = c->mb_w * 8;
@@ -789,9 +779,31 @@ static int launch_decide(ironav_ctx* c, ironav_mbstate* d_states, ironav_mbcode*
     p.C.qp = c->qpp - 6 * (c->bd - 8);
     p.C.bd = c->bd;
     p.C.nrefs = c->nact;
-    p.C.err = c->d_counters + 1;
     p.codes = d_codes;
     fast_thresholds(c->qpp, &p.fast_t, &p.fast_tc);
+    return IRONAV_OK;
+}
+
+extern "C" {
+
+static int launch_decide(ironav_ctx* c, ironav_mbstate* d_states, ironav_mbcode* d_codes, void* y, int ys, void* cb, void* cr, int cs) {
+    DecideParams p;
+    const int s = fill_decide_params(c, p, d_states, d_codes, y, ys, cb, cr, cs);
+    if (s != IRONAV_OK) return s;
+    if (!c->k7_blocks) {
+        int per_sm = 0;
+        const cudaError_t e = c->bd > 8 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, decide_kernel<uint16_t>, K7_WARPS * 32, 0)
+                                        : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, decide_kernel<uint8_t>, K7_WARPS * 32, 0);
+        if (e != cudaSuccess) return cuda_status(e);
+        c->k7_blocks = std::max(1, per_sm) * c->nsm;
+    }
+    AnalyseParams& A = p.C.A;
+    A.order = c->d_order;
+    A.ticket = c->d_counters;
+    A.flags = c->d_flags;
+    A.err = c->d_counters + 1;
+    A.epoch = ++c->epoch;
+    p.C.err = c->d_counters + 1;
     CK(cudaMemsetAsync(c->d_counters, 0, 2 * sizeof(unsigned), c->stream));
     if (c->bd > 8) decide_kernel<uint16_t><<<c->k7_blocks, K7_WARPS * 32, 0, c->stream>>>(p);
     else decide_kernel<uint8_t><<<c->k7_blocks, K7_WARPS * 32, 0, c->stream>>>(p);

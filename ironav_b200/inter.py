@@ -129,7 +129,7 @@ EXPORTS = (
     "ironav_deblock_picture", "ironav_deblock_picture_device",
     "ironav_begin_b_picture", "ironav_begin_b_picture_device", "ironav_analyse_b_replay", "ironav_analyse_b_replay_device",
     "ironav_set_source_chroma", "ironav_push_reference_chroma", "ironav_code_inter_picture", "ironav_code_inter_picture_device",
-    "ironav_decide_p_picture", "ironav_decide_p_picture_device",
+    "ironav_decide_p_picture", "ironav_decide_p_picture_device", "ironav_batch_decide",
 )
 
 SCENE_CUT = 0.8  # codec/change.rs:6
@@ -200,6 +200,9 @@ def _declare(lib: ctypes.CDLL) -> ctypes.CDLL:
         lib.ironav_batch_destroy.argtypes = [_VP]
         lib.ironav_batch_step.argtypes = [_VP] + [ctypes.POINTER(_VP)] * 5
         lib.ironav_batch_sync.argtypes = [_VP]
+    if hasattr(lib, "ironav_batch_decide"):
+        lib.ironav_batch_decide.argtypes = [_VP, ctypes.POINTER(_VP), ctypes.POINTER(_VP), ctypes.POINTER(_VP), ctypes.POINTER(_I),
+                                            ctypes.POINTER(_VP), ctypes.POINTER(_VP), ctypes.POINTER(_I)]
     if hasattr(lib, "ironav_analyse_auto_noalloc"):
         # (d_src, src_stride, d_ref, ref_stride, ref_w, ref_h, d_col, width, height, nslices, qp_prime, lambda,
         #  skip_thresh, fast, sub8, d_planes, d_states, d_results, stream)
@@ -603,6 +606,15 @@ class InterBatch:
         mk = lambda xs: (_VP * n)(*[x if x is not None else None for x in xs])
         InterStage._check(self.lib.ironav_batch_step(self.h, mk(d_src), mk(d_ref), mk(d_col), mk(d_states), mk(d_results)),
                           "ironav_batch_step")
+
+    def decide(self, d_states, d_codes, d_y, y_strides, d_cb, d_cr, c_strides) -> None:
+        """Decide mode for every stream's current P picture in one launch: lists of device pointers (ints)
+        and strides, one entry per stream (ironav_batch_decide)."""
+        n = len(self.stages)
+        vp = lambda xs: (_VP * n)(*xs)
+        ip = lambda xs: (ctypes.c_int * n)(*xs)
+        InterStage._check(self.lib.ironav_batch_decide(self.h, vp(d_states), vp(d_codes), vp(d_y), ip(y_strides), vp(d_cb), vp(d_cr),
+                                                       ip(c_strides)), "ironav_batch_decide")
 
     def sync(self) -> None:
         InterStage._check(self.lib.ironav_batch_sync(self.h), "ironav_batch_sync")

@@ -1096,6 +1096,11 @@ int ironav_batch_step(ironav_batch* b, const uint8_t* const* s, const uint8_t* c
     return IRONAV_HARDWARE_UNAVAILABLE;
 }
 int ironav_batch_sync(ironav_batch* b) { (void)b; return IRONAV_INVALID_ARGUMENT; }
+int ironav_batch_decide(ironav_batch* b, ironav_mbstate* const* s, ironav_mbcode* const* c, void* const* y, const int* ys, void* const* cb,
+                        void* const* cr, const int* cs) {
+    (void)b; (void)s; (void)c; (void)y; (void)ys; (void)cb; (void)cr; (void)cs;
+    return IRONAV_INVALID_ARGUMENT;
+}
 
 /* ---------------------------------------------------------------------------------------------------
  * Scene-cut measure: LowRes::new (codec/change.rs:16-24) on the padded source as H264Encoder::low_res

@@ -437,3 +437,37 @@ def test_gpu_decide_small_and_ragged_pictures(oracle_lib, cuda_lib, size, nslice
         o, _, _ = decide_case(oracle_lib, size=size, nslices=nslices, new_content=new_content, qp=24)
         c, _, _ = decide_case(cuda_lib, size=size, nslices=nslices, new_content=new_content, qp=24, threads=False)
         _same_decisions(c.decide_p_picture(), o.decide_p_picture(), f"{size} {nslices} {new_content}")
+
+
+@pytest.mark.gpu
+def test_gpu_batched_decide_matches_single_streams(oracle_lib, cuda_lib):
+    """Four streams of different sizes, slice layouts and content decided in one launch: each stream's
+    codes, states and reconstruction are those of its own decide call (and so the oracle's)."""
+    import torch
+
+    from ironav_b200.inter import MBSTATE_DTYPE, InterBatch
+
+    cases = [dict(), dict(new_content=True, qp=30), dict(size=(320, 176), nslices=3, fast=True), dict(cfg="1080p", nslices=8, qp=27)]
+    stages = [decide_case(cuda_lib, threads=False, **kw)[0] for kw in cases]
+    want = [st.decide_p_picture() for st in stages]
+    o = decide_case(oracle_lib, **cases[1])[0]
+    _same_decisions(want[1], o.decide_p_picture(), "single stream, intra-heavy")
+    stream = torch.cuda.Stream()
+    for st in stages:
+        st.set_stream(stream.cuda_stream)
+    bufs = []
+    for st in stages:
+        bufs.append((torch.zeros(st.nmb * 72, dtype=torch.uint8, device="cuda"), torch.full((st.nmb * 1516,), 0x5A, dtype=torch.uint8, device="cuda"),
+                     torch.zeros((st.mb_h * 16, st.mb_w * 16), dtype=torch.uint8, device="cuda"),
+                     torch.zeros((2, st.mb_h * 8, st.mb_w * 8), dtype=torch.uint8, device="cuda")))
+    batch = InterBatch(stages)
+    for _ in range(2):  # twice: the flags are cleared every launch
+        batch.decide([b[0].data_ptr() for b in bufs], [b[1].data_ptr() for b in bufs], [b[2].data_ptr() for b in bufs],
+                     [b[2].shape[1] for b in bufs], [b[3][0].data_ptr() for b in bufs], [b[3][1].data_ptr() for b in bufs],
+                     [b[3].shape[2] for b in bufs])
+        batch.sync()
+    for k, (st, b) in enumerate(zip(stages, bufs)):
+        got = (b[0].cpu().numpy().view(MBSTATE_DTYPE), b[1].cpu().numpy().view(MBCODE_DTYPE),
+               (b[2].cpu().numpy(), b[3][0].cpu().numpy(), b[3][1].cpu().numpy()))
+        _same_decisions(got, want[k], f"stream {k} {cases[k]}")
+    batch.close()
