@@ -471,3 +471,48 @@ def test_gpu_batched_decide_matches_single_streams(oracle_lib, cuda_lib):
                (b[2].cpu().numpy(), b[3][0].cpu().numpy(), b[3][1].cpu().numpy()))
         _same_decisions(got, want[k], f"stream {k} {cases[k]}")
     batch.close()
+
+
+@pytest.mark.gpu
+def test_gpu_decide_wait_times_out_and_recovers(oracle_lib, cuda_lib):
+    """A macroblock whose flag is never published (the test withholds it, on the host) makes the waits
+    behind it give up after a bounded number of polls: the call reports a timeout, the context stays
+    usable, and the next picture is the oracle's. The same in a batch, where one stream's wait ends the launch."""
+    import torch
+
+    from ironav_b200.inter import InterBatch, IronavError
+
+    o, _, _ = decide_case(oracle_lib, new_content=True)
+    c, _, _ = decide_case(cuda_lib, new_content=True, threads=False)
+    assert cuda_lib.ironav_debug_wait_limit(c.ctx, 20000) == 0
+    assert cuda_lib.ironav_debug_withhold(c.ctx, 5) == 0
+    with pytest.raises(IronavError) as e:
+        c.decide_p_picture()
+    assert e.value.status == 100
+    assert cuda_lib.ironav_debug_withhold(c.ctx, -1) == 0
+    assert cuda_lib.ironav_debug_wait_limit(c.ctx, 1 << 22) == 0  # the default: a whole picture's waits fit in it
+    _same_decisions(c.decide_p_picture(), o.decide_p_picture(), "after a timeout")
+
+    c2, _, _ = decide_case(cuda_lib, threads=False)
+    stream = torch.cuda.Stream()
+    for st in (c, c2):
+        st.set_stream(stream.cuda_stream)
+    bufs = [(torch.zeros(st.nmb * 72, dtype=torch.uint8, device="cuda"), torch.zeros(st.nmb * 1516, dtype=torch.uint8, device="cuda"),
+             torch.zeros((st.mb_h * 16, st.mb_w * 16), dtype=torch.uint8, device="cuda"),
+             torch.zeros((2, st.mb_h * 8, st.mb_w * 8), dtype=torch.uint8, device="cuda")) for st in (c, c2)]
+    args = ([b[0].data_ptr() for b in bufs], [b[1].data_ptr() for b in bufs], [b[2].data_ptr() for b in bufs], [b[2].shape[1] for b in bufs],
+            [b[3][0].data_ptr() for b in bufs], [b[3][1].data_ptr() for b in bufs], [b[3].shape[2] for b in bufs])
+    batch = InterBatch([c, c2])
+    assert cuda_lib.ironav_debug_withhold(c2.ctx, 40) == 0
+    for st in (c, c2):
+        assert cuda_lib.ironav_debug_wait_limit(st.ctx, 20000) == 0
+    batch.decide(*args)
+    with pytest.raises(IronavError) as e:
+        batch.sync()
+    assert e.value.status == 100
+    assert cuda_lib.ironav_debug_withhold(c2.ctx, -1) == 0
+    for st in (c, c2):
+        assert cuda_lib.ironav_debug_wait_limit(st.ctx, 1 << 22) == 0
+    batch.decide(*args)
+    batch.sync()
+    batch.close()
