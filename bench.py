@@ -910,6 +910,34 @@ def run_decide(args, rank, world):
     ms = e0.elapsed_time(e1)
     k_ms = float(np.mean([a.elapsed_time(b) for a, b in evs]))
     value = world * nmb * args.steps / (ms * 1e-3)
+    # the whole P picture on the device: decide, the filter's records, deblocking (the reference's order,
+    # enc/mod.rs:633-655), one stream
+    from ironav_b200.inter import DBK_MB_DTYPE
+    from ironav_b200.synth import dbk_encoder_slices
+
+    d_mbs = [torch.zeros(nmb * DBK_MB_DTYPE.itemsize, dtype=torch.uint8, device=dev) for _ in range(ring)]
+    slices = dbk_encoder_slices(NSLICES)
+
+    def picture(i):
+        k = i % ring
+        s_, c_, y, c = bufs[k]
+        step(i)
+        r = lib.ironav_decide_dbk_records_device(stages[k].ctx, c_.data_ptr(), s_.data_ptr(), d_mbs[k].data_ptr())
+        if r:
+            raise RuntimeError(f"ironav_decide_dbk_records_device: {r}")
+        stages[k].deblock_device(y.data_ptr(), y.shape[1], c[0].data_ptr(), c[1].data_ptr(), c.shape[2], d_mbs[k].data_ptr(), slices)
+
+    with torch.cuda.stream(stream):
+        for i in range(args.warmup):
+            picture(i)
+        torch.cuda.synchronize()
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        p0.record(stream)
+        for i in range(args.steps):
+            picture(args.warmup + i)
+        p1.record(stream)
+        torch.cuda.synchronize()
+    pic_ms = p0.elapsed_time(p1) / args.steps
     codes = bufs[0][1].cpu().numpy().view(MBCODE_DTYPE)
     kinds = {"skip": int(codes["skip"].sum()), "inter": int(((codes["kind"] == 5) & (codes["skip"] == 0)).sum()),
              "i16": int((codes["kind"] == 3).sum()), "i4": int((codes["kind"] == 1).sum())}
@@ -933,6 +961,9 @@ def run_decide(args, rank, world):
                                f"reference, 8 slice bands, wavefront); decisions: {kinds}",
                    "slices": NSLICES, "mode": "decide (device pointers)",
                    "l2": f"ring of {ring} contexts (reference planes, chroma, states, codes, reconstructions > L2)"},
+        "picture_pipeline": {"ms_per_picture": pic_ms, "MB/s": world * nmb / (pic_ms * 1e-3),
+                             "note": "decide + ironav_decide_dbk_records_device + the deblocking filter (two launches), "
+                                     "device pointers, the same ring, timed after the main region"},
         "gpu_launches": args.steps,
         "e2e": {"value": world * nmb * args.steps / el, "unit": "MB/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": nmb * (72 + MBCODE_DTYPE.itemsize + 384 * B), "ms_per_step": 1e3 * el / args.steps,

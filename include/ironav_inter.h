@@ -348,6 +348,15 @@ typedef struct ironav_dbk_slice {
     int32_t chroma_qp_offset[2];  /* Cb, Cr */
 } ironav_dbk_slice;
 
+/* The filter's record of every macroblock decide mode coded, as finish_mb makes MbInfo
+ * (enc/frame.rs:2323-2339): the slice id (band + 1, enc/mod.rs:608), inter or not, QP_Y of the picture's
+ * parameters, t8x8 and the luma coefficient counts of its code, and for an inter macroblock list 0's
+ * reference index per 8x8 block with its identity (1 + index) and the vectors of its state. codes and
+ * states are one picture's ironav_decide_p_picture outputs; mbs receives mb_w*mb_h records. */
+int ironav_decide_dbk_records(ironav_ctx* ctx, const ironav_mbcode* codes, const ironav_mbstate* states, ironav_dbk_mb* mbs);
+/* The same on device pointers (4-byte aligned), queued on the context's stream. */
+int ironav_decide_dbk_records_device(ironav_ctx* ctx, const ironav_mbcode* d_codes, const ironav_mbstate* d_states, ironav_dbk_mb* d_mbs);
+
 /* Filters a picture of the context's size and sample depth in place: luma 16*mb_w x 16*mb_h samples,
  * rows y_stride samples apart; Cb and Cr 8*mb_w x 8*mb_h, rows c_stride apart (the layout of
  * Picture::planes). mbs: mb_w*mb_h records; slices: nslices entries, the slice ids of mbs index them.

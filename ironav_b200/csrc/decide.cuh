@@ -836,6 +836,41 @@ static __global__ void __launch_bounds__(K7_WARPS * 32, K7_MIN_BLOCKS) decide_ba
     }
 }
 
+// finish_mb's MbInfo for the deblocking filter (enc/frame.rs:2323-2339), a thread per macroblock: slice id
+// band + 1 (enc/mod.rs:608), inter or not, QP_Y, t8x8 and the luma counts of the code; an inter
+// macroblock's list-0 reference per 8x8 block, its identity (1 + index) and vectors from its state.
+static __global__ void dbk_records_kernel(const ironav_mbcode* __restrict__ codes, const ironav_mbstate* __restrict__ states,
+                                          const int* __restrict__ band_start, int mb_w, int nmb, int qp, ironav_dbk_mb* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nmb) return;
+    const int row = i / mb_w;
+    // the band of the row: rows where a band starts, counted up to it
+    int band = 0;
+    for (int r = 1; r <= row; r++) band += band_start[r] == r;
+    const ironav_mbcode& k = codes[i];
+    const ironav_mbstate& st = states[i];
+    ironav_dbk_mb m;
+    m.slice = (uint16_t)(band + 1);
+    m.inter = k.kind == KIND_INTER;
+    m.qp = (int8_t)qp;
+    m.t8x8 = k.res.t8x8;
+    m.keep = 0;
+    m.pad[0] = m.pad[1] = 0;
+    for (int b = 0; b < 16; b++) m.nnz[b] = k.res.nnz[b];
+    for (int b = 0; b < 4; b++) {
+        m.ref_idx[0][b] = m.inter ? st.refs[b] : (int8_t)-1;
+        m.ref_id[0][b] = m.inter ? 1 + st.refs[b] : -1;
+        m.ref_idx[1][b] = -1;
+        m.ref_id[1][b] = -1;
+    }
+    for (int b = 0; b < 16; b++) {
+        m.mv[0][b][0] = m.inter ? st.mvs[b][0] : (int16_t)0;
+        m.mv[0][b][1] = m.inter ? st.mvs[b][1] : (int16_t)0;
+        m.mv[1][b][0] = m.mv[1][b][1] = 0;
+    }
+    out[i] = m;
+}
+
 // Fills decide mode's parameters for the context's current picture (host side, ironav_inter.cu): the
 // coding and the analysis parameters, the outputs; the caller sets the wavefront's fields (order, ticket,
 // flags, epoch, err). Returns IRONAV_INVALID_ARGUMENT when the picture is not ready for decide mode.

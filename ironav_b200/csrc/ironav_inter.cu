@@ -819,6 +819,28 @@ int ironav_decide_p_picture_device(ironav_ctx* c, ironav_mbstate* d_states, iron
     return launch_decide(c, d_states, d_codes, y, ys, cb, cr, cs);
 }
 
+int ironav_decide_dbk_records_device(ironav_ctx* c, const ironav_mbcode* d_codes, const ironav_mbstate* d_states, ironav_dbk_mb* d_mbs) {
+    if (!c || !d_codes || !d_states || !d_mbs || !c->have_params) return IRONAV_INVALID_ARGUMENT;
+    if ((reinterpret_cast<uintptr_t>(d_codes) | reinterpret_cast<uintptr_t>(d_states) | reinterpret_cast<uintptr_t>(d_mbs)) & 3)
+        return IRONAV_INVALID_ARGUMENT;
+    dbk_records_kernel<<<(c->nmb + 127) / 128, 128, 0, c->stream>>>(d_codes, d_states, c->d_band_start, c->mb_w, c->nmb,
+                                                                     c->qpp - 6 * (c->bd - 8), d_mbs);
+    return cuda_status(cudaGetLastError());
+}
+
+int ironav_decide_dbk_records(ironav_ctx* c, const ironav_mbcode* codes, const ironav_mbstate* states, ironav_dbk_mb* mbs) {
+    if (!c || !codes || !states || !mbs || !c->have_params) return IRONAV_INVALID_ARGUMENT;
+    if (!c->d_mbcodes) CK(cudaMalloc(&c->d_mbcodes, sizeof(ironav_mbcode) * c->nmb));
+    if (!c->d_dbk_mbs) CK(cudaMalloc(&c->d_dbk_mbs, sizeof(ironav_dbk_mb) * c->nmb));
+    CK(cudaMemcpyAsync(c->d_mbcodes, codes, sizeof(ironav_mbcode) * c->nmb, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->d_states, states, sizeof(ironav_mbstate) * c->nmb, cudaMemcpyHostToDevice, c->stream));
+    const int s = ironav_decide_dbk_records_device(c, c->d_mbcodes, c->d_states, c->d_dbk_mbs);
+    if (s != IRONAV_OK) return s;
+    CK(cudaMemcpyAsync(mbs, c->d_dbk_mbs, sizeof(ironav_dbk_mb) * c->nmb, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return IRONAV_OK;
+}
+
 int ironav_decide_p_picture(ironav_ctx* c, ironav_mbstate* states, ironav_mbcode* codes, void* y, int ys, void* cb, void* cr, int cs) {
     if (!c || !states || !codes || !y || !cb || !cr || ys < c->pw || cs < c->pw / 2) return IRONAV_INVALID_ARGUMENT;
     const size_t B = (size_t)sample_bytes(c), pw = (size_t)c->pw, ph = (size_t)c->ph;

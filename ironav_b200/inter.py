@@ -129,7 +129,8 @@ EXPORTS = (
     "ironav_deblock_picture", "ironav_deblock_picture_device",
     "ironav_begin_b_picture", "ironav_begin_b_picture_device", "ironav_analyse_b_replay", "ironav_analyse_b_replay_device",
     "ironav_set_source_chroma", "ironav_push_reference_chroma", "ironav_code_inter_picture", "ironav_code_inter_picture_device",
-    "ironav_decide_p_picture", "ironav_decide_p_picture_device", "ironav_batch_decide",
+    "ironav_decide_p_picture", "ironav_decide_p_picture_device", "ironav_batch_decide", "ironav_decide_dbk_records",
+    "ironav_decide_dbk_records_device",
 )
 
 SCENE_CUT = 0.8  # codec/change.rs:6
@@ -191,6 +192,8 @@ def _declare(lib: ctypes.CDLL) -> ctypes.CDLL:
         lib.ironav_code_inter_picture_device.argtypes = [_VP, _I, _VP, _VP, _VP, _I, _VP, _VP, _I]
     if hasattr(lib, "ironav_decide_p_picture"):
         lib.ironav_decide_p_picture.argtypes = [_VP, _VP, _VP, _VP, _I, _VP, _VP, _I]
+        lib.ironav_decide_dbk_records.argtypes = [_VP, _VP, _VP, _VP]
+        lib.ironav_decide_dbk_records_device.argtypes = [_VP, _VP, _VP, _VP]
         lib.ironav_decide_p_picture_device.argtypes = [_VP, _VP, _VP, _VP, _I, _VP, _VP, _I]
     if hasattr(lib, "ironav_deblock_picture"):
         lib.ironav_deblock_picture.argtypes = [_VP, _VP, _I, _VP, _VP, _I, _VP, _VP, _I]
@@ -452,6 +455,14 @@ class InterStage:
         self._check(self.lib.ironav_decide_p_picture(self.ctx, _ptr(states), _ptr(codes), _ptr(y), y.shape[1], _ptr(cb), _ptr(cr),
                                                      cb.shape[1]), "ironav_decide_p_picture")
         return states, codes, (y, cb, cr)
+
+    def decide_dbk_records(self, codes: np.ndarray, states: np.ndarray) -> np.ndarray:
+        """The deblocking filter's macroblock records (DBK_MB_DTYPE) of a picture decide_p_picture coded."""
+        codes = np.ascontiguousarray(codes, dtype=MBCODE_DTYPE)
+        states = np.ascontiguousarray(states, dtype=MBSTATE_DTYPE)
+        mbs = np.zeros(self.nmb, dtype=DBK_MB_DTYPE)
+        self._check(self.lib.ironav_decide_dbk_records(self.ctx, _ptr(codes), _ptr(states), _ptr(mbs)), "ironav_decide_dbk_records")
+        return mbs
 
     # -- deblocking of the reconstruction (h264/deblock.rs) ------------------------------------------------
 

@@ -2733,3 +2733,40 @@ int ironav_decide_p_picture_device(ironav_ctx* c, ironav_mbstate* s, ironav_mbco
     (void)c; (void)s; (void)o; (void)y; (void)ys; (void)cb; (void)cr; (void)cs;
     return IRONAV_HARDWARE_UNAVAILABLE;
 }
+
+/* finish_mb's MbInfo for the deblocking filter, enc/frame.rs:2323-2339 (slice ids: enc/mod.rs:608) */
+int ironav_decide_dbk_records(ironav_ctx* c, const ironav_mbcode* codes, const ironav_mbstate* states, ironav_dbk_mb* mbs) {
+    if (!c || !codes || !states || !mbs || c->nact < 1) return IRONAV_INVALID_ARGUMENT;
+    int band = 0, qp_y = c->qpp - 6 * (c->bd - 8);
+    for (int r = 0; r < c->mb_h; r++) {
+        if (r > 0 && c->band_start[r] == r) band++;
+        for (int x = 0; x < c->mb_w; x++) {
+            size_t i = (size_t)r * c->mb_w + x;
+            const ironav_mbcode* k = &codes[i];
+            ironav_dbk_mb* m = &mbs[i];
+            memset(m, 0, sizeof(*m));
+            m->slice = (uint16_t)(band + 1);
+            m->inter = k->kind == KIND_INTER;
+            m->qp = (int8_t)qp_y;
+            m->t8x8 = k->res.t8x8;
+            memcpy(m->nnz, k->res.nnz, 16);
+            for (int l = 0; l < 2; l++)
+                for (int b = 0; b < 4; b++) {
+                    m->ref_idx[l][b] = -1;
+                    m->ref_id[l][b] = -1;
+                }
+            if (m->inter)
+                for (int b = 0; b < 4; b++) {
+                    m->ref_idx[0][b] = states[i].refs[b];
+                    m->ref_id[0][b] = 1 + states[i].refs[b];
+                }
+            if (m->inter) memcpy(m->mv[0], states[i].mvs, sizeof(m->mv[0]));
+        }
+    }
+    return IRONAV_OK;
+}
+
+int ironav_decide_dbk_records_device(ironav_ctx* c, const ironav_mbcode* d_codes, const ironav_mbstate* d_states, ironav_dbk_mb* d_mbs) {
+    (void)c; (void)d_codes; (void)d_states; (void)d_mbs;
+    return IRONAV_HARDWARE_UNAVAILABLE;
+}

@@ -516,3 +516,77 @@ def test_gpu_decide_wait_times_out_and_recovers(oracle_lib, cuda_lib):
     batch.decide(*args)
     batch.sync()
     batch.close()
+
+
+# ---- the whole P picture: decide, the filter's records, deblocking ------------------------------------
+
+def _py_records(st, codes, states, qp_y, nslices):
+    """finish_mb's MbInfo fields the filter reads (enc/frame.rs:2323-2339), restated from the codes."""
+    from ironav_b200.inter import DBK_MB_DTYPE
+
+    m = np.zeros(st.nmb, dtype=DBK_MB_DTYPE)
+    rows = np.arange(st.nmb) // st.mb_w
+    starts = [(st.mb_h * k) // nslices for k in range(nslices)]
+    m["slice"] = 1 + np.array([sum(1 for s in starts[1:] if s <= r) for r in rows])
+    inter = codes["kind"] == KIND_INTER
+    m["inter"] = inter
+    m["qp"] = qp_y
+    m["t8x8"] = codes["res"]["t8x8"]
+    m["nnz"] = codes["res"]["nnz"]
+    m["ref_idx"] = -1
+    m["ref_id"] = -1
+    m["ref_idx"][inter, 0] = states["refs"][inter]
+    m["ref_id"][inter, 0] = 1 + states["refs"][inter].astype(np.int32)
+    m["mv"][inter, 0] = states["mvs"][inter]
+    return m
+
+
+@pytest.mark.parametrize("kw", [dict(qp=34, nslices=3), dict(new_content=True, qp=30), dict(refs=2, qp=28, nslices=2)])
+def test_oracle_picture_pipeline(oracle_lib, kw):
+    from ironav_b200.synth import dbk_encoder_slices
+
+    st, fr, ch = decide_case(oracle_lib, **kw)
+    states, codes, rec = st.decide_p_picture()
+    mbs = st.decide_dbk_records(codes, states)
+    want = _py_records(st, codes, states, kw["qp"], kw.get("nslices", 2))
+    for f in mbs.dtype.names:
+        assert np.array_equal(mbs[f], want[f]), f
+    y, cb, cr = st.deblock(*rec, mbs, dbk_encoder_slices(kw.get("nslices", 2)))
+    assert not np.array_equal(y, rec[0])  # the filter acted on block edges
+    h, w = fr[1].shape
+    assert psnr(y[:h, :w], fr[1]) > psnr(rec[0][:h, :w], fr[1]) - 0.5
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kw", [dict(qp=34, nslices=3), dict(new_content=True, qp=30), dict(cfg="1080p", nslices=8, qp=27),
+                                dict(bd=10, qp=30, new_content=True)])
+def test_gpu_picture_pipeline_on_the_device(oracle_lib, cuda_lib, kw):
+    """decide → the filter's records → deblocking, all on device pointers, equals the oracle's picture."""
+    import torch
+
+    from ironav_b200.inter import DBK_MB_DTYPE
+    from ironav_b200.synth import dbk_encoder_slices
+
+    ns = kw.get("nslices", 2)
+    o, _, _ = decide_case(oracle_lib, **kw)
+    s_o, c_o, r_o = o.decide_p_picture()
+    m_o = o.decide_dbk_records(c_o, s_o)
+    want = o.deblock(*r_o, m_o, dbk_encoder_slices(ns))
+    c, _, _ = decide_case(cuda_lib, threads=False, **kw)
+    assert np.array_equal(c.decide_dbk_records(c_o, s_o), m_o)
+    c.set_stream(torch.cuda.current_stream().cuda_stream)
+    dt = torch.uint8 if c.bd == 8 else torch.int16
+    y = torch.zeros((c.mb_h * 16, c.mb_w * 16), dtype=dt, device="cuda")
+    cc = torch.zeros((2, c.mb_h * 8, c.mb_w * 8), dtype=dt, device="cuda")
+    ts = torch.zeros(c.nmb * 72, dtype=torch.uint8, device="cuda")
+    tc = torch.zeros(c.nmb * 1516, dtype=torch.uint8, device="cuda")
+    tm = torch.zeros(c.nmb * DBK_MB_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
+    assert c.lib.ironav_decide_p_picture_device(c.ctx, ts.data_ptr(), tc.data_ptr(), y.data_ptr(), y.shape[1], cc[0].data_ptr(),
+                                                cc[1].data_ptr(), cc.shape[2]) == 0
+    assert c.lib.ironav_decide_dbk_records_device(c.ctx, tc.data_ptr(), ts.data_ptr(), tm.data_ptr()) == 0
+    c.deblock_device(y.data_ptr(), y.shape[1], cc[0].data_ptr(), cc[1].data_ptr(), cc.shape[2], tm.data_ptr(), dbk_encoder_slices(ns))
+    c.sync()
+    view = (lambda t: t.cpu().numpy().view(np.uint16)) if c.bd == 10 else (lambda t: t.cpu().numpy())
+    for name, a, b in zip("Y Cb Cr".split(), (view(y), view(cc[0]), view(cc[1])), want):
+        assert np.array_equal(a, b), f"{kw}: {name} differs at {np.argwhere(a != b)[:4].tolist()}"
+    assert np.array_equal(tm.cpu().numpy().view(DBK_MB_DTYPE), m_o)
