@@ -590,3 +590,13 @@ def test_gpu_picture_pipeline_on_the_device(oracle_lib, cuda_lib, kw):
     for name, a, b in zip("Y Cb Cr".split(), (view(y), view(cc[0]), view(cc[1])), want):
         assert np.array_equal(a, b), f"{kw}: {name} differs at {np.argwhere(a != b)[:4].tolist()}"
     assert np.array_equal(tm.cpu().numpy().view(DBK_MB_DTYPE), m_o)
+
+
+@pytest.mark.gpu
+def test_gpu_decide_4k(oracle_lib, cuda_lib):
+    """3840x2160 (32,400 macroblocks, 16 slice bands as the encoder cuts 4K on a 16-core host), two
+    references with sub-8x8 partitions: the largest picture the benchmarks use."""
+    kw = dict(cfg="4k", nslices=16, qp=27, refs=2, sub8=True)
+    o, _, _ = decide_case(oracle_lib, **kw)
+    c, _, _ = decide_case(cuda_lib, threads=False, **kw)
+    _same_decisions(c.decide_p_picture(), o.decide_p_picture(), "4K")
