@@ -132,7 +132,21 @@ class Clocks:
                 "window": "0.6 s of untimed steps, then the timed steps"}
 
 
+def max_over_ranks(value: float, world: int, device) -> float:
+    """The largest of every rank's value: a job's time is its slowest rank's. A tensor on `device` (the
+    GPU for NCCL, the CPU for gloo); one all-reduce when there are several ranks."""
+    import torch
+
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def make_frames(rank: int, n: int, bd: int = 8):
+    """The 1080p sequence of one rank: each replica analyses its own seeded sequence (weak scaling)."""
     from ironav_b200.synth import CONFIGS, Sequence
 
     w, h, seed, pan_q, nobj, vmax, sigma = CONFIGS["1080p"]
@@ -345,10 +359,7 @@ def main():
     st.sync()
     ms = e0.elapsed_time(e1)
     k2_ms = [a.elapsed_time(b) for a, b in k2_ev]
-    t_max = torch.tensor([ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
-    ms_max = float(t_max.item())
+    ms_max = max_over_ranks(ms, world, dev)
     value = world * nmb * args.steps / (ms_max * 1e-3)
 
     # algorithmic work of the timed launches (from the kernel's own per-macroblock counts)
@@ -460,10 +471,7 @@ def run_batched(args, rank, world):
                 fn(args.warmup + i)
             e1.record(stream)
             torch.cuda.synchronize()
-        ms = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=dev)
-        if world > 1:
-            dist.all_reduce(ms, op=dist.ReduceOp.MAX)
-        return float(ms.item())
+        return max_over_ranks(e0.elapsed_time(e1), world, dev)
 
     clocks = Clocks(int(os.environ.get("LOCAL_RANK", "0")))
     clocks.start()
@@ -1426,10 +1434,7 @@ def run_e2e(args, st, frames, d_states, nmb, world, torch, dist, dev, stream):
     t0 = time.perf_counter()
     run(args.warmup, args.steps)
     torch.cuda.synchronize()
-    el = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(el, op=dist.ReduceOp.MAX)
-    el = float(el.item())
+    el = max_over_ranks(time.perf_counter() - t0, world, dev)
     for ws, *_ in workers:
         ws.close()
     return {"value": world * nmb * args.steps / el, "unit": "MB/s",
