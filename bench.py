@@ -187,6 +187,36 @@ def cpu_baseline(frames, states, seconds: float, bd: int = 8):
                       f"{cores} threads, {elapsed:.2f} s; half-sample planes built outside the timing"}
 
 
+def cpu_slice_threads(frames, seconds: float, bd: int = 8):
+    """The reference-faithful CPU form: the oracle's slice loop (auto mode: each band's macroblocks in
+    raster order, deciding as it goes) with one thread per slice band, as the reference's slice threads
+    run (enc/mod.rs:620-628), on as many of the ring's pictures as fit in `seconds`."""
+    from tests.oracle_lib import oracle_library
+    from ironav_b200.inter import InterStage
+
+    lib = oracle_library()
+    threads = min(host_cores(), NSLICES)
+    st = InterStage(WIDTH, HEIGHT, nslices=NSLICES, lib=lib, bd=bd)
+    lib.oracle_set_threads(st.ctx, threads)
+    done_mb, elapsed, pics, prev = 0, 0.0, 0, None
+    while elapsed < seconds:
+        t = 1 + pics % (len(frames) - 1)
+        st.clear_references()
+        st.push_reference(frames[t - 1], col=prev if t >= 2 else None)
+        st.set_source(frames[t])
+        st.begin_p_picture(qp_prime(bd))
+        t0 = time.perf_counter()
+        prev, _ = st.analyse_auto()
+        elapsed += time.perf_counter() - t0
+        done_mb += st.nmb
+        pics += 1
+    st.close()
+    return {"value": done_mb / elapsed, "unit": "MB/s", "cores": threads, "kind": "port",
+            "sample": f"{pics} pictures of the 1080p {bd}-bit ring, auto mode, {NSLICES} slice bands on {threads} threads, "
+                      f"{elapsed:.2f} s; less work a macroblock than the replay workload: macroblocks under the P_Skip "
+                      f"threshold are not searched"}
+
+
 def host_cores() -> int:
     try:
         return len(os.sched_getaffinity(0))
@@ -403,6 +433,7 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         host_states = [None] + [d_states[t].cpu().numpy().view(MBSTATE_DTYPE) for t in range(1, RING)]
         line["cpu_baseline"] = cpu_baseline(frames, host_states, args.cpu_seconds, bd)
+        line["cpu_slice_threads"] = cpu_slice_threads(frames, min(args.cpu_seconds, 6.0), bd)
     if rank == 0:
         print(json.dumps(line), flush=True)
     st.close()
