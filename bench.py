@@ -824,6 +824,27 @@ def run_decide_batched(args, rank, world):
             e2e_step()
         batch.sync()
         el = time.perf_counter() - t0
+    # the whole P picture of every stream: batched decide, each stream's filter records, batched deblocking
+    from ironav_b200.inter import DBK_MB_DTYPE
+    from ironav_b200.synth import dbk_encoder_slices
+
+    d_mbs = [torch.zeros(st.nmb * DBK_MB_DTYPE.itemsize, dtype=torch.uint8, device=dev) for st in stages]
+    slice_tabs = [dbk_encoder_slices(ns) for (_, _, ns, _) in mine]
+
+    def pipeline():
+        batched()
+        for k, st in enumerate(stages):
+            r = lib.ironav_decide_dbk_records_device(st.ctx, bufs[k][1].data_ptr(), bufs[k][0].data_ptr(), d_mbs[k].data_ptr())
+            if r:
+                raise RuntimeError(f"ironav_decide_dbk_records_device: {r}")
+        batch.deblock(dargs[2], dargs[3], dargs[4], dargs[5], dargs[6], [t.data_ptr() for t in d_mbs], slice_tabs)
+
+    with torch.cuda.stream(stream):
+        for _ in range(2):
+            pipeline()
+        batch.sync()
+        pipe_ms = float(np.median(timed(pipeline, max(2, min(args.steps, 5)))))
+        batch.sync()
     value = world * nmb * args.steps / (ms * 1e-3)
     line = {
         "metric": "P-picture macroblock decision + coding MB/s, many streams in one launch (CAVLC code_mb)", "value": value,
@@ -833,6 +854,9 @@ def run_decide_batched(args, rank, world):
         "config": {"workload": f"{args.streams} streams ({n} on rank 0) of 640x360..1920x1080, {nmb} macroblocks per step on rank 0, QP "
                                f"{QP}, one reference each, decide mode, ironav_batch_decide",
                    "per_stream_loop_ms": plain_ms, "batched_ms": float(np.median(per)),
+                   "picture_pipeline_ms": pipe_ms,
+                   "picture_pipeline_note": "ironav_batch_decide + each stream's ironav_decide_dbk_records_device + "
+                                            "ironav_batch_deblock: every stream's P picture decided, coded and deblocked",
                    "l2": "inputs of all streams (planes, chroma, codes, reconstructions) exceed L2"},
         "gpu_launches": args.steps,
         "e2e": {"value": world * nmb * args.steps / el, "unit": "MB/s",

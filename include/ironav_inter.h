@@ -74,7 +74,7 @@ typedef struct ironav_mbresult {
     uint32_t sad_px;      /* samples compared by integer SAD evaluations in the reference's order (work count) */
     uint32_t satd_px;     /* samples compared by sub-sample SATD evaluations (work count) */
     uint32_t pad2;
-} ironav_mbresult;        /* 112 bytes */
+} ironav_mbresult;        /* 104 bytes */
 
 #define IRONAV_RESULT_INTER 1u   /* best_inter was evaluated (fields part..cost16 are valid) */
 #define IRONAV_RESULT_SKIP  2u   /* auto policy only: the macroblock was decided as P_Skip */
@@ -428,6 +428,14 @@ int ironav_batch_sync(ironav_batch* batch);
  * i's outputs as that call's. Asynchronous; ironav_batch_sync waits. */
 int ironav_batch_decide(ironav_batch* batch, ironav_mbstate* const* d_states, ironav_mbcode* const* d_codes, void* const* d_rec_y,
                         const int* y_strides, void* const* d_rec_cb, void* const* d_rec_cr, const int* c_strides);
+/* The deblocking filter of every stream's reconstructed picture, two launches in all (the streams' edge
+ * passes together, then their macroblock rows interleaved): arrays of n device pointers and strides, and
+ * per stream its records (d_mbs[i], 4-byte aligned) and slice table (slices[i], nslices[i]: host
+ * arrays), each as ironav_deblock_picture_device takes them. Asynchronous; ironav_batch_sync waits
+ * (IRONAV_INVALID_INPUT: a record names a slice beyond its stream's table). */
+int ironav_batch_deblock(ironav_batch* batch, void* const* d_y, const int* y_strides, void* const* d_cb, void* const* d_cr,
+                         const int* c_strides, const ironav_dbk_mb* const* d_mbs, const ironav_dbk_slice* const* slices,
+                         const int* nslices);
 
 /* ---- analysis without allocation ------------------------------------------------------------------ */
 

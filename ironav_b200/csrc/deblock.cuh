@@ -174,87 +174,93 @@ static_assert(sizeof(DbkEdges) == 96, "DbkEdges layout");
 
 // Pass 1: the boundary strengths (strength, deblock.rs:391-408) and edge words of every macroblock
 // (deblock_mb's decisions, deblock.rs:608-695), one warp per macroblock, all macroblocks independent.
+// One macroblock's boundary strengths and edge words (pass 1): R holds 3 records of shared memory (the
+// macroblock, its left and its top neighbour), Bs the strengths [dir][edge][segment].
+__device__ __forceinline__ void dbk_edges_mb(const DbkParams& P, DbkEdges* __restrict__ out, int idx, ironav_dbk_mb* R,
+                                             uint8_t (*Bs)[4][4]) {
+    const int lane = threadIdx.x & 31;
+    const int x = idx % P.mb_w, y = idx / P.mb_w;
+    for (int k = lane; k < 3 * 48; k += 32) {
+        const int which = k / 48, wd = k % 48;
+        const int src = which == 0 ? idx : (which == 1 ? (x > 0 ? idx - 1 : idx) : (y > 0 ? idx - P.mb_w : idx));
+        reinterpret_cast<uint32_t*>(&R[which])[wd] = __ldg(reinterpret_cast<const uint32_t*>(&P.mbs[src]) + wd);
+    }
+    __syncwarp();
+    const ironav_dbk_mb& m = R[0];
+    // the neighbours across the left and top edges; at the picture's edges the macroblock itself, whose
+    // outer edges are then not filtered (deblock.rs:618-621)
+    const ironav_dbk_mb& lm = R[1];
+    const ironav_dbk_mb& tm = R[2];
+    bool live = m.slice != 0;
+    if (live && m.slice > P.nslices) {
+        if (lane == 0) atomicOr(P.err, 4u);
+        live = false;
+    }
+    ironav_dbk_slice sp = {};
+    if (live) sp = P.slices[m.slice - 1];
+    live = live && sp.disable_deblocking != 1;
+    const bool left_ok = x > 0 && lm.slice != 0 && (sp.disable_deblocking == 0 || lm.slice == m.slice);
+    const bool top_ok = y > 0 && tm.slice != 0 && (sp.disable_deblocking == 0 || tm.slice == m.slice);
+    // inner edges of an inter macroblock moving as a whole with no coefficients are not filtered
+    // (uniform_motion, deblock.rs:385-389, and deblock.rs:625)
+    bool same = true;
+    if (lane < 16) {
+        same = m.nnz[lane] == 0 && m.mv[0][lane][0] == m.mv[0][0][0] && m.mv[0][lane][1] == m.mv[0][0][1] &&
+               m.mv[1][lane][0] == m.mv[1][0][0] && m.mv[1][lane][1] == m.mv[1][0][1];
+        if (lane < 4)
+            same = same && m.ref_idx[0][lane] == m.ref_idx[0][0] && m.ref_idx[1][lane] == m.ref_idx[1][0] &&
+                   m.ref_id[0][lane] == m.ref_id[0][0] && m.ref_id[1][lane] == m.ref_id[1][0];
+    }
+    const bool still = m.inter && __all_sync(DBK_ALL, same);
+    // boundary strengths: lane = dir * 16 + edge * 4 + segment
+    {
+        const int dir = lane >> 4, e = (lane >> 2) & 3, i = lane & 3;
+        const ironav_dbk_mb& o = e == 0 ? (dir == 0 ? lm : tm) : m;
+        int b = 0;
+        if (!(e > 0 && still)) {
+            if (!m.inter || !o.inter) {
+                b = e == 0 ? 4 : 3;
+            } else {
+                const int qx = dir == 0 ? e : i, qy = dir == 0 ? i : e;
+                const int px = dir == 0 ? (e == 0 ? 3 : e - 1) : i, py = dir == 0 ? i : (e == 0 ? 3 : e - 1);
+                b = (dbk_coded(m, qx, qy) || dbk_coded(o, px, py)) ? 2 : (dbk_motion_differs(o, px, py, m, qx, qy) ? 1 : 0);
+            }
+        }
+        Bs[dir][e][i] = (uint8_t)b;
+    }
+    __syncwarp();
+    DbkEdges& E = out[idx];
+    if (lane < 8) reinterpret_cast<uint32_t*>(E.bs)[lane] = reinterpret_cast<const uint32_t*>(Bs)[lane];
+    // edge words: lanes 0-7 luma (dir, edge), lanes 8-15 chroma (comp, dir, edge / 2)
+    if (lane < 16) {
+        const bool chroma = lane >= 8;
+        const int dir = chroma ? ((lane - 8) >> 1) & 1 : lane >> 2;
+        const int e = chroma ? ((lane - 8) & 1) * 2 : lane & 3;
+        const int comp = (lane - 8) >> 2;
+        const ironav_dbk_mb& o = e == 0 ? (dir == 0 ? lm : tm) : m;
+        const bool any = *reinterpret_cast<const uint32_t*>(Bs[dir][e]) != 0;
+        uint32_t wv = 0;
+        if (live && any && !(e == 0 && !(dir == 0 ? left_ok : top_ok)) && !(!chroma && m.t8x8 && (e & 1))) {
+            if (chroma) {
+                const int off = sp.chroma_qp_offset[comp];
+                wv = dbk_thresholds((dbk_chroma_qp(o.qp, off, P.bd) + dbk_chroma_qp(m.qp, off, P.bd) + 1) >> 1, sp);
+            } else {
+                wv = dbk_thresholds((o.qp + m.qp + 1) >> 1, sp);
+            }
+            if (wv) wv |= (uint32_t)((o.keep ? 1 : 0) | (m.keep ? 2 : 0)) << 28;
+        }
+        if (chroma) E.chroma[comp][dir][e >> 1] = wv;
+        else E.luma[dir][e] = wv;
+    }
+    __syncwarp();
+}
+
 static __global__ void __launch_bounds__(DBK_WARPS * 32) deblock_edges_kernel(const __grid_constant__ DbkParams P, DbkEdges* __restrict__ out) {
     __shared__ ironav_dbk_mb rec[DBK_WARPS][3];
     __shared__ uint8_t bsm[DBK_WARPS][2][4][4];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int wid = threadIdx.x >> 5;
     const int nmb = P.mb_w * P.mb_h;
-    for (int idx = blockIdx.x * DBK_WARPS + wid; idx < nmb; idx += gridDim.x * DBK_WARPS) {
-        const int x = idx % P.mb_w, y = idx / P.mb_w;
-        for (int k = lane; k < 3 * 48; k += 32) {
-            const int which = k / 48, wd = k % 48;
-            const int src = which == 0 ? idx : (which == 1 ? (x > 0 ? idx - 1 : idx) : (y > 0 ? idx - P.mb_w : idx));
-            reinterpret_cast<uint32_t*>(&rec[wid][which])[wd] = __ldg(reinterpret_cast<const uint32_t*>(&P.mbs[src]) + wd);
-        }
-        __syncwarp();
-        const ironav_dbk_mb& m = rec[wid][0];
-        // the neighbours across the left and top edges; at the picture's edges the macroblock itself, whose
-        // outer edges are then not filtered (deblock.rs:618-621)
-        const ironav_dbk_mb& lm = rec[wid][1];
-        const ironav_dbk_mb& tm = rec[wid][2];
-        bool live = m.slice != 0;
-        if (live && m.slice > P.nslices) {
-            if (lane == 0) atomicOr(P.err, 4u);
-            live = false;
-        }
-        ironav_dbk_slice sp = {};
-        if (live) sp = P.slices[m.slice - 1];
-        live = live && sp.disable_deblocking != 1;
-        const bool left_ok = x > 0 && lm.slice != 0 && (sp.disable_deblocking == 0 || lm.slice == m.slice);
-        const bool top_ok = y > 0 && tm.slice != 0 && (sp.disable_deblocking == 0 || tm.slice == m.slice);
-        // inner edges of an inter macroblock moving as a whole with no coefficients are not filtered
-        // (uniform_motion, deblock.rs:385-389, and deblock.rs:625)
-        bool same = true;
-        if (lane < 16) {
-            same = m.nnz[lane] == 0 && m.mv[0][lane][0] == m.mv[0][0][0] && m.mv[0][lane][1] == m.mv[0][0][1] &&
-                   m.mv[1][lane][0] == m.mv[1][0][0] && m.mv[1][lane][1] == m.mv[1][0][1];
-            if (lane < 4)
-                same = same && m.ref_idx[0][lane] == m.ref_idx[0][0] && m.ref_idx[1][lane] == m.ref_idx[1][0] &&
-                       m.ref_id[0][lane] == m.ref_id[0][0] && m.ref_id[1][lane] == m.ref_id[1][0];
-        }
-        const bool still = m.inter && __all_sync(DBK_ALL, same);
-        // boundary strengths: lane = dir * 16 + edge * 4 + segment
-        {
-            const int dir = lane >> 4, e = (lane >> 2) & 3, i = lane & 3;
-            const ironav_dbk_mb& o = e == 0 ? (dir == 0 ? lm : tm) : m;
-            int b = 0;
-            if (!(e > 0 && still)) {
-                if (!m.inter || !o.inter) {
-                    b = e == 0 ? 4 : 3;
-                } else {
-                    const int qx = dir == 0 ? e : i, qy = dir == 0 ? i : e;
-                    const int px = dir == 0 ? (e == 0 ? 3 : e - 1) : i, py = dir == 0 ? i : (e == 0 ? 3 : e - 1);
-                    b = (dbk_coded(m, qx, qy) || dbk_coded(o, px, py)) ? 2 : (dbk_motion_differs(o, px, py, m, qx, qy) ? 1 : 0);
-                }
-            }
-            bsm[wid][dir][e][i] = (uint8_t)b;
-        }
-        __syncwarp();
-        DbkEdges& E = out[idx];
-        if (lane < 8) reinterpret_cast<uint32_t*>(E.bs)[lane] = reinterpret_cast<const uint32_t*>(bsm[wid])[lane];
-        // edge words: lanes 0-7 luma (dir, edge), lanes 8-15 chroma (comp, dir, edge / 2)
-        if (lane < 16) {
-            const bool chroma = lane >= 8;
-            const int dir = chroma ? ((lane - 8) >> 1) & 1 : lane >> 2;
-            const int e = chroma ? ((lane - 8) & 1) * 2 : lane & 3;
-            const int comp = (lane - 8) >> 2;
-            const ironav_dbk_mb& o = e == 0 ? (dir == 0 ? lm : tm) : m;
-            const bool any = *reinterpret_cast<const uint32_t*>(bsm[wid][dir][e]) != 0;
-            uint32_t wv = 0;
-            if (live && any && !(e == 0 && !(dir == 0 ? left_ok : top_ok)) && !(!chroma && m.t8x8 && (e & 1))) {
-                if (chroma) {
-                    const int off = sp.chroma_qp_offset[comp];
-                    wv = dbk_thresholds((dbk_chroma_qp(o.qp, off, P.bd) + dbk_chroma_qp(m.qp, off, P.bd) + 1) >> 1, sp);
-                } else {
-                    wv = dbk_thresholds((o.qp + m.qp + 1) >> 1, sp);
-                }
-                if (wv) wv |= (uint32_t)((o.keep ? 1 : 0) | (m.keep ? 2 : 0)) << 28;
-            }
-            if (chroma) E.chroma[comp][dir][e >> 1] = wv;
-            else E.luma[dir][e] = wv;
-        }
-        __syncwarp();
-    }
+    for (int idx = blockIdx.x * DBK_WARPS + wid; idx < nmb; idx += gridDim.x * DBK_WARPS) dbk_edges_mb(P, out, idx, rec[wid], bsm[wid]);
 }
 
 // ---- pass 2: the samples, in the row wavefront ---------------------------------------------------------
@@ -471,6 +477,56 @@ __global__ void __launch_bounds__(DBK_WARPS * 32) deblock_rows_kernel(const __gr
         if (t & 1u) dbk_row<T, true>(P, edges, (int)(t >> 1), Ls[wid], Es[wid]);
         else dbk_row<T, false>(P, edges, (int)(t >> 1), Ls[wid], Es[wid]);
         if (ld_acquire(P.err) & 1u) return;
+    }
+}
+
+// ---- many streams in one launch per pass (the batched form, 8-bit) -----------------------------------
+
+// One stream of a batched deblocking launch: its parameters (planes, records, slices, progress words, the
+// batch's ticket and error words), its edge records, and its first macroblock in the launch's flat index.
+struct DbkJob {
+    DbkParams P;
+    DbkEdges* edges;
+    int mb0;
+};
+
+// Pass 1 for every stream: the flat macroblock index over the streams (stream by binary search on mb0).
+static __global__ void __launch_bounds__(DBK_WARPS * 32) deblock_edges_batch_kernel(const DbkJob* __restrict__ jobs, int njobs, int total) {
+    __shared__ ironav_dbk_mb rec[DBK_WARPS][3];
+    __shared__ uint8_t bsm[DBK_WARPS][2][4][4];
+    const int wid = threadIdx.x >> 5;
+    for (int idx = blockIdx.x * DBK_WARPS + wid; idx < total; idx += gridDim.x * DBK_WARPS) {
+        int lo = 0, hi = njobs - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (jobs[mid].mb0 <= idx) lo = mid;
+            else hi = mid - 1;
+        }
+        const DbkJob& J = jobs[lo];
+        dbk_edges_mb(J.P, J.edges, idx - J.mb0, rec[wid], bsm[wid]);
+    }
+}
+
+// Pass 2 for every stream: ticket t is order[t] = stream << 20 | the stream's own row ticket (2y luma row y,
+// 2y + 1 chroma row y), the streams' rows interleaved by their own tickets, so a row waits only on its own
+// stream's row above, which holds a smaller ticket.
+static __global__ void __launch_bounds__(DBK_WARPS * 32) deblock_rows_batch_kernel(const DbkJob* __restrict__ jobs,
+                                                                                   const uint32_t* __restrict__ order, unsigned ntickets,
+                                                                                   unsigned* ticket, const unsigned* err) {
+    __shared__ int Ls[DBK_WARPS][20][17];
+    __shared__ DbkEdges Es[DBK_WARPS];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (;;) {
+        unsigned t = 0;
+        if (lane == 0) t = atomicAdd(ticket, 1u);
+        t = __shfl_sync(DBK_ALL, t, 0);
+        if (t >= ntickets) return;
+        const uint32_t e = order[t];
+        const DbkJob& J = jobs[e >> 20];
+        const unsigned lt = e & 0xFFFFFu;
+        if (lt & 1u) dbk_row<uint8_t, true>(J.P, J.edges, (int)(lt >> 1), Ls[wid], Es[wid]);
+        else dbk_row<uint8_t, false>(J.P, J.edges, (int)(lt >> 1), Ls[wid], Es[wid]);
+        if (ld_acquire(err) & 1u) return;
     }
 }
 

@@ -158,6 +158,16 @@ struct ironav_batch {
     DecideParams* d_dtable = nullptr;
     DecideParams* h_dtable = nullptr;
     int k7_blocks = 0;
+    // deblocking (allocated on first use): the streams' jobs, their rows' merged ticket order, progress
+    // words, and the concatenated slice tables (pinned staging reused once the previous copies are done)
+    DbkJob* d_kjobs = nullptr;
+    DbkJob* h_kjobs = nullptr;
+    uint32_t* d_korder = nullptr;
+    unsigned* d_kprogress = nullptr;
+    int total_rows2 = 0;  // sum of 2 * mb_h
+    ironav_dbk_slice* d_kslices = nullptr;
+    ironav_dbk_slice* h_kslices = nullptr;
+    int kslice_cap = 0;
 };
 
 static void free_batch(ironav_batch* b) {
@@ -172,6 +182,12 @@ static void free_batch(ironav_batch* b) {
     cudaFreeHost(b->h_table);
     cudaFree(b->d_dtable);
     cudaFreeHost(b->h_dtable);
+    cudaFree(b->d_kjobs);
+    cudaFreeHost(b->h_kjobs);
+    cudaFree(b->d_korder);
+    cudaFree(b->d_kprogress);
+    cudaFree(b->d_kslices);
+    cudaFreeHost(b->h_kslices);
     if (b->copied) cudaEventDestroy(b->copied);
     delete b;
 }
@@ -307,6 +323,7 @@ extern "C" int ironav_batch_sync(ironav_batch* b) {
     CK(cudaStreamSynchronize(b->stream));
     b->pending = false;  // the staging tables are free again
     if (err & 1u) return IRONAV_TIMEOUT;
+    if (err & 4u) return IRONAV_INVALID_INPUT;  // a record names a slice beyond its stream's table
     return err ? IRONAV_INTERNAL : IRONAV_OK;
 }
 
@@ -345,5 +362,92 @@ extern "C" int ironav_batch_decide(ironav_batch* b, ironav_mbstate* const* d_sta
     CK(cudaMemsetAsync(b->d_counters, 0, sizeof(unsigned) * 2, b->stream));
     decide_batch_kernel<<<b->k7_blocks, K7_WARPS * 32, 0, b->stream>>>(b->d_dtable, b->d_order, (unsigned)b->total_mbs, b->d_counters,
                                                                        b->d_counters + 1);
+    return cuda_status(cudaGetLastError());
+}
+
+extern "C" int ironav_batch_deblock(ironav_batch* b, void* const* d_y, const int* y_strides, void* const* d_cb, void* const* d_cr,
+                                    const int* c_strides, const ironav_dbk_mb* const* d_mbs, const ironav_dbk_slice* const* slices,
+                                    const int* nslices) {
+    if (!b || !d_y || !y_strides || !d_cb || !d_cr || !c_strides || !d_mbs || !slices || !nslices) return IRONAV_INVALID_ARGUMENT;
+    int total_slices = 0;
+    for (int i = 0; i < b->n; i++) {
+        const ironav_ctx* c = b->ctx[i];
+        if (!d_y[i] || !d_cb[i] || !d_cr[i] || !d_mbs[i] || !slices[i] || nslices[i] < 1 || nslices[i] > 65535 || y_strides[i] < c->pw ||
+            c_strides[i] < c->pw / 2)
+            return IRONAV_INVALID_ARGUMENT;
+        // the planes as the single-stream device form (16-byte rows); the records are read as 32-bit words
+        const uintptr_t a = reinterpret_cast<uintptr_t>(d_y[i]) | reinterpret_cast<uintptr_t>(d_cb[i]) | reinterpret_cast<uintptr_t>(d_cr[i]);
+        if ((a & 15) || y_strides[i] % 16 || c_strides[i] % 8 || (reinterpret_cast<uintptr_t>(d_mbs[i]) & 3)) return IRONAV_INVALID_ARGUMENT;
+        total_slices += nslices[i];
+    }
+    if (!b->d_kjobs) {
+        CK(cudaMalloc(&b->d_kjobs, sizeof(DbkJob) * b->n));
+        CK(cudaHostAlloc(&b->h_kjobs, sizeof(DbkJob) * b->n, cudaHostAllocDefault));
+        // every stream's row tickets merged by the stream's own ticket, then stream
+        std::vector<std::pair<int, int>> keys;
+        for (int i = 0; i < b->n; i++)
+            for (int t = 0; t < 2 * b->ctx[i]->mb_h; t++) keys.emplace_back(t, i);
+        std::sort(keys.begin(), keys.end());
+        std::vector<uint32_t> order(keys.size());
+        for (size_t k = 0; k < keys.size(); k++) order[k] = ((uint32_t)keys[k].second << 20) | (uint32_t)keys[k].first;
+        b->total_rows2 = (int)order.size();
+        CK(cudaMalloc(&b->d_korder, sizeof(uint32_t) * order.size()));
+        CK(cudaMemcpy(b->d_korder, order.data(), sizeof(uint32_t) * order.size(), cudaMemcpyHostToDevice));
+        CK(cudaMalloc(&b->d_kprogress, sizeof(unsigned) * order.size()));
+        for (int i = 0; i < b->n; i++)
+            if (!b->ctx[i]->d_dbk_edges) CK(cudaMalloc(&b->ctx[i]->d_dbk_edges, sizeof(DbkEdges) * b->ctx[i]->nmb));
+    }
+    // the staging tables are reused: the previous step's copies must have left them
+    if (b->pending) CK(cudaEventSynchronize(b->copied));
+    if (total_slices > b->kslice_cap) {
+        CK(cudaStreamSynchronize(b->stream));  // the old table may still be read by queued work
+        cudaFree(b->d_kslices);
+        cudaFreeHost(b->h_kslices);
+        b->d_kslices = nullptr;
+        b->h_kslices = nullptr;
+        b->kslice_cap = 0;
+        const int cap = std::max(total_slices, 64);
+        CK(cudaMalloc(&b->d_kslices, sizeof(ironav_dbk_slice) * cap));
+        CK(cudaHostAlloc(&b->h_kslices, sizeof(ironav_dbk_slice) * cap, cudaHostAllocDefault));
+        b->kslice_cap = cap;
+    }
+    int s0 = 0, row0 = 0;
+    for (int i = 0; i < b->n; i++) {
+        ironav_ctx* c = b->ctx[i];
+        memcpy(b->h_kslices + s0, slices[i], sizeof(ironav_dbk_slice) * nslices[i]);
+        DbkJob& J = b->h_kjobs[i];
+        memset(&J, 0, sizeof(J));
+        DbkParams& P = J.P;
+        P.planes[0] = static_cast<uint8_t*>(d_y[i]);
+        P.planes[1] = static_cast<uint8_t*>(d_cb[i]);
+        P.planes[2] = static_cast<uint8_t*>(d_cr[i]);
+        P.ys = y_strides[i];
+        P.cs = c_strides[i];
+        P.mbs = d_mbs[i];
+        P.slices = b->d_kslices + s0;
+        P.nslices = nslices[i];
+        P.mb_w = c->mb_w;
+        P.mb_h = c->mb_h;
+        P.bd = 8;
+        P.progress = b->d_kprogress + row0;
+        P.ticket = b->d_counters;
+        P.err = b->d_counters + 1;
+        P.wait_limit = c->wait_limit;
+        J.edges = static_cast<DbkEdges*>(c->d_dbk_edges);
+        J.mb0 = b->mb0[i];
+        s0 += nslices[i];
+        row0 += 2 * c->mb_h;
+    }
+    CK(cudaMemcpyAsync(b->d_kslices, b->h_kslices, sizeof(ironav_dbk_slice) * total_slices, cudaMemcpyHostToDevice, b->stream));
+    CK(cudaMemcpyAsync(b->d_kjobs, b->h_kjobs, sizeof(DbkJob) * b->n, cudaMemcpyHostToDevice, b->stream));
+    CK(cudaEventRecord(b->copied, b->stream));
+    b->pending = true;
+    CK(cudaMemsetAsync(b->d_kprogress, 0, sizeof(unsigned) * b->total_rows2, b->stream));
+    CK(cudaMemsetAsync(b->d_counters, 0, sizeof(unsigned) * 2, b->stream));
+    const int nsm = b->ctx[0]->nsm;
+    deblock_edges_batch_kernel<<<std::min((b->total_mbs + DBK_WARPS - 1) / DBK_WARPS, nsm * 16), DBK_WARPS * 32, 0, b->stream>>>(
+        b->d_kjobs, b->n, b->total_mbs);
+    deblock_rows_batch_kernel<<<std::min((b->total_rows2 + DBK_WARPS - 1) / DBK_WARPS, nsm * 16), DBK_WARPS * 32, 0, b->stream>>>(
+        b->d_kjobs, b->d_korder, (unsigned)b->total_rows2, b->d_counters, b->d_counters + 1);
     return cuda_status(cudaGetLastError());
 }

@@ -130,7 +130,7 @@ EXPORTS = (
     "ironav_begin_b_picture", "ironav_begin_b_picture_device", "ironav_analyse_b_replay", "ironav_analyse_b_replay_device",
     "ironav_set_source_chroma", "ironav_push_reference_chroma", "ironav_code_inter_picture", "ironav_code_inter_picture_device",
     "ironav_decide_p_picture", "ironav_decide_p_picture_device", "ironav_batch_decide", "ironav_decide_dbk_records",
-    "ironav_decide_dbk_records_device",
+    "ironav_decide_dbk_records_device", "ironav_batch_deblock",
 )
 
 SCENE_CUT = 0.8  # codec/change.rs:6
@@ -203,6 +203,9 @@ def _declare(lib: ctypes.CDLL) -> ctypes.CDLL:
         lib.ironav_batch_destroy.argtypes = [_VP]
         lib.ironav_batch_step.argtypes = [_VP] + [ctypes.POINTER(_VP)] * 5
         lib.ironav_batch_sync.argtypes = [_VP]
+    if hasattr(lib, "ironav_batch_deblock"):
+        lib.ironav_batch_deblock.argtypes = [_VP, ctypes.POINTER(_VP), ctypes.POINTER(_I), ctypes.POINTER(_VP), ctypes.POINTER(_VP),
+                                             ctypes.POINTER(_I), ctypes.POINTER(_VP), ctypes.POINTER(_VP), ctypes.POINTER(_I)]
     if hasattr(lib, "ironav_batch_decide"):
         lib.ironav_batch_decide.argtypes = [_VP, ctypes.POINTER(_VP), ctypes.POINTER(_VP), ctypes.POINTER(_VP), ctypes.POINTER(_I),
                                             ctypes.POINTER(_VP), ctypes.POINTER(_VP), ctypes.POINTER(_I)]
@@ -626,6 +629,16 @@ class InterBatch:
         ip = lambda xs: (ctypes.c_int * n)(*xs)
         InterStage._check(self.lib.ironav_batch_decide(self.h, vp(d_states), vp(d_codes), vp(d_y), ip(y_strides), vp(d_cb), vp(d_cr),
                                                        ip(c_strides)), "ironav_batch_decide")
+
+    def deblock(self, d_y, y_strides, d_cb, d_cr, c_strides, d_mbs, slices) -> None:
+        """The deblocking filter of every stream's picture in place: lists of device pointers (ints) and
+        strides, each stream's device records and its slice table (DBK_SLICE_DTYPE arrays) (ironav_batch_deblock)."""
+        n = len(self.stages)
+        vp = lambda xs: (_VP * n)(*xs)
+        ip = lambda xs: (ctypes.c_int * n)(*xs)
+        tabs = [np.ascontiguousarray(t, dtype=DBK_SLICE_DTYPE) for t in slices]
+        InterStage._check(self.lib.ironav_batch_deblock(self.h, vp(d_y), ip(y_strides), vp(d_cb), vp(d_cr), ip(c_strides), vp(d_mbs),
+                                                        vp([_ptr(t) for t in tabs]), ip([len(t) for t in tabs])), "ironav_batch_deblock")
 
     def sync(self) -> None:
         InterStage._check(self.lib.ironav_batch_sync(self.h), "ironav_batch_sync")

@@ -2770,3 +2770,9 @@ int ironav_decide_dbk_records_device(ironav_ctx* c, const ironav_mbcode* d_codes
     (void)c; (void)d_codes; (void)d_states; (void)d_mbs;
     return IRONAV_HARDWARE_UNAVAILABLE;
 }
+
+int ironav_batch_deblock(ironav_batch* b, void* const* y, const int* ys, void* const* cb, void* const* cr, const int* cs,
+                         const ironav_dbk_mb* const* m, const ironav_dbk_slice* const* sl, const int* ns) {
+    (void)b; (void)y; (void)ys; (void)cb; (void)cr; (void)cs; (void)m; (void)sl; (void)ns;
+    return IRONAV_INVALID_ARGUMENT;
+}
