@@ -406,18 +406,18 @@ int ironav_inloop_set_wait(ironav_ctx* ctx, int wait_ms);
 /* Many streams analysed together: each stream is a context (its own size, slice bands, references and
  * picture parameters); a frame step copies every stream's new picture, builds every stream's new
  * reference planes and then analyses every stream's macroblock wavefronts in auto mode in one
- * persistent launch. All contexts of a batch must be 8-bit (bd = 8) and use the same CUDA stream
- * (ironav_ctx_set_stream); the
- * work is queued there, so a frame step can be captured in a CUDA graph. */
+ * persistent launch. All contexts of a batch must have the same sample depth (bd 8 or 10: every sample
+ * buffer below then holds uint8_t or uint16_t samples) and use the same CUDA stream (ironav_ctx_set_stream);
+ * the work is queued there, so a frame step can be captured in a CUDA graph. */
 typedef struct ironav_batch ironav_batch;
 int ironav_batch_create(ironav_batch** out, ironav_ctx* const* ctxs, int n);
 int ironav_batch_destroy(ironav_batch* batch);
 /* One frame step. Arrays of n device pointers (host arrays): d_src[i], the new picture of stream i
- * (width x height, rows width apart); d_ref[i], the reference it predicts from (same layout; pushed as
+ * (width x height samples, rows width apart); d_ref[i], the reference it predicts from (same layout; pushed as
  * the stream's newest reference); d_col[i], that reference's own decisions (NULL entry or NULL array:
  * none); d_states[i] / d_results[i], where stream i's decisions and results go (mb_w*mb_h each). Each
  * stream's picture parameters are those of its last ironav_begin_p_picture. Asynchronous. */
-int ironav_batch_step(ironav_batch* batch, const uint8_t* const* d_src, const uint8_t* const* d_ref,
+int ironav_batch_step(ironav_batch* batch, const void* const* d_src, const void* const* d_ref,
                       const ironav_mbstate* const* d_col, ironav_mbstate* const* d_states,
                       ironav_mbresult* const* d_results);
 /* Waits for the batch's queued work; IRONAV_TIMEOUT if a wavefront wait gave up. */

@@ -480,7 +480,7 @@ __global__ void __launch_bounds__(DBK_WARPS * 32) deblock_rows_kernel(const __gr
     }
 }
 
-// ---- many streams in one launch per pass (the batched form, 8-bit) -----------------------------------
+// ---- many streams in one launch per pass (the batched form) ------------------------------------------
 
 // One stream of a batched deblocking launch: its parameters (planes, records, slices, progress words, the
 // batch's ticket and error words), its edge records, and its first macroblock in the launch's flat index.
@@ -510,7 +510,8 @@ static __global__ void __launch_bounds__(DBK_WARPS * 32) deblock_edges_batch_ker
 // Pass 2 for every stream: ticket t is order[t] = stream << 20 | the stream's own row ticket (2y luma row y,
 // 2y + 1 chroma row y), the streams' rows interleaved by their own tickets, so a row waits only on its own
 // stream's row above, which holds a smaller ticket.
-static __global__ void __launch_bounds__(DBK_WARPS * 32) deblock_rows_batch_kernel(const DbkJob* __restrict__ jobs,
+template <class T>
+__global__ void __launch_bounds__(DBK_WARPS * 32) deblock_rows_batch_kernel(const DbkJob* __restrict__ jobs,
                                                                                    const uint32_t* __restrict__ order, unsigned ntickets,
                                                                                    unsigned* ticket, const unsigned* err) {
     __shared__ int Ls[DBK_WARPS][20][17];
@@ -524,8 +525,8 @@ static __global__ void __launch_bounds__(DBK_WARPS * 32) deblock_rows_batch_kern
         const uint32_t e = order[t];
         const DbkJob& J = jobs[e >> 20];
         const unsigned lt = e & 0xFFFFFu;
-        if (lt & 1u) dbk_row<uint8_t, true>(J.P, J.edges, (int)(lt >> 1), Ls[wid], Es[wid]);
-        else dbk_row<uint8_t, false>(J.P, J.edges, (int)(lt >> 1), Ls[wid], Es[wid]);
+        if (lt & 1u) dbk_row<T, true>(J.P, J.edges, (int)(lt >> 1), Ls[wid], Es[wid]);
+        else dbk_row<T, false>(J.P, J.edges, (int)(lt >> 1), Ls[wid], Es[wid]);
         if (ld_acquire(err) & 1u) return;
     }
 }

@@ -808,15 +808,16 @@ __global__ void __launch_bounds__(K7_WARPS * 32, K7_MIN_BLOCKS) decide_kernel(co
 // Decide mode for many streams in one launch: ticket t is order[t] = stream << 20 | macroblock, in the
 // streams' merged wavefront order (the batched form's); each stream's parameters in table[stream], copied
 // into the warp's shared memory when the warp moves to another stream.
-static __global__ void __launch_bounds__(K7_WARPS * 32, K7_MIN_BLOCKS) decide_batch_kernel(const DecideParams* __restrict__ table,
+template <class T>
+__global__ void __launch_bounds__(K7_WARPS * 32, K7_MIN_BLOCKS) decide_batch_kernel(const DecideParams* __restrict__ table,
                                                                                   const uint32_t* __restrict__ order, unsigned ntickets,
                                                                                   unsigned* ticket, const unsigned* err) {
-    __shared__ DecideSmem<uint8_t> smem[K7_WARPS];
+    __shared__ DecideSmem<T> smem[K7_WARPS];
     __shared__ DecideParams prm[K7_WARPS];
     __shared__ unsigned i4tab[9 * 17];
     fill_i4tab(i4tab);
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    DecideSmem<uint8_t>& S = smem[wid];
+    DecideSmem<T>& S = smem[wid];
     int cur = -1;
     for (;;) {
         unsigned t = 0;
@@ -832,7 +833,7 @@ static __global__ void __launch_bounds__(K7_WARPS * 32, K7_MIN_BLOCKS) decide_ba
             __syncwarp();
             cur = stream;
         }
-        if (!decide_one<uint8_t>(prm[wid], S, i4tab, (int)(e & 0xFFFFFu))) break;
+        if (!decide_one<T>(prm[wid], S, i4tab, (int)(e & 0xFFFFFu))) break;
     }
 }
 

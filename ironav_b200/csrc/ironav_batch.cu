@@ -51,11 +51,13 @@ __device__ __forceinline__ int find_job(const Job* jobs, int n, int idx, Key key
     return lo;
 }
 
-__global__ void __launch_bounds__(K1_THREADS) planes_batch_kernel(const PlaneJob* __restrict__ jobs, int njobs) {
+template <class T>
+__global__ void __launch_bounds__(K1_THREADS) planes_batch_kernel(const PlaneJob* __restrict__ jobs, int njobs, int maxv) {
     const int j = find_job(jobs, njobs, (int)blockIdx.x, [](const PlaneJob& p) { return p.tile0; });
     const PlaneJob& J = jobs[j];
     const int t = (int)blockIdx.x - J.tile0;
-    planes_tile(J.luma, J.stride, J.w, J.h, J.out, J.psize, J.sw, J.sh, (t % J.tiles_x) * K1_TW, (t / J.tiles_x) * K1_TH, 255);
+    planes_tile(reinterpret_cast<const T*>(J.luma), J.stride, J.w, J.h, reinterpret_cast<T*>(J.out), J.psize, J.sw, J.sh,
+                (t % J.tiles_x) * K1_TW, (t / J.tiles_x) * K1_TH, maxv);
 }
 
 // col_mv, enc/frame.rs:944-947, for every stream's new reference
@@ -76,24 +78,27 @@ __global__ void col_batch_kernel(const PlaneJob* __restrict__ jobs, int njobs, i
     J.col[m] = c;
 }
 
-// H264Encoder::source (enc/mod.rs:502-519) for every stream: one block per padded row.
+// H264Encoder::source (enc/mod.rs:502-519) for every stream: one block per padded row; T the samples'
+// type (strides in samples).
+template <class T>
 __global__ void source_batch_kernel(const SrcJob* __restrict__ jobs, int njobs) {
     const int j = find_job(jobs, njobs, (int)blockIdx.x, [](const SrcJob& p) { return p.row0; });
     const SrcJob& J = jobs[j];
     const int y = (int)blockIdx.x - J.row0;
-    const uint8_t* row = J.src + (size_t)min(y, J.h - 1) * J.stride;
-    uint8_t* out = J.dst + (size_t)y * J.pw;
+    const T* row = reinterpret_cast<const T*>(J.src) + (size_t)min(y, J.h - 1) * J.stride;
+    T* out = reinterpret_cast<T*>(J.dst) + (size_t)y * J.pw;
     for (int x = threadIdx.x; x < J.pw; x += blockDim.x) out[x] = row[min(x, J.w - 1)];
 }
 
 // Every stream's auto-mode analysis in one launch (each stream's parameters in the table).
+template <class T>
 __global__ void __launch_bounds__(K2_WARPS * 32, K2_MIN_BLOCKS) analyse_batch_kernel(const AnalyseParams* __restrict__ table,
                                                                                      const uint32_t* __restrict__ order,
                                                                                      unsigned ntickets, unsigned* ticket,
                                                                                      const unsigned* err) {
-    __shared__ WarpSmem<uint8_t> smem[K2_WARPS];
+    __shared__ WarpSmem<T> smem[K2_WARPS];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    WarpSmem<uint8_t>& S = smem[wid];
+    WarpSmem<T>& S = smem[wid];
     for (;;) {
         unsigned t = 0;
         if (lane == 0) t = atomicAdd(ticket, 1u);
@@ -140,6 +145,7 @@ int cuda_status(cudaError_t e) {
 struct ironav_batch {
     std::vector<ironav_ctx*> ctx;
     cudaStream_t stream = nullptr;
+    int bd = 8;  // every stream's sample depth
     int n = 0, total_mbs = 0, total_tiles = 0, total_rows = 0, k2_blocks = 0;
     std::vector<int> mb0;  // each stream's first flag
     uint32_t* d_order = nullptr;
@@ -196,11 +202,13 @@ extern "C" int ironav_batch_create(ironav_batch** out, ironav_ctx* const* ctxs, 
     if (!out || !ctxs || n < 1 || n > 4096) return IRONAV_INVALID_ARGUMENT;
     *out = nullptr;
     for (int i = 0; i < n; i++)
-        if (!ctxs[i] || ctxs[i]->bd != 8 || ctxs[i]->stream != ctxs[0]->stream || ctxs[i]->nmb > (1 << 20)) return IRONAV_INVALID_ARGUMENT;
+        if (!ctxs[i] || ctxs[i]->bd != ctxs[0]->bd || ctxs[i]->stream != ctxs[0]->stream || ctxs[i]->nmb > (1 << 20))
+            return IRONAV_INVALID_ARGUMENT;
     ironav_batch* b = new ironav_batch();
     b->ctx.assign(ctxs, ctxs + n);
     b->n = n;
     b->stream = ctxs[0]->stream;
+    b->bd = ctxs[0]->bd;
     // the streams' wavefronts merged: key x + 2 * (y - band start), then stream, then raster
     std::vector<std::tuple<int, int, int>> keys;
     for (int i = 0; i < n; i++) {
@@ -237,7 +245,9 @@ extern "C" int ironav_batch_create(ironav_batch** out, ironav_ctx* const* ctxs, 
     if ((e = cudaHostAlloc(&b->h_table, sizeof(AnalyseParams) * n, cudaHostAllocDefault)) != cudaSuccess) return fail(e);
     if ((e = cudaEventCreateWithFlags(&b->copied, cudaEventDisableTiming)) != cudaSuccess) return fail(e);
     int per_sm = 0;
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, analyse_batch_kernel, K2_WARPS * 32, 0)) != cudaSuccess) return fail(e);
+    if ((e = b->bd > 8 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, analyse_batch_kernel<uint16_t>, K2_WARPS * 32, 0)
+                       : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, analyse_batch_kernel<uint8_t>, K2_WARPS * 32, 0)) != cudaSuccess)
+        return fail(e);
     b->k2_blocks = std::max(1, per_sm) * ctxs[0]->nsm;
     *out = b;
     return IRONAV_OK;
@@ -250,7 +260,7 @@ extern "C" int ironav_batch_destroy(ironav_batch* b) {
     return IRONAV_OK;
 }
 
-extern "C" int ironav_batch_step(ironav_batch* b, const uint8_t* const* d_src, const uint8_t* const* d_ref,
+extern "C" int ironav_batch_step(ironav_batch* b, const void* const* d_src, const void* const* d_ref,
                                  const ironav_mbstate* const* d_col, ironav_mbstate* const* d_states,
                                  ironav_mbresult* const* d_results) {
     if (!b || !d_src || !d_ref || !d_states || !d_results) return IRONAV_INVALID_ARGUMENT;
@@ -267,7 +277,7 @@ extern "C" int ironav_batch_step(ironav_batch* b, const uint8_t* const* d_src, c
         ironav_ctx* c = b->ctx[i];
         const int slot = take_ref_slot(c);
         PlaneJob& pj = b->h_pjobs[i];
-        pj.luma = d_ref[i];
+        pj.luma = static_cast<const uint8_t*>(d_ref[i]);
         pj.stride = c->width;
         pj.w = c->width;
         pj.h = c->height;
@@ -283,7 +293,7 @@ extern "C" int ironav_batch_step(ironav_batch* b, const uint8_t* const* d_src, c
         pj.mb0 = b->mb0[i];
         tile += pj.tiles_x * ((c->sh + K1_TH - 1) / K1_TH);
         SrcJob& sj = b->h_sjobs[i];
-        sj.src = d_src[i];
+        sj.src = static_cast<const uint8_t*>(d_src[i]);
         sj.stride = c->width;
         sj.w = c->width;
         sj.h = c->height;
@@ -306,13 +316,22 @@ extern "C" int ironav_batch_step(ironav_batch* b, const uint8_t* const* d_src, c
     CK(cudaMemcpyAsync(b->d_table, b->h_table, sizeof(AnalyseParams) * b->n, cudaMemcpyHostToDevice, b->stream));
     CK(cudaEventRecord(b->copied, b->stream));
     b->pending = true;
-    source_batch_kernel<<<b->total_rows, 128, 0, b->stream>>>(b->d_sjobs, b->n);
-    planes_batch_kernel<<<b->total_tiles, K1_THREADS, 0, b->stream>>>(b->d_pjobs, b->n);
+    if (b->bd > 8) {
+        source_batch_kernel<uint16_t><<<b->total_rows, 128, 0, b->stream>>>(b->d_sjobs, b->n);
+        planes_batch_kernel<uint16_t><<<b->total_tiles, K1_THREADS, 0, b->stream>>>(b->d_pjobs, b->n, (1 << b->bd) - 1);
+    } else {
+        source_batch_kernel<uint8_t><<<b->total_rows, 128, 0, b->stream>>>(b->d_sjobs, b->n);
+        planes_batch_kernel<uint8_t><<<b->total_tiles, K1_THREADS, 0, b->stream>>>(b->d_pjobs, b->n, 255);
+    }
     col_batch_kernel<<<(b->total_mbs + 255) / 256, 256, 0, b->stream>>>(b->d_pjobs, b->n, b->total_mbs);
     CK(cudaMemsetAsync(b->d_flags, 0, sizeof(unsigned) * b->total_mbs, b->stream));
     CK(cudaMemsetAsync(b->d_counters, 0, sizeof(unsigned) * 2, b->stream));
-    analyse_batch_kernel<<<b->k2_blocks, K2_WARPS * 32, 0, b->stream>>>(b->d_table, b->d_order, (unsigned)b->total_mbs,
-                                                                        b->d_counters, b->d_counters + 1);
+    if (b->bd > 8)
+        analyse_batch_kernel<uint16_t><<<b->k2_blocks, K2_WARPS * 32, 0, b->stream>>>(b->d_table, b->d_order, (unsigned)b->total_mbs,
+                                                                                      b->d_counters, b->d_counters + 1);
+    else
+        analyse_batch_kernel<uint8_t><<<b->k2_blocks, K2_WARPS * 32, 0, b->stream>>>(b->d_table, b->d_order, (unsigned)b->total_mbs,
+                                                                                     b->d_counters, b->d_counters + 1);
     return cuda_status(cudaGetLastError());
 }
 
@@ -334,7 +353,8 @@ extern "C" int ironav_batch_decide(ironav_batch* b, ironav_mbstate* const* d_sta
         CK(cudaMalloc(&b->d_dtable, sizeof(DecideParams) * b->n));
         CK(cudaHostAlloc(&b->h_dtable, sizeof(DecideParams) * b->n, cudaHostAllocDefault));
         int per_sm = 0;
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, decide_batch_kernel, K7_WARPS * 32, 0));
+        if (b->bd > 8) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, decide_batch_kernel<uint16_t>, K7_WARPS * 32, 0));
+        else CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, decide_batch_kernel<uint8_t>, K7_WARPS * 32, 0));
         b->k7_blocks = std::max(1, per_sm) * b->ctx[0]->nsm;
     }
     // the staging table is reused: the previous step's copies must have left it
@@ -345,7 +365,8 @@ extern "C" int ironav_batch_decide(ironav_batch* b, ironav_mbstate* const* d_sta
             return IRONAV_INVALID_ARGUMENT;
         // the planes as the single-stream device form; states and codes are written as 32-bit words
         const uintptr_t a = reinterpret_cast<uintptr_t>(d_y[i]) | reinterpret_cast<uintptr_t>(d_cb[i]) | reinterpret_cast<uintptr_t>(d_cr[i]);
-        if ((a & 15) || y_strides[i] % 16 || c_strides[i] % 8) return IRONAV_INVALID_ARGUMENT;
+        const int B = b->bd > 8 ? 2 : 1;
+        if ((a & 15) || (y_strides[i] * B) % 16 || c_strides[i] % 8) return IRONAV_INVALID_ARGUMENT;
         if ((reinterpret_cast<uintptr_t>(d_states[i]) | reinterpret_cast<uintptr_t>(d_codes[i])) & 3) return IRONAV_INVALID_ARGUMENT;
         DecideParams& p = b->h_dtable[i];
         const int s = fill_decide_params(c, p, d_states[i], d_codes[i], d_y[i], y_strides[i], d_cb[i], d_cr[i], c_strides[i]);
@@ -360,8 +381,12 @@ extern "C" int ironav_batch_decide(ironav_batch* b, ironav_mbstate* const* d_sta
     b->pending = true;
     CK(cudaMemsetAsync(b->d_flags, 0, sizeof(unsigned) * b->total_mbs, b->stream));
     CK(cudaMemsetAsync(b->d_counters, 0, sizeof(unsigned) * 2, b->stream));
-    decide_batch_kernel<<<b->k7_blocks, K7_WARPS * 32, 0, b->stream>>>(b->d_dtable, b->d_order, (unsigned)b->total_mbs, b->d_counters,
-                                                                       b->d_counters + 1);
+    if (b->bd > 8)
+        decide_batch_kernel<uint16_t><<<b->k7_blocks, K7_WARPS * 32, 0, b->stream>>>(b->d_dtable, b->d_order, (unsigned)b->total_mbs,
+                                                                                     b->d_counters, b->d_counters + 1);
+    else
+        decide_batch_kernel<uint8_t><<<b->k7_blocks, K7_WARPS * 32, 0, b->stream>>>(b->d_dtable, b->d_order, (unsigned)b->total_mbs,
+                                                                                    b->d_counters, b->d_counters + 1);
     return cuda_status(cudaGetLastError());
 }
 
@@ -377,7 +402,8 @@ extern "C" int ironav_batch_deblock(ironav_batch* b, void* const* d_y, const int
             return IRONAV_INVALID_ARGUMENT;
         // the planes as the single-stream device form (16-byte rows); the records are read as 32-bit words
         const uintptr_t a = reinterpret_cast<uintptr_t>(d_y[i]) | reinterpret_cast<uintptr_t>(d_cb[i]) | reinterpret_cast<uintptr_t>(d_cr[i]);
-        if ((a & 15) || y_strides[i] % 16 || c_strides[i] % 8 || (reinterpret_cast<uintptr_t>(d_mbs[i]) & 3)) return IRONAV_INVALID_ARGUMENT;
+        if ((a & 15) || (y_strides[i] * (b->bd > 8 ? 2 : 1)) % 16 || c_strides[i] % 8 || (reinterpret_cast<uintptr_t>(d_mbs[i]) & 3))
+            return IRONAV_INVALID_ARGUMENT;
         total_slices += nslices[i];
     }
     if (!b->d_kjobs) {
@@ -428,7 +454,7 @@ extern "C" int ironav_batch_deblock(ironav_batch* b, void* const* d_y, const int
         P.nslices = nslices[i];
         P.mb_w = c->mb_w;
         P.mb_h = c->mb_h;
-        P.bd = 8;
+        P.bd = b->bd;
         P.progress = b->d_kprogress + row0;
         P.ticket = b->d_counters;
         P.err = b->d_counters + 1;
@@ -447,7 +473,12 @@ extern "C" int ironav_batch_deblock(ironav_batch* b, void* const* d_y, const int
     const int nsm = b->ctx[0]->nsm;
     deblock_edges_batch_kernel<<<std::min((b->total_mbs + DBK_WARPS - 1) / DBK_WARPS, nsm * 16), DBK_WARPS * 32, 0, b->stream>>>(
         b->d_kjobs, b->n, b->total_mbs);
-    deblock_rows_batch_kernel<<<std::min((b->total_rows2 + DBK_WARPS - 1) / DBK_WARPS, nsm * 16), DBK_WARPS * 32, 0, b->stream>>>(
-        b->d_kjobs, b->d_korder, (unsigned)b->total_rows2, b->d_counters, b->d_counters + 1);
+    const int rblocks = std::min((b->total_rows2 + DBK_WARPS - 1) / DBK_WARPS, nsm * 16);
+    if (b->bd > 8)
+        deblock_rows_batch_kernel<uint16_t><<<rblocks, DBK_WARPS * 32, 0, b->stream>>>(b->d_kjobs, b->d_korder, (unsigned)b->total_rows2,
+                                                                                       b->d_counters, b->d_counters + 1);
+    else
+        deblock_rows_batch_kernel<uint8_t><<<rblocks, DBK_WARPS * 32, 0, b->stream>>>(b->d_kjobs, b->d_korder, (unsigned)b->total_rows2,
+                                                                                      b->d_counters, b->d_counters + 1);
     return cuda_status(cudaGetLastError());
 }

@@ -1090,7 +1090,7 @@ int ironav_inloop_set_wait(ironav_ctx* c, int ms) { return (c && ms > 0) ? IRONA
 /* The batched form is a device form (device pointers); the CPU library has none. */
 int ironav_batch_create(ironav_batch** out, ironav_ctx* const* ctxs, int n) { (void)out; (void)ctxs; (void)n; return IRONAV_HARDWARE_UNAVAILABLE; }
 int ironav_batch_destroy(ironav_batch* b) { (void)b; return IRONAV_INVALID_ARGUMENT; }
-int ironav_batch_step(ironav_batch* b, const uint8_t* const* s, const uint8_t* const* r, const ironav_mbstate* const* c,
+int ironav_batch_step(ironav_batch* b, const void* const* s, const void* const* r, const ironav_mbstate* const* c,
                       ironav_mbstate* const* st, ironav_mbresult* const* res) {
     (void)b; (void)s; (void)r; (void)c; (void)st; (void)res;
     return IRONAV_HARDWARE_UNAVAILABLE;

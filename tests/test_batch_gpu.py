@@ -12,27 +12,29 @@ pytestmark = pytest.mark.gpu
 STREAMS = [(640, 360, 2), (854, 480, 3), (352, 288, 2), (1280, 720, 5), (1920, 1080, 8), (176, 144, 1)]
 
 
-def _frames(i, w, h, n=3):
+def _frames(i, w, h, n=3, bd=8):
     seq = Sequence.config("1080p", n, seed=0x1A2B0300 + i, size=(w, h))
-    return [seq.frame(t) for t in range(n)]
+    return [seq.frame10(t) if bd == 10 else seq.frame(t) for t in range(n)]
 
 
-def test_batch_equals_single_stream_auto_mode(cuda_lib):
+@pytest.mark.parametrize("bd", [8, 10])
+def test_batch_equals_single_stream_auto_mode(cuda_lib, bd):
     import torch
 
+    qpp = 27 + 6 * (bd - 8)
     stream = torch.cuda.Stream()
-    frames = [_frames(i, w, h) for i, (w, h, _) in enumerate(STREAMS)]
+    frames = [_frames(i, w, h, bd=bd) for i, (w, h, _) in enumerate(STREAMS)]
     # each stream alone (host-buffer calls)
     want = []
     for (w, h, ns), f in zip(STREAMS, frames):
-        st = InterStage(w, h, nslices=ns, lib=cuda_lib)
+        st = InterStage(w, h, nslices=ns, lib=cuda_lib, bd=bd)
         per = []
         col = None
         for t in (1, 2):
             st.clear_references()
             st.push_reference(f[t - 1], col=col)
             st.set_source(f[t])
-            st.begin_p_picture(27)
+            st.begin_p_picture(qpp)
             states, res = st.analyse_auto()
             per.append((states, res))
             col = states
@@ -40,12 +42,12 @@ def test_batch_equals_single_stream_auto_mode(cuda_lib):
         want.append(per)
     # all streams together: each context primed with a reference so its picture parameters are valid
     stages = []
-    dev = [[torch.from_numpy(x).cuda() for x in f] for f in frames]
+    dev = [[torch.from_numpy(x.view(np.int16) if bd == 10 else x).cuda() for x in f] for f in frames]
     for (w, h, ns), f in zip(STREAMS, dev):
-        st = InterStage(w, h, nslices=ns, lib=cuda_lib)
+        st = InterStage(w, h, nslices=ns, lib=cuda_lib, bd=bd)
         st.set_stream(stream.cuda_stream)
         st.push_reference_device(f[0].data_ptr(), w, w, h, None)
-        st.begin_p_picture(27)
+        st.begin_p_picture(qpp)
         stages.append(st)
     n = len(stages)
     d_states = [[torch.zeros(s.nmb * 72, dtype=torch.uint8, device="cuda") for _ in range(2)] for s in stages]

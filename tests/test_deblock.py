@@ -323,7 +323,8 @@ def test_gpu_deblock_device_form_checks_alignment(cuda_lib):
 
 
 @pytest.mark.gpu
-def test_gpu_batched_deblock_matches_single_streams(oracle_lib, cuda_lib):
+@pytest.mark.parametrize("bd", [8, 10])
+def test_gpu_batched_deblock_matches_single_streams(oracle_lib, cuda_lib, bd):
     """Four streams of different sizes and slice layouts (encoder bands, a slice per row, slice ids drawn per
     macroblock with disabled and edge-only filtering) deblocked by one batched call: each stream's planes are
     those of its own call (and the first stream's the oracle's); twice, the progress words cleared each time."""
@@ -332,26 +333,26 @@ def test_gpu_batched_deblock_matches_single_streams(oracle_lib, cuda_lib):
     from ironav_b200.inter import InterBatch, InterStage
     from ironav_b200.synth import dbk_planes, dbk_records
 
-    rng = np.random.default_rng(77)
+    rng = np.random.default_rng(77 + bd)
     streams = [(352, 288, 2, True), (1920, 1080, 8, True), (176, 144, 9, True), (640, 360, 3, False)]
     stream = torch.cuda.Stream()
     stages, inputs, want = [], [], []
     for (w, h, ns, rows) in streams:
-        st = InterStage(w, h, nslices=ns, lib=cuda_lib)
+        st = InterStage(w, h, nslices=ns, lib=cuda_lib, bd=bd)
         st.set_stream(stream.cuda_stream)
-        planes = dbk_planes(rng, st.mb_w, st.mb_h)
-        m, s = dbk_records(rng, st.mb_w, st.mb_h, ns, slice_rows=rows)
+        planes = dbk_planes(rng, st.mb_w, st.mb_h, bd)
+        m, s = dbk_records(rng, st.mb_w, st.mb_h, ns, bd, slice_rows=rows)
         stages.append(st)
         inputs.append((planes, m, s))
         want.append(st.deblock(*planes, m, s))
-    o = InterStage(352, 288, nslices=2, lib=oracle_lib)
+    o = InterStage(352, 288, nslices=2, lib=oracle_lib, bd=bd)
     planes, m, s = inputs[0]
     for a, b in zip(want[0], o.deblock(*planes, m, s)):
         assert np.array_equal(a, b)
     batch = InterBatch(stages)
     d_m = [torch.from_numpy(m.view(np.uint8)).cuda() for _, m, _ in inputs]
     for _ in range(2):
-        d_p = [[torch.from_numpy(a.copy()).cuda() for a in planes] for planes, _, _ in inputs]
+        d_p = [[torch.from_numpy(a.view(np.int16) if bd == 10 else a.copy()).cuda() for a in planes] for planes, _, _ in inputs]
         torch.cuda.synchronize()
         batch.deblock([p[0].data_ptr() for p in d_p], [p[0].shape[1] for p in d_p], [p[1].data_ptr() for p in d_p],
                       [p[2].data_ptr() for p in d_p], [p[1].shape[1] for p in d_p], [t.data_ptr() for t in d_m],
@@ -359,6 +360,6 @@ def test_gpu_batched_deblock_matches_single_streams(oracle_lib, cuda_lib):
         batch.sync()
         for k, (p, w) in enumerate(zip(d_p, want)):
             for name, a, b in zip("Y Cb Cr".split(), p, w):
-                got = a.cpu().numpy()
+                got = a.cpu().numpy().view(np.uint16) if bd == 10 else a.cpu().numpy()
                 assert np.array_equal(got, b), f"stream {k} {streams[k]}: {name} differs at {np.argwhere(got != b)[:4].tolist()}"
     batch.close()

@@ -440,14 +440,17 @@ def test_gpu_decide_small_and_ragged_pictures(oracle_lib, cuda_lib, size, nslice
 
 
 @pytest.mark.gpu
-def test_gpu_batched_decide_matches_single_streams(oracle_lib, cuda_lib):
+@pytest.mark.parametrize("bd", [8, 10])
+def test_gpu_batched_decide_matches_single_streams(oracle_lib, cuda_lib, bd):
     """Four streams of different sizes, slice layouts and content decided in one launch: each stream's
-    codes, states and reconstruction are those of its own decide call (and so the oracle's)."""
+    codes, states and reconstruction are those of its own decide call (and so the oracle's); a batch of
+    8-bit streams and one of 10-bit streams."""
     import torch
 
     from ironav_b200.inter import MBSTATE_DTYPE, InterBatch
 
     cases = [dict(), dict(new_content=True, qp=30), dict(size=(320, 176), nslices=3, fast=True), dict(cfg="1080p", nslices=8, qp=27)]
+    cases = [dict(kw, bd=bd) for kw in cases]
     stages = [decide_case(cuda_lib, threads=False, **kw)[0] for kw in cases]
     want = [st.decide_p_picture() for st in stages]
     o = decide_case(oracle_lib, **cases[1])[0]
@@ -456,19 +459,20 @@ def test_gpu_batched_decide_matches_single_streams(oracle_lib, cuda_lib):
     for st in stages:
         st.set_stream(stream.cuda_stream)
     bufs = []
+    dt = torch.uint8 if bd == 8 else torch.int16
     for st in stages:
         bufs.append((torch.zeros(st.nmb * 72, dtype=torch.uint8, device="cuda"), torch.full((st.nmb * 1516,), 0x5A, dtype=torch.uint8, device="cuda"),
-                     torch.zeros((st.mb_h * 16, st.mb_w * 16), dtype=torch.uint8, device="cuda"),
-                     torch.zeros((2, st.mb_h * 8, st.mb_w * 8), dtype=torch.uint8, device="cuda")))
+                     torch.zeros((st.mb_h * 16, st.mb_w * 16), dtype=dt, device="cuda"),
+                     torch.zeros((2, st.mb_h * 8, st.mb_w * 8), dtype=dt, device="cuda")))
     batch = InterBatch(stages)
     for _ in range(2):  # twice: the flags are cleared every launch
         batch.decide([b[0].data_ptr() for b in bufs], [b[1].data_ptr() for b in bufs], [b[2].data_ptr() for b in bufs],
                      [b[2].shape[1] for b in bufs], [b[3][0].data_ptr() for b in bufs], [b[3][1].data_ptr() for b in bufs],
                      [b[3].shape[2] for b in bufs])
         batch.sync()
+    view = (lambda t: t.cpu().numpy().view(np.uint16)) if bd == 10 else (lambda t: t.cpu().numpy())
     for k, (st, b) in enumerate(zip(stages, bufs)):
-        got = (b[0].cpu().numpy().view(MBSTATE_DTYPE), b[1].cpu().numpy().view(MBCODE_DTYPE),
-               (b[2].cpu().numpy(), b[3][0].cpu().numpy(), b[3][1].cpu().numpy()))
+        got = (b[0].cpu().numpy().view(MBSTATE_DTYPE), b[1].cpu().numpy().view(MBCODE_DTYPE), (view(b[2]), view(b[3][0]), view(b[3][1])))
         _same_decisions(got, want[k], f"stream {k} {cases[k]}")
     batch.close()
 
