@@ -286,16 +286,16 @@ def decide_case(lib, cfg="cif", size=None, qp=22, bd=8, nslices=2, refs=1, fast=
                 threads=True):
     """A P picture (frame 1) from frame 0 (and frame 2 when refs == 2); new_content: the references come
     from an unrelated sequence, so that intra competes everywhere."""
-    seq = Sequence.config(cfg, 3, size=size)
-    other = Sequence(seq.width, seq.height, 3, seq.seed + 77, 3, 4, 6, 3.0) if new_content else seq
-    fr = [seq.frame10(t) if bd == 10 else seq.frame(t) for t in range(3)]
-    ch = [seq.chroma(t, bd) for t in range(3)]
-    rf = [other.frame10(t) if bd == 10 else other.frame(t) for t in range(3)] if new_content else fr
-    rc = [other.chroma(t, bd) for t in range(3)] if new_content else ch
-    st = InterStage(seq.width, seq.height, max_refs=2, nslices=nslices, lib=lib, bd=bd)
+    seq = Sequence.config(cfg, 4, size=size)
+    other = Sequence(seq.width, seq.height, 4, seq.seed + 77, 3, 4, 6, 3.0) if new_content else seq
+    fr = [seq.frame10(t) if bd == 10 else seq.frame(t) for t in range(4)]
+    ch = [seq.chroma(t, bd) for t in range(4)]
+    rf = [other.frame10(t) if bd == 10 else other.frame(t) for t in range(4)] if new_content else fr
+    rc = [other.chroma(t, bd) for t in range(4)] if new_content else ch
+    st = InterStage(seq.width, seq.height, max_refs=3, nslices=nslices, lib=lib, bd=bd)
     if threads and hasattr(lib, "oracle_set_threads"):
         lib.oracle_set_threads(st.ctx, os.cpu_count() or 1)
-    for t in ([2, 0] if refs == 2 else [0]):
+    for t in {1: [0], 2: [2, 0], 3: [3, 2, 0]}[refs]:
         st.push_reference(rf[t])
         st.push_reference_chroma(*rc[t])
     st.set_source(fr[1])
@@ -386,6 +386,17 @@ def _same_decisions(got, want, what):
                                 dict(bd=10, qp=24, fast=True), dict(cfg="1080p", nslices=8, qp=27),
                                 dict(cfg="1080p", size=(1280, 720), new_content=True, nslices=4, qp=32)])
 def test_gpu_decide_matches_oracle(oracle_lib, cuda_lib, kw):
+    o, _, _ = decide_case(oracle_lib, **kw)
+    c, _, _ = decide_case(cuda_lib, threads=False, **kw)
+    _same_decisions(c.decide_p_picture(), o.decide_p_picture(), str(kw))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kw", [dict(refs=3, sub8=True, qp=18), dict(refs=3, qp=30, nslices=3, new_content=True),
+                                dict(refs=2, bd=10, fast=True, qp=22), dict(refs=3, bd=10, sub8=True, qp=20, new_content=True)])
+def test_gpu_decide_three_references(oracle_lib, cuda_lib, kw):
+    """Up to three active references (the reference-index bits take their ue(v) length), with sub-8x8
+    partitions, fast mode and 10-bit pictures."""
     o, _, _ = decide_case(oracle_lib, **kw)
     c, _, _ = decide_case(cuda_lib, threads=False, **kw)
     _same_decisions(c.decide_p_picture(), o.decide_p_picture(), str(kw))
