@@ -266,18 +266,29 @@ def check_intra_decodes(st: InterStage, codes, rec, qp_y: int, band_start):
             left = [int(v) for v in plane[cy0:cy0 + 8, cx0 - 1]] if la else [0] * 8
             tl = int(plane[cy0 - 1, cx0 - 1]) if ta and la else 0
             p = pred_chroma(int(c["chroma_mode"]), top, left, tl, ta, la, bd)
-            l4 = c["res"]["cdc"][comp].astype(np.int64)
-            f = np.array([l4[0] + l4[1] + l4[2] + l4[3], l4[0] - l4[1] + l4[2] - l4[3], l4[0] + l4[1] - l4[2] - l4[3],
-                          l4[0] - l4[1] - l4[2] + l4[3]])
-            dcc = ((f * 16 * V[qpc % 6][0]) << (qpc // 6)) >> 5
-            for blk in range(4):
-                d = dequant4(c["res"]["cac"][comp][blk], qpc, skip_dc=True) if cbpc == 2 else np.zeros(16, np.int64)
-                d[0] = dcc[blk] if cbpc > 0 else 0
-                bx, by = blk & 1, blk >> 1
-                want = np.clip(p[by * 4:by * 4 + 4, bx * 4:bx * 4 + 4] + idct4(d), 0, maxv)
-                got = plane[cy0 + by * 4:cy0 + by * 4 + 4, cx0 + bx * 4:cx0 + bx * 4 + 4]
-                assert np.array_equal(got, want), f"intra chroma mb {mb} comp {comp} block {blk} mode {c['chroma_mode']}"
+            want = np.clip(p + chroma_residual(c["res"], comp, qpc), 0, maxv)
+            got = plane[cy0:cy0 + 8, cx0:cx0 + 8]
+            assert np.array_equal(got, want), f"intra chroma mb {mb} comp {comp} mode {c['chroma_mode']} cbp {cbpc}"
     return n4, n16
+
+
+def chroma_residual(res, comp, qpc):
+    """The 8x8 residual of one chroma component (8.5.11: the 2x2 DC transform and scaling, then the 4x4
+    blocks' AC levels), as coded_block_pattern's chroma part says: 0 none, 1 DC only, 2 DC and AC."""
+    cbpc = int(res["cbp"]) >> 4
+    out = np.zeros((8, 8), np.int64)
+    if cbpc == 0:
+        return out
+    l4 = res["cdc"][comp].astype(np.int64)
+    f = np.array([l4[0] + l4[1] + l4[2] + l4[3], l4[0] - l4[1] + l4[2] - l4[3], l4[0] + l4[1] - l4[2] - l4[3],
+                  l4[0] - l4[1] - l4[2] + l4[3]])
+    dcc = ((f * 16 * V[qpc % 6][0]) << (qpc // 6)) >> 5
+    for blk in range(4):
+        d = dequant4(res["cac"][comp][blk], qpc, skip_dc=True) if cbpc == 2 else np.zeros(16, np.int64)
+        d[0] = dcc[blk]
+        bx, by = blk & 1, blk >> 1
+        out[by * 4:by * 4 + 4, bx * 4:bx * 4 + 4] = idct4(d)
+    return out
 
 
 # ---- cases -----------------------------------------------------------------------------------------
