@@ -1916,6 +1916,15 @@ static int q_decimate(const int* lv, int n) {
     return score;
 }
 
+/* Test hooks: the residual's building blocks, called one at a time by the reference's own unit tests of
+ * them (enc/frame.rs:2442-2492, restated in tests/test_residual.py). */
+int oracle_decimate(const int* lv, int n) { return q_decimate(lv, n); }
+void oracle_fdct4(const int* d, int* o) { q_fdct4(d, o); }
+int oracle_quant(int c, int mf, int f, int qbits) { return q_quant(c, mf, f, qbits); }
+void oracle_idct4_add(const int* c, uint16_t* dst, int stride, int maxv) { q_idct4_add(c, dst, stride, maxv); }
+void oracle_quant8(const int* src, const int* pred, int qp, int intra, int* lv, int* co) { q_block8(src, pred, qp, intra, lv, co); }
+void oracle_idct8_add(const int* c, uint16_t* dst, int stride, int maxv) { q_idct8_add(c, dst, stride, maxv); }
+
 /* chroma_mc, h264/inter.rs:549-568: eighth-sample bilinear, coordinates clamped to the plane */
 static void q_chroma_mc(const uint16_t* refp, int pw, int ph, int x, int y, int mx, int my, int w, int h, uint16_t* out) {
     int fx = mx & 7, fy = my & 7, x0 = x + (mx >> 3), y0 = y + (my >> 3);

@@ -35,6 +35,12 @@ def oracle_library() -> ctypes.CDLL:
         lib.oracle_halfpel_predict.argtypes = [ctypes.c_void_p] + [ctypes.c_int] * 6 + [ctypes.c_void_p]
         lib.oracle_halfpel_plane.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
         lib.oracle_satd4.argtypes = [ctypes.c_void_p]
+        lib.oracle_decimate.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        lib.oracle_fdct4.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        lib.oracle_quant.argtypes = [ctypes.c_int] * 4
+        lib.oracle_idct4_add.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+        lib.oracle_quant8.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+        lib.oracle_idct8_add.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
         lib.oracle_dbk_tables.argtypes = [ctypes.c_void_p] * 4
         lib.oracle_set_threads.argtypes = [ctypes.c_void_p, ctypes.c_int]
         lib.oracle_analyse_replay_subset.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,

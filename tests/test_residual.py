@@ -131,6 +131,60 @@ def _random_decisions(rng, nmb, nrefs):
     return d
 
 
+# ---- the reference's unit tests of the building blocks (enc/frame.rs:2442-2492), on the oracle's --------
+
+MF0, V0 = (13107, 5243, 8066), (10, 16, 13)  # quantisation multipliers and scales at QP % 6 == 0
+
+
+def _class(p):
+    r, c = divmod(p, 4)
+    return 0 if r % 2 == 0 and c % 2 == 0 else (1 if r % 2 == 1 and c % 2 == 1 else 2)
+
+
+def test_forward_and_inverse_transforms_round_trip_at_low_qp(oracle_lib):
+    """forward_and_inverse_transforms_round_trip_at_low_qp (enc/frame.rs:2442-2465): fdct4, quant at
+    QP 0 with the intra rounding (f = 2^14, 15 bits), scaling and idct4_add give back the residual
+    within 1."""
+    src = np.array([((i * 37) % 23) * 9 for i in range(16)], np.int32)
+    d = (src - 100).astype(np.int32)
+    c = np.zeros(16, np.int32)
+    oracle_lib.oracle_fdct4(d.ctypes.data, c.ctypes.data)
+    co = np.array([oracle_lib.oracle_quant(int(c[p]), MF0[_class(p)], 1 << 14, 15) * V0[_class(p)] for p in range(16)], np.int32)
+    out = np.full(16, 100, np.uint16)
+    oracle_lib.oracle_idct4_add(co.ctypes.data, out.ctypes.data, 4, 255)
+    assert np.abs(out.astype(np.int64) - src).max() <= 1, (out, src)
+
+
+def test_the_8x8_transform_round_trips_at_low_qp(oracle_lib):
+    """the_8x8_transform_round_trips_at_low_qp (enc/frame.rs:2467-2479): quant8 (intra) and idct8_add
+    within 1 + QP/3 at QP 0, 1, 5 and 6."""
+    src = np.array([((i * 37) % 23) * 9 + (i // 8) * 5 for i in range(64)], np.int32)
+    pred = np.full(64, 100, np.int32)
+    for qp in (0, 1, 5, 6):
+        lv, co = np.zeros(64, np.int32), np.zeros(64, np.int32)
+        oracle_lib.oracle_quant8(src.ctypes.data, pred.ctypes.data, qp, 1, lv.ctypes.data, co.ctypes.data)
+        out = np.full(64, 100, np.uint16)
+        oracle_lib.oracle_idct8_add(co.ctypes.data, out.ctypes.data, 8, 255)
+        assert np.abs(out.astype(np.int64) - src).max() <= 1 + qp // 3, (qp, out, src)
+
+
+def test_decimation_scores_lone_ones_low_and_big_levels_high(oracle_lib):
+    """decimation_scores_lone_ones_low_and_big_levels_high (enc/frame.rs:2481-2492)."""
+    lv = np.zeros(16, np.int32)
+
+    def score():
+        return oracle_lib.oracle_decimate(lv.ctypes.data, 16)
+
+    assert score() == 0
+    lv[15] = 1
+    assert score() == 0, "a lone level after a long run of zeros"
+    lv[15] = 0
+    lv[0] = 1
+    assert score() == 3
+    lv[3] = -2
+    assert score() == 9
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("kw", [dict(), dict(qp=30), dict(cfg="1080p", nslices=8, qp=27), dict(bd=10, qp=24), dict(refs=2, qp=20)])
 @pytest.mark.parametrize("t8", [False, True])
