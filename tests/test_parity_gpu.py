@@ -48,6 +48,30 @@ def test_planes_byte_exact(oracle_lib, cuda_lib, size):
         assert np.array_equal(po[k], pc[k]), f"plane {name} of {w}x{h} differs at {np.argwhere(po[k] != pc[k])[:3]}"
 
 
+def test_planes_rebuilt_in_a_reused_slot(oracle_lib, cuda_lib):
+    """the_threaded_half_sample_planes_equal_the_single_threaded_ones (crates/ironav-codec/src/h264/enc/
+    mod.rs:1302-1330), on its picture (80x112, the 32-bit LCG from seed 5) and its inverse: with one
+    reference held, every push rebuilds the planes in the slot the previous picture used, and each
+    rebuild equals a fresh context's planes of the same picture and the oracle's."""
+    pw, ph = 80, 112
+    seed, vals = 5, []
+    for _ in range(pw * ph):
+        seed = (seed * 1103515245 + 12345) & 0xFFFFFFFF
+        vals.append((seed >> 16) % 256)
+    luma = np.array(vals, np.uint8).reshape(ph, pw)
+    luma2 = (255 - luma).astype(np.uint8)
+    o = InterStage(pw, ph, max_refs=1, lib=oracle_lib)
+    c = InterStage(pw, ph, max_refs=1, lib=cuda_lib)
+    for k, pic in enumerate([luma, luma2, luma, luma2]):
+        o.push_reference(pic)
+        c.push_reference(pic)
+        fresh = InterStage(pw, ph, max_refs=1, lib=cuda_lib)
+        fresh.push_reference(pic)
+        got = c.planes(0)
+        assert np.array_equal(got, fresh.planes(0)), f"push {k}: the reused slot's planes differ from a fresh build"
+        assert np.array_equal(got, o.planes(0)), f"push {k}: planes differ from the oracle's"
+
+
 def test_planes_of_a_macroblock_aligned_reconstruction(oracle_lib, cuda_lib):
     """A reconstruction is 16*mb_w x 16*mb_h and is used as is (no edge repetition inside it)."""
     w, h = 40, 20  # mb 3 x 2

@@ -60,6 +60,38 @@ def test_still_pan_and_cut(oracle_lib):
     assert st.scene_cut(f1, other)
 
 
+def _cut_sequence():
+    """a_scene_cut_starts_an_idr_picture's pictures (crates/ironav-codec/src/h264/enc/mod.rs:1071-1086):
+    96x64 `scene` for pictures 0-4, a vertical gradient (255 - 3 * row) from picture 5 on."""
+    from tests.test_decode_inter import scene
+
+    w, h = 96, 64
+    grad = (255 - np.arange(w * h) // w * 3).astype(np.uint8).reshape(h, w)
+    return w, h, [scene(w, h, t)[0] if t < 5 else grad for t in range(10)]
+
+
+def _idr_pictures(lib):
+    """The pictures the encoder starts as IDR (enc/mod.rs:706-714): the first, and each whose scene-cut
+    measure against the picture before it says cut (the key-picture interval, KEYINT = 250 at
+    enc/mod.rs:27, is not reached in 10 pictures)."""
+    w, h, pics = _cut_sequence()
+    st = InterStage(w, h, lib=lib)
+    return [0] + [t for t in range(1, len(pics)) if st.scene_cut(pics[t - 1], pics[t])]
+
+
+def test_a_scene_cut_starts_an_idr_picture(oracle_lib):
+    assert _idr_pictures(oracle_lib) == [0, 5]
+
+
+@pytest.mark.gpu
+def test_gpu_a_scene_cut_starts_an_idr_picture(oracle_lib, cuda_lib):
+    assert _idr_pictures(cuda_lib) == [0, 5]
+    w, h, pics = _cut_sequence()
+    o, c = InterStage(w, h, lib=oracle_lib), InterStage(w, h, lib=cuda_lib)
+    for t in range(1, len(pics)):
+        assert c.scene_change(pics[t - 1], pics[t]) == o.scene_change(pics[t - 1], pics[t]), t
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("size", [(352, 288), (1920, 1080), (3840, 2160), (40, 24)])
 def test_scene_change_gpu_matches_oracle(oracle_lib, cuda_lib, size):
