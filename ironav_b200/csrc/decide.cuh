@@ -37,7 +37,7 @@ struct DecideSmem {
     int cleft[2][8];       // chroma columns to the left
     int i4rec[256];        // the Intra4x4 trial's reconstruction
     int16_t i4lv[16][16];  // its levels: raster 4x4 blocks, scan order
-    int edge[13];          // the current 4x4 block's edges: top-left, 8 above, 4 to the left
+    int edge[2][13];       // the Intra4x4 trial's two current 4x4 blocks' edges: top-left, 8 above, 4 to the left
     int dcs[16];           // Intra16x16: each block's DC coefficient, then its dequantised DC
     int nbm[8];            // pred_i4_mode: the left macroblock's modes down its right column, then the top's along its
                            // bottom row (2 for a macroblock that is not Intra4x4, -1 unavailable)
@@ -119,25 +119,26 @@ __device__ __forceinline__ unsigned i4_entry(int mode, int x, int y) {
     }
 }
 
-// fdct4 (enc/frame.rs:113-132) of a 4x4 block held one value a lane (lane 4r + c, lanes 0-15): the lane's
-// coefficient at raster position (r, c). Every lane takes part in the shuffles.
+// fdct4 (enc/frame.rs:113-132) of a 4x4 block held one value a lane (lane 4r + c of each half-warp: a block
+// a half): the lane's coefficient at raster position (r, c). Every lane takes part in the shuffles.
 __device__ __forceinline__ int fdct4_lanes(int v) {
-    const int lane = threadIdx.x & 31, r = (lane >> 2) & 3, c = lane & 3, base = lane & ~3;
+    const int lane = threadIdx.x & 31, r = (lane >> 2) & 3, c = lane & 3, base = lane & ~3, hb = (lane & 16) + c;
     const int a0 = __shfl_sync(FULL, v, base), a1 = __shfl_sync(FULL, v, base + 1), a2 = __shfl_sync(FULL, v, base + 2), a3 = __shfl_sync(FULL, v, base + 3);
     int s03 = a0 + a3, d03 = a0 - a3, s12 = a1 + a2, d12 = a1 - a2;
     const int t = c == 0 ? s03 + s12 : (c == 1 ? 2 * d03 + d12 : (c == 2 ? s03 - s12 : d03 - 2 * d12));
-    const int b0 = __shfl_sync(FULL, t, c), b1 = __shfl_sync(FULL, t, 4 + c), b2 = __shfl_sync(FULL, t, 8 + c), b3 = __shfl_sync(FULL, t, 12 + c);
+    const int b0 = __shfl_sync(FULL, t, hb), b1 = __shfl_sync(FULL, t, hb + 4), b2 = __shfl_sync(FULL, t, hb + 8), b3 = __shfl_sync(FULL, t, hb + 12);
     s03 = b0 + b3, d03 = b0 - b3, s12 = b1 + b2, d12 = b1 - b2;
     return r == 0 ? s03 + s12 : (r == 1 ? 2 * d03 + d12 : (r == 2 ? s03 - s12 : d03 - 2 * d12));
 }
 
-// idct4_add (h264/idct.rs:8-31) of raster coefficients held one a lane onto the lane's prediction sample.
+// idct4_add (h264/idct.rs:8-31) of raster coefficients held one a lane (a block a half-warp, as fdct4_lanes)
+// onto the lane's prediction sample.
 __device__ __forceinline__ int idct4_lanes(int co, int pred, int maxv) {
-    const int lane = threadIdx.x & 31, r = (lane >> 2) & 3, c = lane & 3, base = lane & ~3;
+    const int lane = threadIdx.x & 31, r = (lane >> 2) & 3, c = lane & 3, base = lane & ~3, hb = (lane & 16) + c;
     const int c0 = __shfl_sync(FULL, co, base), c1 = __shfl_sync(FULL, co, base + 1), c2 = __shfl_sync(FULL, co, base + 2), c3 = __shfl_sync(FULL, co, base + 3);
     const int e0 = c0 + c2, e1 = c0 - c2, e2 = (c1 >> 1) - c3, e3 = c1 + (c3 >> 1);
     const int t = c == 0 ? e0 + e3 : (c == 1 ? e1 + e2 : (c == 2 ? e1 - e2 : e0 - e3));
-    const int t0 = __shfl_sync(FULL, t, c), t1 = __shfl_sync(FULL, t, 4 + c), t2 = __shfl_sync(FULL, t, 8 + c), t3 = __shfl_sync(FULL, t, 12 + c);
+    const int t0 = __shfl_sync(FULL, t, hb), t1 = __shfl_sync(FULL, t, hb + 4), t2 = __shfl_sync(FULL, t, hb + 8), t3 = __shfl_sync(FULL, t, hb + 12);
     const int g0 = t0 + t2, g1 = t0 - t2, g2 = (t1 >> 1) - t3, g3 = t1 + (t3 >> 1);
     const int h = r == 0 ? g0 + g3 : (r == 1 ? g1 + g2 : (r == 2 ? g1 - g2 : g0 - g3));
     return min(max(pred + ((h + 32) >> 6), 0), maxv);
@@ -276,39 +277,48 @@ __device__ int2 best_i16_d(const DecideParams& P, DecideSmem<T>& S, bool ta, boo
 
 __device__ __forceinline__ int zorder_d(int bx, int by) { return ((by >> 1) << 3) | ((bx >> 1) << 2) | ((by & 1) << 1) | (bx & 1); }
 
-// code_i4, enc/frame.rs:1050-1138, as a trial: block by block in decoding order, each predicted from the
-// reconstruction so far (S.i4rec inside the macroblock, the neighbours' around it), its mode the cheapest
-// by SATD + lambda * (1 for the predicted mode, 4 otherwise; lanes 0-8, a mode each, from the table tab),
-// coded with the intra rounding and reconstructed into S.i4rec (lanes 0-15, a coefficient each). Returns
-// the summed cost (every lane).
+// code_i4, enc/frame.rs:1050-1138, as a trial: each block predicted from the reconstruction so far
+// (S.i4rec inside the macroblock, the neighbours' around it), its mode the cheapest by SATD + lambda * (1
+// for the predicted mode, 4 otherwise; from the table tab), coded with the intra rounding and
+// reconstructed into S.i4rec. A block reads only its left, top-left, top and top-right neighbours, so the
+// blocks go by anti-diagonal t = bx + 2 * by (10 steps of one or two blocks, a block a half-warp: its modes
+// on lanes 0-8 of the half, a coefficient a lane for the coding) rather than one at a time in decoding
+// order; the top-right's availability stays the decoding order's (zorder), and the cost is the same sum.
+// Returns the summed cost (every lane).
 template <class T>
 __device__ int code_i4_trial(const DecideParams& P, DecideSmem<T>& S, const unsigned* tab, bool ta, bool la, bool tra) {
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, hl = lane & 15, half = lane >> 4;
+    const unsigned hmask = half ? 0xffff0000u : 0x0000ffffu;
     const int bd = P.C.bd, maxv = (1 << bd) - 1, lam = P.C.A.lambda;
     const int qp = P.C.qp + 6 * (bd - 8), m6 = qp % 6, qbits = 15 + qp / 6, f = (1 << qbits) / 3;
     const bool tla = ta && la;
     if (lane < 16) S.i4modes[lane] = 2;
     __syncwarp();
     int total = 0;
-    for (int n = 0; n < 16; n++) {
-        const int bx = ((n >> 2) & 1) * 2 + (n & 1), by = ((n >> 3) & 1) * 2 + ((n >> 1) & 1);  // block_pos, 108-110
-        const bool hl = bx > 0 || la, ht = by > 0 || ta;
+    for (int t = 0; t < 10; t++) {
+        // the half's block: the upper one of the diagonal (the one with the smaller by), or the lower one
+        const int by0 = max(0, (t - 2) >> 1), bx0 = t - 2 * by0;
+        const bool two = bx0 >= 2 && by0 < 3;  // the diagonal's second block, (bx0 - 2, by0 + 1)
+        const bool act = half == 0 || two;
+        const int bx = act ? bx0 - 2 * half : 0, by = act ? by0 + half : 0;
+        const bool hlf = bx > 0 || la, ht = by > 0 || ta;
         const bool htl = bx > 0 ? (by > 0 ? true : ta) : (by > 0 ? la : tla);
         // above-right: the macroblocks above for the top row, else a block decoded earlier (zorder, 2363-2365)
         const bool htr = by == 0 ? (bx < 3 ? ta : tra) : (bx == 3 ? false : zorder_d(bx + 1, by - 1) < zorder_d(bx, by));
-        if (lane < 13) {
+        int* edge = S.edge[half];
+        if (hl < 13) {
             int v = 0;
-            if (lane == 0) {
+            if (hl == 0) {
                 if (htl) v = by == 0 ? S.top[bx * 4] : (bx == 0 ? S.left[by * 4 - 1] : S.i4rec[(by * 4 - 1) * 16 + bx * 4 - 1]);
-            } else if (lane < 9) {
-                const int i = lane - 1;
+            } else if (hl < 9) {
+                const int i = hl - 1;
                 const int xi = (i < 4 || htr) ? i : 3;  // above-right not available: the last sample above repeated
                 if (ht) v = by == 0 ? S.top[1 + bx * 4 + xi] : S.i4rec[(by * 4 - 1) * 16 + bx * 4 + xi];
             } else {
-                const int j = lane - 9;
-                if (hl) v = bx == 0 ? S.left[by * 4 + j] : S.i4rec[(by * 4 + j) * 16 + bx * 4 - 1];
+                const int j = hl - 9;
+                if (hlf) v = bx == 0 ? S.left[by * 4 + j] : S.i4rec[(by * 4 + j) * 16 + bx * 4 - 1];
             }
-            S.edge[lane] = v;
+            edge[hl] = v;
         }
         __syncwarp();
         // pred_i4_mode, enc/frame.rs:619-629
@@ -316,43 +326,46 @@ __device__ int code_i4_trial(const DecideParams& P, DecideSmem<T>& S, const unsi
         const int b = by > 0 ? S.i4modes[(by - 1) * 4 + bx] : S.nbm[4 + bx];
         const int predicted = (a >= 0 && b >= 0) ? min(a, b) : 2;
         // the DC value (8.3.1.2.3)
-        const int st = S.edge[1] + S.edge[2] + S.edge[3] + S.edge[4], sl = S.edge[9] + S.edge[10] + S.edge[11] + S.edge[12];
-        const int dcv = (ht && hl) ? (st + sl + 4) >> 3 : (hl ? (sl + 2) >> 2 : (ht ? (st + 2) >> 2 : 1 << (bd - 1)));
+        const int st = edge[1] + edge[2] + edge[3] + edge[4], sl = edge[9] + edge[10] + edge[11] + edge[12];
+        const int dcv = (ht && hlf) ? (st + sl + 4) >> 3 : (hlf ? (sl + 2) >> 2 : (ht ? (st + 2) >> 2 : 1 << (bd - 1)));
         unsigned key = 0xffffffffu;
         {
-            const int mode = lane < 9 ? lane : 2;
-            const bool ok = lane < 9 &&
-                            ((mode == 0 || mode == 3 || mode == 7) ? ht : ((mode == 1 || mode == 8) ? hl : (mode == 2 ? true : (ht && hl && htl))));
+            const int mode = hl < 9 ? hl : 2;
+            const bool ok = hl < 9 &&
+                            ((mode == 0 || mode == 3 || mode == 7) ? ht : ((mode == 1 || mode == 8) ? hlf : (mode == 2 ? true : (ht && hlf && htl))));
             int d[16];
 #pragma unroll
             for (int k = 0; k < 16; k++) {
                 const unsigned e = tab[mode * 17 + k];
-                const int pv = mode == 2 ? dcv : (S.edge[e & 15] + 2 * S.edge[(e >> 4) & 15] + S.edge[(e >> 8) & 15] + 2) >> 2;
+                const int pv = mode == 2 ? dcv : (edge[e & 15] + 2 * edge[(e >> 4) & 15] + edge[(e >> 8) & 15] + 2) >> 2;
                 d[k] = src_at(S.a, bx * 4 + (k & 3), by * 4 + (k >> 2)) - pv;
             }
             const int cost = satd4_d(d) + lam * (mode == predicted ? 1 : 4);
             if (ok) key = ((unsigned)cost << 4) | (unsigned)mode;  // the cheapest, the lowest mode on ties
         }
 #pragma unroll
-        for (int off = 16; off >= 1; off >>= 1) key = min(key, __shfl_xor_sync(FULL, key, off));
+        for (int off = 8; off >= 1; off >>= 1) key = min(key, __shfl_xor_sync(FULL, key, off));
         const int bm = (int)(key & 15u);
-        total += (int)(key >> 4);
+        {
+            const unsigned k0 = __shfl_sync(FULL, key, 0), k1 = __shfl_sync(FULL, key, 16);
+            total += (int)(k0 >> 4) + (two ? (int)(k1 >> 4) : 0);
+        }
         // quant_block (intra), enc/frame.rs:1025-1046, and the reconstruction: a coefficient a lane
-        const int p = lane & 15, r = p >> 2, c = p & 3;
+        const int p = hl, r = p >> 2, c = p & 3;
         const unsigned e = tab[bm * 17 + p];
-        const int pv = bm == 2 ? dcv : (S.edge[e & 15] + 2 * S.edge[(e >> 4) & 15] + S.edge[(e >> 8) & 15] + 2) >> 2;
+        const int pv = bm == 2 ? dcv : (edge[e & 15] + 2 * edge[(e >> 4) & 15] + edge[(e >> 8) & 15] + 2) >> 2;
         const int coef = fdct4_lanes(src_at(S.a, bx * 4 + c, by * 4 + r) - pv);
         const int cls = q_class_d(p);
         const int l = q_quant_d(coef, c_q_mf[m6][cls], f, qbits);
-        const int nz = __popc(__ballot_sync(FULL, lane < 16 && l != 0));
+        const int nz = __popc(__ballot_sync(FULL, l != 0) & hmask);
         const int rec = idct4_lanes((l * c_q_v[m6][cls]) << (qp / 6), pv, maxv);
-        if (lane < 16) {
+        if (act) {
             S.i4lv[by * 4 + bx][invzz4_at(p)] = (int16_t)l;
             S.i4rec[(by * 4 + r) * 16 + bx * 4 + c] = nz > 0 ? rec : pv;
-        }
-        if (lane == 0) {
-            S.i4nnz[by * 4 + bx] = (uint8_t)nz;
-            S.i4modes[by * 4 + bx] = (uint8_t)bm;
+            if (hl == 0) {
+                S.i4nnz[by * 4 + bx] = (uint8_t)nz;
+                S.i4modes[by * 4 + bx] = (uint8_t)bm;
+            }
         }
         __syncwarp();
     }
