@@ -536,7 +536,7 @@ def run_batched(args, rank, world):
     total = nmb * (world if world > 1 else 1)
     mbs = lambda ms: nmb * args.steps / (ms * 1e-3) * (world if world > 1 else 1)
     line = {
-        "metric": "batched inter-analysis MB/s: 64 mixed-resolution streams, auto mode, one launch per stage and step",
+        "metric": f"batched inter-analysis MB/s: {args.streams} mixed-resolution streams, auto mode, one launch per stage and step",
         "value": mbs(ms_b), "unit": "MB/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_b / args.steps, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
         "dtype": "u8", "data": "synthetic: per-stream seeded value noise, pan, 8 moving rectangles, sigma 3",
