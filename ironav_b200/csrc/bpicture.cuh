@@ -49,9 +49,10 @@ static __device__ void load_neighbours_b(const AnalyseParams& __restrict__ P, Wa
 
 // SATD of the prediction of the partition at 4x4 block (bx, by), (4 << lgw) x (4 << lgh) samples, from list
 // 0 with vector v0 (use bit 0), list 1 with v1 (bit 1), or both averaged ((a + b + 1) >> 1, b_pred
-// enc/frame.rs:1766-1770 and decide_b's avg 1567); every lane gets the sum.
+// enc/frame.rs:1766-1770 and decide_b's avg 1567); every lane gets the sum. Out of line: inlined at its five
+// call sites it cost the kernel 6 % in instruction-cache misses.
 template <class T>
-static __device__ __forceinline__ int mix_satd(const AnalyseParams& __restrict__ P, WarpSmemB<T>& __restrict__ S, int bx, int by, int lgw, int lgh, int2 v0,
+static __device__ __noinline__ int mix_satd(const AnalyseParams& __restrict__ P, WarpSmemB<T>& __restrict__ S, int bx, int by, int lgw, int lgh, int2 v0,
                                                int2 v1, int use) {
     const int lane = threadIdx.x & 31;
     const int lg = lgw + lgh, w = 4 << lgw, h = 4 << lgh;
