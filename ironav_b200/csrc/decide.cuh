@@ -285,8 +285,9 @@ __device__ __forceinline__ int zorder_d(int bx, int by) { return ((by >> 1) << 3
 // on lanes 0-8 of the half, a coefficient a lane for the coding) rather than one at a time in decoding
 // order; the top-right's availability stays the decoding order's (zorder), and the cost is the same sum.
 // Returns the summed cost (every lane).
-template <class T>
-__device__ int code_i4_trial(const DecideParams& P, DecideSmem<T>& S, const unsigned* tab, bool ta, bool la, bool tra) {
+template <class T, bool STOPPABLE = false>
+__device__ int code_i4_trial(const DecideParams& P, DecideSmem<T>& S, const unsigned* tab, bool ta, bool la, bool tra,
+                             const volatile int* stop = nullptr, int seq = 0) {
     const int lane = threadIdx.x & 31, hl = lane & 15, half = lane >> 4;
     const unsigned hmask = half ? 0xffff0000u : 0x0000ffffu;
     const int bd = P.C.bd, maxv = (1 << bd) - 1, lam = P.C.A.lambda;
@@ -296,6 +297,9 @@ __device__ int code_i4_trial(const DecideParams& P, DecideSmem<T>& S, const unsi
     __syncwarp();
     int total = 0;
     for (int t = 0; t < 10; t++) {
+        if constexpr (STOPPABLE) {
+            if (__shfl_sync(FULL, (int)(*stop == seq), 0)) return 0;  // not needed after all
+        }
         // the half's block: the upper one of the diagonal (the one with the smaller by), or the lower one
         const int by0 = max(0, (t - 2) >> 1), bx0 = t - 2 * by0;
         const bool two = bx0 >= 2 && by0 < 3;  // the diagonal's second block, (bx0 - 2, by0 + 1)
@@ -599,9 +603,89 @@ __device__ void inter_tail(const DecideParams& P, DecideSmem<T>& S, const ironav
     __syncwarp();
 }
 
-// code_mb for one P macroblock without CABAC, enc/frame.rs:715-790.
+// ---- warp pairs (one stream's latency-bound wavefront) -----------------------------------------------
+// The second warp of a pair works out a macroblock's intra side, best_i16 and then the Intra4x4 trial,
+// while the first runs best_inter. The reference tries Intra4x4 only when intra is competitive after
+// best_inter (766-779); the first warp then takes the trial's result, and otherwise tells the second to
+// stop. The warps meet through sequence words in shared memory (one command, then best_i16's result, then
+// the end of the intra side, per macroblock that reaches the intra stage); every wait is bounded in wall
+// time and gives up when the launch's error word is set.
+struct PairSync {
+    volatile int cmd_seq;   // first warp: its latest command (cmd: 1 the intra side, -1 exit)
+    volatile int cmd;
+    volatile int stop_seq;  // first warp: the trial of this command is not needed
+    volatile int i16_seq;   // second warp: best_i16 of this command is in i16
+    volatile int done_seq;  // second warp: the intra side of this command is finished (c4 when it ran through)
+    int2 i16;
+    int c4;
+    int ta, la, tra;        // the macroblock's neighbour availability
+    int seq;                // the first warp's command count
+};
+constexpr unsigned long long PAIR_WAIT_NS = 20000000000ull;
+
+// Waits until *word == want; false when the launch's error word is set or after PAIR_WAIT_NS (which sets
+// it). The warp polls in step (lane 0's read decides) and fences before it reads what the word guards.
+static __device__ bool pair_wait(const AnalyseParams& A, const volatile int* word, int want) {
+    const unsigned long long t0 = globaltimer();
+    for (unsigned i = 0;; i++) {
+        if (__shfl_sync(FULL, (int)(*word == want), 0)) break;
+        if ((i & 63) == 63) {
+            bool quit = false;
+            if ((threadIdx.x & 31) == 0) {
+                quit = ld_acquire(A.err) != 0;
+                if (!quit && globaltimer() - t0 > PAIR_WAIT_NS) {
+                    atomicOr(A.err, 1u);
+                    quit = true;
+                }
+            }
+            if (__shfl_sync(FULL, quit, 0)) return false;
+        }
+        __nanosleep(i < 64 ? 32 : 256);
+    }
+    __threadfence_block();
+    return true;
+}
+
+// Makes the warp's shared-memory writes visible, then sets *word = v (lane 0).
+static __device__ __forceinline__ void pair_publish(volatile int* word, int v) {
+    __threadfence_block();
+    __syncwarp();
+    if ((threadIdx.x & 31) == 0) *word = v;
+    __syncwarp();
+}
+
+// The first warp's command: returns its sequence number.
+static __device__ __forceinline__ int pair_command(PairSync& X, int cmd) {
+    const int seq = X.seq + 1;
+    __syncwarp();
+    if ((threadIdx.x & 31) == 0) {
+        X.seq = seq;
+        X.cmd = cmd;
+    }
+    pair_publish(&X.cmd_seq, seq);
+    return seq;
+}
+
+// The second warp: the intra side of each macroblock the first warp sends, until told to exit.
 template <class T>
-__device__ void decide_mb(const DecideParams& P, DecideSmem<T>& S, const unsigned* i4tab, int mb, int mbx, int mby) {
+__device__ void pair_helper(const DecideParams& P, DecideSmem<T>& S, PairSync& X, const unsigned* i4tab) {
+    const AnalyseParams& A = P.C.A;
+    for (int seq = 1;; seq++) {
+        if (!pair_wait(A, &X.cmd_seq, seq) || __shfl_sync(FULL, X.cmd, 0) < 0) return;
+        const bool ta = X.ta != 0, la = X.la != 0, tra = X.tra != 0;
+        const int2 i16 = best_i16_d(P, S, ta, la);
+        if ((threadIdx.x & 31) == 0) X.i16 = i16;
+        pair_publish(&X.i16_seq, seq);
+        const int c4 = code_i4_trial<T, true>(P, S, i4tab, ta, la, tra, &X.stop_seq, seq);
+        if ((threadIdx.x & 31) == 0) X.c4 = c4;
+        pair_publish(&X.done_seq, seq);
+    }
+}
+
+// code_mb for one P macroblock without CABAC, enc/frame.rs:715-790. X: the warp pair's meeting words, when
+// the macroblock's intra side runs on the pair's second warp (PAIR).
+template <class T, bool PAIR = false>
+__device__ void decide_mb(const DecideParams& P, DecideSmem<T>& S, const unsigned* i4tab, int mb, int mbx, int mby, PairSync* X = nullptr) {
     const int lane = threadIdx.x & 31;
     const AnalyseParams& A = P.C.A;
     const CodeParams& C = P.C;
@@ -679,8 +763,18 @@ __device__ void decide_mb(const DecideParams& P, DecideSmem<T>& S, const unsigne
         }
     }
     load_intra_neighbours(P, S, mb, mbx, mby, ta, la, tra);
-    const int2 i16 = best_i16_d(P, S, ta, la);
-    int best_intra = i16.y + lam * 4;
+    int2 i16 = make_int2(2, 0);
+    int seq = 0;
+    if constexpr (PAIR) {
+        if (lane == 0) {
+            X->ta = ta;
+            X->la = la;
+            X->tra = tra;
+        }
+        seq = pair_command(*X, 1);
+    } else {
+        i16 = best_i16_d(P, S, ta, la);
+    }
     // best_inter, enc/frame.rs:839-849
     int part = 0, cost = 0, bestr = 0;
     uint32_t sub = 0;
@@ -698,14 +792,29 @@ __device__ void decide_mb(const DecideParams& P, DecideSmem<T>& S, const unsigne
             __syncwarp();
         }
     }
+    if constexpr (PAIR) {
+        // on a failed wait the launch's error word is set and the host discards the picture
+        i16 = pair_wait(A, &X->i16_seq, seq) ? X->i16 : make_int2(2, 1 << 28);
+    }
+    int best_intra = i16.y + lam * 4;
     // Intra4x4 is tried by coding it when intra is competitive (766-779)
     bool i4 = false;
     if (best_intra < cost) {
-        const int c4 = code_i4_trial(P, S, i4tab, ta, la, tra) + lam * 6;
+        int c4;
+        if constexpr (PAIR) {
+            c4 = pair_wait(A, &X->done_seq, seq) ? X->c4 : (1 << 28);
+        } else {
+            c4 = code_i4_trial(P, S, i4tab, ta, la, tra);
+        }
+        c4 += lam * 6;
         if (c4 < best_intra) {
             best_intra = c4;
             i4 = true;
         }
+    } else if constexpr (PAIR) {
+        // the trial is not the reference's here: stop it, and keep the pair in step
+        if (lane == 0) X->stop_seq = seq;
+        pair_wait(A, &X->done_seq, seq);
     }
     if (cost <= best_intra) {
         if (lane == 0) {
@@ -768,8 +877,8 @@ __device__ void decide_mb(const DecideParams& P, DecideSmem<T>& S, const unsigne
 
 // One macroblock of decide mode: waits for its left and top-right (top at the right edge) neighbours,
 // decides and codes it, and publishes it. Returns false when a wait gave up (the launch is abandoned).
-template <class T>
-__device__ bool decide_one(const DecideParams& P, DecideSmem<T>& S, const unsigned* i4tab, int mb) {
+template <class T, bool PAIR = false>
+__device__ bool decide_one(const DecideParams& P, DecideSmem<T>& S, const unsigned* i4tab, int mb, PairSync* X = nullptr) {
     const int lane = threadIdx.x & 31;
     const AnalyseParams& A = P.C.A;
     const int mbx = mb % A.mb_w, mby = mb / A.mb_w;
@@ -786,7 +895,7 @@ __device__ bool decide_one(const DecideParams& P, DecideSmem<T>& S, const unsign
     if (ok && mby > start) ok = wait_published(A, (mbx + 1 < A.mb_w) ? mb - A.mb_w + 1 : mb - A.mb_w);
     if (!__all_sync(FULL, ok)) return false;
     load_neighbours(A, S.a, A.states_out);
-    decide_mb<T>(P, S, i4tab, mb, mbx, mby);
+    decide_mb<T, PAIR>(P, S, i4tab, mb, mbx, mby, X);
     if (lane < 18) reinterpret_cast<uint32_t*>(&A.states_out[mb])[lane] = reinterpret_cast<const uint32_t*>(&S.a.out)[lane];
     // the reconstruction, code and state before the flag
     __threadfence();
@@ -801,21 +910,36 @@ __device__ __forceinline__ void fill_i4tab(unsigned* tab) {
     __syncthreads();
 }
 
+// Decide mode for one stream on warp pairs: the first warp of a pair takes the tickets and decides, the
+// second works out the intra side of the first's macroblock (PairSync). One stream's wavefront keeps far
+// fewer macroblocks in flight than the launch has pairs, so the second warps shorten each macroblock's
+// latency at no cost in concurrency.
 template <class T>
 __global__ void __launch_bounds__(K7_WARPS * 32, K7_MIN_BLOCKS) decide_kernel(const __grid_constant__ DecideParams P) {
-    __shared__ DecideSmem<T> smem[K7_WARPS];
+    __shared__ DecideSmem<T> smem[K7_WARPS / 2];
+    __shared__ PairSync sync[K7_WARPS / 2];
     __shared__ unsigned i4tab[9 * 17];
-    fill_i4tab(i4tab);
-    const int lane = threadIdx.x & 31;
-    DecideSmem<T>& S = smem[threadIdx.x >> 5];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    PairSync& X = sync[w >> 1];
+    if ((w & 1) == 0 && lane == 0) {
+        X.cmd_seq = X.cmd = X.stop_seq = X.i16_seq = X.done_seq = 0;
+        X.seq = 0;
+    }
+    fill_i4tab(i4tab);  // its __syncthreads also publishes the words above
+    DecideSmem<T>& S = smem[w >> 1];
+    if (w & 1) {
+        pair_helper<T>(P, S, X, i4tab);
+        return;
+    }
     const AnalyseParams& A = P.C.A;
     for (;;) {
         unsigned t = 0;
         if (lane == 0) t = atomicAdd(A.ticket, 1u);
         t = __shfl_sync(FULL, t, 0);
         if (t >= (unsigned)A.nmb) break;
-        if (!decide_one<T>(P, S, i4tab, A.order[t])) break;
+        if (!decide_one<T, true>(P, S, i4tab, A.order[t], &X)) break;
     }
+    pair_command(X, -1);
 }
 
 // Decide mode for many streams in one launch: ticket t is order[t] = stream << 20 | macroblock, in the
