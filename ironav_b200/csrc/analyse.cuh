@@ -482,6 +482,7 @@ static __device__ __noinline__ int4 motion_search(const AnalyseParams& __restric
     const bool fast = P.fast != 0;
     const int nsteps = fast ? 2 : 3;
     const int k = g < 4 ? g : g + 1, kx = k % 3, ky = k / 3;
+    int rounds = 0;  // the reference evaluates four moves a round (counted once, after the diamond)
     for (int si = 0; si < nsteps; si++) {
         const int step = fast ? (si == 0 ? 8 : 4) : (16 >> si);
         const int iters = step == 4 ? 32 : 4;
@@ -490,7 +491,7 @@ static __device__ __noinline__ int4 motion_search(const AnalyseParams& __restric
             const int X0 = clx(cx - step), X2 = clx(cx + step), Y0 = cly(cy - step), Y2 = cly(cy + step);
             const int qx = kx == 0 ? X0 : (kx == 1 ? cx : X2), qy = ky == 0 ? Y0 : (ky == 1 ? cy : Y2);
             const int sc = sad_lane<T>(g0, src0, sw, w, h, qx, qy, true) + lam * mvd_bits_d(qx, qy, mvpx, mvpy);
-            if (lane == 0) S.sad_px += (uint32_t)(4 * w * h);
+            rounds++;
             bool moved;
             if (X0 == cx - step && X2 == cx + step && Y0 == cy - step && Y2 == cy + step) {
                 // no clamp: left, else right; then up from that column, else down
@@ -530,6 +531,7 @@ static __device__ __noinline__ int4 motion_search(const AnalyseParams& __restric
             if (!moved) break;
         }
     }
+    if (lane == 0) S.sad_px += (uint32_t)(4 * w * h * rounds);
     // live coding's early exit (990-992)
     if (P.fast && bc < (w * h) / 8 + lam) return make_int4(bc - lam * mvd_bits_d(bxv, byv, mvpx, mvpy), bxv, byv, 0);
     const int lgw = w4 == 4 ? 2 : (w4 == 2 ? 1 : 0), lgh = h4 == 4 ? 2 : (h4 == 2 ? 1 : 0);
@@ -545,18 +547,19 @@ static __device__ __noinline__ int4 motion_search(const AnalyseParams& __restric
     }
     __syncwarp();
     pred_batch(P, S, r, bx, by, lgw, lgh, 9, false);
-    if (lane < 9) S.cost[lane] += lam * mvd_bits_d(S.cand[lane].x, S.cand[lane].y, mvpx, mvpy);
-    __syncwarp();
-    if (lane == 0) S.satd_px += (uint32_t)(9 * w * h);
-    bc = S.cost[0];
-    for (int c = 1; c < 9; c++) {
-        const int v = S.cost[c];
-        if (v < bc) {
-            bxv = S.cand[c].x;
-            byv = S.cand[c].y;
-            bc = v;
-        }
+    // the first of least cost in the square's order (strict <, centre first): min over (cost, position);
+    // costs are SATD + lambda * bits, far below 2^27
+    {
+        unsigned key = 0xffffffffu;
+        if (lane < 9) key = ((unsigned)(S.cost[lane] + lam * mvd_bits_d(S.cand[lane].x, S.cand[lane].y, mvpx, mvpy)) << 4) | (unsigned)lane;
+#pragma unroll
+        for (int off = 16; off >= 1; off >>= 1) key = min(key, __shfl_xor_sync(FULL, key, off));
+        const int c = (int)(key & 15u);
+        bc = (int)(key >> 4);
+        bxv = S.cand[c].x;
+        byv = S.cand[c].y;
     }
+    if (lane == 0) S.satd_px += (uint32_t)(9 * w * h);
     __syncwarp();
     if (!P.fast) {
         // the 4 quarter samples around the new centre: (0,-1) (-1,0) (1,0) (0,1)
@@ -566,20 +569,20 @@ static __device__ __noinline__ int4 motion_search(const AnalyseParams& __restric
         }
         __syncwarp();
         pred_batch(P, S, r, bx, by, lgw, lgh, 4, false);
-        if (lane < 4) S.cost[lane] += lam * mvd_bits_d(S.cand[lane].x, S.cand[lane].y, mvpx, mvpy);
-        __syncwarp();
-        if (lane == 0) S.satd_px += (uint32_t)(4 * w * h);
-        int nbx = bxv, nby = byv;
-        for (int c = 0; c < 4; c++) {
-            const int v = S.cost[c];
-            if (v < bc) {
-                nbx = S.cand[c].x;
-                nby = S.cand[c].y;
-                bc = v;
+        // the centre keeps ties (key position 0), then the four in order
+        {
+            unsigned key = (unsigned)bc << 4;
+            if (lane < 4) key = ((unsigned)(S.cost[lane] + lam * mvd_bits_d(S.cand[lane].x, S.cand[lane].y, mvpx, mvpy)) << 4) | (unsigned)(lane + 1);
+#pragma unroll
+            for (int off = 16; off >= 1; off >>= 1) key = min(key, __shfl_xor_sync(FULL, key, off));
+            const int c = (int)(key & 15u);
+            bc = (int)(key >> 4);
+            if (c > 0) {
+                bxv = S.cand[c - 1].x;
+                byv = S.cand[c - 1].y;
             }
         }
-        bxv = nbx;
-        byv = nby;
+        if (lane == 0) S.satd_px += (uint32_t)(4 * w * h);
         __syncwarp();
     }
     return make_int4(bc - lam * mvd_bits_d(bxv, byv, mvpx, mvpy), bxv, byv, 0);
