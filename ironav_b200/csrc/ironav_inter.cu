@@ -413,7 +413,7 @@ static int load_source(ironav_ctx* c, const void* y, int stride, cudaMemcpyKind 
     const int B = sample_bytes(c);
     CK(cudaMemcpy2DAsync(c->d_src, (size_t)c->pw * B, y, (size_t)stride * B, (size_t)c->width * B, c->height, kind, c->stream));
     if (c->width != c->pw || c->height != c->ph) {
-        dim3 grid((c->pw + 255) / 256, c->ph);
+        const unsigned grid = (unsigned)((pad_edges_count(c->width, c->height, c->pw, c->ph) + 255) / 256);
         if (B == 2) pad_edges_kernel<uint16_t><<<grid, 256, 0, c->stream>>>(reinterpret_cast<uint16_t*>(c->d_src), c->width, c->height, c->pw, c->ph);
         else pad_edges_kernel<uint8_t><<<grid, 256, 0, c->stream>>>(c->d_src, c->width, c->height, c->pw, c->ph);
     }
@@ -644,7 +644,7 @@ static int load_chroma(ironav_ctx* c, uint8_t* dst, const void* src, int stride,
     const int B = sample_bytes(c), cw = c->mb_w * 8, ch = c->mb_h * 8;
     CK(cudaMemcpy2DAsync(dst, (size_t)cw * B, src, (size_t)stride * B, (size_t)w * B, h, kind, c->stream));
     if (w != cw || h != ch) {
-        dim3 grid((cw + 255) / 256, ch);
+        const unsigned grid = (unsigned)((pad_edges_count(w, h, cw, ch) + 255) / 256);
         if (B == 2) pad_edges_kernel<uint16_t><<<grid, 256, 0, c->stream>>>(reinterpret_cast<uint16_t*>(dst), w, h, cw, ch);
         else pad_edges_kernel<uint8_t><<<grid, 256, 0, c->stream>>>(dst, w, h, cw, ch);
     }

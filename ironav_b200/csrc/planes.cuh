@@ -110,11 +110,26 @@ static __global__ void __launch_bounds__(K1_THREADS) halfpel_planes_kernel(const
 }
 
 // Repeats the right and bottom edges of a w x h picture stored in a pw x ph buffer (rows pw apart)
-// to whole macroblocks (H264Encoder::source, enc/mod.rs:502-519). Reads only the w x h part.
+// to whole macroblocks (H264Encoder::source, enc/mod.rs:502-519). Reads only the w x h part. Thread i
+// writes the i-th padding sample: the bottom rows h..ph-1 (pw samples each), then the right columns
+// w..pw-1 of rows 0..h-1 (pad_edges_count of them).
+__host__ __device__ __forceinline__ long long pad_edges_count(int w, int h, int pw, int ph) {
+    return (long long)(ph - h) * pw + (long long)h * (pw - w);
+}
 template <class T>
 static __global__ void pad_edges_kernel(T* __restrict__ p, int w, int h, int pw, int ph) {
-    int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
-    if (x >= pw || y >= ph || (x < w && y < h)) return;
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x, nb = (long long)(ph - h) * pw;
+    int x, y;
+    if (i < nb) {
+        y = h + (int)(i / pw);
+        x = (int)(i % pw);
+    } else if (i < pad_edges_count(w, h, pw, ph)) {  // pw > w here
+        const long long j = i - nb;
+        y = (int)(j / (pw - w));
+        x = w + (int)(j % (pw - w));
+    } else {
+        return;
+    }
     p[(size_t)y * pw + x] = p[(size_t)min(y, h - 1) * pw + min(x, w - 1)];
 }
 
