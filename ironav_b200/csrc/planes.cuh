@@ -82,6 +82,100 @@ __device__ __forceinline__ void planes_tile(const T* __restrict__ luma, int stri
     }
 }
 
+// dp4a with unsigned bytes in a and signed bytes in b: c + sum of a_k * b_k.
+__device__ __forceinline__ int k1_dp4a(uint32_t a, uint32_t b, int c) {
+    int d;
+    asm("dp4a.u32.s32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c));
+    return d;
+}
+// tap6's weights as signed bytes: (1, -5, 20, 20) on four samples, then (-5, 1) on the next two
+constexpr uint32_t K1_TAPS_A = 0x1414FB01u, K1_TAPS_B = 0x000001FBu;
+constexpr int K1_GW = 48;  // staged row pitch in words: 48 = 16 mod 32 banks, so a warp's two rows never share one
+
+// The same tile for 8-bit pictures, four columns a thread: the integer samples are staged as packed bytes
+// (word k of a staged row holds samples x0 - 4 + 4k .. x0 - 1 + 4k), the horizontal taps of four columns
+// are two dp4a each on byte windows of three words, the vertical taps of a column two dp4a on its bytes of
+// six rows gathered with prmt, and the diagonal taps run on the unrounded horizontal sums in shared memory.
+// Every plane is written a 32-bit word (four samples) at a time. Same values as planes_tile.
+__device__ __forceinline__ void planes_tile8(const uint8_t* __restrict__ luma, int stride, int w, int h, uint8_t* __restrict__ out,
+                                             long long psize, int sw, int sh, int x0, int y0) {
+    constexpr int GR = K1_TH + 5, GWORDS = (K1_TW + 8) / 4;  // 21 rows of 18 words: samples x0-4 .. x0+67
+    __shared__ uint32_t g[GR][K1_GW];
+    __shared__ __align__(16) int b1[GR][K1_TW];
+    const int tid = threadIdx.x;
+    // stage rows y0-2 .. y0+18, samples x0-4 .. x0+71: whole words straight from the luma when every one
+    // of them lies inside the picture and the rows are word aligned, else sample by sample with the clamps
+    const bool fast = x0 - 4 - PAD >= 0 && x0 + 4 * GWORDS - 5 - PAD <= w - 1 && x0 + 4 * GWORDS - 5 <= sw - 1 &&
+                      y0 - 2 - PAD >= 0 && y0 + GR - 3 - PAD <= h - 1 &&
+                      ((reinterpret_cast<uintptr_t>(luma) | (uintptr_t)stride) & 3) == 0;
+    for (int i = tid; i < GR * GWORDS; i += K1_THREADS) {
+        const int r = i / GWORDS, k = i % GWORDS;
+        uint32_t v = 0;
+        if (fast) {
+            v = *reinterpret_cast<const uint32_t*>(luma + (size_t)(y0 - 2 + r - PAD) * stride + (x0 - 4 + 4 * k - PAD));
+        } else {
+            const int sy = min(max(min(max(y0 - 2 + r, 0), sh - 1) - PAD, 0), h - 1);
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const int sx = min(max(min(max(x0 - 4 + 4 * k + j, 0), sw - 1) - PAD, 0), w - 1);
+                v |= (uint32_t)luma[(size_t)sy * stride + sx] << (8 * j);
+            }
+        }
+        g[r][k] = v;
+    }
+    __syncthreads();
+    // the unrounded horizontal sums of columns x0 + 4q .. +3 of every staged row (only 2 <= x < sw - 3,
+    // enc/subpel.rs:78-82; elsewhere 0); the 6-tap window of column X + j starts at byte 2 + j of word q
+    for (int i = tid; i < GR * (K1_TW / 4); i += K1_THREADS) {
+        const int r = i / (K1_TW / 4), q = i % (K1_TW / 4);
+        const uint32_t w0 = g[r][q], w1 = g[r][q + 1], w2 = g[r][q + 2];
+        int4 v;
+        int* vp = reinterpret_cast<int*>(&v);
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const uint32_t wa = __funnelshift_r(j < 2 ? w0 : w1, j < 2 ? w1 : w2, 8 * ((2 + j) & 3));
+            const uint32_t wb = __funnelshift_r(j < 2 ? w1 : w2, j < 2 ? w2 : 0u, 8 * ((6 + j) & 3));
+            const int gx = x0 + 4 * q + j;
+            vp[j] = (gx >= 2 && gx < sw - 3) ? k1_dp4a(wa, K1_TAPS_A, k1_dp4a(wb, K1_TAPS_B, 0)) : 0;
+        }
+        *reinterpret_cast<int4*>(&b1[r][4 * q]) = v;
+    }
+    __syncthreads();
+    // a thread: columns X .. X + 3 of one row
+    const int q = tid % (K1_TW / 4), rr = tid / (K1_TW / 4);
+    const int X = x0 + 4 * q, y = y0 + rr;
+    if (X >= sw || y >= sh) return;  // sw is a multiple of 16: a group is all in or all out
+    const bool rows_ok = y >= 2 && y < sh - 3;  // rows of h and j outside stay 0 (enc/subpel.rs:95-97)
+    uint32_t gr[6];
+#pragma unroll
+    for (int k = 0; k < 6; k++) gr[k] = g[rr + k][q + 1];
+    int4 bv[6];
+#pragma unroll
+    for (int k = 0; k < 6; k++) bv[k] = *reinterpret_cast<const int4*>(&b1[rr + k][4 * q]);
+    uint32_t pb = 0, ph = 0, pj = 0;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        const int* b2 = reinterpret_cast<const int*>(&bv[2]);
+        pb |= k1_clip((b2[j] + 16) >> 5, 255) << (8 * j);
+        if (rows_ok) {
+            // byte j of rows y-2 .. y+1, then of rows y+2 .. y+3
+            const unsigned sel = (unsigned)j | ((unsigned)(j + 4) << 4);
+            const uint32_t t01 = __byte_perm(gr[0], gr[1], sel), t23 = __byte_perm(gr[2], gr[3], sel);
+            const uint32_t ca = __byte_perm(t01, t23, 0x5410), cb = __byte_perm(gr[4], gr[5], sel);
+            ph |= k1_clip((k1_dp4a(ca, K1_TAPS_A, k1_dp4a(cb, K1_TAPS_B, 0)) + 16) >> 5, 255) << (8 * j);
+            const int v0 = reinterpret_cast<const int*>(&bv[0])[j], v1 = reinterpret_cast<const int*>(&bv[1])[j];
+            const int v2 = reinterpret_cast<const int*>(&bv[2])[j], v3 = reinterpret_cast<const int*>(&bv[3])[j];
+            const int v4 = reinterpret_cast<const int*>(&bv[4])[j], v5 = reinterpret_cast<const int*>(&bv[5])[j];
+            pj |= k1_clip((k1_tap6(v0, v1, v2, v3, v4, v5) + 512) >> 10, 255) << (8 * j);
+        }
+    }
+    const size_t o = (size_t)y * sw + X;
+    *reinterpret_cast<uint32_t*>(out + o) = gr[2];
+    *reinterpret_cast<uint32_t*>(out + psize + o) = pb;
+    *reinterpret_cast<uint32_t*>(out + 2 * psize + o) = ph;
+    *reinterpret_cast<uint32_t*>(out + 3 * psize + o) = pj;
+}
+
 // The co-located vector of macroblock i (col_mv, enc/frame.rs:944-947) from the reference picture's own
 // decisions; none when the picture was intra coded (states == nullptr).
 __device__ __forceinline__ void col_extract(const ironav_mbstate* __restrict__ states, ColMv* __restrict__ col, int i) {
@@ -106,7 +200,8 @@ static __global__ void __launch_bounds__(K1_THREADS) halfpel_planes_kernel(const
                                                                              ColMv* __restrict__ col, int nmb) {
     const int gi = (blockIdx.y * gridDim.x + blockIdx.x) * K1_THREADS + threadIdx.x;
     if (col && gi < nmb) col_extract(states, col, gi);
-    planes_tile(luma, stride, w, h, out, psize, sw, sh, blockIdx.x * K1_TW, blockIdx.y * K1_TH, maxv);
+    if constexpr (sizeof(T) == 1) planes_tile8(luma, stride, w, h, out, psize, sw, sh, blockIdx.x * K1_TW, blockIdx.y * K1_TH);
+    else planes_tile(luma, stride, w, h, out, psize, sw, sh, blockIdx.x * K1_TW, blockIdx.y * K1_TH, maxv);
 }
 
 // Repeats the right and bottom edges of a w x h picture stored in a pw x ph buffer (rows pw apart)
