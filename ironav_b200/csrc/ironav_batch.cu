@@ -56,8 +56,11 @@ __global__ void __launch_bounds__(K1_THREADS) planes_batch_kernel(const PlaneJob
     const int j = find_job(jobs, njobs, (int)blockIdx.x, [](const PlaneJob& p) { return p.tile0; });
     const PlaneJob& J = jobs[j];
     const int t = (int)blockIdx.x - J.tile0;
-    planes_tile(reinterpret_cast<const T*>(J.luma), J.stride, J.w, J.h, reinterpret_cast<T*>(J.out), J.psize, J.sw, J.sh,
-                (t % J.tiles_x) * K1_TW, (t / J.tiles_x) * K1_TH, maxv);
+    if constexpr (sizeof(T) == 1)
+        planes_tile8(J.luma, J.stride, J.w, J.h, J.out, J.psize, J.sw, J.sh, (t % J.tiles_x) * K1_TW, (t / J.tiles_x) * K1_TH);
+    else
+        planes_tile(reinterpret_cast<const T*>(J.luma), J.stride, J.w, J.h, reinterpret_cast<T*>(J.out), J.psize, J.sw, J.sh,
+                    (t % J.tiles_x) * K1_TW, (t / J.tiles_x) * K1_TH, maxv);
 }
 
 // col_mv, enc/frame.rs:944-947, for every stream's new reference

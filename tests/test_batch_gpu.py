@@ -64,6 +64,12 @@ def test_batch_equals_single_stream_auto_mode(cuda_lib, bd):
             got_r = d_res[i][k].cpu().numpy().view(MBRESULT_DTYPE)
             assert np.array_equal(got_s, want[i][k][0]), f"stream {i} step {k}: decisions"
             assert np.array_equal(got_r, want[i][k][1]), f"stream {i} step {k}: results"
+    # the batched planes kernel built each stream's newest reference as a single stream builds it
+    for i, ((w, h, ns), f) in enumerate(zip(STREAMS, frames)):
+        one = InterStage(w, h, nslices=ns, lib=cuda_lib, bd=bd)
+        one.push_reference(f[1])
+        assert np.array_equal(stages[i].planes(0), one.planes(0)), f"stream {i}: planes"
+        one.close()
 
     # a frame step captured in a CUDA graph replays to the same results
     for i in range(n):
