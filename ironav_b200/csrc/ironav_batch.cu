@@ -59,8 +59,8 @@ __global__ void __launch_bounds__(K1_THREADS) planes_batch_kernel(const PlaneJob
     if constexpr (sizeof(T) == 1)
         planes_tile8(J.luma, J.stride, J.w, J.h, J.out, J.psize, J.sw, J.sh, (t % J.tiles_x) * K1_TW, (t / J.tiles_x) * K1_TH);
     else
-        planes_tile(reinterpret_cast<const T*>(J.luma), J.stride, J.w, J.h, reinterpret_cast<T*>(J.out), J.psize, J.sw, J.sh,
-                    (t % J.tiles_x) * K1_TW, (t / J.tiles_x) * K1_TH, maxv);
+        planes_tile16(reinterpret_cast<const uint16_t*>(J.luma), J.stride, J.w, J.h, reinterpret_cast<uint16_t*>(J.out), J.psize, J.sw,
+                      J.sh, (t % J.tiles_x) * K1_TW, (t / J.tiles_x) * K1_TH, maxv);
 }
 
 // col_mv, enc/frame.rs:944-947, for every stream's new reference
