@@ -419,7 +419,12 @@ def main():
         "e2e": e2e,
         "gpu_launches": 3 * args.steps,  # per step: half-sample planes (+ co-located vectors), edge padding, analysis
         "roofline": {"bound": "int32", "kernel": f"analyse_kernel<MODE_REPLAY, {'uint8_t' if bd == 8 else 'uint16_t'}>", "achieved": achieved, "peak": peak,
-                     "unit": "Tops/s", "frac": achieved / peak if peak else None, "traffic": None,
+                     "unit": "Tops/s", "frac": achieved / peak if peak else None,
+                     # DRAM bytes per launch (dram__bytes_read.sum + write.sum) of one ncu capture of this
+                     # workload at 8 bits (ncu --set full, one launch of a 6-picture ring): the source and the
+                     # reference's planes read once
+                     "traffic": 11637248 + 2304 if bd == 8 else None,
+                     "traffic_source": "one ncu capture of this kernel on this workload (8-bit)" if bd == 8 else None,
                      "ms_per_launch": k2_mean,
                      "note": "achieved = algorithmic ops (3 per SAD sample, 9 per SATD sample, counted by the "
                              "kernel in the reference's evaluation order) / event time; peak = measured 32-bit "
@@ -427,7 +432,11 @@ def main():
         "roofline_planes": {"bound": "hbm", "kernel": f"halfpel_planes_kernel<{'uint8_t' if bd == 8 else 'uint16_t'}>",
                             "achieved": planes_bytes / (planes_ms * 1e-3) / 1e9, "peak": hbm[0], "unit": "GB/s",
                             "frac": planes_bytes / (planes_ms * 1e-3) / 1e9 / hbm[0], "peak_source": hbm[1],
-                            "ms_per_launch": planes_ms, "traffic": None},
+                            "ms_per_launch": planes_ms,
+                            # one ncu capture at 8 bits: the luma read once; the 9.5 MB of planes written stay
+                            # in L2 (the analysis reads them from there)
+                            "traffic": 2670336 if bd == 8 else None,
+                            "traffic_source": "one ncu capture of this kernel on this workload (8-bit)" if bd == 8 else None},
         "clocks": clk,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
