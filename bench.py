@@ -13,7 +13,9 @@ the stage's own auto mode, outside the timed region), so all macroblocks are ind
 - ``e2e``: the same through the host-buffer C ABI calls (ironav_set_source, ironav_push_reference,
   ironav_analyse_picture_replay) from pinned host memory, copies included;
 - ``roofline``: the analysis kernel against the measured 32-bit integer issue rate; ``roofline_planes``:
-  the plane kernel against the measured HBM bandwidth;
+  the plane kernel against the measured HBM bandwidth (the 6.65 TB/s fallback when no measurement is
+  at hand, named in ``peak_source``); ``traffic``: each kernel's DRAM bytes per launch from one ncu
+  capture of the 8-bit workload;
 - ``cpu_baseline``: the C restatement of the reference's stage (oracle/) over all host cores on a
   bounded sample of the same workload, rank 0 only.
 - ``--impl reference``: the reference's algorithm on the host cores (the oracle port: the Rust
