@@ -72,6 +72,30 @@ def test_planes_rebuilt_in_a_reused_slot(oracle_lib, cuda_lib):
         assert np.array_equal(got, o.planes(0)), f"push {k}: planes differ from the oracle's"
 
 
+@pytest.mark.parametrize("bd", [8, 10])
+def test_planes_from_a_misaligned_device_picture(oracle_lib, cuda_lib, bd):
+    """A reference handed over in device memory at an unaligned address, rows an odd number of samples
+    apart, takes the planes kernel's sample-by-sample staging on every tile: its planes equal the
+    oracle's."""
+    import torch
+
+    w, h = 352, 288
+    maxv = (1 << bd) - 1
+    dt = np.uint8 if bd == 8 else np.uint16
+    luma = np.random.default_rng(17 + bd).integers(0, maxv + 1, size=(h, w)).astype(dt)
+    stride, off = w + 3, 1
+    buf = np.zeros(h * stride + 8, dt)
+    buf[off:off + h * stride].reshape(h, stride)[:, :w] = luma
+    tbuf = torch.from_numpy(buf.view(np.int16) if bd == 10 else buf).cuda()
+    c = InterStage(w, h, lib=cuda_lib, bd=bd)
+    c.set_stream(torch.cuda.current_stream().cuda_stream)
+    c.push_reference_device(tbuf.data_ptr() + off * buf.itemsize, stride, w, h, None)
+    c.sync()
+    o = InterStage(w, h, lib=oracle_lib, bd=bd)
+    o.push_reference(luma)
+    assert np.array_equal(c.planes(0), o.planes(0))
+
+
 def test_planes_of_a_macroblock_aligned_reconstruction(oracle_lib, cuda_lib):
     """A reconstruction is 16*mb_w x 16*mb_h and is used as is (no edge repetition inside it)."""
     w, h = 40, 20  # mb 3 x 2
