@@ -240,6 +240,7 @@ extern "C" int ironav_batch_create(ironav_batch** out, ironav_ctx* const* ctxs, 
     if ((e = cudaMemcpy(b->d_order, order.data(), sizeof(uint32_t) * order.size(), cudaMemcpyHostToDevice)) != cudaSuccess) return fail(e);
     if ((e = cudaMalloc(&b->d_flags, sizeof(unsigned) * b->total_mbs)) != cudaSuccess) return fail(e);
     if ((e = cudaMalloc(&b->d_counters, sizeof(unsigned) * 2)) != cudaSuccess) return fail(e);
+    if ((e = cudaMemset(b->d_counters, 0, sizeof(unsigned) * 2)) != cudaSuccess) return fail(e);  // read by a sync before any step
     if ((e = cudaMalloc(&b->d_pjobs, sizeof(PlaneJob) * n)) != cudaSuccess) return fail(e);
     if ((e = cudaMalloc(&b->d_sjobs, sizeof(SrcJob) * n)) != cudaSuccess) return fail(e);
     if ((e = cudaMalloc(&b->d_table, sizeof(AnalyseParams) * n)) != cudaSuccess) return fail(e);

@@ -357,6 +357,8 @@ int ironav_ctx_create(ironav_ctx** out, int width, int height, int bd, int max_r
     if ((e = cudaMalloc(&c->d_order, sizeof(int) * c->nmb)) != cudaSuccess) return fail(e);
     if ((e = cudaMalloc(&c->d_flags, sizeof(unsigned) * c->nmb)) != cudaSuccess) return fail(e);
     if ((e = cudaMalloc(&c->d_counters, sizeof(unsigned) * 2)) != cudaSuccess) return fail(e);
+    // the ticket and the error word: a sync before any launch must read no error
+    if ((e = cudaMemset(c->d_counters, 0, sizeof(unsigned) * 2)) != cudaSuccess) return fail(e);
     if ((e = cudaMalloc(&c->d_states, sizeof(ironav_mbstate) * c->nmb)) != cudaSuccess) return fail(e);
     if ((e = cudaMalloc(&c->d_col_stage, sizeof(ironav_mbstate) * c->nmb)) != cudaSuccess) return fail(e);
     if ((e = cudaMalloc(&c->d_results, sizeof(ironav_mbresult) * c->nmb)) != cudaSuccess) return fail(e);
