@@ -413,6 +413,17 @@ int ironav_ctx_set_stream(ironav_ctx* c, void* s) {
 // The padded source from a picture whose rows are `stride` samples apart (kind: the copy's direction).
 static int load_source(ironav_ctx* c, const void* y, int stride, cudaMemcpyKind kind) {
     const int B = sample_bytes(c);
+    if (kind == cudaMemcpyDeviceToDevice) {
+        // copy and padding in one pass
+        const unsigned grid = (unsigned)(((long long)c->pw * c->ph / (16 / B) + 255) / 256);
+        if (B == 2)
+            copy_pad_kernel<uint16_t><<<grid, 256, 0, c->stream>>>(reinterpret_cast<uint16_t*>(c->d_src), c->pw, c->ph,
+                                                                   static_cast<const uint16_t*>(y), stride, c->width, c->height);
+        else
+            copy_pad_kernel<uint8_t><<<grid, 256, 0, c->stream>>>(c->d_src, c->pw, c->ph, static_cast<const uint8_t*>(y), stride, c->width,
+                                                                  c->height);
+        return cuda_status(cudaGetLastError());
+    }
     CK(cudaMemcpy2DAsync(c->d_src, (size_t)c->pw * B, y, (size_t)stride * B, (size_t)c->width * B, c->height, kind, c->stream));
     if (c->width != c->pw || c->height != c->ph) {
         const unsigned grid = (unsigned)((pad_edges_count(c->width, c->height, c->pw, c->ph) + 255) / 256);

@@ -286,4 +286,21 @@ static __global__ void pad_edges_kernel(T* __restrict__ p, int w, int h, int pw,
     p[(size_t)y * pw + x] = p[(size_t)min(y, h - 1) * pw + min(x, w - 1)];
 }
 
+// The padded source from a picture in device memory in one pass: sample (x, y) of the pw x ph buffer is
+// picture sample (min(x, w - 1), min(y, h - 1)) (H264Encoder::source, enc/mod.rs:502-519). A thread writes
+// 16 bytes; pw is a multiple of 16, so a thread's samples lie in one row.
+template <class T>
+static __global__ void copy_pad_kernel(T* __restrict__ dst, int pw, int ph, const T* __restrict__ src, int stride, int w, int h) {
+    constexpr int PER = 16 / (int)sizeof(T);
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (long long)pw * ph / PER) return;
+    const long long e = i * PER;
+    const int y = (int)(e / pw), x0 = (int)(e % pw);
+    const T* row = src + (size_t)min(y, h - 1) * stride;
+    alignas(16) T v[PER];
+#pragma unroll
+    for (int k = 0; k < PER; k++) v[k] = row[min(x0 + k, w - 1)];
+    *reinterpret_cast<uint4*>(dst + e) = *reinterpret_cast<const uint4*>(v);
+}
+
 }  // namespace ironav

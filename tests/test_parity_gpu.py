@@ -243,6 +243,38 @@ def test_device_forms_match_host_forms(cuda_lib):
     assert_same(dr.cpu().numpy().view(MBRESULT_DTYPE), rep, "device replay results")
 
 
+@pytest.mark.parametrize("bd", [8, 10])
+def test_device_source_with_odd_stride_and_size(cuda_lib, bd):
+    """A source handed over in device memory, rows an odd number of samples apart and a size that is not a
+    whole number of macroblocks, is padded as the host form pads it: the same decisions and results."""
+    import torch
+
+    w, h = 200, 120
+    seq = Sequence.config("cif", 2, size=(w, h))
+    f0, f1 = (seq.frame10(t) if bd == 10 else seq.frame(t) for t in (0, 1))
+    qp = 26 + 6 * (bd - 8)
+    st = InterStage(w, h, nslices=2, lib=cuda_lib, bd=bd)
+    st.push_reference(f0)
+    st.set_source(f1)
+    st.begin_p_picture(qp)
+    states, res = st.analyse_auto()
+    d = InterStage(w, h, nslices=2, lib=cuda_lib, bd=bd)
+    d.set_stream(torch.cuda.current_stream().cuda_stream)
+    d.push_reference(f0)
+    stride = w + 5
+    buf = np.zeros((h, stride), f1.dtype)
+    buf[:, :w] = f1
+    t1 = torch.from_numpy(buf.view(np.int16) if bd == 10 else buf).cuda()
+    d.set_source_device(t1.data_ptr(), stride)
+    d.begin_p_picture(qp)
+    ds = torch.zeros(d.nmb * 72, dtype=torch.uint8, device="cuda")
+    dr = torch.zeros(d.nmb * 104, dtype=torch.uint8, device="cuda")
+    d.analyse_auto_device(ds.data_ptr(), dr.data_ptr())
+    d.sync()
+    assert_same(ds.cpu().numpy().view(MBSTATE_DTYPE), states, "device-source decisions")
+    assert_same(dr.cpu().numpy().view(MBRESULT_DTYPE), res, "device-source results")
+
+
 def test_wavefront_wait_times_out_and_the_context_recovers(oracle_lib, cuda_lib):
     """A macroblock whose decision is never published (the test withholds it) makes the waits behind it
     give up after a bounded number of polls; the call reports a timeout and the next call works."""
