@@ -419,7 +419,7 @@ def main():
         "data": data_desc(bd),
         "config": config_dict(bd),
         "e2e": e2e,
-        "gpu_launches": 3 * args.steps,  # per step: half-sample planes (+ co-located vectors), edge padding, analysis
+        "gpu_launches": 3 * args.steps,  # per step: half-sample planes (+ co-located vectors), the source copied with its padding, analysis
         "roofline": {"bound": "int32", "kernel": f"analyse_kernel<MODE_REPLAY, {'uint8_t' if bd == 8 else 'uint16_t'}>", "achieved": achieved, "peak": peak,
                      "unit": "Tops/s", "frac": achieved / peak if peak else None,
                      # DRAM bytes per launch (dram__bytes_read.sum + write.sum) of one ncu capture of this
