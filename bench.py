@@ -147,6 +147,34 @@ def max_over_ranks(value: float, world: int, device) -> float:
     return float(t.item())
 
 
+def sum_over_ranks(value: float, world: int, device) -> float:
+    """The sum of every rank's value (the macroblocks all ranks processed); one all-reduce when there are
+    several ranks."""
+    import torch
+
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def split_streams(streams, rank: int, world: int):
+    """This rank's share of the batched configuration's streams: every stream goes to exactly one rank,
+    the largest first to the rank with the fewest macroblocks so far (ties to the lower rank), so the
+    ranks' shares of macroblocks stay close and the slowest rank's time, which the job's time is, is not
+    one rank's accident of resolutions. Deterministic: every rank computes the same split."""
+    load = [0] * world
+    owner = [0] * len(streams)
+    order = sorted(range(len(streams)), key=lambda i: (-((streams[i][0] + 15) // 16) * ((streams[i][1] + 15) // 16), i))
+    for i in order:
+        r = min(range(world), key=lambda k: (load[k], k))
+        owner[i] = r
+        load[r] += ((streams[i][0] + 15) // 16) * ((streams[i][1] + 15) // 16)
+    return [s for i, s in enumerate(streams) if owner[i] == rank]
+
+
 def make_frames(rank: int, n: int, bd: int = 8):
     """The 1080p sequence of one rank: each replica analyses its own seeded sequence (weak scaling)."""
     from ironav_b200.synth import CONFIGS, Sequence
@@ -464,7 +492,7 @@ def run_batched(args, rank, world):
 
     lib = cuda_library()
     dev = torch.device("cuda", torch.cuda.current_device())
-    mine = batch_streams(args.streams)[rank::world]
+    mine = split_streams(batch_streams(args.streams), rank, world)
     stream = torch.cuda.Stream()
     stages, frames = [], []
     for (w, h, ns, seed) in mine:
@@ -544,8 +572,9 @@ def run_batched(args, rank, world):
     torch.cuda.synchronize()
     batch.sync()
     ms_g = e0.elapsed_time(e1)
-    total = nmb * (world if world > 1 else 1)
-    mbs = lambda ms: nmb * args.steps / (ms * 1e-3) * (world if world > 1 else 1)
+    # the job's macroblocks: every rank's own share summed (the ranks' shares differ in size)
+    total = sum_over_ranks(nmb, world, dev)
+    mbs = lambda ms: total * args.steps / (ms * 1e-3)
     line = {
         "metric": f"batched inter-analysis MB/s: {args.streams} mixed-resolution streams, auto mode, one launch per stage and step",
         "value": mbs(ms_b), "unit": "MB/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -556,7 +585,7 @@ def run_batched(args, rank, world):
         "plain_loop": {"value": mbs(ms_p), "ms_per_step": ms_p / args.steps,
                        "note": "each stream's own launches (planes, source, auto-mode analysis), one after another"},
         "graph": {"value": nmb * args.steps / (ms_g * 1e-3), "ms_per_step": ms_g / args.steps,
-                  "note": "the batched step captured once in a CUDA graph and replayed"},
+                  "note": "the batched step captured once in a CUDA graph and replayed (rank 0's streams alone)"},
         "speedup_vs_plain_loop": ms_p / ms_b,
         "clocks": clk,
     }
@@ -747,7 +776,7 @@ def run_decide_batched(args, rank, world):
 
     lib = cuda_library()
     dev = torch.device("cuda", torch.cuda.current_device())
-    mine = batch_streams(args.streams)[rank::world]
+    mine = split_streams(batch_streams(args.streams), rank, world)
     stream = torch.cuda.Stream()
     stages, bufs, pin_src, d_src, seqs = [], [], [], [], []
     for (w, h, ns, seed) in mine:
@@ -805,13 +834,17 @@ def run_decide_batched(args, rank, world):
             batched()
             batch.sync()
         torch.cuda.synchronize()
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         per = timed(batched, args.steps)
         e1.record(stream)
         batch.sync()
         clk = clocks.stop()
-        ms = e0.elapsed_time(e1)
+        ms = max_over_ranks(e0.elapsed_time(e1), world, dev)
         plain_ms = float(np.median(timed(plain, max(2, min(args.steps, 5)))))
         # end to end: every stream's source luma from pinned host memory, the launch, and the states, codes
         # and reconstructions back to pinned host memory, each step
@@ -830,11 +863,13 @@ def run_decide_batched(args, rank, world):
         for _ in range(2):
             e2e_step()
         batch.sync()
+        if world > 1:
+            dist.barrier()
         t0 = time.perf_counter()
         for _ in range(args.steps):
             e2e_step()
         batch.sync()
-        el = time.perf_counter() - t0
+        el = max_over_ranks(time.perf_counter() - t0, world, dev)
     # the whole P picture of every stream: batched decide, each stream's filter records, batched deblocking
     from ironav_b200.inter import DBK_MB_DTYPE
     from ironav_b200.synth import dbk_encoder_slices
@@ -856,11 +891,13 @@ def run_decide_batched(args, rank, world):
         batch.sync()
         pipe_ms = float(np.median(timed(pipeline, max(2, min(args.steps, 5)))))
         batch.sync()
-    value = world * nmb * args.steps / (ms * 1e-3)
+    # the job's macroblocks: every rank's own share summed (the ranks' shares differ in size)
+    total = sum_over_ranks(nmb, world, dev)
+    value = total * args.steps / (ms * 1e-3)
     line = {
         "metric": "P-picture macroblock decision + coding MB/s, many streams in one launch (CAVLC code_mb)", "value": value,
         "unit": "MB/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "u8",
         "data": "synthetic: per-stream seeded value noise, pan, 8 moving rectangles, sigma 3; chroma from the 2x2 luma means",
         "config": {"workload": f"{args.streams} streams ({n} on rank 0) of 640x360..1920x1080, {nmb} macroblocks per step on rank 0, QP "
                                f"{QP}, one reference each, decide mode, ironav_batch_decide",
@@ -870,7 +907,7 @@ def run_decide_batched(args, rank, world):
                                             "ironav_batch_deblock: every stream's P picture decided, coded and deblocked",
                    "l2": "inputs of all streams (planes, chroma, codes, reconstructions) exceed L2"},
         "gpu_launches": args.steps,
-        "e2e": {"value": world * nmb * args.steps / el, "unit": "MB/s",
+        "e2e": {"value": total * args.steps / el, "unit": "MB/s",
                 "h2d_bytes_per_step": sum(int(p.numel()) for p in pin_src),
                 "d2h_bytes_per_step": sum(sum(int(t.numel()) for t in b) for b in bufs), "ms_per_step": 1e3 * el / args.steps,
                 "note": "each stream's source luma from pinned host memory (its chroma stays resident) + the launch + states, "

@@ -445,8 +445,8 @@ int ironav_batch_deblock(ironav_batch* batch, void* const* d_y, const int* y_str
  * ironav_ctx. It runs the auto-mode analysis of one P picture against one reference picture, with every
  * input and output in the caller's device memory, and allocates nothing (no cudaMalloc, no library
  * allocation): its scratch (progress flags, counters, slice bands, co-located vectors) is one fixed
- * array of about 444 KB in the library's device memory, which every GPU that loads the library keeps
- * until the process exits.
+ * array of 446,720 bytes (436 KiB) in the library's device memory, which every GPU that loads the
+ * library keeps until the process exits.
  *   d_src      the source, padded to whole macroblocks (16*mb_w x 16*mb_h, edges repeated as
  *              ironav_set_source does), 16-byte aligned, rows src_stride bytes apart (a multiple of 16)
  *   d_ref      the reference luma, ref_w x ref_h = width x height or 16*mb_w x 16*mb_h, rows ref_stride apart
@@ -458,7 +458,10 @@ int ironav_batch_deblock(ironav_batch* batch, void* const* d_y, const int* y_str
  * returns when the work is done (IRONAV_TIMEOUT if a wavefront wait gave up). Every call uses the same
  * scratch array and clears what must start at zero; calls that overlap on the GPU (other streams or
  * host threads) race on it, so make them one after another. The first call on a device looks up the
- * array's address with that device current: make it before any stream capture. */
+ * array's address with that device current: make it before any stream capture (a lookup that fails is
+ * tried again by the next call; a device reset, cudaDeviceReset, is not supported). qp_prime is only
+ * checked (0..63): the analysis reads lambda and skip_thresh, which must come from ironav_lambda and
+ * ironav_skip_threshold for that QP'. */
 #define IRONAV_NOALLOC_MAX_MBS 36864
 int ironav_analyse_auto_noalloc(const uint8_t* d_src, int src_stride, const uint8_t* d_ref, int ref_stride,
                                 int ref_w, int ref_h, const ironav_mbstate* d_col, int width, int height,

@@ -12,17 +12,22 @@
 // Limits and rules:
 //   - at most IRONAV_NOALLOC_MAX_MBS macroblocks (36864: 4096x2304, which covers 4K UHD) and one
 //     reference picture;
-//   - the scratch array is a file-scope __device__ array (about 444 KB), held by every GPU that loads
-//     the library until the process exits;
+//   - the scratch array is a file-scope __device__ array of 446,720 bytes (436 KiB), held by every GPU
+//     that loads the library until the process exits;
 //   - every call shares it and leaves its contents behind; each call clears what must start at zero.
 //     Calls whose work overlaps on the GPU (two streams, or two host threads) race on it: run them one
 //     after another;
 //   - the first call on a device looks up the array's device address (cudaGetSymbolAddress) with that
-//     device current; make that first call before any stream capture;
+//     device current; make that first call before any stream capture. A lookup that fails is not kept:
+//     the next call on that device tries again. A device reset (cudaDeviceReset) is not supported: the
+//     address kept from before it would name memory of a context that no longer exists;
+//   - qp_prime is checked (0..63) but not used: the analysis reads only lambda and skip_thresh, which
+//     the caller takes from ironav_lambda and ironav_skip_threshold for that QP';
 //   - the call is synchronous: it returns when the analysis is done, so it can report a wavefront wait
 //     that gave up (IRONAV_TIMEOUT).
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstring>
 #include <mutex>
 
@@ -47,13 +52,19 @@ constexpr int SCR_WORDS = SCR_COL + 2 * NOALLOC_MAX_MBS;
 
 static __device__ __align__(256) uint32_t g_noalloc_scratch[SCR_WORDS];
 
+// Per device, filled once the lookups succeed (ready); a failed lookup leaves it empty for a retry.
 struct DeviceSetup {
-    std::once_flag once;
-    cudaError_t status = cudaSuccess;
+    std::mutex mu;
+    std::atomic<bool> ready{false};
     uint32_t* scratch = nullptr;  // device address of g_noalloc_scratch on this device
     int blocks = 0;
 };
 DeviceSetup g_setup[MAX_DEVICES];
+
+// Test hooks (ironav_debug_noalloc_wait, not in the public header): a macroblock whose decision is never
+// published, and the polls a wavefront wait makes before it gives up.
+std::atomic<int> g_withhold{-1};
+std::atomic<unsigned> g_wait_limit{1u << 22};
 
 // Clears the flags and counters, writes the slice bands (band i = [i*mb_h/n, (i+1)*mb_h/n), enc/mod.rs:603)
 // and the co-located vectors of the reference picture (col_mv, enc/frame.rs:944-947).
@@ -113,8 +124,26 @@ __global__ void __launch_bounds__(K2_WARPS * 32, K2_MIN_BLOCKS) analyse_noalloc_
         analyse(P, S, true);
         __threadfence();
         __syncwarp();
-        if (lane == 0) st_release(&P.flags[mb], P.epoch);
+        if (lane == 0 && mb != P.withhold) st_release(&P.flags[mb], P.epoch);
     }
+}
+
+// The scratch array's device address and the persistent grid's size on the current device `dev`.
+cudaError_t device_setup(int dev, DeviceSetup& S) {
+    std::lock_guard<std::mutex> lock(S.mu);
+    if (S.ready.load(std::memory_order_acquire)) return cudaSuccess;
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return e;
+    int nsm = 0, per_sm = 0;
+    e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, analyse_noalloc_kernel, K2_WARPS * 32, 0);
+    if (e != cudaSuccess) return e;
+    S.scratch = static_cast<uint32_t*>(p);
+    S.blocks = (per_sm > 0 ? per_sm : 1) * nsm;
+    S.ready.store(true, std::memory_order_release);
+    return cudaSuccess;
 }
 
 int map_status(cudaError_t e) {
@@ -149,18 +178,10 @@ extern "C" int ironav_analyse_auto_noalloc(const uint8_t* d_src, int src_stride,
     if (dev < 0 || dev >= MAX_DEVICES) return IRONAV_INTERNAL;
     // once per device, with that device current: the scratch array's device address
     DeviceSetup& S = g_setup[dev];
-    std::call_once(S.once, [&] {
-        void* p = nullptr;
-        S.status = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (S.status != cudaSuccess) return;
-        S.scratch = static_cast<uint32_t*>(p);
-        int nsm = 0, per_sm = 0;
-        S.status = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-        if (S.status != cudaSuccess) return;
-        S.status = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, analyse_noalloc_kernel, K2_WARPS * 32, 0);
-        S.blocks = (per_sm > 0 ? per_sm : 1) * nsm;
-    });
-    if (S.status != cudaSuccess || !S.scratch) return map_status(S.status);
+    if (!S.ready.load(std::memory_order_acquire)) {
+        e = device_setup(dev, S);
+        if (e != cudaSuccess) return map_status(e);
+    }
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     uint32_t* scr = S.scratch;
 
@@ -195,8 +216,8 @@ extern "C" int ironav_analyse_auto_noalloc(const uint8_t* d_src, int src_stride,
     p.epoch = 1;  // the flags were cleared to 0 above
     p.err = scr + SCR_ERR;
     p.nmb = nmb;
-    p.withhold = -1;
-    p.wait_limit = 1u << 22;
+    p.withhold = g_withhold.load();
+    p.wait_limit = g_wait_limit.load();
     const int max_rows = (mb_h + nslices - 1) / nslices;
     analyse_noalloc_kernel<<<S.blocks, K2_WARPS * 32, 0, s>>>(p, nslices, max_rows);
     e = cudaGetLastError();
@@ -207,4 +228,13 @@ extern "C" int ironav_analyse_auto_noalloc(const uint8_t* d_src, int src_stride,
     if (e != cudaSuccess) return map_status(e);
     if (err & 1u) return IRONAV_TIMEOUT;
     return err ? IRONAV_INTERNAL : IRONAV_OK;
+}
+
+// Test hook (not in the public header): withhold = a macroblock whose decision the next calls never
+// publish (-1: none), polls = how often a wavefront wait polls before it gives up (0: the default).
+extern "C" int ironav_debug_noalloc_wait(int withhold, unsigned polls) {
+    if (withhold < -1 || withhold >= NOALLOC_MAX_MBS) return IRONAV_INVALID_ARGUMENT;
+    g_withhold.store(withhold);
+    g_wait_limit.store(polls ? polls : (1u << 22));
+    return IRONAV_OK;
 }

@@ -217,6 +217,8 @@ def _declare(lib: ctypes.CDLL) -> ctypes.CDLL:
     for name in ("ironav_debug_withhold", "ironav_debug_wait_limit"):
         if hasattr(lib, name):
             getattr(lib, name).argtypes = [_VP, ctypes.c_int if name.endswith("withhold") else ctypes.c_uint]
+    if hasattr(lib, "ironav_debug_noalloc_wait"):
+        lib.ironav_debug_noalloc_wait.argtypes = [_I, ctypes.c_uint]
     return lib
 
 

@@ -1,6 +1,6 @@
 """Extracts the deblocking filter's tables from the reference into tests/golden/deblock_tables.json (run
-from the repository root with the reference checked out at /root/reference:
-`python -m tests.golden.make_deblock_tables`).
+from the repository root with the root of a checkout of the reference as the argument:
+`python -m tests.golden.make_deblock_tables <reference-root>`).
 
 The tables are the standard's (ITU-T H.264 Tables 8-15 to 8-17) as the reference holds them: ALPHA, BETA
 and TC0 of crates/ironav-codec/src/h264/tables.rs (indexed by indexA / indexB, and indexA x bS), and
@@ -13,9 +13,11 @@ import ast
 import json
 import os
 import re
+import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-SRC = "/root/reference/crates/ironav-codec/src/h264"
+# the H.264 module within the reference's tree
+H264 = os.path.join("crates", "ironav-codec", "src", "h264")
 
 
 def _const(text: str, name: str):
@@ -25,9 +27,10 @@ def _const(text: str, name: str):
     return ast.literal_eval(m.group(1))
 
 
-def main() -> None:
-    tables = open(os.path.join(SRC, "tables.rs")).read()
-    mb = open(os.path.join(SRC, "mb.rs")).read()
+def main(reference_root: str) -> None:
+    src = os.path.join(reference_root, H264)
+    tables = open(os.path.join(src, "tables.rs")).read()
+    mb = open(os.path.join(src, "mb.rs")).read()
     out = {
         "alpha": _const(tables, "ALPHA"),
         "beta": _const(tables, "BETA"),
@@ -41,4 +44,6 @@ def main() -> None:
 
 
 if __name__ == "__main__":
-    main()
+    if len(sys.argv) != 2:
+        sys.exit("usage: python -m tests.golden.make_deblock_tables <reference-root>")
+    main(sys.argv[1])

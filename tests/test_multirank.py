@@ -77,3 +77,47 @@ def test_reference_arm_under_torchrun_prints_one_line():
     assert len(lines) == 1, r.stdout[-2000:]
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
+
+
+def _split_main(rank: int, world: int, port: int, q) -> None:
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world),
+                      LOCAL_RANK=str(rank))
+    sys.path.insert(0, ROOT)
+    from datetime import timedelta
+
+    import torch.distributed as dist
+
+    import bench
+    from ironav_b200.synth import batch_streams
+
+    dist.init_process_group("gloo", timeout=timedelta(seconds=60))
+    mine = bench.split_streams(batch_streams(64), rank, world)
+    nmb = sum(((w + 15) // 16) * ((h + 15) // 16) for (w, h, _, _) in mine)
+    total = bench.sum_over_ranks(nmb, world, torch.device("cpu"))
+    q.put((rank, [s[3] for s in mine], nmb, total))
+    dist.destroy_process_group()
+
+
+def test_batched_streams_split_and_summed_on_two_gloo_ranks():
+    """The batched workloads' only multi-GPU form: the 64 streams split across ranks with no collective on
+    the data path. Every stream goes to exactly one rank, the shares of macroblocks are balanced, and the
+    job's macroblock count is the sum over ranks (not rank 0's share times the rank count)."""
+    from ironav_b200.synth import batch_streams
+
+    ctx = mp.get_context("spawn")
+    q = ctx.SimpleQueue()
+    port = _free_port()
+    procs = [ctx.Process(target=_split_main, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(120)
+    assert all(p.exitcode == 0 for p in procs), [p.exitcode for p in procs]
+    got = sorted(q.get() for _ in range(2))
+    streams = batch_streams(64)
+    all_mb = sum(((w + 15) // 16) * ((h + 15) // 16) for (w, h, _, _) in streams)
+    seeds = sorted(got[0][1] + got[1][1])
+    assert seeds == sorted(s[3] for s in streams)  # each stream on exactly one rank
+    assert got[0][3] == got[1][3] == all_mb        # the job's count is the sum over ranks
+    assert got[0][2] + got[1][2] == all_mb
+    assert abs(got[0][2] - got[1][2]) <= 8160      # balanced within one 1080p stream
