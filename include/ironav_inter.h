@@ -319,6 +319,60 @@ int ironav_decide_p_picture(ironav_ctx* ctx, ironav_mbstate* states, ironav_mbco
 int ironav_decide_p_picture_device(ironav_ctx* ctx, ironav_mbstate* d_states, ironav_mbcode* d_codes, void* d_rec_y, int y_stride,
                                    void* d_rec_cb, void* d_rec_cr, int c_stride);
 
+/* ---- intra (IDR) pictures in decide mode ------------------------------------------------------------ */
+
+/* Parameters of an IDR picture (FrameCoder::new without a reference, enc/frame.rs:381-412; the encoder
+ * codes IDR pictures at its QP - 3, QP_OFFSET enc/mod.rs:33): qp_prime = QP'Y, lambda from ironav_lambda,
+ * fast = H264Encoder::realtime (flat macroblocks left to Intra16x16, enc/frame.rs:762-765). Replaces the
+ * P picture's parameters until the next ironav_begin_p_picture. */
+int ironav_begin_i_picture(ironav_ctx* ctx, int qp_prime, int lambda, int fast);
+/* code_mb for every macroblock of the IDR picture (enc/frame.rs:752-790 with no reference: best_i16,
+ * the Intra4x4 trial, code_i16 or the trial's blocks, code_intra_chroma), in each slice band's raster
+ * order, each against the reconstruction of those before it; outputs as ironav_decide_p_picture's
+ * (every state intra: inter 0, refs -1). Needs the source's luma and chroma; no reference is read. */
+int ironav_decide_i_picture(ironav_ctx* ctx, ironav_mbstate* states, ironav_mbcode* codes, void* rec_y, int y_stride, void* rec_cb,
+                            void* rec_cr, int c_stride);
+int ironav_decide_i_picture_device(ironav_ctx* ctx, ironav_mbstate* d_states, ironav_mbcode* d_codes, void* d_rec_y, int y_stride,
+                                   void* d_rec_cb, void* d_rec_cr, int c_stride);
+/* ironav_set_source_chroma and ironav_push_reference_chroma on device pointers (queued on the context's
+ * stream; the source's chroma is width/2 x height/2 samples, rows `stride` apart). */
+int ironav_set_source_chroma_device(ironav_ctx* ctx, const void* d_cb, const void* d_cr, int stride);
+int ironav_push_reference_chroma_device(ironav_ctx* ctx, const void* d_cb, const void* d_cr, int stride, int w, int h);
+
+/* ---- the bitstream (CAVLC, Annex B) ------------------------------------------------------------------ */
+
+/* What the sequence and picture parameter sets say (H264Encoder::sps / pps, enc/mod.rs:296-400, for the
+ * CAVLC encoder: Constrained Baseline at 8 bits, High 10 with CAVLC at 10 bits; no B pictures, picture
+ * order type 2, one slice group, no weighted prediction, deblocking not signalled). */
+typedef struct ironav_stream_params {
+    int32_t width, height;       /* the picture size; the SPS crops the macroblock-aligned size to it */
+    int32_t bd;                  /* 8 or 10 */
+    int32_t fps_num, fps_den;    /* frame rate: the level (Table A-1, enc/mod.rs:154-157) and the VUI timing;
+                                    0, 0: 25 fps for the level, no timing */
+    int32_t refs;                /* max_num_ref_frames: reference pictures the stream keeps (1..16) */
+} ironav_stream_params;
+
+/* The SPS and PPS NAL units (Annex B: 4-byte start codes, emulation prevention, put_nal enc/bitw.rs:91-103)
+ * that the encoder puts ahead of every IDR picture (enc/mod.rs:636-640). Writes *len bytes to out;
+ * IRONAV_INVALID_ARGUMENT when cap is too small (*len then says how many are needed). */
+int ironav_write_parameter_sets(const ironav_stream_params* p, uint8_t* out, size_t cap, size_t* len);
+
+/* The slice NAL units of the current picture (one per slice band, enc/mod.rs:641-643), from its codes
+ * (ironav_decide_i_picture / ironav_decide_p_picture outputs, mb_w*mb_h): the slice header (enc/mod.rs:566-600),
+ * each macroblock's CAVLC syntax (write_mb, enc/frame.rs:1922-2016: mb_skip_run, mb_type, prediction modes,
+ * sub_mb_type, ref_idx, mvd, coded_block_pattern, mb_qp_delta, residual blocks by enc/cavlc.rs:47-122) and
+ * the slice's trailing bits (enc/frame.rs:480-486). idr: the picture is the IDR picture (slice type I, NAL
+ * type 5, idr_pic_id) set up by ironav_begin_i_picture, else a P picture set up by ironav_begin_p_picture
+ * (its active references give num_ref_idx_active and ref_idx's range); frame_num and idr_pic_id as the
+ * encoder counts them (enc/mod.rs:541-545,667-668). Writes *len bytes of Annex B to out; IRONAV_INVALID_ARGUMENT
+ * when cap is too small (*len then says how many are needed). */
+int ironav_write_slices(ironav_ctx* ctx, int idr, int frame_num, int idr_pic_id, const ironav_mbcode* codes, uint8_t* out,
+                        size_t cap, size_t* len);
+/* The same from codes in device memory (4-byte aligned); out is a host buffer. Returns when the bytes
+ * are in out. */
+int ironav_write_slices_device(ironav_ctx* ctx, int idr, int frame_num, int idr_pic_id, const ironav_mbcode* d_codes,
+                               uint8_t* out, size_t cap, size_t* len);
+
 /* ---- deblocking of the reconstruction ------------------------------------------------------------ */
 
 /* The in-loop deblocking filter (h264/deblock.rs:410-720, ITU-T H.264 8.7) of a reconstructed picture,

@@ -60,7 +60,7 @@ def build_cuda(force: bool = False, verbose: bool = False) -> str:
     deps = _sources((".cu", ".cuh"))
     if force or _stale(CUDA_LIB, deps):
         os.makedirs(LIB, exist_ok=True)
-        units = ["ironav_inter.cu", "ironav_batch.cu", "ironav_noalloc.cu"]
+        units = ["ironav_inter.cu", "ironav_batch.cu", "ironav_noalloc.cu", "ironav_stream.cu"]
         cmd = [_nvcc(), *NVCC_FLAGS, *[os.path.join(CSRC, u) for u in units], "-o", CUDA_LIB]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")

@@ -31,6 +31,7 @@ struct ironav_ctx {
     // picture parameters
     int qpp = 0, lambda = 0, skip_thresh = 0, nact = 0, fast = 0, sub8 = 0;
     bool have_params = false;
+    bool intra_pic = false;  // the parameters are an IDR picture's (ironav_begin_i_picture): decide mode only
     int withhold = -1;
     unsigned wait_limit = 1u << 22;
     // in-loop mode: host memory mapped into the device (allocated on first use)
@@ -74,6 +75,17 @@ struct ironav_ctx {
     // decide mode: its persistent grid (from the kernel's occupancy, on first use) and host-form codes
     int k7_blocks = 0;
     ironav_mbcode* d_mbcodes = nullptr;
+    // the CAVLC writer (allocated on first use): slice band boundaries (nslices + 1 rows), per macroblock
+    // its bits, offset and skip run, per slice its bytes, the error word; each slice's first macroblock and
+    // each row's slice; the slices' RBSP regions; pinned host staging for the bytes that come back
+    int band_rows[1025] = {};
+    uint32_t* d_cavlc = nullptr;
+    int* d_slice_tab = nullptr;
+    uint32_t* d_rbsp = nullptr;
+    unsigned long long rbsp_region_words = 0;
+    uint32_t* h_cavlc = nullptr;
+    uint8_t* h_rbsp = nullptr;
+    size_t h_rbsp_cap = 0;
 };
 
 

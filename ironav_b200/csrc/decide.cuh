@@ -21,6 +21,8 @@ struct DecideParams {
     CodeParams C;          // C.A: the analysis' parameters and the wavefront's (order, ticket, flags, epoch, err)
     ironav_mbcode* codes;  // every macroblock's code (neighbours' Intra4x4 modes are read back from here)
     int fast_t, fast_tc;   // the fast mode's P_Skip bounds on the luma and chroma SADs
+    int intra;             // an IDR picture: no reference, every macroblock intra (code_mb of an I slice)
+    int flat_t;            // the fast mode's bound on a flat macroblock's Intra16x16 cost (enc/frame.rs:763)
 };
 
 constexpr int K7_WARPS = 4;
@@ -682,8 +684,10 @@ __device__ void pair_helper(const DecideParams& P, DecideSmem<T>& S, PairSync& X
     }
 }
 
-// code_mb for one P macroblock without CABAC, enc/frame.rs:715-790. X: the warp pair's meeting words, when
-// the macroblock's intra side runs on the pair's second warp (PAIR).
+// code_mb for one macroblock without CABAC, enc/frame.rs:715-790: of a P picture, or of an IDR picture
+// (P.intra: no P_Skip tests and no best_inter; the Intra4x4 trial always runs, but for flat macroblocks in
+// live coding, 762-765). X: the warp pair's meeting words, when the macroblock's intra side runs on the
+// pair's second warp (PAIR).
 template <class T, bool PAIR = false>
 __device__ void decide_mb(const DecideParams& P, DecideSmem<T>& S, const unsigned* i4tab, int mb, int mbx, int mby, PairSync* X = nullptr) {
     const int lane = threadIdx.x & 31;
@@ -699,14 +703,16 @@ __device__ void decide_mb(const DecideParams& P, DecideSmem<T>& S, const unsigne
     }
     stage_source(A, S.a);
     __syncwarp();
+    ironav_interdec& D = *reinterpret_cast<ironav_interdec*>(S.c.dec);
+    int2 sv = make_int2(0, 0);
+    if (!P.intra) {
     // P_Skip first (722-751)
-    const int2 sv = skip_mv(A, S.a);
+    sv = skip_mv(A, S.a);
     if (lane == 0) S.a.cand[0] = sv;
     __syncwarp();
     pred_batch(A, S.a, 0, 0, 0, 2, 2, 1, true);
     const int sad = S.a.cost[0];
     __syncwarp();
-    ironav_interdec& D = *reinterpret_cast<ironav_interdec*>(S.c.dec);
     // the skip vector's decision: 16x16 from reference 0
     if (lane == 0) {
         D.mode = 2;
@@ -762,6 +768,7 @@ __device__ void decide_mb(const DecideParams& P, DecideSmem<T>& S, const unsigne
             return;
         }
     }
+    }  // !P.intra
     load_intra_neighbours(P, S, mb, mbx, mby, ta, la, tra);
     int2 i16 = make_int2(2, 0);
     int seq = 0;
@@ -775,8 +782,8 @@ __device__ void decide_mb(const DecideParams& P, DecideSmem<T>& S, const unsigne
     } else {
         i16 = best_i16_d(P, S, ta, la);
     }
-    // best_inter, enc/frame.rs:839-849
-    int part = 0, cost = 0, bestr = 0;
+    // best_inter, enc/frame.rs:839-849 (none in an IDR picture: nact is 0 there)
+    int part = 0, cost = BIG, bestr = 0;
     uint32_t sub = 0;
     for (int r = 0; r < A.nact; r++) {
         const int4 bi = best_inter_ref(A, S.a, r);
@@ -797,9 +804,10 @@ __device__ void decide_mb(const DecideParams& P, DecideSmem<T>& S, const unsigne
         i16 = pair_wait(A, &X->i16_seq, seq) ? X->i16 : make_int2(2, 1 << 28);
     }
     int best_intra = i16.y + lam * 4;
-    // Intra4x4 is tried by coding it when intra is competitive (766-779)
+    // Intra4x4 is tried by coding it when intra is competitive (766-779); in an IDR picture always, but for
+    // a flat macroblock in live coding (762-765)
     bool i4 = false;
-    if (best_intra < cost) {
+    if (P.intra ? !(A.fast && i16.y < P.flat_t) : best_intra < cost) {
         int c4;
         if constexpr (PAIR) {
             c4 = pair_wait(A, &X->done_seq, seq) ? X->c4 : (1 << 28);
@@ -816,7 +824,7 @@ __device__ void decide_mb(const DecideParams& P, DecideSmem<T>& S, const unsigne
         if (lane == 0) X->stop_seq = seq;
         pair_wait(A, &X->done_seq, seq);
     }
-    if (cost <= best_intra) {
+    if (!P.intra && cost <= best_intra) {
         if (lane == 0) {
             D.mode = 2;
             D.part = (uint8_t)part;

@@ -271,7 +271,7 @@ extern "C" int ironav_batch_step(ironav_batch* b, const void* const* d_src, cons
     for (int i = 0; i < b->n; i++) {
         const ironav_ctx* c = b->ctx[i];
         // the step pushes one reference: afterwards min(nrefs + 1, max_refs) are held
-        if (!d_src[i] || !d_ref[i] || !d_states[i] || !d_results[i] || !c->have_params || c->nact > std::min(c->nrefs + 1, c->max_refs))
+        if (!d_src[i] || !d_ref[i] || !d_states[i] || !d_results[i] || !c->have_params || c->intra_pic || c->nact > std::min(c->nrefs + 1, c->max_refs))
             return IRONAV_INVALID_ARGUMENT;
     }
     // the staging tables are reused: the previous step's copies must have left them

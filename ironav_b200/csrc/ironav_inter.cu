@@ -125,6 +125,11 @@ void free_ctx(ironav_ctx* c) {
     cudaFree(c->d_codes);
     cudaFree(c->d_rec);
     cudaFree(c->d_mbcodes);
+    cudaFree(c->d_cavlc);
+    cudaFree(c->d_slice_tab);
+    cudaFree(c->d_rbsp);
+    cudaFreeHost(c->h_cavlc);
+    cudaFreeHost(c->h_rbsp);
     cudaFreeHost(c->h_results);
     cudaFreeHost(c->h_done);
     cudaFreeHost(c->h_committed);
@@ -328,6 +333,7 @@ int ironav_ctx_create(ironav_ctx** out, int width, int height, int bd, int max_r
     c->sh = c->ph + 2 * PAD;
     c->max_refs = max_refs;
     c->nslices = nslices;
+    for (int i = 0; i <= nslices; i++) c->band_rows[i] = bands[i];
     c->nmb = mb_w * mb_h;
     c->psize = (long long)c->sw * c->sh;
     auto fail = [&](cudaError_t e) {
@@ -489,21 +495,35 @@ int ironav_begin_p_picture(ironav_ctx* c, int qpp, int lambda, int skip_thresh, 
     c->fast = fast ? 1 : 0;
     c->sub8 = sub8 ? 1 : 0;
     c->have_params = true;
+    c->intra_pic = false;
+    return IRONAV_OK;
+}
+
+int ironav_begin_i_picture(ironav_ctx* c, int qpp, int lambda, int fast) {
+    if (!c || lambda < 1 || qpp < 0 || qpp > 63) return IRONAV_INVALID_ARGUMENT;
+    c->qpp = qpp;
+    c->lambda = lambda;
+    c->skip_thresh = 0;
+    c->nact = 0;
+    c->fast = fast ? 1 : 0;
+    c->sub8 = 0;
+    c->have_params = true;
+    c->intra_pic = true;
     return IRONAV_OK;
 }
 
 int ironav_analyse_picture_replay_device(ironav_ctx* c, const ironav_mbstate* d_states, ironav_mbresult* d_out) {
-    if (!c || !d_states || !d_out || !c->have_params || c->nact > c->nrefs) return IRONAV_INVALID_ARGUMENT;
+    if (!c || !d_states || !d_out || !c->have_params || c->intra_pic || c->nact > c->nrefs) return IRONAV_INVALID_ARGUMENT;
     return launch_analyse(c, false, d_states, nullptr, d_out);
 }
 
 int ironav_analyse_picture_auto_device(ironav_ctx* c, ironav_mbstate* d_states, ironav_mbresult* d_out) {
-    if (!c || !d_states || !d_out || !c->have_params || c->nact > c->nrefs) return IRONAV_INVALID_ARGUMENT;
+    if (!c || !d_states || !d_out || !c->have_params || c->intra_pic || c->nact > c->nrefs) return IRONAV_INVALID_ARGUMENT;
     return launch_analyse(c, true, nullptr, d_states, d_out);
 }
 
 int ironav_analyse_picture_replay(ironav_ctx* c, const ironav_mbstate* states, ironav_mbresult* out) {
-    if (!c || !states || !out || !c->have_params || c->nact > c->nrefs) return IRONAV_INVALID_ARGUMENT;
+    if (!c || !states || !out || !c->have_params || c->intra_pic || c->nact > c->nrefs) return IRONAV_INVALID_ARGUMENT;
     CK(cudaMemcpyAsync(c->d_states, states, sizeof(ironav_mbstate) * c->nmb, cudaMemcpyHostToDevice, c->stream));
     int s = launch_analyse(c, false, c->d_states, nullptr, c->d_results);
     if (s != IRONAV_OK) return s;
@@ -512,7 +532,7 @@ int ironav_analyse_picture_replay(ironav_ctx* c, const ironav_mbstate* states, i
 }
 
 int ironav_analyse_picture_auto(ironav_ctx* c, ironav_mbstate* states, ironav_mbresult* out) {
-    if (!c || !states || !out || !c->have_params || c->nact > c->nrefs) return IRONAV_INVALID_ARGUMENT;
+    if (!c || !states || !out || !c->have_params || c->intra_pic || c->nact > c->nrefs) return IRONAV_INVALID_ARGUMENT;
     int s = launch_analyse(c, true, nullptr, c->d_states, c->d_results);
     if (s != IRONAV_OK) return s;
     CK(cudaMemcpyAsync(out, c->d_results, sizeof(ironav_mbresult) * c->nmb, cudaMemcpyDeviceToHost, c->stream));
@@ -582,6 +602,7 @@ static int b_params(ironav_ctx* c, int qpp, int lambda, int l0, int l1, int tb, 
     c->qpp = qpp;
     c->lambda = lambda;
     c->fast = fast ? 1 : 0;
+    c->intra_pic = false;
     c->b_ref[0] = l0;
     c->b_ref[1] = l1;
     c->b_tb = tb;
@@ -675,19 +696,38 @@ int ironav_set_source_chroma(ironav_ctx* c, const void* cb, const void* cr, int 
     return IRONAV_OK;
 }
 
-int ironav_push_reference_chroma(ironav_ctx* c, const void* cb, const void* cr, int stride, int w, int h) {
+int ironav_set_source_chroma_device(ironav_ctx* c, const void* d_cb, const void* d_cr, int stride) {
+    if (!c || !d_cb || !d_cr || stride < c->width / 2) return IRONAV_INVALID_ARGUMENT;
+    const size_t plane = (size_t)c->mb_w * 8 * c->mb_h * 8 * sample_bytes(c);
+    if (!c->d_src_c) CK(cudaMalloc(&c->d_src_c, 2 * plane + 256));
+    int s = load_chroma(c, c->d_src_c, d_cb, stride, c->width / 2, c->height / 2, cudaMemcpyDeviceToDevice);
+    if (s == IRONAV_OK) s = load_chroma(c, c->d_src_c + plane, d_cr, stride, c->width / 2, c->height / 2, cudaMemcpyDeviceToDevice);
+    return s;
+}
+
+static int push_ref_chroma(ironav_ctx* c, const void* cb, const void* cr, int stride, int w, int h, cudaMemcpyKind kind) {
     if (!c || !cb || !cr || c->nrefs < 1) return IRONAV_INVALID_ARGUMENT;
     const int cw = c->mb_w * 8, ch = c->mb_h * 8;
     if (!((w == c->width / 2 && h == c->height / 2) || (w == cw && h == ch)) || stride < w) return IRONAV_INVALID_ARGUMENT;
     const int slot = c->slot_of[0];
     const size_t plane = (size_t)cw * ch * sample_bytes(c);
     if (!c->d_ref_c[slot]) CK(cudaMalloc(&c->d_ref_c[slot], 2 * plane + 256));
-    int s = load_chroma(c, c->d_ref_c[slot], cb, stride, w, h, cudaMemcpyHostToDevice);
-    if (s == IRONAV_OK) s = load_chroma(c, c->d_ref_c[slot] + plane, cr, stride, w, h, cudaMemcpyHostToDevice);
+    int s = load_chroma(c, c->d_ref_c[slot], cb, stride, w, h, kind);
+    if (s == IRONAV_OK) s = load_chroma(c, c->d_ref_c[slot] + plane, cr, stride, w, h, kind);
     if (s != IRONAV_OK) return s;
-    CK(cudaStreamSynchronize(c->stream));
     c->ref_c_ok[slot] = true;
     return IRONAV_OK;
+}
+
+int ironav_push_reference_chroma(ironav_ctx* c, const void* cb, const void* cr, int stride, int w, int h) {
+    const int s = push_ref_chroma(c, cb, cr, stride, w, h, cudaMemcpyHostToDevice);
+    if (s != IRONAV_OK) return s;
+    CK(cudaStreamSynchronize(c->stream));
+    return IRONAV_OK;
+}
+
+int ironav_push_reference_chroma_device(ironav_ctx* c, const void* d_cb, const void* d_cr, int stride, int w, int h) {
+    return push_ref_chroma(c, d_cb, d_cr, stride, w, h, cudaMemcpyDeviceToDevice);
 }
 
 static int launch_code_inter(ironav_ctx* c, int qp, const ironav_interdec* d_decs, ironav_intercode* d_codes, void* y, int ys, void* cb,
@@ -772,10 +812,13 @@ static void fast_thresholds(int qpp, int* luma, int* chroma) {
 // shared with the batched form (ironav_batch.cu)
 int ironav::fill_decide_params(ironav_ctx* c, DecideParams& p, ironav_mbstate* d_states, ironav_mbcode* d_codes, void* y, int ys, void* cb, void* cr,
                                int cs) {
-    if (!c->have_params || c->nact < 1 || c->nact > c->nrefs || !c->d_src_c) return IRONAV_INVALID_ARGUMENT;
+    if (!c->have_params || !c->d_src_c) return IRONAV_INVALID_ARGUMENT;
+    if (!c->intra_pic && (c->nact < 1 || c->nact > c->nrefs)) return IRONAV_INVALID_ARGUMENT;
     for (int i = 0; i < c->nact; i++)
         if (!c->ref_c_ok[c->slot_of[i]]) return IRONAV_INVALID_ARGUMENT;  // an active reference without chroma
     memset(&p, 0, sizeof(p));
+    p.intra = c->intra_pic ? 1 : 0;
+    p.flat_t = (int)std::ceil(256.0 * 0.8 * std::pow(2.0, (double)c->qpp / 6.0));  // enc/frame.rs:763
     fill_params(c, p.C.A);
     p.C.A.states_out = d_states;
     p.C.A.nmb = c->nmb;
@@ -823,13 +866,23 @@ static int launch_decide(ironav_ctx* c, ironav_mbstate* d_states, ironav_mbcode*
     return cuda_status(cudaGetLastError());
 }
 
-int ironav_decide_p_picture_device(ironav_ctx* c, ironav_mbstate* d_states, ironav_mbcode* d_codes, void* y, int ys, void* cb, void* cr, int cs) {
-    if (!c || !d_states || !d_codes || !y || !cb || !cr || ys < c->pw || cs < c->pw / 2) return IRONAV_INVALID_ARGUMENT;
+static int decide_device_checked(ironav_ctx* c, bool intra, ironav_mbstate* d_states, ironav_mbcode* d_codes, void* y, int ys, void* cb,
+                                 void* cr, int cs) {
+    if (!c || !d_states || !d_codes || !y || !cb || !cr || ys < c->pw || cs < c->pw / 2 || c->intra_pic != intra)
+        return IRONAV_INVALID_ARGUMENT;
     // the planes as the deblocking filter's device form; states and codes are written as 32-bit words
     const uintptr_t a = reinterpret_cast<uintptr_t>(y) | reinterpret_cast<uintptr_t>(cb) | reinterpret_cast<uintptr_t>(cr);
     if ((a & 15) || ((size_t)ys * sample_bytes(c)) % 16 || cs % 8) return IRONAV_INVALID_ARGUMENT;
     if ((reinterpret_cast<uintptr_t>(d_states) | reinterpret_cast<uintptr_t>(d_codes)) & 3) return IRONAV_INVALID_ARGUMENT;
     return launch_decide(c, d_states, d_codes, y, ys, cb, cr, cs);
+}
+
+int ironav_decide_p_picture_device(ironav_ctx* c, ironav_mbstate* d_states, ironav_mbcode* d_codes, void* y, int ys, void* cb, void* cr, int cs) {
+    return decide_device_checked(c, false, d_states, d_codes, y, ys, cb, cr, cs);
+}
+
+int ironav_decide_i_picture_device(ironav_ctx* c, ironav_mbstate* d_states, ironav_mbcode* d_codes, void* y, int ys, void* cb, void* cr, int cs) {
+    return decide_device_checked(c, true, d_states, d_codes, y, ys, cb, cr, cs);
 }
 
 int ironav_decide_dbk_records_device(ironav_ctx* c, const ironav_mbcode* d_codes, const ironav_mbstate* d_states, ironav_dbk_mb* d_mbs) {
@@ -854,8 +907,8 @@ int ironav_decide_dbk_records(ironav_ctx* c, const ironav_mbcode* codes, const i
     return IRONAV_OK;
 }
 
-int ironav_decide_p_picture(ironav_ctx* c, ironav_mbstate* states, ironav_mbcode* codes, void* y, int ys, void* cb, void* cr, int cs) {
-    if (!c || !states || !codes || !y || !cb || !cr || ys < c->pw || cs < c->pw / 2) return IRONAV_INVALID_ARGUMENT;
+static int decide_host(ironav_ctx* c, bool intra, ironav_mbstate* states, ironav_mbcode* codes, void* y, int ys, void* cb, void* cr, int cs) {
+    if (!c || !states || !codes || !y || !cb || !cr || ys < c->pw || cs < c->pw / 2 || c->intra_pic != intra) return IRONAV_INVALID_ARGUMENT;
     const size_t B = (size_t)sample_bytes(c), pw = (size_t)c->pw, ph = (size_t)c->ph;
     if (!c->d_mbcodes) CK(cudaMalloc(&c->d_mbcodes, sizeof(ironav_mbcode) * c->nmb));
     if (!c->d_rec) CK(cudaMalloc(&c->d_rec, (pw * ph + 2 * (pw / 2) * (ph / 2)) * B));
@@ -870,6 +923,14 @@ int ironav_decide_p_picture(ironav_ctx* c, ironav_mbstate* states, ironav_mbcode
     CK(cudaMemcpy2DAsync(cb, (size_t)cs * B, dcb, pw / 2 * B, pw / 2 * B, ph / 2, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaMemcpy2DAsync(cr, (size_t)cs * B, dcr, pw / 2 * B, pw / 2 * B, ph / 2, cudaMemcpyDeviceToHost, c->stream));
     return check_device_error(c);
+}
+
+int ironav_decide_p_picture(ironav_ctx* c, ironav_mbstate* states, ironav_mbcode* codes, void* y, int ys, void* cb, void* cr, int cs) {
+    return decide_host(c, false, states, codes, y, ys, cb, cr, cs);
+}
+
+int ironav_decide_i_picture(ironav_ctx* c, ironav_mbstate* states, ironav_mbcode* codes, void* y, int ys, void* cb, void* cr, int cs) {
+    return decide_host(c, true, states, codes, y, ys, cb, cr, cs);
 }
 
 // Measures the 32-bit integer issue rate of the current device (operations per second, 1e12 units in
@@ -908,7 +969,7 @@ int ironav_measure_int32_peak(double* tops) {
 // ---- in-loop mode ----------------------------------------------------------------------------------
 
 int ironav_inloop_begin(ironav_ctx* c, int order) {
-    if (!c || !c->have_params || c->nact > c->nrefs || (order != IRONAV_INLOOP_RASTER && order != IRONAV_INLOOP_BANDS))
+    if (!c || !c->have_params || c->intra_pic || c->nact > c->nrefs || (order != IRONAV_INLOOP_RASTER && order != IRONAV_INLOOP_BANDS))
         return IRONAV_INVALID_ARGUMENT;
     if (c->inloop_active) return IRONAV_INVALID_INPUT;
     if (!c->h_results) {

@@ -131,7 +131,14 @@ EXPORTS = (
     "ironav_set_source_chroma", "ironav_push_reference_chroma", "ironav_code_inter_picture", "ironav_code_inter_picture_device",
     "ironav_decide_p_picture", "ironav_decide_p_picture_device", "ironav_batch_decide", "ironav_decide_dbk_records",
     "ironav_decide_dbk_records_device", "ironav_batch_deblock",
+    "ironav_begin_i_picture", "ironav_decide_i_picture", "ironav_decide_i_picture_device", "ironav_set_source_chroma_device",
+    "ironav_push_reference_chroma_device",
+    "ironav_write_parameter_sets", "ironav_write_slices", "ironav_write_slices_device",
 )
+
+# ironav_stream_params (include/ironav_inter.h): what the SPS and PPS say
+STREAM_PARAMS_DTYPE = np.dtype([("width", "<i4"), ("height", "<i4"), ("bd", "<i4"), ("fps_num", "<i4"), ("fps_den", "<i4"),
+                                ("refs", "<i4")])
 
 SCENE_CUT = 0.8  # codec/change.rs:6
 
@@ -209,6 +216,16 @@ def _declare(lib: ctypes.CDLL) -> ctypes.CDLL:
     if hasattr(lib, "ironav_batch_decide"):
         lib.ironav_batch_decide.argtypes = [_VP, ctypes.POINTER(_VP), ctypes.POINTER(_VP), ctypes.POINTER(_VP), ctypes.POINTER(_I),
                                             ctypes.POINTER(_VP), ctypes.POINTER(_VP), ctypes.POINTER(_I)]
+    if hasattr(lib, "ironav_begin_i_picture"):
+        lib.ironav_begin_i_picture.argtypes = [_VP, _I, _I, _I]
+        lib.ironav_decide_i_picture.argtypes = [_VP, _VP, _VP, _VP, _I, _VP, _VP, _I]
+        lib.ironav_decide_i_picture_device.argtypes = [_VP, _VP, _VP, _VP, _I, _VP, _VP, _I]
+        lib.ironav_set_source_chroma_device.argtypes = [_VP, _VP, _VP, _I]
+        lib.ironav_push_reference_chroma_device.argtypes = [_VP, _VP, _VP, _I, _I, _I]
+        _SZ = ctypes.POINTER(ctypes.c_size_t)
+        lib.ironav_write_parameter_sets.argtypes = [_VP, _VP, ctypes.c_size_t, _SZ]
+        lib.ironav_write_slices.argtypes = [_VP, _I, _I, _I, _VP, _VP, ctypes.c_size_t, _SZ]
+        lib.ironav_write_slices_device.argtypes = [_VP, _I, _I, _I, _VP, _VP, ctypes.c_size_t, _SZ]
     if hasattr(lib, "ironav_analyse_auto_noalloc"):
         # (d_src, src_stride, d_ref, ref_stride, ref_w, ref_h, d_col, width, height, nslices, qp_prime, lambda,
         #  skip_thresh, fast, sub8, d_planes, d_states, d_results, stream)
@@ -461,6 +478,36 @@ class InterStage:
                                                      cb.shape[1]), "ironav_decide_p_picture")
         return states, codes, (y, cb, cr)
 
+    def begin_i_picture(self, qp_prime: int, fast: bool = False) -> None:
+        """Parameters of an IDR picture (FrameCoder::new without a reference, enc/frame.rs:381-412)."""
+        lam = self.lib.ironav_lambda(qp_prime)
+        self._check(self.lib.ironav_begin_i_picture(self.ctx, qp_prime, lam, int(fast)), "ironav_begin_i_picture")
+
+    def decide_i_picture(self):
+        """Decides and codes every macroblock of the current IDR picture (code_mb without a reference):
+        returns (states, codes, (y, cb, cr)) with the unfiltered reconstruction."""
+        dt = np.uint8 if self.bd == 8 else np.uint16
+        y = np.zeros((self.mb_h * 16, self.mb_w * 16), dt)
+        cb = np.zeros((self.mb_h * 8, self.mb_w * 8), dt)
+        cr = np.zeros_like(cb)
+        states = np.zeros(self.nmb, dtype=MBSTATE_DTYPE)
+        codes = np.zeros(self.nmb, dtype=MBCODE_DTYPE)
+        self._check(self.lib.ironav_decide_i_picture(self.ctx, _ptr(states), _ptr(codes), _ptr(y), y.shape[1], _ptr(cb), _ptr(cr),
+                                                     cb.shape[1]), "ironav_decide_i_picture")
+        return states, codes, (y, cb, cr)
+
+    def write_slices(self, idr: bool, frame_num: int, idr_pic_id: int, codes: np.ndarray) -> bytes:
+        """The current picture's slice NAL units (Annex B) from its codes (MBCODE_DTYPE, mb_w*mb_h)."""
+        codes = np.ascontiguousarray(codes, dtype=MBCODE_DTYPE)
+        assert codes.shape == (self.nmb,)
+        return _sized_call(lambda buf, cap, n: self.lib.ironav_write_slices(self.ctx, int(idr), frame_num, idr_pic_id, _ptr(codes),
+                                                                             buf, cap, n), "ironav_write_slices", 1 << 16)
+
+    def write_slices_device(self, idr: bool, frame_num: int, idr_pic_id: int, d_codes: int) -> bytes:
+        return _sized_call(lambda buf, cap, n: self.lib.ironav_write_slices_device(self.ctx, int(idr), frame_num, idr_pic_id, d_codes,
+                                                                                    buf, cap, n), "ironav_write_slices_device",
+                           1 << 16)
+
     def decide_dbk_records(self, codes: np.ndarray, states: np.ndarray) -> np.ndarray:
         """The deblocking filter's macroblock records (DBK_MB_DTYPE) of a picture decide_p_picture coded."""
         codes = np.ascontiguousarray(codes, dtype=MBCODE_DTYPE)
@@ -655,6 +702,31 @@ class InterBatch:
             self.close()
         except Exception:
             pass
+
+
+def _sized_call(fn, what: str, guess: int) -> bytes:
+    """Calls a writer (buf, cap, len*) that reports the bytes it needs when cap is too small; retries once
+    with that size."""
+    n = ctypes.c_size_t(0)
+    for cap in (guess, None):
+        if cap is None:
+            cap = n.value
+        buf = ctypes.create_string_buffer(max(cap, 1))
+        st = fn(buf, cap, ctypes.byref(n))
+        if st == 0:
+            return buf.raw[: n.value]
+        if st != 3 or n.value <= cap:
+            raise IronavError(st, what)
+    raise IronavError(3, what)
+
+
+def write_parameter_sets(width: int, height: int, bd: int = 8, fps: tuple[int, int] = (30, 1), refs: int = 1,
+                         lib: ctypes.CDLL | None = None) -> bytes:
+    """The SPS and PPS NAL units (Annex B) of a CAVLC stream (H264Encoder::sps / pps, enc/mod.rs:296-400)."""
+    lib = lib if lib is not None else cuda_library()
+    p = np.zeros(1, dtype=STREAM_PARAMS_DTYPE)
+    p[0] = (width, height, bd, fps[0], fps[1], refs)
+    return _sized_call(lambda buf, cap, n: lib.ironav_write_parameter_sets(_ptr(p), buf, cap, n), "ironav_write_parameter_sets", 256)
 
 
 def default_bands(mb_h: int, nslices: int) -> list[int]:

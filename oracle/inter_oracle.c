@@ -314,6 +314,7 @@ struct ironav_ctx {
     int nrefs;
     /* picture parameters */
     int qpp, lambda, skip_thresh, nact, fast, sub8;
+    int intra_pic; /* the picture parameters are an IDR picture's (ironav_begin_i_picture) */
     int threads;
     void* inloop; /* in-loop mode state */
     /* B picture parameters */
@@ -949,6 +950,7 @@ int ironav_begin_p_picture(ironav_ctx* c, int qpp, int lambda, int skip_thresh, 
     c->qpp = qpp;
     c->lambda = lambda;
     c->skip_thresh = skip_thresh;
+    c->intra_pic = 0;
     c->nact = nact;
     c->fast = fast ? 1 : 0;
     c->sub8 = sub8 ? 1 : 0;
@@ -2745,7 +2747,7 @@ int ironav_decide_p_picture_device(ironav_ctx* c, ironav_mbstate* s, ironav_mbco
 
 /* finish_mb's MbInfo for the deblocking filter, enc/frame.rs:2323-2339 (slice ids: enc/mod.rs:608) */
 int ironav_decide_dbk_records(ironav_ctx* c, const ironav_mbcode* codes, const ironav_mbstate* states, ironav_dbk_mb* mbs) {
-    if (!c || !codes || !states || !mbs || c->nact < 1) return IRONAV_INVALID_ARGUMENT;
+    if (!c || !codes || !states || !mbs || (c->nact < 1 && !c->intra_pic)) return IRONAV_INVALID_ARGUMENT;
     int band = 0, qp_y = c->qpp - 6 * (c->bd - 8);
     for (int r = 0; r < c->mb_h; r++) {
         if (r > 0 && c->band_start[r] == r) band++;
@@ -2784,4 +2786,633 @@ int ironav_batch_deblock(ironav_batch* b, void* const* y, const int* ys, void* c
                          const ironav_dbk_mb* const* m, const ironav_dbk_slice* const* sl, const int* ns) {
     (void)b; (void)y; (void)ys; (void)cb; (void)cr; (void)cs; (void)m; (void)sl; (void)ns;
     return IRONAV_INVALID_ARGUMENT;
+}
+
+/* ---- intra (IDR) pictures: code_mb without a reference, enc/frame.rs:752-790 ------------------------------------ */
+
+/* The fast mode's flat-macroblock test `i16 < 256 * 0.8 * 2^(QP'/6)` (enc/frame.rs:763) as an integer bound */
+static int flat_threshold(int qpp) { return (int)ceil(256.0 * 0.8 * pow(2.0, (double)qpp / 6.0)); }
+
+/* code_mb for a macroblock of an I slice without CABAC: best_i16, the Intra4x4 trial (always, but for flat
+ * macroblocks in live coding), the cheaper of the two coded, then code_intra_chroma (enc/frame.rs:752-790). */
+static void decide_i_mb(const dctx* D, int mbx, int mby, int flat_t, ironav_mbcode* code, ironav_mbstate* st) {
+    const struct ironav_ctx* c = D->f->c;
+    int lam = c->lambda, i16m, i16c;
+    best_i16(D, mbx, mby, &i16m, &i16c);
+    int best_intra = i16c + lam * 4;
+    int try_i4 = !(c->fast && i16c < flat_t);
+    ironav_mbcode i4code;
+    int i4 = 0;
+    if (try_i4) {
+        int cost = code_i4(D, mbx, mby, &i4code) + lam * 6;
+        if (cost < best_intra) {
+            best_intra = cost;
+            i4 = 1;
+        }
+    }
+    if (i4) *code = i4code;
+    else code_i16(D, mbx, mby, i16m, code);
+    code_intra_chroma(D, mbx, mby, code);
+    d_state(code, st);
+}
+
+int ironav_begin_i_picture(ironav_ctx* c, int qpp, int lambda, int fast) {
+    if (!c || lambda < 1 || qpp < 0 || qpp > 63) return IRONAV_INVALID_ARGUMENT;
+    c->qpp = qpp;
+    c->lambda = lambda;
+    c->skip_thresh = 0;
+    c->nact = 0;
+    c->fast = fast ? 1 : 0;
+    c->sub8 = 0;
+    c->intra_pic = 1;
+    return IRONAV_OK;
+}
+
+int ironav_decide_i_picture(ironav_ctx* c, ironav_mbstate* states, ironav_mbcode* codes, void* rec_y, int ys, void* rec_cb, void* rec_cr,
+                            int cs) {
+    if (!c || !states || !codes || !rec_y || !rec_cb || !rec_cr || ys < c->pw || cs < c->pw / 2 || !c->intra_pic || !c->src_c[0])
+        return IRONAV_INVALID_ARGUMENT;
+    long n = (long)c->mb_w * c->mb_h;
+    int B = sample_bytes(c), cw = c->mb_w * 8, ch = c->mb_h * 8;
+    dctx D;
+    memset(&D, 0, sizeof(D));
+    fc f = {c, states, NULL, 0, NULL};
+    D.f = &f;
+    D.rec[0] = (uint16_t*)calloc((size_t)c->pw * c->ph, sizeof(uint16_t));
+    D.rec[1] = (uint16_t*)calloc((size_t)cw * ch, sizeof(uint16_t));
+    D.rec[2] = (uint16_t*)calloc((size_t)cw * ch, sizeof(uint16_t));
+    D.codes = codes;
+    D.qp = c->qpp;
+    D.qp_y = c->qpp - 6 * (c->bd - 8);
+    int flat_t = flat_threshold(c->qpp);
+    memset(states, 0, sizeof(ironav_mbstate) * (size_t)n);
+    memset(codes, 0, sizeof(ironav_mbcode) * (size_t)n);
+    int nb = 0;
+    int starts[1025];
+    for (int r = 0; r < c->mb_h; r++)
+        if (c->band_start[r] == r) starts[nb++] = r;
+    starts[nb] = c->mb_h;
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 1) num_threads(c->threads)
+#endif
+    for (int b = 0; b < nb; b++)
+        for (int mby = starts[b]; mby < starts[b + 1]; mby++)
+            for (int mbx = 0; mbx < c->mb_w; mbx++) {
+                size_t i = (size_t)mby * c->mb_w + mbx;
+                decide_i_mb(&D, mbx, mby, flat_t, &codes[i], &states[i]);
+            }
+    dbk_copy_out(rec_y, D.rec[0], B, ys, c->pw, c->ph);
+    dbk_copy_out(rec_cb, D.rec[1], B, cs, cw, ch);
+    dbk_copy_out(rec_cr, D.rec[2], B, cs, cw, ch);
+    for (int k = 0; k < 3; k++) free(D.rec[k]);
+    return IRONAV_OK;
+}
+
+int ironav_decide_i_picture_device(ironav_ctx* c, ironav_mbstate* s, ironav_mbcode* o, void* y, int ys, void* cb, void* cr, int cs) {
+    (void)c; (void)s; (void)o; (void)y; (void)ys; (void)cb; (void)cr; (void)cs;
+    return IRONAV_HARDWARE_UNAVAILABLE;
+}
+
+int ironav_set_source_chroma_device(ironav_ctx* c, const void* cb, const void* cr, int stride) {
+    (void)c; (void)cb; (void)cr; (void)stride;
+    return IRONAV_HARDWARE_UNAVAILABLE;
+}
+
+int ironav_push_reference_chroma_device(ironav_ctx* c, const void* cb, const void* cr, int stride, int w, int h) {
+    (void)c; (void)cb; (void)cr; (void)stride; (void)w; (void)h;
+    return IRONAV_HARDWARE_UNAVAILABLE;
+}
+
+/* ---- the bitstream: CAVLC slices and parameter sets (Annex B) ----------------------------------------------- */
+
+#include "cavlc_tables.h"
+
+/* BitWriter, enc/bitw.rs:4-78: bits MSB first into bytes */
+typedef struct bitw {
+    uint8_t* buf;
+    size_t len, cap;
+    uint64_t cur;
+    unsigned n;
+} bitw;
+
+static void bw_init(bitw* w) {
+    memset(w, 0, sizeof(*w));
+    w->cap = 4096;
+    w->buf = (uint8_t*)malloc(w->cap);
+}
+
+static void bw_byte(bitw* w, uint8_t b) {
+    if (w->len == w->cap) {
+        w->cap *= 2;
+        w->buf = (uint8_t*)realloc(w->buf, w->cap);
+    }
+    w->buf[w->len++] = b;
+}
+
+/* put, bitw.rs:16-25: the low n bits of v (n <= 32) */
+static void bw_put(bitw* w, unsigned n, uint32_t v) {
+    w->cur = (w->cur << n) | (uint64_t)v;
+    w->n += n;
+    while (w->n >= 8) {
+        w->n -= 8;
+        bw_byte(w, (uint8_t)(w->cur >> w->n));
+    }
+    w->cur &= (w->n ? ((1ull << w->n) - 1) : 0);
+}
+
+static void bw_flag(bitw* w, int b) { bw_put(w, 1, b ? 1u : 0u); }
+
+/* ue, bitw.rs:31-40 */
+static void bw_ue(bitw* w, uint32_t v) {
+    uint64_t x = (uint64_t)v + 1;
+    unsigned len = 64 - (unsigned)__builtin_clzll(x);
+    if (len > 16) {
+        bw_put(w, len - 1, 0);
+        bw_put(w, len, (uint32_t)x);
+    } else {
+        bw_put(w, 2 * len - 1, (uint32_t)x);
+    }
+}
+
+/* se, bitw.rs:42-44 */
+static void bw_se(bitw* w, int v) { bw_ue(w, v > 0 ? 2u * (uint32_t)v - 1u : (uint32_t)(-2 * (int64_t)v)); }
+
+/* finish, bitw.rs:69-78: rbsp_trailing_bits */
+static void bw_finish(bitw* w) {
+    bw_put(w, 1, 1);
+    if (w->n > 0) bw_put(w, 8 - w->n, 0);
+}
+
+/* put_nal, bitw.rs:91-103: start code, NAL header, emulation prevention */
+static void put_nal(bitw* out, int ref_idc, int kind, const uint8_t* rbsp, size_t n) {
+    bw_byte(out, 0);
+    bw_byte(out, 0);
+    bw_byte(out, 0);
+    bw_byte(out, 1);
+    bw_byte(out, (uint8_t)((ref_idc << 5) | kind));
+    int zeros = 0;
+    for (size_t i = 0; i < n; i++) {
+        uint8_t b = rbsp[i];
+        if (zeros >= 2 && b <= 3) {
+            bw_byte(out, 3);
+            zeros = 0;
+        }
+        bw_byte(out, b);
+        zeros = b == 0 ? zeros + 1 : 0;
+    }
+}
+
+/* put_level, enc/cavlc.rs:12-45 */
+static void put_level(bitw* w, uint32_t code, uint32_t suffix_len) {
+    uint32_t rem = 0;
+    int esc = 0;
+    if (suffix_len == 0) {
+        if (code < 14) bw_put(w, code + 1, 1);
+        else if (code < 30) {
+            bw_put(w, 15, 1);
+            bw_put(w, 4, code - 14);
+        } else {
+            esc = 1;
+            rem = code - 30;
+        }
+    } else if ((code >> suffix_len) < 15) {
+        bw_put(w, (code >> suffix_len) + 1, 1);
+        bw_put(w, suffix_len, code & ((1u << suffix_len) - 1));
+    } else {
+        esc = 1;
+        rem = code - (15u << suffix_len);
+    }
+    if (esc) {
+        if (rem < 4096) {
+            bw_put(w, 16, 1);
+            bw_put(w, 12, rem);
+        } else {
+            unsigned p = 16;
+            while ((uint64_t)rem + 4096 >= (1ull << (p - 2))) p++;
+            bw_put(w, p, 0);
+            bw_put(w, 1, 1);
+            bw_put(w, p - 3, rem + 4096 - (1u << (p - 3)));
+        }
+    }
+}
+
+/* write_block, enc/cavlc.rs:47-122: one residual block, levels in scan order (max = 16, 15 or 4), nc the
+ * neighbour context (-1: chroma DC). Returns the non-zero count. */
+static int write_block(bitw* w, int nc, const int* levels, int max) {
+    int nz[16], runs[16], total = 0, last = -1;
+    memset(runs, 0, sizeof(runs));
+    for (int i = max - 1; i >= 0; i--)
+        if (levels[i] != 0) {
+            if (last >= 0) runs[total - 1] = last - i - 1;
+            nz[total++] = levels[i];
+            last = i;
+        }
+    int ones = 0;
+    while (ones < (total < 3 ? total : 3) && abs(nz[ones]) == 1) ones++;
+    int token = total * 4 + ones;
+    if (nc == -1) bw_put(w, CAVLC_CHROMA_DC_COEFF_TOKEN_LEN[token], CAVLC_CHROMA_DC_COEFF_TOKEN_BITS[token]);
+    else {
+        int cls = nc <= 1 ? 0 : nc <= 3 ? 1 : nc <= 7 ? 2 : 3;
+        bw_put(w, CAVLC_COEFF_TOKEN_LEN[cls][token], CAVLC_COEFF_TOKEN_BITS[cls][token]);
+    }
+    if (total == 0) return 0;
+    for (int i = 0; i < ones; i++) bw_flag(w, nz[i] < 0);
+    uint32_t suffix_len = (total > 10 && ones < 3) ? 1 : 0;
+    for (int i = ones; i < total; i++) {
+        int l = nz[i];
+        uint32_t code = l > 0 ? 2u * (uint32_t)l - 2u : (uint32_t)(-2 * l) - 1u;
+        if (i == ones && ones < 3) code -= 2;
+        put_level(w, code, suffix_len);
+        if (suffix_len == 0) suffix_len = 1;
+        if ((uint32_t)abs(l) > (3u << (suffix_len - 1)) && suffix_len < 6) suffix_len++;
+    }
+    int highest = max - 1;
+    while (levels[highest] == 0) highest--;
+    int zeros_left = highest + 1 - total;
+    if (total < max) {
+        if (nc == -1) bw_put(w, CAVLC_CHROMA_DC_TOTAL_ZEROS_LEN[total - 1][zeros_left], CAVLC_CHROMA_DC_TOTAL_ZEROS_BITS[total - 1][zeros_left]);
+        else bw_put(w, CAVLC_TOTAL_ZEROS_LEN[total - 1][zeros_left], CAVLC_TOTAL_ZEROS_BITS[total - 1][zeros_left]);
+    }
+    for (int i = 0; i < total - 1; i++) {
+        if (zeros_left == 0) break;
+        int zl = zeros_left < 7 ? zeros_left : 7;
+        bw_put(w, CAVLC_RUN_LEN[zl - 1][runs[i]], CAVLC_RUN_BITS[zl - 1][runs[i]]);
+        zeros_left -= runs[i];
+    }
+    return total;
+}
+
+/* One slice's writer: its bits, the skip run, and what the neighbour lookups need */
+typedef struct swr {
+    const struct ironav_ctx* c;
+    const ironav_mbcode* codes;
+    int p_slice, nref, first_row;
+    uint32_t skip_run;
+    bitw w;
+} swr;
+
+/* The neighbour's code when it is in this slice (nb_state, enc/frame.rs:509-515) */
+static const ironav_mbcode* w_nb(const swr* s, int mbx, int mby) {
+    if (mbx < 0 || mby < s->first_row || mbx >= s->c->mb_w || mby >= s->c->mb_h) return NULL;
+    return &s->codes[(size_t)mby * s->c->mb_w + mbx];
+}
+
+/* nc, enc/frame.rs:2354-2361 */
+static int nc_of(int ha, int a, int hb, int b) {
+    if (ha && hb) return (a + b + 1) >> 1;
+    if (ha) return a;
+    if (hb) return b;
+    return 0;
+}
+
+/* nc_luma, enc/frame.rs:606-610 */
+static int w_nc_luma(const swr* s, const uint8_t cur[16], int mbx, int mby, int bx, int by) {
+    int ha = 1, a = 0, hb = 1, b = 0;
+    if (bx > 0) a = cur[by * 4 + bx - 1];
+    else {
+        const ironav_mbcode* n = w_nb(s, mbx - 1, mby);
+        ha = n != NULL;
+        if (n) a = n->res.nnz[by * 4 + 3];
+    }
+    if (by > 0) b = cur[(by - 1) * 4 + bx];
+    else {
+        const ironav_mbcode* n = w_nb(s, mbx, mby - 1);
+        hb = n != NULL;
+        if (n) b = n->res.nnz[12 + bx];
+    }
+    return nc_of(ha, a, hb, b);
+}
+
+/* nc_chroma, enc/frame.rs:612-616 */
+static int w_nc_chroma(const swr* s, const uint8_t cur[4], int comp, int mbx, int mby, int bx, int by) {
+    int ha = 1, a = 0, hb = 1, b = 0;
+    if (bx > 0) a = cur[by * 2];
+    else {
+        const ironav_mbcode* n = w_nb(s, mbx - 1, mby);
+        ha = n != NULL;
+        if (n) a = n->res.cnnz[comp][by * 2 + 1];
+    }
+    if (by > 0) b = cur[bx];
+    else {
+        const ironav_mbcode* n = w_nb(s, mbx, mby - 1);
+        hb = n != NULL;
+        if (n) b = n->res.cnnz[comp][2 + bx];
+    }
+    return nc_of(ha, a, hb, b);
+}
+
+/* pred_i4_mode, enc/frame.rs:619-629 (a neighbour that is not Intra4x4 counts as DC) */
+static int w_pred_i4(const swr* s, const uint8_t cur[16], int mbx, int mby, int bx, int by) {
+    int a = -1, b = -1;
+    if (bx > 0) a = cur[by * 4 + bx - 1];
+    else {
+        const ironav_mbcode* n = w_nb(s, mbx - 1, mby);
+        if (n) a = n->kind == KIND_I4 ? n->modes[by * 4 + 3] : 2;
+    }
+    if (by > 0) b = cur[(by - 1) * 4 + bx];
+    else {
+        const ironav_mbcode* n = w_nb(s, mbx, mby - 1);
+        if (n) b = n->kind == KIND_I4 ? n->modes[12 + bx] : 2;
+    }
+    return (a >= 0 && b >= 0) ? mini(a, b) : 2;
+}
+
+static int cbp_code(const uint8_t* table, int cbp) {
+    for (int i = 0; i < 48; i++)
+        if (table[i] == cbp) return i;
+    return -1;
+}
+
+static int n_rects(int part, const uint8_t sub[4]) {
+    rect4 r[16];
+    return rects(part, sub, r);
+}
+
+/* write_mb, enc/frame.rs:1922-2016 */
+static void write_mb(swr* s, const ironav_mbcode* code, int mbx, int mby) {
+    bitw* w = &s->w;
+    if (s->p_slice) {
+        if (code->skip) {
+            s->skip_run++;
+            return;
+        }
+        bw_ue(w, s->skip_run);
+        s->skip_run = 0;
+    }
+    unsigned base = s->p_slice ? 5 : 0;
+    int cbpl = code->res.cbp & 15, cbpc = code->res.cbp >> 4;
+    if (code->kind == KIND_I4) {
+        bw_ue(w, base);
+        uint8_t so_far[16];
+        memset(so_far, 2, sizeof(so_far));
+        for (int n = 0; n < 16; n++) {
+            int bx = ((n >> 2) & 1) * 2 + (n & 1), by = ((n >> 3) & 1) * 2 + ((n >> 1) & 1);
+            int mode = code->modes[by * 4 + bx];
+            int pred = w_pred_i4(s, so_far, mbx, mby, bx, by);
+            so_far[by * 4 + bx] = (uint8_t)mode;
+            if (mode == pred) bw_flag(w, 1);
+            else {
+                bw_flag(w, 0);
+                bw_put(w, 3, (uint32_t)(mode < pred ? mode : mode - 1));
+            }
+        }
+        bw_ue(w, code->chroma_mode);
+        bw_ue(w, (uint32_t)cbp_code(CAVLC_GOLOMB_TO_INTRA4X4_CBP, code->res.cbp));
+    } else if (code->kind == KIND_I16) {
+        bw_ue(w, base + 1 + code->i16_mode + 4 * (unsigned)cbpc + (cbpl ? 12 : 0));
+        bw_ue(w, code->chroma_mode);
+    } else {
+        bw_ue(w, code->part);
+        if (code->part == 3)
+            for (int k = 0; k < 4; k++) bw_ue(w, code->sub[k]);
+        if (s->nref > 1)
+            for (int k = 0; k < NPARTS[code->part]; k++) {
+                if (s->nref == 2) bw_flag(w, code->refs[k] == 0);
+                else bw_ue(w, code->refs[k]);
+            }
+        int nr = n_rects(code->part, code->sub);
+        for (int k = 0; k < nr; k++) {
+            bw_se(w, code->mvds[k][0]);
+            bw_se(w, code->mvds[k][1]);
+        }
+        bw_ue(w, (uint32_t)cbp_code(CAVLC_GOLOMB_TO_INTER_CBP, code->res.cbp));
+    }
+    if (code->res.cbp == 0 && code->kind != KIND_I16) return;
+    bw_se(w, 0); /* mb_qp_delta */
+    int lv[16];
+    if (code->kind == KIND_I16) {
+        for (int k = 0; k < 16; k++) lv[k] = code->dc[k];
+        write_block(w, w_nc_luma(s, code->res.nnz, mbx, mby, 0, 0), lv, 16);
+    }
+    for (int n = 0; n < 16; n++) {
+        int bx = ((n >> 2) & 1) * 2 + (n & 1), by = ((n >> 3) & 1) * 2 + ((n >> 1) & 1);
+        if (!(cbpl & (1 << (n / 4)))) continue;
+        int nc = w_nc_luma(s, code->res.nnz, mbx, mby, bx, by);
+        const int16_t* b = code->res.luma[by * 4 + bx];
+        if (code->kind == KIND_I16) {
+            for (int k = 0; k < 15; k++) lv[k] = b[1 + k];
+            write_block(w, nc, lv, 15);
+        } else {
+            for (int k = 0; k < 16; k++) lv[k] = b[k];
+            write_block(w, nc, lv, 16);
+        }
+    }
+    if (cbpc > 0)
+        for (int cc = 0; cc < 2; cc++) {
+            for (int k = 0; k < 4; k++) lv[k] = code->res.cdc[cc][k];
+            write_block(w, -1, lv, 4);
+        }
+    if (cbpc == 2)
+        for (int cc = 0; cc < 2; cc++)
+            for (int blk = 0; blk < 4; blk++) {
+                int nc = w_nc_chroma(s, code->res.cnnz[cc], cc, mbx, mby, blk & 1, blk >> 1);
+                for (int k = 0; k < 15; k++) lv[k] = code->res.cac[cc][blk][1 + k];
+                write_block(w, nc, lv, 15);
+            }
+}
+
+static int bands_of(const struct ironav_ctx* c, int starts[1025]) {
+    int nb = 0;
+    for (int r = 0; r < c->mb_h; r++)
+        if (c->band_start[r] == r) starts[nb++] = r;
+    starts[nb] = c->mb_h;
+    return nb;
+}
+
+/* The picture's slices: header (enc/mod.rs:566-600), macroblocks in raster order (FrameCoder::encode,
+ * enc/frame.rs:452-487), trailing skip run and rbsp bits; each a NAL unit of nal_ref_idc 3, type 5 (IDR) or
+ * 1 (enc/mod.rs:641-643). */
+int ironav_write_slices(ironav_ctx* c, int idr, int frame_num, int idr_pic_id, const ironav_mbcode* codes, uint8_t* out, size_t cap,
+                        size_t* len) {
+    if (!c || !codes || !len || (idr != 0) != (c->intra_pic != 0) || (!idr && c->nact < 1) || frame_num < 0 || frame_num > 255 ||
+        idr_pic_id < 0 || idr_pic_id > 65535)
+        return IRONAV_INVALID_ARGUMENT;
+    int starts[1025];
+    int nb = bands_of(c, starts);
+    int qp = c->qpp - 6 * (c->bd - 8);
+    bitw stream;
+    bw_init(&stream);
+    for (int b = 0; b < nb; b++) {
+        swr s;
+        memset(&s, 0, sizeof(s));
+        s.c = c;
+        s.codes = codes;
+        s.p_slice = !idr;
+        s.nref = idr ? 0 : c->nact;
+        s.first_row = starts[b];
+        bw_init(&s.w);
+        bitw* w = &s.w;
+        bw_ue(w, (uint32_t)(starts[b] * c->mb_w)); /* first_mb_in_slice */
+        bw_ue(w, idr ? 7 : 5);                     /* slice_type: I or P, all slices alike */
+        bw_ue(w, 0);                               /* pic_parameter_set_id */
+        bw_put(w, 8, (uint32_t)frame_num);
+        if (idr) bw_ue(w, (uint32_t)idr_pic_id);
+        if (!idr) {
+            if (c->nact > 1) {
+                bw_flag(w, 1); /* num_ref_idx_active_override_flag */
+                bw_ue(w, (uint32_t)(c->nact - 1));
+            } else bw_flag(w, 0);
+            bw_flag(w, 0); /* ref_pic_list_modification_flag_l0 */
+        }
+        if (idr) {
+            bw_flag(w, 0); /* no_output_of_prior_pics_flag */
+            bw_flag(w, 0); /* long_term_reference_flag */
+        } else bw_flag(w, 0); /* adaptive_ref_pic_marking_mode_flag */
+        bw_se(w, qp - 26);    /* slice_qp_delta */
+        for (int mby = starts[b]; mby < starts[b + 1]; mby++)
+            for (int mbx = 0; mbx < c->mb_w; mbx++) write_mb(&s, &codes[(size_t)mby * c->mb_w + mbx], mbx, mby);
+        if (s.skip_run > 0) bw_ue(w, s.skip_run);
+        bw_finish(w);
+        put_nal(&stream, 3, idr ? 5 : 1, w->buf, w->len);
+        free(w->buf);
+    }
+    *len = stream.len;
+    int st = IRONAV_OK;
+    if (!out || cap < stream.len) st = IRONAV_INVALID_ARGUMENT;
+    else memcpy(out, stream.buf, stream.len);
+    free(stream.buf);
+    return st;
+}
+
+int ironav_write_slices_device(ironav_ctx* c, int idr, int frame_num, int idr_pic_id, const ironav_mbcode* d_codes, uint8_t* out, size_t cap,
+                               size_t* len) {
+    (void)c; (void)idr; (void)frame_num; (void)idr_pic_id; (void)d_codes; (void)out; (void)cap; (void)len;
+    return IRONAV_HARDWARE_UNAVAILABLE;
+}
+
+/* (level_idc, MaxFS, MaxMBPS) of Table A-1 (enc/mod.rs:43-63) */
+static const int64_t LEVELS_A1[19][3] = {{10, 99, 1485},      {11, 396, 3000},      {12, 396, 6000},       {13, 396, 11880},
+                                         {20, 396, 11880},    {21, 792, 19800},     {22, 1620, 20250},     {30, 1620, 40500},
+                                         {31, 3600, 108000},  {32, 5120, 216000},   {40, 8192, 245760},    {41, 8192, 245760},
+                                         {42, 8704, 522240},  {50, 22080, 589824},  {51, 36864, 983040},   {52, 36864, 2073600},
+                                         {60, 139264, 4177920}, {61, 139264, 8355840}, {62, 139264, 16711680}};
+
+/* H264Encoder::sps / pps for the CAVLC encoder (enc/mod.rs:296-400) and the level choice (154-157) */
+int ironav_write_parameter_sets(const ironav_stream_params* p, uint8_t* out, size_t cap, size_t* len) {
+    if (!p || !len || p->width <= 0 || p->height <= 0 || (p->width & 1) || (p->height & 1) || (p->bd != 8 && p->bd != 10) || p->refs < 1 ||
+        p->refs > 16)
+        return IRONAV_INVALID_ARGUMENT;
+    int mb_w = (p->width + 15) / 16, mb_h = (p->height + 15) / 16;
+    if (mb_w > 1024 || mb_h > 1024) return IRONAV_INVALID_ARGUMENT;
+    int64_t fs = (int64_t)mb_w * mb_h;
+    int rate_ok = p->fps_num > 0 && p->fps_den > 0;
+    double fps = rate_ok ? (double)p->fps_num / (double)p->fps_den : 25.0;
+    int64_t mbps = (int64_t)ceil((double)fs * fps);
+    int level = -1;
+    for (int i = 0; i < 19 && level < 0; i++)
+        if (LEVELS_A1[i][1] >= fs && LEVELS_A1[i][2] >= mbps) level = (int)LEVELS_A1[i][0];
+    for (int i = 0; i < 19 && level < 0; i++)
+        if (LEVELS_A1[i][1] >= fs) level = (int)LEVELS_A1[i][0];
+    if (level < 0) level = 62;
+    int high = p->bd > 8;
+    bitw w;
+    bw_init(&w);
+    if (high) {
+        bw_put(&w, 8, 110); /* High 10 */
+        bw_put(&w, 8, 0);
+    } else {
+        bw_put(&w, 8, 66);          /* Baseline */
+        bw_put(&w, 8, 0xC0);        /* constraint_set0 and constraint_set1: Constrained Baseline */
+    }
+    bw_put(&w, 8, (uint32_t)level);
+    bw_ue(&w, 0); /* seq_parameter_set_id */
+    if (high) {
+        bw_ue(&w, 1);                          /* chroma_format_idc: 4:2:0 */
+        bw_ue(&w, (uint32_t)(p->bd - 8));      /* bit_depth_luma_minus8 */
+        bw_ue(&w, (uint32_t)(p->bd - 8));      /* bit_depth_chroma_minus8 */
+        bw_flag(&w, 0);                        /* qpprime_y_zero_transform_bypass_flag */
+        bw_flag(&w, 0);                        /* seq_scaling_matrix_present_flag */
+    }
+    bw_ue(&w, 4); /* log2_max_frame_num_minus4 */
+    bw_ue(&w, 2); /* pic_order_cnt_type: output order is decoding order */
+    bw_ue(&w, (uint32_t)p->refs); /* max_num_ref_frames */
+    bw_flag(&w, 0);               /* gaps_in_frame_num_value_allowed_flag */
+    bw_ue(&w, (uint32_t)(mb_w - 1));
+    bw_ue(&w, (uint32_t)(mb_h - 1));
+    bw_flag(&w, 1); /* frame_mbs_only_flag */
+    bw_flag(&w, 1); /* direct_8x8_inference_flag */
+    int cr = (mb_w * 16 - p->width) / 2, cb = (mb_h * 16 - p->height) / 2;
+    bw_flag(&w, cr > 0 || cb > 0);
+    if (cr > 0 || cb > 0) {
+        bw_ue(&w, 0);
+        bw_ue(&w, (uint32_t)cr);
+        bw_ue(&w, 0);
+        bw_ue(&w, (uint32_t)cb);
+    }
+    bw_flag(&w, 1); /* vui_parameters_present_flag */
+    bw_flag(&w, 0); /* aspect_ratio_info_present_flag */
+    bw_flag(&w, 0); /* overscan_info_present_flag */
+    bw_flag(&w, 0); /* video_signal_type_present_flag */
+    bw_flag(&w, 0); /* chroma_loc_info_present_flag */
+    int timing = rate_ok && 2ll * p->fps_num <= 0xFFFFFFFFll;
+    bw_flag(&w, timing);
+    if (timing) {
+        bw_put(&w, 32, (uint32_t)p->fps_den);      /* num_units_in_tick */
+        bw_put(&w, 32, 2u * (uint32_t)p->fps_num); /* time_scale: two ticks per frame */
+        bw_flag(&w, 1);                            /* fixed_frame_rate_flag */
+    }
+    bw_flag(&w, 0); /* nal_hrd_parameters_present_flag */
+    bw_flag(&w, 0); /* vcl_hrd_parameters_present_flag */
+    bw_flag(&w, 0); /* pic_struct_present_flag */
+    bw_flag(&w, 1); /* bitstream_restriction_flag */
+    bw_flag(&w, 1); /* motion_vectors_over_pic_boundaries_flag */
+    bw_ue(&w, 0);   /* max_bytes_per_pic_denom */
+    bw_ue(&w, 0);   /* max_bits_per_mb_denom */
+    bw_ue(&w, 15);  /* log2_max_mv_length_horizontal */
+    bw_ue(&w, 15);  /* log2_max_mv_length_vertical */
+    bw_ue(&w, 0);   /* max_num_reorder_frames */
+    bw_ue(&w, (uint32_t)(p->refs > 1 ? p->refs : 1)); /* max_dec_frame_buffering */
+    bw_finish(&w);
+    bitw pps;
+    bw_init(&pps);
+    bw_ue(&pps, 0);      /* pic_parameter_set_id */
+    bw_ue(&pps, 0);      /* seq_parameter_set_id */
+    bw_flag(&pps, 0);    /* entropy_coding_mode_flag: CAVLC */
+    bw_flag(&pps, 0);    /* bottom_field_pic_order_in_frame_present_flag */
+    bw_ue(&pps, 0);      /* num_slice_groups_minus1 */
+    bw_ue(&pps, 0);      /* num_ref_idx_l0_default_active_minus1 */
+    bw_ue(&pps, 0);      /* num_ref_idx_l1_default_active_minus1 */
+    bw_flag(&pps, 0);    /* weighted_pred_flag */
+    bw_put(&pps, 2, 0);  /* weighted_bipred_idc */
+    bw_se(&pps, 0);      /* pic_init_qp_minus26 */
+    bw_se(&pps, 0);      /* pic_init_qs_minus26 */
+    bw_se(&pps, 0);      /* chroma_qp_index_offset */
+    bw_flag(&pps, 0);    /* deblocking_filter_control_present_flag */
+    bw_flag(&pps, 0);    /* constrained_intra_pred_flag */
+    bw_flag(&pps, 0);    /* redundant_pic_cnt_present_flag */
+    bw_finish(&pps);
+    bitw stream;
+    bw_init(&stream);
+    put_nal(&stream, 3, 7, w.buf, w.len);
+    put_nal(&stream, 3, 8, pps.buf, pps.len);
+    free(w.buf);
+    free(pps.buf);
+    *len = stream.len;
+    int st = IRONAV_OK;
+    if (!out || cap < stream.len) st = IRONAV_INVALID_ARGUMENT;
+    else memcpy(out, stream.buf, stream.len);
+    free(stream.buf);
+    return st;
+}
+
+/* Test hooks (oracle only): write_block of one block, and ue/se bits, for the reference's own writer tests */
+int oracle_write_block(int nc, const int* levels, int max, uint8_t* out, int cap, int* nbits) {
+    bitw w;
+    bw_init(&w);
+    int n = write_block(&w, nc, levels, max);
+    *nbits = (int)(w.len * 8 + w.n);
+    bw_finish(&w);
+    if ((int)w.len <= cap) memcpy(out, w.buf, w.len);
+    free(w.buf);
+    return n;
+}
+
+int oracle_put_nal(int ref_idc, int kind, const uint8_t* rbsp, int n, uint8_t* out, int cap) {
+    bitw w;
+    bw_init(&w);
+    put_nal(&w, ref_idc, kind, rbsp, (size_t)n);
+    int len = (int)w.len;
+    if (len <= cap) memcpy(out, w.buf, w.len);
+    free(w.buf);
+    return len;
 }

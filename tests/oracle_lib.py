@@ -15,8 +15,8 @@ _LIB = None
 
 
 def build_oracle() -> str:
-    src = os.path.join(ORACLE_DIR, "inter_oracle.c")
-    if not os.path.exists(ORACLE_LIB) or os.path.getmtime(ORACLE_LIB) < os.path.getmtime(src):
+    srcs = [os.path.join(ORACLE_DIR, f) for f in ("inter_oracle.c", "cavlc_tables.h")]
+    if not os.path.exists(ORACLE_LIB) or any(os.path.getmtime(ORACLE_LIB) < os.path.getmtime(s) for s in srcs):
         subprocess.run(["make", "-s", "-C", ORACLE_DIR], check=True)
     return ORACLE_LIB
 
@@ -46,5 +46,12 @@ def oracle_library() -> ctypes.CDLL:
         lib.oracle_analyse_replay_subset.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                                      ctypes.c_int, ctypes.c_void_p]
         del u16p
+        declare_stream_hooks(lib)
         _LIB = lib
     return _LIB
+
+
+def declare_stream_hooks(lib) -> None:
+    """The oracle's writer test hooks (not in the public header)."""
+    lib.oracle_write_block.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+    lib.oracle_put_nal.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int]

@@ -86,3 +86,69 @@ def test_batch_equals_single_stream_auto_mode(cuda_lib, bd):
         assert np.array_equal(d_res[i][1].cpu().numpy().view(MBRESULT_DTYPE), want[i][1][1]), f"stream {i}: graph replay"
     del g
     batch.close()
+
+
+def test_config3_64_streams_four_steps(cuda_lib, oracle_lib):
+    """The batched configuration itself: its 64 streams (seeded resolutions from {640x360, 854x480, 1280x720,
+    1920x1080}, QP 27, one reference, the pinned slice bands) stepped together for four frame steps, each step
+    one batch step over all streams; every stream's decisions and results at every step equal its own
+    single-stream auto mode, and the first streams' equal the oracle's."""
+    import torch
+
+    from ironav_b200.synth import batch_streams
+
+    streams = batch_streams(64)
+    steps = 4
+    stream = torch.cuda.Stream()
+    stages, dev, want = [], [], []
+    for i, (w, h, ns, seed) in enumerate(streams):
+        seq = Sequence.config("1080p", steps + 1, seed=seed, size=(w, h))
+        f = [seq.frame(t) for t in range(steps + 1)]
+        one = InterStage(w, h, nslices=ns, lib=cuda_lib)
+        per, col = [], None
+        for t in range(1, steps + 1):
+            one.clear_references()
+            one.push_reference(f[t - 1], col=col)
+            one.set_source(f[t])
+            one.begin_p_picture(27)
+            s, r = one.analyse_auto()
+            per.append((s, r))
+            col = s
+        one.close()
+        if i < 2:  # the single-stream path itself against the oracle on the first streams
+            o = InterStage(w, h, nslices=ns, lib=oracle_lib)
+            col = None
+            for t in range(1, steps + 1):
+                o.clear_references()
+                o.push_reference(f[t - 1], col=col)
+                o.set_source(f[t])
+                o.begin_p_picture(27)
+                s, r = o.analyse_auto()
+                assert np.array_equal(s, per[t - 1][0]) and np.array_equal(r, per[t - 1][1]), f"stream {i} step {t}: oracle"
+                col = s
+            o.close()
+        want.append(per)
+        d = [torch.from_numpy(x).cuda() for x in f]
+        st = InterStage(w, h, nslices=ns, lib=cuda_lib)
+        st.set_stream(stream.cuda_stream)
+        st.push_reference_device(d[0].data_ptr(), w, w, h, None)
+        st.begin_p_picture(27)
+        stages.append(st)
+        dev.append(d)
+    n = len(stages)
+    d_states = [[torch.zeros(s.nmb * 72, dtype=torch.uint8, device="cuda") for _ in range(steps)] for s in stages]
+    d_res = [torch.zeros(s.nmb * 104, dtype=torch.uint8, device="cuda") for s in stages]
+    torch.cuda.synchronize()
+    batch = InterBatch(stages)
+    for k in range(steps):
+        t = k + 1
+        col = [None] * n if k == 0 else [d_states[i][k - 1].data_ptr() for i in range(n)]
+        batch.step([f[t].data_ptr() for f in dev], [f[t - 1].data_ptr() for f in dev], col,
+                   [d_states[i][k].data_ptr() for i in range(n)], [d.data_ptr() for d in d_res])
+        batch.sync()
+        for i in range(n):
+            assert np.array_equal(d_states[i][k].cpu().numpy().view(MBSTATE_DTYPE), want[i][k][0]), f"stream {i} step {t}: decisions"
+            assert np.array_equal(d_res[i].cpu().numpy().view(MBRESULT_DTYPE), want[i][k][1]), f"stream {i} step {t}: results"
+    batch.close()
+    for st in stages:
+        st.close()
