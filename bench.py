@@ -54,7 +54,8 @@ def parse():
     p.add_argument("--ring", type=int, default=RING,
                    help="pictures in the ring (fewer than 36 fits in L2: for profiling runs only)")
     p.add_argument("--no-e2e", action="store_true", help="skip the host-buffer pass (profiling runs)")
-    p.add_argument("--workload", default="1080p", choices=["1080p", "batched", "scenecut", "deblock", "bpicture", "residual", "decide", "decide_batched"],
+    p.add_argument("--workload", default="1080p", choices=["1080p", "batched", "scenecut", "deblock", "bpicture", "residual", "decide",
+                                                         "decide_batched", "inloop", "encode"],
                    help="1080p: one stream, replay mode (the headline); batched: 64 mixed-resolution streams in auto "
                         "mode, one launch per stage and frame step, against the per-stream launch loop")
     p.add_argument("--streams", type=int, default=64, help="streams of the batched workload")
@@ -348,6 +349,12 @@ def main():
     if args.workload == "decide_batched":
         run_decide_batched(args, rank, world)
         return finish(world)
+    if args.workload == "inloop":
+        run_inloop(args, rank, world)
+        return finish(world)
+    if args.workload == "encode":
+        run_encode(args, rank, world)
+        return finish(world)
 
     import torch
     import torch.distributed as dist
@@ -477,6 +484,211 @@ def main():
         print(json.dumps(line), flush=True)
     st.close()
     return finish(world)
+
+
+def run_inloop(args, rank, world):
+    """In-loop mode, the drop-in as the reference's encoder would drive it (FrameCoder::encode's slice loop,
+    enc/frame.rs:467-478, on one thread per slice band, enc/mod.rs:620-628): 1080p, QP 27, one reference,
+    eight bands; one native host thread per band reads each macroblock's analysis, decides it (the auto
+    policy standing in for the host's rate-distortion choice) and commits it through mapped host memory,
+    and the device analyses a macroblock once its left and top-right neighbours are committed. One step is
+    one P picture; wall clock (the picture is host-synchronous by nature), max over ranks. Against the
+    reference-faithful CPU form, the oracle's own slice loop on the same number of threads."""
+    import torch
+    import torch.distributed as dist
+    from ironav_b200.inter import MBRESULT_DTYPE, MBSTATE_DTYPE, InterStage, cuda_library, default_bands, inloop_caller
+
+    lib, drv = cuda_library(), inloop_caller()
+    dev = torch.device("cuda", torch.cuda.current_device())
+    ring = min(RING, 12)
+    frames = make_frames(rank, ring)
+    st = InterStage(WIDTH, HEIGHT, nslices=NSLICES, lib=lib)
+    nmb, thr = st.nmb, lib.ironav_skip_threshold(QP)
+    bands = np.asarray(default_bands(st.mb_h, NSLICES), dtype=np.int32)
+    d_frames = torch.from_numpy(frames).to(dev)
+    fp = lambda t: d_frames[t].data_ptr()
+    # the co-located decisions of each reference: the stage's auto mode (the in-loop decisions under the auto
+    # policy are the same ones; checked below)
+    d_states = torch.zeros((ring, nmb * 72), dtype=torch.uint8, device=dev)
+    d_res = torch.zeros(nmb * 104, dtype=torch.uint8, device=dev)
+    for t in range(1, ring):
+        st.clear_references()
+        st.push_reference_device(fp(t - 1), WIDTH, WIDTH, HEIGHT, d_states[t - 1].data_ptr() if t >= 2 else None)
+        st.set_source_device(fp(t), WIDTH)
+        st.begin_p_picture(QP)
+        st.analyse_auto_device(d_states[t].data_ptr(), d_res.data_ptr())
+    st.sync()
+    states = np.zeros(nmb, dtype=MBSTATE_DTYPE)
+    results = np.zeros(nmb, dtype=MBRESULT_DTYPE)
+
+    def picture(i, host=False):
+        t = 1 + i % (ring - 1)
+        st.clear_references()
+        col = d_states[t - 1].data_ptr() if t >= 2 else None
+        if host:  # the host-buffer calls: the source and the reference luma from host memory
+            st.push_reference(frames[t - 1], col=d_states[t - 1].cpu().numpy().view(MBSTATE_DTYPE) if t >= 2 else None)
+            st.set_source(frames[t])
+        else:
+            st.push_reference_device(fp(t - 1), WIDTH, WIDTH, HEIGHT, col)
+            st.set_source_device(fp(t), WIDTH)
+        st.begin_p_picture(QP)
+        s_ = drv.ironav_inloop_drive_bands(st.ctx, st.mb_w, NSLICES, bands.ctypes.data, thr, states.ctypes.data, results.ctypes.data)
+        if s_ != 0:
+            raise RuntimeError(f"ironav_inloop_drive_bands: status {s_}")
+        return t
+
+    t = picture(0)
+    assert np.array_equal(states, d_states[t].cpu().numpy().view(MBSTATE_DTYPE)), "in-loop decisions differ from auto mode's"
+
+    def timed(k, host):
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for i in range(k):
+            picture(args.warmup + i, host)
+        torch.cuda.synchronize()
+        return max_over_ranks(time.perf_counter() - t0, world, dev)
+
+    for i in range(args.warmup):
+        picture(i)
+    clocks = Clocks(int(os.environ.get("LOCAL_RANK", "0")))
+    clocks.start()
+    t_load = time.perf_counter()
+    i = 0
+    while time.perf_counter() - t_load < 0.6:
+        picture(i)
+        i += 1
+    el = timed(args.steps, False)
+    clk = clocks.stop()
+    el_host = timed(args.steps, True)
+    total = sum_over_ranks(nmb, world, dev)
+    line = {
+        "metric": "1080p in-loop inter analysis MB/s (the host decides and commits every macroblock)", "value": total * args.steps / el,
+        "unit": "MB/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": data_desc(8),
+        "config": {"workload": f"1080p 8-bit P pictures in in-loop mode, QP {QP}, one reference, {NSLICES} slice bands, one native host "
+                               "thread per band (ironav_inloop_result / decide / ironav_inloop_commit per macroblock)",
+                   "width": WIDTH, "height": HEIGHT, "qp": QP, "slices": NSLICES, "mode": "in-loop",
+                   "l2": f"ring of {ring} pictures; the analysis reads each picture once", "parallelism": "replicas"},
+        "e2e": {"value": total * args.steps / el_host, "unit": "MB/s", "h2d_bytes_per_step": 2 * WIDTH * HEIGHT + nmb * 72,
+                "d2h_bytes_per_step": nmb * 104, "ms_per_step": 1e3 * el_host / args.steps,
+                "note": "the source and reference luma and the reference's decisions through the host-buffer calls each step; "
+                        "results reach the host and commits the device through mapped host memory (counted: one result and one "
+                        "decision per macroblock)"},
+        "gpu_launches": 3 * args.steps,  # per picture: planes (+ co-located vectors), source copy and padding, the in-loop analysis
+        "roofline": {"bound": "latency", "kernel": "analyse_kernel<MODE_INLOOP, uint8_t>", "achieved": None, "peak": None, "unit": None,
+                     "frac": None, "traffic": None,
+                     "note": "each band is a chain of host round trips through mapped memory (commit -> device sees it -> analysis -> "
+                             "result -> host sees it), one per macroblock"},
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_slice_threads(frames, min(args.cpu_seconds, 6.0))
+        line["cpu_slice_threads"] = cpu
+        line["cpu_baseline"] = cpu
+        line["ratio_to_cpu_slice_threads"] = line["value"] / cpu["value"]
+    st.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def run_encode(args, rank, world):
+    """The CAVLC encoder's whole P picture on the device (ironav_b200.encoder.DeviceEncoder.encode_device):
+    scene-cut measure, decide mode (code_mb of every macroblock), the slices written on the device from the
+    codes and their bytes brought back as Annex B NAL units, the filter's records, the deblocking filter, and
+    the filtered picture pushed as the next reference. 1080p, QP 27, one reference, eight bands; the IDR
+    picture is coded first, untimed; one step is one P picture. `value` has the sources in device memory;
+    `e2e` uploads each picture's planes from host memory (DeviceEncoder.encode). Against the oracle's encoder
+    loop (the same steps on the host, the decision on one thread per band)."""
+    import torch
+    import torch.distributed as dist
+    from ironav_b200.encoder import DeviceEncoder, Encoder
+    from ironav_b200.synth import Sequence
+
+    dev = torch.device("cuda", torch.cuda.current_device())
+    n = args.warmup + 2 * args.steps + 2
+    from ironav_b200.synth import CONFIGS
+
+    w, h, seed, pan_q, nobj, vmax, sigma = CONFIGS["1080p"]
+    seq = Sequence(w, h, n, seed + 0x1000 * rank, pan_q, nobj, vmax, sigma)
+    ys = [seq.frame(t) for t in range(n)]
+    cs = [seq.chroma(t) for t in range(n)]
+    d_y = torch.from_numpy(np.stack(ys)).to(dev)
+    d_c = torch.from_numpy(np.stack([np.stack(c) for c in cs])).to(dev)
+    enc = DeviceEncoder(w, h, qp=QP, keyint=10 ** 6, refs=1, nslices=NSLICES)
+    nbytes = [0]
+
+    def picture(t):
+        prev = d_y[t - 1].data_ptr() if t > 0 else None
+        nbytes[0] += len(enc.encode_device(d_y[t].data_ptr(), d_c[t][0].data_ptr(), d_c[t][1].data_ptr(), w, prev))
+
+    picture(0)  # the IDR picture
+    t = 1
+    for _ in range(args.warmup):
+        picture(t)
+        t += 1
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = Clocks(int(os.environ.get("LOCAL_RANK", "0")))
+    clocks.start()
+    nbytes[0] = 0
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        picture(t)
+        t += 1
+    torch.cuda.synchronize()
+    el = max_over_ranks(time.perf_counter() - t0, world, dev)
+    clk = clocks.stop()
+    bits_per_picture = 8.0 * nbytes[0] / args.steps
+    # end to end: each picture's planes uploaded from host memory by the encoder itself
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        enc.encode(ys[t], *cs[t])
+        t += 1
+    el_host = max_over_ranks(time.perf_counter() - t0, world, dev)
+    enc.close()
+    nmb = ((w + 15) // 16) * ((h + 15) // 16)
+    total = sum_over_ranks(nmb, world, dev)
+    line = {
+        "metric": "1080p CAVLC encoding MB/s on the device (decide, slices written, deblocking, next reference)",
+        "value": total * args.steps / el, "unit": "MB/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "data": data_desc(8) + "; chroma from the 2x2 luma means",
+        "config": {"workload": f"1080p 8-bit P pictures through DeviceEncoder.encode_device, QP {QP}, one reference, {NSLICES} slice "
+                               "bands: scene cut, decide mode, CAVLC slices (device writer, NAL framing on the host), records, "
+                               "deblocking, reference planes", "width": w, "height": h, "qp": QP, "slices": NSLICES,
+                   "bits_per_picture": bits_per_picture, "l2": "each picture read once from a ring in device memory",
+                   "parallelism": "replicas"},
+        "e2e": {"value": total * args.steps / el_host, "unit": "MB/s", "h2d_bytes_per_step": w * h * 3 // 2,
+                "d2h_bytes_per_step": int(bits_per_picture / 8), "ms_per_step": 1e3 * el_host / args.steps,
+                "note": "DeviceEncoder.encode: the picture's three planes from host memory, the stream's bytes back"},
+        "gpu_launches": 16 * args.steps,  # per picture: scene cut 2, source copy 1, chroma 2, decide 1, writer 3, records 1, deblocking 2, planes 1, chroma copies 2 (and their padding)
+        "roofline": {"bound": "latency", "kernel": "decide_kernel<uint8_t>", "achieved": None, "peak": None, "unit": None, "frac": None,
+                     "traffic": None, "note": "one stream's decide wavefront (a chain of ~136 dependent macroblocks) bounds the picture"},
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from tests.oracle_lib import oracle_library
+
+        lib = oracle_library()
+        threads = min(host_cores(), NSLICES)
+        o = Encoder(w, h, qp=QP, keyint=10 ** 6, refs=1, nslices=NSLICES, lib=lib)
+        lib.oracle_set_threads(o.st.ctx, threads)
+        o.encode(ys[0], *cs[0])
+        k, t0, el_o = 1, time.perf_counter(), 0.0
+        while el_o < min(args.cpu_seconds, 6.0) and k < n:
+            o.encode(ys[k], *cs[k])
+            k += 1
+            el_o = time.perf_counter() - t0
+        o.close()
+        line["cpu_baseline"] = {"value": (k - 1) * nmb / el_o, "unit": "MB/s", "cores": threads, "kind": "port",
+                                "sample": f"{k - 1} P pictures of the same sequence through the oracle's encoder loop (host buffers), "
+                                          f"decide mode on {threads} threads, {el_o:.2f} s"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
 
 
 def run_batched(args, rank, world):

@@ -3,6 +3,7 @@
 - libironav_inter_cuda.so: the sm_100a kernels and the C ABI of include/ironav_inter.h
   (nvcc -gencode arch=compute_100a,code=sm_100a; nvcc cross-compiles without a GPU).
 - libironav_synth.so: the seeded synthetic sequence generator (host C++).
+- libironav_inloop_caller.so: a native caller of in-loop mode (host C++ over the CUDA library's C ABI).
 
 Run `python -m ironav_b200.build` (or call build_all()) before importing the bindings.
 """
@@ -20,6 +21,7 @@ CSRC = os.path.join(PKG, "csrc")
 
 CUDA_LIB = os.path.join(LIB, "libironav_inter_cuda.so")
 SYNTH_LIB = os.path.join(LIB, "libironav_synth.so")
+INLOOP_LIB = os.path.join(LIB, "libironav_inloop_caller.so")
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -76,9 +78,20 @@ def build_synth(force: bool = False) -> str:
     return SYNTH_LIB
 
 
+def build_inloop_caller(force: bool = False) -> str:
+    """libironav_inloop_caller.so: a native caller of in-loop mode (one thread per slice band), linked
+    against the CUDA library (found next to it at run time)."""
+    src = os.path.join(CSRC, "inloop_caller.cpp")
+    if force or _stale(INLOOP_LIB, [src, CUDA_LIB]):
+        subprocess.run([_gxx(), "-O2", "-std=c++17", "-shared", "-fPIC", "-pthread", src, "-L" + LIB, "-lironav_inter_cuda",
+                        "-Wl,-rpath,$ORIGIN", "-o", INLOOP_LIB], check=True)
+    return INLOOP_LIB
+
+
 def build_all(force: bool = False, verbose: bool = False) -> None:
     build_synth(force)
     build_cuda(force, verbose)
+    build_inloop_caller(force)
 
 
 if __name__ == "__main__":

@@ -150,24 +150,30 @@ class DeviceEncoder:
                   non_blocking=False)
 
     def encode(self, y: np.ndarray, cb: np.ndarray, cr: np.ndarray) -> bytes:
-        torch, st, L, lib = self.torch, self.st, self.loop, self.lib
-        w, h = st.width, st.height
-        cur, prev = self.d_src[self.k], self.d_src[self.k ^ 1]
-        with torch.cuda.stream(self.stream):
+        """Codes a picture given as host arrays: its planes go up to the encoder's own device buffers first."""
+        cur = self.d_src[self.k]
+        with self.torch.cuda.stream(self.stream):
             self._up(cur, y)
             self._up(self.d_src_c[0], cb)
             self._up(self.d_src_c[1], cr)
-        cut = False
-        if self.scene_cut and L.count > 0:
-            out = np.zeros(2, dtype=np.int64)
-            self._check(lib.ironav_scene_change_device(st.ctx, prev.data_ptr(), cur.data_ptr(), w, out.ctypes.data),
-                        "ironav_scene_change_device")
-            cut = float(out[0]) > SCENE_CUT * float(out[1])  # enc/mod.rs:707-711
+        prev = self.d_src[self.k ^ 1].data_ptr() if self.loop.count > 0 else None
         self.k ^= 1
+        return self.encode_device(cur.data_ptr(), self.d_src_c[0].data_ptr(), self.d_src_c[1].data_ptr(), self.st.width, prev)
+
+    def encode_device(self, d_y: int, d_cb: int, d_cr: int, stride: int, d_prev_y: int | None) -> bytes:
+        """Codes a picture already in device memory (luma width x height and chroma half that, rows `stride`
+        and `stride // 2` samples apart, on or ordered before the encoder's stream); d_prev_y is the previous
+        picture's luma for the scene-cut measure (None for the first). Returns the picture's Annex B bytes."""
+        st, L, lib = self.st, self.loop, self.lib
+        w = st.width
+        cut = False
+        if self.scene_cut and d_prev_y is not None:
+            out = np.zeros(2, dtype=np.int64)
+            self._check(lib.ironav_scene_change_device(st.ctx, d_prev_y, d_y, stride, out.ctypes.data), "ironav_scene_change_device")
+            cut = float(out[0]) > SCENE_CUT * float(out[1])  # enc/mod.rs:707-711
         idr = L.choose(cut)
-        st.set_source_device(cur.data_ptr(), w)
-        self._check(lib.ironav_set_source_chroma_device(st.ctx, self.d_src_c[0].data_ptr(), self.d_src_c[1].data_ptr(), w // 2),
-                    "ironav_set_source_chroma_device")
+        st.set_source_device(d_y, stride)
+        self._check(lib.ironav_set_source_chroma_device(st.ctx, d_cb, d_cr, stride // 2), "ironav_set_source_chroma_device")
         qpp = L.qp_prime(idr)
         pw, cw = st.mb_w * 16, st.mb_w * 8
         ry, rc, sts, codes = self.d_rec, self.d_rec_c, self.d_states, self.d_codes

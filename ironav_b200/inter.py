@@ -289,6 +289,23 @@ def cuda_library() -> ctypes.CDLL:
     return _CUDA
 
 
+_INLOOP_CALLER = None
+
+
+def inloop_caller() -> ctypes.CDLL:
+    """The native in-loop caller (libironav_inloop_caller.so): ironav_inloop_drive_bands(ctx, mb_w, nbands,
+    band_rows, skip_thresh, states, results) runs one P picture with one host thread per slice band."""
+    global _INLOOP_CALLER
+    if _INLOOP_CALLER is None:
+        from . import build
+
+        cuda_library()
+        lib = ctypes.CDLL(build.INLOOP_LIB)
+        lib.ironav_inloop_drive_bands.argtypes = [_VP, _I, _I, _VP, _I, _VP, _VP]
+        _INLOOP_CALLER = lib
+    return _INLOOP_CALLER
+
+
 def load_library(path: str) -> ctypes.CDLL:
     """Another implementation of include/ironav_inter.h (same entry points, same meaning)."""
     return _declare(ctypes.CDLL(path))

@@ -117,3 +117,28 @@ def test_inloop_wait_for_a_commit_that_never_comes_times_out(cuda_lib):
     # the context is usable afterwards
     states, results = c.analyse_auto()
     assert results["skip_sad"].sum() > 0
+
+
+@pytest.mark.gpu
+def test_native_band_threads_drive_the_picture(oracle_lib, cuda_lib):
+    """The native caller (libironav_inloop_caller.so: one C++ thread per slice band, as the encoder's slice
+    threads) under the analysis policy: its decisions equal the oracle's auto mode and its results the
+    oracle's replay of them, at 1080p with eight bands."""
+    from ironav_b200.inter import default_bands, inloop_caller
+
+    seq = Sequence.config("1080p", 2)
+    c = InterStage(1920, 1080, nslices=8, lib=cuda_lib)
+    o = InterStage(1920, 1080, nslices=8, lib=oracle_lib)
+    for st in (c, o):
+        st.push_reference(seq.frame(0))
+        st.set_source(seq.frame(1))
+        st.begin_p_picture(27)
+    bands = np.asarray(default_bands(c.mb_h, 8), dtype=np.int32)
+    states = np.zeros(c.nmb, dtype=MBSTATE_DTYPE)
+    results = np.zeros(c.nmb, dtype=MBRESULT_DTYPE)
+    s = inloop_caller().ironav_inloop_drive_bands(c.ctx, c.mb_w, 8, bands.ctypes.data, cuda_lib.ironav_skip_threshold(27),
+                                                  states.ctypes.data, results.ctypes.data)
+    assert s == 0
+    auto_states, _ = o.analyse_auto()
+    assert np.array_equal(states, auto_states)
+    assert np.array_equal(results, o.analyse_replay(states))
