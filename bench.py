@@ -757,6 +757,11 @@ def run_batched(args, rank, world):
 
     clocks = Clocks(int(os.environ.get("LOCAL_RANK", "0")))
     clocks.start()
+    ms_fixed = timed(batched, args.steps)  # the default setting (4 CTAs an SM, 16-row plane tiles, order 0)
+    batch.sync()
+    # the project's tuner: every setting timed on this mix (untimed here), the fastest kept
+    with torch.cuda.stream(stream):
+        tune = batch.autotune(*args_of(args.warmup + args.steps), reps=5)
     ms_b = timed(batched, args.steps)
     batch.sync()
     ms_p = timed(plain, args.steps)
@@ -799,6 +804,9 @@ def run_batched(args, rank, world):
         "graph": {"value": nmb * args.steps / (ms_g * 1e-3), "ms_per_step": ms_g / args.steps,
                   "note": "the batched step captured once in a CUDA graph and replayed (rank 0's streams alone)"},
         "speedup_vs_plain_loop": ms_p / ms_b,
+        "autotune": {"best": tune["best"], "fixed_value": mbs(ms_fixed), "fixed_ms_per_step": ms_fixed / args.steps,
+                     "tuned_vs_fixed": ms_fixed / ms_b, "settings": tune["all"],
+                     "note": "value is the tuned setting's; fixed is the default (4 CTAs an SM, 16-row plane tiles, order 0)"},
         "clocks": clk,
     }
     del g

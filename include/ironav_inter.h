@@ -491,6 +491,30 @@ int ironav_batch_deblock(ironav_batch* batch, void* const* d_y, const int* y_str
                          const int* c_strides, const ironav_dbk_mb* const* d_mbs, const ironav_dbk_slice* const* slices,
                          const int* nslices);
 
+/* The batched step's tuning: no counterpart in the reference (its analysis runs on host threads with
+ * nothing to tune). The knobs are the analysis launch's CTAs per SM (4, 5 or 6; its register cap becomes
+ * 128, 96 or 80 a thread: more warps in flight against more spills), the half-sample planes' tile rows
+ * (16 or 8) and the ticket order of the merged wavefronts (0: ties between streams by stream index; 1: by
+ * stream size, largest first). The default is 4, 16, 0. Every setting gives the same results; only the
+ * time changes. */
+typedef struct ironav_batch_tuning {
+    int32_t k2_ctas_per_sm;
+    int32_t k1_tile_rows;
+    int32_t order;
+    float ms;                    /* ironav_batch_autotune: the setting's median step time (milliseconds) */
+} ironav_batch_tuning;
+int ironav_batch_set_tuning(ironav_batch* batch, const ironav_batch_tuning* t);
+int ironav_batch_get_tuning(const ironav_batch* batch, ironav_batch_tuning* t);
+/* Times every setting (3 x 2 x 2) on `reps` batched steps of these inputs (arguments as ironav_batch_step's;
+ * CUDA events on the batch's stream, after a warm-up step each), keeps the fastest by median and returns it
+ * in best (and, when all is not NULL, up to cap settings with their times, *n_all of them). Each context's
+ * reference ring is put back before every step, so the batch ends exactly as after one ironav_batch_step
+ * with these inputs: call it in place of a step. Synchronous. */
+int ironav_batch_autotune(ironav_batch* batch, const void* const* d_src, const void* const* d_ref,
+                          const ironav_mbstate* const* d_col, ironav_mbstate* const* d_states,
+                          ironav_mbresult* const* d_results, int reps, ironav_batch_tuning* best,
+                          ironav_batch_tuning* all, int cap, int* n_all);
+
 /* ---- analysis without allocation ------------------------------------------------------------------ */
 
 /* No counterpart in the reference: an entry point for callers that cannot allocate device memory (a

@@ -26,8 +26,9 @@ INLOOP_LIB = os.path.join(LIB, "libironav_inloop_caller.so")
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo", "-O3", "-std=c++17",
-    "-shared", "-Xcompiler", "-fPIC,-O3",
+    "-Xcompiler", "-fPIC,-O3",
 ]
+UNITS = ["ironav_inter.cu", "ironav_batch.cu", "ironav_noalloc.cu", "ironav_stream.cu"]
 
 
 def _nvcc() -> str:
@@ -59,14 +60,24 @@ def _sources(exts: tuple[str, ...]) -> list[str]:
 
 
 def build_cuda(force: bool = False, verbose: bool = False) -> str:
+    """Compiles each translation unit to an object (in parallel), then links the shared library."""
     deps = _sources((".cu", ".cuh"))
     if force or _stale(CUDA_LIB, deps):
+        from concurrent.futures import ThreadPoolExecutor
+
         os.makedirs(LIB, exist_ok=True)
-        units = ["ironav_inter.cu", "ironav_batch.cu", "ironav_noalloc.cu", "ironav_stream.cu"]
-        cmd = [_nvcc(), *NVCC_FLAGS, *[os.path.join(CSRC, u) for u in units], "-o", CUDA_LIB]
-        if verbose:
-            cmd.insert(1, "-Xptxas=-v")
-        subprocess.run(cmd, check=True)
+        objdir = os.path.join(PKG, "_build")
+        os.makedirs(objdir, exist_ok=True)
+
+        def compile_unit(u: str) -> str:
+            obj = os.path.join(objdir, u.replace(".cu", ".o"))
+            cmd = [_nvcc(), *NVCC_FLAGS, *(["-Xptxas=-v"] if verbose else []), "-c", os.path.join(CSRC, u), "-o", obj]
+            subprocess.run(cmd, check=True)
+            return obj
+
+        with ThreadPoolExecutor(max_workers=len(UNITS)) as pool:
+            objs = list(pool.map(compile_unit, UNITS))
+        subprocess.run([_nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", *objs, "-o", CUDA_LIB], check=True)
     return CUDA_LIB
 
 

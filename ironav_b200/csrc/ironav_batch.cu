@@ -51,16 +51,17 @@ __device__ __forceinline__ int find_job(const Job* jobs, int n, int idx, Key key
     return lo;
 }
 
-template <class T>
-__global__ void __launch_bounds__(K1_THREADS) planes_batch_kernel(const PlaneJob* __restrict__ jobs, int njobs, int maxv) {
+// TH: the tiles' rows (the tuner's choice, 16 or 8), 16 * TH threads a CTA.
+template <class T, int TH>
+__global__ void __launch_bounds__(16 * TH) planes_batch_kernel(const PlaneJob* __restrict__ jobs, int njobs, int maxv) {
     const int j = find_job(jobs, njobs, (int)blockIdx.x, [](const PlaneJob& p) { return p.tile0; });
     const PlaneJob& J = jobs[j];
     const int t = (int)blockIdx.x - J.tile0;
     if constexpr (sizeof(T) == 1)
-        planes_tile8(J.luma, J.stride, J.w, J.h, J.out, J.psize, J.sw, J.sh, (t % J.tiles_x) * K1_TW, (t / J.tiles_x) * K1_TH);
+        planes_tile8<TH>(J.luma, J.stride, J.w, J.h, J.out, J.psize, J.sw, J.sh, (t % J.tiles_x) * K1_TW, (t / J.tiles_x) * TH);
     else
-        planes_tile16(reinterpret_cast<const uint16_t*>(J.luma), J.stride, J.w, J.h, reinterpret_cast<uint16_t*>(J.out), J.psize, J.sw,
-                      J.sh, (t % J.tiles_x) * K1_TW, (t / J.tiles_x) * K1_TH, maxv);
+        planes_tile16<TH>(reinterpret_cast<const uint16_t*>(J.luma), J.stride, J.w, J.h, reinterpret_cast<uint16_t*>(J.out), J.psize,
+                          J.sw, J.sh, (t % J.tiles_x) * K1_TW, (t / J.tiles_x) * TH, maxv);
 }
 
 // col_mv, enc/frame.rs:944-947, for every stream's new reference
@@ -93,9 +94,10 @@ __global__ void source_batch_kernel(const SrcJob* __restrict__ jobs, int njobs) 
     for (int x = threadIdx.x; x < J.pw; x += blockDim.x) out[x] = row[min(x, J.w - 1)];
 }
 
-// Every stream's auto-mode analysis in one launch (each stream's parameters in the table).
-template <class T>
-__global__ void __launch_bounds__(K2_WARPS * 32, K2_MIN_BLOCKS) analyse_batch_kernel(const AnalyseParams* __restrict__ table,
+// Every stream's auto-mode analysis in one launch (each stream's parameters in the table). MINB: the CTAs
+// an SM must hold (the tuner's choice, 4 to 6), which caps the registers a thread at 128, 96 or 80.
+template <class T, int MINB>
+__global__ void __launch_bounds__(K2_WARPS * 32, MINB) analyse_batch_kernel(const AnalyseParams* __restrict__ table,
                                                                                      const uint32_t* __restrict__ order,
                                                                                      unsigned ntickets, unsigned* ticket,
                                                                                      const unsigned* err) {
@@ -145,13 +147,22 @@ int cuda_status(cudaError_t e) {
 
 }  // namespace
 
+// The batched step's knobs (ironav_batch_tuning): the analysis' CTAs per SM (4, 5 or 6: its register cap),
+// the planes' tile rows (16 or 8) and the ticket order (0: the merged wavefront, ties by stream; 1: ties
+// by stream size, largest first).
+constexpr int TUNE_MINB[3] = {4, 5, 6};
+constexpr int TUNE_TH[2] = {16, 8};
+
 struct ironav_batch {
     std::vector<ironav_ctx*> ctx;
     cudaStream_t stream = nullptr;
     int bd = 8;  // every stream's sample depth
     int n = 0, total_mbs = 0, total_tiles = 0, total_rows = 0, k2_blocks = 0;
+    int tiles_th[2] = {0, 0};  // the planes' tiles at each tile height
+    int k2_blocks_v[3] = {0, 0, 0};  // the analysis' persistent grid for each CTAs-per-SM variant
+    int minb_i = 0, th_i = 0, order_i = 0;  // the current tuning (indices into TUNE_MINB, TUNE_TH; the order)
     std::vector<int> mb0;  // each stream's first flag
-    uint32_t* d_order = nullptr;
+    uint32_t* d_order = nullptr;  // the two ticket orders, total_mbs each
     unsigned* d_flags = nullptr;
     unsigned* d_counters = nullptr;  // [0] ticket, [1] error
     PlaneJob* d_pjobs = nullptr;
@@ -212,24 +223,30 @@ extern "C" int ironav_batch_create(ironav_batch** out, ironav_ctx* const* ctxs, 
     b->n = n;
     b->stream = ctxs[0]->stream;
     b->bd = ctxs[0]->bd;
-    // the streams' wavefronts merged: key x + 2 * (y - band start), then stream, then raster
-    std::vector<std::tuple<int, int, int>> keys;
+    // the streams' wavefronts merged: key x + 2 * (y - band start), then (order 0) stream or (order 1) the
+    // stream's size, largest first, then stream, then raster
+    std::vector<std::tuple<int, int, int, int>> keys[2];
     for (int i = 0; i < n; i++) {
         const ironav_ctx* c = ctxs[i];
         std::vector<int> start(c->mb_h);
         cudaMemcpy(start.data(), c->d_band_start, sizeof(int) * c->mb_h, cudaMemcpyDeviceToHost);
         b->mb0.push_back(b->total_mbs);
         for (int m = 0; m < c->nmb; m++) {
-            const int x = m % c->mb_w, y = m / c->mb_w;
-            keys.emplace_back(x + 2 * (y - start[y]), i, m);
+            const int x = m % c->mb_w, y = m / c->mb_w, k = x + 2 * (y - start[y]);
+            keys[0].emplace_back(k, i, i, m);
+            keys[1].emplace_back(k, -c->nmb, i, m);
         }
         b->total_mbs += c->nmb;
-        b->total_tiles += ((c->sw + K1_TW - 1) / K1_TW) * ((c->sh + K1_TH - 1) / K1_TH);
+        for (int v = 0; v < 2; v++) b->tiles_th[v] += ((c->sw + K1_TW - 1) / K1_TW) * ((c->sh + TUNE_TH[v] - 1) / TUNE_TH[v]);
         b->total_rows += c->ph;
     }
-    std::sort(keys.begin(), keys.end());
-    std::vector<uint32_t> order(keys.size());
-    for (size_t k = 0; k < keys.size(); k++) order[k] = ((uint32_t)std::get<1>(keys[k]) << 20) | (uint32_t)std::get<2>(keys[k]);
+    b->total_tiles = b->tiles_th[0];
+    std::vector<uint32_t> order(2 * (size_t)b->total_mbs);
+    for (int v = 0; v < 2; v++) {
+        std::sort(keys[v].begin(), keys[v].end());
+        for (size_t k = 0; k < keys[v].size(); k++)
+            order[v * (size_t)b->total_mbs + k] = ((uint32_t)std::get<2>(keys[v][k]) << 20) | (uint32_t)std::get<3>(keys[v][k]);
+    }
     auto fail = [&](cudaError_t e) {
         const int s = cuda_status(e);
         free_batch(b);
@@ -248,11 +265,20 @@ extern "C" int ironav_batch_create(ironav_batch** out, ironav_ctx* const* ctxs, 
     if ((e = cudaHostAlloc(&b->h_sjobs, sizeof(SrcJob) * n, cudaHostAllocDefault)) != cudaSuccess) return fail(e);
     if ((e = cudaHostAlloc(&b->h_table, sizeof(AnalyseParams) * n, cudaHostAllocDefault)) != cudaSuccess) return fail(e);
     if ((e = cudaEventCreateWithFlags(&b->copied, cudaEventDisableTiming)) != cudaSuccess) return fail(e);
-    int per_sm = 0;
-    if ((e = b->bd > 8 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, analyse_batch_kernel<uint16_t>, K2_WARPS * 32, 0)
-                       : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, analyse_batch_kernel<uint8_t>, K2_WARPS * 32, 0)) != cudaSuccess)
-        return fail(e);
-    b->k2_blocks = std::max(1, per_sm) * ctxs[0]->nsm;
+    // the persistent grid of each analysis variant: every CTA the occupancy allows
+    for (int v = 0; v < 3; v++) {
+        int per_sm = 0;
+        const void* fn = nullptr;
+        if (b->bd > 8)
+            fn = v == 0 ? (const void*)analyse_batch_kernel<uint16_t, 4> : v == 1 ? (const void*)analyse_batch_kernel<uint16_t, 5>
+                                                                                  : (const void*)analyse_batch_kernel<uint16_t, 6>;
+        else
+            fn = v == 0 ? (const void*)analyse_batch_kernel<uint8_t, 4> : v == 1 ? (const void*)analyse_batch_kernel<uint8_t, 5>
+                                                                                 : (const void*)analyse_batch_kernel<uint8_t, 6>;
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, K2_WARPS * 32, 0)) != cudaSuccess) return fail(e);
+        b->k2_blocks_v[v] = std::max(1, per_sm) * ctxs[0]->nsm;
+    }
+    b->k2_blocks = b->k2_blocks_v[0];
     *out = b;
     return IRONAV_OK;
 }
@@ -291,11 +317,12 @@ extern "C" int ironav_batch_step(ironav_batch* b, const void* const* d_src, cons
         pj.sh = c->sh;
         pj.tiles_x = (c->sw + K1_TW - 1) / K1_TW;
         pj.tile0 = tile;
+        const int th = TUNE_TH[b->th_i];
         pj.col_states = d_col ? d_col[i] : nullptr;
         pj.col = c->d_col[slot];
         pj.nmb = c->nmb;
         pj.mb0 = b->mb0[i];
-        tile += pj.tiles_x * ((c->sh + K1_TH - 1) / K1_TH);
+        tile += pj.tiles_x * ((c->sh + th - 1) / th);
         SrcJob& sj = b->h_sjobs[i];
         sj.src = static_cast<const uint8_t*>(d_src[i]);
         sj.stride = c->width;
@@ -320,23 +347,141 @@ extern "C" int ironav_batch_step(ironav_batch* b, const void* const* d_src, cons
     CK(cudaMemcpyAsync(b->d_table, b->h_table, sizeof(AnalyseParams) * b->n, cudaMemcpyHostToDevice, b->stream));
     CK(cudaEventRecord(b->copied, b->stream));
     b->pending = true;
+    const int tiles = b->tiles_th[b->th_i], maxv = (1 << b->bd) - 1;
     if (b->bd > 8) {
         source_batch_kernel<uint16_t><<<b->total_rows, 128, 0, b->stream>>>(b->d_sjobs, b->n);
-        planes_batch_kernel<uint16_t><<<b->total_tiles, K1_THREADS, 0, b->stream>>>(b->d_pjobs, b->n, (1 << b->bd) - 1);
+        if (b->th_i == 0) planes_batch_kernel<uint16_t, 16><<<tiles, 16 * 16, 0, b->stream>>>(b->d_pjobs, b->n, maxv);
+        else planes_batch_kernel<uint16_t, 8><<<tiles, 16 * 8, 0, b->stream>>>(b->d_pjobs, b->n, maxv);
     } else {
         source_batch_kernel<uint8_t><<<b->total_rows, 128, 0, b->stream>>>(b->d_sjobs, b->n);
-        planes_batch_kernel<uint8_t><<<b->total_tiles, K1_THREADS, 0, b->stream>>>(b->d_pjobs, b->n, 255);
+        if (b->th_i == 0) planes_batch_kernel<uint8_t, 16><<<tiles, 16 * 16, 0, b->stream>>>(b->d_pjobs, b->n, maxv);
+        else planes_batch_kernel<uint8_t, 8><<<tiles, 16 * 8, 0, b->stream>>>(b->d_pjobs, b->n, maxv);
     }
     col_batch_kernel<<<(b->total_mbs + 255) / 256, 256, 0, b->stream>>>(b->d_pjobs, b->n, b->total_mbs);
     CK(cudaMemsetAsync(b->d_flags, 0, sizeof(unsigned) * b->total_mbs, b->stream));
     CK(cudaMemsetAsync(b->d_counters, 0, sizeof(unsigned) * 2, b->stream));
-    if (b->bd > 8)
-        analyse_batch_kernel<uint16_t><<<b->k2_blocks, K2_WARPS * 32, 0, b->stream>>>(b->d_table, b->d_order, (unsigned)b->total_mbs,
-                                                                                      b->d_counters, b->d_counters + 1);
-    else
-        analyse_batch_kernel<uint8_t><<<b->k2_blocks, K2_WARPS * 32, 0, b->stream>>>(b->d_table, b->d_order, (unsigned)b->total_mbs,
-                                                                                     b->d_counters, b->d_counters + 1);
+    const uint32_t* order = b->d_order + (size_t)b->order_i * b->total_mbs;
+    const unsigned nt = (unsigned)b->total_mbs;
+    const int grid = b->k2_blocks_v[b->minb_i];
+    unsigned* tk = b->d_counters;
+    const unsigned* er = b->d_counters + 1;
+    if (b->bd > 8) {
+        if (b->minb_i == 0) analyse_batch_kernel<uint16_t, 4><<<grid, K2_WARPS * 32, 0, b->stream>>>(b->d_table, order, nt, tk, er);
+        else if (b->minb_i == 1) analyse_batch_kernel<uint16_t, 5><<<grid, K2_WARPS * 32, 0, b->stream>>>(b->d_table, order, nt, tk, er);
+        else analyse_batch_kernel<uint16_t, 6><<<grid, K2_WARPS * 32, 0, b->stream>>>(b->d_table, order, nt, tk, er);
+    } else {
+        if (b->minb_i == 0) analyse_batch_kernel<uint8_t, 4><<<grid, K2_WARPS * 32, 0, b->stream>>>(b->d_table, order, nt, tk, er);
+        else if (b->minb_i == 1) analyse_batch_kernel<uint8_t, 5><<<grid, K2_WARPS * 32, 0, b->stream>>>(b->d_table, order, nt, tk, er);
+        else analyse_batch_kernel<uint8_t, 6><<<grid, K2_WARPS * 32, 0, b->stream>>>(b->d_table, order, nt, tk, er);
+    }
     return cuda_status(cudaGetLastError());
+}
+
+// ---- the batched step's tuner ---------------------------------------------------------------------------
+
+static int tuning_index(const ironav_batch_tuning* t, int* mi, int* ti) {
+    *mi = -1;
+    *ti = -1;
+    for (int v = 0; v < 3; v++)
+        if (t->k2_ctas_per_sm == TUNE_MINB[v]) *mi = v;
+    for (int v = 0; v < 2; v++)
+        if (t->k1_tile_rows == TUNE_TH[v]) *ti = v;
+    return (*mi < 0 || *ti < 0 || t->order < 0 || t->order > 1) ? IRONAV_INVALID_ARGUMENT : IRONAV_OK;
+}
+
+extern "C" int ironav_batch_set_tuning(ironav_batch* b, const ironav_batch_tuning* t) {
+    if (!b || !t) return IRONAV_INVALID_ARGUMENT;
+    int mi, ti;
+    if (tuning_index(t, &mi, &ti) != IRONAV_OK) return IRONAV_INVALID_ARGUMENT;
+    b->minb_i = mi;
+    b->th_i = ti;
+    b->order_i = t->order;
+    return IRONAV_OK;
+}
+
+extern "C" int ironav_batch_get_tuning(const ironav_batch* b, ironav_batch_tuning* t) {
+    if (!b || !t) return IRONAV_INVALID_ARGUMENT;
+    t->k2_ctas_per_sm = TUNE_MINB[b->minb_i];
+    t->k1_tile_rows = TUNE_TH[b->th_i];
+    t->order = b->order_i;
+    t->ms = 0.f;
+    return IRONAV_OK;
+}
+
+// Every candidate setting (the analysis' CTAs per SM x the planes' tile rows x the ticket order) timed on
+// `reps` batched steps of the caller's inputs with CUDA events on the batch's stream; the fastest (the
+// least median) is kept. Before each step every context's reference ring is put back as it was, so the
+// steps all take the same slot and the batch ends exactly as after one ironav_batch_step with these inputs.
+extern "C" int ironav_batch_autotune(ironav_batch* b, const void* const* d_src, const void* const* d_ref,
+                                     const ironav_mbstate* const* d_col, ironav_mbstate* const* d_states,
+                                     ironav_mbresult* const* d_results, int reps, ironav_batch_tuning* best,
+                                     ironav_batch_tuning* all, int cap, int* n_all) {
+    if (!b || reps < 1 || reps > 64 || !best) return IRONAV_INVALID_ARGUMENT;
+    struct Ring {
+        int nrefs;
+        int slot_of[MAX_REFS];
+    };
+    std::vector<Ring> rings(b->n);
+    for (int i = 0; i < b->n; i++) {
+        rings[i].nrefs = b->ctx[i]->nrefs;
+        memcpy(rings[i].slot_of, b->ctx[i]->slot_of, sizeof(rings[i].slot_of));
+    }
+    auto restore = [&] {
+        for (int i = 0; i < b->n; i++) {
+            b->ctx[i]->nrefs = rings[i].nrefs;
+            memcpy(b->ctx[i]->slot_of, rings[i].slot_of, sizeof(rings[i].slot_of));
+        }
+    };
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    int count = 0, bm = 0, bt = 0, bo = 0;
+    float best_ms = 0.f;
+    int status = IRONAV_OK;
+    for (int mi = 0; mi < 3 && status == IRONAV_OK; mi++)
+        for (int ti = 0; ti < 2 && status == IRONAV_OK; ti++)
+            for (int oi = 0; oi < 2 && status == IRONAV_OK; oi++) {
+                b->minb_i = mi;
+                b->th_i = ti;
+                b->order_i = oi;
+                std::vector<float> ms(reps + 1);
+                for (int r = 0; r <= reps && status == IRONAV_OK; r++) {  // the first step is a warm-up
+                    restore();
+                    cudaEventRecord(e0, b->stream);
+                    status = ironav_batch_step(b, d_src, d_ref, d_col, d_states, d_results);
+                    cudaEventRecord(e1, b->stream);
+                    if (status == IRONAV_OK) status = ironav_batch_sync(b);
+                    if (status == IRONAV_OK && cudaEventElapsedTime(&ms[r], e0, e1) != cudaSuccess) status = IRONAV_INTERNAL;
+                }
+                if (status != IRONAV_OK) break;
+                std::sort(ms.begin() + 1, ms.end());
+                const float med = ms[1 + reps / 2];
+                if (all && count < cap) {
+                    all[count].k2_ctas_per_sm = TUNE_MINB[mi];
+                    all[count].k1_tile_rows = TUNE_TH[ti];
+                    all[count].order = oi;
+                    all[count].ms = med;
+                }
+                if (count == 0 || med < best_ms) {
+                    best_ms = med;
+                    bm = mi;
+                    bt = ti;
+                    bo = oi;
+                }
+                count++;
+            }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    b->minb_i = bm;
+    b->th_i = bt;
+    b->order_i = bo;
+    if (n_all) *n_all = count;
+    if (status != IRONAV_OK) return status;
+    best->k2_ctas_per_sm = TUNE_MINB[bm];
+    best->k1_tile_rows = TUNE_TH[bt];
+    best->order = bo;
+    best->ms = best_ms;
+    return IRONAV_OK;
 }
 
 extern "C" int ironav_batch_sync(ironav_batch* b) {

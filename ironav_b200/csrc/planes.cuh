@@ -40,9 +40,12 @@ constexpr int K1_GW = 48;  // staged row pitch in words: 48 = 16 mod 32 banks, s
 // Every plane is written a 32-bit word (four samples) at a time. Samples outside the w x h picture
 // repeat its edges: both the macroblock padding of H264Encoder::source (enc/mod.rs:502-519) when w x h is
 // the picture size and the plane border of round1 (enc/subpel.rs:72-76).
+// TH: the tile's rows (16 by default; the batched form's tuner may pick 8), with 16 * TH threads.
+template <int TH = K1_TH>
 __device__ __forceinline__ void planes_tile8(const uint8_t* __restrict__ luma, int stride, int w, int h, uint8_t* __restrict__ out,
                                              long long psize, int sw, int sh, int x0, int y0) {
-    constexpr int GR = K1_TH + 5, GWORDS = (K1_TW + 8) / 4;  // 21 rows of 18 words: samples x0-4 .. x0+67
+    constexpr int NT = 16 * TH;                           // threads: 16 groups of four columns x TH rows
+    constexpr int GR = TH + 5, GWORDS = (K1_TW + 8) / 4;  // TH + 5 rows of 18 words: samples x0-4 .. x0+67
     __shared__ uint32_t g[GR][K1_GW];
     __shared__ __align__(16) int b1[GR][K1_TW];
     const int tid = threadIdx.x;
@@ -51,7 +54,7 @@ __device__ __forceinline__ void planes_tile8(const uint8_t* __restrict__ luma, i
     const bool fast = x0 - 4 - PAD >= 0 && x0 + 4 * GWORDS - 5 - PAD <= w - 1 && x0 + 4 * GWORDS - 5 <= sw - 1 &&
                       y0 - 2 - PAD >= 0 && y0 + GR - 3 - PAD <= h - 1 &&
                       ((reinterpret_cast<uintptr_t>(luma) | (uintptr_t)stride) & 3) == 0;
-    for (int i = tid; i < GR * GWORDS; i += K1_THREADS) {
+    for (int i = tid; i < GR * GWORDS; i += NT) {
         const int r = i / GWORDS, k = i % GWORDS;
         uint32_t v = 0;
         if (fast) {
@@ -69,7 +72,7 @@ __device__ __forceinline__ void planes_tile8(const uint8_t* __restrict__ luma, i
     __syncthreads();
     // the unrounded horizontal sums of columns x0 + 4q .. +3 of every staged row (only 2 <= x < sw - 3,
     // enc/subpel.rs:78-82; elsewhere 0); the 6-tap window of column X + j starts at byte 2 + j of word q
-    for (int i = tid; i < GR * (K1_TW / 4); i += K1_THREADS) {
+    for (int i = tid; i < GR * (K1_TW / 4); i += NT) {
         const int r = i / (K1_TW / 4), q = i % (K1_TW / 4);
         const uint32_t w0 = g[r][q], w1 = g[r][q + 1], w2 = g[r][q + 2];
         int4 v;
@@ -142,16 +145,18 @@ __device__ __forceinline__ int k1_tap6_pairs(uint32_t p01, uint32_t p23, uint32_
 // pairs (realigned by a 16-bit funnel shift for odd columns, gathered across rows with prmt for the
 // vertical taps), the diagonal taps on the unrounded horizontal sums, and one 64-bit store per plane.
 // Same values as planes_tile8 at 8 bits; half samples are clipped to maxv = 2^bd - 1.
+template <int TH = K1_TH>
 __device__ __forceinline__ void planes_tile16(const uint16_t* __restrict__ luma, int stride, int w, int h, uint16_t* __restrict__ out,
                                               long long psize, int sw, int sh, int x0, int y0, int maxv) {
-    constexpr int GR = K1_TH + 5, GWORDS = (K1_TW + 8) / 2;  // 21 rows of 36 words: samples x0-4 .. x0+67
+    constexpr int NT = 16 * TH;
+    constexpr int GR = TH + 5, GWORDS = (K1_TW + 8) / 2;  // TH + 5 rows of 36 words: samples x0-4 .. x0+67
     __shared__ __align__(16) uint32_t g[GR][K1_GW];
     __shared__ __align__(16) int b1[GR][K1_TW];
     const int tid = threadIdx.x;
     const bool fast = x0 - 4 - PAD >= 0 && x0 + 2 * GWORDS - 5 - PAD <= w - 1 && x0 + 2 * GWORDS - 5 <= sw - 1 &&
                       y0 - 2 - PAD >= 0 && y0 + GR - 3 - PAD <= h - 1 &&
                       (reinterpret_cast<uintptr_t>(luma) & 3) == 0 && (stride & 1) == 0;
-    for (int i = tid; i < GR * GWORDS; i += K1_THREADS) {
+    for (int i = tid; i < GR * GWORDS; i += NT) {
         const int r = i / GWORDS, k = i % GWORDS;
         uint32_t v = 0;
         if (fast) {
@@ -169,7 +174,7 @@ __device__ __forceinline__ void planes_tile16(const uint16_t* __restrict__ luma,
     __syncthreads();
     // the unrounded horizontal sums of columns X = x0 + 4q .. X + 3 (word 2q holds X - 4, X - 3): the taps
     // of column X + j start at sample X + j - 2, i.e. at half j + 2 of words 2q ..
-    for (int i = tid; i < GR * (K1_TW / 4); i += K1_THREADS) {
+    for (int i = tid; i < GR * (K1_TW / 4); i += NT) {
         const int r = i / (K1_TW / 4), q = i % (K1_TW / 4);
         uint32_t wv[6];  // words 2q .. 2q + 5 (the last pair of column X + 3 starts at half 9)
 #pragma unroll

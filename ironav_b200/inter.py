@@ -134,7 +134,11 @@ EXPORTS = (
     "ironav_begin_i_picture", "ironav_decide_i_picture", "ironav_decide_i_picture_device", "ironav_set_source_chroma_device",
     "ironav_push_reference_chroma_device",
     "ironav_write_parameter_sets", "ironav_write_slices", "ironav_write_slices_device",
+    "ironav_batch_set_tuning", "ironav_batch_get_tuning", "ironav_batch_autotune",
 )
+
+# ironav_batch_tuning (include/ironav_inter.h): the batched step's knobs
+BATCH_TUNING_DTYPE = np.dtype([("k2_ctas_per_sm", "<i4"), ("k1_tile_rows", "<i4"), ("order", "<i4"), ("ms", "<f4")])
 
 # ironav_stream_params (include/ironav_inter.h): what the SPS and PPS say
 STREAM_PARAMS_DTYPE = np.dtype([("width", "<i4"), ("height", "<i4"), ("bd", "<i4"), ("fps_num", "<i4"), ("fps_den", "<i4"),
@@ -210,6 +214,10 @@ def _declare(lib: ctypes.CDLL) -> ctypes.CDLL:
         lib.ironav_batch_destroy.argtypes = [_VP]
         lib.ironav_batch_step.argtypes = [_VP] + [ctypes.POINTER(_VP)] * 5
         lib.ironav_batch_sync.argtypes = [_VP]
+    if hasattr(lib, "ironav_batch_autotune"):
+        lib.ironav_batch_set_tuning.argtypes = [_VP, _VP]
+        lib.ironav_batch_get_tuning.argtypes = [_VP, _VP]
+        lib.ironav_batch_autotune.argtypes = [_VP] + [ctypes.POINTER(_VP)] * 5 + [_I, _VP, _VP, _I, ctypes.POINTER(_I)]
     if hasattr(lib, "ironav_batch_deblock"):
         lib.ironav_batch_deblock.argtypes = [_VP, ctypes.POINTER(_VP), ctypes.POINTER(_I), ctypes.POINTER(_VP), ctypes.POINTER(_VP),
                                              ctypes.POINTER(_I), ctypes.POINTER(_VP), ctypes.POINTER(_VP), ctypes.POINTER(_I)]
@@ -708,6 +716,59 @@ class InterBatch:
 
     def sync(self) -> None:
         InterStage._check(self.lib.ironav_batch_sync(self.h), "ironav_batch_sync")
+
+    # -- the tuner: the batched step's knobs for this stream mix on this GPU ---------------------------------
+
+    def signature(self) -> str:
+        """What a tuning is valid for: the GPU and every stream's size, bands and depth."""
+        import torch
+
+        streams = ",".join(f"{s.width}x{s.height}/{s.mb_h}r/{s.bd}b" for s in self.stages)
+        return f"{torch.cuda.get_device_name()}|{streams}"
+
+    def tuning(self) -> dict:
+        t = np.zeros(1, dtype=BATCH_TUNING_DTYPE)
+        InterStage._check(self.lib.ironav_batch_get_tuning(self.h, _ptr(t)), "ironav_batch_get_tuning")
+        return {k: t[0][k].item() for k in ("k2_ctas_per_sm", "k1_tile_rows", "order")}
+
+    def set_tuning(self, k2_ctas_per_sm: int, k1_tile_rows: int, order: int) -> None:
+        t = np.zeros(1, dtype=BATCH_TUNING_DTYPE)
+        t[0] = (k2_ctas_per_sm, k1_tile_rows, order, 0.0)
+        InterStage._check(self.lib.ironav_batch_set_tuning(self.h, _ptr(t)), "ironav_batch_set_tuning")
+
+    def autotune(self, d_src, d_ref, d_col, d_states, d_results, reps: int = 5, cache: str | None = None) -> dict:
+        """Times every setting on `reps` steps of these inputs (ironav_batch_autotune; the batch ends as after one
+        step of them) and keeps the fastest. With `cache` (a JSON file), a setting found before for the same
+        signature is applied without timing (the step still runs once), and a new one is stored there.
+        Returns {"best": {...}, "all": [...], "cached": bool}."""
+        import json
+
+        sig = self.signature()
+        table = {}
+        if cache and os.path.exists(cache):
+            with open(cache) as f:
+                table = json.load(f)
+        if sig in table:
+            b = table[sig]
+            self.set_tuning(b["k2_ctas_per_sm"], b["k1_tile_rows"], b["order"])
+            self.step(d_src, d_ref, d_col, d_states, d_results)
+            self.sync()
+            return {"best": b, "all": [], "cached": True}
+        n = len(self.stages)
+        mk = lambda xs: (_VP * n)(*[x if x is not None else None for x in xs])
+        best = np.zeros(1, dtype=BATCH_TUNING_DTYPE)
+        allv = np.zeros(16, dtype=BATCH_TUNING_DTYPE)
+        cnt = _I(0)
+        InterStage._check(self.lib.ironav_batch_autotune(self.h, mk(d_src), mk(d_ref), mk(d_col), mk(d_states), mk(d_results), reps,
+                                                         _ptr(best), _ptr(allv), len(allv), ctypes.byref(cnt)), "ironav_batch_autotune")
+        as_dict = lambda r: {k: r[k].item() for k in ("k2_ctas_per_sm", "k1_tile_rows", "order", "ms")}
+        out = {"best": as_dict(best[0]), "all": [as_dict(allv[i]) for i in range(cnt.value)], "cached": False}
+        if cache:
+            table[sig] = out["best"]
+            os.makedirs(os.path.dirname(os.path.abspath(cache)), exist_ok=True)
+            with open(cache, "w") as f:
+                json.dump(table, f, indent=1)
+        return out
 
     def close(self) -> None:
         if getattr(self, "h", None):

@@ -1098,6 +1098,13 @@ int ironav_batch_step(ironav_batch* b, const void* const* s, const void* const* 
     return IRONAV_HARDWARE_UNAVAILABLE;
 }
 int ironav_batch_sync(ironav_batch* b) { (void)b; return IRONAV_INVALID_ARGUMENT; }
+int ironav_batch_set_tuning(ironav_batch* b, const ironav_batch_tuning* t) { (void)b; (void)t; return IRONAV_INVALID_ARGUMENT; }
+int ironav_batch_get_tuning(const ironav_batch* b, ironav_batch_tuning* t) { (void)b; (void)t; return IRONAV_INVALID_ARGUMENT; }
+int ironav_batch_autotune(ironav_batch* b, const void* const* s, const void* const* r, const ironav_mbstate* const* c, ironav_mbstate* const* st,
+                          ironav_mbresult* const* res, int reps, ironav_batch_tuning* best, ironav_batch_tuning* all, int cap, int* n_all) {
+    (void)b; (void)s; (void)r; (void)c; (void)st; (void)res; (void)reps; (void)best; (void)all; (void)cap; (void)n_all;
+    return IRONAV_INVALID_ARGUMENT;
+}
 int ironav_batch_decide(ironav_batch* b, ironav_mbstate* const* s, ironav_mbcode* const* c, void* const* y, const int* ys, void* const* cb,
                         void* const* cr, const int* cs) {
     (void)b; (void)s; (void)c; (void)y; (void)ys; (void)cb; (void)cr; (void)cs;

@@ -152,3 +152,78 @@ def test_config3_64_streams_four_steps(cuda_lib, oracle_lib):
     batch.close()
     for st in stages:
         st.close()
+
+
+def test_every_tuning_gives_the_same_results_and_the_tuner_picks_one(cuda_lib, tmp_path):
+    """The batched step's knobs (CTAs per SM of the analysis, the planes' tile rows, the ticket order) change
+    only its time: every one of the 12 settings gives each stream its single-stream results. The tuner times
+    them all, keeps the fastest, ends as one step of its inputs would, and a second call finds the setting in
+    its cache."""
+    import torch
+
+    streams = STREAMS[:4]
+    frames = [_frames(i, w, h) for i, (w, h, _) in enumerate(streams)]
+    want = []
+    for (w, h, ns), f in zip(streams, frames):
+        one = InterStage(w, h, nslices=ns, lib=cuda_lib)
+        one.push_reference(f[0])
+        one.set_source(f[1])
+        one.begin_p_picture(27)
+        want.append(one.analyse_auto())
+        one.close()
+    stream = torch.cuda.Stream()
+    dev = [[torch.from_numpy(x).cuda() for x in f] for f in frames]
+    stages = []
+    for (w, h, ns), f in zip(streams, dev):
+        st = InterStage(w, h, nslices=ns, lib=cuda_lib)
+        st.set_stream(stream.cuda_stream)
+        st.push_reference_device(f[0].data_ptr(), w, w, h, None)
+        st.begin_p_picture(27)
+        stages.append(st)
+    n = len(stages)
+    d_states = [torch.zeros(s.nmb * 72, dtype=torch.uint8, device="cuda") for s in stages]
+    d_res = [torch.zeros(s.nmb * 104, dtype=torch.uint8, device="cuda") for s in stages]
+    torch.cuda.synchronize()
+    batch = InterBatch(stages)
+    args = ([f[1].data_ptr() for f in dev], [f[0].data_ptr() for f in dev], [None] * n, [d.data_ptr() for d in d_states],
+            [d.data_ptr() for d in d_res])
+
+    def check(what):
+        for i in range(n):
+            assert np.array_equal(d_states[i].cpu().numpy().view(MBSTATE_DTYPE), want[i][0]), f"{what}: stream {i} decisions"
+            assert np.array_equal(d_res[i].cpu().numpy().view(MBRESULT_DTYPE), want[i][1]), f"{what}: stream {i} results"
+            d_res[i].zero_()
+
+    for k2 in (4, 5, 6):
+        for th in (16, 8):
+            for order in (0, 1):
+                for st in stages:  # the step pushes the reference again: start from the ring as it was
+                    st.clear_references()
+                    st.push_reference_device(dev[stages.index(st)][0].data_ptr(), st.width, st.width, st.height, None)
+                    st.begin_p_picture(27)
+                batch.set_tuning(k2, th, order)
+                assert batch.tuning() == {"k2_ctas_per_sm": k2, "k1_tile_rows": th, "order": order}
+                batch.step(*args)
+                batch.sync()
+                check(f"setting {k2}/{th}/{order}")
+    for st, f in zip(stages, dev):
+        st.clear_references()
+        st.push_reference_device(f[0].data_ptr(), st.width, st.width, st.height, None)
+        st.begin_p_picture(27)
+    cache = str(tmp_path / "tuning.json")
+    out = batch.autotune(*args, reps=3, cache=cache)
+    assert not out["cached"] and len(out["all"]) == 12 and out["best"]["ms"] > 0
+    assert min(a["ms"] for a in out["all"]) == out["best"]["ms"]
+    check("after the tuner")
+    assert all(st.lib.ironav_ctx_sync(st.ctx) == 0 for st in stages)
+    # one reference pushed, as by one step: a step with the same inputs again gives the same results
+    for st, f in zip(stages, dev):
+        st.clear_references()
+        st.push_reference_device(f[0].data_ptr(), st.width, st.width, st.height, None)
+        st.begin_p_picture(27)
+    again = batch.autotune(*args, reps=3, cache=cache)
+    assert again["cached"] and again["best"]["k2_ctas_per_sm"] == out["best"]["k2_ctas_per_sm"]
+    check("the cached setting")
+    batch.close()
+    for st in stages:
+        st.close()
