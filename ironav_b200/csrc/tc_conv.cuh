@@ -1,0 +1,230 @@
+// tc_conv.cuh — the learned proposer's 3x3 convolutions on the 5th-generation tensor cores (tcgen05, sm_100a):
+// BF16 operands in shared memory, FP32 accumulators in tensor memory (TMEM).
+//
+// Activation layout ("chunk-major padded"): every sample (one macroblock's input) is a 50 x 50 raster, its
+// 48 x 48 interior plus a ring of zeros; rasters follow each other, Q = samples * 2500 pixels in all. A tensor
+// of C channels is C / 8 planes, plane c holding channels 8c .. 8c + 7 of every pixel as 16 bytes: element
+// (c, q, e) at ((c * Q) + q) * 8 + e. A 3x3 convolution of such a raster is then a 1-D convolution along q with
+// the nine shifts (dy - 1) * 50 + (dx - 1): output pixel q reads input pixel q + shift, and a shift never leaves
+// the sample's own raster for an interior pixel (outputs on the ring are written as zeros).
+//
+// One CTA (4 warps) takes tiles of 128 consecutive output pixels. Per tile: one TMA 3-D box load brings the
+// input halo (pixels q0 - 51 .. q0 + 180 of every plane, zeros beyond the tensor) into shared memory in the
+// same layout; every tap's A operand (128 pixels x 16 channels, K-major, no swizzle) is then just another
+// start address into the halo, so no im2col copy is made. The weights (B: 32 output channels x CIN input
+// channels per tap, K-major) sit in shared memory for the CTA's life. One thread issues 9 taps x CIN / 16
+// MMAs of M = 128, N = 32, K = 16 into one TMEM accumulator (128 lanes x 32 FP32 columns) and commits them to an
+// mbarrier; each warp then reads its 32 lanes (pixels) x 32 columns (channels) with tcgen05.ld, adds the bias,
+// applies ReLU or a gradient mask, zeroes the ring, and stores BF16.
+//
+// The same kernel is the backward pass's data gradient (the convolution with the weights transposed and the
+// taps mirrored, and the mask of the layer's ReLU in the epilogue).
+#pragma once
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cstdint>
+
+namespace ironav {
+namespace tc {
+
+constexpr int RW = 50;                  // raster width (and height): 48 + 2
+constexpr int RPIX = RW * RW;           // pixels a sample
+constexpr int TILE = 128;               // output pixels a tile (the MMA's M)
+constexpr int HALO_LO = RW + 1;         // the most negative shift
+constexpr int HALO = 232;               // halo pixels staged a tile: 51 + 128 + 51, rounded up to 8
+constexpr int COUT = 32;                // output channels (the MMA's N)
+constexpr unsigned WAIT_LIMIT = 1u << 26;  // polls of an mbarrier before the kernel gives up
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+// Waits for the mbarrier's phase `parity` to complete, at most WAIT_LIMIT polls; false when it gave up.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
+    const uint32_t a = smem_u32(bar);
+    for (unsigned i = 0; i < WAIT_LIMIT; i++) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+// TMA: a 3-D box of the tensor map into shared memory, completion counted on the mbarrier.
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int c0, int c1, int c2, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
+        "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
+        : "memory");
+}
+
+// A shared-memory matrix descriptor for tcgen05.mma (K-major, no swizzle): start address, the byte distance
+// between core matrices adjacent in K (lbo) and in M/N (sbo), version 1 (bits 46-47), layout type 0.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) | ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) |
+           (1ull << 46);
+}
+// The instruction descriptor of kind::f16 with BF16 A and B, FP32 D, both K-major, M = 128, N = 32.
+constexpr uint32_t IDESC_BF16_M128_N32 = (1u << 4) | (1u << 7) | (1u << 10) | ((COUT >> 3) << 17) | ((TILE >> 4) << 24);
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// 32 lanes x 32 consecutive FP32 columns of TMEM into 32 registers of each thread (lane = the warp's lane).
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, "
+        "%19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]),
+          "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]),
+          "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]),
+          "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ bool ring_pixel(long long q) {
+    const int p = (int)(q % RPIX), y = p / RW, x = p % RW;
+    return y == 0 || y == RW - 1 || x == 0 || x == RW - 1;
+}
+
+// One 3x3 convolution layer (CIN input channels, 32 output channels) over the chunk-major padded rasters:
+// y = act(conv(x, w) + bias), act = ReLU (relu != 0) or the identity, then times (mask > 0) when `mask` is set
+// (the gradient through the layer's ReLU); the ring pixels of y are zero. w is [9 taps][32 out][CIN in] BF16,
+// tap = 3 * dy + dx. x is read through `map` (planes CIN / 8, Q pixels, 8 channels). tiles = ceil(Q / 128).
+template <int CIN>
+__global__ void __launch_bounds__(128, 1) conv3x3_kernel(const __grid_constant__ CUtensorMap map, const __nv_bfloat16* __restrict__ w,
+                                                         const float* __restrict__ bias, int relu, const __nv_bfloat16* __restrict__ mask,
+                                                         __nv_bfloat16* __restrict__ y, long long Q, int tiles, unsigned* err) {
+    constexpr int KC = CIN / 8;             // 16-byte chunks of input channels
+    constexpr int WBYTES = 9 * KC * COUT * 16;
+    constexpr int HBYTES = KC * HALO * 16;
+    extern __shared__ __align__(1024) uint8_t smem[];
+    uint8_t* ws = smem;                                            // weights: [tap][chunk][out][16 B]
+    uint8_t* halo = smem + WBYTES;                                 // input: [chunk][HALO pixels][16 B]
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + WBYTES + HBYTES);  // [0] the tile's load, [1] its MMAs
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+    // the weights in the canonical K-major layout: element (tap, n, k) at ((tap * KC + k / 8) * 32 + n) * 16 + (k % 8) * 2
+    for (int i = tid; i < 9 * COUT * CIN; i += 128) {
+        const int t = i / (COUT * CIN), n = (i / CIN) % COUT, k = i % CIN;
+        *reinterpret_cast<__nv_bfloat16*>(ws + ((t * KC + k / 8) * COUT + n) * 16 + (k % 8) * 2) = w[i];
+    }
+    if (tid == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    // the generic-proxy writes of the weights before the tensor cores (async proxy) read them
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 32;" ::"r"(smem_u32(tmem_slot)));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+    bool failed = false, mma_pending = false, load_pending = false;
+    unsigned it = 0;
+    for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x, it++) {
+        const long long q0 = (long long)tile * TILE;
+        if (tid == 0) {
+            mbar_expect_tx(&bars[0], HBYTES);
+            tma_load_3d(halo, &map, 0, (int)(q0 - HALO_LO), 0, &bars[0]);
+        }
+        const bool loaded = mbar_wait(&bars[0], it & 1);
+        if (__syncthreads_or(!loaded)) {
+            failed = true;
+            load_pending = true;
+            break;
+        }
+        if (tid == 0) {
+            tc_fence_after();
+            const uint32_t h = smem_u32(halo), wb = smem_u32(ws);
+#pragma unroll 1
+            for (int t = 0; t < 9; t++) {
+                const int shift = (t / 3 - 1) * RW + (t % 3 - 1);
+#pragma unroll
+                for (int k = 0; k < KC / 2; k++) {
+                    const uint64_t ad = smem_desc(h + (uint32_t)((2 * k * HALO + HALO_LO + shift) * 16), HALO * 16, 8 * 16);
+                    const uint64_t bd = smem_desc(wb + (uint32_t)((t * KC + 2 * k) * COUT * 16), COUT * 16, 8 * 16);
+                    mma_bf16(tmem, ad, bd, IDESC_BF16_M128_N32, (t | k) != 0);
+                }
+            }
+            mma_commit(&bars[1]);
+        }
+        const bool computed = mbar_wait(&bars[1], it & 1);
+        if (__syncthreads_or(!computed)) {
+            failed = true;
+            mma_pending = true;
+            break;
+        }
+        tc_fence_after();
+        float v[32];
+        tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16), v);
+        const long long q = q0 + warp * 32 + lane;
+        if (q < Q) {
+            const bool ring = ring_pixel(q);
+#pragma unroll
+            for (int c = 0; c < 4; c++) {
+                uint4 m4 = make_uint4(0, 0, 0, 0);
+                if (mask != nullptr) m4 = *reinterpret_cast<const uint4*>(mask + ((size_t)c * Q + q) * 8);
+                const __nv_bfloat16* mk = reinterpret_cast<const __nv_bfloat16*>(&m4);
+                __align__(16) __nv_bfloat16 o[8];
+#pragma unroll
+                for (int e = 0; e < 8; e++) {
+                    float f = v[c * 8 + e] + (bias != nullptr ? bias[c * 8 + e] : 0.f);
+                    if (relu) f = fmaxf(f, 0.f);
+                    if (mask != nullptr && !(__bfloat162float(mk[e]) > 0.f)) f = 0.f;
+                    o[e] = __float2bfloat16_rn(ring ? 0.f : f);
+                }
+                *reinterpret_cast<uint4*>(y + ((size_t)c * Q + q) * 8) = *reinterpret_cast<const uint4*>(o);
+            }
+        }
+        // the TMEM reads and the halo's use are over before the next tile's MMAs and load
+        tc_fence_before();
+        __syncthreads();
+    }
+    if (failed && tid == 0) atomicOr(err, 1u);
+    // a copy or MMAs of the failed tile may still be in flight: wait for them (bounded) before the CTA's
+    // shared memory and TMEM are given up
+    if (load_pending) mbar_wait(&bars[0], it & 1);
+    if (mma_pending) mbar_wait(&bars[1], it & 1);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 32;" ::"r"(tmem));
+}
+
+template <int CIN>
+constexpr int conv3x3_smem_bytes() {
+    return 9 * (CIN / 8) * COUT * 16 + (CIN / 8) * HALO * 16 + 2 * 8 + 16;
+}
+
+}  // namespace tc
+}  // namespace ironav
