@@ -515,6 +515,72 @@ int ironav_batch_autotune(ironav_batch* batch, const void* const* d_src, const v
                           ironav_mbresult* const* d_results, int reps, ironav_batch_tuning* best,
                           ironav_batch_tuning* all, int cap, int* n_all);
 
+/* ---- the learned proposer (form 4): its network's kernels ------------------------------------------- */
+
+/* The proposer is a small network (4 conv3x3 layers of 32 channels with ReLU, then a linear head) that, from a
+ * macroblock's 16x16 luma tiled 3x3 and the co-located 48x48 reference window, proposes 4 candidate vectors
+ * and 5 partition logits; the exact integer cost then judges the candidates. It has no counterpart in the
+ * reference: these are its building blocks, which the Python driver (ironav_b200/proposer.py) strings into
+ * training steps and proposals. Tensors are "chunk-major padded": each sample a 50 x 50 raster (its 48 x 48
+ * interior and a ring of zeros), C channels as C / 8 planes of 16-byte pixels, element (c, q, e) at
+ * ((c * Q) + q) * 8 + e with Q = samples * 2500; BF16 values, 16-byte aligned. Weights of a layer are
+ * [9 taps][32 out][cin in] (tap = 3 * dy + dx). Every call queues its work on `stream` (a cudaStream_t) and
+ * returns; a device wait that gave up sets bit 0 of *d_err (a word in device memory the caller clears and
+ * reads). All pointers are device pointers. */
+typedef struct ironav_prop_sample {
+    const uint8_t* cur;           /* the current picture's luma (8-bit) */
+    const uint8_t* ref;           /* the reference picture's luma */
+    int32_t w, h, stride;         /* picture size and the current picture's row stride (samples) */
+    int32_t mbx, mby;             /* the macroblock */
+    int32_t ref_stride;           /* the reference's row stride (0: stride) */
+} ironav_prop_sample;             /* 40 bytes */
+
+/* One conv3x3 layer on the tensor cores (tcgen05, BF16 operands, FP32 accumulation in tensor memory):
+ * y = act(conv(x, w) + bias) with act ReLU when relu, then times (mask > 0) when d_mask is not NULL; cin is 16
+ * or 32, 32 output channels, y's ring zero. d_bias may be NULL. */
+int ironav_prop_conv3x3(const void* d_x, int cin, long long samples, const void* d_w, const float* d_bias, int relu, const void* d_mask,
+                        void* d_y, unsigned* d_err, void* stream);
+/* The weight and bias gradients of a conv3x3 layer on the tensor cores: d_dw[t][o][i] += sum_q dz[q][o] x[q +
+ * shift_t][i], d_db[o] += sum_q dz[q][o] (FP32, accumulated; d_db may be NULL). */
+int ironav_prop_wgrad3x3(const void* d_x, int cin, const void* d_dz, long long samples, float* d_dw, float* d_db, unsigned* d_err,
+                         void* stream);
+/* The network's input (two planes: channel 0 the macroblock tiled, channel 1 the reference window, both / 255)
+ * for n samples. */
+int ironav_prop_prep(const ironav_prop_sample* d_samples, int n, void* d_x, void* stream);
+/* The head: d_out[s][j] = d_hb[j] + sum_f d_hw[j][f] feat(s, f), 13 outputs (4 vectors (x, y) in units of 32
+ * luma samples, then 5 logits), features f = ((iy * 48 + ix) * 32 + c) of layer 4's output. */
+int ironav_prop_head_fwd(const void* d_feat, int n, const float* d_hw, const float* d_hb, float* d_out, void* stream);
+/* The loss (winner-takes-all L1 on the vectors against d_target_mv (quarter samples), cross-entropy on the
+ * logits against d_target_part (0 P_Skip, 1 16x16, 2 16x8, 3 8x16, 4 8x8)) and its gradient d_dout (mean over
+ * the n samples); d_sums[0..2] += the vector loss, the partition loss and the partition hits. */
+int ironav_prop_loss(const float* d_out, const int16_t* d_target_mv, const uint8_t* d_target_part, int n, float* d_dout, float* d_sums,
+                     void* stream);
+/* The head's backward pass: d_ghw, d_ghb += its gradients; d_dz = the gradient into layer 4's output through
+ * its ReLU (4 planes). */
+int ironav_prop_head_bwd(const void* d_feat, int n, const float* d_dout, const float* d_hw, float* d_ghw, float* d_ghb, void* d_dz,
+                         void* stream);
+/* Adam on n parameters (bias-corrected at `step` >= 1); the gradients are cleared. */
+int ironav_prop_adam(float* d_p, float* d_g, float* d_m, float* d_v, long long n, float lr, float beta1, float beta2, int step, float eps,
+                     void* stream);
+/* A layer's BF16 weights for its forward convolution (d_wf, [9][32][cin]) and, when d_wt is not NULL (cin 32),
+ * for its data gradient: transposed and mirrored, d_wt[t][i][o] = w[8 - t][o][i]. */
+int ironav_prop_weights(const float* d_w, int cin, void* d_wf, void* d_wt, void* stream);
+/* The judge's inputs from the head's outputs of n macroblocks (in raster order): d_cands[s][k] = the k-th vector
+ * in quarter samples (rounded, clamped to +-2048 x +-512), d_cls[s] = the partition class of largest logit. */
+int ironav_prop_propose(const float* d_out, int n, int16_t* d_cands, uint8_t* d_cls, void* stream);
+
+/* The learned form's judge (no counterpart in the reference: the north star's form 4). With proposals set, the
+ * context's analyses (auto, replay, in-loop and decide modes) judge the newest reference's 16x16 partitioning
+ * from them instead of searching: the exact integer cost (SAD + lambda * the vector's bits) of every integer
+ * vector within +-2 samples of each of the 4 proposals, then the plain search's sub-sample refinement; the
+ * plain search (best_inter) takes over when the proposed partitioning class is not P_Skip or 16x16, or when
+ * the best proposal costs more than the predictor's start plus `margin`. d_cands: per macroblock 4 vectors
+ * (x, y) in quarter samples (int16, mb_w*mb_h*8); d_cls: per macroblock the class (0 P_Skip, 1 16x16, 2 16x8,
+ * 3 8x16, 4 8x8); d_stats: 3 counters the analyses add to (judged from the proposals, fallbacks on the class,
+ * fallbacks on the cost). Device pointers, read when the analyses run; d_cands NULL: the plain search again.
+ * The oracle implements the same judge on host pointers. */
+int ironav_set_learned(ironav_ctx* ctx, const int16_t* d_cands, const uint8_t* d_cls, int margin, unsigned* d_stats);
+
 /* ---- analysis without allocation ------------------------------------------------------------------ */
 
 /* No counterpart in the reference: an entry point for callers that cannot allocate device memory (a

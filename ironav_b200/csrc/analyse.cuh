@@ -749,6 +749,130 @@ static __device__ __noinline__ int4 best_inter_ref(const AnalyseParams& __restri
     return make_int4(best_cost, best_part, (int)sub_out, cost16);
 }
 
+// ---- the learned form's judge ------------------------------------------------------------------------
+
+// The 16x16 partitioning of reference r judged from the learned proposer's candidates instead of searched:
+// the exact integer cost (SAD + lambda * the vector's bits, as the plain search scores it) of every integer
+// vector within +-2 samples of each of the 4 proposals (100 points, eight a batch, the search's clamps), then
+// the plain search's sub-sample refinement (the half-sample square and the quarter-sample diamond by SATD)
+// around the best. Falls back (returns x = -1) when the proposed partitioning is not P_Skip or 16x16, or when
+// the best proposal costs more than the predictor's own start (the plain search's first candidate) plus the
+// margin. Otherwise returns best_inter_ref's result for a 16x16 choice.
+template <class T>
+static __device__ __noinline__ int4 learned_inter(const AnalyseParams& __restrict__ P, WarpSmem<T>& __restrict__ S, int r) {
+    const int lane = threadIdx.x & 31, g = lane & 7;
+    const int lam = P.lambda;
+    if (P.learned_cls[S.mb] >= 2) {
+        if (lane == 0) atomicAdd(&P.learned_stats[1], 1u);
+        return make_int4(-1, 0, 0, 0);
+    }
+    int rb = 0;
+    if (P.nact == 2) rb = lam;
+    else if (P.nact > 2) rb = lam * (2 * (31 - __clz(r + 1)) + 1);
+    const int2 mvp = pred_mv(P, S, S.ext, nullptr, 0, 0, 4, 0, r);
+    const int x0 = S.mbx * 16, y0 = S.mby * 16;
+    const int cxlo = max(-(x0 + 24) * 4, -2048), cxhi = min((P.mb_w * 16 - x0 + 8) * 4, 2047);
+    const int cylo = max(-(y0 + 24) * 4, -512), cyhi = min((P.mb_h * 16 - y0 + 8) * 4, 511);
+    auto clx = [&](int v) { return min(max(v, cxlo), cxhi); };
+    auto cly = [&](int v) { return min(max(v, cylo), cyhi); };
+    auto intr = [](int v) { return (v + 2) & ~3; };
+    const int16_t* cand = P.learned + (size_t)S.mb * 8;
+    const int sw = P.sw;
+    const uint8_t* const g0 = P.planes[r] + ((y0 + PAD) * sw + x0 + PAD) * (int)sizeof(T);
+    const uint32_t* const src0 = &S.src[0];
+    unsigned best = 0xffffffffu, start = 0xffffffffu;
+    for (int b = 0; b < 13; b++) {
+        const int i = b * 8 + g;  // 0..99: proposal i / 25, offset i % 25; 100: the predictor start
+        const bool valid = i <= 100;
+        int px = intr(clx(mvp.x)), py = intr(cly(mvp.y));
+        if (i < 100) {
+            const int k = i / 25, d = i % 25;
+            px = clx(intr(clx(cand[2 * k])) + 4 * (d % 5 - 2));
+            py = cly(intr(cly(cand[2 * k + 1])) + 4 * (d / 5 - 2));
+        }
+        const int sad = sad_lane<T>(g0, src0, sw, 16, 16, px, py, valid);
+        const unsigned cost = (unsigned)(sad + lam * mvd_bits_d(px, py, mvp.x, mvp.y));
+        unsigned kp = (valid && i < 100) ? ((cost << 7) | (unsigned)i) : 0xffffffffu;
+        unsigned ks = (i == 100) ? cost : 0xffffffffu;
+#pragma unroll
+        for (int off = 1; off < 8; off <<= 1) {
+            kp = min(kp, __shfl_xor_sync(FULL, kp, off));
+            ks = min(ks, __shfl_xor_sync(FULL, ks, off));
+        }
+        best = min(best, kp);
+        start = min(start, ks);
+    }
+    if (lane == 0) S.sad_px += 101u * 256u;
+    if ((int)(best >> 7) > (int)start + P.learned_margin) {
+        if (lane == 0) atomicAdd(&P.learned_stats[2], 1u);
+        return make_int4(-1, 0, 0, 0);
+    }
+    const int bi = (int)(best & 127u), k = bi / 25, d = bi % 25;
+    int bxv = clx(intr(clx(cand[2 * k])) + 4 * (d % 5 - 2)), byv = cly(intr(cly(cand[2 * k + 1])) + 4 * (d / 5 - 2));
+    int bc;
+    // the plain search's sub-sample refinement (motion_search, enc/frame.rs:994-1017)
+    if (lane < 9) {
+        int2 q = make_int2(bxv, byv);
+        if (lane > 0) {
+            const int kk = lane <= 4 ? lane - 1 : lane;
+            q = make_int2(clx(bxv + (kk % 3 - 1) * 2), cly(byv + (kk / 3 - 1) * 2));
+        }
+        S.cand[lane] = q;
+    }
+    __syncwarp();
+    pred_batch(P, S, r, 0, 0, 2, 2, 9, false);
+    {
+        unsigned key = 0xffffffffu;
+        if (lane < 9) key = ((unsigned)(S.cost[lane] + lam * mvd_bits_d(S.cand[lane].x, S.cand[lane].y, mvp.x, mvp.y)) << 4) | (unsigned)lane;
+#pragma unroll
+        for (int off = 16; off >= 1; off >>= 1) key = min(key, __shfl_xor_sync(FULL, key, off));
+        const int c = (int)(key & 15u);
+        bc = (int)(key >> 4);
+        bxv = S.cand[c].x;
+        byv = S.cand[c].y;
+    }
+    __syncwarp();
+    if (!P.fast) {
+        if (lane < 4) {
+            const int dx = lane == 1 ? -1 : (lane == 2 ? 1 : 0), dy = lane == 0 ? -1 : (lane == 3 ? 1 : 0);
+            S.cand[lane] = make_int2(clx(bxv + dx), cly(byv + dy));
+        }
+        __syncwarp();
+        pred_batch(P, S, r, 0, 0, 2, 2, 4, false);
+        unsigned key = (unsigned)bc << 4;
+        if (lane < 4) key = ((unsigned)(S.cost[lane] + lam * mvd_bits_d(S.cand[lane].x, S.cand[lane].y, mvp.x, mvp.y)) << 4) | (unsigned)(lane + 1);
+#pragma unroll
+        for (int off = 16; off >= 1; off >>= 1) key = min(key, __shfl_xor_sync(FULL, key, off));
+        const int c = (int)(key & 15u);
+        bc = (int)(key >> 4);
+        if (c > 0) {
+            bxv = S.cand[c - 1].x;
+            byv = S.cand[c - 1].y;
+        }
+        __syncwarp();
+    }
+    if (lane == 0) S.satd_px += (P.fast ? 9u : 13u) * 256u;
+    // bc holds SATD + lambda * bits; the 16x16 cost of best_inter_ref (855-858) adds the mb_type bit and ref_bits
+    const int cost16 = bc + lam + rb;
+    if (lane < 16) {
+        S.best_mvs[lane][0] = (int16_t)bxv;
+        S.best_mvs[lane][1] = (int16_t)byv;
+    }
+    if (lane == 0) atomicAdd(&P.learned_stats[0], 1u);
+    __syncwarp();
+    return make_int4(cost16, 0, 0, cost16);
+}
+
+// best_inter_ref, or the learned form's judge on the newest reference when proposals are given.
+template <class T>
+static __device__ __forceinline__ int4 best_inter_or_learned(const AnalyseParams& __restrict__ P, WarpSmem<T>& __restrict__ S, int r) {
+    if (P.learned != nullptr && r == 0) {
+        const int4 li = learned_inter(P, S, r);
+        if (li.x >= 0) return li;
+    }
+    return best_inter_ref(P, S, r);
+}
+
 // ---- one macroblock --------------------------------------------------------------------------------
 
 // The current macroblock into shared memory: 16 rows of 16 samples, as 128-bit loads (sizeof(T) per row).
@@ -787,7 +911,7 @@ static __device__ void analyse(const AnalyseParams& __restrict__ P, WarpSmem<T>&
     if (!skip) {
         // best_inter, enc/frame.rs:839-849: every reference, the cheapest (first on ties) wins
         for (int r = 0; r < P.nact; r++) {
-            const int4 bi = best_inter_ref(P, S, r);
+            const int4 bi = best_inter_or_learned(P, S, r);
             const int c = bi.x, p = bi.y, c16 = bi.w;
             const uint32_t sb = (uint32_t)bi.z;
             if (r == 0 || c < cost) {

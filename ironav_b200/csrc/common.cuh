@@ -50,6 +50,14 @@ struct AnalyseParams {
     ironav_bresult* bresults;
     const ironav_mbstate* bcol;       // the list-1 picture's decisions, or nullptr (intra)
     int tb, td;                       // picture distances (FrameCoder::dist)
+    // the learned form (nullptr: the plain search): per macroblock 4 proposed vectors (x, y, quarter samples)
+    // and the proposed partitioning class (0 P_Skip, 1 16x16, 2 16x8, 3 8x16, 4 8x8); the margin by which the
+    // best proposal may cost more than the predictor start before the plain search takes over; counters
+    // [0] macroblocks judged from the proposals, [1] fallbacks on the partitioning, [2] fallbacks on the cost
+    const int16_t* learned;
+    const uint8_t* learned_cls;
+    int learned_margin;
+    unsigned* learned_stats;
 };
 
 // Device-scope acquire load and release store of a progress word shared by warps of different CTAs.

@@ -78,6 +78,11 @@ struct ironav_ctx {
     // the CAVLC writer (allocated on first use): slice band boundaries (nslices + 1 rows), per macroblock
     // its bits, offset and skip run, per slice its bytes, the error word; each slice's first macroblock and
     // each row's slice; the slices' RBSP regions; pinned host staging for the bytes that come back
+    // the learned form's proposals (device pointers, nullptr: the plain search) and counters
+    const int16_t* learned = nullptr;
+    const uint8_t* learned_cls = nullptr;
+    int learned_margin = 0;
+    unsigned* learned_stats = nullptr;
     int band_rows[1025] = {};
     uint32_t* d_cavlc = nullptr;
     int* d_slice_tab = nullptr;

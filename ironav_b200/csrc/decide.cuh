@@ -786,7 +786,7 @@ __device__ void decide_mb(const DecideParams& P, DecideSmem<T>& S, const unsigne
     int part = 0, cost = BIG, bestr = 0;
     uint32_t sub = 0;
     for (int r = 0; r < A.nact; r++) {
-        const int4 bi = best_inter_ref(A, S.a, r);
+        const int4 bi = best_inter_or_learned(A, S.a, r);
         if (r == 0 || bi.x < cost) {
             part = bi.y;
             cost = bi.x;

@@ -76,6 +76,10 @@ void fill_params(const ironav_ctx* c, AnalyseParams& p) {
     p.band_start = c->d_band_start;
     p.withhold = -1;
     p.wait_limit = c->wait_limit;
+    p.learned = c->learned;
+    p.learned_cls = c->learned_cls;
+    p.learned_margin = c->learned_margin;
+    p.learned_stats = c->learned_stats;
 }
 
 namespace {
@@ -1027,6 +1031,17 @@ int ironav_inloop_end(ironav_ctx* c) {
     if (!c || !c->inloop_active) return IRONAV_INVALID_ARGUMENT;
     c->inloop_active = false;
     return check_device_error(c);
+}
+
+// The learned form's proposals for the context's next analyses (auto, replay and decide modes): all four
+// pointers set, or d_cands NULL for the plain search again.
+int ironav_set_learned(ironav_ctx* c, const int16_t* d_cands, const uint8_t* d_cls, int margin, unsigned* d_stats) {
+    if (!c || (d_cands && (!d_cls || !d_stats)) || margin < 0) return IRONAV_INVALID_ARGUMENT;
+    c->learned = d_cands;
+    c->learned_cls = d_cands ? d_cls : nullptr;
+    c->learned_stats = d_cands ? d_stats : nullptr;
+    c->learned_margin = margin;
+    return IRONAV_OK;
 }
 
 // How long an in-loop wait for the caller's commit may take on the device (milliseconds).

@@ -1,15 +1,24 @@
-// ironav_proposer.cu — the learned proposer's tensor-core building blocks (tc_conv.cuh) behind the C ABI: one
-// 3x3 convolution layer over chunk-major padded rasters, its TMA tensor map made on the host.
+// ironav_proposer.cu — the learned proposer's kernels behind the C ABI (the north star's form 4): its 3x3
+// convolutions and their weight gradients on the tensor cores (tc_conv.cuh), and its input, head, loss and
+// optimizer on the CUDA cores (proposer.cuh). Every entry point queues its work on the given stream and
+// returns; a device wait that gave up sets bit 0 of the caller's error word `err` (device memory), which the
+// caller reads once a step. The TMA tensor maps are made on the host, through the driver's
+// cuTensorMapEncodeTiled reached via the runtime (no link against libcuda).
 #include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 
 #include "../../include/ironav_inter.h"
+#include "proposer.cuh"
 #include "tc_conv.cuh"
 
 using namespace ironav::tc;
+namespace prop = ironav::prop;
+
+static_assert(sizeof(ironav_prop_sample) == sizeof(prop::Sample), "ironav_prop_sample layout");
 
 namespace {
 
@@ -30,7 +39,7 @@ using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, 
                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion,
                                  CUtensorMapFloatOOBfill);
 
-// cuTensorMapEncodeTiled from the driver, through the runtime (no link against libcuda).
+// cuTensorMapEncodeTiled from the driver, through the runtime.
 EncodeTiled encode_fn() {
     static EncodeTiled fn = nullptr;
     if (!fn) {
@@ -42,8 +51,8 @@ EncodeTiled encode_fn() {
     return fn;
 }
 
-// The tensor map of a chunk-major padded tensor (planes x Q pixels x 8 BF16) read as boxes of HALO pixels of
-// every plane: dims (8, Q, planes), byte strides (16, 16 Q).
+// The tensor map of a chunk-major padded tensor (planes x Q pixels x 8 BF16) read in boxes of `box_pixels`
+// pixels of every plane: dims (8, Q, planes), byte strides (16, 16 Q). Out-of-range pixels read as zeros.
 int plane_map(CUtensorMap* map, const void* base, long long Q, int planes, int box_pixels) {
     EncodeTiled enc = encode_fn();
     if (!enc) return IRONAV_HARDWARE_UNAVAILABLE;
@@ -58,34 +67,120 @@ int plane_map(CUtensorMap* map, const void* base, long long Q, int planes, int b
     return r == CUDA_SUCCESS ? IRONAV_OK : IRONAV_INVALID_ARGUMENT;
 }
 
+int sm_count(int* nsm) {
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(nsm, cudaDevAttrMultiProcessorCount, dev));
+    return IRONAV_OK;
+}
+
+bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+
 }  // namespace
 
-extern "C" int ironav_prop_conv3x3(const void* d_x, int cin, long long samples, const void* d_w, const float* d_bias, int relu,
-                                   const void* d_mask, void* d_y, void* stream) {
-    if (!d_x || !d_w || !d_y || (cin != 16 && cin != 32) || samples < 1 || samples > (1ll << 24)) return IRONAV_INVALID_ARGUMENT;
-    if ((reinterpret_cast<uintptr_t>(d_y) | reinterpret_cast<uintptr_t>(d_mask)) & 15) return IRONAV_INVALID_ARGUMENT;
+extern "C" {
+
+int ironav_prop_conv3x3(const void* d_x, int cin, long long samples, const void* d_w, const float* d_bias, int relu, const void* d_mask,
+                        void* d_y, unsigned* d_err, void* stream) {
+    if (!d_x || !d_w || !d_y || !d_err || (cin != 16 && cin != 32) || samples < 1 || samples > (1ll << 22)) return IRONAV_INVALID_ARGUMENT;
+    if (!aligned16(d_y) || !aligned16(d_mask)) return IRONAV_INVALID_ARGUMENT;
     const long long Q = samples * RPIX;
     const int tiles = (int)((Q + TILE - 1) / TILE);
     CUtensorMap map;
-    const int s = plane_map(&map, d_x, Q, cin / 8, HALO);
+    int s = plane_map(&map, d_x, Q, cin / 8, HALO);
     if (s != IRONAV_OK) return s;
-    int dev = 0, nsm = 0;
-    CK(cudaGetDevice(&dev));
-    CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    unsigned* err = nullptr;
-    CK(cudaMallocAsync(&err, sizeof(unsigned), static_cast<cudaStream_t>(stream)));
-    CK(cudaMemsetAsync(err, 0, sizeof(unsigned), static_cast<cudaStream_t>(stream)));
+    int nsm = 0;
+    if ((s = sm_count(&nsm)) != IRONAV_OK) return s;
     const int grid = std::min(tiles, nsm * 4);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const __nv_bfloat16* w = static_cast<const __nv_bfloat16*>(d_w);
     const __nv_bfloat16* mask = static_cast<const __nv_bfloat16*>(d_mask);
     __nv_bfloat16* y = static_cast<__nv_bfloat16*>(d_y);
-    if (cin == 32) conv3x3_kernel<32><<<grid, 128, conv3x3_smem_bytes<32>(), st>>>(map, w, d_bias, relu, mask, y, Q, tiles, err);
-    else conv3x3_kernel<16><<<grid, 128, conv3x3_smem_bytes<16>(), st>>>(map, w, d_bias, relu, mask, y, Q, tiles, err);
-    CK(cudaGetLastError());
-    unsigned h = 0;
-    CK(cudaMemcpyAsync(&h, err, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
-    CK(cudaFreeAsync(err, st));
-    CK(cudaStreamSynchronize(st));
-    return h ? IRONAV_TIMEOUT : IRONAV_OK;
+    if (cin == 32) conv3x3_kernel<32><<<grid, 128, conv3x3_smem_bytes<32>(), st>>>(map, w, d_bias, relu, mask, y, Q, tiles, d_err);
+    else conv3x3_kernel<16><<<grid, 128, conv3x3_smem_bytes<16>(), st>>>(map, w, d_bias, relu, mask, y, Q, tiles, d_err);
+    return cuda_status(cudaGetLastError());
 }
+
+int ironav_prop_wgrad3x3(const void* d_x, int cin, const void* d_dz, long long samples, float* d_dw, float* d_db, unsigned* d_err,
+                         void* stream) {
+    if (!d_x || !d_dz || !d_dw || !d_err || (cin != 16 && cin != 32) || samples < 1 || samples > (1ll << 22)) return IRONAV_INVALID_ARGUMENT;
+    const long long Q = samples * RPIX;
+    const int tiles = (int)((Q + WG_KT - 1) / WG_KT);
+    CUtensorMap xmap, zmap;
+    int s = plane_map(&xmap, d_x, Q, cin / 8, WG_KT);
+    if (s == IRONAV_OK) s = plane_map(&zmap, d_dz, Q, 4, WG_KT);
+    if (s != IRONAV_OK) return s;
+    int nsm = 0;
+    if ((s = sm_count(&nsm)) != IRONAV_OK) return s;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (cin == 32) {
+        constexpr int bytes = wgrad3x3_smem_bytes<32>();
+        CK(cudaFuncSetAttribute(wgrad3x3_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+        wgrad3x3_kernel<32><<<std::min(tiles, nsm * 2), 128, bytes, st>>>(xmap, zmap, d_dw, d_db, Q, tiles, d_err);
+    } else {
+        constexpr int bytes = wgrad3x3_smem_bytes<16>();
+        CK(cudaFuncSetAttribute(wgrad3x3_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+        wgrad3x3_kernel<16><<<std::min(tiles, nsm * 2), 128, bytes, st>>>(xmap, zmap, d_dw, d_db, Q, tiles, d_err);
+    }
+    return cuda_status(cudaGetLastError());
+}
+
+int ironav_prop_prep(const ironav_prop_sample* d_samples, int n, void* d_x, void* stream) {
+    if (!d_samples || !d_x || n < 1 || n > (1 << 22) || !aligned16(d_x)) return IRONAV_INVALID_ARGUMENT;
+    const long long Q = (long long)n * RPIX;
+    prop::prep_kernel<<<(unsigned)((Q + 255) / 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        reinterpret_cast<const prop::Sample*>(d_samples), n, static_cast<__nv_bfloat16*>(d_x));
+    return cuda_status(cudaGetLastError());
+}
+
+int ironav_prop_head_fwd(const void* d_feat, int n, const float* d_hw, const float* d_hb, float* d_out, void* stream) {
+    if (!d_feat || !d_hw || !d_hb || !d_out || n < 1 || n > (1 << 22)) return IRONAV_INVALID_ARGUMENT;
+    prop::head_fwd_kernel<<<n, 256, 0, static_cast<cudaStream_t>(stream)>>>(static_cast<const __nv_bfloat16*>(d_feat), (long long)n * RPIX,
+                                                                             d_hw, d_hb, d_out);
+    return cuda_status(cudaGetLastError());
+}
+
+int ironav_prop_loss(const float* d_out, const int16_t* d_target_mv, const uint8_t* d_target_part, int n, float* d_dout, float* d_sums,
+                     void* stream) {
+    if (!d_out || !d_target_mv || !d_target_part || !d_dout || !d_sums || n < 1) return IRONAV_INVALID_ARGUMENT;
+    prop::loss_kernel<<<(n + 127) / 128, 128, 0, static_cast<cudaStream_t>(stream)>>>(d_out, d_target_mv, d_target_part, n, d_dout, d_sums);
+    return cuda_status(cudaGetLastError());
+}
+
+int ironav_prop_head_bwd(const void* d_feat, int n, const float* d_dout, const float* d_hw, float* d_ghw, float* d_ghb, void* d_dz,
+                         void* stream) {
+    if (!d_feat || !d_dout || !d_hw || !d_ghw || !d_dz || n < 1 || n > (1 << 22) || !aligned16(d_dz)) return IRONAV_INVALID_ARGUMENT;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const long long Q = (long long)n * RPIX;
+    const __nv_bfloat16* feat = static_cast<const __nv_bfloat16*>(d_feat);
+    // the ring of dz is zero (its interior is written below)
+    CK(cudaMemsetAsync(d_dz, 0, (size_t)4 * Q * 16, st));
+    prop::head_wgrad_kernel<<<(prop::NFEAT + 255) / 256, 256, 0, st>>>(feat, Q, n, d_dout, d_ghw, d_ghb);
+    const long long total = (long long)n * prop::NFEAT;
+    prop::head_dgrad_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(feat, Q, n, d_dout, d_hw, static_cast<__nv_bfloat16*>(d_dz));
+    return cuda_status(cudaGetLastError());
+}
+
+int ironav_prop_adam(float* d_p, float* d_g, float* d_m, float* d_v, long long n, float lr, float beta1, float beta2, int step, float eps,
+                     void* stream) {
+    if (!d_p || !d_g || !d_m || !d_v || n < 1 || step < 1) return IRONAV_INVALID_ARGUMENT;
+    const float c1 = 1.f - std::pow(beta1, (float)step), c2 = 1.f - std::pow(beta2, (float)step);
+    prop::adam_kernel<<<(unsigned)((n + 255) / 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(d_p, d_g, d_m, d_v, n, lr, beta1, beta2, c1,
+                                                                                                   c2, eps);
+    return cuda_status(cudaGetLastError());
+}
+
+int ironav_prop_weights(const float* d_w, int cin, void* d_wf, void* d_wt, void* stream) {
+    if (!d_w || !d_wf || (cin != 16 && cin != 32) || (d_wt && cin != 32)) return IRONAV_INVALID_ARGUMENT;
+    prop::weights_kernel<<<(9 * 32 * cin + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        d_w, cin, static_cast<__nv_bfloat16*>(d_wf), static_cast<__nv_bfloat16*>(d_wt));
+    return cuda_status(cudaGetLastError());
+}
+
+int ironav_prop_propose(const float* d_out, int n, int16_t* d_cands, uint8_t* d_cls, void* stream) {
+    if (!d_out || !d_cands || !d_cls || n < 1 || n > (1 << 22)) return IRONAV_INVALID_ARGUMENT;
+    prop::propose_kernel<<<(n + 127) / 128, 128, 0, static_cast<cudaStream_t>(stream)>>>(d_out, n, d_cands, d_cls);
+    return cuda_status(cudaGetLastError());
+}
+
+}  // extern "C"

@@ -221,6 +221,129 @@ __global__ void __launch_bounds__(128, 1) conv3x3_kernel(const __grid_constant__
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 32;" ::"r"(tmem));
 }
 
+// The weight gradient of a 3x3 layer: dw[t][o][i] += sum over pixels q of dz[q][o] * x[q + shift_t][i] (FP32,
+// accumulated into dw with atomics), and db[o] += sum over q of dz[q][o]. As MMAs: M = 128 rows (a group of
+// 128 / CIN taps x CIN input channels), N = 32 output channels, K = pixels; both operands MN-major (a pixel's 8
+// channels contiguous, pixels 16 bytes apart), so the chunk-major tensors are their own canonical layout. Per
+// tile of KT pixels, TMA stages the nine tap-shifted views of x ([tap slot][plane][pixel][16 B], taps beyond
+// 8 stay zero) and the tile of dz; one thread issues groups x KT / 16 MMAs into one TMEM accumulator per group
+// (32 columns each), accumulating over all the CTA's tiles; at the end each warp reads its 32 rows and adds them
+// to dw. xmap: x as (8, Q, CIN / 8) with boxes of KT pixels; zmap: dz as (8, Q, 4) with the same boxes.
+constexpr int WG_KT = 128;  // pixels a tile (K)
+
+template <int CIN>
+constexpr int wgrad3x3_smem_bytes() {
+    return ((9 + 128 / CIN - 1) / (128 / CIN)) * 128 * WG_KT * 2 + 4 * WG_KT * 16 + 2 * 8 + 16 + 32 * 4;
+}
+
+// MN-major operands for the weight gradient: M (or N) 8 channels of a pixel contiguous, K = pixels 16 bytes apart.
+constexpr uint32_t IDESC_BF16_MN_M128_N32 = (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | (1u << 16) | ((COUT >> 3) << 17) | ((TILE >> 4) << 24);
+
+template <int CIN>
+__global__ void __launch_bounds__(128, 1) wgrad3x3_kernel(const __grid_constant__ CUtensorMap xmap, const __grid_constant__ CUtensorMap zmap,
+                                                          float* __restrict__ dw, float* __restrict__ db, long long Q, int tiles,
+                                                          unsigned* err) {
+    constexpr int KC = CIN / 8, TPG = 128 / CIN, NG = (9 + TPG - 1) / TPG;
+    constexpr int PLANE = WG_KT * 16;          // bytes of one plane's tile
+    constexpr int ABYTES = NG * 16 * PLANE;    // NG groups x 16 planes (TPG taps x KC planes)
+    constexpr int BBYTES = 4 * PLANE;
+    constexpr unsigned TX = 9 * KC * PLANE + BBYTES;
+    constexpr int NCOL = NG * 32 <= 32 ? 32 : (NG * 32 <= 64 ? 64 : 128);
+    extern __shared__ __align__(1024) uint8_t smem[];
+    uint8_t* as = smem;
+    uint8_t* bs = smem + ABYTES;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + ABYTES + BBYTES);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2);
+    float* dbs = reinterpret_cast<float*>(tmem_slot + 4);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    // the slots of taps 9.. stay zero (their rows accumulate nothing)
+    for (int i = tid; i < (NG * TPG - 9) * KC * PLANE / 16; i += 128)
+        reinterpret_cast<uint4*>(as + 9 * KC * PLANE)[i] = make_uint4(0, 0, 0, 0);
+    if (tid < 32) dbs[tid] = 0.f;
+    if (tid == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)), "n"(NCOL));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+    bool failed = false, load_pending = false, mma_pending = false, any = false;
+    unsigned it = 0;
+    float dbsum = 0.f;  // this thread's share of db: channel lane, pixels warp, warp + 4, ...
+    for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x, it++) {
+        const long long q0 = (long long)tile * WG_KT;
+        if (tid == 0) {
+            mbar_expect_tx(&bars[0], TX);
+            for (int t = 0; t < 9; t++) {
+                const int shift = (t / 3 - 1) * RW + (t % 3 - 1);
+                tma_load_3d(as + (t / TPG) * 16 * PLANE + (t % TPG) * KC * PLANE, &xmap, 0, (int)(q0 + shift), 0, &bars[0]);
+            }
+            tma_load_3d(bs, &zmap, 0, (int)q0, 0, &bars[0]);
+        }
+        const bool loaded = mbar_wait(&bars[0], it & 1);
+        if (__syncthreads_or(!loaded)) {
+            failed = load_pending = true;
+            break;
+        }
+        if (tid == 0) {
+            tc_fence_after();
+            const uint32_t a0 = smem_u32(as), b0 = smem_u32(bs);
+#pragma unroll 1
+            for (int g = 0; g < NG; g++)
+#pragma unroll
+                for (int k = 0; k < WG_KT / 16; k++) {
+                    const uint64_t ad = smem_desc(a0 + (uint32_t)(g * 16 * PLANE + k * 256), 128, PLANE);
+                    const uint64_t bd = smem_desc(b0 + (uint32_t)(k * 256), 128, PLANE);
+                    mma_bf16(tmem + (uint32_t)(g * 32), ad, bd, IDESC_BF16_MN_M128_N32, (any || k != 0) ? 1u : 0u);
+                }
+            mma_commit(&bars[1]);
+        }
+        any = true;
+        // the bias gradient from the staged dz tile: thread (warp, lane) sums channel lane over pixels warp, warp + 4, ...
+        {
+            const __nv_bfloat16* z = reinterpret_cast<const __nv_bfloat16*>(bs);
+            for (int p = warp; p < WG_KT; p += 4) dbsum += __bfloat162float(z[((lane >> 3) * WG_KT + p) * 8 + (lane & 7)]);
+        }
+        const bool computed = mbar_wait(&bars[1], it & 1);
+        if (__syncthreads_or(!computed)) {
+            failed = mma_pending = true;
+            break;
+        }
+        tc_fence_before();
+        __syncthreads();
+    }
+    if (failed && tid == 0) atomicOr(err, 1u);
+    if (load_pending) mbar_wait(&bars[0], it & 1);
+    if (mma_pending) mbar_wait(&bars[1], it & 1);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (!failed && any) {
+        atomicAdd(&dbs[lane], dbsum);
+        for (int g = 0; g < NG; g++) {
+            float v[32];
+            tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(g * 32), v);
+            const int m = warp * 32 + lane, t = g * TPG + m / CIN, i = m % CIN;
+            if (t < 9)
+#pragma unroll
+                for (int o = 0; o < 32; o++) atomicAdd(&dw[(t * COUT + o) * CIN + i], v[o]);
+        }
+        __syncthreads();
+        if (tid < 32 && db != nullptr) atomicAdd(&db[tid], dbs[tid]);
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "n"(NCOL));
+}
+
 template <int CIN>
 constexpr int conv3x3_smem_bytes() {
     return 9 * (CIN / 8) * COUT * 16 + (CIN / 8) * HALO * 16 + 2 * 8 + 16;

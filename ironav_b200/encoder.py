@@ -76,6 +76,8 @@ class Encoder:
         self.codes = None
         self.states = None
         self.params = write_parameter_sets(width, height, bd, fps, refs, lib=self.lib)
+        # called as before_p(encoder, y) once a P picture's parameters are set and before it is decided
+        self.before_p = None
 
     def close(self) -> None:
         self.st.close()
@@ -95,6 +97,8 @@ class Encoder:
             data = self.params + st.write_slices(True, L.frame_num, L.idr_id, codes)
         else:
             st.begin_p_picture(qpp, nrefs_active=min(L.held, L.nrefs), fast=self.fast, sub8=self.sub8)
+            if self.before_p is not None:
+                self.before_p(self, y)
             states, codes, rec = st.decide_p_picture()
             data = st.write_slices(False, L.frame_num, 0, codes)
         mbs = st.decide_dbk_records(codes, states)
@@ -137,6 +141,9 @@ class DeviceEncoder:
         self.slices = np.zeros(nslices, dtype=DBK_SLICE_DTYPE)  # every slice filtered, no offsets (enc/mod.rs:648)
         self.k = 0
         self.params = write_parameter_sets(width, height, bd, fps, refs, lib=self.lib)
+        # called as before_p(encoder, d_y, stride) once a P picture's parameters are set and before it is
+        # decided, on the encoder's stream (the learned form computes its proposals there)
+        self.before_p = None
 
     def close(self) -> None:
         self.st.close()
@@ -185,6 +192,8 @@ class DeviceEncoder:
             data = self.params + st.write_slices_device(True, L.frame_num, L.idr_id, codes.data_ptr())
         else:
             st.begin_p_picture(qpp, nrefs_active=min(L.held, L.nrefs), fast=self.fast, sub8=self.sub8)
+            if self.before_p is not None:
+                self.before_p(self, d_y, stride)
             self._check(lib.ironav_decide_p_picture_device(st.ctx, sts.data_ptr(), codes.data_ptr(), ry.data_ptr(), pw,
                                                            rc[0].data_ptr(), rc[1].data_ptr(), cw), "ironav_decide_p_picture_device")
             data = st.write_slices_device(False, L.frame_num, 0, codes.data_ptr())

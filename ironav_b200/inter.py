@@ -135,6 +135,9 @@ EXPORTS = (
     "ironav_push_reference_chroma_device",
     "ironav_write_parameter_sets", "ironav_write_slices", "ironav_write_slices_device",
     "ironav_batch_set_tuning", "ironav_batch_get_tuning", "ironav_batch_autotune",
+    "ironav_prop_conv3x3", "ironav_prop_wgrad3x3", "ironav_prop_prep", "ironav_prop_head_fwd", "ironav_prop_loss",
+    "ironav_prop_head_bwd", "ironav_prop_adam", "ironav_prop_weights", "ironav_set_learned",
+    "ironav_prop_propose",
 )
 
 # ironav_batch_tuning (include/ironav_inter.h): the batched step's knobs
@@ -214,6 +217,20 @@ def _declare(lib: ctypes.CDLL) -> ctypes.CDLL:
         lib.ironav_batch_destroy.argtypes = [_VP]
         lib.ironav_batch_step.argtypes = [_VP] + [ctypes.POINTER(_VP)] * 5
         lib.ironav_batch_sync.argtypes = [_VP]
+    if hasattr(lib, "ironav_prop_conv3x3"):
+        _LL, _F = ctypes.c_longlong, ctypes.c_float
+        lib.ironav_prop_conv3x3.argtypes = [_VP, _I, _LL, _VP, _VP, _I, _VP, _VP, _VP, _VP]
+        lib.ironav_prop_wgrad3x3.argtypes = [_VP, _I, _VP, _LL, _VP, _VP, _VP, _VP]
+        lib.ironav_prop_prep.argtypes = [_VP, _I, _VP, _VP]
+        lib.ironav_prop_head_fwd.argtypes = [_VP, _I, _VP, _VP, _VP, _VP]
+        lib.ironav_prop_loss.argtypes = [_VP, _VP, _VP, _I, _VP, _VP, _VP]
+        lib.ironav_prop_head_bwd.argtypes = [_VP, _I, _VP, _VP, _VP, _VP, _VP, _VP]
+        lib.ironav_prop_adam.argtypes = [_VP, _VP, _VP, _VP, _LL, _F, _F, _F, _I, _F, _VP]
+        lib.ironav_prop_weights.argtypes = [_VP, _I, _VP, _VP, _VP]
+    if hasattr(lib, "ironav_prop_propose"):
+        lib.ironav_prop_propose.argtypes = [_VP, _I, _VP, _VP, _VP]
+    if hasattr(lib, "ironav_set_learned"):
+        lib.ironav_set_learned.argtypes = [_VP, _VP, _VP, _I, _VP]
     if hasattr(lib, "ironav_batch_autotune"):
         lib.ironav_batch_set_tuning.argtypes = [_VP, _VP]
         lib.ironav_batch_get_tuning.argtypes = [_VP, _VP]

@@ -322,6 +322,11 @@ struct ironav_ctx {
     ironav_mbstate* b_col;  /* the list-1 picture's decisions, or NULL */
     int b_tb, b_td, b_set;
     uint16_t* src_c[2]; /* the source's chroma, padded to 8*mb_w x 8*mb_h */
+    /* the learned form's proposals (ironav_set_learned; host pointers here) */
+    const int16_t* learned;
+    const uint8_t* learned_cls;
+    int learned_margin;
+    unsigned* learned_stats;
 };
 
 typedef struct fc {
@@ -721,12 +726,94 @@ static void best_inter_ref(const fc* f, counters* cnt, int mbx, int mby, int r, 
 #undef AT8
 }
 
-/* best_inter, enc/frame.rs:839-849 */
+/* The learned form's judge (no counterpart in the reference): the 16x16 partitioning of the newest reference
+ * from the proposals instead of the search. Every integer vector within +-2 samples of each of the 4 proposals
+ * (rounded to the integer grid and clamped as motion_search clamps its candidates) is scored by SAD + lambda *
+ * bits, the first of least cost in proposal-major, row-major order wins; then motion_search's sub-sample
+ * refinement (994-1017). Returns 0 (the caller searches) when the proposed class is not P_Skip or 16x16, or when
+ * the winner costs more than the predictor's own start plus the margin; counters as ironav_set_learned states. */
+static int learned_inter(const fc* f, counters* cnt, int mbx, int mby, inter_res* best) {
+    const struct ironav_ctx* c = f->c;
+    const int r = 0, lam = c->lambda, mb = mby * c->mb_w + mbx;
+    if (c->learned_cls[mb] >= 2) {
+        __atomic_fetch_add(&c->learned_stats[1], 1u, __ATOMIC_RELAXED);
+        return 0;
+    }
+    int mvp[2];
+    mv_pred(f, mbx, mby, r, mvp);
+    const int x0 = mbx * 16, y0 = mby * 16, w = 16, h = 16;
+    const int cxlo = maxi(-(x0 + 24) * 4, -2048), cxhi = mini((c->mb_w * 16 - x0 + 8) * 4, 2047);
+    const int cylo = maxi(-(y0 + 24) * 4, -512), cyhi = mini((c->mb_h * 16 - y0 + 8) * 4, 511);
+#define CLX(v) clampi((v), cxlo, cxhi)
+#define CLY(v) clampi((v), cylo, cyhi)
+#define INTR(v) (((v) + 2) & ~3)
+#define COST_INT(mx, my) (sad_int(f, r, x0, y0, w, h, (mx), (my)) + lam * mvd_bits((mx), (my), mvp[0], mvp[1]))
+    const int16_t* cand = c->learned + (size_t)mb * 8;
+    int bx = 0, by = 0, bc = 0x7fffffff;
+    for (int i = 0; i < 100; i++) {
+        const int k = i / 25, d = i % 25;
+        const int px = CLX(INTR(CLX(cand[2 * k])) + 4 * (d % 5 - 2)), py = CLY(INTR(CLY(cand[2 * k + 1])) + 4 * (d / 5 - 2));
+        const int cost = COST_INT(px, py);
+        if (cost < bc) {
+            bx = px;
+            by = py;
+            bc = cost;
+        }
+    }
+    const int start = COST_INT(INTR(CLX(mvp[0])), INTR(CLY(mvp[1])));
+    cnt->sad_px += 101u * 256u;
+    if (bc > start + c->learned_margin) {
+        __atomic_fetch_add(&c->learned_stats[2], 1u, __ATOMIC_RELAXED);
+        return 0;
+    }
+    uint16_t pred[256];
+    const halfpel* hp = &c->refs[r].hp;
+#define COST_SUB(mx, my)                                                                                   \
+    (cnt->satd_px += (uint32_t)(w * h), halfpel_predict(hp, x0, y0, (mx), (my), w, h, pred),              \
+     satd_blk(f, x0, y0, w, h, pred) + lam * mvd_bits((mx), (my), mvp[0], mvp[1]))
+    bc = COST_SUB(bx, by);
+    static const int SQUARE[8][2] = {{-1, -1}, {0, -1}, {1, -1}, {-1, 0}, {1, 0}, {-1, 1}, {0, 1}, {1, 1}};
+    static const int DIAMOND[4][2] = {{0, -1}, {-1, 0}, {1, 0}, {0, 1}};
+    for (int stage = 0; stage < 2; stage++) {
+        if (c->fast && stage == 1) break;
+        const int step = stage == 0 ? 2 : 1;
+        const int(*pts)[2] = stage == 0 ? SQUARE : DIAMOND;
+        const int npts = stage == 0 ? 8 : 4;
+        const int ccx = bx, ccy = by;
+        for (int k = 0; k < npts; k++) {
+            const int qx = CLX(ccx + pts[k][0] * step), qy = CLY(ccy + pts[k][1] * step);
+            const int cost = COST_SUB(qx, qy);
+            if (cost < bc) {
+                bx = qx;
+                by = qy;
+                bc = cost;
+            }
+        }
+    }
+#undef CLX
+#undef CLY
+#undef INTR
+#undef COST_INT
+#undef COST_SUB
+    memset(best, 0, sizeof(*best));
+    best->part = 0;
+    for (int i = 0; i < 16; i++) {
+        best->mvs[i][0] = (int16_t)bx;
+        best->mvs[i][1] = (int16_t)by;
+    }
+    /* the 16x16 cost of best_inter_ref (855-858): the vector's bits, the mb_type bit and ref_bits */
+    best->cost = bc + lam + lam * ref_bits(f, r);
+    best->cost16 = best->cost;
+    __atomic_fetch_add(&c->learned_stats[0], 1u, __ATOMIC_RELAXED);
+    return 1;
+}
+
+/* best_inter, enc/frame.rs:839-849 (the newest reference judged from the proposals when they are set) */
 static void best_inter(const fc* f, counters* cnt, int mbx, int mby, ironav_mbresult* out) {
     inter_res best, cur;
     int have = 0, bestr = 0;
     for (int r = 0; r < f->c->nact; r++) {
-        best_inter_ref(f, cnt, mbx, mby, r, &cur);
+        if (!(r == 0 && f->c->learned && learned_inter(f, cnt, mbx, mby, &cur))) best_inter_ref(f, cnt, mbx, mby, r, &cur);
         if (!have || cur.cost < best.cost) {
             best = cur;
             bestr = r;
@@ -3422,4 +3509,45 @@ int oracle_put_nal(int ref_idc, int kind, const uint8_t* rbsp, int n, uint8_t* o
     if (len <= cap) memcpy(out, w.buf, w.len);
     free(w.buf);
     return len;
+}
+
+int ironav_set_learned(ironav_ctx* c, const int16_t* cands, const uint8_t* cls, int margin, unsigned* stats) {
+    if (!c || (cands && (!cls || !stats)) || margin < 0) return IRONAV_INVALID_ARGUMENT;
+    c->learned = cands;
+    c->learned_cls = cands ? cls : NULL;
+    c->learned_stats = cands ? stats : NULL;
+    c->learned_margin = margin;
+    return IRONAV_OK;
+}
+
+/* The learned proposer's kernels exist only on the device */
+int ironav_prop_conv3x3(const void* x, int cin, long long n, const void* w, const float* b, int relu, const void* m, void* y, unsigned* err, void* s) {
+    (void)x; (void)cin; (void)n; (void)w; (void)b; (void)relu; (void)m; (void)y; (void)err; (void)s;
+    return IRONAV_HARDWARE_UNAVAILABLE;
+}
+int ironav_prop_wgrad3x3(const void* x, int cin, const void* dz, long long n, float* dw, float* db, unsigned* err, void* s) {
+    (void)x; (void)cin; (void)dz; (void)n; (void)dw; (void)db; (void)err; (void)s;
+    return IRONAV_HARDWARE_UNAVAILABLE;
+}
+int ironav_prop_prep(const ironav_prop_sample* sm, int n, void* x, void* s) { (void)sm; (void)n; (void)x; (void)s; return IRONAV_HARDWARE_UNAVAILABLE; }
+int ironav_prop_head_fwd(const void* f, int n, const float* hw, const float* hb, float* o, void* s) {
+    (void)f; (void)n; (void)hw; (void)hb; (void)o; (void)s;
+    return IRONAV_HARDWARE_UNAVAILABLE;
+}
+int ironav_prop_loss(const float* o, const int16_t* tm, const uint8_t* tp, int n, float* d, float* sums, void* s) {
+    (void)o; (void)tm; (void)tp; (void)n; (void)d; (void)sums; (void)s;
+    return IRONAV_HARDWARE_UNAVAILABLE;
+}
+int ironav_prop_head_bwd(const void* f, int n, const float* d, const float* hw, float* ghw, float* ghb, void* dz, void* s) {
+    (void)f; (void)n; (void)d; (void)hw; (void)ghw; (void)ghb; (void)dz; (void)s;
+    return IRONAV_HARDWARE_UNAVAILABLE;
+}
+int ironav_prop_adam(float* p, float* g, float* m, float* v, long long n, float lr, float b1, float b2, int step, float eps, void* s) {
+    (void)p; (void)g; (void)m; (void)v; (void)n; (void)lr; (void)b1; (void)b2; (void)step; (void)eps; (void)s;
+    return IRONAV_HARDWARE_UNAVAILABLE;
+}
+int ironav_prop_weights(const float* w, int cin, void* wf, void* wt, void* s) { (void)w; (void)cin; (void)wf; (void)wt; (void)s; return IRONAV_HARDWARE_UNAVAILABLE; }
+int ironav_prop_propose(const float* o, int n, int16_t* c, uint8_t* k, void* s) {
+    (void)o; (void)n; (void)c; (void)k; (void)s;
+    return IRONAV_HARDWARE_UNAVAILABLE;
 }
