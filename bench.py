@@ -55,10 +55,11 @@ def parse():
                    help="pictures in the ring (fewer than 36 fits in L2: for profiling runs only)")
     p.add_argument("--no-e2e", action="store_true", help="skip the host-buffer pass (profiling runs)")
     p.add_argument("--workload", default="1080p", choices=["1080p", "batched", "scenecut", "deblock", "bpicture", "residual", "decide",
-                                                         "decide_batched", "inloop", "encode"],
+                                                         "decide_batched", "inloop", "encode", "learned"],
                    help="1080p: one stream, replay mode (the headline); batched: 64 mixed-resolution streams in auto "
                         "mode, one launch per stage and frame step, against the per-stream launch loop")
     p.add_argument("--streams", type=int, default=64, help="streams of the batched workload")
+    p.add_argument("--learned-samples", type=int, default=2_000_000, help="training samples of the learned workload's proposer")
     p.add_argument("--e2e-threads", type=int, default=8, help="host threads (each with a context) of the e2e pass")
     p.add_argument("--bd", type=int, default=8, choices=[8, 10],
                    help="sample depth of the 1080p workload: 8 (Yuv420p) or 10 (Yuv420p10, QP' = QP + 12)")
@@ -354,6 +355,9 @@ def main():
         return finish(world)
     if args.workload == "encode":
         run_encode(args, rank, world)
+        return finish(world)
+    if args.workload == "learned":
+        run_learned(args, rank, world)
         return finish(world)
 
     import torch
@@ -687,6 +691,202 @@ def run_encode(args, rank, world):
         line["cpu_baseline"] = {"value": (k - 1) * nmb / el_o, "unit": "MB/s", "cores": threads, "kind": "port",
                                 "sample": f"{k - 1} P pictures of the same sequence through the oracle's encoder loop (host buffers), "
                                           f"decide mode on {threads} threads, {el_o:.2f} s"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def run_learned(args, rank, world):
+    """The learned form (ironav_b200.learned, the north star's form 4) on the 1080p sequence. Untimed first: the
+    training data from the plain search on three unseen-seed 1080p sequences (11 pictures each at QP 22, 27
+    and 32, eight bands), Adam on `--learned-samples` samples, and the quality of both forms through the
+    device encoder at QP 22, 27 and 32 (bytes and luma PSNR of the benchmark's sequence, 11 pictures). Timed:
+    one step is one 1080p P picture in auto mode (QP 27, eight bands): the reference's half-sample planes, then
+    the proposer's input, four tcgen05 conv layers, head and proposals, then the analysis with the exact-cost
+    judge; the plain auto-mode step (planes + analysis) is timed the same way beside it. `e2e` uploads each
+    picture from pinned host memory and brings its results back."""
+    import torch
+    import torch.distributed as dist
+    from ironav_b200 import learned
+    from ironav_b200.inter import MBRESULT_DTYPE, MBSTATE_DTYPE, InterStage
+    from ironav_b200.proposer import Proposer
+    from ironav_b200.synth import CONFIGS, Sequence
+
+    dev = torch.device("cuda", torch.cuda.current_device())
+    t0 = time.perf_counter()
+    data = learned.TrainingSet().collect(sequences=3, frames=11, qps=(22, 27, 32), nslices=NSLICES)
+    collect_s = time.perf_counter() - t0
+    n_train = len(data)
+    prop = Proposer(max_batch=512)
+    hist = learned.train(prop, data, samples=args.learned_samples, batch=512, lr=1e-3, log_every=1000)
+    train_s = time.perf_counter() - t0 - collect_s
+    del data
+    torch.cuda.empty_cache()
+    seq_eval = Sequence.config("1080p", 11)
+    quality = []
+    for qp in (22, 27, 32):
+        plain = learned.encode_sequence(seq_eval, qp, 11, nslices=NSLICES)
+        lrn = learned.encode_sequence(seq_eval, qp, 11, prop=prop, nslices=NSLICES)
+        searched = lrn["judged"] + lrn["class_fallback"] + lrn["cost_fallback"]
+        quality.append({"qp": qp, "bytes_plain": plain["bytes"], "bytes_learned": lrn["bytes"],
+                        "bytes_delta_pct": 100.0 * (lrn["bytes"] - plain["bytes"]) / plain["bytes"],
+                        "psnr_y_plain": plain["psnr_y"], "psnr_y_learned": lrn["psnr_y"],
+                        "psnr_delta_db": lrn["psnr_y"] - plain["psnr_y"],
+                        "fallback_rate": (lrn["class_fallback"] + lrn["cost_fallback"]) / max(1, searched),
+                        "judged": lrn["judged"], "class_fallback": lrn["class_fallback"], "cost_fallback": lrn["cost_fallback"]})
+
+    # the timed pictures: a ring of the benchmark sequence in device memory (with its activations, far above L2)
+    w, h, seed, pan_q, nobj, vmax, sigma = CONFIGS["1080p"]
+    npic = args.warmup + args.steps + 1
+    seq = Sequence(w, h, npic, seed + 0x1000 * rank, pan_q, nobj, vmax, sigma)
+    host = [seq.frame(t) for t in range(npic)]
+    d_pics = torch.from_numpy(np.stack(host)).to(dev)
+    st = InterStage(w, h, nslices=NSLICES)
+    stream = torch.cuda.Stream()
+    st.set_stream(stream.cuda_stream)
+    prop.stream = stream
+    n = st.nmb
+    d_states = torch.zeros(n * MBSTATE_DTYPE.itemsize, dtype=torch.uint8, device=dev)
+    d_out = torch.zeros(n * MBRESULT_DTYPE.itemsize, dtype=torch.uint8, device=dev)
+    cands = torch.zeros((n, 8), dtype=torch.int16, device=dev)
+    cls = torch.zeros(n, dtype=torch.uint8, device=dev)
+    stats = torch.zeros(3, dtype=torch.int32, device=dev)
+    smp = [None] + [torch.from_numpy(learned.picture_samples(d_pics[t].data_ptr(), d_pics[t - 1].data_ptr(), w, h, w, w).view(np.uint8))
+                    .to(dev) for t in range(1, npic)]
+    conv_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(npic)]
+
+    def set_learned(on: bool):
+        if on:
+            st._check(st.lib.ironav_set_learned(st.ctx, cands.data_ptr(), cls.data_ptr(), 0, stats.data_ptr()), "ironav_set_learned")
+        else:
+            st._check(st.lib.ironav_set_learned(st.ctx, None, None, 0, None), "ironav_set_learned")
+
+    def step(t: int, on: bool, d_cur=None, d_prev=None, d_smp=None):
+        cur = d_pics[t].data_ptr() if d_cur is None else d_cur
+        prev = d_pics[t - 1].data_ptr() if d_prev is None else d_prev
+        st.clear_references()
+        st.push_reference_device(prev, w, w, h, None)
+        st.set_source_device(cur, w)
+        st.begin_p_picture(QP, 1)
+        if on:
+            prop.set_samples_device((smp[t] if d_smp is None else d_smp).data_ptr(), n)
+            prop.forward(n, conv_events=conv_ev[t] if d_cur is None else None)
+            prop.propose(n, cands.data_ptr(), cls.data_ptr())
+        st.analyse_auto_device(d_states.data_ptr(), d_out.data_ptr())
+
+    def timed(on: bool):
+        set_learned(on)
+        for t in range(1, args.warmup + 1):
+            step(t, on)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for t in range(args.warmup + 1, npic):
+            step(t, on)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return max_over_ranks(e0.elapsed_time(e1) * 1e-3, world, dev)
+
+    el_plain = timed(False)
+    clocks = Clocks(int(os.environ.get("LOCAL_RANK", "0")))
+    clocks.start()
+    stats.zero_()
+    el = timed(True)
+    clk = clocks.stop()
+    conv_ms = float(np.mean([a.elapsed_time(b) for a, b in conv_ev[args.warmup + 1:]]))
+    judge = stats.cpu().numpy()
+
+    # end to end: each picture uploaded from pinned host memory into a two-picture staging ring, the results
+    # brought back to pinned host memory, in stream order
+    pinned = [torch.from_numpy(host[t]).pin_memory() for t in range(npic)]
+    stage = [torch.zeros((h, w), dtype=torch.uint8, device=dev) for _ in range(2)]
+    stage_smp = [torch.from_numpy(learned.picture_samples(stage[k].data_ptr(), stage[k ^ 1].data_ptr(), w, h, w, w).view(np.uint8)).to(dev)
+                 for k in range(2)]
+    res_host = torch.zeros(n * MBRESULT_DTYPE.itemsize, dtype=torch.uint8).pin_memory()
+    set_learned(True)
+    with torch.cuda.stream(stream):
+        stage[0].copy_(pinned[0], non_blocking=True)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for t in range(1, npic):
+        k = t & 1
+        with torch.cuda.stream(stream):
+            stage[k].copy_(pinned[t], non_blocking=True)
+        step(t, True, d_cur=stage[k].data_ptr(), d_prev=stage[k ^ 1].data_ptr(), d_smp=stage_smp[k])
+        with torch.cuda.stream(stream):
+            res_host.copy_(d_out, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    el_e2e = max_over_ranks(e0.elapsed_time(e1) * 1e-3, world, dev)
+    prop.check_errors()
+
+    steps = npic - 1 - args.warmup
+    total = sum_over_ranks(n, world, dev)
+    # algorithmic FLOPs of the four layers on the 48 x 48 interior: 2 input channels, then 32
+    flops = n * 48 * 48 * 9 * 32 * 2 * (2 + 3 * 32)
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+    peak = float(peaks.get("bf16_tflops_sustained", 1400.0))
+    achieved = flops / (conv_ms * 1e-3) / 1e12
+    line = {
+        "metric": METRIC + " (learned form)",
+        "value": total * (npic - 1 - args.warmup) / el, "unit": "MB/s", "n_gpus": world, "steps": steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * el / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "bf16+u8",
+        "data": data_desc(8) + "; proposer trained on three other seeds of the same generator",
+        "config": {"workload": f"1080p 8-bit P pictures in auto mode, QP {QP}, {NSLICES} slice bands: half-sample planes, proposer "
+                               "(input, 4 tcgen05 conv3x3 layers of 32 channels, head, proposals), analysis with the exact-cost judge",
+                   "width": w, "height": h, "qp": QP, "slices": NSLICES,
+                   "plain_mb_per_s": total * steps / el_plain, "plain_ms_per_step": 1e3 * el_plain / steps,
+                   "learned_over_plain": el_plain / el,
+                   "quality_vs_plain": quality,
+                   "judge_timed": {"judged": int(judge[0]), "class_fallback": int(judge[1]), "cost_fallback": int(judge[2])},
+                   "training": {"samples_available": n_train, "samples_seen": hist[-1]["samples"], "collect_s": collect_s, "train_s": train_s,
+                                "first": hist[0], "last": hist[-1]},
+                   "l2": "each step reads its own picture and activations (1.3 GB a layer), far above L2",
+                   "parallelism": "replicas"},
+        "e2e": {"value": total * steps / el_e2e, "unit": "MB/s", "h2d_bytes_per_step": w * h,
+                "d2h_bytes_per_step": n * MBRESULT_DTYPE.itemsize, "ms_per_step": 1e3 * el_e2e / steps,
+                "note": "each picture copied in from pinned host memory, its result records copied out, in stream order"},
+        "gpu_launches": 10 * steps,  # per step: source copy 1, planes 1, prep 1, conv 4, head 1, propose 1, analysis 1
+        "roofline": {"bound": "tensor", "kernel": "conv3x3_kernel (4 layers)", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak, "traffic": None,
+                     "note": f"algorithmic FLOPs of the 48 x 48 interior ({flops / 1e12:.3f} TFLOP a picture) over the four layers' "
+                             f"CUDA-event time ({conv_ms:.3f} ms a step); peak: MEASURED_PEAKS.json bf16_tflops_sustained (measured)"},
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from tests.oracle_lib import oracle_library
+
+        lib = oracle_library()
+        threads = min(host_cores(), NSLICES)
+        o = InterStage(w, h, nslices=NSLICES, lib=lib)
+        lib.oracle_set_threads(o.ctx, threads)
+        hc = np.zeros((n, 8), dtype=np.int16)
+        hk = np.zeros(n, dtype=np.uint8)
+        hs = np.zeros(3, dtype=np.uint32)
+        assert lib.ironav_set_learned(o.ctx, hc.ctypes.data, hk.ctypes.data, 0, hs.ctypes.data) == 0
+        k, el_o = 1, 0.0
+        while el_o < min(args.cpu_seconds, 8.0) and k < npic:
+            step(k, True)  # the proposals of picture k, on the GPU
+            torch.cuda.synchronize()
+            hc[:] = cands.cpu().numpy()
+            hk[:] = cls.cpu().numpy()
+            t1 = time.perf_counter()
+            o.clear_references()
+            o.push_reference(host[k - 1])
+            o.set_source(host[k])
+            o.begin_p_picture(QP, 1)
+            o.analyse_auto()
+            el_o += time.perf_counter() - t1
+            k += 1
+        o.close()
+        line["cpu_baseline"] = {"value": (k - 1) * n / el_o, "unit": "MB/s", "cores": threads, "kind": "port",
+                                "sample": f"{k - 1} P pictures of the same sequence, the oracle's auto-mode analysis with the GPU's "
+                                          f"proposals on {threads} threads (the proposer itself untimed), {el_o:.2f} s"}
+    st.close()
     if rank == 0:
         print(json.dumps(line), flush=True)
 

@@ -566,8 +566,9 @@ int ironav_prop_adam(float* d_p, float* d_g, float* d_m, float* d_v, long long n
  * for its data gradient: transposed and mirrored, d_wt[t][i][o] = w[8 - t][o][i]. */
 int ironav_prop_weights(const float* d_w, int cin, void* d_wf, void* d_wt, void* stream);
 /* The judge's inputs from the head's outputs of n macroblocks (in raster order): d_cands[s][k] = the k-th vector
- * in quarter samples (rounded, clamped to +-2048 x +-512), d_cls[s] = the partition class of largest logit. */
-int ironav_prop_propose(const float* d_out, int n, int16_t* d_cands, uint8_t* d_cls, void* stream);
+ * in quarter samples (rounded, clamped to +-2048 x +-512), d_cls[s] = the partition class of largest logit when
+ * its softmax probability is at least min_conf, else 5 (unsure: the plain search). */
+int ironav_prop_propose(const float* d_out, int n, float min_conf, int16_t* d_cands, uint8_t* d_cls, void* stream);
 
 /* The learned form's judge (no counterpart in the reference: the north star's form 4). With proposals set, the
  * context's analyses (auto, replay, in-loop and decide modes) judge the newest reference's 16x16 partitioning
@@ -576,7 +577,7 @@ int ironav_prop_propose(const float* d_out, int n, int16_t* d_cands, uint8_t* d_
  * plain search (best_inter) takes over when the proposed partitioning class is not P_Skip or 16x16, or when
  * the best proposal costs more than the predictor's start plus `margin`. d_cands: per macroblock 4 vectors
  * (x, y) in quarter samples (int16, mb_w*mb_h*8); d_cls: per macroblock the class (0 P_Skip, 1 16x16, 2 16x8,
- * 3 8x16, 4 8x8); d_stats: 3 counters the analyses add to (judged from the proposals, fallbacks on the class,
+ * 3 8x16, 4 8x8, 5 unsure); d_stats: 3 counters the analyses add to (judged from the proposals, fallbacks on the class,
  * fallbacks on the cost). Device pointers, read when the analyses run; d_cands NULL: the plain search again.
  * The oracle implements the same judge on host pointers. */
 int ironav_set_learned(ironav_ctx* ctx, const int16_t* d_cands, const uint8_t* d_cls, int margin, unsigned* d_stats);

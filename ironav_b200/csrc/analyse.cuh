@@ -413,6 +413,63 @@ static __device__ __noinline__ void pred_batch_ni(const AnalyseParams& __restric
     pred_batch<T>(P, S, r, bx, by, lgw, lgh, n, false);
 }
 
+// One round of the diamond (enc/frame.rs:973-988) at `step` around (bxv, byv) of cost bc: the 3x3 square of the
+// step is scored in one batch (lane group g -> square position k = g < 4 ? g : g + 1), then the reference's four
+// moves are replayed in order (left, else right; then up from that column, else down). Returns whether the
+// centre moved; (bxv, byv, bc) become the new centre. g0 and src0 as for sad_lane, sw the plane stride.
+template <class T, bool MORE>
+static __device__ __forceinline__ bool diamond_round(const AnalyseParams& __restrict__ P, WarpSmem<T>& __restrict__ S, int r, int bx, int by, int w,
+                                                     int h, int mvpx, int mvpy, int step, int cxlo, int cxhi, int cylo, int cyhi,
+                                                     const uint8_t* __restrict__ g0, const uint32_t* __restrict__ src0, int sw, int& bxv,
+                                                     int& byv, int& bc) {
+    const int lane = threadIdx.x & 31, g = lane & 7;
+    const int lam = P.lambda;
+    const int k = g < 4 ? g : g + 1, kx = k % 3, ky = k / 3;
+    auto clx = [&](int v) { return min(max(v, cxlo), cxhi); };
+    auto cly = [&](int v) { return min(max(v, cylo), cyhi); };
+    const int cx = bxv, cy = byv, c0 = bc;
+    const int X0 = clx(cx - step), X2 = clx(cx + step), Y0 = cly(cy - step), Y2 = cly(cy + step);
+    const int qx = kx == 0 ? X0 : (kx == 1 ? cx : X2), qy = ky == 0 ? Y0 : (ky == 1 ? cy : Y2);
+    const int sc = (MORE ? sad_lane_ni<T>(g0, src0, sw, w, h, qx, qy, true) : sad_lane<T>(g0, src0, sw, w, h, qx, qy, true)) + lam * mvd_bits_d(qx, qy, mvpx, mvpy);
+    bool moved;
+    if (X0 == cx - step && X2 == cx + step && Y0 == cy - step && Y2 == cy + step) {
+        // no clamp: left, else right; then up from that column, else down
+        const int sL = __shfl_sync(FULL, sc, 3), sR = __shfl_sync(FULL, sc, 4);
+        int col = 1, b1 = c0;
+        if (sL < c0) {
+            col = 0;
+            b1 = sL;
+        } else if (sR < c0) {
+            col = 2;
+            b1 = sR;
+        }
+        const int sU = __shfl_sync(FULL, sc, col), sD = __shfl_sync(FULL, sc, 5 + col);
+        int row = 1, b2 = b1;
+        if (sU < b1) {
+            row = 0;
+            b2 = sU;
+        } else if (sD < b1) {
+            row = 2;
+            b2 = sD;
+        }
+        bxv = col == 0 ? X0 : (col == 1 ? cx : X2);
+        byv = row == 0 ? Y0 : (row == 1 ? cy : Y2);
+        bc = b2;
+        moved = col != 1 || row != 1;
+    } else {
+        if (lane < 8) S.cost[k] = sc;
+        if (lane == 0) S.cost[4] = c0;
+        __syncwarp();
+        const int4 rc = round_clamped(P, S, r, bx, by, w, h, mvpx, mvpy, step, cxlo, cxhi, cylo, cyhi, bxv, byv, bc);
+        moved = rc.x != 0;
+        bxv = rc.y;
+        byv = rc.z;
+        bc = rc.w;
+        __syncwarp();
+    }
+    return moved;
+}
+
 // Returns the best vector in (ox, oy) and its cost without the vector's bits. The search runs on the
 // half-sample planes P.planes[r]; the neighbour candidates come from the table `ext` of the list searched
 // and count when their reference index is rsel. (e0x, e0y) and (e1x, e1y) are the first extra candidates
@@ -495,54 +552,13 @@ static __device__ __noinline__ int4 motion_search(const AnalyseParams& __restric
     // batch (group g -> square position k = g < 4 ? g : g + 1), then replays the four moves in order
     const bool fast = P.fast != 0;
     const int nsteps = fast ? 2 : 3;
-    const int k = g < 4 ? g : g + 1, kx = k % 3, ky = k / 3;
     int rounds = 0;  // the reference evaluates four moves a round (counted once, after the diamond)
     for (int si = 0; si < nsteps; si++) {
         const int step = fast ? (si == 0 ? 8 : 4) : (16 >> si);
         const int iters = step == 4 ? 32 : 4;
         for (int it = 0; it < iters; it++) {
-            const int cx = bxv, cy = byv, c0 = bc;
-            const int X0 = clx(cx - step), X2 = clx(cx + step), Y0 = cly(cy - step), Y2 = cly(cy + step);
-            const int qx = kx == 0 ? X0 : (kx == 1 ? cx : X2), qy = ky == 0 ? Y0 : (ky == 1 ? cy : Y2);
-            const int sc = (MORE ? sad_lane_ni<T>(g0, src0, sw, w, h, qx, qy, true) : sad_lane<T>(g0, src0, sw, w, h, qx, qy, true)) + lam * mvd_bits_d(qx, qy, mvpx, mvpy);
             rounds++;
-            bool moved;
-            if (X0 == cx - step && X2 == cx + step && Y0 == cy - step && Y2 == cy + step) {
-                // no clamp: left, else right; then up from that column, else down
-                const int sL = __shfl_sync(FULL, sc, 3), sR = __shfl_sync(FULL, sc, 4);
-                int col = 1, b1 = c0;
-                if (sL < c0) {
-                    col = 0;
-                    b1 = sL;
-                } else if (sR < c0) {
-                    col = 2;
-                    b1 = sR;
-                }
-                const int sU = __shfl_sync(FULL, sc, col), sD = __shfl_sync(FULL, sc, 5 + col);
-                int row = 1, b2 = b1;
-                if (sU < b1) {
-                    row = 0;
-                    b2 = sU;
-                } else if (sD < b1) {
-                    row = 2;
-                    b2 = sD;
-                }
-                bxv = col == 0 ? X0 : (col == 1 ? cx : X2);
-                byv = row == 0 ? Y0 : (row == 1 ? cy : Y2);
-                bc = b2;
-                moved = col != 1 || row != 1;
-            } else {
-                if (lane < 8) S.cost[k] = sc;
-                if (lane == 0) S.cost[4] = c0;
-                __syncwarp();
-                const int4 rc = round_clamped(P, S, r, bx, by, w, h, mvpx, mvpy, step, cxlo, cxhi, cylo, cyhi, bxv, byv, bc);
-                moved = rc.x != 0;
-                bxv = rc.y;
-                byv = rc.z;
-                bc = rc.w;
-                __syncwarp();
-            }
-            if (!moved) break;
+            if (!diamond_round<T, MORE>(P, S, r, bx, by, w, h, mvpx, mvpy, step, cxlo, cxhi, cylo, cyhi, g0, src0, sw, bxv, byv, bc)) break;
         }
     }
     if (lane == 0) S.sad_px += (uint32_t)(4 * w * h * rounds);
@@ -753,9 +769,9 @@ static __device__ __noinline__ int4 best_inter_ref(const AnalyseParams& __restri
 
 // The 16x16 partitioning of reference r judged from the learned proposer's candidates instead of searched:
 // the exact integer cost (SAD + lambda * the vector's bits, as the plain search scores it) of every integer
-// vector within +-2 samples of each of the 4 proposals (100 points, eight a batch, the search's clamps), then
-// the plain search's sub-sample refinement (the half-sample square and the quarter-sample diamond by SATD)
-// around the best. Falls back (returns x = -1) when the proposed partitioning is not P_Skip or 16x16, or when
+// vector within +-2 samples of each of the 4 proposals (100 points, eight a batch, the search's clamps), the
+// plain search's small diamond (step 1 sample) from the best of them, then its sub-sample refinement (the
+// half-sample square and the quarter-sample diamond by SATD). Falls back (returns x = -1) when the proposed partitioning is not P_Skip or 16x16, or when
 // the best proposal costs more than the predictor's own start (the plain search's first candidate) plus the
 // margin. Otherwise returns best_inter_ref's result for a 16x16 choice.
 template <class T>
@@ -809,7 +825,16 @@ static __device__ __noinline__ int4 learned_inter(const AnalyseParams& __restric
     }
     const int bi = (int)(best & 127u), k = bi / 25, d = bi % 25;
     int bxv = clx(intr(clx(cand[2 * k])) + 4 * (d % 5 - 2)), byv = cly(intr(cly(cand[2 * k + 1])) + 4 * (d / 5 - 2));
-    int bc;
+    int bc = (int)(best >> 7);
+    // the plain search's small diamond (step 4, at most 32 rounds) from the best of the windows
+    {
+        int rounds = 0;
+        for (int it = 0; it < 32; it++) {
+            rounds++;
+            if (!diamond_round<T, false>(P, S, r, 0, 0, 16, 16, mvp.x, mvp.y, 4, cxlo, cxhi, cylo, cyhi, g0, src0, sw, bxv, byv, bc)) break;
+        }
+        if (lane == 0) S.sad_px += (uint32_t)(4 * 256 * rounds);
+    }
     // the plain search's sub-sample refinement (motion_search, enc/frame.rs:994-1017)
     if (lane < 9) {
         int2 q = make_int2(bxv, byv);

@@ -135,8 +135,8 @@ int ironav_prop_prep(const ironav_prop_sample* d_samples, int n, void* d_x, void
 
 int ironav_prop_head_fwd(const void* d_feat, int n, const float* d_hw, const float* d_hb, float* d_out, void* stream) {
     if (!d_feat || !d_hw || !d_hb || !d_out || n < 1 || n > (1 << 22)) return IRONAV_INVALID_ARGUMENT;
-    prop::head_fwd_kernel<<<n, 256, 0, static_cast<cudaStream_t>(stream)>>>(static_cast<const __nv_bfloat16*>(d_feat), (long long)n * RPIX,
-                                                                             d_hw, d_hb, d_out);
+    prop::head_fwd_kernel<<<(n + prop::HEAD_SPB - 1) / prop::HEAD_SPB, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        static_cast<const __nv_bfloat16*>(d_feat), (long long)n * RPIX, n, d_hw, d_hb, d_out);
     return cuda_status(cudaGetLastError());
 }
 
@@ -177,9 +177,9 @@ int ironav_prop_weights(const float* d_w, int cin, void* d_wf, void* d_wt, void*
     return cuda_status(cudaGetLastError());
 }
 
-int ironav_prop_propose(const float* d_out, int n, int16_t* d_cands, uint8_t* d_cls, void* stream) {
-    if (!d_out || !d_cands || !d_cls || n < 1 || n > (1 << 22)) return IRONAV_INVALID_ARGUMENT;
-    prop::propose_kernel<<<(n + 127) / 128, 128, 0, static_cast<cudaStream_t>(stream)>>>(d_out, n, d_cands, d_cls);
+int ironav_prop_propose(const float* d_out, int n, float min_conf, int16_t* d_cands, uint8_t* d_cls, void* stream) {
+    if (!d_out || !d_cands || !d_cls || n < 1 || n > (1 << 22) || !(min_conf >= 0.f && min_conf <= 1.f)) return IRONAV_INVALID_ARGUMENT;
+    prop::propose_kernel<<<(n + 127) / 128, 128, 0, static_cast<cudaStream_t>(stream)>>>(d_out, n, min_conf, d_cands, d_cls);
     return cuda_status(cudaGetLastError());
 }
 

@@ -56,32 +56,48 @@ __device__ __forceinline__ size_t feat_index(int s, int f, long long Q) {
     return ((size_t)(c >> 3) * Q + q) * 8 + (c & 7);
 }
 
-// out[s][j] = hb[j] + sum_f hw[j][f] * feat(s, f): a CTA of 256 threads per sample.
-__global__ void __launch_bounds__(256) head_fwd_kernel(const __nv_bfloat16* __restrict__ feat, long long Q, const float* __restrict__ hw,
+// out[s][j] = hb[j] + sum_f hw[j][f] * feat(s, f): a CTA of 256 threads per HEAD_SPB samples, so that each
+// weight read from L2 serves HEAD_SPB samples (the head's weights are 3.8 MB; every sample needs all of them).
+constexpr int HEAD_SPB = 8;
+
+__global__ void __launch_bounds__(256) head_fwd_kernel(const __nv_bfloat16* __restrict__ feat, long long Q, int n, const float* __restrict__ hw,
                                                        const float* __restrict__ hb, float* __restrict__ out) {
-    const int s = blockIdx.x, tid = threadIdx.x;
-    float acc[NOUT];
+    const int s0 = blockIdx.x * HEAD_SPB, tid = threadIdx.x;
+    const int ns = min(HEAD_SPB, n - s0);
+    float acc[HEAD_SPB][NOUT];
 #pragma unroll
-    for (int j = 0; j < NOUT; j++) acc[j] = 0.f;
+    for (int i = 0; i < HEAD_SPB; i++)
+#pragma unroll
+        for (int j = 0; j < NOUT; j++) acc[i][j] = 0.f;
     for (int f = tid; f < NFEAT; f += 256) {
-        const float v = __bfloat162float(feat[feat_index(s, f, Q)]);
-        if (v != 0.f)
+        float wj[NOUT];
 #pragma unroll
-            for (int j = 0; j < NOUT; j++) acc[j] += v * hw[(size_t)j * NFEAT + f];
+        for (int j = 0; j < NOUT; j++) wj[j] = __ldg(&hw[(size_t)j * NFEAT + f]);
+#pragma unroll
+        for (int i = 0; i < HEAD_SPB; i++) {
+            const float v = i < ns ? __bfloat162float(feat[feat_index(s0 + i, f, Q)]) : 0.f;
+#pragma unroll
+            for (int j = 0; j < NOUT; j++) acc[i][j] += v * wj[j];
+        }
     }
-    __shared__ float red[8][NOUT];
+    __shared__ float red[8][HEAD_SPB * NOUT];
 #pragma unroll
-    for (int j = 0; j < NOUT; j++) {
-        float a = acc[j];
+    for (int i = 0; i < HEAD_SPB; i++)
 #pragma unroll
-        for (int off = 16; off >= 1; off >>= 1) a += __shfl_xor_sync(0xffffffffu, a, off);
-        if ((tid & 31) == 0) red[tid >> 5][j] = a;
-    }
+        for (int j = 0; j < NOUT; j++) {
+            float a = acc[i][j];
+#pragma unroll
+            for (int off = 16; off >= 1; off >>= 1) a += __shfl_xor_sync(0xffffffffu, a, off);
+            if ((tid & 31) == 0) red[tid >> 5][i * NOUT + j] = a;
+        }
     __syncthreads();
-    if (tid < NOUT) {
-        float a = hb[tid];
-        for (int w = 0; w < 8; w++) a += red[w][tid];
-        out[(size_t)s * NOUT + tid] = a;
+    if (tid < HEAD_SPB * NOUT) {
+        const int i = tid / NOUT, j = tid % NOUT;
+        if (i < ns) {
+            float a = hb[j];
+            for (int w = 0; w < 8; w++) a += red[w][tid];
+            out[(size_t)(s0 + i) * NOUT + j] = a;
+        }
     }
 }
 
@@ -189,8 +205,9 @@ __global__ void weights_kernel(const float* __restrict__ w, int cin, __nv_bfloat
 }
 
 // The judge's inputs: 4 vectors in quarter samples (the outputs times MV_SCALE, rounded to nearest, clamped to
-// the search's range) and the class of largest logit (the first on ties), a thread per sample.
-__global__ void propose_kernel(const float* __restrict__ out, int n, int16_t* __restrict__ cands, uint8_t* __restrict__ cls) {
+// the search's range) and the class of largest logit (the first on ties) when its softmax probability is at
+// least min_conf, else 5 (unsure), a thread per sample.
+__global__ void propose_kernel(const float* __restrict__ out, int n, float min_conf, int16_t* __restrict__ cands, uint8_t* __restrict__ cls) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n) return;
     const float* o = out + (size_t)s * NOUT;
@@ -205,7 +222,9 @@ __global__ void propose_kernel(const float* __restrict__ out, int n, int16_t* __
     float m = o[8];
     for (int c = 1; c < 5; c++)
         if (o[8 + c] > m) m = o[8 + c], arg = c;
-    cls[s] = (uint8_t)arg;
+    float z = 0.f;
+    for (int c = 0; c < 5; c++) z += __expf(o[8 + c] - m);
+    cls[s] = (uint8_t)(1.f / z >= min_conf ? arg : 5);
 }
 
 }  // namespace prop

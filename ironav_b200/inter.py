@@ -228,7 +228,7 @@ def _declare(lib: ctypes.CDLL) -> ctypes.CDLL:
         lib.ironav_prop_adam.argtypes = [_VP, _VP, _VP, _VP, _LL, _F, _F, _F, _I, _F, _VP]
         lib.ironav_prop_weights.argtypes = [_VP, _I, _VP, _VP, _VP]
     if hasattr(lib, "ironav_prop_propose"):
-        lib.ironav_prop_propose.argtypes = [_VP, _I, _VP, _VP, _VP]
+        lib.ironav_prop_propose.argtypes = [_VP, _I, _F, _VP, _VP, _VP]
     if hasattr(lib, "ironav_set_learned"):
         lib.ironav_set_learned.argtypes = [_VP, _VP, _VP, _I, _VP]
     if hasattr(lib, "ironav_batch_autotune"):

@@ -64,7 +64,7 @@ class TrainingSet:
         return sum(len(s) for s in self.samples)
 
     def collect(self, sequences: int = 3, frames: int = 11, qps=(22, 27, 32), config: str = "1080p", size=None,
-                log=None) -> "TrainingSet":
+                nslices: int = 8, log=None) -> "TrainingSet":
         """Codes `sequences` seeded sequences of `config` at each QP with the plain search and keeps every P
         picture as training data."""
         torch = self.torch
@@ -73,7 +73,7 @@ class TrainingSet:
             seq = Sequence.config(config, frames, seed=TRAIN_SEED + k, size=size)
             frames_y = [seq.frame(t) for t in range(frames)]
             for qp in qps:
-                enc = DeviceEncoder(w0, h0, qp)
+                enc = DeviceEncoder(w0, h0, qp, nslices=min(nslices, (h0 + 15) // 16))
                 try:
                     ref = None
                     for t in range(frames):
@@ -156,9 +156,9 @@ class LearnedJudge:
     macroblock (cur = the picture, ref = the newest reference, the encoder's filtered reconstruction) and the
     judge's inputs, set on the encoder's context. Counters: judged, class fallbacks, cost fallbacks."""
 
-    def __init__(self, prop: Proposer, enc: DeviceEncoder, margin: int = 0, timed: bool = False):
+    def __init__(self, prop: Proposer, enc: DeviceEncoder, margin: int = 0, min_conf: float = 0.0, timed: bool = False):
         torch = prop.torch
-        self.prop, self.enc, self.margin = prop, enc, margin
+        self.prop, self.enc, self.margin, self.min_conf = prop, enc, margin, min_conf
         st = enc.st
         self.n = st.nmb
         dev = prop.dev
@@ -189,7 +189,7 @@ class LearnedJudge:
             e0.record(enc.stream)
         self.prop.set_samples_device(d.data_ptr(), self.n)
         self.prop.forward(self.n)
-        self.prop.propose(self.n, self.cands.data_ptr(), self.cls.data_ptr())
+        self.prop.propose(self.n, self.cands.data_ptr(), self.cls.data_ptr(), self.min_conf)
         if self.timed:
             e1.record(enc.stream)
             e1.synchronize()
@@ -210,12 +210,13 @@ def psnr(a: np.ndarray, b: np.ndarray, peak: float = 255.0) -> float:
     return float("inf") if mse == 0 else 10.0 * np.log10(peak * peak / mse)
 
 
-def encode_sequence(seq: Sequence, qp: int, frames: int, prop: Proposer | None = None, margin: int = 0) -> dict:
+def encode_sequence(seq: Sequence, qp: int, frames: int, prop: Proposer | None = None, margin: int = 0, min_conf: float = 0.0,
+                    nslices: int = 8) -> dict:
     """Codes `frames` pictures of `seq` with the device encoder (plain search, or the learned form with `prop`):
     total bytes, mean luma PSNR, the learned form's counters and proposer time."""
     w, h = seq.width, seq.height
-    enc = DeviceEncoder(w, h, qp)
-    judge = LearnedJudge(prop, enc, margin=margin, timed=True) if prop is not None else None
+    enc = DeviceEncoder(w, h, qp, nslices=nslices)
+    judge = LearnedJudge(prop, enc, margin=margin, min_conf=min_conf, timed=True) if prop is not None else None
     total, ps = 0, []
     try:
         for t in range(frames):
@@ -232,6 +233,78 @@ def encode_sequence(seq: Sequence, qp: int, frames: int, prop: Proposer | None =
         return out
     finally:
         enc.close()
+
+
+def analysis_rate(prop: Proposer, seq: Sequence, qp: int, frames: int, margin: int = 0, min_conf: float = 0.0, nslices: int = 8,
+                  reps: int = 3) -> dict:
+    """Auto-mode analysis (ironav_analyse_picture_auto_device) of pictures 1..frames-1 of `seq`, each from the
+    previous source picture, with the plain search and with the learned form (the proposer's input, forward
+    pass and proposals, then the analysis with the judge), timed by CUDA events on one stream: macroblocks per
+    second of each, the proposer's share, and the judge's counters. The reference's planes are built before
+    the timed region in both."""
+    import torch
+
+    from .inter import MBRESULT_DTYPE, MBSTATE_DTYPE, InterStage
+
+    w, h = seq.width, seq.height
+    st = InterStage(w, h, nslices=nslices)
+    stream = torch.cuda.Stream()
+    st.set_stream(stream.cuda_stream)
+    old_stream = prop.stream
+    prop.stream = stream
+    dev = prop.dev
+    try:
+        pics = [torch.from_numpy(seq.frame(t)).to(dev) for t in range(frames)]
+        n = st.nmb
+        d_states = torch.zeros(n * MBSTATE_DTYPE.itemsize, dtype=torch.uint8, device=dev)
+        d_out = torch.zeros(n * MBRESULT_DTYPE.itemsize, dtype=torch.uint8, device=dev)
+        cands = torch.zeros((n, 8), dtype=torch.int16, device=dev)
+        cls = torch.zeros(n, dtype=torch.uint8, device=dev)
+        stats = torch.zeros(3, dtype=torch.int32, device=dev)
+        samples = {}
+        ms = {"plain": 0.0, "learned": 0.0, "proposer": 0.0}
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        pictures = 0
+        for t in range(1, frames):
+            st.clear_references()
+            st.push_reference_device(pics[t - 1].data_ptr(), w, w, h, None)
+            st.set_source_device(pics[t].data_ptr(), w)
+            st.begin_p_picture(qp, 1)
+            smp = samples.setdefault(t, torch.from_numpy(picture_samples(pics[t].data_ptr(), pics[t - 1].data_ptr(), w, h, w, w)
+                                                          .view(np.uint8)).to(dev))
+            for r in range(reps + 1):
+                st._check(st.lib.ironav_set_learned(st.ctx, None, None, 0, None), "ironav_set_learned")
+                ev[0].record(stream)
+                st.analyse_auto_device(d_states.data_ptr(), d_out.data_ptr())
+                ev[1].record(stream)
+                ev[1].synchronize()
+                plain_ms = ev[0].elapsed_time(ev[1])
+                st._check(st.lib.ironav_set_learned(st.ctx, cands.data_ptr(), cls.data_ptr(), margin, stats.data_ptr()),
+                          "ironav_set_learned")
+                ev[0].record(stream)
+                prop.set_samples_device(smp.data_ptr(), n)
+                prop.forward(n)
+                prop.propose(n, cands.data_ptr(), cls.data_ptr(), min_conf)
+                ev[1].record(stream)
+                st.analyse_auto_device(d_states.data_ptr(), d_out.data_ptr())
+                ev[2].record(stream)
+                ev[2].synchronize()
+                if r > 0:  # the first round warms up
+                    ms["plain"] += plain_ms
+                    ms["proposer"] += ev[0].elapsed_time(ev[1])
+                    ms["learned"] += ev[0].elapsed_time(ev[2])
+                    pictures += 1
+        st._check(st.lib.ironav_set_learned(st.ctx, None, None, 0, None), "ironav_set_learned")
+        prop.check_errors()
+        mbs = n * pictures
+        s = stats.cpu().numpy()
+        return {"qp": qp, "pictures": pictures, "plain_mb_per_s": mbs / (ms["plain"] * 1e-3),
+                "learned_mb_per_s": mbs / (ms["learned"] * 1e-3), "proposer_ms_per_picture": ms["proposer"] / pictures,
+                "plain_ms_per_picture": ms["plain"] / pictures, "learned_ms_per_picture": ms["learned"] / pictures,
+                "judged": int(s[0]), "class_fallback": int(s[1]), "cost_fallback": int(s[2])}
+    finally:
+        prop.stream = old_stream
+        st.close()
 
 
 def conv_tflops(prop: Proposer, n: int, reps: int = 5) -> dict:
@@ -273,6 +346,7 @@ def main(argv=None) -> int:
     ap.add_argument("--batch", type=int, default=512)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--margin", type=int, default=0)
+    ap.add_argument("--min-conf", default="0", help="comma-separated class-probability floors to evaluate")
     ap.add_argument("--eval-frames", type=int, default=11)
     ap.add_argument("--qps", default="22,27,32")
     ap.add_argument("--save", default=None, help="write the trained parameters (.npz)")
@@ -300,17 +374,26 @@ def main(argv=None) -> int:
             st = prop.state_dict()
             np.savez(a.save, params=st["params"], step=st["step"])
     seq = Sequence.config("1080p", a.eval_frames)
+    confs = [float(c) for c in a.min_conf.split(",")]
     out["eval"] = []
     for qp in qps:
         plain = encode_sequence(seq, qp, a.eval_frames)
-        lrn = encode_sequence(seq, qp, a.eval_frames, prop=prop, margin=a.margin)
-        rec = {"qp": qp, "plain": plain, "learned": lrn,
-               "bytes_delta_pct": 100.0 * (lrn["bytes"] - plain["bytes"]) / plain["bytes"],
-               "psnr_delta_db": lrn["psnr_y"] - plain["psnr_y"]}
-        searched = lrn["judged"] + lrn["class_fallback"] + lrn["cost_fallback"]
-        rec["fallback_rate"] = (lrn["class_fallback"] + lrn["cost_fallback"]) / max(1, searched)
-        log(rec)
-        out["eval"].append(rec)
+        for conf in confs:
+            lrn = encode_sequence(seq, qp, a.eval_frames, prop=prop, margin=a.margin, min_conf=conf)
+            rec = {"qp": qp, "min_conf": conf, "plain": plain, "learned": lrn,
+                   "bytes_delta_pct": 100.0 * (lrn["bytes"] - plain["bytes"]) / plain["bytes"],
+                   "psnr_delta_db": lrn["psnr_y"] - plain["psnr_y"]}
+            searched = lrn["judged"] + lrn["class_fallback"] + lrn["cost_fallback"]
+            rec["fallback_rate"] = (lrn["class_fallback"] + lrn["cost_fallback"]) / max(1, searched)
+            log(rec)
+            out["eval"].append(rec)
+    out["analysis"] = []
+    for qp in qps:
+        for conf in confs:
+            rec = analysis_rate(prop, seq, qp, a.eval_frames, margin=a.margin, min_conf=conf)
+            rec["min_conf"] = conf
+            log(rec)
+            out["analysis"].append(rec)
     n = (1920 // 16) * (1088 // 16)
     prop._alloc(n)
     out["conv_rate"] = conv_tflops(prop, n)

@@ -136,18 +136,24 @@ class Proposer:
         _check(self.lib.ironav_prop_prep(d_samples, n, self.x0.data_ptr(), self._s), "prep")
         return n
 
-    def propose(self, n: int, d_cands: int, d_cls: int) -> None:
-        """The judge's inputs (ironav_set_learned) from the last forward pass over n macroblocks."""
-        _check(self.lib.ironav_prop_propose(self.out.data_ptr(), n, d_cands, d_cls, self._s), "propose")
+    def propose(self, n: int, d_cands: int, d_cls: int, min_conf: float = 0.0) -> None:
+        """The judge's inputs (ironav_set_learned) from the last forward pass over n macroblocks; a class whose
+        probability is below min_conf becomes 5 (unsure: the plain search)."""
+        _check(self.lib.ironav_prop_propose(self.out.data_ptr(), n, ctypes.c_float(min_conf), d_cands, d_cls, self._s), "propose")
 
-    def forward(self, n: int) -> None:
-        """Layers 1-4 and the head on the batch set up by set_samples: self.out[:n]."""
+    def forward(self, n: int, conv_events=None) -> None:
+        """Layers 1-4 and the head on the batch set up by set_samples: self.out[:n]. conv_events: a pair of CUDA
+        events recorded on the proposer's stream before layer 1 and after layer 4."""
         lib, e = self.lib, self.err.data_ptr()
+        if conv_events is not None:
+            conv_events[0].record(self.stream)
         _check(lib.ironav_prop_conv3x3(self.x0.data_ptr(), 16, n, self.wf[1].data_ptr(), self.views["b1"].data_ptr(), 1, None,
                                        self.z[1].data_ptr(), e, self._s), "conv 1")
         for l in (2, 3, 4):
             _check(lib.ironav_prop_conv3x3(self.z[l - 1].data_ptr(), 32, n, self.wf[l].data_ptr(), self.views[f"b{l}"].data_ptr(), 1, None,
                                            self.z[l].data_ptr(), e, self._s), f"conv {l}")
+        if conv_events is not None:
+            conv_events[1].record(self.stream)
         _check(lib.ironav_prop_head_fwd(self.z[4].data_ptr(), n, self.views["hw"].data_ptr(), self.views["hb"].data_ptr(),
                                         self.out.data_ptr(), self._s), "head")
 

@@ -729,8 +729,8 @@ static void best_inter_ref(const fc* f, counters* cnt, int mbx, int mby, int r, 
 /* The learned form's judge (no counterpart in the reference): the 16x16 partitioning of the newest reference
  * from the proposals instead of the search. Every integer vector within +-2 samples of each of the 4 proposals
  * (rounded to the integer grid and clamped as motion_search clamps its candidates) is scored by SAD + lambda *
- * bits, the first of least cost in proposal-major, row-major order wins; then motion_search's sub-sample
- * refinement (994-1017). Returns 0 (the caller searches) when the proposed class is not P_Skip or 16x16, or when
+ * bits, the first of least cost in proposal-major, row-major order wins; then motion_search's small diamond
+ * (step 4, at most 32 rounds) and its sub-sample refinement (994-1017). Returns 0 (the caller searches) when the proposed class is not P_Skip or 16x16, or when
  * the winner costs more than the predictor's own start plus the margin; counters as ironav_set_learned states. */
 static int learned_inter(const fc* f, counters* cnt, int mbx, int mby, inter_res* best) {
     const struct ironav_ctx* c = f->c;
@@ -765,6 +765,23 @@ static int learned_inter(const fc* f, counters* cnt, int mbx, int mby, inter_res
     if (bc > start + c->learned_margin) {
         __atomic_fetch_add(&c->learned_stats[2], 1u, __ATOMIC_RELAXED);
         return 0;
+    }
+    /* motion_search's small diamond (973-988, step 4) from the best of the windows */
+    for (int it = 0; it < 32; it++) {
+        int moved = 0;
+        const int D[4][2] = {{-4, 0}, {4, 0}, {0, -4}, {0, 4}};
+        for (int dd = 0; dd < 4; dd++) {
+            const int qx = CLX(bx + D[dd][0]), qy = CLY(by + D[dd][1]);
+            const int cost = COST_INT(qx, qy);
+            if (cost < bc) {
+                bx = qx;
+                by = qy;
+                bc = cost;
+                moved = 1;
+            }
+        }
+        cnt->sad_px += 4u * 256u;
+        if (!moved) break;
     }
     uint16_t pred[256];
     const halfpel* hp = &c->refs[r].hp;
@@ -3547,7 +3564,7 @@ int ironav_prop_adam(float* p, float* g, float* m, float* v, long long n, float 
     return IRONAV_HARDWARE_UNAVAILABLE;
 }
 int ironav_prop_weights(const float* w, int cin, void* wf, void* wt, void* s) { (void)w; (void)cin; (void)wf; (void)wt; (void)s; return IRONAV_HARDWARE_UNAVAILABLE; }
-int ironav_prop_propose(const float* o, int n, int16_t* c, uint8_t* k, void* s) {
-    (void)o; (void)n; (void)c; (void)k; (void)s;
+int ironav_prop_propose(const float* o, int n, float min_conf, int16_t* c, uint8_t* k, void* s) {
+    (void)o; (void)n; (void)min_conf; (void)c; (void)k; (void)s;
     return IRONAV_HARDWARE_UNAVAILABLE;
 }
