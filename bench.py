@@ -41,6 +41,7 @@ sys.path.insert(0, ROOT)
 METRIC = "1080p inter-analysis MB/s: plain bit-exact vs learned at ≤1% bitrate delta"
 WIDTH, HEIGHT, QP, NSLICES = 1920, 1080, 27, 8
 RING = 40  # frames in the ring: luma + decisions + results of the ring exceed the 126 MB L2
+E2E_MIN_S = 0.5  # the shortest wall-clock window of the host-buffer (e2e) pass
 
 
 def parse():
@@ -1952,21 +1953,31 @@ def run_e2e(args, st, frames, d_states, nmb, world, torch, dist, dev, stream):
 
     run(0, max(args.warmup, nthreads))
     torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
+    # the timed window is at least E2E_MIN_S of wall clock: K steps, repeated as often as one untimed pass of K
+    # steps says that takes (the same count on every rank)
     t0 = time.perf_counter()
     run(args.warmup, args.steps)
     torch.cuda.synchronize()
+    once = max_over_ranks(time.perf_counter() - t0, world, dev)
+    reps = max(1, int(np.ceil(E2E_MIN_S / max(once, 1e-6))))
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for k in range(reps):
+        run(args.warmup + k * args.steps, args.steps)
+    torch.cuda.synchronize()
     el = max_over_ranks(time.perf_counter() - t0, world, dev)
+    steps = reps * args.steps
     for ws, *_ in workers:
         ws.close()
-    return {"value": world * nmb * args.steps / el, "unit": "MB/s",
+    return {"value": world * nmb * steps / el, "unit": "MB/s",
             "h2d_bytes_per_step": 2 * WIDTH * HEIGHT * fr.itemsize + 2 * nmb * 72, "d2h_bytes_per_step": nmb * 104,
-            "ms_per_step": 1e3 * el / args.steps, "host_threads": nthreads,
+            "ms_per_step": 1e3 * el / steps, "host_threads": nthreads, "steps": steps, "seconds": el,
             "note": "host-buffer C ABI calls (each returns when its work is done) from pinned host memory, "
-                    f"K steps spread over {nthreads} host threads with a context and CUDA stream each; wall clock "
-                    "around the K steps, max over ranks; above the device-resident value when several pictures' "
-                    "copies and kernels overlap on their streams (value runs one stream, step after step)"}
+                    f"steps spread over {nthreads} host threads with a context and CUDA stream each; wall clock "
+                    f"around {reps} x K steps (at least {E2E_MIN_S} s), max over ranks; above the device-resident value "
+                    "when several pictures' copies and kernels overlap on their streams (value runs one stream, step "
+                    "after step)"}
 
 
 def finish(world):

@@ -362,8 +362,9 @@ static __device__ __forceinline__ void pred_batch(const AnalyseParams& __restric
 
 // ---- motion_search, enc/frame.rs:949-1019 --------------------------------------------------------
 
-// One diamond round whose moves were bent by the search clamps: the reference's four moves replayed
-// against the scored 3x3 square (S.cost[0..9), centre at 4), scoring on demand the points it lacks.
+// One diamond round whose moves were bent by the search clamps (or whose centre lies outside them): the
+// reference's four moves replayed against the scored 3x3 square (S.cost[0..9), centre at 4), scoring on demand
+// the points it lacks.
 // Returns whether the best moved.
 template <class T>
 static __device__ __noinline__ int4 round_clamped(const AnalyseParams& __restrict__ P, WarpSmem<T>& __restrict__ S, int r, int bx, int by, int w, int h, int mvpx, int mvpy, int step, int cxlo,
@@ -374,7 +375,9 @@ static __device__ __noinline__ int4 round_clamped(const AnalyseParams& __restric
     const int Y0 = min(max(cy - step, cylo), cyhi), Y2 = min(max(cy + step, cylo), cyhi);
     bool moved = false;
     for (int d = 0; d < 4; d++) {
-        int nx = bxv, ny = byv;
+        // each move clamps both coordinates of the current best (the unmoved one matters when the centre lies
+        // outside the clamps, as a rounded candidate at the +-2048 / +-512 limits can)
+        int nx = min(max(bxv, cxlo), cxhi), ny = min(max(byv, cylo), cyhi);
         if (d == 0) nx = min(max(bxv - step, cxlo), cxhi);
         else if (d == 1) nx = min(max(bxv + step, cxlo), cxhi);
         else if (d == 2) ny = min(max(byv - step, cylo), cyhi);

@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "analyse.cuh"
+#include "analyse_g8.cuh"
 #include "bpicture.cuh"
 #include "ctx.cuh"
 #include "planes.cuh"
@@ -174,6 +175,12 @@ int launch_analyse(ironav_ctx* c, bool auto_mode, const ironav_mbstate* d_in, ir
     p.wait_limit = c->wait_limit;
     if (auto_mode) p.epoch = ++c->epoch;
     CK(cudaMemsetAsync(c->d_counters, 0, 2 * sizeof(unsigned), c->stream));
+    if (!auto_mode && c->replay_form == 0 && p.learned == nullptr) {
+        // replay mode: one macroblock per 8-lane group
+        if (c->bd > 8) g8::analyse_replay_g8_kernel<uint16_t><<<c->g8_blocks, g8::WARPS * 32, 0, c->stream>>>(p);
+        else g8::analyse_replay_g8_kernel<uint8_t><<<c->g8_blocks, g8::WARPS * 32, 0, c->stream>>>(p);
+        return cuda_status(cudaGetLastError());
+    }
     if (c->bd > 8) {
         if (auto_mode) analyse_kernel<MODE_AUTO, uint16_t><<<c->k2_blocks, K2_WARPS * 32, 0, c->stream>>>(p);
         else analyse_kernel<MODE_REPLAY, uint16_t><<<c->k2_blocks, K2_WARPS * 32, 0, c->stream>>>(p);
@@ -355,6 +362,11 @@ int ironav_ctx_create(ironav_ctx** out, int width, int height, int bd, int max_r
                : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, analyse_kernel<MODE_AUTO, uint8_t>, K2_WARPS * 32, 0);
     if (e != cudaSuccess) return fail(e);
     c->k2_blocks = std::max(1, per_sm) * c->nsm;
+    per_sm = 0;
+    e = bd > 8 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, g8::analyse_replay_g8_kernel<uint16_t>, g8::WARPS * 32, 0)
+               : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, g8::analyse_replay_g8_kernel<uint8_t>, g8::WARPS * 32, 0);
+    if (e != cudaSuccess) return fail(e);
+    c->g8_blocks = std::max(1, per_sm) * c->nsm;
     const size_t slack = 256;  // word-granular reads may touch a few bytes past a plane's last sample
     const size_t bytes = (size_t)sample_bytes(c);
     if ((e = cudaMalloc(&c->d_src, (size_t)c->pw * c->ph * bytes + slack)) != cudaSuccess) return fail(e);
@@ -1031,6 +1043,13 @@ int ironav_inloop_end(ironav_ctx* c) {
     if (!c || !c->inloop_active) return IRONAV_INVALID_ARGUMENT;
     c->inloop_active = false;
     return check_device_error(c);
+}
+
+// Replay mode's kernel: 0 one macroblock per 8-lane group (the default), 1 one macroblock per warp.
+int ironav_set_replay_form(ironav_ctx* c, int form) {
+    if (!c || form < 0 || form > 1) return IRONAV_INVALID_ARGUMENT;
+    c->replay_form = form;
+    return IRONAV_OK;
 }
 
 // The learned form's proposals for the context's next analyses (auto, replay and decide modes): all four

@@ -167,6 +167,41 @@ def test_modes_720p(oracle_lib, cuda_lib, mode):
     sc, rc = c.analyse_auto()
     assert_same(sc, so, f"{mode} decisions")
     assert_same(rc, ro, f"{mode} results")
+    assert_same(c.analyse_replay(so), o.analyse_replay(so), f"{mode} replay")
+
+
+@pytest.mark.parametrize("mode", [dict(), dict(fast=True), dict(sub8=True)])
+def test_replay_forms_agree_on_random_decisions(oracle_lib, cuda_lib, mode):
+    """Replay mode's two kernels (one macroblock per 8-lane group, the default; one per warp) and the oracle on
+    three references with arbitrary neighbour decisions up to the level limits, so that predictors, candidates
+    and diamond moves land on the clamps and the rounded candidates just outside them."""
+    seq = Sequence.config("cif", 4)
+    o, c = stage_pair(oracle_lib, cuda_lib, 352, 288, nslices=3, max_refs=3)
+    rng = np.random.default_rng(17 + len(mode))
+    nmb = o.nmb
+    col = np.zeros(nmb, dtype=MBSTATE_DTYPE)
+    col["inter"] = rng.integers(0, 2, nmb)
+    col["mvs"] = rng.integers(-2100, 2100, size=(nmb, 16, 2))
+    for st in (o, c):
+        st.push_reference(seq.frame(0))
+        st.push_reference(seq.frame(1))
+        st.push_reference(seq.frame(2), col=col)
+        st.set_source(seq.frame(3))
+        st.begin_p_picture(18 if mode.get("sub8") else 28, nrefs_active=3, **mode)
+    states = np.zeros(nmb, dtype=MBSTATE_DTYPE)
+    states["inter"] = rng.integers(0, 4, nmb) > 0
+    states["refs"] = np.where(states["inter"][:, None] == 1, rng.integers(-1, 3, size=(nmb, 4)), -1)
+    mv = np.stack([rng.integers(-2048, 2048, size=(nmb, 16)), rng.integers(-512, 512, size=(nmb, 16))], axis=-1)
+    near = rng.integers(0, 3, size=(nmb, 1, 1))
+    edge = np.where(mv >= 0, 1, -1) * np.array([2047, 511]) - rng.integers(0, 3, size=mv.shape)  # at the limits
+    states["mvs"] = np.where(near == 0, mv // 64, np.where(near == 1, edge, mv))
+    want = o.analyse_replay(states)
+    got0 = c.analyse_replay(states)
+    assert cuda_lib.ironav_set_replay_form(c.ctx, 1) == 0
+    got1 = c.analyse_replay(states)
+    assert cuda_lib.ironav_set_replay_form(c.ctx, 0) == 0
+    assert_same(got0, want, f"{mode} group form")
+    assert_same(got1, want, f"{mode} warp form")
 
 
 def test_random_decisions_exercise_the_clamps(oracle_lib, cuda_lib):
