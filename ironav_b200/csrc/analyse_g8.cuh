@@ -21,9 +21,11 @@
 namespace ironav {
 namespace g8 {
 
-constexpr int WARPS = 4;       // warps a CTA
-constexpr int MIN_BLOCKS = 4;  // CTAs an SM the register budget must allow
-constexpr int GROUPS = WARPS * 4;
+constexpr int WARPS = 4;       // warps a CTA (8 and 16-lane groups)
+constexpr int MIN_BLOCKS = 4;  // CTAs an SM the register budget must allow, at 128 registers a thread
+// Warps a CTA for groups of GW lanes: the CTA's groups' shared memory stays within the 48 KB of static shared
+// memory (16 groups of about 1.8 KB), and the CTAs an SM scale so that 16 warps an SM fit 128 registers.
+__host__ __device__ constexpr int warps_for(int gw) { return gw == 4 ? 2 : WARPS; }
 
 // Per-group shared memory; T is the sample type.
 template <class T>
@@ -39,14 +41,17 @@ struct GroupSmem {
     ironav_mbresult res;           // the result being assembled
 };
 
+// A group of GW lanes (8 or 16) analysing one macroblock: its lane index and mask.
+template <int GW>
 struct Grp {
     int gl;         // lane within the group
     unsigned mask;  // the group's lanes
 };
 
-__device__ __forceinline__ Grp grp_of_lane() {
+template <int GW>
+__device__ __forceinline__ Grp<GW> grp_of_lane() {
     const int lane = threadIdx.x & 31;
-    return Grp{lane & 7, 0xffu << (lane & 24)};
+    return Grp<GW>{lane & (GW - 1), (GW == 32 ? 0xffffffffu : ((1u << GW) - 1u)) << (lane & (32 - GW))};
 }
 
 // The macroblock a group analyses and its work counts.
@@ -78,23 +83,23 @@ __device__ __forceinline__ int row_sad(const uint8_t* G, const uint32_t* sr, int
     return sad;
 }
 
-// Integer SAD (sad_int, enc/frame.rs:662-671) of the w x h partition for two vectors at once: lanes 0-3 of
-// the group score (ax, ay), lanes 4-7 (bx, by), four lanes splitting the rows. g0: plane G at the partition's
+// Integer SAD (sad_int, enc/frame.rs:662-671) of the w x h partition for two vectors at once: the first half
+// of the group scores (ax, ay), the second (bx, by), the lanes of a half splitting the rows. g0: plane G at the partition's
 // origin (bytes); src: the partition's first source word; sw: the plane stride in samples. Every lane of the
 // group gets both sums.
-template <class T>
-__device__ __forceinline__ int2 sad2(const Grp& g, const uint8_t* __restrict__ g0, const uint32_t* __restrict__ src, int sw, int w, int h,
+template <class T, int GW>
+__device__ __forceinline__ int2 sad2(const Grp<GW>& g, const uint8_t* __restrict__ g0, const uint32_t* __restrict__ src, int sw, int w, int h,
                                      int ax, int ay, int bx, int by) {
-    constexpr int B = sizeof(T);
-    const bool second = g.gl >= 4;
+    constexpr int B = sizeof(T), H = GW / 2;  // lanes a vector
+    const bool second = g.gl >= H;
     const int px = second ? bx : ax, py = second ? by : ay;
-    const int r0 = g.gl & 3;
+    const int r0 = g.gl & (H - 1);
     const uint8_t* G = g0 + (((py >> 2) + r0) * sw + (px >> 2)) * B;
     int s = 0;
-    for (int row = r0; row < h; row += 4, G += 4 * sw * B) s += row_sad<T>(G, src + row * 4 * B, w);
-    s += __shfl_xor_sync(g.mask, s, 1, 8);
-    s += __shfl_xor_sync(g.mask, s, 2, 8);
-    const int o = __shfl_xor_sync(g.mask, s, 4, 8);
+    for (int row = r0; row < h; row += H, G += H * sw * B) s += row_sad<T>(G, src + row * 4 * B, w);
+#pragma unroll
+    for (int off = 1; off < H; off <<= 1) s += __shfl_xor_sync(g.mask, s, off, GW);
+    const int o = __shfl_xor_sync(g.mask, s, H, GW);
     return second ? make_int2(o, s) : make_int2(s, o);
 }
 
@@ -126,16 +131,17 @@ __device__ __forceinline__ int score4_src(const uint32_t* __restrict__ src, int 
 // Quarter-sample prediction of the partition at 4x4 block (bx, by) of (4 << lgw) x (4 << lgh) samples on the
 // planes of reference r, scored by SATD (or SAD when `sad`) for the n vectors pt(0..n) (a group-uniform
 // function of the index): the sums land in S.cost[0..n). The group's lanes take (vector, 4x4 block) tasks.
-template <class T, class F>
-__device__ __forceinline__ void pred_points(const AnalyseParams& __restrict__ P, GroupSmem<T>& __restrict__ S, const Grp& g, int mbx, int mby, int r,
+template <class T, int GW, class F>
+__device__ __forceinline__ void pred_points(const AnalyseParams& __restrict__ P, GroupSmem<T>& __restrict__ S, const Grp<GW>& g, int mbx, int mby, int r,
                                             int bx, int by, int lgw, int lgh, F pt, int n, bool sad) {
     const int lg = lgw + lgh, total = n << lg, w = 4 << lgw, h = 4 << lgh;
-    if (g.gl < n) S.cost[g.gl] = 0;
-    if (g.gl + 8 < n) S.cost[g.gl + 8] = 0;
+#pragma unroll
+    for (int k = 0; k < (9 + GW - 1) / GW; k++)
+        if (g.gl + GW * k < n) S.cost[g.gl + GW * k] = 0;
     __syncwarp(g.mask);
     const int x0 = mbx * 16 + bx * 4, y0 = mby * 16 + by * 4;
     const uint8_t* base = P.planes[r];
-    for (int t = g.gl; t < total; t += 8) {
+    for (int t = g.gl; t < total; t += GW) {
         const int c = t >> lg, b = t & ((1 << lg) - 1), bxx = b & ((1 << lgw) - 1), byy = b >> lgw;
         uint32_t pr[4][sizeof(T)];
         pred4<T>(P, base, x0, y0, w, h, bxx, byy, pt(c), pr);
@@ -177,18 +183,18 @@ __device__ __forceinline__ int2 pred_mv_g(const Blk* ext, const Blk* cur, int bx
 // beaten — whose cost cannot win — unless a clamp bent the move (or the centre lay outside the clamps, which
 // the candidates' rounding allows at the +-2048 / +-512 limits), and then it is scored on its own. Returns
 // whether the best moved.
-template <class T>
-__device__ __forceinline__ bool round_g(const AnalyseParams& __restrict__ P, const Grp& g, const uint8_t* g0, const uint32_t* src, int w, int h,
+template <class T, int GW>
+__device__ __forceinline__ bool round_g(const AnalyseParams& __restrict__ P, const Grp<GW>& g, const uint8_t* g0, const uint32_t* src, int w, int h,
                                         int mvpx, int mvpy, int step, int cxlo, int cxhi, int cylo, int cyhi, int& bxv, int& byv, int& bc) {
     const int lam = P.lambda, sw = P.sw;
     auto clx = [&](int v) { return min(max(v, cxlo), cxhi); };
     auto cly = [&](int v) { return min(max(v, cylo), cyhi); };
-    auto cost1 = [&](int x, int y) { return sad2<T>(g, g0, src, sw, w, h, x, y, x, y).x + lam * mvd_bits_d(x, y, mvpx, mvpy); };
+    auto cost1 = [&](int x, int y) { return sad2<T, GW>(g, g0, src, sw, w, h, x, y, x, y).x + lam * mvd_bits_d(x, y, mvpx, mvpy); };
     bool moved = false;
     {
         const int cx0 = bxv, cy0 = byv, row = cly(cy0);
         const int lx = clx(cx0 - step), rx = clx(cx0 + step);
-        const int2 s = sad2<T>(g, g0, src, sw, w, h, lx, row, rx, row);
+        const int2 s = sad2<T, GW>(g, g0, src, sw, w, h, lx, row, rx, row);
         const int cl = s.x + lam * mvd_bits_d(lx, row, mvpx, mvpy), cr = s.y + lam * mvd_bits_d(rx, row, mvpx, mvpy);
         if (cl < bc) {
             bxv = lx;
@@ -213,7 +219,7 @@ __device__ __forceinline__ bool round_g(const AnalyseParams& __restrict__ P, con
     {
         const int bx1 = bxv, by1 = byv, col = clx(bx1);
         const int uy = cly(by1 - step), dy = cly(by1 + step);
-        const int2 s = sad2<T>(g, g0, src, sw, w, h, col, uy, col, dy);
+        const int2 s = sad2<T, GW>(g, g0, src, sw, w, h, col, uy, col, dy);
         const int cu = s.x + lam * mvd_bits_d(col, uy, mvpx, mvpy), cd = s.y + lam * mvd_bits_d(col, dy, mvpx, mvpy);
         if (cu < bc) {
             bxv = col;
@@ -242,8 +248,8 @@ __device__ __forceinline__ bool round_g(const AnalyseParams& __restrict__ P, con
 // the candidates (the predictor, zero, the macroblock's left, top and top-right neighbours on this reference,
 // then the extra vectors), the diamond, and the sub-sample refinement by SATD. Returns (cost without the
 // vector's bits, mx, my).
-template <class T>
-__device__ __noinline__ int3 msearch(const AnalyseParams& __restrict__ P, GroupSmem<T>& __restrict__ S, const Grp& g, Mb& M, int r, int bx, int by,
+template <class T, int GW>
+__device__ __noinline__ int3 msearch(const AnalyseParams& __restrict__ P, GroupSmem<T>& __restrict__ S, const Grp<GW>& g, Mb& M, int r, int bx, int by,
                                      int w4, int h4, int mvpx, int mvpy, int e0x, int e0y, int e1x, int e1y, int nextra) {
     constexpr int B = sizeof(T);
     const int lam = P.lambda;
@@ -271,14 +277,14 @@ __device__ __noinline__ int3 msearch(const AnalyseParams& __restrict__ P, GroupS
     };
     {
         const int px = intr(clx(mvpx)), py = intr(cly(mvpy));
-        const int2 s = sad2<T>(g, g0, src, P.sw, w, h, px, py, 0, 0);
+        const int2 s = sad2<T, GW>(g, g0, src, P.sw, w, h, px, py, 0, 0);
         take(true, px, py, s.x);
         take(true, 0, 0, s.y);
     }
     {
         const int ax = intr(clx(na.x)), ay = intr(cly(na.y)), qx = intr(clx(nbb.x)), qy = intr(cly(nbb.y));
         if (va || vb) {
-            const int2 s = sad2<T>(g, g0, src, P.sw, w, h, va ? ax : 0, va ? ay : 0, vb ? qx : 0, vb ? qy : 0);
+            const int2 s = sad2<T, GW>(g, g0, src, P.sw, w, h, va ? ax : 0, va ? ay : 0, vb ? qx : 0, vb ? qy : 0);
             take(va, ax, ay, s.x);
             take(vb, qx, qy, s.y);
             ncand += va + vb;
@@ -288,7 +294,7 @@ __device__ __noinline__ int3 msearch(const AnalyseParams& __restrict__ P, GroupS
         const int cx = intr(clx(nc.x)), cy = intr(cly(nc.y)), fx = intr(clx(e0x)), fy = intr(cly(e0y));
         const bool ve = nextra > 0;
         if (vc || ve) {
-            const int2 s = sad2<T>(g, g0, src, P.sw, w, h, vc ? cx : 0, vc ? cy : 0, ve ? fx : 0, ve ? fy : 0);
+            const int2 s = sad2<T, GW>(g, g0, src, P.sw, w, h, vc ? cx : 0, vc ? cy : 0, ve ? fx : 0, ve ? fy : 0);
             take(vc, cx, cy, s.x);
             take(ve, fx, fy, s.y);
             ncand += vc + ve;
@@ -296,7 +302,7 @@ __device__ __noinline__ int3 msearch(const AnalyseParams& __restrict__ P, GroupS
     }
     if (nextra > 1) {
         const int fx = intr(clx(e1x)), fy = intr(cly(e1y));
-        take(true, fx, fy, sad2<T>(g, g0, src, P.sw, w, h, fx, fy, fx, fy).x);
+        take(true, fx, fy, sad2<T, GW>(g, g0, src, P.sw, w, h, fx, fy, fx, fy).x);
         ncand++;
     }
     M.sad_px += (uint32_t)(ncand * w * h);
@@ -309,7 +315,7 @@ __device__ __noinline__ int3 msearch(const AnalyseParams& __restrict__ P, GroupS
         const int iters = step == 4 ? 32 : 4;
         for (int it = 0; it < iters; it++) {
             rounds++;
-            if (!round_g<T>(P, g, g0, src, w, h, mvpx, mvpy, step, cxlo, cxhi, cylo, cyhi, bxv, byv, bc)) break;
+            if (!round_g<T, GW>(P, g, g0, src, w, h, mvpx, mvpy, step, cxlo, cxhi, cylo, cyhi, bxv, byv, bc)) break;
         }
     }
     M.sad_px += (uint32_t)(4 * w * h * rounds);
@@ -325,7 +331,7 @@ __device__ __noinline__ int3 msearch(const AnalyseParams& __restrict__ P, GroupS
             const int kk = c <= 4 ? c - 1 : c;
             return make_int2(clx(ccx + (kk % 3 - 1) * 2), cly(ccy + (kk / 3 - 1) * 2));
         };
-        pred_points<T>(P, S, g, M.mbx, M.mby, r, bx, by, lgw, lgh, sq, 9, false);
+        pred_points<T, GW>(P, S, g, M.mbx, M.mby, r, bx, by, lgw, lgh, sq, 9, false);
         bc = S.cost[0] + lam * mvd_bits_d(ccx, ccy, mvpx, mvpy);
         for (int c = 1; c < 9; c++) {
             const int2 q = sq(c);
@@ -346,7 +352,7 @@ __device__ __noinline__ int3 msearch(const AnalyseParams& __restrict__ P, GroupS
             const int dx = c == 1 ? -1 : (c == 2 ? 1 : 0), dy = c == 0 ? -1 : (c == 3 ? 1 : 0);
             return make_int2(clx(ccx + dx), cly(ccy + dy));
         };
-        pred_points<T>(P, S, g, M.mbx, M.mby, r, bx, by, lgw, lgh, dm, 4, false);
+        pred_points<T, GW>(P, S, g, M.mbx, M.mby, r, bx, by, lgw, lgh, dm, 4, false);
         for (int c = 0; c < 4; c++) {
             const int2 q = dm(c);
             const int v = S.cost[c] + lam * mvd_bits_d(q.x, q.y, mvpx, mvpy);
@@ -363,21 +369,24 @@ __device__ __noinline__ int3 msearch(const AnalyseParams& __restrict__ P, GroupS
 }
 
 // Block tables of a group (16 entries): the group's lanes take two entries each.
-__device__ __forceinline__ void blk_copy_g(const Grp& g, Blk* dst, const Blk* src) {
-    dst[g.gl] = src[g.gl];
-    dst[g.gl + 8] = src[g.gl + 8];
+template <int GW>
+__device__ __forceinline__ void blk_copy_g(const Grp<GW>& g, Blk* dst, const Blk* src) {
+#pragma unroll
+    for (int k = 0; k < 16 / GW; k++) dst[g.gl + GW * k] = src[g.gl + GW * k];
     __syncwarp(g.mask);
 }
-__device__ __forceinline__ void blk_clear_g(const Grp& g, Blk* dst) {
-    dst[g.gl] = make_int4(0, 0, -1, 0);
-    dst[g.gl + 8] = make_int4(0, 0, -1, 0);
+template <int GW>
+__device__ __forceinline__ void blk_clear_g(const Grp<GW>& g, Blk* dst) {
+#pragma unroll
+    for (int k = 0; k < 16 / GW; k++) dst[g.gl + GW * k] = make_int4(0, 0, -1, 0);
     __syncwarp(g.mask);
 }
 // Marks the w x h blocks at (x, y) decided with vector (mx, my) on reference r.
-__device__ __forceinline__ void blk_paint_g(const Grp& g, Blk* dst, int x, int y, int w, int h, int mx, int my, int r) {
+template <int GW>
+__device__ __forceinline__ void blk_paint_g(const Grp<GW>& g, Blk* dst, int x, int y, int w, int h, int mx, int my, int r) {
 #pragma unroll
-    for (int k = 0; k < 2; k++) {
-        const int i = g.gl + 8 * k, bx = i & 3, by = i >> 2;
+    for (int k = 0; k < 16 / GW; k++) {
+        const int i = g.gl + GW * k, bx = i & 3, by = i >> 2;
         if (bx >= x && bx < x + w && by >= y && by < y + h) dst[i] = make_int4(mx, my, r, 1);
     }
     __syncwarp(g.mask);
@@ -385,8 +394,8 @@ __device__ __forceinline__ void blk_paint_g(const Grp& g, Blk* dst, int x, int y
 
 // sub_search, enc/frame.rs:911-938, for 8x8 block k with the 16x16 vector (ex, ey) as extra candidate:
 // returns (sub_mb_type, its cost) and leaves the block's vectors in S.st.
-template <class T>
-__device__ __noinline__ int2 sub_search_g(const AnalyseParams& __restrict__ P, GroupSmem<T>& __restrict__ S, const Grp& g, Mb& M, int r, int k,
+template <class T, int GW>
+__device__ __noinline__ int2 sub_search_g(const AnalyseParams& __restrict__ P, GroupSmem<T>& __restrict__ S, const Grp<GW>& g, Mb& M, int r, int k,
                                           int ex, int ey) {
     const int lam = P.lambda;
     const int ox = (k & 1) * 2, oy = (k >> 1) * 2;
@@ -398,7 +407,7 @@ __device__ __noinline__ int2 sub_search_g(const AnalyseParams& __restrict__ P, G
         for (int q = 0; q < c_nsub[s]; q++) {
             const int x = ox + c_sub[s][q][0], y = oy + c_sub[s][q][1], w = c_sub[s][q][2], h = c_sub[s][q][3];
             const int2 p = pred_mv_g(S.ext, S.t, x, y, w, 0, r);
-            const int3 ms = msearch<T>(P, S, g, M, r, x, y, w, h, p.x, p.y, ex, ey, 0, 0, 1);
+            const int3 ms = msearch<T, GW>(P, S, g, M, r, x, y, w, h, p.x, p.y, ex, ey, 0, 0, 1);
             cost += ms.x + lam * mvd_bits_d(ms.y, ms.z, p.x, p.y);
             blk_paint_g(g, S.t, x, y, w, h, ms.y, ms.z, r);
         }
@@ -414,22 +423,22 @@ __device__ __noinline__ int2 sub_search_g(const AnalyseParams& __restrict__ P, G
 
 // best_inter_ref, enc/frame.rs:852-905: returns (cost, part, sub (a byte per 8x8 block), cost16) and leaves the
 // winner's vectors, in coding order, in S.best_mvs.
-template <class T>
-__device__ __noinline__ int4 best_inter_ref_g(const AnalyseParams& __restrict__ P, GroupSmem<T>& __restrict__ S, const Grp& g, Mb& M, int r) {
+template <class T, int GW>
+__device__ __noinline__ int4 best_inter_ref_g(const AnalyseParams& __restrict__ P, GroupSmem<T>& __restrict__ S, const Grp<GW>& g, Mb& M, int r) {
     const int lam = P.lambda;
     int rb = 0;
     if (P.nact == 2) rb = lam;  // ref_bits, enc/frame.rs:705-711
     else if (P.nact > 2) rb = lam * (2 * (31 - __clz(r + 1)) + 1);
     const int2 mvp = pred_mv_g(S.ext, nullptr, 0, 0, 4, 0, r);
     const ColMv col = P.col[M.mb];
-    const int3 ms = msearch<T>(P, S, g, M, r, 0, 0, 4, 4, mvp.x, mvp.y, col.mv[0], col.mv[1], 0, 0, col.valid ? 1 : 0);
+    const int3 ms = msearch<T, GW>(P, S, g, M, r, 0, 0, 4, 4, mvp.x, mvp.y, col.mv[0], col.mv[1], 0, 0, col.valid ? 1 : 0);
     const int mx = ms.y, my = ms.z;
     int best_part = 0, best_cost = ms.x + lam * (mvd_bits_d(mx, my, mvp.x, mvp.y) + 1) + rb;
     const int cost16 = best_cost;
     uint32_t sub_out = 0;
     const uint32_t mv16 = (uint32_t)(uint16_t)mx | ((uint32_t)(uint16_t)my << 16);
-    *reinterpret_cast<uint32_t*>(&S.best_mvs[g.gl][0]) = mv16;
-    *reinterpret_cast<uint32_t*>(&S.best_mvs[g.gl + 8][0]) = mv16;
+#pragma unroll
+    for (int k = 0; k < 16 / GW; k++) *reinterpret_cast<uint32_t*>(&S.best_mvs[g.gl + GW * k][0]) = mv16;
     __syncwarp(g.mask);
     if (P.fast) return make_int4(best_cost, 0, 0, cost16);
     // P_8x8 (868-876)
@@ -437,7 +446,7 @@ __device__ __noinline__ int4 best_inter_ref_g(const AnalyseParams& __restrict__ 
     uint32_t sub = 0;
     int cost8 = lam * 9;
     for (int k = 0; k < 4; k++) {
-        const int2 ss = sub_search_g<T>(P, S, g, M, r, k, mx, my);
+        const int2 ss = sub_search_g<T, GW>(P, S, g, M, r, k, mx, my);
         sub |= (uint32_t)ss.x << (8 * k);
         cost8 += ss.y + rb;
         if (cost8 >= best_cost) break;
@@ -476,7 +485,7 @@ __device__ __noinline__ int4 best_inter_ref_g(const AnalyseParams& __restrict__ 
                 const int2 p = pred_mv_g(S.ext, k == 0 ? nullptr : S.t, x, y, w, part, r);
                 const int i0 = part == 1 ? 2 * k : k, i1 = part == 1 ? 2 * k + 1 : k + 2;
                 const Blk a0 = S.st[(i0 / 2) * 8 + (i0 % 2) * 2], a1 = S.st[(i1 / 2) * 8 + (i1 % 2) * 2];
-                const int3 m = msearch<T>(P, S, g, M, r, x, y, w, h, p.x, p.y, a0.x, a0.y, a1.x, a1.y, 2);
+                const int3 m = msearch<T, GW>(P, S, g, M, r, x, y, w, h, p.x, p.y, a0.x, a0.y, a1.x, a1.y, 2);
                 if (k == 0) {
                     m0x = m.y;
                     m0y = m.z;
@@ -494,11 +503,14 @@ __device__ __noinline__ int4 best_inter_ref_g(const AnalyseParams& __restrict__ 
                 best_part = part;
                 best_cost = pc;
                 sub_out = 0;
-                uint32_t v = 0;
-                if (g.gl == 0) v = (uint32_t)(uint16_t)m0x | ((uint32_t)(uint16_t)m0y << 16);
-                else if (g.gl == 1) v = (uint32_t)(uint16_t)m1x | ((uint32_t)(uint16_t)m1y << 16);
-                *reinterpret_cast<uint32_t*>(&S.best_mvs[g.gl][0]) = v;
-                *reinterpret_cast<uint32_t*>(&S.best_mvs[g.gl + 8][0]) = 0u;
+#pragma unroll
+                for (int k = 0; k < 16 / GW; k++) {
+                    const int i = g.gl + GW * k;
+                    uint32_t v = 0;
+                    if (i == 0) v = (uint32_t)(uint16_t)m0x | ((uint32_t)(uint16_t)m0y << 16);
+                    else if (i == 1) v = (uint32_t)(uint16_t)m1x | ((uint32_t)(uint16_t)m1y << 16);
+                    *reinterpret_cast<uint32_t*>(&S.best_mvs[i][0]) = v;
+                }
                 __syncwarp(g.mask);
             }
         }
@@ -508,18 +520,18 @@ __device__ __noinline__ int4 best_inter_ref_g(const AnalyseParams& __restrict__ 
 
 // The macroblock's source rows into the group's shared memory (16 rows of 16 * sizeof(T) bytes, as 128-bit
 // loads) and the table of its neighbours' blocks from the caller's final decisions (load_neighbours).
-template <class T>
-__device__ __forceinline__ void stage_g(const AnalyseParams& __restrict__ P, GroupSmem<T>& __restrict__ S, const Grp& g, const Mb& M) {
+template <class T, int GW>
+__device__ __forceinline__ void stage_g(const AnalyseParams& __restrict__ P, GroupSmem<T>& __restrict__ S, const Grp<GW>& g, const Mb& M) {
     constexpr int B = sizeof(T);
 #pragma unroll
-    for (int k = 0; k < 2 * B; k++) {
-        const int i = g.gl + 8 * k, row = i / B, part = i % B;
+    for (int k = 0; k < 16 * B / GW; k++) {
+        const int i = g.gl + GW * k, row = i / B, part = i % B;
         const uint4 v = *reinterpret_cast<const uint4*>(P.src + ((size_t)(M.mby * 16 + row) * P.ls + M.mbx * 16) * B + part * 16);
         *reinterpret_cast<uint4*>(&S.src[i * 4]) = v;
     }
 #pragma unroll
-    for (int k = 0; k < 4; k++) {
-        const int i = g.gl + 8 * k;
+    for (int k = 0; k < (30 + GW - 1) / GW; k++) {
+        const int i = g.gl + GW * k;
         if (i < 30) {
             const int ex = i % 6 - 1, ey = i / 6 - 1;
             Blk e = make_int4(0, 0, -1, 0);
@@ -547,9 +559,9 @@ __device__ __forceinline__ void stage_g(const AnalyseParams& __restrict__ P, Gro
 
 // One macroblock in replay mode (enc/frame.rs:722-729 and best_inter, 839-849): the P_Skip vector and SAD,
 // then every reference's best_inter_ref, the cheapest (first on ties) winning; the result record.
-template <class T>
-__device__ __forceinline__ void analyse_mb_g(const AnalyseParams& __restrict__ P, GroupSmem<T>& __restrict__ S, const Grp& g, Mb& M) {
-    stage_g<T>(P, S, g, M);
+template <class T, int GW>
+__device__ __forceinline__ void analyse_mb_g(const AnalyseParams& __restrict__ P, GroupSmem<T>& __restrict__ S, const Grp<GW>& g, Mb& M) {
+    stage_g<T, GW>(P, S, g, M);
     // P_Skip (skip_mv, enc/frame.rs:597-603; the SAD of its prediction, 722-729)
     int2 sv = make_int2(0, 0);
     {
@@ -557,22 +569,23 @@ __device__ __forceinline__ void analyse_mb_g(const AnalyseParams& __restrict__ P
         if (!(!a.w || !b.w || (a.z == 0 && a.x == 0 && a.y == 0) || (b.z == 0 && b.x == 0 && b.y == 0)))
             sv = pred_mv_g(S.ext, nullptr, 0, 0, 4, 0, 0);
     }
-    pred_points<T>(P, S, g, M.mbx, M.mby, 0, 0, 0, 2, 2, [&](int) { return sv; }, 1, true);
+    pred_points<T, GW>(P, S, g, M.mbx, M.mby, 0, 0, 0, 2, 2, [&](int) { return sv; }, 1, true);
     const int skip_sad = S.cost[0];
     M.sad_px += 256;
     __syncwarp(g.mask);
     int part = 0, cost = 0, cost16 = 0, bestr = 0;
     uint32_t sub = 0;
     for (int r = 0; r < P.nact; r++) {
-        const int4 bi = best_inter_ref_g<T>(P, S, g, M, r);
+        const int4 bi = best_inter_ref_g<T, GW>(P, S, g, M, r);
         if (r == 0 || bi.x < cost) {
             cost = bi.x;
             part = bi.y;
             sub = (uint32_t)bi.z;
             cost16 = bi.w;
             bestr = r;
-            *reinterpret_cast<uint32_t*>(&S.win_mvs[g.gl][0]) = *reinterpret_cast<const uint32_t*>(&S.best_mvs[g.gl][0]);
-            *reinterpret_cast<uint32_t*>(&S.win_mvs[g.gl + 8][0]) = *reinterpret_cast<const uint32_t*>(&S.best_mvs[g.gl + 8][0]);
+#pragma unroll
+            for (int k = 0; k < 16 / GW; k++)
+                *reinterpret_cast<uint32_t*>(&S.win_mvs[g.gl + GW * k][0]) = *reinterpret_cast<const uint32_t*>(&S.best_mvs[g.gl + GW * k][0]);
             __syncwarp(g.mask);
         }
     }
@@ -594,39 +607,39 @@ __device__ __forceinline__ void analyse_mb_g(const AnalyseParams& __restrict__ P
         R.satd_px = M.satd_px;
         R.pad2 = 0;
     }
-    *reinterpret_cast<uint32_t*>(&R.mvs[g.gl][0]) = *reinterpret_cast<const uint32_t*>(&S.win_mvs[g.gl][0]);
-    *reinterpret_cast<uint32_t*>(&R.mvs[g.gl + 8][0]) = *reinterpret_cast<const uint32_t*>(&S.win_mvs[g.gl + 8][0]);
+#pragma unroll
+    for (int k = 0; k < 16 / GW; k++)
+        *reinterpret_cast<uint32_t*>(&R.mvs[g.gl + GW * k][0]) = *reinterpret_cast<const uint32_t*>(&S.win_mvs[g.gl + GW * k][0]);
     __syncwarp(g.mask);
     uint32_t* out = reinterpret_cast<uint32_t*>(&P.results[M.mb]);
     const uint32_t* in = reinterpret_cast<const uint32_t*>(&R);
 #pragma unroll
-    for (int k = 0; k < 4; k++) {
-        const int i = g.gl + 8 * k;
-        if (i < 26) out[i] = in[i];
-    }
+    for (int k = 0; k < (26 + GW - 1) / GW; k++)
+        if (g.gl + GW * k < 26) out[g.gl + GW * k] = in[g.gl + GW * k];
     __syncwarp(g.mask);
 }
 
-// K2 in replay mode: warps take four tickets at a time, one macroblock per 8-lane group.
-template <class T>
-__global__ void __launch_bounds__(WARPS * 32, MIN_BLOCKS) analyse_replay_g8_kernel(const __grid_constant__ AnalyseParams P) {
-    __shared__ GroupSmem<T> smem[GROUPS];
+// K2 in replay mode: a warp takes 32 / GW tickets at a time, one macroblock per group of GW lanes.
+template <class T, int GW>
+__global__ void __launch_bounds__(warps_for(GW) * 32, MIN_BLOCKS * WARPS / warps_for(GW)) analyse_replay_g8_kernel(const __grid_constant__ AnalyseParams P) {
+    constexpr int MBS = 32 / GW;  // macroblocks a warp
+    __shared__ GroupSmem<T> smem[warps_for(GW) * MBS];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const Grp g = grp_of_lane();
-    GroupSmem<T>& S = smem[wid * 4 + (lane >> 3)];
+    const Grp<GW> g = grp_of_lane<GW>();
+    GroupSmem<T>& S = smem[wid * MBS + lane / GW];
     for (;;) {
         unsigned t = 0;
-        if (lane == 0) t = atomicAdd(P.ticket, 4u);
+        if (lane == 0) t = atomicAdd(P.ticket, (unsigned)MBS);
         t = __shfl_sync(FULL, t, 0);
         if (t >= (unsigned)P.nmb) break;
-        const unsigned mt = t + (unsigned)(lane >> 3);
+        const unsigned mt = t + (unsigned)(lane / GW);
         if (mt < (unsigned)P.nmb) {
             Mb M;
             M.mb = P.order ? P.order[mt] : (int)mt;
             M.mbx = M.mb % P.mb_w;
             M.mby = M.mb / P.mb_w;
             M.sad_px = M.satd_px = 0;
-            analyse_mb_g<T>(P, S, g, M);
+            analyse_mb_g<T, GW>(P, S, g, M);
         }
         __syncwarp();
     }

@@ -12,8 +12,9 @@ struct ironav_ctx {
     int width = 0, height = 0, bd = 8, mb_w = 0, mb_h = 0, pw = 0, ph = 0, sw = 0, sh = 0;
     int max_refs = 0, nslices = 0, nmb = 0;
     int device = 0, nsm = 0, k2_blocks = 0;
-    int g8_blocks = 0;     // the replay analysis' grid in its group form (one macroblock per 8 lanes)
-    int replay_form = 0;   // replay mode's kernel: 0 the group form, 1 one macroblock per warp
+    int g8_blocks = 0;     // the replay analysis' grid in its group forms (one macroblock per 8 / 16 lanes)
+    int g16_blocks = 0, g4_blocks = 0;
+    int replay_form = 0;   // replay mode's kernel: 0 8-lane groups, 1 one macroblock per warp, 2 16-lane groups
     cudaStream_t stream = nullptr;
     long long psize = 0;
     uint8_t* d_src = nullptr;

@@ -175,10 +175,18 @@ int launch_analyse(ironav_ctx* c, bool auto_mode, const ironav_mbstate* d_in, ir
     p.wait_limit = c->wait_limit;
     if (auto_mode) p.epoch = ++c->epoch;
     CK(cudaMemsetAsync(c->d_counters, 0, 2 * sizeof(unsigned), c->stream));
-    if (!auto_mode && c->replay_form == 0 && p.learned == nullptr) {
-        // replay mode: one macroblock per 8-lane group
-        if (c->bd > 8) g8::analyse_replay_g8_kernel<uint16_t><<<c->g8_blocks, g8::WARPS * 32, 0, c->stream>>>(p);
-        else g8::analyse_replay_g8_kernel<uint8_t><<<c->g8_blocks, g8::WARPS * 32, 0, c->stream>>>(p);
+    if (!auto_mode && c->replay_form != 1 && p.learned == nullptr) {
+        // replay mode: one macroblock per group of 8 (or 16) lanes
+        if (c->replay_form == 2) {
+            if (c->bd > 8) g8::analyse_replay_g8_kernel<uint16_t, 16><<<c->g16_blocks, g8::WARPS * 32, 0, c->stream>>>(p);
+            else g8::analyse_replay_g8_kernel<uint8_t, 16><<<c->g16_blocks, g8::WARPS * 32, 0, c->stream>>>(p);
+        } else if (c->replay_form == 3) {
+            if (c->bd > 8) g8::analyse_replay_g8_kernel<uint16_t, 4><<<c->g4_blocks, g8::warps_for(4) * 32, 0, c->stream>>>(p);
+            else g8::analyse_replay_g8_kernel<uint8_t, 4><<<c->g4_blocks, g8::warps_for(4) * 32, 0, c->stream>>>(p);
+        } else {
+            if (c->bd > 8) g8::analyse_replay_g8_kernel<uint16_t, 8><<<c->g8_blocks, g8::WARPS * 32, 0, c->stream>>>(p);
+            else g8::analyse_replay_g8_kernel<uint8_t, 8><<<c->g8_blocks, g8::WARPS * 32, 0, c->stream>>>(p);
+        }
         return cuda_status(cudaGetLastError());
     }
     if (c->bd > 8) {
@@ -363,10 +371,20 @@ int ironav_ctx_create(ironav_ctx** out, int width, int height, int bd, int max_r
     if (e != cudaSuccess) return fail(e);
     c->k2_blocks = std::max(1, per_sm) * c->nsm;
     per_sm = 0;
-    e = bd > 8 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, g8::analyse_replay_g8_kernel<uint16_t>, g8::WARPS * 32, 0)
-               : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, g8::analyse_replay_g8_kernel<uint8_t>, g8::WARPS * 32, 0);
+    e = bd > 8 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, g8::analyse_replay_g8_kernel<uint16_t, 8>, g8::WARPS * 32, 0)
+               : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, g8::analyse_replay_g8_kernel<uint8_t, 8>, g8::WARPS * 32, 0);
     if (e != cudaSuccess) return fail(e);
     c->g8_blocks = std::max(1, per_sm) * c->nsm;
+    per_sm = 0;
+    e = bd > 8 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, g8::analyse_replay_g8_kernel<uint16_t, 16>, g8::WARPS * 32, 0)
+               : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, g8::analyse_replay_g8_kernel<uint8_t, 16>, g8::WARPS * 32, 0);
+    if (e != cudaSuccess) return fail(e);
+    c->g16_blocks = std::max(1, per_sm) * c->nsm;
+    per_sm = 0;
+    e = bd > 8 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, g8::analyse_replay_g8_kernel<uint16_t, 4>, g8::warps_for(4) * 32, 0)
+               : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, g8::analyse_replay_g8_kernel<uint8_t, 4>, g8::warps_for(4) * 32, 0);
+    if (e != cudaSuccess) return fail(e);
+    c->g4_blocks = std::max(1, per_sm) * c->nsm;
     const size_t slack = 256;  // word-granular reads may touch a few bytes past a plane's last sample
     const size_t bytes = (size_t)sample_bytes(c);
     if ((e = cudaMalloc(&c->d_src, (size_t)c->pw * c->ph * bytes + slack)) != cudaSuccess) return fail(e);
@@ -1045,9 +1063,10 @@ int ironav_inloop_end(ironav_ctx* c) {
     return check_device_error(c);
 }
 
-// Replay mode's kernel: 0 one macroblock per 8-lane group (the default), 1 one macroblock per warp.
+// Replay mode's kernel: 0 one macroblock per 8-lane group (the default), 1 one macroblock per warp, 2 one
+// macroblock per 16-lane group.
 int ironav_set_replay_form(ironav_ctx* c, int form) {
-    if (!c || form < 0 || form > 1) return IRONAV_INVALID_ARGUMENT;
+    if (!c || form < 0 || form > 3) return IRONAV_INVALID_ARGUMENT;
     c->replay_form = form;
     return IRONAV_OK;
 }

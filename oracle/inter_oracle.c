@@ -3528,7 +3528,7 @@ int oracle_put_nal(int ref_idc, int kind, const uint8_t* rbsp, int n, uint8_t* o
     return len;
 }
 
-int ironav_set_replay_form(ironav_ctx* c, int form) { return (!c || form < 0 || form > 1) ? IRONAV_INVALID_ARGUMENT : IRONAV_OK; }
+int ironav_set_replay_form(ironav_ctx* c, int form) { return (!c || form < 0 || form > 3) ? IRONAV_INVALID_ARGUMENT : IRONAV_OK; }
 
 int ironav_set_learned(ironav_ctx* c, const int16_t* cands, const uint8_t* cls, int margin, unsigned* stats) {
     if (!c || (cands && (!cls || !stats)) || margin < 0) return IRONAV_INVALID_ARGUMENT;

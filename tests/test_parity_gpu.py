@@ -196,12 +196,10 @@ def test_replay_forms_agree_on_random_decisions(oracle_lib, cuda_lib, mode):
     edge = np.where(mv >= 0, 1, -1) * np.array([2047, 511]) - rng.integers(0, 3, size=mv.shape)  # at the limits
     states["mvs"] = np.where(near == 0, mv // 64, np.where(near == 1, edge, mv))
     want = o.analyse_replay(states)
-    got0 = c.analyse_replay(states)
-    assert cuda_lib.ironav_set_replay_form(c.ctx, 1) == 0
-    got1 = c.analyse_replay(states)
+    for form, name in ((0, "8-lane group"), (1, "warp"), (2, "16-lane group"), (3, "4-lane group")):
+        assert cuda_lib.ironav_set_replay_form(c.ctx, form) == 0
+        assert_same(c.analyse_replay(states), want, f"{mode} {name} form")
     assert cuda_lib.ironav_set_replay_form(c.ctx, 0) == 0
-    assert_same(got0, want, f"{mode} group form")
-    assert_same(got1, want, f"{mode} warp form")
 
 
 def test_random_decisions_exercise_the_clamps(oracle_lib, cuda_lib):
