@@ -177,15 +177,21 @@ int launch_analyse(ironav_ctx* c, bool auto_mode, const ironav_mbstate* d_in, ir
     CK(cudaMemsetAsync(c->d_counters, 0, 2 * sizeof(unsigned), c->stream));
     if (!auto_mode && c->replay_form != 1 && p.learned == nullptr) {
         // replay mode: one macroblock per group of 8 (or 16) lanes
+        // a grid of at most the CTAs the picture's macroblocks fill (one macroblock a group), so that no
+        // SM holds warps that find no work while others hold more than their share
+        auto grid = [&](int resident, int gw) {
+            const int per_cta = g8::warps_for(gw) * (32 / gw);
+            return std::max(1, std::min(resident, (c->nmb + per_cta - 1) / per_cta));
+        };
         if (c->replay_form == 2) {
-            if (c->bd > 8) g8::analyse_replay_g8_kernel<uint16_t, 16><<<c->g16_blocks, g8::WARPS * 32, 0, c->stream>>>(p);
-            else g8::analyse_replay_g8_kernel<uint8_t, 16><<<c->g16_blocks, g8::WARPS * 32, 0, c->stream>>>(p);
+            if (c->bd > 8) g8::analyse_replay_g8_kernel<uint16_t, 16><<<grid(c->g16_blocks, 16), g8::warps_for(16) * 32, 0, c->stream>>>(p);
+            else g8::analyse_replay_g8_kernel<uint8_t, 16><<<grid(c->g16_blocks, 16), g8::warps_for(16) * 32, 0, c->stream>>>(p);
         } else if (c->replay_form == 3) {
-            if (c->bd > 8) g8::analyse_replay_g8_kernel<uint16_t, 4><<<c->g4_blocks, g8::warps_for(4) * 32, 0, c->stream>>>(p);
-            else g8::analyse_replay_g8_kernel<uint8_t, 4><<<c->g4_blocks, g8::warps_for(4) * 32, 0, c->stream>>>(p);
+            if (c->bd > 8) g8::analyse_replay_g8_kernel<uint16_t, 4><<<grid(c->g4_blocks, 4), g8::warps_for(4) * 32, 0, c->stream>>>(p);
+            else g8::analyse_replay_g8_kernel<uint8_t, 4><<<grid(c->g4_blocks, 4), g8::warps_for(4) * 32, 0, c->stream>>>(p);
         } else {
-            if (c->bd > 8) g8::analyse_replay_g8_kernel<uint16_t, 8><<<c->g8_blocks, g8::WARPS * 32, 0, c->stream>>>(p);
-            else g8::analyse_replay_g8_kernel<uint8_t, 8><<<c->g8_blocks, g8::WARPS * 32, 0, c->stream>>>(p);
+            if (c->bd > 8) g8::analyse_replay_g8_kernel<uint16_t, 8><<<grid(c->g8_blocks, 8), g8::warps_for(8) * 32, 0, c->stream>>>(p);
+            else g8::analyse_replay_g8_kernel<uint8_t, 8><<<grid(c->g8_blocks, 8), g8::warps_for(8) * 32, 0, c->stream>>>(p);
         }
         return cuda_status(cudaGetLastError());
     }
@@ -371,13 +377,13 @@ int ironav_ctx_create(ironav_ctx** out, int width, int height, int bd, int max_r
     if (e != cudaSuccess) return fail(e);
     c->k2_blocks = std::max(1, per_sm) * c->nsm;
     per_sm = 0;
-    e = bd > 8 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, g8::analyse_replay_g8_kernel<uint16_t, 8>, g8::WARPS * 32, 0)
-               : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, g8::analyse_replay_g8_kernel<uint8_t, 8>, g8::WARPS * 32, 0);
+    e = bd > 8 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, g8::analyse_replay_g8_kernel<uint16_t, 8>, g8::warps_for(8) * 32, 0)
+               : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, g8::analyse_replay_g8_kernel<uint8_t, 8>, g8::warps_for(8) * 32, 0);
     if (e != cudaSuccess) return fail(e);
     c->g8_blocks = std::max(1, per_sm) * c->nsm;
     per_sm = 0;
-    e = bd > 8 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, g8::analyse_replay_g8_kernel<uint16_t, 16>, g8::WARPS * 32, 0)
-               : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, g8::analyse_replay_g8_kernel<uint8_t, 16>, g8::WARPS * 32, 0);
+    e = bd > 8 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, g8::analyse_replay_g8_kernel<uint16_t, 16>, g8::warps_for(16) * 32, 0)
+               : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, g8::analyse_replay_g8_kernel<uint8_t, 16>, g8::warps_for(16) * 32, 0);
     if (e != cudaSuccess) return fail(e);
     c->g16_blocks = std::max(1, per_sm) * c->nsm;
     per_sm = 0;
