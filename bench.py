@@ -830,11 +830,19 @@ def run_learned(args, rank, world):
 
     steps = npic - 1 - args.warmup
     total = sum_over_ranks(n, world, dev)
-    # algorithmic FLOPs of the four layers on the 48 x 48 interior: 2 input channels, then 32
+    # the four layers' roofline. Their arithmetic intensity (layers 2-4: 2 * 9 * 32 * 32 FLOP per pixel against
+    # 64 bytes read and 64 written) is below the B200's ridge point, so HBM bounds them: bytes per picture =
+    # every layer's input planes read once and its 4 output planes written once, 16 bytes a plane a pixel of
+    # the padded rasters; the tensor-pipe fraction is reported beside it
     flops = n * 48 * 48 * 9 * 32 * 2 * (2 + 3 * 32)
+    conv_bytes = n * 2500 * 16 * ((2 + 4) + 3 * (4 + 4))
     peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
     peak = float(peaks.get("bf16_tflops_sustained", 1400.0))
+    peak_source = ("MEASURED_PEAKS.json bf16_tflops_sustained (measured)" if "bf16_tflops_sustained" in peaks
+                   else "fallback 1.4 PFLOP/s, the pool's sustained bf16 rate (MEASURED_PEAKS.json absent)")
     achieved = flops / (conv_ms * 1e-3) / 1e12
+    hbm = measured_hbm()
+    achieved_gbs = conv_bytes / (conv_ms * 1e-3) / 1e9
     line = {
         "metric": METRIC + " (learned form)",
         "value": total * (npic - 1 - args.warmup) / el, "unit": "MB/s", "n_gpus": world, "steps": steps, "warmup": args.warmup,
@@ -855,10 +863,12 @@ def run_learned(args, rank, world):
                 "d2h_bytes_per_step": n * MBRESULT_DTYPE.itemsize, "ms_per_step": 1e3 * el_e2e / steps,
                 "note": "each picture copied in from pinned host memory, its result records copied out, in stream order"},
         "gpu_launches": 10 * steps,  # per step: source copy 1, planes 1, prep 1, conv 4, head 1, propose 1, analysis 1
-        "roofline": {"bound": "tensor", "kernel": "conv3x3_kernel (4 layers)", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                     "frac": achieved / peak, "traffic": None,
-                     "note": f"algorithmic FLOPs of the 48 x 48 interior ({flops / 1e12:.3f} TFLOP a picture) over the four layers' "
-                             f"CUDA-event time ({conv_ms:.3f} ms a step); peak: MEASURED_PEAKS.json bf16_tflops_sustained (measured)"},
+        "roofline": {"bound": "hbm", "kernel": "conv3x3p_kernel (4 layers)", "achieved": achieved_gbs, "peak": hbm[0], "unit": "GB/s",
+                     "frac": achieved_gbs / hbm[0], "traffic": None, "peak_source": hbm[1],
+                     "tensor": {"achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "peak_source": peak_source},
+                     "note": f"{conv_bytes / 1e9:.2f} GB a picture (each layer's input read and output written once) and "
+                             f"{flops / 1e12:.3f} TFLOP of algorithmic work on the 48 x 48 interior over the four layers' "
+                             f"CUDA-event time ({conv_ms:.3f} ms a step)"},
         "clocks": clk,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -550,6 +550,13 @@ int ironav_prop_prep(const ironav_prop_sample* d_samples, int n, void* d_x, void
 /* The head: d_out[s][j] = d_hb[j] + sum_f d_hw[j][f] feat(s, f), 13 outputs (4 vectors (x, y) in units of 32
  * luma samples, then 5 logits), features f = ((iy * 48 + ix) * 32 + c) of layer 4's output. */
 int ironav_prop_head_fwd(const void* d_feat, int n, const float* d_hw, const float* d_hb, float* d_out, void* stream);
+/* The head's weights packed for ironav_prop_head_fwd_packed: d_hwt[f][16] = d_hw[j][f] (j < 13; zero after),
+ * 73,728 x 16 floats, 16-byte aligned. */
+int ironav_prop_head_pack(const float* d_hw, float* d_hwt, void* stream);
+/* The head as ironav_prop_head_fwd, from the packed weights: one thread per sample over slices of the pixels,
+ * the slices' sums added atomically into d_out (so the order of the additions, and the last bits of the
+ * outputs, vary from run to run). */
+int ironav_prop_head_fwd_packed(const void* d_feat, int n, const float* d_hwt, const float* d_hb, float* d_out, void* stream);
 /* The loss (winner-takes-all L1 on the vectors against d_target_mv (quarter samples), cross-entropy on the
  * logits against d_target_part (0 P_Skip, 1 16x16, 2 16x8, 3 8x16, 4 8x8)) and its gradient d_dout (mean over
  * the n samples); d_sums[0..2] += the vector loss, the partition loss and the partition hits. */

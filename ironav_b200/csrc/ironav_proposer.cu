@@ -91,13 +91,21 @@ int ironav_prop_conv3x3(const void* d_x, int cin, long long samples, const void*
     if (s != IRONAV_OK) return s;
     int nsm = 0;
     if ((s = sm_count(&nsm)) != IRONAV_OK) return s;
-    const int grid = std::min(tiles, nsm * 4);
+    // the pipelined form: two persistent CTAs an SM (78 KB of shared memory and 64 TMEM columns each)
+    const int grid = std::min(tiles, nsm * 2);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const __nv_bfloat16* w = static_cast<const __nv_bfloat16*>(d_w);
     const __nv_bfloat16* mask = static_cast<const __nv_bfloat16*>(d_mask);
     __nv_bfloat16* y = static_cast<__nv_bfloat16*>(d_y);
-    if (cin == 32) conv3x3_kernel<32><<<grid, 128, conv3x3_smem_bytes<32>(), st>>>(map, w, d_bias, relu, mask, y, Q, tiles, d_err);
-    else conv3x3_kernel<16><<<grid, 128, conv3x3_smem_bytes<16>(), st>>>(map, w, d_bias, relu, mask, y, Q, tiles, d_err);
+    if (cin == 32) {
+        constexpr int bytes = conv3x3p_smem_bytes<32>();
+        CK(cudaFuncSetAttribute(conv3x3p_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+        conv3x3p_kernel<32><<<grid, CP_THREADS, bytes, st>>>(map, w, d_bias, relu, mask, y, Q, tiles, d_err);
+    } else {
+        constexpr int bytes = conv3x3p_smem_bytes<16>();
+        CK(cudaFuncSetAttribute(conv3x3p_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+        conv3x3p_kernel<16><<<grid, CP_THREADS, bytes, st>>>(map, w, d_bias, relu, mask, y, Q, tiles, d_err);
+    }
     return cuda_status(cudaGetLastError());
 }
 
@@ -137,6 +145,22 @@ int ironav_prop_head_fwd(const void* d_feat, int n, const float* d_hw, const flo
     if (!d_feat || !d_hw || !d_hb || !d_out || n < 1 || n > (1 << 22)) return IRONAV_INVALID_ARGUMENT;
     prop::head_fwd_kernel<<<(n + prop::HEAD_SPB - 1) / prop::HEAD_SPB, 256, 0, static_cast<cudaStream_t>(stream)>>>(
         static_cast<const __nv_bfloat16*>(d_feat), (long long)n * RPIX, n, d_hw, d_hb, d_out);
+    return cuda_status(cudaGetLastError());
+}
+
+int ironav_prop_head_pack(const float* d_hw, float* d_hwt, void* stream) {
+    if (!d_hw || !d_hwt || !aligned16(d_hwt)) return IRONAV_INVALID_ARGUMENT;
+    prop::head_pack_kernel<<<(prop::NFEAT * 16 + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(d_hw, d_hwt);
+    return cuda_status(cudaGetLastError());
+}
+
+int ironav_prop_head_fwd_packed(const void* d_feat, int n, const float* d_hwt, const float* d_hb, float* d_out, void* stream) {
+    if (!d_feat || !d_hwt || !d_hb || !d_out || n < 1 || n > (1 << 22) || !aligned16(d_hwt)) return IRONAV_INVALID_ARGUMENT;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    CK(cudaMemsetAsync(d_out, 0, (size_t)n * prop::NOUT * sizeof(float), st));
+    const dim3 grid((n + 127) / 128, (48 * 48 + prop::HEAD_PIX - 1) / prop::HEAD_PIX);
+    prop::head_fwd_packed_kernel<<<grid, 128, 0, st>>>(static_cast<const __nv_bfloat16*>(d_feat), (long long)n * RPIX, n,
+                                                       reinterpret_cast<const float4*>(d_hwt), d_hb, d_out);
     return cuda_status(cudaGetLastError());
 }
 

@@ -101,6 +101,58 @@ __global__ void __launch_bounds__(256) head_fwd_kernel(const __nv_bfloat16* __re
     }
 }
 
+// The head's weights packed for head_fwd_packed_kernel: hwt[f][16] = hw[j][f] for j < 13, zero after, so that
+// a feature's 13 weights are four 16-byte loads.
+__global__ void head_pack_kernel(const float* __restrict__ hw, float* __restrict__ hwt) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= NFEAT * 16) return;
+    const int f = i >> 4, j = i & 15;
+    hwt[i] = j < NOUT ? hw[(size_t)j * NFEAT + f] : 0.f;
+}
+
+constexpr int HEAD_PIX = 128;  // interior pixels (of 2304) a CTA of head_fwd_packed_kernel sums over
+
+// The head with one thread per sample: CTA (x, y) takes samples 128x .. 128x + 127 and interior pixels
+// HEAD_PIX * y .. + HEAD_PIX - 1; a thread reads its sample's 32 channels of each pixel (four 16-byte loads)
+// and the features' packed weights, the same for every thread (broadcast loads), and adds its partial sums
+// to out (which CTAs y = 0 start from the bias; out must be zero before the launch).
+__global__ void __launch_bounds__(128) head_fwd_packed_kernel(const __nv_bfloat16* __restrict__ feat, long long Q, int n,
+                                                              const float4* __restrict__ hwt, const float* __restrict__ hb,
+                                                              float* __restrict__ out) {
+    const int s = blockIdx.x * 128 + threadIdx.x;
+    const int p0 = blockIdx.y * HEAD_PIX;
+    float acc[16];
+#pragma unroll
+    for (int j = 0; j < 16; j++) acc[j] = 0.f;
+    if (s < n) {
+#pragma unroll 2
+        for (int pix = p0; pix < p0 + HEAD_PIX && pix < 48 * 48; pix++) {
+            const int iy = pix / 48, ix = pix - iy * 48;
+            const long long q = (long long)s * tc::RPIX + (iy + 1) * tc::RW + (ix + 1);
+#pragma unroll
+            for (int c = 0; c < 4; c++) {
+                const uint4 raw = *reinterpret_cast<const uint4*>(feat + ((size_t)c * Q + q) * 8);
+                const __nv_bfloat16* v = reinterpret_cast<const __nv_bfloat16*>(&raw);
+#pragma unroll
+                for (int e = 0; e < 8; e++) {
+                    const float x = __bfloat162float(v[e]);
+                    const float4* wf = hwt + ((size_t)(pix * 32 + c * 8 + e) << 2);
+#pragma unroll
+                    for (int k = 0; k < 4; k++) {
+                        const float4 w4 = __ldg(wf + k);
+                        acc[4 * k] += x * w4.x;
+                        acc[4 * k + 1] += x * w4.y;
+                        acc[4 * k + 2] += x * w4.z;
+                        acc[4 * k + 3] += x * w4.w;
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < NOUT; j++) atomicAdd(&out[(size_t)s * NOUT + j], acc[j] + (blockIdx.y == 0 ? hb[j] : 0.f));
+    }
+}
+
 // The loss of n samples and its gradient d_out (already divided by n): winner-takes-all L1 on the vectors (the
 // candidate nearest the target, plus 0.05 of every candidate's distance so that none is left untrained) and
 // cross-entropy on the partition logits. target_mv in quarter samples; target_part in 0..4. sums[0] += the

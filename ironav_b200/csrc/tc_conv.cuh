@@ -8,14 +8,14 @@
 // the nine shifts (dy - 1) * 50 + (dx - 1): output pixel q reads input pixel q + shift, and a shift never leaves
 // the sample's own raster for an interior pixel (outputs on the ring are written as zeros).
 //
-// One CTA (4 warps) takes tiles of 128 consecutive output pixels. Per tile: one TMA 3-D box load brings the
-// input halo (pixels q0 - 51 .. q0 + 180 of every plane, zeros beyond the tensor) into shared memory in the
-// same layout; every tap's A operand (128 pixels x 16 channels, K-major, no swizzle) is then just another
-// start address into the halo, so no im2col copy is made. The weights (B: 32 output channels x CIN input
-// channels per tap, K-major) sit in shared memory for the CTA's life. One thread issues 9 taps x CIN / 16
-// MMAs of M = 128, N = 32, K = 16 into one TMEM accumulator (128 lanes x 32 FP32 columns) and commits them to an
-// mbarrier; each warp then reads its 32 lanes (pixels) x 32 columns (channels) with tcgen05.ld, adds the bias,
-// applies ReLU or a gradient mask, zeroes the ring, and stores BF16.
+// A CTA takes tiles of 128 consecutive output pixels. Per tile: one TMA 3-D box load brings the input halo
+// (pixels q0 - 51 .. q0 + 180 of every plane, zeros beyond the tensor) into shared memory in the same layout;
+// every tap's A operand (128 pixels x 16 channels, K-major, no swizzle) is then just another start address into
+// the halo, so no im2col copy is made. The weights (B: 32 output channels x CIN input channels per tap, K-major)
+// sit in shared memory for the CTA's life. One thread issues 9 taps x CIN / 16 MMAs of M = 128, N = 32, K = 16
+// into a TMEM accumulator (128 lanes x 32 FP32 columns); the epilogue warps read their 32 lanes (pixels) x 32
+// columns (channels) back with tcgen05.ld, add the bias, apply ReLU or a gradient mask, zero the ring, and
+// store BF16. Loads, MMAs and epilogues of successive tiles overlap (conv3x3p_kernel, below).
 //
 // The same kernel is the backward pass's data gradient (the convolution with the weights transposed and the
 // taps mirrored, and the mask of the layer's ReLU in the epilogue).
@@ -104,121 +104,6 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
     for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
-}
-
-__device__ __forceinline__ bool ring_pixel(long long q) {
-    const int p = (int)(q % RPIX), y = p / RW, x = p % RW;
-    return y == 0 || y == RW - 1 || x == 0 || x == RW - 1;
-}
-
-// One 3x3 convolution layer (CIN input channels, 32 output channels) over the chunk-major padded rasters:
-// y = act(conv(x, w) + bias), act = ReLU (relu != 0) or the identity, then times (mask > 0) when `mask` is set
-// (the gradient through the layer's ReLU); the ring pixels of y are zero. w is [9 taps][32 out][CIN in] BF16,
-// tap = 3 * dy + dx. x is read through `map` (planes CIN / 8, Q pixels, 8 channels). tiles = ceil(Q / 128).
-template <int CIN>
-__global__ void __launch_bounds__(128, 1) conv3x3_kernel(const __grid_constant__ CUtensorMap map, const __nv_bfloat16* __restrict__ w,
-                                                         const float* __restrict__ bias, int relu, const __nv_bfloat16* __restrict__ mask,
-                                                         __nv_bfloat16* __restrict__ y, long long Q, int tiles, unsigned* err) {
-    constexpr int KC = CIN / 8;             // 16-byte chunks of input channels
-    constexpr int WBYTES = 9 * KC * COUT * 16;
-    constexpr int HBYTES = KC * HALO * 16;
-    extern __shared__ __align__(1024) uint8_t smem[];
-    uint8_t* ws = smem;                                            // weights: [tap][chunk][out][16 B]
-    uint8_t* halo = smem + WBYTES;                                 // input: [chunk][HALO pixels][16 B]
-    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + WBYTES + HBYTES);  // [0] the tile's load, [1] its MMAs
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2);
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-
-    // the weights in the canonical K-major layout: element (tap, n, k) at ((tap * KC + k / 8) * 32 + n) * 16 + (k % 8) * 2
-    for (int i = tid; i < 9 * COUT * CIN; i += 128) {
-        const int t = i / (COUT * CIN), n = (i / CIN) % COUT, k = i % CIN;
-        *reinterpret_cast<__nv_bfloat16*>(ws + ((t * KC + k / 8) * COUT + n) * 16 + (k % 8) * 2) = w[i];
-    }
-    if (tid == 0) {
-        mbar_init(&bars[0], 1);
-        mbar_init(&bars[1], 1);
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    // the generic-proxy writes of the weights before the tensor cores (async proxy) read them
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 32;" ::"r"(smem_u32(tmem_slot)));
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
-    }
-    tc_fence_before();
-    __syncthreads();
-    tc_fence_after();
-    const uint32_t tmem = *tmem_slot;
-    bool failed = false, mma_pending = false, load_pending = false;
-    unsigned it = 0;
-    for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x, it++) {
-        const long long q0 = (long long)tile * TILE;
-        if (tid == 0) {
-            mbar_expect_tx(&bars[0], HBYTES);
-            tma_load_3d(halo, &map, 0, (int)(q0 - HALO_LO), 0, &bars[0]);
-        }
-        const bool loaded = mbar_wait(&bars[0], it & 1);
-        if (__syncthreads_or(!loaded)) {
-            failed = true;
-            load_pending = true;
-            break;
-        }
-        if (tid == 0) {
-            tc_fence_after();
-            const uint32_t h = smem_u32(halo), wb = smem_u32(ws);
-#pragma unroll 1
-            for (int t = 0; t < 9; t++) {
-                const int shift = (t / 3 - 1) * RW + (t % 3 - 1);
-#pragma unroll
-                for (int k = 0; k < KC / 2; k++) {
-                    const uint64_t ad = smem_desc(h + (uint32_t)((2 * k * HALO + HALO_LO + shift) * 16), HALO * 16, 8 * 16);
-                    const uint64_t bd = smem_desc(wb + (uint32_t)((t * KC + 2 * k) * COUT * 16), COUT * 16, 8 * 16);
-                    mma_bf16(tmem, ad, bd, IDESC_BF16_M128_N32, (t | k) != 0);
-                }
-            }
-            mma_commit(&bars[1]);
-        }
-        const bool computed = mbar_wait(&bars[1], it & 1);
-        if (__syncthreads_or(!computed)) {
-            failed = true;
-            mma_pending = true;
-            break;
-        }
-        tc_fence_after();
-        float v[32];
-        tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16), v);
-        const long long q = q0 + warp * 32 + lane;
-        if (q < Q) {
-            const bool ring = ring_pixel(q);
-#pragma unroll
-            for (int c = 0; c < 4; c++) {
-                uint4 m4 = make_uint4(0, 0, 0, 0);
-                if (mask != nullptr) m4 = *reinterpret_cast<const uint4*>(mask + ((size_t)c * Q + q) * 8);
-                const __nv_bfloat16* mk = reinterpret_cast<const __nv_bfloat16*>(&m4);
-                __align__(16) __nv_bfloat16 o[8];
-#pragma unroll
-                for (int e = 0; e < 8; e++) {
-                    float f = v[c * 8 + e] + (bias != nullptr ? bias[c * 8 + e] : 0.f);
-                    if (relu) f = fmaxf(f, 0.f);
-                    if (mask != nullptr && !(__bfloat162float(mk[e]) > 0.f)) f = 0.f;
-                    o[e] = __float2bfloat16_rn(ring ? 0.f : f);
-                }
-                *reinterpret_cast<uint4*>(y + ((size_t)c * Q + q) * 8) = *reinterpret_cast<const uint4*>(o);
-            }
-        }
-        // the TMEM reads and the halo's use are over before the next tile's MMAs and load
-        tc_fence_before();
-        __syncthreads();
-    }
-    if (failed && tid == 0) atomicOr(err, 1u);
-    // a copy or MMAs of the failed tile may still be in flight: wait for them (bounded) before the CTA's
-    // shared memory and TMEM are given up
-    if (load_pending) mbar_wait(&bars[0], it & 1);
-    if (mma_pending) mbar_wait(&bars[1], it & 1);
-    tc_fence_before();
-    __syncthreads();
-    tc_fence_after();
-    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 32;" ::"r"(tmem));
 }
 
 // The weight gradient of a 3x3 layer: dw[t][o][i] += sum over pixels q of dz[q][o] * x[q + shift_t][i] (FP32,
@@ -344,9 +229,189 @@ __global__ void __launch_bounds__(128, 1) wgrad3x3_kernel(const __grid_constant_
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "n"(NCOL));
 }
 
+
+
+// ---- the pipelined form of the 3x3 convolution ----------------------------------------------------------
+//
+// The same convolution with the tile loop overlapped: warp-specialised CTAs of 6 warps. Warp 4 (one thread)
+// streams the tiles' halos by TMA into a ring of CP_STAGES stages; warp 5 (one thread) issues each tile's
+// MMAs into one of two TMEM accumulators as soon as its halo has landed and that accumulator is free, and
+// commits them to the stage's "empty" barrier (the halo may be overwritten) and to the accumulator's
+// "full" barrier; warps 0-3 read a full accumulator back (each its 32 TMEM lanes), release it at once and run
+// the epilogue while the next tile's MMAs fill the other accumulator. Every wait is bounded: a role that
+// gives up sets the CTA's failure flag, every other role stops at its next wait, and the tile loop ends; the
+// copies and MMAs still in flight are then waited for (bounded) before the TMEM is freed.
+constexpr int CP_STAGES = 4;
+constexpr int CP_THREADS = 192;
+
 template <int CIN>
-constexpr int conv3x3_smem_bytes() {
-    return 9 * (CIN / 8) * COUT * 16 + (CIN / 8) * HALO * 16 + 2 * 8 + 16;
+constexpr int conv3x3p_smem_bytes() {
+    return 9 * (CIN / 8) * COUT * 16 + CP_STAGES * (CIN / 8) * HALO * 16 + (2 * CP_STAGES + 4) * 8 + 16;
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// One 3x3 convolution layer (CIN input channels, 32 output channels) over the chunk-major padded rasters:
+// y = act(conv(x, w) + bias), act = ReLU (relu != 0) or the identity, then times (mask > 0) when `mask` is set
+// (the gradient through the layer's ReLU); the ring pixels of y are zero. w is [9 taps][32 out][CIN in] BF16,
+// tap = 3 * dy + dx. x is read through `map` (planes CIN / 8, Q pixels, 8 channels). tiles = ceil(Q / 128).
+template <int CIN>
+__global__ void __launch_bounds__(CP_THREADS, 1) conv3x3p_kernel(const __grid_constant__ CUtensorMap map, const __nv_bfloat16* __restrict__ w,
+                                                                 const float* __restrict__ bias, int relu, const __nv_bfloat16* __restrict__ mask,
+                                                                 __nv_bfloat16* __restrict__ y, long long Q, int tiles, unsigned* err) {
+    constexpr int KC = CIN / 8;
+    constexpr int WBYTES = 9 * KC * COUT * 16;
+    constexpr int HBYTES = KC * HALO * 16;
+    extern __shared__ __align__(1024) uint8_t smem[];
+    uint8_t* ws = smem;                                        // weights: [tap][chunk][out][16 B]
+    uint8_t* halos = smem + WBYTES;                            // CP_STAGES x [chunk][HALO pixels][16 B]
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + WBYTES + CP_STAGES * HBYTES);  // [CP_STAGES]
+    uint64_t* empty = full + CP_STAGES;                        // [CP_STAGES]
+    uint64_t* accf = empty + CP_STAGES;                        // [2] accumulator written
+    uint64_t* acce = accf + 2;                                 // [2] accumulator read back
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acce + 2);
+    volatile int* failed = reinterpret_cast<volatile int*>(tmem_slot + 1);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int ntiles = tiles > (int)blockIdx.x ? (tiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;  // this CTA's tiles
+
+    for (int i = tid; i < 9 * COUT * CIN; i += CP_THREADS) {
+        const int t = i / (COUT * CIN), n = (i / CIN) % COUT, k = i % CIN;
+        *reinterpret_cast<__nv_bfloat16*>(ws + ((t * KC + k / 8) * COUT + n) * 16 + (k % 8) * 2) = w[i];
+    }
+    if (tid == 0) {
+        for (int s = 0; s < CP_STAGES; s++) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        for (int a = 0; a < 2; a++) {
+            mbar_init(&accf[a], 1);
+            mbar_init(&acce[a], 4);
+        }
+        *failed = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    if (warp == 5) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 64;" ::"r"(smem_u32(tmem_slot)));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+    __shared__ int s_loaded, s_issued;
+    if (warp == 4) {
+        // the producer: the halo of tile it into stage it % CP_STAGES once the MMAs of its previous use are done
+        int loaded = 0;
+        if (lane == 0) {
+            for (int it = 0; it < ntiles; it++) {
+                const int s = it % CP_STAGES, k = it / CP_STAGES;
+                if (k > 0 && !mbar_wait(&empty[s], (k - 1) & 1)) {
+                    *failed = 1;
+                    break;
+                }
+                if (*failed) break;
+                const long long q0 = ((long long)blockIdx.x + (long long)it * gridDim.x) * TILE;
+                mbar_expect_tx(&full[s], HBYTES);
+                tma_load_3d(halos + s * HBYTES, &map, 0, (int)(q0 - HALO_LO), 0, &full[s]);
+                loaded = it + 1;
+            }
+            s_loaded = loaded;
+        }
+    } else if (warp == 5) {
+        // the MMA issuer: tile it into accumulator it & 1
+        int issued = 0;
+        if (lane == 0) {
+            for (int it = 0; it < ntiles; it++) {
+                const int s = it % CP_STAGES, k = it / CP_STAGES, a = it & 1, j = it >> 1;
+                if (!mbar_wait(&full[s], k & 1)) {
+                    *failed = 1;
+                    break;
+                }
+                if (j > 0 && !mbar_wait(&acce[a], (j - 1) & 1)) {
+                    *failed = 1;
+                    break;
+                }
+                if (*failed) break;
+                tc_fence_after();
+                const uint32_t h = smem_u32(halos + s * HBYTES), wb = smem_u32(ws), d = tmem + (uint32_t)(a * COUT);
+#pragma unroll 1
+                for (int t = 0; t < 9; t++) {
+                    const int shift = (t / 3 - 1) * RW + (t % 3 - 1);
+#pragma unroll
+                    for (int kk = 0; kk < KC / 2; kk++) {
+                        const uint64_t ad = smem_desc(h + (uint32_t)((2 * kk * HALO + HALO_LO + shift) * 16), HALO * 16, 8 * 16);
+                        const uint64_t bd = smem_desc(wb + (uint32_t)((t * KC + 2 * kk) * COUT * 16), COUT * 16, 8 * 16);
+                        mma_bf16(d, ad, bd, IDESC_BF16_M128_N32, (t | kk) != 0);
+                    }
+                }
+                mma_commit(&empty[s]);
+                mma_commit(&accf[a]);
+                issued = it + 1;
+            }
+            s_issued = issued;
+        }
+    } else {
+        // the epilogue: warp w reads TMEM lanes 32w .. 32w + 31 (pixels), releases the accumulator, stores.
+        // The bias stays in registers; a pixel's raster position comes from its tile's (one 64-bit remainder
+        // a tile, the rest in 32 bits).
+        float bv[32];
+#pragma unroll
+        for (int c = 0; c < 32; c++) bv[c] = bias != nullptr ? bias[c] : 0.f;
+        for (int it = 0; it < ntiles; it++) {
+            const int a = it & 1, j = it >> 1;
+            const bool ok = mbar_wait(&accf[a], j & 1);
+            if (!__all_sync(0xffffffffu, ok)) {
+                if (lane == 0) *failed = 1;
+                break;
+            }
+            tc_fence_after();
+            float v[32];
+            tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(a * COUT), v);
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&acce[a]);
+            const long long q0 = ((long long)blockIdx.x + (long long)it * gridDim.x) * TILE;
+            const long long q = q0 + warp * 32 + lane;
+            if (q < Q) {
+                int p = (int)(q0 % RPIX) + warp * 32 + lane;
+                if (p >= RPIX) p -= RPIX;
+                const int ry = p / RW, rx = p - ry * RW;
+                const bool ring = ry == 0 || ry == RW - 1 || rx == 0 || rx == RW - 1;
+#pragma unroll
+                for (int c = 0; c < 4; c++) {
+                    uint4 m4 = make_uint4(0, 0, 0, 0);
+                    if (mask != nullptr) m4 = *reinterpret_cast<const uint4*>(mask + ((size_t)c * Q + q) * 8);
+                    const __nv_bfloat16* mk = reinterpret_cast<const __nv_bfloat16*>(&m4);
+                    __align__(16) __nv_bfloat16 o[8];
+#pragma unroll
+                    for (int e = 0; e < 8; e++) {
+                        float f = v[c * 8 + e] + bv[c * 8 + e];
+                        if (relu) f = fmaxf(f, 0.f);
+                        if (mask != nullptr && !(__bfloat162float(mk[e]) > 0.f)) f = 0.f;
+                        o[e] = __float2bfloat16_rn(ring ? 0.f : f);
+                    }
+                    *reinterpret_cast<uint4*>(y + ((size_t)c * Q + q) * 8) = *reinterpret_cast<const uint4*>(o);
+                }
+            }
+            if (__any_sync(0xffffffffu, *failed != 0)) break;
+        }
+    }
+    __syncthreads();
+    if (tid == 0 && *failed) atomicOr(err, 1u);
+    if (warp == 4 && lane == 0) {
+        // copies issued but never consumed, then the MMAs' last arrivals on the stages (bounded waits)
+        for (int it = s_issued; it < s_loaded; it++) mbar_wait(&full[it % CP_STAGES], (it / CP_STAGES) & 1);
+        for (int it = s_issued > CP_STAGES ? s_issued - CP_STAGES : 0; it < s_issued; it++)
+            mbar_wait(&empty[it % CP_STAGES], (it / CP_STAGES) & 1);
+    }
+    if (warp == 5 && lane == 0 && s_issued > 0) mbar_wait(&accf[(s_issued - 1) & 1], ((s_issued - 1) >> 1) & 1);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 5) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 64;" ::"r"(tmem));
 }
 
 }  // namespace tc

@@ -137,7 +137,7 @@ EXPORTS = (
     "ironav_batch_set_tuning", "ironav_batch_get_tuning", "ironav_batch_autotune",
     "ironav_prop_conv3x3", "ironav_prop_wgrad3x3", "ironav_prop_prep", "ironav_prop_head_fwd", "ironav_prop_loss",
     "ironav_prop_head_bwd", "ironav_prop_adam", "ironav_prop_weights", "ironav_set_learned",
-    "ironav_prop_propose", "ironav_set_replay_form",
+    "ironav_prop_propose", "ironav_set_replay_form", "ironav_prop_head_pack", "ironav_prop_head_fwd_packed",
 )
 
 # ironav_batch_tuning (include/ironav_inter.h): the batched step's knobs
@@ -227,6 +227,9 @@ def _declare(lib: ctypes.CDLL) -> ctypes.CDLL:
         lib.ironav_prop_head_bwd.argtypes = [_VP, _I, _VP, _VP, _VP, _VP, _VP, _VP]
         lib.ironav_prop_adam.argtypes = [_VP, _VP, _VP, _VP, _LL, _F, _F, _F, _I, _F, _VP]
         lib.ironav_prop_weights.argtypes = [_VP, _I, _VP, _VP, _VP]
+    if hasattr(lib, "ironav_prop_head_pack"):
+        lib.ironav_prop_head_pack.argtypes = [_VP, _VP, _VP]
+        lib.ironav_prop_head_fwd_packed.argtypes = [_VP, _I, _VP, _VP, _VP, _VP]
     if hasattr(lib, "ironav_prop_propose"):
         lib.ironav_prop_propose.argtypes = [_VP, _I, _F, _VP, _VP, _VP]
     if hasattr(lib, "ironav_set_replay_form"):

@@ -67,6 +67,7 @@ class Proposer:
         for l in (2, 3, 4):
             self.wf[l] = torch.zeros((9, 32, 32), dtype=bf, device=self.dev)
             self.wt[l] = torch.zeros((9, 32, 32), dtype=bf, device=self.dev)
+        self.hwt = torch.zeros((NFEAT, 16), dtype=torch.float32, device=self.dev)  # the head's packed weights
         self.err = torch.zeros(1, dtype=torch.int32, device=self.dev)
         self.sums = torch.zeros(3, dtype=torch.float32, device=self.dev)
         self.step_count = 0
@@ -113,8 +114,10 @@ class Proposer:
         return self.stream.cuda_stream
 
     def refresh_weights(self) -> None:
-        """The BF16 copies of the conv weights (and the data gradient's transposed ones) from the masters."""
+        """The BF16 copies of the conv weights (and the data gradient's transposed ones) and the head's packed
+        weights, from the masters."""
         lib = self.lib
+        _check(lib.ironav_prop_head_pack(self.views["hw"].data_ptr(), self.hwt.data_ptr(), self._s), "head pack")
         _check(lib.ironav_prop_weights(self.views["w1"].data_ptr(), 16, self.wf[1].data_ptr(), None, self._s), "weights 1")
         for l in (2, 3, 4):
             _check(lib.ironav_prop_weights(self.views[f"w{l}"].data_ptr(), 32, self.wf[l].data_ptr(), self.wt[l].data_ptr(), self._s),
@@ -154,8 +157,8 @@ class Proposer:
                                            self.z[l].data_ptr(), e, self._s), f"conv {l}")
         if conv_events is not None:
             conv_events[1].record(self.stream)
-        _check(lib.ironav_prop_head_fwd(self.z[4].data_ptr(), n, self.views["hw"].data_ptr(), self.views["hb"].data_ptr(),
-                                        self.out.data_ptr(), self._s), "head")
+        _check(lib.ironav_prop_head_fwd_packed(self.z[4].data_ptr(), n, self.hwt.data_ptr(), self.views["hb"].data_ptr(),
+                                               self.out.data_ptr(), self._s), "head")
 
     def backward(self, n: int, target_mv, target_part) -> None:
         """The loss of the last forward pass against the targets (device tensors: int16 [n, 2] quarter samples,

@@ -3566,6 +3566,14 @@ int ironav_prop_adam(float* p, float* g, float* m, float* v, long long n, float 
     return IRONAV_HARDWARE_UNAVAILABLE;
 }
 int ironav_prop_weights(const float* w, int cin, void* wf, void* wt, void* s) { (void)w; (void)cin; (void)wf; (void)wt; (void)s; return IRONAV_HARDWARE_UNAVAILABLE; }
+int ironav_prop_head_pack(const float* hw, float* hwt, void* s) {
+    (void)hw; (void)hwt; (void)s;
+    return IRONAV_HARDWARE_UNAVAILABLE;
+}
+int ironav_prop_head_fwd_packed(const void* f, int n, const float* hwt, const float* hb, float* o, void* s) {
+    (void)f; (void)n; (void)hwt; (void)hb; (void)o; (void)s;
+    return IRONAV_HARDWARE_UNAVAILABLE;
+}
 int ironav_prop_propose(const float* o, int n, float min_conf, int16_t* c, uint8_t* k, void* s) {
     (void)o; (void)n; (void)min_conf; (void)c; (void)k; (void)s;
     return IRONAV_HARDWARE_UNAVAILABLE;

@@ -147,6 +147,16 @@ def test_head_and_loss_match_torch_autograd(cuda_lib):
     B = hb.clone().requires_grad_(True)
     o = f @ W.t() + B
     torch.testing.assert_close(out, o.detach(), rtol=1e-4, atol=1e-5)
+    # the packed form of the head (one thread per sample, slices of pixels added atomically): the same sums
+    # in another order, so the same FP32 tolerance
+    hwt = torch.zeros((32 * 48 * 48, 16), device="cuda")
+    out2 = torch.full_like(out, 7.0)
+    assert cuda_lib.ironav_prop_head_pack(hw.data_ptr(), hwt.data_ptr(), s) == 0
+    assert cuda_lib.ironav_prop_head_fwd_packed(fp.data_ptr(), n, hwt.data_ptr(), hb.data_ptr(), out2.data_ptr(), s) == 0
+    torch.cuda.synchronize()
+    torch.testing.assert_close(hwt[:, :13], hw.t())
+    assert torch.all(hwt[:, 13:] == 0)
+    torch.testing.assert_close(out2, o.detach(), rtol=1e-4, atol=1e-5)
     t = tmv.float() / 128.0
     dist = (o[:, :8].reshape(n, 4, 2) - t[:, None, :]).abs().sum(-1)
     lmv = dist.min(dim=1).values + 0.05 * dist.sum(dim=1)
