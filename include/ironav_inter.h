@@ -495,17 +495,19 @@ int ironav_batch_deblock(ironav_batch* batch, void* const* d_y, const int* y_str
  * nothing to tune). The knobs are the analysis launch's CTAs per SM (4, 5 or 6; its register cap becomes
  * 128, 96 or 80 a thread: more warps in flight against more spills), the half-sample planes' tile rows
  * (16 or 8) and the ticket order of the merged wavefronts (0: ties between streams by stream index; 1: by
- * stream size, largest first). The default is 4, 16, 0. Every setting gives the same results; only the
- * time changes. */
+ * stream size, largest first). k2_group picks the analysis' form: 0, one macroblock a warp; 8, one macroblock
+ * per 8-lane group, four a warp, so that the search's control runs once for four macroblocks (k2_ctas_per_sm
+ * is then 4). The default is 4, 16, 0, 0. Every setting gives the same results; only the time changes. */
 typedef struct ironav_batch_tuning {
     int32_t k2_ctas_per_sm;
     int32_t k1_tile_rows;
     int32_t order;
+    int32_t k2_group;
     float ms;                    /* ironav_batch_autotune: the setting's median step time (milliseconds) */
 } ironav_batch_tuning;
 int ironav_batch_set_tuning(ironav_batch* batch, const ironav_batch_tuning* t);
 int ironav_batch_get_tuning(const ironav_batch* batch, ironav_batch_tuning* t);
-/* Times every setting (3 x 2 x 2) on `reps` batched steps of these inputs (arguments as ironav_batch_step's;
+/* Times every setting ((3 + 1) x 2 x 2: the warp form at 4, 5 and 6 CTAs an SM and the group form) on `reps` batched steps of these inputs (arguments as ironav_batch_step's;
  * CUDA events on the batch's stream, after a warm-up step each), keeps the fastest by median and returns it
  * in best (and, when all is not NULL, up to cap settings with their times, *n_all of them). Each context's
  * reference ring is put back before every step, so the batch ends exactly as after one ironav_batch_step

@@ -580,7 +580,8 @@ __device__ __noinline__ int4 best_inter_ref_g(const AnalyseParams& __restrict__ 
 // The macroblock's source rows into the group's shared memory (16 rows of 16 * sizeof(T) bytes, as 128-bit
 // loads) and the table of its neighbours' blocks from the caller's final decisions (load_neighbours).
 template <class T, int GW>
-__device__ __forceinline__ void stage_g(const AnalyseParams& __restrict__ P, GroupSmem<T>& __restrict__ S, const Grp<GW>& g, const Mb& M) {
+__device__ __forceinline__ void stage_g(const AnalyseParams& __restrict__ P, GroupSmem<T>& __restrict__ S, const Grp<GW>& g, const Mb& M,
+                                        const ironav_mbstate* __restrict__ states) {
     constexpr int B = sizeof(T);
 #pragma unroll
     for (int k = 0; k < 16 * B / GW; k++) {
@@ -599,7 +600,7 @@ __device__ __forceinline__ void stage_g(const AnalyseParams& __restrict__ P, Gro
                 const int bx = ex < 0 ? 3 : (ex >= 4 ? 0 : ex), by = ey < 0 ? 3 : ey;
                 // macroblocks of earlier slices are not available (enc/frame.rs:509-515)
                 if (nx >= 0 && nx < P.mb_w && ny >= P.band_start[M.mby] && ny < P.mb_h) {
-                    const ironav_mbstate* st = &P.states_in[(size_t)ny * P.mb_w + nx];
+                    const ironav_mbstate* st = &states[(size_t)ny * P.mb_w + nx];
                     e.w = 1;
                     const int rf = st->refs[(by >> 1) * 2 + (bx >> 1)];
                     if (st->inter && rf >= 0) {
@@ -616,11 +617,14 @@ __device__ __forceinline__ void stage_g(const AnalyseParams& __restrict__ P, Gro
     __syncwarp(g.mask);
 }
 
-// One macroblock in replay mode (enc/frame.rs:722-729 and best_inter, 839-849): the P_Skip vector and SAD,
-// then every reference's best_inter_ref, the cheapest (first on ties) winning; the result record.
-template <class T, int GW>
+// One macroblock (enc/frame.rs:722-729 and best_inter, 839-849): the P_Skip vector and SAD, then every
+// reference's best_inter_ref, the cheapest (first on ties) winning; the result record. Replay mode reads the
+// neighbours from the caller's decisions; AUTO (auto mode) reads them from the decisions already published,
+// stops at the P_Skip test when its SAD is under the threshold, and writes the macroblock's own decision
+// (its MbState, finish_mb, enc/frame.rs:2281-2321) for the macroblocks after it.
+template <class T, int GW, bool AUTO = false>
 __device__ __forceinline__ void analyse_mb_g(const AnalyseParams& __restrict__ P, GroupSmem<T>& __restrict__ S, const Grp<GW>& g, Mb& M) {
-    stage_g<T, GW>(P, S, g, M);
+    stage_g<T, GW>(P, S, g, M, AUTO ? P.states_out : P.states_in);
     // P_Skip (skip_mv, enc/frame.rs:597-603; the SAD of its prediction, 722-729)
     int2 sv = make_int2(0, 0);
     {
@@ -632,9 +636,10 @@ __device__ __forceinline__ void analyse_mb_g(const AnalyseParams& __restrict__ P
     const int skip_sad = S.cost[0];
     M.sad_px += 256;
     __syncwarp(g.mask);
+    const bool skip = AUTO && skip_sad < P.skip_thresh;
     int part = 0, cost = 0, cost16 = 0, bestr = 0;
     uint32_t sub = 0;
-    for (int r = 0; r < P.nact; r++) {
+    for (int r = 0; r < (skip ? 0 : P.nact); r++) {
         const int4 bi = best_inter_ref_g<T, GW>(P, S, g, M, r);
         if (r == 0 || bi.x < cost) {
             cost = bi.x;
@@ -658,7 +663,7 @@ __device__ __forceinline__ void analyse_mb_g(const AnalyseParams& __restrict__ P
             R.refs[i] = (uint8_t)bestr;
             R.sub[i] = (uint8_t)((sub >> (8 * i)) & 0xff);
         }
-        R.flags = IRONAV_RESULT_INTER;
+        R.flags = skip ? IRONAV_RESULT_SKIP : IRONAV_RESULT_INTER;
         R.pad[0] = R.pad[1] = 0;
         R.cost = cost;
         R.cost16 = cost16;
@@ -668,8 +673,37 @@ __device__ __forceinline__ void analyse_mb_g(const AnalyseParams& __restrict__ P
     }
 #pragma unroll
     for (int k = 0; k < 16 / GW; k++)
-        *reinterpret_cast<uint32_t*>(&R.mvs[g.gl + GW * k][0]) = *reinterpret_cast<const uint32_t*>(&S.win_mvs[g.gl + GW * k][0]);
+        *reinterpret_cast<uint32_t*>(&R.mvs[g.gl + GW * k][0]) = skip ? 0u : *reinterpret_cast<const uint32_t*>(&S.win_mvs[g.gl + GW * k][0]);
     __syncwarp(g.mask);
+    if constexpr (AUTO) {
+        // the decision's MbState: the vector of the rectangle of rects(part, sub) holding each 4x4 block, the
+        // reference of each 8x8 block
+        uint32_t* so = reinterpret_cast<uint32_t*>(&P.states_out[M.mb]);
+#pragma unroll
+        for (int k = 0; k < 16 / GW; k++) {
+            const int i = g.gl + GW * k, bx = i & 3, by = i >> 2;
+            uint32_t mv = (uint32_t)(uint16_t)sv.x | ((uint32_t)(uint16_t)sv.y << 16);
+            if (!skip) {
+                int idx = 0;
+                if (part == 1) idx = by >> 1;
+                else if (part == 2) idx = bx >> 1;
+                else if (part == 3) {
+                    const int kk = (by >> 1) * 2 + (bx >> 1);
+                    int n = 0;
+                    for (int q = 0; q < kk; q++) n += c_nsub[(sub >> (8 * q)) & 0xff];
+                    const int s8 = (sub >> (8 * kk)) & 0xff, lx = bx & 1, ly = by & 1;
+                    idx = n + (s8 == 0 ? 0 : (s8 == 1 ? ly : (s8 == 2 ? lx : ly * 2 + lx)));
+                }
+                mv = *reinterpret_cast<const uint32_t*>(&S.win_mvs[idx][0]);
+            }
+            so[2 + i] = mv;
+        }
+        if (g.gl == 0) {
+            const uint32_t rf = (uint32_t)(uint8_t)(int8_t)(skip ? 0 : bestr);
+            so[0] = 1u | (rf << 8) | (rf << 16) | (rf << 24);  // inter, refs[0..2]
+            so[1] = rf;                                         // refs[3], pad
+        }
+    }
     uint32_t* out = reinterpret_cast<uint32_t*>(&P.results[M.mb]);
     const uint32_t* in = reinterpret_cast<const uint32_t*>(&R);
 #pragma unroll
@@ -699,6 +733,50 @@ __global__ void __launch_bounds__(warps_for(GW) * 32, MIN_BLOCKS * WARPS / warps
             M.mby = M.mb / P.mb_w;
             M.sad_px = M.satd_px = 0;
             analyse_mb_g<T, GW>(P, S, g, M);
+        }
+        __syncwarp();
+    }
+}
+
+// Every stream's auto-mode analysis in one launch with one macroblock per 8-lane group (the batched form's
+// group variant): a warp takes four tickets of the merged wavefront order; each group looks its stream up in
+// the table, waits (bounded) until its left and top-right neighbours are published, analyses its macroblock and
+// publishes it. A group may wait on another group of its own warp (tickets of one block can follow each other
+// in a stream's wavefront); no barrier of the whole warp sits between a group's wait and its publication, so the
+// waiting group never holds the other back.
+template <class T>
+__global__ void __launch_bounds__(WARPS * 32, MIN_BLOCKS) analyse_batch_g8_kernel(const AnalyseParams* __restrict__ table,
+                                                                                  const uint32_t* __restrict__ order, unsigned ntickets,
+                                                                                  unsigned* ticket, const unsigned* err) {
+    __shared__ GroupSmem<T> smem[WARPS * 4];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const Grp<8> g = grp_of_lane<8>();
+    GroupSmem<T>& S = smem[wid * 4 + (lane >> 3)];
+    for (;;) {
+        unsigned t = 0;
+        if (lane == 0) t = atomicAdd(ticket, 4u);
+        t = __shfl_sync(FULL, t, 0);
+        if (t >= ntickets || ld_acquire(err) != 0) break;
+        const unsigned mt = t + (unsigned)(lane >> 3);
+        if (mt < ntickets) {
+            const uint32_t e = order[mt];
+            const AnalyseParams& P = table[e >> 20];
+            Mb M;
+            M.mb = (int)(e & 0xFFFFFu);
+            M.mbx = M.mb % P.mb_w;
+            M.mby = M.mb / P.mb_w;
+            M.sad_px = M.satd_px = 0;
+            const int start = P.band_start[M.mby];
+            bool ok = true;
+            if (M.mbx > 0) ok = wait_published(P, M.mb - 1);
+            if (ok && M.mby > start) ok = wait_published(P, (M.mbx + 1 < P.mb_w) ? M.mb - P.mb_w + 1 : M.mb - P.mb_w);
+            ok = __all_sync(g.mask, ok);
+            if (ok) {
+                analyse_mb_g<T, 8, true>(P, S, g, M);
+                __threadfence();
+                __syncwarp(g.mask);
+                if (g.gl == 0) st_release(&P.flags[M.mb], P.epoch);
+            }
         }
         __syncwarp();
     }

@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "analyse.cuh"
+#include "analyse_g8.cuh"
 #include "ctx.cuh"
 #include "decide.cuh"
 #include "planes.cuh"
@@ -159,8 +160,8 @@ struct ironav_batch {
     int bd = 8;  // every stream's sample depth
     int n = 0, total_mbs = 0, total_tiles = 0, total_rows = 0, k2_blocks = 0;
     int tiles_th[2] = {0, 0};  // the planes' tiles at each tile height
-    int k2_blocks_v[3] = {0, 0, 0};  // the analysis' persistent grid for each CTAs-per-SM variant
-    int minb_i = 0, th_i = 0, order_i = 0;  // the current tuning (indices into TUNE_MINB, TUNE_TH; the order)
+    int k2_blocks_v[4] = {0, 0, 0, 0};  // the analysis' persistent grid for each variant (TUNE_MINB's, then the group form)
+    int minb_i = 0, th_i = 0, order_i = 0;  // the current tuning (indices into TUNE_MINB or 3 for the group form, TUNE_TH; the order)
     std::vector<int> mb0;  // each stream's first flag
     uint32_t* d_order = nullptr;  // the two ticket orders, total_mbs each
     unsigned* d_flags = nullptr;
@@ -278,6 +279,12 @@ extern "C" int ironav_batch_create(ironav_batch** out, ironav_ctx* const* ctxs, 
         if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, K2_WARPS * 32, 0)) != cudaSuccess) return fail(e);
         b->k2_blocks_v[v] = std::max(1, per_sm) * ctxs[0]->nsm;
     }
+    {
+        int per_sm = 0;
+        const void* fn = b->bd > 8 ? (const void*)g8::analyse_batch_g8_kernel<uint16_t> : (const void*)g8::analyse_batch_g8_kernel<uint8_t>;
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, g8::WARPS * 32, 0)) != cudaSuccess) return fail(e);
+        b->k2_blocks_v[3] = std::max(1, per_sm) * ctxs[0]->nsm;
+    }
     b->k2_blocks = b->k2_blocks_v[0];
     *out = b;
     return IRONAV_OK;
@@ -362,16 +369,25 @@ extern "C" int ironav_batch_step(ironav_batch* b, const void* const* d_src, cons
     CK(cudaMemsetAsync(b->d_counters, 0, sizeof(unsigned) * 2, b->stream));
     const uint32_t* order = b->d_order + (size_t)b->order_i * b->total_mbs;
     const unsigned nt = (unsigned)b->total_mbs;
-    const int grid = b->k2_blocks_v[b->minb_i];
     unsigned* tk = b->d_counters;
     const unsigned* er = b->d_counters + 1;
+    bool group = b->minb_i == 3;
+    for (int i = 0; i < b->n && group; i++)
+        if (b->ctx[i]->learned) group = false;  // the group form has no learned judge: the warp form then
+    if (group) {
+        if (b->bd > 8) g8::analyse_batch_g8_kernel<uint16_t><<<b->k2_blocks_v[3], g8::WARPS * 32, 0, b->stream>>>(b->d_table, order, nt, tk, er);
+        else g8::analyse_batch_g8_kernel<uint8_t><<<b->k2_blocks_v[3], g8::WARPS * 32, 0, b->stream>>>(b->d_table, order, nt, tk, er);
+        return cuda_status(cudaGetLastError());
+    }
+    const int minb = b->minb_i == 3 ? 0 : b->minb_i;
+    const int grid = b->k2_blocks_v[minb];
     if (b->bd > 8) {
-        if (b->minb_i == 0) analyse_batch_kernel<uint16_t, 4><<<grid, K2_WARPS * 32, 0, b->stream>>>(b->d_table, order, nt, tk, er);
-        else if (b->minb_i == 1) analyse_batch_kernel<uint16_t, 5><<<grid, K2_WARPS * 32, 0, b->stream>>>(b->d_table, order, nt, tk, er);
+        if (minb == 0) analyse_batch_kernel<uint16_t, 4><<<grid, K2_WARPS * 32, 0, b->stream>>>(b->d_table, order, nt, tk, er);
+        else if (minb == 1) analyse_batch_kernel<uint16_t, 5><<<grid, K2_WARPS * 32, 0, b->stream>>>(b->d_table, order, nt, tk, er);
         else analyse_batch_kernel<uint16_t, 6><<<grid, K2_WARPS * 32, 0, b->stream>>>(b->d_table, order, nt, tk, er);
     } else {
-        if (b->minb_i == 0) analyse_batch_kernel<uint8_t, 4><<<grid, K2_WARPS * 32, 0, b->stream>>>(b->d_table, order, nt, tk, er);
-        else if (b->minb_i == 1) analyse_batch_kernel<uint8_t, 5><<<grid, K2_WARPS * 32, 0, b->stream>>>(b->d_table, order, nt, tk, er);
+        if (minb == 0) analyse_batch_kernel<uint8_t, 4><<<grid, K2_WARPS * 32, 0, b->stream>>>(b->d_table, order, nt, tk, er);
+        else if (minb == 1) analyse_batch_kernel<uint8_t, 5><<<grid, K2_WARPS * 32, 0, b->stream>>>(b->d_table, order, nt, tk, er);
         else analyse_batch_kernel<uint8_t, 6><<<grid, K2_WARPS * 32, 0, b->stream>>>(b->d_table, order, nt, tk, er);
     }
     return cuda_status(cudaGetLastError());
@@ -382,8 +398,12 @@ extern "C" int ironav_batch_step(ironav_batch* b, const void* const* d_src, cons
 static int tuning_index(const ironav_batch_tuning* t, int* mi, int* ti) {
     *mi = -1;
     *ti = -1;
-    for (int v = 0; v < 3; v++)
-        if (t->k2_ctas_per_sm == TUNE_MINB[v]) *mi = v;
+    if (t->k2_group == 8) {
+        if (t->k2_ctas_per_sm == 4) *mi = 3;
+    } else if (t->k2_group == 0) {
+        for (int v = 0; v < 3; v++)
+            if (t->k2_ctas_per_sm == TUNE_MINB[v]) *mi = v;
+    }
     for (int v = 0; v < 2; v++)
         if (t->k1_tile_rows == TUNE_TH[v]) *ti = v;
     return (*mi < 0 || *ti < 0 || t->order < 0 || t->order > 1) ? IRONAV_INVALID_ARGUMENT : IRONAV_OK;
@@ -401,9 +421,10 @@ extern "C" int ironav_batch_set_tuning(ironav_batch* b, const ironav_batch_tunin
 
 extern "C" int ironav_batch_get_tuning(const ironav_batch* b, ironav_batch_tuning* t) {
     if (!b || !t) return IRONAV_INVALID_ARGUMENT;
-    t->k2_ctas_per_sm = TUNE_MINB[b->minb_i];
+    t->k2_ctas_per_sm = b->minb_i == 3 ? 4 : TUNE_MINB[b->minb_i];
     t->k1_tile_rows = TUNE_TH[b->th_i];
     t->order = b->order_i;
+    t->k2_group = b->minb_i == 3 ? 8 : 0;
     t->ms = 0.f;
     return IRONAV_OK;
 }
@@ -438,7 +459,7 @@ extern "C" int ironav_batch_autotune(ironav_batch* b, const void* const* d_src, 
     int count = 0, bm = 0, bt = 0, bo = 0;
     float best_ms = 0.f;
     int status = IRONAV_OK;
-    for (int mi = 0; mi < 3 && status == IRONAV_OK; mi++)
+    for (int mi = 0; mi < 4 && status == IRONAV_OK; mi++)
         for (int ti = 0; ti < 2 && status == IRONAV_OK; ti++)
             for (int oi = 0; oi < 2 && status == IRONAV_OK; oi++) {
                 b->minb_i = mi;
@@ -457,9 +478,10 @@ extern "C" int ironav_batch_autotune(ironav_batch* b, const void* const* d_src, 
                 std::sort(ms.begin() + 1, ms.end());
                 const float med = ms[1 + reps / 2];
                 if (all && count < cap) {
-                    all[count].k2_ctas_per_sm = TUNE_MINB[mi];
+                    all[count].k2_ctas_per_sm = mi == 3 ? 4 : TUNE_MINB[mi];
                     all[count].k1_tile_rows = TUNE_TH[ti];
                     all[count].order = oi;
+                    all[count].k2_group = mi == 3 ? 8 : 0;
                     all[count].ms = med;
                 }
                 if (count == 0 || med < best_ms) {
@@ -477,9 +499,10 @@ extern "C" int ironav_batch_autotune(ironav_batch* b, const void* const* d_src, 
     b->order_i = bo;
     if (n_all) *n_all = count;
     if (status != IRONAV_OK) return status;
-    best->k2_ctas_per_sm = TUNE_MINB[bm];
+    best->k2_ctas_per_sm = bm == 3 ? 4 : TUNE_MINB[bm];
     best->k1_tile_rows = TUNE_TH[bt];
     best->order = bo;
+    best->k2_group = bm == 3 ? 8 : 0;
     best->ms = best_ms;
     return IRONAV_OK;
 }

@@ -141,7 +141,7 @@ EXPORTS = (
 )
 
 # ironav_batch_tuning (include/ironav_inter.h): the batched step's knobs
-BATCH_TUNING_DTYPE = np.dtype([("k2_ctas_per_sm", "<i4"), ("k1_tile_rows", "<i4"), ("order", "<i4"), ("ms", "<f4")])
+BATCH_TUNING_DTYPE = np.dtype([("k2_ctas_per_sm", "<i4"), ("k1_tile_rows", "<i4"), ("order", "<i4"), ("k2_group", "<i4"), ("ms", "<f4")])
 
 # ironav_stream_params (include/ironav_inter.h): what the SPS and PPS say
 STREAM_PARAMS_DTYPE = np.dtype([("width", "<i4"), ("height", "<i4"), ("bd", "<i4"), ("fps_num", "<i4"), ("fps_den", "<i4"),
@@ -751,11 +751,12 @@ class InterBatch:
     def tuning(self) -> dict:
         t = np.zeros(1, dtype=BATCH_TUNING_DTYPE)
         InterStage._check(self.lib.ironav_batch_get_tuning(self.h, _ptr(t)), "ironav_batch_get_tuning")
-        return {k: t[0][k].item() for k in ("k2_ctas_per_sm", "k1_tile_rows", "order")}
+        return {k: t[0][k].item() for k in ("k2_ctas_per_sm", "k1_tile_rows", "order", "k2_group")}
 
-    def set_tuning(self, k2_ctas_per_sm: int, k1_tile_rows: int, order: int) -> None:
+    def set_tuning(self, k2_ctas_per_sm: int, k1_tile_rows: int, order: int, k2_group: int = 0) -> None:
+        """k2_group: 0, the analysis with one macroblock a warp; 8, one per 8-lane group (k2_ctas_per_sm 4)."""
         t = np.zeros(1, dtype=BATCH_TUNING_DTYPE)
-        t[0] = (k2_ctas_per_sm, k1_tile_rows, order, 0.0)
+        t[0] = (k2_ctas_per_sm, k1_tile_rows, order, k2_group, 0.0)
         InterStage._check(self.lib.ironav_batch_set_tuning(self.h, _ptr(t)), "ironav_batch_set_tuning")
 
     def autotune(self, d_src, d_ref, d_col, d_states, d_results, reps: int = 5, cache: str | None = None) -> dict:
@@ -772,18 +773,18 @@ class InterBatch:
                 table = json.load(f)
         if sig in table:
             b = table[sig]
-            self.set_tuning(b["k2_ctas_per_sm"], b["k1_tile_rows"], b["order"])
+            self.set_tuning(b["k2_ctas_per_sm"], b["k1_tile_rows"], b["order"], b.get("k2_group", 0))
             self.step(d_src, d_ref, d_col, d_states, d_results)
             self.sync()
             return {"best": b, "all": [], "cached": True}
         n = len(self.stages)
         mk = lambda xs: (_VP * n)(*[x if x is not None else None for x in xs])
         best = np.zeros(1, dtype=BATCH_TUNING_DTYPE)
-        allv = np.zeros(16, dtype=BATCH_TUNING_DTYPE)
+        allv = np.zeros(32, dtype=BATCH_TUNING_DTYPE)
         cnt = _I(0)
         InterStage._check(self.lib.ironav_batch_autotune(self.h, mk(d_src), mk(d_ref), mk(d_col), mk(d_states), mk(d_results), reps,
                                                          _ptr(best), _ptr(allv), len(allv), ctypes.byref(cnt)), "ironav_batch_autotune")
-        as_dict = lambda r: {k: r[k].item() for k in ("k2_ctas_per_sm", "k1_tile_rows", "order", "ms")}
+        as_dict = lambda r: {k: r[k].item() for k in ("k2_ctas_per_sm", "k1_tile_rows", "order", "k2_group", "ms")}
         out = {"best": as_dict(best[0]), "all": [as_dict(allv[i]) for i in range(cnt.value)], "cached": False}
         if cache:
             table[sig] = out["best"]

@@ -194,25 +194,25 @@ def test_every_tuning_gives_the_same_results_and_the_tuner_picks_one(cuda_lib, t
             assert np.array_equal(d_res[i].cpu().numpy().view(MBRESULT_DTYPE), want[i][1]), f"{what}: stream {i} results"
             d_res[i].zero_()
 
-    for k2 in (4, 5, 6):
+    for k2, group in ((4, 0), (5, 0), (6, 0), (4, 8)):
         for th in (16, 8):
             for order in (0, 1):
                 for st in stages:  # the step pushes the reference again: start from the ring as it was
                     st.clear_references()
                     st.push_reference_device(dev[stages.index(st)][0].data_ptr(), st.width, st.width, st.height, None)
                     st.begin_p_picture(27)
-                batch.set_tuning(k2, th, order)
-                assert batch.tuning() == {"k2_ctas_per_sm": k2, "k1_tile_rows": th, "order": order}
+                batch.set_tuning(k2, th, order, group)
+                assert batch.tuning() == {"k2_ctas_per_sm": k2, "k1_tile_rows": th, "order": order, "k2_group": group}
                 batch.step(*args)
                 batch.sync()
-                check(f"setting {k2}/{th}/{order}")
+                check(f"setting {k2}/{th}/{order}/{group}")
     for st, f in zip(stages, dev):
         st.clear_references()
         st.push_reference_device(f[0].data_ptr(), st.width, st.width, st.height, None)
         st.begin_p_picture(27)
     cache = str(tmp_path / "tuning.json")
     out = batch.autotune(*args, reps=3, cache=cache)
-    assert not out["cached"] and len(out["all"]) == 12 and out["best"]["ms"] > 0
+    assert not out["cached"] and len(out["all"]) == 16 and out["best"]["ms"] > 0
     assert min(a["ms"] for a in out["all"]) == out["best"]["ms"]
     check("after the tuner")
     assert all(st.lib.ironav_ctx_sync(st.ctx) == 0 for st in stages)
