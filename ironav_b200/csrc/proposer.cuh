@@ -111,43 +111,54 @@ __global__ void head_pack_kernel(const float* __restrict__ hw, float* __restrict
 }
 
 constexpr int HEAD_PIX = 128;  // interior pixels (of 2304) a CTA of head_fwd_packed_kernel sums over
+constexpr int HEAD_CHUNK = 16;  // pixels whose packed weights (32 KB) a CTA holds in shared memory at a time
 
 // The head with one thread per sample: CTA (x, y) takes samples 128x .. 128x + 127 and interior pixels
-// HEAD_PIX * y .. + HEAD_PIX - 1; a thread reads its sample's 32 channels of each pixel (four 16-byte loads)
-// and the features' packed weights, the same for every thread (broadcast loads), and adds its partial sums
-// to out (which CTAs y = 0 start from the bias; out must be zero before the launch).
+// HEAD_PIX * y .. + HEAD_PIX - 1. The CTA stages the packed weights of HEAD_CHUNK pixels at a time in shared
+// memory (coalesced); each thread then reads its sample's 32 channels of a pixel (four 16-byte loads) and the
+// weights from shared memory, the same address for every thread (broadcast), and adds its partial sums to out
+// (which CTAs y = 0 start from the bias; out must be zero before the launch).
 __global__ void __launch_bounds__(128) head_fwd_packed_kernel(const __nv_bfloat16* __restrict__ feat, long long Q, int n,
                                                               const float4* __restrict__ hwt, const float* __restrict__ hb,
                                                               float* __restrict__ out) {
+    __shared__ float4 ws[HEAD_CHUNK * 32 * 4];
     const int s = blockIdx.x * 128 + threadIdx.x;
     const int p0 = blockIdx.y * HEAD_PIX;
     float acc[16];
 #pragma unroll
     for (int j = 0; j < 16; j++) acc[j] = 0.f;
-    if (s < n) {
+    for (int c0 = p0; c0 < p0 + HEAD_PIX && c0 < 48 * 48; c0 += HEAD_CHUNK) {
+        const int np = min(HEAD_CHUNK, 48 * 48 - c0);
+        __syncthreads();
+        for (int i = threadIdx.x; i < np * 32 * 4; i += 128) ws[i] = __ldg(hwt + (size_t)c0 * 32 * 4 + i);
+        __syncthreads();
+        if (s < n) {
 #pragma unroll 2
-        for (int pix = p0; pix < p0 + HEAD_PIX && pix < 48 * 48; pix++) {
-            const int iy = pix / 48, ix = pix - iy * 48;
-            const long long q = (long long)s * tc::RPIX + (iy + 1) * tc::RW + (ix + 1);
+            for (int pp = 0; pp < np; pp++) {
+                const int pix = c0 + pp, iy = pix / 48, ix = pix - iy * 48;
+                const long long q = (long long)s * tc::RPIX + (iy + 1) * tc::RW + (ix + 1);
 #pragma unroll
-            for (int c = 0; c < 4; c++) {
-                const uint4 raw = *reinterpret_cast<const uint4*>(feat + ((size_t)c * Q + q) * 8);
-                const __nv_bfloat16* v = reinterpret_cast<const __nv_bfloat16*>(&raw);
+                for (int c = 0; c < 4; c++) {
+                    const uint4 raw = *reinterpret_cast<const uint4*>(feat + ((size_t)c * Q + q) * 8);
+                    const __nv_bfloat16* v = reinterpret_cast<const __nv_bfloat16*>(&raw);
 #pragma unroll
-                for (int e = 0; e < 8; e++) {
-                    const float x = __bfloat162float(v[e]);
-                    const float4* wf = hwt + ((size_t)(pix * 32 + c * 8 + e) << 2);
+                    for (int e = 0; e < 8; e++) {
+                        const float x = __bfloat162float(v[e]);
+                        const float4* wf = ws + ((pp * 32 + c * 8 + e) << 2);
 #pragma unroll
-                    for (int k = 0; k < 4; k++) {
-                        const float4 w4 = __ldg(wf + k);
-                        acc[4 * k] += x * w4.x;
-                        acc[4 * k + 1] += x * w4.y;
-                        acc[4 * k + 2] += x * w4.z;
-                        acc[4 * k + 3] += x * w4.w;
+                        for (int k = 0; k < 4; k++) {
+                            const float4 w4 = wf[k];
+                            acc[4 * k] += x * w4.x;
+                            acc[4 * k + 1] += x * w4.y;
+                            acc[4 * k + 2] += x * w4.z;
+                            acc[4 * k + 3] += x * w4.w;
+                        }
                     }
                 }
             }
         }
+    }
+    if (s < n) {
 #pragma unroll
         for (int j = 0; j < NOUT; j++) atomicAdd(&out[(size_t)s * NOUT + j], acc[j] + (blockIdx.y == 0 ? hb[j] : 0.f));
     }

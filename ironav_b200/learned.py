@@ -332,6 +332,40 @@ def conv_tflops(prop: Proposer, n: int, reps: int = 5) -> dict:
     return res
 
 
+def time_proposer(n: int, reps: int = 5) -> dict:
+    """The proposer's forward pass, untrained (seeded random weights), on the first n macroblocks of the 1080p
+    sequence's second picture against its first: CUDA-event times of the input, the four layers, the head and
+    the whole pass, per call."""
+    import torch
+
+    seq = Sequence.config("1080p", 2)
+    f0, f1 = (torch.from_numpy(seq.frame(t)).cuda() for t in range(2))
+    prop = Proposer(max_batch=n)
+    smp = picture_samples(f1.data_ptr(), f0.data_ptr(), 1920, 1080, 1920, 1920)[:n]
+    prop.set_samples(smp)
+    for _ in range(2):
+        prop.forward(n)
+    torch.cuda.synchronize()
+    out = conv_tflops(prop, n, reps=reps)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+    conv = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
+    ev[0].record(prop.stream)
+    for _ in range(reps):
+        prop.set_samples_device(prop.samples_d.data_ptr(), n)
+    ev[1].record(prop.stream)
+    for r in range(reps):
+        prop.forward(n, conv_events=conv[r])
+    ev[2].record(prop.stream)
+    ev[2].synchronize()
+    prop.check_errors()
+    out["input_ms"] = ev[0].elapsed_time(ev[1]) / reps
+    out["forward_ms"] = ev[1].elapsed_time(ev[2]) / reps
+    out["layers_ms"] = sum(a.elapsed_time(b) for a, b in conv) / reps
+    out["head_ms"] = out["forward_ms"] - out["layers_ms"]
+    out["samples"] = n
+    return out
+
+
 def main(argv=None) -> int:
     import argparse
     import json
@@ -352,7 +386,12 @@ def main(argv=None) -> int:
     ap.add_argument("--save", default=None, help="write the trained parameters (.npz)")
     ap.add_argument("--load", default=None, help="start from saved parameters (.npz) and skip training")
     ap.add_argument("--json", default=None, help="write the results as JSON")
+    ap.add_argument("--time-proposer", type=int, default=0, metavar="N",
+                    help="only time the untrained proposer's forward pass on N macroblocks of a 1080p picture, and exit")
     a = ap.parse_args(argv)
+    if a.time_proposer:
+        print(json.dumps(time_proposer(a.time_proposer)), flush=True)
+        return 0
     qps = tuple(int(q) for q in a.qps.split(","))
     log = lambda m: print(m, flush=True)  # noqa: E731
     out = {}
