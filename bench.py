@@ -60,8 +60,9 @@ def parse():
                    help="1080p: one stream, replay mode (the headline); batched: 64 mixed-resolution streams in auto "
                         "mode, one launch per stage and frame step, against the per-stream launch loop")
     p.add_argument("--streams", type=int, default=64, help="streams of the batched workload")
-    p.add_argument("--replay-form", type=int, default=0, choices=[0, 1, 2, 3],
-                   help="replay mode's kernel (ironav_set_replay_form): 0 8-lane groups, 1 one macroblock a warp, 2 16-lane groups")
+    p.add_argument("--replay-form", type=int, default=None, choices=[0, 1, 2, 3],
+                   help="replay mode's kernel (ironav_set_replay_form): 0 8-lane groups, 1 one macroblock a warp, 2 16-lane "
+                        "groups, 3 4-lane groups; default the library's choice for the depth (0 at 8 bits, 1 at 10)")
     p.add_argument("--learned-samples", type=int, default=2_000_000, help="training samples of the learned workload's proposer")
     p.add_argument("--e2e-threads", type=int, default=8, help="host threads (each with a context) of the e2e pass")
     p.add_argument("--bd", type=int, default=8, choices=[8, 10],
@@ -374,7 +375,8 @@ def main():
     stream = torch.cuda.Stream()
     st = InterStage(WIDTH, HEIGHT, nslices=NSLICES, lib=lib, bd=bd)
     st.set_stream(stream.cuda_stream)
-    st._check(lib.ironav_set_replay_form(st.ctx, args.replay_form), "ironav_set_replay_form")
+    if args.replay_form is not None:
+        st._check(lib.ironav_set_replay_form(st.ctx, args.replay_form), "ironav_set_replay_form")
     nmb = st.nmb
     d_frames = torch.from_numpy(frames.view(np.int16) if bd > 8 else frames).to(dev)
     d_states = torch.zeros((RING, nmb * 72), dtype=torch.uint8, device=dev)
@@ -463,7 +465,7 @@ def main():
         "config": config_dict(bd),
         "e2e": e2e,
         "gpu_launches": 3 * args.steps,  # per step: half-sample planes (+ co-located vectors), the source copied with its padding, analysis
-        "roofline": {"bound": "int32", "kernel": replay_kernel_name(args.replay_form, bd), "achieved": achieved, "peak": peak,
+        "roofline": {"bound": "int32", "kernel": replay_kernel_name(args.replay_form if args.replay_form is not None else (1 if bd > 8 else 0), bd), "achieved": achieved, "peak": peak,
                      "unit": "Tops/s", "frac": achieved / peak if peak else None,
                      # DRAM bytes per launch (dram__bytes_read.sum + write.sum) of one ncu capture of this
                      # workload at 8 bits (ncu --set full, one launch of a 6-picture ring): the source and the
@@ -1992,7 +1994,8 @@ def run_e2e(args, st, frames, d_states, nmb, world, torch, dist, dev, stream):
     workers = []
     for k in range(nthreads):
         ws = InterStage(WIDTH, HEIGHT, nslices=NSLICES, lib=lib, bd=args.bd)
-        ws._check(lib.ironav_set_replay_form(ws.ctx, args.replay_form), "ironav_set_replay_form")
+        if args.replay_form is not None:
+            ws._check(lib.ironav_set_replay_form(ws.ctx, args.replay_form), "ironav_set_replay_form")
         wstream = torch.cuda.Stream()
         ws.set_stream(wstream.cuda_stream)
         out = torch.zeros((nmb * 104,), dtype=torch.uint8).pin_memory()

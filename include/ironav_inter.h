@@ -579,10 +579,11 @@ int ironav_prop_weights(const float* d_w, int cin, void* d_wf, void* d_wt, void*
  * its softmax probability is at least min_conf, else 5 (unsure: the plain search). */
 int ironav_prop_propose(const float* d_out, int n, float min_conf, int16_t* d_cands, uint8_t* d_cls, void* stream);
 
-/* Replay mode's kernel (all give the same results): 0, the default, one macroblock per 8-lane group (four a
- * warp: the search's control runs once for four macroblocks); 1, one macroblock per warp (the form auto, in-loop
- * and decide modes use, where each macroblock's latency is on the wavefront's path); 2, one macroblock per
- * 16-lane group. The oracle accepts and ignores it. */
+/* Replay mode's kernel (all give the same results): 0, one macroblock per 8-lane group (four a warp: the
+ * search's control runs once for four macroblocks; the default at 8 bits); 1, one macroblock per warp (the
+ * default at 10 bits, where a row of samples is twice the words and 32 lanes share them better; the form auto,
+ * in-loop and decide modes use); 2, one macroblock per 16-lane group; 3, per 4-lane group. The oracle accepts
+ * and ignores it. */
 int ironav_set_replay_form(ironav_ctx* ctx, int form);
 
 /* The learned form's judge (no counterpart in the reference: the north star's form 4). With proposals set, the

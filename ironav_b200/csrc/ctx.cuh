@@ -14,7 +14,7 @@ struct ironav_ctx {
     int device = 0, nsm = 0, k2_blocks = 0;
     int g8_blocks = 0;     // the replay analysis' grid in its group forms (one macroblock per 8 / 16 lanes)
     int g16_blocks = 0, g4_blocks = 0;
-    int replay_form = 0;   // replay mode's kernel: 0 8-lane groups, 1 one macroblock per warp, 2 16-lane groups
+    int replay_form = 0;   // replay mode's kernel: 0 8-lane groups, 1 one macroblock per warp, 2 16-lane groups, 3 4-lane groups
     cudaStream_t stream = nullptr;
     long long psize = 0;
     uint8_t* d_src = nullptr;

@@ -350,6 +350,7 @@ int ironav_ctx_create(ironav_ctx** out, int width, int height, int bd, int max_r
     c->width = width;
     c->height = height;
     c->bd = bd;
+    c->replay_form = bd > 8 ? 1 : 0;  // the faster replay kernel at each depth (8-lane groups at 8 bits)
     c->mb_w = mb_w;
     c->mb_h = mb_h;
     c->pw = mb_w * 16;

@@ -169,7 +169,10 @@ def test_gpu_10bit_random_decisions_and_two_references(oracle_lib, cuda_lib):
     states["refs"] = np.where(states["inter"][:, None] == 1, rng.integers(0, 2, size=(nmb, 4)), -1)
     states["mvs"] = np.stack([rng.integers(-2048, 2048, size=(nmb, 16)), rng.integers(-512, 512, size=(nmb, 16))],
                              axis=-1)
-    assert_same(c.analyse_replay(states), o.analyse_replay(states), "10-bit replay on random decisions")
+    want = o.analyse_replay(states)
+    for form in (1, 0, 2):  # replay mode's kernels: the warp form (the 10-bit default), 8- and 16-lane groups
+        assert cuda_lib.ironav_set_replay_form(c.ctx, form) == 0
+        assert_same(c.analyse_replay(states), want, f"10-bit replay on random decisions, form {form}")
     so, ro = o.analyse_auto()
     sc, rc = c.analyse_auto()
     assert_same(sc, so, "10-bit two-reference decisions")
