@@ -244,58 +244,6 @@ __device__ __forceinline__ bool round_g(const AnalyseParams& __restrict__ P, con
     return moved;
 }
 
-// One diamond round for a partition at most 8 samples wide, in a single pass: lane l of the group scores the
-// whole of square point k = l < 4 ? l : l + 1 (the 3x3 square of the step around the centre, clamped), so no
-// shuffle reduction sits between the passes of a round; the reference's four moves (each from the current
-// best, both coordinates clamped) are then replayed against the square, a point the square lacks (a clamp-bent
-// move, or a centre outside the clamps) scored on its own. Same moves, costs and result as round_g.
-template <class T, int GW>
-__device__ __forceinline__ bool round_sq(const AnalyseParams& __restrict__ P, const Grp<GW>& g, const uint8_t* g0, const uint32_t* src, int w,
-                                         int h, int mvpx, int mvpy, int step, int cxlo, int cxhi, int cylo, int cyhi, int& bxv, int& byv,
-                                         int& bc) {
-    static_assert(GW == 8, "one lane a square point");
-    constexpr int B = sizeof(T);
-    const int lam = P.lambda, sw = P.sw;
-    auto clx = [&](int v) { return min(max(v, cxlo), cxhi); };
-    auto cly = [&](int v) { return min(max(v, cylo), cyhi); };
-    const int cx = bxv, cy = byv, c0 = bc;
-    const int X0 = clx(cx - step), X2 = clx(cx + step), Y0 = cly(cy - step), Y2 = cly(cy + step);
-    const int k = g.gl < 4 ? g.gl : g.gl + 1, kx = k % 3, ky = k / 3;
-    const int qx = kx == 0 ? X0 : (kx == 1 ? cx : X2), qy = ky == 0 ? Y0 : (ky == 1 ? cy : Y2);
-    int sq = 0;
-    {
-        const uint8_t* G = g0 + ((qy >> 2) * sw + (qx >> 2)) * B;
-        for (int row = 0; row < h; row++, G += sw * B) sq += row_sad<T>(G, src + row * 4 * B, w);
-        sq += lam * mvd_bits_d(qx, qy, mvpx, mvpy);
-    }
-    bool moved = false;
-#pragma unroll
-    for (int d = 0; d < 4; d++) {
-        int nx = clx(bxv), ny = cly(byv);
-        if (d == 0) nx = clx(bxv - step);
-        else if (d == 1) nx = clx(bxv + step);
-        else if (d == 2) ny = cly(byv - step);
-        else ny = cly(byv + step);
-        const int ix = nx == X0 ? 0 : (nx == cx ? 1 : (nx == X2 ? 2 : -1));
-        const int iy = ny == Y0 ? 0 : (ny == cy ? 1 : (ny == Y2 ? 2 : -1));
-        int v;
-        if (ix >= 0 && iy >= 0) {
-            const int kk = iy * 3 + ix;
-            const int o = __shfl_sync(g.mask, sq, kk < 4 ? kk : (kk == 4 ? 0 : kk - 1), GW);
-            v = kk == 4 ? c0 : o;
-        } else {
-            v = sad2<T, GW>(g, g0, src, sw, w, h, nx, ny, nx, ny).x + lam * mvd_bits_d(nx, ny, mvpx, mvpy);
-        }
-        if (v < bc) {
-            bxv = nx;
-            byv = ny;
-            bc = v;
-            moved = true;
-        }
-    }
-    return moved;
-}
-
 // motion_search, enc/frame.rs:949-1019 (list 0), for the partition at 4x4 block (bx, by) of w4 x h4 blocks:
 // the candidates (the predictor, zero, the macroblock's left, top and top-right neighbours on this reference,
 // then the extra vectors), the diamond, and the sub-sample refinement by SATD. Returns (cost without the
@@ -367,14 +315,7 @@ __device__ __noinline__ int3 msearch(const AnalyseParams& __restrict__ P, GroupS
         const int iters = step == 4 ? 32 : 4;
         for (int it = 0; it < iters; it++) {
             rounds++;
-            bool moved;
-            if constexpr (GW == 8) {
-                if (w <= 8) moved = round_sq<T, GW>(P, g, g0, src, w, h, mvpx, mvpy, step, cxlo, cxhi, cylo, cyhi, bxv, byv, bc);
-                else moved = round_g<T, GW>(P, g, g0, src, w, h, mvpx, mvpy, step, cxlo, cxhi, cylo, cyhi, bxv, byv, bc);
-            } else {
-                moved = round_g<T, GW>(P, g, g0, src, w, h, mvpx, mvpy, step, cxlo, cxhi, cylo, cyhi, bxv, byv, bc);
-            }
-            if (!moved) break;
+            if (!round_g<T, GW>(P, g, g0, src, w, h, mvpx, mvpy, step, cxlo, cxhi, cylo, cyhi, bxv, byv, bc)) break;
         }
     }
     M.sad_px += (uint32_t)(4 * w * h * rounds);
