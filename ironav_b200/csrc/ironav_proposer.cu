@@ -158,8 +158,8 @@ int ironav_prop_head_fwd_packed(const void* d_feat, int n, const float* d_hwt, c
     if (!d_feat || !d_hwt || !d_hb || !d_out || n < 1 || n > (1 << 22) || !aligned16(d_hwt)) return IRONAV_INVALID_ARGUMENT;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     CK(cudaMemsetAsync(d_out, 0, (size_t)n * prop::NOUT * sizeof(float), st));
-    const dim3 grid((n + 127) / 128, (48 * 48 + prop::HEAD_PIX - 1) / prop::HEAD_PIX);
-    prop::head_fwd_packed_kernel<<<grid, 128, 0, st>>>(static_cast<const __nv_bfloat16*>(d_feat), (long long)n * RPIX, n,
+    const dim3 grid((n + prop::HEAD_SAMPLES - 1) / prop::HEAD_SAMPLES, (48 * 48 + prop::HEAD_PIX - 1) / prop::HEAD_PIX);
+    prop::head_fwd_packed_kernel<<<grid, 256, 0, st>>>(static_cast<const __nv_bfloat16*>(d_feat), (long long)n * RPIX, n,
                                                        reinterpret_cast<const float4*>(d_hwt), d_hb, d_out);
     return cuda_status(cudaGetLastError());
 }

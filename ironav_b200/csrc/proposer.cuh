@@ -110,57 +110,82 @@ __global__ void head_pack_kernel(const float* __restrict__ hw, float* __restrict
     hwt[i] = j < NOUT ? hw[(size_t)j * NFEAT + f] : 0.f;
 }
 
-constexpr int HEAD_PIX = 128;  // interior pixels (of 2304) a CTA of head_fwd_packed_kernel sums over
-constexpr int HEAD_CHUNK = 16;  // pixels whose packed weights (32 KB) a CTA holds in shared memory at a time
+constexpr int HEAD_PIX = 128;   // interior pixels (of 2304) a CTA of head_fwd_packed_kernel sums over
+constexpr int HEAD_CHUNK = 16;  // pixels whose packed weights a CTA holds in shared memory at a time
+constexpr int HEAD_WPIX = 32 * 4 + 1;  // float4s a pixel's weights take in shared memory: 32 channels x 4, and a
+                                       // pad that puts a warp's four pixels on different banks
+constexpr int HEAD_SPL = 4;       // samples a lane
+constexpr int HEAD_SAMPLES = 256; // samples a CTA (8 warps of 8 x HEAD_SPL samples x 4 pixels)
 
-// The head with one thread per sample: CTA (x, y) takes samples 128x .. 128x + 127 and interior pixels
-// HEAD_PIX * y .. + HEAD_PIX - 1. The CTA stages the packed weights of HEAD_CHUNK pixels at a time in shared
-// memory (coalesced); each thread then reads its sample's 32 channels of a pixel (four 16-byte loads) and the
-// weights from shared memory, the same address for every thread (broadcast), and adds its partial sums to out
-// (which CTAs y = 0 start from the bias; out must be zero before the launch).
-__global__ void __launch_bounds__(128) head_fwd_packed_kernel(const __nv_bfloat16* __restrict__ feat, long long Q, int n,
+// The head: CTA (x, y) takes samples 256x .. 256x + 255 and interior pixels HEAD_PIX * y .. + HEAD_PIX - 1. Lane
+// l of warp w takes samples 256x + 32w + 4 (l / 4) + k (k < 4) and every fourth pixel from l % 4, so a warp's
+// feature loads are 64 contiguous bytes a sample (four pixels of one plane), and each weight read from shared
+// memory serves four samples. The CTA stages the packed weights of HEAD_CHUNK pixels at a time in shared memory
+// (coalesced); a warp reads four pixels' weights at once (four addresses on different banks). The four lanes of
+// a sample are summed by shuffles and added to out (which CTAs y = 0 start from the bias; out must be zero
+// before the launch).
+__global__ void __launch_bounds__(256) head_fwd_packed_kernel(const __nv_bfloat16* __restrict__ feat, long long Q, int n,
                                                               const float4* __restrict__ hwt, const float* __restrict__ hb,
                                                               float* __restrict__ out) {
-    __shared__ float4 ws[HEAD_CHUNK * 32 * 4];
-    const int s = blockIdx.x * 128 + threadIdx.x;
+    __shared__ float4 ws[HEAD_CHUNK * HEAD_WPIX];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, pl = lane & 3;
+    const int s0 = blockIdx.x * HEAD_SAMPLES + warp * 32 + (lane >> 2) * HEAD_SPL;
     const int p0 = blockIdx.y * HEAD_PIX;
-    float acc[16];
+    float acc[HEAD_SPL][16];
 #pragma unroll
-    for (int j = 0; j < 16; j++) acc[j] = 0.f;
+    for (int k = 0; k < HEAD_SPL; k++)
+#pragma unroll
+        for (int j = 0; j < 16; j++) acc[k][j] = 0.f;
     for (int c0 = p0; c0 < p0 + HEAD_PIX && c0 < 48 * 48; c0 += HEAD_CHUNK) {
-        const int np = min(HEAD_CHUNK, 48 * 48 - c0);
+        const int np = min(HEAD_CHUNK, 48 * 48 - c0);  // a multiple of 4: 2304 and the chunk are
         __syncthreads();
-        for (int i = threadIdx.x; i < np * 32 * 4; i += 128) ws[i] = __ldg(hwt + (size_t)c0 * 32 * 4 + i);
+        for (int i = threadIdx.x; i < np * 128; i += 256) ws[(i >> 7) * HEAD_WPIX + (i & 127)] = __ldg(hwt + (size_t)c0 * 128 + i);
         __syncthreads();
-        if (s < n) {
-#pragma unroll 2
-            for (int pp = 0; pp < np; pp++) {
-                const int pix = c0 + pp, iy = pix / 48, ix = pix - iy * 48;
-                const long long q = (long long)s * tc::RPIX + (iy + 1) * tc::RW + (ix + 1);
+        for (int pp = pl; pp < np; pp += 4) {
+            const int pix = c0 + pp, iy = pix / 48, ix = pix - iy * 48;
+            const int rq = (iy + 1) * tc::RW + (ix + 1);
+            const float4* wp = ws + pp * HEAD_WPIX;
+#pragma unroll 1
+            for (int c = 0; c < 4; c++) {
+                uint4 raw[HEAD_SPL];
 #pragma unroll
-                for (int c = 0; c < 4; c++) {
-                    const uint4 raw = *reinterpret_cast<const uint4*>(feat + ((size_t)c * Q + q) * 8);
-                    const __nv_bfloat16* v = reinterpret_cast<const __nv_bfloat16*>(&raw);
+                for (int k = 0; k < HEAD_SPL; k++) {
+                    const int s = s0 + k;
+                    raw[k] = s < n ? *reinterpret_cast<const uint4*>(feat + ((size_t)c * Q + (long long)s * tc::RPIX + rq) * 8)
+                                   : make_uint4(0, 0, 0, 0);
+                }
 #pragma unroll
-                    for (int e = 0; e < 8; e++) {
-                        const float x = __bfloat162float(v[e]);
-                        const float4* wf = ws + ((pp * 32 + c * 8 + e) << 2);
+                for (int e = 0; e < 8; e++) {
+                    const float4* wf = wp + ((c * 8 + e) << 2);
 #pragma unroll
-                        for (int k = 0; k < 4; k++) {
-                            const float4 w4 = wf[k];
-                            acc[4 * k] += x * w4.x;
-                            acc[4 * k + 1] += x * w4.y;
-                            acc[4 * k + 2] += x * w4.z;
-                            acc[4 * k + 3] += x * w4.w;
+                    for (int kk = 0; kk < 4; kk++) {
+                        const float4 w4 = wf[kk];
+#pragma unroll
+                        for (int k = 0; k < HEAD_SPL; k++) {
+                            const float x = __bfloat162float(reinterpret_cast<const __nv_bfloat16*>(&raw[k])[e]);
+                            acc[k][4 * kk] += x * w4.x;
+                            acc[k][4 * kk + 1] += x * w4.y;
+                            acc[k][4 * kk + 2] += x * w4.z;
+                            acc[k][4 * kk + 3] += x * w4.w;
                         }
                     }
                 }
             }
         }
     }
-    if (s < n) {
 #pragma unroll
-        for (int j = 0; j < NOUT; j++) atomicAdd(&out[(size_t)s * NOUT + j], acc[j] + (blockIdx.y == 0 ? hb[j] : 0.f));
+    for (int k = 0; k < HEAD_SPL; k++)
+#pragma unroll
+        for (int j = 0; j < NOUT; j++) {
+            acc[k][j] += __shfl_xor_sync(0xffffffffu, acc[k][j], 1);
+            acc[k][j] += __shfl_xor_sync(0xffffffffu, acc[k][j], 2);
+        }
+    if (pl == 0) {
+#pragma unroll
+        for (int k = 0; k < HEAD_SPL; k++)
+            if (s0 + k < n)
+#pragma unroll
+                for (int j = 0; j < NOUT; j++) atomicAdd(&out[(size_t)(s0 + k) * NOUT + j], acc[k][j] + (blockIdx.y == 0 ? hb[j] : 0.f));
     }
 }
 
