@@ -52,14 +52,15 @@ EncodeTiled encode_fn() {
 }
 
 // The tensor map of a chunk-major padded tensor (planes x Q pixels x 8 BF16) read in boxes of `box_pixels`
-// pixels of every plane: dims (8, Q, planes), byte strides (16, 16 Q). Out-of-range pixels read as zeros.
-int plane_map(CUtensorMap* map, const void* base, long long Q, int planes, int box_pixels) {
+// pixels of `box_planes` planes (0: every plane): dims (8, Q, planes), byte strides (16, 16 Q). Out-of-range
+// pixels read as zeros.
+int plane_map(CUtensorMap* map, const void* base, long long Q, int planes, int box_pixels, int box_planes = 0) {
     EncodeTiled enc = encode_fn();
     if (!enc) return IRONAV_HARDWARE_UNAVAILABLE;
     if (reinterpret_cast<uintptr_t>(base) & 15) return IRONAV_INVALID_ARGUMENT;
     const cuuint64_t dims[3] = {8, (cuuint64_t)Q, (cuuint64_t)planes};
     const cuuint64_t strides[2] = {16, (cuuint64_t)Q * 16};
-    const cuuint32_t box[3] = {8, (cuuint32_t)box_pixels, (cuuint32_t)planes};
+    const cuuint32_t box[3] = {8, (cuuint32_t)box_pixels, (cuuint32_t)(box_planes > 0 ? box_planes : planes)};
     const cuuint32_t estr[3] = {1, 1, 1};
     const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<void*>(base), dims, strides, box, estr,
                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
@@ -80,31 +81,34 @@ bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 
 
 extern "C" {
 
+// The convolution's tile: CONV_MT x 128 output pixels (conv3x3p_kernel's MT).
+constexpr int CONV_MT = 2;
+
 int ironav_prop_conv3x3(const void* d_x, int cin, long long samples, const void* d_w, const float* d_bias, int relu, const void* d_mask,
                         void* d_y, unsigned* d_err, void* stream) {
     if (!d_x || !d_w || !d_y || !d_err || (cin != 16 && cin != 32) || samples < 1 || samples > (1ll << 22)) return IRONAV_INVALID_ARGUMENT;
     if (!aligned16(d_y) || !aligned16(d_mask)) return IRONAV_INVALID_ARGUMENT;
     const long long Q = samples * RPIX;
-    const int tiles = (int)((Q + TILE - 1) / TILE);
+    const int tiles = (int)((Q + CONV_MT * TILE - 1) / (CONV_MT * TILE));
     CUtensorMap map;
-    int s = plane_map(&map, d_x, Q, cin / 8, HALO);
+    int s = plane_map(&map, d_x, Q, cin / 8, cp_box<CONV_MT>(), CONV_MT == 1 ? 0 : 1);
     if (s != IRONAV_OK) return s;
     int nsm = 0;
     if ((s = sm_count(&nsm)) != IRONAV_OK) return s;
-    // the pipelined form: two persistent CTAs an SM (78 KB of shared memory and 64 TMEM columns each)
+    // the pipelined form: two persistent CTAs an SM
     const int grid = std::min(tiles, nsm * 2);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const __nv_bfloat16* w = static_cast<const __nv_bfloat16*>(d_w);
     const __nv_bfloat16* mask = static_cast<const __nv_bfloat16*>(d_mask);
     __nv_bfloat16* y = static_cast<__nv_bfloat16*>(d_y);
     if (cin == 32) {
-        constexpr int bytes = conv3x3p_smem_bytes<32>();
-        CK(cudaFuncSetAttribute(conv3x3p_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-        conv3x3p_kernel<32><<<grid, CP_THREADS, bytes, st>>>(map, w, d_bias, relu, mask, y, Q, tiles, d_err);
+        constexpr int bytes = conv3x3p_smem_bytes<32, CONV_MT>();
+        CK(cudaFuncSetAttribute(conv3x3p_kernel<32, CONV_MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+        conv3x3p_kernel<32, CONV_MT><<<grid, CP_THREADS, bytes, st>>>(map, w, d_bias, relu, mask, y, Q, tiles, d_err);
     } else {
-        constexpr int bytes = conv3x3p_smem_bytes<16>();
-        CK(cudaFuncSetAttribute(conv3x3p_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-        conv3x3p_kernel<16><<<grid, CP_THREADS, bytes, st>>>(map, w, d_bias, relu, mask, y, Q, tiles, d_err);
+        constexpr int bytes = conv3x3p_smem_bytes<16, CONV_MT>();
+        CK(cudaFuncSetAttribute(conv3x3p_kernel<16, CONV_MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+        conv3x3p_kernel<16, CONV_MT><<<grid, CP_THREADS, bytes, st>>>(map, w, d_bias, relu, mask, y, Q, tiles, d_err);
     }
     return cuda_status(cudaGetLastError());
 }

@@ -244,9 +244,21 @@ __global__ void __launch_bounds__(128, 1) wgrad3x3_kernel(const __grid_constant_
 constexpr int CP_STAGES = 4;
 constexpr int CP_THREADS = 192;
 
-template <int CIN>
+// A tile of MT x 128 output pixels: MT MMAs of M = 128 a tap and K chunk. The halo it stages (51 pixels each
+// side): 232 pixels for MT = 1, loaded as one box of every plane; 368 for MT = 2, each plane as two boxes of 184
+// (the box limit is 256 pixels, and every box must land on a 128-byte boundary: 8 pixels). Stages: as many as
+// keep two CTAs an SM (4 of 15 KB, or 3 of 23 KB, at CIN 32).
+template <int MT>
+__host__ __device__ constexpr int cp_halo() { return MT == 1 ? 232 : 368; }
+template <int MT>
+__host__ __device__ constexpr int cp_box() { return MT == 1 ? cp_halo<MT>() : cp_halo<MT>() / 2; }
+template <int MT>
+__host__ __device__ constexpr int cp_stages() { return MT == 1 ? 4 : 3; }
+static_assert(cp_halo<1>() >= TILE + 2 * HALO_LO && cp_halo<2>() >= 2 * TILE + 2 * HALO_LO, "the halo covers every tap's rows");
+
+template <int CIN, int MT = 1>
 constexpr int conv3x3p_smem_bytes() {
-    return 9 * (CIN / 8) * COUT * 16 + CP_STAGES * (CIN / 8) * HALO * 16 + (2 * CP_STAGES + 4) * 8 + 16;
+    return 9 * (CIN / 8) * COUT * 16 + cp_stages<MT>() * (CIN / 8) * cp_halo<MT>() * 16 + (2 * cp_stages<MT>() + 4) * 8 + 16;
 }
 
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
@@ -256,17 +268,22 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
 // One 3x3 convolution layer (CIN input channels, 32 output channels) over the chunk-major padded rasters:
 // y = act(conv(x, w) + bias), act = ReLU (relu != 0) or the identity, then times (mask > 0) when `mask` is set
 // (the gradient through the layer's ReLU); the ring pixels of y are zero. w is [9 taps][32 out][CIN in] BF16,
-// tap = 3 * dy + dx. x is read through `map` (planes CIN / 8, Q pixels, 8 channels). tiles = ceil(Q / 128).
-template <int CIN>
+// tap = 3 * dy + dx. x is read through `map` (planes CIN / 8, Q pixels, 8 channels; boxes of cp_box<MT>() pixels of
+// every plane (MT = 1) or of one plane (MT = 2)). tiles = ceil(Q / (MT x 128)).
+template <int CIN, int MT = 1>
 __global__ void __launch_bounds__(CP_THREADS, 1) conv3x3p_kernel(const __grid_constant__ CUtensorMap map, const __nv_bfloat16* __restrict__ w,
                                                                  const float* __restrict__ bias, int relu, const __nv_bfloat16* __restrict__ mask,
                                                                  __nv_bfloat16* __restrict__ y, long long Q, int tiles, unsigned* err) {
     constexpr int KC = CIN / 8;
+    constexpr int CP_STAGES = cp_stages<MT>();  // this form's ring of stages
     constexpr int WBYTES = 9 * KC * COUT * 16;
-    constexpr int HBYTES = KC * HALO * 16;
+    constexpr int HP = cp_halo<MT>();                          // halo pixels a stage
+    constexpr int HBYTES = KC * HP * 16;
+    constexpr int TP = MT * TILE;                              // output pixels a tile
+    constexpr int ACOLS = MT * COUT;                           // TMEM columns an accumulator
     extern __shared__ __align__(1024) uint8_t smem[];
     uint8_t* ws = smem;                                        // weights: [tap][chunk][out][16 B]
-    uint8_t* halos = smem + WBYTES;                            // CP_STAGES x [chunk][HALO pixels][16 B]
+    uint8_t* halos = smem + WBYTES;                            // CP_STAGES x [chunk][HP pixels][16 B]
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + WBYTES + CP_STAGES * HBYTES);  // [CP_STAGES]
     uint64_t* empty = full + CP_STAGES;                        // [CP_STAGES]
     uint64_t* accf = empty + CP_STAGES;                        // [2] accumulator written
@@ -294,7 +311,7 @@ __global__ void __launch_bounds__(CP_THREADS, 1) conv3x3p_kernel(const __grid_co
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     if (warp == 5) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 64;" ::"r"(smem_u32(tmem_slot)));
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)), "r"(2 * ACOLS));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     tc_fence_before();
@@ -313,9 +330,18 @@ __global__ void __launch_bounds__(CP_THREADS, 1) conv3x3p_kernel(const __grid_co
                     break;
                 }
                 if (*failed) break;
-                const long long q0 = ((long long)blockIdx.x + (long long)it * gridDim.x) * TILE;
+                const long long q0 = ((long long)blockIdx.x + (long long)it * gridDim.x) * TP;
                 mbar_expect_tx(&full[s], HBYTES);
-                tma_load_3d(halos + s * HBYTES, &map, 0, (int)(q0 - HALO_LO), 0, &full[s]);
+                if constexpr (MT == 1) {
+                    tma_load_3d(halos + s * HBYTES, &map, 0, (int)(q0 - HALO_LO), 0, &full[s]);
+                } else {
+#pragma unroll
+                    for (int c = 0; c < KC; c++)
+#pragma unroll
+                        for (int m = 0; m < 2; m++)
+                            tma_load_3d(halos + s * HBYTES + (c * HP + m * (HP / 2)) * 16, &map, 0, (int)(q0 - HALO_LO) + m * (HP / 2), c,
+                                        &full[s]);
+                }
                 loaded = it + 1;
             }
             s_loaded = loaded;
@@ -336,15 +362,18 @@ __global__ void __launch_bounds__(CP_THREADS, 1) conv3x3p_kernel(const __grid_co
                 }
                 if (*failed) break;
                 tc_fence_after();
-                const uint32_t h = smem_u32(halos + s * HBYTES), wb = smem_u32(ws), d = tmem + (uint32_t)(a * COUT);
+                const uint32_t h = smem_u32(halos + s * HBYTES), wb = smem_u32(ws), d = tmem + (uint32_t)(a * ACOLS);
 #pragma unroll 1
                 for (int t = 0; t < 9; t++) {
                     const int shift = (t / 3 - 1) * RW + (t % 3 - 1);
 #pragma unroll
                     for (int kk = 0; kk < KC / 2; kk++) {
-                        const uint64_t ad = smem_desc(h + (uint32_t)((2 * kk * HALO + HALO_LO + shift) * 16), HALO * 16, 8 * 16);
                         const uint64_t bd = smem_desc(wb + (uint32_t)((t * KC + 2 * kk) * COUT * 16), COUT * 16, 8 * 16);
-                        mma_bf16(d, ad, bd, IDESC_BF16_M128_N32, (t | kk) != 0);
+#pragma unroll
+                        for (int mh = 0; mh < MT; mh++) {
+                            const uint64_t ad = smem_desc(h + (uint32_t)((2 * kk * HP + HALO_LO + shift + mh * TILE) * 16), HP * 16, 8 * 16);
+                            mma_bf16(d + (uint32_t)(mh * COUT), ad, bd, IDESC_BF16_M128_N32, (t | kk) != 0);
+                        }
                     }
                 }
                 mma_commit(&empty[s]);
@@ -368,32 +397,38 @@ __global__ void __launch_bounds__(CP_THREADS, 1) conv3x3p_kernel(const __grid_co
                 break;
             }
             tc_fence_after();
-            float v[32];
-            tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(a * COUT), v);
+            float vv[MT][32];
+#pragma unroll
+            for (int mh = 0; mh < MT; mh++) tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(a * ACOLS + mh * COUT), vv[mh]);
             tc_fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive(&acce[a]);
-            const long long q0 = ((long long)blockIdx.x + (long long)it * gridDim.x) * TILE;
-            const long long q = q0 + warp * 32 + lane;
-            if (q < Q) {
-                int p = (int)(q0 % RPIX) + warp * 32 + lane;
-                if (p >= RPIX) p -= RPIX;
-                const int ry = p / RW, rx = p - ry * RW;
-                const bool ring = ry == 0 || ry == RW - 1 || rx == 0 || rx == RW - 1;
+            const long long q0 = ((long long)blockIdx.x + (long long)it * gridDim.x) * TP;
+            const int r0 = (int)(q0 % RPIX);
 #pragma unroll
-                for (int c = 0; c < 4; c++) {
-                    uint4 m4 = make_uint4(0, 0, 0, 0);
-                    if (mask != nullptr) m4 = *reinterpret_cast<const uint4*>(mask + ((size_t)c * Q + q) * 8);
-                    const __nv_bfloat16* mk = reinterpret_cast<const __nv_bfloat16*>(&m4);
-                    __align__(16) __nv_bfloat16 o[8];
+            for (int mh = 0; mh < MT; mh++) {
+                const float (&v)[32] = vv[mh];
+                const long long q = q0 + mh * TILE + warp * 32 + lane;
+                if (q < Q) {
+                    int p = r0 + mh * TILE + warp * 32 + lane;
+                    if (p >= RPIX) p -= RPIX;
+                    const int ry = p / RW, rx = p - ry * RW;
+                    const bool ring = ry == 0 || ry == RW - 1 || rx == 0 || rx == RW - 1;
 #pragma unroll
-                    for (int e = 0; e < 8; e++) {
-                        float f = v[c * 8 + e] + bv[c * 8 + e];
-                        if (relu) f = fmaxf(f, 0.f);
-                        if (mask != nullptr && !(__bfloat162float(mk[e]) > 0.f)) f = 0.f;
-                        o[e] = __float2bfloat16_rn(ring ? 0.f : f);
+                    for (int c = 0; c < 4; c++) {
+                        uint4 m4 = make_uint4(0, 0, 0, 0);
+                        if (mask != nullptr) m4 = *reinterpret_cast<const uint4*>(mask + ((size_t)c * Q + q) * 8);
+                        const __nv_bfloat16* mk = reinterpret_cast<const __nv_bfloat16*>(&m4);
+                        __align__(16) __nv_bfloat16 o[8];
+#pragma unroll
+                        for (int e = 0; e < 8; e++) {
+                            float f = v[c * 8 + e] + bv[c * 8 + e];
+                            if (relu) f = fmaxf(f, 0.f);
+                            if (mask != nullptr && !(__bfloat162float(mk[e]) > 0.f)) f = 0.f;
+                            o[e] = __float2bfloat16_rn(ring ? 0.f : f);
+                        }
+                        *reinterpret_cast<uint4*>(y + ((size_t)c * Q + q) * 8) = *reinterpret_cast<const uint4*>(o);
                     }
-                    *reinterpret_cast<uint4*>(y + ((size_t)c * Q + q) * 8) = *reinterpret_cast<const uint4*>(o);
                 }
             }
             if (__any_sync(0xffffffffu, *failed != 0)) break;
@@ -411,7 +446,7 @@ __global__ void __launch_bounds__(CP_THREADS, 1) conv3x3p_kernel(const __grid_co
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    if (warp == 5) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 64;" ::"r"(tmem));
+    if (warp == 5) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * ACOLS));
 }
 
 }  // namespace tc
