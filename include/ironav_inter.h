@@ -290,15 +290,18 @@ int ironav_code_inter_picture_device(ironav_ctx* ctx, int qp, const ironav_inter
  * threshold, active references, fast, sub8x8); the source and every active reference need their chroma.
  * The code of one macroblock (MbCode, 275-300): */
 typedef struct ironav_mbcode {
-    ironav_intercode res;  /* levels: luma (4x4 blocks; Intra16x16: AC, scan position 0 unused), cdc, cac,
-                              nnz, cnnz, cbp (luma bits 0-3, chroma 4-5); luma8 and t8x8 are zero (the
-                              CAVLC encoder codes no 8x8 transform) */
+    ironav_intercode res;  /* levels: luma (4x4 blocks; Intra16x16: AC, scan position 0 unused), luma8 and
+                              t8x8 (the 8x8 transform: Intra8x8, and inter macroblocks under CABAC with
+                              transform8; CAVLC codes none), cdc, cac, nnz, cnnz, cbp (luma bits 0-3,
+                              chroma 4-5) */
     int16_t dc[16];        /* Intra16x16 luma DC levels, zigzag order */
     int16_t mvs[16][2];    /* inter: a vector per partition in coding order (rects(part, sub)); P_Skip and
                               16x16: the vector in all 16 */
     int16_t mvds[16][2];   /* inter, not skipped: each vector less its predictor (part_mvps) */
-    uint8_t modes[16];     /* Intra4x4 prediction modes, raster 4x4 order (2 elsewhere) */
-    uint8_t kind;          /* the reference's Kind: 1 Intra4x4, 3 Intra16x16, 5 inter */
+    uint8_t modes[16];     /* Intra4x4 prediction modes, raster 4x4 order (Intra8x8: each 8x8 block's mode in
+                              its four 4x4 blocks; 2 elsewhere) */
+    uint8_t kind;          /* the reference's Kind: 1 Intra4x4, 2 Intra8x8 (CABAC with the 8x8 transform),
+                              3 Intra16x16, 5 inter */
     uint8_t skip;          /* P_Skip */
     uint8_t i16_mode;      /* Intra16x16 prediction mode */
     uint8_t chroma_mode;   /* intra chroma prediction mode */
@@ -318,6 +321,21 @@ int ironav_decide_p_picture(ironav_ctx* ctx, ironav_mbstate* states, ironav_mbco
  * ironav_deblock_picture_device; states and codes 4-byte aligned). */
 int ironav_decide_p_picture_device(ironav_ctx* ctx, ironav_mbstate* d_states, ironav_mbcode* d_codes, void* d_rec_y, int y_stride,
                                    void* d_rec_cb, void* d_rec_cr, int c_stride);
+
+/* ---- High profile: CABAC with rate-distortion decisions ------------------------------------------- */
+
+/* The entropy coding that decide mode and the slice writer follow (H264Encoder's cabac and transform8,
+ * enc/mod.rs:136-283: the default encoder and low_latency code CABAC with the 8x8 transform,
+ * constrained_baseline codes CAVLC). cabac = 0: CAVLC, a new context's setting; 1: CABAC. transform8
+ * (CABAC only, else ignored) = transform_8x8_mode_flag. Under CABAC the decisions are FrameCoder's
+ * decide_rd (enc/frame.rs:1462-1513): after code_mb's P_Skip tests (715-751), P_Skip, best_inter's
+ * partitioning (4x4 transform, and with transform8 the 8x8 transform when no 8x8 block is split),
+ * Intra16x16 in its best mode, Intra4x4 and (transform8) Intra8x8 (code_i8, 1307-1388), each with intra
+ * chroma, are coded and the one of least SSD + lambda2 * bits is kept, lambda2 = 1.6 * 2^((QP'Y - 12) / 3)
+ * and the bits those of CABAC (CabacCost, enc/cabac.rs:150-192) from the slice's contexts after the
+ * macroblocks before it. Each slice band is then one chain in raster order: a macroblock's cost depends on
+ * every earlier one's bins. The slices are written by ironav_write_slices with the same contexts. */
+int ironav_set_entropy(ironav_ctx* ctx, int cabac, int transform8);
 
 /* ---- intra (IDR) pictures in decide mode ------------------------------------------------------------ */
 
@@ -339,17 +357,20 @@ int ironav_decide_i_picture_device(ironav_ctx* ctx, ironav_mbstate* d_states, ir
 int ironav_set_source_chroma_device(ironav_ctx* ctx, const void* d_cb, const void* d_cr, int stride);
 int ironav_push_reference_chroma_device(ironav_ctx* ctx, const void* d_cb, const void* d_cr, int stride, int w, int h);
 
-/* ---- the bitstream (CAVLC, Annex B) ------------------------------------------------------------------ */
+/* ---- the bitstream (Annex B) ------------------------------------------------------------------------ */
 
-/* What the sequence and picture parameter sets say (H264Encoder::sps / pps, enc/mod.rs:296-400, for the
- * CAVLC encoder: Constrained Baseline at 8 bits, High 10 with CAVLC at 10 bits; no B pictures, picture
- * order type 2, one slice group, no weighted prediction, deblocking not signalled). */
+/* What the sequence and picture parameter sets say (H264Encoder::sps / pps, enc/mod.rs:296-400, without B
+ * pictures: Constrained Baseline (CAVLC at 8 bits), Main (CABAC without the 8x8 transform), High (CABAC
+ * with it) or High 10 (10 bits); picture order type 2, one slice group, no weighted prediction,
+ * deblocking not signalled). */
 typedef struct ironav_stream_params {
     int32_t width, height;       /* the picture size; the SPS crops the macroblock-aligned size to it */
     int32_t bd;                  /* 8 or 10 */
     int32_t fps_num, fps_den;    /* frame rate: the level (Table A-1, enc/mod.rs:154-157) and the VUI timing;
                                     0, 0: 25 fps for the level, no timing */
     int32_t refs;                /* max_num_ref_frames: reference pictures the stream keeps (1..16) */
+    int32_t cabac;               /* entropy_coding_mode_flag (0 CAVLC, 1 CABAC) */
+    int32_t transform8;          /* transform_8x8_mode_flag (with CABAC only) */
 } ironav_stream_params;
 
 /* The SPS and PPS NAL units (Annex B: 4-byte start codes, emulation prevention, put_nal enc/bitw.rs:91-103)
@@ -361,7 +382,10 @@ int ironav_write_parameter_sets(const ironav_stream_params* p, uint8_t* out, siz
  * (ironav_decide_i_picture / ironav_decide_p_picture outputs, mb_w*mb_h): the slice header (enc/mod.rs:566-600),
  * each macroblock's CAVLC syntax (write_mb, enc/frame.rs:1922-2016: mb_skip_run, mb_type, prediction modes,
  * sub_mb_type, ref_idx, mvd, coded_block_pattern, mb_qp_delta, residual blocks by enc/cavlc.rs:47-122) and
- * the slice's trailing bits (enc/frame.rs:480-486). idr: the picture is the IDR picture (slice type I, NAL
+ * the slice's trailing bits (enc/frame.rs:480-486); under CABAC (ironav_set_entropy) cabac_init_idc 0 in
+ * the header, cabac_alignment_one_bit, and each macroblock's bins (write_mb_cabac / mb_bins,
+ * enc/frame.rs:2020-2279, residual blocks by enc/cabac.rs:194-250) arithmetic coded (CabacWriter,
+ * enc/cabac.rs:42-147) with end_of_slice_flag after each. idr: the picture is the IDR picture (slice type I, NAL
  * type 5, idr_pic_id) set up by ironav_begin_i_picture, else a P picture set up by ironav_begin_p_picture
  * (its active references give num_ref_idx_active and ref_idx's range); frame_num and idr_pic_id as the
  * encoder counts them (enc/mod.rs:541-545,667-668). Writes *len bytes of Annex B to out; IRONAV_INVALID_ARGUMENT

@@ -28,7 +28,7 @@ NVCC_FLAGS = [
     "-lineinfo", "-O3", "-std=c++17",
     "-Xcompiler", "-fPIC,-O3",
 ]
-UNITS = ["ironav_inter.cu", "ironav_batch.cu", "ironav_noalloc.cu", "ironav_stream.cu", "ironav_proposer.cu"]
+UNITS = ["ironav_inter.cu", "ironav_batch.cu", "ironav_noalloc.cu", "ironav_stream.cu", "ironav_proposer.cu", "ironav_cabac.cu"]
 
 
 def _nvcc() -> str:

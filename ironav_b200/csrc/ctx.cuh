@@ -2,6 +2,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <vector>
+
 #include "common.cuh"
 
 using ironav::ColMv;
@@ -94,9 +96,28 @@ struct ironav_ctx {
     uint32_t* h_cavlc = nullptr;
     uint8_t* h_rbsp = nullptr;
     size_t h_rbsp_cap = 0;
+    // CABAC (ironav_set_entropy): the setting; the contexts' step table; the slice bands' rows on the device;
+    // the rate-distortion decision's per-band scratch (candidate codes and reconstructions); the writer's
+    // per-band data regions, byte counts (and overflow word) and their pinned host copy
+    int cabac = 0, t8 = 0;
+    uint32_t* d_cab_step = nullptr;
+    int* d_band_rows = nullptr;
+    ironav_mbcode* d_rd_cand = nullptr;
+    uint8_t* d_rd_rec = nullptr;
+    uint32_t* d_cab_out = nullptr;
+    unsigned long long cab_region_words = 0;
+    uint32_t* d_cab_bytes = nullptr;
+    uint32_t* h_cab_bytes = nullptr;
 };
 
 
 // Helpers the translation units share (ironav_inter.cu).
 int take_ref_slot(ironav_ctx* c);
 void fill_params(const ironav_ctx* c, ironav::AnalyseParams& p);
+// CABAC (ironav_cabac.cu): the step table and band rows on first use; decide mode under CABAC (the
+// rate-distortion decision, one chain per slice band) on the device buffers given; the CABAC data of the
+// current picture's slices from codes in device memory, one host vector of bytes per slice (each begins on
+// the byte after its header's cabac_alignment_one_bit).
+int cabac_setup(ironav_ctx* c);
+int launch_decide_rd(ironav_ctx* c, ironav_mbstate* d_states, ironav_mbcode* d_codes, void* y, int ys, void* cb, void* cr, int cs);
+int cabac_slice_data(ironav_ctx* c, int idr, const ironav_mbcode* d_codes, std::vector<std::vector<uint8_t>>* slices);

@@ -27,7 +27,7 @@ struct DecideParams {
 
 constexpr int K7_WARPS = 4;
 constexpr int K7_MIN_BLOCKS = 2;  // the wavefront keeps few macroblocks in flight: registers (255, no spills) over occupancy
-constexpr int KIND_I4 = 1, KIND_I16 = 3, KIND_INTER = 5;  // Kind, h264/mb.rs:21-30
+constexpr int KIND_I4 = 1, KIND_I8 = 2, KIND_I16 = 3, KIND_INTER = 5;  // Kind, h264/mb.rs:21-30
 
 template <class T>
 struct DecideSmem {
@@ -235,7 +235,8 @@ __device__ void load_intra_neighbours(const DecideParams& P, DecideSmem<T>& S, i
         int m = -1;
         if (ok) {
             const ironav_mbcode* n = &P.codes[left ? mb - 1 : mb - C.A.mb_w];
-            m = n->kind == KIND_I4 ? (int)n->modes[left ? lane * 4 + 3 : 12 + (lane - 4)] : 2;
+            // Intra8x8 macroblocks (CABAC with the 8x8 transform) give their modes too (MbState::i4, 2309)
+            m = (n->kind == KIND_I4 || n->kind == KIND_I8) ? (int)n->modes[left ? lane * 4 + 3 : 12 + (lane - 4)] : 2;
         }
         S.nbm[lane] = m;
     }
@@ -684,30 +685,18 @@ __device__ void pair_helper(const DecideParams& P, DecideSmem<T>& S, PairSync& X
     }
 }
 
-// code_mb for one macroblock without CABAC, enc/frame.rs:715-790: of a P picture, or of an IDR picture
-// (P.intra: no P_Skip tests and no best_inter; the Intra4x4 trial always runs, but for flat macroblocks in
-// live coding, 762-765). X: the warp pair's meeting words, when the macroblock's intra side runs on the
-// pair's second warp (PAIR).
-template <class T, bool PAIR = false>
-__device__ void decide_mb(const DecideParams& P, DecideSmem<T>& S, const unsigned* i4tab, int mb, int mbx, int mby, PairSync* X = nullptr) {
+// code_mb's P_Skip tests, enc/frame.rs:722-751: the fast one on the luma and chroma SADs (live coding), then
+// code_inter with the skip vector when its SAD is under the threshold. Returns true (every lane) when the
+// macroblock is P_Skip, its code, state and reconstruction written; else false with the skip vector in *sv_out
+// and S.c.dec holding the skip vector's 16x16 decision (mode 2, the 4x4 transform).
+template <class T>
+__device__ bool skip_tests_d(const DecideParams& P, DecideSmem<T>& S, int mb, int mbx, int mby, ironav_mbcode* out, int2* sv_out) {
     const int lane = threadIdx.x & 31;
     const AnalyseParams& A = P.C.A;
     const CodeParams& C = P.C;
-    const int lam = A.lambda, x0 = mbx * 16, y0 = mby * 16;
-    const bool ta = mby > A.band_start[mby], la = mbx > 0, tra = ta && mbx + 1 < A.mb_w;
-    ironav_mbcode* out = &P.codes[mb];
-    // the code starts as MbCode::new: zero, Intra4x4 modes 2
-    {
-        uint32_t* w = reinterpret_cast<uint32_t*>(out);
-        for (int k = lane; k < (int)(sizeof(ironav_mbcode) / 4); k += 32) w[k] = (k >= 371 && k < 375) ? 0x02020202u : 0u;
-    }
-    stage_source(A, S.a);
-    __syncwarp();
     ironav_interdec& D = *reinterpret_cast<ironav_interdec*>(S.c.dec);
-    int2 sv = make_int2(0, 0);
-    if (!P.intra) {
     // P_Skip first (722-751)
-    sv = skip_mv(A, S.a);
+    const int2 sv = skip_mv(A, S.a);
     if (lane == 0) S.a.cand[0] = sv;
     __syncwarp();
     pred_batch(A, S.a, 0, 0, 0, 2, 2, 1, true);
@@ -755,7 +744,7 @@ __device__ void decide_mb(const DecideParams& P, DecideSmem<T>& S, const unsigne
             D.mode = 2;
             inter_tail(P, S, D, out);
             if (lane < 16) out->mvds[lane][0] = out->mvds[lane][1] = 0;  // a P_Skip code carries no differences
-            return;
+            return true;
         }
         if (lane == 0) D.mode = 2;
         __syncwarp();
@@ -765,10 +754,35 @@ __device__ void decide_mb(const DecideParams& P, DecideSmem<T>& S, const unsigne
         if (cbp == 0) {
             inter_tail(P, S, D, out);
             if (lane == 0) out->skip = 1;
-            return;
+            return true;
         }
     }
-    }  // !P.intra
+    *sv_out = sv;
+    return false;
+}
+
+// code_mb for one macroblock without CABAC, enc/frame.rs:715-790: of a P picture, or of an IDR picture
+// (P.intra: no P_Skip tests and no best_inter; the Intra4x4 trial always runs, but for flat macroblocks in
+// live coding, 762-765). X: the warp pair's meeting words, when the macroblock's intra side runs on the
+// pair's second warp (PAIR).
+template <class T, bool PAIR = false>
+__device__ void decide_mb(const DecideParams& P, DecideSmem<T>& S, const unsigned* i4tab, int mb, int mbx, int mby, PairSync* X = nullptr) {
+    const int lane = threadIdx.x & 31;
+    const AnalyseParams& A = P.C.A;
+    const CodeParams& C = P.C;
+    const int lam = A.lambda, x0 = mbx * 16, y0 = mby * 16;
+    const bool ta = mby > A.band_start[mby], la = mbx > 0, tra = ta && mbx + 1 < A.mb_w;
+    ironav_mbcode* out = &P.codes[mb];
+    // the code starts as MbCode::new: zero, Intra4x4 modes 2
+    {
+        uint32_t* w = reinterpret_cast<uint32_t*>(out);
+        for (int k = lane; k < (int)(sizeof(ironav_mbcode) / 4); k += 32) w[k] = (k >= 371 && k < 375) ? 0x02020202u : 0u;
+    }
+    stage_source(A, S.a);
+    __syncwarp();
+    ironav_interdec& D = *reinterpret_cast<ironav_interdec*>(S.c.dec);
+    int2 sv = make_int2(0, 0);
+    if (!P.intra && skip_tests_d<T>(P, S, mb, mbx, mby, out, &sv)) return;
     load_intra_neighbours(P, S, mb, mbx, mby, ta, la, tra);
     int2 i16 = make_int2(2, 0);
     int seq = 0;

@@ -1,0 +1,655 @@
+// decide_rd.cuh — K9: code_mb with CABAC on the device (the reference encoder's default decision: decide_rd,
+// enc/frame.rs:1462-1513, after code_mb's P_Skip tests, best_i16 and best_inter, 715-760), and the CABAC
+// slice writer.
+//
+// Under CABAC a macroblock's rate-distortion cost counts its bins against the slice's contexts as the
+// macroblocks before it left them, so a slice band is one chain in raster order: a warp walks a band (one
+// CTA a band, the bands side by side). For each macroblock the warp codes every candidate the reference
+// tries, in its order (P_Skip, best_inter's partitioning with the 4x4 and, with transform8, the 8x8
+// transform, Intra16x16, Intra4x4, Intra8x8, each intra one with its chroma), each into the picture and
+// then into the chain's scratch (code and reconstruction), with its squared error; then lanes 0-5 count
+// the candidates' bins at once, each on its own copy of the contexts (the counter of cabac.cuh); lane 0
+// keeps the least SSD + lambda2 * bits in the reference's order (strict '<'), and the warp copies the
+// kept candidate's code, reconstruction and advanced contexts into place.
+//
+// The candidates reuse decide mode's warp-level coders (decide.cuh, residual.cuh); Intra8x8 (code_i8,
+// enc/frame.rs:1307-1388) is coded here: block by block, its edges filtered (8.3.2.2.1), nine modes'
+// SATD over 36 lane-units of (mode, 4x4 quadrant), the chosen block's 8x8 transform on eight lanes.
+#pragma once
+#include "cabac.cuh"
+#include "decide.cuh"
+
+namespace ironav {
+
+constexpr int RD_CANDS = 6;  // P_Skip, inter with the 4x4 transform, inter with the 8x8, Intra16x16, Intra4x4, Intra8x8
+
+struct RdParams {
+    DecideParams D;         // decide mode's parameters: the analysis, the coder, the outputs (codes, states)
+    ironav_mbcode* cand;    // the chains' scratch: RD_CANDS codes a chain
+    uint8_t* cand_rec;      // RD_CANDS reconstructions a chain, 384 samples each (luma, Cb, Cr)
+    const int* band_rows;   // chain i walks the rows [band_rows[i], band_rows[i + 1])
+    const uint32_t* step;   // the contexts' step table (cab::STEP_ENTRIES)
+    double lam2;            // 1.6 * 2^((QP'Y - 12) / 3), computed on the host in f64 as the reference does
+    int nbands;
+    int t8;                 // transform_8x8_mode_flag
+};
+
+template <class T>
+struct RdSmem {
+    DecideSmem<T> s;
+    uint8_t live[1024];              // the chain's contexts after the macroblocks before this one
+    uint8_t cst[RD_CANDS][1024];     // each candidate's copy, advanced by its bins
+    uint32_t step[cab::STEP_ENTRIES];
+    cab::Nb nb[2];                   // the left and top neighbours as the contexts see them
+    ironav_mbstate state[RD_CANDS];  // each candidate's MbState
+    long long ssd[RD_CANDS];
+    uint32_t bits[RD_CANDS];
+    int valid[RD_CANDS];
+    int best;
+    // the Intra8x8 trial
+    int i8rec[256];       // its reconstruction
+    int raw[25], e8[25];  // a block's edges, raw and filtered: [0] top-left, [1 + i] the 16 above, [17 + j] the 8 left
+    int sat[36];          // SATD per (mode, 4x4 quadrant)
+    int pred8[64];
+    int t8b[8][9];
+    int co8b[64];
+    int16_t lv8b[64];
+    uint8_t i8modes[16];
+    int i8meta[4];        // chosen mode, predicted mode, DC value, non-zero levels
+};
+
+// predict_nxn for n = 8, h264/intra.rs:30-128 (8.3.2.2.2-8.3.2.2.10), of sample (x, y) from the filtered
+// edges E; dcv the DC mode's value.
+__device__ __forceinline__ int i8_sample(const int* E, int mode, int x, int y, int dcv) {
+#define T8(i) ((i) < 0 ? E[0] : E[1 + (i)])
+#define L8(j) ((j) < 0 ? E[0] : E[17 + (j)])
+    switch (mode) {
+    case 0: return T8(x);
+    case 1: return L8(y);
+    case 2: return dcv;
+    case 3: return (x == 7 && y == 7) ? (T8(14) + 3 * T8(15) + 2) >> 2 : (T8(x + y) + 2 * T8(x + y + 1) + T8(x + y + 2) + 2) >> 2;
+    case 4:
+        if (x > y) return (T8(x - y - 2) + 2 * T8(x - y - 1) + T8(x - y) + 2) >> 2;
+        if (x < y) return (L8(y - x - 2) + 2 * L8(y - x - 1) + L8(y - x) + 2) >> 2;
+        return (T8(0) + 2 * E[0] + L8(0) + 2) >> 2;
+    case 5: {
+        const int z = 2 * x - y, i = x - (y >> 1);
+        if (z >= 0 && (z & 1) == 0) return (T8(i - 1) + T8(i) + 1) >> 1;
+        if (z >= 0) return (T8(i - 2) + 2 * T8(i - 1) + T8(i) + 2) >> 2;
+        if (z == -1) return (L8(0) + 2 * E[0] + T8(0) + 2) >> 2;
+        return (L8(y - 2 * x - 1) + 2 * L8(y - 2 * x - 2) + L8(y - 2 * x - 3) + 2) >> 2;
+    }
+    case 6: {
+        const int z = 2 * y - x, j = y - (x >> 1);
+        if (z >= 0 && (z & 1) == 0) return (L8(j - 1) + L8(j) + 1) >> 1;
+        if (z >= 0) return (L8(j - 2) + 2 * L8(j - 1) + L8(j) + 2) >> 2;
+        if (z == -1) return (L8(0) + 2 * E[0] + T8(0) + 2) >> 2;
+        return (T8(x - 2 * y - 1) + 2 * T8(x - 2 * y - 2) + T8(x - 2 * y - 3) + 2) >> 2;
+    }
+    case 7: {
+        const int i = x + (y >> 1);
+        return (y & 1) == 0 ? (T8(i) + T8(i + 1) + 1) >> 1 : (T8(i) + 2 * T8(i + 1) + T8(i + 2) + 2) >> 2;
+    }
+    default: {
+        const int z = x + 2 * y, j = y + (x >> 1);
+        if (z > 13) return L8(7);
+        if (z == 13) return (L8(6) + 3 * L8(7) + 2) >> 2;
+        if ((z & 1) == 0) return (L8(j) + L8(j + 1) + 1) >> 1;
+        return (L8(j) + 2 * L8(j + 1) + L8(j + 2) + 2) >> 2;
+    }
+    }
+#undef T8
+#undef L8
+}
+
+// code_i8, enc/frame.rs:1307-1388: the luma of an Intra8x8 macroblock, block by block in S.i8rec (each
+// block predicted from the filtered edges of the reconstruction so far, its mode the cheapest by SATD +
+// lambda * (1 predicted, 4 otherwise), quantised with the intra rounding), its levels, modes and counts
+// into out (zeroed by the caller with the Intra4x4 modes 2), and the reconstruction into the picture.
+// Returns the luma coded block pattern (every lane).
+template <class T>
+__device__ uint32_t code_i8_d(const DecideParams& P, RdSmem<T>& R, int mbx, int mby, bool ta, bool la, bool tra, ironav_mbcode* out) {
+    const int lane = threadIdx.x & 31;
+    DecideSmem<T>& S = R.s;
+    const CodeParams& C = P.C;
+    const int bd = C.bd, maxv = (1 << bd) - 1, lam = C.A.lambda;
+    const int qp = C.qp + 6 * (bd - 8), m6 = qp % 6, qbits = 16 + qp / 6, f = (1 << qbits) / 3;
+    const T* Y = reinterpret_cast<const T*>(C.rec[0]);
+    const int x0 = mbx * 16, y0 = mby * 16;
+    if (lane < 16) R.i8modes[lane] = 2;
+    __syncwarp();
+    uint32_t cbp = 0;
+    for (int i8 = 0; i8 < 4; i8++) {
+        const int bx = i8 & 1, by = i8 >> 1;
+        const bool hl = bx > 0 || la, ht = by > 0 || ta;
+        const bool htl = bx > 0 ? (by > 0 ? true : ta) : (by > 0 ? la : (la && ta));
+        const bool htr = i8 == 0 ? ta : (i8 == 1 ? tra : i8 == 2);
+        // the raw edges: the row above (the top-right half after the rest), the column to the left, the corner
+        if (lane < 8) {
+            const int x = bx * 8 + lane;
+            R.raw[1 + lane] = !ht ? 0 : (by == 0 ? S.top[1 + x] : R.i8rec[7 * 16 + x]);
+            R.raw[17 + lane] = !hl ? 0 : (bx == 0 ? S.left[by * 8 + lane] : R.i8rec[(by * 8 + lane) * 16 + 7]);
+        } else if (lane == 8) {
+            int v = 0;
+            if (htl) v = by == 0 ? S.top[bx * 8] : (bx == 0 ? S.left[7] : R.i8rec[7 * 16 + 7]);
+            R.raw[0] = v;
+        }
+        __syncwarp();
+        if (lane < 8) {
+            int v = 0;
+            if (ht) {
+                if (!htr) v = R.raw[8];  // the last sample above, repeated
+                else if (by == 1) v = R.i8rec[7 * 16 + 8 + lane];
+                else if (bx == 0) v = S.top[1 + 8 + lane];
+                else v = (int)Y[(size_t)(y0 - 1) * C.ys + x0 + 16 + lane];  // the top-right macroblock's bottom row
+            }
+            R.raw[9 + lane] = v;
+        }
+        __syncwarp();
+        // filter_8x8_edges, h264/intra.rs:131-158
+        if (lane < 25) {
+            const int* p = R.raw;
+            int v = p[lane];
+            if (lane == 0) {
+                if (htl) {
+                    if (ht && hl) v = (p[1] + 2 * p[0] + p[17] + 2) >> 2;
+                    else if (ht) v = (3 * p[0] + p[1] + 2) >> 2;
+                    else if (hl) v = (3 * p[0] + p[17] + 2) >> 2;
+                }
+            } else if (lane <= 16) {
+                const int x = lane - 1;
+                if (ht) {
+                    if (x == 0) v = htl ? (p[0] + 2 * p[1] + p[2] + 2) >> 2 : (3 * p[1] + p[2] + 2) >> 2;
+                    else if (x == 15) v = (p[15] + 3 * p[16] + 2) >> 2;
+                    else v = (p[x] + 2 * p[x + 1] + p[x + 2] + 2) >> 2;
+                }
+            } else {
+                const int y = lane - 17;
+                if (hl) {
+                    if (y == 0) v = htl ? (p[0] + 2 * p[17] + p[18] + 2) >> 2 : (3 * p[17] + p[18] + 2) >> 2;
+                    else if (y == 7) v = (p[23] + 3 * p[24] + 2) >> 2;
+                    else v = (p[16 + y] + 2 * p[17 + y] + p[18 + y] + 2) >> 2;
+                }
+            }
+            R.e8[lane] = v;
+        }
+        __syncwarp();
+        if (lane == 0) {
+            const int* E = R.e8;
+            int st = 0, sl = 0;
+            for (int i = 0; i < 8; i++) st += E[1 + i], sl += E[17 + i];
+            R.i8meta[2] = (ht && hl) ? (st + sl + 8) >> 4 : (hl ? (sl + 4) >> 3 : (ht ? (st + 4) >> 3 : 1 << (bd - 1)));
+            R.i8meta[1] = cab::pred_mode(S.nbm, R.i8modes, bx * 2, by * 2);
+        }
+        __syncwarp();
+        // the nine modes' SATD, a lane per (mode, 4x4 quadrant)
+        for (int u = lane; u < 36; u += 32) {
+            const int mode = u >> 2, q = u & 3;
+            const bool ok = (mode == 0 || mode == 3 || mode == 7) ? ht : (mode == 1 || mode == 8) ? hl : mode == 2 ? true : (ht && hl && htl);
+            int s = 0;
+            if (ok) {
+                int d[16];
+#pragma unroll
+                for (int r = 0; r < 4; r++)
+#pragma unroll
+                    for (int k = 0; k < 4; k++) {
+                        const int px = (q & 1) * 4 + k, py = (q >> 1) * 4 + r;
+                        d[r * 4 + k] = src_at(S.a, bx * 8 + px, by * 8 + py) - i8_sample(R.e8, mode, px, py, R.i8meta[2]);
+                    }
+                s = satd4_d(d);
+            }
+            R.sat[u] = ok ? s : -1;
+        }
+        __syncwarp();
+        if (lane == 0) {
+            int bm = 2, bc = 0x7fffffff;
+            for (int mode = 0; mode < 9; mode++) {
+                if (R.sat[mode * 4] < 0) continue;
+                const int c = R.sat[mode * 4] + R.sat[mode * 4 + 1] + R.sat[mode * 4 + 2] + R.sat[mode * 4 + 3] +
+                              lam * (mode == R.i8meta[1] ? 1 : 4);
+                if (c < bc) bm = mode, bc = c;
+            }
+            R.i8meta[0] = bm;
+        }
+        __syncwarp();
+        const int bm = R.i8meta[0];
+        for (int i = lane; i < 64; i += 32) R.pred8[i] = i8_sample(R.e8, bm, i & 7, i >> 3, R.i8meta[2]);
+        __syncwarp();
+        // quant8 (intra rounding) and idct8_add, enc/frame.rs:56-72 and h264/idct.rs:33-74, eight lanes
+        const int j = lane & 7;
+        if (lane < 8) {
+            int d[8], o[8];
+#pragma unroll
+            for (int k = 0; k < 8; k++) d[k] = src_at(S.a, bx * 8 + k, by * 8 + j) - R.pred8[j * 8 + k];
+            q_fdct8_1d_d(d, o);
+#pragma unroll
+            for (int k = 0; k < 8; k++) R.t8b[j][k] = o[k];
+        }
+        __syncwarp();
+        if (lane < 8) {
+            int d[8], o[8];
+#pragma unroll
+            for (int k = 0; k < 8; k++) d[k] = R.t8b[k][j];
+            q_fdct8_1d_d(d, o);
+#pragma unroll
+            for (int k = 0; k < 8; k++) R.co8b[k * 8 + j] = o[k];
+        }
+        __syncwarp();
+        int dq[8];
+        int nz = 0;
+        if (lane < 8) {
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                const int sk = j * 8 + k, pz = c_zz8[sk];
+                const int l = q_quant_d(R.co8b[pz], c_q_mf8[m6][q_class8_d(pz)], f, qbits);
+                R.lv8b[sk] = (int16_t)l;
+                nz += l != 0;
+                int v = 0;
+                if (l != 0) {
+                    const int vv = l * 16 * c_q_dq8[m6][q_class8_d(pz)];
+                    v = qp >= 36 ? vv << (qp / 6 - 6) : (vv + (1 << (5 - qp / 6))) >> (6 - qp / 6);
+                }
+                dq[k] = v;
+            }
+        }
+        __syncwarp();
+        if (lane < 8) {
+#pragma unroll
+            for (int k = 0; k < 8; k++) R.co8b[c_zz8[j * 8 + k]] = dq[k];
+        }
+#pragma unroll
+        for (int off = 16; off >= 1; off >>= 1) nz += __shfl_xor_sync(FULL, nz, off);
+        __syncwarp();
+        if (lane < 8 && nz > 0) {
+            int d[8], o[8];
+#pragma unroll
+            for (int k = 0; k < 8; k++) d[k] = R.co8b[j * 8 + k];
+            q_row8_d(d, o);
+#pragma unroll
+            for (int k = 0; k < 8; k++) R.t8b[j][k] = o[k];
+        }
+        __syncwarp();
+        if (lane < 8) {
+            int o[8];
+            if (nz > 0) {
+                int d[8];
+#pragma unroll
+                for (int k = 0; k < 8; k++) d[k] = R.t8b[k][j];
+                q_row8_d(d, o);
+            }
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+                const int pv = R.pred8[i * 8 + j];
+                R.i8rec[(by * 8 + i) * 16 + bx * 8 + j] = nz > 0 ? min(max(pv + ((o[i] + 32) >> 6), 0), maxv) : pv;
+            }
+        }
+        for (int k = lane; k < 64; k += 32) out->res.luma8[i8][k] = R.lv8b[k];
+        if (lane < 4) {
+            const int b = (by * 2 + (lane >> 1)) * 4 + bx * 2 + (lane & 1);
+            R.i8modes[b] = (uint8_t)bm;
+            out->res.nnz[b] = (uint8_t)nz;
+        }
+        if (nz > 0) cbp |= 1u << i8;
+        __syncwarp();
+    }
+    T* RY = reinterpret_cast<T*>(C.rec[0]);
+    for (int i = lane; i < 256; i += 32) RY[(size_t)(y0 + (i >> 4)) * C.ys + x0 + (i & 15)] = (T)R.i8rec[i];
+    if (lane < 16) out->modes[lane] = R.i8modes[lane];
+    if (lane == 0) {
+        out->kind = KIND_I8;
+        out->res.t8x8 = 1;
+    }
+    __syncwarp();
+    return cbp;
+}
+
+// MbCode::new (enc/frame.rs:302-306): zero, the Intra4x4 modes 2 (words 371-374 of the code).
+__device__ __forceinline__ void code_init(ironav_mbcode* o) {
+    const int lane = threadIdx.x & 31;
+    uint32_t* w = reinterpret_cast<uint32_t*>(o);
+    for (int k = lane; k < (int)(sizeof(ironav_mbcode) / 4); k += 32) w[k] = (k >= 371 && k < 375) ? 0x02020202u : 0u;
+    __syncwarp();
+}
+
+// A candidate coded into the picture: its squared error (ssd_mb, enc/frame.rs:1432-1449) and a copy of its
+// reconstruction (save_mb, 1406-1417) in the chain's scratch; the candidate counts from here on.
+template <class T>
+__device__ void rd_take(const RdParams& P, RdSmem<T>& R, int chain, int k, int mbx, int mby) {
+    const int lane = threadIdx.x & 31;
+    const CodeParams& C = P.D.C;
+    const T* SC = reinterpret_cast<const T*>(C.src_c);
+    T* dst = reinterpret_cast<T*>(P.cand_rec) + ((size_t)chain * RD_CANDS + k) * 384;
+    __syncwarp();
+    long long ssd = 0;
+    for (int i = lane; i < 384; i += 32) {
+        int r, s;
+        if (i < 256) {
+            r = reinterpret_cast<const T*>(C.rec[0])[(size_t)(mby * 16 + (i >> 4)) * C.ys + mbx * 16 + (i & 15)];
+            s = src_at(R.s.a, i & 15, i >> 4);
+        } else {
+            const int cc = (i - 256) >> 6, j = (i - 256) & 63, cy = mby * 8 + (j >> 3), cx = mbx * 8 + (j & 7);
+            r = reinterpret_cast<const T*>(C.rec[1 + cc])[(size_t)cy * C.cs + cx];
+            s = SC[(size_t)cc * C.cw * C.ch + (size_t)cy * C.cw + cx];
+        }
+        dst[i] = (T)r;
+        const long long d = s - r;
+        ssd += d * d;
+    }
+#pragma unroll
+    for (int off = 16; off >= 1; off >>= 1) ssd += __shfl_xor_sync(FULL, ssd, off);
+    if (lane == 0) {
+        R.ssd[k] = ssd;
+        R.valid[k] = 1;
+    }
+    __syncwarp();
+}
+
+// The MbState of a coded candidate: the inter ones' from inter_tail (S.a.out), the intra ones' without motion.
+template <class T>
+__device__ __forceinline__ void rd_state(RdSmem<T>& R, int k, bool inter) {
+    const int lane = threadIdx.x & 31;
+    __syncwarp();
+    uint32_t* d = reinterpret_cast<uint32_t*>(&R.state[k]);
+    if (inter) {
+        if (lane < 18) d[lane] = reinterpret_cast<const uint32_t*>(&R.s.a.out)[lane];
+    } else {
+        if (lane < 16) d[lane] = 0;  // mvs
+        if (lane == 16) d[lane] = 0xFFFFFFFFu;  // refs -1
+        if (lane == 17) d[lane] = 0;            // inter 0
+    }
+    __syncwarp();
+}
+
+// decide_rd for one macroblock (after code_mb's P_Skip tests, best_i16 and best_inter; enc/frame.rs:715-760,
+// 1462-1513), its bins then carried into the chain's contexts (write_mb_cabac's effect on them, 2020-2025).
+template <class T>
+__device__ void rd_mb(const RdParams& P, RdSmem<T>& R, const unsigned* i4tab, int chain, int mb, int mbx, int mby) {
+    const int lane = threadIdx.x & 31;
+    const DecideParams& D = P.D;
+    const AnalyseParams& A = D.C.A;
+    const CodeParams& C = D.C;
+    DecideSmem<T>& S = R.s;
+    const bool ta = mby > A.band_start[mby], la = mbx > 0, tra = ta && mbx + 1 < A.mb_w;
+    const cab::Slice sl = {D.intra ? 0 : 1, P.t8, D.intra ? 0 : A.nact};
+    ironav_mbcode* out = &D.codes[mb];
+    ironav_mbcode* cand = P.cand + (size_t)chain * RD_CANDS;
+    code_init(out);
+    stage_source(A, S.a);
+    if (lane == 0) {
+        R.nb[0].avail = R.nb[1].avail = 0;
+        if (la) cab::nb_of(&D.codes[mb - 1], &R.nb[0]);
+        if (ta) cab::nb_of(&D.codes[mb - A.mb_w], &R.nb[1]);
+    }
+    if (lane < RD_CANDS) R.valid[lane] = 0;
+    __syncwarp();
+    int2 sv = make_int2(0, 0);
+    if (!D.intra && skip_tests_d<T>(D, S, mb, mbx, mby, out, &sv)) {
+        // P_Skip without a rate-distortion choice; its one bin still moves the contexts
+        if (lane == 0) {
+            cab::Counter c = {R.live, R.step, 0};
+            cab::mb_bins(c, sl, out, R.nb[0], R.nb[1], S.nbm);
+        }
+        if (lane < 18) reinterpret_cast<uint32_t*>(&A.states_out[mb])[lane] = reinterpret_cast<const uint32_t*>(&S.a.out)[lane];
+        __syncwarp();
+        return;
+    }
+    load_intra_neighbours(D, S, mb, mbx, mby, ta, la, tra);
+    const int2 i16 = best_i16_d(D, S, ta, la);
+    // best_inter, enc/frame.rs:839-849 (none in an IDR picture)
+    int part = 0, cost = BIG, bestr = 0;
+    uint32_t sub = 0;
+    for (int r = 0; r < A.nact && !D.intra; r++) {
+        const int4 bi = best_inter_or_learned(A, S.a, r);
+        if (r == 0 || bi.x < cost) {
+            part = bi.y;
+            cost = bi.x;
+            bestr = r;
+            sub = (uint32_t)bi.z;
+            if (lane < 16) {
+                S.a.win_mvs[lane][0] = S.a.best_mvs[lane][0];
+                S.a.win_mvs[lane][1] = S.a.best_mvs[lane][1];
+            }
+            __syncwarp();
+        }
+    }
+    ironav_interdec& Dd = *reinterpret_cast<ironav_interdec*>(S.c.dec);
+    if (!D.intra) {
+        // P_Skip: the skip vector's prediction is the reconstruction (put_inter_pred, 1391-1394)
+        ironav_mbcode* o = &cand[0];
+        code_init(o);
+        if (lane == 0) {
+            Dd.mode = 1;
+            Dd.part = 0;
+            Dd.t8 = 0;
+            for (int k = 0; k < 4; k++) Dd.sub[k] = Dd.refs[k] = 0;
+        }
+        if (lane < 16) {
+            Dd.mvs[lane][0] = (int16_t)sv.x;
+            Dd.mvs[lane][1] = (int16_t)sv.y;
+        }
+        __syncwarp();
+        code_inter_mb<T>(C, S.c, mb, &o->res);
+        inter_tail(D, S, Dd, o);
+        if (lane < 16) o->mvds[lane][0] = o->mvds[lane][1] = 0;
+        if (lane == 0) o->skip = 1;
+        rd_state(R, 0, true);
+        rd_take(P, R, chain, 0, mbx, mby);
+        // best_inter's partitioning with the 4x4 transform; with nothing coded and the skip vector, it would be
+        // P_Skip at a higher price
+        o = &cand[1];
+        code_init(o);
+        if (lane == 0) {
+            Dd.mode = 2;
+            Dd.part = (uint8_t)part;
+            Dd.t8 = 0;
+            for (int k = 0; k < 4; k++) {
+                Dd.sub[k] = (uint8_t)((sub >> (8 * k)) & 0xff);
+                Dd.refs[k] = (uint8_t)bestr;
+            }
+        }
+        if (lane < 16) {
+            Dd.mvs[lane][0] = S.a.win_mvs[lane][0];
+            Dd.mvs[lane][1] = S.a.win_mvs[lane][1];
+        }
+        __syncwarp();
+        const uint32_t cbp = code_inter_mb<T>(C, S.c, mb, &o->res);
+        inter_tail(D, S, Dd, o);
+        rd_state(R, 1, true);
+        rd_take(P, R, chain, 1, mbx, mby);
+        if (lane == 0 && cbp == 0 && part == 0 && Dd.mvs[0][0] == sv.x && Dd.mvs[0][1] == sv.y && bestr == 0) R.valid[1] = 0;
+        __syncwarp();
+        // the 8x8 transform needs every 8x8 block of P_8x8 to be a single 8x8 partition; without luma levels it
+        // would be the 4x4 candidate again
+        if (P.t8 && sub == 0) {
+            o = &cand[2];
+            code_init(o);
+            if (lane == 0) Dd.t8 = 1;
+            __syncwarp();
+            code_inter_mb<T>(C, S.c, mb, &o->res);
+            inter_tail(D, S, Dd, o);
+            rd_state(R, 2, true);
+            rd_take(P, R, chain, 2, mbx, mby);
+            if (lane == 0 && !o->res.t8x8) R.valid[2] = 0;
+            __syncwarp();
+        }
+    }
+    // Intra16x16 in best_i16's mode, with its chroma
+    {
+        ironav_mbcode* o = &cand[3];
+        code_init(o);
+        uint32_t cbp = code_i16_d(D, S, mbx, mby, i16.x, ta, la, o);
+        cbp |= code_intra_chroma_d(D, S, mbx, mby, ta, la, o);
+        if (lane == 0) {
+            o->kind = KIND_I16;
+            o->i16_mode = (uint8_t)i16.x;
+            o->res.cbp = (uint8_t)cbp;
+        }
+        rd_state(R, 3, false);
+        rd_take(P, R, chain, 3, mbx, mby);
+    }
+    // Intra4x4, block by block from its own reconstruction, with its chroma
+    {
+        ironav_mbcode* o = &cand[4];
+        code_init(o);
+        code_i4_trial(D, S, i4tab, ta, la, tra);
+        T* RY = reinterpret_cast<T*>(C.rec[0]);
+        for (int i = lane; i < 256; i += 32) RY[(size_t)(mby * 16 + (i >> 4)) * C.ys + mbx * 16 + (i & 15)] = (T)S.i4rec[i];
+        if (lane < 16) {
+            uint32_t* lw = reinterpret_cast<uint32_t*>(o->res.luma[lane]);
+            const uint32_t* src = reinterpret_cast<const uint32_t*>(S.i4lv[lane]);
+#pragma unroll
+            for (int k = 0; k < 8; k++) lw[k] = src[k];
+            o->res.nnz[lane] = S.i4nnz[lane];
+            o->modes[lane] = S.i4modes[lane];
+        }
+        const unsigned bal = __ballot_sync(FULL, lane < 16 && S.i4nnz[lane] > 0);
+        uint32_t cbp = 0;
+#pragma unroll
+        for (int i8 = 0; i8 < 4; i8++)
+            if (bal & (0x33u << ((i8 >> 1) * 8 + (i8 & 1) * 2))) cbp |= 1u << i8;
+        __syncwarp();
+        cbp |= code_intra_chroma_d(D, S, mbx, mby, ta, la, o);
+        if (lane == 0) {
+            o->kind = KIND_I4;
+            o->res.cbp = (uint8_t)cbp;
+        }
+        rd_state(R, 4, false);
+        rd_take(P, R, chain, 4, mbx, mby);
+    }
+    // Intra8x8 with its chroma
+    if (P.t8) {
+        ironav_mbcode* o = &cand[5];
+        code_init(o);
+        uint32_t cbp = code_i8_d(D, R, mbx, mby, ta, la, tra, o);
+        cbp |= code_intra_chroma_d(D, S, mbx, mby, ta, la, o);
+        if (lane == 0) o->res.cbp = (uint8_t)cbp;
+        rd_state(R, 5, false);
+        rd_take(P, R, chain, 5, mbx, mby);
+    }
+    // each candidate's bins counted from its own copy of the contexts (rd_cost, 1453-1457), a lane a candidate
+    for (int k = 0; k < RD_CANDS; k++) {
+        if (!R.valid[k]) continue;
+        const uint32_t* s32 = reinterpret_cast<const uint32_t*>(R.live);
+        uint32_t* d32 = reinterpret_cast<uint32_t*>(R.cst[k]);
+        for (int i = lane; i < 256; i += 32) d32[i] = s32[i];
+    }
+    __syncwarp();
+    if (lane < RD_CANDS && R.valid[lane]) {
+        cab::Counter c = {R.cst[lane], R.step, 0};
+        cab::mb_bins(c, sl, &cand[lane], R.nb[0], R.nb[1], S.nbm);
+        R.bits[lane] = c.bits;
+    }
+    __syncwarp();
+    if (lane == 0) {
+        // SSD + lam2 * bits in f64, rounded as the reference's expression is (no fused multiply-add)
+        int best = -1;
+        double bj = 0.0;
+        for (int k = 0; k < RD_CANDS; k++) {
+            if (!R.valid[k]) continue;
+            const double j = __dadd_rn(__ll2double_rn(R.ssd[k]), __dmul_rn(P.lam2, __dmul_rn((double)R.bits[k], 0.00390625)));
+            if (best < 0 || j < bj) best = k, bj = j;
+        }
+        R.best = best;
+    }
+    __syncwarp();
+    const int b = R.best;
+    {
+        const uint32_t* s32 = reinterpret_cast<const uint32_t*>(&cand[b]);
+        uint32_t* d32 = reinterpret_cast<uint32_t*>(out);
+        for (int i = lane; i < (int)(sizeof(ironav_mbcode) / 4); i += 32) d32[i] = s32[i];
+        const uint32_t* c32 = reinterpret_cast<const uint32_t*>(R.cst[b]);
+        uint32_t* l32 = reinterpret_cast<uint32_t*>(R.live);
+        for (int i = lane; i < 256; i += 32) l32[i] = c32[i];
+        const T* rec = reinterpret_cast<const T*>(P.cand_rec) + ((size_t)chain * RD_CANDS + b) * 384;
+        for (int i = lane; i < 384; i += 32) {
+            if (i < 256) {
+                reinterpret_cast<T*>(C.rec[0])[(size_t)(mby * 16 + (i >> 4)) * C.ys + mbx * 16 + (i & 15)] = rec[i];
+            } else {
+                const int cc = (i - 256) >> 6, j = (i - 256) & 63;
+                reinterpret_cast<T*>(C.rec[1 + cc])[(size_t)(mby * 8 + (j >> 3)) * C.cs + mbx * 8 + (j & 7)] = rec[i];
+            }
+        }
+        if (lane < 18) reinterpret_cast<uint32_t*>(&A.states_out[mb])[lane] = reinterpret_cast<const uint32_t*>(&R.state[b])[lane];
+    }
+    __syncwarp();
+}
+
+// Decide mode under CABAC: CTA i, one warp, walks slice band i in raster order (FrameCoder::encode,
+// enc/frame.rs:461-478) from the slice's initial contexts (cabac_init_idc 0, QP_Y).
+template <class T>
+__global__ void __launch_bounds__(32) decide_rd_kernel(const __grid_constant__ RdParams P) {
+    __shared__ RdSmem<T> R;
+    __shared__ unsigned i4tab[9 * 17];
+    fill_i4tab(i4tab);
+    const int chain = blockIdx.x, lane = threadIdx.x & 31;
+    if (chain >= P.nbands) return;
+    const AnalyseParams& A = P.D.C.A;
+    for (int i = lane; i < cab::STEP_ENTRIES; i += 32) R.step[i] = P.step[i];
+    cab::init_states(R.live, P.D.intra != 0, 0, P.D.C.qp, lane, 32);
+    __syncwarp();
+    for (int mby = P.band_rows[chain]; mby < P.band_rows[chain + 1]; mby++)
+        for (int mbx = 0; mbx < A.mb_w; mbx++) {
+            const int mb = mby * A.mb_w + mbx;
+            if (lane == 0) {
+                R.s.a.mb = mb;
+                R.s.a.mbx = mbx;
+                R.s.a.mby = mby;
+            }
+            __syncwarp();
+            load_neighbours(A, R.s.a, A.states_out);
+            rd_mb<T>(P, R, i4tab, chain, mb, mbx, mby);
+        }
+}
+
+// ---- the CABAC slice writer ---------------------------------------------------------------------------
+
+struct CabacWriteParams {
+    const ironav_mbcode* codes;
+    const int* band_rows;
+    const uint32_t* step;
+    uint32_t* out;          // slice i's data at out + i * region_words
+    uint32_t region_words;
+    uint32_t* slice_bytes;  // per slice: its data's bytes; [nbands]: set when a slice outgrew its region
+    int mb_w, nbands, intra, t8, nref, qp;
+};
+
+// A slice band's data (FrameCoder::encode with write_mb_cabac, enc/frame.rs:461-486): each macroblock's bins
+// (mb_bins) then end_of_slice_flag, arithmetic coded from the slice's contexts; the data starts on the byte
+// that follows the header's cabac_alignment_one_bit (written on the host). CTA i, lane 0, slice band i.
+__global__ void __launch_bounds__(32) cabac_write_kernel(const __grid_constant__ CabacWriteParams P) {
+    __shared__ uint8_t st[1024];
+    __shared__ uint32_t step[cab::STEP_ENTRIES];
+    __shared__ cab::Nb nb[2];
+    __shared__ int nbm[8];
+    const int chain = blockIdx.x, lane = threadIdx.x & 31;
+    if (chain >= P.nbands) return;
+    for (int i = lane; i < cab::STEP_ENTRIES; i += 32) step[i] = P.step[i];
+    cab::init_states(st, P.intra != 0, 0, P.qp, lane, 32);
+    __syncwarp();
+    if (lane != 0) return;
+    cab::BitOut bo = {P.out + (size_t)chain * P.region_words, P.region_words, 0, 0ull, 0, false};
+    cab::Coder k = {st, step, &bo, 0u, 510u, 0u, true};
+    const cab::Slice sl = {P.intra ? 0 : 1, P.t8, P.intra ? 0 : P.nref};
+    const int r0 = P.band_rows[chain], r1 = P.band_rows[chain + 1];
+    for (int mby = r0; mby < r1; mby++)
+        for (int mbx = 0; mbx < P.mb_w; mbx++) {
+            const int mb = mby * P.mb_w + mbx;
+            const ironav_mbcode* L = mbx > 0 ? &P.codes[mb - 1] : nullptr;
+            const ironav_mbcode* Tp = mby > r0 ? &P.codes[mb - P.mb_w] : nullptr;
+            nb[0].avail = nb[1].avail = 0;
+            if (L) cab::nb_of(L, &nb[0]);
+            if (Tp) cab::nb_of(Tp, &nb[1]);
+            for (int q = 0; q < 4; q++) {
+                nbm[q] = L ? (cab::nxn(L->kind) ? (int)L->modes[q * 4 + 3] : 2) : -1;
+                nbm[4 + q] = Tp ? (cab::nxn(Tp->kind) ? (int)Tp->modes[12 + q] : 2) : -1;
+            }
+            cab::mb_bins(k, sl, &P.codes[mb], nb[0], nb[1], nbm);
+            k.terminate(mby + 1 == r1 && mbx + 1 == P.mb_w);
+            if (bo.over) break;
+        }
+    const uint32_t bytes = bo.finish();
+    P.slice_bytes[chain] = bytes;
+    if (bo.over) atomicOr(&P.slice_bytes[P.nbands], 1u);
+}
+
+}  // namespace ironav

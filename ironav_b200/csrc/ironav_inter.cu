@@ -133,6 +133,13 @@ void free_ctx(ironav_ctx* c) {
     cudaFree(c->d_cavlc);
     cudaFree(c->d_slice_tab);
     cudaFree(c->d_rbsp);
+    cudaFree(c->d_cab_step);
+    cudaFree(c->d_band_rows);
+    cudaFree(c->d_rd_cand);
+    cudaFree(c->d_rd_rec);
+    cudaFree(c->d_cab_out);
+    cudaFree(c->d_cab_bytes);
+    cudaFreeHost(c->h_cab_bytes);
     cudaFreeHost(c->h_cavlc);
     cudaFreeHost(c->h_rbsp);
     cudaFreeHost(c->h_results);
@@ -884,6 +891,7 @@ int ironav::fill_decide_params(ironav_ctx* c, DecideParams& p, ironav_mbstate* d
 extern "C" {
 
 static int launch_decide(ironav_ctx* c, ironav_mbstate* d_states, ironav_mbcode* d_codes, void* y, int ys, void* cb, void* cr, int cs) {
+    if (c->cabac) return launch_decide_rd(c, d_states, d_codes, y, ys, cb, cr, cs);
     DecideParams p;
     const int s = fill_decide_params(c, p, d_states, d_codes, y, ys, cb, cr, cs);
     if (s != IRONAV_OK) return s;
@@ -1072,6 +1080,17 @@ int ironav_inloop_end(ironav_ctx* c) {
 
 // Replay mode's kernel: 0 one macroblock per 8-lane group (the default), 1 one macroblock per warp, 2 one
 // macroblock per 16-lane group.
+int ironav_set_entropy(ironav_ctx* c, int cabac, int transform8) {
+    if (!c || cabac < 0 || cabac > 1 || transform8 < 0 || transform8 > 1) return IRONAV_INVALID_ARGUMENT;
+    if (cabac) {
+        const int s = cabac_setup(c);
+        if (s != IRONAV_OK) return s;
+    }
+    c->cabac = cabac;
+    c->t8 = cabac && transform8;  // FrameCoder::new, enc/frame.rs:405: the 8x8 transform with CABAC only
+    return IRONAV_OK;
+}
+
 int ironav_set_replay_form(ironav_ctx* c, int form) {
     if (!c || form < 0 || form > 3) return IRONAV_INVALID_ARGUMENT;
     c->replay_form = form;

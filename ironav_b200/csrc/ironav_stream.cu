@@ -1,5 +1,6 @@
 // ironav_stream.cu — the bitstream entry points of include/ironav_inter.h: the CAVLC slices of a picture
-// written on the device from its codes (cavlc.cuh), and the sequence and picture parameter sets.
+// written on the device from its codes (cavlc.cuh), or its CABAC slices (the data arithmetic coded on the
+// device, ironav_cabac.cu, behind headers written here), and the sequence and picture parameter sets.
 //
 // A picture's slices: three launches on the context's stream (sizes, per-slice scan with header and
 // trailer, the macroblocks' bits), then each slice's RBSP bytes come back to pinned host memory and go
@@ -78,6 +79,9 @@ struct HostBits {
         put(1, 1);
         if (n > 0) put(8 - n, 0);
     }
+    void align_ones() {  // cabac_alignment_one_bit, enc/bitw.rs:52-58
+        if (n > 0) put(8 - n, (1u << (8 - n)) - 1);
+    }
 };
 
 // The writer's device buffers, on first use: per macroblock 3 words, per slice 1, the error word; the
@@ -103,12 +107,55 @@ int writer_setup(ironav_ctx* c) {
     return IRONAV_OK;
 }
 
+// The CABAC slices (enc/mod.rs:566-600 and 641-643; FrameCoder::encode, enc/frame.rs:461-486): each slice's
+// header with cabac_init_idc (P slices) and cabac_alignment_one_bit, then its arithmetic-coded data.
+int write_slices_cabac(ironav_ctx* c, int idr, int frame_num, int idr_pic_id, const ironav_mbcode* d_codes, uint8_t* out, size_t cap,
+                       size_t* len) {
+    std::vector<std::vector<uint8_t>> data;
+    const int s = cabac_slice_data(c, idr, d_codes, &data);
+    if (s != IRONAV_OK) return s;
+    std::vector<uint8_t> stream;
+    for (int i = 0; i < c->nslices; i++) {
+        HostBits h;
+        h.ue((uint32_t)(c->band_rows[i] * c->mb_w));  // first_mb_in_slice
+        h.ue(idr ? 7 : 5);                            // slice_type: I or P, all slices alike
+        h.ue(0);                                      // pic_parameter_set_id
+        h.put(8, (uint32_t)frame_num);
+        if (idr) h.ue((uint32_t)idr_pic_id);
+        if (!idr) {
+            if (c->nact > 1) {
+                h.flag(true);  // num_ref_idx_active_override_flag
+                h.ue((uint32_t)(c->nact - 1));
+            } else {
+                h.flag(false);
+            }
+            h.flag(false);  // ref_pic_list_modification_flag_l0
+        }
+        if (idr) {
+            h.flag(false);  // no_output_of_prior_pics_flag
+            h.flag(false);  // long_term_reference_flag
+        } else {
+            h.flag(false);  // adaptive_ref_pic_marking_mode_flag
+        }
+        if (!idr) h.ue(0);                             // cabac_init_idc
+        h.se((c->qpp - 6 * (c->bd - 8)) - 26);         // slice_qp_delta
+        h.align_ones();
+        h.buf.insert(h.buf.end(), data[i].begin(), data[i].end());
+        put_nal(stream, 3, idr ? 5 : 1, h.buf.data(), h.buf.size());
+    }
+    *len = stream.size();
+    if (!out || cap < stream.size()) return IRONAV_INVALID_ARGUMENT;
+    memcpy(out, stream.data(), stream.size());
+    return IRONAV_OK;
+}
+
 int write_slices(ironav_ctx* c, int idr, int frame_num, int idr_pic_id, const ironav_mbcode* d_codes, uint8_t* out, size_t cap,
                  size_t* len) {
     if (!c || !d_codes || !len || !c->have_params || (idr != 0) != c->intra_pic || (!idr && (c->nact < 1 || c->nact > c->nrefs)) ||
         frame_num < 0 || frame_num > 255 || idr_pic_id < 0 || idr_pic_id > 65535)
         return IRONAV_INVALID_ARGUMENT;
     if (reinterpret_cast<uintptr_t>(d_codes) & 3) return IRONAV_INVALID_ARGUMENT;
+    if (c->cabac) return write_slices_cabac(c, idr, frame_num, idr_pic_id, d_codes, out, cap, len);
     int s = writer_setup(c);
     if (s != IRONAV_OK) return s;
     const int ns = c->nslices, nmb = c->nmb;
@@ -195,10 +242,10 @@ int ironav_write_slices(ironav_ctx* c, int idr, int frame_num, int idr_pic_id, c
     return write_slices(c, idr, frame_num, idr_pic_id, c->d_mbcodes, out, cap, len);
 }
 
-// H264Encoder::sps / pps for the CAVLC encoder (enc/mod.rs:296-400) and its level (154-157)
+// H264Encoder::sps / pps without B pictures (enc/mod.rs:296-400) and its level (154-157)
 int ironav_write_parameter_sets(const ironav_stream_params* p, uint8_t* out, size_t cap, size_t* len) {
     if (!p || !len || p->width <= 0 || p->height <= 0 || (p->width & 1) || (p->height & 1) || (p->bd != 8 && p->bd != 10) || p->refs < 1 ||
-        p->refs > 16)
+        p->refs > 16 || p->cabac < 0 || p->cabac > 1 || p->transform8 < 0 || p->transform8 > 1)
         return IRONAV_INVALID_ARGUMENT;
     const int mb_w = (p->width + 15) / 16, mb_h = (p->height + 15) / 16;
     if (mb_w > 1024 || mb_h > 1024) return IRONAV_INVALID_ARGUMENT;
@@ -212,11 +259,17 @@ int ironav_write_parameter_sets(const ironav_stream_params* p, uint8_t* out, siz
     for (int i = 0; i < 19 && level < 0; i++)
         if (LEVELS[i][1] >= fs) level = (int)LEVELS[i][0];
     if (level < 0) level = 62;
-    const bool high = p->bd > 8;
+    const bool t8 = p->cabac && p->transform8, high = t8 || p->bd > 8;
     HostBits w;
-    if (high) {
+    if (p->bd > 8) {
         w.put(8, 110);  // High 10
         w.put(8, 0);
+    } else if (high) {
+        w.put(8, 100);  // High
+        w.put(8, 0);
+    } else if (p->cabac) {
+        w.put(8, 77);    // Main
+        w.put(8, 0x40);  // constraint_set1: Main
     } else {
         w.put(8, 66);    // Baseline
         w.put(8, 0xC0);  // constraint_set0 and constraint_set1: Constrained Baseline
@@ -273,7 +326,7 @@ int ironav_write_parameter_sets(const ironav_stream_params* p, uint8_t* out, siz
     HostBits q;
     q.ue(0);        // pic_parameter_set_id
     q.ue(0);        // seq_parameter_set_id
-    q.flag(false);  // entropy_coding_mode_flag: CAVLC
+    q.flag(p->cabac != 0);  // entropy_coding_mode_flag
     q.flag(false);  // bottom_field_pic_order_in_frame_present_flag
     q.ue(0);        // num_slice_groups_minus1
     q.ue(0);        // num_ref_idx_l0_default_active_minus1
@@ -286,6 +339,11 @@ int ironav_write_parameter_sets(const ironav_stream_params* p, uint8_t* out, siz
     q.flag(false);  // deblocking_filter_control_present_flag
     q.flag(false);  // constrained_intra_pred_flag
     q.flag(false);  // redundant_pic_cnt_present_flag
+    if (t8) {
+        q.flag(true);   // transform_8x8_mode_flag
+        q.flag(false);  // pic_scaling_matrix_present_flag
+        q.se(0);        // second_chroma_qp_index_offset
+    }
     q.finish();
     std::vector<uint8_t> stream;
     put_nal(stream, 3, 7, w.buf.data(), w.buf.size());  // enc/mod.rs:637-638

@@ -1,6 +1,7 @@
-"""An IPPP H.264 encoder with CAVLC built on the library's entry points: the encoder loop of ironav-codec's
-H264Encoder (crates/ironav-codec/src/h264/enc/mod.rs) for the settings the CAVLC stream uses: no B pictures
-(`constrained_baseline`, enc/mod.rs:236-243), IDR pictures every `keyint` pictures or at a scene cut
+"""An IPPP H.264 encoder built on the library's entry points: the encoder loop of ironav-codec's H264Encoder
+(crates/ironav-codec/src/h264/enc/mod.rs) without B pictures, with CAVLC (`constrained_baseline`,
+enc/mod.rs:236-243) or with CABAC, rate-distortion decisions and the 8x8 transform (the High stream of
+`low_latency`, enc/mod.rs:210-215), IDR pictures every `keyint` pictures or at a scene cut
 (encode, enc/mod.rs:700-724), a constant quantiser with the IDR picture's offset of -3 (QP_OFFSET and
 next_qp, enc/mod.rs:33,403-417), `refs` reference pictures, and `nslices` slice bands.
 
@@ -65,9 +66,10 @@ class Encoder:
 
     def __init__(self, width: int, height: int, qp: int, keyint: int = 250, refs: int = 1, nslices: int = 1,
                  fps: tuple[int, int] = (30, 1), bd: int = 8, fast: bool = False, sub8: bool = False, scene_cut: bool = True,
-                 lib: ctypes.CDLL | None = None):
+                 lib: ctypes.CDLL | None = None, cabac: bool = False, transform8: bool = True):
         self.lib = lib if lib is not None else cuda_library()
         self.st = InterStage(width, height, max_refs=refs, nslices=nslices, lib=self.lib, bd=bd)
+        self.st.set_entropy(cabac, transform8)
         self.loop = _Loop(width, height, qp, keyint, refs, bd, fps)
         self.fast, self.sub8, self.scene_cut = fast, sub8, scene_cut
         self.slices = np.zeros(nslices, dtype=DBK_SLICE_DTYPE)  # every slice filtered, no offsets (enc/mod.rs:648)
@@ -75,7 +77,7 @@ class Encoder:
         self.recon = None
         self.codes = None
         self.states = None
-        self.params = write_parameter_sets(width, height, bd, fps, refs, lib=self.lib)
+        self.params = write_parameter_sets(width, height, bd, fps, refs, lib=self.lib, cabac=cabac, transform8=transform8)
         # called as before_p(encoder, y) once a P picture's parameters are set and before it is decided
         self.before_p = None
 

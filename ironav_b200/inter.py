@@ -138,6 +138,7 @@ EXPORTS = (
     "ironav_prop_conv3x3", "ironav_prop_wgrad3x3", "ironav_prop_prep", "ironav_prop_head_fwd", "ironav_prop_loss",
     "ironav_prop_head_bwd", "ironav_prop_adam", "ironav_prop_weights", "ironav_set_learned",
     "ironav_prop_propose", "ironav_set_replay_form", "ironav_prop_head_pack", "ironav_prop_head_fwd_packed",
+    "ironav_set_entropy",
 )
 
 # ironav_batch_tuning (include/ironav_inter.h): the batched step's knobs
@@ -145,7 +146,7 @@ BATCH_TUNING_DTYPE = np.dtype([("k2_ctas_per_sm", "<i4"), ("k1_tile_rows", "<i4"
 
 # ironav_stream_params (include/ironav_inter.h): what the SPS and PPS say
 STREAM_PARAMS_DTYPE = np.dtype([("width", "<i4"), ("height", "<i4"), ("bd", "<i4"), ("fps_num", "<i4"), ("fps_den", "<i4"),
-                                ("refs", "<i4")])
+                                ("refs", "<i4"), ("cabac", "<i4"), ("transform8", "<i4")])
 
 SCENE_CUT = 0.8  # codec/change.rs:6
 
@@ -256,6 +257,8 @@ def _declare(lib: ctypes.CDLL) -> ctypes.CDLL:
         lib.ironav_write_parameter_sets.argtypes = [_VP, _VP, ctypes.c_size_t, _SZ]
         lib.ironav_write_slices.argtypes = [_VP, _I, _I, _I, _VP, _VP, ctypes.c_size_t, _SZ]
         lib.ironav_write_slices_device.argtypes = [_VP, _I, _I, _I, _VP, _VP, ctypes.c_size_t, _SZ]
+    if hasattr(lib, "ironav_set_entropy"):
+        lib.ironav_set_entropy.argtypes = [_VP, _I, _I]
     if hasattr(lib, "ironav_analyse_auto_noalloc"):
         # (d_src, src_stride, d_ref, ref_stride, ref_w, ref_h, d_col, width, height, nslices, qp_prime, lambda,
         #  skip_thresh, fast, sub8, d_planes, d_states, d_results, stream)
@@ -524,6 +527,11 @@ class InterStage:
         self._check(self.lib.ironav_decide_p_picture(self.ctx, _ptr(states), _ptr(codes), _ptr(y), y.shape[1], _ptr(cb), _ptr(cr),
                                                      cb.shape[1]), "ironav_decide_p_picture")
         return states, codes, (y, cb, cr)
+
+    def set_entropy(self, cabac: bool, transform8: bool = True) -> None:
+        """CABAC (with rate-distortion decisions, and the 8x8 transform when transform8) or CAVLC for the
+        decide and write entry points (H264Encoder's cabac and transform8 settings)."""
+        self._check(self.lib.ironav_set_entropy(self.ctx, int(cabac), int(transform8)), "ironav_set_entropy")
 
     def begin_i_picture(self, qp_prime: int, fast: bool = False) -> None:
         """Parameters of an IDR picture (FrameCoder::new without a reference, enc/frame.rs:381-412)."""
@@ -822,11 +830,12 @@ def _sized_call(fn, what: str, guess: int) -> bytes:
 
 
 def write_parameter_sets(width: int, height: int, bd: int = 8, fps: tuple[int, int] = (30, 1), refs: int = 1,
-                         lib: ctypes.CDLL | None = None) -> bytes:
-    """The SPS and PPS NAL units (Annex B) of a CAVLC stream (H264Encoder::sps / pps, enc/mod.rs:296-400)."""
+                         lib: ctypes.CDLL | None = None, cabac: bool = False, transform8: bool = False) -> bytes:
+    """The SPS and PPS NAL units (Annex B) of a stream without B pictures (H264Encoder::sps / pps,
+    enc/mod.rs:296-400): CAVLC, or CABAC with or without the 8x8 transform."""
     lib = lib if lib is not None else cuda_library()
     p = np.zeros(1, dtype=STREAM_PARAMS_DTYPE)
-    p[0] = (width, height, bd, fps[0], fps[1], refs)
+    p[0] = (width, height, bd, fps[0], fps[1], refs, int(cabac), int(transform8))
     return _sized_call(lambda buf, cap, n: lib.ironav_write_parameter_sets(_ptr(p), buf, cap, n), "ironav_write_parameter_sets", 256)
 
 

@@ -315,6 +315,7 @@ struct ironav_ctx {
     /* picture parameters */
     int qpp, lambda, skip_thresh, nact, fast, sub8;
     int intra_pic; /* the picture parameters are an IDR picture's (ironav_begin_i_picture) */
+    int cabac, t8; /* entropy coding: CABAC, and transform_8x8_mode_flag with it (ironav_set_entropy) */
     int threads;
     void* inloop; /* in-loop mode state */
     /* B picture parameters */
@@ -2287,7 +2288,10 @@ int ironav_code_inter_picture_device(ironav_ctx* c, int qp, const ironav_interde
  * The P macroblock decision (decide mode): code_mb without CABAC, enc/frame.rs:715-790
  * ------------------------------------------------------------------------------------------------- */
 
-enum { KIND_I4 = 1, KIND_I16 = 3, KIND_INTER = 5 }; /* Kind, h264/mb.rs:21-30 */
+enum { KIND_I4 = 1, KIND_I8 = 2, KIND_I16 = 3, KIND_INTER = 5 }; /* Kind, h264/mb.rs:21-30 */
+
+/* MbState::i4, enc/frame.rs:2309: Intra4x4 and Intra8x8 macroblocks give their prediction modes */
+static int kind_nxn(int kind) { return kind == KIND_I4 || kind == KIND_I8; }
 
 /* Edges, h264/intra.rs:17-26 (a 4x4 block: 8 samples above, 4 to the left) */
 typedef struct i_edges { int top[8], left[4], topleft, have_top, have_left, have_topleft; } i_edges;
@@ -2493,12 +2497,12 @@ static int pred_i4_mode(const dctx* D, const uint8_t cur[16], int mbx, int mby, 
     if (bx > 0) a = cur[by * 4 + bx - 1];
     else {
         long i = nb_index(D->f, mbx - 1, mby, mby);
-        if (i >= 0) a = D->codes[i].kind == KIND_I4 ? D->codes[i].modes[by * 4 + 3] : 2;
+        if (i >= 0) a = kind_nxn(D->codes[i].kind) ? D->codes[i].modes[by * 4 + 3] : 2;
     }
     if (by > 0) b = cur[(by - 1) * 4 + bx];
     else {
         long i = nb_index(D->f, mbx, mby - 1, mby);
-        if (i >= 0) b = D->codes[i].kind == KIND_I4 ? D->codes[i].modes[12 + bx] : 2;
+        if (i >= 0) b = kind_nxn(D->codes[i].kind) ? D->codes[i].modes[12 + bx] : 2;
     }
     return (a >= 0 && b >= 0) ? mini(a, b) : 2;
 }
@@ -2690,9 +2694,9 @@ static void part_mvps(const fc* f, int mbx, int mby, int part, const uint8_t sub
     }
 }
 
-/* code_inter, enc/frame.rs:1202-1215, with the 4x4 transform */
+/* code_inter, enc/frame.rs:1202-1215, with the 4x4 transform, or the 8x8 transform when t8 */
 static void d_code_inter(const dctx* D, int mbx, int mby, int part, const uint8_t sub[4], const uint8_t refs[4], const int16_t mvs[16][2],
-                         ironav_mbcode* code) {
+                         int t8, ironav_mbcode* code) {
     const struct ironav_ctx* c = D->f->c;
     code_new(code, KIND_INTER);
     code->part = (uint8_t)part;
@@ -2706,6 +2710,7 @@ static void d_code_inter(const dctx* D, int mbx, int mby, int part, const uint8_
     ironav_interdec d;
     memset(&d, 0, sizeof(d));
     d.mode = 2;
+    d.t8 = (uint8_t)(t8 != 0);
     d.part = (uint8_t)part;
     memcpy(d.sub, sub, 4);
     memcpy(d.refs, refs, 4);
@@ -2729,14 +2734,14 @@ static void d_state(const ironav_mbcode* code, ironav_mbstate* s) {
     state_from_result(&r, 0, s);
 }
 
-/* code_mb for a P macroblock without CABAC, enc/frame.rs:715-790 */
-static void decide_mb(const dctx* D, int mbx, int mby, ironav_mbcode* code, ironav_mbstate* st) {
+/* code_mb's P_Skip tests, enc/frame.rs:722-751: the fast one on luma and chroma SADs (live coding), then
+ * code_inter with the skip vector when its SAD is under the threshold. Returns 1 when the macroblock is
+ * P_Skip (code and reconstruction done), else 0 with the skip vector in sv. */
+static int skip_tests(const dctx* D, int mbx, int mby, int sv[2], ironav_mbcode* code) {
     const fc* f = D->f;
     const struct ironav_ctx* c = f->c;
-    int x0 = mbx * 16, y0 = mby * 16, lam = c->lambda, cw = c->mb_w * 8;
+    int x0 = mbx * 16, y0 = mby * 16, cw = c->mb_w * 8;
     static const uint8_t zero4[4] = {0, 0, 0, 0};
-    /* P_Skip first (722-751) */
-    int sv[2];
     skip_mv(f, mbx, mby, sv);
     uint16_t pred[256];
     halfpel_predict(&c->refs[0].hp, x0, y0, sv[0], sv[1], 16, 16, pred);
@@ -2760,17 +2765,28 @@ static void decide_mb(const dctx* D, int mbx, int mby, ironav_mbcode* code, iron
             for (int i = 0; i < 256; i++) D->rec[0][(size_t)(y0 + i / 16) * c->pw + x0 + i % 16] = pred[i]; /* put_pred, 1397-1403 */
             for (int cc = 0; cc < 2; cc++)
                 for (int i = 0; i < 64; i++) D->rec[1 + cc][(size_t)(mby * 8 + i / 8) * cw + mbx * 8 + i % 8] = cp[cc][i];
-            d_state(code, st);
-            return;
+            return 1;
         }
     }
     if (sad < c->skip_thresh) {
-        d_code_inter(D, mbx, mby, 0, zero4, zero4, smv, code);
+        d_code_inter(D, mbx, mby, 0, zero4, zero4, smv, 0, code);
         if (code->res.cbp == 0) {
             code->skip = 1;
-            d_state(code, st);
-            return;
+            return 1;
         }
+    }
+    return 0;
+}
+
+/* code_mb for a P macroblock without CABAC, enc/frame.rs:715-790 */
+static void decide_mb(const dctx* D, int mbx, int mby, ironav_mbcode* code, ironav_mbstate* st) {
+    const fc* f = D->f;
+    const struct ironav_ctx* c = f->c;
+    int lam = c->lambda;
+    int sv[2];
+    if (skip_tests(D, mbx, mby, sv, code)) {
+        d_state(code, st);
+        return;
     }
     int i16m, i16c;
     best_i16(D, mbx, mby, &i16m, &i16c);
@@ -2790,7 +2806,7 @@ static void decide_mb(const dctx* D, int mbx, int mby, ironav_mbcode* code, iron
         }
     }
     if (r.cost <= best_intra) {
-        d_code_inter(D, mbx, mby, r.part, r.sub, r.refs, (const int16_t(*)[2])r.mvs, code);
+        d_code_inter(D, mbx, mby, r.part, r.sub, r.refs, (const int16_t(*)[2])r.mvs, 0, code);
         if (code->res.cbp == 0 && r.part == 0 && r.mvs[0][0] == sv[0] && r.mvs[0][1] == sv[1] && r.refs[0] == 0) code->skip = 1;
         d_state(code, st);
         return;
@@ -2808,6 +2824,8 @@ static void fast_thresholds(int qpp, int* luma, int* chroma) {
     *luma = (int)ceil(256.0 * 0.05 * step);
     *chroma = (int)ceil(128.0 * 0.05 * step);
 }
+
+static void decide_band_cabac(const dctx* D, int row0, int row1);
 
 int ironav_decide_p_picture(ironav_ctx* c, ironav_mbstate* states, ironav_mbcode* codes, void* rec_y, int ys, void* rec_cb, void* rec_cr,
                             int cs) {
@@ -2838,12 +2856,17 @@ int ironav_decide_p_picture(ironav_ctx* c, ironav_mbstate* states, ironav_mbcode
 #ifdef _OPENMP
 #pragma omp parallel for schedule(dynamic, 1) num_threads(c->threads)
 #endif
-    for (int b = 0; b < nb; b++)
+    for (int b = 0; b < nb; b++) {
+        if (c->cabac) {
+            decide_band_cabac(&D, starts[b], starts[b + 1]);
+            continue;
+        }
         for (int mby = starts[b]; mby < starts[b + 1]; mby++)
             for (int mbx = 0; mbx < c->mb_w; mbx++) {
                 size_t i = (size_t)mby * c->mb_w + mbx;
                 decide_mb(&D, mbx, mby, &codes[i], &states[i]);
             }
+    }
     dbk_copy_out(rec_y, D.rec[0], B, ys, c->pw, c->ph);
     dbk_copy_out(rec_cb, D.rec[1], B, cs, cw, ch);
     dbk_copy_out(rec_cr, D.rec[2], B, cs, cw, ch);
@@ -2966,12 +2989,17 @@ int ironav_decide_i_picture(ironav_ctx* c, ironav_mbstate* states, ironav_mbcode
 #ifdef _OPENMP
 #pragma omp parallel for schedule(dynamic, 1) num_threads(c->threads)
 #endif
-    for (int b = 0; b < nb; b++)
+    for (int b = 0; b < nb; b++) {
+        if (c->cabac) {
+            decide_band_cabac(&D, starts[b], starts[b + 1]);
+            continue;
+        }
         for (int mby = starts[b]; mby < starts[b + 1]; mby++)
             for (int mbx = 0; mbx < c->mb_w; mbx++) {
                 size_t i = (size_t)mby * c->mb_w + mbx;
                 decide_i_mb(&D, mbx, mby, flat_t, &codes[i], &states[i]);
             }
+    }
     dbk_copy_out(rec_y, D.rec[0], B, ys, c->pw, c->ph);
     dbk_copy_out(rec_cb, D.rec[1], B, cs, cw, ch);
     dbk_copy_out(rec_cr, D.rec[2], B, cs, cw, ch);
@@ -3218,12 +3246,12 @@ static int w_pred_i4(const swr* s, const uint8_t cur[16], int mbx, int mby, int 
     if (bx > 0) a = cur[by * 4 + bx - 1];
     else {
         const ironav_mbcode* n = w_nb(s, mbx - 1, mby);
-        if (n) a = n->kind == KIND_I4 ? n->modes[by * 4 + 3] : 2;
+        if (n) a = kind_nxn(n->kind) ? n->modes[by * 4 + 3] : 2;
     }
     if (by > 0) b = cur[(by - 1) * 4 + bx];
     else {
         const ironav_mbcode* n = w_nb(s, mbx, mby - 1);
-        if (n) b = n->kind == KIND_I4 ? n->modes[12 + bx] : 2;
+        if (n) b = kind_nxn(n->kind) ? n->modes[12 + bx] : 2;
     }
     return (a >= 0 && b >= 0) ? mini(a, b) : 2;
 }
@@ -3330,6 +3358,8 @@ static int bands_of(const struct ironav_ctx* c, int starts[1025]) {
     return nb;
 }
 
+static void write_band_cabac(const struct ironav_ctx* c, const ironav_mbcode* codes, int row0, int row1, bitw* w);
+
 /* The picture's slices: header (enc/mod.rs:566-600), macroblocks in raster order (FrameCoder::encode,
  * enc/frame.rs:452-487), trailing skip run and rbsp bits; each a NAL unit of nal_ref_idc 3, type 5 (IDR) or
  * 1 (enc/mod.rs:641-643). */
@@ -3369,11 +3399,15 @@ int ironav_write_slices(ironav_ctx* c, int idr, int frame_num, int idr_pic_id, c
             bw_flag(w, 0); /* no_output_of_prior_pics_flag */
             bw_flag(w, 0); /* long_term_reference_flag */
         } else bw_flag(w, 0); /* adaptive_ref_pic_marking_mode_flag */
+        if (c->cabac && !idr) bw_ue(w, 0); /* cabac_init_idc */
         bw_se(w, qp - 26);    /* slice_qp_delta */
-        for (int mby = starts[b]; mby < starts[b + 1]; mby++)
-            for (int mbx = 0; mbx < c->mb_w; mbx++) write_mb(&s, &codes[(size_t)mby * c->mb_w + mbx], mbx, mby);
-        if (s.skip_run > 0) bw_ue(w, s.skip_run);
-        bw_finish(w);
+        if (c->cabac) write_band_cabac(c, codes, starts[b], starts[b + 1], w);
+        else {
+            for (int mby = starts[b]; mby < starts[b + 1]; mby++)
+                for (int mbx = 0; mbx < c->mb_w; mbx++) write_mb(&s, &codes[(size_t)mby * c->mb_w + mbx], mbx, mby);
+            if (s.skip_run > 0) bw_ue(w, s.skip_run);
+            bw_finish(w);
+        }
         put_nal(&stream, 3, idr ? 5 : 1, w->buf, w->len);
         free(w->buf);
     }
@@ -3398,7 +3432,7 @@ static const int64_t LEVELS_A1[19][3] = {{10, 99, 1485},      {11, 396, 3000},  
                                          {42, 8704, 522240},  {50, 22080, 589824},  {51, 36864, 983040},   {52, 36864, 2073600},
                                          {60, 139264, 4177920}, {61, 139264, 8355840}, {62, 139264, 16711680}};
 
-/* H264Encoder::sps / pps for the CAVLC encoder (enc/mod.rs:296-400) and the level choice (154-157) */
+/* H264Encoder::sps / pps without B pictures (enc/mod.rs:296-400) and the level choice (154-157) */
 int ironav_write_parameter_sets(const ironav_stream_params* p, uint8_t* out, size_t cap, size_t* len) {
     if (!p || !len || p->width <= 0 || p->height <= 0 || (p->width & 1) || (p->height & 1) || (p->bd != 8 && p->bd != 10) || p->refs < 1 ||
         p->refs > 16)
@@ -3415,12 +3449,19 @@ int ironav_write_parameter_sets(const ironav_stream_params* p, uint8_t* out, siz
     for (int i = 0; i < 19 && level < 0; i++)
         if (LEVELS_A1[i][1] >= fs) level = (int)LEVELS_A1[i][0];
     if (level < 0) level = 62;
-    int high = p->bd > 8;
+    if (p->cabac < 0 || p->cabac > 1 || p->transform8 < 0 || p->transform8 > 1) return IRONAV_INVALID_ARGUMENT;
+    int t8 = p->cabac && p->transform8, high = t8 || p->bd > 8;
     bitw w;
     bw_init(&w);
-    if (high) {
+    if (p->bd > 8) {
         bw_put(&w, 8, 110); /* High 10 */
         bw_put(&w, 8, 0);
+    } else if (high) {
+        bw_put(&w, 8, 100); /* High */
+        bw_put(&w, 8, 0);
+    } else if (p->cabac) {
+        bw_put(&w, 8, 77);   /* Main */
+        bw_put(&w, 8, 0x40); /* constraint_set1: Main */
     } else {
         bw_put(&w, 8, 66);          /* Baseline */
         bw_put(&w, 8, 0xC0);        /* constraint_set0 and constraint_set1: Constrained Baseline */
@@ -3478,7 +3519,7 @@ int ironav_write_parameter_sets(const ironav_stream_params* p, uint8_t* out, siz
     bw_init(&pps);
     bw_ue(&pps, 0);      /* pic_parameter_set_id */
     bw_ue(&pps, 0);      /* seq_parameter_set_id */
-    bw_flag(&pps, 0);    /* entropy_coding_mode_flag: CAVLC */
+    bw_flag(&pps, p->cabac); /* entropy_coding_mode_flag */
     bw_flag(&pps, 0);    /* bottom_field_pic_order_in_frame_present_flag */
     bw_ue(&pps, 0);      /* num_slice_groups_minus1 */
     bw_ue(&pps, 0);      /* num_ref_idx_l0_default_active_minus1 */
@@ -3491,6 +3532,11 @@ int ironav_write_parameter_sets(const ironav_stream_params* p, uint8_t* out, siz
     bw_flag(&pps, 0);    /* deblocking_filter_control_present_flag */
     bw_flag(&pps, 0);    /* constrained_intra_pred_flag */
     bw_flag(&pps, 0);    /* redundant_pic_cnt_present_flag */
+    if (t8) {
+        bw_flag(&pps, 1); /* transform_8x8_mode_flag */
+        bw_flag(&pps, 0); /* pic_scaling_matrix_present_flag */
+        bw_se(&pps, 0);   /* second_chroma_qp_index_offset */
+    }
     bw_finish(&pps);
     bitw stream;
     bw_init(&stream);
@@ -3577,4 +3623,789 @@ int ironav_prop_head_fwd_packed(const void* f, int n, const float* hwt, const fl
 int ironav_prop_propose(const float* o, int n, float min_conf, int16_t* c, uint8_t* k, void* s) {
     (void)o; (void)n; (void)min_conf; (void)c; (void)k; (void)s;
     return IRONAV_HARDWARE_UNAVAILABLE;
+}
+
+/* ==== High profile: CABAC and rate-distortion decisions (the encoder's default entropy coding) ==== */
+
+#include "cabac_tables.h"
+
+int ironav_set_entropy(ironav_ctx* c, int cabac, int transform8) {
+    if (!c || cabac < 0 || cabac > 1 || transform8 < 0 || transform8 > 1) return IRONAV_INVALID_ARGUMENT;
+    c->cabac = cabac;
+    c->t8 = cabac && transform8; /* FrameCoder::new, enc/frame.rs:405: transform8 with CABAC only */
+    return IRONAV_OK;
+}
+
+/* Bins, enc/cabac.rs:10-30: the arithmetic coder (CabacWriter, 42-147: w set) or the bit counter (CabacCost,
+ * 150-192: w NULL). Both adapt their own contexts the same way. */
+typedef struct cab {
+    uint8_t st[1024]; /* per context: pStateIdx * 2 + valMPS */
+    uint32_t bits;    /* the counter's total, 1/256 bits */
+    bitw* w;
+    uint32_t low, range, outstanding;
+    int first;
+} cab;
+
+/* entropy(), enc/cabac.rs:162-173: -log2 of the MPS and LPS probabilities per pStateIdx in 1/256 bits, with
+ * pLPS = 0.5 * (0.01875 / 0.5)^(p / 63) */
+static uint32_t CAB_ENTROPY[64][2];
+
+__attribute__((constructor)) static void cab_entropy_init(void) {
+    for (int p = 0; p < 64; p++) {
+        double lps = 0.5 * pow(0.01875 / 0.5, (double)p / 63.0);
+        CAB_ENTROPY[p][0] = (uint32_t)round(-log2(1.0 - lps) * 256.0);
+        CAB_ENTROPY[p][1] = (uint32_t)round(-log2(lps) * 256.0);
+    }
+}
+
+/* the contexts of a slice, CabacWriter::new, enc/cabac.rs:54-64 (9.3.1.1) */
+static void cab_states(uint8_t st[1024], int intra, int idc, int slice_qp) {
+    int qp = clampi(slice_qp, 0, 51);
+    for (int i = 0; i < 1024; i++) {
+        int m = intra ? CABAC_INIT_I[i][0] : CABAC_INIT_PB[idc][i][0];
+        int n = intra ? CABAC_INIT_I[i][1] : CABAC_INIT_PB[idc][i][1];
+        int pre = clampi(((m * qp) >> 4) + n, 1, 126);
+        st[i] = (uint8_t)(pre <= 63 ? (63 - pre) << 1 : ((pre - 64) << 1) | 1);
+    }
+}
+
+/* next_state, enc/cabac.rs:32-40 */
+static uint8_t cab_next(uint8_t s, int bin) {
+    int p = s >> 1, mps = s & 1;
+    if (bin != mps) return (uint8_t)((TRANS_LPS[p] << 1) | (p == 0 ? !mps : mps));
+    return (uint8_t)(((p < 62 ? p + 1 : p) << 1) | mps);
+}
+
+/* put_bit and renorm, enc/cabac.rs:70-97 (9.3.4.2) */
+static void cab_put_bit(cab* c, uint32_t b) {
+    if (c->first) c->first = 0;
+    else bw_put(c->w, 1, b);
+    for (; c->outstanding > 0; c->outstanding--) bw_put(c->w, 1, 1 - b);
+}
+
+static void cab_renorm(cab* c) {
+    while (c->range < 256) {
+        if (c->low < 256) cab_put_bit(c, 0);
+        else if (c->low >= 512) {
+            c->low -= 512;
+            cab_put_bit(c, 1);
+        } else {
+            c->low -= 256;
+            c->outstanding++;
+        }
+        c->range <<= 1;
+        c->low <<= 1;
+    }
+}
+
+/* decision, enc/cabac.rs:105-116 (coder) and 176-180 (counter) */
+static void cab_decision(cab* c, int ctx, int bin) {
+    uint8_t s = c->st[ctx];
+    int p = s >> 1, mps = s & 1;
+    bin = bin != 0;
+    c->st[ctx] = cab_next(s, bin);
+    if (!c->w) {
+        c->bits += CAB_ENTROPY[p][bin != mps];
+        return;
+    }
+    uint32_t lps = LPS_RANGE[p][(c->range >> 6) & 3];
+    c->range -= lps;
+    if (bin != mps) {
+        c->low += c->range;
+        c->range = lps;
+    }
+    cab_renorm(c);
+}
+
+/* bypass, enc/cabac.rs:118-132 and 182-184 */
+static void cab_bypass(cab* c, int bin) {
+    if (!c->w) {
+        c->bits += 256;
+        return;
+    }
+    c->low <<= 1;
+    if (bin) c->low += c->range;
+    if (c->low >= 1024) {
+        cab_put_bit(c, 1);
+        c->low -= 1024;
+    } else if (c->low < 512) cab_put_bit(c, 0);
+    else {
+        c->low -= 512;
+        c->outstanding++;
+    }
+}
+
+/* terminate, enc/cabac.rs:134-146 and 186-188: end_of_slice_flag, or the I_PCM test of an intra mb_type */
+static void cab_terminate(cab* c, int bin) {
+    if (!c->w) {
+        c->bits += bin ? 7 * 256 : 1;
+        return;
+    }
+    c->range -= 2;
+    if (bin) {
+        c->low += c->range;
+        c->range = 2;
+        cab_renorm(c);
+        cab_put_bit(c, (c->low >> 9) & 1);
+        bw_put(c->w, 2, ((c->low >> 7) & 3) | 1); /* the last of the two bits is the rbsp_stop_one_bit */
+    } else cab_renorm(c);
+}
+
+/* exp_golomb, enc/cabac.rs:17-29: the bypass-coded k-th order Exp-Golomb suffix (9.3.2.3) */
+static void cab_egk(cab* c, uint32_t v, uint32_t k) {
+    while (v >= (1u << k)) {
+        cab_bypass(c, 1);
+        v -= 1u << k;
+        k++;
+    }
+    cab_bypass(c, 0);
+    while (k > 0) {
+        k--;
+        cab_bypass(c, (v >> k) & 1);
+    }
+}
+
+/* write_block, enc/cabac.rs:194-250: coded_block_flag (context cbf_ctx, none when < 0) and the max levels of
+ * category cat in scan order. Returns the non-zero count. */
+static int cab_block(cab* c, int cat, int cbf_ctx, const int16_t* lv, int max) {
+    int total = 0, last = -1;
+    for (int i = 0; i < max; i++)
+        if (lv[i]) {
+            total++;
+            last = i;
+        }
+    if (cbf_ctx >= 0) cab_decision(c, cbf_ctx, total > 0);
+    if (total == 0) return 0;
+    for (int i = 0; i < max - 1; i++) {
+        /* 4:2:0 chroma DC has three significance contexts, one per position; 8x8 blocks share theirs */
+        int sig = cat == 3 ? mini(i, 2) : cat == 5 ? SIG_OFF_8X8[0][i] : i;
+        int lst = cat == 3 ? mini(i, 2) : cat == 5 ? LAST_OFF_8X8[i] : i;
+        cab_decision(c, SIG_OFF[0][cat] + sig, lv[i] != 0);
+        if (lv[i]) {
+            cab_decision(c, LAST_OFF[0][cat] + lst, i == last);
+            if (i == last) break;
+        }
+    }
+    int base = ABS_OFF[cat], eq1 = 0, gt1 = 0;
+    for (int i = last; i >= 0; i--) {
+        int l = lv[i];
+        if (!l) continue;
+        uint32_t a = (uint32_t)abs(l);
+        int inc0 = gt1 ? 0 : mini(1 + eq1, 4);
+        if (a == 1) {
+            cab_decision(c, base + inc0, 0);
+            eq1++;
+        } else {
+            cab_decision(c, base + inc0, 1);
+            int incn = base + 5 + mini(gt1, 4 - (cat == 3));
+            /* abs - 2 ones and a zero, the ones capped at 13 with the rest in an Exp-Golomb suffix */
+            for (uint32_t k = 0; k < (a - 2 < 13 ? a - 2 : 13); k++) cab_decision(c, incn, 1);
+            if (a < 15) cab_decision(c, incn, 0);
+            else cab_egk(c, a - 15, 0);
+            gt1++;
+        }
+        cab_bypass(c, l < 0);
+    }
+    return total;
+}
+
+/* mvd_bins, enc/frame.rs:2393-2414: mvd_l0 of one component, sum = the neighbours' absolute differences */
+static void cab_mvd(cab* c, int comp, int d, uint32_t sum) {
+    int base = comp == 0 ? 40 : 47, inc = sum < 3 ? 0 : sum > 32 ? 2 : 1;
+    uint32_t a = (uint32_t)abs(d);
+    cab_decision(c, base + inc, a > 0);
+    if (a == 0) return;
+    int ctx = base + 3;
+    for (uint32_t k = 1; k < (a < 9 ? a : 9); k++) {
+        cab_decision(c, ctx, 1);
+        if (ctx < base + 6) ctx++;
+    }
+    if (a < 9) cab_decision(c, ctx, 0);
+    else cab_egk(c, a - 9, 3);
+    cab_bypass(c, d < 0);
+}
+
+/* What the contexts read of a neighbouring macroblock (the CABAC fields of MbState, enc/frame.rs:245-272, as
+ * finish_mb sets them, 2281-2321), from its code. */
+typedef struct cnb {
+    int skip, kind, inter, cbp, t8x8, chroma_mode, cbf_dc;
+    int8_t r8[4];        /* list 0 reference index per 8x8 block (-1 intra) */
+    uint8_t mvd[16][2];  /* absolute vector differences per 4x4 block, capped at 64 (mvd_grid, 238-241) */
+    const uint8_t* nnz;  /* coefficients per luma 4x4 block */
+    const uint8_t (*cnnz)[4];
+} cnb;
+
+static void cnb_of(const ironav_mbcode* k, cnb* n) {
+    memset(n, 0, sizeof(*n));
+    n->skip = k->skip;
+    n->kind = k->kind;
+    n->inter = k->kind == KIND_INTER;
+    n->cbp = k->res.cbp;
+    n->t8x8 = k->res.t8x8;
+    n->chroma_mode = n->inter ? 0 : k->chroma_mode;
+    int cbpc = k->res.cbp >> 4, any[3] = {0, 0, 0};
+    for (int i = 0; i < 16; i++) any[0] |= k->dc[i] != 0;
+    for (int i = 0; i < 4; i++) any[1] |= k->res.cdc[0][i] != 0, any[2] |= k->res.cdc[1][i] != 0;
+    n->cbf_dc = (k->kind == KIND_I16 && any[0]) | ((cbpc > 0 && any[1]) << 1) | ((cbpc > 0 && any[2]) << 2);
+    n->nnz = k->res.nnz;
+    n->cnnz = k->res.cnnz;
+    for (int b8 = 0; b8 < 4; b8++) n->r8[b8] = -1;
+    if (!n->inter) return;
+    /* spread of the partitions' indices, enc/frame.rs:185-196,2301-2302 */
+    for (int b8 = 0; b8 < 4; b8++)
+        n->r8[b8] = (int8_t)k->refs[k->part == 0 ? 0 : k->part == 1 ? b8 >> 1 : k->part == 2 ? b8 & 1 : b8];
+    if (k->skip) return;
+    rect4 rs[16];
+    int nr = rects(k->part, k->sub, rs);
+    for (int q = 0; q < nr; q++)
+        for (int by = rs[q].y; by < rs[q].y + rs[q].h; by++)
+            for (int bx = rs[q].x; bx < rs[q].x + rs[q].w; bx++)
+                for (int comp = 0; comp < 2; comp++) n->mvd[by * 4 + bx][comp] = (uint8_t)mini(abs(k->mvds[q][comp]), 64);
+}
+
+/* What mb_bins reads besides the macroblock's own code: the picture's codes so far (its neighbours) and
+ * the slice's parameters. */
+typedef struct cabx {
+    const struct ironav_ctx* c;
+    const ironav_mbcode* codes;
+    int first_row;       /* the slice band's first macroblock row */
+    int p_slice, t8, nref;
+} cabx;
+
+/* nb_state, enc/frame.rs:509-515: a neighbour in the same slice, or NULL */
+static const ironav_mbcode* cx_nb(const cabx* X, int mbx, int mby) {
+    if (mbx < 0 || mby < X->first_row || mbx >= X->c->mb_w || mby >= X->c->mb_h) return NULL;
+    return &X->codes[(size_t)mby * X->c->mb_w + mbx];
+}
+
+/* pred_i4_mode, enc/frame.rs:619-627 */
+static int cx_pred_mode(const cabx* X, const uint8_t cur[16], int mbx, int mby, int bx, int by) {
+    int a = -1, b = -1;
+    if (bx > 0) a = cur[by * 4 + bx - 1];
+    else {
+        const ironav_mbcode* n = cx_nb(X, mbx - 1, mby);
+        if (n) a = kind_nxn(n->kind) ? n->modes[by * 4 + 3] : 2;
+    }
+    if (by > 0) b = cur[(by - 1) * 4 + bx];
+    else {
+        const ironav_mbcode* n = cx_nb(X, mbx, mby - 1);
+        if (n) b = kind_nxn(n->kind) ? n->modes[12 + bx] : 2;
+    }
+    return (a >= 0 && b >= 0) ? mini(a, b) : 2;
+}
+
+/* mb_bins, enc/frame.rs:2028-2279, for I and P slices: the bins of a macroblock up to end_of_slice_flag,
+ * with the contexts of 9.3.3.1.1 and 9.3.3.1.3 from its neighbours in the slice */
+static void mb_bins(cab* c, const cabx* X, const ironav_mbcode* code, int mbx, int mby) {
+    const ironav_mbcode* lk = cx_nb(X, mbx - 1, mby);
+    const ironav_mbcode* tk = cx_nb(X, mbx, mby - 1);
+    cnb L, T;
+    if (lk) cnb_of(lk, &L);
+    if (tk) cnb_of(tk, &T);
+    const cnb* l = lk ? &L : NULL;
+    const cnb* t = tk ? &T : NULL;
+    if (X->p_slice) {
+        cab_decision(c, 11 + (l && !l->skip) + (t && !t->skip), code->skip);
+        if (code->skip) return;
+    }
+    int kind = code->kind, cbp = code->res.cbp, cbpl = cbp & 15, cbpc = cbp >> 4;
+    /* mb_type */
+    if (kind == KIND_INTER) {
+        /* P_L0_16x16 000, P_L0_L0_16x8 011, P_L0_L0_8x16 010, P_8x8 001 */
+        static const int B1[4] = {0, 1, 1, 0}, B2[4] = {0, 1, 0, 1};
+        cab_decision(c, 14, 0);
+        cab_decision(c, 15, B1[code->part]);
+        cab_decision(c, B1[code->part] ? 17 : 16, B2[code->part]);
+    } else {
+        int pre = X->p_slice, base = pre ? 17 : 3, first;
+        if (pre) {
+            cab_decision(c, 14, 1);
+            first = 17;
+        } else first = 3 + (l && !kind_nxn(l->kind)) + (t && !kind_nxn(t->kind));
+        if (kind_nxn(kind)) {
+            cab_decision(c, first, 0);
+            if (X->t8) cab_decision(c, 399 + (l && l->t8x8) + (t && t->t8x8), kind == KIND_I8);
+        } else {
+            cab_decision(c, first, 1);
+            cab_terminate(c, 0); /* not I_PCM */
+            int b1 = pre ? base + 1 : base + 3, b2 = pre ? base + 2 : base + 4, b3 = pre ? base + 3 : base + 6;
+            cab_decision(c, b1, cbpl != 0);
+            cab_decision(c, b2, cbpc != 0);
+            if (cbpc) cab_decision(c, pre ? base + 2 : base + 5, cbpc == 2);
+            cab_decision(c, b3, (code->i16_mode >> 1) == 1);
+            cab_decision(c, pre ? base + 3 : base + 7, code->i16_mode & 1);
+        }
+    }
+    if (kind_nxn(kind)) {
+        int t8 = kind == KIND_I8;
+        uint8_t so_far[16];
+        memset(so_far, 2, sizeof(so_far));
+        for (int n = 0; n < (t8 ? 4 : 16); n++) {
+            int bx = t8 ? (n & 1) * 2 : ((n >> 2) & 1) * 2 + (n & 1), by = t8 ? (n >> 1) * 2 : ((n >> 3) & 1) * 2 + ((n >> 1) & 1);
+            int mode = code->modes[by * 4 + bx];
+            int pred = cx_pred_mode(X, so_far, mbx, mby, bx, by);
+            so_far[by * 4 + bx] = (uint8_t)mode;
+            if (t8) so_far[by * 4 + bx + 1] = so_far[(by + 1) * 4 + bx] = so_far[(by + 1) * 4 + bx + 1] = (uint8_t)mode;
+            cab_decision(c, 68, mode == pred);
+            if (mode != pred) {
+                int rem = mode < pred ? mode : mode - 1;
+                for (int k = 0; k < 3; k++) cab_decision(c, 69, (rem >> k) & 1);
+            }
+        }
+    }
+    if (kind != KIND_INTER) {
+        int m = code->chroma_mode;
+        cab_decision(c, 64 + (l && !l->inter && l->chroma_mode != 0) + (t && !t->inter && t->chroma_mode != 0), m > 0);
+        if (m > 0) {
+            cab_decision(c, 67, m > 1);
+            if (m > 1) cab_decision(c, 67, m > 2);
+        }
+    } else {
+        /* sub_mb_type of each 8x8 block of P_8x8 (Table 9-38: 1, 00, 011, 010; contexts 21 to 23) */
+        if (code->part == 3)
+            for (int k = 0; k < 4; k++) {
+                int s = code->sub[k];
+                if (s == 0) cab_decision(c, 21, 1);
+                else if (s == 1) {
+                    cab_decision(c, 21, 0);
+                    cab_decision(c, 22, 0);
+                } else {
+                    cab_decision(c, 21, 0);
+                    cab_decision(c, 22, 1);
+                    cab_decision(c, 23, s == 2);
+                }
+            }
+        /* ref_idx_l0 per partition (per 8x8 block for P_8x8), unary, with the contexts of 9.3.3.1.1.6 */
+        if (X->nref > 1) {
+            uint8_t grid[4] = {0, 0, 0, 0};
+            static const int P4[4][4][4] = {{{0, 0, 4, 4}}, {{0, 0, 4, 2}, {0, 2, 4, 2}}, {{0, 0, 2, 4}, {2, 0, 2, 4}},
+                                            {{0, 0, 2, 2}, {2, 0, 2, 2}, {0, 2, 2, 2}, {2, 2, 2, 2}}};
+            static const int NP[4] = {1, 2, 2, 4};
+            for (int k = 0; k < NP[code->part]; k++) {
+                int bx = P4[code->part][k][0], by = P4[code->part][k][1], w = P4[code->part][k][2], h = P4[code->part][k][3];
+                int a = bx > 0 ? grid[(by / 2) * 2 + (bx - 1) / 2] > 0 : (l && l->r8[(by / 2) * 2 + 1] > 0);
+                int b = by > 0 ? grid[((by - 1) / 2) * 2 + bx / 2] > 0 : (t && t->r8[2 + bx / 2] > 0);
+                int r = code->refs[k], base = 54 + a + 2 * b;
+                for (int i = 0; i <= r; i++) cab_decision(c, i == 0 ? base : i == 1 ? 58 : 59, i < r);
+                for (int y8 = by / 2; y8 <= (by + h - 1) / 2; y8++)
+                    for (int x8 = bx / 2; x8 <= (bx + w - 1) / 2; x8++) grid[y8 * 2 + x8] = code->refs[k];
+            }
+        }
+        /* mvd_l0 per partition; the blocks left of and above a partition in the macroblock belong to earlier ones */
+        cnb self;
+        cnb_of(code, &self);
+        rect4 rs[16];
+        int nr = rects(code->part, code->sub, rs);
+        for (int k = 0; k < nr; k++) {
+            int bx = rs[k].x, by = rs[k].y;
+            for (int comp = 0; comp < 2; comp++) {
+                uint32_t a = bx > 0 ? self.mvd[by * 4 + bx - 1][comp] : (l ? l->mvd[by * 4 + 3][comp] : 0);
+                uint32_t b = by > 0 ? self.mvd[(by - 1) * 4 + bx][comp] : (t ? t->mvd[12 + bx][comp] : 0);
+                cab_mvd(c, comp, code->mvds[k][comp], a + b);
+            }
+        }
+    }
+    if (kind != KIND_I16) {
+        int luma = 0;
+        for (int b8 = 0; b8 < 4; b8++) {
+            int ca = (b8 & 1) ? ((luma >> (b8 - 1)) & 1) == 0 : (l && ((l->cbp >> (b8 + 1)) & 1) == 0);
+            int cb = b8 >= 2 ? ((luma >> (b8 - 2)) & 1) == 0 : (t && ((t->cbp >> (b8 + 2)) & 1) == 0);
+            int bit = (cbpl >> b8) & 1;
+            cab_decision(c, 73 + ca + 2 * cb, bit);
+            luma |= bit << b8;
+        }
+        cab_decision(c, 77 + (l && (l->cbp >> 4) != 0) + 2 * (t && (t->cbp >> 4) != 0), cbpc != 0);
+        if (cbpc) cab_decision(c, 81 + (l && (l->cbp >> 4) == 2) + 2 * (t && (t->cbp >> 4) == 2), cbpc == 2);
+    }
+    /* transform_size_8x8_flag is absent from P_8x8 with any sub-partition smaller than 8x8 */
+    if (kind == KIND_INTER && X->t8 && cbpl && (code->part != 3 || !(code->sub[0] | code->sub[1] | code->sub[2] | code->sub[3])))
+        cab_decision(c, 399 + (l && l->t8x8) + (t && t->t8x8), code->res.t8x8);
+    if (!cbp && kind != KIND_I16) return;
+    cab_decision(c, 60, 0); /* mb_qp_delta 0, after a macroblock without a change */
+    /* an unavailable neighbour counts as a coded block for an intra macroblock */
+    int un = kind != KIND_INTER;
+#define FLAG(has, v) ((has) ? ((v) > 0) : un)
+    if (kind == KIND_I16)
+        cab_block(c, 0, 85 + FLAG(l, l ? l->cbf_dc & 1 : 0) + 2 * FLAG(t, t ? t->cbf_dc & 1 : 0), code->dc, 16);
+    int cat = kind == KIND_I16 ? 1 : 2, base = kind == KIND_I16 ? 89 : 93;
+    if (code->res.t8x8)
+        for (int i8 = 0; i8 < 4; i8++)
+            if (cbpl & (1 << i8)) cab_block(c, 5, -1, code->res.luma8[i8], 64);
+    for (int n = 0; n < 16 && !code->res.t8x8; n++) {
+        int bx = ((n >> 2) & 1) * 2 + (n & 1), by = ((n >> 3) & 1) * 2 + ((n >> 1) & 1);
+        if (!(cbpl & (1 << (n / 4)))) continue;
+        int ha = bx > 0 || l, hb = by > 0 || t;
+        int a = bx > 0 ? code->res.nnz[by * 4 + bx - 1] : (l ? l->nnz[by * 4 + 3] : 0);
+        int b = by > 0 ? code->res.nnz[(by - 1) * 4 + bx] : (t ? t->nnz[12 + bx] : 0);
+        const int16_t* blk = code->res.luma[by * 4 + bx];
+        cab_block(c, cat, base + FLAG(ha, a) + 2 * FLAG(hb, b), cat == 1 ? blk + 1 : blk, cat == 1 ? 15 : 16);
+    }
+    if (cbpc > 0)
+        for (int comp = 0; comp < 2; comp++) {
+            int m = 2 << comp;
+            cab_block(c, 3, 97 + FLAG(l, l ? l->cbf_dc & m : 0) + 2 * FLAG(t, t ? t->cbf_dc & m : 0), code->res.cdc[comp], 4);
+        }
+    if (cbpc == 2)
+        for (int comp = 0; comp < 2; comp++)
+            for (int blk = 0; blk < 4; blk++) {
+                int bx = blk & 1, by = blk >> 1;
+                const uint8_t* cur = code->res.cnnz[comp];
+                int ha = bx > 0 || l, hb = by > 0 || t;
+                int a = bx > 0 ? cur[by * 2] : (l ? l->cnnz[comp][by * 2 + 1] : 0);
+                int b = by > 0 ? cur[bx] : (t ? t->cnnz[comp][2 + bx] : 0);
+                cab_block(c, 4, 101 + FLAG(ha, a) + 2 * FLAG(hb, b), code->res.cac[comp][blk] + 1, 15);
+            }
+#undef FLAG
+}
+
+/* Edges of an 8x8 block (h264/intra.rs:17-26: 16 samples above, the second half above-right, 8 left) */
+typedef struct i_edges8 { int top[16], left[8], topleft, have_top, have_left, have_topleft; } i_edges8;
+
+/* predict_nxn for n = 8, h264/intra.rs:30-128 (ITU-T H.264 8.3.2.2) */
+static void i_pred8(int mode, const i_edges8* e, int bd, int out[64]) {
+#define T(i) ((i) < 0 ? e->topleft : e->top[(i)])
+#define L(j) ((j) < 0 ? e->topleft : e->left[(j)])
+    for (int y = 0; y < 8; y++)
+        for (int x = 0; x < 8; x++) {
+            int v;
+            switch (mode) {
+            case 0: v = T(x); break;
+            case 1: v = L(y); break;
+            case 2: {
+                int st = 0, sl = 0;
+                for (int i = 0; i < 8; i++) st += T(i), sl += L(i);
+                if (e->have_top && e->have_left) v = (st + sl + 8) >> 4;
+                else if (e->have_left) v = (sl + 4) >> 3;
+                else if (e->have_top) v = (st + 4) >> 3;
+                else v = 1 << (bd - 1);
+                break;
+            }
+            case 3: v = (x == 7 && y == 7) ? (T(14) + 3 * T(15) + 2) >> 2 : (T(x + y) + 2 * T(x + y + 1) + T(x + y + 2) + 2) >> 2; break;
+            case 4:
+                if (x > y) v = (T(x - y - 2) + 2 * T(x - y - 1) + T(x - y) + 2) >> 2;
+                else if (x < y) v = (L(y - x - 2) + 2 * L(y - x - 1) + L(y - x) + 2) >> 2;
+                else v = (T(0) + 2 * e->topleft + L(0) + 2) >> 2;
+                break;
+            case 5: {
+                int z = 2 * x - y, i = x - (y >> 1);
+                if (z >= 0 && (z & 1) == 0) v = (T(i - 1) + T(i) + 1) >> 1;
+                else if (z >= 0) v = (T(i - 2) + 2 * T(i - 1) + T(i) + 2) >> 2;
+                else if (z == -1) v = (L(0) + 2 * e->topleft + T(0) + 2) >> 2;
+                else v = (L(y - 2 * x - 1) + 2 * L(y - 2 * x - 2) + L(y - 2 * x - 3) + 2) >> 2;
+                break;
+            }
+            case 6: {
+                int z = 2 * y - x, j = y - (x >> 1);
+                if (z >= 0 && (z & 1) == 0) v = (L(j - 1) + L(j) + 1) >> 1;
+                else if (z >= 0) v = (L(j - 2) + 2 * L(j - 1) + L(j) + 2) >> 2;
+                else if (z == -1) v = (L(0) + 2 * e->topleft + T(0) + 2) >> 2;
+                else v = (T(x - 2 * y - 1) + 2 * T(x - 2 * y - 2) + T(x - 2 * y - 3) + 2) >> 2;
+                break;
+            }
+            case 7: {
+                int i = x + (y >> 1);
+                v = (y & 1) == 0 ? (T(i) + T(i + 1) + 1) >> 1 : (T(i) + 2 * T(i + 1) + T(i + 2) + 2) >> 2;
+                break;
+            }
+            default: {
+                int z = x + 2 * y, j = y + (x >> 1);
+                if (z > 13) v = L(7);
+                else if (z == 13) v = (L(6) + 3 * L(7) + 2) >> 2;
+                else if ((z & 1) == 0) v = (L(j) + L(j + 1) + 1) >> 1;
+                else v = (L(j) + 2 * L(j + 1) + L(j + 2) + 2) >> 2;
+                break;
+            }
+            }
+            out[y * 8 + x] = v;
+        }
+#undef T
+#undef L
+}
+
+/* filter_8x8_edges, h264/intra.rs:131-158 (8.3.2.2.1): the reference-sample smoothing before Intra 8x8 prediction */
+static void i_filter8(i_edges8* e) {
+    i_edges8 p = *e;
+    if (p.have_top) {
+        e->top[0] = p.have_topleft ? (p.topleft + 2 * p.top[0] + p.top[1] + 2) >> 2 : (3 * p.top[0] + p.top[1] + 2) >> 2;
+        for (int x = 1; x < 15; x++) e->top[x] = (p.top[x - 1] + 2 * p.top[x] + p.top[x + 1] + 2) >> 2;
+        e->top[15] = (p.top[14] + 3 * p.top[15] + 2) >> 2;
+    }
+    if (p.have_topleft) {
+        if (p.have_top && p.have_left) e->topleft = (p.top[0] + 2 * p.topleft + p.left[0] + 2) >> 2;
+        else if (p.have_top) e->topleft = (3 * p.topleft + p.top[0] + 2) >> 2;
+        else if (p.have_left) e->topleft = (3 * p.topleft + p.left[0] + 2) >> 2;
+    }
+    if (p.have_left) {
+        e->left[0] = p.have_topleft ? (p.topleft + 2 * p.left[0] + p.left[1] + 2) >> 2 : (3 * p.left[0] + p.left[1] + 2) >> 2;
+        for (int y = 1; y < 7; y++) e->left[y] = (p.left[y - 1] + 2 * p.left[y] + p.left[y + 1] + 2) >> 2;
+        e->left[7] = (p.left[6] + 3 * p.left[7] + 2) >> 2;
+    }
+}
+
+/* code_i8, enc/frame.rs:1307-1388: the luma of an Intra8x8 macroblock block by block into the reconstruction,
+ * each 8x8 block's mode the cheapest by SATD + lambda * (1 predicted, 4 otherwise) over the filtered edges */
+static void code_i8(const dctx* D, int mbx, int mby, ironav_mbcode* code) {
+    const struct ironav_ctx* c = D->f->c;
+    code_new(code, KIND_I8);
+    code->res.t8x8 = 1;
+    int ta = d_up(c, mby), la = mbx > 0, tla = la && ta, tra = ta && mbx + 1 < c->mb_w;
+    uint16_t* p = D->rec[0];
+    int ls = c->pw, maxv = (1 << c->bd) - 1;
+    for (int i8 = 0; i8 < 4; i8++) {
+        int bx = i8 & 1, by = i8 >> 1, x = mbx * 16 + bx * 8, y = mby * 16 + by * 8;
+        i_edges8 e;
+        memset(&e, 0, sizeof(e));
+        e.have_left = bx > 0 || la;
+        e.have_top = by > 0 || ta;
+        e.have_topleft = bx > 0 ? (by > 0 ? 1 : ta) : (by > 0 ? la : tla);
+        int have_tr = i8 == 0 ? ta : i8 == 1 ? tra : i8 == 2;
+        if (e.have_top) {
+            for (int i = 0; i < 8; i++) e.top[i] = p[(size_t)(y - 1) * ls + x + i];
+            for (int i = 8; i < 16; i++) e.top[i] = have_tr ? p[(size_t)(y - 1) * ls + x + i] : e.top[7];
+        }
+        if (e.have_left)
+            for (int j = 0; j < 8; j++) e.left[j] = p[(size_t)(y + j) * ls + x - 1];
+        if (e.have_topleft) e.topleft = p[(size_t)(y - 1) * ls + x - 1];
+        i_filter8(&e);
+        int predicted = pred_i4_mode(D, code->modes, mbx, mby, bx * 2, by * 2);
+        int bm = 2, bc = INT32_MAX, bp[64];
+        for (int mode = 0; mode < 9; mode++) {
+            int ok = (mode == 0 || mode == 3 || mode == 7) ? e.have_top
+                   : (mode == 1 || mode == 8) ? e.have_left
+                   : mode == 2 ? 1 : (e.have_top && e.have_left && e.have_topleft);
+            if (!ok) continue;
+            int pr[64], cc = c->lambda * (mode == predicted ? 1 : 4);
+            i_pred8(mode, &e, c->bd, pr);
+            for (int q = 0; q < 4; q++) {
+                int pb[16];
+                for (int r = 0; r < 4; r++)
+                    for (int k = 0; k < 4; k++) pb[r * 4 + k] = pr[((q >> 1) * 4 + r) * 8 + (q & 1) * 4 + k];
+                cc += d_satd4(D, 0, x + (q & 1) * 4, y + (q >> 1) * 4, pb);
+            }
+            if (cc < bc) {
+                bm = mode;
+                bc = cc;
+                memcpy(bp, pr, sizeof(bp));
+            }
+        }
+        int s[64], lv[64], co[64];
+        for (int k = 0; k < 64; k++) s[k] = c->src[(size_t)(y + k / 8) * c->pw + x + k % 8];
+        q_block8(s, bp, D->qp, 1, lv, co);
+        for (int k = 0; k < 64; k++) p[(size_t)(y + k / 8) * ls + x + k % 8] = (uint16_t)bp[k];
+        int n = 0;
+        for (int k = 0; k < 64; k++) {
+            code->res.luma8[i8][k] = (int16_t)lv[k];
+            n += lv[k] != 0;
+        }
+        if (n) {
+            q_idct8_add(co, p + (size_t)y * ls + x, ls, maxv);
+            code->res.cbp |= (uint8_t)(1 << i8);
+        }
+        for (int j = 0; j < 4; j++) {
+            int b = (by * 2 + (j >> 1)) * 4 + bx * 2 + (j & 1);
+            code->modes[b] = (uint8_t)bm;
+            code->res.nnz[b] = (uint8_t)n;
+        }
+    }
+}
+
+/* save_mb / restore_mb, enc/frame.rs:1406-1429: a macroblock's reconstruction, luma then Cb and Cr */
+static void save_mb(const dctx* D, int mbx, int mby, uint16_t rec[384]) {
+    const struct ironav_ctx* c = D->f->c;
+    int cs = c->mb_w * 8;
+    for (int r = 0; r < 16; r++) memcpy(rec + r * 16, D->rec[0] + (size_t)(mby * 16 + r) * c->pw + mbx * 16, 32);
+    for (int k = 0; k < 2; k++)
+        for (int r = 0; r < 8; r++) memcpy(rec + 256 + k * 64 + r * 8, D->rec[1 + k] + (size_t)(mby * 8 + r) * cs + mbx * 8, 16);
+}
+
+static void restore_mb(const dctx* D, int mbx, int mby, const uint16_t rec[384]) {
+    const struct ironav_ctx* c = D->f->c;
+    int cs = c->mb_w * 8;
+    for (int r = 0; r < 16; r++) memcpy(D->rec[0] + (size_t)(mby * 16 + r) * c->pw + mbx * 16, rec + r * 16, 32);
+    for (int k = 0; k < 2; k++)
+        for (int r = 0; r < 8; r++) memcpy(D->rec[1 + k] + (size_t)(mby * 8 + r) * cs + mbx * 8, rec + 256 + k * 64 + r * 8, 16);
+}
+
+/* ssd_mb, enc/frame.rs:1432-1449: the squared error of the macroblock's reconstruction, luma and chroma */
+static int64_t ssd_mb(const dctx* D, int mbx, int mby) {
+    const struct ironav_ctx* c = D->f->c;
+    int cs = c->mb_w * 8;
+    int64_t ssd = 0;
+    for (int i = 0; i < 256; i++) {
+        int64_t d = (int64_t)c->src[(size_t)(mby * 16 + i / 16) * c->pw + mbx * 16 + i % 16] -
+                    D->rec[0][(size_t)(mby * 16 + i / 16) * c->pw + mbx * 16 + i % 16];
+        ssd += d * d;
+    }
+    for (int k = 0; k < 2; k++)
+        for (int j = 0; j < 64; j++) {
+            int64_t d = (int64_t)c->src_c[k][(size_t)(mby * 8 + j / 8) * cs + mbx * 8 + j % 8] - D->rec[1 + k][(size_t)(mby * 8 + j / 8) * cs + mbx * 8 + j % 8];
+            ssd += d * d;
+        }
+    return ssd;
+}
+
+/* rd_cost, enc/frame.rs:1453-1457: SSD + lam2 * the bits CABAC would spend from the slice's contexts st */
+static double rd_cost(const dctx* D, const cabx* X, const uint8_t st[1024], const ironav_mbcode* code, int mbx, int mby, double lam2) {
+    cab k;
+    memcpy(k.st, st, sizeof(k.st));
+    k.bits = 0;
+    k.w = NULL;
+    mb_bins(&k, X, code, mbx, mby);
+    return (double)ssd_mb(D, mbx, mby) + lam2 * ((double)k.bits / 256.0);
+}
+
+/* decide_rd, enc/frame.rs:1462-1513: P_Skip, the best inter partitioning (and with the 8x8 transform when no
+ * 8x8 block is split), Intra16x16, Intra4x4 and Intra8x8, each coded, the one of least rate-distortion cost
+ * kept (strict '<', first wins) with its reconstruction. inter NULL: an I slice. */
+static void decide_rd(const dctx* D, const cabx* X, const uint8_t st[1024], int mbx, int mby, int i16, const ironav_mbresult* inter,
+                      ironav_mbcode* out) {
+    const struct ironav_ctx* c = D->f->c;
+    /* larger than the usual 0.85 * 2^((qp - 12) / 3): the residual decisions are not RD optimised */
+    double lam2 = 1.6 * pow(2.0, ((double)c->qpp - 12.0) / 3.0);
+    double bj = 0.0;
+    int have = 0;
+    uint16_t brec[384];
+    ironav_mbcode code;
+#define KEEP(j)                                  \
+    do {                                         \
+        double j_ = (j);                         \
+        if (!have || j_ < bj) {                  \
+            have = 1;                            \
+            bj = j_;                             \
+            *out = code;                         \
+            save_mb(D, mbx, mby, brec);          \
+        }                                        \
+    } while (0)
+    if (inter) {
+        int sv[2];
+        skip_mv(D->f, mbx, mby, sv);
+        code_new(&code, KIND_INTER);
+        code.skip = 1;
+        for (int i = 0; i < 16; i++) code.mvs[i][0] = (int16_t)sv[0], code.mvs[i][1] = (int16_t)sv[1];
+        ironav_interdec d;
+        memset(&d, 0, sizeof(d));
+        d.mode = 1; /* put_inter_pred, 1391-1394: the prediction is the reconstruction */
+        memcpy(d.mvs, code.mvs, sizeof(d.mvs));
+        q_code_inter(c, mbx, mby, D->qp_y, &d, &code.res, D->rec, c->pw, c->mb_w * 8);
+        KEEP(rd_cost(D, X, st, &code, mbx, mby, lam2));
+        const int16_t(*mvs)[2] = (const int16_t(*)[2])inter->mvs;
+        d_code_inter(D, mbx, mby, inter->part, inter->sub, inter->refs, mvs, 0, &code);
+        /* with nothing coded and the skip vector, this is P_Skip at a higher price */
+        if (!(code.res.cbp == 0 && inter->part == 0 && mvs[0][0] == sv[0] && mvs[0][1] == sv[1] && inter->refs[0] == 0))
+            KEEP(rd_cost(D, X, st, &code, mbx, mby, lam2));
+        /* the 8x8 transform needs every 8x8 block of P_8x8 to be a single 8x8 partition */
+        if (c->t8 && !(inter->sub[0] | inter->sub[1] | inter->sub[2] | inter->sub[3])) {
+            d_code_inter(D, mbx, mby, inter->part, inter->sub, inter->refs, mvs, 1, &code);
+            if (code.res.t8x8) KEEP(rd_cost(D, X, st, &code, mbx, mby, lam2)); /* else the 4x4 candidate again */
+        }
+    }
+    code_i16(D, mbx, mby, i16, &code);
+    code_intra_chroma(D, mbx, mby, &code);
+    KEEP(rd_cost(D, X, st, &code, mbx, mby, lam2));
+    /* Intra4x4 predicts from its own reconstruction, block by block, so it can overwrite the others' */
+    code_i4(D, mbx, mby, &code);
+    code_intra_chroma(D, mbx, mby, &code);
+    KEEP(rd_cost(D, X, st, &code, mbx, mby, lam2));
+    if (c->t8) {
+        code_i8(D, mbx, mby, &code);
+        code_intra_chroma(D, mbx, mby, &code);
+        KEEP(rd_cost(D, X, st, &code, mbx, mby, lam2));
+    }
+#undef KEEP
+    restore_mb(D, mbx, mby, brec);
+}
+
+/* One slice band under CABAC, in raster order (FrameCoder::encode, enc/frame.rs:461-478): code_mb (its P_Skip
+ * tests, best_i16 and best_inter, then decide_rd, 715-760) against the contexts the macroblocks before it
+ * left, then those contexts carried past its bins as write_mb_cabac moves them. */
+static void decide_band_cabac(const dctx* D, int row0, int row1) {
+    const struct ironav_ctx* c = D->f->c;
+    cab live;
+    memset(&live, 0, sizeof(live));
+    int qp_y = c->qpp - 6 * (c->bd - 8);
+    cab_states(live.st, c->intra_pic, 0, qp_y);
+    cabx X = {c, D->codes, row0, !c->intra_pic, c->t8, c->intra_pic ? 0 : c->nact};
+    ironav_mbstate* states = (ironav_mbstate*)D->f->states;
+    for (int mby = row0; mby < row1; mby++)
+        for (int mbx = 0; mbx < c->mb_w; mbx++) {
+            size_t i = (size_t)mby * c->mb_w + mbx;
+            ironav_mbcode* code = &D->codes[i];
+            int sv[2], done = 0;
+            if (!c->intra_pic) done = skip_tests(D, mbx, mby, sv, code);
+            if (!done) {
+                int i16m, i16c;
+                best_i16(D, mbx, mby, &i16m, &i16c);
+                ironav_mbresult r;
+                memset(&r, 0, sizeof(r));
+                if (!c->intra_pic) {
+                    counters cnt = {0, 0};
+                    best_inter(D->f, &cnt, mbx, mby, &r);
+                }
+                decide_rd(D, &X, live.st, mbx, mby, i16m, c->intra_pic ? NULL : &r, code);
+            }
+            d_state(code, &states[i]);
+            mb_bins(&live, &X, code, mbx, mby);
+        }
+}
+
+/* A slice band's data under CABAC (FrameCoder::encode, enc/frame.rs:461-486): cabac_alignment_one_bit, the
+ * contexts of the slice, each macroblock's bins (write_mb_cabac, 2020-2025) and end_of_slice_flag, the last
+ * byte padded with zeros (into_bytes, enc/bitw.rs:60-67). */
+static void write_band_cabac(const struct ironav_ctx* c, const ironav_mbcode* codes, int row0, int row1, bitw* w) {
+    if (w->n > 0) bw_put(w, 8 - w->n, (1u << (8 - w->n)) - 1); /* align_ones, enc/bitw.rs:52-58 */
+    cab k;
+    memset(&k, 0, sizeof(k));
+    k.w = w;
+    k.range = 510;
+    k.first = 1;
+    cab_states(k.st, c->intra_pic, 0, c->qpp - 6 * (c->bd - 8));
+    cabx X = {c, codes, row0, !c->intra_pic, c->t8, c->intra_pic ? 0 : c->nact};
+    for (int mby = row0; mby < row1; mby++)
+        for (int mbx = 0; mbx < c->mb_w; mbx++) {
+            mb_bins(&k, &X, &codes[(size_t)mby * c->mb_w + mbx], mbx, mby);
+            cab_terminate(&k, mby + 1 == row1 && mbx + 1 == c->mb_w);
+        }
+    if (w->n > 0) bw_put(w, 8 - w->n, 0);
+}
+
+/* Test hook (oracle only): the arithmetic coder on a list of bins, as the reference's coder test drives it
+ * (bins_read_back_through_the_decoder, enc/cabac.rs:252-291): 5 header bits 10110 and cabac_alignment_one_bit,
+ * the contexts of a slice (intra, idc, qp), then per op a decision (kind 0, context ctx[i]), a bypass (1) or a
+ * terminating 0 (2), then a terminating 1 and the padded last byte. Returns the byte count, or -1 when cap is
+ * too small. */
+int oracle_cabac_ops(const int* kind, const int* ctx, const int* val, int n, int intra, int idc, int qp, uint8_t* out, int cap) {
+    bitw w;
+    bw_init(&w);
+    bw_put(&w, 5, 0x16);
+    if (w.n > 0) bw_put(&w, 8 - w.n, (1u << (8 - w.n)) - 1);
+    cab k;
+    memset(&k, 0, sizeof(k));
+    k.w = &w;
+    k.range = 510;
+    k.first = 1;
+    cab_states(k.st, intra, idc, qp);
+    for (int i = 0; i < n; i++) {
+        if (kind[i] == 0) cab_decision(&k, ctx[i], val[i]);
+        else if (kind[i] == 1) cab_bypass(&k, val[i]);
+        else cab_terminate(&k, 0);
+    }
+    cab_terminate(&k, 1);
+    if (w.n > 0) bw_put(&w, 8 - w.n, 0);
+    int len = (int)w.len;
+    if (len <= cap) memcpy(out, w.buf, w.len);
+    free(w.buf);
+    return len <= cap ? len : -1;
+}
+
+/* Test hook (oracle only): the bits, in 1/256, the counter gives the same ops from the same contexts */
+uint32_t oracle_cabac_cost(const int* kind, const int* ctx, const int* val, int n, int intra, int idc, int qp) {
+    cab k;
+    memset(&k, 0, sizeof(k));
+    cab_states(k.st, intra, idc, qp);
+    for (int i = 0; i < n; i++) {
+        if (kind[i] == 0) cab_decision(&k, ctx[i], val[i]);
+        else if (kind[i] == 1) cab_bypass(&k, val[i]);
+        else cab_terminate(&k, 0);
+    }
+    return k.bits;
 }

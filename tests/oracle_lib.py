@@ -15,7 +15,7 @@ _LIB = None
 
 
 def build_oracle() -> str:
-    srcs = [os.path.join(ORACLE_DIR, f) for f in ("inter_oracle.c", "cavlc_tables.h")]
+    srcs = [os.path.join(ORACLE_DIR, f) for f in ("inter_oracle.c", "cavlc_tables.h", "cabac_tables.h")]
     if not os.path.exists(ORACLE_LIB) or any(os.path.getmtime(ORACLE_LIB) < os.path.getmtime(s) for s in srcs):
         subprocess.run(["make", "-s", "-C", ORACLE_DIR], check=True)
     return ORACLE_LIB
