@@ -353,9 +353,8 @@ __device__ __forceinline__ void rd_state(RdSmem<T>& R, int k, bool inter) {
     if (inter) {
         if (lane < 18) d[lane] = reinterpret_cast<const uint32_t*>(&R.s.a.out)[lane];
     } else {
-        if (lane < 16) d[lane] = 0;  // mvs
-        if (lane == 16) d[lane] = 0xFFFFFFFFu;  // refs -1
-        if (lane == 17) d[lane] = 0;            // inter 0
+        // inter 0, refs -1, pad 0, no motion (bytes 0-7, then the vectors)
+        if (lane < 18) d[lane] = lane == 0 ? 0xFFFFFF00u : (lane == 1 ? 0x000000FFu : 0u);
     }
     __syncwarp();
 }

@@ -119,12 +119,14 @@ class DeviceEncoder:
     the stream's bytes come back. Needs the CUDA library and torch for device buffers."""
 
     def __init__(self, width: int, height: int, qp: int, keyint: int = 250, refs: int = 1, nslices: int = 1,
-                 fps: tuple[int, int] = (30, 1), bd: int = 8, fast: bool = False, sub8: bool = False, scene_cut: bool = True):
+                 fps: tuple[int, int] = (30, 1), bd: int = 8, fast: bool = False, sub8: bool = False, scene_cut: bool = True,
+                 cabac: bool = False, transform8: bool = True):
         import torch
 
         self.torch = torch
         self.lib = cuda_library()
         self.st = InterStage(width, height, max_refs=refs, nslices=nslices, lib=self.lib, bd=bd)
+        self.st.set_entropy(cabac, transform8)
         self.loop = _Loop(width, height, qp, keyint, refs, bd, fps)
         self.fast, self.sub8, self.scene_cut = fast, sub8, scene_cut
         self.stream = torch.cuda.Stream()
@@ -142,7 +144,7 @@ class DeviceEncoder:
         self.d_mbs = torch.zeros(nmb * DBK_MB_DTYPE.itemsize, dtype=torch.uint8, device=dev)
         self.slices = np.zeros(nslices, dtype=DBK_SLICE_DTYPE)  # every slice filtered, no offsets (enc/mod.rs:648)
         self.k = 0
-        self.params = write_parameter_sets(width, height, bd, fps, refs, lib=self.lib)
+        self.params = write_parameter_sets(width, height, bd, fps, refs, lib=self.lib, cabac=cabac, transform8=transform8)
         # called as before_p(encoder, d_y, stride) once a P picture's parameters are set and before it is
         # decided, on the encoder's stream (the learned form computes its proposals there)
         self.before_p = None

@@ -215,3 +215,13 @@ def test_a_planted_decision_error_is_seen(oracle_lib, tmp_path):
     recons[2] = (y, cb, cr)
     with pytest.raises(AssertionError, match="luma differs"):
         check_stream_decodes_to(str(tmp_path), "planted_cabac", stream, recons, 96, 64)
+
+
+def test_the_cuda_library_writes_the_oracles_high_parameter_sets(oracle_lib):
+    from ironav_b200.inter import cuda_library, write_parameter_sets
+
+    cuda = cuda_library()
+    for args in ((352, 288, 8, (30, 1), 1), (1920, 1080, 8, (30, 1), 3), (200, 120, 10, (30000, 1001), 2)):
+        for cabac, t8 in ((True, True), (True, False)):
+            assert write_parameter_sets(*args, lib=cuda, cabac=cabac, transform8=t8) == \
+                write_parameter_sets(*args, lib=oracle_lib, cabac=cabac, transform8=t8), (args, cabac, t8)
