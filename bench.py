@@ -65,6 +65,9 @@ def parse():
                         "groups, 3 4-lane groups; default the library's choice for the depth (0 at 8 bits, 1 at 10)")
     p.add_argument("--learned-samples", type=int, default=2_000_000, help="training samples of the learned workload's proposer")
     p.add_argument("--e2e-threads", type=int, default=8, help="host threads (each with a context) of the e2e pass")
+    p.add_argument("--cabac", action="store_true",
+                   help="decide workload: CABAC with rate-distortion decisions and the 8x8 transform (the reference "
+                        "encoder's default entropy coding) instead of CAVLC")
     p.add_argument("--bd", type=int, default=8, choices=[8, 10],
                    help="sample depth of the 1080p workload: 8 (Yuv420p) or 10 (Yuv420p10, QP' = QP + 12)")
     return p.parse_args()
@@ -1265,7 +1268,8 @@ def run_decide_batched(args, rank, world):
     """Decide mode for many streams in one launch (ironav_batch_decide): streams with resolutions drawn
     from {640x360, 854x480, 1280x720, 1920x1080} (the batched configuration's), QP 27, one reference each;
     one step = every stream's P picture decided and coded. Compared with the per-stream loop (each
-    stream's own decide launch, one after another). Streams are split across ranks."""
+    stream's own decide launch, one after another). Streams are split across ranks. With --cabac, the
+    default encoder's decision (decide_rd under CABAC): every stream's slice bands as chains of one launch."""
     import torch
     from ironav_b200.inter import MBCODE_DTYPE, InterBatch, InterStage, cuda_library
     from ironav_b200.synth import Sequence, batch_streams
@@ -1282,6 +1286,7 @@ def run_decide_batched(args, rank, world):
         st.push_reference_chroma(*seq.chroma(0))
         st.set_source(seq.frame(1))
         st.set_source_chroma(*seq.chroma(1))
+        st.set_entropy(args.cabac, True)
         st.begin_p_picture(QP)
         st.set_stream(stream.cuda_stream)
         stages.append(st)
@@ -1391,7 +1396,8 @@ def run_decide_batched(args, rank, world):
     total = sum_over_ranks(nmb, world, dev)
     value = total * args.steps / (ms * 1e-3)
     line = {
-        "metric": "P-picture macroblock decision + coding MB/s, many streams in one launch (CAVLC code_mb)", "value": value,
+        "metric": "P-picture macroblock decision + coding MB/s, many streams in one launch "
+                  f"({'CABAC decide_rd, High' if args.cabac else 'CAVLC code_mb'})", "value": value,
         "unit": "MB/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
         "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "u8",
         "data": "synthetic: per-stream seeded value noise, pan, 8 moving rectangles, sigma 3; chroma from the 2x2 luma means",
@@ -1408,7 +1414,8 @@ def run_decide_batched(args, rank, world):
                 "d2h_bytes_per_step": sum(sum(int(t.numel()) for t in b) for b in bufs), "ms_per_step": 1e3 * el / args.steps,
                 "note": "each stream's source luma from pinned host memory (its chroma stays resident) + the launch + states, "
                         "codes and reconstructions back to pinned host memory"},
-        "roofline": {"bound": "latency", "kernel": "decide_batch_kernel", "achieved": None, "peak": None, "unit": None, "frac": None,
+        "roofline": {"bound": "latency", "kernel": "decide_rd_batch_kernel" if args.cabac else "decide_batch_kernel", "achieved": None,
+                     "peak": None, "unit": None, "frac": None,
                      "traffic": None, "ms_per_launch": float(np.median(per)),
                      "note": "many wavefronts interleaved; the per-stream loop above is the same work one stream at a time"},
         "clocks": clk,
@@ -1421,6 +1428,7 @@ def run_decide_batched(args, rank, world):
         (w, h, ns, seed) = mine[0]
         o = InterStage(w, h, nslices=ns, lib=olib)
         olib.oracle_set_threads(o.ctx, cores)
+        o.set_entropy(args.cabac, True)
         f0, c0, f1, c1 = seqs[0]
         o.push_reference(f0)
         o.push_reference_chroma(*c0)
@@ -1447,9 +1455,10 @@ def run_decide(args, rank, world):
     """The whole P macroblock decision of the CAVLC encoder at 1080p (code_mb, enc/frame.rs:715-790: P_Skip
     tests, best_i16, best_inter, the Intra4x4 trial, the coding of the chosen macroblock into the unfiltered
     reconstruction) in the device wavefront, device-resident: one step = every macroblock of one P picture.
-    A ring of contexts (reference planes and chroma, states, codes, reconstructions) larger than L2. The
-    oracle decides the same picture on all host cores (slice bands in parallel, as the reference's slice
-    threads)."""
+    With --cabac, the default encoder's decision instead (decide_rd, enc/frame.rs:1462-1513: every candidate
+    coded and the least SSD + lambda2 * CABAC bits kept), one chain per slice band. A ring of contexts
+    (reference planes and chroma, states, codes, reconstructions) larger than L2. The oracle decides the same
+    picture on all host cores (slice bands in parallel, as the reference's slice threads)."""
     import torch
     from ironav_b200.inter import MBCODE_DTYPE, InterStage, cuda_library
     from ironav_b200.synth import CONFIGS, Sequence
@@ -1471,6 +1480,7 @@ def run_decide(args, rank, world):
         st.push_reference_chroma(*seq.chroma(k, bd))
         st.set_source(frame(k + 1))
         st.set_source_chroma(*seq.chroma(k + 1, bd))
+        st.set_entropy(args.cabac, True)
         st.begin_p_picture(qpp)
         st.set_stream(stream.cuda_stream)
         stages.append(st)
@@ -1548,6 +1558,10 @@ def run_decide(args, rank, world):
     codes = bufs[0][1].cpu().numpy().view(MBCODE_DTYPE)
     kinds = {"skip": int(codes["skip"].sum()), "inter": int(((codes["kind"] == 5) & (codes["skip"] == 0)).sum()),
              "i16": int((codes["kind"] == 3).sum()), "i4": int((codes["kind"] == 1).sum())}
+    if args.cabac:
+        kinds["i8"] = int((codes["kind"] == 2).sum())
+        kinds["inter_t8"] = int(((codes["kind"] == 5) & (codes["res"]["t8x8"] != 0)).sum())
+    how = "CABAC decide_rd, High" if args.cabac else "CAVLC code_mb"
     # end to end through the host-buffer call (states, codes and the reconstruction back every step)
     for st in stages:
         st.set_stream(None)
@@ -1559,13 +1573,13 @@ def run_decide(args, rank, world):
     el = time.perf_counter() - t0
     B = 1 if bd == 8 else 2
     line = {
-        "metric": f"1080p P-picture macroblock decision + coding MB/s ({bd}-bit, CAVLC code_mb)", "value": value, "unit": "MB/s",
+        "metric": f"1080p P-picture macroblock decision + coding MB/s ({bd}-bit, {how})", "value": value, "unit": "MB/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int32",
         "data": "synthetic: seeded 4-octave value noise panned per frame + 8 moving rectangles, sigma 3; chroma from the 2x2 "
                 "luma means",
         "config": {"workload": f"decide and code every macroblock of one 1920x1088 {bd}-bit P picture per step (QP {QP}, one "
-                               f"reference, 8 slice bands, wavefront); decisions: {kinds}",
+                               f"reference, 8 slice bands, {'one chain a band' if args.cabac else 'wavefront'}); decisions: {kinds}",
                    "slices": NSLICES, "mode": "decide (device pointers)",
                    "l2": f"ring of {ring} contexts (reference planes, chroma, states, codes, reconstructions > L2)"},
         "picture_pipeline": {"ms_per_picture": pic_ms, "MB/s": world * nmb / (pic_ms * 1e-3),
@@ -1575,10 +1589,13 @@ def run_decide(args, rank, world):
         "e2e": {"value": world * nmb * args.steps / el, "unit": "MB/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": nmb * (72 + MBCODE_DTYPE.itemsize + 384 * B), "ms_per_step": 1e3 * el / args.steps,
                 "note": "ironav_decide_p_picture with host buffers (sources and references already held by the contexts)"},
-        "roofline": {"bound": "latency", "kernel": f"decide_kernel<{'uint8_t' if bd == 8 else 'uint16_t'}>", "achieved": None,
-                     "peak": None, "unit": None, "frac": None, "traffic": None, "ms_per_launch": k_ms,
-                     "note": f"one stream's wavefront: a critical path of mb_w + 2 (band rows - 1) = {mb_w + 2 * (-(-mb_h // NSLICES) - 1)} "
-                             "dependent macroblocks; see the per-macroblock latency in the profile"},
+        "roofline": {"bound": "latency", "kernel": f"{'decide_rd_kernel' if args.cabac else 'decide_kernel'}<{'uint8_t' if bd == 8 else 'uint16_t'}>",
+                     "achieved": None, "peak": None, "unit": None, "frac": None, "traffic": None, "ms_per_launch": k_ms,
+                     "note": (f"one chain a slice band: {nmb // NSLICES} dependent macroblocks (each macroblock's CABAC cost reads "
+                              "the contexts every earlier one in its slice left), a warp each"
+                              if args.cabac else
+                              f"one stream's wavefront: a critical path of mb_w + 2 (band rows - 1) = {mb_w + 2 * (-(-mb_h // NSLICES) - 1)} "
+                              "dependent macroblocks; see the per-macroblock latency in the profile")},
         "clocks": clk,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -1588,6 +1605,7 @@ def run_decide(args, rank, world):
         cores = host_cores()
         o = InterStage(w, h, max_refs=1, nslices=NSLICES, lib=olib, bd=bd)
         olib.oracle_set_threads(o.ctx, cores)
+        o.set_entropy(args.cabac, True)
         f0, c0, f1, c1 = srcs[0]
         o.push_reference(f0)
         o.push_reference_chroma(*c0)

@@ -231,6 +231,59 @@ __device__ __forceinline__ void nb_of(const ironav_mbcode* k, Nb* n) {
     mvd_grid(k, n->mvd);
 }
 
+// The partition (rects order) that holds 4x4 block (bx, by) of a P macroblock.
+__device__ __forceinline__ int part_index(int part, const uint8_t* sub, int bx, int by) {
+    if (part == 0) return 0;
+    if (part == 1) return by >> 1;
+    if (part == 2) return bx >> 1;
+    const int k = (by >> 1) * 2 + (bx >> 1);
+    int n = 0;
+    for (int q = 0; q < k; q++) n += sub[q] == 0 ? 1 : (sub[q] == 3 ? 4 : 2);
+    const int s = sub[k];
+    return n + (s == 0 ? 0 : s == 1 ? (by & 1) : s == 2 ? (bx & 1) : (by & 1) * 2 + (bx & 1));
+}
+
+constexpr int NB_WORDS = (int)(sizeof(Nb) / 4);
+static_assert(sizeof(Nb) % 4 == 0, "Nb in whole words");
+
+// nb_of with the warp: every lane calls; the code in shared or global memory.
+__device__ __forceinline__ void nb_of_warp(const ironav_mbcode* k, Nb* n) {
+    const int lane = threadIdx.x & 31;
+    const int kind = k->kind, skip = k->skip, cbp = k->res.cbp;
+    const bool inter = kind == KIND_INTER;
+    bool nz = false;
+    if (lane < 16) nz = k->dc[lane] != 0;
+    else if (lane < 24) nz = k->res.cdc[(lane - 16) >> 2][(lane - 16) & 3] != 0;
+    const unsigned bal = __ballot_sync(0xffffffffu, nz);
+    if (lane < 16) {
+        n->nnz[lane] = k->res.nnz[lane];
+        uint8_t ax = 0, ay = 0;
+        if (inter && !skip) {
+            const int q = part_index(k->part, k->sub, lane & 3, lane >> 2);
+            ax = (uint8_t)min(abs((int)k->mvds[q][0]), 64);
+            ay = (uint8_t)min(abs((int)k->mvds[q][1]), 64);
+        }
+        n->mvd[lane][0] = ax;
+        n->mvd[lane][1] = ay;
+    } else if (lane < 24) {
+        n->cnnz[(lane - 16) >> 2][(lane - 16) & 3] = k->res.cnnz[(lane - 16) >> 2][(lane - 16) & 3];
+    } else if (lane < 28) {
+        const int b8 = lane - 24;
+        n->r8[b8] = inter ? (int8_t)k->refs[k->part == 0 ? 0 : k->part == 1 ? b8 >> 1 : k->part == 2 ? (b8 & 1) : b8] : (int8_t)-1;
+    } else if (lane == 28) {
+        const int cbpc = cbp >> 4;
+        n->avail = 1;
+        n->skip = (uint8_t)skip;
+        n->kind = (uint8_t)kind;
+        n->inter = inter;
+        n->cbp = (uint8_t)cbp;
+        n->t8x8 = k->res.t8x8;
+        n->chroma_mode = inter ? 0 : k->chroma_mode;
+        n->cbf_dc = (uint8_t)((kind == KIND_I16 && (bal & 0xFFFFu)) | ((cbpc > 0 && (bal & 0xF0000u)) << 1) | ((cbpc > 0 && (bal & 0xF00000u)) << 2));
+    }
+    __syncwarp();
+}
+
 __device__ __forceinline__ bool nxn(int kind) { return kind == KIND_I4 || kind == KIND_I8; }
 
 // pred_i4_mode, enc/frame.rs:619-627, with the neighbours' modes in nbm (left column then top row: a mode, 2

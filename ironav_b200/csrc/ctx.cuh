@@ -97,13 +97,12 @@ struct ironav_ctx {
     uint8_t* h_rbsp = nullptr;
     size_t h_rbsp_cap = 0;
     // CABAC (ironav_set_entropy): the setting; the contexts' step table; the slice bands' rows on the device;
-    // the rate-distortion decision's per-band scratch (candidate codes and reconstructions); the writer's
+    // the rate-distortion decision's per-macroblock neighbour summaries (cab::Nb); the writer's
     // per-band data regions, byte counts (and overflow word) and their pinned host copy
     int cabac = 0, t8 = 0;
     uint32_t* d_cab_step = nullptr;
     int* d_band_rows = nullptr;
-    ironav_mbcode* d_rd_cand = nullptr;
-    uint8_t* d_rd_rec = nullptr;
+    uint32_t* d_rd_nb = nullptr;
     uint32_t* d_cab_out = nullptr;
     unsigned long long cab_region_words = 0;
     uint32_t* d_cab_bytes = nullptr;

@@ -7,7 +7,7 @@
 // CTA a band, the bands side by side). For each macroblock the warp codes every candidate the reference
 // tries, in its order (P_Skip, best_inter's partitioning with the 4x4 and, with transform8, the 8x8
 // transform, Intra16x16, Intra4x4, Intra8x8, each intra one with its chroma), each into the picture and
-// then into the chain's scratch (code and reconstruction), with its squared error; then lanes 0-5 count
+// then into shared memory (code and reconstruction), with its squared error; then lanes 0-5 count
 // the candidates' bins at once, each on its own copy of the contexts (the counter of cabac.cuh); lane 0
 // keeps the least SSD + lambda2 * bits in the reference's order (strict '<'), and the warp copies the
 // kept candidate's code, reconstruction and advanced contexts into place.
@@ -25,8 +25,7 @@ constexpr int RD_CANDS = 6;  // P_Skip, inter with the 4x4 transform, inter with
 
 struct RdParams {
     DecideParams D;         // decide mode's parameters: the analysis, the coder, the outputs (codes, states)
-    ironav_mbcode* cand;    // the chains' scratch: RD_CANDS codes a chain
-    uint8_t* cand_rec;      // RD_CANDS reconstructions a chain, 384 samples each (luma, Cb, Cr)
+    uint32_t* nbs;          // per macroblock, what the contexts read of it as a neighbour (cab::Nb, NB_WORDS words)
     const int* band_rows;   // chain i walks the rows [band_rows[i], band_rows[i + 1])
     const uint32_t* step;   // the contexts' step table (cab::STEP_ENTRIES)
     double lam2;            // 1.6 * 2^((QP'Y - 12) / 3), computed on the host in f64 as the reference does
@@ -37,10 +36,13 @@ struct RdParams {
 template <class T>
 struct RdSmem {
     DecideSmem<T> s;
+    ironav_mbcode cand[RD_CANDS];    // the candidates' codes
+    T crec[RD_CANDS][384];           // and reconstructions (luma, Cb, Cr)
     uint8_t live[1024];              // the chain's contexts after the macroblocks before this one
     uint8_t cst[RD_CANDS][1024];     // each candidate's copy, advanced by its bins
     uint32_t step[cab::STEP_ENTRIES];
     cab::Nb nb[2];                   // the left and top neighbours as the contexts see them
+    cab::Nb done;                    // the macroblock just decided, the next one's left
     ironav_mbstate state[RD_CANDS];  // each candidate's MbState
     long long ssd[RD_CANDS];
     uint32_t bits[RD_CANDS];
@@ -312,13 +314,13 @@ __device__ __forceinline__ void code_init(ironav_mbcode* o) {
 }
 
 // A candidate coded into the picture: its squared error (ssd_mb, enc/frame.rs:1432-1449) and a copy of its
-// reconstruction (save_mb, 1406-1417) in the chain's scratch; the candidate counts from here on.
+// reconstruction (save_mb, 1406-1417); the candidate counts from here on.
 template <class T>
-__device__ void rd_take(const RdParams& P, RdSmem<T>& R, int chain, int k, int mbx, int mby) {
+__device__ void rd_take(const RdParams& P, RdSmem<T>& R, int k, int mbx, int mby) {
     const int lane = threadIdx.x & 31;
     const CodeParams& C = P.D.C;
     const T* SC = reinterpret_cast<const T*>(C.src_c);
-    T* dst = reinterpret_cast<T*>(P.cand_rec) + ((size_t)chain * RD_CANDS + k) * 384;
+    T* dst = R.crec[k];
     __syncwarp();
     long long ssd = 0;
     for (int i = lane; i < 384; i += 32) {
@@ -362,7 +364,7 @@ __device__ __forceinline__ void rd_state(RdSmem<T>& R, int k, bool inter) {
 // decide_rd for one macroblock (after code_mb's P_Skip tests, best_i16 and best_inter; enc/frame.rs:715-760,
 // 1462-1513), its bins then carried into the chain's contexts (write_mb_cabac's effect on them, 2020-2025).
 template <class T>
-__device__ void rd_mb(const RdParams& P, RdSmem<T>& R, const unsigned* i4tab, int chain, int mb, int mbx, int mby) {
+__device__ void rd_mb(const RdParams& P, RdSmem<T>& R, const unsigned* i4tab, int mb, int mbx, int mby) {
     const int lane = threadIdx.x & 31;
     const DecideParams& D = P.D;
     const AnalyseParams& A = D.C.A;
@@ -371,13 +373,15 @@ __device__ void rd_mb(const RdParams& P, RdSmem<T>& R, const unsigned* i4tab, in
     const bool ta = mby > A.band_start[mby], la = mbx > 0, tra = ta && mbx + 1 < A.mb_w;
     const cab::Slice sl = {D.intra ? 0 : 1, P.t8, D.intra ? 0 : A.nact};
     ironav_mbcode* out = &D.codes[mb];
-    ironav_mbcode* cand = P.cand + (size_t)chain * RD_CANDS;
+    ironav_mbcode* cand = R.cand;
     code_init(out);
     stage_source(A, S.a);
-    if (lane == 0) {
-        R.nb[0].avail = R.nb[1].avail = 0;
-        if (la) cab::nb_of(&D.codes[mb - 1], &R.nb[0]);
-        if (ta) cab::nb_of(&D.codes[mb - A.mb_w], &R.nb[1]);
+    // the neighbours for the contexts: the left one is the macroblock just decided, the top one's was kept
+    if (lane < cab::NB_WORDS) {
+        uint32_t* l = reinterpret_cast<uint32_t*>(&R.nb[0]);
+        uint32_t* t = reinterpret_cast<uint32_t*>(&R.nb[1]);
+        l[lane] = la ? reinterpret_cast<const uint32_t*>(&R.done)[lane] : 0u;
+        t[lane] = ta ? P.nbs[(size_t)(mb - A.mb_w) * cab::NB_WORDS + lane] : 0u;
     }
     if (lane < RD_CANDS) R.valid[lane] = 0;
     __syncwarp();
@@ -389,6 +393,9 @@ __device__ void rd_mb(const RdParams& P, RdSmem<T>& R, const unsigned* i4tab, in
             cab::mb_bins(c, sl, out, R.nb[0], R.nb[1], S.nbm);
         }
         if (lane < 18) reinterpret_cast<uint32_t*>(&A.states_out[mb])[lane] = reinterpret_cast<const uint32_t*>(&S.a.out)[lane];
+        __syncwarp();
+        cab::nb_of_warp(out, &R.done);
+        if (lane < cab::NB_WORDS) P.nbs[(size_t)mb * cab::NB_WORDS + lane] = reinterpret_cast<const uint32_t*>(&R.done)[lane];
         __syncwarp();
         return;
     }
@@ -432,7 +439,7 @@ __device__ void rd_mb(const RdParams& P, RdSmem<T>& R, const unsigned* i4tab, in
         if (lane < 16) o->mvds[lane][0] = o->mvds[lane][1] = 0;
         if (lane == 0) o->skip = 1;
         rd_state(R, 0, true);
-        rd_take(P, R, chain, 0, mbx, mby);
+        rd_take(P, R, 0, mbx, mby);
         // best_inter's partitioning with the 4x4 transform; with nothing coded and the skip vector, it would be
         // P_Skip at a higher price
         o = &cand[1];
@@ -454,7 +461,7 @@ __device__ void rd_mb(const RdParams& P, RdSmem<T>& R, const unsigned* i4tab, in
         const uint32_t cbp = code_inter_mb<T>(C, S.c, mb, &o->res);
         inter_tail(D, S, Dd, o);
         rd_state(R, 1, true);
-        rd_take(P, R, chain, 1, mbx, mby);
+        rd_take(P, R, 1, mbx, mby);
         if (lane == 0 && cbp == 0 && part == 0 && Dd.mvs[0][0] == sv.x && Dd.mvs[0][1] == sv.y && bestr == 0) R.valid[1] = 0;
         __syncwarp();
         // the 8x8 transform needs every 8x8 block of P_8x8 to be a single 8x8 partition; without luma levels it
@@ -467,7 +474,7 @@ __device__ void rd_mb(const RdParams& P, RdSmem<T>& R, const unsigned* i4tab, in
             code_inter_mb<T>(C, S.c, mb, &o->res);
             inter_tail(D, S, Dd, o);
             rd_state(R, 2, true);
-            rd_take(P, R, chain, 2, mbx, mby);
+            rd_take(P, R, 2, mbx, mby);
             if (lane == 0 && !o->res.t8x8) R.valid[2] = 0;
             __syncwarp();
         }
@@ -484,7 +491,7 @@ __device__ void rd_mb(const RdParams& P, RdSmem<T>& R, const unsigned* i4tab, in
             o->res.cbp = (uint8_t)cbp;
         }
         rd_state(R, 3, false);
-        rd_take(P, R, chain, 3, mbx, mby);
+        rd_take(P, R, 3, mbx, mby);
     }
     // Intra4x4, block by block from its own reconstruction, with its chroma
     {
@@ -513,7 +520,7 @@ __device__ void rd_mb(const RdParams& P, RdSmem<T>& R, const unsigned* i4tab, in
             o->res.cbp = (uint8_t)cbp;
         }
         rd_state(R, 4, false);
-        rd_take(P, R, chain, 4, mbx, mby);
+        rd_take(P, R, 4, mbx, mby);
     }
     // Intra8x8 with its chroma
     if (P.t8) {
@@ -523,7 +530,7 @@ __device__ void rd_mb(const RdParams& P, RdSmem<T>& R, const unsigned* i4tab, in
         cbp |= code_intra_chroma_d(D, S, mbx, mby, ta, la, o);
         if (lane == 0) o->res.cbp = (uint8_t)cbp;
         rd_state(R, 5, false);
-        rd_take(P, R, chain, 5, mbx, mby);
+        rd_take(P, R, 5, mbx, mby);
     }
     // each candidate's bins counted from its own copy of the contexts (rd_cost, 1453-1457), a lane a candidate
     for (int k = 0; k < RD_CANDS; k++) {
@@ -559,7 +566,7 @@ __device__ void rd_mb(const RdParams& P, RdSmem<T>& R, const unsigned* i4tab, in
         const uint32_t* c32 = reinterpret_cast<const uint32_t*>(R.cst[b]);
         uint32_t* l32 = reinterpret_cast<uint32_t*>(R.live);
         for (int i = lane; i < 256; i += 32) l32[i] = c32[i];
-        const T* rec = reinterpret_cast<const T*>(P.cand_rec) + ((size_t)chain * RD_CANDS + b) * 384;
+        const T* rec = R.crec[b];
         for (int i = lane; i < 384; i += 32) {
             if (i < 256) {
                 reinterpret_cast<T*>(C.rec[0])[(size_t)(mby * 16 + (i >> 4)) * C.ys + mbx * 16 + (i & 15)] = rec[i];
@@ -571,22 +578,21 @@ __device__ void rd_mb(const RdParams& P, RdSmem<T>& R, const unsigned* i4tab, in
         if (lane < 18) reinterpret_cast<uint32_t*>(&A.states_out[mb])[lane] = reinterpret_cast<const uint32_t*>(&R.state[b])[lane];
     }
     __syncwarp();
+    cab::nb_of_warp(&cand[b], &R.done);
+    if (lane < cab::NB_WORDS) P.nbs[(size_t)mb * cab::NB_WORDS + lane] = reinterpret_cast<const uint32_t*>(&R.done)[lane];
+    __syncwarp();
 }
 
-// Decide mode under CABAC: CTA i, one warp, walks slice band i in raster order (FrameCoder::encode,
-// enc/frame.rs:461-478) from the slice's initial contexts (cabac_init_idc 0, QP_Y).
+// One chain: slice band `band` in raster order (FrameCoder::encode, enc/frame.rs:461-478) from the slice's
+// initial contexts (cabac_init_idc 0, QP_Y).
 template <class T>
-__global__ void __launch_bounds__(32) decide_rd_kernel(const __grid_constant__ RdParams P) {
-    __shared__ RdSmem<T> R;
-    __shared__ unsigned i4tab[9 * 17];
-    fill_i4tab(i4tab);
-    const int chain = blockIdx.x, lane = threadIdx.x & 31;
-    if (chain >= P.nbands) return;
+__device__ void rd_chain(const RdParams& P, RdSmem<T>& R, const unsigned* i4tab, int band) {
+    const int lane = threadIdx.x & 31;
     const AnalyseParams& A = P.D.C.A;
     for (int i = lane; i < cab::STEP_ENTRIES; i += 32) R.step[i] = P.step[i];
     cab::init_states(R.live, P.D.intra != 0, 0, P.D.C.qp, lane, 32);
     __syncwarp();
-    for (int mby = P.band_rows[chain]; mby < P.band_rows[chain + 1]; mby++)
+    for (int mby = P.band_rows[band]; mby < P.band_rows[band + 1]; mby++)
         for (int mbx = 0; mbx < A.mb_w; mbx++) {
             const int mb = mby * A.mb_w + mbx;
             if (lane == 0) {
@@ -596,8 +602,36 @@ __global__ void __launch_bounds__(32) decide_rd_kernel(const __grid_constant__ R
             }
             __syncwarp();
             load_neighbours(A, R.s.a, A.states_out);
-            rd_mb<T>(P, R, i4tab, chain, mb, mbx, mby);
+            rd_mb<T>(P, R, i4tab, mb, mbx, mby);
         }
+}
+
+// Decide mode under CABAC for one stream: CTA i, one warp, walks slice band i.
+template <class T>
+__global__ void __launch_bounds__(32) decide_rd_kernel(const __grid_constant__ RdParams P) {
+    __shared__ RdSmem<T> R;
+    __shared__ unsigned i4tab[9 * 17];
+    fill_i4tab(i4tab);
+    if ((int)blockIdx.x >= P.nbands) return;
+    rd_chain<T>(P, R, i4tab, blockIdx.x);
+}
+
+// Decide mode under CABAC for many streams in one launch: CTA i walks chains[i] = stream << 16 | band, with
+// the stream's parameters from table[stream] (copied into shared memory).
+template <class T>
+__global__ void __launch_bounds__(32) decide_rd_batch_kernel(const RdParams* __restrict__ table, const uint32_t* __restrict__ chains,
+                                                             int nchains) {
+    __shared__ RdSmem<T> R;
+    __shared__ RdParams prm;
+    __shared__ unsigned i4tab[9 * 17];
+    fill_i4tab(i4tab);
+    if ((int)blockIdx.x >= nchains) return;
+    const int lane = threadIdx.x & 31;
+    const uint32_t e = chains[blockIdx.x];
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(&table[e >> 16]);
+    for (int k = lane; k < (int)(sizeof(RdParams) / 4); k += 32) reinterpret_cast<uint32_t*>(&prm)[k] = src[k];
+    __syncwarp();
+    rd_chain<T>(prm, R, i4tab, (int)(e & 0xFFFFu));
 }
 
 // ---- the CABAC slice writer ---------------------------------------------------------------------------
@@ -614,41 +648,65 @@ struct CabacWriteParams {
 
 // A slice band's data (FrameCoder::encode with write_mb_cabac, enc/frame.rs:461-486): each macroblock's bins
 // (mb_bins) then end_of_slice_flag, arithmetic coded from the slice's contexts; the data starts on the byte
-// that follows the header's cabac_alignment_one_bit (written on the host). CTA i, lane 0, slice band i.
-__global__ void __launch_bounds__(32) cabac_write_kernel(const __grid_constant__ CabacWriteParams P) {
+// that follows the header's cabac_alignment_one_bit (written on the host). CTA i walks slice band i: the warp
+// stages each macroblock's code and its top neighbour's into shared memory and works out their Nb, and
+// lane 0 codes the bins.
+static __global__ void __launch_bounds__(32) cabac_write_kernel(const __grid_constant__ CabacWriteParams P) {
     __shared__ uint8_t st[1024];
     __shared__ uint32_t step[cab::STEP_ENTRIES];
-    __shared__ cab::Nb nb[2];
+    __shared__ ironav_mbcode code[2];  // the macroblock, then its top neighbour
+    __shared__ cab::Nb nb[3];          // left, top, and the macroblock itself (the next one's left)
     __shared__ int nbm[8];
+    __shared__ int left_modes[4];      // the macroblock's right column of Intra NxN modes (2 otherwise)
+    __shared__ int over;
     const int chain = blockIdx.x, lane = threadIdx.x & 31;
     if (chain >= P.nbands) return;
     for (int i = lane; i < cab::STEP_ENTRIES; i += 32) step[i] = P.step[i];
     cab::init_states(st, P.intra != 0, 0, P.qp, lane, 32);
+    if (lane == 0) over = 0;
     __syncwarp();
-    if (lane != 0) return;
     cab::BitOut bo = {P.out + (size_t)chain * P.region_words, P.region_words, 0, 0ull, 0, false};
     cab::Coder k = {st, step, &bo, 0u, 510u, 0u, true};
     const cab::Slice sl = {P.intra ? 0 : 1, P.t8, P.intra ? 0 : P.nref};
     const int r0 = P.band_rows[chain], r1 = P.band_rows[chain + 1];
+    constexpr int W = (int)(sizeof(ironav_mbcode) / 4);
     for (int mby = r0; mby < r1; mby++)
         for (int mbx = 0; mbx < P.mb_w; mbx++) {
             const int mb = mby * P.mb_w + mbx;
-            const ironav_mbcode* L = mbx > 0 ? &P.codes[mb - 1] : nullptr;
-            const ironav_mbcode* Tp = mby > r0 ? &P.codes[mb - P.mb_w] : nullptr;
-            nb[0].avail = nb[1].avail = 0;
-            if (L) cab::nb_of(L, &nb[0]);
-            if (Tp) cab::nb_of(Tp, &nb[1]);
-            for (int q = 0; q < 4; q++) {
-                nbm[q] = L ? (cab::nxn(L->kind) ? (int)L->modes[q * 4 + 3] : 2) : -1;
-                nbm[4 + q] = Tp ? (cab::nxn(Tp->kind) ? (int)Tp->modes[12 + q] : 2) : -1;
+            const bool la = mbx > 0, ta = mby > r0;
+            uint32_t* c0 = reinterpret_cast<uint32_t*>(&code[0]);
+            uint32_t* c1 = reinterpret_cast<uint32_t*>(&code[1]);
+            const uint32_t* g0 = reinterpret_cast<const uint32_t*>(&P.codes[mb]);
+            for (int i = lane; i < W; i += 32) c0[i] = g0[i];
+            if (ta) {
+                const uint32_t* g1 = reinterpret_cast<const uint32_t*>(&P.codes[mb - P.mb_w]);
+                for (int i = lane; i < W; i += 32) c1[i] = g1[i];
             }
-            cab::mb_bins(k, sl, &P.codes[mb], nb[0], nb[1], nbm);
-            k.terminate(mby + 1 == r1 && mbx + 1 == P.mb_w);
-            if (bo.over) break;
+            if (lane < cab::NB_WORDS) {
+                reinterpret_cast<uint32_t*>(&nb[0])[lane] = la ? reinterpret_cast<const uint32_t*>(&nb[2])[lane] : 0u;
+                if (!ta) reinterpret_cast<uint32_t*>(&nb[1])[lane] = 0u;
+            }
+            if (lane < 4) nbm[lane] = la ? left_modes[lane] : -1;
+            __syncwarp();
+            if (ta) cab::nb_of_warp(&code[1], &nb[1]);
+            if (lane >= 4 && lane < 8) nbm[lane] = ta ? (cab::nxn(code[1].kind) ? (int)code[1].modes[12 + lane - 4] : 2) : -1;
+            __syncwarp();
+            if (lane == 0) {
+                cab::mb_bins(k, sl, &code[0], nb[0], nb[1], nbm);
+                k.terminate(mby + 1 == r1 && mbx + 1 == P.mb_w);
+                over = bo.over;
+            }
+            __syncwarp();
+            cab::nb_of_warp(&code[0], &nb[2]);
+            if (lane < 4) left_modes[lane] = cab::nxn(code[0].kind) ? (int)code[0].modes[lane * 4 + 3] : 2;
+            __syncwarp();
+            if (over) mbx = P.mb_w, mby = r1;  // the region is full: stop (reported below)
         }
-    const uint32_t bytes = bo.finish();
-    P.slice_bytes[chain] = bytes;
-    if (bo.over) atomicOr(&P.slice_bytes[P.nbands], 1u);
+    if (lane == 0) {
+        const uint32_t bytes = bo.finish();
+        P.slice_bytes[chain] = bytes;
+        if (bo.over) atomicOr(&P.slice_bytes[P.nbands], 1u);
+    }
 }
 
 }  // namespace ironav

@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <tuple>
 #include <vector>
@@ -15,6 +16,7 @@
 #include "analyse_g8.cuh"
 #include "ctx.cuh"
 #include "decide.cuh"
+#include "decide_rd.cuh"
 #include "planes.cuh"
 
 using namespace ironav;
@@ -179,6 +181,12 @@ struct ironav_batch {
     DecideParams* d_dtable = nullptr;
     DecideParams* h_dtable = nullptr;
     int k7_blocks = 0;
+    // decide mode under CABAC (allocated on first use): the streams' parameters and the chains (stream << 16 |
+    // slice band), one CTA each
+    RdParams* d_rdtable = nullptr;
+    RdParams* h_rdtable = nullptr;
+    uint32_t* d_chains = nullptr;
+    int nchains = 0;
     // deblocking (allocated on first use): the streams' jobs, their rows' merged ticket order, progress
     // words, and the concatenated slice tables (pinned staging reused once the previous copies are done)
     DbkJob* d_kjobs = nullptr;
@@ -203,6 +211,9 @@ static void free_batch(ironav_batch* b) {
     cudaFreeHost(b->h_table);
     cudaFree(b->d_dtable);
     cudaFreeHost(b->h_dtable);
+    cudaFree(b->d_rdtable);
+    cudaFreeHost(b->h_rdtable);
+    cudaFree(b->d_chains);
     cudaFree(b->d_kjobs);
     cudaFreeHost(b->h_kjobs);
     cudaFree(b->d_korder);
@@ -518,9 +529,50 @@ extern "C" int ironav_batch_sync(ironav_batch* b) {
     return err ? IRONAV_INTERNAL : IRONAV_OK;
 }
 
+// ironav_batch_decide under CABAC: every stream's slice bands as chains of one launch (decide_rd_batch_kernel).
+static int batch_decide_rd(ironav_batch* b, ironav_mbstate* const* d_states, ironav_mbcode* const* d_codes, void* const* d_y,
+                           const int* y_strides, void* const* d_cb, void* const* d_cr, const int* c_strides) {
+    if (!b->d_rdtable) {
+        CK(cudaMalloc(&b->d_rdtable, sizeof(RdParams) * b->n));
+        CK(cudaHostAlloc(&b->h_rdtable, sizeof(RdParams) * b->n, cudaHostAllocDefault));
+        std::vector<uint32_t> chains;
+        for (int i = 0; i < b->n; i++)
+            for (int k = 0; k < b->ctx[i]->nslices; k++) chains.push_back((uint32_t)i << 16 | (uint32_t)k);
+        CK(cudaMalloc(&b->d_chains, sizeof(uint32_t) * chains.size()));
+        CK(cudaMemcpy(b->d_chains, chains.data(), sizeof(uint32_t) * chains.size(), cudaMemcpyHostToDevice));
+        b->nchains = (int)chains.size();
+    }
+    if (b->pending) CK(cudaEventSynchronize(b->copied));
+    for (int i = 0; i < b->n; i++) {
+        ironav_ctx* c = b->ctx[i];
+        RdParams& p = b->h_rdtable[i];
+        memset(&p, 0, sizeof(p));
+        int s = fill_decide_params(c, p.D, d_states[i], d_codes[i], d_y[i], y_strides[i], d_cb[i], d_cr[i], c_strides[i]);
+        if (s == IRONAV_OK) s = cabac_setup(c);
+        if (s != IRONAV_OK) return s;
+        p.D.C.A.err = b->d_counters + 1;
+        p.D.C.err = b->d_counters + 1;
+        p.nbs = c->d_rd_nb;
+        p.band_rows = c->d_band_rows;
+        p.step = c->d_cab_step;
+        p.lam2 = 1.6 * std::pow(2.0, ((double)c->qpp - 12.0) / 3.0);  // decide_rd's lambda2, enc/frame.rs:1464
+        p.nbands = c->nslices;
+        p.t8 = c->t8;
+    }
+    CK(cudaMemcpyAsync(b->d_rdtable, b->h_rdtable, sizeof(RdParams) * b->n, cudaMemcpyHostToDevice, b->stream));
+    CK(cudaEventRecord(b->copied, b->stream));
+    b->pending = true;
+    CK(cudaMemsetAsync(b->d_counters, 0, sizeof(unsigned) * 2, b->stream));
+    if (b->bd > 8) decide_rd_batch_kernel<uint16_t><<<b->nchains, 32, 0, b->stream>>>(b->d_rdtable, b->d_chains, b->nchains);
+    else decide_rd_batch_kernel<uint8_t><<<b->nchains, 32, 0, b->stream>>>(b->d_rdtable, b->d_chains, b->nchains);
+    return cuda_status(cudaGetLastError());
+}
+
 extern "C" int ironav_batch_decide(ironav_batch* b, ironav_mbstate* const* d_states, ironav_mbcode* const* d_codes, void* const* d_y,
                                    const int* y_strides, void* const* d_cb, void* const* d_cr, const int* c_strides) {
     if (!b || !d_states || !d_codes || !d_y || !y_strides || !d_cb || !d_cr || !c_strides) return IRONAV_INVALID_ARGUMENT;
+    for (int i = 1; i < b->n; i++)
+        if (b->ctx[i]->cabac != b->ctx[0]->cabac) return IRONAV_INVALID_ARGUMENT;  // one entropy coding for the batch
     if (!b->d_dtable) {
         CK(cudaMalloc(&b->d_dtable, sizeof(DecideParams) * b->n));
         CK(cudaHostAlloc(&b->h_dtable, sizeof(DecideParams) * b->n, cudaHostAllocDefault));
@@ -540,6 +592,7 @@ extern "C" int ironav_batch_decide(ironav_batch* b, ironav_mbstate* const* d_sta
         const int B = b->bd > 8 ? 2 : 1;
         if ((a & 15) || (y_strides[i] * B) % 16 || c_strides[i] % 8) return IRONAV_INVALID_ARGUMENT;
         if ((reinterpret_cast<uintptr_t>(d_states[i]) | reinterpret_cast<uintptr_t>(d_codes[i])) & 3) return IRONAV_INVALID_ARGUMENT;
+        if (c->cabac) continue;
         DecideParams& p = b->h_dtable[i];
         const int s = fill_decide_params(c, p, d_states[i], d_codes[i], d_y[i], y_strides[i], d_cb[i], d_cr[i], c_strides[i]);
         if (s != IRONAV_OK) return s;
@@ -548,6 +601,7 @@ extern "C" int ironav_batch_decide(ironav_batch* b, ironav_mbstate* const* d_sta
         p.C.A.err = b->d_counters + 1;
         p.C.err = b->d_counters + 1;
     }
+    if (b->ctx[0]->cabac) return batch_decide_rd(b, d_states, d_codes, d_y, y_strides, d_cb, d_cr, c_strides);
     CK(cudaMemcpyAsync(b->d_dtable, b->h_dtable, sizeof(DecideParams) * b->n, cudaMemcpyHostToDevice, b->stream));
     CK(cudaEventRecord(b->copied, b->stream));
     b->pending = true;

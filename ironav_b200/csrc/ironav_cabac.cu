@@ -58,9 +58,7 @@ int cabac_setup(ironav_ctx* c) {
     CK(cudaMemcpy(c->d_cab_step, step, sizeof(step), cudaMemcpyHostToDevice));
     CK(cudaMalloc(&c->d_band_rows, sizeof(int) * (c->nslices + 1)));
     CK(cudaMemcpy(c->d_band_rows, c->band_rows, sizeof(int) * (c->nslices + 1), cudaMemcpyHostToDevice));
-    const size_t B = c->bd > 8 ? 2 : 1;
-    CK(cudaMalloc(&c->d_rd_cand, sizeof(ironav_mbcode) * RD_CANDS * c->nslices));
-    CK(cudaMalloc(&c->d_rd_rec, 384 * B * RD_CANDS * c->nslices));
+    CK(cudaMalloc(&c->d_rd_nb, sizeof(cab::Nb) * c->nmb));
     return IRONAV_OK;
 }
 
@@ -73,8 +71,7 @@ int launch_decide_rd(ironav_ctx* c, ironav_mbstate* d_states, ironav_mbcode* d_c
     if (t != IRONAV_OK) return t;
     p.D.C.A.err = c->d_counters + 1;
     p.D.C.err = c->d_counters + 1;
-    p.cand = c->d_rd_cand;
-    p.cand_rec = c->d_rd_rec;
+    p.nbs = c->d_rd_nb;
     p.band_rows = c->d_band_rows;
     p.step = c->d_cab_step;
     // decide_rd's lambda2, enc/frame.rs:1464, in f64 on the host as the reference computes it

@@ -21,6 +21,15 @@
  *   col_mv, motion_search .................. enc/frame.rs:839-1019
  *   slice bands ............................ enc/mod.rs:192,603
  *   source padding ......................... enc/mod.rs:481-529
+ * and beyond the stage, the encoder around it (decide mode, the bitstream), among them the High profile
+ * with CABAC (the reference encoder's default):
+ *   CabacWriter, CabacCost, write_block .... enc/cabac.rs:10-250
+ *   mb_bins / write_mb_cabac, mvd_bins ..... enc/frame.rs:2020-2279,2393-2414
+ *   decide_rd, rd_cost, ssd_mb, save/restore enc/frame.rs:1406-1513
+ *   code_i8, filter_8x8_edges, predict_nxn(8)  enc/frame.rs:1307-1388; intra.rs:30-158
+ *   sps / pps (Main, High), cabac_init_idc . enc/mod.rs:296-400,566-600
+ * whose streams FFmpeg decodes to the oracle's reconstruction (tests/test_cabac.py), and whose arithmetic
+ * coder reads back through a decoder of the standard on the reference's own coder test.
  *
  * Pinning. The interpolation (planes + predict) is pinned by the reference's own known-answer test,
  * predict == the decoder's interpolation over the same grid of blocks and vectors (enc/subpel.rs:160-194,

@@ -59,3 +59,49 @@ def test_host_forms_write_the_same_cabac_stream(oracle_lib, cuda_lib):
         assert a.encode(*f) == b.encode(*f), f"picture {t}"
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("bd", [8, 10])
+def test_batched_cabac_decide_matches_single_streams_and_the_oracle(oracle_lib, cuda_lib, bd):
+    """Four streams of different sizes, slice layouts, references and content decided under CABAC in one launch
+    (every stream's slice bands as chains, decide_rd_batch_kernel): each stream's codes, states and
+    reconstruction are those of its own decide call, and the oracle's."""
+    import numpy as np
+    import torch
+
+    from ironav_b200.inter import MBCODE_DTYPE, MBSTATE_DTYPE, InterBatch
+    from tests.test_decide import _same_decisions, decide_case
+
+    cases = [dict(), dict(new_content=True, qp=30), dict(size=(320, 176), nslices=3, fast=True, refs=2), dict(cfg="1080p", nslices=8, qp=27)]
+    cases = [dict(kw, bd=bd) for kw in cases]
+    stages = []
+    for kw in cases:
+        st = decide_case(cuda_lib, threads=False, **kw)[0]
+        st.set_entropy(True, True)
+        stages.append(st)
+    want = [st.decide_p_picture() for st in stages]
+    for k in (1, 2):
+        o = decide_case(oracle_lib, **cases[k])[0]
+        o.set_entropy(True, True)
+        _same_decisions(want[k], o.decide_p_picture(), f"single stream {cases[k]} against the oracle")
+        o.close()
+    stream = torch.cuda.Stream()
+    for st in stages:
+        st.set_stream(stream.cuda_stream)
+    dt = torch.uint8 if bd == 8 else torch.int16
+    bufs = [(torch.zeros(st.nmb * 72, dtype=torch.uint8, device="cuda"), torch.full((st.nmb * 1516,), 0x5A, dtype=torch.uint8, device="cuda"),
+             torch.zeros((st.mb_h * 16, st.mb_w * 16), dtype=dt, device="cuda"), torch.zeros((2, st.mb_h * 8, st.mb_w * 8), dtype=dt, device="cuda"))
+            for st in stages]
+    batch = InterBatch(stages)
+    for _ in range(2):
+        batch.decide([b[0].data_ptr() for b in bufs], [b[1].data_ptr() for b in bufs], [b[2].data_ptr() for b in bufs],
+                     [b[2].shape[1] for b in bufs], [b[3][0].data_ptr() for b in bufs], [b[3][1].data_ptr() for b in bufs],
+                     [b[3].shape[2] for b in bufs])
+        batch.sync()
+    view = (lambda t: t.cpu().numpy().view(np.uint16)) if bd == 10 else (lambda t: t.cpu().numpy())
+    for k, (st, b) in enumerate(zip(stages, bufs)):
+        got = (b[0].cpu().numpy().view(MBSTATE_DTYPE), b[1].cpu().numpy().view(MBCODE_DTYPE), (view(b[2]), view(b[3][0]), view(b[3][1])))
+        _same_decisions(got, want[k], f"stream {k} {cases[k]}")
+    batch.close()
+    for st in stages:
+        st.close()
