@@ -5,7 +5,7 @@
 // lanes can each count another candidate's bins from their own copy of the contexts.
 //
 // The walk reads the macroblock's code and what the contexts need of its left and top neighbours in the
-// slice (CabNb, the CABAC fields of MbState, enc/frame.rs:245-272). Only I and P slices are coded here.
+// slice (Nb, the CABAC fields of MbState, enc/frame.rs:245-272). Only I and P slices are coded here.
 #pragma once
 #include <stdint.h>
 

@@ -7,14 +7,15 @@
 // CTA a band, the bands side by side). For each macroblock the warp codes every candidate the reference
 // tries, in its order (P_Skip, best_inter's partitioning with the 4x4 and, with transform8, the 8x8
 // transform, Intra16x16, Intra4x4, Intra8x8, each intra one with its chroma), each into the picture and
-// then into shared memory (code and reconstruction), with its squared error; then lanes 0-5 count
-// the candidates' bins at once, each on its own copy of the contexts (the counter of cabac.cuh); lane 0
-// keeps the least SSD + lambda2 * bits in the reference's order (strict '<'), and the warp copies the
-// kept candidate's code, reconstruction and advanced contexts into place.
+// then into shared memory (code and reconstruction), with its squared error; then, in the reference's
+// order, lane 0 counts each candidate's bins on its own copy of the contexts (the counter of cabac.cuh)
+// unless its squared error alone already rules it out, keeps the least SSD + lambda2 * bits (strict '<'),
+// and the warp copies the kept candidate's code, reconstruction and advanced contexts into place.
 //
 // The candidates reuse decide mode's warp-level coders (decide.cuh, residual.cuh); Intra8x8 (code_i8,
 // enc/frame.rs:1307-1388) is coded here: block by block, its edges filtered (8.3.2.2.1), nine modes'
-// SATD over 36 lane-units of (mode, 4x4 quadrant), the chosen block's 8x8 transform on eight lanes.
+// SATD over 36 lane-units of (mode, 4x4 quadrant) from a table of the predictors (i8_entry), the chosen
+// block's 8x8 transform on eight lanes.
 #pragma once
 #include "cabac.cuh"
 #include "decide.cuh"
@@ -45,12 +46,13 @@ struct RdSmem {
     cab::Nb done;                    // the macroblock just decided, the next one's left
     ironav_mbstate state[RD_CANDS];  // each candidate's MbState
     long long ssd[RD_CANDS];
-    uint32_t bits[RD_CANDS];
     int valid[RD_CANDS];
     int best;
     // the Intra8x8 trial
     int i8rec[256];       // its reconstruction
-    int raw[25], e8[25];  // a block's edges, raw and filtered: [0] top-left, [1 + i] the 16 above, [17 + j] the 8 left
+    int raw[25], e8[26];  // a block's edges, raw and filtered: [0] top-left, [1 + i] the 16 above, [17 + j] the 8 left,
+                          // e8[25] the DC mode's value
+    unsigned i8tab[9 * 64];  // i8_entry per mode and sample
     int sat[36];          // SATD per (mode, 4x4 quadrant)
     int pred8[64];
     int t8b[8][9];
@@ -60,49 +62,53 @@ struct RdSmem {
     int i8meta[4];        // chosen mode, predicted mode, DC value, non-zero levels
 };
 
-// predict_nxn for n = 8, h264/intra.rs:30-128 (8.3.2.2.2-8.3.2.2.10), of sample (x, y) from the filtered
-// edges E; dcv the DC mode's value.
-__device__ __forceinline__ int i8_sample(const int* E, int mode, int x, int y, int dcv) {
-#define T8(i) ((i) < 0 ? E[0] : E[1 + (i)])
-#define L8(j) ((j) < 0 ? E[0] : E[17 + (j)])
+// The 8x8 intra predictors as a table, as decide mode's 4x4 ones (i4_entry): every sample of every mode is
+// (E[a] + 2 E[b] + E[c] + 2) >> 2 over the block's filtered edge array E (E[0] the top-left sample, E[1 + i]
+// the 16 above, E[17 + j] the 8 to the left, E[25] the DC mode's value): a copy has a = b = c, a two-sample
+// average (p + q + 1) >> 1 has a = c = p, b = q, and (p + 3q + 2) >> 2 has b = c = q. Entry: a | b << 5 | c << 10.
+// The cases are predict_nxn's for n = 8 (h264/intra.rs:30-128; ITU-T H.264 8.3.2.2.2-8.3.2.2.10).
+__device__ __forceinline__ unsigned i8_entry(int mode, int x, int y) {
+    auto T = [](int i) { return i < 0 ? 0 : 1 + i; };
+    auto L = [](int j) { return j < 0 ? 0 : 17 + j; };
+    auto E3 = [](int a, int b, int c) { return (unsigned)(a | b << 5 | c << 10); };
     switch (mode) {
-    case 0: return T8(x);
-    case 1: return L8(y);
-    case 2: return dcv;
-    case 3: return (x == 7 && y == 7) ? (T8(14) + 3 * T8(15) + 2) >> 2 : (T8(x + y) + 2 * T8(x + y + 1) + T8(x + y + 2) + 2) >> 2;
+    case 0: return E3(T(x), T(x), T(x));
+    case 1: return E3(L(y), L(y), L(y));
+    case 2: return E3(25, 25, 25);
+    case 3: return (x == 7 && y == 7) ? E3(T(14), T(15), T(15)) : E3(T(x + y), T(x + y + 1), T(x + y + 2));
     case 4:
-        if (x > y) return (T8(x - y - 2) + 2 * T8(x - y - 1) + T8(x - y) + 2) >> 2;
-        if (x < y) return (L8(y - x - 2) + 2 * L8(y - x - 1) + L8(y - x) + 2) >> 2;
-        return (T8(0) + 2 * E[0] + L8(0) + 2) >> 2;
+        if (x > y) return E3(T(x - y - 2), T(x - y - 1), T(x - y));
+        if (x < y) return E3(L(y - x - 2), L(y - x - 1), L(y - x));
+        return E3(T(0), 0, L(0));
     case 5: {
         const int z = 2 * x - y, i = x - (y >> 1);
-        if (z >= 0 && (z & 1) == 0) return (T8(i - 1) + T8(i) + 1) >> 1;
-        if (z >= 0) return (T8(i - 2) + 2 * T8(i - 1) + T8(i) + 2) >> 2;
-        if (z == -1) return (L8(0) + 2 * E[0] + T8(0) + 2) >> 2;
-        return (L8(y - 2 * x - 1) + 2 * L8(y - 2 * x - 2) + L8(y - 2 * x - 3) + 2) >> 2;
+        if (z >= 0 && (z & 1) == 0) return E3(T(i - 1), T(i), T(i - 1));
+        if (z >= 0) return E3(T(i - 2), T(i - 1), T(i));
+        if (z == -1) return E3(L(0), 0, T(0));
+        return E3(L(y - 2 * x - 1), L(y - 2 * x - 2), L(y - 2 * x - 3));
     }
     case 6: {
         const int z = 2 * y - x, j = y - (x >> 1);
-        if (z >= 0 && (z & 1) == 0) return (L8(j - 1) + L8(j) + 1) >> 1;
-        if (z >= 0) return (L8(j - 2) + 2 * L8(j - 1) + L8(j) + 2) >> 2;
-        if (z == -1) return (L8(0) + 2 * E[0] + T8(0) + 2) >> 2;
-        return (T8(x - 2 * y - 1) + 2 * T8(x - 2 * y - 2) + T8(x - 2 * y - 3) + 2) >> 2;
+        if (z >= 0 && (z & 1) == 0) return E3(L(j - 1), L(j), L(j - 1));
+        if (z >= 0) return E3(L(j - 2), L(j - 1), L(j));
+        if (z == -1) return E3(L(0), 0, T(0));
+        return E3(T(x - 2 * y - 1), T(x - 2 * y - 2), T(x - 2 * y - 3));
     }
     case 7: {
         const int i = x + (y >> 1);
-        return (y & 1) == 0 ? (T8(i) + T8(i + 1) + 1) >> 1 : (T8(i) + 2 * T8(i + 1) + T8(i + 2) + 2) >> 2;
+        return (y & 1) == 0 ? E3(T(i), T(i + 1), T(i)) : E3(T(i), T(i + 1), T(i + 2));
     }
     default: {
         const int z = x + 2 * y, j = y + (x >> 1);
-        if (z > 13) return L8(7);
-        if (z == 13) return (L8(6) + 3 * L8(7) + 2) >> 2;
-        if ((z & 1) == 0) return (L8(j) + L8(j + 1) + 1) >> 1;
-        return (L8(j) + 2 * L8(j + 1) + L8(j + 2) + 2) >> 2;
+        if (z > 13) return E3(L(7), L(7), L(7));
+        if (z == 13) return E3(L(6), L(7), L(7));
+        if ((z & 1) == 0) return E3(L(j), L(j + 1), L(j));
+        return E3(L(j), L(j + 1), L(j + 2));
     }
     }
-#undef T8
-#undef L8
 }
+
+__device__ __forceinline__ int i8_pred(const int* E, unsigned e) { return (E[e & 31] + 2 * E[(e >> 5) & 31] + E[e >> 10] + 2) >> 2; }
 
 // code_i8, enc/frame.rs:1307-1388: the luma of an Intra8x8 macroblock, block by block in S.i8rec (each
 // block predicted from the filtered edges of the reconstruction so far, its mode the cheapest by SATD +
@@ -111,6 +117,7 @@ __device__ __forceinline__ int i8_sample(const int* E, int mode, int x, int y, i
 // Returns the luma coded block pattern (every lane).
 template <class T>
 __device__ uint32_t code_i8_d(const DecideParams& P, RdSmem<T>& R, int mbx, int mby, bool ta, bool la, bool tra, ironav_mbcode* out) {
+    // the predictor table of R.i8tab is filled once a chain (rd_chain)
     const int lane = threadIdx.x & 31;
     DecideSmem<T>& S = R.s;
     const CodeParams& C = P.C;
@@ -181,6 +188,7 @@ __device__ uint32_t code_i8_d(const DecideParams& P, RdSmem<T>& R, int mbx, int 
             int st = 0, sl = 0;
             for (int i = 0; i < 8; i++) st += E[1 + i], sl += E[17 + i];
             R.i8meta[2] = (ht && hl) ? (st + sl + 8) >> 4 : (hl ? (sl + 4) >> 3 : (ht ? (st + 4) >> 3 : 1 << (bd - 1)));
+            R.e8[25] = R.i8meta[2];
             R.i8meta[1] = cab::pred_mode(S.nbm, R.i8modes, bx * 2, by * 2);
         }
         __syncwarp();
@@ -196,7 +204,7 @@ __device__ uint32_t code_i8_d(const DecideParams& P, RdSmem<T>& R, int mbx, int 
 #pragma unroll
                     for (int k = 0; k < 4; k++) {
                         const int px = (q & 1) * 4 + k, py = (q >> 1) * 4 + r;
-                        d[r * 4 + k] = src_at(S.a, bx * 8 + px, by * 8 + py) - i8_sample(R.e8, mode, px, py, R.i8meta[2]);
+                        d[r * 4 + k] = src_at(S.a, bx * 8 + px, by * 8 + py) - i8_pred(R.e8, R.i8tab[mode * 64 + py * 8 + px]);
                     }
                 s = satd4_d(d);
             }
@@ -215,7 +223,7 @@ __device__ uint32_t code_i8_d(const DecideParams& P, RdSmem<T>& R, int mbx, int 
         }
         __syncwarp();
         const int bm = R.i8meta[0];
-        for (int i = lane; i < 64; i += 32) R.pred8[i] = i8_sample(R.e8, bm, i & 7, i >> 3, R.i8meta[2]);
+        for (int i = lane; i < 64; i += 32) R.pred8[i] = i8_pred(R.e8, R.i8tab[bm * 64 + i]);
         __syncwarp();
         // quant8 (intra rounding) and idct8_add, enc/frame.rs:56-72 and h264/idct.rs:33-74, eight lanes
         const int j = lane & 7;
@@ -532,30 +540,34 @@ __device__ void rd_mb(const RdParams& P, RdSmem<T>& R, const unsigned* i4tab, in
         rd_state(R, 5, false);
         rd_take(P, R, 5, mbx, mby);
     }
-    // each candidate's bins counted from its own copy of the contexts (rd_cost, 1453-1457), a lane a candidate
+    // rd_cost (1453-1457) in the reference's order, each candidate's bins counted by lane 0 from its own copy of
+    // the contexts; SSD + lam2 * bits in f64, rounded as the reference's expression is (no fused multiply-add).
+    // A candidate whose SSD alone is not below the best cost so far cannot win (its bits add a non-negative
+    // amount, and '<' keeps the earlier one), so it is not counted.
+    if (lane == 0) R.best = -1;
+    double bj = 0.0;
     for (int k = 0; k < RD_CANDS; k++) {
+        __syncwarp();
         if (!R.valid[k]) continue;
+        const long long ssd = R.ssd[k];
+        if (R.best >= 0 && __ll2double_rn(ssd) >= bj) continue;
         const uint32_t* s32 = reinterpret_cast<const uint32_t*>(R.live);
         uint32_t* d32 = reinterpret_cast<uint32_t*>(R.cst[k]);
         for (int i = lane; i < 256; i += 32) d32[i] = s32[i];
-    }
-    __syncwarp();
-    if (lane < RD_CANDS && R.valid[lane]) {
-        cab::Counter c = {R.cst[lane], R.step, 0};
-        cab::mb_bins(c, sl, &cand[lane], R.nb[0], R.nb[1], S.nbm);
-        R.bits[lane] = c.bits;
-    }
-    __syncwarp();
-    if (lane == 0) {
-        // SSD + lam2 * bits in f64, rounded as the reference's expression is (no fused multiply-add)
-        int best = -1;
-        double bj = 0.0;
-        for (int k = 0; k < RD_CANDS; k++) {
-            if (!R.valid[k]) continue;
-            const double j = __dadd_rn(__ll2double_rn(R.ssd[k]), __dmul_rn(P.lam2, __dmul_rn((double)R.bits[k], 0.00390625)));
-            if (best < 0 || j < bj) best = k, bj = j;
+        __syncwarp();
+        uint32_t bits = 0;
+        if (lane == 0) {
+            cab::Counter c = {R.cst[k], R.step, 0};
+            cab::mb_bins(c, sl, &cand[k], R.nb[0], R.nb[1], S.nbm);
+            bits = c.bits;
         }
-        R.best = best;
+        bits = __shfl_sync(FULL, bits, 0);
+        const double j = __dadd_rn(__ll2double_rn(ssd), __dmul_rn(P.lam2, __dmul_rn((double)bits, 0.00390625)));
+        if (R.best < 0 || j < bj) {
+            bj = j;
+            __syncwarp();
+            if (lane == 0) R.best = k;
+        }
     }
     __syncwarp();
     const int b = R.best;
@@ -590,6 +602,7 @@ __device__ void rd_chain(const RdParams& P, RdSmem<T>& R, const unsigned* i4tab,
     const int lane = threadIdx.x & 31;
     const AnalyseParams& A = P.D.C.A;
     for (int i = lane; i < cab::STEP_ENTRIES; i += 32) R.step[i] = P.step[i];
+    for (int i = lane; i < 9 * 64; i += 32) R.i8tab[i] = i8_entry(i >> 6, i & 7, (i >> 3) & 7);
     cab::init_states(R.live, P.D.intra != 0, 0, P.D.C.qp, lane, 32);
     __syncwarp();
     for (int mby = P.band_rows[band]; mby < P.band_rows[band + 1]; mby++)
