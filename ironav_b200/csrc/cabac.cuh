@@ -384,16 +384,18 @@ struct Slice {
     int p_slice, t8, nref;
 };
 
-// mb_bins, enc/frame.rs:2028-2279, for I and P slices: the bins of the macroblock `code` up to
-// end_of_slice_flag; l and t its left and top neighbours (avail 0: not in the slice), nbm their Intra NxN
-// modes as pred_mode reads them.
+// The bins of a macroblock fall in groups whose contexts are disjoint: its syntax up to mb_qp_delta
+// (contexts below 85, and 399-401), and the residual blocks of each category with their coded_block_flag
+// (Intra16x16 DC; the luma blocks, 4x4 or 8x8; chroma DC; chroma AC: contexts 85-104 by category, 105 and
+// up by category). So the bits of a macroblock are the sum of the groups' bits, each group walked on its
+// own from the same contexts, and the contexts after it are the union of the groups' updates.
+enum Group { ALL = -1, HEAD = 0, DC16 = 1, LUMA = 2, CDC = 3, CAC = 4, NGROUPS = 5 };
+
+// mb_bins' HEAD group after mb_skip_flag (enc/frame.rs:2046-2244): mb_type, the prediction modes,
+// sub_mb_type, ref_idx, mvd, coded_block_pattern, transform_size_8x8_flag and mb_qp_delta.
 template <class S>
-__device__ void mb_bins(S& c, const Slice& sl, const ironav_mbcode* code, const Nb& L, const Nb& T, const int* nbm) {
+__device__ void head_bins(S& c, const Slice& sl, const ironav_mbcode* code, const Nb& L, const Nb& T, const int* nbm) {
     const bool la = L.avail, ta = T.avail;
-    if (sl.p_slice) {
-        c.decision(11 + (la && !L.skip) + (ta && !T.skip), code->skip);
-        if (code->skip) return;
-    }
     const int kind = code->kind, cbp = code->res.cbp, cbpl = cbp & 15, cbpc = cbp >> 4;
     // mb_type
     if (kind == KIND_INTER) {
@@ -509,15 +511,30 @@ __device__ void mb_bins(S& c, const Slice& sl, const ironav_mbcode* code, const 
         c.decision(399 + (la && L.t8x8) + (ta && T.t8x8), code->res.t8x8);
     if (!cbp && kind != KIND_I16) return;
     c.decision(60, 0);  // mb_qp_delta 0, after a macroblock without a change
+}
+
+// mb_bins, enc/frame.rs:2028-2279, for I and P slices: the bins of the macroblock `code` up to
+// end_of_slice_flag (all of them, or one group's); l and t its left and top neighbours (avail 0: not in
+// the slice), nbm their Intra NxN modes as pred_mode reads them.
+template <class S>
+__device__ void mb_bins(S& c, const Slice& sl, const ironav_mbcode* code, const Nb& L, const Nb& T, const int* nbm, int group = ALL) {
+    const bool la = L.avail, ta = T.avail;
+    if (sl.p_slice) {
+        if (group == ALL || group == HEAD) c.decision(11 + (la && !L.skip) + (ta && !T.skip), code->skip);
+        if (code->skip) return;
+    }
+    if (group == ALL || group == HEAD) head_bins(c, sl, code, L, T, nbm);
+    const int kind = code->kind, cbp = code->res.cbp, cbpl = cbp & 15, cbpc = cbp >> 4;
+    if (!cbp && kind != KIND_I16) return;
     // an unavailable neighbour counts as a coded block for an intra macroblock
     const int un = kind != KIND_INTER;
-    if (kind == KIND_I16)
+    if (kind == KIND_I16 && (group == ALL || group == DC16))
         block(c, 0, 85 + (la ? (L.cbf_dc & 1) != 0 : un) + 2 * (ta ? (T.cbf_dc & 1) != 0 : un), code->dc, 16);
     const int cat = kind == KIND_I16 ? 1 : 2, base = kind == KIND_I16 ? 89 : 93;
-    if (code->res.t8x8) {
+    if (code->res.t8x8 && (group == ALL || group == LUMA)) {
         for (int i8 = 0; i8 < 4; i8++)
             if (cbpl & (1 << i8)) block(c, 5, -1, code->res.luma8[i8], 64);
-    } else {
+    } else if (group == ALL || group == LUMA) {
         for (int n = 0; n < 16; n++) {
             if (!(cbpl & (1 << (n >> 2)))) continue;
             const int bx = ((n >> 2) & 1) * 2 + (n & 1), by = ((n >> 3) & 1) * 2 + ((n >> 1) & 1);
@@ -527,12 +544,12 @@ __device__ void mb_bins(S& c, const Slice& sl, const ironav_mbcode* code, const 
             block(c, cat, base + fa + 2 * fb, cat == 1 ? blk + 1 : blk, cat == 1 ? 15 : 16);
         }
     }
-    if (cbpc > 0)
+    if (cbpc > 0 && (group == ALL || group == CDC))
         for (int comp = 0; comp < 2; comp++) {
             const int m = 2 << comp;
             block(c, 3, 97 + (la ? (L.cbf_dc & m) != 0 : un) + 2 * (ta ? (T.cbf_dc & m) != 0 : un), code->res.cdc[comp], 4);
         }
-    if (cbpc == 2)
+    if (cbpc == 2 && (group == ALL || group == CAC))
         for (int comp = 0; comp < 2; comp++)
             for (int blk = 0; blk < 4; blk++) {
                 const int bx = blk & 1, by = blk >> 1;

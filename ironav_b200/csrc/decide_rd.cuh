@@ -7,10 +7,11 @@
 // CTA a band, the bands side by side). For each macroblock the warp codes every candidate the reference
 // tries, in its order (P_Skip, best_inter's partitioning with the 4x4 and, with transform8, the 8x8
 // transform, Intra16x16, Intra4x4, Intra8x8, each intra one with its chroma), each into the picture and
-// then into shared memory (code and reconstruction), with its squared error; then, in the reference's
-// order, lane 0 counts each candidate's bins on its own copy of the contexts (the counter of cabac.cuh)
-// unless its squared error alone already rules it out, keeps the least SSD + lambda2 * bits (strict '<'),
-// and the warp copies the kept candidate's code, reconstruction and advanced contexts into place.
+// then into shared memory (code and reconstruction), with its squared error; then the candidates' bins are
+// counted at once, each on its own copy of the contexts (the counter of cabac.cuh), five lanes a candidate
+// (one per group of disjoint contexts); lane 0 keeps the least SSD + lambda2 * bits in the reference's
+// order (strict '<'), and the warp copies the kept candidate's code, reconstruction and advanced contexts
+// into place.
 //
 // The candidates reuse decide mode's warp-level coders (decide.cuh, residual.cuh); Intra8x8 (code_i8,
 // enc/frame.rs:1307-1388) is coded here: block by block, its edges filtered (8.3.2.2.1), nine modes'
@@ -46,6 +47,7 @@ struct RdSmem {
     cab::Nb done;                    // the macroblock just decided, the next one's left
     ironav_mbstate state[RD_CANDS];  // each candidate's MbState
     long long ssd[RD_CANDS];
+    unsigned bits[RD_CANDS];
     int valid[RD_CANDS];
     int best;
     // the Intra8x8 trial
@@ -354,6 +356,20 @@ __device__ void rd_take(const RdParams& P, RdSmem<T>& R, int k, int mbx, int mby
     __syncwarp();
 }
 
+// An intra candidate's chroma taken from another's (code_intra_chroma's outputs: mode, DC and AC levels, counts).
+__device__ __forceinline__ void rd_chroma_copy(const ironav_mbcode& from, ironav_mbcode* o) {
+    const int lane = threadIdx.x & 31;
+    __syncwarp();
+    const uint32_t* ac = reinterpret_cast<const uint32_t*>(from.res.cac);
+    uint32_t* oc = reinterpret_cast<uint32_t*>(o->res.cac);
+    for (int i = lane; i < (int)(sizeof(from.res.cac) / 4); i += 32) oc[i] = ac[i];
+    if (lane < (int)(sizeof(from.res.cdc) / 4)) reinterpret_cast<uint32_t*>(o->res.cdc)[lane] = reinterpret_cast<const uint32_t*>(from.res.cdc)[lane];
+    if (lane < (int)(sizeof(from.res.cnnz) / 4))
+        reinterpret_cast<uint32_t*>(o->res.cnnz)[lane] = reinterpret_cast<const uint32_t*>(from.res.cnnz)[lane];
+    if (lane == 0) o->chroma_mode = from.chroma_mode;
+    __syncwarp();
+}
+
 // The MbState of a coded candidate: the inter ones' from inter_tail (S.a.out), the intra ones' without motion.
 template <class T>
 __device__ __forceinline__ void rd_state(RdSmem<T>& R, int k, bool inter) {
@@ -487,12 +503,16 @@ __device__ void rd_mb(const RdParams& P, RdSmem<T>& R, const unsigned* i4tab, in
             __syncwarp();
         }
     }
-    // Intra16x16 in best_i16's mode, with its chroma
+    // Intra16x16 in best_i16's mode, with its chroma. code_intra_chroma reads only the chroma around the
+    // macroblock and writes only its chroma, so the Intra4x4 and Intra8x8 candidates take this one's
+    // (its mode, levels, counts and pattern; the reconstruction stays in the picture)
+    uint32_t ccbp = 0;
     {
         ironav_mbcode* o = &cand[3];
         code_init(o);
         uint32_t cbp = code_i16_d(D, S, mbx, mby, i16.x, ta, la, o);
-        cbp |= code_intra_chroma_d(D, S, mbx, mby, ta, la, o);
+        ccbp = code_intra_chroma_d(D, S, mbx, mby, ta, la, o);
+        cbp |= ccbp;
         if (lane == 0) {
             o->kind = KIND_I16;
             o->i16_mode = (uint8_t)i16.x;
@@ -522,7 +542,8 @@ __device__ void rd_mb(const RdParams& P, RdSmem<T>& R, const unsigned* i4tab, in
         for (int i8 = 0; i8 < 4; i8++)
             if (bal & (0x33u << ((i8 >> 1) * 8 + (i8 & 1) * 2))) cbp |= 1u << i8;
         __syncwarp();
-        cbp |= code_intra_chroma_d(D, S, mbx, mby, ta, la, o);
+        rd_chroma_copy(cand[3], o);
+        cbp |= ccbp;
         if (lane == 0) {
             o->kind = KIND_I4;
             o->res.cbp = (uint8_t)cbp;
@@ -535,39 +556,42 @@ __device__ void rd_mb(const RdParams& P, RdSmem<T>& R, const unsigned* i4tab, in
         ironav_mbcode* o = &cand[5];
         code_init(o);
         uint32_t cbp = code_i8_d(D, R, mbx, mby, ta, la, tra, o);
-        cbp |= code_intra_chroma_d(D, S, mbx, mby, ta, la, o);
+        rd_chroma_copy(cand[3], o);
+        cbp |= ccbp;
         if (lane == 0) o->res.cbp = (uint8_t)cbp;
         rd_state(R, 5, false);
         rd_take(P, R, 5, mbx, mby);
     }
-    // rd_cost (1453-1457) in the reference's order, each candidate's bins counted by lane 0 from its own copy of
-    // the contexts; SSD + lam2 * bits in f64, rounded as the reference's expression is (no fused multiply-add).
-    // A candidate whose SSD alone is not below the best cost so far cannot win (its bits add a non-negative
-    // amount, and '<' keeps the earlier one), so it is not counted.
-    if (lane == 0) R.best = -1;
-    double bj = 0.0;
+    // rd_cost (1453-1457): each candidate's bins counted from its own copy of the contexts, on five lanes a
+    // candidate, one per group of disjoint contexts (cab::Group), the groups' bits summed; then lane 0 keeps
+    // the least SSD + lam2 * bits in the reference's order (strict '<'), in f64 rounded as the reference's
+    // expression is (no fused multiply-add).
     for (int k = 0; k < RD_CANDS; k++) {
-        __syncwarp();
         if (!R.valid[k]) continue;
-        const long long ssd = R.ssd[k];
-        if (R.best >= 0 && __ll2double_rn(ssd) >= bj) continue;
         const uint32_t* s32 = reinterpret_cast<const uint32_t*>(R.live);
         uint32_t* d32 = reinterpret_cast<uint32_t*>(R.cst[k]);
         for (int i = lane; i < 256; i += 32) d32[i] = s32[i];
-        __syncwarp();
-        uint32_t bits = 0;
-        if (lane == 0) {
+    }
+    if (lane < RD_CANDS) R.bits[lane] = 0;
+    __syncwarp();
+    {
+        const int k = lane / cab::NGROUPS, g = lane % cab::NGROUPS;
+        if (k < RD_CANDS && R.valid[k]) {
             cab::Counter c = {R.cst[k], R.step, 0};
-            cab::mb_bins(c, sl, &cand[k], R.nb[0], R.nb[1], S.nbm);
-            bits = c.bits;
+            cab::mb_bins(c, sl, &cand[k], R.nb[0], R.nb[1], S.nbm, g);
+            if (c.bits) atomicAdd(&R.bits[k], c.bits);
         }
-        bits = __shfl_sync(FULL, bits, 0);
-        const double j = __dadd_rn(__ll2double_rn(ssd), __dmul_rn(P.lam2, __dmul_rn((double)bits, 0.00390625)));
-        if (R.best < 0 || j < bj) {
-            bj = j;
-            __syncwarp();
-            if (lane == 0) R.best = k;
+    }
+    __syncwarp();
+    if (lane == 0) {
+        int best = -1;
+        double bj = 0.0;
+        for (int k = 0; k < RD_CANDS; k++) {
+            if (!R.valid[k]) continue;
+            const double j = __dadd_rn(__ll2double_rn(R.ssd[k]), __dmul_rn(P.lam2, __dmul_rn((double)R.bits[k], 0.00390625)));
+            if (best < 0 || j < bj) best = k, bj = j;
         }
+        R.best = best;
     }
     __syncwarp();
     const int b = R.best;
