@@ -103,6 +103,7 @@ struct ironav_ctx {
     uint32_t* d_cab_step = nullptr;
     int* d_band_rows = nullptr;
     uint32_t* d_rd_nb = nullptr;
+    uint8_t* d_rd_scr = nullptr;  // the three-warp decision's scratch planes
     uint32_t* d_cab_out = nullptr;
     unsigned long long cab_region_words = 0;
     uint32_t* d_cab_bytes = nullptr;

@@ -33,11 +33,15 @@ struct RdParams {
     double lam2;            // 1.6 * 2^((QP'Y - 12) / 3), computed on the host in f64 as the reference does
     int nbands;
     int t8;                 // transform_8x8_mode_flag
+    // the three-warp form: the intra warps' scratch planes (warp 1's luma; warp 2's luma, Cb, Cr), pw x ph and
+    // cw x ch samples, rows scr_ys and scr_cs samples apart
+    uint8_t* scr[4];
+    int scr_ys, scr_cs;
 };
 
-template <class T>
+template <class T, int W>
 struct RdSmem {
-    DecideSmem<T> s;
+    DecideSmem<T> s[W];              // each warp's working set
     ironav_mbcode cand[RD_CANDS];    // the candidates' codes
     T crec[RD_CANDS][384];           // and reconstructions (luma, Cb, Cr)
     uint8_t live[1024];              // the chain's contexts after the macroblocks before this one
@@ -47,9 +51,12 @@ struct RdSmem {
     cab::Nb done;                    // the macroblock just decided, the next one's left
     ironav_mbstate state[RD_CANDS];  // each candidate's MbState
     long long ssd[RD_CANDS];
+    long long cssd[RD_CANDS];        // the chroma part of ssd
     unsigned bits[RD_CANDS];
     int valid[RD_CANDS];
     int best;
+    int skip;                        // the three-warp form: the P_Skip tests' verdict, and the intra chroma's
+    uint32_t ccbp;                   // coded block pattern bits
     // the Intra8x8 trial
     int i8rec[256];       // its reconstruction
     int raw[25], e8[26];  // a block's edges, raw and filtered: [0] top-left, [1 + i] the 16 above, [17 + j] the 8 left,
@@ -115,13 +122,14 @@ __device__ __forceinline__ int i8_pred(const int* E, unsigned e) { return (E[e &
 // code_i8, enc/frame.rs:1307-1388: the luma of an Intra8x8 macroblock, block by block in S.i8rec (each
 // block predicted from the filtered edges of the reconstruction so far, its mode the cheapest by SATD +
 // lambda * (1 predicted, 4 otherwise), quantised with the intra rounding), its levels, modes and counts
-// into out (zeroed by the caller with the Intra4x4 modes 2), and the reconstruction into the picture.
+// into out (zeroed by the caller with the Intra4x4 modes 2), and the reconstruction into wy.
 // Returns the luma coded block pattern (every lane).
-template <class T>
-__device__ uint32_t code_i8_d(const DecideParams& P, RdSmem<T>& R, int mbx, int mby, bool ta, bool la, bool tra, ironav_mbcode* out) {
-    // the predictor table of R.i8tab is filled once a chain (rd_chain)
+template <class T, int W>
+__device__ uint32_t code_i8_d(const DecideParams& P, DecideSmem<T>& S, RdSmem<T, W>& R, int mbx, int mby, bool ta, bool la, bool tra,
+                              ironav_mbcode* out, T* wy, int wys) {
+    // P.C.rec: the picture the edges are read from; wy (rows wys samples apart): where the luma goes. The
+    // predictor table of R.i8tab is filled once a chain (rd_chain)
     const int lane = threadIdx.x & 31;
-    DecideSmem<T>& S = R.s;
     const CodeParams& C = P.C;
     const int bd = C.bd, maxv = (1 << bd) - 1, lam = C.A.lambda;
     const int qp = C.qp + 6 * (bd - 8), m6 = qp % 6, qbits = 16 + qp / 6, f = (1 << qbits) / 3;
@@ -304,8 +312,7 @@ __device__ uint32_t code_i8_d(const DecideParams& P, RdSmem<T>& R, int mbx, int 
         if (nz > 0) cbp |= 1u << i8;
         __syncwarp();
     }
-    T* RY = reinterpret_cast<T*>(C.rec[0]);
-    for (int i = lane; i < 256; i += 32) RY[(size_t)(y0 + (i >> 4)) * C.ys + x0 + (i & 15)] = (T)R.i8rec[i];
+    for (int i = lane; i < 256; i += 32) wy[(size_t)(y0 + (i >> 4)) * wys + x0 + (i & 15)] = (T)R.i8rec[i];
     if (lane < 16) out->modes[lane] = R.i8modes[lane];
     if (lane == 0) {
         out->kind = KIND_I8;
@@ -323,21 +330,21 @@ __device__ __forceinline__ void code_init(ironav_mbcode* o) {
     __syncwarp();
 }
 
-// A candidate coded into the picture: its squared error (ssd_mb, enc/frame.rs:1432-1449) and a copy of its
-// reconstruction (save_mb, 1406-1417); the candidate counts from here on.
-template <class T>
-__device__ void rd_take(const RdParams& P, RdSmem<T>& R, int k, int mbx, int mby) {
+// A candidate coded into the planes C (the picture, or a warp's scratch planes): its squared error (ssd_mb,
+// enc/frame.rs:1432-1449) and a copy of its reconstruction (save_mb, 1406-1417); chroma false: the luma
+// only, the chroma added later from another candidate's. The candidate counts from here on.
+template <class T, int W>
+__device__ void rd_take(const CodeParams& C, RdSmem<T, W>& R, const DecideSmem<T>& S, int k, int mbx, int mby, bool chroma = true) {
     const int lane = threadIdx.x & 31;
-    const CodeParams& C = P.D.C;
     const T* SC = reinterpret_cast<const T*>(C.src_c);
     T* dst = R.crec[k];
     __syncwarp();
-    long long ssd = 0;
-    for (int i = lane; i < 384; i += 32) {
+    long long ssd = 0, cssd = 0;
+    for (int i = lane; i < (chroma ? 384 : 256); i += 32) {
         int r, s;
         if (i < 256) {
             r = reinterpret_cast<const T*>(C.rec[0])[(size_t)(mby * 16 + (i >> 4)) * C.ys + mbx * 16 + (i & 15)];
-            s = src_at(R.s.a, i & 15, i >> 4);
+            s = src_at(S.a, i & 15, i >> 4);
         } else {
             const int cc = (i - 256) >> 6, j = (i - 256) & 63, cy = mby * 8 + (j >> 3), cx = mbx * 8 + (j & 7);
             r = reinterpret_cast<const T*>(C.rec[1 + cc])[(size_t)cy * C.cs + cx];
@@ -345,12 +352,17 @@ __device__ void rd_take(const RdParams& P, RdSmem<T>& R, int k, int mbx, int mby
         }
         dst[i] = (T)r;
         const long long d = s - r;
-        ssd += d * d;
+        if (i < 256) ssd += d * d;
+        else cssd += d * d;
     }
 #pragma unroll
-    for (int off = 16; off >= 1; off >>= 1) ssd += __shfl_xor_sync(FULL, ssd, off);
+    for (int off = 16; off >= 1; off >>= 1) {
+        ssd += __shfl_xor_sync(FULL, ssd, off);
+        cssd += __shfl_xor_sync(FULL, cssd, off);
+    }
     if (lane == 0) {
-        R.ssd[k] = ssd;
+        R.ssd[k] = ssd + cssd;
+        R.cssd[k] = cssd;
         R.valid[k] = 1;
     }
     __syncwarp();
@@ -371,13 +383,13 @@ __device__ __forceinline__ void rd_chroma_copy(const ironav_mbcode& from, ironav
 }
 
 // The MbState of a coded candidate: the inter ones' from inter_tail (S.a.out), the intra ones' without motion.
-template <class T>
-__device__ __forceinline__ void rd_state(RdSmem<T>& R, int k, bool inter) {
+template <class T, int W>
+__device__ __forceinline__ void rd_state(RdSmem<T, W>& R, const DecideSmem<T>& S, int k, bool inter) {
     const int lane = threadIdx.x & 31;
     __syncwarp();
     uint32_t* d = reinterpret_cast<uint32_t*>(&R.state[k]);
     if (inter) {
-        if (lane < 18) d[lane] = reinterpret_cast<const uint32_t*>(&R.s.a.out)[lane];
+        if (lane < 18) d[lane] = reinterpret_cast<const uint32_t*>(&S.a.out)[lane];
     } else {
         // inter 0, refs -1, pad 0, no motion (bytes 0-7, then the vectors)
         if (lane < 18) d[lane] = lane == 0 ? 0xFFFFFF00u : (lane == 1 ? 0x000000FFu : 0u);
@@ -388,12 +400,12 @@ __device__ __forceinline__ void rd_state(RdSmem<T>& R, int k, bool inter) {
 // decide_rd for one macroblock (after code_mb's P_Skip tests, best_i16 and best_inter; enc/frame.rs:715-760,
 // 1462-1513), its bins then carried into the chain's contexts (write_mb_cabac's effect on them, 2020-2025).
 template <class T>
-__device__ void rd_mb(const RdParams& P, RdSmem<T>& R, const unsigned* i4tab, int mb, int mbx, int mby) {
+__device__ void rd_mb(const RdParams& P, RdSmem<T, 1>& R, const unsigned* i4tab, int mb, int mbx, int mby) {
     const int lane = threadIdx.x & 31;
     const DecideParams& D = P.D;
     const AnalyseParams& A = D.C.A;
     const CodeParams& C = D.C;
-    DecideSmem<T>& S = R.s;
+    DecideSmem<T>& S = R.s[0];
     const bool ta = mby > A.band_start[mby], la = mbx > 0, tra = ta && mbx + 1 < A.mb_w;
     const cab::Slice sl = {D.intra ? 0 : 1, P.t8, D.intra ? 0 : A.nact};
     ironav_mbcode* out = &D.codes[mb];
@@ -462,8 +474,8 @@ __device__ void rd_mb(const RdParams& P, RdSmem<T>& R, const unsigned* i4tab, in
         inter_tail(D, S, Dd, o);
         if (lane < 16) o->mvds[lane][0] = o->mvds[lane][1] = 0;
         if (lane == 0) o->skip = 1;
-        rd_state(R, 0, true);
-        rd_take(P, R, 0, mbx, mby);
+        rd_state(R, S, 0, true);
+        rd_take(C, R, S, 0, mbx, mby);
         // best_inter's partitioning with the 4x4 transform; with nothing coded and the skip vector, it would be
         // P_Skip at a higher price
         o = &cand[1];
@@ -484,8 +496,8 @@ __device__ void rd_mb(const RdParams& P, RdSmem<T>& R, const unsigned* i4tab, in
         __syncwarp();
         const uint32_t cbp = code_inter_mb<T>(C, S.c, mb, &o->res);
         inter_tail(D, S, Dd, o);
-        rd_state(R, 1, true);
-        rd_take(P, R, 1, mbx, mby);
+        rd_state(R, S, 1, true);
+        rd_take(C, R, S, 1, mbx, mby);
         if (lane == 0 && cbp == 0 && part == 0 && Dd.mvs[0][0] == sv.x && Dd.mvs[0][1] == sv.y && bestr == 0) R.valid[1] = 0;
         __syncwarp();
         // the 8x8 transform needs every 8x8 block of P_8x8 to be a single 8x8 partition; without luma levels it
@@ -497,8 +509,8 @@ __device__ void rd_mb(const RdParams& P, RdSmem<T>& R, const unsigned* i4tab, in
             __syncwarp();
             code_inter_mb<T>(C, S.c, mb, &o->res);
             inter_tail(D, S, Dd, o);
-            rd_state(R, 2, true);
-            rd_take(P, R, 2, mbx, mby);
+            rd_state(R, S, 2, true);
+            rd_take(C, R, S, 2, mbx, mby);
             if (lane == 0 && !o->res.t8x8) R.valid[2] = 0;
             __syncwarp();
         }
@@ -518,8 +530,8 @@ __device__ void rd_mb(const RdParams& P, RdSmem<T>& R, const unsigned* i4tab, in
             o->i16_mode = (uint8_t)i16.x;
             o->res.cbp = (uint8_t)cbp;
         }
-        rd_state(R, 3, false);
-        rd_take(P, R, 3, mbx, mby);
+        rd_state(R, S, 3, false);
+        rd_take(C, R, S, 3, mbx, mby);
     }
     // Intra4x4, block by block from its own reconstruction, with its chroma
     {
@@ -548,19 +560,19 @@ __device__ void rd_mb(const RdParams& P, RdSmem<T>& R, const unsigned* i4tab, in
             o->kind = KIND_I4;
             o->res.cbp = (uint8_t)cbp;
         }
-        rd_state(R, 4, false);
-        rd_take(P, R, 4, mbx, mby);
+        rd_state(R, S, 4, false);
+        rd_take(C, R, S, 4, mbx, mby);
     }
     // Intra8x8 with its chroma
     if (P.t8) {
         ironav_mbcode* o = &cand[5];
         code_init(o);
-        uint32_t cbp = code_i8_d(D, R, mbx, mby, ta, la, tra, o);
+        uint32_t cbp = code_i8_d(D, S, R, mbx, mby, ta, la, tra, o, reinterpret_cast<T*>(C.rec[0]), C.ys);
         rd_chroma_copy(cand[3], o);
         cbp |= ccbp;
         if (lane == 0) o->res.cbp = (uint8_t)cbp;
-        rd_state(R, 5, false);
-        rd_take(P, R, 5, mbx, mby);
+        rd_state(R, S, 5, false);
+        rd_take(C, R, S, 5, mbx, mby);
     }
     // rd_cost (1453-1457): each candidate's bins counted from its own copy of the contexts, on five lanes a
     // candidate, one per group of disjoint contexts (cab::Group), the groups' bits summed; then lane 0 keeps
@@ -622,7 +634,7 @@ __device__ void rd_mb(const RdParams& P, RdSmem<T>& R, const unsigned* i4tab, in
 // One chain: slice band `band` in raster order (FrameCoder::encode, enc/frame.rs:461-478) from the slice's
 // initial contexts (cabac_init_idc 0, QP_Y).
 template <class T>
-__device__ void rd_chain(const RdParams& P, RdSmem<T>& R, const unsigned* i4tab, int band) {
+__device__ void rd_chain(const RdParams& P, RdSmem<T, 1>& R, const unsigned* i4tab, int band) {
     const int lane = threadIdx.x & 31;
     const AnalyseParams& A = P.D.C.A;
     for (int i = lane; i < cab::STEP_ENTRIES; i += 32) R.step[i] = P.step[i];
@@ -633,12 +645,12 @@ __device__ void rd_chain(const RdParams& P, RdSmem<T>& R, const unsigned* i4tab,
         for (int mbx = 0; mbx < A.mb_w; mbx++) {
             const int mb = mby * A.mb_w + mbx;
             if (lane == 0) {
-                R.s.a.mb = mb;
-                R.s.a.mbx = mbx;
-                R.s.a.mby = mby;
+                R.s[0].a.mb = mb;
+                R.s[0].a.mbx = mbx;
+                R.s[0].a.mby = mby;
             }
             __syncwarp();
-            load_neighbours(A, R.s.a, A.states_out);
+            load_neighbours(A, R.s[0].a, A.states_out);
             rd_mb<T>(P, R, i4tab, mb, mbx, mby);
         }
 }
@@ -646,7 +658,7 @@ __device__ void rd_chain(const RdParams& P, RdSmem<T>& R, const unsigned* i4tab,
 // Decide mode under CABAC for one stream: CTA i, one warp, walks slice band i.
 template <class T>
 __global__ void __launch_bounds__(32) decide_rd_kernel(const __grid_constant__ RdParams P) {
-    __shared__ RdSmem<T> R;
+    __shared__ RdSmem<T, 1> R;
     __shared__ unsigned i4tab[9 * 17];
     fill_i4tab(i4tab);
     if ((int)blockIdx.x >= P.nbands) return;
@@ -658,7 +670,7 @@ __global__ void __launch_bounds__(32) decide_rd_kernel(const __grid_constant__ R
 template <class T>
 __global__ void __launch_bounds__(32) decide_rd_batch_kernel(const RdParams* __restrict__ table, const uint32_t* __restrict__ chains,
                                                              int nchains) {
-    __shared__ RdSmem<T> R;
+    __shared__ RdSmem<T, 1> R;
     __shared__ RdParams prm;
     __shared__ unsigned i4tab[9 * 17];
     fill_i4tab(i4tab);
@@ -670,6 +682,293 @@ __global__ void __launch_bounds__(32) decide_rd_batch_kernel(const RdParams* __r
     __syncwarp();
     rd_chain<T>(prm, R, i4tab, (int)(e & 0xFFFFu));
 }
+
+// ---- the three-warp form: one chain's macroblock on three warps ----------------------------------------
+// Warp 0 runs code_mb's P_Skip tests, best_inter and the inter candidates into the picture (as the one-warp
+// form); when the macroblock passes the P_Skip tests, warp 1 codes Intra4x4 and warp 2 Intra16x16 (with the
+// intra chroma) and then Intra8x8 beside it, each into its own scratch planes (their edges read from the
+// picture, which warp 0 writes only inside the macroblock). Warp 0 then prices every candidate and commits
+// the kept one. The warps meet at three CTA barriers a macroblock (after the P_Skip tests; after the
+// candidates, when there are any; after the commit), every warp at every one.
+constexpr int RD3_WARPS = 3;
+
+template <class T>
+__device__ void rd_mb3(const RdParams& P, const DecideParams* dw, RdSmem<T, RD3_WARPS>& R, const unsigned* i4tab, int mb, int mbx,
+                       int mby) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const DecideParams& D = P.D;
+    const AnalyseParams& A = D.C.A;
+    const CodeParams& C = D.C;
+    DecideSmem<T>& S = R.s[w];
+    const bool ta = mby > A.band_start[mby], la = mbx > 0, tra = ta && mbx + 1 < A.mb_w;
+    const cab::Slice sl = {D.intra ? 0 : 1, P.t8, D.intra ? 0 : A.nact};
+    ironav_mbcode* out = &D.codes[mb];
+    ironav_mbcode* cand = R.cand;
+    if (lane == 0) {
+        S.a.mb = mb;
+        S.a.mbx = mbx;
+        S.a.mby = mby;
+    }
+    __syncwarp();
+    stage_source(A, S.a);
+    int2 sv = make_int2(0, 0);
+    if (w == 0) {
+        load_neighbours(A, S.a, A.states_out);
+        code_init(out);
+        if (lane < cab::NB_WORDS) {
+            reinterpret_cast<uint32_t*>(&R.nb[0])[lane] = la ? reinterpret_cast<const uint32_t*>(&R.done)[lane] : 0u;
+            reinterpret_cast<uint32_t*>(&R.nb[1])[lane] = ta ? P.nbs[(size_t)(mb - A.mb_w) * cab::NB_WORDS + lane] : 0u;
+        }
+        if (lane < RD_CANDS) R.valid[lane] = 0;
+        __syncwarp();
+        const bool skip = !D.intra && skip_tests_d<T>(D, S, mb, mbx, mby, out, &sv);
+        if (lane == 0) R.skip = skip;
+    }
+    __syncthreads();
+    if (R.skip) {
+        if (w == 0) {
+            // P_Skip without a rate-distortion choice; its one bin still moves the contexts
+            if (lane == 0) {
+                cab::Counter c = {R.live, R.step, 0};
+                cab::mb_bins(c, sl, out, R.nb[0], R.nb[1], S.nbm);
+            }
+            if (lane < 18) reinterpret_cast<uint32_t*>(&A.states_out[mb])[lane] = reinterpret_cast<const uint32_t*>(&S.a.out)[lane];
+            __syncwarp();
+            cab::nb_of_warp(out, &R.done);
+            if (lane < cab::NB_WORDS) P.nbs[(size_t)mb * cab::NB_WORDS + lane] = reinterpret_cast<const uint32_t*>(&R.done)[lane];
+            __syncwarp();
+        }
+        __syncthreads();
+        return;
+    }
+    load_intra_neighbours(D, S, mb, mbx, mby, ta, la, tra);
+    if (w == 0 && !D.intra) {
+        // best_inter, enc/frame.rs:839-849, and the inter candidates (as rd_mb)
+        int part = 0, cost = BIG, bestr = 0;
+        uint32_t sub = 0;
+        for (int r = 0; r < A.nact; r++) {
+            const int4 bi = best_inter_or_learned(A, S.a, r);
+            if (r == 0 || bi.x < cost) {
+                part = bi.y;
+                cost = bi.x;
+                bestr = r;
+                sub = (uint32_t)bi.z;
+                if (lane < 16) {
+                    S.a.win_mvs[lane][0] = S.a.best_mvs[lane][0];
+                    S.a.win_mvs[lane][1] = S.a.best_mvs[lane][1];
+                }
+                __syncwarp();
+            }
+        }
+        ironav_interdec& Dd = *reinterpret_cast<ironav_interdec*>(S.c.dec);
+        ironav_mbcode* o = &cand[0];
+        code_init(o);
+        if (lane == 0) {
+            Dd.mode = 1;
+            Dd.part = 0;
+            Dd.t8 = 0;
+            for (int k = 0; k < 4; k++) Dd.sub[k] = Dd.refs[k] = 0;
+        }
+        if (lane < 16) {
+            Dd.mvs[lane][0] = (int16_t)sv.x;
+            Dd.mvs[lane][1] = (int16_t)sv.y;
+        }
+        __syncwarp();
+        code_inter_mb<T>(C, S.c, mb, &o->res);
+        inter_tail(D, S, Dd, o);
+        if (lane < 16) o->mvds[lane][0] = o->mvds[lane][1] = 0;
+        if (lane == 0) o->skip = 1;
+        rd_state(R, S, 0, true);
+        rd_take(C, R, S, 0, mbx, mby);
+        o = &cand[1];
+        code_init(o);
+        if (lane == 0) {
+            Dd.mode = 2;
+            Dd.part = (uint8_t)part;
+            Dd.t8 = 0;
+            for (int k = 0; k < 4; k++) {
+                Dd.sub[k] = (uint8_t)((sub >> (8 * k)) & 0xff);
+                Dd.refs[k] = (uint8_t)bestr;
+            }
+        }
+        if (lane < 16) {
+            Dd.mvs[lane][0] = S.a.win_mvs[lane][0];
+            Dd.mvs[lane][1] = S.a.win_mvs[lane][1];
+        }
+        __syncwarp();
+        const uint32_t cbp = code_inter_mb<T>(C, S.c, mb, &o->res);
+        inter_tail(D, S, Dd, o);
+        rd_state(R, S, 1, true);
+        rd_take(C, R, S, 1, mbx, mby);
+        if (lane == 0 && cbp == 0 && part == 0 && Dd.mvs[0][0] == sv.x && Dd.mvs[0][1] == sv.y && bestr == 0) R.valid[1] = 0;
+        __syncwarp();
+        if (P.t8 && sub == 0) {
+            o = &cand[2];
+            code_init(o);
+            if (lane == 0) Dd.t8 = 1;
+            __syncwarp();
+            code_inter_mb<T>(C, S.c, mb, &o->res);
+            inter_tail(D, S, Dd, o);
+            rd_state(R, S, 2, true);
+            rd_take(C, R, S, 2, mbx, mby);
+            if (lane == 0 && !o->res.t8x8) R.valid[2] = 0;
+            __syncwarp();
+        }
+    } else if (w == 1) {
+        // Intra4x4 into warp 1's luma plane; its chroma is Intra16x16's (taken after the barrier)
+        const DecideParams& Dw = dw[0];
+        ironav_mbcode* o = &cand[4];
+        code_init(o);
+        code_i4_trial(Dw, S, i4tab, ta, la, tra);
+        T* RY = reinterpret_cast<T*>(Dw.C.rec[0]);
+        for (int i = lane; i < 256; i += 32) RY[(size_t)(mby * 16 + (i >> 4)) * Dw.C.ys + mbx * 16 + (i & 15)] = (T)S.i4rec[i];
+        if (lane < 16) {
+            uint32_t* lw = reinterpret_cast<uint32_t*>(o->res.luma[lane]);
+            const uint32_t* src = reinterpret_cast<const uint32_t*>(S.i4lv[lane]);
+#pragma unroll
+            for (int k = 0; k < 8; k++) lw[k] = src[k];
+            o->res.nnz[lane] = S.i4nnz[lane];
+            o->modes[lane] = S.i4modes[lane];
+        }
+        const unsigned bal = __ballot_sync(FULL, lane < 16 && S.i4nnz[lane] > 0);
+        uint32_t cbp = 0;
+#pragma unroll
+        for (int i8 = 0; i8 < 4; i8++)
+            if (bal & (0x33u << ((i8 >> 1) * 8 + (i8 & 1) * 2))) cbp |= 1u << i8;
+        if (lane == 0) {
+            o->kind = KIND_I4;
+            o->res.cbp = (uint8_t)cbp;
+        }
+        rd_state(R, S, 4, false);
+        rd_take(Dw.C, R, S, 4, mbx, mby, false);
+    } else if (w == 2) {
+        // Intra16x16 in best_i16's mode with the intra chroma, then Intra8x8, into warp 2's planes
+        const DecideParams& Dw = dw[1];
+        const int2 i16 = best_i16_d(Dw, S, ta, la);
+        ironav_mbcode* o = &cand[3];
+        code_init(o);
+        uint32_t cbp = code_i16_d(Dw, S, mbx, mby, i16.x, ta, la, o);
+        const uint32_t ccbp = code_intra_chroma_d(Dw, S, mbx, mby, ta, la, o);
+        cbp |= ccbp;
+        if (lane == 0) {
+            o->kind = KIND_I16;
+            o->i16_mode = (uint8_t)i16.x;
+            o->res.cbp = (uint8_t)cbp;
+            R.ccbp = ccbp;
+        }
+        rd_state(R, S, 3, false);
+        rd_take(Dw.C, R, S, 3, mbx, mby);
+        if (P.t8) {
+            o = &cand[5];
+            code_init(o);
+            uint32_t cbp8 = code_i8_d(D, S, R, mbx, mby, ta, la, tra, o, reinterpret_cast<T*>(Dw.C.rec[0]), Dw.C.ys);
+            rd_chroma_copy(cand[3], o);
+            cbp8 |= ccbp;
+            if (lane == 0) o->res.cbp = (uint8_t)cbp8;
+            rd_state(R, S, 5, false);
+            rd_take(Dw.C, R, S, 5, mbx, mby);  // the chroma in warp 2's planes is Intra16x16's
+        }
+    }
+    __syncthreads();
+    if (w == 0) {
+        // Intra4x4's chroma: Intra16x16's code, reconstruction and squared error
+        rd_chroma_copy(cand[3], &cand[4]);
+        if (lane == 0) {
+            cand[4].res.cbp |= (uint8_t)R.ccbp;
+            R.ssd[4] += R.cssd[3];
+            R.cssd[4] = R.cssd[3];
+        }
+        for (int i = 256 + lane; i < 384; i += 32) R.crec[4][i] = R.crec[3][i];
+        // the candidates priced at once, five lanes each (as rd_mb), the least cost kept in order
+        for (int k = 0; k < RD_CANDS; k++) {
+            if (!R.valid[k]) continue;
+            const uint32_t* s32 = reinterpret_cast<const uint32_t*>(R.live);
+            uint32_t* d32 = reinterpret_cast<uint32_t*>(R.cst[k]);
+            for (int i = lane; i < 256; i += 32) d32[i] = s32[i];
+        }
+        if (lane < RD_CANDS) R.bits[lane] = 0;
+        __syncwarp();
+        {
+            const int k = lane / cab::NGROUPS, g = lane % cab::NGROUPS;
+            if (k < RD_CANDS && R.valid[k]) {
+                cab::Counter c = {R.cst[k], R.step, 0};
+                cab::mb_bins(c, sl, &cand[k], R.nb[0], R.nb[1], S.nbm, g);
+                if (c.bits) atomicAdd(&R.bits[k], c.bits);
+            }
+        }
+        __syncwarp();
+        if (lane == 0) {
+            int best = -1;
+            double bj = 0.0;
+            for (int k = 0; k < RD_CANDS; k++) {
+                if (!R.valid[k]) continue;
+                const double j = __dadd_rn(__ll2double_rn(R.ssd[k]), __dmul_rn(P.lam2, __dmul_rn((double)R.bits[k], 0.00390625)));
+                if (best < 0 || j < bj) best = k, bj = j;
+            }
+            R.best = best;
+        }
+        __syncwarp();
+        const int b = R.best;
+        const uint32_t* s32 = reinterpret_cast<const uint32_t*>(&cand[b]);
+        uint32_t* d32 = reinterpret_cast<uint32_t*>(out);
+        for (int i = lane; i < (int)(sizeof(ironav_mbcode) / 4); i += 32) d32[i] = s32[i];
+        const uint32_t* c32 = reinterpret_cast<const uint32_t*>(R.cst[b]);
+        uint32_t* l32 = reinterpret_cast<uint32_t*>(R.live);
+        for (int i = lane; i < 256; i += 32) l32[i] = c32[i];
+        const T* rec = R.crec[b];
+        for (int i = lane; i < 384; i += 32) {
+            if (i < 256) {
+                reinterpret_cast<T*>(C.rec[0])[(size_t)(mby * 16 + (i >> 4)) * C.ys + mbx * 16 + (i & 15)] = rec[i];
+            } else {
+                const int cc = (i - 256) >> 6, j = (i - 256) & 63;
+                reinterpret_cast<T*>(C.rec[1 + cc])[(size_t)(mby * 8 + (j >> 3)) * C.cs + mbx * 8 + (j & 7)] = rec[i];
+            }
+        }
+        if (lane < 18) reinterpret_cast<uint32_t*>(&A.states_out[mb])[lane] = reinterpret_cast<const uint32_t*>(&R.state[b])[lane];
+        __syncwarp();
+        cab::nb_of_warp(&cand[b], &R.done);
+        if (lane < cab::NB_WORDS) P.nbs[(size_t)mb * cab::NB_WORDS + lane] = reinterpret_cast<const uint32_t*>(&R.done)[lane];
+        __syncwarp();
+    }
+    __syncthreads();
+}
+
+// Decide mode under CABAC for one stream, three warps a chain: CTA i walks slice band i.
+template <class T>
+__global__ void __launch_bounds__(RD3_WARPS * 32) decide_rd3_kernel(const __grid_constant__ RdParams P) {
+    extern __shared__ __align__(16) unsigned char rd3_smem[];
+    RdSmem<T, RD3_WARPS>& R = *reinterpret_cast<RdSmem<T, RD3_WARPS>*>(rd3_smem);
+    __shared__ DecideParams dw[2];
+    __shared__ unsigned i4tab[9 * 17];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (w > 0) {
+        // this warp's copy of the parameters, its coder writing into its scratch planes
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(&P.D);
+        uint32_t* dst = reinterpret_cast<uint32_t*>(&dw[w - 1]);
+        for (int k = lane; k < (int)(sizeof(DecideParams) / 4); k += 32) dst[k] = src[k];
+        __syncwarp();
+        if (lane == 0) {
+            dw[w - 1].C.rec[0] = P.scr[w - 1];
+            dw[w - 1].C.rec[1] = P.scr[2];
+            dw[w - 1].C.rec[2] = P.scr[3];
+            dw[w - 1].C.ys = P.scr_ys;
+            dw[w - 1].C.cs = P.scr_cs;
+        }
+    }
+    fill_i4tab(i4tab);  // its __syncthreads also publishes dw
+    const int band = blockIdx.x;
+    if (band >= P.nbands) return;
+    const AnalyseParams& A = P.D.C.A;
+    for (int i = threadIdx.x; i < cab::STEP_ENTRIES; i += blockDim.x) R.step[i] = P.step[i];
+    for (int i = threadIdx.x; i < 9 * 64; i += blockDim.x) R.i8tab[i] = i8_entry(i >> 6, i & 7, (i >> 3) & 7);
+    cab::init_states(R.live, P.D.intra != 0, 0, P.D.C.qp, threadIdx.x, blockDim.x);
+    __syncthreads();
+    for (int mby = P.band_rows[band]; mby < P.band_rows[band + 1]; mby++)
+        for (int mbx = 0; mbx < A.mb_w; mbx++) rd_mb3<T>(P, dw, R, i4tab, mby * A.mb_w + mbx, mbx, mby);
+}
+
+template <class T>
+constexpr size_t rd3_smem_bytes() { return sizeof(RdSmem<T, RD3_WARPS>); }
 
 // ---- the CABAC slice writer ---------------------------------------------------------------------------
 

@@ -59,6 +59,12 @@ int cabac_setup(ironav_ctx* c) {
     CK(cudaMalloc(&c->d_band_rows, sizeof(int) * (c->nslices + 1)));
     CK(cudaMemcpy(c->d_band_rows, c->band_rows, sizeof(int) * (c->nslices + 1), cudaMemcpyHostToDevice));
     CK(cudaMalloc(&c->d_rd_nb, sizeof(cab::Nb) * c->nmb));
+    // the three-warp form's scratch planes: warp 1's luma, warp 2's luma, Cb and Cr
+    const size_t B = c->bd > 8 ? 2 : 1, ly = (size_t)c->pw * c->ph * B, cy = (size_t)(c->pw / 2) * (c->ph / 2) * B;
+    CK(cudaMalloc(&c->d_rd_scr, 2 * ly + 2 * cy));
+    const size_t s8 = rd3_smem_bytes<uint8_t>(), s16 = rd3_smem_bytes<uint16_t>();
+    CK(cudaFuncSetAttribute(decide_rd3_kernel<uint8_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s8));
+    CK(cudaFuncSetAttribute(decide_rd3_kernel<uint16_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s16));
     return IRONAV_OK;
 }
 
@@ -78,9 +84,17 @@ int launch_decide_rd(ironav_ctx* c, ironav_mbstate* d_states, ironav_mbcode* d_c
     p.lam2 = 1.6 * std::pow(2.0, ((double)c->qpp - 12.0) / 3.0);
     p.nbands = c->nslices;
     p.t8 = c->t8;
+    const size_t B = c->bd > 8 ? 2 : 1, ly = (size_t)c->pw * c->ph * B, cy = (size_t)(c->pw / 2) * (c->ph / 2) * B;
+    p.scr[0] = c->d_rd_scr;
+    p.scr[1] = c->d_rd_scr + ly;
+    p.scr[2] = c->d_rd_scr + 2 * ly;
+    p.scr[3] = c->d_rd_scr + 2 * ly + cy;
+    p.scr_ys = c->pw;
+    p.scr_cs = c->pw / 2;
     CK(cudaMemsetAsync(c->d_counters, 0, 2 * sizeof(unsigned), c->stream));
-    if (c->bd > 8) decide_rd_kernel<uint16_t><<<c->nslices, 32, 0, c->stream>>>(p);
-    else decide_rd_kernel<uint8_t><<<c->nslices, 32, 0, c->stream>>>(p);
+    // one stream: three warps a chain (its bands are few, so each chain's latency is the picture's)
+    if (c->bd > 8) decide_rd3_kernel<uint16_t><<<c->nslices, RD3_WARPS * 32, rd3_smem_bytes<uint16_t>(), c->stream>>>(p);
+    else decide_rd3_kernel<uint8_t><<<c->nslices, RD3_WARPS * 32, rd3_smem_bytes<uint8_t>(), c->stream>>>(p);
     return cuda_status(cudaGetLastError());
 }
 

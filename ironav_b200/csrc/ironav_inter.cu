@@ -136,6 +136,7 @@ void free_ctx(ironav_ctx* c) {
     cudaFree(c->d_cab_step);
     cudaFree(c->d_band_rows);
     cudaFree(c->d_rd_nb);
+    cudaFree(c->d_rd_scr);
     cudaFree(c->d_cab_out);
     cudaFree(c->d_cab_bytes);
     cudaFreeHost(c->h_cab_bytes);
