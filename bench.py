@@ -66,8 +66,8 @@ def parse():
     p.add_argument("--learned-samples", type=int, default=2_000_000, help="training samples of the learned workload's proposer")
     p.add_argument("--e2e-threads", type=int, default=8, help="host threads (each with a context) of the e2e pass")
     p.add_argument("--cabac", action="store_true",
-                   help="decide workload: CABAC with rate-distortion decisions and the 8x8 transform (the reference "
-                        "encoder's default entropy coding) instead of CAVLC")
+                   help="decide, decide_batched and encode workloads: CABAC with rate-distortion decisions and the 8x8 "
+                        "transform (the reference encoder's default entropy coding) instead of CAVLC")
     p.add_argument("--bd", type=int, default=8, choices=[8, 10],
                    help="sample depth of the 1080p workload: 8 (Yuv420p) or 10 (Yuv420p10, QP' = QP + 12)")
     return p.parse_args()
@@ -613,7 +613,8 @@ def run_encode(args, rank, world):
     the filtered picture pushed as the next reference. 1080p, QP 27, one reference, eight bands; the IDR
     picture is coded first, untimed; one step is one P picture. `value` has the sources in device memory;
     `e2e` uploads each picture's planes from host memory (DeviceEncoder.encode). Against the oracle's encoder
-    loop (the same steps on the host, the decision on one thread per band)."""
+    loop (the same steps on the host, the decision on one thread per band). With --cabac, the default
+    encoder's stream instead (High: CABAC decisions by rate-distortion cost, the CABAC writer)."""
     import torch
     import torch.distributed as dist
     from ironav_b200.encoder import DeviceEncoder, Encoder
@@ -629,7 +630,8 @@ def run_encode(args, rank, world):
     cs = [seq.chroma(t) for t in range(n)]
     d_y = torch.from_numpy(np.stack(ys)).to(dev)
     d_c = torch.from_numpy(np.stack([np.stack(c) for c in cs])).to(dev)
-    enc = DeviceEncoder(w, h, qp=QP, keyint=10 ** 6, refs=1, nslices=NSLICES)
+    enc = DeviceEncoder(w, h, qp=QP, keyint=10 ** 6, refs=1, nslices=NSLICES, cabac=args.cabac)
+    how = "CABAC (High)" if args.cabac else "CAVLC"
     nbytes = [0]
 
     def picture(t):
@@ -666,21 +668,25 @@ def run_encode(args, rank, world):
     nmb = ((w + 15) // 16) * ((h + 15) // 16)
     total = sum_over_ranks(nmb, world, dev)
     line = {
-        "metric": "1080p CAVLC encoding MB/s on the device (decide, slices written, deblocking, next reference)",
+        "metric": f"1080p {how} encoding MB/s on the device (decide, slices written, deblocking, next reference)",
         "value": total * args.steps / el, "unit": "MB/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
         "data": data_desc(8) + "; chroma from the 2x2 luma means",
         "config": {"workload": f"1080p 8-bit P pictures through DeviceEncoder.encode_device, QP {QP}, one reference, {NSLICES} slice "
-                               "bands: scene cut, decide mode, CAVLC slices (device writer, NAL framing on the host), records, "
+                               f"bands: scene cut, decide mode, {how} slices (device writer, NAL framing on the host), records, "
                                "deblocking, reference planes", "width": w, "height": h, "qp": QP, "slices": NSLICES,
                    "bits_per_picture": bits_per_picture, "l2": "each picture read once from a ring in device memory",
                    "parallelism": "replicas"},
         "e2e": {"value": total * args.steps / el_host, "unit": "MB/s", "h2d_bytes_per_step": w * h * 3 // 2,
                 "d2h_bytes_per_step": int(bits_per_picture / 8), "ms_per_step": 1e3 * el_host / args.steps,
                 "note": "DeviceEncoder.encode: the picture's three planes from host memory, the stream's bytes back"},
-        "gpu_launches": 16 * args.steps,  # per picture: scene cut 2, source copy 1, chroma 2, decide 1, writer 3, records 1, deblocking 2, planes 1, chroma copies 2 (and their padding)
-        "roofline": {"bound": "latency", "kernel": "decide_kernel<uint8_t>", "achieved": None, "peak": None, "unit": None, "frac": None,
-                     "traffic": None, "note": "one stream's decide wavefront (a chain of ~136 dependent macroblocks) bounds the picture"},
+        # per picture: scene cut 2, source copy 1, chroma 2, decide 1, writer 3 (CABAC: 1), records 1, deblocking 2, planes 1, chroma
+        # copies 2 (and their padding)
+        "gpu_launches": (14 if args.cabac else 16) * args.steps,
+        "roofline": {"bound": "latency", "kernel": "decide_rd3_kernel<uint8_t>" if args.cabac else "decide_kernel<uint8_t>", "achieved": None,
+                     "peak": None, "unit": None, "frac": None, "traffic": None,
+                     "note": ("one stream's slice bands under CABAC: 8 chains of ~1020 dependent macroblocks bound the picture"
+                              if args.cabac else "one stream's decide wavefront (a chain of ~136 dependent macroblocks) bounds the picture")},
         "clocks": clk,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -688,7 +694,7 @@ def run_encode(args, rank, world):
 
         lib = oracle_library()
         threads = min(host_cores(), NSLICES)
-        o = Encoder(w, h, qp=QP, keyint=10 ** 6, refs=1, nslices=NSLICES, lib=lib)
+        o = Encoder(w, h, qp=QP, keyint=10 ** 6, refs=1, nslices=NSLICES, lib=lib, cabac=args.cabac)
         lib.oracle_set_threads(o.st.ctx, threads)
         o.encode(ys[0], *cs[0])
         k, t0, el_o = 1, time.perf_counter(), 0.0
