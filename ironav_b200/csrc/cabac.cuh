@@ -394,7 +394,7 @@ enum Group { ALL = -1, HEAD = 0, DC16 = 1, LUMA = 2, CDC = 3, CAC = 4, NGROUPS =
 // mb_bins' HEAD group after mb_skip_flag (enc/frame.rs:2046-2244): mb_type, the prediction modes,
 // sub_mb_type, ref_idx, mvd, coded_block_pattern, transform_size_8x8_flag and mb_qp_delta.
 template <class S>
-__device__ void head_bins(S& c, const Slice& sl, const ironav_mbcode* code, const Nb& L, const Nb& T, const int* nbm) {
+__device__ __forceinline__ void head_bins(S& c, const Slice& sl, const ironav_mbcode* code, const Nb& L, const Nb& T, const int* nbm) {
     const bool la = L.avail, ta = T.avail;
     const int kind = code->kind, cbp = code->res.cbp, cbpl = cbp & 15, cbpc = cbp >> 4;
     // mb_type
@@ -517,7 +517,7 @@ __device__ void head_bins(S& c, const Slice& sl, const ironav_mbcode* code, cons
 // end_of_slice_flag (all of them, or one group's); l and t its left and top neighbours (avail 0: not in
 // the slice), nbm their Intra NxN modes as pred_mode reads them.
 template <class S>
-__device__ void mb_bins(S& c, const Slice& sl, const ironav_mbcode* code, const Nb& L, const Nb& T, const int* nbm, int group = ALL) {
+__device__ __forceinline__ void mb_bins(S& c, const Slice& sl, const ironav_mbcode* code, const Nb& L, const Nb& T, const int* nbm, int group = ALL) {
     const bool la = L.avail, ta = T.avail;
     if (sl.p_slice) {
         if (group == ALL || group == HEAD) c.decision(11 + (la && !L.skip) + (ta && !T.skip), code->skip);

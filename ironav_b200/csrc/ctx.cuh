@@ -107,6 +107,7 @@ struct ironav_ctx {
     uint32_t* d_cab_out = nullptr;
     unsigned long long cab_region_words = 0;
     uint32_t* d_cab_bytes = nullptr;
+    uint8_t* d_cab_wnb = nullptr;  // the writer's per-macroblock neighbour records
     uint32_t* h_cab_bytes = nullptr;
 };
 

@@ -972,72 +972,101 @@ constexpr size_t rd3_smem_bytes() { return sizeof(RdSmem<T, RD3_WARPS>); }
 
 // ---- the CABAC slice writer ---------------------------------------------------------------------------
 
+// What the writer reads of a macroblock as a neighbour: its Nb, and the Intra NxN modes of its right column
+// and bottom row (2 for a macroblock that is neither Intra4x4 nor Intra8x8), as pred_mode reads them.
+struct WrNb {
+    cab::Nb nb;
+    int8_t rmodes[4], bmodes[4];
+};
+constexpr int WRNB_WORDS = (int)(sizeof(WrNb) / 4);
+static_assert(sizeof(WrNb) % 4 == 0, "WrNb in whole words");
+
 struct CabacWriteParams {
     const ironav_mbcode* codes;
+    WrNb* nbs;              // per macroblock, filled by cabac_nb_kernel
     const int* band_rows;
     const uint32_t* step;
     uint32_t* out;          // slice i's data at out + i * region_words
     uint32_t region_words;
     uint32_t* slice_bytes;  // per slice: its data's bytes; [nbands]: set when a slice outgrew its region
-    int mb_w, nbands, intra, t8, nref, qp;
+    int mb_w, nmb, nbands, intra, t8, nref, qp;
 };
+
+// Every macroblock's WrNb, a warp a macroblock (grid-stride): the neighbours' side of the writer's walk,
+// worked out for the whole picture at once.
+static __global__ void __launch_bounds__(128) cabac_nb_kernel(const __grid_constant__ CabacWriteParams P) {
+    const int lane = threadIdx.x & 31;
+    const int warps = (int)(gridDim.x * blockDim.x) >> 5;
+    for (int mb = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); mb < P.nmb; mb += warps) {
+        const ironav_mbcode* k = &P.codes[mb];
+        cab::nb_of_warp(k, &P.nbs[mb].nb);
+        if (lane < 8) {
+            const bool n = cab::nxn(k->kind);
+            if (lane < 4) P.nbs[mb].rmodes[lane] = (int8_t)(n ? k->modes[lane * 4 + 3] : 2);
+            else P.nbs[mb].bmodes[lane - 4] = (int8_t)(n ? k->modes[12 + lane - 4] : 2);
+        }
+        __syncwarp();
+    }
+}
 
 // A slice band's data (FrameCoder::encode with write_mb_cabac, enc/frame.rs:461-486): each macroblock's bins
 // (mb_bins) then end_of_slice_flag, arithmetic coded from the slice's contexts; the data starts on the byte
-// that follows the header's cabac_alignment_one_bit (written on the host). CTA i walks slice band i: the warp
-// stages each macroblock's code and its top neighbour's into shared memory and works out their Nb, and
-// lane 0 codes the bins.
+// that follows the header's cabac_alignment_one_bit (written on the host). CTA i walks slice band i: lane 0
+// codes a macroblock's bins while lanes 1-31 bring the next one's code and its neighbours' WrNb into the
+// other half of a double buffer in shared memory.
 static __global__ void __launch_bounds__(32) cabac_write_kernel(const __grid_constant__ CabacWriteParams P) {
     __shared__ uint8_t st[1024];
     __shared__ uint32_t step[cab::STEP_ENTRIES];
-    __shared__ ironav_mbcode code[2];  // the macroblock, then its top neighbour
-    __shared__ cab::Nb nb[3];          // left, top, and the macroblock itself (the next one's left)
-    __shared__ int nbm[8];
-    __shared__ int left_modes[4];      // the macroblock's right column of Intra NxN modes (2 otherwise)
+    __shared__ ironav_mbcode code[2];
+    __shared__ WrNb nb[2][2];  // [buffer][left, top]
     __shared__ int over;
     const int chain = blockIdx.x, lane = threadIdx.x & 31;
     if (chain >= P.nbands) return;
     for (int i = lane; i < cab::STEP_ENTRIES; i += 32) step[i] = P.step[i];
     cab::init_states(st, P.intra != 0, 0, P.qp, lane, 32);
     if (lane == 0) over = 0;
-    __syncwarp();
     cab::BitOut bo = {P.out + (size_t)chain * P.region_words, P.region_words, 0, 0ull, 0, false};
     cab::Coder k = {st, step, &bo, 0u, 510u, 0u, true};
     const cab::Slice sl = {P.intra ? 0 : 1, P.t8, P.intra ? 0 : P.nref};
     const int r0 = P.band_rows[chain], r1 = P.band_rows[chain + 1];
+    const int first = r0 * P.mb_w, end = r1 * P.mb_w;
     constexpr int W = (int)(sizeof(ironav_mbcode) / 4);
-    for (int mby = r0; mby < r1; mby++)
-        for (int mbx = 0; mbx < P.mb_w; mbx++) {
-            const int mb = mby * P.mb_w + mbx;
-            const bool la = mbx > 0, ta = mby > r0;
-            uint32_t* c0 = reinterpret_cast<uint32_t*>(&code[0]);
-            uint32_t* c1 = reinterpret_cast<uint32_t*>(&code[1]);
-            const uint32_t* g0 = reinterpret_cast<const uint32_t*>(&P.codes[mb]);
-            for (int i = lane; i < W; i += 32) c0[i] = g0[i];
-            if (ta) {
-                const uint32_t* g1 = reinterpret_cast<const uint32_t*>(&P.codes[mb - P.mb_w]);
-                for (int i = lane; i < W; i += 32) c1[i] = g1[i];
-            }
-            if (lane < cab::NB_WORDS) {
-                reinterpret_cast<uint32_t*>(&nb[0])[lane] = la ? reinterpret_cast<const uint32_t*>(&nb[2])[lane] : 0u;
-                if (!ta) reinterpret_cast<uint32_t*>(&nb[1])[lane] = 0u;
-            }
-            if (lane < 4) nbm[lane] = la ? left_modes[lane] : -1;
-            __syncwarp();
-            if (ta) cab::nb_of_warp(&code[1], &nb[1]);
-            if (lane >= 4 && lane < 8) nbm[lane] = ta ? (cab::nxn(code[1].kind) ? (int)code[1].modes[12 + lane - 4] : 2) : -1;
-            __syncwarp();
-            if (lane == 0) {
-                cab::mb_bins(k, sl, &code[0], nb[0], nb[1], nbm);
-                k.terminate(mby + 1 == r1 && mbx + 1 == P.mb_w);
-                over = bo.over;
-            }
-            __syncwarp();
-            cab::nb_of_warp(&code[0], &nb[2]);
-            if (lane < 4) left_modes[lane] = cab::nxn(code[0].kind) ? (int)code[0].modes[lane * 4 + 3] : 2;
-            __syncwarp();
-            if (over) mbx = P.mb_w, mby = r1;  // the region is full: stop (reported below)
+    // macroblock `mb`'s code and its neighbours' WrNb into buffer b, by lanes lo..31 (zeros: not in the slice)
+    auto fetch = [&](int mb, int b, int lo) {
+        const int mbx = mb % P.mb_w;
+        const bool la = mbx > 0, ta = mb - P.mb_w >= first;
+        const uint32_t* g = reinterpret_cast<const uint32_t*>(&P.codes[mb]);
+        uint32_t* c = reinterpret_cast<uint32_t*>(&code[b]);
+        for (int i = lane - lo; i < W; i += 32 - lo) c[i] = g[i];
+        uint32_t* l = reinterpret_cast<uint32_t*>(&nb[b][0]);
+        uint32_t* t = reinterpret_cast<uint32_t*>(&nb[b][1]);
+        const uint32_t* gl = reinterpret_cast<const uint32_t*>(&P.nbs[la ? mb - 1 : mb]);
+        const uint32_t* gt = reinterpret_cast<const uint32_t*>(&P.nbs[ta ? mb - P.mb_w : mb]);
+        for (int i = lane - lo; i < 2 * WRNB_WORDS; i += 32 - lo) {
+            if (i < WRNB_WORDS) l[i] = la ? gl[i] : 0u;
+            else t[i - WRNB_WORDS] = ta ? gt[i - WRNB_WORDS] : 0u;
         }
+    };
+    fetch(first, 0, 0);
+    __syncwarp();
+    for (int mb = first; mb < end; mb++) {
+        const int b = (mb - first) & 1;
+        if (lane == 0) {
+            int nbm[8];
+            const bool la = nb[b][0].nb.avail, ta = nb[b][1].nb.avail;
+            for (int q = 0; q < 4; q++) {
+                nbm[q] = la ? nb[b][0].rmodes[q] : -1;
+                nbm[4 + q] = ta ? nb[b][1].bmodes[q] : -1;
+            }
+            cab::mb_bins(k, sl, &code[b], nb[b][0].nb, nb[b][1].nb, nbm);
+            k.terminate(mb + 1 == end);
+            over = bo.over;
+        } else if (mb + 1 < end) {
+            fetch(mb + 1, b ^ 1, 1);
+        }
+        __syncwarp();
+        if (over) break;
+    }
     if (lane == 0) {
         const uint32_t bytes = bo.finish();
         P.slice_bytes[chain] = bytes;

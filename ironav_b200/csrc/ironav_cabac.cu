@@ -108,11 +108,14 @@ int cabac_slice_data(ironav_ctx* c, int idr, const ironav_mbcode* d_codes, std::
         c->cab_region_words = ((unsigned long long)most * CAB_MB_BYTES) / 4 + 2;
         CK(cudaMalloc(&c->d_cab_out, sizeof(uint32_t) * c->cab_region_words * ns));
         CK(cudaMalloc(&c->d_cab_bytes, sizeof(uint32_t) * (ns + 1)));
+        CK(cudaMalloc(&c->d_cab_wnb, sizeof(WrNb) * c->nmb));
         CK(cudaMallocHost(&c->h_cab_bytes, sizeof(uint32_t) * (ns + 1)));
     }
     CabacWriteParams p;
     memset(&p, 0, sizeof(p));
     p.codes = d_codes;
+    p.nbs = reinterpret_cast<WrNb*>(c->d_cab_wnb);
+    p.nmb = c->nmb;
     p.band_rows = c->d_band_rows;
     p.step = c->d_cab_step;
     p.out = c->d_cab_out;
@@ -125,6 +128,7 @@ int cabac_slice_data(ironav_ctx* c, int idr, const ironav_mbcode* d_codes, std::
     p.nref = idr ? 0 : c->nact;
     p.qp = c->qpp - 6 * (c->bd - 8);
     CK(cudaMemsetAsync(c->d_cab_bytes, 0, sizeof(uint32_t) * (ns + 1), c->stream));
+    cabac_nb_kernel<<<std::min((c->nmb + 3) / 4, c->nsm * 16), 128, 0, c->stream>>>(p);
     cabac_write_kernel<<<ns, 32, 0, c->stream>>>(p);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(c->h_cab_bytes, c->d_cab_bytes, sizeof(uint32_t) * (ns + 1), cudaMemcpyDeviceToHost, c->stream));

@@ -139,6 +139,7 @@ void free_ctx(ironav_ctx* c) {
     cudaFree(c->d_rd_scr);
     cudaFree(c->d_cab_out);
     cudaFree(c->d_cab_bytes);
+    cudaFree(c->d_cab_wnb);
     cudaFreeHost(c->h_cab_bytes);
     cudaFreeHost(c->h_cavlc);
     cudaFreeHost(c->h_rbsp);
