@@ -556,12 +556,17 @@ class InterStage:
         codes = np.ascontiguousarray(codes, dtype=MBCODE_DTYPE)
         assert codes.shape == (self.nmb,)
         return _sized_call(lambda buf, cap, n: self.lib.ironav_write_slices(self.ctx, int(idr), frame_num, idr_pic_id, _ptr(codes),
-                                                                             buf, cap, n), "ironav_write_slices", 1 << 16)
+                                                                             buf, cap, n), "ironav_write_slices", self._stream_guess(idr))
 
     def write_slices_device(self, idr: bool, frame_num: int, idr_pic_id: int, d_codes: int) -> bytes:
         return _sized_call(lambda buf, cap, n: self.lib.ironav_write_slices_device(self.ctx, int(idr), frame_num, idr_pic_id, d_codes,
                                                                                     buf, cap, n), "ironav_write_slices_device",
-                           1 << 16)
+                           self._stream_guess(idr))
+
+    def _stream_guess(self, idr: bool) -> int:
+        # a buffer most pictures fit, so that the writer rarely runs twice (a call that is short of room
+        # reports the size it needs and is made again): 128 bytes a macroblock for an IDR picture, 16 for P
+        return max(1 << 16, self.nmb * (128 if idr else 16))
 
     def decide_dbk_records(self, codes: np.ndarray, states: np.ndarray) -> np.ndarray:
         """The deblocking filter's macroblock records (DBK_MB_DTYPE) of a picture decide_p_picture coded."""
