@@ -33,9 +33,9 @@ struct RdParams {
     double lam2;            // 1.6 * 2^((QP'Y - 12) / 3), computed on the host in f64 as the reference does
     int nbands;
     int t8;                 // transform_8x8_mode_flag
-    // the three-warp form: the intra warps' scratch planes (warp 1's luma; warp 2's luma, Cb, Cr), pw x ph and
+    // the three-warp form: warps 1 and 2's scratch planes (luma, Cb, Cr of warp 1, then of warp 2), pw x ph and
     // cw x ch samples, rows scr_ys and scr_cs samples apart
-    uint8_t* scr[4];
+    uint8_t* scr[6];
     int scr_ys, scr_cs;
 };
 
@@ -55,8 +55,11 @@ struct RdSmem {
     unsigned bits[RD_CANDS];
     int valid[RD_CANDS];
     int best;
-    int skip;                        // the three-warp form: the P_Skip tests' verdict, and the intra chroma's
-    uint32_t ccbp;                   // coded block pattern bits
+    int skip;                        // the three-warp form: the P_Skip tests' verdict and the skip vector; the
+    int2 sv;                         // intra chroma's coded block pattern bits; best_inter's decision for the
+    uint32_t ccbp;                   // 8x8-transform candidate (warp 2), and whether that candidate is tried
+    uint16_t idec[40];
+    int try_t8;
     // the Intra8x8 trial
     int i8rec[256];       // its reconstruction
     int raw[25], e8[26];  // a block's edges, raw and filtered: [0] top-left, [1 + i] the 16 above, [17 + j] the 8 left,
@@ -684,12 +687,14 @@ __global__ void __launch_bounds__(32) decide_rd_batch_kernel(const RdParams* __r
 }
 
 // ---- the three-warp form: one chain's macroblock on three warps ----------------------------------------
-// Warp 0 runs code_mb's P_Skip tests, best_inter and the inter candidates into the picture (as the one-warp
-// form); when the macroblock passes the P_Skip tests, warp 1 codes Intra4x4 and warp 2 Intra16x16 (with the
-// intra chroma) and then Intra8x8 beside it, each into its own scratch planes (their edges read from the
-// picture, which warp 0 writes only inside the macroblock). Warp 0 then prices every candidate and commits
-// the kept one. The warps meet at three CTA barriers a macroblock (after the P_Skip tests; after the
-// candidates, when there are any; after the commit), every warp at every one.
+// Warp 0 runs code_mb's P_Skip tests; when the macroblock passes them, warp 0 runs best_inter and codes its
+// partitioning with the 4x4 transform into the picture, warp 1 codes P_Skip and then Intra4x4, and warp 2
+// Intra16x16 (with the intra chroma), Intra8x8 and then the partitioning with the 8x8 transform (best_inter's
+// decision handed over through named barrier 1, which warp 0 arrives at and warp 2 waits on), warps 1 and
+// 2 each into their own scratch planes (their edges read from the picture, which warp 0 writes only inside
+// the macroblock). Warp 0 then prices every candidate and commits the kept one. The warps meet at three CTA
+// barriers a macroblock (after the P_Skip tests; after the candidates, when there are any; after the
+// commit), every warp at every one.
 constexpr int RD3_WARPS = 3;
 
 template <class T>
@@ -722,7 +727,10 @@ __device__ void rd_mb3(const RdParams& P, const DecideParams* dw, RdSmem<T, RD3_
         if (lane < RD_CANDS) R.valid[lane] = 0;
         __syncwarp();
         const bool skip = !D.intra && skip_tests_d<T>(D, S, mb, mbx, mby, out, &sv);
-        if (lane == 0) R.skip = skip;
+        if (lane == 0) {
+            R.skip = skip;
+            R.sv = sv;
+        }
     }
     __syncthreads();
     if (R.skip) {
@@ -743,7 +751,8 @@ __device__ void rd_mb3(const RdParams& P, const DecideParams* dw, RdSmem<T, RD3_
     }
     load_intra_neighbours(D, S, mb, mbx, mby, ta, la, tra);
     if (w == 0 && !D.intra) {
-        // best_inter, enc/frame.rs:839-849, and the inter candidates (as rd_mb)
+        // best_inter, enc/frame.rs:839-849; its decision goes to warp 2 (the 8x8-transform candidate) through
+        // named barrier 1, and warp 0 codes it with the 4x4 transform
         int part = 0, cost = BIG, bestr = 0;
         uint32_t sub = 0;
         for (int r = 0; r < A.nact; r++) {
@@ -761,27 +770,6 @@ __device__ void rd_mb3(const RdParams& P, const DecideParams* dw, RdSmem<T, RD3_
             }
         }
         ironav_interdec& Dd = *reinterpret_cast<ironav_interdec*>(S.c.dec);
-        ironav_mbcode* o = &cand[0];
-        code_init(o);
-        if (lane == 0) {
-            Dd.mode = 1;
-            Dd.part = 0;
-            Dd.t8 = 0;
-            for (int k = 0; k < 4; k++) Dd.sub[k] = Dd.refs[k] = 0;
-        }
-        if (lane < 16) {
-            Dd.mvs[lane][0] = (int16_t)sv.x;
-            Dd.mvs[lane][1] = (int16_t)sv.y;
-        }
-        __syncwarp();
-        code_inter_mb<T>(C, S.c, mb, &o->res);
-        inter_tail(D, S, Dd, o);
-        if (lane < 16) o->mvds[lane][0] = o->mvds[lane][1] = 0;
-        if (lane == 0) o->skip = 1;
-        rd_state(R, S, 0, true);
-        rd_take(C, R, S, 0, mbx, mby);
-        o = &cand[1];
-        code_init(o);
         if (lane == 0) {
             Dd.mode = 2;
             Dd.part = (uint8_t)part;
@@ -790,33 +778,59 @@ __device__ void rd_mb3(const RdParams& P, const DecideParams* dw, RdSmem<T, RD3_
                 Dd.sub[k] = (uint8_t)((sub >> (8 * k)) & 0xff);
                 Dd.refs[k] = (uint8_t)bestr;
             }
+            R.try_t8 = P.t8 && sub == 0;
         }
         if (lane < 16) {
             Dd.mvs[lane][0] = S.a.win_mvs[lane][0];
             Dd.mvs[lane][1] = S.a.win_mvs[lane][1];
         }
         __syncwarp();
+        if (P.t8) {
+            for (int i = lane; i < 40; i += 32) R.idec[i] = S.c.dec[i];
+            __threadfence_block();
+            __syncwarp();
+            asm volatile("bar.arrive 1, 64;" ::: "memory");
+        }
+        ironav_mbcode* o = &cand[1];
+        code_init(o);
         const uint32_t cbp = code_inter_mb<T>(C, S.c, mb, &o->res);
         inter_tail(D, S, Dd, o);
         rd_state(R, S, 1, true);
         rd_take(C, R, S, 1, mbx, mby);
+        const int2 sv = R.sv;
         if (lane == 0 && cbp == 0 && part == 0 && Dd.mvs[0][0] == sv.x && Dd.mvs[0][1] == sv.y && bestr == 0) R.valid[1] = 0;
         __syncwarp();
-        if (P.t8 && sub == 0) {
-            o = &cand[2];
-            code_init(o);
-            if (lane == 0) Dd.t8 = 1;
-            __syncwarp();
-            code_inter_mb<T>(C, S.c, mb, &o->res);
-            inter_tail(D, S, Dd, o);
-            rd_state(R, S, 2, true);
-            rd_take(C, R, S, 2, mbx, mby);
-            if (lane == 0 && !o->res.t8x8) R.valid[2] = 0;
-            __syncwarp();
-        }
     } else if (w == 1) {
-        // Intra4x4 into warp 1's luma plane; its chroma is Intra16x16's (taken after the barrier)
         const DecideParams& Dw = dw[0];
+        if (!D.intra) {
+            // P_Skip: the skip vector's prediction is the reconstruction (put_inter_pred, 1391-1394), into warp
+            // 1's planes; a P_Skip code carries no differences, its state the vector over the macroblock
+            const int2 sv = R.sv;
+            ironav_mbcode* o = &cand[0];
+            code_init(o);
+            ironav_interdec& Dd = *reinterpret_cast<ironav_interdec*>(S.c.dec);
+            if (lane == 0) {
+                Dd.mode = 1;
+                Dd.part = 0;
+                Dd.t8 = 0;
+                for (int k = 0; k < 4; k++) Dd.sub[k] = Dd.refs[k] = 0;
+                o->kind = KIND_INTER;
+                o->skip = 1;
+            }
+            if (lane < 16) {
+                Dd.mvs[lane][0] = (int16_t)sv.x;
+                Dd.mvs[lane][1] = (int16_t)sv.y;
+                o->mvs[lane][0] = (int16_t)sv.x;
+                o->mvs[lane][1] = (int16_t)sv.y;
+            }
+            __syncwarp();
+            code_inter_mb<T>(Dw.C, S.c, mb, &o->res);
+            uint32_t* d = reinterpret_cast<uint32_t*>(&R.state[0]);
+            if (lane < 18) d[lane] = lane == 0 ? 1u : (lane == 1 ? 0u : ((uint32_t)(uint16_t)sv.x | (uint32_t)(uint16_t)sv.y << 16));
+            __syncwarp();
+            rd_take(Dw.C, R, S, 0, mbx, mby);
+        }
+        // Intra4x4 into warp 1's luma plane; its chroma is Intra16x16's (taken after the barrier)
         ironav_mbcode* o = &cand[4];
         code_init(o);
         code_i4_trial(Dw, S, i4tab, ta, la, tra);
@@ -867,6 +881,27 @@ __device__ void rd_mb3(const RdParams& P, const DecideParams* dw, RdSmem<T, RD3_
             if (lane == 0) o->res.cbp = (uint8_t)cbp8;
             rd_state(R, S, 5, false);
             rd_take(Dw.C, R, S, 5, mbx, mby);  // the chroma in warp 2's planes is Intra16x16's
+        }
+        if (P.t8 && !D.intra) {
+            // best_inter's partitioning with the 8x8 transform (when no 8x8 block is split; without luma levels it
+            // would be the 4x4 candidate again), once warp 0 has handed its decision over
+            asm volatile("bar.sync 1, 64;" ::: "memory");
+            if (R.try_t8) {
+                load_neighbours(A, S.a, A.states_out);
+                for (int i = lane; i < 40; i += 32) S.c.dec[i] = R.idec[i];
+                __syncwarp();
+                ironav_interdec& Dd = *reinterpret_cast<ironav_interdec*>(S.c.dec);
+                if (lane == 0) Dd.t8 = 1;
+                __syncwarp();
+                o = &cand[2];
+                code_init(o);
+                code_inter_mb<T>(Dw.C, S.c, mb, &o->res);
+                inter_tail(D, S, Dd, o);
+                rd_state(R, S, 2, true);
+                rd_take(Dw.C, R, S, 2, mbx, mby);
+                if (lane == 0 && !o->res.t8x8) R.valid[2] = 0;
+                __syncwarp();
+            }
         }
     }
     __syncthreads();
@@ -948,9 +983,7 @@ __global__ void __launch_bounds__(RD3_WARPS * 32) decide_rd3_kernel(const __grid
         for (int k = lane; k < (int)(sizeof(DecideParams) / 4); k += 32) dst[k] = src[k];
         __syncwarp();
         if (lane == 0) {
-            dw[w - 1].C.rec[0] = P.scr[w - 1];
-            dw[w - 1].C.rec[1] = P.scr[2];
-            dw[w - 1].C.rec[2] = P.scr[3];
+            for (int k = 0; k < 3; k++) dw[w - 1].C.rec[k] = P.scr[3 * (w - 1) + k];
             dw[w - 1].C.ys = P.scr_ys;
             dw[w - 1].C.cs = P.scr_cs;
         }

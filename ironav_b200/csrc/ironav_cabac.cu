@@ -59,9 +59,9 @@ int cabac_setup(ironav_ctx* c) {
     CK(cudaMalloc(&c->d_band_rows, sizeof(int) * (c->nslices + 1)));
     CK(cudaMemcpy(c->d_band_rows, c->band_rows, sizeof(int) * (c->nslices + 1), cudaMemcpyHostToDevice));
     CK(cudaMalloc(&c->d_rd_nb, sizeof(cab::Nb) * c->nmb));
-    // the three-warp form's scratch planes: warp 1's luma, warp 2's luma, Cb and Cr
+    // the three-warp form's scratch planes: luma, Cb and Cr of warp 1, then of warp 2
     const size_t B = c->bd > 8 ? 2 : 1, ly = (size_t)c->pw * c->ph * B, cy = (size_t)(c->pw / 2) * (c->ph / 2) * B;
-    CK(cudaMalloc(&c->d_rd_scr, 2 * ly + 2 * cy));
+    CK(cudaMalloc(&c->d_rd_scr, 2 * (ly + 2 * cy)));
     const size_t s8 = rd3_smem_bytes<uint8_t>(), s16 = rd3_smem_bytes<uint16_t>();
     CK(cudaFuncSetAttribute(decide_rd3_kernel<uint8_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s8));
     CK(cudaFuncSetAttribute(decide_rd3_kernel<uint16_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s16));
@@ -85,10 +85,12 @@ int launch_decide_rd(ironav_ctx* c, ironav_mbstate* d_states, ironav_mbcode* d_c
     p.nbands = c->nslices;
     p.t8 = c->t8;
     const size_t B = c->bd > 8 ? 2 : 1, ly = (size_t)c->pw * c->ph * B, cy = (size_t)(c->pw / 2) * (c->ph / 2) * B;
-    p.scr[0] = c->d_rd_scr;
-    p.scr[1] = c->d_rd_scr + ly;
-    p.scr[2] = c->d_rd_scr + 2 * ly;
-    p.scr[3] = c->d_rd_scr + 2 * ly + cy;
+    for (int k = 0; k < 2; k++) {
+        uint8_t* base = c->d_rd_scr + k * (ly + 2 * cy);
+        p.scr[3 * k] = base;
+        p.scr[3 * k + 1] = base + ly;
+        p.scr[3 * k + 2] = base + ly + cy;
+    }
     p.scr_ys = c->pw;
     p.scr_cs = c->pw / 2;
     CK(cudaMemsetAsync(c->d_counters, 0, 2 * sizeof(unsigned), c->stream));
