@@ -295,25 +295,30 @@ __device__ __forceinline__ int pred_mode(const int* nbm, const uint8_t* cur, int
 }
 
 // write_block, enc/cabac.rs:194-250: coded_block_flag (context cbf, none when < 0) and max levels of
-// category cat in scan order.
+// category cat in scan order; part 0 all of it, 1 its significance map (coded_block_flag,
+// significant_coeff_flag, last_significant_coeff_flag), 2 its levels (coeff_abs_level_minus1 and the signs):
+// the two parts' contexts are disjoint.
 template <class S>
-__device__ __forceinline__ void block(S& c, int cat, int cbf, const int16_t* lv, int max) {
+__device__ __forceinline__ void block(S& c, int cat, int cbf, const int16_t* lv, int max, int part = 0) {
     int last = -1;
     for (int i = 0; i < max; i++)
         if (lv[i]) last = i;
-    if (cbf >= 0) c.decision(cbf, last >= 0);
+    if (cbf >= 0 && part != 2) c.decision(cbf, last >= 0);
     if (last < 0) return;
-    const int so = SIG_OFF[0][cat], lo = LAST_OFF[0][cat];
-    for (int i = 0; i < max - 1; i++) {
-        // 4:2:0 chroma DC has three significance contexts, one per position; 8x8 blocks share theirs
-        const int sig = cat == 3 ? min(i, 2) : cat == 5 ? SIG_OFF_8X8[0][i] : i;
-        const int lst = cat == 3 ? min(i, 2) : cat == 5 ? LAST_OFF_8X8[i] : i;
-        c.decision(so + sig, lv[i] != 0);
-        if (lv[i]) {
-            c.decision(lo + lst, i == last);
-            if (i == last) break;
+    if (part != 2) {
+        const int so = SIG_OFF[0][cat], lo = LAST_OFF[0][cat];
+        for (int i = 0; i < max - 1; i++) {
+            // 4:2:0 chroma DC has three significance contexts, one per position; 8x8 blocks share theirs
+            const int sig = cat == 3 ? min(i, 2) : cat == 5 ? SIG_OFF_8X8[0][i] : i;
+            const int lst = cat == 3 ? min(i, 2) : cat == 5 ? LAST_OFF_8X8[i] : i;
+            c.decision(so + sig, lv[i] != 0);
+            if (lv[i]) {
+                c.decision(lo + lst, i == last);
+                if (i == last) break;
+            }
         }
     }
+    if (part == 1) return;
     const int base = ABS_OFF[cat];
     int eq1 = 0, gt1 = 0;
     for (int i = last; i >= 0; i--) {
@@ -389,7 +394,18 @@ struct Slice {
 // (Intra16x16 DC; the luma blocks, 4x4 or 8x8; chroma DC; chroma AC: contexts 85-104 by category, 105 and
 // up by category). So the bits of a macroblock are the sum of the groups' bits, each group walked on its
 // own from the same contexts, and the contexts after it are the union of the groups' updates.
-enum Group { ALL = -1, HEAD = 0, DC16 = 1, LUMA = 2, CDC = 3, CAC = 4, NGROUPS = 5 };
+// Each category's significance map and levels use disjoint contexts too, so a category is two groups.
+enum Group { ALL = -1, HEAD = 0, DC16_MAP, DC16_LEV, LUMA_MAP, LUMA_LEV, CDC_MAP, CDC_LEV, CAC_MAP, CAC_LEV, NGROUPS };
+
+// The groups of a residual category: whether `group` walks it, and which part of its blocks.
+__device__ __forceinline__ bool in_group(int group, int map_group, int* part) {
+    if (group == ALL) {
+        *part = 0;
+        return true;
+    }
+    *part = group == map_group ? 1 : 2;
+    return group == map_group || group == map_group + 1;
+}
 
 // mb_bins' HEAD group after mb_skip_flag (enc/frame.rs:2046-2244): mb_type, the prediction modes,
 // sub_mb_type, ref_idx, mvd, coded_block_pattern, transform_size_8x8_flag and mb_qp_delta.
@@ -528,35 +544,37 @@ __device__ __forceinline__ void mb_bins(S& c, const Slice& sl, const ironav_mbco
     if (!cbp && kind != KIND_I16) return;
     // an unavailable neighbour counts as a coded block for an intra macroblock
     const int un = kind != KIND_INTER;
-    if (kind == KIND_I16 && (group == ALL || group == DC16))
-        block(c, 0, 85 + (la ? (L.cbf_dc & 1) != 0 : un) + 2 * (ta ? (T.cbf_dc & 1) != 0 : un), code->dc, 16);
+    int part;
+    if (kind == KIND_I16 && in_group(group, DC16_MAP, &part))
+        block(c, 0, 85 + (la ? (L.cbf_dc & 1) != 0 : un) + 2 * (ta ? (T.cbf_dc & 1) != 0 : un), code->dc, 16, part);
     const int cat = kind == KIND_I16 ? 1 : 2, base = kind == KIND_I16 ? 89 : 93;
-    if (code->res.t8x8 && (group == ALL || group == LUMA)) {
+    const bool luma = in_group(group, LUMA_MAP, &part);
+    if (code->res.t8x8 && luma) {
         for (int i8 = 0; i8 < 4; i8++)
-            if (cbpl & (1 << i8)) block(c, 5, -1, code->res.luma8[i8], 64);
-    } else if (group == ALL || group == LUMA) {
+            if (cbpl & (1 << i8)) block(c, 5, -1, code->res.luma8[i8], 64, part);
+    } else if (luma) {
         for (int n = 0; n < 16; n++) {
             if (!(cbpl & (1 << (n >> 2)))) continue;
             const int bx = ((n >> 2) & 1) * 2 + (n & 1), by = ((n >> 3) & 1) * 2 + ((n >> 1) & 1);
             const int fa = bx > 0 ? code->res.nnz[by * 4 + bx - 1] > 0 : (la ? L.nnz[by * 4 + 3] > 0 : un);
             const int fb = by > 0 ? code->res.nnz[(by - 1) * 4 + bx] > 0 : (ta ? T.nnz[12 + bx] > 0 : un);
             const int16_t* blk = code->res.luma[by * 4 + bx];
-            block(c, cat, base + fa + 2 * fb, cat == 1 ? blk + 1 : blk, cat == 1 ? 15 : 16);
+            block(c, cat, base + fa + 2 * fb, cat == 1 ? blk + 1 : blk, cat == 1 ? 15 : 16, part);
         }
     }
-    if (cbpc > 0 && (group == ALL || group == CDC))
+    if (cbpc > 0 && in_group(group, CDC_MAP, &part))
         for (int comp = 0; comp < 2; comp++) {
             const int m = 2 << comp;
-            block(c, 3, 97 + (la ? (L.cbf_dc & m) != 0 : un) + 2 * (ta ? (T.cbf_dc & m) != 0 : un), code->res.cdc[comp], 4);
+            block(c, 3, 97 + (la ? (L.cbf_dc & m) != 0 : un) + 2 * (ta ? (T.cbf_dc & m) != 0 : un), code->res.cdc[comp], 4, part);
         }
-    if (cbpc == 2 && (group == ALL || group == CAC))
+    if (cbpc == 2 && in_group(group, CAC_MAP, &part))
         for (int comp = 0; comp < 2; comp++)
             for (int blk = 0; blk < 4; blk++) {
                 const int bx = blk & 1, by = blk >> 1;
                 const uint8_t* cur = code->res.cnnz[comp];
                 const int fa = bx > 0 ? cur[by * 2] > 0 : (la ? L.cnnz[comp][by * 2 + 1] > 0 : un);
                 const int fb = by > 0 ? cur[bx] > 0 : (ta ? T.cnnz[comp][2 + bx] > 0 : un);
-                block(c, 4, 101 + fa + 2 * fb, code->res.cac[comp][blk] + 1, 15);
+                block(c, 4, 101 + fa + 2 * fb, code->res.cac[comp][blk] + 1, 15, part);
             }
 }
 

@@ -8,10 +8,9 @@
 // tries, in its order (P_Skip, best_inter's partitioning with the 4x4 and, with transform8, the 8x8
 // transform, Intra16x16, Intra4x4, Intra8x8, each intra one with its chroma), each into the picture and
 // then into shared memory (code and reconstruction), with its squared error; then the candidates' bins are
-// counted at once, each on its own copy of the contexts (the counter of cabac.cuh), five lanes a candidate
-// (one per group of disjoint contexts); lane 0 keeps the least SSD + lambda2 * bits in the reference's
-// order (strict '<'), and the warp copies the kept candidate's code, reconstruction and advanced contexts
-// into place.
+// counted, each on its own copy of the contexts (the counter of cabac.cuh), a lane per group of disjoint
+// contexts (nine a candidate); lane 0 keeps the least SSD + lambda2 * bits in the reference's order (strict
+// '<'), and the warp copies the kept candidate's code, reconstruction and advanced contexts into place.
 //
 // The candidates reuse decide mode's warp-level coders (decide.cuh, residual.cuh); Intra8x8 (code_i8,
 // enc/frame.rs:1307-1388) is coded here: block by block, its edges filtered (8.3.2.2.1), nine modes'
@@ -385,6 +384,28 @@ __device__ __forceinline__ void rd_chroma_copy(const ironav_mbcode& from, ironav
     __syncwarp();
 }
 
+// Candidates k0 .. k0 + nk - 1 priced on this warp (rd_cost, enc/frame.rs:1453-1457): each from its own copy
+// of the contexts, a lane per (candidate, group of disjoint contexts), the groups' bits summed into R.bits.
+template <class T, int W>
+__device__ void rd_count(RdSmem<T, W>& R, const cab::Slice& sl, const int* nbm, int k0, int nk) {
+    const int lane = threadIdx.x & 31;
+    for (int k = k0; k < k0 + nk; k++) {
+        if (!R.valid[k]) continue;
+        const uint32_t* s32 = reinterpret_cast<const uint32_t*>(R.live);
+        uint32_t* d32 = reinterpret_cast<uint32_t*>(R.cst[k]);
+        for (int i = lane; i < 256; i += 32) d32[i] = s32[i];
+    }
+    if (lane < nk) R.bits[k0 + lane] = 0;
+    __syncwarp();
+    const int k = k0 + lane / cab::NGROUPS, g = lane % cab::NGROUPS;
+    if (lane < nk * cab::NGROUPS && R.valid[k]) {
+        cab::Counter c = {R.cst[k], R.step, 0};
+        cab::mb_bins(c, sl, &R.cand[k], R.nb[0], R.nb[1], nbm, g);
+        if (c.bits) atomicAdd(&R.bits[k], c.bits);
+    }
+    __syncwarp();
+}
+
 // The MbState of a coded candidate: the inter ones' from inter_tail (S.a.out), the intra ones' without motion.
 template <class T, int W>
 __device__ __forceinline__ void rd_state(RdSmem<T, W>& R, const DecideSmem<T>& S, int k, bool inter) {
@@ -577,27 +598,11 @@ __device__ void rd_mb(const RdParams& P, RdSmem<T, 1>& R, const unsigned* i4tab,
         rd_state(R, S, 5, false);
         rd_take(C, R, S, 5, mbx, mby);
     }
-    // rd_cost (1453-1457): each candidate's bins counted from its own copy of the contexts, on five lanes a
-    // candidate, one per group of disjoint contexts (cab::Group), the groups' bits summed; then lane 0 keeps
-    // the least SSD + lam2 * bits in the reference's order (strict '<'), in f64 rounded as the reference's
-    // expression is (no fused multiply-add).
-    for (int k = 0; k < RD_CANDS; k++) {
-        if (!R.valid[k]) continue;
-        const uint32_t* s32 = reinterpret_cast<const uint32_t*>(R.live);
-        uint32_t* d32 = reinterpret_cast<uint32_t*>(R.cst[k]);
-        for (int i = lane; i < 256; i += 32) d32[i] = s32[i];
-    }
-    if (lane < RD_CANDS) R.bits[lane] = 0;
-    __syncwarp();
-    {
-        const int k = lane / cab::NGROUPS, g = lane % cab::NGROUPS;
-        if (k < RD_CANDS && R.valid[k]) {
-            cab::Counter c = {R.cst[k], R.step, 0};
-            cab::mb_bins(c, sl, &cand[k], R.nb[0], R.nb[1], S.nbm, g);
-            if (c.bits) atomicAdd(&R.bits[k], c.bits);
-        }
-    }
-    __syncwarp();
+    // rd_cost (1453-1457): the candidates priced three at a time (nine groups of disjoint contexts each); then
+    // lane 0 keeps the least SSD + lam2 * bits in the reference's order (strict '<'), in f64 rounded as the
+    // reference's expression is (no fused multiply-add).
+    rd_count(R, sl, S.nbm, 0, 3);
+    rd_count(R, sl, S.nbm, 3, 3);
     if (lane == 0) {
         int best = -1;
         double bj = 0.0;
@@ -692,9 +697,9 @@ __global__ void __launch_bounds__(32) decide_rd_batch_kernel(const RdParams* __r
 // Intra16x16 (with the intra chroma), Intra8x8 and then the partitioning with the 8x8 transform (best_inter's
 // decision handed over through named barrier 1, which warp 0 arrives at and warp 2 waits on), warps 1 and
 // 2 each into their own scratch planes (their edges read from the picture, which warp 0 writes only inside
-// the macroblock). Warp 0 then prices every candidate and commits the kept one. The warps meet at three CTA
-// barriers a macroblock (after the P_Skip tests; after the candidates, when there are any; after the
-// commit), every warp at every one.
+// the macroblock). The three warps then price two candidates each, and warp 0 commits the kept one. The
+// warps meet at CTA barriers (after the P_Skip tests; when there are candidates, after them and after the
+// pricing; after the commit), every warp at every one.
 constexpr int RD3_WARPS = 3;
 
 template <class T>
@@ -905,8 +910,9 @@ __device__ void rd_mb3(const RdParams& P, const DecideParams* dw, RdSmem<T, RD3_
         }
     }
     __syncthreads();
-    if (w == 0) {
-        // Intra4x4's chroma: Intra16x16's code, reconstruction and squared error
+    // the candidates priced two a warp (warp 2 first gives Intra4x4 Intra16x16's chroma: code, reconstruction and
+    // squared error), then warp 0 keeps the least cost in order and commits it
+    if (w == 2) {
         rd_chroma_copy(cand[3], &cand[4]);
         if (lane == 0) {
             cand[4].res.cbp |= (uint8_t)R.ccbp;
@@ -914,24 +920,11 @@ __device__ void rd_mb3(const RdParams& P, const DecideParams* dw, RdSmem<T, RD3_
             R.cssd[4] = R.cssd[3];
         }
         for (int i = 256 + lane; i < 384; i += 32) R.crec[4][i] = R.crec[3][i];
-        // the candidates priced at once, five lanes each (as rd_mb), the least cost kept in order
-        for (int k = 0; k < RD_CANDS; k++) {
-            if (!R.valid[k]) continue;
-            const uint32_t* s32 = reinterpret_cast<const uint32_t*>(R.live);
-            uint32_t* d32 = reinterpret_cast<uint32_t*>(R.cst[k]);
-            for (int i = lane; i < 256; i += 32) d32[i] = s32[i];
-        }
-        if (lane < RD_CANDS) R.bits[lane] = 0;
         __syncwarp();
-        {
-            const int k = lane / cab::NGROUPS, g = lane % cab::NGROUPS;
-            if (k < RD_CANDS && R.valid[k]) {
-                cab::Counter c = {R.cst[k], R.step, 0};
-                cab::mb_bins(c, sl, &cand[k], R.nb[0], R.nb[1], S.nbm, g);
-                if (c.bits) atomicAdd(&R.bits[k], c.bits);
-            }
-        }
-        __syncwarp();
+    }
+    rd_count(R, sl, S.nbm, 2 * w, 2);
+    __syncthreads();
+    if (w == 0) {
         if (lane == 0) {
             int best = -1;
             double bj = 0.0;
