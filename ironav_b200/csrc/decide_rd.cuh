@@ -386,8 +386,10 @@ __device__ __forceinline__ void rd_chroma_copy(const ironav_mbcode& from, ironav
 
 // Candidates k0 .. k0 + nk - 1 priced on this warp (rd_cost, enc/frame.rs:1453-1457): each from its own copy
 // of the contexts, a lane per (candidate, group of disjoint contexts), the groups' bits summed into R.bits.
+// coarse: five lanes a candidate, each residual category's map and levels on one lane (six candidates fit
+// the warp at once).
 template <class T, int W>
-__device__ void rd_count(RdSmem<T, W>& R, const cab::Slice& sl, const int* nbm, int k0, int nk) {
+__device__ void rd_count(RdSmem<T, W>& R, const cab::Slice& sl, const int* nbm, int k0, int nk, bool coarse = false) {
     const int lane = threadIdx.x & 31;
     for (int k = k0; k < k0 + nk; k++) {
         if (!R.valid[k]) continue;
@@ -397,10 +399,16 @@ __device__ void rd_count(RdSmem<T, W>& R, const cab::Slice& sl, const int* nbm, 
     }
     if (lane < nk) R.bits[k0 + lane] = 0;
     __syncwarp();
-    const int k = k0 + lane / cab::NGROUPS, g = lane % cab::NGROUPS;
-    if (lane < nk * cab::NGROUPS && R.valid[k]) {
+    const int ng = coarse ? (cab::NGROUPS + 1) / 2 : cab::NGROUPS;
+    const int k = k0 + lane / ng, g = lane % ng;
+    if (lane < nk * ng && R.valid[k]) {
         cab::Counter c = {R.cst[k], R.step, 0};
-        cab::mb_bins(c, sl, &R.cand[k], R.nb[0], R.nb[1], nbm, g);
+        if (!coarse || g == 0) {
+            cab::mb_bins(c, sl, &R.cand[k], R.nb[0], R.nb[1], nbm, g);
+        } else {
+            cab::mb_bins(c, sl, &R.cand[k], R.nb[0], R.nb[1], nbm, 2 * g - 1);
+            cab::mb_bins(c, sl, &R.cand[k], R.nb[0], R.nb[1], nbm, 2 * g);
+        }
         if (c.bits) atomicAdd(&R.bits[k], c.bits);
     }
     __syncwarp();
@@ -598,11 +606,10 @@ __device__ void rd_mb(const RdParams& P, RdSmem<T, 1>& R, const unsigned* i4tab,
         rd_state(R, S, 5, false);
         rd_take(C, R, S, 5, mbx, mby);
     }
-    // rd_cost (1453-1457): the candidates priced three at a time (nine groups of disjoint contexts each); then
-    // lane 0 keeps the least SSD + lam2 * bits in the reference's order (strict '<'), in f64 rounded as the
-    // reference's expression is (no fused multiply-add).
-    rd_count(R, sl, S.nbm, 0, 3);
-    rd_count(R, sl, S.nbm, 3, 3);
+    // rd_cost (1453-1457): the candidates priced at once (five lanes each); then lane 0 keeps the least SSD +
+    // lam2 * bits in the reference's order (strict '<'), in f64 rounded as the reference's expression is (no
+    // fused multiply-add).
+    rd_count(R, sl, S.nbm, 0, RD_CANDS, true);
     if (lane == 0) {
         int best = -1;
         double bj = 0.0;
