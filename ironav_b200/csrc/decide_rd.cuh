@@ -700,8 +700,8 @@ __global__ void __launch_bounds__(32) decide_rd_batch_kernel(const RdParams* __r
 
 // ---- the three-warp form: one chain's macroblock on three warps ----------------------------------------
 // Warp 0 runs code_mb's P_Skip tests; when the macroblock passes them, warp 0 runs best_inter and codes its
-// partitioning with the 4x4 transform into the picture, warp 1 codes P_Skip and then Intra4x4, and warp 2
-// Intra16x16 (with the intra chroma), Intra8x8 and then the partitioning with the 8x8 transform (best_inter's
+// partitioning with the 4x4 transform into the picture, warp 1 codes P_Skip, Intra4x4 and Intra8x8, and warp 2
+// Intra16x16 (with the intra chroma) and then the partitioning with the 8x8 transform (best_inter's
 // decision handed over through named barrier 1, which warp 0 arrives at and warp 2 waits on), warps 1 and
 // 2 each into their own scratch planes (their edges read from the picture, which warp 0 writes only inside
 // the macroblock). The three warps then price two candidates each, and warp 0 commits the kept one. The
@@ -867,6 +867,15 @@ __device__ void rd_mb3(const RdParams& P, const DecideParams* dw, RdSmem<T, RD3_
         }
         rd_state(R, S, 4, false);
         rd_take(Dw.C, R, S, 4, mbx, mby, false);
+        if (P.t8) {
+            // Intra8x8 into warp 1's luma plane (its edges from the picture); its chroma too is Intra16x16's
+            o = &cand[5];
+            code_init(o);
+            const uint32_t cbp8 = code_i8_d(D, S, R, mbx, mby, ta, la, tra, o, reinterpret_cast<T*>(Dw.C.rec[0]), Dw.C.ys);
+            if (lane == 0) o->res.cbp = (uint8_t)cbp8;
+            rd_state(R, S, 5, false);
+            rd_take(Dw.C, R, S, 5, mbx, mby, false);
+        }
     } else if (w == 2) {
         // Intra16x16 in best_i16's mode with the intra chroma, then Intra8x8, into warp 2's planes
         const DecideParams& Dw = dw[1];
@@ -884,16 +893,6 @@ __device__ void rd_mb3(const RdParams& P, const DecideParams* dw, RdSmem<T, RD3_
         }
         rd_state(R, S, 3, false);
         rd_take(Dw.C, R, S, 3, mbx, mby);
-        if (P.t8) {
-            o = &cand[5];
-            code_init(o);
-            uint32_t cbp8 = code_i8_d(D, S, R, mbx, mby, ta, la, tra, o, reinterpret_cast<T*>(Dw.C.rec[0]), Dw.C.ys);
-            rd_chroma_copy(cand[3], o);
-            cbp8 |= ccbp;
-            if (lane == 0) o->res.cbp = (uint8_t)cbp8;
-            rd_state(R, S, 5, false);
-            rd_take(Dw.C, R, S, 5, mbx, mby);  // the chroma in warp 2's planes is Intra16x16's
-        }
         if (P.t8 && !D.intra) {
             // best_inter's partitioning with the 8x8 transform (when no 8x8 block is split; without luma levels it
             // would be the 4x4 candidate again), once warp 0 has handed its decision over
@@ -917,17 +916,19 @@ __device__ void rd_mb3(const RdParams& P, const DecideParams* dw, RdSmem<T, RD3_
         }
     }
     __syncthreads();
-    // the candidates priced two a warp (warp 2 first gives Intra4x4 Intra16x16's chroma: code, reconstruction and
-    // squared error), then warp 0 keeps the least cost in order and commits it
+    // the candidates priced two a warp (warp 2 first gives Intra4x4 and Intra8x8 Intra16x16's chroma: code,
+    // reconstruction and squared error), then warp 0 keeps the least cost in order and commits it
     if (w == 2) {
-        rd_chroma_copy(cand[3], &cand[4]);
-        if (lane == 0) {
-            cand[4].res.cbp |= (uint8_t)R.ccbp;
-            R.ssd[4] += R.cssd[3];
-            R.cssd[4] = R.cssd[3];
+        for (int k = 4; k <= (P.t8 ? 5 : 4); k++) {
+            rd_chroma_copy(cand[3], &cand[k]);
+            if (lane == 0) {
+                cand[k].res.cbp |= (uint8_t)R.ccbp;
+                R.ssd[k] += R.cssd[3];
+                R.cssd[k] = R.cssd[3];
+            }
+            for (int i = 256 + lane; i < 384; i += 32) R.crec[k][i] = R.crec[3][i];
+            __syncwarp();
         }
-        for (int i = 256 + lane; i < 384; i += 32) R.crec[4][i] = R.crec[3][i];
-        __syncwarp();
     }
     rd_count(R, sl, S.nbm, 2 * w, 2);
     __syncthreads();
