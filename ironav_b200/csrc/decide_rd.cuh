@@ -969,16 +969,13 @@ __device__ void rd_mb3(const RdParams& P, const DecideParams* dw, RdSmem<T, RD3_
     __syncthreads();
 }
 
-// Decide mode under CABAC for one stream, three warps a chain: CTA i walks slice band i.
+// The three-warp form's set-up and chain walk for the parameters P (in parameter space or shared memory):
+// warps 1 and 2's parameter copies writing into their scratch planes, the CTA's tables and contexts, then
+// slice band `band` in raster order.
 template <class T>
-__global__ void __launch_bounds__(RD3_WARPS * 32) decide_rd3_kernel(const __grid_constant__ RdParams P) {
-    extern __shared__ __align__(16) unsigned char rd3_smem[];
-    RdSmem<T, RD3_WARPS>& R = *reinterpret_cast<RdSmem<T, RD3_WARPS>*>(rd3_smem);
-    __shared__ DecideParams dw[2];
-    __shared__ unsigned i4tab[9 * 17];
+__device__ void rd3_chain(const RdParams& P, DecideParams* dw, RdSmem<T, RD3_WARPS>& R, unsigned* i4tab, int band) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     if (w > 0) {
-        // this warp's copy of the parameters, its coder writing into its scratch planes
         const uint32_t* src = reinterpret_cast<const uint32_t*>(&P.D);
         uint32_t* dst = reinterpret_cast<uint32_t*>(&dw[w - 1]);
         for (int k = lane; k < (int)(sizeof(DecideParams) / 4); k += 32) dst[k] = src[k];
@@ -990,8 +987,6 @@ __global__ void __launch_bounds__(RD3_WARPS * 32) decide_rd3_kernel(const __grid
         }
     }
     fill_i4tab(i4tab);  // its __syncthreads also publishes dw
-    const int band = blockIdx.x;
-    if (band >= P.nbands) return;
     const AnalyseParams& A = P.D.C.A;
     for (int i = threadIdx.x; i < cab::STEP_ENTRIES; i += blockDim.x) R.step[i] = P.step[i];
     for (int i = threadIdx.x; i < 9 * 64; i += blockDim.x) R.i8tab[i] = i8_entry(i >> 6, i & 7, (i >> 3) & 7);
@@ -999,6 +994,33 @@ __global__ void __launch_bounds__(RD3_WARPS * 32) decide_rd3_kernel(const __grid
     __syncthreads();
     for (int mby = P.band_rows[band]; mby < P.band_rows[band + 1]; mby++)
         for (int mbx = 0; mbx < A.mb_w; mbx++) rd_mb3<T>(P, dw, R, i4tab, mby * A.mb_w + mbx, mbx, mby);
+}
+
+// Decide mode under CABAC for one stream, three warps a chain: CTA i walks slice band i.
+template <class T>
+__global__ void __launch_bounds__(RD3_WARPS * 32) decide_rd3_kernel(const __grid_constant__ RdParams P) {
+    extern __shared__ __align__(16) unsigned char rd3_smem[];
+    __shared__ DecideParams dw[2];
+    __shared__ unsigned i4tab[9 * 17];
+    if ((int)blockIdx.x >= P.nbands) return;
+    rd3_chain<T>(P, dw, *reinterpret_cast<RdSmem<T, RD3_WARPS>*>(rd3_smem), i4tab, blockIdx.x);
+}
+
+// The same for many streams' chains: CTA i walks chains[i] = stream << 16 | band with the stream's
+// parameters from table[stream] (copied into shared memory).
+template <class T>
+__global__ void __launch_bounds__(RD3_WARPS * 32) decide_rd3_batch_kernel(const RdParams* __restrict__ table,
+                                                                          const uint32_t* __restrict__ chains, int nchains) {
+    extern __shared__ __align__(16) unsigned char rd3_smem[];
+    __shared__ RdParams prm;
+    __shared__ DecideParams dw[2];
+    __shared__ unsigned i4tab[9 * 17];
+    if ((int)blockIdx.x >= nchains) return;
+    const uint32_t e = chains[blockIdx.x];
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(&table[e >> 16]);
+    for (int k = threadIdx.x; k < (int)(sizeof(RdParams) / 4); k += blockDim.x) reinterpret_cast<uint32_t*>(&prm)[k] = src[k];
+    __syncthreads();
+    rd3_chain<T>(prm, dw, *reinterpret_cast<RdSmem<T, RD3_WARPS>*>(rd3_smem), i4tab, (int)(e & 0xFFFFu));
 }
 
 template <class T>

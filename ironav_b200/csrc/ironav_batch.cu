@@ -186,7 +186,9 @@ struct ironav_batch {
     RdParams* d_rdtable = nullptr;
     RdParams* h_rdtable = nullptr;
     uint32_t* d_chains = nullptr;
-    int nchains = 0;
+    int nchains = 0, nchains3 = 0;  // the first nchains3 (the longest bands) on three warps each
+    cudaStream_t aux = nullptr;     // the one-warp launch runs beside the three-warp one
+    cudaEvent_t fork = nullptr, join = nullptr;
     // deblocking (allocated on first use): the streams' jobs, their rows' merged ticket order, progress
     // words, and the concatenated slice tables (pinned staging reused once the previous copies are done)
     DbkJob* d_kjobs = nullptr;
@@ -214,6 +216,9 @@ static void free_batch(ironav_batch* b) {
     cudaFree(b->d_rdtable);
     cudaFreeHost(b->h_rdtable);
     cudaFree(b->d_chains);
+    if (b->fork) cudaEventDestroy(b->fork);
+    if (b->join) cudaEventDestroy(b->join);
+    if (b->aux) cudaStreamDestroy(b->aux);
     cudaFree(b->d_kjobs);
     cudaFreeHost(b->h_kjobs);
     cudaFree(b->d_korder);
@@ -535,12 +540,32 @@ static int batch_decide_rd(ironav_batch* b, ironav_mbstate* const* d_states, iro
     if (!b->d_rdtable) {
         CK(cudaMalloc(&b->d_rdtable, sizeof(RdParams) * b->n));
         CK(cudaHostAlloc(&b->h_rdtable, sizeof(RdParams) * b->n, cudaHostAllocDefault));
+        // the longest bands (at least 3/4 of the longest's macroblocks) first, on three warps each; the rest on one
+        std::vector<std::pair<int, uint32_t>> len;
+        int most = 0;
+        for (int i = 0; i < b->n; i++) {
+            const ironav_ctx* c = b->ctx[i];
+            for (int k = 0; k < c->nslices; k++) {
+                const int mbs = (c->band_rows[k + 1] - c->band_rows[k]) * c->mb_w;
+                len.emplace_back(mbs, (uint32_t)i << 16 | (uint32_t)k);
+                most = std::max(most, mbs);
+            }
+        }
         std::vector<uint32_t> chains;
-        for (int i = 0; i < b->n; i++)
-            for (int k = 0; k < b->ctx[i]->nslices; k++) chains.push_back((uint32_t)i << 16 | (uint32_t)k);
+        for (const auto& e : len)
+            if (4 * e.first >= 3 * most) chains.push_back(e.second);
+        b->nchains3 = (int)chains.size();
+        for (const auto& e : len)
+            if (4 * e.first < 3 * most) chains.push_back(e.second);
         CK(cudaMalloc(&b->d_chains, sizeof(uint32_t) * chains.size()));
         CK(cudaMemcpy(b->d_chains, chains.data(), sizeof(uint32_t) * chains.size(), cudaMemcpyHostToDevice));
         b->nchains = (int)chains.size();
+        CK(cudaStreamCreateWithFlags(&b->aux, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&b->join, cudaEventDisableTiming));
+        CK(cudaFuncSetAttribute(decide_rd3_batch_kernel<uint8_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rd3_smem_bytes<uint8_t>()));
+        CK(cudaFuncSetAttribute(decide_rd3_batch_kernel<uint16_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)rd3_smem_bytes<uint16_t>()));
     }
     if (b->pending) CK(cudaEventSynchronize(b->copied));
     for (int i = 0; i < b->n; i++) {
@@ -558,14 +583,41 @@ static int batch_decide_rd(ironav_batch* b, ironav_mbstate* const* d_states, iro
         p.lam2 = 1.6 * std::pow(2.0, ((double)c->qpp - 12.0) / 3.0);  // decide_rd's lambda2, enc/frame.rs:1464
         p.nbands = c->nslices;
         p.t8 = c->t8;
+        const size_t B = c->bd > 8 ? 2 : 1, ly = (size_t)c->pw * c->ph * B, cy = (size_t)(c->pw / 2) * (c->ph / 2) * B;
+        for (int k = 0; k < 2; k++) {
+            uint8_t* base = c->d_rd_scr + k * (ly + 2 * cy);
+            p.scr[3 * k] = base;
+            p.scr[3 * k + 1] = base + ly;
+            p.scr[3 * k + 2] = base + ly + cy;
+        }
+        p.scr_ys = c->pw;
+        p.scr_cs = c->pw / 2;
     }
     CK(cudaMemcpyAsync(b->d_rdtable, b->h_rdtable, sizeof(RdParams) * b->n, cudaMemcpyHostToDevice, b->stream));
     CK(cudaEventRecord(b->copied, b->stream));
     b->pending = true;
     CK(cudaMemsetAsync(b->d_counters, 0, sizeof(unsigned) * 2, b->stream));
-    if (b->bd > 8) decide_rd_batch_kernel<uint16_t><<<b->nchains, 32, 0, b->stream>>>(b->d_rdtable, b->d_chains, b->nchains);
-    else decide_rd_batch_kernel<uint8_t><<<b->nchains, 32, 0, b->stream>>>(b->d_rdtable, b->d_chains, b->nchains);
-    return cuda_status(cudaGetLastError());
+    // the short bands' one-warp launch on the side stream, beside the long bands' three-warp launch
+    const int n1 = b->nchains - b->nchains3;
+    if (n1 > 0) {
+        CK(cudaEventRecord(b->fork, b->stream));
+        CK(cudaStreamWaitEvent(b->aux, b->fork, 0));
+        if (b->bd > 8) decide_rd_batch_kernel<uint16_t><<<n1, 32, 0, b->aux>>>(b->d_rdtable, b->d_chains + b->nchains3, n1);
+        else decide_rd_batch_kernel<uint8_t><<<n1, 32, 0, b->aux>>>(b->d_rdtable, b->d_chains + b->nchains3, n1);
+        CK(cudaGetLastError());
+    }
+    if (b->bd > 8)
+        decide_rd3_batch_kernel<uint16_t><<<b->nchains3, RD3_WARPS * 32, rd3_smem_bytes<uint16_t>(), b->stream>>>(b->d_rdtable, b->d_chains,
+                                                                                                              b->nchains3);
+    else
+        decide_rd3_batch_kernel<uint8_t><<<b->nchains3, RD3_WARPS * 32, rd3_smem_bytes<uint8_t>(), b->stream>>>(b->d_rdtable, b->d_chains,
+                                                                                                            b->nchains3);
+    CK(cudaGetLastError());
+    if (n1 > 0) {
+        CK(cudaEventRecord(b->join, b->aux));
+        CK(cudaStreamWaitEvent(b->stream, b->join, 0));
+    }
+    return IRONAV_OK;
 }
 
 extern "C" int ironav_batch_decide(ironav_batch* b, ironav_mbstate* const* d_states, ironav_mbcode* const* d_codes, void* const* d_y,
