@@ -503,7 +503,10 @@ int ironav_batch_sync(ironav_batch* batch);
 /* Decide mode for the current P picture of every stream in one persistent launch (the streams' wavefronts
  * merged as in ironav_batch_step): each context prepared as for ironav_decide_p_picture_device (source,
  * chroma, references with chroma, picture parameters); arrays of n device pointers and strides, stream
- * i's outputs as that call's. Asynchronous; ironav_batch_sync waits. */
+ * i's outputs as that call's. Under CABAC (every context of the batch with the same ironav_set_entropy
+ * setting, else IRONAV_INVALID_ARGUMENT) every stream's slice bands are chains of the rate-distortion
+ * decision, the longest on three warps each and the rest on one, in two launches side by side.
+ * Asynchronous; ironav_batch_sync waits. */
 int ironav_batch_decide(ironav_batch* batch, ironav_mbstate* const* d_states, ironav_mbcode* const* d_codes, void* const* d_rec_y,
                         const int* y_strides, void* const* d_rec_cb, void* const* d_rec_cr, const int* c_strides);
 /* The deblocking filter of every stream's reconstructed picture, two launches in all (the streams' edge
